@@ -1,0 +1,123 @@
+"""ctypes binding of libcathode_b200.so (the C ABI of include/cathode_b200.h).
+
+The binding is the only path from Python to the product: every call goes
+through the shared library's extern "C" entry points.  There is no CPU
+fallback; loading fails loudly when the library is missing or was built
+without CUDA.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcathode_b200.so")
+
+CTH_OK = 0
+CTH_NOT_CONVERGED = 1
+CTH_NONFINITE = 2
+CTH_ERR_ARG = -1
+CTH_ERR_CUDA = -2
+CTH_ERR_ALLOC = -3
+CTH_ERR_UNSUPPORTED = -4
+
+CTH_PREC_FP64 = 0
+CTH_PREC_MIXED = 1
+
+# every symbol include/cathode_b200.h declares
+EXPORTS = (
+    "cth_version", "cth_last_error", "cth_grid_create", "cth_grid_destroy", "cth_grid_ld",
+    "cth_grid_levels", "cth_grid_set_cycle", "cth_smg_solve", "cth_smg_solve_dev", "cth_sor_solve",
+    "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
+    "cth_launch_count", "cth_profile", "cth_profile_read",
+)
+
+CTH_PROF_RELAX0 = 0
+CTH_PROF_UPDATE = 1
+CTH_PROF_RESTRICT0 = 2
+CTH_PROF_SETUP = 3
+
+
+class Status(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int),
+        ("converged", ctypes.c_int),
+        ("nonfinite", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+        ("residual", ctypes.c_double),
+        ("initial_residual", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class CathodeError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cathode_b200 error {code}: {msg}")
+        self.code = code
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+_LIB = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the library (raises if it is absent: there is no fallback)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with build.py (nvcc, sm_100a)")
+    L = ctypes.CDLL(path)
+    L.cth_version.restype = ctypes.c_char_p
+    L.cth_last_error.restype = ctypes.c_char_p
+    L.cth_grid_create.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(_vp)]
+    L.cth_grid_create.restype = ctypes.c_int
+    L.cth_grid_destroy.argtypes = [_vp]
+    L.cth_grid_destroy.restype = None
+    L.cth_grid_ld.argtypes = [_vp]
+    L.cth_grid_ld.restype = ctypes.c_int
+    L.cth_grid_levels.argtypes = [_vp]
+    L.cth_grid_levels.restype = ctypes.c_int
+    L.cth_grid_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+    L.cth_grid_set_cycle.restype = ctypes.c_int
+    L.cth_smg_solve.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp,
+                                                    ctypes.POINTER(Status)]
+    L.cth_smg_solve.restype = ctypes.c_int
+    L.cth_smg_solve_dev.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                        _vp, _vp, ctypes.POINTER(Status)]
+    L.cth_smg_solve_dev.restype = ctypes.c_int
+    L.cth_sor_solve.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_double, ctypes.c_int, ctypes.c_double, _vp,
+                                                    ctypes.POINTER(Status)]
+    L.cth_sor_solve.restype = ctypes.c_int
+    L.cth_sor_solve_dev.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                                        _vp, _vp, ctypes.POINTER(Status)]
+    L.cth_sor_solve_dev.restype = ctypes.c_int
+    L.cth_residual_dev.argtypes = [_vp] + [_vp] * 7 + [_vp, _dp, _dp, _vp]
+    L.cth_residual_dev.restype = ctypes.c_int
+    L.cth_to_device_layout.argtypes = [_vp, _vp, _vp, _vp]
+    L.cth_to_device_layout.restype = ctypes.c_int
+    L.cth_from_device_layout.argtypes = [_vp, _vp, _vp, _vp]
+    L.cth_from_device_layout.restype = ctypes.c_int
+    L.cth_launch_count.argtypes = [_vp]
+    L.cth_launch_count.restype = ctypes.c_longlong
+    L.cth_profile.argtypes = [_vp, ctypes.c_int]
+    L.cth_profile.restype = ctypes.c_int
+    L.cth_profile_read.argtypes = [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong), _dp]
+    L.cth_profile_read.restype = ctypes.c_int
+    _LIB = L
+    return L
+
+
+def last_error() -> str:
+    return load().cth_last_error().decode()
+
+
+def check(rc: int, allow_positive: bool = True) -> int:
+    if rc < 0 or (rc > 0 and not allow_positive):
+        raise CathodeError(rc, last_error())
+    return rc

@@ -1,0 +1,418 @@
+// capi.cu — extern "C" entry points of libcathode_b200.so (include/cathode_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "grid.h"
+
+namespace cth {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+
+int cuda_fail(cudaError_t e, const char* what) {
+    g_err = std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) +
+            ") at " + what;
+    return CTH_ERR_CUDA;
+}
+
+int configure_kernels(cth_grid* g);
+
+// [i][j] (i outer, row length nj+2) -> device layout (j outer, ld): 32x32 tiles
+__global__ void k_ij_to_dev(const double* __restrict__ src, double* __restrict__ dst, int ni2,
+                            int nj2, int ld) {
+    __shared__ double tile[32][33];
+    const int j0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int i = i0 + k, j = j0 + threadIdx.x;
+        if (i < ni2 && j < nj2) tile[k][threadIdx.x] = src[(size_t)i * nj2 + j];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int j = j0 + k, i = i0 + threadIdx.x;
+        if (i < ni2 && j < nj2) dst[(size_t)j * ld + i] = tile[threadIdx.x][k];
+    }
+}
+
+__global__ void k_dev_to_ij(const double* __restrict__ src, double* __restrict__ dst, int ni2,
+                            int nj2, int ld) {
+    __shared__ double tile[32][33];
+    const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int j = j0 + k, i = i0 + threadIdx.x;
+        if (i < ni2 && j < nj2) tile[k][threadIdx.x] = src[(size_t)j * ld + i];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int i = i0 + k, j = j0 + threadIdx.x;
+        if (i < ni2 && j < nj2) dst[(size_t)i * nj2 + j] = tile[threadIdx.x][k];
+    }
+}
+
+int to_device_layout(cth_grid* g, const double* src, double* dst, cudaStream_t s) {
+    dim3 blk(32, 8), grd((g->nj + 2 + 31) / 32, (g->ni + 2 + 31) / 32);
+    k_ij_to_dev<<<grd, blk, 0, s>>>(src, dst, g->ni + 2, g->nj + 2, g->ld);
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+int from_device_layout(cth_grid* g, const double* src, double* dst, cudaStream_t s) {
+    dim3 blk(32, 8), grd((g->ni + 2 + 31) / 32, (g->nj + 2 + 31) / 32);
+    k_dev_to_ij<<<grd, blk, 0, s>>>(src, dst, g->ni + 2, g->nj + 2, g->ld);
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+int prof_mark(cth_grid* g, int c, double bytes, cudaStream_t s) {
+    Profiler& p = g->prof;
+    if (!p.on) return -1;
+    if (p.used * 2 + 2 > p.ev.size()) {
+        for (int k = 0; k < 64; k++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return -1;
+            p.ev.push_back(e);
+        }
+        p.cls.resize(p.ev.size() / 2);
+        p.bytes.resize(p.ev.size() / 2);
+    }
+    const size_t k = p.used++;
+    p.cls[k] = c;
+    p.bytes[k] = bytes;
+    cudaEventRecord(p.ev[2 * k], s);
+    return (int)k;
+}
+
+void prof_done(cth_grid* g, int slot, cudaStream_t s) {
+    if (slot < 0) return;
+    cudaEventRecord(g->prof.ev[2 * slot + 1], s);
+}
+
+void prof_collect(cth_grid* g) {
+    Profiler& p = g->prof;
+    for (size_t k = 0; k < p.used; k++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.ev[2 * k], p.ev[2 * k + 1]) == cudaSuccess) {
+            p.ms[p.cls[k]] += ms;
+            p.n[p.cls[k]] += 1;
+            p.nbytes[p.cls[k]] += p.bytes[k];
+        }
+    }
+    p.used = 0;
+}
+
+int ensure_staging(cth_grid* g) {
+    Workspace& w = g->ws;
+    if (w.stage) return CTH_OK;
+    CTH_CUDA(cudaSetDevice(g->device));
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    CTH_CUDA(cudaMalloc(&w.stage, 7 * g->plane * sizeof(double)));
+    CTH_CUDA(cudaMemset(w.stage, 0, 7 * g->plane * sizeof(double)));
+    CTH_CUDA(cudaMalloc(&w.stage_ij, nij * sizeof(double)));
+    return CTH_OK;
+}
+
+static void free_grid(cth_grid* g) {
+    if (!g) return;
+    cudaSetDevice(g->device);
+    auto fr = [](void* p) { if (p) cudaFree(p); };
+    fr(g->mask_full);
+    for (auto p : g->mask) fr(p);
+    for (auto* v : {&g->h32.a, &g->h32.x, &g->h32.b, &g->h32.wS, &g->h32.wN})
+        for (auto p : *v) fr(p);
+    for (auto* v : {&g->h64.a, &g->h64.x, &g->h64.b, &g->h64.wS, &g->h64.wN})
+        for (auto p : *v) fr(p);
+    fr(g->ws.x64[0]);
+    fr(g->ws.x64[1]);
+    fr(g->ws.part);
+    fr(g->ws.stat);
+    fr(g->ws.stage);
+    fr(g->ws.stage_ij);
+    if (g->ws.h_stat) cudaFreeHost(g->ws.h_stat);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    for (auto e : g->prof.ev) cudaEventDestroy(e);
+    delete g;
+}
+
+}  // namespace cth
+
+using namespace cth;
+
+static const char kVersion[] = "cathode_b200 0.1 (sm_100a)";
+
+// host mask of the reference's [i][j] layout (solverFuncs.hpp:43-47)
+static std::vector<unsigned char> host_mask(int ni, int nj, const std::vector<int>& ibl,
+                                            const std::vector<int>& jbl) {
+    std::vector<unsigned char> m((size_t)(ni + 2) * (nj + 2), 0);
+    const int nb = (int)ibl.size() / 2;
+    for (int b = 0; b < nb; b++)
+        for (int i = std::max(0, ibl[2 * b]); i <= std::min(ni + 1, ibl[2 * b + 1]); i++)
+            for (int j = std::max(0, jbl[2 * b]); j <= std::min(nj + 1, jbl[2 * b + 1]); j++)
+                m[(size_t)i * (nj + 2) + j] = 1;
+    return m;
+}
+
+extern "C" {
+
+const char* cth_version(void) { return kVersion; }
+const char* cth_last_error(void) { return g_err.c_str(); }
+
+int cth_grid_create(int ni, int nj, const int* i_bl, const int* j_bl, int n_bl, int device,
+                    cth_grid** out) {
+    if (!out || ni < 1 || nj < 1 || n_bl < 1 || !i_bl || !j_bl) {
+        set_error("cth_grid_create: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    *out = nullptr;
+    cth_grid* g = new cth_grid();
+    g->ni = ni;
+    g->nj = nj;
+    g->n_bl = n_bl;
+    g->ibl.assign(i_bl, i_bl + 2 * n_bl);
+    g->jbl.assign(j_bl, j_bl + 2 * n_bl);
+    g->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { free_grid(g); return cuda_fail(e, "cudaSetDevice"); }
+    g->ld = ((ni + 2 + 31) / 32) * 32;
+    g->plane = (size_t)(nj + 2) * g->ld;
+    std::vector<unsigned char> hm = host_mask(ni, nj, g->ibl, g->jbl);
+    // bounding box
+    g->i0 = ni + 2; g->i1 = -1; g->j0 = nj + 2; g->j1 = -1;
+    for (int i = 0; i <= ni + 1; i++)
+        for (int j = 0; j <= nj + 1; j++)
+            if (hm[(size_t)i * (nj + 2) + j]) {
+                g->i0 = std::min(g->i0, i); g->i1 = std::max(g->i1, i);
+                g->j0 = std::min(g->j0, j); g->j1 = std::max(g->j1, j);
+            }
+    if (g->i1 < 0) {
+        set_error("cth_grid_create: the block union is empty");
+        free_grid(g);
+        return CTH_ERR_ARG;
+    }
+    g->ncol = g->i1 - g->i0 + 1;
+    g->ldl = ((g->ncol + 31) / 32) * 32;
+    if (g->ncol > 4096) {
+        set_error("cth_grid_create: z-lines longer than 4096 cells are not supported");
+        free_grid(g);
+        return CTH_ERR_UNSUPPORTED;
+    }
+    g->bd = std::min(1024, ((g->ncol + 31) / 32) * 32);
+    g->ept = (g->ncol + g->bd - 1) / g->bd;
+    if (g->ept == 3) g->ept = 4;
+    // levels
+    for (int r = g->j1 - g->j0 + 1;; r = (r + 1) / 2) {
+        g->nrow.push_back(r);
+        if (r == 1) break;
+    }
+    g->nlev = (int)g->nrow.size();
+    // masks: device layout + per-level layout
+    std::vector<unsigned char> mfull(g->plane, 0);
+    for (int i = 0; i <= ni + 1; i++)
+        for (int j = 0; j <= nj + 1; j++) mfull[(size_t)j * g->ld + i] = hm[(size_t)i * (nj + 2) + j];
+    std::vector<std::vector<unsigned char>> ml(g->nlev);
+    ml[0].assign((size_t)g->nrow[0] * g->ldl, 0);
+    for (int r = 0; r < g->nrow[0]; r++)
+        for (int c = 0; c < g->ncol; c++)
+            ml[0][(size_t)r * g->ldl + c] = hm[(size_t)(c + g->i0) * (nj + 2) + (r + g->j0)];
+    for (int l = 1; l < g->nlev; l++) {
+        ml[l].assign((size_t)g->nrow[l] * g->ldl, 0);
+        for (int r = 0; r < g->nrow[l]; r++)
+            for (int c = 0; c < g->ncol; c++)
+                ml[l][(size_t)r * g->ldl + c] = ml[l - 1][(size_t)(2 * r) * g->ldl + c];
+    }
+    int rc = CTH_OK;
+    auto chk = [&](cudaError_t ce, const char* w) {
+        if (ce != cudaSuccess && rc == CTH_OK) rc = cuda_fail(ce, w);
+    };
+    chk(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    chk(cudaMalloc(&g->mask_full, g->plane), "cudaMalloc mask");
+    if (rc == CTH_OK) chk(cudaMemcpy(g->mask_full, mfull.data(), g->plane, cudaMemcpyHostToDevice), "memcpy mask");
+    g->mask.assign(g->nlev, nullptr);
+    for (int l = 0; l < g->nlev && rc == CTH_OK; l++) {
+        chk(cudaMalloc(&g->mask[l], ml[l].size()), "cudaMalloc level mask");
+        if (rc == CTH_OK) chk(cudaMemcpy(g->mask[l], ml[l].data(), ml[l].size(), cudaMemcpyHostToDevice), "memcpy level mask");
+    }
+    const size_t n0 = (size_t)g->nrow[0] * g->ldl;
+    if (rc == CTH_OK) chk(cudaMalloc(&g->ws.x64[0], n0 * sizeof(double)), "cudaMalloc x64");
+    if (rc == CTH_OK) chk(cudaMalloc(&g->ws.x64[1], n0 * sizeof(double)), "cudaMalloc x64");
+    // partial-sum blocks: enough for 256-wide blocks over the full padded index space, twice
+    g->ws.npart = 2 * (((ni + 2 + 255) / 256) * (nj + 2) + 64);
+    if (rc == CTH_OK) chk(cudaMalloc(&g->ws.part, (size_t)g->ws.npart * sizeof(double)), "cudaMalloc part");
+    if (rc == CTH_OK) chk(cudaMalloc(&g->ws.stat, 32 * sizeof(double)), "cudaMalloc stat");
+    if (rc == CTH_OK) chk(cudaMemset(g->ws.stat, 0, 32 * sizeof(double)), "memset stat");
+    if (rc == CTH_OK) chk(cudaMallocHost(&g->ws.h_stat, 32 * sizeof(double)), "cudaMallocHost");
+    if (rc == CTH_OK) rc = configure_kernels(g);
+    if (rc != CTH_OK) {
+        free_grid(g);
+        return rc;
+    }
+    *out = g;
+    return CTH_OK;
+}
+
+void cth_grid_destroy(cth_grid* g) { free_grid(g); }
+
+int cth_grid_ld(const cth_grid* g) { return g ? g->ld : 0; }
+int cth_grid_levels(const cth_grid* g) { return g ? g->nlev : 0; }
+
+long long cth_launch_count(const cth_grid* g) { return g ? g->launches : -1; }
+
+int cth_profile(cth_grid* g, int enable) {
+    if (!g) { set_error("cth_profile: null grid"); return CTH_ERR_ARG; }
+    Profiler& p = g->prof;
+    p.on = enable != 0;
+    p.used = 0;
+    for (int c = 0; c < PROF_NCLASS; c++) { p.ms[c] = 0; p.n[c] = 0; p.nbytes[c] = 0; }
+    return CTH_OK;
+}
+
+int cth_profile_read(const cth_grid* g, int cls, double* ms, long long* launches, double* bytes) {
+    if (!g || cls < 0 || cls >= PROF_NCLASS) { set_error("cth_profile_read: invalid arguments"); return CTH_ERR_ARG; }
+    if (ms) *ms = g->prof.ms[cls];
+    if (launches) *launches = g->prof.n[cls];
+    if (bytes) *bytes = g->prof.nbytes[cls];
+    return CTH_OK;
+}
+
+int cth_grid_set_cycle(cth_grid* g, int nu_pre, int nu_post) {
+    if (!g || nu_pre < 1 || nu_post < 1 || nu_pre > 8 || nu_post > 8) {
+        set_error("cth_grid_set_cycle: sweeps must be in 1..8");
+        return CTH_ERR_ARG;
+    }
+    g->nu1 = nu_pre;
+    g->nu2 = nu_post;
+    return CTH_OK;
+}
+
+static int upload_inputs(cth_grid* g, const double* const* src, int n, double* base) {
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    for (int k = 0; k < n; k++) {
+        CTH_CUDA(cudaMemcpyAsync(g->ws.stage_ij, src[k], nij * sizeof(double), cudaMemcpyHostToDevice,
+                                 g->stream));
+        int rc = to_device_layout(g, g->ws.stage_ij, base + k * g->plane, g->stream);
+        if (rc != CTH_OK) return rc;
+    }
+    return CTH_OK;
+}
+
+// copy the grid cells of a device-layout plane into the caller's [i][j] array
+static int download_grid_cells(cth_grid* g, const double* dev_plane, double* host_ij) {
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    int rc = from_device_layout(g, dev_plane, g->ws.stage_ij, g->stream);
+    if (rc != CTH_OK) return rc;
+    std::vector<double> tmp(nij);
+    CTH_CUDA(cudaMemcpyAsync(tmp.data(), g->ws.stage_ij, nij * sizeof(double), cudaMemcpyDeviceToHost,
+                             g->stream));
+    CTH_CUDA(cudaStreamSynchronize(g->stream));
+    // write back block cells only (solverFuncs.hpp:143-152)
+    const int nb = g->n_bl, nj2 = g->nj + 2;
+    for (int b = 0; b < nb; b++)
+        for (int i = std::max(0, g->ibl[2 * b]); i <= std::min(g->ni + 1, g->ibl[2 * b + 1]); i++)
+            for (int j = std::max(0, g->jbl[2 * b]); j <= std::min(g->nj + 1, g->jbl[2 * b + 1]); j++)
+                host_ij[(size_t)i * nj2 + j] = tmp[(size_t)i * nj2 + j];
+    return CTH_OK;
+}
+
+int cth_smg_solve(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                  const double* aN, const double* aS, const double* b, int maxITR,
+                  double error_cnv, int precision, double* solution, cth_status* st) {
+    if (!g || !aP || !aE || !aW || !aN || !aS || !b || !solution || maxITR < 0) {
+        set_error("cth_smg_solve: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    int rc = ensure_staging(g);
+    if (rc != CTH_OK) return rc;
+    const double* src[6] = {aP, aE, aW, aN, aS, b};
+    double* base = g->ws.stage;
+    rc = upload_inputs(g, src, 6, base);
+    if (rc != CTH_OK) return rc;
+    double* xdev = base + 6 * g->plane;
+    const double* P_ = base;
+    int res = smg_solve_dev(g, P_, P_ + g->plane, P_ + 2 * g->plane, P_ + 3 * g->plane,
+                            P_ + 4 * g->plane, P_ + 5 * g->plane, maxITR, error_cnv, precision, xdev,
+                            g->stream, st);
+    if (res < 0) return res;
+    rc = download_grid_cells(g, xdev, solution);
+    if (rc != CTH_OK) return rc;
+    return res;
+}
+
+int cth_smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                      const double* aN, const double* aS, const double* b, int maxITR,
+                      double error_cnv, int precision, double* solution, void* stream,
+                      cth_status* st) {
+    if (!g || !aP || !aE || !aW || !aN || !aS || !b || !solution || maxITR < 0) {
+        set_error("cth_smg_solve_dev: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    return smg_solve_dev(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, precision, solution,
+                         (cudaStream_t)stream, st);
+}
+
+int cth_sor_solve(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                  const double* aN, const double* aS, const double* b, double alpha_SOR,
+                  int maxITR, double error_cnv, double* solution, cth_status* st) {
+    if (!g || !aP || !aE || !aW || !aN || !aS || !b || !solution) {
+        set_error("cth_sor_solve: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    int rc = ensure_staging(g);
+    if (rc != CTH_OK) return rc;
+    const double* src[7] = {aP, aE, aW, aN, aS, b, solution};
+    double* base = g->ws.stage;
+    rc = upload_inputs(g, src, 7, base);
+    if (rc != CTH_OK) return rc;
+    double* xdev = base + 6 * g->plane;
+    const double* P_ = base;
+    int res = sor_solve_dev(g, P_, P_ + g->plane, P_ + 2 * g->plane, P_ + 3 * g->plane,
+                            P_ + 4 * g->plane, P_ + 5 * g->plane, alpha_SOR, maxITR, error_cnv, xdev,
+                            g->stream, st);
+    if (res < 0) return res;
+    rc = download_grid_cells(g, xdev, solution);
+    if (rc != CTH_OK) return rc;
+    return res;
+}
+
+int cth_sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                      const double* aN, const double* aS, const double* b, double alpha_SOR,
+                      int maxITR, double error_cnv, double* solution, void* stream,
+                      cth_status* st) {
+    if (!g || !aP || !aE || !aW || !aN || !aS || !b || !solution) {
+        set_error("cth_sor_solve_dev: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    return sor_solve_dev(g, aP, aE, aW, aN, aS, b, alpha_SOR, maxITR, error_cnv, solution,
+                         (cudaStream_t)stream, st);
+}
+
+int cth_residual_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                     const double* aN, const double* aS, const double* b, const double* x,
+                     double* r, double* rnorm, double* bnorm, void* stream) {
+    if (!g || !aP || !aE || !aW || !aN || !aS || !b || !x) {
+        set_error("cth_residual_dev: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    return residual_dev(g, aP, aE, aW, aN, aS, b, x, r, rnorm, bnorm, (cudaStream_t)stream);
+}
+
+int cth_to_device_layout(cth_grid* g, const double* src_ij, double* dst_dev, void* stream) {
+    if (!g || !src_ij || !dst_dev) { set_error("cth_to_device_layout: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(g->device));
+    return to_device_layout(g, src_ij, dst_dev, (cudaStream_t)stream);
+}
+
+int cth_from_device_layout(cth_grid* g, const double* src_dev, double* dst_ij, void* stream) {
+    if (!g || !src_dev || !dst_ij) { set_error("cth_from_device_layout: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(g->device));
+    return from_device_layout(g, src_dev, dst_ij, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,115 @@
+// grid.h — internal state of a cth_grid (not part of the C ABI).
+//
+// HBM layout
+//   * "device layout": ghost-padded (ni+2) x (nj+2) planes, r-major:
+//     element (i,j) at j*ld + i, ld = round_up(ni+2, 32).  z-lines (fixed j)
+//     are contiguous, which is what the z-line smoothers read.
+//   * "level layout": the multigrid levels cover the bounding box of the grid
+//     cells, [i0..i1] x [j0..j1].  Level l has nrow[l] rows (semicoarsened in
+//     r: row J of level l+1 is row 2J of level l) and ncol = i1-i0+1 columns,
+//     element (c, r) at r*ldl + c, ldl = round_up(ncol, 32).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cathode_b200.h"
+
+namespace cth {
+
+// stencil slots: level 0 stores the first 5, coarse levels all 9.
+// Convention of the reference: (A x)_P = a[P] x_P - sum_k a[k] x_k.
+enum Slot { P = 0, W = 1, E = 2, S = 3, N = 4, SW = 5, SE = 6, NW = 7, NE = 8 };
+
+template <typename T>
+struct Hierarchy {
+    bool allocated = false;
+    std::vector<T*> a;   // per level: npt planes of nrow*ldl
+    std::vector<T*> x;   // per level
+    std::vector<T*> b;   // per level
+    std::vector<T*> wS;  // per level (F rows used): weight toward the C row below
+    std::vector<T*> wN;  // per level: weight toward the C row above
+};
+
+// per-kernel-class timing with CUDA events on the launching stream
+enum ProfClass { PROF_RELAX0 = 0, PROF_UPDATE = 1, PROF_RESTRICT0 = 2, PROF_SETUP = 3, PROF_NCLASS = 4 };
+
+struct Profiler {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;      // pairs (start, stop)
+    std::vector<int> cls;             // class of each pair
+    std::vector<double> bytes;        // algorithmic bytes of each pair
+    size_t used = 0;
+    double ms[PROF_NCLASS] = {0, 0, 0, 0};
+    long long n[PROF_NCLASS] = {0, 0, 0, 0};
+    double nbytes[PROF_NCLASS] = {0, 0, 0, 0};
+};
+
+struct Workspace {
+    double* x64[2] = {nullptr, nullptr};  // level-0 layout accumulated solution
+    double* part = nullptr;               // per-block partial sums
+    int npart = 0;
+    double* stat = nullptr;               // device status words
+    double* h_stat = nullptr;             // pinned mirror
+    // host-API staging: 6 input planes + solution in device layout, one [i][j] buffer
+    double* stage = nullptr;
+    double* stage_ij = nullptr;
+    double* h_pinned = nullptr;           // pinned [i][j] buffer for transfers
+};
+
+}  // namespace cth
+
+struct cth_grid {
+    int ni = 0, nj = 0, n_bl = 0;
+    std::vector<int> ibl, jbl;
+    int device = 0;
+    int ld = 0;          // device layout leading dimension
+    size_t plane = 0;    // (nj+2)*ld
+    int i0 = 0, i1 = -1, j0 = 0, j1 = -1;
+    int ncol = 0, ldl = 0;
+    int nlev = 0;
+    std::vector<int> nrow;
+    int nu1 = 1, nu2 = 1;
+    int bd = 32, ept = 1;      // line-solve block size / elements per thread
+    unsigned char* mask_full = nullptr;          // device layout
+    std::vector<unsigned char*> mask;            // per level, level layout
+    cth::Hierarchy<float> h32;
+    cth::Hierarchy<double> h64;
+    cth::Workspace ws;
+    cudaStream_t stream = nullptr;
+    long long launches = 0;    // kernels launched by this grid since creation
+    cth::Profiler prof;
+};
+
+namespace cth {
+void set_error(const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+int ensure_hierarchy_f32(cth_grid* g);
+int ensure_hierarchy_f64(cth_grid* g);
+int ensure_staging(cth_grid* g);
+int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                  const double* aN, const double* aS, const double* b, int maxITR,
+                  double error_cnv, int precision, double* solution, cudaStream_t s,
+                  cth_status* st);
+int sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                  const double* aN, const double* aS, const double* b, double alpha,
+                  int maxITR, double error_cnv, double* solution, cudaStream_t s,
+                  cth_status* st);
+int residual_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                 const double* aN, const double* aS, const double* b, const double* x,
+                 double* r, double* rnorm, double* bnorm, cudaStream_t s);
+int to_device_layout(cth_grid* g, const double* src_ij_dev, double* dst, cudaStream_t s);
+// profiling: mark() before a launch of class c, done() after it; collect() after a sync
+int prof_mark(cth_grid* g, int c, double bytes, cudaStream_t s);
+void prof_done(cth_grid* g, int slot, cudaStream_t s);
+void prof_collect(cth_grid* g);
+int from_device_layout(cth_grid* g, const double* src, double* dst_ij_dev, cudaStream_t s);
+}  // namespace cth
+
+#define CTH_CUDA(call)                                        \
+    do {                                                      \
+        cudaError_t _e = (call);                              \
+        if (_e != cudaSuccess) return cth::cuda_fail(_e, #call); \
+    } while (0)

@@ -1,0 +1,714 @@
+// smg.cu — semicoarsening multigrid for the reference's 5-point solves.
+//
+// Replaces HYPRE Struct SMG as called by solver_SMG
+// (include/solverFuncs.hpp:26-163).  Algorithm (Schaffer's semicoarsening MG,
+// the published method behind HYPRE SMG, restated for sm_100a):
+//   * coarsen in r only: row J of level l+1 is row 2J of level l;
+//   * smoother: zebra z-line Gauss-Seidel, each z-line (fixed r row) solved
+//     exactly by parallel cyclic reduction in shared memory, one CTA per line;
+//   * interpolation of the odd (F) rows: the F line's own tridiagonal operator
+//     applied inversely to its lumped coupling toward the C row below / above;
+//   * Galerkin coarse operators R A P with R = P^T (9-point on coarse levels);
+//   * outer loop = defect correction: FP64 residual b - A x on the caller's
+//     FP64 coefficients, V-cycle on the residual in the working precision
+//     (FP32 for CTH_PREC_MIXED, FP64 for CTH_PREC_FP64), x += e.
+// Stopping rule of HYPRE SMG: ||b - A x||_2 / ||b||_2 < tol, at most maxITR
+// cycles, zero initial guess (solverFuncs.hpp:106-126).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+
+#include "grid.h"
+
+namespace cth {
+
+
+// ---------------------------------------------------------------------------
+// block reductions (fixed order -> deterministic)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// sum over the block; result valid in thread 0
+__device__ double block_sum(double v, double* red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (wid == 0) {
+        s = (lane < nw) ? red[lane] : 0.0;
+        s = warp_sum(s);
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// parallel cyclic reduction of one tridiagonal line in shared memory.
+//   lo_i x_{i-1} + dg_i x_i + up_i x_{i+1} = d_i,   i = 0..n-1
+// NR right-hand sides stored as sd[r*n + i].  sr holds 1/dg.  On return the
+// solution is sd[r*n+i] * sr[i].
+// ---------------------------------------------------------------------------
+template <typename T, int EPT, int NR>
+__device__ __forceinline__ void pcr(T* sa, T* sb, T* sc, T* sd, T* sr, int n) {
+    const int t = threadIdx.x, bd = blockDim.x;
+    for (int s = 1; s < n; s <<= 1) {
+        T na[EPT], nb[EPT], nc[EPT], nd[EPT][NR];
+#pragma unroll
+        for (int e = 0; e < EPT; e++) {
+            const int i = t + e * bd;
+            if (i < n) {
+                T ai = sa[i], bi = sb[i], ci = sc[i];
+                T di[NR];
+#pragma unroll
+                for (int r = 0; r < NR; r++) di[r] = sd[r * n + i];
+                T an = T(0), cn = T(0);
+                if (i >= s) {
+                    const int m = i - s;
+                    const T k = -ai * sr[m];
+                    an = k * sa[m];
+                    bi += k * sc[m];
+#pragma unroll
+                    for (int r = 0; r < NR; r++) di[r] += k * sd[r * n + m];
+                }
+                if (i + s < n) {
+                    const int m = i + s;
+                    const T k = -ci * sr[m];
+                    cn = k * sc[m];
+                    bi += k * sa[m];
+#pragma unroll
+                    for (int r = 0; r < NR; r++) di[r] += k * sd[r * n + m];
+                }
+                na[e] = an; nb[e] = bi; nc[e] = cn;
+#pragma unroll
+                for (int r = 0; r < NR; r++) nd[e][r] = di[r];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < EPT; e++) {
+            const int i = t + e * bd;
+            if (i < n) {
+                sa[i] = na[e]; sb[i] = nb[e]; sc[i] = nc[e];
+                sr[i] = T(1) / nb[e];
+#pragma unroll
+                for (int r = 0; r < NR; r++) sd[r * n + i] = nd[e][r];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+struct LevelArgs {
+    const T* a;       // npt planes
+    size_t plane;     // nrow*ld
+    T* x;
+    const T* b;
+    int nrow, ncol, ld;
+};
+
+// ---------------------------------------------------------------------------
+// level-0 preparation: masked copy of the caller's FP64 planes into the level
+// layout in precision T (couplings to non-grid cells dropped, non-grid cells
+// identity), b0 = b (grid cells), partial sums of b^2.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_prep0(const double* __restrict__ aP, const double* __restrict__ aE,
+                        const double* __restrict__ aW, const double* __restrict__ aN,
+                        const double* __restrict__ aS, const double* __restrict__ b,
+                        const unsigned char* __restrict__ mask, int ld_u, int i0, int j0,
+                        int ncol, int nrow, int ldl, T* __restrict__ a0, T* __restrict__ b0,
+                        double* __restrict__ part) {
+    __shared__ double red[32];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    double bb = 0.0;
+    if (c < ncol) {
+        const size_t plane = (size_t)nrow * ldl;
+        const size_t p = (size_t)r * ldl + c;
+        const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
+        T vP = T(1), vW = T(0), vE = T(0), vS = T(0), vN = T(0), vb = T(0);
+        if (mask[p]) {
+            vP = (T)aP[q];
+            if (c > 0 && mask[p - 1]) vW = (T)aW[q];
+            if (c + 1 < ncol && mask[p + 1]) vE = (T)aE[q];
+            if (r > 0 && mask[p - ldl]) vS = (T)aS[q];
+            if (r + 1 < nrow && mask[p + ldl]) vN = (T)aN[q];
+            const double bv = b[q];
+            vb = (T)bv;
+            bb = bv * bv;
+        }
+        a0[P * plane + p] = vP;
+        a0[W * plane + p] = vW;
+        a0[E * plane + p] = vE;
+        a0[S * plane + p] = vS;
+        a0[N * plane + p] = vN;
+        b0[p] = vb;
+    }
+    const double s = block_sum(bb, red);
+    if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+// ---------------------------------------------------------------------------
+// interpolation weights of the F rows (odd rows) of one level: two line solves
+// per F row, right-hand sides = lumped couplings toward the C rows.
+// ---------------------------------------------------------------------------
+template <typename T, int NPT, int EPT>
+__global__ void k_weights(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ wS,
+                          T* __restrict__ wN) {
+    const int j = 2 * blockIdx.x + 1;
+    if (j >= L.nrow) return;
+    extern __shared__ unsigned char smem_raw[];
+    const int n = L.ncol;
+    T* sa = reinterpret_cast<T*>(smem_raw);
+    T* sb = sa + n;
+    T* sc = sb + n;
+    T* sr = sc + n;
+    T* sd = sr + n;  // 2 rhs
+    const T* a = L.a;
+    const size_t pl = L.plane;
+#pragma unroll
+    for (int e = 0; e < EPT; e++) {
+        const int i = threadIdx.x + e * blockDim.x;
+        if (i < n) {
+            const size_t p = (size_t)j * L.ld + i;
+            const T dg = a[P * pl + p];
+            T rs = T(0), rn = T(0);
+            if (mask[p]) {
+                if (mask[p - L.ld]) {
+                    rs = a[S * pl + p];
+                    if (NPT == 9) rs += a[SW * pl + p] + a[SE * pl + p];
+                }
+                if (j + 1 < L.nrow && mask[p + L.ld]) {
+                    rn = a[N * pl + p];
+                    if (NPT == 9) rn += a[NW * pl + p] + a[NE * pl + p];
+                }
+            }
+            sa[i] = (i > 0) ? -a[W * pl + p] : T(0);
+            sc[i] = (i + 1 < n) ? -a[E * pl + p] : T(0);
+            sb[i] = dg;
+            sr[i] = T(1) / dg;
+            sd[i] = rs;
+            sd[n + i] = rn;
+        }
+    }
+    __syncthreads();
+    pcr<T, EPT, 2>(sa, sb, sc, sd, sr, n);
+#pragma unroll
+    for (int e = 0; e < EPT; e++) {
+        const int i = threadIdx.x + e * blockDim.x;
+        if (i < n) {
+            const size_t p = (size_t)j * L.ld + i;
+            wS[p] = sd[i] * sr[i];
+            wN[p] = sd[n + i] * sr[i];
+        }
+    }
+}
+
+// P(g, i -> J): weight of coarse row J in fine row g at column i
+template <typename T>
+__device__ __forceinline__ T pw(const unsigned char* __restrict__ mask, const T* __restrict__ wS,
+                                const T* __restrict__ wN, int g, int i, int J, int ld) {
+    const size_t p = (size_t)g * ld + i;
+    if ((g & 1) == 0) return (g / 2 == J && mask[p]) ? T(1) : T(0);
+    if ((g - 1) / 2 == J) return wS[p];
+    if ((g + 1) / 2 == J) return wN[p];
+    return T(0);
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin coarse operator: one thread per coarse cell.
+// ---------------------------------------------------------------------------
+template <typename T, int NPT>
+__global__ void k_galerkin(LevelArgs<T> F, const unsigned char* __restrict__ maskf,
+                           const T* __restrict__ wS, const T* __restrict__ wN, T* __restrict__ ac,
+                           int nrowc, const unsigned char* __restrict__ maskc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int J = blockIdx.y;
+    if (i >= F.ncol) return;
+    const int ld = F.ld, ncol = F.ncol;
+    const size_t plc = (size_t)nrowc * ld;
+    const size_t q = (size_t)J * ld + i;
+    const int oi[9] = {0, -1, 1, 0, 0, -1, 1, -1, 1};
+    const int oj[9] = {0, 0, 0, -1, 1, -1, -1, 1, 1};
+    T acc[3][3];
+#pragma unroll
+    for (int u = 0; u < 3; u++)
+#pragma unroll
+        for (int v = 0; v < 3; v++) acc[u][v] = T(0);
+    const bool active = maskc[q] != 0;
+    if (active) {
+        const int c = 2 * J;
+        for (int f = c - 1; f <= c + 1; f++) {
+            if (f < 0 || f >= F.nrow) continue;
+            const T rw = pw(maskf, wS, wN, f, i, J, ld);
+            if (rw == T(0)) continue;
+            const size_t pf = (size_t)f * ld + i;
+#pragma unroll
+            for (int k = 0; k < NPT; k++) {
+                const int ii = i + oi[k], g = f + oj[k];
+                if (ii < 0 || ii >= ncol || g < 0 || g >= F.nrow) continue;
+                const T av = F.a[k * F.plane + pf];
+                if (av == T(0)) continue;
+                const T mv = (k == P) ? av : -av;
+#pragma unroll
+                for (int dJ = -1; dJ <= 1; dJ++) {
+                    const int Jp = J + dJ;
+                    if (Jp < 0 || Jp >= nrowc) continue;
+                    const T pv = pw(maskf, wS, wN, g, ii, Jp, ld);
+                    if (pv != T(0)) acc[dJ + 1][oi[k] + 1] += rw * mv * pv;
+                }
+            }
+        }
+    }
+    if (!active || acc[1][1] == T(0)) {
+        ac[P * plc + q] = T(1);
+#pragma unroll
+        for (int k = 1; k < 9; k++) ac[k * plc + q] = T(0);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const T v = acc[oj[k] + 1][oi[k] + 1];
+        ac[k * plc + q] = (k == P) ? v : -v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// zebra z-line relaxation: one CTA per row of the given parity.
+//   zero_guess: the level's x is zero except rows relaxed earlier in this
+//               kernel sequence (first C-row relaxation of a cycle).
+//   prolong:    add the coarse-grid correction to the F-row neighbours on the
+//               fly (first C-row relaxation after the coarse solve).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct ProlongArgs {
+    const T* ec;   // coarse x
+    const T* wS;
+    const T* wN;
+    int nrowc;
+};
+
+template <typename T, int NPT>
+__device__ __forceinline__ T xnb(const LevelArgs<T>& L, const ProlongArgs<T>& pa, bool prolong,
+                                 int ii, int jj) {
+    const size_t p = (size_t)jj * L.ld + ii;
+    T v = L.x[p];
+    if (prolong) {
+        // jj is an F row (odd)
+        v += pa.wS[p] * pa.ec[(size_t)((jj - 1) >> 1) * L.ld + ii];
+        const int Jn = (jj + 1) >> 1;
+        if (Jn < pa.nrowc) v += pa.wN[p] * pa.ec[(size_t)Jn * L.ld + ii];
+    }
+    return v;
+}
+
+template <typename T, int NPT, int EPT>
+__global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong, ProlongArgs<T> pa) {
+    const int j = 2 * blockIdx.x + parity;
+    if (j >= L.nrow) return;
+    extern __shared__ unsigned char smem_raw[];
+    const int n = L.ncol;
+    T* sa = reinterpret_cast<T*>(smem_raw);
+    T* sb = sa + n;
+    T* sc = sb + n;
+    T* sr = sc + n;
+    T* sd = sr + n;
+    const T* a = L.a;
+    const size_t pl = L.plane;
+    const bool pr = prolong != 0;
+#pragma unroll
+    for (int e = 0; e < EPT; e++) {
+        const int i = threadIdx.x + e * blockDim.x;
+        if (i < n) {
+            const size_t p = (size_t)j * L.ld + i;
+            const T dg = a[P * pl + p];
+            T d = L.b[p];
+            if (!zero_guess) {
+                if (j > 0) {
+                    d += a[S * pl + p] * xnb<T, NPT>(L, pa, pr, i, j - 1);
+                    if (NPT == 9) {
+                        if (i > 0) d += a[SW * pl + p] * xnb<T, NPT>(L, pa, pr, i - 1, j - 1);
+                        if (i + 1 < n) d += a[SE * pl + p] * xnb<T, NPT>(L, pa, pr, i + 1, j - 1);
+                    }
+                }
+                if (j + 1 < L.nrow) {
+                    d += a[N * pl + p] * xnb<T, NPT>(L, pa, pr, i, j + 1);
+                    if (NPT == 9) {
+                        if (i > 0) d += a[NW * pl + p] * xnb<T, NPT>(L, pa, pr, i - 1, j + 1);
+                        if (i + 1 < n) d += a[NE * pl + p] * xnb<T, NPT>(L, pa, pr, i + 1, j + 1);
+                    }
+                }
+            }
+            sa[i] = (i > 0) ? -a[W * pl + p] : T(0);
+            sc[i] = (i + 1 < n) ? -a[E * pl + p] : T(0);
+            sb[i] = dg;
+            sr[i] = T(1) / dg;
+            sd[i] = d;
+        }
+    }
+    __syncthreads();
+    pcr<T, EPT, 1>(sa, sb, sc, sd, sr, n);
+#pragma unroll
+    for (int e = 0; e < EPT; e++) {
+        const int i = threadIdx.x + e * blockDim.x;
+        if (i < n) L.x[(size_t)j * L.ld + i] = sd[i] * sr[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// restriction: after the pre-smoother ends with the F rows, the F-row residual
+// vanishes, so R r = residual of the C rows.  One thread per coarse cell.
+// ---------------------------------------------------------------------------
+template <typename T, int NPT>
+__global__ void k_restrict(LevelArgs<T> L, T* __restrict__ bc, int nrowc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int J = blockIdx.y;
+    if (i >= L.ncol || J >= nrowc) return;
+    const int j = 2 * J, n = L.ncol;
+    const size_t p = (size_t)j * L.ld + i;
+    const T* a = L.a;
+    const size_t pl = L.plane;
+    const T* x = L.x;
+    T r = L.b[p] - a[P * pl + p] * x[p];
+    if (i > 0) r += a[W * pl + p] * x[p - 1];
+    if (i + 1 < n) r += a[E * pl + p] * x[p + 1];
+    if (j > 0) {
+        r += a[S * pl + p] * x[p - L.ld];
+        if (NPT == 9) {
+            if (i > 0) r += a[SW * pl + p] * x[p - L.ld - 1];
+            if (i + 1 < n) r += a[SE * pl + p] * x[p - L.ld + 1];
+        }
+    }
+    if (j + 1 < L.nrow) {
+        r += a[N * pl + p] * x[p + L.ld];
+        if (NPT == 9) {
+            if (i > 0) r += a[NW * pl + p] * x[p + L.ld - 1];
+            if (i + 1 < n) r += a[NE * pl + p] * x[p + L.ld + 1];
+        }
+    }
+    bc[(size_t)J * L.ld + i] = r;
+}
+
+// ---------------------------------------------------------------------------
+// defect correction: x64_out = x64_in + e; r = b - A x64_out with the caller's
+// FP64 coefficients; next cycle's right-hand side b0 = r (precision T).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_update(const double* __restrict__ aP, const double* __restrict__ aE,
+                         const double* __restrict__ aW, const double* __restrict__ aN,
+                         const double* __restrict__ aS, const double* __restrict__ b,
+                         const unsigned char* __restrict__ mask, int ld_u, int i0, int j0,
+                         int ncol, int nrow, int ldl, const double* __restrict__ xin,
+                         const T* __restrict__ e, double* __restrict__ xout, T* __restrict__ b0,
+                         double* __restrict__ part) {
+    __shared__ double red[32];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    double rr = 0.0;
+    if (c < ncol) {
+        const size_t p = (size_t)r * ldl + c;
+        const double xc = xin[p] + (double)e[p];
+        double res = 0.0;
+        if (mask[p]) {
+            const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
+            res = b[q] - aP[q] * xc;
+            if (c + 1 < ncol) res += aE[q] * (xin[p + 1] + (double)e[p + 1]);
+            if (c > 0) res += aW[q] * (xin[p - 1] + (double)e[p - 1]);
+            if (r + 1 < nrow) res += aN[q] * (xin[p + ldl] + (double)e[p + ldl]);
+            if (r > 0) res += aS[q] * (xin[p - ldl] + (double)e[p - ldl]);
+        }
+        xout[p] = xc;
+        b0[p] = (T)res;
+        rr = res * res;
+    }
+    const double s = block_sum(rr, red);
+    if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+// stat[0] = sum of partials, stat[1] = sqrt(sum)/sqrt(ref) (ref = stat[2] if
+// use_ref else the sum itself), stat[3] = 1 if non-finite
+__global__ void k_finish(const double* __restrict__ part, int n, double* __restrict__ stat,
+                         int store_ref) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) s += part[k];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) {
+        stat[0] = s;
+        if (store_ref) stat[2] = s;
+        const double ref = stat[2];
+        stat[1] = (ref > 0.0) ? sqrt(s) / sqrt(ref) : 0.0;
+        stat[3] = isfinite(s) ? 0.0 : 1.0;
+    }
+}
+
+// write the accumulated solution into the caller's device-layout array
+__global__ void k_store(const double* __restrict__ x, const unsigned char* __restrict__ mask,
+                        int ncol, int nrow, int ldl, int ld_u, int i0, int j0,
+                        double* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    if (c >= ncol) return;
+    const size_t p = (size_t)r * ldl + c;
+    if (mask[p]) out[(size_t)(r + j0) * ld_u + (c + i0)] = x[p];
+}
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+template <typename T>
+static Hierarchy<T>& hier(cth_grid* g);
+template <>
+Hierarchy<float>& hier<float>(cth_grid* g) { return g->h32; }
+template <>
+Hierarchy<double>& hier<double>(cth_grid* g) { return g->h64; }
+
+template <typename T>
+static int alloc_hierarchy(cth_grid* g) {
+    Hierarchy<T>& h = hier<T>(g);
+    if (h.allocated) return CTH_OK;
+    CTH_CUDA(cudaSetDevice(g->device));
+    h.a.assign(g->nlev, nullptr);
+    h.x.assign(g->nlev, nullptr);
+    h.b.assign(g->nlev, nullptr);
+    h.wS.assign(g->nlev, nullptr);
+    h.wN.assign(g->nlev, nullptr);
+    for (int l = 0; l < g->nlev; l++) {
+        const size_t n = (size_t)g->nrow[l] * g->ldl;
+        const int npt = (l == 0) ? 5 : 9;
+        CTH_CUDA(cudaMalloc(&h.a[l], n * npt * sizeof(T)));
+        CTH_CUDA(cudaMalloc(&h.x[l], n * sizeof(T)));
+        CTH_CUDA(cudaMalloc(&h.b[l], n * sizeof(T)));
+        CTH_CUDA(cudaMalloc(&h.wS[l], n * sizeof(T)));
+        CTH_CUDA(cudaMalloc(&h.wN[l], n * sizeof(T)));
+        CTH_CUDA(cudaMemset(h.a[l], 0, n * npt * sizeof(T)));
+        CTH_CUDA(cudaMemset(h.x[l], 0, n * sizeof(T)));
+        CTH_CUDA(cudaMemset(h.b[l], 0, n * sizeof(T)));
+        CTH_CUDA(cudaMemset(h.wS[l], 0, n * sizeof(T)));
+        CTH_CUDA(cudaMemset(h.wN[l], 0, n * sizeof(T)));
+    }
+    h.allocated = true;
+    return CTH_OK;
+}
+
+int ensure_hierarchy_f32(cth_grid* g) { return alloc_hierarchy<float>(g); }
+int ensure_hierarchy_f64(cth_grid* g) { return alloc_hierarchy<double>(g); }
+
+template <typename T>
+static LevelArgs<T> level_args(cth_grid* g, int l) {
+    Hierarchy<T>& h = hier<T>(g);
+    LevelArgs<T> L;
+    L.a = h.a[l];
+    L.plane = (size_t)g->nrow[l] * g->ldl;
+    L.x = h.x[l];
+    L.b = h.b[l];
+    L.nrow = g->nrow[l];
+    L.ncol = g->ncol;
+    L.ld = g->ldl;
+    return L;
+}
+
+template <typename T, int NPT>
+static void launch_relax(cth_grid* g, int l, int parity, int zero_guess, int prolong,
+                         cudaStream_t s) {
+    const int nr = g->nrow[l];
+    const int rows = parity == 0 ? (nr + 1) / 2 : nr / 2;
+    if (rows <= 0) return;
+    Hierarchy<T>& h = hier<T>(g);
+    ProlongArgs<T> pa{nullptr, nullptr, nullptr, 0};
+    if (prolong) {
+        pa.ec = h.x[l + 1];
+        pa.wS = h.wS[l];
+        pa.wN = h.wN[l];
+        pa.nrowc = g->nrow[l + 1];
+    }
+    const size_t smem = 5 * (size_t)g->ncol * sizeof(T);
+    LevelArgs<T> L = level_args<T>(g, l);
+    // algorithmic bytes: 5 coefficients + b + x written + neighbour-row x, per cell
+    const int slot = (l == 0) ? prof_mark(g, PROF_RELAX0, (double)rows * g->ncol * 8.0 * sizeof(T), s) : -1;
+    switch (g->ept) {
+        case 1: k_relax<T, NPT, 1><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa); break;
+        case 2: k_relax<T, NPT, 2><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa); break;
+        default: k_relax<T, NPT, 4><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa); break;
+    }
+    g->launches++;
+    if (slot >= 0) prof_done(g, slot, s);
+}
+
+template <typename T>
+static void relax(cth_grid* g, int l, int parity, int zero_guess, int prolong, cudaStream_t s) {
+    if (l == 0) launch_relax<T, 5>(g, l, parity, zero_guess, prolong, s);
+    else launch_relax<T, 9>(g, l, parity, zero_guess, prolong, s);
+}
+
+template <typename T>
+static void vcycle(cth_grid* g, int l, cudaStream_t s) {
+    if (l == g->nlev - 1) {
+        relax<T>(g, l, 0, 1, 0, s);
+        if (g->nrow[l] > 1) relax<T>(g, l, 1, 0, 0, s);
+        return;
+    }
+    for (int k = 0; k < g->nu1; k++) {
+        relax<T>(g, l, 0, k == 0, 0, s);
+        relax<T>(g, l, 1, 0, 0, s);
+    }
+    {
+        LevelArgs<T> L = level_args<T>(g, l);
+        Hierarchy<T>& h = hier<T>(g);
+        dim3 blk(256), grd((g->ncol + 255) / 256, g->nrow[l + 1]);
+        const int slot = (l == 0) ? prof_mark(g, PROF_RESTRICT0, (double)g->nrow[1] * g->ncol * 9.0 * sizeof(T), s) : -1;
+        if (l == 0) k_restrict<T, 5><<<grd, blk, 0, s>>>(L, h.b[l + 1], g->nrow[l + 1]);
+        else k_restrict<T, 9><<<grd, blk, 0, s>>>(L, h.b[l + 1], g->nrow[l + 1]);
+        g->launches++;
+        if (slot >= 0) prof_done(g, slot, s);
+    }
+    vcycle<T>(g, l + 1, s);
+    for (int k = 0; k < g->nu2; k++) {
+        relax<T>(g, l, 0, 0, k == 0, s);
+        relax<T>(g, l, 1, 0, 0, s);
+    }
+}
+
+template <typename T>
+static void setup_levels(cth_grid* g, cudaStream_t s) {
+    Hierarchy<T>& h = hier<T>(g);
+    const int slot = prof_mark(g, PROF_SETUP, 0.0, s);
+    for (int l = 0; l + 1 < g->nlev; l++) {
+        LevelArgs<T> L = level_args<T>(g, l);
+        const int frows = g->nrow[l] / 2;
+        const size_t smem = 6 * (size_t)g->ncol * sizeof(T);
+        if (frows > 0) {
+#define CTH_W(NPT, EPT) k_weights<T, NPT, EPT><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l])
+            if (l == 0) {
+                if (g->ept == 1) CTH_W(5, 1); else if (g->ept == 2) CTH_W(5, 2); else CTH_W(5, 4);
+            } else {
+                if (g->ept == 1) CTH_W(9, 1); else if (g->ept == 2) CTH_W(9, 2); else CTH_W(9, 4);
+            }
+#undef CTH_W
+            g->launches++;
+        }
+        dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
+        if (l == 0)
+            k_galerkin<T, 5><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
+                                                 g->nrow[l + 1], g->mask[l + 1]);
+        else
+            k_galerkin<T, 9><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
+                                                 g->nrow[l + 1], g->mask[l + 1]);
+        g->launches++;
+    }
+    prof_done(g, slot, s);
+}
+
+template <typename T>
+static int solve_impl(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                      const double* aN, const double* aS, const double* b, int maxITR,
+                      double tol, double* solution, cudaStream_t s, cth_status* st) {
+    int rc = alloc_hierarchy<T>(g);
+    if (rc != CTH_OK) return rc;
+    Hierarchy<T>& h = hier<T>(g);
+    Workspace& w = g->ws;
+    const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
+    dim3 blk(256), grd((ncol + 255) / 256, nrow0);
+    const int npart = grd.x * grd.y;
+    if (npart > w.npart) {
+        set_error("partial-sum buffer too small");
+        return CTH_ERR_ALLOC;
+    }
+    k_prep0<T><<<grd, blk, 0, s>>>(aP, aE, aW, aN, aS, b, g->mask[0], g->ld, g->i0, g->j0, ncol,
+                                   nrow0, ldl, h.a[0], h.b[0], w.part);
+    k_finish<<<1, 1024, 0, s>>>(w.part, npart, w.stat, 1);
+    g->launches += 2;
+    setup_levels<T>(g, s);
+    CTH_CUDA(cudaMemsetAsync(w.x64[0], 0, sizeof(double) * (size_t)nrow0 * ldl, s));
+    CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CTH_CUDA(cudaStreamSynchronize(s));
+    CTH_CUDA(cudaGetLastError());
+    const double bb = w.h_stat[0];
+    cth_status loc{};
+    loc.initial_residual = std::sqrt(bb);
+    int cur = 0;
+    int result = CTH_NOT_CONVERGED;
+    if (!std::isfinite(bb)) {
+        loc.nonfinite = 1;
+        result = CTH_NONFINITE;
+    } else if (bb == 0.0) {
+        loc.converged = 1;
+        result = CTH_OK;
+    } else {
+        for (int it = 1; it <= maxITR; it++) {
+            vcycle<T>(g, 0, s);
+            const int slot = prof_mark(g, PROF_UPDATE,
+                                       (double)nrow0 * ncol * (8.0 * 8.0 + 2.0 * sizeof(T) + 1.0), s);
+            k_update<T><<<grd, blk, 0, s>>>(aP, aE, aW, aN, aS, b, g->mask[0], g->ld, g->i0, g->j0,
+                                            ncol, nrow0, ldl, w.x64[cur], h.x[0], w.x64[1 - cur],
+                                            h.b[0], w.part);
+            prof_done(g, slot, s);
+            k_finish<<<1, 1024, 0, s>>>(w.part, npart, w.stat, 0);
+            g->launches += 2;
+            cur = 1 - cur;
+            CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CTH_CUDA(cudaStreamSynchronize(s));
+            loc.iterations = it;
+            loc.residual = w.h_stat[1];
+            if (w.h_stat[3] != 0.0 || !std::isfinite(loc.residual)) {
+                loc.nonfinite = 1;
+                result = CTH_NONFINITE;
+                break;
+            }
+            if (loc.residual < tol) {
+                loc.converged = 1;
+                result = CTH_OK;
+                break;
+            }
+        }
+    }
+    k_store<<<grd, blk, 0, s>>>(w.x64[cur], g->mask[0], ncol, nrow0, ldl, g->ld, g->i0, g->j0,
+                                solution);
+    g->launches++;
+    CTH_CUDA(cudaGetLastError());
+    CTH_CUDA(cudaStreamSynchronize(s));
+    prof_collect(g);
+    if (st) *st = loc;
+    return result;
+}
+
+int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                  const double* aN, const double* aS, const double* b, int maxITR,
+                  double error_cnv, int precision, double* solution, cudaStream_t s,
+                  cth_status* st) {
+    if (precision == CTH_PREC_MIXED)
+        return solve_impl<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, st);
+    if (precision == CTH_PREC_FP64)
+        return solve_impl<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, st);
+    set_error("unknown precision mode");
+    return CTH_ERR_ARG;
+}
+
+// dynamic shared memory limits for the line kernels (called once per grid)
+int configure_kernels(cth_grid* g) {
+    const int smem64 = (int)(6 * (size_t)g->ncol * sizeof(double));
+    const int smem32 = (int)(6 * (size_t)g->ncol * sizeof(float));
+#define CTH_ATTR(K, BYTES) CTH_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, BYTES))
+#define CTH_ATTR_ALL(T, BYTES)                                        \
+    CTH_ATTR((k_relax<T, 5, 1>), BYTES); CTH_ATTR((k_relax<T, 5, 2>), BYTES); \
+    CTH_ATTR((k_relax<T, 5, 4>), BYTES); CTH_ATTR((k_relax<T, 9, 1>), BYTES); \
+    CTH_ATTR((k_relax<T, 9, 2>), BYTES); CTH_ATTR((k_relax<T, 9, 4>), BYTES); \
+    CTH_ATTR((k_weights<T, 5, 1>), BYTES); CTH_ATTR((k_weights<T, 5, 2>), BYTES); \
+    CTH_ATTR((k_weights<T, 5, 4>), BYTES); CTH_ATTR((k_weights<T, 9, 1>), BYTES); \
+    CTH_ATTR((k_weights<T, 9, 2>), BYTES); CTH_ATTR((k_weights<T, 9, 4>), BYTES);
+    if (smem64 > 48 * 1024) { CTH_ATTR_ALL(double, smem64) }
+    if (smem32 > 48 * 1024) { CTH_ATTR_ALL(float, smem32) }
+#undef CTH_ATTR_ALL
+#undef CTH_ATTR
+    return CTH_OK;
+}
+
+}  // namespace cth

@@ -1,0 +1,226 @@
+"""Host-side mirror of the reference's solver interface over the C ABI.
+
+``solver_SMG`` and ``solver_SOR`` keep the argument list and meaning of
+include/solverFuncs.hpp:26-37 and :169-180 (numpy (ni+2, nj+2) float64
+arrays indexed [i][j], block tables i_bl/j_bl of shape (n_bl, 2) or longer,
+n_bl, iteration cap, tolerance, message flag, in/out solution).  As in the
+reference, only the grid cells of ``solution`` are written and
+non-convergence is not an exception: the returned ``Status`` says what
+happened (the reference returns nothing).  Argument, CUDA and allocation
+failures raise ``CathodeError``.
+
+``Grid`` exposes the device-resident path: device planes in the library
+layout (torch tensors of shape (nj+2, ld) on the grid's device), solved
+without host round trips.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, Tuple
+
+import numpy as np
+
+from . import capi
+
+
+def _ptr(a) -> int:
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+def _as_ij(a: np.ndarray, ni: int, nj: int, name: str) -> np.ndarray:
+    a = np.asarray(a)
+    if a.shape != (ni + 2, nj + 2):
+        raise ValueError(f"{name}: expected shape {(ni + 2, nj + 2)}, got {a.shape}")
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Grid:
+    """A cth_grid: block union, device mask and multigrid hierarchy."""
+
+    def __init__(self, ni: int, nj: int, i_bl, j_bl, n_bl: int | None = None, device: int = 0):
+        L = capi.load()
+        ib = np.ascontiguousarray(np.asarray(i_bl, dtype=np.int32).reshape(-1, 2))
+        jb = np.ascontiguousarray(np.asarray(j_bl, dtype=np.int32).reshape(-1, 2))
+        if n_bl is None:
+            n_bl = ib.shape[0]
+        if n_bl > ib.shape[0] or n_bl > jb.shape[0] or n_bl < 1:
+            raise ValueError("n_bl exceeds the block tables")
+        ib = np.ascontiguousarray(ib[:n_bl])
+        jb = np.ascontiguousarray(jb[:n_bl])
+        h = ctypes.c_void_p()
+        capi.check(L.cth_grid_create(ni, nj, ib.ctypes.data_as(capi._ip), jb.ctypes.data_as(capi._ip),
+                                     n_bl, device, ctypes.byref(h)), allow_positive=False)
+        self._h = h
+        self._L = L
+        self.ni, self.nj, self.n_bl, self.device = ni, nj, n_bl, device
+        self.i_bl, self.j_bl = ib, jb
+        self.ld = L.cth_grid_ld(h)
+        self.levels = L.cth_grid_levels(h)
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.cth_grid_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def launch_count(self) -> int:
+        return int(self._L.cth_launch_count(self._h))
+
+    def profile(self, enable: bool = True):
+        capi.check(self._L.cth_profile(self._h, int(enable)), allow_positive=False)
+
+    def profile_read(self, cls: int):
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        by = ctypes.c_double()
+        capi.check(self._L.cth_profile_read(self._h, cls, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(by)),
+                   allow_positive=False)
+        return ms.value, n.value, by.value
+
+    def set_cycle(self, nu_pre: int, nu_post: int):
+        capi.check(self._L.cth_grid_set_cycle(self._h, nu_pre, nu_post), allow_positive=False)
+
+    # -- host-array solves (reference layout) ------------------------------
+    def smg_solve(self, aP, aE, aW, aN, aS, b, solution, maxITR=30, error_cnv=1e-10,
+                  precision=capi.CTH_PREC_FP64) -> capi.Status:
+        ni, nj = self.ni, self.nj
+        arrs = [_as_ij(a, ni, nj, n) for a, n in zip((aP, aE, aW, aN, aS, b), "aP aE aW aN aS b".split())]
+        if not (isinstance(solution, np.ndarray) and solution.dtype == np.float64 and
+                solution.flags.c_contiguous and solution.shape == (ni + 2, nj + 2)):
+            raise ValueError("solution must be a C-contiguous float64 (ni+2, nj+2) array")
+        st = capi.Status()
+        rc = self._L.cth_smg_solve(self._h, *[a.ctypes.data for a in arrs], maxITR, error_cnv, precision,
+                                   solution.ctypes.data, ctypes.byref(st))
+        capi.check(rc)
+        return st
+
+    def sor_solve(self, aP, aE, aW, aN, aS, b, solution, alpha_SOR=1.9, maxITR=2000,
+                  error_cnv=1e-8) -> capi.Status:
+        ni, nj = self.ni, self.nj
+        arrs = [_as_ij(a, ni, nj, n) for a, n in zip((aP, aE, aW, aN, aS, b), "aP aE aW aN aS b".split())]
+        if not (isinstance(solution, np.ndarray) and solution.dtype == np.float64 and
+                solution.flags.c_contiguous and solution.shape == (ni + 2, nj + 2)):
+            raise ValueError("solution must be a C-contiguous float64 (ni+2, nj+2) array")
+        st = capi.Status()
+        rc = self._L.cth_sor_solve(self._h, *[a.ctypes.data for a in arrs], alpha_SOR, maxITR, error_cnv,
+                                   solution.ctypes.data, ctypes.byref(st))
+        capi.check(rc)
+        return st
+
+    # -- device-resident path (library layout) -----------------------------
+    def device_plane(self, n: int = 1):
+        """Zeroed float64 device planes of the library layout, shape (n, nj+2, ld)."""
+        import torch
+        return torch.zeros((n, self.nj + 2, self.ld), dtype=torch.float64, device=f"cuda:{self.device}")
+
+    def to_device(self, a_ij: np.ndarray):
+        """Copy a host [i][j] array into a new device-layout plane."""
+        import torch
+        src = torch.from_numpy(_as_ij(a_ij, self.ni, self.nj, "array")).to(f"cuda:{self.device}")
+        dst = self.device_plane(1)[0]
+        s = torch.cuda.current_stream(self.device)
+        capi.check(self._L.cth_to_device_layout(self._h, src.data_ptr(), dst.data_ptr(), s.cuda_stream),
+                   allow_positive=False)
+        s.synchronize()
+        return dst
+
+    def to_host(self, plane) -> np.ndarray:
+        """Copy a device-layout plane into a new host [i][j] array."""
+        import torch
+        dst = torch.empty((self.ni + 2, self.nj + 2), dtype=torch.float64, device=f"cuda:{self.device}")
+        s = torch.cuda.current_stream(self.device)
+        capi.check(self._L.cth_from_device_layout(self._h, plane.data_ptr(), dst.data_ptr(), s.cuda_stream),
+                   allow_positive=False)
+        s.synchronize()
+        return dst.cpu().numpy()
+
+    def smg_solve_dev(self, aP, aE, aW, aN, aS, b, solution, maxITR=30, error_cnv=1e-10,
+                      precision=capi.CTH_PREC_FP64, stream=None) -> capi.Status:
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        st = capi.Status()
+        rc = self._L.cth_smg_solve_dev(self._h, *[_ptr(a) for a in (aP, aE, aW, aN, aS, b)], maxITR,
+                                       error_cnv, precision, _ptr(solution), s.cuda_stream, ctypes.byref(st))
+        capi.check(rc)
+        return st
+
+    def sor_solve_dev(self, aP, aE, aW, aN, aS, b, solution, alpha_SOR=1.9, maxITR=2000,
+                      error_cnv=1e-8, stream=None) -> capi.Status:
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        st = capi.Status()
+        rc = self._L.cth_sor_solve_dev(self._h, *[_ptr(a) for a in (aP, aE, aW, aN, aS, b)], alpha_SOR,
+                                       maxITR, error_cnv, _ptr(solution), s.cuda_stream, ctypes.byref(st))
+        capi.check(rc)
+        return st
+
+    def residual_dev(self, aP, aE, aW, aN, aS, b, x, r=None, stream=None) -> Tuple[float, float]:
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        rn = ctypes.c_double()
+        bn = ctypes.c_double()
+        capi.check(self._L.cth_residual_dev(self._h, *[_ptr(a) for a in (aP, aE, aW, aN, aS, b, x)],
+                                            None if r is None else _ptr(r), ctypes.byref(rn), ctypes.byref(bn),
+                                            s.cuda_stream), allow_positive=False)
+        return rn.value, bn.value
+
+
+# grids are reused across calls with the same shape and blocks, as a
+# persistent solver would be (the reference rebuilds HYPRE objects per call)
+_GRIDS: Dict[tuple, Grid] = {}
+
+
+def _grid_for(ni, nj, i_bl, j_bl, n_bl, device=0) -> Grid:
+    ib = np.asarray(i_bl, dtype=np.int32).reshape(-1, 2)[:n_bl]
+    jb = np.asarray(j_bl, dtype=np.int32).reshape(-1, 2)[:n_bl]
+    key = (ni, nj, ib.tobytes(), jb.tobytes(), device)
+    g = _GRIDS.get(key)
+    if g is None:
+        g = Grid(ni, nj, ib, jb, n_bl, device)
+        _GRIDS[key] = g
+    return g
+
+
+def solver_SMG(aP, aE, aW, aN, aS, b, i_bl, j_bl, n_bl, maxITR, error_cnv, flag_msg, solution,
+               precision=capi.CTH_PREC_FP64, device=0) -> capi.Status:
+    """solver_SMG (include/solverFuncs.hpp:26-163) on the GPU.
+
+    Zero initial guess; stops when ||b-Ax||_2/||b||_2 < error_cnv or after
+    maxITR cycles; writes the grid cells of ``solution`` in place.
+    ``flag_msg == 1`` prints the iteration count and final relative residual
+    as the reference does (solverFuncs.hpp:131-141).
+    """
+    ni, nj = solution.shape[0] - 2, solution.shape[1] - 2
+    g = _grid_for(ni, nj, i_bl, j_bl, n_bl, device)
+    st = g.smg_solve(aP, aE, aW, aN, aS, b, solution, maxITR=maxITR, error_cnv=error_cnv,
+                     precision=precision)
+    if flag_msg == 1:
+        print(f"Number of Iterations: {st.iterations}")
+        print(f"Final Relative Residual Norm: {st.residual}")
+    return st
+
+
+def solver_SOR(aP, aE, aW, aN, aS, b, i_bl, j_bl, n_bl, alpha_SOR, maxITR, error_cnv, flag_msg,
+               solution, device=0) -> capi.Status:
+    """solver_SOR (include/solverFuncs.hpp:169-217) on the GPU, red-black order."""
+    ni, nj = solution.shape[0] - 2, solution.shape[1] - 2
+    g = _grid_for(ni, nj, i_bl, j_bl, n_bl, device)
+    st = g.sor_solve(aP, aE, aW, aN, aS, b, solution, alpha_SOR=alpha_SOR, maxITR=maxITR,
+                     error_cnv=error_cnv)
+    if flag_msg == 1:
+        print(f"ncount = {st.iterations} error_max = {st.residual}")
+    return st

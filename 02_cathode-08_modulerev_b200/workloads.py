@@ -1,0 +1,131 @@
+"""Seeded synthetic inputs in the reference's shapes.
+
+The reference ships no benchmark data; these generators build the inputs of
+the measured workloads from fixed seeds, in the reference's array convention
+((ni+2) x (nj+2) float64 arrays indexed [i][j], i = axial z, j = radial r,
+cell centres x_i = xL + (i-0.5) dx, r_j = rmin + (j-0.5) dr as in
+initialModule.hpp:77-84).
+
+``poisson_slab`` is the isolated 512x1024 r-z potential system: the
+reference's 5-point Poisson stencil (fluidModule.hpp:2693-2703: x faces
+weighted dr^2, r faces weighted q dx^2 with q = r_face / r_cell) with a
+face permittivity taking the place of the dielectric-relaxation factor,
+Dirichlet electrodes by ghost reflection (fluidModule.hpp:2156-2240: ghost
+= -phi at 0 V, ghost = 2 V - phi at the biased electrode) and the axis
+handled by q = 0 at r = 0.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+E0 = 1.60217662e-19  # constants.hpp:6
+EPS0 = 8.8541878128e-12  # constants.hpp:7
+MU0 = 1.2566370614e-6  # constants.hpp:8
+BOLTZ = 1.380649e-23  # constants.hpp:5
+
+
+def grid(ni: int, nj: int, Lz: float = 10e-3, Lr: float = 5e-3):
+    dx = Lz / ni
+    dr = Lr / nj
+    x = (np.arange(ni + 2) - 0.5) * dx
+    r = (np.arange(nj + 2) - 0.5) * dr
+    return dx, dr, x, r
+
+
+def poisson_slab(ni: int = 1024, nj: int = 512, seed: int = 1, V_bias: float = 20.0,
+                 epsr_slab: float = 3.8, slab=(2e-3, 3e-3)) -> dict:
+    """Isolated potential system on the 10 mm (z) x 5 mm (r) rectangle.
+
+    Permittivity eps0, except epsr_slab*eps0 for slab[0] <= z <= slab[1];
+    face values are harmonic means of the two cells.  Space charge
+    rho = e (n_i - n_e) with n_e log-uniform in [1e15, 1e18] m^-3 and
+    n_i = n_e (1 + 0.01 N(0,1)), both drawn from default_rng(seed) in that
+    order, each as an (ni, nj) interior array.
+    Boundaries: z = 0 at 0 V, z = L at V_bias, r = R at 0 V (ghost
+    reflection), r = 0 axis (q = 0).  Returns the reference's solver inputs
+    aP, aE, aW, aN, aS, b (shape (ni+2, nj+2)) plus the one-block table.
+    """
+    dx, dr, x, r = grid(ni, nj)
+    rng = np.random.default_rng(seed)
+    ne = np.zeros((ni + 2, nj + 2))
+    nion = np.zeros((ni + 2, nj + 2))
+    ne[1:-1, 1:-1] = 10.0 ** rng.uniform(15.0, 18.0, size=(ni, nj))
+    nion[1:-1, 1:-1] = ne[1:-1, 1:-1] * (1.0 + 0.01 * rng.standard_normal(size=(ni, nj)))
+    eps = np.full((ni + 2, nj + 2), EPS0)
+    in_slab = (x >= slab[0]) & (x <= slab[1])
+    eps[in_slab, :] = epsr_slab * EPS0
+
+    def hm(a, b):
+        return 2.0 * a * b / (a + b)
+
+    I = slice(1, ni + 1)
+    J = slice(1, nj + 1)
+    rc = r[J][None, :]
+    rR = 0.5 * (r[1:nj + 1] + r[2:nj + 2])[None, :]
+    rL = 0.5 * (r[1:nj + 1] + r[0:nj])[None, :]
+    qR = rR / rc
+    qL = rL / rc
+    eRx = hm(eps[I, J], eps[2:ni + 2, J])
+    eLx = hm(eps[I, J], eps[0:ni, J])
+    eRr = hm(eps[I, J], eps[I, 2:nj + 2])
+    eLr = hm(eps[I, J], eps[I, 0:nj])
+
+    shape = (ni + 2, nj + 2)
+    aE = np.zeros(shape); aW = np.zeros(shape); aN = np.zeros(shape); aS = np.zeros(shape)
+    aP = np.zeros(shape); b = np.zeros(shape)
+    aE[I, J] = eRx * dr * dr
+    aW[I, J] = eLx * dr * dr
+    aN[I, J] = qR * eRr * dx * dx
+    aS[I, J] = qL * eLr * dx * dx
+    aP[I, J] = aE[I, J] + aW[I, J] + aN[I, J] + aS[I, J]
+    b[I, J] = E0 * (nion[I, J] - ne[I, J]) * dx * dx * dr * dr
+
+    # z = 0 electrode (0 V): ghost = -phi
+    aP[1, J] += aW[1, J]
+    aW[1, J] = 0.0
+    # z = L electrode (V_bias): ghost = 2 V - phi
+    aP[ni, J] += aE[ni, J]
+    b[ni, J] += 2.0 * V_bias * aE[ni, J]
+    aE[ni, J] = 0.0
+    # r = R wall (0 V): ghost = -phi
+    aP[I, nj] += aN[I, nj]
+    aN[I, nj] = 0.0
+    # r = 0 axis: qL = 0 already makes aS vanish at j = 1
+    aS[I, 1] = 0.0
+
+    return dict(ni=ni, nj=nj, dx=dx, dr=dr,
+                i_bl=np.array([[1, ni]], dtype=np.int32), j_bl=np.array([[1, nj]], dtype=np.int32),
+                aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b)
+
+
+def random_mmatrix(ni: int, nj: int, seed: int = 0, diag_extra: float = 0.0, blocks=None,
+                   aniso: float = 1.0, jump: float = 1.0) -> dict:
+    """Random variable-coefficient 5-point M-matrix system for solver tests.
+
+    Face conductances are log-uniform over [1, jump] (both directions share
+    each face, so the operator is symmetric), the x faces are scaled by
+    ``aniso``, and ``diag_extra`` adds a time-derivative-like diagonal term.
+    Couplings across the outer boundary are folded as Dirichlet walls
+    (aP += a_nb, a_nb = 0).  ``blocks`` defaults to one block covering the
+    interior.
+    """
+    rng = np.random.default_rng(seed)
+    shape = (ni + 2, nj + 2)
+    cx = np.exp(rng.uniform(0.0, np.log(jump), size=(ni + 1, nj))) * aniso  # x faces i-1/2 .. ni+1/2
+    cr = np.exp(rng.uniform(0.0, np.log(jump), size=(ni, nj + 1)))  # r faces
+    aE = np.zeros(shape); aW = np.zeros(shape); aN = np.zeros(shape); aS = np.zeros(shape)
+    aW[1:-1, 1:-1] = cx[:-1, :]
+    aE[1:-1, 1:-1] = cx[1:, :]
+    aS[1:-1, 1:-1] = cr[:, :-1]
+    aN[1:-1, 1:-1] = cr[:, 1:]
+    aP = np.zeros(shape)
+    aP[1:-1, 1:-1] = aE[1:-1, 1:-1] + aW[1:-1, 1:-1] + aN[1:-1, 1:-1] + aS[1:-1, 1:-1] + diag_extra
+    b = np.zeros(shape)
+    b[1:-1, 1:-1] = rng.standard_normal(size=(ni, nj))
+    if blocks is None:
+        i_bl = np.array([[1, ni]], dtype=np.int32)
+        j_bl = np.array([[1, nj]], dtype=np.int32)
+    else:
+        i_bl = np.asarray(blocks[0], dtype=np.int32)
+        j_bl = np.asarray(blocks[1], dtype=np.int32)
+    return dict(ni=ni, nj=nj, i_bl=i_bl, j_bl=j_bl, aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b)

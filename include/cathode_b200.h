@@ -1,0 +1,153 @@
+/*
+ * cathode_b200.h — C ABI of the B200 implicit-solve library (libcathode_b200.so).
+ *
+ * Plain C types only: pointers, sizes, doubles.  Every entry point returns an
+ * int status (CTH_OK = 0; > 0 = the solve ran but did not meet its stopping
+ * rule or produced a non-finite residual; < 0 = argument / CUDA / allocation
+ * error, nothing was written).  A human-readable message for the last error
+ * on the calling thread is returned by cth_last_error().
+ *
+ * Array conventions
+ * -----------------
+ * Host arrays use the reference's convention: a field of the (ni+2) x (nj+2)
+ * ghost-padded grid, indexed [i][j] (i = axial z index, j = radial r index),
+ * flattened row-major: a[i*(nj+2) + j].  This is exactly the data of the
+ * reference's vector<vector<double>> arguments (include/solverFuncs.hpp:26-37).
+ *
+ * Device arrays ("_dev" entry points) use the library's HBM layout: r-major
+ * planes, element (i,j) at a[j*ld + i] with ld = cth_grid_ld(g) >= ni+2, so
+ * that z-lines (fixed j) are contiguous.  ld is a multiple of 32 elements.
+ *
+ * Block tables: i_bl[2*b+0], i_bl[2*b+1] (and j_bl likewise) are the
+ * inclusive index ranges of box b, as in solverFuncs.hpp:43-47.  Cells in the
+ * union of the boxes are grid cells; couplings from a grid cell to a non-grid
+ * cell are dropped (HYPRE StructMatrix semantics) by the SMG-replacement
+ * solves, while the SOR replacement reads non-grid neighbours from the
+ * solution array exactly as solver_SOR does (solverFuncs.hpp:193-194).
+ *
+ * Stencil convention (solverFuncs.hpp:77-81):
+ *     aP*x_P - aE*x_{i+1} - aW*x_{i-1} - aN*x_{j+1} - aS*x_{j-1} = b_P.
+ */
+#ifndef CATHODE_B200_H
+#define CATHODE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CTH_OK 0
+#define CTH_NOT_CONVERGED 1
+#define CTH_NONFINITE 2
+#define CTH_ERR_ARG -1
+#define CTH_ERR_CUDA -2
+#define CTH_ERR_ALLOC -3
+#define CTH_ERR_UNSUPPORTED -4
+
+/* arithmetic of the multigrid cycle */
+#define CTH_PREC_FP64 0  /* plain FP64 multigrid                                  */
+#define CTH_PREC_MIXED 1 /* FP32 multigrid + FP64 defect correction (FP64 residual) */
+
+typedef struct cth_status {
+    int iterations;          /* V-cycles (SMG replacement) or sweeps (SOR replacement) */
+    int converged;           /* 1 when the stopping rule was met                        */
+    int nonfinite;           /* 1 when a NaN/Inf residual or update was seen             */
+    int reserved;
+    double residual;         /* SMG: final ||b-Ax||_2/||b||_2; SOR: last max relative update */
+    double initial_residual; /* SMG: ||b||_2 of the grid cells; SOR: 0                  */
+} cth_status;
+
+typedef struct cth_grid cth_grid; /* opaque: grid shape, block union, device workspace */
+
+/* Library / device information ------------------------------------------- */
+const char* cth_version(void);
+const char* cth_last_error(void);
+
+/* Grid ------------------------------------------------------------------- */
+/* Creates the grid of an (ni+2) x (nj+2) index space with n_bl boxes on CUDA
+ * device `device`.  Replaces the HYPRE_StructGrid set-up that solver_SMG
+ * repeats on every call (include/solverFuncs.hpp:38-49): the block union,
+ * its device mask and the multigrid hierarchy are built once per grid. */
+int cth_grid_create(int ni, int nj, const int* i_bl, const int* j_bl, int n_bl, int device,
+                    cth_grid** out);
+void cth_grid_destroy(cth_grid* g);
+/* leading dimension (elements) of the device layout */
+int cth_grid_ld(const cth_grid* g);
+/* number of multigrid levels of the hierarchy */
+int cth_grid_levels(const cth_grid* g);
+/* set smoothing sweeps per level (pre, post; default 1, 1) */
+int cth_grid_set_cycle(cth_grid* g, int nu_pre, int nu_post);
+
+/* Instrumentation ------------------------------------------------------------
+ * cth_launch_count: kernels this grid has launched since creation.
+ * cth_profile(g, 1) resets and enables per-kernel-class timing (CUDA events
+ * recorded on the launching stream around each launch of the class);
+ * cth_profile_read returns the summed device time (ms), the number of timed
+ * launches and the summed algorithmic bytes of a class:
+ *   CTH_PROF_RELAX0    finest-level z-line relaxation (one colour per launch)
+ *   CTH_PROF_UPDATE    FP64 defect-correction residual
+ *   CTH_PROF_RESTRICT0 finest-level restriction
+ *   CTH_PROF_SETUP     per-solve set-up (weights + Galerkin products) */
+#define CTH_PROF_RELAX0 0
+#define CTH_PROF_UPDATE 1
+#define CTH_PROF_RESTRICT0 2
+#define CTH_PROF_SETUP 3
+long long cth_launch_count(const cth_grid* g);
+int cth_profile(cth_grid* g, int enable);
+int cth_profile_read(const cth_grid* g, int cls, double* ms, long long* launches, double* bytes);
+
+/* SMG replacement (host arrays) ----------------------------------------------
+ * Drop-in for solver_SMG (include/solverFuncs.hpp:26-163): solves the 5-point
+ * system on the block union from a zero initial guess and stops when
+ * ||b-Ax||_2/||b||_2 < error_cnv or after maxITR cycles.  Only grid cells of
+ * `solution` are written (solverFuncs.hpp:143-152).  `precision` is
+ * CTH_PREC_FP64 or CTH_PREC_MIXED.  `st` may be NULL. */
+int cth_smg_solve(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                  const double* aN, const double* aS, const double* b, int maxITR,
+                  double error_cnv, int precision, double* solution, cth_status* st);
+
+/* SMG replacement (device arrays, library layout, caller's stream) -----------
+ * Same contract on device-resident planes.  All pointers are device pointers
+ * in the layout above; `solution` grid cells are written, other cells are left
+ * untouched.  `stream` is a cudaStream_t (NULL = legacy default stream).  The
+ * call returns after the solve completes on `stream` (the convergence test
+ * reads a 40-byte status per cycle). */
+int cth_smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                      const double* aN, const double* aS, const double* b, int maxITR,
+                      double error_cnv, int precision, double* solution, void* stream,
+                      cth_status* st);
+
+/* SOR replacement (host arrays) ----------------------------------------------
+ * Drop-in for solver_SOR (include/solverFuncs.hpp:169-217) with red-black
+ * ordering on the GPU: same update formula (neighbours read from `solution`,
+ * division by aP+1e-100, relaxation alpha_SOR), same stopping rule (max over
+ * grid cells of fabs((new-old)/(new+old+1e-6))*2 <= error_cnv, or the sweep
+ * that takes the count past maxITR).  `solution` is the in/out initial guess
+ * including its non-grid (ghost) values, which are read but not written. */
+int cth_sor_solve(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                  const double* aN, const double* aS, const double* b, double alpha_SOR,
+                  int maxITR, double error_cnv, double* solution, cth_status* st);
+
+/* SOR replacement (device arrays, library layout) */
+int cth_sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                      const double* aN, const double* aS, const double* b, double alpha_SOR,
+                      int maxITR, double error_cnv, double* solution, void* stream,
+                      cth_status* st);
+
+/* Residual (device arrays): r = b - A x on grid cells (couplings to non-grid
+ * cells dropped), r = 0 elsewhere; *rnorm = ||r||_2, *bnorm = ||b||_2 over grid
+ * cells (either may be NULL). */
+int cth_residual_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                     const double* aN, const double* aS, const double* b, const double* x,
+                     double* r, double* rnorm, double* bnorm, void* stream);
+
+/* Layout helpers (device arrays): copy between the reference's [i][j] layout
+ * and the library layout. */
+int cth_to_device_layout(cth_grid* g, const double* src_ij, double* dst_dev, void* stream);
+int cth_from_device_layout(cth_grid* g, const double* src_dev, double* dst_ij, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

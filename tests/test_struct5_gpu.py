@@ -1,0 +1,119 @@
+"""Parity of the CUDA 5-point solves with the oracle, through the C ABI.
+
+SMG replacement: bit-level parity is not defined (HYPRE SMG stops at a
+residual tolerance), so the GPU solution is compared with the oracle's exact
+solve at relative L2 <= 1e-8 after converging to ||b-Ax||/||b|| < 1e-11, and
+the FP64 residual of the returned solution is recomputed on the CPU.
+SOR replacement: red-black and lexicographic SOR share the fixed point; both
+are run to a tight update tolerance and compared at relative L2 <= 1e-9.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_SOLVE = 1e-11      # stopping tolerance given to the solver
+TOL_PARITY = 1e-8      # relative L2 vs the oracle's exact solve
+
+
+def _solve(pkg, s, precision, maxITR=40, tol=TOL_SOLVE, x0=None):
+    x = np.zeros((s["ni"] + 2, s["nj"] + 2)) if x0 is None else x0
+    st = pkg.solver_SMG(s["aP"], s["aE"], s["aW"], s["aN"], s["aS"], s["b"], s["i_bl"], s["j_bl"],
+                        len(s["i_bl"]), maxITR, tol, 0, x, precision=precision)
+    return x, st
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("shape", [(96, 48), (200, 100), (37, 23), (5, 3), (64, 1), (1, 40)])
+def test_smg_slab_vs_oracle(pkg, orc, cuda_device, precision, shape):
+    ni, nj = shape
+    s = pkg.workloads.poisson_slab(ni=ni, nj=nj, seed=1)
+    x, st = _solve(pkg, s, precision)
+    assert st.converged == 1 and st.residual < TOL_SOLVE, st.as_dict()
+    ref = orc.direct_solve(s)
+    err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+    assert err < TOL_PARITY, err
+    _, rn, bn = orc.residual(s, x)
+    assert rn / bn < 2 * TOL_SOLVE
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("kw", [dict(aniso=100.0), dict(aniso=0.01), dict(jump=30.0, diag_extra=0.5),
+                                dict(blocks=([[1, 40], [41, 64]], [[1, 32], [10, 20]])),
+                                dict(blocks=([[3, 3], [1, 64]], [[1, 32], [5, 5]]))])
+def test_smg_random_vs_oracle(pkg, orc, cuda_device, precision, kw):
+    s = pkg.workloads.random_mmatrix(64, 32, seed=11, **kw)
+    x0 = np.full((66, 34), -3.0)
+    x, st = _solve(pkg, s, precision, maxITR=60, x0=x0)
+    assert st.converged == 1, st.as_dict()
+    ref = orc.direct_solve(s, solution=np.full((66, 34), -3.0))
+    m = orc.active_mask(64, 32, s["i_bl"], s["j_bl"])
+    assert np.all(x[m == 0] == -3.0)  # only grid cells are written
+    err = np.linalg.norm((x - ref)[m == 1]) / np.linalg.norm(ref[m == 1])
+    assert err < TOL_PARITY, err
+
+
+def test_smg_zero_rhs_and_status(pkg, orc, cuda_device):
+    s = pkg.workloads.poisson_slab(ni=32, nj=16)
+    s["b"][:] = 0.0
+    x = np.full((34, 18), 5.0)
+    _, st = _solve(pkg, s, 1, x0=x)
+    assert st.converged == 1 and st.iterations == 0
+    assert np.all(x[1:-1, 1:-1] == 0.0) and np.all(x[0, :] == 5.0)
+
+
+def test_smg_not_converged_and_nonfinite(pkg, orc, cuda_device):
+    s = pkg.workloads.poisson_slab(ni=64, nj=32)
+    _, st = _solve(pkg, s, 0, maxITR=1, tol=1e-14)
+    assert st.converged == 0 and st.iterations == 1
+    s["b"][10, 10] = np.nan
+    _, st = _solve(pkg, s, 0)
+    assert st.nonfinite == 1 and st.converged == 0
+
+
+def test_smg_deterministic(pkg, cuda_device):
+    s = pkg.workloads.poisson_slab(ni=128, nj=64)
+    x1, _ = _solve(pkg, s, 1)
+    x2, _ = _solve(pkg, s, 1)
+    assert np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_smg_full_size_device_path(pkg, orc, cuda_device, precision):
+    """512 x 1024 r-z slab system on device-resident planes: residual property."""
+    s = pkg.workloads.poisson_slab(ni=1024, nj=512, seed=1)
+    g = pkg.Grid(s["ni"], s["nj"], s["i_bl"], s["j_bl"])
+    planes = [g.to_device(s[k]) for k in ("aP", "aE", "aW", "aN", "aS", "b")]
+    x = g.device_plane(1)[0]
+    st = g.smg_solve_dev(*planes, x, maxITR=30, error_cnv=1e-10, precision=precision)
+    assert st.converged == 1 and st.iterations <= 20, st.as_dict()
+    rn, bn = g.residual_dev(*planes, x)
+    assert rn / bn < 1e-10
+    xh = g.to_host(x)
+    _, rn2, bn2 = orc.residual(s, xh)
+    assert rn2 / bn2 < 1e-10
+    g.close()
+
+
+@pytest.mark.parametrize("shape", [(24, 16), (31, 9)])
+def test_sor_vs_oracle(pkg, orc, cuda_device, shape):
+    ni, nj = shape
+    s = pkg.workloads.random_mmatrix(ni, nj, seed=2, diag_extra=0.2)
+    x0 = np.zeros((ni + 2, nj + 2))
+    x0[0, :] = 0.3  # non-grid (ghost) values are read by solver_SOR
+    xg = x0.copy()
+    st = pkg.solver_SOR(s["aP"], s["aE"], s["aW"], s["aN"], s["aS"], s["b"], s["i_bl"], s["j_bl"], 1,
+                        1.9, 50000, 1e-13, 0, xg)
+    assert st.converged == 1
+    xc, n, e = orc.sor_solve(s, alpha=1.9, maxITR=50000, error_cnv=1e-13, solution=x0.copy())
+    assert np.all(xg[0, :] == 0.3)
+    err = np.linalg.norm(xg - xc) / np.linalg.norm(xc)
+    assert err < 1e-9, err
+
+
+def test_sor_loop_exit_count(pkg, cuda_device):
+    s = pkg.workloads.random_mmatrix(16, 8, seed=1)
+    x = np.zeros((18, 10))
+    st = pkg.solver_SOR(s["aP"], s["aE"], s["aW"], s["aN"], s["aS"], s["b"], s["i_bl"], s["j_bl"], 1,
+                        1.9, 5, 1e-30, 0, x)
+    assert st.iterations == 6 and st.converged == 0
