@@ -29,7 +29,7 @@ EXPORTS = (
     "cth_version", "cth_last_error", "cth_grid_create", "cth_grid_destroy", "cth_grid_ld",
     "cth_grid_levels", "cth_grid_set_cycle", "cth_smg_solve", "cth_smg_solve_dev", "cth_sor_solve",
     "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
-    "cth_launch_count", "cth_profile", "cth_profile_read",
+    "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -103,6 +103,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_to_device_layout.restype = ctypes.c_int
     L.cth_from_device_layout.argtypes = [_vp, _vp, _vp, _vp]
     L.cth_from_device_layout.restype = ctypes.c_int
+    L.cth_residual_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _ip, ctypes.c_int] + \
+        [_vp] * 8 + [_dp, _dp, _vp]
+    L.cth_residual_noalloc.restype = ctypes.c_int
     L.cth_launch_count.argtypes = [_vp]
     L.cth_launch_count.restype = ctypes.c_longlong
     L.cth_profile.argtypes = [_vp, ctypes.c_int]

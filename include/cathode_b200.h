@@ -142,6 +142,26 @@ int cth_residual_dev(cth_grid* g, const double* aP, const double* aE, const doub
                      const double* aN, const double* aS, const double* b, const double* x,
                      double* r, double* rnorm, double* bnorm, void* stream);
 
+/* Residual without allocation (device arrays) ---------------------------------
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory when they need a residual (a program whose own pool owns all device
+ * memory, work being recorded into a stream capture, a loop that cannot take
+ * the synchronisation an allocation can cause): same result as
+ * cth_residual_dev, but it needs no cth_grid and calls no allocator.  Its
+ * scratch is one static device array of CTH_NOALLOC_SCRATCH_BYTES per GPU
+ * (held until exit); (nj+2)*ld may not exceed CTH_NOALLOC_MAX_PLANE and n_bl
+ * may not exceed 64, otherwise CTH_ERR_ARG.  ld >= ni+2 is the caller's leading
+ * dimension of the library layout.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and may return
+ * wrong norms.  Returns after the norms are on the host. */
+#define CTH_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
+#define CTH_NOALLOC_MAX_PLANE (CTH_NOALLOC_SCRATCH_BYTES - 256u * 1024u)
+int cth_residual_noalloc(int ni, int nj, int ld, const int* i_bl, const int* j_bl, int n_bl,
+                         const double* aP, const double* aE, const double* aW, const double* aN,
+                         const double* aS, const double* b, const double* x, double* r,
+                         double* rnorm, double* bnorm, void* stream);
+
 /* Layout helpers (device arrays): copy between the reference's [i][j] layout
  * and the library layout. */
 int cth_to_device_layout(cth_grid* g, const double* src_ij, double* dst_dev, void* stream);
