@@ -199,9 +199,9 @@ int cth_grid_create(int ni, int nj, const int* i_bl, const int* j_bl, int n_bl, 
         free_grid(g);
         return CTH_ERR_UNSUPPORTED;
     }
-    g->bd = std::min(1024, ((g->ncol + 31) / 32) * 32);
-    g->ept = (g->ncol + g->bd - 1) / g->bd;
-    if (g->ept == 3) g->ept = 4;
+    // line solver: 4 cells per thread, 32..1024 threads per z-line
+    g->bd = std::max(32, (((g->ncol + 3) / 4 + 31) / 32) * 32);
+    g->ept = 4;
     // levels
     for (int r = g->j1 - g->j0 + 1;; r = (r + 1) / 2) {
         g->nrow.push_back(r);

@@ -72,7 +72,7 @@ struct cth_grid {
     int nlev = 0;
     std::vector<int> nrow;
     int nu1 = 1, nu2 = 1;
-    int bd = 32, ept = 1;      // line-solve block size / elements per thread
+    int bd = 32, ept = 1;      // line solve: threads per z-line / cells per thread (chunk)
     unsigned char* mask_full = nullptr;          // device layout
     std::vector<unsigned char*> mask;            // per level, level layout
     cth::Hierarchy<float> h32;

@@ -50,58 +50,142 @@ __device__ double block_sum(double v, double* red) {
 }
 
 // ---------------------------------------------------------------------------
-// parallel cyclic reduction of one tridiagonal line in shared memory.
-//   lo_i x_{i-1} + dg_i x_i + up_i x_{i+1} = d_i,   i = 0..n-1
-// NR right-hand sides stored as sd[r*n + i].  sr holds 1/dg.  On return the
-// solution is sd[r*n+i] * sr[i].
+// Exact solve of one tridiagonal z-line by one CTA (substructuring):
+//   lo_i x_{i-1} + dg_i x_i + up_i x_{i+1} = d_i,   i = 0..n-1.
+// Thread t owns the 4 cells [4t, 4t+4) in registers (one 16-byte vector load
+// per array); the chunk's last cell is its separator u_t.  Each thread
+// eliminates its chunk interior (Thomas) and writes it as
+// x = y + v u_{t-1} + w u_t; the separators satisfy a tridiagonal system of
+// blockDim.x unknowns, solved by parallel cyclic reduction in shared memory;
+// the interiors follow.  O(n) work, log2(blockDim.x) barrier steps.
 // ---------------------------------------------------------------------------
-template <typename T, int EPT, int NR>
-__device__ __forceinline__ void pcr(T* sa, T* sb, T* sc, T* sd, T* sr, int n) {
-    const int t = threadIdx.x, bd = blockDim.x;
-    for (int s = 1; s < n; s <<= 1) {
-        T na[EPT], nb[EPT], nc[EPT], nd[EPT][NR];
+constexpr int CH = 4;  // cells per thread
+
+// shared-memory bytes of the separator system with NR right-hand sides
+template <typename T>
+__host__ __device__ inline size_t line_smem(int nt, int nr) {
+    return (size_t)(5 + 3 * nr) * nt * sizeof(T);
+}
+
+// 4 consecutive elements, 16-byte aligned
+__device__ __forceinline__ void ld4(const float* p, float v[4]) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double v[4]) {
+    const double2 q0 = reinterpret_cast<const double2*>(p)[0];
+    const double2 q1 = reinterpret_cast<const double2*>(p)[1];
+    v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+}
+__device__ __forceinline__ void st4(float* p, const float v[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double v[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// lo/dg/up/d: the thread's 4 cells.  Cells past the end of the line must be
+// decoupled identity rows (lo = up = 0, dg = 1, d = 0) and the line's last
+// cell must have up = 0, so every chunk is handled alike: cells 0..2 are the
+// interior, cell 3 the separator.  x: the solution of the 4 cells.
+// red: (5+3NR)*blockDim.x shared elements.
+template <typename T, int NR>
+__device__ __forceinline__ void line_solve(const T lo[CH], const T dg[CH], const T up[CH], const T d[NR][CH],
+                                           T* red, T x[NR][CH]) {
+    const int nt = blockDim.x, t = threadIdx.x;
+    T* ra = red;
+    T* rb = ra + nt;
+    T* rc = rb + nt;
+    T* rd = rc + nt;          // NR * nt
+    T* fy = rd + NR * nt;     // NR * nt
+    T* fv = fy + NR * nt;
+    T* fw = fv + nt;
+    T* uu = fw + nt;          // NR * nt
+
+    // forward elimination of the interior cells 0..2
+    const T i0 = T(1) / dg[0];
+    const T c0 = up[0] * i0;
+    const T v0p = -lo[0] * i0;
+    const T i1 = T(1) / (dg[1] - lo[1] * c0);
+    const T c1 = up[1] * i1;
+    const T v1p = -lo[1] * v0p * i1;
+    const T i2 = T(1) / (dg[2] - lo[2] * c1);
+    const T v2p = -lo[2] * v1p * i2;
+    const T w2p = -up[2] * i2;
+    T y0p[NR], y1p[NR], y2p[NR];
 #pragma unroll
-        for (int e = 0; e < EPT; e++) {
-            const int i = t + e * bd;
-            if (i < n) {
-                T ai = sa[i], bi = sb[i], ci = sc[i];
-                T di[NR];
+    for (int r = 0; r < NR; r++) {
+        y0p[r] = d[r][0] * i0;
+        y1p[r] = (d[r][1] - lo[1] * y0p[r]) * i1;
+        y2p[r] = (d[r][2] - lo[2] * y1p[r]) * i2;
+    }
+    // first-interior relation x_0 = yF + vF u_{t-1} + wF u_t
+    const T v1 = v1p - c1 * v2p, w1 = -c1 * w2p;
+    const T vF = v0p - c0 * v1, wF = -c0 * w1;
+    T yF[NR];
 #pragma unroll
-                for (int r = 0; r < NR; r++) di[r] = sd[r * n + i];
-                T an = T(0), cn = T(0);
-                if (i >= s) {
-                    const int m = i - s;
-                    const T k = -ai * sr[m];
-                    an = k * sa[m];
-                    bi += k * sc[m];
+    for (int r = 0; r < NR; r++) yF[r] = y0p[r] - c0 * (y1p[r] - c1 * y2p[r]);
 #pragma unroll
-                    for (int r = 0; r < NR; r++) di[r] += k * sd[r * n + m];
-                }
-                if (i + s < n) {
-                    const int m = i + s;
-                    const T k = -ci * sr[m];
-                    cn = k * sc[m];
-                    bi += k * sa[m];
+    for (int r = 0; r < NR; r++) fy[r * nt + t] = yF[r];
+    fv[t] = vF;
+    fw[t] = wF;
+    __syncthreads();
+    // separator row: lo3 x_2 + dg3 u_t + up3 x_{next,0} = d3, with
+    // x_2 = y2p + v2p u_{t-1} + w2p u_t (last-interior relation)
+    {
+        const bool nxt = (t + 1 < nt);
+        const T vN = nxt ? fv[t + 1] : T(0), wN = nxt ? fw[t + 1] : T(0);
+        ra[t] = lo[3] * v2p;
+        rb[t] = dg[3] + lo[3] * w2p + up[3] * vN;
+        rc[t] = up[3] * wN;
 #pragma unroll
-                    for (int r = 0; r < NR; r++) di[r] += k * sd[r * n + m];
-                }
-                na[e] = an; nb[e] = bi; nc[e] = cn;
+        for (int r = 0; r < NR; r++) {
+            const T yN = nxt ? fy[r * nt + t + 1] : T(0);
+            rd[r * nt + t] = d[r][3] - lo[3] * y2p[r] - up[3] * yN;
+        }
+    }
+    __syncthreads();
+    for (int s = 1; s < nt; s <<= 1) {
+        T a_ = ra[t], b_ = rb[t], c_ = rc[t];
+        T d_[NR];
 #pragma unroll
-                for (int r = 0; r < NR; r++) nd[e][r] = di[r];
-            }
+        for (int r = 0; r < NR; r++) d_[r] = rd[r * nt + t];
+        T an = T(0), cn = T(0);
+        if (t >= s) {
+            const T k1 = -a_ / rb[t - s];
+            an = k1 * ra[t - s];
+            b_ += k1 * rc[t - s];
+#pragma unroll
+            for (int r = 0; r < NR; r++) d_[r] += k1 * rd[r * nt + t - s];
+        }
+        if (t + s < nt) {
+            const T k2 = -c_ / rb[t + s];
+            cn = k2 * rc[t + s];
+            b_ += k2 * ra[t + s];
+#pragma unroll
+            for (int r = 0; r < NR; r++) d_[r] += k2 * rd[r * nt + t + s];
         }
         __syncthreads();
+        ra[t] = an; rb[t] = b_; rc[t] = cn;
 #pragma unroll
-        for (int e = 0; e < EPT; e++) {
-            const int i = t + e * bd;
-            if (i < n) {
-                sa[i] = na[e]; sb[i] = nb[e]; sc[i] = nc[e];
-                sr[i] = T(1) / nb[e];
-#pragma unroll
-                for (int r = 0; r < NR; r++) sd[r * n + i] = nd[e][r];
-            }
-        }
+        for (int r = 0; r < NR; r++) rd[r * nt + t] = d_[r];
         __syncthreads();
+    }
+    {
+        const T ib = T(1) / rb[t];
+#pragma unroll
+        for (int r = 0; r < NR; r++) uu[r * nt + t] = rd[r * nt + t] * ib;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        const T uR = uu[r * nt + t];
+        const T uL = (t > 0) ? uu[r * nt + t - 1] : T(0);
+        const T x2 = y2p[r] + v2p * uL + w2p * uR;
+        const T x1 = y1p[r] + v1p * uL - c1 * x2;
+        const T x0 = y0p[r] + v0p * uL - c0 * x1;
+        x[r][0] = x0; x[r][1] = x1; x[r][2] = x2; x[r][3] = uR;
     }
 }
 
@@ -160,55 +244,56 @@ __global__ void k_prep0(const double* __restrict__ aP, const double* __restrict_
 // interpolation weights of the F rows (odd rows) of one level: two line solves
 // per F row, right-hand sides = lumped couplings toward the C rows.
 // ---------------------------------------------------------------------------
-template <typename T, int NPT, int EPT>
+template <typename T, int NPT>
 __global__ void k_weights(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ wS,
                           T* __restrict__ wN) {
     const int j = 2 * blockIdx.x + 1;
     if (j >= L.nrow) return;
     extern __shared__ unsigned char smem_raw[];
-    const int n = L.ncol;
-    T* sa = reinterpret_cast<T*>(smem_raw);
-    T* sb = sa + n;
-    T* sc = sb + n;
-    T* sr = sc + n;
-    T* sd = sr + n;  // 2 rhs
-    const T* a = L.a;
+    T* red = reinterpret_cast<T*>(smem_raw);
+    const int n = L.ncol, s0 = CH * threadIdx.x;
+    const int cnt = max(0, min(CH, n - s0));
     const size_t pl = L.plane;
+    const size_t p = (size_t)j * L.ld + s0;
+    T lo[CH], dg[CH], up[CH], d[2][CH];
 #pragma unroll
-    for (int e = 0; e < EPT; e++) {
-        const int i = threadIdx.x + e * blockDim.x;
-        if (i < n) {
-            const size_t p = (size_t)j * L.ld + i;
-            const T dg = a[P * pl + p];
-            T rs = T(0), rn = T(0);
-            if (mask[p]) {
-                if (mask[p - L.ld]) {
-                    rs = a[S * pl + p];
-                    if (NPT == 9) rs += a[SW * pl + p] + a[SE * pl + p];
+    for (int k = 0; k < CH; k++) { lo[k] = T(0); dg[k] = T(1); up[k] = T(0); d[0][k] = T(0); d[1][k] = T(0); }
+    if (cnt > 0) {
+        const T* a = L.a;
+        T aw[CH], ae[CH], as_[CH], an[CH];
+        ld4(a + P * pl + p, dg);
+        ld4(a + W * pl + p, aw);
+        ld4(a + E * pl + p, ae);
+        ld4(a + S * pl + p, as_);
+        ld4(a + N * pl + p, an);
+        T sw[CH] = {0, 0, 0, 0}, se[CH] = {0, 0, 0, 0}, nw[CH] = {0, 0, 0, 0}, ne[CH] = {0, 0, 0, 0};
+        if (NPT == 9) {
+            ld4(a + SW * pl + p, sw);
+            ld4(a + SE * pl + p, se);
+            ld4(a + NW * pl + p, nw);
+            ld4(a + NE * pl + p, ne);
+        }
+#pragma unroll
+        for (int k = 0; k < CH; k++) {
+            const int i = s0 + k;
+            if (k < cnt) {
+                lo[k] = (i > 0) ? -aw[k] : T(0);
+                up[k] = (i + 1 < n) ? -ae[k] : T(0);
+                const size_t pk = p + k;
+                if (mask[pk]) {
+                    if (mask[pk - L.ld]) d[0][k] = as_[k] + ((NPT == 9) ? sw[k] + se[k] : T(0));
+                    if (j + 1 < L.nrow && mask[pk + L.ld]) d[1][k] = an[k] + ((NPT == 9) ? nw[k] + ne[k] : T(0));
                 }
-                if (j + 1 < L.nrow && mask[p + L.ld]) {
-                    rn = a[N * pl + p];
-                    if (NPT == 9) rn += a[NW * pl + p] + a[NE * pl + p];
-                }
+            } else {
+                dg[k] = T(1);
             }
-            sa[i] = (i > 0) ? -a[W * pl + p] : T(0);
-            sc[i] = (i + 1 < n) ? -a[E * pl + p] : T(0);
-            sb[i] = dg;
-            sr[i] = T(1) / dg;
-            sd[i] = rs;
-            sd[n + i] = rn;
         }
     }
-    __syncthreads();
-    pcr<T, EPT, 2>(sa, sb, sc, sd, sr, n);
-#pragma unroll
-    for (int e = 0; e < EPT; e++) {
-        const int i = threadIdx.x + e * blockDim.x;
-        if (i < n) {
-            const size_t p = (size_t)j * L.ld + i;
-            wS[p] = sd[i] * sr[i];
-            wN[p] = sd[n + i] * sr[i];
-        }
+    T x[2][CH];
+    line_solve<T, 2>(lo, dg, up, d, red, x);
+    if (cnt > 0) {
+        st4(wS + p, x[0]);
+        st4(wN + p, x[1]);
     }
 }
 
@@ -310,57 +395,107 @@ __device__ __forceinline__ T xnb(const LevelArgs<T>& L, const ProlongArgs<T>& pa
     return v;
 }
 
-template <typename T, int NPT, int EPT>
+// 4 cells [s0, s0+4) of row jj of x (with the coarse correction when prolong)
+template <typename T>
+__device__ __forceinline__ void xrow4(const LevelArgs<T>& L, const ProlongArgs<T>& pa, bool prolong,
+                                      int s0, int jj, T v[CH]) {
+    const size_t p = (size_t)jj * L.ld + s0;
+    ld4(L.x + p, v);
+    if (prolong) {
+        T ws[CH], wn[CH], e0[CH];
+        ld4(pa.wS + p, ws);
+        ld4(pa.ec + (size_t)((jj - 1) >> 1) * L.ld + s0, e0);
+#pragma unroll
+        for (int k = 0; k < CH; k++) v[k] += ws[k] * e0[k];
+        const int Jn = (jj + 1) >> 1;
+        if (Jn < pa.nrowc) {
+            T e1[CH];
+            ld4(pa.wN + p, wn);
+            ld4(pa.ec + (size_t)Jn * L.ld + s0, e1);
+#pragma unroll
+            for (int k = 0; k < CH; k++) v[k] += wn[k] * e1[k];
+        }
+    }
+}
+
+template <typename T, int NPT>
 __global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong, ProlongArgs<T> pa) {
     const int j = 2 * blockIdx.x + parity;
     if (j >= L.nrow) return;
     extern __shared__ unsigned char smem_raw[];
-    const int n = L.ncol;
-    T* sa = reinterpret_cast<T*>(smem_raw);
-    T* sb = sa + n;
-    T* sc = sb + n;
-    T* sr = sc + n;
-    T* sd = sr + n;
-    const T* a = L.a;
+    T* red = reinterpret_cast<T*>(smem_raw);
+    const int n = L.ncol, s0 = CH * threadIdx.x;
+    const int cnt = max(0, min(CH, n - s0));
     const size_t pl = L.plane;
+    const size_t p = (size_t)j * L.ld + s0;
     const bool pr = prolong != 0;
+    T lo[CH], dg[CH], up[CH], d[1][CH];
 #pragma unroll
-    for (int e = 0; e < EPT; e++) {
-        const int i = threadIdx.x + e * blockDim.x;
-        if (i < n) {
-            const size_t p = (size_t)j * L.ld + i;
-            const T dg = a[P * pl + p];
-            T d = L.b[p];
-            if (!zero_guess) {
-                if (j > 0) {
-                    d += a[S * pl + p] * xnb<T, NPT>(L, pa, pr, i, j - 1);
-                    if (NPT == 9) {
-                        if (i > 0) d += a[SW * pl + p] * xnb<T, NPT>(L, pa, pr, i - 1, j - 1);
-                        if (i + 1 < n) d += a[SE * pl + p] * xnb<T, NPT>(L, pa, pr, i + 1, j - 1);
-                    }
-                }
-                if (j + 1 < L.nrow) {
-                    d += a[N * pl + p] * xnb<T, NPT>(L, pa, pr, i, j + 1);
-                    if (NPT == 9) {
-                        if (i > 0) d += a[NW * pl + p] * xnb<T, NPT>(L, pa, pr, i - 1, j + 1);
-                        if (i + 1 < n) d += a[NE * pl + p] * xnb<T, NPT>(L, pa, pr, i + 1, j + 1);
-                    }
+    for (int k = 0; k < CH; k++) { lo[k] = T(0); dg[k] = T(1); up[k] = T(0); d[0][k] = T(0); }
+    if (cnt > 0) {
+        const T* a = L.a;
+        T aw[CH], ae[CH];
+        ld4(a + P * pl + p, dg);
+        ld4(a + W * pl + p, aw);
+        ld4(a + E * pl + p, ae);
+        ld4(L.b + p, d[0]);
+        if (!zero_guess) {
+            if (j > 0) {
+                T as_[CH], xs[CH];
+                ld4(a + S * pl + p, as_);
+                xrow4<T>(L, pa, pr, s0, j - 1, xs);
+#pragma unroll
+                for (int k = 0; k < CH; k++) d[0][k] += as_[k] * xs[k];
+                if (NPT == 9) {
+                    T sw[CH], se[CH];
+                    ld4(a + SW * pl + p, sw);
+                    ld4(a + SE * pl + p, se);
+                    const T xl = (s0 > 0) ? xnb<T, NPT>(L, pa, pr, s0 - 1, j - 1) : T(0);
+                    const T xr = (s0 + CH < n) ? xnb<T, NPT>(L, pa, pr, s0 + CH, j - 1) : T(0);
+                    d[0][0] += sw[0] * xl;
+#pragma unroll
+                    for (int k = 1; k < CH; k++) d[0][k] += sw[k] * xs[k - 1];
+#pragma unroll
+                    for (int k = 0; k < CH - 1; k++) d[0][k] += se[k] * xs[k + 1];
+                    d[0][CH - 1] += se[CH - 1] * xr;
                 }
             }
-            sa[i] = (i > 0) ? -a[W * pl + p] : T(0);
-            sc[i] = (i + 1 < n) ? -a[E * pl + p] : T(0);
-            sb[i] = dg;
-            sr[i] = T(1) / dg;
-            sd[i] = d;
+            if (j + 1 < L.nrow) {
+                T an[CH], xn[CH];
+                ld4(a + N * pl + p, an);
+                xrow4<T>(L, pa, pr, s0, j + 1, xn);
+#pragma unroll
+                for (int k = 0; k < CH; k++) d[0][k] += an[k] * xn[k];
+                if (NPT == 9) {
+                    T nw[CH], ne[CH];
+                    ld4(a + NW * pl + p, nw);
+                    ld4(a + NE * pl + p, ne);
+                    const T xl = (s0 > 0) ? xnb<T, NPT>(L, pa, pr, s0 - 1, j + 1) : T(0);
+                    const T xr = (s0 + CH < n) ? xnb<T, NPT>(L, pa, pr, s0 + CH, j + 1) : T(0);
+                    d[0][0] += nw[0] * xl;
+#pragma unroll
+                    for (int k = 1; k < CH; k++) d[0][k] += nw[k] * xn[k - 1];
+#pragma unroll
+                    for (int k = 0; k < CH - 1; k++) d[0][k] += ne[k] * xn[k + 1];
+                    d[0][CH - 1] += ne[CH - 1] * xr;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < CH; k++) {
+            const int i = s0 + k;
+            if (k < cnt) {
+                lo[k] = (i > 0) ? -aw[k] : T(0);
+                up[k] = (i + 1 < n) ? -ae[k] : T(0);
+            } else {
+                dg[k] = T(1);
+                d[0][k] = T(0);
+            }
         }
     }
-    __syncthreads();
-    pcr<T, EPT, 1>(sa, sb, sc, sd, sr, n);
-#pragma unroll
-    for (int e = 0; e < EPT; e++) {
-        const int i = threadIdx.x + e * blockDim.x;
-        if (i < n) L.x[(size_t)j * L.ld + i] = sd[i] * sr[i];
-    }
+    T x[1][CH];
+    line_solve<T, 1>(lo, dg, up, d, red, x);
+    if (cnt > 0) st4(L.x + p, x[0]);
 }
 
 // ---------------------------------------------------------------------------
@@ -530,15 +665,11 @@ static void launch_relax(cth_grid* g, int l, int parity, int zero_guess, int pro
         pa.wN = h.wN[l];
         pa.nrowc = g->nrow[l + 1];
     }
-    const size_t smem = 5 * (size_t)g->ncol * sizeof(T);
+    const size_t smem = line_smem<T>(g->bd, 1);
     LevelArgs<T> L = level_args<T>(g, l);
     // algorithmic bytes: 5 coefficients + b + x written + neighbour-row x, per cell
     const int slot = (l == 0) ? prof_mark(g, PROF_RELAX0, (double)rows * g->ncol * 8.0 * sizeof(T), s) : -1;
-    switch (g->ept) {
-        case 1: k_relax<T, NPT, 1><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa); break;
-        case 2: k_relax<T, NPT, 2><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa); break;
-        default: k_relax<T, NPT, 4><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa); break;
-    }
+    k_relax<T, NPT><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa);
     g->launches++;
     if (slot >= 0) prof_done(g, slot, s);
 }
@@ -584,15 +715,10 @@ static void setup_levels(cth_grid* g, cudaStream_t s) {
     for (int l = 0; l + 1 < g->nlev; l++) {
         LevelArgs<T> L = level_args<T>(g, l);
         const int frows = g->nrow[l] / 2;
-        const size_t smem = 6 * (size_t)g->ncol * sizeof(T);
+        const size_t smem = line_smem<T>(g->bd, 2);
         if (frows > 0) {
-#define CTH_W(NPT, EPT) k_weights<T, NPT, EPT><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l])
-            if (l == 0) {
-                if (g->ept == 1) CTH_W(5, 1); else if (g->ept == 2) CTH_W(5, 2); else CTH_W(5, 4);
-            } else {
-                if (g->ept == 1) CTH_W(9, 1); else if (g->ept == 2) CTH_W(9, 2); else CTH_W(9, 4);
-            }
-#undef CTH_W
+            if (l == 0) k_weights<T, 5><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
+            else k_weights<T, 9><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
             g->launches++;
         }
         dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
@@ -694,19 +820,21 @@ int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double*
 
 // dynamic shared memory limits for the line kernels (called once per grid)
 int configure_kernels(cth_grid* g) {
-    const int smem64 = (int)(6 * (size_t)g->ncol * sizeof(double));
-    const int smem32 = (int)(6 * (size_t)g->ncol * sizeof(float));
+    const int smem64 = (int)line_smem<double>(g->bd, 2);
+    const int smem32 = (int)line_smem<float>(g->bd, 2);
+    if (smem64 > 227 * 1024) {
+        set_error("z-line too long for the shared-memory line solver");
+        return CTH_ERR_UNSUPPORTED;
+    }
 #define CTH_ATTR(K, BYTES) CTH_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, BYTES))
-#define CTH_ATTR_ALL(T, BYTES)                                        \
-    CTH_ATTR((k_relax<T, 5, 1>), BYTES); CTH_ATTR((k_relax<T, 5, 2>), BYTES); \
-    CTH_ATTR((k_relax<T, 5, 4>), BYTES); CTH_ATTR((k_relax<T, 9, 1>), BYTES); \
-    CTH_ATTR((k_relax<T, 9, 2>), BYTES); CTH_ATTR((k_relax<T, 9, 4>), BYTES); \
-    CTH_ATTR((k_weights<T, 5, 1>), BYTES); CTH_ATTR((k_weights<T, 5, 2>), BYTES); \
-    CTH_ATTR((k_weights<T, 5, 4>), BYTES); CTH_ATTR((k_weights<T, 9, 1>), BYTES); \
-    CTH_ATTR((k_weights<T, 9, 2>), BYTES); CTH_ATTR((k_weights<T, 9, 4>), BYTES);
-    if (smem64 > 48 * 1024) { CTH_ATTR_ALL(double, smem64) }
-    if (smem32 > 48 * 1024) { CTH_ATTR_ALL(float, smem32) }
-#undef CTH_ATTR_ALL
+    if (smem64 > 48 * 1024) {
+        CTH_ATTR((k_relax<double, 5>), smem64); CTH_ATTR((k_relax<double, 9>), smem64);
+        CTH_ATTR((k_weights<double, 5>), smem64); CTH_ATTR((k_weights<double, 9>), smem64);
+    }
+    if (smem32 > 48 * 1024) {
+        CTH_ATTR((k_relax<float, 5>), smem32); CTH_ATTR((k_relax<float, 9>), smem32);
+        CTH_ATTR((k_weights<float, 5>), smem32); CTH_ATTR((k_weights<float, 9>), smem32);
+    }
 #undef CTH_ATTR
     return CTH_OK;
 }
