@@ -132,6 +132,14 @@ static void free_grid(cth_grid* g) {
     fr(g->ws.stage);
     fr(g->ws.stage_ij);
     if (g->ws.h_stat) cudaFreeHost(g->ws.h_stat);
+    if (g->ws.h_args) cudaFreeHost(g->ws.h_args);
+    fr(g->ws.d_args);
+    fr(g->ws.counter);
+    for (auto& G : g->graphs) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        if (G.graph) cudaGraphDestroy(G.graph);
+    }
+    for (auto c : g->cap) if (c) cudaStreamDestroy(c);
     if (g->stream) cudaStreamDestroy(g->stream);
     for (auto e : g->prof.ev) cudaEventDestroy(e);
     delete g;
@@ -244,6 +252,12 @@ int cth_grid_create(int ni, int nj, const int* i_bl, const int* j_bl, int n_bl, 
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.stat, 32 * sizeof(double)), "cudaMalloc stat");
     if (rc == CTH_OK) chk(cudaMemset(g->ws.stat, 0, 32 * sizeof(double)), "memset stat");
     if (rc == CTH_OK) chk(cudaMallocHost(&g->ws.h_stat, 32 * sizeof(double)), "cudaMallocHost");
+    if (rc == CTH_OK) chk(cudaMallocHost(&g->ws.h_args, sizeof(cth::SolveArgs)), "cudaMallocHost args");
+    if (rc == CTH_OK) chk(cudaMalloc(&g->ws.d_args, sizeof(cth::SolveArgs)), "cudaMalloc args");
+    if (rc == CTH_OK) chk(cudaMalloc(&g->ws.counter, 64), "cudaMalloc counter");
+    if (rc == CTH_OK) chk(cudaMemset(g->ws.counter, 0, 64), "memset counter");
+    if (rc == CTH_OK) chk(cudaStreamCreateWithFlags(&g->cap[0], cudaStreamNonBlocking), "capture stream");
+    if (rc == CTH_OK) chk(cudaStreamCreateWithFlags(&g->cap[1], cudaStreamNonBlocking), "capture stream");
     if (rc == CTH_OK) rc = configure_kernels(g);
     if (rc != CTH_OK) {
         free_grid(g);
@@ -274,6 +288,12 @@ int cth_profile_read(const cth_grid* g, int cls, double* ms, long long* launches
     if (ms) *ms = g->prof.ms[cls];
     if (launches) *launches = g->prof.n[cls];
     if (bytes) *bytes = g->prof.nbytes[cls];
+    return CTH_OK;
+}
+
+int cth_grid_set_graphs(cth_grid* g, int enable) {
+    if (!g) { set_error("cth_grid_set_graphs: null grid"); return CTH_ERR_ARG; }
+    g->use_graphs = enable != 0;
     return CTH_OK;
 }
 

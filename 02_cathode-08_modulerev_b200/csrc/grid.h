@@ -47,6 +47,32 @@ struct Profiler {
     double nbytes[PROF_NCLASS] = {0, 0, 0, 0};
 };
 
+// caller arguments of one solve, read by the kernels from device memory so
+// that a captured graph stays valid for any caller arrays
+struct SolveArgs {
+    const double* aP;
+    const double* aE;
+    const double* aW;
+    const double* aN;
+    const double* aS;
+    const double* b;
+    double* solution;
+    double tol;
+    int maxit;
+    int pad;
+};
+
+// device status words of a solve (double array)
+enum StatWord { ST_RR = 0, ST_RELRES = 1, ST_BB = 2, ST_NONFINITE = 3, ST_ITER = 4, ST_CONV = 5, ST_KEEP = 6 };
+
+struct SolveGraph {
+    bool valid = false;
+    int nu1 = 0, nu2 = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int n_pre = 0, n_body = 0, n_post = 0;  // kernels per section
+};
+
 struct Workspace {
     double* x64[2] = {nullptr, nullptr};  // level-0 layout accumulated solution
     double* part = nullptr;               // per-block partial sums
@@ -57,6 +83,9 @@ struct Workspace {
     double* stage = nullptr;
     double* stage_ij = nullptr;
     double* h_pinned = nullptr;           // pinned [i][j] buffer for transfers
+    SolveArgs* d_args = nullptr;
+    SolveArgs* h_args = nullptr;          // pinned
+    unsigned int* counter = nullptr;      // last-block reduction counter
 };
 
 }  // namespace cth
@@ -81,6 +110,9 @@ struct cth_grid {
     cudaStream_t stream = nullptr;
     long long launches = 0;    // kernels launched by this grid since creation
     cth::Profiler prof;
+    cth::SolveGraph graphs[2]; // per precision (CTH_PREC_FP64, CTH_PREC_MIXED)
+    cudaStream_t cap[2] = {nullptr, nullptr};  // capture streams
+    bool use_graphs = true;
 };
 
 namespace cth {

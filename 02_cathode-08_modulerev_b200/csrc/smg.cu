@@ -64,8 +64,12 @@ constexpr int CH = 4;  // cells per thread
 // shared-memory bytes of the separator system with NR right-hand sides
 template <typename T>
 __host__ __device__ inline size_t line_smem(int nt, int nr) {
-    return (size_t)(5 + 3 * nr) * nt * sizeof(T);
+    return (size_t)(6 + 3 * nr) * nt * sizeof(T);
 }
+
+// correctly rounded reciprocal (one reciprocal per cell and reduction step)
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
 
 // 4 consecutive elements, 16-byte aligned
 __device__ __forceinline__ void ld4(const float* p, float v[4]) {
@@ -89,7 +93,7 @@ __device__ __forceinline__ void st4(double* p, const double v[4]) {
 // decoupled identity rows (lo = up = 0, dg = 1, d = 0) and the line's last
 // cell must have up = 0, so every chunk is handled alike: cells 0..2 are the
 // interior, cell 3 the separator.  x: the solution of the 4 cells.
-// red: (5+3NR)*blockDim.x shared elements.
+// red: (6+3NR)*blockDim.x shared elements.
 template <typename T, int NR>
 __device__ __forceinline__ void line_solve(const T lo[CH], const T dg[CH], const T up[CH], const T d[NR][CH],
                                            T* red, T x[NR][CH]) {
@@ -102,15 +106,16 @@ __device__ __forceinline__ void line_solve(const T lo[CH], const T dg[CH], const
     T* fv = fy + NR * nt;
     T* fw = fv + nt;
     T* uu = fw + nt;          // NR * nt
+    T* ri = uu + NR * nt;     // 1 / rb
 
     // forward elimination of the interior cells 0..2
-    const T i0 = T(1) / dg[0];
+    const T i0 = rcp(dg[0]);
     const T c0 = up[0] * i0;
     const T v0p = -lo[0] * i0;
-    const T i1 = T(1) / (dg[1] - lo[1] * c0);
+    const T i1 = rcp(dg[1] - lo[1] * c0);
     const T c1 = up[1] * i1;
     const T v1p = -lo[1] * v0p * i1;
-    const T i2 = T(1) / (dg[2] - lo[2] * c1);
+    const T i2 = rcp(dg[2] - lo[2] * c1);
     const T v2p = -lo[2] * v1p * i2;
     const T w2p = -up[2] * i2;
     T y0p[NR], y1p[NR], y2p[NR];
@@ -137,7 +142,9 @@ __device__ __forceinline__ void line_solve(const T lo[CH], const T dg[CH], const
         const bool nxt = (t + 1 < nt);
         const T vN = nxt ? fv[t + 1] : T(0), wN = nxt ? fw[t + 1] : T(0);
         ra[t] = lo[3] * v2p;
-        rb[t] = dg[3] + lo[3] * w2p + up[3] * vN;
+        const T bsep = dg[3] + lo[3] * w2p + up[3] * vN;
+        rb[t] = bsep;
+        ri[t] = rcp(bsep);
         rc[t] = up[3] * wN;
 #pragma unroll
         for (int r = 0; r < NR; r++) {
@@ -153,14 +160,14 @@ __device__ __forceinline__ void line_solve(const T lo[CH], const T dg[CH], const
         for (int r = 0; r < NR; r++) d_[r] = rd[r * nt + t];
         T an = T(0), cn = T(0);
         if (t >= s) {
-            const T k1 = -a_ / rb[t - s];
+            const T k1 = -a_ * ri[t - s];
             an = k1 * ra[t - s];
             b_ += k1 * rc[t - s];
 #pragma unroll
             for (int r = 0; r < NR; r++) d_[r] += k1 * rd[r * nt + t - s];
         }
         if (t + s < nt) {
-            const T k2 = -c_ / rb[t + s];
+            const T k2 = -c_ * ri[t + s];
             cn = k2 * rc[t + s];
             b_ += k2 * ra[t + s];
 #pragma unroll
@@ -168,12 +175,13 @@ __device__ __forceinline__ void line_solve(const T lo[CH], const T dg[CH], const
         }
         __syncthreads();
         ra[t] = an; rb[t] = b_; rc[t] = cn;
+        ri[t] = rcp(b_);
 #pragma unroll
         for (int r = 0; r < NR; r++) rd[r * nt + t] = d_[r];
         __syncthreads();
     }
     {
-        const T ib = T(1) / rb[t];
+        const T ib = ri[t];
 #pragma unroll
         for (int r = 0; r < NR; r++) uu[r * nt + t] = rd[r * nt + t] * ib;
     }
@@ -199,33 +207,62 @@ struct LevelArgs {
 };
 
 // ---------------------------------------------------------------------------
+// Deterministic grid-wide sum: every block stores its partial, the last block
+// to arrive (atomic ticket) sums all partials in a fixed order.  Returns true
+// in the last block (the sum is valid in its thread 0).
+// ---------------------------------------------------------------------------
+__device__ bool last_block_sum(double v, double* part, unsigned int* counter, double* red,
+                               double* total) {
+    __shared__ bool am_last;
+    const int nb = gridDim.x * gridDim.y;
+    const double s = block_sum(v, red);
+    if (threadIdx.x == 0) {
+        part[blockIdx.y * gridDim.x + blockIdx.x] = s;
+        __threadfence();
+        const unsigned int ticket = atomicAdd(counter, 1u);
+        am_last = (ticket == (unsigned int)(nb - 1));
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) acc += __ldcg(part + k);
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) {
+        *total = acc;
+        *counter = 0u;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // level-0 preparation: masked copy of the caller's FP64 planes into the level
 // layout in precision T (couplings to non-grid cells dropped, non-grid cells
-// identity), b0 = b (grid cells), partial sums of b^2.
+// identity), b0 = b (grid cells); the last block records ||b||^2 and whether
+// the cycle loop runs at all (sets the graph's loop condition when use_cond).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_prep0(const double* __restrict__ aP, const double* __restrict__ aE,
-                        const double* __restrict__ aW, const double* __restrict__ aN,
-                        const double* __restrict__ aS, const double* __restrict__ b,
-                        const unsigned char* __restrict__ mask, int ld_u, int i0, int j0,
-                        int ncol, int nrow, int ldl, T* __restrict__ a0, T* __restrict__ b0,
-                        double* __restrict__ part) {
+__global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask,
+                        int ld_u, int i0, int j0, int ncol, int nrow, int ldl, T* __restrict__ a0,
+                        T* __restrict__ b0, double* __restrict__ part, unsigned int* counter,
+                        double* __restrict__ stat, cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ double red[32];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
     double bb = 0.0;
     if (c < ncol) {
+        const double* __restrict__ aP = args->aP;
         const size_t plane = (size_t)nrow * ldl;
         const size_t p = (size_t)r * ldl + c;
         const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
         T vP = T(1), vW = T(0), vE = T(0), vS = T(0), vN = T(0), vb = T(0);
         if (mask[p]) {
             vP = (T)aP[q];
-            if (c > 0 && mask[p - 1]) vW = (T)aW[q];
-            if (c + 1 < ncol && mask[p + 1]) vE = (T)aE[q];
-            if (r > 0 && mask[p - ldl]) vS = (T)aS[q];
-            if (r + 1 < nrow && mask[p + ldl]) vN = (T)aN[q];
-            const double bv = b[q];
+            if (c > 0 && mask[p - 1]) vW = (T)args->aW[q];
+            if (c + 1 < ncol && mask[p + 1]) vE = (T)args->aE[q];
+            if (r > 0 && mask[p - ldl]) vS = (T)args->aS[q];
+            if (r + 1 < nrow && mask[p + ldl]) vN = (T)args->aN[q];
+            const double bv = args->b[q];
             vb = (T)bv;
             bb = bv * bv;
         }
@@ -236,8 +273,19 @@ __global__ void k_prep0(const double* __restrict__ aP, const double* __restrict_
         a0[N * plane + p] = vN;
         b0[p] = vb;
     }
-    const double s = block_sum(bb, red);
-    if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = s;
+    double tot;
+    if (last_block_sum(bb, part, counter, red, &tot) && threadIdx.x == 0) {
+        const bool fin = isfinite(tot);
+        const bool keep = fin && tot > 0.0 && args->maxit > 0;
+        stat[ST_RR] = tot;
+        stat[ST_BB] = tot;
+        stat[ST_RELRES] = (tot > 0.0) ? 1.0 : 0.0;
+        stat[ST_NONFINITE] = fin ? 0.0 : 1.0;
+        stat[ST_ITER] = 0.0;
+        stat[ST_CONV] = (fin && tot == 0.0) ? 1.0 : 0.0;
+        stat[ST_KEEP] = keep ? 1.0 : 0.0;
+        if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -418,8 +466,65 @@ __device__ __forceinline__ void xrow4(const LevelArgs<T>& L, const ProlongArgs<T
     }
 }
 
-template <typename T, int NPT>
-__global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong, ProlongArgs<T> pa) {
+// residual r = b - A x of the 4 cells [s0, s0+4) of row f of level F
+// (NPTF-point stencil); used to restrict into the next coarser level on the fly
+template <typename T, int NPTF>
+__device__ __forceinline__ void resid4(const LevelArgs<T>& F, int f, int s0, T r[CH]) {
+    const int n = F.ncol;
+    const size_t pl = F.plane;
+    const size_t p = (size_t)f * F.ld + s0;
+    const T* a = F.a;
+    T ap[CH], aw[CH], ae[CH], xc[CH];
+    ld4(F.b + p, r);
+    ld4(a + P * pl + p, ap);
+    ld4(a + W * pl + p, aw);
+    ld4(a + E * pl + p, ae);
+    ld4(F.x + p, xc);
+    const T xl = (s0 > 0) ? F.x[p - 1] : T(0);
+    const T xr = (s0 + CH < n) ? F.x[p + CH] : T(0);
+#pragma unroll
+    for (int k = 0; k < CH; k++) r[k] -= ap[k] * xc[k];
+    r[0] += aw[0] * xl;
+#pragma unroll
+    for (int k = 1; k < CH; k++) r[k] += aw[k] * xc[k - 1];
+#pragma unroll
+    for (int k = 0; k < CH - 1; k++) r[k] += ae[k] * xc[k + 1];
+    r[CH - 1] += ae[CH - 1] * xr;
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+        const int g = side == 0 ? f - 1 : f + 1;
+        if (g < 0 || g >= F.nrow) continue;
+        const size_t q = (size_t)g * F.ld + s0;
+        T as_[CH], xg[CH];
+        ld4(a + (side == 0 ? S : N) * pl + p, as_);
+        ld4(F.x + q, xg);
+#pragma unroll
+        for (int k = 0; k < CH; k++) r[k] += as_[k] * xg[k];
+        if (NPTF == 9) {
+            T dl[CH], dr[CH];
+            ld4(a + (side == 0 ? SW : NW) * pl + p, dl);
+            ld4(a + (side == 0 ? SE : NE) * pl + p, dr);
+            const T gl = (s0 > 0) ? F.x[q - 1] : T(0);
+            const T gr = (s0 + CH < n) ? F.x[q + CH] : T(0);
+            r[0] += dl[0] * gl;
+#pragma unroll
+            for (int k = 1; k < CH; k++) r[k] += dl[k] * xg[k - 1];
+#pragma unroll
+            for (int k = 0; k < CH - 1; k++) r[k] += dr[k] * xg[k + 1];
+            r[CH - 1] += dr[CH - 1] * gr;
+        }
+    }
+}
+
+// zebra z-line relaxation, one CTA per row of the given parity.
+//   zero_guess: x of this level is zero (first C-row relaxation of a cycle);
+//   prolong:    add the coarse correction to the F-row neighbours on the fly;
+//   NPTF > 0:   (with zero_guess, C rows) the right-hand side is the residual
+//               of the finer level F restricted on the fly (its C rows 2j and
+//               2j+2), stored into this level's b for rows j and j+1.
+template <typename T, int NPT, int NPTF>
+__global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong, ProlongArgs<T> pa,
+                        LevelArgs<T> F) {
     const int j = 2 * blockIdx.x + parity;
     if (j >= L.nrow) return;
     extern __shared__ unsigned char smem_raw[];
@@ -438,7 +543,17 @@ __global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong,
         ld4(a + P * pl + p, dg);
         ld4(a + W * pl + p, aw);
         ld4(a + E * pl + p, ae);
-        ld4(L.b + p, d[0]);
+        if (NPTF > 0) {
+            resid4<T, NPTF>(F, 2 * j, s0, d[0]);
+            st4(const_cast<T*>(L.b) + p, d[0]);
+            if (j + 1 < L.nrow) {
+                T r1[CH];
+                resid4<T, NPTF>(F, 2 * j + 2, s0, r1);
+                st4(const_cast<T*>(L.b) + p + L.ld, r1);
+            }
+        } else {
+            ld4(L.b + p, d[0]);
+        }
         if (!zero_guess) {
             if (j > 0) {
                 T as_[CH], xs[CH];
@@ -498,53 +613,24 @@ __global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong,
     if (cnt > 0) st4(L.x + p, x[0]);
 }
 
-// ---------------------------------------------------------------------------
-// restriction: after the pre-smoother ends with the F rows, the F-row residual
-// vanishes, so R r = residual of the C rows.  One thread per coarse cell.
-// ---------------------------------------------------------------------------
-template <typename T, int NPT>
-__global__ void k_restrict(LevelArgs<T> L, T* __restrict__ bc, int nrowc) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int J = blockIdx.y;
-    if (i >= L.ncol || J >= nrowc) return;
-    const int j = 2 * J, n = L.ncol;
-    const size_t p = (size_t)j * L.ld + i;
-    const T* a = L.a;
-    const size_t pl = L.plane;
-    const T* x = L.x;
-    T r = L.b[p] - a[P * pl + p] * x[p];
-    if (i > 0) r += a[W * pl + p] * x[p - 1];
-    if (i + 1 < n) r += a[E * pl + p] * x[p + 1];
-    if (j > 0) {
-        r += a[S * pl + p] * x[p - L.ld];
-        if (NPT == 9) {
-            if (i > 0) r += a[SW * pl + p] * x[p - L.ld - 1];
-            if (i + 1 < n) r += a[SE * pl + p] * x[p - L.ld + 1];
-        }
-    }
-    if (j + 1 < L.nrow) {
-        r += a[N * pl + p] * x[p + L.ld];
-        if (NPT == 9) {
-            if (i > 0) r += a[NW * pl + p] * x[p + L.ld - 1];
-            if (i + 1 < n) r += a[NE * pl + p] * x[p + L.ld + 1];
-        }
-    }
-    bc[(size_t)J * L.ld + i] = r;
-}
 
 // ---------------------------------------------------------------------------
-// defect correction: x64_out = x64_in + e; r = b - A x64_out with the caller's
-// FP64 coefficients; next cycle's right-hand side b0 = r (precision T).
+// defect correction, iteration it = stat[ST_ITER] + 1: x_it = x_{it-1} + e with
+// x_k in x64[k & 1]; r = b - A x_it with the caller's FP64 coefficients; next
+// cycle's right-hand side b0 = r (precision T).  The last block finishes the
+// FP64 norm, the iteration count, the stopping rule and the loop condition.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_update(const double* __restrict__ aP, const double* __restrict__ aE,
-                         const double* __restrict__ aW, const double* __restrict__ aN,
-                         const double* __restrict__ aS, const double* __restrict__ b,
-                         const unsigned char* __restrict__ mask, int ld_u, int i0, int j0,
-                         int ncol, int nrow, int ldl, const double* __restrict__ xin,
-                         const T* __restrict__ e, double* __restrict__ xout, T* __restrict__ b0,
-                         double* __restrict__ part) {
+__global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask,
+                         int ld_u, int i0, int j0, int ncol, int nrow, int ldl,
+                         double* __restrict__ x64a, double* __restrict__ x64b,
+                         const T* __restrict__ e, T* __restrict__ b0, double* __restrict__ part,
+                         unsigned int* counter, double* __restrict__ stat,
+                         cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ double red[32];
+    const int it = (int)stat[ST_ITER] + 1;
+    const double* __restrict__ xin = (it & 1) ? x64a : x64b;
+    double* __restrict__ xout = (it & 1) ? x64b : x64a;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
     double rr = 0.0;
@@ -554,46 +640,45 @@ __global__ void k_update(const double* __restrict__ aP, const double* __restrict
         double res = 0.0;
         if (mask[p]) {
             const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
-            res = b[q] - aP[q] * xc;
-            if (c + 1 < ncol) res += aE[q] * (xin[p + 1] + (double)e[p + 1]);
-            if (c > 0) res += aW[q] * (xin[p - 1] + (double)e[p - 1]);
-            if (r + 1 < nrow) res += aN[q] * (xin[p + ldl] + (double)e[p + ldl]);
-            if (r > 0) res += aS[q] * (xin[p - ldl] + (double)e[p - ldl]);
+            res = args->b[q] - args->aP[q] * xc;
+            if (c + 1 < ncol) res += args->aE[q] * (xin[p + 1] + (double)e[p + 1]);
+            if (c > 0) res += args->aW[q] * (xin[p - 1] + (double)e[p - 1]);
+            if (r + 1 < nrow) res += args->aN[q] * (xin[p + ldl] + (double)e[p + ldl]);
+            if (r > 0) res += args->aS[q] * (xin[p - ldl] + (double)e[p - ldl]);
         }
         xout[p] = xc;
         b0[p] = (T)res;
         rr = res * res;
     }
-    const double s = block_sum(rr, red);
-    if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = s;
-}
-
-// stat[0] = sum of partials, stat[1] = sqrt(sum)/sqrt(ref) (ref = stat[2] if
-// use_ref else the sum itself), stat[3] = 1 if non-finite
-__global__ void k_finish(const double* __restrict__ part, int n, double* __restrict__ stat,
-                         int store_ref) {
-    __shared__ double red[32];
-    double s = 0.0;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) s += part[k];
-    s = block_sum(s, red);
-    if (threadIdx.x == 0) {
-        stat[0] = s;
-        if (store_ref) stat[2] = s;
-        const double ref = stat[2];
-        stat[1] = (ref > 0.0) ? sqrt(s) / sqrt(ref) : 0.0;
-        stat[3] = isfinite(s) ? 0.0 : 1.0;
+    double tot;
+    if (last_block_sum(rr, part, counter, red, &tot) && threadIdx.x == 0) {
+        const double bb = stat[ST_BB];
+        const double rel = (bb > 0.0) ? sqrt(tot) / sqrt(bb) : 0.0;
+        const bool fin = isfinite(tot);
+        const bool conv = fin && rel < args->tol;
+        const bool keep = fin && !conv && it < args->maxit;
+        stat[ST_RR] = tot;
+        stat[ST_RELRES] = rel;
+        stat[ST_NONFINITE] = fin ? 0.0 : 1.0;
+        stat[ST_ITER] = (double)it;
+        stat[ST_CONV] = conv ? 1.0 : 0.0;
+        stat[ST_KEEP] = keep ? 1.0 : 0.0;
+        if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
     }
 }
 
-// write the accumulated solution into the caller's device-layout array
-__global__ void k_store(const double* __restrict__ x, const unsigned char* __restrict__ mask,
-                        int ncol, int nrow, int ldl, int ld_u, int i0, int j0,
-                        double* __restrict__ out) {
+// write the accumulated solution x64[it & 1] into the caller's solution array
+__global__ void k_store(const SolveArgs* __restrict__ args, const double* __restrict__ x64a,
+                        const double* __restrict__ x64b, const double* __restrict__ stat,
+                        const unsigned char* __restrict__ mask, int ncol, int nrow, int ldl,
+                        int ld_u, int i0, int j0) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
     if (c >= ncol) return;
+    const int it = (int)stat[ST_ITER];
+    const double* __restrict__ x = (it & 1) ? x64b : x64a;
     const size_t p = (size_t)r * ldl + c;
-    if (mask[p]) out[(size_t)(r + j0) * ld_u + (c + i0)] = x[p];
+    if (mask[p]) args->solution[(size_t)(r + j0) * ld_u + (c + i0)] = x[p];
 }
 
 // ---------------------------------------------------------------------------
@@ -651,7 +736,7 @@ static LevelArgs<T> level_args(cth_grid* g, int l) {
     return L;
 }
 
-template <typename T, int NPT>
+template <typename T, int NPT, int NPTF>
 static void launch_relax(cth_grid* g, int l, int parity, int zero_guess, int prolong,
                          cudaStream_t s) {
     const int nr = g->nrow[l];
@@ -668,38 +753,39 @@ static void launch_relax(cth_grid* g, int l, int parity, int zero_guess, int pro
     const size_t smem = line_smem<T>(g->bd, 1);
     LevelArgs<T> L = level_args<T>(g, l);
     // algorithmic bytes: 5 coefficients + b + x written + neighbour-row x, per cell
-    const int slot = (l == 0) ? prof_mark(g, PROF_RELAX0, (double)rows * g->ncol * 8.0 * sizeof(T), s) : -1;
-    k_relax<T, NPT><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa);
+    LevelArgs<T> F = L;
+    if (NPTF > 0) F = level_args<T>(g, l - 1);
+    int slot = -1;
+    if (l == 0) slot = prof_mark(g, PROF_RELAX0, (double)rows * g->ncol * 8.0 * sizeof(T), s);
+    else if (l == 1 && NPTF > 0)
+        slot = prof_mark(g, PROF_RESTRICT0, (double)g->nrow[1] * g->ncol * (9.0 + 8.0) * sizeof(T), s);
+    k_relax<T, NPT, NPTF><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa, F);
     g->launches++;
     if (slot >= 0) prof_done(g, slot, s);
 }
 
 template <typename T>
-static void relax(cth_grid* g, int l, int parity, int zero_guess, int prolong, cudaStream_t s) {
-    if (l == 0) launch_relax<T, 5>(g, l, parity, zero_guess, prolong, s);
-    else launch_relax<T, 9>(g, l, parity, zero_guess, prolong, s);
+static void relax(cth_grid* g, int l, int parity, int zero_guess, int prolong, cudaStream_t s,
+                  bool restrict_from_finer = false) {
+    if (l == 0) launch_relax<T, 5, 0>(g, l, parity, zero_guess, prolong, s);
+    else if (!restrict_from_finer) launch_relax<T, 9, 0>(g, l, parity, zero_guess, prolong, s);
+    else if (l == 1) launch_relax<T, 9, 5>(g, l, parity, 1, 0, s);
+    else launch_relax<T, 9, 9>(g, l, parity, 1, 0, s);
 }
 
+// V(nu1, nu2) cycle on level l.  The first C-row relaxation of every coarse
+// level computes its right-hand side by restricting the finer residual.
 template <typename T>
 static void vcycle(cth_grid* g, int l, cudaStream_t s) {
+    const bool fused = l > 0;
     if (l == g->nlev - 1) {
-        relax<T>(g, l, 0, 1, 0, s);
+        relax<T>(g, l, 0, 1, 0, s, fused);
         if (g->nrow[l] > 1) relax<T>(g, l, 1, 0, 0, s);
         return;
     }
     for (int k = 0; k < g->nu1; k++) {
-        relax<T>(g, l, 0, k == 0, 0, s);
+        relax<T>(g, l, 0, k == 0, 0, s, fused && k == 0);
         relax<T>(g, l, 1, 0, 0, s);
-    }
-    {
-        LevelArgs<T> L = level_args<T>(g, l);
-        Hierarchy<T>& h = hier<T>(g);
-        dim3 blk(256), grd((g->ncol + 255) / 256, g->nrow[l + 1]);
-        const int slot = (l == 0) ? prof_mark(g, PROF_RESTRICT0, (double)g->nrow[1] * g->ncol * 9.0 * sizeof(T), s) : -1;
-        if (l == 0) k_restrict<T, 5><<<grd, blk, 0, s>>>(L, h.b[l + 1], g->nrow[l + 1]);
-        else k_restrict<T, 9><<<grd, blk, 0, s>>>(L, h.b[l + 1], g->nrow[l + 1]);
-        g->launches++;
-        if (slot >= 0) prof_done(g, slot, s);
     }
     vcycle<T>(g, l + 1, s);
     for (int k = 0; k < g->nu2; k++) {
@@ -733,77 +819,160 @@ static void setup_levels(cth_grid* g, cudaStream_t s) {
     prof_done(g, slot, s);
 }
 
+// kernel sequence of one solve, split into the part before the cycle loop,
+// one loop iteration, and the part after it; each returns its kernel count
 template <typename T>
-static int solve_impl(cth_grid* g, const double* aP, const double* aE, const double* aW,
-                      const double* aN, const double* aS, const double* b, int maxITR,
-                      double tol, double* solution, cudaStream_t s, cth_status* st) {
-    int rc = alloc_hierarchy<T>(g);
-    if (rc != CTH_OK) return rc;
+static int enqueue_pre(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle cond, int use_cond) {
     Hierarchy<T>& h = hier<T>(g);
     Workspace& w = g->ws;
     const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
     dim3 blk(256), grd((ncol + 255) / 256, nrow0);
-    const int npart = grd.x * grd.y;
-    if (npart > w.npart) {
-        set_error("partial-sum buffer too small");
-        return CTH_ERR_ALLOC;
-    }
-    k_prep0<T><<<grd, blk, 0, s>>>(aP, aE, aW, aN, aS, b, g->mask[0], g->ld, g->i0, g->j0, ncol,
-                                   nrow0, ldl, h.a[0], h.b[0], w.part);
-    k_finish<<<1, 1024, 0, s>>>(w.part, npart, w.stat, 1);
-    g->launches += 2;
+    k_prep0<T><<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, h.a[0],
+                                   h.b[0], w.part, w.counter, w.stat, cond, use_cond);
+    const long long l0 = g->launches;
     setup_levels<T>(g, s);
-    CTH_CUDA(cudaMemsetAsync(w.x64[0], 0, sizeof(double) * (size_t)nrow0 * ldl, s));
-    CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CTH_CUDA(cudaStreamSynchronize(s));
-    CTH_CUDA(cudaGetLastError());
-    const double bb = w.h_stat[0];
-    cth_status loc{};
-    loc.initial_residual = std::sqrt(bb);
-    int cur = 0;
-    int result = CTH_NOT_CONVERGED;
-    if (!std::isfinite(bb)) {
-        loc.nonfinite = 1;
-        result = CTH_NONFINITE;
-    } else if (bb == 0.0) {
-        loc.converged = 1;
-        result = CTH_OK;
-    } else {
-        for (int it = 1; it <= maxITR; it++) {
-            vcycle<T>(g, 0, s);
-            const int slot = prof_mark(g, PROF_UPDATE,
-                                       (double)nrow0 * ncol * (8.0 * 8.0 + 2.0 * sizeof(T) + 1.0), s);
-            k_update<T><<<grd, blk, 0, s>>>(aP, aE, aW, aN, aS, b, g->mask[0], g->ld, g->i0, g->j0,
-                                            ncol, nrow0, ldl, w.x64[cur], h.x[0], w.x64[1 - cur],
-                                            h.b[0], w.part);
-            prof_done(g, slot, s);
-            k_finish<<<1, 1024, 0, s>>>(w.part, npart, w.stat, 0);
-            g->launches += 2;
-            cur = 1 - cur;
-            CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
-            CTH_CUDA(cudaStreamSynchronize(s));
-            loc.iterations = it;
-            loc.residual = w.h_stat[1];
-            if (w.h_stat[3] != 0.0 || !std::isfinite(loc.residual)) {
-                loc.nonfinite = 1;
-                result = CTH_NONFINITE;
-                break;
-            }
-            if (loc.residual < tol) {
-                loc.converged = 1;
-                result = CTH_OK;
-                break;
-            }
+    const int n = 1 + (int)(g->launches - l0);
+    g->launches = l0;
+    cudaMemsetAsync(w.x64[0], 0, sizeof(double) * (size_t)nrow0 * ldl, s);
+    return n;
+}
+
+template <typename T>
+static int enqueue_body(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle cond, int use_cond) {
+    Hierarchy<T>& h = hier<T>(g);
+    Workspace& w = g->ws;
+    const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
+    dim3 blk(256), grd((ncol + 255) / 256, nrow0);
+    const long long l0 = g->launches;
+    vcycle<T>(g, 0, s);
+    const int slot = prof_mark(g, PROF_UPDATE, (double)nrow0 * ncol * (8.0 * 8.0 + 2.0 * sizeof(T) + 1.0), s);
+    k_update<T><<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, w.x64[0],
+                                    w.x64[1], h.x[0], h.b[0], w.part, w.counter, w.stat, cond, use_cond);
+    prof_done(g, slot, s);
+    const int n = 1 + (int)(g->launches - l0);
+    g->launches = l0;
+    return n;
+}
+
+static int enqueue_post(cth_grid* g, cudaStream_t s) {
+    Workspace& w = g->ws;
+    dim3 blk(256), grd((g->ncol + 255) / 256, g->nrow[0]);
+    k_store<<<grd, blk, 0, s>>>(w.d_args, w.x64[0], w.x64[1], w.stat, g->mask[0], g->ncol, g->nrow[0],
+                                g->ldl, g->ld, g->i0, g->j0);
+    return 1;
+}
+
+// capture the whole solve as one graph: pre -> while(keep){ body } -> post
+template <typename T>
+static int build_graph(cth_grid* g, SolveGraph& G) {
+    if (G.valid && G.nu1 == g->nu1 && G.nu2 == g->nu2) return CTH_OK;
+    if (G.exec) { cudaGraphExecDestroy(G.exec); G.exec = nullptr; }
+    if (G.graph) { cudaGraphDestroy(G.graph); G.graph = nullptr; }
+    G.valid = false;
+    cudaStream_t cs = g->cap[0], cs2 = g->cap[1];
+    CTH_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps);
+    cudaGraphConditionalHandle cond = 0;
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) {
+        cudaGraph_t junk;
+        cudaStreamEndCapture(cs, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        return cuda_fail(e, "graph conditional handle");
+    }
+    G.n_pre = enqueue_pre<T>(g, cs, cond, 1);
+    e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps);
+    cudaGraphNode_t cnode = nullptr;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, deps, ndeps, &cp);
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(cs2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            G.n_body = enqueue_body<T>(g, cs2, cond, 1);
+            cudaGraph_t bout = nullptr;
+            e = cudaStreamEndCapture(cs2, &bout);
         }
     }
-    k_store<<<grd, blk, 0, s>>>(w.x64[cur], g->mask[0], ncol, nrow0, ldl, g->ld, g->i0, g->j0,
-                                solution);
-    g->launches++;
+    if (e == cudaSuccess) G.n_post = enqueue_post(g, cs);
+    cudaGraph_t out = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(cs, &out);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&G.exec, out, 0);
+    if (e != cudaSuccess) {
+        if (out) cudaGraphDestroy(out);
+        cudaGetLastError();
+        return cuda_fail(e, "solve graph capture");
+    }
+    G.graph = out;
+    G.nu1 = g->nu1;
+    G.nu2 = g->nu2;
+    G.valid = true;
+    return CTH_OK;
+}
+
+template <typename T>
+static int solve_impl(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                      const double* aN, const double* aS, const double* b, int maxITR,
+                      double tol, double* solution, cudaStream_t s, cth_status* st, int prec) {
+    int rc = alloc_hierarchy<T>(g);
+    if (rc != CTH_OK) return rc;
+    Workspace& w = g->ws;
+    {
+        dim3 grd((g->ncol + 255) / 256, g->nrow[0]);
+        if ((int)(grd.x * grd.y) > w.npart) {
+            set_error("partial-sum buffer too small");
+            return CTH_ERR_ALLOC;
+        }
+    }
+    SolveArgs* ha = w.h_args;
+    ha->aP = aP; ha->aE = aE; ha->aW = aW; ha->aN = aN; ha->aS = aS; ha->b = b;
+    ha->solution = solution;
+    ha->tol = tol;
+    ha->maxit = maxITR;
+    CTH_CUDA(cudaMemcpyAsync(w.d_args, ha, sizeof(SolveArgs), cudaMemcpyHostToDevice, s));
+    const bool graph = g->use_graphs && !g->prof.on;
+    if (graph) {
+        SolveGraph& G = g->graphs[prec];
+        rc = build_graph<T>(g, G);
+        if (rc != CTH_OK) return rc;
+        CTH_CUDA(cudaGraphLaunch(G.exec, s));
+        CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CTH_CUDA(cudaStreamSynchronize(s));
+        g->launches += G.n_pre + (long long)G.n_body * (long long)w.h_stat[ST_ITER] + G.n_post;
+    } else {
+        g->launches += enqueue_pre<T>(g, s, 0, 0);
+        CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CTH_CUDA(cudaStreamSynchronize(s));
+        while (w.h_stat[ST_KEEP] != 0.0) {
+            g->launches += enqueue_body<T>(g, s, 0, 0);
+            CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CTH_CUDA(cudaStreamSynchronize(s));
+        }
+        g->launches += enqueue_post(g, s);
+        CTH_CUDA(cudaGetLastError());
+        CTH_CUDA(cudaStreamSynchronize(s));
+        prof_collect(g);
+    }
     CTH_CUDA(cudaGetLastError());
-    CTH_CUDA(cudaStreamSynchronize(s));
-    prof_collect(g);
+    cth_status loc{};
+    loc.initial_residual = std::sqrt(w.h_stat[ST_BB]);
+    loc.iterations = (int)w.h_stat[ST_ITER];
+    loc.residual = w.h_stat[ST_RELRES];
+    loc.nonfinite = w.h_stat[ST_NONFINITE] != 0.0;
+    loc.converged = w.h_stat[ST_CONV] != 0.0;
     if (st) *st = loc;
-    return result;
+    if (loc.nonfinite) return CTH_NONFINITE;
+    return loc.converged ? CTH_OK : CTH_NOT_CONVERGED;
 }
 
 int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
@@ -811,9 +980,9 @@ int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double*
                   double error_cnv, int precision, double* solution, cudaStream_t s,
                   cth_status* st) {
     if (precision == CTH_PREC_MIXED)
-        return solve_impl<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, st);
+        return solve_impl<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, st, precision);
     if (precision == CTH_PREC_FP64)
-        return solve_impl<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, st);
+        return solve_impl<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, st, precision);
     set_error("unknown precision mode");
     return CTH_ERR_ARG;
 }
@@ -828,11 +997,13 @@ int configure_kernels(cth_grid* g) {
     }
 #define CTH_ATTR(K, BYTES) CTH_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, BYTES))
     if (smem64 > 48 * 1024) {
-        CTH_ATTR((k_relax<double, 5>), smem64); CTH_ATTR((k_relax<double, 9>), smem64);
+        CTH_ATTR((k_relax<double, 5, 0>), smem64); CTH_ATTR((k_relax<double, 9, 0>), smem64);
+        CTH_ATTR((k_relax<double, 9, 5>), smem64); CTH_ATTR((k_relax<double, 9, 9>), smem64);
         CTH_ATTR((k_weights<double, 5>), smem64); CTH_ATTR((k_weights<double, 9>), smem64);
     }
     if (smem32 > 48 * 1024) {
-        CTH_ATTR((k_relax<float, 5>), smem32); CTH_ATTR((k_relax<float, 9>), smem32);
+        CTH_ATTR((k_relax<float, 5, 0>), smem32); CTH_ATTR((k_relax<float, 9, 0>), smem32);
+        CTH_ATTR((k_relax<float, 9, 5>), smem32); CTH_ATTR((k_relax<float, 9, 9>), smem32);
         CTH_ATTR((k_weights<float, 5>), smem32); CTH_ATTR((k_weights<float, 9>), smem32);
     }
 #undef CTH_ATTR

@@ -91,6 +91,9 @@ class Grid:
                    allow_positive=False)
         return ms.value, n.value, by.value
 
+    def set_graphs(self, enable: bool):
+        capi.check(self._L.cth_grid_set_graphs(self._h, int(enable)), allow_positive=False)
+
     def set_cycle(self, nu_pre: int, nu_post: int):
         capi.check(self._L.cth_grid_set_cycle(self._h, nu_pre, nu_post), allow_positive=False)
 

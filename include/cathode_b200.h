@@ -78,6 +78,11 @@ int cth_grid_ld(const cth_grid* g);
 int cth_grid_levels(const cth_grid* g);
 /* set smoothing sweeps per level (pre, post; default 1, 1) */
 int cth_grid_set_cycle(cth_grid* g, int nu_pre, int nu_post);
+/* enable (default) or disable running each SMG-replacement solve as one
+ * captured CUDA graph whose cycle loop is a device-side conditional node; when
+ * disabled, or while profiling is on, kernels are launched one by one and the
+ * host tests convergence after every cycle.  Results are identical. */
+int cth_grid_set_graphs(cth_grid* g, int enable);
 
 /* Instrumentation ------------------------------------------------------------
  * cth_launch_count: kernels this grid has launched since creation.
@@ -111,8 +116,8 @@ int cth_smg_solve(cth_grid* g, const double* aP, const double* aE, const double*
  * Same contract on device-resident planes.  All pointers are device pointers
  * in the layout above; `solution` grid cells are written, other cells are left
  * untouched.  `stream` is a cudaStream_t (NULL = legacy default stream).  The
- * call returns after the solve completes on `stream` (the convergence test
- * reads a 40-byte status per cycle). */
+ * call returns after the solve completes on `stream`.  Calls on one grid must
+ * not overlap (the grid's workspace is shared). */
 int cth_smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
                       const double* aN, const double* aS, const double* b, int maxITR,
                       double error_cnv, int precision, double* solution, void* stream,
