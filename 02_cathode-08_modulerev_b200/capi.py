@@ -30,6 +30,7 @@ EXPORTS = (
     "cth_grid_levels", "cth_grid_set_cycle", "cth_smg_solve", "cth_smg_solve_dev", "cth_sor_solve",
     "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
     "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs",
+    "cth_c5_solve", "cth_c5_solve_dev",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -83,6 +84,11 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_grid_ld.restype = ctypes.c_int
     L.cth_grid_levels.argtypes = [_vp]
     L.cth_grid_levels.restype = ctypes.c_int
+    L.cth_c5_solve.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_int, ctypes.c_double, _vp, ctypes.POINTER(Status)]
+    L.cth_c5_solve.restype = ctypes.c_int
+    L.cth_c5_solve_dev.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_int, ctypes.c_double, _vp, _vp,
+                                                       ctypes.POINTER(Status)]
+    L.cth_c5_solve_dev.restype = ctypes.c_int
     L.cth_grid_set_graphs.argtypes = [_vp, ctypes.c_int]
     L.cth_grid_set_graphs.restype = ctypes.c_int
     L.cth_grid_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]

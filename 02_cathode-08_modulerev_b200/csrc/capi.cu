@@ -53,6 +53,37 @@ __global__ void k_dev_to_ij(const double* __restrict__ src, double* __restrict__
     }
 }
 
+// complex (16-byte) element versions
+__global__ void k_ij_to_dev_c(const double2* __restrict__ src, double2* __restrict__ dst, int ni2, int nj2,
+                              int ld) {
+    __shared__ double2 tile[32][33];
+    const int j0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int i = i0 + k, j = j0 + threadIdx.x;
+        if (i < ni2 && j < nj2) tile[k][threadIdx.x] = src[(size_t)i * nj2 + j];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int j = j0 + k, i = i0 + threadIdx.x;
+        if (i < ni2 && j < nj2) dst[(size_t)j * ld + i] = tile[threadIdx.x][k];
+    }
+}
+
+__global__ void k_dev_to_ij_c(const double2* __restrict__ src, double2* __restrict__ dst, int ni2, int nj2,
+                              int ld) {
+    __shared__ double2 tile[32][33];
+    const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int j = j0 + k, i = i0 + threadIdx.x;
+        if (i < ni2 && j < nj2) tile[k][threadIdx.x] = src[(size_t)j * ld + i];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int i = i0 + k, j = j0 + threadIdx.x;
+        if (i < ni2 && j < nj2) dst[(size_t)i * nj2 + j] = tile[threadIdx.x][k];
+    }
+}
+
 int to_device_layout(cth_grid* g, const double* src, double* dst, cudaStream_t s) {
     dim3 blk(32, 8), grd((g->nj + 2 + 31) / 32, (g->ni + 2 + 31) / 32);
     k_ij_to_dev<<<grd, blk, 0, s>>>(src, dst, g->ni + 2, g->nj + 2, g->ld);
@@ -135,6 +166,13 @@ static void free_grid(cth_grid* g) {
     if (g->ws.h_args) cudaFreeHost(g->ws.h_args);
     fr(g->ws.d_args);
     fr(g->ws.counter);
+    fr(g->c5.buf);
+    fr(g->c5.sc);
+    fr(g->c5.part);
+    fr(g->c5.cstage);
+    fr(g->c5.cstage_ij);
+    if (g->c5graph.exec) cudaGraphExecDestroy(g->c5graph.exec);
+    if (g->c5graph.graph) cudaGraphDestroy(g->c5graph.graph);
     for (auto& G : g->graphs) {
         if (G.exec) cudaGraphExecDestroy(G.exec);
         if (G.graph) cudaGraphDestroy(G.graph);
@@ -259,6 +297,7 @@ int cth_grid_create(int ni, int nj, const int* i_bl, const int* j_bl, int n_bl, 
     if (rc == CTH_OK) chk(cudaStreamCreateWithFlags(&g->cap[0], cudaStreamNonBlocking), "capture stream");
     if (rc == CTH_OK) chk(cudaStreamCreateWithFlags(&g->cap[1], cudaStreamNonBlocking), "capture stream");
     if (rc == CTH_OK) rc = configure_kernels(g);
+    if (rc == CTH_OK) rc = c5_configure(g);
     if (rc != CTH_OK) {
         free_grid(g);
         return rc;
@@ -410,6 +449,60 @@ int cth_sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const dou
     CTH_CUDA(cudaSetDevice(g->device));
     return sor_solve_dev(g, aP, aE, aW, aN, aS, b, alpha_SOR, maxITR, error_cnv, solution,
                          (cudaStream_t)stream, st);
+}
+
+int cth_c5_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                     const double* aN, const double* aS, const double* b, int maxITR, double tol,
+                     double* solution, void* stream, cth_status* st) {
+    if (!g || !aP || !aE || !aW || !aN || !aS || !b || !solution || maxITR < 0) {
+        set_error("cth_c5_solve_dev: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    return c5_solve_dev(g, aP, aE, aW, aN, aS, b, maxITR, tol, solution, (cudaStream_t)stream, st);
+}
+
+int cth_c5_solve(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
+                 const double* aS, const double* b, int maxITR, double tol, double* solution,
+                 cth_status* st) {
+    if (!g || !aP || !aE || !aW || !aN || !aS || !b || !solution || maxITR < 0) {
+        set_error("cth_c5_solve: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    C5Work& c = g->c5;
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    if (!c.cstage) {
+        CTH_CUDA(cudaMalloc(&c.cstage, 7 * g->plane * 2 * sizeof(double)));
+        CTH_CUDA(cudaMemset(c.cstage, 0, 7 * g->plane * 2 * sizeof(double)));
+        CTH_CUDA(cudaMalloc(&c.cstage_ij, nij * 2 * sizeof(double)));
+    }
+    const double* src[6] = {aP, aE, aW, aN, aS, b};
+    dim3 blk(32, 8), g1((g->nj + 2 + 31) / 32, (g->ni + 2 + 31) / 32), g2((g->ni + 2 + 31) / 32, (g->nj + 2 + 31) / 32);
+    for (int k = 0; k < 6; k++) {
+        CTH_CUDA(cudaMemcpyAsync(c.cstage_ij, src[k], nij * 2 * sizeof(double), cudaMemcpyHostToDevice, g->stream));
+        k_ij_to_dev_c<<<g1, blk, 0, g->stream>>>(reinterpret_cast<const double2*>(c.cstage_ij),
+                                                 reinterpret_cast<double2*>(c.cstage + k * g->plane * 2),
+                                                 g->ni + 2, g->nj + 2, g->ld);
+    }
+    double* base = c.cstage;
+    const size_t pl = g->plane * 2;
+    int res = c5_solve_dev(g, base, base + pl, base + 2 * pl, base + 3 * pl, base + 4 * pl, base + 5 * pl,
+                           maxITR, tol, base + 6 * pl, g->stream, st);
+    if (res < 0) return res;
+    k_dev_to_ij_c<<<g2, blk, 0, g->stream>>>(reinterpret_cast<const double2*>(base + 6 * pl),
+                                             reinterpret_cast<double2*>(c.cstage_ij), g->ni + 2, g->nj + 2, g->ld);
+    std::vector<double> tmp(nij * 2);
+    CTH_CUDA(cudaMemcpyAsync(tmp.data(), c.cstage_ij, nij * 2 * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
+    CTH_CUDA(cudaStreamSynchronize(g->stream));
+    const int nj2 = g->nj + 2;
+    for (int bl = 0; bl < g->n_bl; bl++)
+        for (int i = std::max(0, g->ibl[2 * bl]); i <= std::min(g->ni + 1, g->ibl[2 * bl + 1]); i++)
+            for (int j = std::max(0, g->jbl[2 * bl]); j <= std::min(g->nj + 1, g->jbl[2 * bl + 1]); j++) {
+                solution[2 * ((size_t)i * nj2 + j)] = tmp[2 * ((size_t)i * nj2 + j)];
+                solution[2 * ((size_t)i * nj2 + j) + 1] = tmp[2 * ((size_t)i * nj2 + j) + 1];
+            }
+    return res;
 }
 
 int cth_residual_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,

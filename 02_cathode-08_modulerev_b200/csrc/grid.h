@@ -19,6 +19,28 @@
 
 namespace cth {
 
+// complex double of the frequency-domain solves; interleaved (re, im) in memory
+struct cd {
+    double x, y;
+    __host__ __device__ cd() : x(0.0), y(0.0) {}
+    __host__ __device__ cd(double r) : x(r), y(0.0) {}
+    __host__ __device__ cd(double r, double i) : x(r), y(i) {}
+};
+__host__ __device__ inline cd operator+(cd a, cd b) { return cd(a.x + b.x, a.y + b.y); }
+__host__ __device__ inline cd operator-(cd a, cd b) { return cd(a.x - b.x, a.y - b.y); }
+__host__ __device__ inline cd operator-(cd a) { return cd(-a.x, -a.y); }
+__host__ __device__ inline cd operator*(cd a, cd b) { return cd(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__host__ __device__ inline cd& operator+=(cd& a, cd b) { a.x += b.x; a.y += b.y; return a; }
+__host__ __device__ inline cd& operator-=(cd& a, cd b) { a.x -= b.x; a.y -= b.y; return a; }
+__host__ __device__ inline bool operator==(cd a, cd b) { return a.x == b.x && a.y == b.y; }
+__host__ __device__ inline bool operator!=(cd a, cd b) { return !(a == b); }
+__host__ __device__ inline cd conj(cd a) { return cd(a.x, -a.y); }
+__host__ __device__ inline double abs2(cd a) { return a.x * a.x + a.y * a.y; }
+__host__ __device__ inline cd cdiv(cd a, cd b) {
+    const double s = 1.0 / (b.x * b.x + b.y * b.y);
+    return cd((a.x * b.x + a.y * b.y) * s, (a.y * b.x - a.x * b.y) * s);
+}
+
 // stencil slots: level 0 stores the first 5, coarse levels all 9.
 // Convention of the reference: (A x)_P = a[P] x_P - sum_k a[k] x_k.
 enum Slot { P = 0, W = 1, E = 2, S = 3, N = 4, SW = 5, SE = 6, NW = 7, NE = 8 };
@@ -73,6 +95,16 @@ struct SolveGraph {
     int n_pre = 0, n_body = 0, n_post = 0;  // kernels per section
 };
 
+// complex 5-point solver workspace (level-0 layout, 14 complex planes)
+struct C5Work {
+    void* buf = nullptr;      // 9 planes of complex doubles (Krylov vectors)
+    double* sc = nullptr;     // recurrence scalars
+    double* part = nullptr;   // reduction partials
+    int npart = 0;
+    double* cstage = nullptr;     // host-API staging: 7 complex planes in device layout
+    double* cstage_ij = nullptr;  // one complex [i][j] array
+};
+
 struct Workspace {
     double* x64[2] = {nullptr, nullptr};  // level-0 layout accumulated solution
     double* part = nullptr;               // per-block partial sums
@@ -111,6 +143,9 @@ struct cth_grid {
     long long launches = 0;    // kernels launched by this grid since creation
     cth::Profiler prof;
     cth::SolveGraph graphs[2]; // per precision (CTH_PREC_FP64, CTH_PREC_MIXED)
+    cth::C5Work c5;
+    cth::Hierarchy<cth::cd> hc;    // complex hierarchy (preconditioner of the complex solves)
+    cth::SolveGraph c5graph;
     cudaStream_t cap[2] = {nullptr, nullptr};  // capture streams
     bool use_graphs = true;
 };
@@ -138,6 +173,10 @@ int prof_mark(cth_grid* g, int c, double bytes, cudaStream_t s);
 void prof_done(cth_grid* g, int slot, cudaStream_t s);
 void prof_collect(cth_grid* g);
 int from_device_layout(cth_grid* g, const double* src, double* dst_ij_dev, cudaStream_t s);
+int c5_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
+                 const double* aS, const double* b, int maxit, double tol, double* solution, cudaStream_t s,
+                 cth_status* st);
+int c5_configure(cth_grid* g);
 }  // namespace cth
 
 #define CTH_CUDA(call)                                        \

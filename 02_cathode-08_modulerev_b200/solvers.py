@@ -124,6 +124,35 @@ class Grid:
         capi.check(rc)
         return st
 
+    def c5_solve(self, aP, aE, aW, aN, aS, b, solution, maxITR=500, error_cnv=1e-10) -> capi.Status:
+        """Complex 5-point solve (host complex128 (ni+2, nj+2) arrays, [i][j])."""
+        ni, nj = self.ni, self.nj
+        arrs = []
+        for a, n in zip((aP, aE, aW, aN, aS, b), "aP aE aW aN aS b".split()):
+            a = np.asarray(a)
+            if a.shape != (ni + 2, nj + 2):
+                raise ValueError(f"{n}: expected shape {(ni + 2, nj + 2)}")
+            arrs.append(np.ascontiguousarray(a, dtype=np.complex128))
+        if not (isinstance(solution, np.ndarray) and solution.dtype == np.complex128 and
+                solution.flags.c_contiguous and solution.shape == (ni + 2, nj + 2)):
+            raise ValueError("solution must be a C-contiguous complex128 (ni+2, nj+2) array")
+        st = capi.Status()
+        rc = self._L.cth_c5_solve(self._h, *[a.ctypes.data for a in arrs], maxITR, error_cnv,
+                                  solution.ctypes.data, ctypes.byref(st))
+        capi.check(rc)
+        return st
+
+    def c5_solve_dev(self, aP, aE, aW, aN, aS, b, solution, maxITR=500, error_cnv=1e-10,
+                     stream=None) -> capi.Status:
+        """Complex 5-point solve on device planes (torch complex128, shape (nj+2, ld))."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        st = capi.Status()
+        rc = self._L.cth_c5_solve_dev(self._h, *[_ptr(a) for a in (aP, aE, aW, aN, aS, b)], maxITR,
+                                      error_cnv, _ptr(solution), s.cuda_stream, ctypes.byref(st))
+        capi.check(rc)
+        return st
+
     # -- device-resident path (library layout) -----------------------------
     def device_plane(self, n: int = 1):
         """Zeroed float64 device planes of the library layout, shape (n, nj+2, ld)."""

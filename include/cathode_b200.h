@@ -140,6 +140,26 @@ int cth_sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const dou
                       int maxITR, double error_cnv, double* solution, void* stream,
                       cth_status* st);
 
+/* Complex 5-point solve (frequency-domain microwave systems) -----------------
+ * Replaces the direct sparse factorisation of the reference's complex field
+ * systems (Eigen SparseLU, include/emfieldModule.hpp:2995-2998 in
+ * solve_Microwave, :5780-5783 in solve_Microwave_impedanceTest): solves
+ *     aP x_P - aE x_E - aW x_W - aN x_N - aS x_S = b
+ * on the block union (the field's unknowns; couplings to other cells dropped,
+ * as the Eigen assembly inserts only unknown-to-unknown entries) by BiCGStab
+ * in complex FP64, preconditioned with exact complex z-line solves, from a zero
+ * guess until ||r||_2/||b||_2 < tol or maxITR iterations.  Complex arrays are
+ * interleaved (re, im) doubles: host arrays [i][j] of (ni+2)*(nj+2) complex
+ * values, device arrays planes of (nj+2)*ld complex values, element (i,j) at
+ * 2*(j*ld+i).  Only grid cells of `solution` are written.  `st->iterations`
+ * counts BiCGStab iterations (two preconditioned products each). */
+int cth_c5_solve(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
+                 const double* aS, const double* b, int maxITR, double tol, double* solution,
+                 cth_status* st);
+int cth_c5_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                     const double* aN, const double* aS, const double* b, int maxITR, double tol,
+                     double* solution, void* stream, cth_status* st);
+
 /* Residual (device arrays): r = b - A x on grid cells (couplings to non-grid
  * cells dropped), r = 0 elsewhere; *rnorm = ||r||_2, *bnorm = ||b||_2 over grid
  * cells (either may be NULL). */

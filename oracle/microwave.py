@@ -1,0 +1,208 @@
+"""CPU restatement of the reference's microwave (frequency-domain) solve.
+
+TEST INFRASTRUCTURE ONLY (checker and CPU baseline; the product never imports it).
+
+Restated here:
+  * the coax impedance test, EmfieldModule::solve_Microwave_impedanceTest
+    (include/emfieldModule.hpp:5528-6099) on the boundary lists of
+    InitialModule::makeBoundary_impedanceTest (include/initialModule.hpp:1061-1330):
+    Er-only 5-point complex system, port excitation (code 7) at z=0, first-order
+    open boundary (code 1) at z=L, Gauss-law walls (code 2) at r=r1 and r=r2,
+    direct sparse solve (Eigen SparseLU in the reference, SuperLU here: the same
+    supernodal-LU family), ghost post-processing, port V/I, forward power and the
+    rescaling to Pmw;
+  * the cell-centred output of OutputModule::output_phase
+    (include/outputModule.hpp:81-83 for Er, :136-139 for the analytic TEM field).
+Arrays follow the reference: (ni+2, nj+2) complex128, [i][j], Er at r-faces j-1/2.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+E0 = 1.60217662e-19
+EPS0 = 8.8541878128e-12
+MU0 = 1.2566370614e-6
+
+
+def coax_params() -> dict:
+    """Parameters of the reference calibration run (test/校正/setup.yaml)."""
+    ni, nj = 194, 7
+    xL, xR, rmin, rmax = 0.0, 0.0388, 0.0006, 0.002
+    fmw = 4.25e9
+    p = dict(ni=ni, nj=nj, xL=xL, xR=xR, rmin=rmin, rmax=rmax, fmw=fmw, Pmw=8.0, Z0=50.0,
+             J1r_exc=0.212687, epsr_diele=2.083825280349, nu_eff=2.0e9, masse=9.10938356e-31)
+    # iniParam (initialModule.hpp:54-84)
+    p["dx"] = (xR - xL) / ni
+    p["dr"] = (rmax - rmin) / nj
+    p["omegam"] = 2.0 * np.pi * fmw
+    p["x"] = xL + (np.arange(ni + 2) - 0.5) * p["dx"]
+    p["r"] = rmin + (np.arange(nj + 2) - 0.5) * p["dr"]
+    # makeBoundary_impedanceTest: r1 = rmin, r2 = rmax, Er faces i=1..ni, j=2..nj,
+    # epsr = epsr_diele in the cells (initialModule.hpp:1068-1072, :1090-1093, :1320-1325)
+    p["r1"], p["r2"] = rmin, rmax
+    epsr = np.ones((ni + 2, nj + 2))
+    epsr[1:ni + 1, 1:nj + 1] = p["epsr_diele"]
+    p["epsr"] = epsr
+    return p
+
+
+def coax_er_system(p: dict):
+    """Er coefficients of solve_Microwave_impedanceTest after the BC surgery.
+
+    Returns dict with complex (ni+2, nj+2) arrays aP, aE, aW, aN, aS, b and the
+    unknown mask (Er faces i=1..ni, j=2..nj).  Stencil convention as the
+    reference: aP x_P - aE x_E - aW x_W - aN x_N - aS x_S = b.
+    """
+    ni, nj, dx, dr, w = p["ni"], p["nj"], p["dx"], p["dr"], p["omegam"]
+    r, epsr = p["r"], p["epsr"]
+    shape = (ni + 2, nj + 2)
+    aP = np.zeros(shape, complex); aE = np.zeros(shape, complex); aW = np.zeros(shape, complex)
+    aN = np.zeros(shape, complex); aS = np.zeros(shape, complex); b = np.zeros(shape, complex)
+    mask = np.zeros(shape, bool)
+    # rho = 0 in the test (emfieldModule.hpp:5531-5536): sigma = 0
+    for i in range(1, ni + 1):
+        for j in range(2, nj + 1):
+            rC = (r[j - 1] + r[j]) / 2.0
+            rR = (r[j] + r[j + 1]) / 2.0
+            rL = (r[j - 2] + r[j - 1]) / 2.0
+            eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+            aP[i, j] = (rC * (1.0 / r[j] + 1.0 / r[j - 1]) * dx * dx + 2.0 * dr * dr
+                        - EPS0 * eps_t * MU0 * w * w * dx * dx * dr * dr)
+            aE[i, j] = dr * dr
+            aW[i, j] = dr * dr
+            aN[i, j] = rR / r[j] * dx * dx
+            aS[i, j] = rL / r[j - 1] * dx * dx
+            mask[i, j] = True
+    # left (code 7, excitation), emfieldModule.hpp:5616-5633
+    for j in range(2, nj + 1):
+        i = 1
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        c0 = np.sqrt(1.0 / (EPS0 * eps_t * MU0))
+        deno = complex(2.0 * c0, w * dx)
+        R = complex(2.0 * c0, -w * dx)
+        r_t = (r[j] + r[j - 1]) / 2.0
+        Er_Fw = p["J1r_exc"] / r_t / np.log(p["r2"] / p["r1"]) * 1e3
+        S = complex(0.0, 4.0 * w * dx) * Er_Fw
+        aP[i, j] = aP[i, j] - aW[i, j] * R / (deno + 1e-100)
+        b[i, j] = b[i, j] + aW[i, j] * S / (deno + 1e-100)
+        aW[i, j] = 0.0
+    # right (code 1, open), emfieldModule.hpp:5642-5657
+    for j in range(2, nj + 1):
+        i = ni
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        c0 = np.sqrt(1.0 / (EPS0 * eps_t * MU0))
+        deno = (2.0 * c0) ** 2 + (w * dx) ** 2
+        R = complex((2.0 * c0) ** 2 - (w * dx) ** 2, -4.0 * c0 * w * dx)
+        aP[i, j] = aP[i, j] - aE[i, j] * R / (deno + 1e-100)
+        aE[i, j] = 0.0
+    # lower (code 2, Gauss), emfieldModule.hpp:5675-5682; the SE/SW terms couple to Ex,
+    # which the impedance test does not solve
+    for i in range(1, ni + 1):
+        j = 2
+        rR = (r[j] + r[j - 1]) / 2.0
+        rL = (r[j - 1] + r[j - 2]) / 2.0
+        aP[i, j] = aP[i, j] - aS[i, j] * rR / rL
+        aS[i, j] = 0.0
+    # upper (code 2, Gauss), emfieldModule.hpp:5706-5712
+    for i in range(1, ni + 1):
+        j = nj
+        rR = (r[j + 1] + r[j]) / 2.0
+        rL = (r[j] + r[j - 1]) / 2.0
+        aP[i, j] = aP[i, j] - aN[i, j] * rL / rR
+        aN[i, j] = 0.0
+    return dict(aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b, mask=mask)
+
+
+def solve_c5_direct(sysd: dict) -> np.ndarray:
+    """Sparse direct solve of a complex 5-point system on its unknown mask
+    (couplings to non-unknowns dropped, as the Eigen assembly at
+    emfieldModule.hpp:5749-5766 inserts only unknown-to-unknown entries)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    m = sysd["mask"]
+    idx = -np.ones(m.shape, int)
+    cells = np.argwhere(m)
+    idx[m] = np.arange(len(cells))
+    rows, cols, vals = [], [], []
+    rhs = np.zeros(len(cells), complex)
+    for k, (i, j) in enumerate(cells):
+        rows.append(k); cols.append(k); vals.append(sysd["aP"][i, j])
+        rhs[k] = sysd["b"][i, j]
+        for name, di, dj in (("aE", 1, 0), ("aW", -1, 0), ("aN", 0, 1), ("aS", 0, -1)):
+            ii, jj = i + di, j + dj
+            if 0 <= ii < m.shape[0] and 0 <= jj < m.shape[1] and idx[ii, jj] >= 0:
+                rows.append(k); cols.append(idx[ii, jj]); vals.append(-sysd[name][i, j])
+    A = sp.csc_matrix((vals, (rows, cols)), shape=(len(cells), len(cells)))
+    xk = spla.spsolve(A, rhs)
+    x = np.zeros(m.shape, complex)
+    x[m] = xk
+    return x
+
+
+def coax_postprocess(E1r: np.ndarray, p: dict):
+    """Ghost values, port V/I, forward power and rescaling to Pmw
+    (emfieldModule.hpp:5788-5815, :5835-5861, :5880-5960 and :6001-6036).
+    Returns (scaled E1r, scaled J1r_exc scalar, dict of port quantities)."""
+    ni, nj, dx, dr, w = p["ni"], p["nj"], p["dx"], p["dr"], p["omegam"]
+    r, epsr = p["r"], p["epsr"]
+    E = E1r.copy()
+    # left ghost (code 7)
+    for j in range(2, nj + 1):
+        i = 1
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        c0 = np.sqrt(1.0 / (EPS0 * eps_t * MU0))
+        deno = complex(2.0 * c0, w * dx)
+        R = complex(2.0 * c0, -w * dx)
+        r_t = (r[j] + r[j - 1]) / 2.0
+        Er_Fw = p["J1r_exc"] / r_t / np.log(p["r2"] / p["r1"]) * 1e3
+        S = complex(0.0, 4.0 * w * dx) * Er_Fw
+        E[i - 1, j] = R / (deno + 1e-100) * E[i, j] + S / (deno + 1e-100)
+    # lower / upper Gauss ghosts with E1x = 0
+    for i in range(1, ni + 1):
+        j = 2
+        rR = (r[j] + r[j - 1]) / 2.0
+        rL = (r[j - 1] + r[j - 2]) / 2.0
+        E[i, j - 1] = rR / rL * E[i, j]
+        j = nj
+        rR = (r[j + 1] + r[j]) / 2.0
+        rL = (r[j] + r[j - 1]) / 2.0
+        E[i, j + 1] = rL / rR * E[i, j]
+    # reference plane i_ref = int(0/dx + 1.5) = 1
+    i = int(0.0 / dx + 1.5)
+    I_ref = 0.0j
+    coef = 0.0j
+    n = 0
+    for j in range(2, nj + 1):
+        r_t = (r[j] + r[j - 1]) / 2.0
+        H = (E[i, j] - E[i - 1, j]) / dx / (w * MU0) * 1j
+        I_ref += 2.0 * np.pi * r_t * H
+        coef += (E[i, j] + E[i - 1, j]) / 2.0 * r_t
+        n += 1
+    I_ref /= n
+    coef /= n
+    V_ref = coef * np.log(p["r2"] / p["r1"])
+    Z0 = p["Z0"]
+    a2 = (V_ref - Z0 * I_ref) / (2.0 * np.sqrt(2.0 * Z0))
+    b2 = (V_ref + Z0 * I_ref) / (2.0 * np.sqrt(2.0 * Z0))
+    P_fwd = abs(b2) ** 2
+    ratio = p["Pmw"] / P_fwd
+    return E * np.sqrt(ratio), p["J1r_exc"] * np.sqrt(ratio), dict(V=V_ref, I=I_ref, P_fwd=P_fwd,
+                                                                   P_ref=abs(a2) ** 2, ratio=ratio)
+
+
+def coax_output(Es: np.ndarray, J1r_exc: float, p: dict, n: int = 0):
+    """Cell-centred Er and the analytic TEM field of phase snapshot n of 18
+    (outputModule.hpp:81-83, :136-139).  Returns (Er, Er_anly) of shape (ni, nj)."""
+    ni, nj, w = p["ni"], p["nj"], p["omegam"]
+    r, x, epsr = p["r"], p["x"], p["epsr"]
+    deg = 2.0 * np.pi / 18 * n
+    Er = np.zeros((ni, nj), complex)
+    An = np.zeros((ni, nj), complex)
+    for i in range(1, ni + 1):
+        for j in range(1, nj + 1):
+            rL = (r[j - 1] + r[j]) / 2.0
+            rR = (r[j + 1] + r[j]) / 2.0
+            Er[i - 1, j - 1] = (rR * Es[i, j + 1] + rL * Es[i, j]) / (2.0 * r[j]) * np.exp(1j * deg)
+            c0 = np.sqrt(1.0 / (EPS0 * epsr[i, j] * MU0))
+            An[i - 1, j - 1] = J1r_exc / r[j] * 1e3 / np.log(p["r2"] / p["r1"]) * np.exp(1j * (-w / c0 * x[i] + deg))
+    return Er, An

@@ -1,0 +1,81 @@
+"""GPU complex solves of the microwave path against the oracle and the
+reference's coax calibration fixture (tests/golden/coax_er_deg*.csv)."""
+import csv
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _golden(n):
+    g = np.zeros((194, 7), complex)
+    for r in csv.DictReader(open(os.path.join(HERE, "golden", f"coax_er_deg{n}.csv"))):
+        g[int(r["i"]) - 1, int(r["j"]) - 1] = float(r["Er(R)"]) + 1j * float(r["Er(I)"])
+    return g
+
+
+def test_coax_gpu_solve_reproduces_reference_fixture(pkg, cuda_device):
+    from oracle import microwave as mw
+    p = mw.coax_params()
+    s = mw.coax_er_system(p)
+    g = pkg.Grid(p["ni"], p["nj"], [[1, p["ni"]]], [[2, p["nj"]]])
+    x = np.zeros((p["ni"] + 2, p["nj"] + 2), complex)
+    st = g.c5_solve(s["aP"], s["aE"], s["aW"], s["aN"], s["aS"], s["b"], x, maxITR=400, error_cnv=1e-13)
+    assert st.converged == 1, st.as_dict()
+    ref = mw.solve_c5_direct(s)
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-9
+    Es, J, port = mw.coax_postprocess(x, p)
+    for n in (0, 5):
+        Er, _ = mw.coax_output(Es, J, p, n)
+        gold = _golden(n)
+        assert np.linalg.norm(Er - gold) / np.linalg.norm(gold) < 5e-6
+    g.close()
+
+
+def _plasma_helmholtz(ni, nj, seed, nu_lo=1e8, nu_hi=1e10, ne_hi=1e18):
+    """Eφ-type complex 5-point system: r-weighted Laplacian + k0^2 eps_p with the
+    cold-plasma permittivity eps_p = 1 - wp^2 / (w (w - i nu)), Dirichlet walls."""
+    rng = np.random.default_rng(seed)
+    w = 2.67e10
+    dx = 10e-3 / ni
+    dr = 5e-3 / nj
+    r = (np.arange(nj + 2) - 0.5) * dr
+    ne = 10 ** rng.uniform(15, np.log10(ne_hi), (ni + 2, nj + 2))
+    nu = 10 ** rng.uniform(np.log10(nu_lo), np.log10(nu_hi), (ni + 2, nj + 2))
+    wp2 = ne * 1.60217662e-19 ** 2 / (9.10938356e-31 * 8.8541878128e-12)
+    epsp = 1.0 - wp2 / (w * (w - 1j * nu))
+    k02 = (w / 299792458.0) ** 2
+    sh = (ni + 2, nj + 2)
+    aP = np.zeros(sh, complex); aE = np.zeros(sh, complex); aW = np.zeros(sh, complex)
+    aN = np.zeros(sh, complex); aS = np.zeros(sh, complex); b = np.zeros(sh, complex)
+    I, J = slice(1, ni + 1), slice(1, nj + 1)
+    rc = r[J][None, :]
+    rR = 0.5 * (r[1:nj + 1] + r[2:nj + 2])[None, :]
+    rL = 0.5 * (r[1:nj + 1] + r[0:nj])[None, :]
+    aE[I, J] = dr * dr
+    aW[I, J] = dr * dr
+    aN[I, J] = rR / rc * dx * dx
+    aS[I, J] = rL / rc * dx * dx
+    aP[I, J] = aE[I, J] + aW[I, J] + aN[I, J] + aS[I, J] + 1.0 / (rc * rc) * dx * dx * dr * dr \
+        - k02 * epsp[I, J] * dx * dx * dr * dr
+    b[I, J] = (rng.standard_normal((ni, nj)) + 1j * rng.standard_normal((ni, nj))) * dx * dx * dr * dr
+    mask = np.zeros(sh, bool)
+    mask[I, J] = True
+    return dict(aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b, mask=mask)
+
+
+@pytest.mark.parametrize("shape", [(64, 32), (100, 37)])
+def test_plasma_helmholtz_vs_oracle(pkg, cuda_device, shape):
+    from oracle import microwave as mw
+    ni, nj = shape
+    s = _plasma_helmholtz(ni, nj, seed=ni)
+    g = pkg.Grid(ni, nj, [[1, ni]], [[1, nj]])
+    x = np.zeros((ni + 2, nj + 2), complex)
+    st = g.c5_solve(s["aP"], s["aE"], s["aW"], s["aN"], s["aS"], s["b"], x, maxITR=2000, error_cnv=1e-12)
+    assert st.converged == 1, st.as_dict()
+    ref = mw.solve_c5_direct(s)
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-8
+    g.close()
