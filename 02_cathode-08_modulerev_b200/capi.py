@@ -30,7 +30,7 @@ EXPORTS = (
     "cth_grid_levels", "cth_grid_set_cycle", "cth_smg_solve", "cth_smg_solve_dev", "cth_sor_solve",
     "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
     "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs",
-    "cth_c5_solve", "cth_c5_solve_dev",
+    "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -51,6 +51,10 @@ class Status(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class MWParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("dx", "dr", "rmin", "omegam", "J1r_exc", "r1", "r2", "masse")]
 
 
 class CathodeError(RuntimeError):
@@ -89,6 +93,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_c5_solve_dev.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_int, ctypes.c_double, _vp, _vp,
                                                        ctypes.POINTER(Status)]
     L.cth_c5_solve_dev.restype = ctypes.c_int
+    L.cth_mw_er_assemble_dev.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(MWParams)] + [_vp] * 6 + [_vp]
+    L.cth_mw_er_assemble_dev.restype = ctypes.c_int
     L.cth_grid_set_graphs.argtypes = [_vp, ctypes.c_int]
     L.cth_grid_set_graphs.restype = ctypes.c_int
     L.cth_grid_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]

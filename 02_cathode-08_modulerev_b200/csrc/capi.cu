@@ -505,6 +505,18 @@ int cth_c5_solve(cth_grid* g, const double* aP, const double* aE, const double* 
     return res;
 }
 
+int cth_mw_er_assemble_dev(cth_grid* g, const double* ne, const double* nu, const double* epsr,
+                           const cth_mw_params* prm, double* aP, double* aE, double* aW, double* aN,
+                           double* aS, double* b, void* stream) {
+    if (!g || !ne || !nu || !epsr || !prm || !aP || !aE || !aW || !aN || !aS || !b || prm->dx <= 0.0 ||
+        prm->dr <= 0.0 || !(prm->r2 > prm->r1) || prm->r1 <= 0.0) {
+        set_error("cth_mw_er_assemble_dev: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    return mw_er_assemble_dev(g, ne, nu, epsr, prm, aP, aE, aW, aN, aS, b, (cudaStream_t)stream);
+}
+
 int cth_residual_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
                      const double* aN, const double* aS, const double* b, const double* x,
                      double* r, double* rnorm, double* bnorm, void* stream) {

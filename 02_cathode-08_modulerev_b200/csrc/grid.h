@@ -177,6 +177,9 @@ int c5_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* 
                  const double* aS, const double* b, int maxit, double tol, double* solution, cudaStream_t s,
                  cth_status* st);
 int c5_configure(cth_grid* g);
+int mw_er_assemble_dev(cth_grid* g, const double* ne, const double* nu, const double* epsr,
+                       const cth_mw_params* prm, double* aP, double* aE, double* aW, double* aN, double* aS,
+                       double* b, cudaStream_t s);
 }  // namespace cth
 
 #define CTH_CUDA(call)                                        \

@@ -153,6 +153,18 @@ class Grid:
         capi.check(rc)
         return st
 
+    def mw_er_assemble_dev(self, ne, nu, epsr, params: dict, stream=None):
+        """Er system of the microwave path on the device: returns complex planes
+        (aP, aE, aW, aN, aS, b), each torch complex128 of shape (nj+2, ld)."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        out = [torch.zeros((self.nj + 2, self.ld), dtype=torch.complex128, device=f"cuda:{self.device}")
+               for _ in range(6)]
+        prm = capi.MWParams(**{k: float(params[k]) for k, _ in capi.MWParams._fields_})
+        capi.check(self._L.cth_mw_er_assemble_dev(self._h, _ptr(ne), _ptr(nu), _ptr(epsr), ctypes.byref(prm),
+                                                  *[_ptr(o) for o in out], s.cuda_stream), allow_positive=False)
+        return out
+
     # -- device-resident path (library layout) -----------------------------
     def device_plane(self, n: int = 1):
         """Zeroed float64 device planes of the library layout, shape (n, nj+2, ld)."""

@@ -129,3 +129,23 @@ def random_mmatrix(ni: int, nj: int, seed: int = 0, diag_extra: float = 0.0, blo
         i_bl = np.asarray(blocks[0], dtype=np.int32)
         j_bl = np.asarray(blocks[1], dtype=np.int32)
     return dict(ni=ni, nj=nj, i_bl=i_bl, j_bl=j_bl, aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b)
+
+
+def mw_er_rect(ni: int = 1024, nj: int = 512, seed: int = 2, omegam: float = 2.67e10) -> dict:
+    """Isolated microwave Er system on the 10 mm (z) x 5 mm (r) rectangle.
+
+    Cold-plasma medium: n_e log-uniform in [1e15, 1e18] m^-3 and the collision
+    frequency nu log-uniform in [1e8, 1e10] s^-1, drawn from default_rng(seed) in
+    that order as (ni+2, nj+2) cell arrays; epsr = 1; w = 2.67e10 rad/s; port
+    radii of the cathode's coax feed r1 = 0.6 mm, r2 = 2.0 mm.  The Er unknowns are
+    the r-faces i = 1..ni, j = 2..nj (block i_bl = [1, ni], j_bl = [2, nj]).
+    """
+    rng = np.random.default_rng(seed)
+    ne = 10.0 ** rng.uniform(15.0, 18.0, size=(ni + 2, nj + 2))
+    nu = 10.0 ** rng.uniform(8.0, 10.0, size=(ni + 2, nj + 2))
+    epsr = np.ones((ni + 2, nj + 2))
+    dx, dr, x, r = grid(ni, nj)
+    params = dict(dx=dx, dr=dr, rmin=0.0, omegam=omegam, J1r_exc=0.212687, r1=0.6e-3, r2=2.0e-3,
+                  masse=9.10938356e-31)
+    return dict(ni=ni, nj=nj, ne=ne, nu=nu, epsr=epsr, params=params,
+                i_bl=np.array([[1, ni]], dtype=np.int32), j_bl=np.array([[2, nj]], dtype=np.int32))

@@ -160,6 +160,28 @@ int cth_c5_solve_dev(cth_grid* g, const double* aP, const double* aE, const doub
                      const double* aN, const double* aS, const double* b, int maxITR, double tol,
                      double* solution, void* stream, cth_status* st);
 
+/* Microwave Er system (device arrays) ------------------------------------------
+ * Assembles the Er equation of EmfieldModule::solve_Microwave
+ * (include/emfieldModule.hpp:2350-2395) with B = 0 — sigma_rr = n e^2/(m(nu+iw)),
+ * no Hall coupling to Ex or Ephi — on the r-z rectangle with the impedance test's
+ * boundary codes: port excitation (code 7) on the z = 0 faces with
+ * r1 <= r <= r2, open (code 1) on the other z = 0 faces and at z = L, Gauss
+ * (code 2) at r = R, Er = 0 on the axis face.  ne, nu, epsr: real device planes
+ * of cell values (library layout); outputs: complex planes (aP..aS, b) for the
+ * Er faces i = 1..ni, j = 2..nj (zero elsewhere).  Solve them with
+ * cth_c5_solve_dev on a grid whose single block is i in [1,ni], j in [2,nj]. */
+typedef struct cth_mw_params {
+    double dx, dr;     /* cell sizes in z and r                       */
+    double rmin;       /* r of the lower domain edge (0 on the axis)  */
+    double omegam;     /* microwave angular frequency                 */
+    double J1r_exc;    /* port excitation current                     */
+    double r1, r2;     /* port radii                                  */
+    double masse;      /* electron mass                               */
+} cth_mw_params;
+int cth_mw_er_assemble_dev(cth_grid* g, const double* ne, const double* nu, const double* epsr,
+                           const cth_mw_params* prm, double* aP, double* aE, double* aW, double* aN,
+                           double* aS, double* b, void* stream);
+
 /* Residual (device arrays): r = b - A x on grid cells (couplings to non-grid
  * cells dropped), r = 0 elsewhere; *rnorm = ||r||_2, *bnorm = ||b||_2 over grid
  * cells (either may be NULL). */

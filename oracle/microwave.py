@@ -120,22 +120,27 @@ def solve_c5_direct(sysd: dict) -> np.ndarray:
     import scipy.sparse as sp
     import scipy.sparse.linalg as spla
     m = sysd["mask"]
-    idx = -np.ones(m.shape, int)
-    cells = np.argwhere(m)
-    idx[m] = np.arange(len(cells))
-    rows, cols, vals = [], [], []
-    rhs = np.zeros(len(cells), complex)
-    for k, (i, j) in enumerate(cells):
-        rows.append(k); cols.append(k); vals.append(sysd["aP"][i, j])
-        rhs[k] = sysd["b"][i, j]
-        for name, di, dj in (("aE", 1, 0), ("aW", -1, 0), ("aN", 0, 1), ("aS", 0, -1)):
-            ii, jj = i + di, j + dj
-            if 0 <= ii < m.shape[0] and 0 <= jj < m.shape[1] and idx[ii, jj] >= 0:
-                rows.append(k); cols.append(idx[ii, jj]); vals.append(-sysd[name][i, j])
-    A = sp.csc_matrix((vals, (rows, cols)), shape=(len(cells), len(cells)))
-    xk = spla.spsolve(A, rhs)
+    n = int(m.sum())
+    idx = -np.ones(m.shape, np.int64)
+    idx[m] = np.arange(n)
+    ci, cj = np.nonzero(m)
+    k = idx[ci, cj]
+    rows = [k]
+    cols = [k]
+    vals = [sysd["aP"][ci, cj]]
+    for name, di, dj in (("aE", 1, 0), ("aW", -1, 0), ("aN", 0, 1), ("aS", 0, -1)):
+        ii, jj = ci + di, cj + dj
+        ok = (ii >= 0) & (ii < m.shape[0]) & (jj >= 0) & (jj < m.shape[1])
+        nb = np.full(ci.shape, -1, np.int64)
+        nb[ok] = idx[ii[ok], jj[ok]]
+        sel = nb >= 0
+        rows.append(k[sel])
+        cols.append(nb[sel])
+        vals.append(-sysd[name][ci[sel], cj[sel]])
+    A = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    xk = spla.spsolve(A, sysd["b"][ci, cj])
     x = np.zeros(m.shape, complex)
-    x[m] = xk
+    x[ci, cj] = xk
     return x
 
 
@@ -206,3 +211,81 @@ def coax_output(Es: np.ndarray, J1r_exc: float, p: dict, n: int = 0):
             c0 = np.sqrt(1.0 / (EPS0 * epsr[i, j] * MU0))
             An[i - 1, j - 1] = J1r_exc / r[j] * 1e3 / np.log(p["r2"] / p["r1"]) * np.exp(1j * (-w / c0 * x[i] + deg))
     return Er, An
+
+
+def er_rect_params(ni: int, nj: int, Lz: float = 10e-3, Lr: float = 5e-3, fmw: float = 2.67e10 / (2 * np.pi),
+                   J1r_exc: float = 0.212687, r1: float = 0.6e-3, r2: float = 2.0e-3) -> dict:
+    """Rectangle r in [0, Lr], z in [0, Lz] with the coax feed radii r1, r2."""
+    dx, dr = Lz / ni, Lr / nj
+    return dict(ni=ni, nj=nj, dx=dx, dr=dr, omegam=2.0 * np.pi * fmw, J1r_exc=J1r_exc, r1=r1, r2=r2,
+                masse=9.10938356e-31, x=(np.arange(ni + 2) - 0.5) * dx, r=(np.arange(nj + 2) - 0.5) * dr)
+
+
+def er_rect_system(ne: np.ndarray, nu: np.ndarray, epsr: np.ndarray, p: dict):
+    """Er equation of solve_Microwave (emfieldModule.hpp:2350-2395) with B = 0,
+    so that sigma_rr = n e^2 / (m (nu + i w)) and every Hall coupling to Ex / Ephi
+    vanishes, on the rectangle with the impedance test's boundary codes:
+    port excitation (code 7, :5616-5633) on the z = 0 faces with r1 <= r <= r2 and
+    first-order open (code 1, :5602-5612) on the other z = 0 faces, open (code 1,
+    :5642-5657) at z = L, Gauss (code 2, :5706-5712) at r = R (its coupling to Ex
+    dropped: Ex is not part of this system), and Er = 0 on the axis face r = 0
+    (the axis face is not an unknown).  Unknowns: Er faces i = 1..ni, j = 2..nj."""
+    ni, nj, dx, dr, w = p["ni"], p["nj"], p["dx"], p["dr"], p["omegam"]
+    r, me = p["r"], p["masse"]
+    sh = (ni + 2, nj + 2)
+    aP = np.zeros(sh, complex); aE = np.zeros(sh, complex); aW = np.zeros(sh, complex)
+    aN = np.zeros(sh, complex); aS = np.zeros(sh, complex); b = np.zeros(sh, complex)
+    mask = np.zeros(sh, bool)
+    EPS = complex(1e-100, 1e-100)
+    iwm = complex(0.0, w * MU0)
+    I = slice(1, ni + 1)
+    jj = np.arange(2, nj + 1)
+    r_t = ((r[jj - 1] + r[jj]) / 2.0)[None, :]
+    rR = ((r[jj] + r[jj + 1]) / 2.0)[None, :]
+    rL = ((r[jj - 2] + r[jj - 1]) / 2.0)[None, :]
+    nu_t = (nu[I, 2:nj + 1] + nu[I, 1:nj]) / 2.0
+    rho_t = (ne[I, 2:nj + 1] + ne[I, 1:nj]) / 2.0
+    eps_t = (epsr[I, 2:nj + 1] + epsr[I, 1:nj]) / 2.0
+    coef = rho_t * E0 * E0 / (me * (nu_t + 1j * w) + EPS) / (1.0 + EPS)
+    J = slice(2, nj + 1)
+    aP[I, J] = (r_t * (1.0 / r[jj][None, :] + 1.0 / r[jj - 1][None, :]) * dx * dx + 2.0 * dr * dr
+                - EPS0 * eps_t * MU0 * w * w * dx * dx * dr * dr + iwm * coef * dx * dx * dr * dr)
+    aE[I, J] = dr * dr
+    aW[I, J] = dr * dr
+    aN[I, J] = rR / r[jj][None, :] * dx * dx
+    aS[I, J] = rL / r[jj - 1][None, :] * dx * dx
+    mask[I, J] = True
+    for j in range(2, nj + 1):
+        # left: port on [r1, r2], open elsewhere
+        i = 1
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        c0 = np.sqrt(1.0 / (EPS0 * eps_t * MU0))
+        r_t = (r[j] + r[j - 1]) / 2.0
+        if p["r1"] <= r_t <= p["r2"]:
+            deno = complex(2.0 * c0, w * dx)
+            R = complex(2.0 * c0, -w * dx)
+            Er_Fw = p["J1r_exc"] / r_t / np.log(p["r2"] / p["r1"]) * 1e3
+            S = complex(0.0, 4.0 * w * dx) * Er_Fw
+            aP[i, j] -= aW[i, j] * R / (deno + 1e-100)
+            b[i, j] += aW[i, j] * S / (deno + 1e-100)
+        else:
+            deno = (2.0 * c0) ** 2 + (w * dx) ** 2
+            R = complex((2.0 * c0) ** 2 - (w * dx) ** 2, -4.0 * c0 * w * dx) / (deno + 1e-100)
+            aP[i, j] -= aW[i, j] * R
+        aW[i, j] = 0.0
+        # right: open
+        i = ni
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        c0 = np.sqrt(1.0 / (EPS0 * eps_t * MU0))
+        deno = (2.0 * c0) ** 2 + (w * dx) ** 2
+        R = complex((2.0 * c0) ** 2 - (w * dx) ** 2, -4.0 * c0 * w * dx)
+        aP[i, j] -= aE[i, j] * R / (deno + 1e-100)
+        aE[i, j] = 0.0
+    for i in range(1, ni + 1):
+        j = nj
+        rR = (r[j + 1] + r[j]) / 2.0
+        rL = (r[j] + r[j - 1]) / 2.0
+        aP[i, j] -= aN[i, j] * rL / rR
+        aN[i, j] = 0.0
+        aS[i, 2] = 0.0
+    return dict(aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b, mask=mask)

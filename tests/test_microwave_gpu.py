@@ -79,3 +79,55 @@ def test_plasma_helmholtz_vs_oracle(pkg, cuda_device, shape):
     ref = mw.solve_c5_direct(s)
     assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-8
     g.close()
+
+
+def _er_case(pkg, ni, nj, seed=2):
+    from oracle import microwave as mw
+    w = pkg.workloads.mw_er_rect(ni, nj, seed=seed)
+    p = mw.er_rect_params(ni, nj)
+    for k in ("dx", "dr", "omegam", "J1r_exc", "r1", "r2", "masse"):
+        assert p[k] == pytest.approx(w["params"][k], rel=1e-15)
+    return w, p, mw
+
+
+@pytest.mark.parametrize("shape", [(64, 32), (50, 9)])
+def test_mw_er_assembly_and_solve_vs_oracle(pkg, cuda_device, shape):
+    ni, nj = shape
+    w, p, mw = _er_case(pkg, ni, nj)
+    ref = mw.er_rect_system(w["ne"], w["nu"], w["epsr"], p)
+    g = pkg.Grid(ni, nj, w["i_bl"], w["j_bl"])
+    planes = g.mw_er_assemble_dev(g.to_device(w["ne"]), g.to_device(w["nu"]), g.to_device(w["epsr"]), w["params"])
+    for name, pl in zip(("aP", "aE", "aW", "aN", "aS", "b"), planes):
+        got = pl[:, :ni + 2].cpu().numpy().T
+        scale = np.abs(ref[name]).max() + 1e-300
+        assert np.max(np.abs(got - ref[name])) / scale < 1e-13, name
+    x = g.device_plane(1)[0].to(dtype=__import__("torch").complex128)
+    st = g.c5_solve_dev(*planes, x, maxITR=200, error_cnv=1e-12)
+    assert st.converged == 1, st.as_dict()
+    xr = mw.solve_c5_direct(ref)
+    xg = x[:, :ni + 2].cpu().numpy().T
+    assert np.linalg.norm(xg - xr) / np.linalg.norm(xr) < 1e-8
+    g.close()
+
+
+def test_mw_er_full_size(pkg, cuda_device):
+    """512 x 1024 Er system: converged residual recomputed on the CPU."""
+    import torch
+    ni, nj = 1024, 512
+    w, p, mw = _er_case(pkg, ni, nj)
+    g = pkg.Grid(ni, nj, w["i_bl"], w["j_bl"])
+    planes = g.mw_er_assemble_dev(g.to_device(w["ne"]), g.to_device(w["nu"]), g.to_device(w["epsr"]), w["params"])
+    x = torch.zeros_like(planes[0])
+    st = g.c5_solve_dev(*planes, x, maxITR=200, error_cnv=1e-10)
+    assert st.converged == 1 and st.iterations <= 60, st.as_dict()
+    A = [pl[:, :ni + 2].cpu().numpy().T for pl in planes]
+    xg = x[:, :ni + 2].cpu().numpy().T
+    r = A[5] - A[0] * xg
+    r[:-1] += A[1][:-1] * xg[1:]
+    r[1:] += A[2][1:] * xg[:-1]
+    r[:, :-1] += A[3][:, :-1] * xg[:, 1:]
+    r[:, 1:] += A[4][:, 1:] * xg[:, :-1]
+    m = np.zeros(r.shape, bool)
+    m[1:ni + 1, 2:nj + 1] = True
+    assert np.linalg.norm(r[m]) / np.linalg.norm(A[5][m]) < 2e-10
+    g.close()
