@@ -31,6 +31,8 @@ EXPORTS = (
     "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
     "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs",
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
+    "cth_fields_create", "cth_fields_destroy", "cth_field", "cth_field_upload", "cth_field_download",
+    "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -55,6 +57,11 @@ class Status(ctypes.Structure):
 
 class MWParams(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("dx", "dr", "rmin", "omegam", "J1r_exc", "r1", "r2", "masse")]
+
+
+class TransportParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("masse", "massi", "Ti", "nu_eff", "dTe", "dEi", "dr", "rmin")] + \
+               [("flag_Bohm", ctypes.c_int), ("flag_Sagdeev", ctypes.c_int)]
 
 
 class CathodeError(RuntimeError):
@@ -95,6 +102,22 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_c5_solve_dev.restype = ctypes.c_int
     L.cth_mw_er_assemble_dev.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(MWParams)] + [_vp] * 6 + [_vp]
     L.cth_mw_er_assemble_dev.restype = ctypes.c_int
+    L.cth_fields_create.argtypes = [_vp, ctypes.POINTER(_vp)]
+    L.cth_fields_create.restype = ctypes.c_int
+    L.cth_fields_destroy.argtypes = [_vp]
+    L.cth_fields_destroy.restype = None
+    L.cth_field.argtypes = [_vp, ctypes.c_char_p]
+    L.cth_field.restype = ctypes.c_void_p
+    L.cth_field_upload.argtypes = [_vp, ctypes.c_char_p, _vp]
+    L.cth_field_upload.restype = ctypes.c_int
+    L.cth_field_download.argtypes = [_vp, ctypes.c_char_p, _vp]
+    L.cth_field_download.restype = ctypes.c_int
+    L.cth_flags_upload.argtypes = [_vp, _vp]
+    L.cth_flags_upload.restype = ctypes.c_int
+    L.cth_table_upload.argtypes = [_vp, ctypes.c_char_p, _vp, ctypes.c_int]
+    L.cth_table_upload.restype = ctypes.c_int
+    L.cth_update_transport_coef.argtypes = [_vp, ctypes.POINTER(TransportParams), _vp]
+    L.cth_update_transport_coef.restype = ctypes.c_int
     L.cth_grid_set_graphs.argtypes = [_vp, ctypes.c_int]
     L.cth_grid_set_graphs.restype = ctypes.c_int
     L.cth_grid_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]

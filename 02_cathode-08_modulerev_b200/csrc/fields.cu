@@ -1,0 +1,400 @@
+// fields.cu — device field store of the fluid state and the transport-coefficient
+// update of FluidModule.
+//
+// A cth_fields holds named planes of the grid's library layout (cell, x-face and
+// r-face arrays share the (ni+2) x (nj+2) index space as in the reference,
+// fluidModule.hpp:156-173), the per-cell side-flag plane that encodes the
+// reference's block-wall expressions, and the rate tables of BolsigVec
+// (arrays.hpp:703-716).  Kernels take raw plane pointers.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "grid.h"
+#include "line.cuh"
+
+struct cth_fields {
+    cth_grid* g = nullptr;
+    std::map<std::string, double*> planes;
+    unsigned char* flags = nullptr;  // device layout
+    std::map<std::string, std::pair<double*, int>> tables;
+    double* scal = nullptr;          // device scalars (reductions)
+    double* part = nullptr;
+    int npart = 0;
+};
+
+namespace cth {
+
+// side flags of a cell (1 = ordinary interior face on that side)
+enum { F_BLX = 1, F_BRX = 2, F_BLR_WALL = 4, F_BLR_CEN = 8, F_BRR_WALL = 16, F_BRR_OPEN = 32 };
+
+constexpr double kBoltz = 1.380649e-23;    // constants.hpp:5
+constexpr double kE0f = 1.60217662e-19;    // constants.hpp:6
+constexpr double kEps0f = 8.8541878128e-12;// constants.hpp:7
+
+// uniform-step table lookups of miniFuncs.hpp:35-91
+__device__ __forceinline__ double d_func_Te(const double* __restrict__ v, int n, double Te, double dTe) {
+    const int iL = (int)(Te / dTe);
+    const int iR = iL + 1;
+    const double Te_L = iL * dTe;
+    if (iR < n - 1) return (v[iR] - v[iL]) / (dTe + 1e-100) * (Te - Te_L) + v[iL];
+    return v[n - 1];
+}
+
+__device__ __forceinline__ double d_func_dTe(const double* __restrict__ v, int n, double Te, double dTe) {
+    int iL = (int)(Te / dTe);
+    int iR = iL + 1;
+    if (iR >= n - 1) {
+        iL = n - 2;
+        iR = n - 1;
+    }
+    return (v[iR] - v[iL]) / (iR * dTe - iL * dTe + 1e-100);
+}
+
+__device__ __forceinline__ double d_func_Ei(const double* __restrict__ v, int n, double Ei, double dEi,
+                                            double massi) {
+    const int iL = (int)(Ei / dEi);
+    const int iR = iL + 1;
+    const double Ei_L = iL * dEi;
+    if (iR < n - 1) return (v[iR] - v[iL]) / (dEi + 1e-100) * (Ei - Ei_L) + v[iL];
+    const double imax = n - 1;
+    const double v_max = sqrt(imax * dEi / massi);
+    const double v_tmp = sqrt(Ei / massi);
+    return v[n - 1] / v_max * v_tmp;
+}
+
+struct Tab {
+    const double* v;
+    int n;
+};
+
+struct TransportArgs {
+    // inputs
+    const double *rhoe, *rhoi, *rhon, *rhom, *Te, *Bx, *Br, *nu_ano, *Uip, *Uix, *rhoUex, *Uir, *rhoUer;
+    // in/out and outputs
+    double *nu_ano_IAT, *Mache, *nu_elas, *nu_exc, *nu_excReso, *nu_excMeta, *nu_ionz, *nu_ionzStep,
+        *nu_excStep, *nu_super, *nu_m, *nu_m1, *rate_ionize, *nui_m, *rate_eloss, *delossdeps, *mu_para,
+        *mu_xx, *mu_rr, *mu_xr, *mu_perp, *mu_min;
+    Tab t_elas, t_exc, t_excReso, t_excMeta, t_ionz, t_ionzStep, t_excStep, t_super, t_eloss_n, t_eloss_m,
+        t_nui;
+    const unsigned char* flags;
+    const double* rhoe_max;
+    cth_transport_params prm;
+    int ni, nj, ld;
+};
+
+// maximum of rhoe over the fluid cells (flags != 0); the last block stores it
+__global__ void k_max_flagged(const double* __restrict__ v, const unsigned char* __restrict__ flags, int ni,
+                              int nj, int ld, double* __restrict__ part, unsigned int* counter,
+                              double* __restrict__ out) {
+    __shared__ double red[32];
+    __shared__ bool am_last;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    double m = 0.0;
+    if (i <= ni + 1) {
+        const size_t p = (size_t)j * ld + i;
+        if (flags[p]) m = v[p];
+    }
+    // block max
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < ((int)blockDim.x + 31) / 32; k++) s = fmax(s, red[k]);
+        const int nb = gridDim.x * gridDim.y;
+        part[blockIdx.y * gridDim.x + blockIdx.x] = s;
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        am_last = (t == (unsigned int)(nb - 1));
+    }
+    __syncthreads();
+    if (am_last && threadIdx.x == 0) {
+        __threadfence();
+        const int nb = gridDim.x * gridDim.y;
+        double s = 0.0;
+        for (int k = 0; k < nb; k++) s = fmax(s, __ldcg(part + k));
+        *out = s;
+        *counter = 0u;
+    }
+}
+
+// FluidModule::update_transport_coef (fluidModule.hpp:5799-5976), one thread
+// per cell of the (ni+2) x (nj+2) index space
+__global__ void k_transport(TransportArgs A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i > A.ni + 1) return;
+    const int ld = A.ld;
+    const size_t p = (size_t)j * ld + i;
+    const cth_transport_params& P = A.prm;
+    const double dr = P.dr;
+    const double rj = P.rmin + (j - 0.5) * dr;
+    double iat = A.nu_ano_IAT[p];
+    const unsigned char fl = A.flags[p];
+    if (fl) {
+        // anomalous (Sagdeev / ion-acoustic) frequency on fluid cells (:5818-5908)
+        const double rhoe_max = *A.rhoe_max;
+        const double bLx = (fl & F_BLX) ? 1.0 : 0.0, bRx = (fl & F_BRX) ? 1.0 : 0.0;
+        const double bLr = (fl & F_BLR_WALL) ? 1.0 : 0.0, bRr = (fl & F_BRR_WALL) ? 1.0 : 0.0;
+        const double Te = A.Te[p];
+        const double ut = sqrt(2.0 * kBoltz * Te / P.masse);
+        const double rjm = P.rmin + (j - 1.5) * dr, rjp = P.rmin + (j + 0.5) * dr;
+        const double rL = (rj + rjm) / 2.0, rR = (rj + rjp) / 2.0;
+        const double rhoUex_t = (A.rhoUex[p + 1] * bRx + A.rhoUex[p] * bLx) / 2.0;
+        const double rhoUer_t = (rR * A.rhoUer[p + ld] * bRr + rL * A.rhoUer[p] * bLr) / (2.0 * rj);
+        const double den = A.rhoe[p] + rhoe_max * 0.001;
+        const double Uex = rhoUex_t / den, Uer = rhoUer_t / den;
+        const double Uix = (A.Uix[p] + A.Uix[p + 1]) / 2.0;
+        const double Uir = (rL * A.Uir[p] + rR * A.Uir[p + ld]) / (2.0 * rj);
+        A.Mache[p] = sqrt(Uex * Uex + Uer * Uer) / (ut + 100.0);
+        const double cs = sqrt(2.0 * kBoltz * (Te + P.Ti) / P.massi);
+        const double omega_pi = sqrt(A.rhoi[p] * kE0f * kE0f / (P.massi * kEps0f));
+        const double ud = sqrt((Uex - Uix) * (Uex - Uix) + (Uer - Uir) * (Uer - Uir));
+        iat = 0.01 * omega_pi * ud / cs * Te / P.Ti;
+        A.nu_ano_IAT[p] = iat;
+    }
+    // collision frequencies, sources and mobility tensor on every cell (:5912-5973)
+    const double Te = A.Te[p], rhon = A.rhon[p], rhom = A.rhom[p], dTe = P.dTe;
+    const double elas = d_func_Te(A.t_elas.v, A.t_elas.n, Te, dTe);
+    A.nu_elas[p] = rhon * elas;
+    A.nu_exc[p] = rhon * d_func_Te(A.t_exc.v, A.t_exc.n, Te, dTe);
+    A.nu_excReso[p] = rhon * d_func_Te(A.t_excReso.v, A.t_excReso.n, Te, dTe);
+    A.nu_excMeta[p] = rhon * d_func_Te(A.t_excMeta.v, A.t_excMeta.n, Te, dTe);
+    const double ionz = rhon * d_func_Te(A.t_ionz.v, A.t_ionz.n, Te, dTe);
+    const double ionzStep = rhom * d_func_Te(A.t_ionzStep.v, A.t_ionzStep.n, Te, dTe);
+    A.nu_ionz[p] = ionz;
+    A.nu_ionzStep[p] = ionzStep;
+    A.nu_excStep[p] = rhom * d_func_Te(A.t_excStep.v, A.t_excStep.n, Te, dTe);
+    A.nu_super[p] = rhom * d_func_Te(A.t_super.v, A.t_super.n, Te, dTe);
+    const double nu_m_real = rhon * elas;
+    const double nu_m = nu_m_real + (double)P.flag_Bohm * A.nu_ano[p] + (double)P.flag_Sagdeev * iat;
+    A.nu_m[p] = nu_m;
+    A.nu_m1[p] = nu_m_real + P.nu_eff;
+    A.rate_ionize[p] = A.rhoe[p] * (ionz + ionzStep);
+    double vv = 0.0;
+    if (i != 0 && i != A.ni + 1 && j != 0 && j != A.nj + 1) {
+        const double rjm = P.rmin + (j - 1.5) * dr, rjp = P.rmin + (j + 0.5) * dr;
+        const double rL = (rj + rjm) / 2.0, rR = (rj + rjp) / 2.0;
+        const double Uix = (A.Uix[p] + A.Uix[p + 1]) / 2.0;
+        const double Uir = (rL * A.Uir[p] + rR * A.Uir[p + ld]) / (2.0 * rj);
+        const double Uip = A.Uip[p];
+        vv = Uix * Uix + Uir * Uir + Uip * Uip;
+    }
+    A.nui_m[p] = rhon * d_func_Ei(A.t_nui.v, A.t_nui.n, P.massi * vv, P.dEi, P.massi);
+    A.rate_eloss[p] = rhon * d_func_Te(A.t_eloss_n.v, A.t_eloss_n.n, Te, dTe) +
+                      rhom * d_func_Te(A.t_eloss_m.v, A.t_eloss_m.n, Te, dTe);
+    A.delossdeps[p] = 2.0 / (3.0 * kBoltz) * rhon * d_func_dTe(A.t_eloss_n.v, A.t_eloss_n.n, Te, dTe) +
+                      2.0 / (3.0 * kBoltz) * rhom * d_func_dTe(A.t_eloss_m.v, A.t_eloss_m.n, Te, dTe);
+    const double mu_para = kE0f / (P.masse * nu_m + 1e-100);
+    A.mu_para[p] = mu_para;
+    const double Bx = A.Bx[p], Br = A.Br[p];
+    const double Bmag = sqrt(Bx * Bx + Br * Br);
+    const double Om = kE0f * Bmag / (P.masse * nu_m + 1e-100);
+    const double Omx = kE0f * Bx / (P.masse * nu_m + 1e-100);
+    const double Omr = kE0f * Br / (P.masse * nu_m + 1e-100);
+    const double deno = 1.0 + Om * Om;
+    A.mu_xx[p] = mu_para * (1.0 + Omx * Omx) / deno;
+    A.mu_rr[p] = mu_para * (1.0 + Omr * Omr) / deno;
+    A.mu_xr[p] = mu_para * (Omx * Omr) / deno;
+    A.mu_perp[p] = mu_para / deno;
+    A.mu_min[p] = mu_para * 2.0 / deno;
+}
+
+static double* field_ptr(cth_fields* fs, const std::string& name) {
+    auto it = fs->planes.find(name);
+    if (it != fs->planes.end()) return it->second;
+    double* p = nullptr;
+    const size_t bytes = fs->g->plane * sizeof(double);
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    if (cudaMemset(p, 0, bytes) != cudaSuccess) { cudaFree(p); return nullptr; }
+    fs->planes[name] = p;
+    return p;
+}
+
+static Tab table(cth_fields* fs, const char* name, bool* ok) {
+    auto it = fs->tables.find(name);
+    if (it == fs->tables.end() || it->second.second < 2) {
+        *ok = false;
+        return Tab{nullptr, 0};
+    }
+    return Tab{it->second.first, it->second.second};
+}
+
+int update_transport_coef(cth_fields* fs, const cth_transport_params* prm, cudaStream_t s) {
+    cth_grid* g = fs->g;
+    if (!fs->flags) {
+        set_error("cth_update_transport_coef: boundary flags not uploaded");
+        return CTH_ERR_ARG;
+    }
+    TransportArgs A;
+    const char* in_names[13] = {"rhoe", "rhoi", "rhon", "rhom", "Te", "Bx", "Br", "nu_ano", "Uip", "Uix",
+                                "rhoUex", "Uir", "rhoUer"};
+    const double** in_ptrs[13] = {&A.rhoe, &A.rhoi, &A.rhon, &A.rhom, &A.Te, &A.Bx, &A.Br, &A.nu_ano,
+                                  &A.Uip, &A.Uix, &A.rhoUex, &A.Uir, &A.rhoUer};
+    for (int k = 0; k < 13; k++) {
+        double* q = field_ptr(fs, in_names[k]);
+        if (!q) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
+        *in_ptrs[k] = q;
+    }
+    const char* out_names[22] = {"nu_ano_IAT", "Mache", "nu_elas", "nu_exc", "nu_excReso", "nu_excMeta",
+                                 "nu_ionz", "nu_ionzStep", "nu_excStep", "nu_super", "nu_m", "nu_m1",
+                                 "rate_ionize", "nui_m", "rate_eloss", "delossdeps", "mu_para", "mu_xx",
+                                 "mu_rr", "mu_xr", "mu_perp", "mu_min"};
+    double** out_ptrs[22] = {&A.nu_ano_IAT, &A.Mache, &A.nu_elas, &A.nu_exc, &A.nu_excReso, &A.nu_excMeta,
+                             &A.nu_ionz, &A.nu_ionzStep, &A.nu_excStep, &A.nu_super, &A.nu_m, &A.nu_m1,
+                             &A.rate_ionize, &A.nui_m, &A.rate_eloss, &A.delossdeps, &A.mu_para, &A.mu_xx,
+                             &A.mu_rr, &A.mu_xr, &A.mu_perp, &A.mu_min};
+    for (int k = 0; k < 22; k++) {
+        double* q = field_ptr(fs, out_names[k]);
+        if (!q) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
+        *out_ptrs[k] = q;
+    }
+    bool ok = true;
+    A.t_elas = table(fs, "nu_elas_N", &ok);
+    A.t_exc = table(fs, "nu_exc_N", &ok);
+    A.t_excReso = table(fs, "nu_excReso_N", &ok);
+    A.t_excMeta = table(fs, "nu_excMeta_N", &ok);
+    A.t_ionz = table(fs, "nu_ionz_N", &ok);
+    A.t_ionzStep = table(fs, "nu_ionzStep_N", &ok);
+    A.t_excStep = table(fs, "nu_excStep_N", &ok);
+    A.t_super = table(fs, "nu_super_N", &ok);
+    A.t_eloss_n = table(fs, "rate_eloss_n_N", &ok);
+    A.t_eloss_m = table(fs, "rate_eloss_m_N", &ok);
+    A.t_nui = table(fs, "nui_m_N", &ok);
+    if (!ok) {
+        set_error("cth_update_transport_coef: a rate table is missing (upload all eleven BolsigVec tables)");
+        return CTH_ERR_ARG;
+    }
+    A.flags = fs->flags;
+    A.rhoe_max = fs->scal;
+    A.prm = *prm;
+    A.ni = g->ni;
+    A.nj = g->nj;
+    A.ld = g->ld;
+    dim3 blk(128), grd((g->ni + 2 + 127) / 128, g->nj + 2);
+    k_max_flagged<<<grd, blk, 0, s>>>(A.rhoe, fs->flags, g->ni, g->nj, g->ld, fs->part, g->ws.counter, fs->scal);
+    k_transport<<<grd, blk, 0, s>>>(A);
+    g->launches += 2;
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+}  // namespace cth
+
+using namespace cth;
+
+extern "C" {
+
+int cth_fields_create(cth_grid* g, cth_fields** out) {
+    if (!g || !out) { set_error("cth_fields_create: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(g->device));
+    cth_fields* fs = new cth_fields();
+    fs->g = g;
+    fs->npart = ((g->ni + 2 + 127) / 128) * (g->nj + 2) + 8;
+    if (cudaMalloc(&fs->part, fs->npart * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&fs->scal, 16 * sizeof(double)) != cudaSuccess) {
+        if (fs->part) cudaFree(fs->part);
+        delete fs;
+        set_error("cth_fields_create: allocation failed");
+        return CTH_ERR_ALLOC;
+    }
+    cudaMemset(fs->scal, 0, 16 * sizeof(double));
+    *out = fs;
+    return CTH_OK;
+}
+
+void cth_fields_destroy(cth_fields* fs) {
+    if (!fs) return;
+    cudaSetDevice(fs->g->device);
+    for (auto& kv : fs->planes) cudaFree(kv.second);
+    for (auto& kv : fs->tables) cudaFree(kv.second.first);
+    if (fs->flags) cudaFree(fs->flags);
+    if (fs->part) cudaFree(fs->part);
+    if (fs->scal) cudaFree(fs->scal);
+    delete fs;
+}
+
+double* cth_field(cth_fields* fs, const char* name) {
+    if (!fs || !name) { set_error("cth_field: invalid arguments"); return nullptr; }
+    cudaSetDevice(fs->g->device);
+    double* p = field_ptr(fs, name);
+    if (!p) set_error("cth_field: allocation failed");
+    return p;
+}
+
+int cth_field_upload(cth_fields* fs, const char* name, const double* host_ij) {
+    if (!fs || !name || !host_ij) { set_error("cth_field_upload: invalid arguments"); return CTH_ERR_ARG; }
+    cth_grid* g = fs->g;
+    CTH_CUDA(cudaSetDevice(g->device));
+    int rc = ensure_staging(g);
+    if (rc != CTH_OK) return rc;
+    double* dst = field_ptr(fs, name);
+    if (!dst) { set_error("cth_field_upload: allocation failed"); return CTH_ERR_ALLOC; }
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    CTH_CUDA(cudaMemcpyAsync(g->ws.stage_ij, host_ij, nij * sizeof(double), cudaMemcpyHostToDevice, g->stream));
+    rc = to_device_layout(g, g->ws.stage_ij, dst, g->stream);
+    if (rc != CTH_OK) return rc;
+    CTH_CUDA(cudaStreamSynchronize(g->stream));
+    return CTH_OK;
+}
+
+int cth_field_download(cth_fields* fs, const char* name, double* host_ij) {
+    if (!fs || !name || !host_ij) { set_error("cth_field_download: invalid arguments"); return CTH_ERR_ARG; }
+    cth_grid* g = fs->g;
+    CTH_CUDA(cudaSetDevice(g->device));
+    int rc = ensure_staging(g);
+    if (rc != CTH_OK) return rc;
+    auto it = fs->planes.find(name);
+    if (it == fs->planes.end()) { set_error(std::string("cth_field_download: no field ") + name); return CTH_ERR_ARG; }
+    rc = from_device_layout(g, it->second, g->ws.stage_ij, g->stream);
+    if (rc != CTH_OK) return rc;
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    CTH_CUDA(cudaMemcpyAsync(host_ij, g->ws.stage_ij, nij * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
+    CTH_CUDA(cudaStreamSynchronize(g->stream));
+    return CTH_OK;
+}
+
+int cth_flags_upload(cth_fields* fs, const unsigned char* host_ij) {
+    if (!fs || !host_ij) { set_error("cth_flags_upload: invalid arguments"); return CTH_ERR_ARG; }
+    cth_grid* g = fs->g;
+    CTH_CUDA(cudaSetDevice(g->device));
+    std::vector<unsigned char> lay(g->plane, 0);
+    // the ghost frame never carries a fluid cell (the kernels read its neighbours)
+    for (int i = 1; i <= g->ni; i++)
+        for (int j = 1; j <= g->nj; j++) lay[(size_t)j * g->ld + i] = host_ij[(size_t)i * (g->nj + 2) + j];
+    if (!fs->flags) CTH_CUDA(cudaMalloc(&fs->flags, g->plane));
+    CTH_CUDA(cudaMemcpy(fs->flags, lay.data(), g->plane, cudaMemcpyHostToDevice));
+    return CTH_OK;
+}
+
+int cth_table_upload(cth_fields* fs, const char* name, const double* values, int n) {
+    if (!fs || !name || !values || n < 2) { set_error("cth_table_upload: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(fs->g->device));
+    auto it = fs->tables.find(name);
+    if (it != fs->tables.end()) {
+        cudaFree(it->second.first);
+        fs->tables.erase(it);
+    }
+    double* d = nullptr;
+    CTH_CUDA(cudaMalloc(&d, n * sizeof(double)));
+    CTH_CUDA(cudaMemcpy(d, values, n * sizeof(double), cudaMemcpyHostToDevice));
+    fs->tables[name] = std::make_pair(d, n);
+    return CTH_OK;
+}
+
+int cth_update_transport_coef(cth_fields* fs, const cth_transport_params* prm, void* stream) {
+    if (!fs || !prm || prm->dTe <= 0.0 || prm->dEi <= 0.0) {
+        set_error("cth_update_transport_coef: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(fs->g->device));
+    return update_transport_coef(fs, prm, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -17,6 +17,8 @@
 
 #include "../../include/cathode_b200.h"
 
+#include <cuda_runtime.h>
+
 namespace cth {
 
 // complex double of the frequency-domain solves; interleaved (re, im) in memory

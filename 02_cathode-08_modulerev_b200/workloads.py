@@ -149,3 +149,47 @@ def mw_er_rect(ni: int = 1024, nj: int = 512, seed: int = 2, omegam: float = 2.6
                   masse=9.10938356e-31)
     return dict(ni=ni, nj=nj, ne=ne, nu=nu, epsr=epsr, params=params,
                 i_bl=np.array([[1, ni]], dtype=np.int32), j_bl=np.array([[2, nj]], dtype=np.int32))
+
+
+MASSE = 9.10938356e-31               # params.hpp:34
+MASSI_XE = 131.293e-3 / 6.02214076e23  # params.hpp:35
+
+
+def plasma_state(ni: int, nj: int, seed: int = 3, dr: float | None = None) -> dict:
+    """Seeded fluid state in the reference's field names and shapes.
+
+    Cell fields (ni+2, nj+2): rhoe log-uniform in [1e15, 1e19] m^-3, rhoi =
+    rhoe (1 + 0.01 N(0,1)), rhon log-uniform in [1e20, 1e22], rhom = 1e-3 rhon,
+    Te uniform in [0.5, 20] eV (in K) with 1 % of the cells in [150, 250] eV
+    (past the end of the rate tables), Bx, Br N(0, 0.05) T, nu_ano log-uniform
+    in [1e6, 1e8] s^-1, nu_ano_IAT = 0, Uip N(0, 100) m/s; face fields Uix, Uir
+    N(0, 100) m/s with 10 % of the faces N(0, 3000), rhoUex, rhoUer = rhoe N(0, 1e5).
+    Transport parameters: the xenon discharge of params.hpp:34-83 (Ti = 300 K,
+    nu_eff = 1e9 s^-1) with the Bohm and Sagdeev terms switched on.
+    """
+    rng = np.random.default_rng(seed)
+    sh = (ni + 2, nj + 2)
+    f = {}
+    f["rhoe"] = 10.0 ** rng.uniform(15.0, 19.0, sh)
+    f["rhoi"] = f["rhoe"] * (1.0 + 0.01 * rng.standard_normal(sh))
+    f["rhon"] = 10.0 ** rng.uniform(20.0, 22.0, sh)
+    f["rhom"] = 1e-3 * f["rhon"]
+    te_ev = rng.uniform(0.5, 20.0, sh)
+    hot = rng.random(sh) < 0.01
+    te_ev[hot] = rng.uniform(150.0, 250.0, hot.sum())
+    f["Te"] = te_ev * E0 / BOLTZ
+    f["Bx"] = 0.05 * rng.standard_normal(sh)
+    f["Br"] = 0.05 * rng.standard_normal(sh)
+    f["nu_ano"] = 10.0 ** rng.uniform(6.0, 8.0, sh)
+    f["nu_ano_IAT"] = np.zeros(sh)
+    f["Uip"] = 100.0 * rng.standard_normal(sh)
+    for k in ("Uix", "Uir"):
+        u = 100.0 * rng.standard_normal(sh)
+        fast = rng.random(sh) < 0.1
+        u[fast] = 3000.0 * rng.standard_normal(fast.sum())
+        f[k] = u
+    f["rhoUex"] = f["rhoe"] * 1e5 * rng.standard_normal(sh)
+    f["rhoUer"] = f["rhoe"] * 1e5 * rng.standard_normal(sh)
+    prm = dict(masse=MASSE, massi=MASSI_XE, Ti=300.0, nu_eff=1e9, flag_Bohm=1, flag_Sagdeev=1,
+               dr=dr if dr is not None else 5e-3 / nj, rmin=0.0)
+    return dict(fields=f, prm=prm)

@@ -182,6 +182,47 @@ int cth_mw_er_assemble_dev(cth_grid* g, const double* ne, const double* nu, cons
                            const cth_mw_params* prm, double* aP, double* aE, double* aW, double* aN,
                            double* aS, double* b, void* stream);
 
+/* Fluid state in HBM -----------------------------------------------------------
+ * A field store holds named device planes of the grid's library layout (cell
+ * arrays and the x-face (i-1/2) / r-face (j-1/2) arrays share the (ni+2)x(nj+2)
+ * index space, as in the reference, fluidModule.hpp:156-173), the per-cell side
+ * flags of the fluid blocks and the BolsigVec rate tables (arrays.hpp:703-716).
+ * Field names are the reference's member names (rhoe, Te, mu_perp, rhoUex, ...).
+ * cth_field returns the device plane (created zeroed on first use).
+ * Side-flag bits (1 = ordinary face on that side, 0 = the wall / axis / open
+ * boundary of the reference's bLx_wall, bRx_wall, bLr_wall, bLr_cen, bRr_wall,
+ * bRr_open expressions, e.g. fluidModule.hpp:2660-2686); a zero byte marks a
+ * cell outside the fluid blocks. */
+#define CTH_F_BLX 1
+#define CTH_F_BRX 2
+#define CTH_F_BLR_WALL 4
+#define CTH_F_BLR_CEN 8
+#define CTH_F_BRR_WALL 16
+#define CTH_F_BRR_OPEN 32
+typedef struct cth_fields cth_fields;
+int cth_fields_create(cth_grid* g, cth_fields** out);
+void cth_fields_destroy(cth_fields* fs);
+double* cth_field(cth_fields* fs, const char* name);
+int cth_field_upload(cth_fields* fs, const char* name, const double* host_ij);
+int cth_field_download(cth_fields* fs, const char* name, double* host_ij);
+int cth_flags_upload(cth_fields* fs, const unsigned char* host_ij);
+/* table names: nu_elas_N nu_exc_N nu_excReso_N nu_excMeta_N nu_ionz_N nu_ionzStep_N
+ * nu_excStep_N nu_super_N rate_eloss_n_N rate_eloss_m_N nui_m_N */
+int cth_table_upload(cth_fields* fs, const char* name, const double* values, int n);
+
+/* FluidModule::update_transport_coef (fluidModule.hpp:5799-5976): anomalous
+ * ion-acoustic frequency and Mach number on the fluid cells, collision
+ * frequencies from the rate tables (uniform-step lookups of miniFuncs.hpp:35-91),
+ * ionisation source rate_ionize, ion momentum frequency, energy-loss rate and
+ * its Te derivative, and the magnetised mobility tensor on every cell. */
+typedef struct cth_transport_params {
+    double masse, massi, Ti, nu_eff;
+    double dTe, dEi;      /* table steps (Params::dTe, Params::dEi)        */
+    double dr, rmin;      /* radial grid: r_j = rmin + (j - 1/2) dr       */
+    int flag_Bohm, flag_Sagdeev;
+} cth_transport_params;
+int cth_update_transport_coef(cth_fields* fs, const cth_transport_params* prm, void* stream);
+
 /* Residual (device arrays): r = b - A x on grid cells (couplings to non-grid
  * cells dropped), r = 0 elsewhere; *rnorm = ||r||_2, *bnorm = ||b||_2 over grid
  * cells (either may be NULL). */

@@ -1,0 +1,32 @@
+"""Build the rate-table fixture from the reference's BOLSIG+ input files.
+
+Source: the reference's input/rateCoef_e.csv (electron collision rates against
+mean energy, 1800 rows) and input/rateCoef_i.csv (ion momentum-transfer rate),
+read the way InputModule::input_BOLSIG_data does (inputModule.hpp:1413-1655),
+restated by oracle.fluid.bolsig_tables.  Output: rate_tables.npz with the eleven
+BolsigVec tables and the steps dTe (K) and dEi (J).
+Run in a checkout that has the reference under /root/reference.
+"""
+import os
+import sys
+
+import numpy as np
+
+SRC = "/root/reference/input"
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import fluid  # noqa: E402
+
+
+def main():
+    te = open(os.path.join(SRC, "rateCoef_e.csv")).read()
+    ti = open(os.path.join(SRC, "rateCoef_i.csv")).read()
+    tb, dTe, dEi = fluid.bolsig_tables(te, ti)
+    out = os.path.join(HERE, "rate_tables.npz")
+    np.savez_compressed(out, dTe=dTe, dEi=dEi, **tb)
+    print(out, {k: v.shape for k, v in tb.items()}, dTe, dEi)
+
+
+if __name__ == "__main__":
+    main()
