@@ -32,7 +32,7 @@ EXPORTS = (
     "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs",
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_fields_create", "cth_fields_destroy", "cth_field", "cth_field_upload", "cth_field_download",
-    "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef",
+    "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -62,6 +62,20 @@ class MWParams(ctypes.Structure):
 class TransportParams(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("masse", "massi", "Ti", "nu_eff", "dTe", "dEi", "dr", "rmin")] + \
                [("flag_Bohm", ctypes.c_int), ("flag_Sagdeev", ctypes.c_int)]
+
+
+class PhiParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("dt", "dx", "dr", "rmin", "V_bias", "masse", "coefIISEE_ts",
+                                               "coefMISEE_ts", "dTe_SEE", "error_cnv_HES_phi",
+                                               "error_cnv_SOR_phi")] + \
+               [(k, ctypes.c_int) for k in ("maxITR_HES_phi", "maxITR_SOR_phi", "flag_error", "flag_iter_phi",
+                                            "precision")]
+
+
+class PCResult(ctypes.Structure):
+    _fields_ = [("ncount", ctypes.c_int), ("solver_rc", ctypes.c_int), ("error_phi", ctypes.c_double),
+                ("error_nUex", ctypes.c_double), ("error_nUer", ctypes.c_double),
+                ("error_iter", ctypes.c_double * 3), ("solver", Status)]
 
 
 class CathodeError(RuntimeError):
@@ -118,6 +132,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_table_upload.restype = ctypes.c_int
     L.cth_update_transport_coef.argtypes = [_vp, ctypes.POINTER(TransportParams), _vp]
     L.cth_update_transport_coef.restype = ctypes.c_int
+    L.cth_solve_phi_pc.argtypes = [_vp, ctypes.POINTER(PhiParams), _vp, ctypes.POINTER(PCResult)]
+    L.cth_solve_phi_pc.restype = ctypes.c_int
     L.cth_grid_set_graphs.argtypes = [_vp, ctypes.c_int]
     L.cth_grid_set_graphs.restype = ctypes.c_int
     L.cth_grid_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]

@@ -13,63 +13,10 @@
 #include <string>
 #include <vector>
 
-#include "grid.h"
+#include "fluid.cuh"
 #include "line.cuh"
 
-struct cth_fields {
-    cth_grid* g = nullptr;
-    std::map<std::string, double*> planes;
-    unsigned char* flags = nullptr;  // device layout
-    std::map<std::string, std::pair<double*, int>> tables;
-    double* scal = nullptr;          // device scalars (reductions)
-    double* part = nullptr;
-    int npart = 0;
-};
-
 namespace cth {
-
-// side flags of a cell (1 = ordinary interior face on that side)
-enum { F_BLX = 1, F_BRX = 2, F_BLR_WALL = 4, F_BLR_CEN = 8, F_BRR_WALL = 16, F_BRR_OPEN = 32 };
-
-constexpr double kBoltz = 1.380649e-23;    // constants.hpp:5
-constexpr double kE0f = 1.60217662e-19;    // constants.hpp:6
-constexpr double kEps0f = 8.8541878128e-12;// constants.hpp:7
-
-// uniform-step table lookups of miniFuncs.hpp:35-91
-__device__ __forceinline__ double d_func_Te(const double* __restrict__ v, int n, double Te, double dTe) {
-    const int iL = (int)(Te / dTe);
-    const int iR = iL + 1;
-    const double Te_L = iL * dTe;
-    if (iR < n - 1) return (v[iR] - v[iL]) / (dTe + 1e-100) * (Te - Te_L) + v[iL];
-    return v[n - 1];
-}
-
-__device__ __forceinline__ double d_func_dTe(const double* __restrict__ v, int n, double Te, double dTe) {
-    int iL = (int)(Te / dTe);
-    int iR = iL + 1;
-    if (iR >= n - 1) {
-        iL = n - 2;
-        iR = n - 1;
-    }
-    return (v[iR] - v[iL]) / (iR * dTe - iL * dTe + 1e-100);
-}
-
-__device__ __forceinline__ double d_func_Ei(const double* __restrict__ v, int n, double Ei, double dEi,
-                                            double massi) {
-    const int iL = (int)(Ei / dEi);
-    const int iR = iL + 1;
-    const double Ei_L = iL * dEi;
-    if (iR < n - 1) return (v[iR] - v[iL]) / (dEi + 1e-100) * (Ei - Ei_L) + v[iL];
-    const double imax = n - 1;
-    const double v_max = sqrt(imax * dEi / massi);
-    const double v_tmp = sqrt(Ei / massi);
-    return v[n - 1] / v_max * v_tmp;
-}
-
-struct Tab {
-    const double* v;
-    int n;
-};
 
 struct TransportArgs {
     // inputs
@@ -206,7 +153,7 @@ __global__ void k_transport(TransportArgs A) {
     A.mu_min[p] = mu_para * 2.0 / deno;
 }
 
-static double* field_ptr(cth_fields* fs, const std::string& name) {
+double* field_ptr(cth_fields* fs, const std::string& name) {
     auto it = fs->planes.find(name);
     if (it != fs->planes.end()) return it->second;
     double* p = nullptr;
@@ -217,7 +164,7 @@ static double* field_ptr(cth_fields* fs, const std::string& name) {
     return p;
 }
 
-static Tab table(cth_fields* fs, const char* name, bool* ok) {
+Tab table(cth_fields* fs, const char* name, bool* ok) {
     auto it = fs->tables.find(name);
     if (it == fs->tables.end() || it->second.second < 2) {
         *ok = false;
@@ -296,15 +243,18 @@ int cth_fields_create(cth_grid* g, cth_fields** out) {
     CTH_CUDA(cudaSetDevice(g->device));
     cth_fields* fs = new cth_fields();
     fs->g = g;
-    fs->npart = ((g->ni + 2 + 127) / 128) * (g->nj + 2) + 8;
+    const int nblk = ((g->ni + 2 + 127) / 128) * (g->nj + 2) + 8;
+    fs->npart = nblk * CTH_FS_NPART_PER_BLOCK;
     if (cudaMalloc(&fs->part, fs->npart * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&fs->scal, 16 * sizeof(double)) != cudaSuccess) {
+        cudaMalloc(&fs->scal, CTH_FS_NSCAL * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&fs->h_scal, CTH_FS_NSCAL * sizeof(double)) != cudaSuccess) {
         if (fs->part) cudaFree(fs->part);
+        if (fs->scal) cudaFree(fs->scal);
         delete fs;
         set_error("cth_fields_create: allocation failed");
         return CTH_ERR_ALLOC;
     }
-    cudaMemset(fs->scal, 0, 16 * sizeof(double));
+    cudaMemset(fs->scal, 0, CTH_FS_NSCAL * sizeof(double));
     *out = fs;
     return CTH_OK;
 }
@@ -317,6 +267,7 @@ void cth_fields_destroy(cth_fields* fs) {
     if (fs->flags) cudaFree(fs->flags);
     if (fs->part) cudaFree(fs->part);
     if (fs->scal) cudaFree(fs->scal);
+    if (fs->h_scal) cudaFreeHost(fs->h_scal);
     delete fs;
 }
 

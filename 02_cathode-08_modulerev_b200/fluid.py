@@ -16,6 +16,7 @@ import numpy as np
 from . import capi
 
 F_BLX, F_BRX, F_BLR_WALL, F_BLR_CEN, F_BRR_WALL, F_BRR_OPEN = 1, 2, 4, 8, 16, 32
+F_BRX_BIAS = 64  # the right wall of the cell is the biased electrode
 TABLES = ("nu_elas_N", "nu_exc_N", "nu_excReso_N", "nu_excMeta_N", "nu_ionz_N", "nu_ionzStep_N",
           "nu_excStep_N", "nu_super_N", "rate_eloss_n_N", "rate_eloss_m_N", "nui_m_N")
 
@@ -49,7 +50,7 @@ def cathode_flags(ni, nj, ib, jb) -> np.ndarray:
         bRrw = ((J != jb[0][1]) | (b > 2)) & ((J != jb[3][1]) | (I < ib[1][1] + 1) | (I > ib[3][1]))
         bRro = (J != jb[4][1]) | (b != 4)
         code = (F_BLX * bLx + F_BRX * bRx + F_BLR_WALL * bLrw + F_BLR_CEN * bLrc + F_BRR_WALL * bRrw +
-                F_BRR_OPEN * bRro)
+                F_BRR_OPEN * bRro + F_BRX_BIAS * ((I == ib[4][1]) & (b == 4)))
         fl[ib[b][0]:ib[b][1] + 1, jb[b][0]:jb[b][1] + 1] = code.astype(np.uint8)
     return fl
 
@@ -59,7 +60,7 @@ def rectangle_flags(ni, nj) -> np.ndarray:
     fl = np.zeros((ni + 2, nj + 2), np.uint8)
     I, J = np.meshgrid(np.arange(1, ni + 1), np.arange(1, nj + 1), indexing="ij")
     fl[1:ni + 1, 1:nj + 1] = (F_BLX * (I != 1) + F_BRX * (I != ni) + F_BLR_WALL + F_BLR_CEN * (J != 1) +
-                              F_BRR_WALL * (J != nj) + F_BRR_OPEN).astype(np.uint8)
+                              F_BRR_WALL * (J != nj) + F_BRR_OPEN + F_BRX_BIAS * (I == ni)).astype(np.uint8)
     return fl
 
 
@@ -108,6 +109,19 @@ class Fields:
     def set_table(self, name: str, values):
         v = np.ascontiguousarray(values, dtype=np.float64)
         capi.check(self._L.cth_table_upload(self._h, name.encode(), v.ctypes.data, v.size), allow_positive=False)
+
+    def solve_phi_pc(self, prm: dict, stream=None) -> dict:
+        """FluidModule::solve_phi_couple_wdTe_wSEE_PC on the device (fluidModule.hpp:2080-3075).
+
+        prm holds the cth_phi_params fields (dTe_SEE included); returns the PC
+        result (iterations, calcRes errors, inner-solver status)."""
+        p = capi.PhiParams(**{k: prm[k] for k, _ in capi.PhiParams._fields_})
+        res = capi.PCResult()
+        s = 0 if stream is None else stream.cuda_stream
+        capi.check(self._L.cth_solve_phi_pc(self._h, ctypes.byref(p), s, ctypes.byref(res)), allow_positive=False)
+        return dict(ncount=res.ncount, solver_rc=res.solver_rc, error_phi=res.error_phi,
+                    error_nUex=res.error_nUex, error_nUer=res.error_nUer, error_iter=list(res.error_iter),
+                    solver=res.solver.as_dict())
 
     def update_transport_coef(self, prm: dict, stream=None):
         """FluidModule::update_transport_coef on the device (fluidModule.hpp:5799-5976)."""

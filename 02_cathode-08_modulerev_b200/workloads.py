@@ -193,3 +193,61 @@ def plasma_state(ni: int, nj: int, seed: int = 3, dr: float | None = None) -> di
     prm = dict(masse=MASSE, massi=MASSI_XE, Ti=300.0, nu_eff=1e9, flag_Bohm=1, flag_Sagdeev=1,
                dr=dr if dr is not None else 5e-3 / nj, rmin=0.0)
     return dict(fields=f, prm=prm)
+
+
+def pc_state(ni: int, nj: int, seed: int = 4, Lz: float = 10e-3, Lr: float = 5e-3) -> dict:
+    """Seeded state of the potential predictor-corrector in the reference's names.
+
+    rhoe = 1e17 exp(-((z - Lz/2)^2 + r^2) / (2 (Lr/5)^2)) x lognormal(0, 0.1) + 1e14
+    m^-3; rhoi, rhoe_old = rhoe (1 + 0.01 N(0,1)); Te uniform in [1, 10] eV (K);
+    phi = 20 z / Lz + 0.1 N(0,1) V with Ex, Er its face differences (+ 1 % noise);
+    nUex, nUer = rhoe 1e4 N(0,1); Uix, Uir N(0, 1000) m/s; rhoUmx, rhoUmr 1e19 N(0,1);
+    rate_ionize = rhoe 1e5 U(0,1); mobility tensor of B ~ N(0, 0.05) T and a
+    momentum frequency log-uniform in [1e8, 1e10] s^-1 (fluidModule.hpp:5957-5973).
+    Physics parameters: dt 1e-10 s, V_bias 20 V, SEE coefficients 0.08 (params.hpp:62-63),
+    the inner solve of the shipped setup (SMG, 30 iterations, 1e-10) and 2 PC iterations
+    with calcRes mode 3 (input/setup.yaml)."""
+    rng = np.random.default_rng(seed)
+    sh = (ni + 2, nj + 2)
+    dx, dr = Lz / ni, Lr / nj
+    z = (np.arange(ni + 2) - 0.5) * dx
+    r = (np.arange(nj + 2) - 0.5) * dr
+    sig = Lr / 5.0
+    prof = np.exp(-(((z[:, None] - Lz / 2) ** 2) + r[None, :] ** 2) / (2 * sig * sig))
+    f = {}
+    f["rhoe"] = 1e17 * prof * np.exp(0.1 * rng.standard_normal(sh)) + 1e14
+    f["rhoi"] = f["rhoe"] * (1.0 + 0.01 * rng.standard_normal(sh))
+    f["rhoe_old"] = f["rhoe"] * (1.0 + 0.01 * rng.standard_normal(sh))
+    f["Te"] = rng.uniform(1.0, 10.0, sh) * E0 / BOLTZ
+    phi = 20.0 * z[:, None] / Lz + 0.1 * rng.standard_normal(sh)
+    f["phi"] = phi
+    Ex = np.zeros(sh)
+    Er = np.zeros(sh)
+    Ex[1:, :] = -(phi[1:, :] - phi[:-1, :]) / dx
+    Er[:, 1:] = -(phi[:, 1:] - phi[:, :-1]) / dr
+    f["Ex"] = Ex * (1.0 + 0.01 * rng.standard_normal(sh))
+    f["Er"] = Er * (1.0 + 0.01 * rng.standard_normal(sh))
+    f["nUex"] = f["rhoe"] * 1e4 * rng.standard_normal(sh)
+    f["nUer"] = f["rhoe"] * 1e4 * rng.standard_normal(sh)
+    f["Uix"] = 1000.0 * rng.standard_normal(sh)
+    f["Uir"] = 1000.0 * rng.standard_normal(sh)
+    f["rhoUmx"] = 1e19 * rng.standard_normal(sh)
+    f["rhoUmr"] = 1e19 * rng.standard_normal(sh)
+    f["rate_ionize"] = f["rhoe"] * 1e5 * rng.random(sh)
+    Bx = 0.05 * rng.standard_normal(sh)
+    Br = 0.05 * rng.standard_normal(sh)
+    nu_m = 10.0 ** rng.uniform(8.0, 10.0, sh)
+    mu_para = E0 / (MASSE * nu_m + 1e-100)
+    Om = E0 * np.sqrt(Bx * Bx + Br * Br) / (MASSE * nu_m + 1e-100)
+    Omx = E0 * Bx / (MASSE * nu_m + 1e-100)
+    Omr = E0 * Br / (MASSE * nu_m + 1e-100)
+    deno = 1.0 + Om * Om
+    f["mu_para"] = mu_para
+    f["mu_xx"] = mu_para * (1.0 + Omx * Omx) / deno
+    f["mu_rr"] = mu_para * (1.0 + Omr * Omr) / deno
+    f["mu_xr"] = mu_para * (Omx * Omr) / deno
+    f["mu_perp"] = mu_para / deno
+    prm = dict(dt=1e-10, dx=dx, dr=dr, rmin=0.0, V_bias=20.0, masse=MASSE, coefIISEE_ts=0.08,
+               coefMISEE_ts=0.08, error_cnv_HES_phi=1e-21, error_cnv_SOR_phi=1e-10, maxITR_HES_phi=2,
+               maxITR_SOR_phi=30, flag_error=3, flag_iter_phi=1, precision=1)
+    return dict(fields=f, prm=prm)

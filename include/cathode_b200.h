@@ -199,6 +199,7 @@ int cth_mw_er_assemble_dev(cth_grid* g, const double* ne, const double* nu, cons
 #define CTH_F_BLR_CEN 8
 #define CTH_F_BRR_WALL 16
 #define CTH_F_BRR_OPEN 32
+#define CTH_F_BRX_BIAS 64 /* the right wall is the biased electrode (z5, fluidModule.hpp:2196-2199) */
 typedef struct cth_fields cth_fields;
 int cth_fields_create(cth_grid* g, cth_fields** out);
 void cth_fields_destroy(cth_fields* fs);
@@ -222,6 +223,37 @@ typedef struct cth_transport_params {
     int flag_Bohm, flag_Sagdeev;
 } cth_transport_params;
 int cth_update_transport_coef(cth_fields* fs, const cth_transport_params* prm, void* stream);
+
+/* FluidModule::solve_phi_couple_wdTe_wSEE_PC (fluidModule.hpp:2080-3075):
+ * predictor-corrector for the potential with dielectric relaxation.  Reads the
+ * store's rhoe, rhoe_old, rhoi, Te, mu_para, mu_perp, mu_rr, mu_xr, mu_xx,
+ * rate_ionize, Uix, Uir, rhoUmx, rhoUmr and the SEE tables coefEISEE_eb_table,
+ * coefEISEE_rd_table, coefEISEE_ts_table; updates phi, Ex, Er, nUex, nUer and
+ * phi_old, nUex_old, nUer_old (the values at entry).  The grid's blocks must be
+ * the fluid blocks the side flags describe.  The inner solve is the SMG
+ * replacement (flag_iter_phi != 0, precision as cth_smg_solve_dev) or SOR with
+ * alpha 1.9 (flag_iter_phi == 0), from zero, with maxITR_SOR_phi and
+ * error_cnv_SOR_phi.  The loop ends when the largest calcRes of phi, nUex, nUer
+ * over one iteration is below error_cnv_HES_phi or after maxITR_HES_phi
+ * iterations.  Synchronises the stream once per iteration. */
+typedef struct cth_phi_params {
+    double dt, dx, dr, rmin, V_bias, masse;
+    double coefIISEE_ts, coefMISEE_ts, dTe_SEE;
+    double error_cnv_HES_phi, error_cnv_SOR_phi;
+    int maxITR_HES_phi, maxITR_SOR_phi;
+    int flag_error;     /* calcRes mode 0..3 (miniFuncs.hpp:292-376) */
+    int flag_iter_phi;  /* 0: SOR, otherwise SMG                     */
+    int precision;      /* CTH_PREC_MIXED or CTH_PREC_FP64           */
+} cth_phi_params;
+
+typedef struct cth_pc_result {
+    int ncount;            /* PC iterations taken                                 */
+    int solver_rc;         /* largest positive return of the inner solves (0 ok)  */
+    double error_phi, error_nUex, error_nUer;  /* calcRes against the entry values */
+    double error_iter[3];  /* calcRes of the last iteration (phi, nUex, nUer)      */
+    cth_status solver;     /* status of the last inner solve                      */
+} cth_pc_result;
+int cth_solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, void* stream, cth_pc_result* res);
 
 /* Residual (device arrays): r = b - A x on grid cells (couplings to non-grid
  * cells dropped), r = 0 elsewhere; *rnorm = ||r||_2, *bnorm = ||b||_2 over grid

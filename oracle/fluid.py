@@ -13,8 +13,10 @@ BOLTZ = 1.380649e-23
 E0 = 1.60217662e-19
 EPS0 = 8.8541878128e-12
 
-# boundary flag bits of a cell (1 = the side is an ordinary interior face)
+# boundary flag bits of a cell (1 = the side is an ordinary interior face);
+# F_BRX_BIAS marks the cells whose right wall is the biased electrode
 F_BLX, F_BRX, F_BLR_WALL, F_BLR_CEN, F_BRR_WALL, F_BRR_OPEN = 1, 2, 4, 8, 16, 32
+F_BRX_BIAS = 64
 
 
 def cathode_blocks(ni: int = 194, nj: int = 70, xR: float = 0.0388, rmax: float = 0.014):
@@ -55,7 +57,8 @@ def cathode_flags(ni, nj, ib, jb) -> np.ndarray:
                 bRr_wall = bRr_wall and (j != jb[3][1] or i < ib[1][1] + 1 or i > ib[3][1])
                 bRr_open = (j != jb[4][1] or blk != 4)
                 fl[i, j] = (F_BLX * bLx | F_BRX * bRx | F_BLR_WALL * bLr_wall | F_BLR_CEN * bLr_cen |
-                            F_BRR_WALL * bRr_wall | F_BRR_OPEN * bRr_open)
+                            F_BRR_WALL * bRr_wall | F_BRR_OPEN * bRr_open |
+                            F_BRX_BIAS * (blk == 4 and i == ib[4][1]))
     return fl
 
 
@@ -65,7 +68,8 @@ def rectangle_flags(ni, nj) -> np.ndarray:
     i = np.arange(1, ni + 1)[:, None]
     j = np.arange(1, nj + 1)[None, :]
     fl[1:ni + 1, 1:nj + 1] = (F_BLX * (i != 1) | F_BRX * (i != ni) | F_BLR_WALL |
-                              F_BLR_CEN * (j != 1) | F_BRR_WALL * (j != nj) | F_BRR_OPEN)
+                              F_BLR_CEN * (j != 1) | F_BRR_WALL * (j != nj) | F_BRR_OPEN |
+                              F_BRX_BIAS * (i == ni))
     return fl
 
 
@@ -243,3 +247,297 @@ def bolsig_tables(text_e: str, text_i: str):
     tb["nui_m_N"] = data_i.sum(axis=1)
     delta_i = float(rows_i[3][0]) - float(rows_i[2][0])
     return tb, delta * 2.0 / 3.0 * E0 / BOLTZ, delta_i * E0
+
+
+def see_tables(text: str):
+    """InputModule::input_SEE_data (inputModule.hpp:605-657): columns EB, RD, TS
+    of coefEISEE.csv against mean energy; dTe_SEE = delta*0.5*e/k_B."""
+    rows = [ln.split(",") for ln in text.splitlines() if ln.strip()][1:]
+    a = np.array([[float(v) for v in r[:4]] for r in rows])
+    return a[:, 1].copy(), a[:, 2].copy(), a[:, 3].copy(), (a[1, 0] - a[0, 0]) * 0.5 * E0 / BOLTZ
+
+
+# ----------------------------------------------------------------------------
+# geometry of the PC sweeps: cell blocks, face blocks and the wall segments in
+# the order the reference visits them
+# ----------------------------------------------------------------------------
+
+def cathode_geometry(ni: int = 194, nj: int = 70, xR: float = 0.0388, rmax: float = 0.014) -> dict:
+    """Cell blocks, x-/r-face blocks (initialModule.hpp:219-345) and the wall
+    segments of solve_phi_couple_wdTe_wSEE_PC (fluidModule.hpp:2149-2240):
+    kind L/R/RB (left, right, right at V_bias), D/U (lower, upper wall),
+    O (upper open); each (kind, i0, i1, j0, j1) over cells."""
+    dx, dr = xR / ni, rmax / nj
+    x2, x3, x4, x5, x6 = 5.6e-3 + 7.8e-3, 10.0e-3 + 7.8e-3, 15.0e-3 + 7.8e-3, 20.0e-3 + 7.8e-3, 7.8e-3
+    r1, r3, r4, r5 = 0.6e-3, 4.0e-3, 9.0e-3, 2.0e-3
+    ib, jb = cathode_blocks(ni, nj, xR, rmax)
+    lo = lambda v, d, k: int(v / d + 0.5) + k
+    hi = lambda v, d, k: int(v / d - 0.5) + k
+    fxi = [[lo(x6, dx, 2), hi(x2, dx, 2)], [lo(x2, dx, 2), hi(x4, dx, 1)], [lo(x2, dx, 2), hi(x3, dx, 2)],
+           [lo(x3, dx, 2), hi(x5, dx, 2)], [lo(x5, dx, 2), hi(xR, dx, 1)]]
+    fxj = [[lo(r3, dr, 1), hi(r4, dr, 1)], [lo(r5, dr, 1), hi(r4, dr, 1)], [lo(r1, dr, 1), hi(r5, dr, 1)],
+           [lo(0.0, dr, 1), hi(r5, dr, 1)], [lo(0.0, dr, 1), hi(rmax, dr, 1)]]
+    fri = [[lo(x6, dx, 1), hi(x2, dx, 1)], [lo(x2, dx, 1), hi(x4, dx, 1)], [lo(x2, dx, 1), hi(x3, dx, 1)],
+           [lo(x3, dx, 1), hi(x5, dx, 1)], [lo(x5, dx, 1), hi(xR, dx, 1)]]
+    frj = [[lo(r3, dr, 2), hi(r4, dr, 1)], [lo(r5, dr, 1), hi(r4, dr, 1)], [lo(r1, dr, 2), hi(r5, dr, 1)],
+           [lo(0.0, dr, 2), hi(r5, dr, 1)], [lo(0.0, dr, 2), hi(rmax, dr, 1)]]
+    segs = [("L", ib[0][0], ib[0][0], jb[0][0], jb[0][1]),          # z0
+            ("L", ib[2][0], ib[2][0], jb[2][0], jb[0][0] - 1),      # z1
+            ("L", ib[3][0], ib[3][0], jb[3][0], jb[2][0] - 1),      # z2
+            ("L", ib[4][0], ib[4][0], jb[1][0], jb[4][1]),          # z4
+            ("R", ib[1][1], ib[1][1], jb[1][0], jb[1][1]),          # z3
+            ("RB", ib[4][1], ib[4][1], jb[4][0], jb[4][1]),         # z5
+            ("D", ib[0][0], ib[0][1], jb[0][0], jb[0][0]),          # x0
+            ("D", ib[2][0], ib[2][1], jb[2][0], jb[2][0]),          # x2
+            ("U", ib[0][0], ib[1][1], jb[0][1], jb[0][1]),          # x1
+            ("U", ib[1][1] + 1, ib[3][1], jb[3][1], jb[3][1]),      # x4
+            ("O", ib[4][0], ib[4][1], jb[4][1], jb[4][1])]          # x5
+    return dict(ni=ni, nj=nj, dx=dx, dr=dr, ib=ib, jb=jb, fxi=np.array(fxi), fxj=np.array(fxj),
+                fri=np.array(fri), frj=np.array(frj), segs=segs, flags=cathode_flags(ni, nj, ib, jb))
+
+
+def rectangle_geometry(ni: int, nj: int, Lz: float = 10e-3, Lr: float = 5e-3) -> dict:
+    """The r-z rectangle as one fluid block: z = 0 wall (0 V, like z0), z = L
+    biased electrode (like z5), r = R wall (like x1), r = 0 axis."""
+    one = lambda a, b: np.array([[a, b]])
+    segs = [("L", 1, 1, 1, nj), ("RB", ni, ni, 1, nj), ("U", 1, ni, nj, nj)]
+    return dict(ni=ni, nj=nj, dx=Lz / ni, dr=Lr / nj, ib=one(1, ni), jb=one(1, nj), fxi=one(2, ni),
+                fxj=one(1, nj), fri=one(1, ni), frj=one(2, nj), segs=segs, flags=rectangle_flags(ni, nj))
+
+
+def calc_res(new, old, ib, jb, eps, flag_error):
+    """calcRes (miniFuncs.hpp:292-376) over the blocks (ib, jb)."""
+    d = np.concatenate([(new[a:b + 1, c:e + 1] - old[a:b + 1, c:e + 1]).ravel()
+                        for (a, b), (c, e) in zip(ib, jb)])
+    o = np.concatenate([old[a:b + 1, c:e + 1].ravel() for (a, b), (c, e) in zip(ib, jb)])
+    if flag_error == 0:
+        return float(np.abs(d).max())
+    if flag_error == 1:
+        return float(np.sqrt(np.sum(d ** 2 / (o ** 2 + eps)) / d.size))
+    if flag_error == 2:
+        return float(np.abs(d).max() / np.abs(o).max())
+    return float(np.sqrt(np.sum(d ** 2) / np.sum(o ** 2)))
+
+
+PHI_FIELDS = ("phi", "Ex", "Er", "nUex", "nUer")
+
+
+def _wall_flux(Te, rhoe, rhoe_old, rhoi, Ui, rhoUm, E_old, h, sign, prm, see):
+    """Thermal + SEE electron flux through a wall face (fluidModule.hpp:2348-2457):
+    sign -1 for a wall on the low side of the cell, +1 on the high side."""
+    vth = np.sqrt(8.0 * BOLTZ * Te / (np.pi * prm["masse"]))
+    delta_phi = np.fmax(sign * E_old * h / 2.0, 0.0)
+    gpn = sign * 0.25 * vth * np.exp(np.fmin(-E0 * delta_phi / (BOLTZ * Te + 1e-100), 100.0))
+    eb, rd, ts, dTe_SEE = see
+    c = func_Te(eb, Te, dTe_SEE) + func_Te(rd, Te, dTe_SEE) + func_Te(ts, Te, dTe_SEE)
+    see_flux = -prm["coefIISEE_ts"] * rhoi * Ui - c * rhoe_old * gpn - prm["coefMISEE_ts"] * rhoUm
+    return rhoe * gpn + see_flux
+
+
+def solve_phi_pc(st: dict, prm: dict, geo: dict, see, solve) -> dict:
+    """FluidModule::solve_phi_couple_wdTe_wSEE_PC (fluidModule.hpp:2080-3075).
+
+    st: phi, Ex, Er, nUex, nUer, rhoe, rhoe_old, rhoi, Te, mu_para, mu_perp,
+    mu_rr, mu_xr, mu_xx, rate_ionize, Uix, Uir, rhoUmx, rhoUmr (updated copies of
+    phi, Ex, Er, nUex, nUer are returned with the residuals).  prm: dt, dx, dr,
+    rmin, V_bias, masse, coefIISEE_ts, coefMISEE_ts, maxITR_HES_phi,
+    error_cnv_HES_phi, flag_error.  see: (eb, rd, ts, dTe_SEE).
+    solve(aP, aE, aW, aN, aS, b, ib, jb) -> block-cell solution (zero start).
+    The sweeps run block by block over the face / cell blocks of ``geo`` and
+    the wall segments in the reference's order."""
+    ni, nj = geo["ni"], geo["nj"]
+    dx, dr, dt = prm["dx"], prm["dr"], prm["dt"]
+    r = prm["rmin"] + (np.arange(nj + 2) - 0.5) * dr
+    fl = geo["flags"].astype(np.int64)
+    bLx_c = (fl & F_BLX) != 0
+    bRx_c = (fl & F_BRX) != 0
+    bLr_c = ((fl & F_BLR_WALL) != 0) & ((fl & F_BLR_CEN) != 0)
+    bRrw_c = (fl & F_BRR_WALL) != 0
+    bRr_c = bRrw_c & ((fl & F_BRR_OPEN) != 0)
+    g = {k: st[k] for k in st}
+    phi, Ex, Er = st["phi"].copy(), st["Ex"].copy(), st["Er"].copy()
+    nUex, nUer = st["nUex"].copy(), st["nUer"].copy()
+    phi_old, Ex_old, Er_old, nUex_old, nUer_old = phi.copy(), Ex.copy(), Er.copy(), nUex.copy(), nUer.copy()
+    dphi = phi - phi_old
+    segs = geo["segs"]
+    # ghost potentials of the walls, once before the iteration (:2149-2240)
+    for kind, i0, i1, j0, j1 in segs:
+        I, J = slice(i0, i1 + 1), slice(j0, j1 + 1)
+        if kind == "L":
+            phi[i0 - 1, J] = -phi[i0, J]
+        elif kind == "R":
+            phi[i0 + 1, J] = -phi[i0, J]
+        elif kind == "RB":
+            phi[i0 + 1, J] = 2.0 * prm["V_bias"] - phi[i0, J]
+        elif kind in ("D",):
+            phi[I, j0 - 1] = -phi[I, j0]
+        elif kind == "U":
+            phi[I, j0 + 1] = -phi[I, j0]
+        else:
+            phi[I, j0 + 1] = phi[I, j0]
+    mu_para, mu_perp, rhoe, Te = g["mu_para"], g["mu_perp"], g["rhoe"], g["Te"]
+    ncount = 0
+    errs = (0.0, 0.0, 0.0)
+    while True:
+        ncount += 1
+        phi_t, nUex_t, nUer_t = phi.copy(), nUex.copy(), nUer.copy()
+        # predicted x flux on the x-face blocks (:2266-2343)
+        for (a, b), (c, e) in zip(geo["fxi"], geo["fxj"]):
+            I = np.arange(a, b + 1)[:, None]
+            J = np.arange(c, e + 1)[None, :]
+            rL = (r[J] + r[J - 1]) / 2.0
+            rR = (r[J] + r[J + 1]) / 2.0
+            mpa = (mu_para[I, J] + mu_para[I - 1, J]) / 2.0
+            mpe = (mu_perp[I, J] + mu_perp[I - 1, J]) / 2.0
+            mst = mpe * 1.0
+            mrr = (g["mu_rr"][I, J] + g["mu_rr"][I - 1, J]) / 2.0
+            mxr = (g["mu_xr"][I, J] + g["mu_xr"][I - 1, J]) / 2.0
+            ixx = mrr / (mpa * mpe)
+            ixr = -mxr / (mpa * mpe)
+            rho_t = (rhoe[I, J] + rhoe[I - 1, J]) / 2.0
+            dphidx = (phi[I, J] - phi[I - 1, J]) / dx
+            dpedx = BOLTZ * (rhoe[I, J] * Te[I, J] - rhoe[I - 1, J] * Te[I - 1, J]) / dx
+            bLr, bLrD = bLr_c[I, J], bLr_c[I - 1, J]
+            bRr, bRrD = bRrw_c[I, J], bRrw_c[I - 1, J]
+            nUer_i = (rR * nUer_t[I, J + 1] * bRr + rL * nUer_t[I, J] * bLr
+                      + rR * nUer_t[I - 1, J + 1] * bRrD + rL * nUer_t[I - 1, J] * bLrD) / (4.0 * r[J])
+            nUex[I, J] = (nUex_t[I, J] - (ixx * nUex_t[I, J] + ixr * nUer_i) * mst
+                          + mst * (rho_t * dphidx - dpedx / E0))
+        # x walls (:2346-2457)
+        for kind, i0, i1, j0, j1 in segs:
+            J = np.arange(j0, j1 + 1)
+            if kind == "L":
+                nUex[i0, J] = _wall_flux(Te[i0, J], rhoe[i0, J], g["rhoe_old"][i0, J], g["rhoi"][i0, J],
+                                         g["Uix"][i0, J], g["rhoUmx"][i0, J], Ex_old[i0, J], dx, -1.0, prm, see)
+            elif kind in ("R", "RB"):
+                nUex[i0 + 1, J] = _wall_flux(Te[i0, J], rhoe[i0, J], g["rhoe_old"][i0, J], g["rhoi"][i0, J],
+                                             g["Uix"][i0 + 1, J], g["rhoUmx"][i0 + 1, J], Ex_old[i0 + 1, J], dx,
+                                             1.0, prm, see)
+        # predicted r flux on the r-face blocks (:2459-2541)
+        for (a, b), (c, e) in zip(geo["fri"], geo["frj"]):
+            I = np.arange(a, b + 1)[:, None]
+            J = np.arange(c, e + 1)[None, :]
+            r_t = (r[J] + r[J - 1]) / 2.0
+            mpa = (mu_para[I, J] + mu_para[I, J - 1]) / 2.0
+            mpe = (mu_perp[I, J] + mu_perp[I, J - 1]) / 2.0
+            mst = mpe * 1.0
+            mxx = (g["mu_xx"][I, J] + g["mu_xx"][I, J - 1]) / 2.0
+            mxr = (g["mu_xr"][I, J] + g["mu_xr"][I, J - 1]) / 2.0
+            irr = mxx / (mpa * mpe)
+            ixr = -mxr / (mpa * mpe)
+            rho_t = (rhoe[I, J] + rhoe[I, J - 1]) / 2.0
+            dphidr = (phi[I, J] - phi[I, J - 1]) / dr
+            dpedr = BOLTZ * (rhoe[I, J] * Te[I, J] - rhoe[I, J - 1] * Te[I, J - 1]) / dr
+            bLx, bLxD = bLx_c[I, J], bLx_c[I, J - 1]
+            bRx, bRxD = bRx_c[I, J], bRx_c[I, J - 1]
+            nUex_i = (r[J] * nUex_t[I + 1, J] * bRx + r[J] * nUex_t[I, J] * bLx
+                      + r[J - 1] * nUex_t[I + 1, J - 1] * bRxD + r[J - 1] * nUex_t[I, J - 1] * bLxD) / (4.0 * r_t)
+            nUer[I, J] = (nUer_t[I, J] - (ixr * nUex_i + irr * nUer_t[I, J]) * mst
+                          + mst * (rho_t * dphidr - dpedr / E0))
+        # r walls and the open top (:2544-2633)
+        for kind, i0, i1, j0, j1 in segs:
+            I = np.arange(i0, i1 + 1)
+            if kind == "D":
+                nUer[I, j0] = _wall_flux(Te[I, j0], rhoe[I, j0], g["rhoe_old"][I, j0], g["rhoi"][I, j0],
+                                         g["Uir"][I, j0], g["rhoUmr"][I, j0], Er_old[I, j0], dr, -1.0, prm, see)
+            elif kind == "U":
+                nUer[I, j0 + 1] = _wall_flux(Te[I, j0], rhoe[I, j0], g["rhoe_old"][I, j0], g["rhoi"][I, j0],
+                                             g["Uir"][I, j0 + 1], g["rhoUmr"][I, j0 + 1], Er_old[I, j0 + 1], dr,
+                                             1.0, prm, see)
+            elif kind == "O":
+                nUer[I, j0 + 1] = g["rhoi"][I, j0] * g["Uir"][I, j0 + 1]
+        # Poisson coefficients with dielectric relaxation (:2636-2716)
+        sh = (ni + 2, nj + 2)
+        aP, aE, aW, aN, aS, bb = (np.zeros(sh) for _ in range(6))
+        for (a, b), (c, e) in zip(geo["ib"], geo["jb"]):
+            I = np.arange(a, b + 1)[:, None]
+            J = np.arange(c, e + 1)[None, :]
+            rR = (r[J] + r[J + 1]) / 2.0
+            rL = (r[J] + r[J - 1]) / 2.0
+            qR = (r[J] + r[J + 1]) / 2.0 / r[J]
+            qL = (r[J] + r[J - 1]) / 2.0 / r[J]
+            mLx = (mu_perp[I, J] + mu_perp[I - 1, J]) / 2.0 * 1.0
+            mRx = (mu_perp[I, J] + mu_perp[I + 1, J]) / 2.0 * 1.0
+            mLr = (mu_perp[I, J] + mu_perp[I, J - 1]) / 2.0 * 1.0
+            mRr = (mu_perp[I, J] + mu_perp[I, J + 1]) / 2.0 * 1.0
+            nLx = (rhoe[I, J] + rhoe[I - 1, J]) / 2.0
+            nRx = (rhoe[I, J] + rhoe[I + 1, J]) / 2.0
+            nLr = (rhoe[I, J] + rhoe[I, J - 1]) / 2.0
+            nRr = (rhoe[I, J] + rhoe[I, J + 1]) / 2.0
+            bLx, bRx, bLr, bRr = bLx_c[I, J], bRx_c[I, J], bLr_c[I, J], bRr_c[I, J]
+            aP[I, J] = (((EPS0 + E0 * dt * nRx * mRx * bRx) + (EPS0 + E0 * dt * nLx * mLx * bLx)) * dr * dr
+                        + (qR * (EPS0 + E0 * dt * nRr * mRr * bRr) + qL * (EPS0 + E0 * dt * nLr * mLr * bLr))
+                        * dx * dx)
+            aE[I, J] = (EPS0 + E0 * dt * nRx * mRx * bRx) * dr * dr
+            aW[I, J] = (EPS0 + E0 * dt * nLx * mLx * bLx) * dr * dr
+            aN[I, J] = qR * (EPS0 + E0 * dt * nRr * mRr * bRr) * dx * dx
+            aS[I, J] = qL * (EPS0 + E0 * dt * nLr * mLr * bLr) * dx * dx
+            div = (nUex[I + 1, J] - nUex[I, J]) / dx + (qR * nUer[I, J + 1] - qL * nUer[I, J]) / dr
+            lap = -(Ex[I + 1, J] - Ex[I, J]) / dx - (qR * Er[I, J + 1] - qL * Er[I, J]) / dr
+            bb[I, J] = ((E0 * g["rhoi"][I, J] - E0 * rhoe[I, J] - E0 * dt * g["rate_ionize"][I, J]
+                         + EPS0 * lap + E0 * dt * div) * dx * dx * dr * dr)
+        # wall conditions on the coefficients (:2720-2816)
+        for kind, i0, i1, j0, j1 in segs:
+            I, J = slice(i0, i1 + 1), slice(j0, j1 + 1)
+            if kind == "L":
+                aP[i0, J] += aW[i0, J]; aW[i0, J] = 0.0
+            elif kind in ("R", "RB"):
+                aP[i0, J] += aE[i0, J]; aE[i0, J] = 0.0
+            elif kind == "D":
+                aP[I, j0] += aS[I, j0]; aS[I, j0] = 0.0
+            elif kind == "U":
+                aP[I, j0] += aN[I, j0]; aN[I, j0] = 0.0
+            else:
+                aP[I, j0] -= aN[I, j0]; aN[I, j0] = 0.0
+        x = solve(aP, aE, aW, aN, aS, bb, geo["ib"], geo["jb"])
+        for (a, b), (c, e) in zip(geo["ib"], geo["jb"]):
+            dphi[a:b + 1, c:e + 1] = x[a:b + 1, c:e + 1]
+        # ghost corrections and wall fields (:2836-2928)
+        for kind, i0, i1, j0, j1 in segs:
+            I, J = slice(i0, i1 + 1), slice(j0, j1 + 1)
+            if kind == "L":
+                dphi[i0 - 1, J] = -dphi[i0, J]
+                Ex[i0, J] = Ex[i0, J] - (dphi[i0, J] - dphi[i0 - 1, J]) / dx
+            elif kind in ("R", "RB"):
+                dphi[i0 + 1, J] = -dphi[i0, J]
+                Ex[i0 + 1, J] = Ex[i0 + 1, J] - (dphi[i0 + 1, J] - dphi[i0, J]) / dx
+            elif kind == "D":
+                dphi[I, j0 - 1] = -dphi[I, j0]
+                Er[I, j0] = Er[I, j0] - (dphi[I, j0] - dphi[I, j0 - 1]) / dr
+            elif kind == "U":
+                dphi[I, j0 + 1] = -dphi[I, j0]
+                Er[I, j0 + 1] = Er[I, j0 + 1] - (dphi[I, j0 + 1] - dphi[I, j0]) / dr
+            else:
+                dphi[I, j0 + 1] = dphi[I, j0]
+                Er[I, j0 + 1] = 0.0
+        phi = phi + dphi
+        # fields and flux corrections on the face blocks (:2932-3024)
+        for (a, b), (c, e) in zip(geo["fxi"], geo["fxj"]):
+            I, J = slice(a, b + 1), slice(c, e + 1)
+            Im = slice(a - 1, b)
+            Ex[I, J] = -(phi[I, J] - phi[Im, J]) / dx
+        for (a, b), (c, e) in zip(geo["fri"], geo["frj"]):
+            I, J, Jm = slice(a, b + 1), slice(c, e + 1), slice(c - 1, e)
+            Er[I, J] = -(phi[I, J] - phi[I, Jm]) / dr
+        for (a, b), (c, e) in zip(geo["fxi"], geo["fxj"]):
+            I, J, Im = slice(a, b + 1), slice(c, e + 1), slice(a - 1, b)
+            mst = (mu_perp[I, J] + mu_perp[Im, J]) / 2.0 * 1.0
+            rho_t = (rhoe[I, J] + rhoe[Im, J]) / 2.0
+            nUex[I, J] = nUex[I, J] + mst * rho_t * ((dphi[I, J] - dphi[Im, J]) / dx)
+        for (a, b), (c, e) in zip(geo["fri"], geo["frj"]):
+            I, J, Jm = slice(a, b + 1), slice(c, e + 1), slice(c - 1, e)
+            mst = (mu_perp[I, J] + mu_perp[I, Jm]) / 2.0 * 1.0
+            rho_t = (rhoe[I, J] + rhoe[I, Jm]) / 2.0
+            nUer[I, J] = nUer[I, J] + mst * rho_t * ((dphi[I, J] - dphi[I, Jm]) / dr)
+        fe = prm["flag_error"]
+        errs = (calc_res(phi, phi_t, geo["ib"], geo["jb"], 1e-100, fe),
+                calc_res(nUex, nUex_t, geo["fxi"], geo["fxj"], 1e-100, fe),
+                calc_res(nUer, nUer_t, geo["fri"], geo["frj"], 1e-100, fe))
+        if max(errs) < prm["error_cnv_HES_phi"] or ncount >= prm["maxITR_HES_phi"]:
+            break
+    fe = prm["flag_error"]
+    out = dict(phi=phi, Ex=Ex, Er=Er, nUex=nUex, nUer=nUer, ncount=ncount, errors_last=errs)
+    out["error_phi"] = calc_res(phi, phi_old, geo["ib"], geo["jb"], 1e-100, fe)
+    out["error_nUex"] = calc_res(nUex, nUex_old, geo["fxi"], geo["fxj"], 1e-100, fe)
+    out["error_nUer"] = calc_res(nUer, nUer_old, geo["fri"], geo["frj"], 1e-100, fe)
+    return out

@@ -1,10 +1,12 @@
-"""Build the rate-table fixture from the reference's BOLSIG+ input files.
+"""Build the rate-table fixtures from the reference's input files.
 
 Source: the reference's input/rateCoef_e.csv (electron collision rates against
 mean energy, 1800 rows) and input/rateCoef_i.csv (ion momentum-transfer rate),
 read the way InputModule::input_BOLSIG_data does (inputModule.hpp:1413-1655),
-restated by oracle.fluid.bolsig_tables.  Output: rate_tables.npz with the eleven
-BolsigVec tables and the steps dTe (K) and dEi (J).
+restated by oracle.fluid.bolsig_tables -> rate_tables.npz with the eleven
+BolsigVec tables and the steps dTe (K) and dEi (J); input/coefEISEE.csv read as
+InputModule::input_SEE_data (inputModule.hpp:605-657), oracle.fluid.see_tables
+-> see_tables.npz with the EB, RD, TS yields and dTe_SEE (K).
 Run in a checkout that has the reference under /root/reference.
 """
 import os
@@ -26,6 +28,11 @@ def main():
     out = os.path.join(HERE, "rate_tables.npz")
     np.savez_compressed(out, dTe=dTe, dEi=dEi, **tb)
     print(out, {k: v.shape for k, v in tb.items()}, dTe, dEi)
+    eb, rd, ts, dTe_SEE = fluid.see_tables(open(os.path.join(SRC, "coefEISEE.csv")).read())
+    out = os.path.join(HERE, "see_tables.npz")
+    np.savez_compressed(out, coefEISEE_eb_table=eb, coefEISEE_rd_table=rd, coefEISEE_ts_table=ts,
+                        dTe_SEE=dTe_SEE)
+    print(out, eb.shape, dTe_SEE)
 
 
 if __name__ == "__main__":

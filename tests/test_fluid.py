@@ -87,7 +87,7 @@ def test_cathode_flags_host_helper_matches_oracle(pkg):
     b = pkg.fluid.cathode_flags(194, 70, *pkg.fluid.cathode_blocks())
     assert (a == b).all()
     # the axis and the anode (last column) are the only boundaries of block 4's corner cell
-    assert a[194, 1] == fluid.F_BLX | fluid.F_BLR_WALL | fluid.F_BRR_WALL | fluid.F_BRR_OPEN
+    assert a[194, 1] == fluid.F_BLX | fluid.F_BLR_WALL | fluid.F_BRR_WALL | fluid.F_BRR_OPEN | fluid.F_BRX_BIAS
     assert (a[0, :] == 0).all() and (a[:, 0] == 0).all() and (a[:, -1] == 0).all()
     assert (pkg.fluid.rectangle_flags(12, 9) == fluid.rectangle_flags(12, 9)).all()
 
@@ -114,3 +114,68 @@ def test_transport_oracle_limits():
     assert np.all(out["mu_xr"] == 0)
     assert np.allclose(out["nu_m"], out["nu_elas"] + f["nu_ano"] + out["nu_ano_IAT"], rtol=1e-14)
     assert out["nu_ano_IAT"][3, 3] == 0.0 and out["nu_ano_IAT"][4, 4] > 0.0
+
+
+@pytest.mark.parametrize("kind", ["cathode", "rectangle"])
+def test_pc_geometry_flags_match_reference_blocks(kind):
+    """The side-flag rules the device kernels use (interior face = both cells in
+    the fluid, wall face = cleared bit) select exactly the reference's face
+    blocks and wall segments."""
+    from oracle import fluid
+    geo = fluid.cathode_geometry() if kind == "cathode" else fluid.rectangle_geometry(30, 20)
+    fl = geo["flags"]
+    F = fl != 0
+    ix = np.zeros_like(F); ix[1:, :] = F[1:, :] & F[:-1, :]
+    ir = np.zeros_like(F); ir[:, 1:] = F[:, 1:] & F[:, :-1]
+    bx = np.zeros_like(F); br = np.zeros_like(F)
+    for (a, b), (c, e) in zip(geo["fxi"], geo["fxj"]):
+        assert not bx[a:b + 1, c:e + 1].any()
+        bx[a:b + 1, c:e + 1] = True
+    for (a, b), (c, e) in zip(geo["fri"], geo["frj"]):
+        assert not br[a:b + 1, c:e + 1].any()
+        br[a:b + 1, c:e + 1] = True
+    assert (ix == bx).all() and (ir == br).all()
+    seg = {k: np.zeros_like(F) for k in ("L", "R", "RB", "D", "U", "O")}
+    for k, i0, i1, j0, j1 in geo["segs"]:
+        seg[k][i0:i1 + 1, j0:j1 + 1] = True
+    cleared = lambda bit: F & ((fl & bit) == 0)
+    assert (cleared(fluid.F_BLX) == seg["L"]).all()
+    assert (cleared(fluid.F_BRX) == (seg["R"] | seg["RB"])).all()
+    assert (((fl & fluid.F_BRX_BIAS) != 0) == seg["RB"]).all()
+    assert (cleared(fluid.F_BLR_WALL) == seg["D"]).all()
+    assert (cleared(fluid.F_BRR_WALL) == seg["U"]).all()
+    assert (cleared(fluid.F_BRR_OPEN) == seg["O"]).all()
+    # every wall ghost lies outside the fluid
+    assert not (F[:-1, :] & seg["L"][1:, :]).any() and not (F[1:, :] & (seg["R"] | seg["RB"])[:-1, :]).any()
+    assert not (F[:, :-1] & seg["D"][:, 1:]).any() and not (F[:, 1:] & (seg["U"] | seg["O"])[:, :-1]).any()
+
+
+def test_phi_pc_oracle_properties(orc):
+    """Rectangle PC step in the oracle: the wall ghosts keep their Dirichlet
+    relations, the interior fields are the potential's differences, and the
+    assembled Poisson system is solved."""
+    from oracle import fluid
+    import importlib
+    import __graft_entry__
+    wl = importlib.import_module(__graft_entry__.load_package().__name__ + ".workloads")
+    geo = fluid.rectangle_geometry(24, 16)
+    st = wl.pc_state(24, 16, seed=7)
+    z = np.load(os.path.join(HERE, "golden", "see_tables.npz"))
+    see = (z["coefEISEE_eb_table"], z["coefEISEE_rd_table"], z["coefEISEE_ts_table"], float(z["dTe_SEE"]))
+    prm = dict(st["prm"], dTe_SEE=float(z["dTe_SEE"]))
+    res = []
+
+    def solve(aP, aE, aW, aN, aS, b, ib, jb):
+        s = dict(ni=24, nj=16, i_bl=ib, j_bl=jb, aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b)
+        x = orc.direct_solve(s)
+        res.append(orc.residual(s, x)[1] / orc.residual(s, np.zeros_like(x))[1])
+        return x
+
+    out = fluid.solve_phi_pc(st["fields"], prm, geo, see, solve)
+    phi = out["phi"]
+    assert out["ncount"] == 2 and max(res) < 1e-12
+    np.testing.assert_allclose(phi[0, 1:17], -phi[1, 1:17], rtol=1e-12)
+    np.testing.assert_allclose(phi[25, 1:17], 2 * 20.0 - phi[24, 1:17], rtol=1e-12)
+    np.testing.assert_allclose(phi[1:25, 17], -phi[1:25, 16], rtol=1e-12)
+    np.testing.assert_allclose(out["Ex"][2:25, 1:17], -(phi[2:25, 1:17] - phi[1:24, 1:17]) / prm["dx"], rtol=1e-12)
+    np.testing.assert_allclose(out["Er"][1:25, 2:17], -(phi[1:25, 2:17] - phi[1:25, 1:16]) / prm["dr"], rtol=1e-12)
