@@ -33,6 +33,7 @@ EXPORTS = (
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_fields_create", "cth_fields_destroy", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
+    "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -75,7 +76,15 @@ class PhiParams(ctypes.Structure):
 class PCResult(ctypes.Structure):
     _fields_ = [("ncount", ctypes.c_int), ("solver_rc", ctypes.c_int), ("error_phi", ctypes.c_double),
                 ("error_nUex", ctypes.c_double), ("error_nUer", ctypes.c_double),
-                ("error_iter", ctypes.c_double * 3), ("solver", Status)]
+                ("error_iter", ctypes.c_double * 3), ("solver", Status), ("Ii_Anode", ctypes.c_double),
+                ("Ie_Anode", ctypes.c_double), ("I_Anode", ctypes.c_double)]
+
+
+class SGParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("dt", "dx", "dr", "rmin", "masse", "coefIISEE_ts", "coefMISEE_ts",
+                                               "dTe_SEE", "Te_emitSEE_eV", "ratioEngy_EISEE_rd", "error_cnv_HES",
+                                               "error_cnv_SOR")] + \
+               [(k, ctypes.c_int) for k in ("maxITR_HES", "maxITR_SOR", "flag_error", "flag_iter", "precision")]
 
 
 class CathodeError(RuntimeError):
@@ -134,6 +143,11 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_update_transport_coef.restype = ctypes.c_int
     L.cth_solve_phi_pc.argtypes = [_vp, ctypes.POINTER(PhiParams), _vp, ctypes.POINTER(PCResult)]
     L.cth_solve_phi_pc.restype = ctypes.c_int
+    L.cth_ghost_rules_upload.argtypes = [_vp, _vp, ctypes.c_int]
+    L.cth_ghost_rules_upload.restype = ctypes.c_int
+    for nm in ("cth_solve_rhoe_pc", "cth_solve_Te_pc"):
+        getattr(L, nm).argtypes = [_vp, ctypes.POINTER(SGParams), _vp, ctypes.POINTER(PCResult)]
+        getattr(L, nm).restype = ctypes.c_int
     L.cth_grid_set_graphs.argtypes = [_vp, ctypes.c_int]
     L.cth_grid_set_graphs.restype = ctypes.c_int
     L.cth_grid_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]

@@ -153,6 +153,28 @@ __global__ void k_transport(TransportArgs A) {
     A.mu_min[p] = mu_para * 2.0 / deno;
 }
 
+// ghost rules, one CTA visiting the rules in order (later rules win)
+__global__ void k_ghost_rules(const int* __restrict__ rules, int nrules, double* __restrict__ a, int which,
+                              int ld) {
+    for (int q = 0; q < nrules; q++) {
+        const int* R = rules + 7 * q;
+        const int wi = R[1] - R[0] + 1, wj = R[3] - R[2] + 1;
+        for (int k = threadIdx.x; k < wi * wj; k += blockDim.x) {
+            const int i = R[0] + k % wi, j = R[2] + k / wi;
+            const size_t src = (size_t)j * ld + i;
+            const size_t dst = (size_t)(j + R[5]) * ld + (i + R[4]);
+            a[dst] = (which == 0 && R[6] == 0) ? 0.0 : a[src];
+        }
+        __syncthreads();
+    }
+}
+
+void apply_ghost_rules(cth_fields* fs, double* plane, int which, cudaStream_t s) {
+    if (fs->n_ghost_rules == 0) return;
+    k_ghost_rules<<<1, 256, 0, s>>>(fs->ghost_rules, fs->n_ghost_rules, plane, which, fs->g->ld);
+    fs->g->launches++;
+}
+
 double* field_ptr(cth_fields* fs, const std::string& name) {
     auto it = fs->planes.find(name);
     if (it != fs->planes.end()) return it->second;
@@ -265,6 +287,7 @@ void cth_fields_destroy(cth_fields* fs) {
     for (auto& kv : fs->planes) cudaFree(kv.second);
     for (auto& kv : fs->tables) cudaFree(kv.second.first);
     if (fs->flags) cudaFree(fs->flags);
+    if (fs->ghost_rules) cudaFree(fs->ghost_rules);
     if (fs->part) cudaFree(fs->part);
     if (fs->scal) cudaFree(fs->scal);
     if (fs->h_scal) cudaFreeHost(fs->h_scal);
@@ -321,6 +344,30 @@ int cth_flags_upload(cth_fields* fs, const unsigned char* host_ij) {
         for (int j = 1; j <= g->nj; j++) lay[(size_t)j * g->ld + i] = host_ij[(size_t)i * (g->nj + 2) + j];
     if (!fs->flags) CTH_CUDA(cudaMalloc(&fs->flags, g->plane));
     CTH_CUDA(cudaMemcpy(fs->flags, lay.data(), g->plane, cudaMemcpyHostToDevice));
+    return CTH_OK;
+}
+
+int cth_ghost_rules_upload(cth_fields* fs, const int* rules, int n) {
+    if (!fs || n < 0 || (n > 0 && !rules)) { set_error("cth_ghost_rules_upload: invalid arguments"); return CTH_ERR_ARG; }
+    cth_grid* g = fs->g;
+    for (int q = 0; q < n; q++) {
+        const int* R = rules + 7 * q;
+        const bool x = (R[4] == 1 || R[4] == -1) && R[5] == 0 && R[0] == R[1];
+        const bool r = (R[5] == 1 || R[5] == -1) && R[4] == 0 && R[2] == R[3];
+        const bool in = R[0] <= R[1] && R[2] <= R[3] && R[0] >= 1 && R[1] <= g->ni && R[2] >= 1 && R[3] <= g->nj;
+        if (!(x || r) || !in || (R[6] != 0 && R[6] != 1)) {
+            set_error("cth_ghost_rules_upload: a rule must be a one-cell-wide segment of grid cells with a unit "
+                      "offset across it and mode 0 or 1");
+            return CTH_ERR_ARG;
+        }
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    if (fs->ghost_rules) { cudaFree(fs->ghost_rules); fs->ghost_rules = nullptr; }
+    fs->n_ghost_rules = 0;
+    if (n == 0) return CTH_OK;
+    CTH_CUDA(cudaMalloc(&fs->ghost_rules, 7 * n * sizeof(int)));
+    CTH_CUDA(cudaMemcpy(fs->ghost_rules, rules, 7 * n * sizeof(int), cudaMemcpyHostToDevice));
+    fs->n_ghost_rules = n;
     return CTH_OK;
 }
 

@@ -16,6 +16,8 @@
 
 struct cth_fields {
     cth_grid* g = nullptr;
+    int* ghost_rules = nullptr;      // device, 7 ints per rule (i0, i1, j0, j1, di, dj, rhoe_mode)
+    int n_ghost_rules = 0;
     std::map<std::string, double*> planes;
     unsigned char* flags = nullptr;  // device layout
     std::map<std::string, std::pair<double*, int>> tables;
@@ -75,6 +77,82 @@ struct Tab {
     const double* v;
     int n;
 };
+
+// Deterministic reduction of K per-thread values over a 2-D grid: every block
+// writes its partial, the last block to finish combines the partials in block
+// order and writes out[0..K).  Entry k is max-reduced when bit k of maxmask is
+// set, summed otherwise.  Every thread of every block must call it.
+template <int K>
+__device__ void grid_reduce(const double (&s)[K], unsigned maxmask, double* __restrict__ part,
+                            unsigned int* counter, double* __restrict__ out) {
+    __shared__ double red[K][32];
+    __shared__ bool am_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const bool mx = (maxmask >> k) & 1u;
+        double v = s[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double u = __shfl_down_sync(0xffffffffu, v, o);
+            v = mx ? fmax(v, u) : v + u;
+        }
+        if (lane == 0) red[k][wid] = v;
+    }
+    __syncthreads();
+    const int nb = gridDim.x * gridDim.y;
+    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const bool mx = (maxmask >> k) & 1u;
+        double v = red[k][0];
+        for (int w = 1; w < nw; w++) v = mx ? fmax(v, red[k][w]) : v + red[k][w];
+        part[(size_t)k * nb + bid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        am_last = (t == (unsigned int)(nb - 1));
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const bool mx = (maxmask >> k) & 1u;
+        double v = 0.0;
+        for (int q = 0; q < nb; q++) {
+            const double u = __ldcg(part + (size_t)k * nb + q);
+            v = mx ? fmax(v, u) : v + u;
+        }
+        out[k] = v;
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+}
+
+// calcRes statistics of one comparison (miniFuncs.hpp:292-376), as the pair (a, b):
+// mode 0 (max|d|, 0), 1 (sum d^2/(o^2+eps), count), 2 (max|d|, max|o|), 3 (sum d^2, sum o^2)
+__device__ __forceinline__ void res_stat(int mode, double nw, double od, double& a, double& b) {
+    const double d = nw - od;
+    if (mode == 0) { a = fabs(d); b = 0.0; }
+    else if (mode == 1) { a = (d * d) / (od * od + 1e-100); b = 1.0; }
+    else if (mode == 2) { a = fabs(d); b = fabs(od); }
+    else { a = d * d; b = od * od; }
+}
+
+inline double finish_res(int mode, double a, double b) {
+    if (mode == 0) return a;
+    if (mode == 1) return sqrt(a / b);
+    if (mode == 2) return a / b;
+    return sqrt(a / b);
+}
+
+// maximum of v over the fluid cells (flags != 0), written to *out (fields.cu)
+__global__ void k_max_flagged(const double* __restrict__ v, const unsigned char* __restrict__ flags, int ni,
+                              int nj, int ld, double* __restrict__ part, unsigned int* counter,
+                              double* __restrict__ out);
+
+// ghost rules of the fluid store applied in order to a plane (fields.cu);
+// which = 0: rhoe (rule mode 0 zeroes, 1 copies), 1: copy always
+void apply_ghost_rules(cth_fields* fs, double* plane, int which, cudaStream_t s);
 
 // named device planes of the store (created zeroed on first use), and tables
 double* field_ptr(cth_fields* fs, const std::string& name);

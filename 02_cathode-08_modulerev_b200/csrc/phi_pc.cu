@@ -240,16 +240,6 @@ __global__ void k_phi_correct_a(PhiArgs A) {
     A.phi[p] = A.phi[p] + d;
 }
 
-// calcRes statistics of one comparison (miniFuncs.hpp:292-376):
-// mode 0 (max|d|, -), 1 (sum d^2/(o^2+eps), count), 2 (max|d|, max|o|), 3 (sum d^2, sum o^2)
-__device__ __forceinline__ void res_stat(int mode, double nw, double od, double& a, double& b) {
-    const double d = nw - od;
-    if (mode == 0) { a = fabs(d); b = 0.0; }
-    else if (mode == 1) { a = (d * d) / (od * od + 1e-100); b = 1.0; }
-    else if (mode == 2) { a = fabs(d); b = fabs(od); }
-    else { a = d * d; b = od * od; }
-}
-
 constexpr int kNStat = 12;  // (phi, nUex, nUer) x (vs iteration start, vs call start) x 2
 
 // interior fields and flux corrections, then the residual reductions
@@ -259,7 +249,6 @@ __global__ void k_phi_correct_b(PhiArgs A, double* __restrict__ part, unsigned i
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     const int mode = A.prm.flag_error;
-    const bool use_max = (mode == 0 || mode == 2);
     double s[kNStat];
 #pragma unroll
     for (int k = 0; k < kNStat; k++) s[k] = 0.0;
@@ -292,57 +281,10 @@ __global__ void k_phi_correct_b(PhiArgs A, double* __restrict__ part, unsigned i
             res_stat(mode, v, A.phi_old[p], s[6], s[7]);
         }
     }
-    // block reduction (fixed order: deterministic)
-    __shared__ double red[kNStat][32];
-    __shared__ bool am_last;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int k = 0; k < kNStat; k++) {
-        double v = s[k];
-        for (int o = 16; o > 0; o >>= 1) {
-            const double u = __shfl_down_sync(0xffffffffu, v, o);
-            v = use_max ? fmax(v, u) : v + u;
-        }
-        if (lane == 0) red[k][wid] = v;
-    }
-    __syncthreads();
-    const int nb = gridDim.x * gridDim.y;
-    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
-    if (threadIdx.x < kNStat) {
-        const int k = threadIdx.x;
-        double v = red[k][0];
-        for (int w = 1; w < nw; w++) v = use_max ? fmax(v, red[k][w]) : v + red[k][w];
-        part[(size_t)k * nb + bid] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned int t = atomicAdd(counter, 1u);
-        am_last = (t == (unsigned int)(nb - 1));
-    }
-    __syncthreads();
-    if (!am_last) return;
-    __threadfence();
-    if (threadIdx.x < kNStat) {
-        const int k = threadIdx.x;
-        double v = 0.0;
-        for (int q = 0; q < nb; q++) {
-            const double u = __ldcg(part + (size_t)k * nb + q);
-            v = use_max ? fmax(v, u) : v + u;
-        }
-        out[k] = v;
-    }
-    if (threadIdx.x == 0) *counter = 0u;
+    grid_reduce<kNStat>(s, (mode == 0 || mode == 2) ? 0xfffu : 0u, part, counter, out);
 }
 
 #undef FL
-
-static double finish_res(int mode, double a, double b) {
-    if (mode == 0) return a;
-    if (mode == 1) return sqrt(a / b);
-    if (mode == 2) return a / b;
-    return sqrt(a / b);
-}
 
 int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_pc_result* res) {
     cth_grid* g = fs->g;
@@ -437,6 +379,7 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
         res->error_iter[1] = e_it[1];
         res->error_iter[2] = e_it[2];
         res->solver = st_last;
+        res->Ii_Anode = res->Ie_Anode = res->I_Anode = 0.0;
     }
     return CTH_OK;
 }

@@ -123,6 +123,28 @@ class Fields:
                     error_nUex=res.error_nUex, error_nUer=res.error_nUer, error_iter=list(res.error_iter),
                     solver=res.solver.as_dict())
 
+    def set_ghost_rules(self, rules):
+        """Rules (i0, i1, j0, j1, di, dj, rhoe_mode) applied after the electron sweeps."""
+        a = np.ascontiguousarray(np.asarray(rules, dtype=np.int32).reshape(-1, 7))
+        capi.check(self._L.cth_ghost_rules_upload(self._h, a.ctypes.data, a.shape[0]), allow_positive=False)
+
+    def _sg(self, fn, prm, stream):
+        p = capi.SGParams(**{k: prm[k] for k, _ in capi.SGParams._fields_})
+        res = capi.PCResult()
+        s = 0 if stream is None else stream.cuda_stream
+        capi.check(fn(self._h, ctypes.byref(p), s, ctypes.byref(res)), allow_positive=False)
+        return dict(ncount=res.ncount, solver_rc=res.solver_rc, errors=(res.error_phi, res.error_nUex, res.error_nUer),
+                    error_iter=list(res.error_iter), solver=res.solver.as_dict(), Ii_Anode=res.Ii_Anode,
+                    Ie_Anode=res.Ie_Anode, I_Anode=res.I_Anode)
+
+    def solve_rhoe_pc(self, prm: dict, stream=None) -> dict:
+        """FluidModule::solve_rhoe_wdTe_wSEE_PC on the device (fluidModule.hpp:3082-3970)."""
+        return self._sg(self._L.cth_solve_rhoe_pc, prm, stream)
+
+    def solve_Te_pc(self, prm: dict, stream=None) -> dict:
+        """FluidModule::solve_Te_wdTe_wSEE_PC on the device (fluidModule.hpp:4006-4957)."""
+        return self._sg(self._L.cth_solve_Te_pc, prm, stream)
+
     def update_transport_coef(self, prm: dict, stream=None):
         """FluidModule::update_transport_coef on the device (fluidModule.hpp:5799-5976)."""
         p = capi.TransportParams(**{k: prm[k] for k, _ in capi.TransportParams._fields_})

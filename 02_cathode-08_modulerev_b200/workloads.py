@@ -198,10 +198,11 @@ def plasma_state(ni: int, nj: int, seed: int = 3, dr: float | None = None) -> di
 def pc_state(ni: int, nj: int, seed: int = 4, Lz: float = 10e-3, Lr: float = 5e-3) -> dict:
     """Seeded state of the potential predictor-corrector in the reference's names.
 
-    rhoe = 1e17 exp(-((z - Lz/2)^2 + r^2) / (2 (Lr/5)^2)) x lognormal(0, 0.1) + 1e14
-    m^-3; rhoi, rhoe_old = rhoe (1 + 0.01 N(0,1)); Te uniform in [1, 10] eV (K);
-    phi = 20 z / Lz + 0.1 N(0,1) V with Ex, Er its face differences (+ 1 % noise);
-    nUex, nUer = rhoe 1e4 N(0,1); Uix, Uir N(0, 1000) m/s; rhoUmx, rhoUmr 1e19 N(0,1);
+    rhoe = 1e17 P x lognormal(0, 0.1) + 1e14 m^-3 with the profile
+    P = exp(-((z - Lz/2)^2 + r^2) / (2 (Lr/5)^2)); rhoi, rhoe_old = rhoe (1 + 0.01 N(0,1));
+    Te = (1 + 4 P)(1 + 0.01 N(0,1)) eV (in K); phi = 20 z / Lz + 0.01 N(0,1) V with
+    Ex, Er its face differences (+ 1 % noise); nUex, nUer = rhoe 1e3 N(0,1);
+    Uix, Uir N(0, 1000) m/s; rhoUmx, rhoUmr 1e19 N(0,1);
     rate_ionize = rhoe 1e5 U(0,1); mobility tensor of B ~ N(0, 0.05) T and a
     momentum frequency log-uniform in [1e8, 1e10] s^-1 (fluidModule.hpp:5957-5973).
     Physics parameters: dt 1e-10 s, V_bias 20 V, SEE coefficients 0.08 (params.hpp:62-63),
@@ -218,8 +219,8 @@ def pc_state(ni: int, nj: int, seed: int = 4, Lz: float = 10e-3, Lr: float = 5e-
     f["rhoe"] = 1e17 * prof * np.exp(0.1 * rng.standard_normal(sh)) + 1e14
     f["rhoi"] = f["rhoe"] * (1.0 + 0.01 * rng.standard_normal(sh))
     f["rhoe_old"] = f["rhoe"] * (1.0 + 0.01 * rng.standard_normal(sh))
-    f["Te"] = rng.uniform(1.0, 10.0, sh) * E0 / BOLTZ
-    phi = 20.0 * z[:, None] / Lz + 0.1 * rng.standard_normal(sh)
+    f["Te"] = (1.0 + 4.0 * prof) * (1.0 + 0.01 * rng.standard_normal(sh)) * E0 / BOLTZ
+    phi = 20.0 * z[:, None] / Lz + 0.01 * rng.standard_normal(sh)
     f["phi"] = phi
     Ex = np.zeros(sh)
     Er = np.zeros(sh)
@@ -227,8 +228,8 @@ def pc_state(ni: int, nj: int, seed: int = 4, Lz: float = 10e-3, Lr: float = 5e-
     Er[:, 1:] = -(phi[:, 1:] - phi[:, :-1]) / dr
     f["Ex"] = Ex * (1.0 + 0.01 * rng.standard_normal(sh))
     f["Er"] = Er * (1.0 + 0.01 * rng.standard_normal(sh))
-    f["nUex"] = f["rhoe"] * 1e4 * rng.standard_normal(sh)
-    f["nUer"] = f["rhoe"] * 1e4 * rng.standard_normal(sh)
+    f["nUex"] = f["rhoe"] * 1e3 * rng.standard_normal(sh)
+    f["nUer"] = f["rhoe"] * 1e3 * rng.standard_normal(sh)
     f["Uix"] = 1000.0 * rng.standard_normal(sh)
     f["Uir"] = 1000.0 * rng.standard_normal(sh)
     f["rhoUmx"] = 1e19 * rng.standard_normal(sh)
@@ -250,4 +251,32 @@ def pc_state(ni: int, nj: int, seed: int = 4, Lz: float = 10e-3, Lr: float = 5e-
     prm = dict(dt=1e-10, dx=dx, dr=dr, rmin=0.0, V_bias=20.0, masse=MASSE, coefIISEE_ts=0.08,
                coefMISEE_ts=0.08, error_cnv_HES_phi=1e-21, error_cnv_SOR_phi=1e-10, maxITR_HES_phi=2,
                maxITR_SOR_phi=30, flag_error=3, flag_iter_phi=1, precision=1)
+    return dict(fields=f, prm=prm)
+
+
+def sg_state(ni: int, nj: int, seed: int = 6, Lz: float = 10e-3, Lr: float = 5e-3) -> dict:
+    """pc_state extended with the arrays of the electron density and energy sweeps:
+    rhoeps = 3/2 rhoe k Te, Gx, Gr = rhoeps 1e3 N(0,1), rhoUex, rhoUer = rhoe 1e3 N(0,1),
+    rhoUix_wall = rhoi 1e3 N(0,1), Pabs U(0, 1e8) W/m^3, rate_eloss U(0, 8e-10) J/s,
+    zero wall-flux arrays.  Parameters: the electron sweeps of input/setup.yaml
+    (SMG, 30 iterations, 1e-10; 2 PC iterations; calcRes mode 3), Te_emitSEE 2.5 eV,
+    ratioEngy_EISEE_rd 0.5 (params.hpp:64-65), dt 1e-10 s."""
+    st = pc_state(ni, nj, seed=seed, Lz=Lz, Lr=Lr)
+    f = st["fields"]
+    rng = np.random.default_rng(seed + 1000)
+    sh = f["rhoe"].shape
+    f["rhoeps"] = 1.5 * f["rhoe"] * BOLTZ * f["Te"]
+    f["Gx"] = f["rhoeps"] * 1e3 * rng.standard_normal(sh)
+    f["Gr"] = f["rhoeps"] * 1e3 * rng.standard_normal(sh)
+    f["rhoUex"] = f["rhoe"] * 1e3 * rng.standard_normal(sh)
+    f["rhoUer"] = f["rhoe"] * 1e3 * rng.standard_normal(sh)
+    f["rhoUix_wall"] = f["rhoi"] * 1e3 * rng.standard_normal(sh)
+    f["Pabs"] = rng.uniform(0.0, 1e8, sh)
+    f["rate_eloss"] = rng.uniform(0.0, 8e-10, sh)
+    for k in ("rhoUex_wall", "rhoUer_wall", "Gx_wall", "Gr_wall"):
+        f[k] = np.zeros(sh)
+    p = st["prm"]
+    prm = dict(dt=p["dt"], dx=p["dx"], dr=p["dr"], rmin=p["rmin"], masse=MASSE, coefIISEE_ts=0.08,
+               coefMISEE_ts=0.08, Te_emitSEE_eV=2.5, ratioEngy_EISEE_rd=0.5, error_cnv_HES=1e-21,
+               error_cnv_SOR=1e-10, maxITR_HES=2, maxITR_SOR=30, flag_error=3, flag_iter=1, precision=1)
     return dict(fields=f, prm=prm)

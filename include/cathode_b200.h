@@ -252,8 +252,37 @@ typedef struct cth_pc_result {
     double error_phi, error_nUex, error_nUer;  /* calcRes against the entry values */
     double error_iter[3];  /* calcRes of the last iteration (phi, nUex, nUer)      */
     cth_status solver;     /* status of the last inner solve                      */
+    double Ii_Anode, Ie_Anode, I_Anode;  /* anode currents (density sweep only)    */
 } cth_pc_result;
 int cth_solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, void* stream, cth_pc_result* res);
+
+/* Ghost rules applied after the electron sweeps (fluidModule.hpp:3884-3921 for
+ * rhoe, :4878-4914 for Te): n rules of 7 ints (i0, i1, j0, j1, di, dj, mode),
+ * each a one-cell-wide segment of grid cells whose neighbour (i+di, j+dj) is
+ * set to 0 (mode 0, rhoe only) or to the cell's value (mode 1; Te is always
+ * copied).  Later rules win where targets coincide. */
+int cth_ghost_rules_upload(cth_fields* fs, const int* rules, int n);
+
+/* Scharfetter-Gummel predictor-correctors of the electron density
+ * (cth_solve_rhoe_pc: FluidModule::solve_rhoe_wdTe_wSEE_PC, fluidModule.hpp:3082-3970)
+ * and energy (cth_solve_Te_pc: solve_Te_wdTe_wSEE_PC, fluidModule.hpp:4006-4957).
+ * Density: reads Te, mu_*, Ex, Er, rhoi, Uix, Uir, rhoUmx, rhoUmr, rate_ionize,
+ * rhoUix_wall; updates rhoe, rhoUex, rhoUer, rhoUex_wall, rhoUer_wall and
+ * rhoe_old / rhoUex_old / rhoUer_old (entry values); reports the anode currents.
+ * Energy: reads rhoe, rhoe_old, rhoUex, rhoUer, Pabs, rate_eloss and the same
+ * fields; updates rhoeps, Gx, Gr, Gx_wall, Gr_wall, Te (recovered from rhoeps)
+ * and rhoeps_old, Gx_old, Gr_old, Te_old.  In cth_pc_result the three calcRes
+ * errors are those of (n, x flux, r flux). */
+typedef struct cth_sg_params {
+    double dt, dx, dr, rmin, masse;
+    double coefIISEE_ts, coefMISEE_ts, dTe_SEE;
+    double Te_emitSEE_eV, ratioEngy_EISEE_rd;  /* energy sweep only */
+    double error_cnv_HES, error_cnv_SOR;
+    int maxITR_HES, maxITR_SOR;
+    int flag_error, flag_iter, precision;
+} cth_sg_params;
+int cth_solve_rhoe_pc(cth_fields* fs, const cth_sg_params* prm, void* stream, cth_pc_result* res);
+int cth_solve_Te_pc(cth_fields* fs, const cth_sg_params* prm, void* stream, cth_pc_result* res);
 
 /* Residual (device arrays): r = b - A x on grid cells (couplings to non-grid
  * cells dropped), r = 0 elsewhere; *rnorm = ||r||_2, *bnorm = ||b||_2 over grid

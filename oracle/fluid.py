@@ -292,8 +292,17 @@ def cathode_geometry(ni: int = 194, nj: int = 70, xR: float = 0.0388, rmax: floa
             ("U", ib[0][0], ib[1][1], jb[0][1], jb[0][1]),          # x1
             ("U", ib[1][1] + 1, ib[3][1], jb[3][1], jb[3][1]),      # x4
             ("O", ib[4][0], ib[4][1], jb[4][1], jb[4][1])]          # x5
+    # ghost values set after the electron sweeps (fluidModule.hpp:3884-3921 for rhoe,
+    # :4878-4914 for Te): (i0, i1, j0, j1, di, dj, rhoe_mode) with rhoe_mode 0 = zero,
+    # 1 = copy of the cell; Te is always copied
+    ghosts = [(ib[0][0], ib[0][0], jb[0][0], jb[0][1], -1, 0, 0),            # chamber
+              (ib[1][0], ib[1][0], jb[1][0], jb[0][0] - 1, -1, 0, 0),        # magnet
+              (ib[0][0], ib[0][1], jb[0][0], jb[0][0], 0, -1, 0),            # antenna
+              (ib[1][1], ib[1][1], jb[1][0], jb[1][1], 1, 0, 1),             # right open
+              (ib[0][0], ib[1][1], jb[0][1], jb[0][1], 0, 1, 1)]             # upper open
     return dict(ni=ni, nj=nj, dx=dx, dr=dr, ib=ib, jb=jb, fxi=np.array(fxi), fxj=np.array(fxj),
-                fri=np.array(fri), frj=np.array(frj), segs=segs, flags=cathode_flags(ni, nj, ib, jb))
+                fri=np.array(fri), frj=np.array(frj), segs=segs, flags=cathode_flags(ni, nj, ib, jb),
+                ghosts=ghosts)
 
 
 def rectangle_geometry(ni: int, nj: int, Lz: float = 10e-3, Lr: float = 5e-3) -> dict:
@@ -301,8 +310,10 @@ def rectangle_geometry(ni: int, nj: int, Lz: float = 10e-3, Lr: float = 5e-3) ->
     biased electrode (like z5), r = R wall (like x1), r = 0 axis."""
     one = lambda a, b: np.array([[a, b]])
     segs = [("L", 1, 1, 1, nj), ("RB", ni, ni, 1, nj), ("U", 1, ni, nj, nj)]
+    ghosts = [(1, 1, 1, nj, -1, 0, 0), (ni, ni, 1, nj, 1, 0, 1), (1, ni, nj, nj, 0, 1, 1)]
     return dict(ni=ni, nj=nj, dx=Lz / ni, dr=Lr / nj, ib=one(1, ni), jb=one(1, nj), fxi=one(2, ni),
-                fxj=one(1, nj), fri=one(1, ni), frj=one(2, nj), segs=segs, flags=rectangle_flags(ni, nj))
+                fxj=one(1, nj), fri=one(1, ni), frj=one(2, nj), segs=segs, flags=rectangle_flags(ni, nj),
+                ghosts=ghosts)
 
 
 def calc_res(new, old, ib, jb, eps, flag_error):
@@ -540,4 +551,266 @@ def solve_phi_pc(st: dict, prm: dict, geo: dict, see, solve) -> dict:
     out["error_phi"] = calc_res(phi, phi_old, geo["ib"], geo["jb"], 1e-100, fe)
     out["error_nUex"] = calc_res(nUex, nUex_old, geo["fxi"], geo["fxj"], 1e-100, fe)
     out["error_nUer"] = calc_res(nUer, nUer_old, geo["fri"], geo["frj"], 1e-100, fe)
+    return out
+
+
+# ----------------------------------------------------------------------------
+# Scharfetter-Gummel predictor-correctors of the electron density and energy
+# ----------------------------------------------------------------------------
+
+LIM_EXP = 1.0e2  # fluidModule.hpp:3099
+EPS_VD = 1.0e-3  # fluidModule.hpp:3100
+
+
+def _sg(vd, z):
+    """Upwind / downwind weights vd/(1-e^-z), vd/(e^z-1) with the exponent clipped at 100."""
+    return vd / (1.0 - np.exp(np.fmin(-z, LIM_EXP))), vd / (np.exp(np.fmin(z, LIM_EXP)) - 1.0)
+
+
+def _sg_face_x(Te, Ex, mu_perp, I, J, dx):
+    mst = (mu_perp[I, J] + mu_perp[I - 1, J]) / 2.0 * 1.0
+    Tt = (Te[I, J] + Te[I - 1, J]) / 2.0
+    dT = (Te[I, J] - Te[I - 1, J]) / dx
+    vd = mst * (-Ex[I, J] - BOLTZ / E0 * dT) + EPS_VD
+    D = BOLTZ * Tt / E0 * mst
+    return mst, vd, vd * dx / D
+
+
+def _sg_face_r(Te, Er, mu_perp, I, J, dr):
+    mst = (mu_perp[I, J] + mu_perp[I, J - 1]) / 2.0 * 1.0
+    Tt = (Te[I, J] + Te[I, J - 1]) / 2.0
+    dT = (Te[I, J] - Te[I, J - 1]) / dr
+    vd = mst * (-Er[I, J] - BOLTZ / E0 * dT) + EPS_VD
+    D = BOLTZ * Tt / E0 * mst
+    return mst, vd, vd * dr / D
+
+
+def _masks(geo):
+    fl = geo["flags"].astype(np.int64)
+    return dict(bLx=(fl & F_BLX) != 0, bRx=(fl & F_BRX) != 0, bLrw=(fl & F_BLR_WALL) != 0,
+                bLr=((fl & F_BLR_WALL) != 0) & ((fl & F_BLR_CEN) != 0), bRrw=(fl & F_BRR_WALL) != 0,
+                bRr=((fl & F_BRR_WALL) != 0) & ((fl & F_BRR_OPEN) != 0))
+
+
+def _energy_wall(Te_old, Te, E, rhoeps, rhoeps_old, rhoe_old, rhoi, Ui, rhoUm, h, sign, prm, see):
+    """Electron energy flux through a wall face (fluidModule.hpp:4175-4190)."""
+    vth = np.sqrt(8.0 * BOLTZ * Te_old / (np.pi * prm["masse"]))
+    delta_phi = np.fmax(sign * E * h / 2.0, 0.0)
+    ex = np.exp(np.fmin(-E0 * delta_phi / (BOLTZ * Te_old + 1e-100), LIM_EXP))
+    gpn_eps = sign * vth * ex / 3.0 * 1.0
+    eps_emit = 2.0 * E0 * prm["Te_emitSEE_eV"]
+    gpn = sign * 0.25 * 1.0 * vth * ex
+    eb, rd, ts, dTe_SEE = see
+    ceb, crd, cts = func_Te(eb, Te, dTe_SEE), func_Te(rd, Te, dTe_SEE), func_Te(ts, Te, dTe_SEE)
+    see_flux = (-eps_emit * prm["coefIISEE_ts"] * rhoi * Ui - (ceb + prm["ratioEngy_EISEE_rd"] * crd) * rhoeps_old * gpn_eps
+                - eps_emit * cts * rhoe_old * gpn - eps_emit * prm["coefMISEE_ts"] * rhoUm)
+    return rhoeps * gpn_eps + see_flux
+
+
+def _apply_ghosts(a, geo, which):
+    for i0, i1, j0, j1, di, dj, mode in geo["ghosts"]:
+        I, J = slice(i0, i1 + 1), slice(j0, j1 + 1)
+        It, Jt = slice(i0 + di, i1 + di + 1), slice(j0 + dj, j1 + dj + 1)
+        if which == "rhoe" and mode == 0:
+            a[It, Jt] = 0.0
+        else:
+            a[It, Jt] = a[I, J]
+
+
+def solve_sg_pc(st: dict, prm: dict, geo: dict, see, solve, species: str) -> dict:
+    """FluidModule::solve_rhoe_wdTe_wSEE_PC (species "rhoe", fluidModule.hpp:3082-3970)
+    and solve_Te_wdTe_wSEE_PC (species "rhoeps", fluidModule.hpp:4006-4957).
+
+    rhoe: st holds rhoe, rhoUex, rhoUer, rhoUex_wall, rhoUer_wall, Te, mu_para,
+    mu_perp, mu_rr, mu_xr, mu_xx, Ex, Er, rhoi, Uix, Uir, rhoUmx, rhoUmr,
+    rate_ionize, rhoUix_wall.  rhoeps: rhoeps, Gx, Gr, Gx_wall, Gr_wall, Te, rhoe,
+    rhoe_old, rhoUex, rhoUer, Pabs, rate_eloss and the same mobility, field, ion
+    and metastable arrays.  prm: dt, dx, dr, rmin, masse, coefIISEE_ts,
+    coefMISEE_ts, Te_emitSEE_eV, ratioEngy_EISEE_rd, maxITR_HES, error_cnv_HES,
+    flag_error.  Returns the updated arrays with the calcRes errors and, for rhoe,
+    the anode currents Ii_Anode, Ie_Anode, I_Anode."""
+    en = species == "rhoeps"
+    nk, fxk, frk = ("rhoeps", "Gx", "Gr") if en else ("rhoe", "rhoUex", "rhoUer")
+    fac = 5.0 / 3.0 if en else 1.0
+    ni, nj = geo["ni"], geo["nj"]
+    dx, dr, dt = prm["dx"], prm["dr"], prm["dt"]
+    r = prm["rmin"] + (np.arange(nj + 2) - 0.5) * dr
+    m = _masks(geo)
+    g = dict(st)
+    n = st[nk].copy()
+    Fx, Fr = st[fxk].copy(), st[frk].copy()
+    Fx_w, Fr_w = st[fxk + "_wall"].copy(), st[frk + "_wall"].copy()
+    Te = st["Te"].copy()
+    Te_old = Te.copy()
+    n_old, Fx_old, Fr_old = n.copy(), Fx.copy(), Fr.copy()
+    Tsg = Te_old if en else Te            # temperature of the SG weights
+    rhoe_old = g["rhoe_old"] if en else n_old
+    d = n - n_old
+    mu_para, mu_perp, Ex, Er = g["mu_para"], g["mu_perp"], g["Ex"], g["Er"]
+    ncount = 0
+    while True:
+        ncount += 1
+        n_t, Fx_t, Fr_t = n.copy(), Fx.copy(), Fr.copy()
+        for (a, b), (c, e) in zip(geo["fxi"], geo["fxj"]):
+            I = np.arange(a, b + 1)[:, None]
+            J = np.arange(c, e + 1)[None, :]
+            rL = (r[J] + r[J - 1]) / 2.0
+            rR = (r[J] + r[J + 1]) / 2.0
+            mpa = (mu_para[I, J] + mu_para[I - 1, J]) / 2.0
+            mpe = (mu_perp[I, J] + mu_perp[I - 1, J]) / 2.0
+            mrr = (g["mu_rr"][I, J] + g["mu_rr"][I - 1, J]) / 2.0
+            mxr = (g["mu_xr"][I, J] + g["mu_xr"][I - 1, J]) / 2.0
+            ixx = mrr / (mpa * mpe)
+            ixr = -mxr / (mpa * mpe)
+            mst, vd, z = _sg_face_x(Tsg, Ex, mu_perp, I, J, dx)
+            A, B = _sg(vd, z)
+            Fr_i = (rR * Fr_t[I, J + 1] * m["bRrw"][I, J] + rL * Fr_t[I, J] * m["bLr"][I, J]
+                    + rR * Fr_t[I - 1, J + 1] * m["bRrw"][I - 1, J] + rL * Fr_t[I - 1, J] * m["bLr"][I - 1, J]) / (4.0 * r[J])
+            if en:
+                Fx[I, J] = ((A * n[I - 1, J] - B * n[I, J]) * 5.0 / 3.0 + Fx_t[I, J]
+                            - mst * (ixx * Fx_t[I, J] + ixr * Fr_i))
+            else:
+                Fx[I, J] = (A * n[I - 1, J] - B * n[I, J] + Fx_t[I, J] - mst * (ixx * Fx_t[I, J] + ixr * Fr_i))
+        for kind, i0, i1, j0, j1 in geo["segs"]:
+            J = np.arange(j0, j1 + 1)
+            if kind not in ("L", "R", "RB"):
+                continue
+            c, f, sg = (i0, i0, -1.0) if kind == "L" else (i0, i0 + 1, 1.0)
+            if en:
+                v = _energy_wall(Te_old[c, J], Te[c, J], Ex[f, J], n[c, J], n_old[c, J], rhoe_old[c, J], g["rhoi"][c, J],
+                                 g["Uix"][f, J], g["rhoUmx"][f, J], dx, sg, prm, see)
+            else:
+                v = _wall_flux(Te[c, J], n[c, J], n_old[c, J], g["rhoi"][c, J], g["Uix"][f, J], g["rhoUmx"][f, J],
+                               Ex[f, J], dx, sg, prm, see)
+            Fx[f, J] = v
+            Fx_w[f, J] = v
+        for (a, b), (c, e) in zip(geo["fri"], geo["frj"]):
+            I = np.arange(a, b + 1)[:, None]
+            J = np.arange(c, e + 1)[None, :]
+            r_t = (r[J] + r[J - 1]) / 2.0
+            mpa = (mu_para[I, J] + mu_para[I, J - 1]) / 2.0
+            mpe = (mu_perp[I, J] + mu_perp[I, J - 1]) / 2.0
+            mxx = (g["mu_xx"][I, J] + g["mu_xx"][I, J - 1]) / 2.0
+            mxr = (g["mu_xr"][I, J] + g["mu_xr"][I, J - 1]) / 2.0
+            irr = mxx / (mpa * mpe)
+            ixr = -mxr / (mpa * mpe)
+            mst, vd, z = _sg_face_r(Tsg, Er, mu_perp, I, J, dr)
+            A, B = _sg(vd, z)
+            Fx_i = (r[J] * Fx_t[I + 1, J] * m["bRx"][I, J] + r[J] * Fx_t[I, J] * m["bLx"][I, J]
+                    + r[J - 1] * Fx_t[I + 1, J - 1] * m["bRx"][I, J - 1] + r[J - 1] * Fx_t[I, J - 1] * m["bLx"][I, J - 1]) / (4.0 * r_t)
+            if en:
+                Fr[I, J] = ((A * n[I, J - 1] - B * n[I, J]) * 5.0 / 3.0 + Fr_t[I, J]
+                            - mst * (ixr * Fx_i + irr * Fr_t[I, J]))
+            else:
+                Fr[I, J] = (A * n[I, J - 1] - B * n[I, J] + Fr_t[I, J] - mst * (ixr * Fx_i + irr * Fr_t[I, J]))
+        for kind, i0, i1, j0, j1 in geo["segs"]:
+            I = np.arange(i0, i1 + 1)
+            if kind in ("D", "U"):
+                c, f, sg = (j0, j0, -1.0) if kind == "D" else (j0, j0 + 1, 1.0)
+                if en:
+                    v = _energy_wall(Te_old[I, c], Te[I, c], Er[I, f], n[I, c], n_old[I, c], rhoe_old[I, c],
+                                     g["rhoi"][I, c], g["Uir"][I, f], g["rhoUmr"][I, f], dr, sg, prm, see)
+                else:
+                    v = _wall_flux(Te[I, c], n[I, c], n_old[I, c], g["rhoi"][I, c], g["Uir"][I, f], g["rhoUmr"][I, f],
+                                   Er[I, f], dr, sg, prm, see)
+                Fr[I, f] = v
+                Fr_w[I, f] = v
+            elif kind == "O":
+                if en:
+                    Fr[I, j0 + 1] = 5.0 / 2.0 * BOLTZ * Te_old[I, j0] * np.fmax(g["rhoUer"][I, j0 + 1], 0.0)
+                else:
+                    Fr[I, j0 + 1] = g["rhoi"][I, j0] * g["Uir"][I, j0 + 1]
+                Fr_w[I, j0 + 1] = 0.0
+        sh = (ni + 2, nj + 2)
+        aP, aE, aW, aN, aS, bb = (np.zeros(sh) for _ in range(6))
+        for (a, b), (c, e) in zip(geo["ib"], geo["jb"]):
+            I = np.arange(a, b + 1)[:, None]
+            J = np.arange(c, e + 1)[None, :]
+            rR = (r[J] + r[J + 1]) / 2.0
+            rL = (r[J] + r[J - 1]) / 2.0
+            qR = (r[J] + r[J + 1]) / 2.0 / r[J]
+            qL = (r[J] + r[J - 1]) / 2.0 / r[J]
+            _, vLx, zLx = _sg_face_x(Tsg, Ex, mu_perp, I, J, dx)
+            _, vRx, zRx = _sg_face_x(Tsg, Ex, mu_perp, I + 1, J, dx)
+            _, vLr, zLr = _sg_face_r(Tsg, Er, mu_perp, I, J, dr)
+            _, vRr, zRr = _sg_face_r(Tsg, Er, mu_perp, I, J + 1, dr)
+            bLx, bRx, bLr, bRr = m["bLx"][I, J], m["bRx"][I, J], m["bLr"][I, J], m["bRr"][I, J]
+            ex = np.exp
+            tterm = 3.0 / 5.0 * dx * dr / dt if en else dx * dr / dt
+            aP[I, J] = (vRx / (1.0 - ex(np.fmin(-zRx, LIM_EXP))) * bRx * dr
+                        + vLx / (ex(np.fmin(zLx, LIM_EXP)) - 1.0) * bLx * dr
+                        + qR * vRr / (1.0 - ex(np.fmin(-zRr, LIM_EXP))) * bRr * dx
+                        + qL * vLr / (ex(np.fmin(zLr, LIM_EXP)) - 1.0) * bLr * dx + tterm)
+            aE[I, J] = vRx / (ex(np.fmin(zRx, LIM_EXP)) - 1.0) * bRx * dr
+            aW[I, J] = vLx / (1.0 - ex(np.fmin(-zLx, LIM_EXP))) * bLx * dr
+            aN[I, J] = qR * vRr / (ex(np.fmin(zRr, LIM_EXP)) - 1.0) * bRr * dx
+            aS[I, J] = qL * vLr / (1.0 - ex(np.fmin(-zLr, LIM_EXP))) * bLr * dx
+            div = (Fx[I + 1, J] - Fx[I, J]) / dx + (qR * Fr[I, J + 1] - qL * Fr[I, J]) / dr
+            if en:
+                bLxw, bRxw, bLrw, bRrw = m["bLx"][I, J], m["bRx"][I, J], m["bLrw"][I, J], m["bRrw"][I, J]
+                jx = -E0 * (g["rhoUex"][I + 1, J] * Ex[I + 1, J] * bRxw + g["rhoUex"][I, J] * Ex[I, J] * bLxw) / 2.0
+                jr = -E0 * (rR * g["rhoUer"][I, J + 1] * Er[I, J + 1] * bRrw + rL * g["rhoUer"][I, J] * Er[I, J] * bLrw) / (2.0 * r[J])
+                R1 = (-n[I, J] + n_old[I, J]) / dt
+                R3 = g["Pabs"][I, J] - g["rhoe"][I, J] * g["rate_eloss"][I, J]
+                bb[I, J] = 3.0 / 5.0 * (R1 + (jx + jr) + R3 + (-div)) * dx * dr
+            else:
+                bb[I, J] = (-div + g["rate_ionize"][I, J] - (n[I, J] - n_old[I, J]) / dt) * dx * dr
+        x = solve(aP, aE, aW, aN, aS, bb, geo["ib"], geo["jb"])
+        for (a, b), (c, e) in zip(geo["ib"], geo["jb"]):
+            d[a:b + 1, c:e + 1] = x[a:b + 1, c:e + 1]
+        for (a, b), (c, e) in zip(geo["fxi"], geo["fxj"]):
+            I = np.arange(a, b + 1)[:, None]
+            J = np.arange(c, e + 1)[None, :]
+            _, vd, z = _sg_face_x(Tsg, Ex, mu_perp, I, J, dx)
+            A, B = _sg(vd, z)
+            Fx[I, J] = Fx[I, J] + ((A * d[I - 1, J] - B * d[I, J]) * 5.0 / 3.0 if en else A * d[I - 1, J] - B * d[I, J])
+        for (a, b), (c, e) in zip(geo["fri"], geo["frj"]):
+            I = np.arange(a, b + 1)[:, None]
+            J = np.arange(c, e + 1)[None, :]
+            _, vd, z = _sg_face_r(Tsg, Er, mu_perp, I, J, dr)
+            A, B = _sg(vd, z)
+            Fr[I, J] = Fr[I, J] + ((A * d[I, J - 1] - B * d[I, J]) * 5.0 / 3.0 if en else A * d[I, J - 1] - B * d[I, J])
+        for (a, b), (c, e) in zip(geo["ib"], geo["jb"]):
+            sl = (slice(a, b + 1), slice(c, e + 1))
+            nn = n[sl] + d[sl]
+            n[sl] = np.where(nn > 0.0, nn, n[sl])
+        fe = prm["flag_error"]
+        errs = (calc_res(n, n_t, geo["ib"], geo["jb"], 1e-100, fe),
+                calc_res(Fx, Fx_t, geo["fxi"], geo["fxj"], 1e-100, fe),
+                calc_res(Fr, Fr_t, geo["fri"], geo["frj"], 1e-100, fe))
+        if max(errs) < prm["error_cnv_HES"] or ncount >= prm["maxITR_HES"]:
+            break
+    out = {nk: n, fxk: Fx, frk: Fr, fxk + "_wall": Fx_w, frk + "_wall": Fr_w, "ncount": ncount,
+           "errors_last": errs}
+    if en:
+        for (a, b), (c, e) in zip(geo["ib"], geo["jb"]):
+            sl = (slice(a, b + 1), slice(c, e + 1))
+            n[sl] = np.where(n[sl] < 0.0, np.fmax(n_old[sl], 0.0), n[sl])
+        blk = geo["flags"] != 0
+        rhoe = g["rhoe"]
+        rmax = rhoe[blk].max() if blk.any() else 0.0
+        Te_max = 1000.0 * E0 / BOLTZ
+        Te = Te.copy()
+        for (a, b), (c, e) in zip(geo["ib"], geo["jb"]):
+            sl = (slice(a, b + 1), slice(c, e + 1))
+            Te[sl] = np.fmin(n[sl] / (3.0 / 2.0 * (rhoe[sl] + rmax * 0.001) * BOLTZ + 1e-100), Te_max)
+        _apply_ghosts(Te, geo, "Te")
+        out["Te"] = Te
+        out["Te_old"] = Te_old
+    else:
+        _apply_ghosts(n, geo, "rhoe")
+        Ii = Ie = 0.0
+        for kind, i0, i1, j0, j1 in geo["segs"]:
+            if kind != "RB":
+                continue
+            for j in range(j0, j1 + 1):
+                di = g["rhoUix_wall"][i0 + 1, j] * 2.0 * np.pi * r[j] * dr * E0
+                de = Fx_w[i0 + 1, j] * 2.0 * np.pi * r[j] * dr * (-E0)
+                Ii += di
+                Ie += de
+        out.update(Ii_Anode=Ii, Ie_Anode=Ie, I_Anode=Ii + Ie, rhoe_old=n_old)
+    fe = prm["flag_error"]
+    out["error_" + nk] = calc_res(n, n_old, geo["ib"], geo["jb"], 1e-100, fe)
+    out["error_" + fxk] = calc_res(Fx, Fx_old, geo["fxi"], geo["fxj"], 1e-100, fe)
+    out["error_" + frk] = calc_res(Fr, Fr_old, geo["fri"], geo["frj"], 1e-100, fe)
     return out

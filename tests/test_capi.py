@@ -12,7 +12,7 @@ def declared_symbols():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        for m in re.finditer(r"\b(cth_[a-z0-9_]+)\s*\(", src):
+        for m in re.finditer(r"\b(cth_[A-Za-z0-9_]+)\s*\(", src):
             names.add(m.group(1))
     return names
 

@@ -179,3 +179,42 @@ def test_phi_pc_oracle_properties(orc):
     np.testing.assert_allclose(phi[1:25, 17], -phi[1:25, 16], rtol=1e-12)
     np.testing.assert_allclose(out["Ex"][2:25, 1:17], -(phi[2:25, 1:17] - phi[1:24, 1:17]) / prm["dx"], rtol=1e-12)
     np.testing.assert_allclose(out["Er"][1:25, 2:17], -(phi[1:25, 2:17] - phi[1:25, 1:16]) / prm["dr"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("species", ["rhoe", "rhoeps"])
+def test_sg_oracle_properties(orc, species):
+    """Electron sweeps in the oracle: the assembled increment systems are solved,
+    the density stays positive, Te follows rhoeps and the ghost rules hold."""
+    from oracle import fluid
+    import importlib
+    import __graft_entry__
+    wl = importlib.import_module(__graft_entry__.load_package().__name__ + ".workloads")
+    geo = fluid.rectangle_geometry(24, 16)
+    st = wl.sg_state(24, 16, seed=8)
+    z = np.load(os.path.join(HERE, "golden", "see_tables.npz"))
+    see = (z["coefEISEE_eb_table"], z["coefEISEE_rd_table"], z["coefEISEE_ts_table"], float(z["dTe_SEE"]))
+    prm = dict(st["prm"], dTe_SEE=float(z["dTe_SEE"]))
+    res = []
+
+    def solve(aP, aE, aW, aN, aS, b, ib, jb):
+        s = dict(ni=24, nj=16, i_bl=ib, j_bl=jb, aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b)
+        x = orc.direct_solve(s)
+        res.append(orc.residual(s, x)[1] / orc.residual(s, np.zeros_like(x))[1])
+        return x
+
+    out = fluid.solve_sg_pc(st["fields"], prm, geo, see, solve, species)
+    assert out["ncount"] == 2 and max(res) < 1e-12
+    n = out[species]
+    assert (n[1:25, 1:17] > 0).all()
+    if species == "rhoeps":
+        rhoe = st["fields"]["rhoe"]
+        Te = out["Te"]
+        rmax = rhoe[1:25, 1:17].max()
+        np.testing.assert_allclose(Te[1:25, 1:17], n[1:25, 1:17] / (1.5 * (rhoe[1:25, 1:17] + 1e-3 * rmax) * fluid.BOLTZ),
+                                   rtol=1e-12)
+        np.testing.assert_array_equal(Te[0, 1:17], Te[1, 1:17])
+        np.testing.assert_array_equal(Te[25, 1:17], Te[24, 1:17])
+    else:
+        assert (n[0, 1:17] == 0).all()
+        np.testing.assert_array_equal(n[25, 1:17], n[24, 1:17])
+        np.testing.assert_array_equal(n[1:25, 17], n[1:25, 16])
