@@ -33,7 +33,8 @@ EXPORTS = (
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_fields_create", "cth_fields_destroy", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
-    "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc",
+    "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
+    "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -85,6 +86,30 @@ class SGParams(ctypes.Structure):
                                                "dTe_SEE", "Te_emitSEE_eV", "ratioEngy_EISEE_rd", "error_cnv_HES",
                                                "error_cnv_SOR")] + \
                [(k, ctypes.c_int) for k in ("maxITR_HES", "maxITR_SOR", "flag_error", "flag_iter", "precision")]
+
+
+class CFL(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("CFL", ctypes.c_double), ("masse", ctypes.c_double),
+                ("rmin", ctypes.c_double), ("dr", ctypes.c_double), ("flag_adp_dt", ctypes.c_int)] + \
+               [(k, ctypes.c_double) for k in ("dt_min", "rhoe_max", "mu_max", "Te_max", "ue_max")]
+
+
+class IonParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("dt", "dx", "dr", "rmin", "rmax", "massi", "Ti", "V_bias",
+                                               "Te_rep_eV", "CFL", "error_cnv_SOR")] + \
+               [(k, ctypes.c_int) for k in ("ndt_i", "maxITR_SOR", "flag_iter", "precision", "flag_error")]
+
+
+class IonResult(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("error_rhoi", "error_Uix", "error_Uir", "error_Uip")] + \
+               [("solver_rc", ctypes.c_int), ("reserved", ctypes.c_int), ("solver", Status * 4)]
+
+
+ION_OP_FIELDS = ("kind", "i0", "i1", "j0", "j1", "di", "dj", "dir", "sign", "bias", "pair", "scale")
+
+
+class IonOp(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int) for k in ION_OP_FIELDS]
 
 
 class CathodeError(RuntimeError):
@@ -143,6 +168,14 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_update_transport_coef.restype = ctypes.c_int
     L.cth_solve_phi_pc.argtypes = [_vp, ctypes.POINTER(PhiParams), _vp, ctypes.POINTER(PCResult)]
     L.cth_solve_phi_pc.restype = ctypes.c_int
+    L.cth_ion_program_upload.argtypes = [_vp, ctypes.c_int, _vp, ctypes.c_int]
+    L.cth_ion_program_upload.restype = ctypes.c_int
+    L.cth_ion_boxes_upload.argtypes = [_vp, ctypes.c_int, _vp, ctypes.c_int]
+    L.cth_ion_boxes_upload.restype = ctypes.c_int
+    L.cth_ion_step.argtypes = [_vp, _vp, _vp, ctypes.POINTER(IonParams), _vp, ctypes.POINTER(IonResult)]
+    L.cth_ion_step.restype = ctypes.c_int
+    L.cth_check_cfl.argtypes = [_vp, ctypes.POINTER(CFL), _vp]
+    L.cth_check_cfl.restype = ctypes.c_int
     L.cth_ghost_rules_upload.argtypes = [_vp, _vp, ctypes.c_int]
     L.cth_ghost_rules_upload.restype = ctypes.c_int
     for nm in ("cth_solve_rhoe_pc", "cth_solve_Te_pc"):

@@ -175,6 +175,31 @@ void apply_ghost_rules(cth_fields* fs, double* plane, int which, cudaStream_t s)
     fs->g->launches++;
 }
 
+// FluidModule::check_CFL (fluidModule.hpp:57-115): maxima of rhoe, mu_para, Te
+// over the index space and of the electron speed over the grid cells
+__global__ void k_cfl(const double* __restrict__ rhoe, const double* __restrict__ mu_para,
+                      const double* __restrict__ Te, const double* __restrict__ rhoUex,
+                      const double* __restrict__ rhoUer, double rmin, double dr, int ni, int nj, int ld,
+                      double* __restrict__ part, unsigned int* counter, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    if (i <= ni + 1) {
+        const size_t p = (size_t)j * ld + i;
+        s[0] = fmax(0.0, rhoe[p]);
+        s[1] = fmax(0.0, mu_para[p]);
+        s[2] = fmax(0.0, Te[p]);
+        if (i >= 1 && i <= ni && j >= 1 && j <= nj) {
+            const double rj = rmin + (j - 0.5) * dr;
+            const double rL = (rj + (rmin + (j - 1.5) * dr)) / 2.0, rR = (rj + (rmin + (j + 0.5) * dr)) / 2.0;
+            const double ux = (rhoUex[p + 1] + rhoUex[p]) / 2.0 / (rhoe[p] + 1e-100);
+            const double ur = (rR * rhoUer[p + ld] + rL * rhoUer[p]) / (2.0 * rj) / (rhoe[p] + 1e-100);
+            s[3] = fmax(0.0, sqrt(ux * ux + ur * ur));
+        }
+    }
+    grid_reduce<4>(s, 0xfu, part, counter, out);
+}
+
 double* field_ptr(cth_fields* fs, const std::string& name) {
     auto it = fs->planes.find(name);
     if (it != fs->planes.end()) return it->second;
@@ -288,6 +313,10 @@ void cth_fields_destroy(cth_fields* fs) {
     for (auto& kv : fs->tables) cudaFree(kv.second.first);
     if (fs->flags) cudaFree(fs->flags);
     if (fs->ghost_rules) cudaFree(fs->ghost_rules);
+    for (int k = 0; k < CTH_ION_NPROG; k++)
+        if (fs->ion_ops[k]) cudaFree(fs->ion_ops[k]);
+    for (int k = 0; k < 4; k++)
+        if (fs->ion_boxes[k]) cudaFree(fs->ion_boxes[k]);
     if (fs->part) cudaFree(fs->part);
     if (fs->scal) cudaFree(fs->scal);
     if (fs->h_scal) cudaFreeHost(fs->h_scal);
@@ -368,6 +397,37 @@ int cth_ghost_rules_upload(cth_fields* fs, const int* rules, int n) {
     CTH_CUDA(cudaMalloc(&fs->ghost_rules, 7 * n * sizeof(int)));
     CTH_CUDA(cudaMemcpy(fs->ghost_rules, rules, 7 * n * sizeof(int), cudaMemcpyHostToDevice));
     fs->n_ghost_rules = n;
+    return CTH_OK;
+}
+
+int cth_check_cfl(cth_fields* fs, cth_cfl* io, void* stream) {
+    if (!fs || !io) { set_error("cth_check_cfl: invalid arguments"); return CTH_ERR_ARG; }
+    cth_grid* g = fs->g;
+    CTH_CUDA(cudaSetDevice(g->device));
+    const char* names[5] = {"rhoe", "mu_para", "Te", "rhoUex", "rhoUer"};
+    double* q[5];
+    for (int k = 0; k < 5; k++) {
+        q[k] = field_ptr(fs, names[k]);
+        if (!q[k]) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    dim3 blk(128), grd((g->ni + 2 + 127) / 128, g->nj + 2);
+    k_cfl<<<grd, blk, 0, s>>>(q[0], q[1], q[2], q[3], q[4], io->rmin, io->dr, g->ni, g->nj, g->ld, fs->part,
+                              g->ws.counter, fs->scal + 40);
+    g->launches++;
+    CTH_CUDA(cudaGetLastError());
+    CTH_CUDA(cudaMemcpyAsync(fs->h_scal, fs->scal + 40, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CTH_CUDA(cudaStreamSynchronize(s));
+    const double* h = fs->h_scal;
+    io->rhoe_max = h[0];
+    io->mu_max = h[1];
+    io->Te_max = h[2];
+    io->ue_max = h[3] + sqrt(8.0 * kBoltz * h[2] / (M_PI * io->masse));
+    io->dt_min = kEps0f / (kE0f * h[0] * h[1]);
+    if (io->flag_adp_dt == 1)
+        io->dt = io->dt_min * io->CFL;
+    else
+        io->CFL = io->dt / io->dt_min;
     return CTH_OK;
 }
 

@@ -18,6 +18,11 @@ struct cth_fields {
     cth_grid* g = nullptr;
     int* ghost_rules = nullptr;      // device, 7 ints per rule (i0, i1, j0, j1, di, dj, rhoe_mode)
     int n_ghost_rules = 0;
+    cth_ion_op* ion_ops[CTH_ION_NPROG] = {};  // wall programs of the ion step
+    int ion_nops[CTH_ION_NPROG] = {};
+    int* ion_boxes[4] = {};                    // residual boxes (rhoi, Uix, Uir, Uip)
+    int ion_nbox[4] = {};
+    int ion_box_total[4] = {};
     std::map<std::string, double*> planes;
     unsigned char* flags = nullptr;  // device layout
     std::map<std::string, std::pair<double*, int>> tables;

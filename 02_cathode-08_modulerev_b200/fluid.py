@@ -123,6 +123,38 @@ class Fields:
                     error_nUex=res.error_nUex, error_nUer=res.error_nUer, error_iter=list(res.error_iter),
                     solver=res.solver.as_dict())
 
+    def set_ion_geometry(self, geo: dict):
+        """Upload the ion wall programs and residual boxes of a geometry dict."""
+        for k, prog in enumerate(ion_programs(geo["seg"])):
+            a = (capi.IonOp * max(1, len(prog)))()
+            for q, o in enumerate(prog):
+                for f, v in zip(capi.ION_OP_FIELDS, o):
+                    setattr(a[q], f, int(v))
+            capi.check(self._L.cth_ion_program_upload(self._h, k, ctypes.addressof(a), len(prog)),
+                       allow_positive=False)
+        for k, boxes in enumerate(ion_boxes(geo)):
+            b = np.ascontiguousarray(np.asarray(boxes, dtype=np.int32).reshape(-1, 4))
+            capi.check(self._L.cth_ion_boxes_upload(self._h, k, b.ctypes.data, b.shape[0]), allow_positive=False)
+
+    def ion_step(self, grid_x, grid_r, prm: dict, stream=None) -> dict:
+        """The ion sub-step (src/main.cpp:191-197) on the device; grid_x / grid_r are
+        Grids of the x-face and r-face blocks."""
+        p = capi.IonParams(**{k: prm[k] for k, _ in capi.IonParams._fields_})
+        res = capi.IonResult()
+        s = 0 if stream is None else stream.cuda_stream
+        capi.check(self._L.cth_ion_step(self._h, grid_x._h, grid_r._h, ctypes.byref(p), s, ctypes.byref(res)),
+                   allow_positive=False)
+        return dict(error_rhoi=res.error_rhoi, error_Uix=res.error_Uix, error_Uir=res.error_Uir,
+                    error_Uip=res.error_Uip, solver_rc=res.solver_rc, solver=[res.solver[k].as_dict() for k in range(4)])
+
+    def check_cfl(self, dt: float, CFL: float, masse: float, rmin: float, dr: float, flag_adp_dt: int = 0,
+                  stream=None) -> dict:
+        """FluidModule::check_CFL (fluidModule.hpp:57-115); returns dt, CFL and the maxima."""
+        c = capi.CFL(dt=dt, CFL=CFL, masse=masse, rmin=rmin, dr=dr, flag_adp_dt=flag_adp_dt)
+        s = 0 if stream is None else stream.cuda_stream
+        capi.check(self._L.cth_check_cfl(self._h, ctypes.byref(c), s), allow_positive=False)
+        return {k: getattr(c, k) for k, _ in capi.CFL._fields_}
+
     def set_ghost_rules(self, rules):
         """Rules (i0, i1, j0, j1, di, dj, rhoe_mode) applied after the electron sweeps."""
         a = np.ascontiguousarray(np.asarray(rules, dtype=np.int32).reshape(-1, 7))
@@ -150,3 +182,148 @@ class Fields:
         p = capi.TransportParams(**{k: prm[k] for k, _ in capi.TransportParams._fields_})
         s = 0 if stream is None else stream.cuda_stream
         capi.check(self._L.cth_update_transport_coef(self._h, ctypes.byref(p), s), allow_positive=False)
+
+
+# ---------------------------------------------------------------------------
+# geometries: cell / face blocks, wall segments, ghost rules, ion wall programs
+# ---------------------------------------------------------------------------
+
+def cathode_geometry(ni=194, nj=70, xR=0.0388, rmax=0.014) -> dict:
+    """The cathode's fluid blocks with their x-face and r-face blocks
+    (initialModule.hpp:219-345), side flags, ghost rules of the electron sweeps
+    (fluidModule.hpp:3884-3921, :4878-4914) and the named wall segments of the ion
+    sweeps on the cell, x-face and r-face index sets (fluidModule.hpp:218-360,
+    :700-800, :1130-1200)."""
+    dx, dr = xR / ni, rmax / nj
+    x2, x3, x4, x5, x6 = 13.4e-3, 17.8e-3, 22.8e-3, 27.8e-3, 7.8e-3
+    r1, r3, r4, r5 = 0.6e-3, 4.0e-3, 9.0e-3, 2.0e-3
+    lo = lambda v, d, k: int(v / d + 0.5) + k
+    hi = lambda v, d, k: int(v / d - 0.5) + k
+    ib, jb = cathode_blocks(ni, nj, xR, rmax)
+    fxi = np.array([[lo(x6, dx, 2), hi(x2, dx, 2)], [lo(x2, dx, 2), hi(x4, dx, 1)], [lo(x2, dx, 2), hi(x3, dx, 2)],
+                    [lo(x3, dx, 2), hi(x5, dx, 2)], [lo(x5, dx, 2), hi(xR, dx, 1)]], np.int32)
+    fxj = np.array([[lo(r3, dr, 1), hi(r4, dr, 1)], [lo(r5, dr, 1), hi(r4, dr, 1)], [lo(r1, dr, 1), hi(r5, dr, 1)],
+                    [lo(0.0, dr, 1), hi(r5, dr, 1)], [lo(0.0, dr, 1), hi(rmax, dr, 1)]], np.int32)
+    fri = np.array([[lo(x6, dx, 1), hi(x2, dx, 1)], [lo(x2, dx, 1), hi(x4, dx, 1)], [lo(x2, dx, 1), hi(x3, dx, 1)],
+                    [lo(x3, dx, 1), hi(x5, dx, 1)], [lo(x5, dx, 1), hi(xR, dx, 1)]], np.int32)
+    frj = np.array([[lo(r3, dr, 2), hi(r4, dr, 1)], [lo(r5, dr, 1), hi(r4, dr, 1)], [lo(r1, dr, 2), hi(r5, dr, 1)],
+                    [lo(0.0, dr, 2), hi(r5, dr, 1)], [lo(0.0, dr, 2), hi(rmax, dr, 1)]], np.int32)
+
+    def segs(I, J, axis):
+        t = dict(z0=(I[0][0], I[0][0], J[0][0], J[0][1]), z1=(I[2][0], I[2][0], J[2][0], J[0][0] - 1),
+                 z2=(I[3][0], I[3][0], J[3][0], J[2][0] - 1), z4=(I[4][0], I[4][0], J[1][0], J[4][1]),
+                 z3=(I[1][1], I[1][1], J[1][0], J[1][1]), z5=(I[4][1], I[4][1], J[4][0], J[4][1]),
+                 x0=(I[0][0], I[0][1], J[0][0], J[0][0]), x2=(I[2][0], I[2][1], J[2][0], J[2][0]),
+                 x1=(I[0][0], I[1][1], J[0][1], J[0][1]), x4=(I[1][1] + 1, I[3][1], J[3][1], J[3][1]),
+                 x5=(I[4][0], I[4][1], J[4][1], J[4][1]),
+                 x6=(I[3][0], I[4][1], J[3][0], J[3][0]) if axis else None)
+        return {k: (tuple(int(v) for v in s) if s is not None else None) for k, s in t.items()}
+
+    ghosts = [(ib[0][0], ib[0][0], jb[0][0], jb[0][1], -1, 0, 0), (ib[1][0], ib[1][0], jb[1][0], jb[0][0] - 1, -1, 0, 0),
+              (ib[0][0], ib[0][1], jb[0][0], jb[0][0], 0, -1, 0), (ib[1][1], ib[1][1], jb[1][0], jb[1][1], 1, 0, 1),
+              (ib[0][0], ib[1][1], jb[0][1], jb[0][1], 0, 1, 1)]
+    return dict(ni=ni, nj=nj, dx=dx, dr=dr, ib=ib, jb=jb, fxi=fxi, fxj=fxj, fri=fri, frj=frj,
+                flags=cathode_flags(ni, nj, ib, jb), ghosts=[tuple(int(v) for v in g) for g in ghosts],
+                seg=dict(c=segs(ib, jb, False), x=segs(fxi, fxj, False), r=segs(fri, frj, True)))
+
+
+def rectangle_geometry(ni, nj, Lz=10e-3, Lr=5e-3) -> dict:
+    """The r-z rectangle as one fluid block: z = 0 grounded wall (the reference's
+    z0), z = L the biased electrode (z5), r = R a grounded wall (x1), r = 0 the axis."""
+    one = lambda a, b: np.array([[a, b]], np.int32)
+    empty = dict(z1=None, z2=None, z3=None, z4=None, x0=None, x2=None, x4=None, x5=None)
+    seg = dict(c=dict(empty, z0=(1, 1, 1, nj), z5=(ni, ni, 1, nj), x1=(1, ni, nj, nj), x6=None),
+               x=dict(empty, z0=(2, 2, 1, nj), z5=(ni, ni, 1, nj), x1=(2, ni, nj, nj), x6=None),
+               r=dict(empty, z0=(1, 1, 2, nj), z5=(ni, ni, 2, nj), x1=(1, ni, nj, nj), x6=(1, ni, 2, 2)))
+    ghosts = [(1, 1, 1, nj, -1, 0, 0), (ni, ni, 1, nj, 1, 0, 1), (1, ni, nj, nj, 0, 1, 1)]
+    return dict(ni=ni, nj=nj, dx=Lz / ni, dr=Lr / nj, ib=one(1, ni), jb=one(1, nj), fxi=one(2, ni), fxj=one(1, nj),
+                fri=one(1, ni), frj=one(2, nj), flags=rectangle_flags(ni, nj), ghosts=ghosts, seg=seg)
+
+
+_K = dict(WALL_FOLD=1, ZERO_COEF=2, FOLD_SUB=3, OPEN_FOLD=4, SET_WALL=5, SET_ZERO=6, COPY=7, SET_OPEN=8)
+_D = dict(W=0, E=1, S=2, N=3)
+
+
+def _op(kind, s, di0=0, di1=0, dj0=0, dj1=0, di=0, dj=0, dir="W", sign=0, bias=0, pair=0, scale=0):
+    if s is None:
+        return None
+    i0, i1, j0, j1 = s[0] + di0, s[1] + di1, s[2] + dj0, s[3] + dj1
+    if i0 > i1 or j0 > j1:
+        return None
+    return (_K[kind], i0, i1, j0, j1, di, dj, _D[dir], sign, bias, pair, scale)
+
+
+def ion_programs(seg: dict) -> list:
+    """The wall programs of the ion momentum sweeps, in the reference's loop order:
+    [Uix assembly, Uix after solve, Uir assembly, Uir after solve, Uip assembly,
+    Uip after solve] (fluidModule.hpp:216-579, :675-1046, :1114-1399)."""
+    X, R, C = seg["x"], seg["r"], seg["c"]
+    left, right = ("z0", "z1", "z2", "z4"), ("z3", "z5")
+    P = [[] for _ in range(6)]
+    # Uix
+    for n in left:
+        P[0].append(_op("WALL_FOLD", X[n], dir="W", sign=-1, pair=0))
+    for n in right:
+        P[0].append(_op("WALL_FOLD", X[n], dir="E", sign=1, bias=int(n == "z5"), pair=0))
+    for n in ("x0", "x2"):
+        P[0].append(_op("ZERO_COEF", X[n], dir="S"))
+    for n in ("x1", "x4", "x5"):
+        P[0].append(_op("ZERO_COEF", X[n], dir="N"))
+    for n in left:
+        P[1].append(_op("SET_WALL", X[n], di=-1, sign=-1, pair=0))
+    for n in right:
+        P[1].append(_op("SET_WALL", X[n], di=1, sign=1, bias=int(n == "z5"), pair=0))
+    P[1].append(_op("SET_ZERO", X["x0"], di1=-1, dj=-1))
+    P[1].append(_op("SET_ZERO", X["x2"], di1=-1, dj=-1))
+    P[1].append(_op("SET_ZERO", X["x1"], dj=-1))          # the row below the top row, as the reference writes it
+    P[1].append(_op("SET_ZERO", X["x4"], di0=1, di1=-1, dj=1))
+    P[1].append(_op("SET_ZERO", X["x5"], dj=1))
+    # Uir
+    for n in left:
+        P[2].append(_op("ZERO_COEF", R[n], dir="W"))
+    for n in right:
+        P[2].append(_op("ZERO_COEF", R[n], dir="E"))
+    for n in ("x0", "x2"):
+        P[2].append(_op("WALL_FOLD", R[n], dir="S", sign=-1, pair=1))
+    P[2].append(_op("ZERO_COEF", R["x6"], dir="S"))
+    for n in ("x1", "x4"):
+        P[2].append(_op("WALL_FOLD", R[n], dir="N", sign=1, pair=1))
+    P[2].append(_op("OPEN_FOLD", R["x5"], dir="N"))
+    for n, adj in (("z0", (0, 0)), ("z1", (0, -1)), ("z2", (0, -1)), ("z4", (1, 0))):
+        P[3].append(_op("SET_ZERO", R[n], dj0=adj[0], dj1=adj[1], di=-1))
+    for n, adj in (("z3", (1, 0)), ("z5", (0, 0))):
+        P[3].append(_op("SET_ZERO", R[n], dj0=adj[0], dj1=adj[1], di=1))
+    for n in ("x0", "x2"):
+        P[3].append(_op("SET_WALL", R[n], dj=-1, sign=-1, pair=1))
+    P[3].append(_op("SET_ZERO", R["x6"], dj=-1))
+    for n in ("x1", "x4"):
+        P[3].append(_op("SET_WALL", R[n], dj=1, sign=1, pair=1))
+    P[3].append(_op("SET_OPEN", R["x5"], dj=1))
+    # Uip
+    for n in left:
+        P[4].append(_op("FOLD_SUB", C[n], dir="W"))
+    for n in right:
+        P[4].append(_op("FOLD_SUB", C[n], dir="E"))
+    for n in ("x0", "x2"):
+        P[4].append(_op("FOLD_SUB", C[n], dir="S", scale=1))
+    for n in ("x1", "x4", "x5"):
+        P[4].append(_op("FOLD_SUB", C[n], dir="N", scale=2))
+    for n in left:
+        P[5].append(_op("COPY", C[n], di=-1))
+    for n in right:
+        P[5].append(_op("COPY", C[n], di=1))
+    for n in ("x0", "x2"):
+        P[5].append(_op("COPY", C[n], dj=-1, scale=1))
+    for n in ("x1", "x4", "x5"):
+        P[5].append(_op("COPY", C[n], dj=1, scale=2))
+    return [[o for o in prog if o is not None] for prog in P]
+
+
+def ion_boxes(geo: dict) -> list:
+    """Residual boxes of correct_Ui_constTe (fluidModule.hpp:1960-2070): rhoi and Uip
+    over the cell blocks, Uix over the x-face blocks extended by one face in i, Uir
+    over the r-face blocks without their first face in j."""
+    cells = [(a, b, c, e) for (a, b), (c, e) in zip(geo["ib"], geo["jb"])]
+    xs = [(a, b + 1, c, e) for (a, b), (c, e) in zip(geo["fxi"], geo["fxj"])]
+    rs = [(a, b, c + 1, e) for (a, b), (c, e) in zip(geo["fri"], geo["frj"])]
+    return [cells, xs, rs, cells]

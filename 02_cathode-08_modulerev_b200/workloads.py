@@ -280,3 +280,27 @@ def sg_state(ni: int, nj: int, seed: int = 6, Lz: float = 10e-3, Lr: float = 5e-
                coefMISEE_ts=0.08, Te_emitSEE_eV=2.5, ratioEngy_EISEE_rd=0.5, error_cnv_HES=1e-21,
                error_cnv_SOR=1e-10, maxITR_HES=2, maxITR_SOR=30, flag_error=3, flag_iter=1, precision=1)
     return dict(fields=f, prm=prm)
+
+
+def ion_state(ni: int, nj: int, seed: int = 7, Lz: float = 10e-3, Lr: float = 5e-3) -> dict:
+    """pc_state extended with the ion arrays: Uix, Uir N(0, 300) m/s, Uip N(0, 100) m/s,
+    nui_m log-uniform in [1e4, 1e6] s^-1, zero ion fluxes.  Parameters of the shipped
+    setup (input/setup.yaml): Ti 300 K, Te_rep 0.1 eV, SMG 30 iterations to 1e-10,
+    ndt_i 1, calcRes mode 3, CFL 1; dt 1e-10 s, rmax = Lr."""
+    st = pc_state(ni, nj, seed=seed, Lz=Lz, Lr=Lr)
+    f = st["fields"]
+    rng = np.random.default_rng(seed + 2000)
+    sh = f["rhoe"].shape
+    f["Uix"] = 300.0 * rng.standard_normal(sh)
+    f["Uir"] = 300.0 * rng.standard_normal(sh)
+    f["Uip"] = 100.0 * rng.standard_normal(sh)
+    f["nui_m"] = 10.0 ** rng.uniform(4.0, 6.0, sh)
+    f["Bx"] = 0.05 * rng.standard_normal(sh)
+    f["Br"] = 0.05 * rng.standard_normal(sh)
+    for k in ("rhoUix", "rhoUir", "rhoUix_wall", "rhoUir_wall"):
+        f[k] = np.zeros(sh)
+    p = st["prm"]
+    prm = dict(dt=p["dt"], dx=p["dx"], dr=p["dr"], rmin=0.0, rmax=Lr, massi=MASSI_XE, Ti=300.0, V_bias=20.0,
+               Te_rep_eV=0.1, CFL=1.0, error_cnv_SOR=1e-10, ndt_i=1, maxITR_SOR=30, flag_iter=1, precision=1,
+               flag_error=3)
+    return dict(fields=f, prm=prm)

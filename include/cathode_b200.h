@@ -256,6 +256,18 @@ typedef struct cth_pc_result {
 } cth_pc_result;
 int cth_solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, void* stream, cth_pc_result* res);
 
+/* FluidModule::check_CFL (fluidModule.hpp:57-115): dt_min = eps0 / (e max(rhoe)
+ * max(mu_para)) over the index space; flag_adp_dt == 1 sets dt = dt_min CFL,
+ * otherwise CFL = dt / dt_min.  ue_max = max electron speed over the grid cells
+ * + the thermal speed at max(Te). */
+typedef struct cth_cfl {
+    double dt, CFL;           /* in/out                      */
+    double masse, rmin, dr;   /* in                          */
+    int flag_adp_dt;          /* in                          */
+    double dt_min, rhoe_max, mu_max, Te_max, ue_max;  /* out */
+} cth_cfl;
+int cth_check_cfl(cth_fields* fs, cth_cfl* io, void* stream);
+
 /* Ghost rules applied after the electron sweeps (fluidModule.hpp:3884-3921 for
  * rhoe, :4878-4914 for Te): n rules of 7 ints (i0, i1, j0, j1, di, dj, mode),
  * each a one-cell-wide segment of grid cells whose neighbour (i+di, j+dj) is
@@ -283,6 +295,56 @@ typedef struct cth_sg_params {
 } cth_sg_params;
 int cth_solve_rhoe_pc(cth_fields* fs, const cth_sg_params* prm, void* stream, cth_pc_result* res);
 int cth_solve_Te_pc(cth_fields* fs, const cth_sg_params* prm, void* stream, cth_pc_result* res);
+
+/* Ion sub-step (src/main.cpp:191-197): FluidModule::solve_Uix_tmp, solve_Uir_tmp,
+ * solve_Uip_tmp (fluidModule.hpp:123-1404), solve_rhoi_constTe (:1405-1755) and
+ * correct_Ui_constTe (:1763-2072).  gx / gr are grids of the same shape whose
+ * blocks are the x-face / r-face blocks (the Uix / Uir unknowns); the store's grid
+ * holds the cell blocks.  Reads phi, Ex, Er, Bx, Br, rate_ionize, nui_m; updates
+ * Uix, Uir, Uip, rhoi, rhoUix, rhoUir, rhoUix_wall, rhoUir_wall and the *_old
+ * copies.  The wall conditions of the three momentum equations are wall programs
+ * (ordered segment operations, cth_ion_program_upload) built from the named wall
+ * segments of the reference's loops; the residuals run over the boxes of
+ * cth_ion_boxes_upload (0 rhoi, 1 Uix, 2 Uir, 3 Uip; 4 ints each: i0, i1, j0, j1). */
+typedef struct cth_ion_params {
+    double dt, dx, dr, rmin, rmax, massi, Ti, V_bias, Te_rep_eV, CFL, error_cnv_SOR;
+    int ndt_i, maxITR_SOR, flag_iter, precision, flag_error;
+} cth_ion_params;
+
+typedef struct cth_ion_result {
+    double error_rhoi, error_Uix, error_Uir, error_Uip;
+    int solver_rc;
+    int reserved;
+    cth_status solver[4];  /* Uix, Uir, Uip, rhoi */
+} cth_ion_result;
+
+/* wall-program operation over the points (i, j) of [i0, i1] x [j0, j1] */
+enum {
+    CTH_ION_WALL_FOLD = 1, /* b += a_dir U_wall, a_dir = 0                                   */
+    CTH_ION_ZERO_COEF = 2, /* a_dir = 0                                                       */
+    CTH_ION_FOLD_SUB = 3,  /* aP -= a_dir * scale, a_dir = 0                                  */
+    CTH_ION_OPEN_FOLD = 4, /* b += aN r_face/r_up max(U_old, 0), aN = 0 (open top)            */
+    CTH_ION_SET_WALL = 5,  /* U(i+di, j+dj) = U_wall                                          */
+    CTH_ION_SET_ZERO = 6,  /* U(i+di, j+dj) = 0                                               */
+    CTH_ION_COPY = 7,      /* U(i+di, j+dj) = scale * U(i, j)                                 */
+    CTH_ION_SET_OPEN = 8   /* U(i+di, j+dj) = r_face/r_up max(U_old(i, j), 0)                 */
+};
+/* programs: assembly / after-solve for Uix, Uir, Uip */
+enum { CTH_ION_PROG_UIX_ASM = 0, CTH_ION_PROG_UIX_POST = 1, CTH_ION_PROG_UIR_ASM = 2, CTH_ION_PROG_UIR_POST = 3,
+       CTH_ION_PROG_UIP_ASM = 4, CTH_ION_PROG_UIP_POST = 5, CTH_ION_NPROG = 6 };
+typedef struct cth_ion_op {
+    int kind, i0, i1, j0, j1;
+    int di, dj;   /* target offset (SET_*, COPY)                                         */
+    int dir;      /* coefficient: 0 aW, 1 aE, 2 aS, 3 aN                                  */
+    int sign;     /* U_wall sign (-1 low side, +1 high side)                              */
+    int bias;     /* U_wall measured from V_bias (the biased electrode)                   */
+    int pair;     /* U_wall potential: 0 mean of cells i-1, i; 1 mean of cells j-1, j       */
+    int scale;    /* 0: 1, 1: r_j / r_{j-1}, 2: r_j / r_{j+1}                              */
+} cth_ion_op;
+int cth_ion_program_upload(cth_fields* fs, int which, const cth_ion_op* ops, int n);
+int cth_ion_boxes_upload(cth_fields* fs, int which, const int* boxes, int n);
+int cth_ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_params* prm, void* stream,
+                 cth_ion_result* res);
 
 /* Residual (device arrays): r = b - A x on grid cells (couplings to non-grid
  * cells dropped), r = 0 elsewhere; *rnorm = ||r||_2, *bnorm = ||b||_2 over grid

@@ -814,3 +814,398 @@ def solve_sg_pc(st: dict, prm: dict, geo: dict, see, solve, species: str) -> dic
     out["error_" + fxk] = calc_res(Fx, Fx_old, geo["fxi"], geo["fxj"], 1e-100, fe)
     out["error_" + frk] = calc_res(Fr, Fr_old, geo["fri"], geo["frj"], 1e-100, fe)
     return out
+
+
+def check_cfl(f: dict, prm: dict) -> dict:
+    """FluidModule::check_CFL (fluidModule.hpp:57-115)."""
+    rhoe, Te = f["rhoe"], f["Te"]
+    ni, nj = rhoe.shape[0] - 2, rhoe.shape[1] - 2
+    r = prm["rmin"] + (np.arange(nj + 2) - 0.5) * prm["dr"]
+    rhoe_max = max(0.0, rhoe.max())
+    mu_max = max(0.0, f["mu_para"].max())
+    Te_max = max(0.0, Te.max())
+    I, J = slice(1, ni + 1), slice(1, nj + 1)
+    rL = (r[1:nj + 1] + r[0:nj]) / 2.0
+    rR = (r[1:nj + 1] + r[2:nj + 2]) / 2.0
+    ux = (f["rhoUex"][2:ni + 2, J] + f["rhoUex"][I, J]) / 2.0 / (rhoe[I, J] + 1e-100)
+    ur = (rR * f["rhoUer"][I, 2:nj + 2] + rL * f["rhoUer"][I, J]) / (2.0 * r[J]) / (rhoe[I, J] + 1e-100)
+    ue_max = max(0.0, np.sqrt(ux * ux + ur * ur).max()) + np.sqrt(8.0 * BOLTZ * Te_max / (np.pi * prm["masse"]))
+    dt_min = EPS0 / (E0 * rhoe_max * mu_max)
+    out = dict(rhoe_max=rhoe_max, mu_max=mu_max, Te_max=Te_max, ue_max=ue_max, dt_min=dt_min)
+    if prm.get("flag_adp_dt", 0) == 1:
+        out.update(dt=dt_min * prm["CFL"], CFL=prm["CFL"])
+    else:
+        out.update(dt=prm["dt"], CFL=prm["dt"] / dt_min)
+    return out
+
+
+# ----------------------------------------------------------------------------
+# ion step: momentum (Uix, Uir, Uip), continuity and velocity correction
+# ----------------------------------------------------------------------------
+
+def ion_segments(geo: dict) -> dict:
+    """Wall segments of the ion sweeps on the cell ('c'), x-face ('x') and r-face
+    ('r') index spaces, named as in the reference (z0..z5 axial walls, x0..x5 radial
+    walls, x6 the axis), each (i0, i1, j0, j1) or None.  Cathode: the loop bounds of
+    fluidModule.hpp:218-360 (x faces), :700-800 (r faces), :1130-1200 (cells);
+    rectangle: z0 at z = 0, z5 the biased electrode, x1 the wall at r = R, x6 the axis."""
+    if len(geo["ib"]) == 5:
+        ib, jb, fxi, fxj, fri, frj = geo["ib"], geo["jb"], geo["fxi"], geo["fxj"], geo["fri"], geo["frj"]
+
+        def table(I, J, axis):
+            t = dict(z0=(I[0][0], I[0][0], J[0][0], J[0][1]), z1=(I[2][0], I[2][0], J[2][0], J[0][0] - 1),
+                     z2=(I[3][0], I[3][0], J[3][0], J[2][0] - 1), z4=(I[4][0], I[4][0], J[1][0], J[4][1]),
+                     z3=(I[1][1], I[1][1], J[1][0], J[1][1]), z5=(I[4][1], I[4][1], J[4][0], J[4][1]),
+                     x0=(I[0][0], I[0][1], J[0][0], J[0][0]), x2=(I[2][0], I[2][1], J[2][0], J[2][0]),
+                     x1=(I[0][0], I[1][1], J[0][1], J[0][1]), x4=(I[1][1] + 1, I[3][1], J[3][1], J[3][1]),
+                     x5=(I[4][0], I[4][1], J[4][1], J[4][1]))
+            t["x6"] = (I[3][0], I[4][1], J[3][0], J[3][0]) if axis else None
+            return {k: tuple(int(v) for v in s) if s is not None else None for k, s in t.items()}
+
+        return dict(c=table(ib, jb, False), x=table(fxi, fxj, False), r=table(fri, frj, True))
+    ni, nj = geo["ni"], geo["nj"]
+    empty = dict(z1=None, z2=None, z3=None, z4=None, x0=None, x2=None, x4=None, x5=None)
+    return dict(c=dict(empty, z0=(1, 1, 1, nj), z5=(ni, ni, 1, nj), x1=(1, ni, nj, nj), x6=None),
+                x=dict(empty, z0=(2, 2, 1, nj), z5=(ni, ni, 1, nj), x1=(2, ni, nj, nj), x6=None),
+                r=dict(empty, z0=(1, 1, 2, nj), z5=(ni, ni, 2, nj), x1=(1, ni, nj, nj), x6=(1, ni, 2, 2)))
+
+
+def _pts(s, di0=0, di1=0, dj0=0, dj1=0):
+    """Points of a segment with adjusted bounds, in loop order."""
+    if s is None:
+        return []
+    i0, i1, j0, j1 = s
+    return [(i, j) for i in range(i0 + di0, i1 + di1 + 1) for j in range(j0 + dj0, j1 + dj1 + 1)]
+
+
+def _ui_wall(Uold, phi_a, phi_b, sign, bias, prm):
+    dphi = (phi_a + phi_b) / 2.0 - bias
+    return sign * np.sqrt(Uold ** 2 + max(2.0 * E0 * dphi / prm["massi"], 0.0))
+
+
+def _erf(x):
+    from scipy.special import erf
+    return erf(x)
+
+
+def ion_step(st: dict, prm: dict, geo: dict, solve_c, solve_x, solve_r) -> dict:
+    """The ion sub-step of the time loop (src/main.cpp:191-197): solve_Uix_tmp,
+    solve_Uir_tmp, solve_Uip_tmp (fluidModule.hpp:123-1404), solve_rhoi_constTe
+    (:1405-1755) and correct_Ui_constTe (:1763-2072).
+
+    st: Uix, Uir, Uip, rhoi, phi, Ex, Er, Bx, Br, rate_ionize, nui_m, rhoUix, rhoUir,
+    rhoUix_wall, rhoUir_wall.  prm: dt, ndt_i, dx, dr, rmin, rmax, massi, Ti,
+    V_bias, Te_rep_eV, CFL, flag_error.  solve_c / solve_x / solve_r(aP, aE, aW, aN,
+    aS, b, ib, jb) return the block solutions of the cell, x-face and r-face
+    systems (zero start)."""
+    ni, nj = geo["ni"], geo["nj"]
+    dx, dr = prm["dx"], prm["dr"]
+    dt_i = prm["dt"] * float(prm["ndt_i"])
+    massi, Ti = prm["massi"], prm["Ti"]
+    r = prm["rmin"] + (np.arange(nj + 2) - 0.5) * dr
+    S = ion_segments(geo)
+    m = _masks(geo)
+    g = {k: v.copy() for k, v in st.items()}
+    phi = g["phi"]
+    Uix_old, Uir_old, Uip_old, rhoi_old = g["Uix"].copy(), g["Uir"].copy(), g["Uip"].copy(), g["rhoi"].copy()
+    sh = (ni + 2, nj + 2)
+
+    # --- solve_Uix_tmp (:123-594) -------------------------------------------
+    aP, aE, aW, aN, aS, b = (np.zeros(sh) for _ in range(6))
+    for (a0, a1), (c0, c1) in zip(geo["fxi"], geo["fxj"]):
+        I = np.arange(a0, a1 + 1)[:, None]
+        J = np.arange(c0, c1 + 1)[None, :]
+        rL = (r[J] + r[J - 1]) / 2.0
+        rR = (r[J] + r[J + 1]) / 2.0
+        qL, qR = rL / r[J], rR / r[J]
+        ULx = (Uix_old[I, J] + Uix_old[I - 1, J]) / 2.0
+        URx = (Uix_old[I, J] + Uix_old[I + 1, J]) / 2.0
+        ULr = (Uir_old[I, J] + Uir_old[I - 1, J]) / 2.0
+        URr = (Uir_old[I, J + 1] + Uir_old[I - 1, J + 1]) / 2.0
+        rho_t = (g["rhoi"][I, J] + g["rhoi"][I - 1, J]) / 2.0
+        riz = (g["rate_ionize"][I, J] + g["rate_ionize"][I - 1, J]) / 2.0
+        nui = (g["nui_m"][I, J] + g["nui_m"][I - 1, J]) / 2.0
+        dndx = (g["rhoi"][I, J] - g["rhoi"][I - 1, J]) / dx
+        Uip_t = (Uip_old[I, J] + Uip_old[I - 1, J]) / 2.0
+        Br_t = (g["Br"][I, J] + g["Br"][I - 1, J]) / 2.0
+        lor = -E0 * Uip_t * Br_t
+        aE[I, J] = -(URx - np.abs(URx)) / (2.0 * dx)
+        aW[I, J] = (ULx + np.abs(ULx)) / (2.0 * dx)
+        aN[I, J] = -qR * (URr - np.abs(URr)) / (2.0 * dr)
+        aS[I, J] = qL * (ULr + np.abs(ULr)) / (2.0 * dr)
+        aP[I, J] = 1.0 / dt_i + riz / (rho_t + 1e-100) + nui + aE[I, J] + aW[I, J] + aN[I, J] + aS[I, J]
+        b[I, J] = (Uix_old[I, J] / dt_i + (E0 * g["Ex"][I, J] + lor) / massi
+                   - BOLTZ * Ti / (massi * rho_t + 1e-100) * dndx)
+    X = S["x"]
+    for name, sign, coef, bias in (("z0", -1, aW, 0), ("z1", -1, aW, 0), ("z2", -1, aW, 0), ("z4", -1, aW, 0),
+                                   ("z3", 1, aE, 0), ("z5", 1, aE, 1)):
+        for i, j in _pts(X[name]):
+            Uw = _ui_wall(Uix_old[i, j], phi[i, j], phi[i - 1, j], sign, prm["V_bias"] * bias, prm)
+            b[i, j] = b[i, j] + coef[i, j] * Uw
+            coef[i, j] = 0.0
+    for name, coef in (("x0", aS), ("x2", aS), ("x1", aN), ("x4", aN), ("x5", aN)):
+        for i, j in _pts(X[name]):
+            coef[i, j] = 0.0
+    x = solve_x(aP, aE, aW, aN, aS, b, geo["fxi"], geo["fxj"])
+    for (a0, a1), (c0, c1) in zip(geo["fxi"], geo["fxj"]):
+        g["Uix"][a0:a1 + 1, c0:c1 + 1] = x[a0:a1 + 1, c0:c1 + 1]
+    for name, sign, di, bias in (("z0", -1, -1, 0), ("z1", -1, -1, 0), ("z2", -1, -1, 0), ("z4", -1, -1, 0),
+                                 ("z3", 1, 1, 0), ("z5", 1, 1, 1)):
+        for i, j in _pts(X[name]):
+            g["Uix"][i + di, j] = _ui_wall(Uix_old[i, j], phi[i, j], phi[i - 1, j], sign, prm["V_bias"] * bias, prm)
+    for i, j in _pts(X["x0"], di1=-1):
+        g["Uix"][i, j - 1] = 0.0
+    for i, j in _pts(X["x2"], di1=-1):
+        g["Uix"][i, j - 1] = 0.0
+    for i, j in _pts(X["x1"]):
+        g["Uix"][i, j - 1] = 0.0          # the reference writes the row below the top row here
+    for i, j in _pts(X["x4"], di0=1, di1=-1):
+        g["Uix"][i, j + 1] = 0.0
+    for i, j in _pts(X["x5"]):
+        g["Uix"][i, j + 1] = 0.0
+
+    # --- solve_Uir_tmp (:601-1053) ------------------------------------------
+    aP, aE, aW, aN, aS, b = (np.zeros(sh) for _ in range(6))
+    for (a0, a1), (c0, c1) in zip(geo["fri"], geo["frj"]):
+        I = np.arange(a0, a1 + 1)[:, None]
+        J = np.arange(c0, c1 + 1)[None, :]
+        r_t = (r[J] + r[J - 1]) / 2.0
+        rL = (r[J - 1] + r[J - 2]) / 2.0
+        rR = (r[J + 1] + r[J]) / 2.0
+        ULx = (r[J] * Uix_old[I, J] + r[J - 1] * Uix_old[I, J - 1]) / (2.0 * r_t)
+        URx = (r[J] * Uix_old[I + 1, J] + r[J - 1] * Uix_old[I + 1, J - 1]) / (2.0 * r_t)
+        ULr = (r_t * Uir_old[I, J] + rL * Uir_old[I, J - 1]) / (2.0 * r[J - 1])
+        URr = (r_t * Uir_old[I, J] + rR * Uir_old[I, J + 1]) / (2.0 * r[J])
+        rho_t = (g["rhoi"][I, J] + g["rhoi"][I, J - 1]) / 2.0
+        riz = (g["rate_ionize"][I, J] + g["rate_ionize"][I, J - 1]) / 2.0
+        nui = (g["nui_m"][I, J] + g["nui_m"][I, J - 1]) / 2.0
+        dndr = (g["rhoi"][I, J] - g["rhoi"][I, J - 1]) / dr
+        Bx_t = (r[J] * g["Bx"][I, J] + r[J - 1] * g["Bx"][I, J - 1]) / (2.0 * r_t)
+        Uip_t = (r[J] * Uip_old[I, J] + r[J - 1] * Uip_old[I, J - 1]) / (2.0 * r_t)
+        lor = E0 * Uip_t * Bx_t
+        cen = -Uip_t * Uip_t / r_t
+        aE[I, J] = -(URx - np.abs(URx)) / (2.0 * dx)
+        aW[I, J] = (ULx + np.abs(ULx)) / (2.0 * dx)
+        aN[I, J] = -r[J] / r_t * (URr - np.abs(URr)) / (2.0 * dr)
+        aS[I, J] = r[J - 1] / r_t * (ULr + np.abs(ULr)) / (2.0 * dr)
+        aP[I, J] = 1.0 / dt_i + riz / (rho_t + 1e-100) + nui + aE[I, J] + aW[I, J] + aN[I, J] + aS[I, J]
+        b[I, J] = (Uir_old[I, J] / dt_i + (E0 * g["Er"][I, J] + lor) / massi
+                   - BOLTZ * Ti / (massi * rho_t + 1e-100) * dndr + cen)
+    R = S["r"]
+    for name, coef in (("z0", aW), ("z1", aW), ("z2", aW), ("z4", aW), ("z3", aE), ("z5", aE)):
+        for i, j in _pts(R[name]):
+            coef[i, j] = 0.0
+    for name, sign, coef in (("x0", -1, aS), ("x2", -1, aS)):
+        for i, j in _pts(R[name]):
+            Uw = _ui_wall(Uir_old[i, j], phi[i, j], phi[i, j - 1], sign, 0.0, prm)
+            b[i, j] = b[i, j] + coef[i, j] * Uw
+            coef[i, j] = 0.0
+    for i, j in _pts(R["x6"]):
+        aS[i, j] = 0.0
+    for name in ("x1", "x4"):
+        for i, j in _pts(R[name]):
+            Uw = _ui_wall(Uir_old[i, j], phi[i, j], phi[i, j - 1], 1, 0.0, prm)
+            b[i, j] = b[i, j] + aN[i, j] * Uw
+            aN[i, j] = 0.0
+    for i, j in _pts(R["x5"]):
+        r_t = (r[j] + r[j - 1]) / 2.0
+        rR = (r[j + 1] + r[j]) / 2.0
+        b[i, j] = b[i, j] + aN[i, j] * r_t / rR * max(Uir_old[i, j], 0.0)
+        aN[i, j] = 0.0
+    x = solve_r(aP, aE, aW, aN, aS, b, geo["fri"], geo["frj"])
+    for (a0, a1), (c0, c1) in zip(geo["fri"], geo["frj"]):
+        g["Uir"][a0:a1 + 1, c0:c1 + 1] = x[a0:a1 + 1, c0:c1 + 1]
+    for name, di, adj in (("z0", -1, (0, 0)), ("z1", -1, (0, -1)), ("z2", -1, (0, -1)), ("z4", -1, (1, 0)),
+                          ("z3", 1, (1, 0)), ("z5", 1, (0, 0))):
+        for i, j in _pts(R[name], dj0=adj[0], dj1=adj[1]):
+            g["Uir"][i + di, j] = 0.0
+    for name in ("x0", "x2"):
+        for i, j in _pts(R[name]):
+            g["Uir"][i, j - 1] = _ui_wall(Uir_old[i, j], phi[i, j], phi[i, j - 1], -1, 0.0, prm)
+    for i, j in _pts(R["x6"]):
+        g["Uir"][i, j - 1] = 0.0
+    for name in ("x1", "x4"):
+        for i, j in _pts(R[name]):
+            g["Uir"][i, j + 1] = _ui_wall(Uir_old[i, j], phi[i, j], phi[i, j - 1], 1, 0.0, prm)
+    for i, j in _pts(R["x5"]):
+        r_t = (r[j] + r[j - 1]) / 2.0
+        rR = (r[j + 1] + r[j]) / 2.0
+        g["Uir"][i, j + 1] = r_t / rR * max(Uir_old[i, j], 0.0)
+
+    # --- solve_Uip_tmp (:1054-1404) -----------------------------------------
+    aP, aE, aW, aN, aS, b = (np.zeros(sh) for _ in range(6))
+    for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
+        I = np.arange(a0, a1 + 1)[:, None]
+        J = np.arange(c0, c1 + 1)[None, :]
+        rL = (r[J] + r[J - 1]) / 2.0
+        rR = (r[J] + r[J + 1]) / 2.0
+        qL, qR = rL / r[J], rR / r[J]
+        ULx, URx = Uix_old[I, J], Uix_old[I + 1, J]
+        ULr, URr = Uir_old[I, J], Uir_old[I, J + 1]
+        Ux_t = (Uix_old[I + 1, J] + Uix_old[I, J]) / 2.0
+        Ur_t = (rL * Uir_old[I, J] + rR * Uir_old[I, J + 1]) / (2.0 * r[J])
+        lor = E0 * (Ux_t * g["Br"][I, J] - Ur_t * g["Bx"][I, J])
+        cen = g["Uip"][I, J] * Ur_t / r[J]
+        aE[I, J] = -(URx - np.abs(URx)) / (2.0 * dx)
+        aW[I, J] = (ULx + np.abs(ULx)) / (2.0 * dx)
+        aN[I, J] = -qR * (URr - np.abs(URr)) / (2.0 * dr)
+        aS[I, J] = qL * (ULr + np.abs(ULr)) / (2.0 * dr)
+        aP[I, J] = (1.0 / dt_i + g["rate_ionize"][I, J] / (g["rhoi"][I, J] + 1e-100) + g["nui_m"][I, J]
+                    + aE[I, J] + aW[I, J] + aN[I, J] + aS[I, J])
+        b[I, J] = Uip_old[I, J] / dt_i + lor / massi + cen
+    C = S["c"]
+    for name, coef in (("z0", aW), ("z1", aW), ("z2", aW), ("z4", aW), ("z3", aE), ("z5", aE)):
+        for i, j in _pts(C[name]):
+            aP[i, j] = aP[i, j] - coef[i, j]
+            coef[i, j] = 0.0
+    for name in ("x0", "x2"):
+        for i, j in _pts(C[name]):
+            aP[i, j] = aP[i, j] - aS[i, j] * r[j] / r[j - 1]
+            aS[i, j] = 0.0
+    for name in ("x1", "x4", "x5"):
+        for i, j in _pts(C[name]):
+            aP[i, j] = aP[i, j] - aN[i, j] * r[j] / r[j + 1]
+            aN[i, j] = 0.0
+    x = solve_c(aP, aE, aW, aN, aS, b, geo["ib"], geo["jb"])
+    for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
+        g["Uip"][a0:a1 + 1, c0:c1 + 1] = x[a0:a1 + 1, c0:c1 + 1]
+    for name, di in (("z0", -1), ("z1", -1), ("z2", -1), ("z4", -1), ("z3", 1), ("z5", 1)):
+        for i, j in _pts(C[name]):
+            g["Uip"][i + di, j] = g["Uip"][i, j]
+    for name in ("x0", "x2"):
+        for i, j in _pts(C[name]):
+            g["Uip"][i, j - 1] = r[j] / r[j - 1] * g["Uip"][i, j]
+    for name in ("x1", "x4", "x5"):
+        for i, j in _pts(C[name]):
+            g["Uip"][i, j + 1] = r[j] / r[j + 1] * g["Uip"][i, j]
+
+    # --- solve_rhoi_constTe (:1405-1755) ------------------------------------
+    Uix, Uir = g["Uix"], g["Uir"]
+    Te_rep = prm["Te_rep_eV"] * E0 / BOLTZ
+    nu_star = 1.0 / prm["rmax"] * np.sqrt(BOLTZ * Te_rep / massi)
+    vth = np.sqrt(8.0 * BOLTZ * Ti / (np.pi * massi))
+    um = np.sqrt(2.0 * BOLTZ * Ti / massi)
+    sq = np.sqrt(np.pi)
+    aP, aE, aW, aN, aS, b = (np.zeros(sh) for _ in range(6))
+    nui_m = g["nui_m"]
+    for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
+        I = np.arange(a0, a1 + 1)[:, None]
+        J = np.arange(c0, c1 + 1)[None, :]
+        rL = (r[J] + r[J - 1]) / 2.0
+        rR = (r[J] + r[J + 1]) / 2.0
+        qL, qR = rL / r[J], rR / r[J]
+        ULx, URx, ULr, URr = Uix[I, J], Uix[I + 1, J], Uir[I, J], Uir[I, J + 1]
+        D = lambda nu: BOLTZ * (Ti + Te_rep) / (massi * (nu + nu_star) + 1e-100)
+        DLx = D((nui_m[I, J] + nui_m[I - 1, J]) / 2.0)
+        DRx = D((nui_m[I, J] + nui_m[I + 1, J]) / 2.0)
+        DLr = D((nui_m[I, J] + nui_m[I, J - 1]) / 2.0)
+        DRr = D((nui_m[I, J] + nui_m[I, J + 1]) / 2.0)
+        bLx, bRx, bLr, bRr = m["bLx"][I, J], m["bRx"][I, J], m["bLr"][I, J], m["bRrw"][I, J]
+        bLrw = m["bLrw"][I, J]
+        utx = ULx / (um + 1e-100)
+        GLx = np.where(bLx, 0.0, -0.25 * vth * (np.exp(-utx * utx) + utx * sq * (_erf(utx) - 1.0)))
+        utx = URx / (um + 1e-100)
+        GRx = np.where(bRx, 0.0, 0.25 * vth * (np.exp(-utx * utx) + utx * sq * (_erf(utx) + 1.0)))
+        utr = ULr / (um + 1e-100)
+        GLr = np.where(bLrw, 0.0, -0.25 * vth * (np.exp(-utr * utr) + utr * sq * (_erf(utr) - 1.0)))
+        utr = URr / (um + 1e-100)
+        GRr = np.where(bRr, 0.0, 0.25 * vth * (np.exp(-utr * utr) + utr * sq * (_erf(utr) + 1.0)))
+        aP[I, J] = ((URx + np.abs(URx)) / (2.0 * dx) * bRx - (ULx - np.abs(ULx)) / (2.0 * dx) * bLx
+                    + qR * (URr + np.abs(URr)) / (2.0 * dr) * bRr - qL * (ULr - np.abs(ULr)) / (2.0 * dr) * bLr
+                    + ((DRx * bRx + DLx * bLx) / (dx * dx) + (qR * DRr * bRr + qL * DLr * bLr) / (dr * dr))
+                    - GLx / dx + GRx / dx - qL * GLr / dr + qR * GRr / dr + 1.0 / dt_i)
+        aE[I, J] = (-(URx - np.abs(URx)) / (2.0 * dx) + DRx / (dx * dx)) * bRx
+        aW[I, J] = ((ULx + np.abs(ULx)) / (2.0 * dx) + DLx / (dx * dx)) * bLx
+        aN[I, J] = (-qR * (URr - np.abs(URr)) / (2.0 * dr) + qR * DRr / (dr * dr)) * bRr
+        aS[I, J] = (qL * (ULr + np.abs(ULr)) / (2.0 * dr) + qL * DLr / (dr * dr)) * bLr
+        ro = rhoi_old
+        div = ((DRx * ro[I + 1, J] * bRx - (DRx * bRx + DLx * bLx) * ro[I, J] + DLx * ro[I - 1, J] * bLx) / (dx * dx)
+               + (qR * DRr * ro[I, J + 1] * bRr - (qR * DRr * bRr + qL * DLr * bLr) * ro[I, J]
+                  + qL * DLr * ro[I, J - 1] * bLr) / (dr * dr))
+        b[I, J] = ro[I, J] / dt_i + g["rate_ionize"][I, J] - div
+    for i, j in _pts(C["x5"]):
+        aP[i, j] = aP[i, j] - aN[i, j]
+        aN[i, j] = 0.0
+    x = solve_c(aP, aE, aW, aN, aS, b, geo["ib"], geo["jb"])
+    rhoi = g["rhoi"]
+    for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
+        rhoi[a0:a1 + 1, c0:c1 + 1] = x[a0:a1 + 1, c0:c1 + 1]
+
+    def gpn(u, sign):
+        ut = u / (um + 1e-100)
+        return sign * 0.25 * vth * (np.exp(-ut * ut) + ut * sq * (_erf(ut) + sign * 1.0))
+
+    for name in ("z0", "z1", "z2", "z4"):
+        for i, j in _pts(C[name]):
+            g["rhoUix_wall"][i, j] = rhoi[i, j] * gpn(Uix[i, j], -1.0)
+    for name in ("z3", "z5"):
+        for i, j in _pts(C[name]):
+            g["rhoUix_wall"][i + 1, j] = rhoi[i, j] * gpn(Uix[i + 1, j], 1.0)
+    for name in ("x0", "x2"):
+        for i, j in _pts(C[name]):
+            g["rhoUir_wall"][i, j] = rhoi[i, j] * gpn(Uir[i, j], -1.0)
+    for name in ("x1", "x4"):
+        for i, j in _pts(C[name]):
+            g["rhoUir_wall"][i, j + 1] = rhoi[i, j] * gpn(Uir[i, j + 1], 1.0)
+    for i, j in _pts(C["x5"]):
+        g["rhoUir"][i, j + 1] = rhoi[i, j] * Uir[i, j + 1]
+        g["rhoUir_wall"][i, j + 1] = 0.0
+    for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
+        sl = (slice(a0, a1 + 1), slice(c0, c1 + 1))
+        rhoi[sl] = np.where(rhoi[sl] < 0.0, np.fmax(rhoi_old[sl], 0.0), rhoi[sl])
+    for i, j in _pts(C["x5"]):
+        rhoi[i, j + 1] = rhoi[i, j]
+
+    # --- correct_Ui_constTe (:1763-2072) -------------------------------------
+    for (a0, a1), (c0, c1) in zip(geo["fxi"], geo["fxj"]):
+        I = np.arange(a0, a1 + 1)[:, None]
+        J = np.arange(c0, c1 + 1)[None, :]
+        D = BOLTZ * (Ti + Te_rep) / (massi * ((nui_m[I, J] + nui_m[I - 1, J]) / 2.0 + nu_star) + 1e-100)
+        rho_t = (rhoi[I, J] + rhoi[I - 1, J]) / 2.0
+        dndx_old = (rhoi_old[I, J] - rhoi_old[I - 1, J]) / dx
+        dndx = (rhoi[I, J] - rhoi[I - 1, J]) / dx
+        U = Uix[I, J]
+        flux = rhoi[I - 1, J] * (U + np.abs(U)) / 2.0 + rhoi[I, J] * (U - np.abs(U)) / 2.0
+        g["rhoUix"][I, J] = flux - D * (dndx - dndx_old)
+        Uix[I, J] = U - D / (rho_t + 1e-100) * (dndx - dndx_old)
+    for blk, ((a0, a1), (c0, c1)) in enumerate(zip(geo["fri"], geo["frj"])):
+        top = c1 + (1 if (blk == 4 or (len(geo["fri"]) == 1 and S["c"]["x5"] is not None)) else 0)
+        I = np.arange(a0, a1 + 1)[:, None]
+        J = np.arange(c0, top + 1)[None, :]
+        D = BOLTZ * (Ti + Te_rep) / (massi * ((nui_m[I, J] + nui_m[I, J - 1]) / 2.0 + nu_star) + 1e-100)
+        rho_t = (rhoi[I, J] + rhoi[I, J - 1]) / 2.0
+        dndr_old = (rhoi_old[I, J] - rhoi_old[I, J - 1]) / dr
+        dndr = (rhoi[I, J] - rhoi[I, J - 1]) / dr
+        U = Uir[I, J]
+        flux = rhoi[I, J - 1] * (U + np.abs(U)) / 2.0 + rhoi[I, J] * (U - np.abs(U)) / 2.0
+        g["rhoUir"][I, J] = flux - D * (dndr - dndr_old)
+        Uir[I, J] = U - D / (rho_t + 1e-100) * (dndr - dndr_old)
+    out = {k: g[k] for k in ("Uix", "Uir", "Uip", "rhoi", "rhoUix", "rhoUir", "rhoUix_wall", "rhoUir_wall")}
+    out.update(Uix_old=Uix_old, Uir_old=Uir_old, Uip_old=Uip_old, rhoi_old=rhoi_old)
+    out.update(ion_errors(out, prm, geo))
+    return out
+
+
+def ion_boxes(geo: dict) -> dict:
+    """Index boxes of the ion residuals of correct_Ui_constTe (fluidModule.hpp:1960-2070):
+    rhoi and Uip over the cell blocks, Uix over the x-face blocks extended by one
+    face in i, Uir over the r-face blocks without their first face in j."""
+    cells = [(a, b, c, e) for (a, b), (c, e) in zip(geo["ib"], geo["jb"])]
+    xs = [(a, b + 1, c, e) for (a, b), (c, e) in zip(geo["fxi"], geo["fxj"])]
+    rs = [(a, b, c + 1, e) for (a, b), (c, e) in zip(geo["fri"], geo["frj"])]
+    return dict(rhoi=cells, Uix=xs, Uir=rs, Uip=cells)
+
+
+def ion_errors(o: dict, prm: dict, geo: dict) -> dict:
+    """The ion residuals of correct_Ui_constTe (fluidModule.hpp:1960-2070)."""
+    bx = ion_boxes(geo)
+    CFL = prm["CFL"]
+    out = {}
+    for k, eps_l2 in (("rhoi", 1e10), ("Uix", 1e-6), ("Uir", 1e-6), ("Uip", 1e-6)):
+        nw = np.concatenate([o[k][a:b + 1, c:e + 1].ravel() for a, b, c, e in bx[k]])
+        od = np.concatenate([o[k + "_old"][a:b + 1, c:e + 1].ravel() for a, b, c, e in bx[k]])
+        if prm["flag_error"] == 0:
+            out["error_" + k] = float(np.abs((nw - od) / (nw + od + 1e-100) * 2.0 / CFL).max())
+        else:
+            out["error_" + k] = float(np.sqrt(np.sum((nw - od) ** 2 / (od ** 2 + eps_l2) / CFL) / nw.size))
+    return out

@@ -82,3 +82,22 @@ def test_transport_missing_table_is_an_error(pkg, cuda_device):
         fs.update_transport_coef(prm)
     fs.close()
     g.close()
+
+
+@pytest.mark.parametrize("adp", [0, 1])
+def test_check_cfl(pkg, cuda_device, adp):
+    from oracle import fluid
+    st = pkg.workloads.sg_state(64, 48, seed=9)
+    f = st["fields"]
+    g = pkg.Grid(64, 48, [[1, 64]], [[1, 48]])
+    fs = pkg.Fields(g)
+    for k in ("rhoe", "mu_para", "Te", "rhoUex", "rhoUer"):
+        fs.upload(k, f[k])
+    prm = dict(dt=1e-10, CFL=0.5, masse=pkg.workloads.MASSE, rmin=0.0, dr=5e-3 / 48, flag_adp_dt=adp)
+    got = fs.check_cfl(**prm)
+    ref = fluid.check_cfl(f, prm)
+    for k in ("rhoe_max", "mu_max", "Te_max", "dt_min", "dt", "CFL"):
+        assert got[k] == pytest.approx(ref[k], rel=1e-14), k
+    assert got["ue_max"] == pytest.approx(ref["ue_max"], rel=1e-13)
+    fs.close()
+    g.close()
