@@ -34,7 +34,7 @@ EXPORTS = (
     "cth_fields_create", "cth_fields_destroy", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
     "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
-    "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step",
+    "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -112,6 +112,18 @@ class IonOp(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int) for k in ION_OP_FIELDS]
 
 
+class NeutralParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("dt", "dx", "dr", "rmin", "fn_In", "Tn", "ri", "massi", "DmN",
+                                               "error_cnv_SOR")] + \
+               [(k, ctypes.c_int) for k in ("ndt_n", "ndt_m", "maxITR_SOR", "flag_iter", "precision", "flag_error",
+                                            "n_pos_box")] + [("pos_box", (ctypes.c_int * 4) * 8)]
+
+
+class NeutralResult(ctypes.Structure):
+    _fields_ = [("error_rhon", ctypes.c_double), ("error_rhom", ctypes.c_double), ("solver_rc", ctypes.c_int),
+                ("reserved", ctypes.c_int), ("solver", Status * 2)]
+
+
 class CathodeError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"cathode_b200 error {code}: {msg}")
@@ -174,6 +186,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_ion_boxes_upload.restype = ctypes.c_int
     L.cth_ion_step.argtypes = [_vp, _vp, _vp, ctypes.POINTER(IonParams), _vp, ctypes.POINTER(IonResult)]
     L.cth_ion_step.restype = ctypes.c_int
+    L.cth_update_neutrals.argtypes = [_vp, ctypes.POINTER(NeutralParams), _vp, ctypes.POINTER(NeutralResult)]
+    L.cth_update_neutrals.restype = ctypes.c_int
     L.cth_check_cfl.argtypes = [_vp, ctypes.POINTER(CFL), _vp]
     L.cth_check_cfl.restype = ctypes.c_int
     L.cth_ghost_rules_upload.argtypes = [_vp, _vp, ctypes.c_int]

@@ -35,7 +35,8 @@ struct cth_fields {
 namespace cth {
 
 // side flags of a cell (1 = ordinary interior face on that side)
-enum { F_BLX = 1, F_BRX = 2, F_BLR_WALL = 4, F_BLR_CEN = 8, F_BRR_WALL = 16, F_BRR_OPEN = 32, F_BRX_BIAS = 64 };
+enum { F_BLX = 1, F_BRX = 2, F_BLR_WALL = 4, F_BLR_CEN = 8, F_BRR_WALL = 16, F_BRR_OPEN = 32, F_BRX_BIAS = 64,
+       F_BRR_INLET = 128 };
 
 // flag of cell (i, j); 0 outside the (ni+2) x (nj+2) index space
 __device__ __forceinline__ unsigned flag_at(const unsigned char* __restrict__ f, int i, int j, int ni, int nj,

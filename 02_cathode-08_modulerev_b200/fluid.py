@@ -17,6 +17,7 @@ from . import capi
 
 F_BLX, F_BRX, F_BLR_WALL, F_BLR_CEN, F_BRR_WALL, F_BRR_OPEN = 1, 2, 4, 8, 16, 32
 F_BRX_BIAS = 64  # the right wall of the cell is the biased electrode
+F_BRR_INLET = 128  # the upper wall of the cell is the neutral gas inlet
 TABLES = ("nu_elas_N", "nu_exc_N", "nu_excReso_N", "nu_excMeta_N", "nu_ionz_N", "nu_ionzStep_N",
           "nu_excStep_N", "nu_super_N", "rate_eloss_n_N", "rate_eloss_m_N", "nui_m_N")
 
@@ -147,6 +148,20 @@ class Fields:
         return dict(error_rhoi=res.error_rhoi, error_Uix=res.error_Uix, error_Uir=res.error_Uir,
                     error_Uip=res.error_Uip, solver_rc=res.solver_rc, solver=[res.solver[k].as_dict() for k in range(4)])
 
+    def update_neutrals(self, prm: dict, pos_boxes, stream=None) -> dict:
+        """FluidModule::update_rhon then update_rhom on the device (fluidModule.hpp:4963-5792)."""
+        p = capi.NeutralParams(**{k: prm[k] for k, _ in capi.NeutralParams._fields_
+                                  if k not in ("n_pos_box", "pos_box")})
+        p.n_pos_box = len(pos_boxes)
+        for q, bx in enumerate(pos_boxes):
+            for k in range(4):
+                p.pos_box[q][k] = int(bx[k])
+        res = capi.NeutralResult()
+        s = 0 if stream is None else stream.cuda_stream
+        capi.check(self._L.cth_update_neutrals(self._h, ctypes.byref(p), s, ctypes.byref(res)), allow_positive=False)
+        return dict(error_rhon=res.error_rhon, error_rhom=res.error_rhom, solver_rc=res.solver_rc,
+                    solver=[res.solver[k].as_dict() for k in range(2)])
+
     def check_cfl(self, dt: float, CFL: float, masse: float, rmin: float, dr: float, flag_adp_dt: int = 0,
                   stream=None) -> dict:
         """FluidModule::check_CFL (fluidModule.hpp:57-115); returns dt, CFL and the maxima."""
@@ -188,7 +203,7 @@ class Fields:
 # geometries: cell / face blocks, wall segments, ghost rules, ion wall programs
 # ---------------------------------------------------------------------------
 
-def cathode_geometry(ni=194, nj=70, xR=0.0388, rmax=0.014) -> dict:
+def cathode_geometry(ni=194, nj=70, xR=0.0388, rmax=0.014, width_neutIn=0.0055) -> dict:
     """The cathode's fluid blocks with their x-face and r-face blocks
     (initialModule.hpp:219-345), side flags, ghost rules of the electron sweeps
     (fluidModule.hpp:3884-3921, :4878-4914) and the named wall segments of the ion
@@ -222,22 +237,37 @@ def cathode_geometry(ni=194, nj=70, xR=0.0388, rmax=0.014) -> dict:
     ghosts = [(ib[0][0], ib[0][0], jb[0][0], jb[0][1], -1, 0, 0), (ib[1][0], ib[1][0], jb[1][0], jb[0][0] - 1, -1, 0, 0),
               (ib[0][0], ib[0][1], jb[0][0], jb[0][0], 0, -1, 0), (ib[1][1], ib[1][1], jb[1][0], jb[1][1], 1, 0, 1),
               (ib[0][0], ib[1][1], jb[0][1], jb[0][1], 0, 1, 1)]
-    return dict(ni=ni, nj=nj, dx=dx, dr=dr, ib=ib, jb=jb, fxi=fxi, fxj=fxj, fri=fri, frj=frj,
-                flags=cathode_flags(ni, nj, ib, jb), ghosts=[tuple(int(v) for v in g) for g in ghosts],
-                seg=dict(c=segs(ib, jb, False), x=segs(fxi, fxj, False), r=segs(fri, frj, True)))
+    seg = dict(c=segs(ib, jb, False), x=segs(fxi, fxj, False), r=segs(fri, frj, True))
+    flags = cathode_flags(ni, nj, ib, jb)
+    # neutral inlet: the cells of the x1 wall with x_i <= width_neutIn + x6 (fluidModule.hpp:5040-5041)
+    i0, i1, j0, _ = seg["c"]["x1"]
+    for i in range(i0, i1 + 1):
+        if 0.0 + (i - 0.5) * dx <= width_neutIn + x6:
+            flags[i, j0] |= F_BRR_INLET
+    return dict(ni=ni, nj=nj, dx=dx, dr=dr, ib=ib, jb=jb, fxi=fxi, fxj=fxj, fri=fri, frj=frj, flags=flags,
+                ghosts=[tuple(int(v) for v in g) for g in ghosts], seg=seg, x6=x6, xL=0.0,
+                width_neutIn=width_neutIn, pos_boxes=[tuple(int(v) for v in (ib[b][0], ib[b][1], jb[b][0], jb[b][1]))
+                                                      for b in range(2)])
 
 
-def rectangle_geometry(ni, nj, Lz=10e-3, Lr=5e-3) -> dict:
+def rectangle_geometry(ni, nj, Lz=10e-3, Lr=5e-3, width_neutIn=0.0) -> dict:
     """The r-z rectangle as one fluid block: z = 0 grounded wall (the reference's
-    z0), z = L the biased electrode (z5), r = R a grounded wall (x1), r = 0 the axis."""
+    z0), z = L the biased electrode (z5), r = R a grounded wall (x1) with the neutral
+    inlet over z <= width_neutIn, r = 0 the axis."""
     one = lambda a, b: np.array([[a, b]], np.int32)
     empty = dict(z1=None, z2=None, z3=None, z4=None, x0=None, x2=None, x4=None, x5=None)
     seg = dict(c=dict(empty, z0=(1, 1, 1, nj), z5=(ni, ni, 1, nj), x1=(1, ni, nj, nj), x6=None),
                x=dict(empty, z0=(2, 2, 1, nj), z5=(ni, ni, 1, nj), x1=(2, ni, nj, nj), x6=None),
                r=dict(empty, z0=(1, 1, 2, nj), z5=(ni, ni, 2, nj), x1=(1, ni, nj, nj), x6=(1, ni, 2, 2)))
     ghosts = [(1, 1, 1, nj, -1, 0, 0), (ni, ni, 1, nj, 1, 0, 1), (1, ni, nj, nj, 0, 1, 1)]
-    return dict(ni=ni, nj=nj, dx=Lz / ni, dr=Lr / nj, ib=one(1, ni), jb=one(1, nj), fxi=one(2, ni), fxj=one(1, nj),
-                fri=one(1, ni), frj=one(2, nj), flags=rectangle_flags(ni, nj), ghosts=ghosts, seg=seg)
+    flags = rectangle_flags(ni, nj)
+    dx = Lz / ni
+    for i in range(1, ni + 1):
+        if 0.0 + (i - 0.5) * dx <= width_neutIn:
+            flags[i, nj] |= F_BRR_INLET
+    return dict(ni=ni, nj=nj, dx=dx, dr=Lr / nj, ib=one(1, ni), jb=one(1, nj), fxi=one(2, ni), fxj=one(1, nj),
+                fri=one(1, ni), frj=one(2, nj), flags=flags, ghosts=ghosts, seg=seg, x6=0.0, xL=0.0,
+                width_neutIn=width_neutIn, pos_boxes=[(1, ni, 1, nj)])
 
 
 _K = dict(WALL_FOLD=1, ZERO_COEF=2, FOLD_SUB=3, OPEN_FOLD=4, SET_WALL=5, SET_ZERO=6, COPY=7, SET_OPEN=8)

@@ -304,3 +304,31 @@ def ion_state(ni: int, nj: int, seed: int = 7, Lz: float = 10e-3, Lr: float = 5e
                Te_rep_eV=0.1, CFL=1.0, error_cnv_SOR=1e-10, ndt_i=1, maxITR_SOR=30, flag_iter=1, precision=1,
                flag_error=3)
     return dict(fields=f, prm=prm)
+
+
+def neutral_state(ni: int, nj: int, seed: int = 8, Lz: float = 10e-3, Lr: float = 5e-3) -> dict:
+    """Seeded state of the neutral sweeps: rhon = 1e21 (1 + 0.1 U(0,1)) m^-3, rhom =
+    1e17 lognormal(0, 0.2), face fluxes N(0, 1e19), ion and metastable wall fluxes
+    N(0, 1e18), rhoe = 1e17 lognormal(0, 0.3), collision frequencies log-uniform in
+    [1e5, 1e7] s^-1.  Parameters: Tn 300 K, Xe radius 216 pm, DmN 5.2e19 (input/setup.yaml),
+    the inlet flux of 0.069 mg/s through 2 pi r4 x 5.5 mm (initialModule.hpp:234-237),
+    the inner solve of the potential (SMG, 30 iterations, 1e-10), dt 1e-10 s."""
+    rng = np.random.default_rng(seed)
+    sh = (ni + 2, nj + 2)
+    f = {}
+    f["rhon"] = 1e21 * (1.0 + 0.1 * rng.random(sh))
+    f["rhom"] = 1e17 * np.exp(0.2 * rng.standard_normal(sh))
+    for k in ("rhoUnx", "rhoUnr", "rhoUmx", "rhoUmr"):
+        f[k] = 1e19 * rng.standard_normal(sh)
+    for k in ("rhoUix_wall", "rhoUir_wall", "rhoUmx_wall", "rhoUmr_wall"):
+        f[k] = 1e18 * rng.standard_normal(sh)
+    for k in ("rhoUnx_wall", "rhoUnr_wall"):
+        f[k] = np.zeros(sh)
+    f["rhoe"] = 1e17 * np.exp(0.3 * rng.standard_normal(sh))
+    for k in ("nu_excStep", "nu_super", "nu_excMeta", "nu_exc", "nu_ionz", "nu_ionzStep"):
+        f[k] = 10.0 ** rng.uniform(5.0, 7.0, sh)
+    fn_In = 0.069e-6 / MASSI_XE / (2.0 * np.pi * 9.0e-3 * 5.5e-3)
+    prm = dict(dt=1e-10, dx=Lz / ni, dr=Lr / nj, rmin=0.0, fn_In=fn_In, Tn=300.0, ri=216.0e-12, massi=MASSI_XE,
+               DmN=5.2e19, error_cnv_SOR=1e-10, ndt_n=1, ndt_m=1, maxITR_SOR=30, flag_iter=1, precision=1,
+               flag_error=3)
+    return dict(fields=f, prm=prm)

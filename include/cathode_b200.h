@@ -200,6 +200,7 @@ int cth_mw_er_assemble_dev(cth_grid* g, const double* ne, const double* nu, cons
 #define CTH_F_BRR_WALL 16
 #define CTH_F_BRR_OPEN 32
 #define CTH_F_BRX_BIAS 64 /* the right wall is the biased electrode (z5, fluidModule.hpp:2196-2199) */
+#define CTH_F_BRR_INLET 128 /* the upper wall is the neutral gas inlet (fluidModule.hpp:5040-5041) */
 typedef struct cth_fields cth_fields;
 int cth_fields_create(cth_grid* g, cth_fields** out);
 void cth_fields_destroy(cth_fields* fs);
@@ -345,6 +346,27 @@ int cth_ion_program_upload(cth_fields* fs, int which, const cth_ion_op* ops, int
 int cth_ion_boxes_upload(cth_fields* fs, int which, const int* boxes, int n);
 int cth_ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_params* prm, void* stream,
                  cth_ion_result* res);
+
+/* Neutrals: FluidModule::update_rhon (fluidModule.hpp:4963-5410) then update_rhom
+ * (:5416-5792).  Reads rhoUix_wall, rhoUir_wall, rhoe and the collision
+ * frequencies nu_excStep, nu_super, nu_excMeta, nu_exc, nu_ionz, nu_ionzStep;
+ * updates rhon, rhom, their face fluxes rhoUnx, rhoUnr, rhoUmx, rhoUmr, the wall
+ * fluxes *_wall and the *_old copies.  Cells flagged CTH_F_BRR_INLET take the
+ * inlet flux fn_In through their upper face.  rhom is kept non-negative on the
+ * pos_box boxes (the reference: fluid blocks 0 and 1). */
+typedef struct cth_neutral_params {
+    double dt, dx, dr, rmin, fn_In, Tn, ri, massi, DmN, error_cnv_SOR;
+    int ndt_n, ndt_m, maxITR_SOR, flag_iter, precision, flag_error;
+    int n_pos_box;
+    int pos_box[8][4];  /* i0, i1, j0, j1 */
+} cth_neutral_params;
+typedef struct cth_neutral_result {
+    double error_rhon, error_rhom;
+    int solver_rc;
+    int reserved;
+    cth_status solver[2];
+} cth_neutral_result;
+int cth_update_neutrals(cth_fields* fs, const cth_neutral_params* prm, void* stream, cth_neutral_result* res);
 
 /* Residual (device arrays): r = b - A x on grid cells (couplings to non-grid
  * cells dropped), r = 0 elsewhere; *rnorm = ||r||_2, *bnorm = ||b||_2 over grid

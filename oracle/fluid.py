@@ -1209,3 +1209,206 @@ def ion_errors(o: dict, prm: dict, geo: dict) -> dict:
         else:
             out["error_" + k] = float(np.sqrt(np.sum((nw - od) ** 2 / (od ** 2 + eps_l2) / CFL) / nw.size))
     return out
+
+
+# ----------------------------------------------------------------------------
+# neutrals: ground-state (rhon) and metastable (rhom) diffusion
+# ----------------------------------------------------------------------------
+
+def _neutral_masks(geo, prm, i, j, blk):
+    """Side flags of update_rhon / update_rhom for cell (i, j) of block blk
+    (fluidModule.hpp:5021-5041, :5478-5501); the x1 wall of blocks 0-2 has a
+    neutral inlet where x_i <= width_neutIn + x6."""
+    fl = int(geo["flags"][i, j])
+    x = prm["xL"] + (i - 0.5) * prm["dx"]
+    inlet = (fl & F_BRR_WALL) == 0 and geo["seg_x1"] is not None and \
+        geo["seg_x1"][0] <= i <= geo["seg_x1"][1] and j == geo["seg_x1"][2] and x <= prm["width_neutIn"] + prm["x6"]
+    return dict(bLx=float((fl & F_BLX) != 0), bRx=float((fl & F_BRX) != 0), bLrw=float((fl & F_BLR_WALL) != 0),
+                bLr=float((fl & F_BLR_WALL) != 0 and (fl & F_BLR_CEN) != 0),
+                bRrw=float((fl & F_BRR_WALL) != 0), bRro=float((fl & F_BRR_OPEN) != 0), inlet=inlet)
+
+
+def update_neutrals(st: dict, prm: dict, geo: dict, solve) -> dict:
+    """FluidModule::update_rhon (fluidModule.hpp:4963-5410) then update_rhom
+    (:5416-5792).  st: rhon, rhom, rhoUnx, rhoUnr, rhoUnx_wall, rhoUnr_wall, rhoUmx,
+    rhoUmr, rhoUmx_wall, rhoUmr_wall, rhoUix_wall, rhoUir_wall, rhoe, nu_excStep,
+    nu_super, nu_excMeta, nu_exc, nu_ionz, nu_ionzStep.  prm: dt, ndt_n, ndt_m, dx,
+    dr, rmin, xL, x6, width_neutIn, fn_In, Tn, ri, massi, DmN, flag_error.  The
+    cell loops follow the blocks; the walls follow the named segments of the
+    reference (z0..z5, x0..x5)."""
+    ni, nj = geo["ni"], geo["nj"]
+    dx, dr = prm["dx"], prm["dr"]
+    r = prm["rmin"] + (np.arange(nj + 2) - 0.5) * dr
+    C = ion_segments(geo)["c"]
+    geo = dict(geo, seg_x1=C["x1"])
+    g = {k: v.copy() for k, v in st.items()}
+    sh = (ni + 2, nj + 2)
+    nb = len(geo["ib"])
+
+    # --- update_rhon -----------------------------------------------------------
+    dt_n = prm["dt"] * float(prm["ndt_n"])
+    sigma = np.pi * (2.0 * prm["ri"]) * (2.0 * prm["ri"])
+    DnN = 2.0 / (3.0 * sigma) * np.sqrt(BOLTZ * prm["Tn"] / (np.pi * prm["massi"]))
+    rhon_old, Unx_old, Unr_old = g["rhon"].copy(), g["rhoUnx"].copy(), g["rhoUnr"].copy()
+    aP, aE, aW, aN, aS, b = (np.zeros(sh) for _ in range(6))
+    for blk in range(nb):
+        for i in range(geo["ib"][blk][0], geo["ib"][blk][1] + 1):
+            for j in range(geo["jb"][blk][0], geo["jb"][blk][1] + 1):
+                rL = (r[j] + r[j - 1]) / 2.0
+                rR = (r[j] + r[j + 1]) / 2.0
+                qL = (r[j] + r[j - 1]) / 2.0 / r[j]
+                qR = (r[j] + r[j + 1]) / 2.0 / r[j]
+                DLx = DnN / ((rhon_old[i, j] + rhon_old[i - 1, j]) / 2.0 + 1e-100)
+                DRx = DnN / ((rhon_old[i, j] + rhon_old[i + 1, j]) / 2.0 + 1e-100)
+                DLr = DnN / ((rhon_old[i, j] + rhon_old[i, j - 1]) / 2.0 + 1e-100)
+                DRr = DnN / ((rhon_old[i, j] + rhon_old[i, j + 1]) / 2.0 + 1e-100)
+                m = _neutral_masks(geo, prm, i, j, blk)
+                bRr_wall = 1.0 if m["inlet"] else m["bRrw"]
+                bRr_in = 0.0 if m["inlet"] else 1.0
+                bRr = bRr_wall * bRr_in * m["bRro"]
+                GLx = -g["rhoUix_wall"][i, j] - g["rhoUmx_wall"][i, j] if m["bLx"] == 0 else 0.0
+                GRx = -g["rhoUix_wall"][i + 1, j] - g["rhoUmx_wall"][i + 1, j] if m["bRx"] == 0 else 0.0
+                GLr = -g["rhoUir_wall"][i, j] - g["rhoUmr_wall"][i, j] if m["bLrw"] == 0 else 0.0
+                GRr = -g["rhoUir_wall"][i, j + 1] - g["rhoUmr_wall"][i, j + 1] if bRr_wall == 0 else 0.0
+                Gin = (-g["rhoUir_wall"][i, j + 1] - g["rhoUmr_wall"][i, j + 1] - prm["fn_In"]) if bRr_in == 0 else 0.0
+                Gop = max(rL / rR * Unr_old[i, j], 0.0) if m["bRro"] == 0 else 0.0
+                bLx, bRx, bLr = m["bLx"], m["bRx"], m["bLr"]
+                aP[i, j] = ((DRx * bRx + DLx * bLx) * dr * dr + (qR * DRr * bRr + qL * DLr * bLr) * dx * dx
+                            + dx * dx * dr * dr / dt_n)
+                aE[i, j] = DRx * dr * dr * bRx
+                aW[i, j] = DLx * dr * dr * bLx
+                aN[i, j] = qR * DRr * dx * dx * bRr
+                aS[i, j] = qL * DLr * dx * dx * bLr
+                G = (g["nu_excStep"][i, j] + g["nu_super"][i, j]) * g["rhoe"][i, j]
+                L = (g["nu_excMeta"][i, j] + 0.5 * g["nu_exc"][i, j] + g["nu_ionz"][i, j]) * g["rhoe"][i, j]
+                b[i, j] = (rhon_old[i, j] / dt_n * dx * dx * dr * dr + (G - L) * dx * dx * dr * dr
+                           + (GLx) * dr * dx * dr - (GRx) * dr * dx * dr + qL * (GLr) * dx * dx * dr
+                           - qR * (GRr + Gop + Gin) * dx * dx * dr)
+    x = solve(aP, aE, aW, aN, aS, b, geo["ib"], geo["jb"])
+    rhon = g["rhon"]
+    for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
+        rhon[a0:a1 + 1, c0:c1 + 1] = x[a0:a1 + 1, c0:c1 + 1]
+    for (a0, a1), (c0, c1) in zip(geo["fxi"], geo["fxj"]):
+        I, J, Im = slice(a0, a1 + 1), slice(c0, c1 + 1), slice(a0 - 1, a1)
+        D = DnN / ((rhon_old[I, J] + rhon_old[Im, J]) / 2.0 + 1e-100)
+        g["rhoUnx"][I, J] = -D * (rhon[I, J] - rhon[Im, J]) / dx
+    for (a0, a1), (c0, c1) in zip(geo["fri"], geo["frj"]):
+        I, J, Jm = slice(a0, a1 + 1), slice(c0, c1 + 1), slice(c0 - 1, c1)
+        D = DnN / ((rhon_old[I, J] + rhon_old[I, Jm]) / 2.0 + 1e-100)
+        g["rhoUnr"][I, J] = -D * (rhon[I, J] - rhon[I, Jm]) / dr
+    for name in ("z0", "z1", "z2", "z4"):
+        for i, j in _pts(C[name]):
+            v = -g["rhoUix_wall"][i, j] - g["rhoUmx_wall"][i, j]
+            g["rhoUnx"][i, j] = v
+            g["rhoUnx_wall"][i, j] = v
+    for name in ("z3", "z5"):
+        for i, j in _pts(C[name]):
+            v = -g["rhoUix_wall"][i + 1, j] - g["rhoUmx_wall"][i + 1, j]
+            g["rhoUnx"][i + 1, j] = v
+            g["rhoUnx_wall"][i + 1, j] = v
+    for name in ("x0", "x2"):
+        for i, j in _pts(C[name]):
+            v = -g["rhoUir_wall"][i, j] - g["rhoUmr_wall"][i, j]
+            g["rhoUnr"][i, j] = v
+            g["rhoUnr_wall"][i, j] = v
+    for i, j in _pts(C["x1"]):
+        x = prm["xL"] + (i - 0.5) * dx
+        if x < prm["width_neutIn"] + prm["x6"]:
+            g["rhoUnr"][i, j + 1] = -g["rhoUir_wall"][i, j + 1] - g["rhoUmr_wall"][i, j + 1] - prm["fn_In"]
+        else:
+            v = -g["rhoUir_wall"][i, j + 1] - g["rhoUmr_wall"][i, j + 1]
+            g["rhoUnr"][i, j + 1] = v
+            g["rhoUnr_wall"][i, j + 1] = v
+    for i, j in _pts(C["x4"]):
+        v = -g["rhoUir_wall"][i, j + 1] - g["rhoUmr_wall"][i, j + 1]
+        g["rhoUnr"][i, j + 1] = v
+        g["rhoUnr_wall"][i, j + 1] = v
+    for i, j in _pts(C["x5"]):
+        rL = (r[j] + r[j - 1]) / 2.0
+        rR = (r[j] + r[j + 1]) / 2.0
+        g["rhoUnr"][i, j + 1] = max(rL / rR * Unr_old[i, j], 0.0)
+        g["rhoUnr_wall"][i, j + 1] = 0.0
+    for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
+        sl = (slice(a0, a1 + 1), slice(c0, c1 + 1))
+        rhon[sl] = np.where(rhon[sl] < 0.0, np.fmax(rhon_old[sl], 0.0), rhon[sl])
+    fe = prm["flag_error"]
+    err_n = calc_res(rhon, rhon_old, geo["ib"], geo["jb"], 1e-100, fe)
+
+    # --- update_rhom -----------------------------------------------------------
+    dt_m = prm["dt"] * float(prm["ndt_m"])
+    vth = np.sqrt(8.0 * BOLTZ * prm["Tn"] / (np.pi * prm["massi"]))
+    rhom_old, Umr_old = g["rhom"].copy(), g["rhoUmr"].copy()
+    DmN = prm["DmN"]
+    aP, aE, aW, aN, aS, b = (np.zeros(sh) for _ in range(6))
+    for blk in range(nb):
+        for i in range(geo["ib"][blk][0], geo["ib"][blk][1] + 1):
+            for j in range(geo["jb"][blk][0], geo["jb"][blk][1] + 1):
+                rL = (r[j] + r[j - 1]) / 2.0
+                rR = (r[j] + r[j + 1]) / 2.0
+                qL = (r[j] + r[j - 1]) / 2.0 / r[j]
+                qR = (r[j] + r[j + 1]) / 2.0 / r[j]
+                DLx = DmN / ((rhon[i, j] + rhon[i - 1, j]) / 2.0 + 1e-100)
+                DRx = DmN / ((rhon[i, j] + rhon[i + 1, j]) / 2.0 + 1e-100)
+                DLr = DmN / ((rhon[i, j] + rhon[i, j - 1]) / 2.0 + 1e-100)
+                DRr = DmN / ((rhon[i, j] + rhon[i, j + 1]) / 2.0 + 1e-100)
+                m = _neutral_masks(geo, prm, i, j, blk)
+                bLx, bRx, bLr = m["bLx"], m["bRx"], m["bLr"]
+                bRr = m["bRrw"] * m["bRro"]
+                GLx = -0.25 * vth if m["bLx"] == 0 else 0.0
+                GRx = 0.25 * vth if m["bRx"] == 0 else 0.0
+                GLr = -0.25 * vth if m["bLrw"] == 0 else 0.0
+                GRr = 0.25 * vth if m["bRrw"] == 0 else 0.0
+                Gop = rL / rR * Umr_old[i, j] if m["bRro"] == 0 else 0.0
+                aP[i, j] = ((DRx * bRx + DLx * bLx) * dr * dr + (qR * DRr * bRr + qL * DLr * bLr) * dx * dx
+                            - GLx * dr * dx * dr + GRx * dr * dx * dr - qL * GLr * dx * dx * dr
+                            + qR * GRr * dx * dx * dr + dx * dx * dr * dr / dt_m)
+                aE[i, j] = DRx * dr * dr * bRx
+                aW[i, j] = DLx * dr * dr * bLx
+                aN[i, j] = qR * DRr * dx * dx * bRr
+                aS[i, j] = qL * DLr * dx * dx * bLr
+                G = g["rhoe"][i, j] * (g["nu_excMeta"][i, j] + 0.5 * g["nu_exc"][i, j])
+                L = g["rhoe"][i, j] * (g["nu_ionzStep"][i, j] + g["nu_excStep"][i, j] + g["nu_super"][i, j])
+                b[i, j] = (rhom_old[i, j] / dt_m * dx * dx * dr * dr + (G - L) * dx * dx * dr * dr
+                           + (0.0) * dr * dx * dr - (0.0) * dr * dx * dr + qL * (0.0) * dx * dx * dr
+                           - qR * (Gop) * dx * dx * dr)
+    x = solve(aP, aE, aW, aN, aS, b, geo["ib"], geo["jb"])
+    rhom = g["rhom"]
+    for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
+        rhom[a0:a1 + 1, c0:c1 + 1] = x[a0:a1 + 1, c0:c1 + 1]
+    for (a0, a1), (c0, c1) in list(zip(geo["ib"], geo["jb"]))[:2]:
+        sl = (slice(a0, a1 + 1), slice(c0, c1 + 1))
+        rhom[sl] = np.where(rhom[sl] < 0.0, np.fmax(rhom_old[sl], 0.0), rhom[sl])
+    for (a0, a1), (c0, c1) in zip(geo["fxi"], geo["fxj"]):
+        I, J, Im = slice(a0, a1 + 1), slice(c0, c1 + 1), slice(a0 - 1, a1)
+        D = DmN / ((rhon[I, J] + rhon[Im, J]) / 2.0 + 1e-100)
+        g["rhoUmx"][I, J] = -D * (rhom[I, J] - rhom[Im, J]) / dx
+    for (a0, a1), (c0, c1) in zip(geo["fri"], geo["frj"]):
+        I, J, Jm = slice(a0, a1 + 1), slice(c0, c1 + 1), slice(c0 - 1, c1)
+        D = DmN / ((rhon[I, J] + rhon[I, Jm]) / 2.0 + 1e-100)
+        g["rhoUmr"][I, J] = -D * (rhom[I, J] - rhom[I, Jm]) / dr
+    for name in ("z0", "z1", "z2", "z4"):
+        for i, j in _pts(C[name]):
+            g["rhoUmx"][i, j] = -0.25 * rhom[i, j] * vth
+            g["rhoUmx_wall"][i, j] = g["rhoUmx"][i, j]
+    for name in ("z3", "z5"):
+        for i, j in _pts(C[name]):
+            g["rhoUmx"][i + 1, j] = 0.25 * rhom[i, j] * vth
+            g["rhoUmx_wall"][i + 1, j] = g["rhoUmx"][i + 1, j]
+    for name in ("x0", "x2"):
+        for i, j in _pts(C[name]):
+            g["rhoUmr"][i, j] = -0.25 * rhom[i, j] * vth
+            g["rhoUmr_wall"][i, j] = g["rhoUmr"][i, j]
+    for name in ("x1", "x4"):
+        for i, j in _pts(C[name]):
+            g["rhoUmr"][i, j + 1] = 0.25 * rhom[i, j] * vth
+            g["rhoUmr_wall"][i, j + 1] = g["rhoUmr"][i, j + 1]
+    for i, j in _pts(C["x5"]):
+        rL = (r[j] + r[j - 1]) / 2.0
+        rR = (r[j] + r[j + 1]) / 2.0
+        g["rhoUmr"][i, j + 1] = Umr_old[i, j] * rL / rR
+        g["rhoUmr_wall"][i, j + 1] = 0.0
+    err_m = calc_res(rhom, rhom_old, geo["ib"], geo["jb"], 1e-100, fe)
+    out = {k: g[k] for k in ("rhon", "rhom", "rhoUnx", "rhoUnr", "rhoUnx_wall", "rhoUnr_wall", "rhoUmx", "rhoUmr",
+                             "rhoUmx_wall", "rhoUmr_wall")}
+    out.update(rhon_old=rhon_old, rhom_old=rhom_old, error_rhon=err_n, error_rhom=err_m)
+    return out
