@@ -34,7 +34,7 @@ EXPORTS = (
     "cth_fields_create", "cth_fields_destroy", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
     "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
-    "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals",
+    "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -116,12 +116,26 @@ class NeutralParams(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("dt", "dx", "dr", "rmin", "fn_In", "Tn", "ri", "massi", "DmN",
                                                "error_cnv_SOR")] + \
                [(k, ctypes.c_int) for k in ("ndt_n", "ndt_m", "maxITR_SOR", "flag_iter", "precision", "flag_error",
-                                            "n_pos_box")] + [("pos_box", (ctypes.c_int * 4) * 8)]
+                                            "n_pos_box")] + [("pos_box", (ctypes.c_int * 4) * 8),
+                                                             ("do_rhon", ctypes.c_int), ("do_rhom", ctypes.c_int)]
 
 
 class NeutralResult(ctypes.Structure):
     _fields_ = [("error_rhon", ctypes.c_double), ("error_rhom", ctypes.c_double), ("solver_rc", ctypes.c_int),
                 ("reserved", ctypes.c_int), ("solver", Status * 2)]
+
+
+class StepParams(ctypes.Structure):
+    _fields_ = [("itime", ctypes.c_int), ("ndt_i", ctypes.c_int), ("ndt_n", ctypes.c_int), ("ndt_m", ctypes.c_int),
+                ("flag_adp_dt", ctypes.c_int), ("dt", ctypes.c_double), ("CFL", ctypes.c_double),
+                ("gtime", ctypes.c_double), ("ion", IonParams), ("phi", PhiParams), ("rhoe", SGParams),
+                ("eps", SGParams), ("neutral", NeutralParams), ("transport", TransportParams)]
+
+
+class StepResult(ctypes.Structure):
+    _fields_ = [("ion", IonResult), ("phi", PCResult), ("rhoe", PCResult), ("eps", PCResult),
+                ("neutral", NeutralResult), ("cfl", CFL), ("ran_ion", ctypes.c_int), ("ran_rhon", ctypes.c_int),
+                ("ran_rhom", ctypes.c_int), ("solver_rc", ctypes.c_int)]
 
 
 class CathodeError(RuntimeError):
@@ -188,6 +202,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_ion_step.restype = ctypes.c_int
     L.cth_update_neutrals.argtypes = [_vp, ctypes.POINTER(NeutralParams), _vp, ctypes.POINTER(NeutralResult)]
     L.cth_update_neutrals.restype = ctypes.c_int
+    L.cth_fluid_step.argtypes = [_vp, _vp, _vp, ctypes.POINTER(StepParams), _vp, ctypes.POINTER(StepResult)]
+    L.cth_fluid_step.restype = ctypes.c_int
     L.cth_check_cfl.argtypes = [_vp, ctypes.POINTER(CFL), _vp]
     L.cth_check_cfl.restype = ctypes.c_int
     L.cth_ghost_rules_upload.argtypes = [_vp, _vp, ctypes.c_int]

@@ -308,21 +308,27 @@ static int update_neutrals(cth_fields* fs, const cth_neutral_params* prm, cudaSt
         return rc;
     };
     double* out = fs->scal + 56;
-    k_neut_begin<0><<<grd, blk, 0, s>>>(A);
-    k_rhon_assemble<<<grd, blk, 0, s>>>(A);
-    g->launches += 2;
-    CTH_CUDA(cudaGetLastError());
-    if (solve(A.rhon, 0) < 0) return CTH_ERR_CUDA;
-    k_rhon_fluxes<<<grd, blk, 0, s>>>(A);
-    k_rhon_fix<<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out);
-    k_neut_begin<1><<<grd, blk, 0, s>>>(A);
-    k_rhom_assemble<<<grd, blk, 0, s>>>(A);
-    g->launches += 4;
-    CTH_CUDA(cudaGetLastError());
-    if (solve(A.rhom, 1) < 0) return CTH_ERR_CUDA;
-    k_rhom_fix<<<grd, blk, 0, s>>>(A);
-    k_rhom_fluxes<<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out + 2);
-    g->launches += 2;
+    CTH_CUDA(cudaMemsetAsync(out, 0, 4 * sizeof(double), s));
+    if (prm->do_rhon) {
+        k_neut_begin<0><<<grd, blk, 0, s>>>(A);
+        k_rhon_assemble<<<grd, blk, 0, s>>>(A);
+        g->launches += 2;
+        CTH_CUDA(cudaGetLastError());
+        if (solve(A.rhon, 0) < 0) return CTH_ERR_CUDA;
+        k_rhon_fluxes<<<grd, blk, 0, s>>>(A);
+        k_rhon_fix<<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out);
+        g->launches += 2;
+    }
+    if (prm->do_rhom) {
+        k_neut_begin<1><<<grd, blk, 0, s>>>(A);
+        k_rhom_assemble<<<grd, blk, 0, s>>>(A);
+        g->launches += 2;
+        CTH_CUDA(cudaGetLastError());
+        if (solve(A.rhom, 1) < 0) return CTH_ERR_CUDA;
+        k_rhom_fix<<<grd, blk, 0, s>>>(A);
+        k_rhom_fluxes<<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out + 2);
+        g->launches += 2;
+    }
     CTH_CUDA(cudaGetLastError());
     CTH_CUDA(cudaMemcpyAsync(fs->h_scal, out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CTH_CUDA(cudaStreamSynchronize(s));

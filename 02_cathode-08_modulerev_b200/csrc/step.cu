@@ -1,0 +1,64 @@
+// step.cu — one time step of the fluid model in the order of the reference's
+// time loop (src/main.cpp:170-251), on one stream; every sub-step is the
+// device implementation behind its own entry point.
+#include <cuda_runtime.h>
+
+#include "fluid.cuh"
+
+extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_step_params* p, void* stream,
+                              cth_step_result* res) {
+    if (!fs || !gx || !gr || !p || p->ndt_i < 1 || p->ndt_n < 1 || p->ndt_m < 1) {
+        cth::set_error("cth_fluid_step: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    cth_step_result local{};
+    cth_step_result* R = res ? res : &local;
+    *R = cth_step_result{};
+    // check_CFL: dt (adaptive) or CFL (fixed dt)
+    R->cfl.dt = p->dt;
+    R->cfl.CFL = p->CFL;
+    R->cfl.masse = p->transport.masse;
+    R->cfl.rmin = p->transport.rmin;
+    R->cfl.dr = p->transport.dr;
+    R->cfl.flag_adp_dt = p->flag_adp_dt;
+    int rc = cth_check_cfl(fs, &R->cfl, stream);
+    if (rc < 0) return rc;
+    p->dt = R->cfl.dt;
+    p->CFL = R->cfl.CFL;
+    p->gtime += p->dt;
+    p->itime += 1;
+    p->ion.dt = p->phi.dt = p->rhoe.dt = p->eps.dt = p->neutral.dt = p->dt;
+    p->ion.CFL = p->CFL;
+    p->ion.ndt_i = p->ndt_i;
+    p->neutral.ndt_n = p->ndt_n;
+    p->neutral.ndt_m = p->ndt_m;
+    int worst = 0;
+    if (p->itime % p->ndt_i == 0) {
+        rc = cth_ion_step(fs, gx, gr, &p->ion, stream, &R->ion);
+        if (rc < 0) return rc;
+        R->ran_ion = 1;
+        if (R->ion.solver_rc > worst) worst = R->ion.solver_rc;
+    }
+    rc = cth_solve_phi_pc(fs, &p->phi, stream, &R->phi);
+    if (rc < 0) return rc;
+    if (R->phi.solver_rc > worst) worst = R->phi.solver_rc;
+    rc = cth_solve_rhoe_pc(fs, &p->rhoe, stream, &R->rhoe);
+    if (rc < 0) return rc;
+    if (R->rhoe.solver_rc > worst) worst = R->rhoe.solver_rc;
+    rc = cth_solve_Te_pc(fs, &p->eps, stream, &R->eps);
+    if (rc < 0) return rc;
+    if (R->eps.solver_rc > worst) worst = R->eps.solver_rc;
+    p->neutral.do_rhon = (p->itime % p->ndt_n == 0);
+    p->neutral.do_rhom = (p->itime % p->ndt_m == 0);
+    if (p->neutral.do_rhon || p->neutral.do_rhom) {
+        rc = cth_update_neutrals(fs, &p->neutral, stream, &R->neutral);
+        if (rc < 0) return rc;
+        if (R->neutral.solver_rc > worst) worst = R->neutral.solver_rc;
+    }
+    R->ran_rhon = p->neutral.do_rhon;
+    R->ran_rhom = p->neutral.do_rhom;
+    rc = cth_update_transport_coef(fs, &p->transport, stream);
+    if (rc < 0) return rc;
+    R->solver_rc = worst;
+    return CTH_OK;
+}

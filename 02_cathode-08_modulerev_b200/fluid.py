@@ -151,7 +151,9 @@ class Fields:
     def update_neutrals(self, prm: dict, pos_boxes, stream=None) -> dict:
         """FluidModule::update_rhon then update_rhom on the device (fluidModule.hpp:4963-5792)."""
         p = capi.NeutralParams(**{k: prm[k] for k, _ in capi.NeutralParams._fields_
-                                  if k not in ("n_pos_box", "pos_box")})
+                                  if k not in ("n_pos_box", "pos_box", "do_rhon", "do_rhom")})
+        p.do_rhon = int(prm.get("do_rhon", 1))
+        p.do_rhom = int(prm.get("do_rhom", 1))
         p.n_pos_box = len(pos_boxes)
         for q, bx in enumerate(pos_boxes):
             for k in range(4):
@@ -161,6 +163,39 @@ class Fields:
         capi.check(self._L.cth_update_neutrals(self._h, ctypes.byref(p), s, ctypes.byref(res)), allow_positive=False)
         return dict(error_rhon=res.error_rhon, error_rhom=res.error_rhom, solver_rc=res.solver_rc,
                     solver=[res.solver[k].as_dict() for k in range(2)])
+
+    def fluid_step(self, grid_x, grid_r, params: dict, stream=None) -> dict:
+        """One time step (src/main.cpp:170-251) through cth_fluid_step; params holds
+        the step fields and the sub-step blocks (ion, phi, rhoe, eps, neutral,
+        transport) as dicts, plus pos_boxes; itime, dt, CFL and gtime are updated."""
+        P = capi.StepParams()
+        for k in ("itime", "ndt_i", "ndt_n", "ndt_m", "flag_adp_dt", "dt", "CFL", "gtime"):
+            setattr(P, k, params[k])
+        for blk, cls in (("ion", capi.IonParams), ("phi", capi.PhiParams), ("rhoe", capi.SGParams),
+                         ("eps", capi.SGParams), ("transport", capi.TransportParams)):
+            setattr(P, blk, cls(**{k: params[blk][k] for k, _ in cls._fields_}))
+        nb = params["neutral"]
+        P.neutral = capi.NeutralParams(**{k: nb[k] for k, _ in capi.NeutralParams._fields_
+                                          if k not in ("n_pos_box", "pos_box", "do_rhon", "do_rhom")})
+        boxes = params.get("pos_boxes", [])
+        P.neutral.n_pos_box = len(boxes)
+        for q, bx in enumerate(boxes):
+            for k in range(4):
+                P.neutral.pos_box[q][k] = int(bx[k])
+        R = capi.StepResult()
+        s = 0 if stream is None else stream.cuda_stream
+        capi.check(self._L.cth_fluid_step(self._h, grid_x._h, grid_r._h, ctypes.byref(P), s, ctypes.byref(R)),
+                   allow_positive=False)
+        for k in ("itime", "dt", "CFL", "gtime"):
+            params[k] = getattr(P, k)
+        return dict(solver_rc=R.solver_rc, ran_ion=R.ran_ion, cfl=R.cfl.CFL, dt=R.cfl.dt,
+                    errors=dict(rhoi=R.ion.error_rhoi, Uix=R.ion.error_Uix, Uir=R.ion.error_Uir, Uip=R.ion.error_Uip,
+                                phi=R.phi.error_phi, rhoe=R.rhoe.error_phi, rhoeps=R.eps.error_phi,
+                                rhon=R.neutral.error_rhon, rhom=R.neutral.error_rhom),
+                    anode=dict(Ii=R.rhoe.Ii_Anode, Ie=R.rhoe.Ie_Anode, I=R.rhoe.I_Anode),
+                    iterations=dict(phi=R.phi.solver.iterations, rhoe=R.rhoe.solver.iterations,
+                                    eps=R.eps.solver.iterations, rhoi=R.ion.solver[3].iterations,
+                                    rhon=R.neutral.solver[0].iterations))
 
     def check_cfl(self, dt: float, CFL: float, masse: float, rmin: float, dr: float, flag_adp_dt: int = 0,
                   stream=None) -> dict:

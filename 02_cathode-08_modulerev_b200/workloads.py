@@ -332,3 +332,85 @@ def neutral_state(ni: int, nj: int, seed: int = 8, Lz: float = 10e-3, Lr: float 
                DmN=5.2e19, error_cnv_SOR=1e-10, ndt_n=1, ndt_m=1, maxITR_SOR=30, flag_iter=1, precision=1,
                flag_error=3)
     return dict(fields=f, prm=prm)
+
+
+RATE_TABLES = ("nu_elas_N", "nu_exc_N", "nu_excReso_N", "nu_excMeta_N", "nu_ionz_N", "nu_ionzStep_N",
+               "nu_excStep_N", "nu_super_N", "rate_eloss_n_N", "rate_eloss_m_N", "nui_m_N")
+
+
+def synthetic_rate_tables(n_e: int = 1801, n_i: int = 39, d_eps_eV: float = 0.1, d_ei_eV: float = 0.001):
+    """Rate tables of the synthetic xenon discharge on the reference's uniform
+    mean-energy grid (inputModule.hpp:1413-1655; Te = 2/3 mean energy): ionisation
+    k = 1e-13 Te^0.5 exp(-12.13/Te) m^3/s with its 12.13 eV loss, elastic 2e-13 m^3/s,
+    ion momentum transfer 5.2e-16 m^3/s.  Returns (tables, dTe [K], dEi [J])."""
+    eps = np.arange(n_e) * d_eps_eV
+    Te = 2.0 / 3.0 * eps
+    kion = np.zeros(n_e)
+    pos = Te > 0
+    kion[pos] = 1e-13 * np.sqrt(Te[pos]) * np.exp(-12.13 / Te[pos])
+    tb = {k: np.zeros(n_e) for k in RATE_TABLES if k != "nui_m_N"}
+    tb["nu_elas_N"] = np.full(n_e, 2e-13)
+    tb["nu_ionz_N"] = kion
+    tb["rate_eloss_n_N"] = kion * 12.13 * E0
+    tb["nui_m_N"] = np.full(n_i, 5.2e-16)
+    return tb, d_eps_eV * 2.0 / 3.0 * E0 / BOLTZ, d_ei_eV * E0
+
+
+def discharge_state(ni: int, nj: int, Lz: float = 10e-3, Lr: float = 5e-3, seed: int = 0) -> dict:
+    """Initial state of the synthetic xenon discharge on the r-z rectangle: ne = ni =
+    1e17 exp(-((z - Lz/2)^2 + r^2) / (2 (1 mm)^2)) x lognormal(0, 0.1) from
+    default_rng(seed), floor 1e12 m^-3; neutrals 1e20 m^-3; Te 5 eV;
+    cusp field Bz = 0.25 T cos(pi z/Lz) e^(-r/2 mm), Br = 0.25 T sin(pi z/Lz) e^(-r/2 mm)
+    sampled on the (ni+1) x (nj+1) cell corners and averaged to the cells; zero
+    potential, fields, fluxes and velocities."""
+    rng = np.random.default_rng(seed)
+    sh = (ni + 2, nj + 2)
+    dx, dr = Lz / ni, Lr / nj
+    z = (np.arange(ni + 2) - 0.5) * dx
+    r = (np.arange(nj + 2) - 0.5) * dr
+    sig = 1e-3
+    ne = 1e17 * np.exp(-(((z[:, None] - Lz / 2) ** 2) + r[None, :] ** 2) / (2 * sig * sig))
+    ne = np.maximum(ne * np.exp(0.1 * rng.standard_normal(sh)), 1e12)
+    zn = np.arange(ni + 1) * dx
+    rn = np.arange(nj + 1) * dr
+    Bz_n = 0.25 * np.cos(np.pi * zn[:, None] / Lz) * np.exp(-rn[None, :] / 2e-3)
+    Br_n = 0.25 * np.sin(np.pi * zn[:, None] / Lz) * np.exp(-rn[None, :] / 2e-3)
+    Bx = np.zeros(sh)
+    Br = np.zeros(sh)
+    Bx[1:-1, 1:-1] = (Bz_n[:-1, :-1] + Bz_n[1:, :-1] + Bz_n[:-1, 1:] + Bz_n[1:, 1:]) / 4.0
+    Br[1:-1, 1:-1] = (Br_n[:-1, :-1] + Br_n[1:, :-1] + Br_n[:-1, 1:] + Br_n[1:, 1:]) / 4.0
+    Te = np.full(sh, 5.0 * E0 / BOLTZ)
+    f = dict(rhoe=ne.copy(), rhoi=ne.copy(), rhon=np.full(sh, 1e20), rhom=np.zeros(sh), Te=Te, Bx=Bx, Br=Br,
+             rhoeps=1.5 * ne * BOLTZ * Te)
+    return dict(fields=f, dx=dx, dr=dr)
+
+
+def discharge_params(geo: dict, dr: float, rmax: float) -> dict:
+    """Parameter blocks of one predictor-corrector time step of the synthetic
+    discharge with the solver settings of input/setup.yaml (SMG, 30 iterations,
+    1e-10 relative residual; 2 PC iterations; calcRes mode 3), dt 1e-10 s, bias 20 V,
+    Ti 0.05 eV, ion-induced SEE yield 0.05 and no electron-induced SEE, neutral inlet
+    flux of 0.069 mg/s through 2 pi r4 x 5.5 mm (initialModule.hpp:234-237)."""
+    dx = geo["dx"]
+    tb, dTe, dEi = synthetic_rate_tables()
+    Ti = 0.05 * E0 / BOLTZ
+    solve = dict(error_cnv_SOR=1e-10, maxITR_SOR=30, flag_iter=1, precision=1)
+    p = dict(
+        itime=0, ndt_i=1, ndt_n=1, ndt_m=1, flag_adp_dt=0, dt=1e-10, CFL=1.0, gtime=0.0,
+        pos_boxes=list(geo.get("pos_boxes", [])),
+        ion=dict(dt=1e-10, dx=dx, dr=dr, rmin=0.0, rmax=rmax, massi=MASSI_XE, Ti=Ti, V_bias=20.0, Te_rep_eV=0.1,
+                 CFL=1.0, ndt_i=1, flag_error=3, **solve),
+        phi=dict(dt=1e-10, dx=dx, dr=dr, rmin=0.0, V_bias=20.0, masse=MASSE, coefIISEE_ts=0.05, coefMISEE_ts=0.05,
+                 dTe_SEE=0.5 * E0 / BOLTZ, error_cnv_HES_phi=1e-21, error_cnv_SOR_phi=1e-10, maxITR_HES_phi=2,
+                 maxITR_SOR_phi=30, flag_error=3, flag_iter_phi=1, precision=1),
+        rhoe=dict(dt=1e-10, dx=dx, dr=dr, rmin=0.0, masse=MASSE, coefIISEE_ts=0.05, coefMISEE_ts=0.05,
+                  dTe_SEE=0.5 * E0 / BOLTZ, Te_emitSEE_eV=2.5, ratioEngy_EISEE_rd=0.5, error_cnv_HES=1e-21,
+                  maxITR_HES=2, flag_error=3, **solve),
+        neutral=dict(dt=1e-10, dx=dx, dr=dr, rmin=0.0, fn_In=0.069e-6 / MASSI_XE / (2.0 * np.pi * 9.0e-3 * 5.5e-3),
+                     Tn=300.0, ri=216.0e-12, massi=MASSI_XE, DmN=5.2e19, ndt_n=1, ndt_m=1, flag_error=3,
+                     do_rhon=1, do_rhom=1, **solve),
+        transport=dict(masse=MASSE, massi=MASSI_XE, Ti=Ti, nu_eff=1e9, dTe=dTe, dEi=dEi, dr=dr, rmin=0.0,
+                       flag_Bohm=0, flag_Sagdeev=0))
+    p["eps"] = dict(p["rhoe"])
+    return dict(params=p, tables=tb, see=dict(coefEISEE_eb_table=np.zeros(201), coefEISEE_rd_table=np.zeros(201),
+                                               coefEISEE_ts_table=np.zeros(201)))

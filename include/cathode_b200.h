@@ -359,6 +359,7 @@ typedef struct cth_neutral_params {
     int ndt_n, ndt_m, maxITR_SOR, flag_iter, precision, flag_error;
     int n_pos_box;
     int pos_box[8][4];  /* i0, i1, j0, j1 */
+    int do_rhon, do_rhom;  /* run update_rhon / update_rhom (the time loop's ndt_n / ndt_m) */
 } cth_neutral_params;
 typedef struct cth_neutral_result {
     double error_rhon, error_rhom;
@@ -367,6 +368,33 @@ typedef struct cth_neutral_result {
     cth_status solver[2];
 } cth_neutral_result;
 int cth_update_neutrals(cth_fields* fs, const cth_neutral_params* prm, void* stream, cth_neutral_result* res);
+
+/* One time step of the fluid model in the order of the reference's time loop
+ * (src/main.cpp:170-251): check_CFL (dt or CFL), the ion sub-step every ndt_i
+ * steps, the potential, electron density and energy predictor-correctors, the
+ * neutral sweeps every ndt_n / ndt_m steps and the transport coefficients.  The
+ * dt and CFL of the sub-step parameter blocks are overwritten by the step's. */
+typedef struct cth_step_params {
+    int itime;                 /* in/out: incremented at the start of the step   */
+    int ndt_i, ndt_n, ndt_m;
+    int flag_adp_dt;
+    double dt, CFL, gtime;     /* in/out                                        */
+    cth_ion_params ion;
+    cth_phi_params phi;
+    cth_sg_params rhoe, eps;
+    cth_neutral_params neutral;
+    cth_transport_params transport;
+} cth_step_params;
+typedef struct cth_step_result {
+    cth_ion_result ion;
+    cth_pc_result phi, rhoe, eps;
+    cth_neutral_result neutral;
+    cth_cfl cfl;
+    int ran_ion, ran_rhon, ran_rhom;
+    int solver_rc;             /* largest positive inner-solve return          */
+} cth_step_result;
+int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_step_params* p, void* stream,
+                   cth_step_result* res);
 
 /* Residual (device arrays): r = b - A x on grid cells (couplings to non-grid
  * cells dropped), r = 0 elsewhere; *rnorm = ||r||_2, *bnorm = ||b||_2 over grid

@@ -327,7 +327,8 @@ def calc_res(new, old, ib, jb, eps, flag_error):
         return float(np.sqrt(np.sum(d ** 2 / (o ** 2 + eps)) / d.size))
     if flag_error == 2:
         return float(np.abs(d).max() / np.abs(o).max())
-    return float(np.sqrt(np.sum(d ** 2) / np.sum(o ** 2)))
+    with np.errstate(divide="ignore", invalid="ignore"):   # an all-zero field gives NaN, as in the reference
+        return float(np.sqrt(np.sum(d ** 2) / np.sum(o ** 2)))
 
 
 PHI_FIELDS = ("phi", "Ex", "Er", "nUex", "nUer")
@@ -1412,3 +1413,34 @@ def update_neutrals(st: dict, prm: dict, geo: dict, solve) -> dict:
                              "rhoUmx_wall", "rhoUmr_wall")}
     out.update(rhon_old=rhon_old, rhom_old=rhom_old, error_rhon=err_n, error_rhom=err_m)
     return out
+
+
+def fluid_step(st: dict, P: dict, geo: dict, see, tb: dict, solve) -> dict:
+    """One time step in the order of src/main.cpp:170-251 chained from the
+    restatements above: check_CFL, ion sub-step, potential, electron density and
+    energy predictor-correctors, neutrals, transport coefficients.  P holds itime,
+    ndt_*, flag_adp_dt, dt, CFL, gtime and the blocks ion, phi, rhoe, eps, neutral
+    (with xL, x6, width_neutIn), transport; it is updated in place.  Returns the
+    new state."""
+    s = dict(st)
+    c = check_cfl(s, dict(rmin=P["transport"]["rmin"], dr=P["transport"]["dr"], masse=P["transport"]["masse"],
+                          flag_adp_dt=P["flag_adp_dt"], CFL=P["CFL"], dt=P["dt"]))
+    P["dt"], P["CFL"] = c["dt"], c["CFL"]
+    P["gtime"] += P["dt"]
+    P["itime"] += 1
+    for blk in ("ion", "phi", "rhoe", "eps", "neutral"):
+        P[blk]["dt"] = P["dt"]
+    P["ion"]["CFL"] = P["CFL"]
+    if P["itime"] % P["ndt_i"] == 0:
+        s.update({k: v for k, v in ion_step(s, P["ion"], geo, solve, solve, solve).items()
+                  if not k.startswith("error")})
+    s.update({k: v for k, v in solve_phi_pc(s, P["phi"], geo, see, solve).items()
+              if k in ("phi", "Ex", "Er", "nUex", "nUer")})
+    s.update({k: v for k, v in solve_sg_pc(s, P["rhoe"], geo, see, solve, "rhoe").items()
+              if k in ("rhoe", "rhoUex", "rhoUer", "rhoUex_wall", "rhoUer_wall", "rhoe_old")})
+    s.update({k: v for k, v in solve_sg_pc(s, P["eps"], geo, see, solve, "rhoeps").items()
+              if k in ("rhoeps", "Gx", "Gr", "Gx_wall", "Gr_wall", "Te", "Te_old")})
+    if P["itime"] % P["ndt_n"] == 0 and P["itime"] % P["ndt_m"] == 0:
+        s.update({k: v for k, v in update_neutrals(s, P["neutral"], geo, solve).items() if not k.startswith("error")})
+    s.update(update_transport_coef(s, tb, P["transport"], geo["flags"]))
+    return s
