@@ -1,34 +1,37 @@
 #!/usr/bin/env python
-"""Throughput of the implicit solve path on one B200 (or N replicas).
+"""Throughput of the implicit time step of the cathode fluid model on one B200
+(or N independent replicas).
 
-Workload: the two isolated 512 (r) x 1024 (z) systems of the cathode code.
-  (a) potential: the reference's Poisson stencil with a 1:3.8 dielectric slab,
-      Dirichlet electrodes at z = 0 / z = L, axis at r = 0, seeded space charge;
-  (b) microwave Er: the reference's Er equation with B = 0 (cold-plasma
-      conductivity from seeded n_e, nu), port excitation, open and Gauss
-      boundaries; assembled on the device.
-Both are solved from a zero guess to ||b-Ax||_2/||b||_2 < 1e-10.  One step =
-solve (a) + assemble and solve (b).
+Workload: the synthetic xenon discharge on the 512 (r) x 1024 (z) r-z rectangle
+(Gaussian plasma 1e17 m^-3 with log-normal noise, neutrals 1e20 m^-3, Te 5 eV,
+cusp B field, 20 V on the z = L electrode, dt 1e-10 s), one time step =
+cth_fluid_step in the reference's loop order (check_CFL, ion momentum x3 +
+continuity + correction, potential predictor-corrector (2 iterations), electron
+density and energy Scharfetter-Gummel predictor-correctors (2 iterations each),
+ground-state and metastable neutrals, transport coefficients: 12 implicit
+5-point solves to 1e-10 relative residual, as input/setup.yaml sets them) plus
+the microwave Er solve every 100 steps (ndiv_MW).
 
 Reported line (rank 0):
-  value        steps/s with (a) on the mixed-precision path (FP32 multigrid
-               + FP64 defect correction) and (b) in complex FP64 (BiCGStab +
-               complex multigrid), inputs resident in HBM, L2 flushed
-               (256 MiB memset) before every step, CUDA events on the stream
-  fp64         the same with (a) on the plain FP64 multigrid
-  e2e          steps/s through the public API with pinned host inputs: (a)
-               via the host C ABI (cth_smg_solve: H2D of six arrays, D2H of
-               the solution), (b) H2D of n_e, nu, epsr, device assembly and
-               solve, D2H of the complex Er plane
-  roofline     finest-level z-line relaxation kernel: algorithmic bytes /
-               CUDA-event time vs the measured HBM copy bandwidth
-  cpu_baseline the CPU restatement (oracle, OpenMP) on a bounded sample
+  value        time steps/s with every inner solve on the mixed-precision path
+               (FP32 multigrid + FP64 defect correction), state resident in HBM,
+               CUDA events on the stream around each step (the working set of
+               ~60 planes x 4.2 MB exceeds L2, so no flush is needed)
+  fp64         the same from the same initial state with plain FP64 multigrid
+  e2e          steps/s through the public API with the 12 prognostic fields
+               uploaded from pinned host arrays before and downloaded after
+               every step (the layout transposes included)
+  roofline     finest-level z-line relaxation kernel of the cell-grid solves:
+               algorithmic bytes / CUDA-event time vs the measured HBM copy
+               bandwidth
+  linear_systems  the isolated 512 x 1024 potential (slab epsr 3.8) and
+               microwave Er systems, mixed vs FP64, to 1e-10
+  cpu_baseline the CPU restatement of the step (oracle: numpy assembly, the
+               semicoarsening MG in C with OpenMP) on a bounded sample
 
---impl reference times the CPU restatement of the reference path (the
-reference itself needs HYPRE/MPI/Eigen/yaml-cpp, which are not installed)
-on the same workload and prints the same metric: (a) by the CPU
-semicoarsening multigrid (OpenMP), (b) by a sparse direct LU (SuperLU, the
-family of the reference's Eigen SparseLU) after the same assembly.
+--impl reference times the CPU restatement of the reference path on the same
+workload (the reference itself needs HYPRE/MPI/Eigen/yaml-cpp, which are not
+installed here) and prints the same metric.
 """
 from __future__ import annotations
 
@@ -50,15 +53,20 @@ TOL = 1e-10
 MAXIT = 30
 
 
+NDIV_MW = 100
+PROGNOSTIC = ("rhoe", "rhoi", "rhoeps", "Te", "rhon", "rhom", "phi", "Ex", "Er", "Uix", "Uir", "Uip")
+STATE = ("rhoe", "rhoi", "rhon", "rhom", "Te", "Bx", "Br", "rhoeps", "rhoe_old")
+
+
 def workload_config(extra=None):
     c = {
-        "workload": "isolated 512 (r) x 1024 (z) systems: (a) potential (slab epsr 3.8, electrodes 0/20 V, axis) "
-                    "+ (b) microwave Er (B=0 cold plasma, n_e 1e15-1e18, nu 1e8-1e10, port/open/Gauss); "
-                    "one step = solve (a) + assemble and solve (b), each to 1e-10 relative residual",
-        "ni_z": NI, "nj_r": NJ, "tol": TOL, "maxit": MAXIT,
-        "l2": "256 MiB memset between timed steps (working set < L2)",
-        "method": "(a) semicoarsening MG (z-line zebra smoother, Galerkin), FP32 cycles + FP64 defect "
-                  "correction; (b) complex FP64 BiCGStab preconditioned by one complex semicoarsening V-cycle",
+        "workload": "synthetic xenon discharge, 512 (r) x 1024 (z) r-z rectangle: one predictor-corrector time step "
+                    "(ions, potential, electron density and energy, neutrals, transport: 12 implicit 5-point "
+                    "solves to 1e-10) + the microwave Er solve every 100 steps",
+        "ni_z": NI, "nj_r": NJ, "tol": TOL, "maxit": MAXIT, "dt": 1e-10, "ndiv_mw": NDIV_MW,
+        "l2": "no flush: the step's working set (~60 planes x 4.2 MB) exceeds the 126 MB L2",
+        "method": "semicoarsening MG (z-line zebra smoother, Galerkin), FP32 cycles + FP64 defect correction; "
+                  "microwave: complex FP64 BiCGStab preconditioned by one complex semicoarsening V-cycle",
     }
     if extra:
         c.update(extra)
@@ -139,29 +147,45 @@ def ncu_traffic():
 # --------------------------------------------------------------------------
 # CPU legs (oracle = test infrastructure, timed as the CPU baseline only)
 # --------------------------------------------------------------------------
-def cpu_step(sa, wb):
-    """One step on the CPU restatement: (a) multigrid, (b) assembly + sparse LU."""
+def cpu_setup(pkg):
+    """The bench workload on the CPU restatement (assembly in numpy, solves by the
+    C semicoarsening multigrid with OpenMP, as solver_SMG)."""
+    import numpy as np
     import oracle
-    from oracle import microwave as mw
-    _, rc, it, rel = oracle.smg_solve(sa, MAXIT, TOL)
-    p = mw.er_rect_params(NI, NJ)
-    sysb = mw.er_rect_system(wb["ne"], wb["nu"], wb["epsr"], p)
-    mw.solve_c5_direct(sysb)
-    return rel
-
-
-def cpu_sample(sa, wb, budget_s=25.0, max_steps=20):
-    import oracle
+    from oracle import fluid
     oracle.build()
+    geo = pkg.fluid.rectangle_geometry(NI, NJ, width_neutIn=2.03e-3)
+    og = fluid.rectangle_geometry(NI, NJ)
+    ds = pkg.workloads.discharge_state(NI, NJ, seed=0)
+    cfg = pkg.workloads.discharge_params(geo, ds["dr"], 5e-3)
+    st = {k: np.zeros((NI + 2, NJ + 2)) for k in FIELD_NAMES}
+    st.update(ds["fields"])
+    st["rhoe_old"] = st["rhoe"].copy()
+    P = {k: (dict(v) if isinstance(v, dict) else v) for k, v in cfg["params"].items()}
+    P["neutral"].update(xL=geo["xL"], x6=geo["x6"], width_neutIn=geo["width_neutIn"])
+    see = (cfg["see"]["coefEISEE_eb_table"], cfg["see"]["coefEISEE_rd_table"], cfg["see"]["coefEISEE_ts_table"],
+           P["phi"]["dTe_SEE"])
+
+    def solve(aP, aE, aW, aN, aS, b, ib, jb):
+        return oracle.smg_solve(dict(ni=NI, nj=NJ, i_bl=ib, j_bl=jb, aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b),
+                                MAXIT, TOL)[0]
+
+    so = fluid.update_transport_coef(st, cfg["tables"], P["transport"], og["flags"])
+    return dict(state=so, P=P, geo=og, see=see, tables=cfg["tables"], solve=solve)
+
+
+def cpu_steps(c, budget_s, max_steps):
+    from oracle import fluid
     n = 0
-    t0 = time.perf_counter()
+    times = []
     while True:
-        cpu_step(sa, wb)
+        t0 = time.perf_counter()
+        c["state"] = fluid.fluid_step(c["state"], c["P"], c["geo"], c["see"], c["tables"], c["solve"])
+        times.append(time.perf_counter() - t0)
         n += 1
-        el = time.perf_counter() - t0
-        if el > budget_s or n >= max_steps:
+        if sum(times) > budget_s or n >= max_steps:
             break
-    return n / el, n, el
+    return times
 
 
 def run_reference(args, rank, world):
@@ -169,46 +193,97 @@ def run_reference(args, rank, world):
         return 0
     import __graft_entry__
     pkg = __graft_entry__.load_package()
-    import oracle
-    oracle.build()
-    sa = pkg.workloads.poisson_slab(NI, NJ, seed=1)
-    wb = pkg.workloads.mw_er_rect(NI, NJ, seed=2)
+    c = cpu_setup(pkg)
     threads = os.cpu_count()
-    # bounded sample: each CPU step takes ~10-20 s; keep the whole run to a few minutes
-    t0 = time.perf_counter()
-    cpu_step(sa, wb)
-    t_first = time.perf_counter() - t0
-    steps = max(1, min(args.steps, int(150.0 / max(t_first, 1e-3))))
-    times = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        cpu_step(sa, wb)
-        times.append(time.perf_counter() - t0)
+    warm = cpu_steps(c, 0.0, 1)
+    times = cpu_steps(c, 150.0, max(1, args.steps))
     tot = sum(times)
-    v = steps / tot
+    v = len(times) / tot
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": 1, "ms_per_step": 1e3 * tot / steps,
+        "steps": len(times), "warmup": 1, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)", "config": workload_config({"parallelism": "host threads"}),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{steps} full steps after 1 warm-up (requested {args.steps}/{args.warmup}; "
-                                   f"capped to ~150 s): (a) CPU restatement of solver_SMG (semicoarsening MG, "
-                                   f"OpenMP over {threads} threads), (b) assembly + SuperLU direct solve "
-                                   f"(single thread), as the reference's SparseLU; the reference's own build "
-                                   f"needs HYPRE/MPI/Eigen/yaml-cpp, not installable here"},
+                         "sample": f"{len(times)} full time steps after {len(warm)} warm-up (requested "
+                                   f"{args.steps}/{args.warmup}; capped to ~150 s): the CPU restatement of "
+                                   f"the step (numpy assembly, C semicoarsening MG for the 12 solves with "
+                                   f"OpenMP over {threads} threads), microwave solve not included; the "
+                                   f"reference's own build needs HYPRE/MPI/Eigen/yaml-cpp, not installable here"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+FIELD_NAMES = ("rhoe", "rhoi", "rhon", "rhom", "Te", "Bx", "Br", "rhoeps", "phi", "Ex", "Er", "nUex", "nUer", "Uix",
+               "Uir", "Uip", "rhoUix", "rhoUir", "rhoUix_wall", "rhoUir_wall", "rhoUex", "rhoUer", "rhoUex_wall",
+               "rhoUer_wall", "Gx", "Gr", "Gx_wall", "Gr_wall", "rhoUnx", "rhoUnr", "rhoUnx_wall", "rhoUnr_wall",
+               "rhoUmx", "rhoUmr", "rhoUmx_wall", "rhoUmr_wall", "nu_ano", "nu_ano_IAT", "Pabs", "rhoe_old")
+
+
+class _Plane:
+    """A raw device pointer with the data_ptr() of a torch tensor."""
+
+    def __init__(self, p):
+        self.p = p
+
+    def data_ptr(self):
+        return self.p
+
+
+def linear_systems(pkg, dev, stream, steps=10):
+    """The isolated 512 x 1024 potential and microwave Er systems: ms per solve."""
+    import torch
+    capi = pkg.capi
+    sa = pkg.workloads.poisson_slab(NI, NJ, seed=1)
+    wb = pkg.workloads.mw_er_rect(NI, NJ, seed=2)
+    g = pkg.Grid(NI, NJ, sa["i_bl"], sa["j_bl"], device=dev.index)
+    gb = pkg.Grid(NI, NJ, wb["i_bl"], wb["j_bl"], device=dev.index)
+    planes = [g.to_device(sa[k]) for k in ("aP", "aE", "aW", "aN", "aS", "b")]
+    fields = [gb.to_device(wb[k]) for k in ("ne", "nu", "epsr")]
+    x = g.device_plane(1)[0]
+    eb = torch.zeros((NJ + 2, gb.ld), dtype=torch.complex128, device=dev)
+    out = {}
+    for name, prec in (("poisson_mixed_ms", capi.CTH_PREC_MIXED), ("poisson_fp64_ms", capi.CTH_PREC_FP64)):
+        for _ in range(3):
+            g.smg_solve_dev(*planes, x, maxITR=MAXIT, error_cnv=TOL, precision=prec, stream=stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            st = g.smg_solve_dev(*planes, x, maxITR=MAXIT, error_cnv=TOL, precision=prec, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        out[name] = e0.elapsed_time(e1) / steps
+        out[name.replace("_ms", "_cycles")] = st.iterations
+    pb = gb.mw_er_assemble_dev(*fields, wb["params"], stream=stream)
+    for _ in range(2):
+        gb.c5_solve_dev(*pb, eb, maxITR=200, error_cnv=TOL, stream=stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        pb = gb.mw_er_assemble_dev(*fields, wb["params"], stream=stream)
+        stb = gb.c5_solve_dev(*pb, eb, maxITR=200, error_cnv=TOL, stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    out["helmholtz_ms"] = e0.elapsed_time(e1) / steps
+    out["helmholtz_iterations"] = stb.iterations
+    out["poisson_mixed_over_fp64"] = out["poisson_fp64_ms"] / out["poisson_mixed_ms"]
+    out["workload"] = ("(a) potential with a 1:3.8 dielectric slab, electrodes 0/20 V, axis; (b) microwave Er, "
+                       "B = 0 cold plasma (n_e 1e15-1e18, nu 1e8-1e10), port/open/Gauss; each to 1e-10 from zero")
+    g.close()
+    gb.close()
+    return out
+
+
 # --------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cathode", choices=["cathode", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
@@ -227,130 +302,154 @@ def main():
     dev = torch.device("cuda", local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
-
-    # independent instance per rank (replicas: the path has no exchange step)
-    sa = pkg.workloads.poisson_slab(NI, NJ, seed=1 + rank)
-    wb = pkg.workloads.mw_er_rect(NI, NJ, seed=2 + rank)
-    g = pkg.Grid(NI, NJ, sa["i_bl"], sa["j_bl"], device=local)
-    gb = pkg.Grid(NI, NJ, wb["i_bl"], wb["j_bl"], device=local)
-    planes = [g.to_device(sa[k]) for k in ("aP", "aE", "aW", "aN", "aS", "b")]
-    fields = [gb.to_device(wb[k]) for k in ("ne", "nu", "epsr")]
-    x = g.device_plane(1)[0]
-    eb = torch.zeros((NJ + 2, gb.ld), dtype=torch.complex128, device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def solve_a(prec):
-        return g.smg_solve_dev(*planes, x, maxITR=MAXIT, error_cnv=TOL, precision=prec, stream=stream)
+    # one independent discharge per rank (replicas: the step has no exchange)
+    geo = pkg.fluid.rectangle_geometry(NI, NJ, width_neutIn=2.03e-3)
+    ds = pkg.workloads.discharge_state(NI, NJ, seed=rank)
+    cfg = pkg.workloads.discharge_params(geo, ds["dr"], 5e-3)
+    init = {k: np.zeros((NI + 2, NJ + 2)) for k in FIELD_NAMES}
+    init.update(ds["fields"])
+    init["rhoe_old"] = init["rhoe"].copy()
+    g = pkg.Grid(NI, NJ, geo["ib"], geo["jb"], device=local)
+    gx = pkg.Grid(NI, NJ, geo["fxi"], geo["fxj"], device=local)
+    gr = pkg.Grid(NI, NJ, geo["fri"], geo["frj"], device=local)
+    wb = pkg.workloads.mw_er_rect(NI, NJ, seed=2)
+    gb = pkg.Grid(NI, NJ, wb["i_bl"], wb["j_bl"], device=local)
+    fs = pkg.Fields(g)
+    fs.set_flags(geo["flags"])
+    fs.set_ghost_rules(geo["ghosts"])
+    fs.set_ion_geometry(geo)
+    for k, v in cfg["tables"].items():
+        fs.set_table(k, v)
+    for k, v in cfg["see"].items():
+        fs.set_table(k, v)
+    fs.upload("epsr_mw", np.ones((NI + 2, NJ + 2)))
+    eb = torch.zeros((NJ + 2, gb.ld), dtype=torch.complex128, device=dev)
+    grids = (g, gx, gr, gb)
 
-    def solve_b():
-        pb = gb.mw_er_assemble_dev(*fields, wb["params"], stream=stream)
-        return gb.c5_solve_dev(*pb, eb, maxITR=200, error_cnv=TOL, stream=stream), pb
+    def reset(prec):
+        for k, v in init.items():
+            fs.upload(k, v)
+        P = {k: (dict(v) if isinstance(v, dict) else v) for k, v in cfg["params"].items()}
+        for blk in ("ion", "rhoe", "eps", "neutral"):
+            P[blk]["precision"] = prec
+        P["phi"]["precision"] = prec
+        fs.update_transport_coef(P["transport"])
+        torch.cuda.synchronize(dev)
+        return P
+
+    def microwave():
+        ne, nu, ep = (_Plane(fs.ptr(k)) for k in ("rhoe", "nu_m", "epsr_mw"))
+        pb = gb.mw_er_assemble_dev(ne, nu, ep, wb["params"], stream=stream)
+        return gb.c5_solve_dev(*pb, eb, maxITR=200, error_cnv=TOL, stream=stream)
+
+    def step(P):
+        r = fs.fluid_step(gx, gr, P, stream=stream)
+        if P["itime"] % NDIV_MW == 0:
+            r["mw"] = microwave()
+        return r
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def timed(prec, steps, profile=False):
-        if profile:
-            g.profile(True)
-        ms = ms_a = 0.0
-        its = []
-        l0 = g.launch_count() + gb.launch_count()
+    def timed(prec, steps, warmup):
+        P = reset(prec)
+        for _ in range(warmup):
+            step(P)
+        barrier()
+        l0 = sum(x.launch_count() for x in grids)
+        ms = 0.0
+        last = None
+        mw_solves = 0
         for _ in range(steps):
-            flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
-            e2 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            st = solve_a(prec)
+            last = step(P)
             e1.record(stream)
-            stb, _ = solve_b()
-            e2.record(stream)
-            e2.synchronize()
-            ms += e0.elapsed_time(e2)
-            ms_a += e0.elapsed_time(e1)
-            its.append((st.iterations, stb.iterations))
-            if not (st.converged and stb.converged):
-                raise RuntimeError(f"solve did not converge: {st.as_dict()} {stb.as_dict()}")
-        launches = g.launch_count() + gb.launch_count() - l0
-        prof = None
-        if profile:
-            prof = {c: g.profile_read(c) for c in (capi.CTH_PROF_RELAX0, capi.CTH_PROF_UPDATE,
-                                                   capi.CTH_PROF_RESTRICT0, capi.CTH_PROF_SETUP)}
-            g.profile(False)
-        t = torch.tensor([ms, ms_a], dtype=torch.float64, device=dev)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            mw_solves += int("mw" in last)
+            if last["solver_rc"] != 0:
+                raise RuntimeError(f"an inner solve did not converge: {last}")
+        launches = sum(x.launch_count() for x in grids) - l0
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t[0].item()), float(t[1].item()), its, launches, prof
-
-    # warm-up (both precisions)
-    for _ in range(max(args.warmup, 3)):
-        solve_a(capi.CTH_PREC_MIXED)
-        solve_a(capi.CTH_PREC_FP64)
-        solve_b()
-    barrier()
+        return float(t.item()), launches, last, mw_solves, P
 
     clk = ClockSampler(local)
     clk.start()
     barrier()
-    ms_mixed, ms_a_mixed, its_mixed, launches, _ = timed(capi.CTH_PREC_MIXED, args.steps)
+    ms_mixed, launches, last_mixed, mw_mixed, P_mixed = timed(capi.CTH_PREC_MIXED, args.steps, args.warmup)
     barrier()
-    ms_fp64, ms_a_fp64, its_fp64, _, _ = timed(capi.CTH_PREC_FP64, args.steps)
+    ms_fp64, _, last_fp64, _, _ = timed(capi.CTH_PREC_FP64, args.steps, args.warmup)
     barrier()
     clocks = clk.stop()
-    # kernel-level profile pass (events around kernels of (a); not part of value)
-    nprof = max(3, args.steps // 2)
-    _, _, _, _, prof = timed(capi.CTH_PREC_MIXED, nprof, profile=True)
-    barrier()
 
-    # solution checks of the last solves (FP64 residuals on the device / host)
-    solve_a(capi.CTH_PREC_MIXED)
-    rn, bn = g.residual_dev(*planes, x)
-    stb, pb = solve_b()
-    relres_b = stb.residual
+    # profile pass (not part of value): finest-level relaxation of the cell-grid solves and
+    # a per-sub-step breakdown through the individual entry points
+    P = reset(capi.CTH_PREC_MIXED)
+    for _ in range(2):
+        step(P)
+    torch.cuda.synchronize(dev)
+    g.profile(True)
+    nprof = 5
+    for _ in range(nprof):
+        step(P)
+    torch.cuda.synchronize(dev)
+    prof = {c: g.profile_read(c) for c in (capi.CTH_PROF_RELAX0, capi.CTH_PROF_UPDATE, capi.CTH_PROF_SETUP)}
+    g.profile(False)
+    parts = {}
+    sub = [("ions", lambda: fs.ion_step(gx, gr, P["ion"], stream=stream)),
+           ("potential_pc", lambda: fs.solve_phi_pc(P["phi"], stream=stream)),
+           ("electron_density_pc", lambda: fs.solve_rhoe_pc(P["rhoe"], stream=stream)),
+           ("electron_energy_pc", lambda: fs.solve_Te_pc(P["eps"], stream=stream)),
+           ("neutrals", lambda: fs.update_neutrals(P["neutral"], P["pos_boxes"], stream=stream)),
+           ("transport", lambda: fs.update_transport_coef(P["transport"], stream=stream)),
+           ("microwave", microwave)]
+    for name, fn in sub:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        parts[name] = e0.elapsed_time(e1)
 
-    # end-to-end through the public API with pinned host buffers
-    pin = {k: torch.from_numpy(sa[k]).pin_memory().numpy() for k in ("aP", "aE", "aW", "aN", "aS", "b")}
-    pinb = {k: torch.from_numpy(wb[k]).pin_memory() for k in ("ne", "nu", "epsr")}
-    xs = torch.zeros((NI + 2, NJ + 2), dtype=torch.float64).pin_memory().numpy()
-    eb_host = torch.empty((NJ + 2, gb.ld), dtype=torch.complex128).pin_memory()
-    dfields = [torch.empty((NI + 2, NJ + 2), dtype=torch.float64, device=dev) for _ in range(3)]
+    # end-to-end through the public API: prognostic fields from pinned host arrays
+    P = reset(capi.CTH_PREC_MIXED)
+    host = {k: torch.from_numpy(init[k]).pin_memory().numpy() for k in PROGNOSTIC}
+    out = {k: torch.empty((NI + 2, NJ + 2), dtype=torch.float64).pin_memory().numpy() for k in PROGNOSTIC}
 
     def e2e_step():
-        pkg.solver_SMG(pin["aP"], pin["aE"], pin["aW"], pin["aN"], pin["aS"], pin["b"], sa["i_bl"],
-                       sa["j_bl"], 1, MAXIT, TOL, 0, xs, precision=capi.CTH_PREC_MIXED, device=local)
-        for d, k in zip(dfields, ("ne", "nu", "epsr")):
-            d.copy_(pinb[k], non_blocking=True)
-        dev_fields = []
-        for d in dfields:
-            plane = gb.device_plane(1)[0]
-            capi.check(gb._L.cth_to_device_layout(gb._h, d.data_ptr(), plane.data_ptr(), stream.cuda_stream),
-                       allow_positive=False)
-            dev_fields.append(plane)
-        pbx = gb.mw_er_assemble_dev(*dev_fields, wb["params"], stream=stream)
-        gb.c5_solve_dev(*pbx, eb, maxITR=200, error_cnv=TOL, stream=stream)
-        eb_host.copy_(eb, non_blocking=True)
-        torch.cuda.synchronize(dev)
+        for k in PROGNOSTIC:
+            fs.upload(k, host[k])
+        step(P)
+        for k in PROGNOSTIC:
+            out[k][...] = fs.download(k)
+        for k in PROGNOSTIC:
+            host[k][...] = out[k]
 
     for _ in range(2):
         e2e_step()
     barrier()
-    e2e_steps = max(3, args.steps // 2)
+    e2e_steps = max(3, args.steps // 5)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        flush.zero_()
-        torch.cuda.synchronize(dev)
         e2e_step()
+    torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_s = float(te.item())
 
+    lin = linear_systems(pkg, dev, stream) if rank == 0 else None
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -370,22 +469,21 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (a), complex f64 (b)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 MG cycles + f64 residuals/assembly; complex f64 (mw)",
         "data": "synthetic (seeded)",
         "config": workload_config({"parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
-        "poisson_ms": ms_a_mixed / args.steps, "helmholtz_ms": (ms_mixed - ms_a_mixed) / args.steps,
-        "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms_fp64 / args.steps,
-                 "poisson_ms": ms_a_fp64 / args.steps},
+        "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms_fp64 / args.steps},
         "mixed_over_fp64": value / fp64_value,
-        "poisson_mixed_over_fp64": ms_a_fp64 / ms_a_mixed,
-        "cycles_poisson": its_mixed[-1][0], "iterations_helmholtz": its_mixed[-1][1],
-        "final_relres": {"poisson": rn / bn, "helmholtz": relres_b},
+        "learned_warm_start": "not built: the reported steps/s are the mixed-precision path without it",
+        "microwave_solves_in_timed_steps": mw_mixed,
+        "inner_iterations_last_step": last_mixed["iterations"],
+        "step_breakdown_ms": parts,
         "gpu_launches": launches,
         "e2e": {"value": world * e2e_steps / e2e_s, "unit": UNIT,
-                "h2d_bytes_per_step": 6 * nbytes_ij + 3 * nbytes_ij,
-                "d2h_bytes_per_step": nbytes_ij + (NJ + 2) * gb.ld * 16,
-                "timing": "host wall clock around the synchronous public-API calls"},
-        "roofline": {"bound": "hbm", "kernel": "k_relax<float,5,0> (finest-level z-line relaxation of (a))",
+                "h2d_bytes_per_step": len(PROGNOSTIC) * nbytes_ij,
+                "d2h_bytes_per_step": len(PROGNOSTIC) * nbytes_ij,
+                "timing": "host wall clock around the public-API calls (upload, step, download)"},
+        "roofline": {"bound": "hbm", "kernel": "k_relax<float,5,0> (finest-level z-line relaxation, cell-grid solves)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": traffic,
@@ -394,17 +492,21 @@ def main():
                      "algorithmic_bytes_per_launch": r_bytes / r_n if r_n else None},
         "kernels": {
             "update_fp64_residual": {"GB/s": upd, "launch_us": 1e3 * u_ms / u_n if u_n else None},
-            "setup_ms_per_solve": prof[capi.CTH_PROF_SETUP][0] / max(1, prof[capi.CTH_PROF_SETUP][1]),
             "relax0_share_of_step": (r_ms / nprof) / (ms_mixed / args.steps),
         },
+        "linear_systems": lin,
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu:
-        v, n, el = cpu_sample(sa, wb)
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                                "sample": f"{n} full steps in {el:.1f} s: (a) CPU restatement of solver_SMG "
-                                          f"(OpenMP over {os.cpu_count()} threads), (b) assembly + SuperLU "
-                                          f"direct solve (single thread)"}
+        c = cpu_setup(pkg)
+        cpu_steps(c, 0.0, 1)
+        times = cpu_steps(c, 20.0, 5)
+        line["cpu_baseline"] = {"value": len(times) / sum(times), "unit": UNIT, "cores": os.cpu_count(),
+                                "kind": "port",
+                                "sample": f"{len(times)} full time steps ({sum(times):.1f} s) after 1 warm-up: the "
+                                          f"CPU restatement of the step (numpy assembly, C semicoarsening MG for the "
+                                          f"12 solves, OpenMP over {os.cpu_count()} threads), microwave solve not "
+                                          f"included"}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -135,27 +135,31 @@ def update_transport_coef(f: dict, tb: dict, prm: dict, flags: np.ndarray) -> di
     me, mi, Ti = prm["masse"], prm["massi"], prm["Ti"]
     Mache = f.get("Mache", np.zeros_like(f["rhoe"])).copy()
     IAT = f["nu_ano_IAT"].copy()
-    for i in range(1, ni + 1):
-        for j in range(1, nj + 1):
-            if not blk[i, j]:
-                continue
-            fl = int(flags[i, j])
-            bLx = float(bool(fl & F_BLX)); bRx = float(bool(fl & F_BRX))
-            bLr = float(bool(fl & F_BLR_WALL)); bRr = float(bool(fl & F_BRR_WALL))
-            ut = np.sqrt(2.0 * BOLTZ * f["Te"][i, j] / me)
-            rL = (r[j] + r[j - 1]) / 2.0
-            rR = (r[j] + r[j + 1]) / 2.0
-            rhoUex_t = (f["rhoUex"][i + 1, j] * bRx + f["rhoUex"][i, j] * bLx) / 2.0
-            rhoUer_t = (rR * f["rhoUer"][i, j + 1] * bRr + rL * f["rhoUer"][i, j] * bLr) / (2.0 * r[j])
-            Uex = rhoUex_t / (f["rhoe"][i, j] + rhoe_max * ratio_rhoe)
-            Uer = rhoUer_t / (f["rhoe"][i, j] + rhoe_max * ratio_rhoe)
-            Uix = (f["Uix"][i, j] + f["Uix"][i + 1, j]) / 2.0
-            Uir = (rL * f["Uir"][i, j] + rR * f["Uir"][i, j + 1]) / (2.0 * r[j])
-            Mache[i, j] = np.sqrt(Uex ** 2 + Uer ** 2) / (ut + 100.0)
-            cs = np.sqrt(2.0 * BOLTZ * (f["Te"][i, j] + Ti) / mi)
-            omega_pi = np.sqrt(f["rhoi"][i, j] * E0 * E0 / (mi * EPS0))
-            ud = np.sqrt((Uex - Uix) ** 2 + (Uer - Uir) ** 2)
-            IAT[i, j] = 0.01 * omega_pi * ud / cs * f["Te"][i, j] / Ti
+    # anomalous frequency on the fluid cells (:5818-5908), evaluated for all grid cells
+    # and kept where the cell is in a block
+    I, J = slice(1, ni + 1), slice(1, nj + 1)
+    fl = flags[I, J].astype(np.int64)
+    bLx = ((fl & F_BLX) != 0).astype(float); bRx = ((fl & F_BRX) != 0).astype(float)
+    bLr = ((fl & F_BLR_WALL) != 0).astype(float); bRr = ((fl & F_BRR_WALL) != 0).astype(float)
+    Te = f["Te"][I, J]
+    rj = r[J][None, :]
+    rL = (r[1:nj + 1] + r[0:nj])[None, :] / 2.0
+    rR = (r[1:nj + 1] + r[2:nj + 2])[None, :] / 2.0
+    ut = np.sqrt(2.0 * BOLTZ * Te / me)
+    rhoUex_t = (f["rhoUex"][2:ni + 2, J] * bRx + f["rhoUex"][I, J] * bLx) / 2.0
+    rhoUer_t = (rR * f["rhoUer"][I, 2:nj + 2] * bRr + rL * f["rhoUer"][I, J] * bLr) / (2.0 * rj)
+    den = f["rhoe"][I, J] + rhoe_max * ratio_rhoe
+    Uex = rhoUex_t / den
+    Uer = rhoUer_t / den
+    Uix = (f["Uix"][I, J] + f["Uix"][2:ni + 2, J]) / 2.0
+    Uir = (rL * f["Uir"][I, J] + rR * f["Uir"][I, 2:nj + 2]) / (2.0 * rj)
+    cs = np.sqrt(2.0 * BOLTZ * (Te + Ti) / mi)
+    omega_pi = np.sqrt(f["rhoi"][I, J] * E0 * E0 / (mi * EPS0))
+    ud = np.sqrt((Uex - Uix) * (Uex - Uix) + (Uer - Uir) * (Uer - Uir))
+    sel = blk[I, J]
+    with np.errstate(all="ignore"):
+        Mache[I, J] = np.where(sel, np.sqrt(Uex * Uex + Uer * Uer) / (ut + 100.0), Mache[I, J])
+        IAT[I, J] = np.where(sel, 0.01 * omega_pi * ud / cs * Te / Ti, IAT[I, J])
     out["Mache"] = Mache
     out["nu_ano_IAT"] = IAT
     Te, dTe = f["Te"], prm["dTe"]
@@ -1252,39 +1256,50 @@ def update_neutrals(st: dict, prm: dict, geo: dict, solve) -> dict:
     DnN = 2.0 / (3.0 * sigma) * np.sqrt(BOLTZ * prm["Tn"] / (np.pi * prm["massi"]))
     rhon_old, Unx_old, Unr_old = g["rhon"].copy(), g["rhoUnx"].copy(), g["rhoUnr"].copy()
     aP, aE, aW, aN, aS, b = (np.zeros(sh) for _ in range(6))
+    x1 = geo["seg_x1"]
     for blk in range(nb):
-        for i in range(geo["ib"][blk][0], geo["ib"][blk][1] + 1):
-            for j in range(geo["jb"][blk][0], geo["jb"][blk][1] + 1):
-                rL = (r[j] + r[j - 1]) / 2.0
-                rR = (r[j] + r[j + 1]) / 2.0
-                qL = (r[j] + r[j - 1]) / 2.0 / r[j]
-                qR = (r[j] + r[j + 1]) / 2.0 / r[j]
-                DLx = DnN / ((rhon_old[i, j] + rhon_old[i - 1, j]) / 2.0 + 1e-100)
-                DRx = DnN / ((rhon_old[i, j] + rhon_old[i + 1, j]) / 2.0 + 1e-100)
-                DLr = DnN / ((rhon_old[i, j] + rhon_old[i, j - 1]) / 2.0 + 1e-100)
-                DRr = DnN / ((rhon_old[i, j] + rhon_old[i, j + 1]) / 2.0 + 1e-100)
-                m = _neutral_masks(geo, prm, i, j, blk)
-                bRr_wall = 1.0 if m["inlet"] else m["bRrw"]
-                bRr_in = 0.0 if m["inlet"] else 1.0
-                bRr = bRr_wall * bRr_in * m["bRro"]
-                GLx = -g["rhoUix_wall"][i, j] - g["rhoUmx_wall"][i, j] if m["bLx"] == 0 else 0.0
-                GRx = -g["rhoUix_wall"][i + 1, j] - g["rhoUmx_wall"][i + 1, j] if m["bRx"] == 0 else 0.0
-                GLr = -g["rhoUir_wall"][i, j] - g["rhoUmr_wall"][i, j] if m["bLrw"] == 0 else 0.0
-                GRr = -g["rhoUir_wall"][i, j + 1] - g["rhoUmr_wall"][i, j + 1] if bRr_wall == 0 else 0.0
-                Gin = (-g["rhoUir_wall"][i, j + 1] - g["rhoUmr_wall"][i, j + 1] - prm["fn_In"]) if bRr_in == 0 else 0.0
-                Gop = max(rL / rR * Unr_old[i, j], 0.0) if m["bRro"] == 0 else 0.0
-                bLx, bRx, bLr = m["bLx"], m["bRx"], m["bLr"]
-                aP[i, j] = ((DRx * bRx + DLx * bLx) * dr * dr + (qR * DRr * bRr + qL * DLr * bLr) * dx * dx
-                            + dx * dx * dr * dr / dt_n)
-                aE[i, j] = DRx * dr * dr * bRx
-                aW[i, j] = DLx * dr * dr * bLx
-                aN[i, j] = qR * DRr * dx * dx * bRr
-                aS[i, j] = qL * DLr * dx * dx * bLr
-                G = (g["nu_excStep"][i, j] + g["nu_super"][i, j]) * g["rhoe"][i, j]
-                L = (g["nu_excMeta"][i, j] + 0.5 * g["nu_exc"][i, j] + g["nu_ionz"][i, j]) * g["rhoe"][i, j]
-                b[i, j] = (rhon_old[i, j] / dt_n * dx * dx * dr * dr + (G - L) * dx * dx * dr * dr
-                           + (GLx) * dr * dx * dr - (GRx) * dr * dx * dr + qL * (GLr) * dx * dx * dr
-                           - qR * (GRr + Gop + Gin) * dx * dx * dr)
+        I = np.arange(geo["ib"][blk][0], geo["ib"][blk][1] + 1)[:, None]
+        J = np.arange(geo["jb"][blk][0], geo["jb"][blk][1] + 1)[None, :]
+        rL = (r[J] + r[J - 1]) / 2.0
+        rR = (r[J] + r[J + 1]) / 2.0
+        qL = (r[J] + r[J - 1]) / 2.0 / r[J]
+        qR = (r[J] + r[J + 1]) / 2.0 / r[J]
+        DLx = DnN / ((rhon_old[I, J] + rhon_old[I - 1, J]) / 2.0 + 1e-100)
+        DRx = DnN / ((rhon_old[I, J] + rhon_old[I + 1, J]) / 2.0 + 1e-100)
+        DLr = DnN / ((rhon_old[I, J] + rhon_old[I, J - 1]) / 2.0 + 1e-100)
+        DRr = DnN / ((rhon_old[I, J] + rhon_old[I, J + 1]) / 2.0 + 1e-100)
+        fl = geo["flags"][I, J].astype(np.int64)
+        bLx = ((fl & F_BLX) != 0).astype(float)
+        bRx = ((fl & F_BRX) != 0).astype(float)
+        bLrw = ((fl & F_BLR_WALL) != 0).astype(float)
+        bLr = (((fl & F_BLR_WALL) != 0) & ((fl & F_BLR_CEN) != 0)).astype(float)
+        bRrw = ((fl & F_BRR_WALL) != 0).astype(float)
+        bRro = ((fl & F_BRR_OPEN) != 0).astype(float)
+        x = prm["xL"] + (I - 0.5) * dx
+        inlet = ((fl & F_BRR_WALL) == 0) & (x <= prm["width_neutIn"] + prm["x6"]) & (x1 is not None)
+        if x1 is not None:
+            inlet &= (I >= x1[0]) & (I <= x1[1]) & (J == x1[2])
+        bRr_wall = np.where(inlet, 1.0, bRrw)
+        bRr_in = np.where(inlet, 0.0, 1.0)
+        bRr = bRr_wall * bRr_in * bRro
+        W = g
+        GLx = np.where(bLx == 0, -W["rhoUix_wall"][I, J] - W["rhoUmx_wall"][I, J], 0.0)
+        GRx = np.where(bRx == 0, -W["rhoUix_wall"][I + 1, J] - W["rhoUmx_wall"][I + 1, J], 0.0)
+        GLr = np.where(bLrw == 0, -W["rhoUir_wall"][I, J] - W["rhoUmr_wall"][I, J], 0.0)
+        GRr = np.where(bRr_wall == 0, -W["rhoUir_wall"][I, J + 1] - W["rhoUmr_wall"][I, J + 1], 0.0)
+        Gin = np.where(bRr_in == 0, -W["rhoUir_wall"][I, J + 1] - W["rhoUmr_wall"][I, J + 1] - prm["fn_In"], 0.0)
+        Gop = np.where(bRro == 0, np.fmax(rL / rR * Unr_old[I, J], 0.0), 0.0)
+        aP[I, J] = ((DRx * bRx + DLx * bLx) * dr * dr + (qR * DRr * bRr + qL * DLr * bLr) * dx * dx
+                    + dx * dx * dr * dr / dt_n)
+        aE[I, J] = DRx * dr * dr * bRx
+        aW[I, J] = DLx * dr * dr * bLx
+        aN[I, J] = qR * DRr * dx * dx * bRr
+        aS[I, J] = qL * DLr * dx * dx * bLr
+        G = (g["nu_excStep"][I, J] + g["nu_super"][I, J]) * g["rhoe"][I, J]
+        L = (g["nu_excMeta"][I, J] + 0.5 * g["nu_exc"][I, J] + g["nu_ionz"][I, J]) * g["rhoe"][I, J]
+        b[I, J] = (rhon_old[I, J] / dt_n * dx * dx * dr * dr + (G - L) * dx * dx * dr * dr
+                   + (GLx) * dr * dx * dr - (GRx) * dr * dx * dr + qL * (GLr) * dx * dx * dr
+                   - qR * (GRr + Gop + Gin) * dx * dx * dr)
     x = solve(aP, aE, aW, aN, aS, b, geo["ib"], geo["jb"])
     rhon = g["rhon"]
     for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
@@ -1342,36 +1357,41 @@ def update_neutrals(st: dict, prm: dict, geo: dict, solve) -> dict:
     DmN = prm["DmN"]
     aP, aE, aW, aN, aS, b = (np.zeros(sh) for _ in range(6))
     for blk in range(nb):
-        for i in range(geo["ib"][blk][0], geo["ib"][blk][1] + 1):
-            for j in range(geo["jb"][blk][0], geo["jb"][blk][1] + 1):
-                rL = (r[j] + r[j - 1]) / 2.0
-                rR = (r[j] + r[j + 1]) / 2.0
-                qL = (r[j] + r[j - 1]) / 2.0 / r[j]
-                qR = (r[j] + r[j + 1]) / 2.0 / r[j]
-                DLx = DmN / ((rhon[i, j] + rhon[i - 1, j]) / 2.0 + 1e-100)
-                DRx = DmN / ((rhon[i, j] + rhon[i + 1, j]) / 2.0 + 1e-100)
-                DLr = DmN / ((rhon[i, j] + rhon[i, j - 1]) / 2.0 + 1e-100)
-                DRr = DmN / ((rhon[i, j] + rhon[i, j + 1]) / 2.0 + 1e-100)
-                m = _neutral_masks(geo, prm, i, j, blk)
-                bLx, bRx, bLr = m["bLx"], m["bRx"], m["bLr"]
-                bRr = m["bRrw"] * m["bRro"]
-                GLx = -0.25 * vth if m["bLx"] == 0 else 0.0
-                GRx = 0.25 * vth if m["bRx"] == 0 else 0.0
-                GLr = -0.25 * vth if m["bLrw"] == 0 else 0.0
-                GRr = 0.25 * vth if m["bRrw"] == 0 else 0.0
-                Gop = rL / rR * Umr_old[i, j] if m["bRro"] == 0 else 0.0
-                aP[i, j] = ((DRx * bRx + DLx * bLx) * dr * dr + (qR * DRr * bRr + qL * DLr * bLr) * dx * dx
-                            - GLx * dr * dx * dr + GRx * dr * dx * dr - qL * GLr * dx * dx * dr
-                            + qR * GRr * dx * dx * dr + dx * dx * dr * dr / dt_m)
-                aE[i, j] = DRx * dr * dr * bRx
-                aW[i, j] = DLx * dr * dr * bLx
-                aN[i, j] = qR * DRr * dx * dx * bRr
-                aS[i, j] = qL * DLr * dx * dx * bLr
-                G = g["rhoe"][i, j] * (g["nu_excMeta"][i, j] + 0.5 * g["nu_exc"][i, j])
-                L = g["rhoe"][i, j] * (g["nu_ionzStep"][i, j] + g["nu_excStep"][i, j] + g["nu_super"][i, j])
-                b[i, j] = (rhom_old[i, j] / dt_m * dx * dx * dr * dr + (G - L) * dx * dx * dr * dr
-                           + (0.0) * dr * dx * dr - (0.0) * dr * dx * dr + qL * (0.0) * dx * dx * dr
-                           - qR * (Gop) * dx * dx * dr)
+        I = np.arange(geo["ib"][blk][0], geo["ib"][blk][1] + 1)[:, None]
+        J = np.arange(geo["jb"][blk][0], geo["jb"][blk][1] + 1)[None, :]
+        rL = (r[J] + r[J - 1]) / 2.0
+        rR = (r[J] + r[J + 1]) / 2.0
+        qL = (r[J] + r[J - 1]) / 2.0 / r[J]
+        qR = (r[J] + r[J + 1]) / 2.0 / r[J]
+        DLx = DmN / ((rhon[I, J] + rhon[I - 1, J]) / 2.0 + 1e-100)
+        DRx = DmN / ((rhon[I, J] + rhon[I + 1, J]) / 2.0 + 1e-100)
+        DLr = DmN / ((rhon[I, J] + rhon[I, J - 1]) / 2.0 + 1e-100)
+        DRr = DmN / ((rhon[I, J] + rhon[I, J + 1]) / 2.0 + 1e-100)
+        fl = geo["flags"][I, J].astype(np.int64)
+        bLx = ((fl & F_BLX) != 0).astype(float)
+        bRx = ((fl & F_BRX) != 0).astype(float)
+        bLrw = ((fl & F_BLR_WALL) != 0).astype(float)
+        bLr = (((fl & F_BLR_WALL) != 0) & ((fl & F_BLR_CEN) != 0)).astype(float)
+        bRrw = ((fl & F_BRR_WALL) != 0).astype(float)
+        bRro = ((fl & F_BRR_OPEN) != 0).astype(float)
+        bRr = bRrw * bRro
+        GLx = np.where(bLx == 0, -0.25 * vth, 0.0)
+        GRx = np.where(bRx == 0, 0.25 * vth, 0.0)
+        GLr = np.where(bLrw == 0, -0.25 * vth, 0.0)
+        GRr = np.where(bRrw == 0, 0.25 * vth, 0.0)
+        Gop = np.where(bRro == 0, rL / rR * Umr_old[I, J], 0.0)
+        aP[I, J] = ((DRx * bRx + DLx * bLx) * dr * dr + (qR * DRr * bRr + qL * DLr * bLr) * dx * dx
+                    - GLx * dr * dx * dr + GRx * dr * dx * dr - qL * GLr * dx * dx * dr
+                    + qR * GRr * dx * dx * dr + dx * dx * dr * dr / dt_m)
+        aE[I, J] = DRx * dr * dr * bRx
+        aW[I, J] = DLx * dr * dr * bLx
+        aN[I, J] = qR * DRr * dx * dx * bRr
+        aS[I, J] = qL * DLr * dx * dx * bLr
+        G = g["rhoe"][I, J] * (g["nu_excMeta"][I, J] + 0.5 * g["nu_exc"][I, J])
+        L = g["rhoe"][I, J] * (g["nu_ionzStep"][I, J] + g["nu_excStep"][I, J] + g["nu_super"][I, J])
+        b[I, J] = (rhom_old[I, J] / dt_m * dx * dx * dr * dr + (G - L) * dx * dx * dr * dr
+                   + (0.0) * dr * dx * dr - (0.0) * dr * dx * dr + qL * (0.0) * dx * dx * dr
+                   - qR * (Gop) * dx * dx * dr)
     x = solve(aP, aE, aW, aN, aS, b, geo["ib"], geo["jb"])
     rhom = g["rhom"]
     for (a0, a1), (c0, c1) in zip(geo["ib"], geo["jb"]):
