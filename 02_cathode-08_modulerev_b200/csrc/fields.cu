@@ -37,38 +37,14 @@ struct TransportArgs {
 __global__ void k_max_flagged(const double* __restrict__ v, const unsigned char* __restrict__ flags, int ni,
                               int nj, int ld, double* __restrict__ part, unsigned int* counter,
                               double* __restrict__ out) {
-    __shared__ double red[32];
-    __shared__ bool am_last;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
-    double m = 0.0;
+    double s[1] = {0.0};
     if (i <= ni + 1) {
         const size_t p = (size_t)j * ld + i;
-        if (flags[p]) m = v[p];
+        if (flags[p]) s[0] = fmax(0.0, v[p]);
     }
-    // block max
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) red[wid] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int k = 0; k < ((int)blockDim.x + 31) / 32; k++) s = fmax(s, red[k]);
-        const int nb = gridDim.x * gridDim.y;
-        part[blockIdx.y * gridDim.x + blockIdx.x] = s;
-        __threadfence();
-        const unsigned int t = atomicAdd(counter, 1u);
-        am_last = (t == (unsigned int)(nb - 1));
-    }
-    __syncthreads();
-    if (am_last && threadIdx.x == 0) {
-        __threadfence();
-        const int nb = gridDim.x * gridDim.y;
-        double s = 0.0;
-        for (int k = 0; k < nb; k++) s = fmax(s, __ldcg(part + k));
-        *out = s;
-        *counter = 0u;
-    }
+    grid_reduce<1>(s, 0x1u, part, counter, out);
 }
 
 // FluidModule::update_transport_coef (fluidModule.hpp:5799-5976), one thread
@@ -313,6 +289,10 @@ void cth_fields_destroy(cth_fields* fs) {
     for (auto& kv : fs->tables) cudaFree(kv.second.first);
     if (fs->flags) cudaFree(fs->flags);
     if (fs->ghost_rules) cudaFree(fs->ghost_rules);
+    if (fs->aux_ready) {
+        for (int k = 0; k < 2; k++) cudaStreamDestroy(fs->aux_stream[k]);
+        for (int k = 0; k < 3; k++) cudaEventDestroy(fs->aux_event[k]);
+    }
     for (int k = 0; k < CTH_ION_NPROG; k++)
         if (fs->ion_ops[k]) cudaFree(fs->ion_ops[k]);
     for (int k = 0; k < 4; k++)

@@ -23,6 +23,9 @@ struct cth_fields {
     int* ion_boxes[4] = {};                    // residual boxes (rhoi, Uix, Uir, Uip)
     int ion_nbox[4] = {};
     int ion_box_total[4] = {};
+    bool aux_ready = false;                    // streams / events of the concurrent ion solves
+    cudaStream_t aux_stream[2] = {};
+    cudaEvent_t aux_event[3] = {};
     std::map<std::string, double*> planes;
     unsigned char* flags = nullptr;  // device layout
     std::map<std::string, std::pair<double*, int>> tables;
@@ -122,14 +125,28 @@ __device__ void grid_reduce(const double (&s)[K], unsigned maxmask, double* __re
     __syncthreads();
     if (!am_last) return;
     __threadfence();
-    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    // the last block combines the partials with all its threads: thread t takes the
+    // partials t, t + blockDim, ... in order, then a fixed warp / cross-warp tree
+    __shared__ double fin[32];
+    for (int k = 0; k < K; k++) {
         const bool mx = (maxmask >> k) & 1u;
         double v = 0.0;
-        for (int q = 0; q < nb; q++) {
+        for (int q = threadIdx.x; q < nb; q += blockDim.x) {
             const double u = __ldcg(part + (size_t)k * nb + q);
             v = mx ? fmax(v, u) : v + u;
         }
-        out[k] = v;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double u = __shfl_down_sync(0xffffffffu, v, o);
+            v = mx ? fmax(v, u) : v + u;
+        }
+        if (lane == 0) fin[wid] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = fin[0];
+            for (int w = 1; w < nw; w++) t = mx ? fmax(t, fin[w]) : t + fin[w];
+            out[k] = t;
+        }
+        __syncthreads();
     }
     if (threadIdx.x == 0) *counter = 0u;
 }

@@ -150,6 +150,8 @@ struct cth_grid {
     cth::SolveGraph c5graph;
     cudaStream_t cap[2] = {nullptr, nullptr};  // capture streams
     bool use_graphs = true;
+    cudaStream_t pending_stream = nullptr;  // stream of the last enqueued graph solve
+    int pending_prec = 0;
 };
 
 namespace cth {
@@ -162,6 +164,11 @@ int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double*
                   const double* aN, const double* aS, const double* b, int maxITR,
                   double error_cnv, int precision, double* solution, cudaStream_t s,
                   cth_status* st);
+// split form of smg_solve_dev: enqueue on s, then read the status (see smg.cu)
+int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
+                     const double* aS, const double* b, int maxITR, double error_cnv, int precision,
+                     double* solution, cudaStream_t s, int* pending);
+int solve_finish(cth_grid* g, int pending, cth_status* st);
 int sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
                   const double* aN, const double* aS, const double* b, double alpha,
                   int maxITR, double error_cnv, double* solution, cudaStream_t s,

@@ -439,34 +439,87 @@ static int ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_pa
         if (rc > solver_rc) solver_rc = rc;
         return rc;
     };
-    auto program = [&](int which, double* U, const double* Uold) {
+    auto program = [&](const IonArgs& AA, int which, double* U, const double* Uold, cudaStream_t ss) {
         if (fs->ion_nops[which] > 0) {
-            k_wall_program<<<1, 256, 0, s>>>(A, fs->ion_ops[which], fs->ion_nops[which], U, Uold);
+            k_wall_program<<<1, 256, 0, ss>>>(AA, fs->ion_ops[which], fs->ion_nops[which], U, Uold);
             g->launches++;
         }
     };
+    // the three momentum components use only the values at the start of the ion
+    // step, so each gets its own coefficient planes and their solves (on three
+    // grids) run concurrently on three streams; results equal the sequential order
+    IonArgs AX = A, AR = A, AC = A;
+    {
+        const char* pre[3] = {"ionx_", "ionr_", "ionp_"};
+        IonArgs* dst[3] = {&AX, &AR, &AC};
+        const char* nm[6] = {"aP", "aE", "aW", "aN", "aS", "b"};
+        for (int c = 0; c < 3; c++) {
+            double** q[6] = {&dst[c]->aP, &dst[c]->aE, &dst[c]->aW, &dst[c]->aN, &dst[c]->aS, &dst[c]->b};
+            for (int k = 0; k < 6; k++) {
+                *q[k] = field_ptr(fs, std::string(pre[c]) + nm[k]);
+                if (!*q[k]) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
+            }
+        }
+    }
     k_ion_begin<<<grd, blk, 0, s>>>(A);
-    // Uix on the x-face grid
-    k_uix_assemble<<<grd, blk, 0, s>>>(A);
-    g->launches += 2;
-    program(CTH_ION_PROG_UIX_ASM, A.Uix, A.Uix_old);
+    k_uix_assemble<<<grd, blk, 0, s>>>(AX);
+    k_uir_assemble<<<grd, blk, 0, s>>>(AR);
+    k_uip_assemble<<<grd, blk, 0, s>>>(AC);
+    g->launches += 4;
+    program(AX, CTH_ION_PROG_UIX_ASM, A.Uix, A.Uix_old, s);
+    program(AR, CTH_ION_PROG_UIR_ASM, A.Uir, A.Uir_old, s);
+    program(AC, CTH_ION_PROG_UIP_ASM, A.Uip, A.Uip_old, s);
     CTH_CUDA(cudaGetLastError());
-    if (solve(gx, A.Uix, 0) < 0) return CTH_ERR_CUDA;
-    program(CTH_ION_PROG_UIX_POST, A.Uix, A.Uix_old);
-    // Uir on the r-face grid
-    k_uir_assemble<<<grd, blk, 0, s>>>(A);
-    g->launches++;
-    program(CTH_ION_PROG_UIR_ASM, A.Uir, A.Uir_old);
+    if (prm->flag_iter == 0) {
+        // SOR: sequential, each component on its own coefficient planes
+        const IonArgs* As[3] = {&AX, &AR, &AC};
+        cth_grid* gs[3] = {gx, gr, g};
+        double* Us[3] = {A.Uix, A.Uir, A.Uip};
+        const double* Uo[3] = {A.Uix_old, A.Uir_old, A.Uip_old};
+        const int post[3] = {CTH_ION_PROG_UIX_POST, CTH_ION_PROG_UIR_POST, CTH_ION_PROG_UIP_POST};
+        for (int c = 0; c < 3; c++) {
+            const IonArgs& C = *As[c];
+            const int rc = sor_solve_dev(gs[c], C.aP, C.aE, C.aW, C.aN, C.aS, C.b, 1.9, prm->maxITR_SOR,
+                                         prm->error_cnv_SOR, Us[c], s, &st[c]);
+            if (rc < 0) return rc;
+            if (rc > solver_rc) solver_rc = rc;
+            program(C, post[c], Us[c], Uo[c], s);
+        }
+    } else {
+        if (!fs->aux_ready) {
+            for (int k = 0; k < 2; k++) CTH_CUDA(cudaStreamCreateWithFlags(&fs->aux_stream[k], cudaStreamNonBlocking));
+            for (int k = 0; k < 3; k++) CTH_CUDA(cudaEventCreateWithFlags(&fs->aux_event[k], cudaEventDisableTiming));
+            fs->aux_ready = true;
+        }
+        cudaStream_t s1 = fs->aux_stream[0], s2 = fs->aux_stream[1];
+        CTH_CUDA(cudaEventRecord(fs->aux_event[0], s));
+        CTH_CUDA(cudaStreamWaitEvent(s1, fs->aux_event[0], 0));
+        CTH_CUDA(cudaStreamWaitEvent(s2, fs->aux_event[0], 0));
+        int pend[3] = {0, 0, 0};
+        int rc = smg_solve_launch(gx, AX.aP, AX.aE, AX.aW, AX.aN, AX.aS, AX.b, prm->maxITR_SOR, prm->error_cnv_SOR,
+                                  prm->precision, A.Uix, s1, &pend[0]);
+        if (rc < 0) return rc;
+        program(AX, CTH_ION_PROG_UIX_POST, A.Uix, A.Uix_old, s1);
+        rc = smg_solve_launch(gr, AR.aP, AR.aE, AR.aW, AR.aN, AR.aS, AR.b, prm->maxITR_SOR, prm->error_cnv_SOR,
+                              prm->precision, A.Uir, s2, &pend[1]);
+        if (rc < 0) return rc;
+        program(AR, CTH_ION_PROG_UIR_POST, A.Uir, A.Uir_old, s2);
+        rc = smg_solve_launch(g, AC.aP, AC.aE, AC.aW, AC.aN, AC.aS, AC.b, prm->maxITR_SOR, prm->error_cnv_SOR,
+                              prm->precision, A.Uip, s, &pend[2]);
+        if (rc < 0) return rc;
+        program(AC, CTH_ION_PROG_UIP_POST, A.Uip, A.Uip_old, s);
+        CTH_CUDA(cudaEventRecord(fs->aux_event[1], s1));
+        CTH_CUDA(cudaEventRecord(fs->aux_event[2], s2));
+        CTH_CUDA(cudaStreamWaitEvent(s, fs->aux_event[1], 0));
+        CTH_CUDA(cudaStreamWaitEvent(s, fs->aux_event[2], 0));
+        cth_grid* gs[3] = {gx, gr, g};
+        for (int c = 0; c < 3; c++) {
+            rc = solve_finish(gs[c], pend[c], &st[c]);
+            if (rc < 0) return rc;
+            if (rc > solver_rc) solver_rc = rc;
+        }
+    }
     CTH_CUDA(cudaGetLastError());
-    if (solve(gr, A.Uir, 1) < 0) return CTH_ERR_CUDA;
-    program(CTH_ION_PROG_UIR_POST, A.Uir, A.Uir_old);
-    // Uip on the cells
-    k_uip_assemble<<<grd, blk, 0, s>>>(A);
-    g->launches++;
-    program(CTH_ION_PROG_UIP_ASM, A.Uip, A.Uip_old);
-    CTH_CUDA(cudaGetLastError());
-    if (solve(g, A.Uip, 2) < 0) return CTH_ERR_CUDA;
-    program(CTH_ION_PROG_UIP_POST, A.Uip, A.Uip_old);
     // continuity and correction
     k_rhoi_assemble<<<grd, blk, 0, s>>>(A);
     g->launches++;

@@ -721,10 +721,15 @@ static int build_graph(cth_grid* g, SolveGraph& G) {
     return CTH_OK;
 }
 
+// Enqueues a solve on stream s.  With graphs on, the call returns after the graph
+// launch and the asynchronous status copy (*pending = 1): solve_finish reads the
+// status after synchronising s, so several grids can solve concurrently on
+// different streams.  Without graphs the solve completes here (*pending = 0).
 template <typename T>
-static int solve_impl(cth_grid* g, const double* aP, const double* aE, const double* aW,
-                      const double* aN, const double* aS, const double* b, int maxITR,
-                      double tol, double* solution, cudaStream_t s, cth_status* st, int prec) {
+static int solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                        const double* aN, const double* aS, const double* b, int maxITR,
+                        double tol, double* solution, cudaStream_t s, int prec, int* pending) {
+    *pending = 0;
     int rc = alloc_hierarchy<T>(g);
     if (rc != CTH_OK) return rc;
     Workspace& w = g->ws;
@@ -748,21 +753,32 @@ static int solve_impl(cth_grid* g, const double* aP, const double* aE, const dou
         if (rc != CTH_OK) return rc;
         CTH_CUDA(cudaGraphLaunch(G.exec, s));
         CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CTH_CUDA(cudaStreamSynchronize(s));
-        g->launches += G.n_pre + (long long)G.n_body * (long long)w.h_stat[ST_ITER] + G.n_post;
-    } else {
-        g->launches += enqueue_pre<T>(g, s, 0, 0);
+        g->pending_stream = s;
+        g->pending_prec = prec;
+        *pending = 1;
+        return CTH_OK;
+    }
+    g->launches += enqueue_pre<T>(g, s, 0, 0);
+    CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CTH_CUDA(cudaStreamSynchronize(s));
+    while (w.h_stat[ST_KEEP] != 0.0) {
+        g->launches += enqueue_body<T>(g, s, 0, 0);
         CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
         CTH_CUDA(cudaStreamSynchronize(s));
-        while (w.h_stat[ST_KEEP] != 0.0) {
-            g->launches += enqueue_body<T>(g, s, 0, 0);
-            CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
-            CTH_CUDA(cudaStreamSynchronize(s));
-        }
-        g->launches += enqueue_post(g, s);
-        CTH_CUDA(cudaGetLastError());
-        CTH_CUDA(cudaStreamSynchronize(s));
-        prof_collect(g);
+    }
+    g->launches += enqueue_post(g, s);
+    CTH_CUDA(cudaGetLastError());
+    CTH_CUDA(cudaStreamSynchronize(s));
+    prof_collect(g);
+    return CTH_OK;
+}
+
+int solve_finish(cth_grid* g, int pending, cth_status* st) {
+    Workspace& w = g->ws;
+    if (pending) {
+        CTH_CUDA(cudaStreamSynchronize(g->pending_stream));
+        const SolveGraph& G = g->graphs[g->pending_prec];
+        g->launches += G.n_pre + (long long)G.n_body * (long long)w.h_stat[ST_ITER] + G.n_post;
     }
     CTH_CUDA(cudaGetLastError());
     cth_status loc{};
@@ -776,16 +792,25 @@ static int solve_impl(cth_grid* g, const double* aP, const double* aE, const dou
     return loc.converged ? CTH_OK : CTH_NOT_CONVERGED;
 }
 
+int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
+                     const double* aS, const double* b, int maxITR, double error_cnv, int precision,
+                     double* solution, cudaStream_t s, int* pending) {
+    if (precision == CTH_PREC_MIXED)
+        return solve_launch<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending);
+    if (precision == CTH_PREC_FP64)
+        return solve_launch<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending);
+    set_error("unknown precision mode");
+    return CTH_ERR_ARG;
+}
+
 int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
                   const double* aN, const double* aS, const double* b, int maxITR,
                   double error_cnv, int precision, double* solution, cudaStream_t s,
                   cth_status* st) {
-    if (precision == CTH_PREC_MIXED)
-        return solve_impl<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, st, precision);
-    if (precision == CTH_PREC_FP64)
-        return solve_impl<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, st, precision);
-    set_error("unknown precision mode");
-    return CTH_ERR_ARG;
+    int pending = 0;
+    const int rc = smg_solve_launch(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, precision, solution, s, &pending);
+    if (rc != CTH_OK) return rc;
+    return solve_finish(g, pending, st);
 }
 
 // complex multigrid used as the preconditioner of the complex Krylov solves
