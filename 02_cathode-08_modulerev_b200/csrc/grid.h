@@ -150,6 +150,7 @@ struct cth_grid {
     cth::SolveGraph c5graph;
     cudaStream_t cap[2] = {nullptr, nullptr};  // capture streams
     bool use_graphs = true;
+    bool pdl = true;  // relaxations launched with programmatic dependent launch
     cudaStream_t pending_stream = nullptr;  // stream of the last enqueued graph solve
     int pending_prec = 0;
 };

@@ -321,6 +321,15 @@ __device__ __forceinline__ void resid4(const LevelArgs<T>& F, int f, int s0, T r
 //   NPTF > 0:   (with zero_guess, C rows) the right-hand side is the residual
 //               of the finer level F restricted on the fly (its C rows 2j and
 //               2j+2), stored into this level's b for rows j and j+1.
+// programmatic dependent launch: wait for the preceding kernel of the stream / graph
+// (a no-op when the kernel was launched without the attribute), and let the next
+// kernel start its own prologue
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// The coefficients of a level are never written inside a cycle, so they are read
+// before the wait; b, the restricted residual and x come from earlier kernels of
+// the cycle and are read after it.
 template <typename T, int NPT, int NPTF>
 __global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong, ProlongArgs<T> pa,
                         LevelArgs<T> F) {
@@ -333,15 +342,37 @@ __global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong,
     const size_t pl = L.plane;
     const size_t p = (size_t)j * L.ld + s0;
     const bool pr = prolong != 0;
+    const bool has_s = !zero_guess && j > 0, has_n = !zero_guess && j + 1 < L.nrow;
     T lo[CH], dg[CH], up[CH], d[1][CH];
+    T aw[CH], ae[CH], as_[CH], an[CH], sw[CH], se[CH], nw[CH], ne[CH];
 #pragma unroll
-    for (int k = 0; k < CH; k++) { lo[k] = T(0); dg[k] = T(1); up[k] = T(0); d[0][k] = T(0); }
+    for (int k = 0; k < CH; k++) {
+        lo[k] = T(0); dg[k] = T(1); up[k] = T(0); d[0][k] = T(0);
+        as_[k] = an[k] = sw[k] = se[k] = nw[k] = ne[k] = T(0);
+    }
+    const T* a = L.a;
     if (cnt > 0) {
-        const T* a = L.a;
-        T aw[CH], ae[CH];
         ld4(a + P * pl + p, dg);
         ld4(a + W * pl + p, aw);
         ld4(a + E * pl + p, ae);
+        if (has_s) {
+            ld4(a + S * pl + p, as_);
+            if (NPT == 9) {
+                ld4(a + SW * pl + p, sw);
+                ld4(a + SE * pl + p, se);
+            }
+        }
+        if (has_n) {
+            ld4(a + N * pl + p, an);
+            if (NPT == 9) {
+                ld4(a + NW * pl + p, nw);
+                ld4(a + NE * pl + p, ne);
+            }
+        }
+    }
+    griddep_wait();
+    griddep_launch();
+    if (cnt > 0) {
         if (NPTF > 0) {
             resid4<T, NPTF>(F, 2 * j, s0, d[0]);
             st4(const_cast<T*>(L.b) + p, d[0]);
@@ -353,46 +384,36 @@ __global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong,
         } else {
             ld4(L.b + p, d[0]);
         }
-        if (!zero_guess) {
-            if (j > 0) {
-                T as_[CH], xs[CH];
-                ld4(a + S * pl + p, as_);
-                xrow4<T>(L, pa, pr, s0, j - 1, xs);
+        if (has_s) {
+            T xs[CH];
+            xrow4<T>(L, pa, pr, s0, j - 1, xs);
 #pragma unroll
-                for (int k = 0; k < CH; k++) d[0][k] += as_[k] * xs[k];
-                if (NPT == 9) {
-                    T sw[CH], se[CH];
-                    ld4(a + SW * pl + p, sw);
-                    ld4(a + SE * pl + p, se);
-                    const T xl = (s0 > 0) ? xnb<T, NPT>(L, pa, pr, s0 - 1, j - 1) : T(0);
-                    const T xr = (s0 + CH < n) ? xnb<T, NPT>(L, pa, pr, s0 + CH, j - 1) : T(0);
-                    d[0][0] += sw[0] * xl;
+            for (int k = 0; k < CH; k++) d[0][k] += as_[k] * xs[k];
+            if (NPT == 9) {
+                const T xl = (s0 > 0) ? xnb<T, NPT>(L, pa, pr, s0 - 1, j - 1) : T(0);
+                const T xr = (s0 + CH < n) ? xnb<T, NPT>(L, pa, pr, s0 + CH, j - 1) : T(0);
+                d[0][0] += sw[0] * xl;
 #pragma unroll
-                    for (int k = 1; k < CH; k++) d[0][k] += sw[k] * xs[k - 1];
+                for (int k = 1; k < CH; k++) d[0][k] += sw[k] * xs[k - 1];
 #pragma unroll
-                    for (int k = 0; k < CH - 1; k++) d[0][k] += se[k] * xs[k + 1];
-                    d[0][CH - 1] += se[CH - 1] * xr;
-                }
+                for (int k = 0; k < CH - 1; k++) d[0][k] += se[k] * xs[k + 1];
+                d[0][CH - 1] += se[CH - 1] * xr;
             }
-            if (j + 1 < L.nrow) {
-                T an[CH], xn[CH];
-                ld4(a + N * pl + p, an);
-                xrow4<T>(L, pa, pr, s0, j + 1, xn);
+        }
+        if (has_n) {
+            T xn[CH];
+            xrow4<T>(L, pa, pr, s0, j + 1, xn);
 #pragma unroll
-                for (int k = 0; k < CH; k++) d[0][k] += an[k] * xn[k];
-                if (NPT == 9) {
-                    T nw[CH], ne[CH];
-                    ld4(a + NW * pl + p, nw);
-                    ld4(a + NE * pl + p, ne);
-                    const T xl = (s0 > 0) ? xnb<T, NPT>(L, pa, pr, s0 - 1, j + 1) : T(0);
-                    const T xr = (s0 + CH < n) ? xnb<T, NPT>(L, pa, pr, s0 + CH, j + 1) : T(0);
-                    d[0][0] += nw[0] * xl;
+            for (int k = 0; k < CH; k++) d[0][k] += an[k] * xn[k];
+            if (NPT == 9) {
+                const T xl = (s0 > 0) ? xnb<T, NPT>(L, pa, pr, s0 - 1, j + 1) : T(0);
+                const T xr = (s0 + CH < n) ? xnb<T, NPT>(L, pa, pr, s0 + CH, j + 1) : T(0);
+                d[0][0] += nw[0] * xl;
 #pragma unroll
-                    for (int k = 1; k < CH; k++) d[0][k] += nw[k] * xn[k - 1];
+                for (int k = 1; k < CH; k++) d[0][k] += nw[k] * xn[k - 1];
 #pragma unroll
-                    for (int k = 0; k < CH - 1; k++) d[0][k] += ne[k] * xn[k + 1];
-                    d[0][CH - 1] += ne[CH - 1] * xr;
-                }
+                for (int k = 0; k < CH - 1; k++) d[0][k] += ne[k] * xn[k + 1];
+                d[0][CH - 1] += ne[CH - 1] * xr;
             }
         }
 #pragma unroll
@@ -560,7 +581,21 @@ static void launch_relax(cth_grid* g, int l, int parity, int zero_guess, int pro
     if (l == 0) slot = prof_mark(g, PROF_RELAX0, (double)rows * g->ncol * 8.0 * sizeof(T), s);
     else if (l == 1 && NPTF > 0)
         slot = prof_mark(g, PROF_RESTRICT0, (double)g->nrow[1] * g->ncol * (9.0 + 8.0) * sizeof(T), s);
-    k_relax<T, NPT, NPTF><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa, F);
+    if (g->pdl) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(rows);
+        cfg.blockDim = dim3(g->bd);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_relax<T, NPT, NPTF>, L, parity, zero_guess, prolong, pa, F);
+    } else {
+        k_relax<T, NPT, NPTF><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa, F);
+    }
     g->launches++;
     if (slot >= 0) prof_done(g, slot, s);
 }
