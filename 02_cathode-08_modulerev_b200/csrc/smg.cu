@@ -177,10 +177,38 @@ __global__ void k_galerkin(LevelArgs<T> F, const unsigned char* __restrict__ mas
         for (int v = 0; v < 3; v++) acc[u][v] = T(0);
     const bool active = maskc[q] != 0;
     if (active) {
+        // interpolation weights of the fine points (2J-2+gg, i-1+ci) toward the
+        // coarse rows J-1+jj, gathered once (P couples rows only: semicoarsening)
+        T W[5][3][3];
+#pragma unroll
+        for (int gg = 0; gg < 5; gg++)
+#pragma unroll
+            for (int ci = 0; ci < 3; ci++)
+#pragma unroll
+                for (int jj = 0; jj < 3; jj++) W[gg][ci][jj] = T(0);
+#pragma unroll
+        for (int gg = 0; gg < 5; gg++) {
+            const int g = 2 * J - 2 + gg;
+            if (g < 0 || g >= F.nrow) continue;
+#pragma unroll
+            for (int ci = 0; ci < 3; ci++) {
+                const int ii = i - 1 + ci;
+                if (ii < 0 || ii >= ncol) continue;
+                const size_t pp = (size_t)g * ld + ii;
+                if ((gg & 1) == 0) {
+                    W[gg][ci][gg / 2] = maskf[pp] ? T(1) : T(0);
+                } else {
+                    W[gg][ci][(gg - 1) / 2] = wS[pp];
+                    W[gg][ci][(gg + 1) / 2] = wN[pp];
+                }
+            }
+        }
         const int c = 2 * J;
-        for (int f = c - 1; f <= c + 1; f++) {
+#pragma unroll
+        for (int gf = 1; gf <= 3; gf++) {
+            const int f = c - 2 + gf;
             if (f < 0 || f >= F.nrow) continue;
-            const T rw = pw(maskf, wS, wN, f, i, J, ld);
+            const T rw = W[gf][1][1];
             if (rw == T(0)) continue;
             const size_t pf = (size_t)f * ld + i;
 #pragma unroll
@@ -194,7 +222,7 @@ __global__ void k_galerkin(LevelArgs<T> F, const unsigned char* __restrict__ mas
                 for (int dJ = -1; dJ <= 1; dJ++) {
                     const int Jp = J + dJ;
                     if (Jp < 0 || Jp >= nrowc) continue;
-                    const T pv = pw(maskf, wS, wN, g, ii, Jp, ld);
+                    const T pv = W[gf + oj[k]][1 + oi[k]][dJ + 1];
                     if (pv != T(0)) acc[dJ + 1][oi[k] + 1] += rw * mv * pv;
                 }
             }
