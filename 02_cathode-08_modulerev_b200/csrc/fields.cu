@@ -270,7 +270,8 @@ int cth_fields_create(cth_grid* g, cth_fields** out) {
     fs->npart = nblk * CTH_FS_NPART_PER_BLOCK;
     if (cudaMalloc(&fs->part, fs->npart * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&fs->scal, CTH_FS_NSCAL * sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&fs->h_scal, CTH_FS_NSCAL * sizeof(double)) != cudaSuccess) {
+        cudaMallocHost(&fs->h_scal, CTH_FS_NSCAL * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&fs->h_solve, 8 * 8 * sizeof(double)) != cudaSuccess) {
         if (fs->part) cudaFree(fs->part);
         if (fs->scal) cudaFree(fs->scal);
         delete fs;
@@ -300,6 +301,7 @@ void cth_fields_destroy(cth_fields* fs) {
     if (fs->part) cudaFree(fs->part);
     if (fs->scal) cudaFree(fs->scal);
     if (fs->h_scal) cudaFreeHost(fs->h_scal);
+    if (fs->h_solve) cudaFreeHost(fs->h_solve);
     delete fs;
 }
 

@@ -31,6 +31,7 @@ struct cth_fields {
     std::map<std::string, std::pair<double*, int>> tables;
     double* scal = nullptr;          // device scalars (reductions), CTH_FS_NSCAL doubles
     double* h_scal = nullptr;        // pinned host copy
+    double* h_solve = nullptr;       // pinned status slots of enqueued MG solves, 8 doubles each
     double* part = nullptr;          // per-block partials, CTH_FS_NPART_PER_BLOCK per block
     int npart = 0;
 };

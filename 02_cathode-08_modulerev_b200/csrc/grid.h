@@ -152,7 +152,6 @@ struct cth_grid {
     bool use_graphs = true;
     bool pdl = true;  // relaxations launched with programmatic dependent launch
     cudaStream_t pending_stream = nullptr;  // stream of the last enqueued graph solve
-    int pending_prec = 0;
 };
 
 namespace cth {
@@ -165,11 +164,14 @@ int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double*
                   const double* aN, const double* aS, const double* b, int maxITR,
                   double error_cnv, int precision, double* solution, cudaStream_t s,
                   cth_status* st);
-// split form of smg_solve_dev: enqueue on s, then read the status (see smg.cu)
+// split form of smg_solve_dev: enqueue on s with the status copied to h_dst (pinned
+// host, 8 doubles; null = the grid's own), then either solve_finish (synchronise and
+// read the grid's copy) or, after the caller's own synchronisation, solve_parse(h_dst)
 int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
                      const double* aS, const double* b, int maxITR, double error_cnv, int precision,
-                     double* solution, cudaStream_t s, int* pending);
+                     double* solution, cudaStream_t s, int* pending, double* h_dst);
 int solve_finish(cth_grid* g, int pending, cth_status* st);
+int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st);
 int sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
                   const double* aN, const double* aS, const double* b, double alpha,
                   int maxITR, double error_cnv, double* solution, cudaStream_t s,

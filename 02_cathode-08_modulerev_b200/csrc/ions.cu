@@ -470,6 +470,7 @@ static int ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_pa
     program(AR, CTH_ION_PROG_UIR_ASM, A.Uir, A.Uir_old, s);
     program(AC, CTH_ION_PROG_UIP_ASM, A.Uip, A.Uip_old, s);
     CTH_CUDA(cudaGetLastError());
+    int pend_m[4] = {0, 0, 0, 0};  // MG solves whose status is read after the last synchronisation
     if (prm->flag_iter == 0) {
         // SOR: sequential, each component on its own coefficient planes
         const IonArgs* As[3] = {&AX, &AR, &AC};
@@ -497,34 +498,35 @@ static int ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_pa
         CTH_CUDA(cudaStreamWaitEvent(s2, fs->aux_event[0], 0));
         int pend[3] = {0, 0, 0};
         int rc = smg_solve_launch(gx, AX.aP, AX.aE, AX.aW, AX.aN, AX.aS, AX.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                                  prm->precision, A.Uix, s1, &pend[0]);
+                                  prm->precision, A.Uix, s1, &pend[0], fs->h_solve + 0);
         if (rc < 0) return rc;
         program(AX, CTH_ION_PROG_UIX_POST, A.Uix, A.Uix_old, s1);
         rc = smg_solve_launch(gr, AR.aP, AR.aE, AR.aW, AR.aN, AR.aS, AR.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                              prm->precision, A.Uir, s2, &pend[1]);
+                              prm->precision, A.Uir, s2, &pend[1], fs->h_solve + 8);
         if (rc < 0) return rc;
         program(AR, CTH_ION_PROG_UIR_POST, A.Uir, A.Uir_old, s2);
         rc = smg_solve_launch(g, AC.aP, AC.aE, AC.aW, AC.aN, AC.aS, AC.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                              prm->precision, A.Uip, s, &pend[2]);
+                              prm->precision, A.Uip, s, &pend[2], fs->h_solve + 16);
         if (rc < 0) return rc;
         program(AC, CTH_ION_PROG_UIP_POST, A.Uip, A.Uip_old, s);
         CTH_CUDA(cudaEventRecord(fs->aux_event[1], s1));
         CTH_CUDA(cudaEventRecord(fs->aux_event[2], s2));
         CTH_CUDA(cudaStreamWaitEvent(s, fs->aux_event[1], 0));
         CTH_CUDA(cudaStreamWaitEvent(s, fs->aux_event[2], 0));
-        cth_grid* gs[3] = {gx, gr, g};
-        for (int c = 0; c < 3; c++) {
-            rc = solve_finish(gs[c], pend[c], &st[c]);
-            if (rc < 0) return rc;
-            if (rc > solver_rc) solver_rc = rc;
-        }
+        for (int c = 0; c < 3; c++) pend_m[c] = pend[c];
     }
     CTH_CUDA(cudaGetLastError());
     // continuity and correction
     k_rhoi_assemble<<<grd, blk, 0, s>>>(A);
     g->launches++;
     CTH_CUDA(cudaGetLastError());
-    if (solve(g, A.rhoi, 3) < 0) return CTH_ERR_CUDA;
+    if (prm->flag_iter == 0) {
+        if (solve(g, A.rhoi, 3) < 0) return CTH_ERR_CUDA;
+    } else {
+        const int rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
+                                        prm->precision, A.rhoi, s, &pend_m[3], fs->h_solve + 24);
+        if (rc < 0) return rc;
+    }
     k_rhoi_post<<<grd, blk, 0, s>>>(A);
     k_ion_correct<<<grd, blk, 0, s>>>(A);
     g->launches += 2;
@@ -542,6 +544,14 @@ static int ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_pa
     CTH_CUDA(cudaGetLastError());
     CTH_CUDA(cudaMemcpyAsync(fs->h_scal, out, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CTH_CUDA(cudaStreamSynchronize(s));
+    if (prm->flag_iter != 0) {
+        cth_grid* gs[4] = {gx, gr, g, g};
+        for (int c = 0; c < 4; c++) {
+            const int rc = solve_parse(gs[c], pend_m[c], fs->h_solve + 8 * c, &st[c]);
+            if (rc < 0) return rc;
+            if (rc > solver_rc) solver_rc = rc;
+        }
+    }
     if (res) {
         double e[4];
         for (int k = 0; k < 4; k++) {

@@ -296,15 +296,17 @@ static int update_neutrals(cth_fields* fs, const cth_neutral_params* prm, cudaSt
     dim3 blk(128), grd((g->ni + 2 + 127) / 128, g->nj + 2);
     cth_status st[2] = {};
     int solver_rc = 0;
+    int pend[2] = {0, 0};  // MG statuses are read after the final synchronisation
     auto solve = [&](double* x, int k) -> int {
         int rc;
-        if (prm->flag_iter == 0)
+        if (prm->flag_iter == 0) {
             rc = sor_solve_dev(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, 1.9, prm->maxITR_SOR, prm->error_cnv_SOR, x, s,
                                &st[k]);
-        else
-            rc = smg_solve_dev(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                               prm->precision, x, s, &st[k]);
-        if (rc > solver_rc) solver_rc = rc;
+            if (rc > solver_rc) solver_rc = rc;
+        } else {
+            rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
+                                  prm->precision, x, s, &pend[k], fs->h_solve + 8 * k);
+        }
         return rc;
     };
     double* out = fs->scal + 56;
@@ -332,6 +334,12 @@ static int update_neutrals(cth_fields* fs, const cth_neutral_params* prm, cudaSt
     CTH_CUDA(cudaGetLastError());
     CTH_CUDA(cudaMemcpyAsync(fs->h_scal, out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CTH_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < 2; k++) {
+        if (!pend[k]) continue;
+        const int rc = solve_parse(g, pend[k], fs->h_solve + 8 * k, &st[k]);
+        if (rc < 0) return rc;
+        if (rc > solver_rc) solver_rc = rc;
+    }
     if (res) {
         const int m = prm->flag_error;
         res->error_rhon = finish_res(m, fs->h_scal[0], fs->h_scal[1]);

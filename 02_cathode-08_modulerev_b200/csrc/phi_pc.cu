@@ -345,21 +345,25 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
         k_phi_assemble<<<grd, blk, 0, s>>>(A);
         g->launches += 3;
         CTH_CUDA(cudaGetLastError());
-        int rc;
+        // the MG solve is enqueued without a host round trip; its status is read after
+        // the one synchronisation of the iteration
+        int rc, pend = 0;
         if (prm->flag_iter_phi == 0)
             rc = sor_solve_dev(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, 1.9, prm->maxITR_SOR_phi,
                                prm->error_cnv_SOR_phi, A.dphi, s, &st_last);
         else
-            rc = smg_solve_dev(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR_phi, prm->error_cnv_SOR_phi,
-                               prm->precision, A.dphi, s, &st_last);
+            rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR_phi,
+                                  prm->error_cnv_SOR_phi, prm->precision, A.dphi, s, &pend, fs->h_solve);
         if (rc < 0) return rc;
-        if (rc > solver_rc) solver_rc = rc;
         k_phi_correct_a<<<grd, blk, 0, s>>>(A);
         k_phi_correct_b<<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out);
         g->launches += 2;
         CTH_CUDA(cudaGetLastError());
         CTH_CUDA(cudaMemcpyAsync(fs->h_scal, out, kNStat * sizeof(double), cudaMemcpyDeviceToHost, s));
         CTH_CUDA(cudaStreamSynchronize(s));
+        if (pend) rc = solve_parse(g, pend, fs->h_solve, &st_last);
+        if (rc < 0) return rc;
+        if (rc > solver_rc) solver_rc = rc;
         const double* h = fs->h_scal;
         const int m = prm->flag_error;
         for (int k = 0; k < 3; k++) {

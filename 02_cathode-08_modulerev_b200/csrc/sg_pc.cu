@@ -388,20 +388,22 @@ static int solve_sg_pc(cth_fields* fs, const cth_sg_params* prm, cudaStream_t s,
         k_sg_assemble<EN><<<grd, blk, 0, s>>>(A);
         g->launches += 3;
         CTH_CUDA(cudaGetLastError());
-        int rc;
+        int rc, pend = 0;
         if (prm->flag_iter == 0)
             rc = sor_solve_dev(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, 1.9, prm->maxITR_SOR, prm->error_cnv_SOR, A.d, s,
                                &st_last);
         else
-            rc = smg_solve_dev(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                               prm->precision, A.d, s, &st_last);
+            rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
+                                  prm->precision, A.d, s, &pend, fs->h_solve);
         if (rc < 0) return rc;
-        if (rc > solver_rc) solver_rc = rc;
         k_sg_correct<EN><<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out);
         g->launches++;
         CTH_CUDA(cudaGetLastError());
         CTH_CUDA(cudaMemcpyAsync(fs->h_scal, out, kSgStat * sizeof(double), cudaMemcpyDeviceToHost, s));
         CTH_CUDA(cudaStreamSynchronize(s));
+        if (pend) rc = solve_parse(g, pend, fs->h_solve, &st_last);
+        if (rc < 0) return rc;
+        if (rc > solver_rc) solver_rc = rc;
         const double* h = fs->h_scal;
         for (int k = 0; k < 3; k++) {
             e_it[k] = finish_res(m, h[2 * k], h[2 * k + 1]);

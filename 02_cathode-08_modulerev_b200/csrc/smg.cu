@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstring>
 #include <cstdio>
 
 #include "grid.h"
@@ -788,10 +789,15 @@ static int build_graph(cth_grid* g, SolveGraph& G) {
 // launch and the asynchronous status copy (*pending = 1): solve_finish reads the
 // status after synchronising s, so several grids can solve concurrently on
 // different streams.  Without graphs the solve completes here (*pending = 0).
+// the solve's arguments reach the device as kernel parameters (copied at launch), so
+// the host may enqueue the next solve on the same grid before this one has run
+__global__ void k_set_args(SolveArgs a, SolveArgs* dst) { *dst = a; }
+
 template <typename T>
 static int solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW,
                         const double* aN, const double* aS, const double* b, int maxITR,
-                        double tol, double* solution, cudaStream_t s, int prec, int* pending) {
+                        double tol, double* solution, cudaStream_t s, int prec, int* pending,
+                        double* h_dst) {
     *pending = 0;
     int rc = alloc_hierarchy<T>(g);
     if (rc != CTH_OK) return rc;
@@ -808,17 +814,16 @@ static int solve_launch(cth_grid* g, const double* aP, const double* aE, const d
     ha->solution = solution;
     ha->tol = tol;
     ha->maxit = maxITR;
-    CTH_CUDA(cudaMemcpyAsync(w.d_args, ha, sizeof(SolveArgs), cudaMemcpyHostToDevice, s));
+    k_set_args<<<1, 1, 0, s>>>(*ha, w.d_args);
     const bool graph = g->use_graphs && !g->prof.on;
     if (graph) {
         SolveGraph& G = g->graphs[prec];
         rc = build_graph<T>(g, G);
         if (rc != CTH_OK) return rc;
         CTH_CUDA(cudaGraphLaunch(G.exec, s));
-        CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CTH_CUDA(cudaMemcpyAsync(h_dst ? h_dst : w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
         g->pending_stream = s;
-        g->pending_prec = prec;
-        *pending = 1;
+        *pending = 1 + prec;
         return CTH_OK;
     }
     g->launches += enqueue_pre<T>(g, s, 0, 0);
@@ -833,35 +838,41 @@ static int solve_launch(cth_grid* g, const double* aP, const double* aE, const d
     CTH_CUDA(cudaGetLastError());
     CTH_CUDA(cudaStreamSynchronize(s));
     prof_collect(g);
+    if (h_dst) std::memcpy(h_dst, w.h_stat, 8 * sizeof(double));
     return CTH_OK;
 }
 
-int solve_finish(cth_grid* g, int pending, cth_status* st) {
-    Workspace& w = g->ws;
+int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st) {
     if (pending) {
-        CTH_CUDA(cudaStreamSynchronize(g->pending_stream));
-        const SolveGraph& G = g->graphs[g->pending_prec];
-        g->launches += G.n_pre + (long long)G.n_body * (long long)w.h_stat[ST_ITER] + G.n_post;
+        const SolveGraph& G = g->graphs[pending - 1];
+        g->launches += G.n_pre + (long long)G.n_body * (long long)h[ST_ITER] + G.n_post;
     }
     CTH_CUDA(cudaGetLastError());
     cth_status loc{};
-    loc.initial_residual = std::sqrt(w.h_stat[ST_BB]);
-    loc.iterations = (int)w.h_stat[ST_ITER];
-    loc.residual = w.h_stat[ST_RELRES];
-    loc.nonfinite = w.h_stat[ST_NONFINITE] != 0.0;
-    loc.converged = w.h_stat[ST_CONV] != 0.0;
+    loc.initial_residual = std::sqrt(h[ST_BB]);
+    loc.iterations = (int)h[ST_ITER];
+    loc.residual = h[ST_RELRES];
+    loc.nonfinite = h[ST_NONFINITE] != 0.0;
+    loc.converged = h[ST_CONV] != 0.0;
     if (st) *st = loc;
     if (loc.nonfinite) return CTH_NONFINITE;
     return loc.converged ? CTH_OK : CTH_NOT_CONVERGED;
 }
 
+int solve_finish(cth_grid* g, int pending, cth_status* st) {
+    if (pending) CTH_CUDA(cudaStreamSynchronize(g->pending_stream));
+    return solve_parse(g, pending, g->ws.h_stat, st);
+}
+
 int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
                      const double* aS, const double* b, int maxITR, double error_cnv, int precision,
-                     double* solution, cudaStream_t s, int* pending) {
+                     double* solution, cudaStream_t s, int* pending, double* h_dst) {
     if (precision == CTH_PREC_MIXED)
-        return solve_launch<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending);
+        return solve_launch<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending,
+                                   h_dst);
     if (precision == CTH_PREC_FP64)
-        return solve_launch<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending);
+        return solve_launch<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending,
+                                    h_dst);
     set_error("unknown precision mode");
     return CTH_ERR_ARG;
 }
@@ -871,7 +882,8 @@ int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double*
                   double error_cnv, int precision, double* solution, cudaStream_t s,
                   cth_status* st) {
     int pending = 0;
-    const int rc = smg_solve_launch(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, precision, solution, s, &pending);
+    const int rc = smg_solve_launch(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, precision, solution, s, &pending,
+                                    nullptr);
     if (rc != CTH_OK) return rc;
     return solve_finish(g, pending, st);
 }
