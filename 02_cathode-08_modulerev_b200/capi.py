@@ -29,7 +29,7 @@ EXPORTS = (
     "cth_version", "cth_last_error", "cth_grid_create", "cth_grid_destroy", "cth_grid_ld",
     "cth_grid_levels", "cth_grid_set_cycle", "cth_smg_solve", "cth_smg_solve_dev", "cth_sor_solve",
     "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
-    "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs",
+    "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs", "cth_grid_set_tail",
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_fields_create", "cth_fields_destroy", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
@@ -213,6 +213,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         getattr(L, nm).restype = ctypes.c_int
     L.cth_grid_set_graphs.argtypes = [_vp, ctypes.c_int]
     L.cth_grid_set_graphs.restype = ctypes.c_int
+    L.cth_grid_set_tail.argtypes = [_vp, ctypes.c_int]
+    L.cth_grid_set_tail.restype = ctypes.c_int
     L.cth_grid_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
     L.cth_grid_set_cycle.restype = ctypes.c_int
     L.cth_smg_solve.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp,

@@ -336,6 +336,27 @@ int cth_grid_set_graphs(cth_grid* g, int enable) {
     return CTH_OK;
 }
 
+static void drop_graph(cth::SolveGraph& G) {
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    if (G.graph) cudaGraphDestroy(G.graph);
+    G.exec = nullptr;
+    G.graph = nullptr;
+    G.valid = false;
+}
+
+int cth_grid_set_tail(cth_grid* g, int enable) {
+    if (!g) { set_error("cth_grid_set_tail: null grid"); return CTH_ERR_ARG; }
+    if ((enable != 0) != g->tail) {
+        CTH_CUDA(cudaSetDevice(g->device));
+        CTH_CUDA(cudaDeviceSynchronize());
+        g->tail = enable != 0;
+        drop_graph(g->graphs[0]);
+        drop_graph(g->graphs[1]);
+        drop_graph(g->c5graph);
+    }
+    return CTH_OK;
+}
+
 int cth_grid_set_cycle(cth_grid* g, int nu_pre, int nu_post) {
     if (!g || nu_pre < 1 || nu_post < 1 || nu_pre > 8 || nu_post > 8) {
         set_error("cth_grid_set_cycle: sweeps must be in 1..8");

@@ -257,37 +257,72 @@ struct ProlongArgs {
     int nrowc;
 };
 
-template <typename T, int NPT>
+// Loads of x and b.  CG = true reads through L2: in the fused coarse tail the
+// data were written by other CTAs of the same cluster earlier in the kernel,
+// and an SM's L1 may hold an older copy of the line.
+template <bool CG> __device__ __forceinline__ float ldg(const float* p) {
+    if constexpr (CG) return __ldcg(p); else return *p;
+}
+template <bool CG> __device__ __forceinline__ double ldg(const double* p) {
+    if constexpr (CG) return __ldcg(p); else return *p;
+}
+template <bool CG> __device__ __forceinline__ cd ldg(const cd* p) {
+    if constexpr (CG) {
+        const double2 q = __ldcg(reinterpret_cast<const double2*>(p));
+        return cd(q.x, q.y);
+    } else {
+        return *p;
+    }
+}
+__device__ __forceinline__ void ld4cg(const float* p, float v[4]) {
+    const float4 q = __ldcg(reinterpret_cast<const float4*>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4cg(const double* p, double v[4]) {
+    const double2 q0 = __ldcg(reinterpret_cast<const double2*>(p));
+    const double2 q1 = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+}
+__device__ __forceinline__ void ld4cg(const cd* p, cd v[4]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int k = 0; k < 4; k++) { const double2 t = __ldcg(q + k); v[k] = cd(t.x, t.y); }
+}
+template <bool CG, typename T> __device__ __forceinline__ void ld4g(const T* p, T v[4]) {
+    if constexpr (CG) ld4cg(p, v); else ld4(p, v);
+}
+
+template <typename T, int NPT, bool CG>
 __device__ __forceinline__ T xnb(const LevelArgs<T>& L, const ProlongArgs<T>& pa, bool prolong,
                                  int ii, int jj) {
     const size_t p = (size_t)jj * L.ld + ii;
-    T v = L.x[p];
+    T v = ldg<CG>(L.x + p);
     if (prolong) {
         // jj is an F row (odd)
-        v += pa.wS[p] * pa.ec[(size_t)((jj - 1) >> 1) * L.ld + ii];
+        v += pa.wS[p] * ldg<CG>(pa.ec + (size_t)((jj - 1) >> 1) * L.ld + ii);
         const int Jn = (jj + 1) >> 1;
-        if (Jn < pa.nrowc) v += pa.wN[p] * pa.ec[(size_t)Jn * L.ld + ii];
+        if (Jn < pa.nrowc) v += pa.wN[p] * ldg<CG>(pa.ec + (size_t)Jn * L.ld + ii);
     }
     return v;
 }
 
 // 4 cells [s0, s0+4) of row jj of x (with the coarse correction when prolong)
-template <typename T>
+template <typename T, bool CG>
 __device__ __forceinline__ void xrow4(const LevelArgs<T>& L, const ProlongArgs<T>& pa, bool prolong,
                                       int s0, int jj, T v[CH]) {
     const size_t p = (size_t)jj * L.ld + s0;
-    ld4(L.x + p, v);
+    ld4g<CG>(L.x + p, v);
     if (prolong) {
         T ws[CH], wn[CH], e0[CH];
         ld4(pa.wS + p, ws);
-        ld4(pa.ec + (size_t)((jj - 1) >> 1) * L.ld + s0, e0);
+        ld4g<CG>(pa.ec + (size_t)((jj - 1) >> 1) * L.ld + s0, e0);
 #pragma unroll
         for (int k = 0; k < CH; k++) v[k] += ws[k] * e0[k];
         const int Jn = (jj + 1) >> 1;
         if (Jn < pa.nrowc) {
             T e1[CH];
             ld4(pa.wN + p, wn);
-            ld4(pa.ec + (size_t)Jn * L.ld + s0, e1);
+            ld4g<CG>(pa.ec + (size_t)Jn * L.ld + s0, e1);
 #pragma unroll
             for (int k = 0; k < CH; k++) v[k] += wn[k] * e1[k];
         }
@@ -296,20 +331,20 @@ __device__ __forceinline__ void xrow4(const LevelArgs<T>& L, const ProlongArgs<T
 
 // residual r = b - A x of the 4 cells [s0, s0+4) of row f of level F
 // (NPTF-point stencil); used to restrict into the next coarser level on the fly
-template <typename T, int NPTF>
+template <typename T, int NPTF, bool CG>
 __device__ __forceinline__ void resid4(const LevelArgs<T>& F, int f, int s0, T r[CH]) {
     const int n = F.ncol;
     const size_t pl = F.plane;
     const size_t p = (size_t)f * F.ld + s0;
     const T* a = F.a;
     T ap[CH], aw[CH], ae[CH], xc[CH];
-    ld4(F.b + p, r);
+    ld4g<CG>(F.b + p, r);
     ld4(a + P * pl + p, ap);
     ld4(a + W * pl + p, aw);
     ld4(a + E * pl + p, ae);
-    ld4(F.x + p, xc);
-    const T xl = (s0 > 0) ? F.x[p - 1] : T(0);
-    const T xr = (s0 + CH < n) ? F.x[p + CH] : T(0);
+    ld4g<CG>(F.x + p, xc);
+    const T xl = (s0 > 0) ? ldg<CG>(F.x + p - 1) : T(0);
+    const T xr = (s0 + CH < n) ? ldg<CG>(F.x + p + CH) : T(0);
 #pragma unroll
     for (int k = 0; k < CH; k++) r[k] -= ap[k] * xc[k];
     r[0] += aw[0] * xl;
@@ -325,15 +360,15 @@ __device__ __forceinline__ void resid4(const LevelArgs<T>& F, int f, int s0, T r
         const size_t q = (size_t)g * F.ld + s0;
         T as_[CH], xg[CH];
         ld4(a + (side == 0 ? S : N) * pl + p, as_);
-        ld4(F.x + q, xg);
+        ld4g<CG>(F.x + q, xg);
 #pragma unroll
         for (int k = 0; k < CH; k++) r[k] += as_[k] * xg[k];
         if (NPTF == 9) {
             T dl[CH], dr[CH];
             ld4(a + (side == 0 ? SW : NW) * pl + p, dl);
             ld4(a + (side == 0 ? SE : NE) * pl + p, dr);
-            const T gl = (s0 > 0) ? F.x[q - 1] : T(0);
-            const T gr = (s0 + CH < n) ? F.x[q + CH] : T(0);
+            const T gl = (s0 > 0) ? ldg<CG>(F.x + q - 1) : T(0);
+            const T gr = (s0 + CH < n) ? ldg<CG>(F.x + q + CH) : T(0);
             r[0] += dl[0] * gl;
 #pragma unroll
             for (int k = 1; k < CH; k++) r[k] += dl[k] * xg[k - 1];
@@ -359,13 +394,12 @@ __device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.
 // The coefficients of a level are never written inside a cycle, so they are read
 // before the wait; b, the restricted residual and x come from earlier kernels of
 // the cycle and are read after it.
-template <typename T, int NPT, int NPTF>
-__global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong, ProlongArgs<T> pa,
-                        LevelArgs<T> F) {
-    const int j = 2 * blockIdx.x + parity;
-    if (j >= L.nrow) return;
-    extern __shared__ unsigned char smem_raw[];
-    T* red = reinterpret_cast<T*>(smem_raw);
+// relax_line: relaxation of row j by the whole CTA (red: the line solver's
+// shared memory).  DEP: launched with programmatic dependent launch; CG: x and
+// b may have been written by other CTAs of the running kernel.
+template <typename T, int NPT, int NPTF, bool DEP, bool CG>
+__device__ __forceinline__ void relax_line(const LevelArgs<T>& L, int j, int zero_guess, int prolong,
+                                           const ProlongArgs<T>& pa, const LevelArgs<T>& F, T* red) {
     const int n = L.ncol, s0 = CH * threadIdx.x;
     const int cnt = max(0, min(CH, n - s0));
     const size_t pl = L.plane;
@@ -399,28 +433,30 @@ __global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong,
             }
         }
     }
-    griddep_wait();
-    griddep_launch();
+    if constexpr (DEP) {
+        griddep_wait();
+        griddep_launch();
+    }
     if (cnt > 0) {
         if (NPTF > 0) {
-            resid4<T, NPTF>(F, 2 * j, s0, d[0]);
+            resid4<T, NPTF, CG>(F, 2 * j, s0, d[0]);
             st4(const_cast<T*>(L.b) + p, d[0]);
             if (j + 1 < L.nrow) {
                 T r1[CH];
-                resid4<T, NPTF>(F, 2 * j + 2, s0, r1);
+                resid4<T, NPTF, CG>(F, 2 * j + 2, s0, r1);
                 st4(const_cast<T*>(L.b) + p + L.ld, r1);
             }
         } else {
-            ld4(L.b + p, d[0]);
+            ld4g<CG>(L.b + p, d[0]);
         }
         if (has_s) {
             T xs[CH];
-            xrow4<T>(L, pa, pr, s0, j - 1, xs);
+            xrow4<T, CG>(L, pa, pr, s0, j - 1, xs);
 #pragma unroll
             for (int k = 0; k < CH; k++) d[0][k] += as_[k] * xs[k];
             if (NPT == 9) {
-                const T xl = (s0 > 0) ? xnb<T, NPT>(L, pa, pr, s0 - 1, j - 1) : T(0);
-                const T xr = (s0 + CH < n) ? xnb<T, NPT>(L, pa, pr, s0 + CH, j - 1) : T(0);
+                const T xl = (s0 > 0) ? xnb<T, NPT, CG>(L, pa, pr, s0 - 1, j - 1) : T(0);
+                const T xr = (s0 + CH < n) ? xnb<T, NPT, CG>(L, pa, pr, s0 + CH, j - 1) : T(0);
                 d[0][0] += sw[0] * xl;
 #pragma unroll
                 for (int k = 1; k < CH; k++) d[0][k] += sw[k] * xs[k - 1];
@@ -431,12 +467,12 @@ __global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong,
         }
         if (has_n) {
             T xn[CH];
-            xrow4<T>(L, pa, pr, s0, j + 1, xn);
+            xrow4<T, CG>(L, pa, pr, s0, j + 1, xn);
 #pragma unroll
             for (int k = 0; k < CH; k++) d[0][k] += an[k] * xn[k];
             if (NPT == 9) {
-                const T xl = (s0 > 0) ? xnb<T, NPT>(L, pa, pr, s0 - 1, j + 1) : T(0);
-                const T xr = (s0 + CH < n) ? xnb<T, NPT>(L, pa, pr, s0 + CH, j + 1) : T(0);
+                const T xl = (s0 > 0) ? xnb<T, NPT, CG>(L, pa, pr, s0 - 1, j + 1) : T(0);
+                const T xr = (s0 + CH < n) ? xnb<T, NPT, CG>(L, pa, pr, s0 + CH, j + 1) : T(0);
                 d[0][0] += nw[0] * xl;
 #pragma unroll
                 for (int k = 1; k < CH; k++) d[0][k] += nw[k] * xn[k - 1];
@@ -462,6 +498,86 @@ __global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong,
     if (cnt > 0) st4(L.x + p, x[0]);
 }
 
+template <typename T, int NPT, int NPTF>
+__global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong, ProlongArgs<T> pa,
+                        LevelArgs<T> F) {
+    const int j = 2 * blockIdx.x + parity;
+    if (j >= L.nrow) return;
+    extern __shared__ unsigned char smem_raw[];
+    relax_line<T, NPT, NPTF, true, false>(L, j, zero_guess, prolong, pa, F, reinterpret_cast<T*>(smem_raw));
+}
+
+// ---------------------------------------------------------------------------
+// Fused coarse tail of the V-cycle.  The levels l0..nlev-1 (at most TAIL_ROWS
+// rows each, hence at most TAIL_CTAS lines of one colour) run in one launch of
+// a single thread-block cluster: CTA c relaxes row 2c + parity in every phase,
+// a phase ends with a cluster barrier (release / acquire at cluster scope),
+// and x and b are read through L2.  The phases are those of vcycle() from l0
+// down, in the same order, so the tail replaces ~4 launches per coarse level.
+// ---------------------------------------------------------------------------
+constexpr int TAIL_CTAS = 8;
+constexpr int TAIL_ROWS = 2 * TAIL_CTAS;
+constexpr int TAIL_MAXLEV = 8;
+
+template <typename T>
+struct TailArgs {
+    LevelArgs<T> lev[TAIL_MAXLEV + 1];  // lev[0]: level l0-1 (restriction source); lev[1+k]: level l0+k
+    const T* wS[TAIL_MAXLEV];           // interpolation weights of level l0+k toward level l0+k+1
+    const T* wN[TAIL_MAXLEV];
+    int nl;     // number of tail levels
+    int nu1, nu2;
+    int fine5;  // the restriction source is level 0 (5-point operator)
+};
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ void tail_phase(const TailArgs<T>& A, int k, int parity, int zero, int prolong,
+                                           int restr, T* red) {
+    const LevelArgs<T>& L = A.lev[1 + k];
+    const int j = 2 * (int)blockIdx.x + parity;
+    if (j < L.nrow) {
+        ProlongArgs<T> pa{nullptr, nullptr, nullptr, 0};
+        if (prolong) {
+            pa.ec = A.lev[2 + k].x;
+            pa.wS = A.wS[k];
+            pa.wN = A.wN[k];
+            pa.nrowc = A.lev[2 + k].nrow;
+        }
+        if (restr) {
+            if (A.fine5 && k == 0) relax_line<T, 9, 5, false, true>(L, j, 1, 0, pa, A.lev[k], red);
+            else relax_line<T, 9, 9, false, true>(L, j, 1, 0, pa, A.lev[k], red);
+        } else {
+            relax_line<T, 9, 0, false, true>(L, j, zero, prolong, pa, L, red);
+        }
+    }
+    cluster_sync_all();
+}
+
+template <typename T>
+__global__ void k_tail(TailArgs<T> A) {
+    extern __shared__ unsigned char smem_raw[];
+    T* red = reinterpret_cast<T*>(smem_raw);
+    griddep_wait();
+    griddep_launch();
+    const int last = A.nl - 1;
+    for (int k = 0; k < last; k++) {
+        for (int it = 0; it < A.nu1; it++) {
+            tail_phase<T>(A, k, 0, it == 0, 0, it == 0, red);
+            tail_phase<T>(A, k, 1, 0, 0, 0, red);
+        }
+    }
+    tail_phase<T>(A, last, 0, 1, 0, 1, red);
+    if (A.lev[1 + last].nrow > 1) tail_phase<T>(A, last, 1, 0, 0, 0, red);
+    for (int k = last - 1; k >= 0; k--) {
+        for (int it = 0; it < A.nu2; it++) {
+            tail_phase<T>(A, k, 0, 0, it == 0, 0, red);
+            tail_phase<T>(A, k, 1, 0, 0, 0, red);
+        }
+    }
+}
 
 // ---------------------------------------------------------------------------
 // defect correction, iteration it = stat[ST_ITER] + 1: x_it = x_{it-1} + e with
@@ -638,10 +754,60 @@ static void relax(cth_grid* g, int l, int parity, int zero_guess, int prolong, c
     else launch_relax<T, 9, 9>(g, l, parity, 1, 0, s);
 }
 
+// the levels l0..nlev-1 as one cluster launch (k_tail)
+template <typename T>
+static void launch_tail(cth_grid* g, int l0, cudaStream_t s) {
+    Hierarchy<T>& h = hier<T>(g);
+    TailArgs<T> A{};
+    A.nl = g->nlev - l0;
+    A.nu1 = g->nu1;
+    A.nu2 = g->nu2;
+    A.fine5 = l0 == 1;
+    A.lev[0] = level_args<T>(g, l0 - 1);
+    for (int k = 0; k < A.nl; k++) {
+        A.lev[1 + k] = level_args<T>(g, l0 + k);
+        if (l0 + k + 1 < g->nlev) {
+            A.wS[k] = h.wS[l0 + k];
+            A.wN[k] = h.wN[l0 + k];
+        }
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(TAIL_CTAS);
+    cfg.blockDim = dim3(g->bd);
+    cfg.dynamicSmemBytes = line_smem<T>(g->bd, 1);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = TAIL_CTAS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = g->pdl ? 2 : 1;
+    cudaLaunchKernelEx(&cfg, k_tail<T>, A);
+    g->launches++;
+}
+
+// the levels from l down are handled by the fused tail
+template <typename T> constexpr int tail_bit() { return 1; }
+template <> constexpr int tail_bit<double>() { return 2; }
+template <> constexpr int tail_bit<cd>() { return 4; }
+
+template <typename T>
+static bool tail_from(const cth_grid* g, int l) {
+    return g->tail && (g->tail_types & tail_bit<T>()) && l > 0 && g->nrow[l] <= TAIL_ROWS &&
+           g->nlev - l <= TAIL_MAXLEV;
+}
+
 // V(nu1, nu2) cycle on level l.  The first C-row relaxation of every coarse
 // level computes its right-hand side by restricting the finer residual.
 template <typename T>
 static void vcycle(cth_grid* g, int l, cudaStream_t s) {
+    if (tail_from<T>(g, l)) {
+        launch_tail<T>(g, l, s);
+        return;
+    }
     const bool fused = l > 0;
     if (l == g->nlev - 1) {
         relax<T>(g, l, 0, 1, 0, s, fused);
@@ -934,6 +1100,17 @@ int configure_kernels(cth_grid* g) {
         CTH_ATTR((k_relax<float, 9, 5>), smem32); CTH_ATTR((k_relax<float, 9, 9>), smem32);
         CTH_ATTR((k_weights<float, 5>), smem32); CTH_ATTR((k_weights<float, 9>), smem32);
     }
+    // the fused tail runs only where a CTA of the line's width fits the registers
+    g->tail_types = 0;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_tail<float>) == cudaSuccess && fa.maxThreadsPerBlock >= g->bd) g->tail_types |= 1;
+    if (cudaFuncGetAttributes(&fa, k_tail<double>) == cudaSuccess && fa.maxThreadsPerBlock >= g->bd) g->tail_types |= 2;
+    if (cudaFuncGetAttributes(&fa, k_tail<cd>) == cudaSuccess && fa.maxThreadsPerBlock >= g->bd) g->tail_types |= 4;
+    cudaGetLastError();
+    // the fused tail needs one right-hand side of line-solver memory
+    if (line_smem<cd>(g->bd, 1) > 48 * 1024) CTH_ATTR((k_tail<cd>), (int)line_smem<cd>(g->bd, 1));
+    if (line_smem<double>(g->bd, 1) > 48 * 1024) CTH_ATTR((k_tail<double>), (int)line_smem<double>(g->bd, 1));
+    if (line_smem<float>(g->bd, 1) > 48 * 1024) CTH_ATTR((k_tail<float>), (int)line_smem<float>(g->bd, 1));
 #undef CTH_ATTR
     return CTH_OK;
 }

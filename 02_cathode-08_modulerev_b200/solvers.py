@@ -94,6 +94,10 @@ class Grid:
     def set_graphs(self, enable: bool):
         capi.check(self._L.cth_grid_set_graphs(self._h, int(enable)), allow_positive=False)
 
+    def set_tail(self, enable: bool):
+        """Fused coarse tail (levels of at most 16 rows in one cluster launch) on / off."""
+        capi.check(self._L.cth_grid_set_tail(self._h, int(enable)), allow_positive=False)
+
     def set_cycle(self, nu_pre: int, nu_post: int):
         capi.check(self._L.cth_grid_set_cycle(self._h, nu_pre, nu_post), allow_positive=False)
 

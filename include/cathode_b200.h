@@ -83,6 +83,11 @@ int cth_grid_set_cycle(cth_grid* g, int nu_pre, int nu_post);
  * disabled, or while profiling is on, kernels are launched one by one and the
  * host tests convergence after every cycle.  Results are identical. */
 int cth_grid_set_graphs(cth_grid* g, int enable);
+/* enable (default) or disable the fused coarse tail: the multigrid levels of
+ * at most 16 rows run as one thread-block-cluster launch per cycle instead of
+ * one launch per relaxation.  Same sweeps in the same order; results agree to
+ * rounding. */
+int cth_grid_set_tail(cth_grid* g, int enable);
 
 /* Instrumentation ------------------------------------------------------------
  * cth_launch_count: kernels this grid has launched since creation.

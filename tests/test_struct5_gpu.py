@@ -143,3 +143,50 @@ def test_smg_graph_and_stream_paths_agree(pkg, orc, cuda_device):
     err = np.linalg.norm(g.to_host(x3) - ref) / np.linalg.norm(ref)
     assert st3.converged == 1 and err < TOL_PARITY
     g.close()
+
+
+@pytest.mark.parametrize("shape", [(200, 100), (1024, 512)])
+def test_smg_fused_tail_matches_level_launches(pkg, cuda_device, shape):
+    """The coarse levels of at most 16 rows run as one cluster launch per cycle;
+    the same relaxations in the same order as one launch per relaxation, so the
+    iteration counts are equal and the solutions agree to rounding."""
+    ni, nj = shape
+    s = pkg.workloads.poisson_slab(ni=ni, nj=nj, seed=3)
+    g = pkg.Grid(s["ni"], s["nj"], s["i_bl"], s["j_bl"])
+    planes = [g.to_device(s[k]) for k in ("aP", "aE", "aW", "aN", "aS", "b")]
+    for prec in (0, 1):
+        x1 = g.device_plane(1)[0]
+        n0 = g.launch_count()
+        st1 = g.smg_solve_dev(*planes, x1, maxITR=30, error_cnv=1e-11, precision=prec)
+        n_fused = g.launch_count() - n0
+        g.set_tail(False)
+        x2 = g.device_plane(1)[0]
+        n0 = g.launch_count()
+        st2 = g.smg_solve_dev(*planes, x2, maxITR=30, error_cnv=1e-11, precision=prec)
+        n_level = g.launch_count() - n0
+        g.set_tail(True)
+        assert st1.converged == 1 and st2.converged == 1
+        assert st1.iterations == st2.iterations
+        a, b = x1.cpu().numpy(), x2.cpu().numpy()
+        assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b)
+        assert n_fused < n_level
+    g.close()
+
+
+def test_complex_fused_tail_matches_level_launches(pkg, cuda_device):
+    import torch
+    from test_microwave_gpu import _er_case
+    ni, nj = 128, 64
+    w, p, mw = _er_case(pkg, ni, nj)
+    g = pkg.Grid(ni, nj, w["i_bl"], w["j_bl"])
+    planes = g.mw_er_assemble_dev(g.to_device(w["ne"]), g.to_device(w["nu"]), g.to_device(w["epsr"]), w["params"])
+    out = []
+    for tail in (True, False):
+        g.set_tail(tail)
+        x = torch.zeros_like(planes[0])
+        st = g.c5_solve_dev(*planes, x, maxITR=200, error_cnv=1e-11)
+        assert st.converged == 1, st.as_dict()
+        out.append((st.iterations, x.cpu().numpy()))
+    assert out[0][0] == out[1][0]
+    assert np.linalg.norm(out[0][1] - out[1][1]) <= 1e-10 * np.linalg.norm(out[1][1])
+    g.close()
