@@ -152,9 +152,9 @@ static void free_grid(cth_grid* g) {
     auto fr = [](void* p) { if (p) cudaFree(p); };
     fr(g->mask_full);
     for (auto p : g->mask) fr(p);
-    for (auto* v : {&g->h32.a, &g->h32.x, &g->h32.b, &g->h32.wS, &g->h32.wN})
+    for (auto* v : {&g->h32.a, &g->h32.x, &g->h32.b, &g->h32.wS, &g->h32.wN, &g->h32.fac})
         for (auto p : *v) fr(p);
-    for (auto* v : {&g->h64.a, &g->h64.x, &g->h64.b, &g->h64.wS, &g->h64.wN})
+    for (auto* v : {&g->h64.a, &g->h64.x, &g->h64.b, &g->h64.wS, &g->h64.wN, &g->h64.fac})
         for (auto p : *v) fr(p);
     fr(g->ws.x64[0]);
     fr(g->ws.x64[1]);

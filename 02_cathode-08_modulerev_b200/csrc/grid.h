@@ -55,6 +55,7 @@ struct Hierarchy {
     std::vector<T*> b;   // per level
     std::vector<T*> wS;  // per level (F rows used): weight toward the C row below
     std::vector<T*> wN;  // per level: weight toward the C row above
+    std::vector<T*> fac; // per level: factorised z-line operators (real precisions)
 };
 
 // per-kernel-class timing with CUDA events on the launching stream

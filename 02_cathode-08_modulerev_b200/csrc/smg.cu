@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <cstdio>
+#include <type_traits>
 
 #include "grid.h"
 #include "line.cuh"
@@ -33,7 +34,12 @@ struct LevelArgs {
     T* x;
     const T* b;
     int nrow, ncol, ld;
+    const T* fac;     // factorised line operators (real precisions)
 };
+
+// the real precisions relax with factorised line operators; the complex
+// hierarchy eliminates each line in every relaxation
+template <typename T> constexpr bool kFac = !std::is_same<T, cd>::value;
 
 // ---------------------------------------------------------------------------
 // level-0 preparation: masked copy of the caller's FP64 planes into the level
@@ -139,6 +145,72 @@ __global__ void k_weights(LevelArgs<T> L, const unsigned char* __restrict__ mask
     }
     T x[2][CH];
     line_solve<T, 2>(lo, dg, up, d, red, x);
+    if (cnt > 0) {
+        st4(wS + p, x[0]);
+        st4(wN + p, x[1]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// line factorisation of every row of one level (real precisions), once per
+// solve; for the odd (F) rows of a non-coarsest level also the interpolation
+// weights (two right-hand sides through the fresh factors).
+// ---------------------------------------------------------------------------
+template <typename T, int NPT>
+__global__ void k_factor(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ fac,
+                         T* __restrict__ wS, T* __restrict__ wN, int weights) {
+    __shared__ T sh[(8 + LG_N) * 32];
+    const int j = blockIdx.x;
+    const int n = L.ncol, s0 = CH * threadIdx.x;
+    const int cnt = max(0, min(CH, n - s0));
+    const size_t pl = L.plane;
+    const size_t p = (size_t)j * L.ld + s0;
+    const bool wts = weights && (j & 1);
+    T lo[CH], dg[CH], up[CH], d[2][CH];
+#pragma unroll
+    for (int k = 0; k < CH; k++) { lo[k] = T(0); dg[k] = T(1); up[k] = T(0); d[0][k] = T(0); d[1][k] = T(0); }
+    if (cnt > 0) {
+        const T* a = L.a;
+        T aw[CH], ae[CH];
+        ld4(a + P * pl + p, dg);
+        ld4(a + W * pl + p, aw);
+        ld4(a + E * pl + p, ae);
+        T as_[CH] = {0, 0, 0, 0}, an[CH] = {0, 0, 0, 0};
+        T sw[CH] = {0, 0, 0, 0}, se[CH] = {0, 0, 0, 0}, nw[CH] = {0, 0, 0, 0}, ne[CH] = {0, 0, 0, 0};
+        if (wts) {
+            ld4(a + S * pl + p, as_);
+            ld4(a + N * pl + p, an);
+            if (NPT == 9) {
+                ld4(a + SW * pl + p, sw);
+                ld4(a + SE * pl + p, se);
+                ld4(a + NW * pl + p, nw);
+                ld4(a + NE * pl + p, ne);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < CH; k++) {
+            const int i = s0 + k;
+            if (k < cnt) {
+                lo[k] = (i > 0) ? -aw[k] : T(0);
+                up[k] = (i + 1 < n) ? -ae[k] : T(0);
+                const size_t pk = p + k;
+                if (wts && mask[pk]) {
+                    if (mask[pk - L.ld]) d[0][k] = as_[k] + ((NPT == 9) ? sw[k] + se[k] : T(0));
+                    if (j + 1 < L.nrow && mask[pk + L.ld]) d[1][k] = an[k] + ((NPT == 9) ? nw[k] + ne[k] : T(0));
+                }
+            } else {
+                dg[k] = T(1);
+            }
+        }
+    }
+    T* frow = fac + (size_t)j * line_fac_size<T>(blockDim.x);
+    line_factor<T>(lo, dg, up, sh, frow);
+    if (!wts) return;
+    __syncthreads();
+    LineFacRegs<T> R;
+    line_fac_load<T>(frow, R, sh);
+    T x[2][CH];
+    line_solve_fac<T, 2>(R, d, sh, x);
     if (cnt > 0) {
         st4(wS + p, x[0]);
         st4(wN + p, x[1]);
@@ -414,10 +486,14 @@ __device__ __forceinline__ void relax_line(const LevelArgs<T>& L, int j, int zer
         as_[k] = an[k] = sw[k] = se[k] = nw[k] = ne[k] = T(0);
     }
     const T* a = L.a;
+    LineFacRegs<T> R;
+    if constexpr (kFac<T>) line_fac_load<T>(L.fac + (size_t)j * line_fac_size<T>(blockDim.x), R, red);
     if (cnt > 0) {
-        ld4(a + P * pl + p, dg);
-        ld4(a + W * pl + p, aw);
-        ld4(a + E * pl + p, ae);
+        if constexpr (!kFac<T>) {
+            ld4(a + P * pl + p, dg);
+            ld4(a + W * pl + p, aw);
+            ld4(a + E * pl + p, ae);
+        }
         if (has_s) {
             ld4(a + S * pl + p, as_);
             if (NPT == 9) {
@@ -494,7 +570,8 @@ __device__ __forceinline__ void relax_line(const LevelArgs<T>& L, int j, int zer
         }
     }
     T x[1][CH];
-    line_solve<T, 1>(lo, dg, up, d, red, x);
+    if constexpr (kFac<T>) line_solve_fac<T, 1>(R, d, red, x);
+    else line_solve<T, 1>(lo, dg, up, d, red, x);
     if (cnt > 0) st4(L.x + p, x[0]);
 }
 
@@ -668,6 +745,7 @@ static int alloc_hierarchy(cth_grid* g) {
     h.b.assign(g->nlev, nullptr);
     h.wS.assign(g->nlev, nullptr);
     h.wN.assign(g->nlev, nullptr);
+    h.fac.assign(g->nlev, nullptr);
     for (int l = 0; l < g->nlev; l++) {
         const size_t n = (size_t)g->nrow[l] * g->ldl;
         const int npt = (l == 0) ? 5 : 9;
@@ -681,6 +759,11 @@ static int alloc_hierarchy(cth_grid* g) {
         CTH_CUDA(cudaMemset(h.b[l], 0, n * sizeof(T)));
         CTH_CUDA(cudaMemset(h.wS[l], 0, n * sizeof(T)));
         CTH_CUDA(cudaMemset(h.wN[l], 0, n * sizeof(T)));
+        if constexpr (kFac<T>) {
+            const size_t nf = (size_t)g->nrow[l] * line_fac_size<T>(g->bd);
+            CTH_CUDA(cudaMalloc(&h.fac[l], nf * sizeof(T)));
+            CTH_CUDA(cudaMemset(h.fac[l], 0, nf * sizeof(T)));
+        }
     }
     h.allocated = true;
     return CTH_OK;
@@ -700,7 +783,15 @@ static LevelArgs<T> level_args(cth_grid* g, int l) {
     L.nrow = g->nrow[l];
     L.ncol = g->ncol;
     L.ld = g->ldl;
+    L.fac = h.fac.empty() ? nullptr : h.fac[l];
     return L;
+}
+
+// dynamic shared memory of a relaxation CTA
+template <typename T>
+static size_t relax_smem(int bd) {
+    if constexpr (kFac<T>) return line_fac_smem<T>();
+    else return line_smem<T>(bd, 1);
 }
 
 template <typename T, int NPT, int NPTF>
@@ -717,7 +808,7 @@ static void launch_relax(cth_grid* g, int l, int parity, int zero_guess, int pro
         pa.wN = h.wN[l];
         pa.nrowc = g->nrow[l + 1];
     }
-    const size_t smem = line_smem<T>(g->bd, 1);
+    const size_t smem = relax_smem<T>(g->bd);
     LevelArgs<T> L = level_args<T>(g, l);
     // algorithmic bytes: 5 coefficients + b + x written + neighbour-row x, per cell
     LevelArgs<T> F = L;
@@ -774,7 +865,7 @@ static void launch_tail(cth_grid* g, int l0, cudaStream_t s) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(TAIL_CTAS);
     cfg.blockDim = dim3(g->bd);
-    cfg.dynamicSmemBytes = line_smem<T>(g->bd, 1);
+    cfg.dynamicSmemBytes = relax_smem<T>(g->bd);
     cfg.stream = s;
     cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -829,23 +920,44 @@ template <typename T>
 static void setup_levels(cth_grid* g, cudaStream_t s) {
     Hierarchy<T>& h = hier<T>(g);
     const int slot = prof_mark(g, PROF_SETUP, 0.0, s);
-    for (int l = 0; l + 1 < g->nlev; l++) {
-        LevelArgs<T> L = level_args<T>(g, l);
-        const int frows = g->nrow[l] / 2;
-        const size_t smem = line_smem<T>(g->bd, 2);
-        if (frows > 0) {
-            if (l == 0) k_weights<T, 5><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
-            else k_weights<T, 9><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
+    if constexpr (kFac<T>) {
+        // per level: factorise every line (and the F-row weights), then the
+        // Galerkin operator of the next level
+        for (int l = 0; l < g->nlev; l++) {
+            LevelArgs<T> L = level_args<T>(g, l);
+            const int wts = l + 1 < g->nlev;
+            if (l == 0) k_factor<T, 5><<<g->nrow[l], g->bd, 0, s>>>(L, g->mask[l], h.fac[l], h.wS[l], h.wN[l], wts);
+            else k_factor<T, 9><<<g->nrow[l], g->bd, 0, s>>>(L, g->mask[l], h.fac[l], h.wS[l], h.wN[l], wts);
+            g->launches++;
+            if (!wts) break;
+            dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
+            if (l == 0)
+                k_galerkin<T, 5><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
+                                                     g->nrow[l + 1], g->mask[l + 1]);
+            else
+                k_galerkin<T, 9><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
+                                                     g->nrow[l + 1], g->mask[l + 1]);
             g->launches++;
         }
-        dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
-        if (l == 0)
-            k_galerkin<T, 5><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
-                                                 g->nrow[l + 1], g->mask[l + 1]);
-        else
-            k_galerkin<T, 9><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
-                                                 g->nrow[l + 1], g->mask[l + 1]);
-        g->launches++;
+    } else {
+        for (int l = 0; l + 1 < g->nlev; l++) {
+            LevelArgs<T> L = level_args<T>(g, l);
+            const int frows = g->nrow[l] / 2;
+            const size_t smem = line_smem<T>(g->bd, 2);
+            if (frows > 0) {
+                if (l == 0) k_weights<T, 5><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
+                else k_weights<T, 9><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
+                g->launches++;
+            }
+            dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
+            if (l == 0)
+                k_galerkin<T, 5><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
+                                                     g->nrow[l + 1], g->mask[l + 1]);
+            else
+                k_galerkin<T, 9><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
+                                                     g->nrow[l + 1], g->mask[l + 1]);
+            g->launches++;
+        }
     }
     prof_done(g, slot, s);
 }
