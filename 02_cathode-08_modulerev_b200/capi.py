@@ -27,7 +27,7 @@ CTH_PREC_MIXED = 1
 # every symbol include/cathode_b200.h declares
 EXPORTS = (
     "cth_version", "cth_last_error", "cth_grid_create", "cth_grid_destroy", "cth_grid_ld",
-    "cth_grid_levels", "cth_grid_set_cycle", "cth_smg_solve", "cth_smg_solve_dev", "cth_sor_solve",
+    "cth_grid_levels", "cth_grid_set_cycle", "cth_smg_solve", "cth_smg_solve_dev", "cth_smg_solve_guess_dev", "cth_sor_solve",
     "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
     "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs", "cth_grid_set_tail",
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
@@ -35,6 +35,9 @@ EXPORTS = (
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
     "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
+    "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_set_params", "cth_unet_get_params",
+    "cth_unet_get_grads", "cth_unet_set_loss_weights", "cth_unet_forward", "cth_unet_backward",
+    "cth_unet_train_step", "cth_unet_set_stats", "cth_unet_features", "cth_unet_predict_dphi",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -48,13 +51,14 @@ class Status(ctypes.Structure):
         ("iterations", ctypes.c_int),
         ("converged", ctypes.c_int),
         ("nonfinite", ctypes.c_int),
-        ("reserved", ctypes.c_int),
+        ("guess", ctypes.c_int),
         ("residual", ctypes.c_double),
         ("initial_residual", ctypes.c_double),
+        ("guess_residual", ctypes.c_double),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class MWParams(ctypes.Structure):
@@ -71,14 +75,15 @@ class PhiParams(ctypes.Structure):
                                                "coefMISEE_ts", "dTe_SEE", "error_cnv_HES_phi",
                                                "error_cnv_SOR_phi")] + \
                [(k, ctypes.c_int) for k in ("maxITR_HES_phi", "maxITR_SOR_phi", "flag_error", "flag_iter_phi",
-                                            "precision")]
+                                            "precision", "warm_start")] + \
+               [("guess_max_relres", ctypes.c_double)]
 
 
 class PCResult(ctypes.Structure):
     _fields_ = [("ncount", ctypes.c_int), ("solver_rc", ctypes.c_int), ("error_phi", ctypes.c_double),
                 ("error_nUex", ctypes.c_double), ("error_nUer", ctypes.c_double),
                 ("error_iter", ctypes.c_double * 3), ("solver", Status), ("Ii_Anode", ctypes.c_double),
-                ("Ie_Anode", ctypes.c_double), ("I_Anode", ctypes.c_double)]
+                ("Ie_Anode", ctypes.c_double), ("I_Anode", ctypes.c_double), ("first", Status)]
 
 
 class SGParams(ctypes.Structure):
@@ -129,7 +134,8 @@ class StepParams(ctypes.Structure):
     _fields_ = [("itime", ctypes.c_int), ("ndt_i", ctypes.c_int), ("ndt_n", ctypes.c_int), ("ndt_m", ctypes.c_int),
                 ("flag_adp_dt", ctypes.c_int), ("dt", ctypes.c_double), ("CFL", ctypes.c_double),
                 ("gtime", ctypes.c_double), ("ion", IonParams), ("phi", PhiParams), ("rhoe", SGParams),
-                ("eps", SGParams), ("neutral", NeutralParams), ("transport", TransportParams)]
+                ("eps", SGParams), ("neutral", NeutralParams), ("transport", TransportParams),
+                ("net", ctypes.c_void_p)]
 
 
 class StepResult(ctypes.Structure):
@@ -223,6 +229,32 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_smg_solve_dev.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                                         _vp, _vp, ctypes.POINTER(Status)]
     L.cth_smg_solve_dev.restype = ctypes.c_int
+    L.cth_smg_solve_guess_dev.argtypes = [_vp] + [_vp] * 7 + [ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                                              ctypes.c_int, _vp, _vp, ctypes.POINTER(Status)]
+    L.cth_smg_solve_guess_dev.restype = ctypes.c_int
+    L.cth_unet_create.argtypes = [ctypes.c_int] * 6
+    L.cth_unet_create.restype = _vp
+    L.cth_unet_destroy.argtypes = [_vp]
+    L.cth_unet_destroy.restype = None
+    L.cth_unet_nparams.argtypes = [_vp]
+    L.cth_unet_nparams.restype = ctypes.c_longlong
+    for f in ("cth_unet_set_params", "cth_unet_get_params", "cth_unet_get_grads"):
+        getattr(L, f).argtypes = [_vp, _vp, ctypes.c_longlong]
+        getattr(L, f).restype = ctypes.c_int
+    for f in ("cth_unet_set_loss_weights", "cth_unet_set_stats"):
+        getattr(L, f).argtypes = [_vp, _vp]
+        getattr(L, f).restype = ctypes.c_int
+    L.cth_unet_forward.argtypes = [_vp, _vp, _vp, _vp]
+    L.cth_unet_forward.restype = ctypes.c_int
+    L.cth_unet_backward.argtypes = [_vp, _vp, _vp]
+    L.cth_unet_backward.restype = ctypes.c_int
+    L.cth_unet_train_step.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_float, ctypes.c_int, _vp,
+                                      ctypes.POINTER(ctypes.c_double)]
+    L.cth_unet_train_step.restype = ctypes.c_int
+    L.cth_unet_features.argtypes = [_vp, _vp, _vp, _vp]
+    L.cth_unet_features.restype = ctypes.c_int
+    L.cth_unet_predict_dphi.argtypes = [_vp, _vp, _vp]
+    L.cth_unet_predict_dphi.restype = ctypes.c_int
     L.cth_sor_solve.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_double, ctypes.c_int, ctypes.c_double, _vp,
                                                     ctypes.POINTER(Status)]
     L.cth_sor_solve.restype = ctypes.c_int

@@ -434,6 +434,23 @@ int cth_smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const dou
                          (cudaStream_t)stream, st);
 }
 
+int cth_smg_solve_guess_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                            const double* aN, const double* aS, const double* b, const double* x0,
+                            double max_guess_relres, int maxITR, double error_cnv, int precision,
+                            double* solution, void* stream, cth_status* st) {
+    if (!g || !aP || !aE || !aW || !aN || !aS || !b || !x0 || !solution || maxITR < 0 ||
+        !(max_guess_relres >= 0.0)) {
+        set_error("cth_smg_solve_guess_dev: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    int pending = 0;
+    const int rc = smg_solve_launch(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, precision, solution,
+                                    (cudaStream_t)stream, &pending, nullptr, x0, max_guess_relres);
+    if (rc < 0) return rc;
+    return solve_finish(g, pending, st);
+}
+
 int cth_sor_solve(cth_grid* g, const double* aP, const double* aE, const double* aW,
                   const double* aN, const double* aS, const double* b, double alpha_SOR,
                   int maxITR, double error_cnv, double* solution, cth_status* st) {

@@ -85,10 +85,14 @@ struct SolveArgs {
     double tol;
     int maxit;
     int pad;
+    const double* x0;   // initial guess (null: zero, the reference's start)
+    double guess_tol;   // the guess is used when ||b - A x0|| <= guess_tol ||b||
 };
 
-// device status words of a solve (double array)
-enum StatWord { ST_RR = 0, ST_RELRES = 1, ST_BB = 2, ST_NONFINITE = 3, ST_ITER = 4, ST_CONV = 5, ST_KEEP = 6 };
+// device status words of a solve (double array).  ST_GUESS: 0 no guess;
+// 1 + r0 guess used; -(1 + r0) guess rejected (r0 = its relative residual)
+enum StatWord { ST_RR = 0, ST_RELRES = 1, ST_BB = 2, ST_NONFINITE = 3, ST_ITER = 4, ST_CONV = 5, ST_KEEP = 6,
+                ST_GUESS = 7 };
 
 struct SolveGraph {
     bool valid = false;
@@ -172,7 +176,8 @@ int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double*
 // read the grid's copy) or, after the caller's own synchronisation, solve_parse(h_dst)
 int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
                      const double* aS, const double* b, int maxITR, double error_cnv, int precision,
-                     double* solution, cudaStream_t s, int* pending, double* h_dst);
+                     double* solution, cudaStream_t s, int* pending, double* h_dst,
+                     const double* x0 = nullptr, double guess_tol = 0.0);
 int solve_finish(cth_grid* g, int pending, cth_status* st);
 int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st);
 int sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,

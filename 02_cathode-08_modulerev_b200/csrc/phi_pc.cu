@@ -333,6 +333,14 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
         return CTH_ERR_ARG;
     }
     double* out = fs->scal + 16;
+    const double* guess = nullptr;
+    double* dphi_prev = nullptr;
+    if (prm->warm_start != 0 && prm->flag_iter_phi != 0) {
+        dphi_prev = field_ptr(fs, "dphi_prev");
+        guess = (prm->warm_start == 1) ? field_ptr(fs, "dphi_guess") : dphi_prev;
+        if (!dphi_prev || !guess) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
+    }
+    cth_status st_first{};
     k_phi_begin<<<grd, blk, 0, s>>>(A);
     g->launches++;
     int ncount = 0, solver_rc = 0;
@@ -353,8 +361,11 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
                                prm->error_cnv_SOR_phi, A.dphi, s, &st_last);
         else
             rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR_phi,
-                                  prm->error_cnv_SOR_phi, prm->precision, A.dphi, s, &pend, fs->h_solve);
+                                  prm->error_cnv_SOR_phi, prm->precision, A.dphi, s, &pend, fs->h_solve,
+                                  ncount == 1 ? guess : nullptr, prm->guess_max_relres);
         if (rc < 0) return rc;
+        if (ncount == 1 && dphi_prev)
+            CTH_CUDA(cudaMemcpyAsync(dphi_prev, A.dphi, g->plane * sizeof(double), cudaMemcpyDeviceToDevice, s));
         k_phi_correct_a<<<grd, blk, 0, s>>>(A);
         k_phi_correct_b<<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out);
         g->launches += 2;
@@ -364,6 +375,7 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
         if (pend) rc = solve_parse(g, pend, fs->h_solve, &st_last);
         if (rc < 0) return rc;
         if (rc > solver_rc) solver_rc = rc;
+        if (ncount == 1) st_first = st_last;
         const double* h = fs->h_scal;
         const int m = prm->flag_error;
         for (int k = 0; k < 3; k++) {
@@ -383,6 +395,7 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
         res->error_iter[1] = e_it[1];
         res->error_iter[2] = e_it[2];
         res->solver = st_last;
+        res->first = st_first;
         res->Ii_Anode = res->Ie_Anode = res->I_Anode = 0.0;
     }
     return CTH_OK;
@@ -392,7 +405,8 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
 
 extern "C" int cth_solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, void* stream, cth_pc_result* res) {
     if (!fs || !prm || prm->dx <= 0.0 || prm->dr <= 0.0 || prm->maxITR_HES_phi < 1 || prm->flag_error < 0 ||
-        prm->flag_error > 3) {
+        prm->flag_error > 3 || prm->warm_start < 0 || prm->warm_start > 2 ||
+        (prm->warm_start != 0 && !(prm->guess_max_relres >= 0.0))) {
         cth::set_error("cth_solve_phi_pc: invalid arguments");
         return CTH_ERR_ARG;
     }

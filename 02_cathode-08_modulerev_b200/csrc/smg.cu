@@ -47,15 +47,62 @@ template <typename T> constexpr bool kFac = !std::is_same<T, cd>::value;
 // identity), b0 = b (grid cells); the last block records ||b||^2 and whether
 // the cycle loop runs at all (sets the graph's loop condition when use_cond).
 // ---------------------------------------------------------------------------
+// FP64 residual r = b - A x0 of one grid cell (couplings to non-grid cells dropped)
+__device__ __forceinline__ double guess_resid(const SolveArgs* __restrict__ args,
+                                              const unsigned char* __restrict__ mask, size_t p, size_t q,
+                                              int c, int r, int ncol, int nrow, int ldl, int ld_u) {
+    const double* x0 = args->x0;
+    double v = args->b[q] - args->aP[q] * x0[q];
+    if (c > 0 && mask[p - 1]) v += args->aW[q] * x0[q - 1];
+    if (c + 1 < ncol && mask[p + 1]) v += args->aE[q] * x0[q + 1];
+    if (r > 0 && mask[p - ldl]) v += args->aS[q] * x0[q - ld_u];
+    if (r + 1 < nrow && mask[p + ldl]) v += args->aN[q] * x0[q + ld_u];
+    return v;
+}
+
+// Initial-guess test: ||b - A x0||^2 and ||b||^2 over the grid cells; the last
+// block records in ST_GUESS whether k_prep0 starts from x0 (relative residual
+// at most guess_tol) or from zero.  No guess: one thread writes 0.
+__global__ void k_guess(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask, int ld_u,
+                        int i0, int j0, int ncol, int nrow, int ldl, double* __restrict__ part,
+                        unsigned int* counter, double* __restrict__ stat) {
+    __shared__ double red[32];
+    if (args->x0 == nullptr) {
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) stat[ST_GUESS] = 0.0;
+        return;
+    }
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    double v[2] = {0.0, 0.0};
+    if (c < ncol) {
+        const size_t p = (size_t)r * ldl + c;
+        const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
+        if (mask[p]) {
+            const double rv = guess_resid(args, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
+            const double bv = args->b[q];
+            v[0] = rv * rv;
+            v[1] = bv * bv;
+        }
+    }
+    double tot[2];
+    if (last_block_sumk<2>(v, part, counter, red, tot) && threadIdx.x == 0) {
+        const double r0 = (tot[1] > 0.0) ? sqrt(tot[0] / tot[1]) : 0.0;
+        const bool use = isfinite(tot[0]) && tot[1] > 0.0 && r0 <= args->guess_tol;
+        stat[ST_GUESS] = use ? 1.0 + r0 : -(1.0 + (isfinite(r0) ? r0 : 0.0));
+    }
+}
+
 template <typename T>
 __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask,
                         int ld_u, int i0, int j0, int ncol, int nrow, int ldl, T* __restrict__ a0,
-                        T* __restrict__ b0, double* __restrict__ part, unsigned int* counter,
-                        double* __restrict__ stat, cudaGraphConditionalHandle cond, int use_cond) {
+                        T* __restrict__ b0, double* __restrict__ x64, double* __restrict__ part,
+                        unsigned int* counter, double* __restrict__ stat, cudaGraphConditionalHandle cond,
+                        int use_cond) {
     __shared__ double red[32];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
-    double bb = 0.0;
+    const bool guess = stat[ST_GUESS] >= 1.0;
+    double v2[2] = {0.0, 0.0};  // ||r0||^2, ||b||^2
     if (c < ncol) {
         const double* __restrict__ aP = args->aP;
         const size_t plane = (size_t)nrow * ldl;
@@ -69,8 +116,16 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
             if (r > 0 && mask[p - ldl]) vS = (T)args->aS[q];
             if (r + 1 < nrow && mask[p + ldl]) vN = (T)args->aN[q];
             const double bv = args->b[q];
-            vb = (T)bv;
-            bb = bv * bv;
+            v2[1] = bv * bv;
+            if (guess) {
+                const double rv = guess_resid(args, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
+                vb = (T)rv;
+                v2[0] = rv * rv;
+                x64[p] = args->x0[q];
+            } else {
+                vb = (T)bv;
+                v2[0] = v2[1];
+            }
         }
         a0[P * plane + p] = vP;
         a0[W * plane + p] = vW;
@@ -79,16 +134,20 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
         a0[N * plane + p] = vN;
         b0[p] = vb;
     }
-    double tot;
-    if (last_block_sum(bb, part, counter, red, &tot) && threadIdx.x == 0) {
-        const bool fin = isfinite(tot);
-        const bool keep = fin && tot > 0.0 && args->maxit > 0;
-        stat[ST_RR] = tot;
-        stat[ST_BB] = tot;
-        stat[ST_RELRES] = (tot > 0.0) ? 1.0 : 0.0;
+    double t2[2];
+    if (last_block_sumk<2>(v2, part, counter, red, t2) && threadIdx.x == 0) {
+        const double rr = t2[0], bb = t2[1];
+        const bool fin = isfinite(rr) && isfinite(bb);
+        // from zero: run at least one cycle (reference SMG); from a guess: stop
+        // at once when it already meets the tolerance
+        const bool met = guess && rr <= args->tol * args->tol * bb;
+        const bool keep = fin && rr > 0.0 && args->maxit > 0 && !met;
+        stat[ST_RR] = rr;
+        stat[ST_BB] = bb;
+        stat[ST_RELRES] = (bb > 0.0) ? sqrt(rr / bb) : 0.0;
         stat[ST_NONFINITE] = fin ? 0.0 : 1.0;
         stat[ST_ITER] = 0.0;
-        stat[ST_CONV] = (fin && tot == 0.0) ? 1.0 : 0.0;
+        stat[ST_CONV] = (fin && (rr == 0.0 || met)) ? 1.0 : 0.0;
         stat[ST_KEEP] = keep ? 1.0 : 0.0;
         if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
     }
@@ -970,13 +1029,15 @@ static int enqueue_pre(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle c
     Workspace& w = g->ws;
     const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
     dim3 blk(256), grd((ncol + 255) / 256, nrow0);
+    cudaMemsetAsync(w.x64[0], 0, sizeof(double) * (size_t)nrow0 * ldl, s);
+    k_guess<<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, w.part, w.counter,
+                                w.stat);
     k_prep0<T><<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, h.a[0],
-                                   h.b[0], w.part, w.counter, w.stat, cond, use_cond);
+                                   h.b[0], w.x64[0], w.part, w.counter, w.stat, cond, use_cond);
     const long long l0 = g->launches;
     setup_levels<T>(g, s);
-    const int n = 1 + (int)(g->launches - l0);
+    const int n = 2 + (int)(g->launches - l0);
     g->launches = l0;
-    cudaMemsetAsync(w.x64[0], 0, sizeof(double) * (size_t)nrow0 * ldl, s);
     return n;
 }
 
@@ -1075,14 +1136,14 @@ template <typename T>
 static int solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW,
                         const double* aN, const double* aS, const double* b, int maxITR,
                         double tol, double* solution, cudaStream_t s, int prec, int* pending,
-                        double* h_dst) {
+                        double* h_dst, const double* x0, double guess_tol) {
     *pending = 0;
     int rc = alloc_hierarchy<T>(g);
     if (rc != CTH_OK) return rc;
     Workspace& w = g->ws;
     {
         dim3 grd((g->ncol + 255) / 256, g->nrow[0]);
-        if ((int)(grd.x * grd.y) > w.npart) {
+        if (2 * (int)(grd.x * grd.y) > w.npart) {
             set_error("partial-sum buffer too small");
             return CTH_ERR_ALLOC;
         }
@@ -1092,6 +1153,8 @@ static int solve_launch(cth_grid* g, const double* aP, const double* aE, const d
     ha->solution = solution;
     ha->tol = tol;
     ha->maxit = maxITR;
+    ha->x0 = x0;
+    ha->guess_tol = guess_tol;
     k_set_args<<<1, 1, 0, s>>>(*ha, w.d_args);
     const bool graph = g->use_graphs && !g->prof.on;
     if (graph) {
@@ -1132,6 +1195,9 @@ int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st) {
     loc.residual = h[ST_RELRES];
     loc.nonfinite = h[ST_NONFINITE] != 0.0;
     loc.converged = h[ST_CONV] != 0.0;
+    const double gw = h[ST_GUESS];
+    loc.guess = gw >= 1.0 ? 1 : (gw <= -1.0 ? -1 : 0);
+    loc.guess_residual = gw >= 1.0 ? gw - 1.0 : (gw <= -1.0 ? -gw - 1.0 : -1.0);
     if (st) *st = loc;
     if (loc.nonfinite) return CTH_NONFINITE;
     return loc.converged ? CTH_OK : CTH_NOT_CONVERGED;
@@ -1144,13 +1210,14 @@ int solve_finish(cth_grid* g, int pending, cth_status* st) {
 
 int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
                      const double* aS, const double* b, int maxITR, double error_cnv, int precision,
-                     double* solution, cudaStream_t s, int* pending, double* h_dst) {
+                     double* solution, cudaStream_t s, int* pending, double* h_dst, const double* x0,
+                     double guess_tol) {
     if (precision == CTH_PREC_MIXED)
         return solve_launch<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending,
-                                   h_dst);
+                                   h_dst, x0, guess_tol);
     if (precision == CTH_PREC_FP64)
         return solve_launch<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending,
-                                    h_dst);
+                                    h_dst, x0, guess_tol);
     set_error("unknown precision mode");
     return CTH_ERR_ARG;
 }

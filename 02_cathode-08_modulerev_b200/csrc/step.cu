@@ -39,6 +39,10 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
         R->ran_ion = 1;
         if (R->ion.solver_rc > worst) worst = R->ion.solver_rc;
     }
+    if (p->net && p->phi.warm_start == 1) {
+        rc = cth_unet_predict_dphi(p->net, fs, stream);
+        if (rc < 0) return rc;
+    }
     rc = cth_solve_phi_pc(fs, &p->phi, stream, &R->phi);
     if (rc < 0) return rc;
     if (R->phi.solver_rc > worst) worst = R->phi.solver_rc;

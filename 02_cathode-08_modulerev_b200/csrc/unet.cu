@@ -1,0 +1,953 @@
+// unet.cu — the learned warm start: a 4-level convolutional U-Net trained on
+// snapshots that the plain solver generates, predicting the first potential
+// correction of a time step (and the microwave field) as an initial guess for
+// the multigrid, which then converges to the unchanged tolerance.  The network
+// has no counterpart in the reference.
+//
+// Tensors are NHWC bfloat16 (channels innermost, a channel stride per tensor so
+// that the skip connections live inside the concatenation buffers), weights
+// [Cout][3][3][Cin] bfloat16 with FP32 master copies, FP32 accumulation.
+// Convolutions are implicit GEMMs on the tensor cores (mma.sync m16n8k16 bf16):
+//   forward       D[pixel][co] = sum_{tap,ci} X[pixel+tap][ci] W[co][tap][ci]
+//   input grad    the forward kernel with W'[ci][tap][co] = W[co][8-tap][ci]
+//   weight grad   dW[co][tap][ci] = sum_pixel dY[pixel][co] X[pixel+tap][ci]
+// The ReLU derivative is applied by every kernel that writes a gradient into a
+// ReLU output (gate = that output > 0), so no pre-activations are stored.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fluid.cuh"
+
+typedef __nv_bfloat16 bf16;
+
+namespace cth {
+namespace unet {
+
+constexpr int TH = 8, TW = 16;           // output tile of a conv CTA (pixels)
+constexpr int HP = TH + 2, WP = TW + 2;  // with the 3x3 halo
+constexpr int SR16 = 24;                 // smem row stride (bf16) of 16-channel rows: 48 B
+constexpr int SR32 = 40;                 // smem row stride (bf16) of 32-channel rows: 80 B
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+__device__ __forceinline__ void mma16816(float c[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// a channel slice of an NHWC tensor
+struct TensorRef {
+    bf16* p;
+    int cs;    // channel stride (pixel pitch)
+    int coff;  // first channel
+};
+
+struct ConvArgs {
+    const bf16* in;
+    int in_cs, in_coff, Cin;
+    const bf16* w;       // [Cout][9][Cin]
+    const float* bias;   // null: none
+    bf16* out;
+    int out_cs, out_coff, Cout;
+    int H, W;
+    int relu;
+    const bf16* gate;    // null: none; else out *= (gate > 0)
+    int gate_cs, gate_coff;
+    int accumulate;      // add to the existing output
+};
+
+// 3x3 convolution, SAME zero padding.  CTA: 8 x 16 output pixels x 32 output
+// channels, 4 warps (two image rows each); Cin in chunks of 16 staged in
+// shared memory with the halo.
+__global__ void __launch_bounds__(128) k_conv3_fwd(ConvArgs a) {
+    __shared__ alignas(16) bf16 s_in[HP * WP * SR16];
+    __shared__ alignas(16) bf16 s_w[32 * 9 * SR16];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH, co0 = blockIdx.z * 32;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) acc[i][j][k] = 0.f;
+    for (int c0 = 0; c0 < a.Cin; c0 += 16) {
+        for (int idx = tid; idx < HP * WP * 2; idx += 128) {
+            const int pix = idx >> 1, half = idx & 1;
+            const int gy = y0 + pix / WP - 1, gx = x0 + pix % WP - 1;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W)
+                v = *reinterpret_cast<const uint4*>(a.in + ((size_t)gy * a.W + gx) * a.in_cs + a.in_coff + c0 +
+                                                    half * 8);
+            *reinterpret_cast<uint4*>(s_in + pix * SR16 + half * 8) = v;
+        }
+        for (int idx = tid; idx < 32 * 9 * 2; idx += 128) {
+            const int row = idx >> 1, half = idx & 1;
+            const int co = co0 + row / 9, tap = row % 9;
+            const uint4 v = *reinterpret_cast<const uint4*>(a.w + ((size_t)co * 9 + tap) * a.Cin + c0 + half * 8);
+            *reinterpret_cast<uint4*>(s_w + row * SR16 + half * 8) = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int tap = 0; tap < 9; tap++) {
+            const int dy = tap / 3, dx = tap % 3;
+            uint32_t b[4][2];
+#pragma unroll
+            for (int nb = 0; nb < 2; nb++) {
+                const int m = lane >> 3, r = lane & 7;
+                const int col = nb * 16 + (m >> 1) * 8 + r;
+                const int koff = (m & 1) * 8;
+                ldsm_x4(smem_u32(s_w + (col * 9 + tap) * SR16 + koff), b[2 * nb][0], b[2 * nb][1],
+                        b[2 * nb + 1][0], b[2 * nb + 1][1]);
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++) {
+                const int ry = warp * 2 + mt;
+                const int m = lane >> 3, r = lane & 7;
+                const int px = (m & 1) * 8 + r, koff = (m >> 1) * 8;
+                uint32_t a0, a1, a2, a3;
+                ldsm_x4(smem_u32(s_in + ((ry + dy) * WP + px + dx) * SR16 + koff), a0, a1, a2, a3);
+#pragma unroll
+                for (int nt = 0; nt < 4; nt++) mma16816(acc[mt][nt], a0, a1, a2, a3, b[nt][0], b[nt][1]);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+        const int gy = y0 + warp * 2 + mt;
+        if (gy >= a.H) continue;
+#pragma unroll
+        for (int hf = 0; hf < 2; hf++) {
+            const int gx = x0 + (lane >> 2) + hf * 8;
+            if (gx >= a.W) continue;
+            const size_t pix = (size_t)gy * a.W + gx;
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++) {
+                const int co = co0 + nt * 8 + 2 * (lane & 3);
+                float v0 = acc[mt][nt][2 * hf], v1 = acc[mt][nt][2 * hf + 1];
+                if (a.bias) { v0 += a.bias[co]; v1 += a.bias[co + 1]; }
+                if (a.relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+                if (a.gate) {
+                    const __nv_bfloat162 g =
+                        *reinterpret_cast<const __nv_bfloat162*>(a.gate + pix * a.gate_cs + a.gate_coff + co);
+                    if (!(__bfloat162float(g.x) > 0.f)) v0 = 0.f;
+                    if (!(__bfloat162float(g.y) > 0.f)) v1 = 0.f;
+                }
+                __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(a.out + pix * a.out_cs + a.out_coff + co);
+                if (a.accumulate) {
+                    const __nv_bfloat162 q = *o;
+                    v0 += __bfloat162float(q.x);
+                    v1 += __bfloat162float(q.y);
+                }
+                *o = __floats2bfloat162_rn(v0, v1);
+            }
+        }
+    }
+}
+
+struct WgradArgs {
+    const bf16* dy;
+    int dy_cs, dy_coff, Cout;
+    const bf16* in;
+    int in_cs, in_coff, Cin;
+    int H, W;
+    float* dw;   // [Cout][9][Cin], accumulated
+    int patches_per_cta;
+};
+
+// weight gradient: CTA = 32 output channels x 32 input channels x 9 taps (one
+// warp per tap) over a run of 8 x 16 pixel patches; partial sums are added to
+// dw with FP32 atomics.
+__global__ void __launch_bounds__(288) k_conv3_wgrad(WgradArgs a) {
+    __shared__ alignas(16) bf16 s_dy[TH * TW * SR32];
+    __shared__ alignas(16) bf16 s_in[HP * WP * SR32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int co0 = blockIdx.y * 32, ci0 = blockIdx.z * 32;
+    const int npx = (a.W + TW - 1) / TW, npy = (a.H + TH - 1) / TH, npatch = npx * npy;
+    const int tap = warp, dy_ = tap / 3, dx_ = tap % 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) acc[i][j][k] = 0.f;
+    const int p_begin = blockIdx.x * a.patches_per_cta;
+    const int p_end = min(npatch, p_begin + a.patches_per_cta);
+    for (int pt = p_begin; pt < p_end; pt++) {
+        const int y0 = (pt / npx) * TH, x0 = (pt % npx) * TW;
+        for (int idx = tid; idx < TH * TW * 4; idx += 288) {
+            const int pix = idx >> 2, q = idx & 3;
+            const int gy = y0 + pix / TW, gx = x0 + pix % TW;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy < a.H && gx < a.W)
+                v = *reinterpret_cast<const uint4*>(a.dy + ((size_t)gy * a.W + gx) * a.dy_cs + a.dy_coff + co0 + q * 8);
+            *reinterpret_cast<uint4*>(s_dy + pix * SR32 + q * 8) = v;
+        }
+        for (int idx = tid; idx < HP * WP * 4; idx += 288) {
+            const int pix = idx >> 2, q = idx & 3;
+            const int gy = y0 + pix / WP - 1, gx = x0 + pix % WP - 1;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W)
+                v = *reinterpret_cast<const uint4*>(a.in + ((size_t)gy * a.W + gx) * a.in_cs + a.in_coff + ci0 + q * 8);
+            *reinterpret_cast<uint4*>(s_in + pix * SR32 + q * 8) = v;
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int r = 0; r < TH; r++) {
+            const int m = lane >> 3, rr = lane & 7;
+            uint32_t af[2][4];
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++) {
+                const int px = (m >> 1) * 8 + rr, coff = mt * 16 + (m & 1) * 8;
+                ldsm_x4_t(smem_u32(s_dy + (r * TW + px) * SR32 + coff), af[mt][0], af[mt][1], af[mt][2],
+                          af[mt][3]);
+            }
+            uint32_t bfr[4][2];
+#pragma unroll
+            for (int nb = 0; nb < 2; nb++) {
+                const int px = (m & 1) * 8 + rr, cioff = nb * 16 + (m >> 1) * 8;
+                ldsm_x4_t(smem_u32(s_in + ((r + dy_) * WP + px + dx_) * SR32 + cioff), bfr[2 * nb][0],
+                          bfr[2 * nb][1], bfr[2 * nb + 1][0], bfr[2 * nb + 1][1]);
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+                for (int nt = 0; nt < 4; nt++)
+                    mma16816(acc[mt][nt], af[mt][0], af[mt][1], af[mt][2], af[mt][3], bfr[nt][0], bfr[nt][1]);
+        }
+        __syncthreads();
+    }
+    if (p_begin >= p_end) return;
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int hf = 0; hf < 2; hf++) {
+                const int co = co0 + mt * 16 + (lane >> 2) + hf * 8;
+                const int ci = ci0 + nt * 8 + 2 * (lane & 3);
+                float* d = a.dw + ((size_t)co * 9 + tap) * a.Cin + ci;
+                atomicAdd(d, acc[mt][nt][2 * hf]);
+                atomicAdd(d + 1, acc[mt][nt][2 * hf + 1]);
+            }
+}
+
+// bias gradient db[c] += sum over pixels of dy[.][c]; 256 threads, C <= 512
+__global__ void k_bias_grad(const bf16* __restrict__ dy, int cs, int coff, int C, int npix, int ppb,
+                            float* __restrict__ db) {
+    const int c = threadIdx.x;
+    const int p0 = blockIdx.x * ppb, p1 = min(npix, p0 + ppb);
+    for (int cc = c; cc < C; cc += blockDim.x) {
+        float s = 0.f;
+        for (int p = p0; p < p1; p++) s += __bfloat162float(dy[(size_t)p * cs + coff + cc]);
+        atomicAdd(db + cc, s);
+    }
+}
+
+// W'[ci][tap][co] = W[co][8-tap][ci]
+__global__ void k_wtrans(const bf16* __restrict__ w, int Cout, int Cin, bf16* __restrict__ wt) {
+    const size_t n = (size_t)Cout * 9 * Cin;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int ci = (int)(e % Cin);
+        const int tap = (int)((e / Cin) % 9);
+        const int co = (int)(e / ((size_t)Cin * 9));
+        wt[((size_t)ci * 9 + (8 - tap)) * Cout + co] = w[e];
+    }
+}
+
+// 2x2 average pooling: out[y][x][c] = mean of in[2y..2y+1][2x..2x+1][c]
+__global__ void k_pool2(const bf16* __restrict__ in, int in_cs, int in_coff, int C, int Ho, int Wo,
+                        bf16* __restrict__ out, int out_cs) {
+    const size_t n = (size_t)Ho * Wo * C;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const size_t pix = e / C;
+        const int y = (int)(pix / Wo), x = (int)(pix % Wo);
+        const int Wi = 2 * Wo;
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            s += __bfloat162float(in[((size_t)(2 * y + (k >> 1)) * Wi + 2 * x + (k & 1)) * in_cs + in_coff + c]);
+        out[pix * out_cs + c] = __float2bfloat16_rn(0.25f * s);
+    }
+}
+
+// gradient of k_pool2 added into the ReLU output it pooled:
+// din[2y+a][2x+b][c] += dout[y][x][c] / 4 where x_in > 0
+__global__ void k_pool2_bwd(const bf16* __restrict__ dout, int dout_cs, int C, int Ho, int Wo,
+                            bf16* __restrict__ din, int din_cs, int din_coff, const bf16* __restrict__ gate,
+                            int gate_cs, int gate_coff) {
+    const int Wi = 2 * Wo;
+    const size_t n = (size_t)4 * Ho * Wo * C;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const size_t pi = e / C;
+        const int yi = (int)(pi / Wi), xi = (int)(pi % Wi);
+        const float g = 0.25f * __bfloat162float(dout[((size_t)(yi >> 1) * Wo + (xi >> 1)) * dout_cs + c]);
+        const bool on = __bfloat162float(gate[pi * gate_cs + gate_coff + c]) > 0.f;
+        bf16* d = din + pi * din_cs + din_coff + c;
+        *d = __float2bfloat16_rn(__bfloat162float(*d) + (on ? g : 0.f));
+    }
+}
+
+// nearest 2x upsampling into a channel slice: out[y][x][c] = in[y/2][x/2][c]
+__global__ void k_up2(const bf16* __restrict__ in, int in_cs, int C, int Hi, int Wi, bf16* __restrict__ out,
+                      int out_cs, int out_coff) {
+    const int Wo = 2 * Wi;
+    const size_t n = (size_t)4 * Hi * Wi * C;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const size_t po = e / C;
+        const int y = (int)(po / Wo), x = (int)(po % Wo);
+        out[po * out_cs + out_coff + c] = in[((size_t)(y >> 1) * Wi + (x >> 1)) * in_cs + c];
+    }
+}
+
+// gradient of k_up2: din[y][x][c] = sum of the 4 children's gradients
+__global__ void k_up2_bwd(const bf16* __restrict__ dout, int dout_cs, int dout_coff, int C, int Hi, int Wi,
+                          bf16* __restrict__ din, int din_cs) {
+    const int Wo = 2 * Wi;
+    const size_t n = (size_t)Hi * Wi * C;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const size_t pi = e / C;
+        const int y = (int)(pi / Wi), x = (int)(pi % Wi);
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            s += __bfloat162float(dout[((size_t)(2 * y + (k >> 1)) * Wo + 2 * x + (k & 1)) * dout_cs + dout_coff + c]);
+        din[pi * din_cs + c] = __float2bfloat16_rn(s);
+    }
+}
+
+// FP32 NHWC input (cin channels) -> bf16 with cpad channels (zeros beyond cin)
+__global__ void k_pack(const float* __restrict__ in, int cin, int npix, int cpad, bf16* __restrict__ out) {
+    const size_t n = (size_t)npix * cpad;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % cpad);
+        const size_t p = e / cpad;
+        out[e] = __float2bfloat16_rn(c < cin ? in[p * cin + c] : 0.f);
+    }
+}
+
+// 1x1 output layer (linear): out[p][c] = sum_k wh[c][k] y[p][k] + bh[c], FP32
+__global__ void k_head_fwd(const bf16* __restrict__ y, int C, int npix, const float* __restrict__ wh,
+                           const float* __restrict__ bh, int cout, float* __restrict__ out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    for (int c = 0; c < cout; c++) {
+        float s = bh[c];
+        for (int k = 0; k < C; k++) s += wh[c * C + k] * __bfloat162float(y[(size_t)p * C + k]);
+        out[(size_t)p * cout + c] = s;
+    }
+}
+
+// backward of the output layer: dy = wh^T dout where y > 0 (bf16), dwh, dbh
+// accumulated per block (shared memory) and added with atomics.  C, cout <= 32.
+__global__ void k_head_bwd(const bf16* __restrict__ y, int C, int npix, const float* __restrict__ wh, int cout,
+                           const float* __restrict__ dout, bf16* __restrict__ dy, float* __restrict__ dwh,
+                           float* __restrict__ dbh) {
+    __shared__ float s_dw[32 * 33];
+    for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) s_dw[e] = 0.f;
+    __syncthreads();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < npix) {
+        float d[32];
+        for (int c = 0; c < cout; c++) d[c] = dout[(size_t)p * cout + c];
+        for (int k = 0; k < C; k++) {
+            const float yk = __bfloat162float(y[(size_t)p * C + k]);
+            float g = 0.f;
+            for (int c = 0; c < cout; c++) {
+                g += wh[c * C + k] * d[c];
+                atomicAdd(&s_dw[c * 33 + k], d[c] * yk);
+            }
+            dy[(size_t)p * C + k] = __float2bfloat16_rn(yk > 0.f ? g : 0.f);
+        }
+        for (int c = 0; c < cout; c++) atomicAdd(&s_dw[c * 33 + 32], d[c]);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < cout * 33; e += blockDim.x) {
+        const int c = e / 33, k = e % 33;
+        if (k < C) atomicAdd(dwh + c * C + k, s_dw[e]);
+        else if (k == 32) atomicAdd(dbh + c, s_dw[e]);
+    }
+}
+
+// weighted masked MSE: loss = sum_p m_p sum_c w_c (o - t)^2 / sum_p m_p,
+// dout = dloss/do; msum = sum_p m_p (host value)
+__global__ void k_mse(const float* __restrict__ o, const float* __restrict__ t, const float* __restrict__ m, int npix,
+                      int cout, const float* __restrict__ cw, double inv_msum, float* __restrict__ dout,
+                      double* __restrict__ loss) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        const float mp = m[p];
+        for (int c = 0; c < cout; c++) {
+            const float diff = o[(size_t)p * cout + c] - t[(size_t)p * cout + c];
+            acc += (double)mp * cw[c] * diff * diff;
+            dout[(size_t)p * cout + c] = (float)(2.0 * mp * cw[c] * diff * inv_msum);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
+        atomicAdd(loss, s * inv_msum);
+    }
+}
+
+// Adam on the FP32 master parameters; bf16 copies of the conv weights follow
+__global__ void k_adam(float* __restrict__ prm, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, size_t n, float lr, float b1, float b2, float eps, float c1, float c2) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const float gi = g[e];
+        const float mi = b1 * m[e] + (1.f - b1) * gi;
+        const float vi = b2 * v[e] + (1.f - b2) * gi * gi;
+        m[e] = mi;
+        v[e] = vi;
+        prm[e] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+    }
+}
+
+__global__ void k_to_bf16(const float* __restrict__ src, bf16* __restrict__ dst, size_t n) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        dst[e] = __float2bfloat16_rn(src[e]);
+}
+
+// normalisation of the network's input and output channels
+struct Stats {
+    float in_mean[6], in_std[6], out_mean[3], out_std[3];
+};
+
+// input channels of the warm-start network from the field planes (library
+// layout, grid cell (i, j) -> pixel (j-1, i-1)): log10 n_e, log10 nu_m, |B|,
+// Re / Im of the microwave field (zero here), previous potential correction;
+// normalised, zero outside the grid
+__global__ void k_features(const double* __restrict__ rhoe, const double* __restrict__ nu_m,
+                           const double* __restrict__ Bx, const double* __restrict__ Br,
+                           const double* __restrict__ dphi_prev, int ni, int nj, int ld, int H, int W, Stats st,
+                           float* __restrict__ out) {
+    const int npix = H * W;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npix; q += gridDim.x * blockDim.x) {
+        const int y = q / W, x = q % W;
+        float f[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (y < nj && x < ni) {
+            const size_t p = (size_t)(y + 1) * ld + (x + 1);
+            f[0] = (float)log10(fmax(rhoe[p], 1.0));
+            f[1] = (float)log10(fmax(nu_m[p], 1.0));
+            f[2] = (float)sqrt(Bx[p] * Bx[p] + Br[p] * Br[p]);
+            f[5] = (float)dphi_prev[p];
+#pragma unroll
+            for (int c = 0; c < 6; c++) f[c] = (f[c] - st.in_mean[c]) / st.in_std[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 6; c++) out[(size_t)q * 6 + c] = f[c];
+    }
+}
+
+// guess = base + channel c of the network output (de-normalised) in the grid
+// cells: the network predicts the change from the previous step's correction
+__global__ void k_unpack(const float* __restrict__ o, int cout, int c, int ni, int nj, int ld, int W, float om,
+                         float os, const double* __restrict__ base, double* __restrict__ dst) {
+    const int n = ni * nj;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int y = q / ni, x = q % ni;
+        const size_t p = (size_t)(y + 1) * ld + (x + 1);
+        dst[p] = base[p] + (double)(o[((size_t)y * W + x) * cout + c] * os + om);
+    }
+}
+
+inline dim3 grid1(size_t n, int bs = 256) {
+    size_t b = (n + bs - 1) / bs;
+    if (b > 148 * 32) b = 148 * 32;
+    if (b < 1) b = 1;
+    return dim3((unsigned)b);
+}
+
+}  // namespace unet
+}  // namespace cth
+
+using namespace cth;
+using namespace cth::unet;
+
+// ---------------------------------------------------------------------------
+// the network object
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Conv {
+    int cin, cout, H, W;
+    size_t w_off, b_off;  // into the FP32 parameter vector (weights [cout][9][cin], bias [cout])
+    size_t wb_off;        // into the bf16 weight vector
+    TensorRef in, out;    // forward operands
+    TensorRef din, dout;  // gradients (din.p null: not needed)
+    const bf16* out_gate_for_din;  // ReLU output that din belongs to (null: din is not gated)
+    int din_accumulate;
+};
+
+}  // namespace
+
+struct cth_unet {
+    int device = 0;
+    int H = 0, W = 0, cin = 0, cout = 0, base = 0;
+    int cpad = 32;
+    std::vector<Conv> convs;
+    size_t nparam = 0, nw_bf16 = 0;
+    size_t head_w = 0, head_b = 0;
+    float* prm = nullptr;  // FP32 master parameters
+    float* grad = nullptr;
+    float* adam_m = nullptr;
+    float* adam_v = nullptr;
+    bf16* wb = nullptr;    // bf16 conv weights
+    bf16* wt = nullptr;    // transposed / flipped conv weights (input gradients)
+    std::vector<void*> bufs;
+    bf16* x_in = nullptr;  // packed input
+    bf16* y_last = nullptr;  // last decoder activation (input of the head)
+    bf16* dy_last = nullptr;
+    float* out = nullptr;    // last forward output (FP32 NHWC)
+    float* dout = nullptr;
+    double* loss = nullptr;
+    float* cw = nullptr;     // per-output-channel loss weights
+    Stats stats{};
+    float* feat = nullptr;   // input features of the warm-start prediction
+    struct Pool { TensorRef src; bf16* dst; int C, Ho, Wo; bf16* ddst; };
+    struct Up { bf16* src; int C, Hi, Wi; TensorRef dst; bf16* dsrc; TensorRef ddst; };
+    std::vector<Pool> pools;
+    std::vector<Up> ups;
+};
+
+namespace {
+
+bf16* alloc_bf16(cth_unet* n, size_t count) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, count * sizeof(bf16)) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, count * sizeof(bf16));
+    n->bufs.push_back(p);
+    return (bf16*)p;
+}
+
+// forward order of the layers (indices into convs):
+//   0 e0a 1 e0b | 2 e1a 3 e1b | 4 e2a 5 e2b | 6 ba 7 bb | 8 d2a 9 d2b | 10 d1a 11 d1b | 12 d0a 13 d0b
+int build(cth_unet* n) {
+    const int H0 = n->H, W0 = n->W, B = n->base;
+    const int Hs[4] = {H0, H0 / 2, H0 / 4, H0 / 8}, Ws[4] = {W0, W0 / 2, W0 / 4, W0 / 8};
+    const int C[4] = {B, 2 * B, 4 * B, 8 * B};
+    auto px = [&](int l) { return (size_t)Hs[l] * Ws[l]; };
+    n->x_in = alloc_bf16(n, px(0) * n->cpad);
+    // activations and their gradients
+    bf16 *e_a[3], *cat[3], *pool[3], *d_a[3], *d_b[3];
+    bf16 *ge_a[3], *gcat[3], *gpool[3], *gd_a[3], *gd_b[3];
+    for (int l = 0; l < 3; l++) {
+        e_a[l] = alloc_bf16(n, px(l) * C[l]);
+        cat[l] = alloc_bf16(n, px(l) * 3 * C[l]);
+        pool[l] = alloc_bf16(n, px(l + 1) * C[l]);
+        d_a[l] = alloc_bf16(n, px(l) * C[l]);
+        d_b[l] = alloc_bf16(n, px(l) * C[l]);
+        ge_a[l] = alloc_bf16(n, px(l) * C[l]);
+        gcat[l] = alloc_bf16(n, px(l) * 3 * C[l]);
+        gpool[l] = alloc_bf16(n, px(l + 1) * C[l]);
+        gd_a[l] = alloc_bf16(n, px(l) * C[l]);
+        gd_b[l] = alloc_bf16(n, px(l) * C[l]);
+    }
+    bf16* ba = alloc_bf16(n, px(3) * C[3]);
+    bf16* bb = alloc_bf16(n, px(3) * C[3]);
+    bf16* gba = alloc_bf16(n, px(3) * C[3]);
+    bf16* gbb = alloc_bf16(n, px(3) * C[3]);
+    for (void* p : n->bufs)
+        if (!p) return CTH_ERR_ALLOC;
+    size_t off = 0, woff = 0;
+    auto add = [&](int cin, int cout, int l, TensorRef in, TensorRef out, TensorRef din, TensorRef dout,
+                   const bf16* gate, int acc) {
+        Conv c;
+        c.cin = cin; c.cout = cout; c.H = Hs[l]; c.W = Ws[l];
+        c.w_off = off; off += (size_t)cout * 9 * cin;
+        c.b_off = off; off += cout;
+        c.wb_off = woff; woff += (size_t)cout * 9 * cin;
+        c.in = in; c.out = out; c.din = din; c.dout = dout;
+        c.out_gate_for_din = gate;
+        c.din_accumulate = acc;
+        n->convs.push_back(c);
+    };
+    const TensorRef none{nullptr, 0, 0};
+    // encoder
+    TensorRef xin{n->x_in, n->cpad, 0};
+    TensorRef src = xin;
+    TensorRef dsrc = none;
+    const bf16* gsrc = nullptr;
+    for (int l = 0; l < 3; l++) {
+        const int cin = (l == 0) ? n->cpad : C[l - 1];
+        add(cin, C[l], l, src, TensorRef{e_a[l], C[l], 0}, dsrc, TensorRef{ge_a[l], C[l], 0}, gsrc, 0);
+        add(C[l], C[l], l, TensorRef{e_a[l], C[l], 0}, TensorRef{cat[l], 3 * C[l], 0}, TensorRef{ge_a[l], C[l], 0},
+            TensorRef{gcat[l], 3 * C[l], 0}, e_a[l], 0);
+        n->pools.push_back({TensorRef{cat[l], 3 * C[l], 0}, pool[l], C[l], Hs[l + 1], Ws[l + 1], gpool[l]});
+        src = TensorRef{pool[l], C[l], 0};
+        dsrc = TensorRef{gpool[l], C[l], 0};
+        gsrc = nullptr;  // pooled tensors are linear in the ReLU outputs
+    }
+    // bottom
+    add(C[2], C[3], 3, src, TensorRef{ba, C[3], 0}, dsrc, TensorRef{gba, C[3], 0}, nullptr, 0);
+    add(C[3], C[3], 3, TensorRef{ba, C[3], 0}, TensorRef{bb, C[3], 0}, TensorRef{gba, C[3], 0},
+        TensorRef{gbb, C[3], 0}, ba, 0);
+    // decoder
+    bf16* below = bb;
+    bf16* gbelow = gbb;
+    int cbelow = C[3];
+    for (int l = 2; l >= 0; l--) {
+        n->ups.push_back({below, cbelow, Hs[l + 1], Ws[l + 1], TensorRef{cat[l], 3 * C[l], C[l]}, gbelow,
+                          TensorRef{gcat[l], 3 * C[l], C[l]}});
+        add(3 * C[l], C[l], l, TensorRef{cat[l], 3 * C[l], 0}, TensorRef{d_a[l], C[l], 0},
+            TensorRef{gcat[l], 3 * C[l], 0}, TensorRef{gd_a[l], C[l], 0}, cat[l], 0);
+        add(C[l], C[l], l, TensorRef{d_a[l], C[l], 0}, TensorRef{d_b[l], C[l], 0}, TensorRef{gd_a[l], C[l], 0},
+            TensorRef{gd_b[l], C[l], 0}, d_a[l], 0);
+        below = d_b[l];
+        gbelow = gd_b[l];
+        cbelow = C[l];
+    }
+    n->y_last = d_b[0];
+    n->dy_last = gd_b[0];
+    n->head_w = off; off += (size_t)n->cout * B;
+    n->head_b = off; off += n->cout;
+    n->nparam = off;
+    n->nw_bf16 = woff;
+    const size_t npx0 = px(0);
+    CTH_CUDA(cudaMalloc(&n->prm, off * sizeof(float)));
+    CTH_CUDA(cudaMalloc(&n->grad, off * sizeof(float)));
+    CTH_CUDA(cudaMalloc(&n->adam_m, off * sizeof(float)));
+    CTH_CUDA(cudaMalloc(&n->adam_v, off * sizeof(float)));
+    CTH_CUDA(cudaMemset(n->prm, 0, off * sizeof(float)));
+    CTH_CUDA(cudaMemset(n->grad, 0, off * sizeof(float)));
+    CTH_CUDA(cudaMemset(n->adam_m, 0, off * sizeof(float)));
+    CTH_CUDA(cudaMemset(n->adam_v, 0, off * sizeof(float)));
+    CTH_CUDA(cudaMalloc(&n->wb, woff * sizeof(bf16)));
+    CTH_CUDA(cudaMalloc(&n->wt, woff * sizeof(bf16)));
+    CTH_CUDA(cudaMalloc(&n->out, npx0 * n->cout * sizeof(float)));
+    CTH_CUDA(cudaMalloc(&n->dout, npx0 * n->cout * sizeof(float)));
+    CTH_CUDA(cudaMalloc(&n->loss, sizeof(double)));
+    CTH_CUDA(cudaMalloc(&n->cw, n->cout * sizeof(float)));
+    std::vector<float> ones(n->cout, 1.f);
+    CTH_CUDA(cudaMemcpy(n->cw, ones.data(), n->cout * sizeof(float), cudaMemcpyHostToDevice));
+    return CTH_OK;
+}
+
+// bf16 weights (and their transposes) from the FP32 parameters
+int sync_weights(cth_unet* n, cudaStream_t s) {
+    for (const Conv& c : n->convs) {
+        const size_t nw = (size_t)c.cout * 9 * c.cin;
+        k_to_bf16<<<grid1(nw), 256, 0, s>>>(n->prm + c.w_off, n->wb + c.wb_off, nw);
+        k_wtrans<<<grid1(nw), 256, 0, s>>>(n->wb + c.wb_off, c.cout, c.cin, n->wt + c.wb_off);
+    }
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+void conv_fwd(cth_unet* n, const Conv& c, cudaStream_t s) {
+    ConvArgs a{};
+    a.in = c.in.p; a.in_cs = c.in.cs; a.in_coff = c.in.coff; a.Cin = c.cin;
+    a.w = n->wb + c.wb_off;
+    a.bias = n->prm + c.b_off;
+    a.out = c.out.p; a.out_cs = c.out.cs; a.out_coff = c.out.coff; a.Cout = c.cout;
+    a.H = c.H; a.W = c.W;
+    a.relu = 1;
+    dim3 grd((c.W + TW - 1) / TW, (c.H + TH - 1) / TH, c.cout / 32);
+    k_conv3_fwd<<<grd, 128, 0, s>>>(a);
+}
+
+void conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
+    // weight and bias gradients
+    WgradArgs w{};
+    w.dy = c.dout.p; w.dy_cs = c.dout.cs; w.dy_coff = c.dout.coff; w.Cout = c.cout;
+    w.in = c.in.p; w.in_cs = c.in.cs; w.in_coff = c.in.coff; w.Cin = c.cin;
+    w.H = c.H; w.W = c.W;
+    w.dw = n->grad + c.w_off;
+    const int npatch = ((c.W + TW - 1) / TW) * ((c.H + TH - 1) / TH);
+    const int tiles = (c.cout / 32) * (c.cin / 32);
+    int ppc = (int)std::ceil((double)npatch * tiles / (148.0 * 4.0));
+    ppc = std::max(1, std::min(ppc, npatch));
+    w.patches_per_cta = ppc;
+    dim3 gw((npatch + ppc - 1) / ppc, c.cout / 32, c.cin / 32);
+    k_conv3_wgrad<<<gw, 288, 0, s>>>(w);
+    const int npix = c.H * c.W;
+    const int ppb = 256;
+    k_bias_grad<<<(npix + ppb - 1) / ppb, 256, 0, s>>>(c.dout.p, c.dout.cs, c.dout.coff, c.cout, npix, ppb,
+                                                       n->grad + c.b_off);
+    if (!c.din.p) return;
+    ConvArgs a{};
+    a.in = c.dout.p; a.in_cs = c.dout.cs; a.in_coff = c.dout.coff; a.Cin = c.cout;
+    a.w = n->wt + c.wb_off;
+    a.bias = nullptr;
+    a.out = c.din.p; a.out_cs = c.din.cs; a.out_coff = c.din.coff; a.Cout = c.cin;
+    a.H = c.H; a.W = c.W;
+    a.relu = 0;
+    a.gate = c.out_gate_for_din;
+    a.gate_cs = c.din.cs; a.gate_coff = c.din.coff;
+    a.accumulate = c.din_accumulate;
+    dim3 grd((c.W + TW - 1) / TW, (c.H + TH - 1) / TH, c.cin / 32);
+    k_conv3_fwd<<<grd, 128, 0, s>>>(a);
+}
+
+int forward(cth_unet* n, const float* in, cudaStream_t s) {
+    const size_t npx = (size_t)n->H * n->W;
+    k_pack<<<grid1(npx * n->cpad), 256, 0, s>>>(in, n->cin, (int)npx, n->cpad, n->x_in);
+    const auto& C = n->convs;
+    int up = 0;
+    for (size_t k = 0; k < C.size(); k++) {
+        conv_fwd(n, C[k], s);
+        if (k == 1 || k == 3 || k == 5) {
+            const auto& p = n->pools[k / 2];
+            k_pool2<<<grid1((size_t)p.Ho * p.Wo * p.C), 256, 0, s>>>(p.src.p, p.src.cs, p.src.coff, p.C, p.Ho, p.Wo,
+                                                                      p.dst, p.C);
+        }
+        if (k == 7 || k == 9 || k == 11) {
+            const auto& u = n->ups[up++];
+            k_up2<<<grid1((size_t)4 * u.Hi * u.Wi * u.C), 256, 0, s>>>(u.src, u.C, u.C, u.Hi, u.Wi, u.dst.p, u.dst.cs,
+                                                                        u.dst.coff);
+        }
+    }
+    const int B = n->base;
+    k_head_fwd<<<(unsigned)((npx + 255) / 256), 256, 0, s>>>(n->y_last, B, (int)npx, n->prm + n->head_w,
+                                                             n->prm + n->head_b, n->cout, n->out);
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+int backward(cth_unet* n, const float* dout, cudaStream_t s) {
+    const size_t npx = (size_t)n->H * n->W;
+    const int B = n->base;
+    k_head_bwd<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(n->y_last, B, (int)npx, n->prm + n->head_w, n->cout,
+                                                            dout, n->dy_last, n->grad + n->head_w,
+                                                            n->grad + n->head_b);
+    const auto& C = n->convs;
+    // the decoder convs write the concatenation gradients whole; the pooling
+    // gradients are then added into their skip channels
+    for (int k = (int)C.size() - 1; k >= 0; k--) {
+        conv_bwd(n, C[k], s);
+        if (k == 12 || k == 10 || k == 8) {
+            const auto& u = n->ups[(k - 8) / 2];
+            k_up2_bwd<<<grid1((size_t)u.Hi * u.Wi * u.C), 256, 0, s>>>(u.ddst.p, u.ddst.cs, u.ddst.coff, u.C, u.Hi,
+                                                                      u.Wi, u.dsrc, u.C);
+        }
+        if (k == 6 || k == 4 || k == 2) {
+            const auto& p = n->pools[k / 2 - 1];
+            const TensorRef dskip = n->convs[k - 1].dout;
+            k_pool2_bwd<<<grid1((size_t)4 * p.Ho * p.Wo * p.C), 256, 0, s>>>(p.ddst, p.C, p.C, p.Ho, p.Wo, dskip.p,
+                                                                             dskip.cs, dskip.coff, p.src.p, p.src.cs,
+                                                                             p.src.coff);
+        }
+    }
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+cth_unet* cth_unet_create(int H, int W, int cin, int cout, int base, int device) {
+    if (H < 8 || W < 8 || H % 8 || W % 8 || cin < 1 || cin > 32 || cout < 1 || cout > 32 || base != 32) {
+        set_error("cth_unet_create: H, W multiples of 8, 1 <= cin, cout <= 32, base 32");
+        return nullptr;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        set_error("cth_unet_create: cudaSetDevice failed");
+        return nullptr;
+    }
+    cth_unet* n = new cth_unet();
+    n->device = device;
+    n->H = H; n->W = W; n->cin = cin; n->cout = cout; n->base = base;
+    if (build(n) != CTH_OK) {
+        cth_unet_destroy(n);
+        return nullptr;
+    }
+    return n;
+}
+
+void cth_unet_destroy(cth_unet* n) {
+    if (!n) return;
+    cudaSetDevice(n->device);
+    cudaDeviceSynchronize();
+    for (void* p : n->bufs) cudaFree(p);
+    for (void* p : {(void*)n->prm, (void*)n->grad, (void*)n->adam_m, (void*)n->adam_v, (void*)n->wb, (void*)n->wt,
+                    (void*)n->out, (void*)n->dout, (void*)n->loss, (void*)n->cw, (void*)n->feat})
+        if (p) cudaFree(p);
+    delete n;
+}
+
+long long cth_unet_nparams(const cth_unet* n) { return n ? (long long)n->nparam : -1; }
+
+int cth_unet_set_params(cth_unet* n, const float* host, long long count) {
+    if (!n || !host || count != (long long)n->nparam) { set_error("cth_unet_set_params: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(n->device));
+    CTH_CUDA(cudaMemcpy(n->prm, host, n->nparam * sizeof(float), cudaMemcpyHostToDevice));
+    CTH_CUDA(cudaMemset(n->adam_m, 0, n->nparam * sizeof(float)));
+    CTH_CUDA(cudaMemset(n->adam_v, 0, n->nparam * sizeof(float)));
+    int rc = sync_weights(n, 0);
+    if (rc != CTH_OK) return rc;
+    CTH_CUDA(cudaDeviceSynchronize());
+    return CTH_OK;
+}
+
+int cth_unet_get_params(const cth_unet* n, float* host, long long count) {
+    if (!n || !host || count != (long long)n->nparam) { set_error("cth_unet_get_params: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(n->device));
+    CTH_CUDA(cudaDeviceSynchronize());
+    CTH_CUDA(cudaMemcpy(host, n->prm, n->nparam * sizeof(float), cudaMemcpyDeviceToHost));
+    return CTH_OK;
+}
+
+int cth_unet_get_grads(const cth_unet* n, float* host, long long count) {
+    if (!n || !host || count != (long long)n->nparam) { set_error("cth_unet_get_grads: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(n->device));
+    CTH_CUDA(cudaDeviceSynchronize());
+    CTH_CUDA(cudaMemcpy(host, n->grad, n->nparam * sizeof(float), cudaMemcpyDeviceToHost));
+    return CTH_OK;
+}
+
+int cth_unet_set_loss_weights(cth_unet* n, const float* w_host) {
+    if (!n || !w_host) { set_error("cth_unet_set_loss_weights: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(n->device));
+    CTH_CUDA(cudaMemcpy(n->cw, w_host, n->cout * sizeof(float), cudaMemcpyHostToDevice));
+    return CTH_OK;
+}
+
+// forward pass of the FP32 NHWC input (H x W x cin, device); the FP32 NHWC
+// output (H x W x cout) is copied to out (device) when out is not null
+int cth_unet_forward(cth_unet* n, const float* in, float* out, void* stream) {
+    if (!n || !in) { set_error("cth_unet_forward: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(n->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = forward(n, in, s);
+    if (rc != CTH_OK) return rc;
+    if (out)
+        CTH_CUDA(cudaMemcpyAsync(out, n->out, (size_t)n->H * n->W * n->cout * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    return CTH_OK;
+}
+
+// gradients of <dout, forward output> after cth_unet_forward (zeroed first)
+int cth_unet_backward(cth_unet* n, const float* dout, void* stream) {
+    if (!n || !dout) { set_error("cth_unet_backward: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(n->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    CTH_CUDA(cudaMemsetAsync(n->grad, 0, n->nparam * sizeof(float), s));
+    return backward(n, dout, s);
+}
+
+// one Adam step on the weighted masked MSE between the output and target
+// (device FP32 NHWC, mask one value per pixel, msum = sum of the mask);
+// step t >= 1 (bias correction); loss (host) receives the loss before the step
+int cth_unet_train_step(cth_unet* n, const float* in, const float* target, const float* mask, double msum, float lr,
+                        int t, void* stream, double* loss) {
+    if (!n || !in || !target || !mask || !(msum > 0.0) || t < 1) {
+        set_error("cth_unet_train_step: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(n->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = forward(n, in, s);
+    if (rc != CTH_OK) return rc;
+    const size_t npx = (size_t)n->H * n->W;
+    CTH_CUDA(cudaMemsetAsync(n->loss, 0, sizeof(double), s));
+    k_mse<<<grid1(npx), 256, 0, s>>>(n->out, target, mask, (int)npx, n->cout, n->cw, 1.0 / msum, n->dout, n->loss);
+    CTH_CUDA(cudaMemsetAsync(n->grad, 0, n->nparam * sizeof(float), s));
+    rc = backward(n, n->dout, s);
+    if (rc != CTH_OK) return rc;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f / (1.f - std::pow(b1, (float)t)), c2 = 1.f / (1.f - std::pow(b2, (float)t));
+    k_adam<<<grid1(n->nparam), 256, 0, s>>>(n->prm, n->grad, n->adam_m, n->adam_v, n->nparam, lr, b1, b2, 1e-8f, c1,
+                                            c2);
+    rc = sync_weights(n, s);
+    if (rc != CTH_OK) return rc;
+    if (loss) {
+        CTH_CUDA(cudaMemcpyAsync(loss, n->loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CTH_CUDA(cudaStreamSynchronize(s));
+    }
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+// 18 values: input mean[6], input std[6], output mean[3], output std[3]
+int cth_unet_set_stats(cth_unet* n, const float* stats) {
+    if (!n || !stats) { set_error("cth_unet_set_stats: invalid arguments"); return CTH_ERR_ARG; }
+    for (int k = 0; k < 6; k++) {
+        n->stats.in_mean[k] = stats[k];
+        n->stats.in_std[k] = stats[6 + k] > 0.f ? stats[6 + k] : 1.f;
+    }
+    for (int k = 0; k < 3; k++) {
+        n->stats.out_mean[k] = stats[12 + k];
+        n->stats.out_std[k] = stats[15 + k] > 0.f ? stats[15 + k] : 1.f;
+    }
+    return CTH_OK;
+}
+
+// the network's input (H x W x 6, FP32, device) from a field store whose grid is
+// at most H x W cells
+int cth_unet_features(cth_unet* n, cth_fields* fs, float* out, void* stream) {
+    if (!n || !fs || !out || n->cin != 6 || fs->g->ni > n->W || fs->g->nj > n->H) {
+        set_error("cth_unet_features: invalid arguments (6 input channels, grid within the image)");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(n->device));
+    const char* names[5] = {"rhoe", "nu_m", "Bx", "Br", "dphi_prev"};
+    const double* q[5];
+    for (int k = 0; k < 5; k++) {
+        q[k] = field_ptr(fs, names[k]);
+        if (!q[k]) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t npx = (size_t)n->H * n->W;
+    k_features<<<grid1(npx), 256, 0, s>>>(q[0], q[1], q[2], q[3], q[4], fs->g->ni, fs->g->nj, fs->g->ld, n->H, n->W,
+                                          n->stats, out);
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+// warm-start prediction: features -> network; "dphi_guess" = "dphi_prev" +
+// output channel 2 (the initial guess of cth_solve_phi_pc with warm_start = 1)
+int cth_unet_predict_dphi(cth_unet* n, cth_fields* fs, void* stream) {
+    if (!n || !fs || n->cout < 3) { set_error("cth_unet_predict_dphi: invalid arguments"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(n->device));
+    const size_t npx = (size_t)n->H * n->W;
+    if (!n->feat) CTH_CUDA(cudaMalloc(&n->feat, npx * 6 * sizeof(float)));
+    int rc = cth_unet_features(n, fs, n->feat, stream);
+    if (rc != CTH_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = forward(n, n->feat, s);
+    if (rc != CTH_OK) return rc;
+    double* dst = field_ptr(fs, "dphi_guess");
+    const double* prev = field_ptr(fs, "dphi_prev");
+    if (!dst || !prev) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
+    const int ncell = fs->g->ni * fs->g->nj;
+    k_unpack<<<grid1((size_t)ncell), 256, 0, s>>>(n->out, n->cout, 2, fs->g->ni, fs->g->nj, fs->g->ld, n->W,
+                                                   n->stats.out_mean[2], n->stats.out_std[2], prev, dst);
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+}  // extern "C"

@@ -65,6 +65,15 @@ def rectangle_flags(ni, nj) -> np.ndarray:
     return fl
 
 
+# optional trailing fields of the parameter blocks (no counterpart in the
+# reference) and their defaults
+_PARAM_DEFAULTS = {"warm_start": 0, "guess_max_relres": 1.0}
+
+
+def _param_fields(cls, prm: dict) -> dict:
+    return {k: (prm[k] if k in prm or k not in _PARAM_DEFAULTS else _PARAM_DEFAULTS[k]) for k, _ in cls._fields_}
+
+
 class Fields:
     """A cth_fields store bound to a Grid."""
 
@@ -91,6 +100,18 @@ class Fields:
             raise capi.CathodeError(capi.CTH_ERR_ALLOC, capi.last_error())
         return p
 
+    def plane(self, name: str):
+        """Zero-copy torch view (nj+2, ld) float64 of a device plane (library layout)."""
+        import torch
+        g = self.grid
+
+        class _View:
+            pass
+        v = _View()
+        v.__cuda_array_interface__ = {"shape": (g.nj + 2, g.ld), "typestr": "<f8", "data": (self.ptr(name), False),
+                                      "version": 3, "strides": None}
+        return torch.as_tensor(v, device=f"cuda:{g.device}")
+
     def upload(self, name: str, a: np.ndarray):
         g = self.grid
         a = np.ascontiguousarray(a, dtype=np.float64)
@@ -116,13 +137,13 @@ class Fields:
 
         prm holds the cth_phi_params fields (dTe_SEE included); returns the PC
         result (iterations, calcRes errors, inner-solver status)."""
-        p = capi.PhiParams(**{k: prm[k] for k, _ in capi.PhiParams._fields_})
+        p = capi.PhiParams(**_param_fields(capi.PhiParams, prm))
         res = capi.PCResult()
         s = 0 if stream is None else stream.cuda_stream
         capi.check(self._L.cth_solve_phi_pc(self._h, ctypes.byref(p), s, ctypes.byref(res)), allow_positive=False)
         return dict(ncount=res.ncount, solver_rc=res.solver_rc, error_phi=res.error_phi,
                     error_nUex=res.error_nUex, error_nUer=res.error_nUer, error_iter=list(res.error_iter),
-                    solver=res.solver.as_dict())
+                    solver=res.solver.as_dict(), first=res.first.as_dict())
 
     def set_ion_geometry(self, geo: dict):
         """Upload the ion wall programs and residual boxes of a geometry dict."""
@@ -173,7 +194,9 @@ class Fields:
             setattr(P, k, params[k])
         for blk, cls in (("ion", capi.IonParams), ("phi", capi.PhiParams), ("rhoe", capi.SGParams),
                          ("eps", capi.SGParams), ("transport", capi.TransportParams)):
-            setattr(P, blk, cls(**{k: params[blk][k] for k, _ in cls._fields_}))
+            setattr(P, blk, cls(**_param_fields(cls, params[blk])))
+        net = params.get("net")
+        P.net = net.handle if net is not None else None
         nb = params["neutral"]
         P.neutral = capi.NeutralParams(**{k: nb[k] for k, _ in capi.NeutralParams._fields_
                                           if k not in ("n_pos_box", "pos_box", "do_rhon", "do_rhom")})
@@ -195,7 +218,8 @@ class Fields:
                     anode=dict(Ii=R.rhoe.Ii_Anode, Ie=R.rhoe.Ie_Anode, I=R.rhoe.I_Anode),
                     iterations=dict(phi=R.phi.solver.iterations, rhoe=R.rhoe.solver.iterations,
                                     eps=R.eps.solver.iterations, rhoi=R.ion.solver[3].iterations,
-                                    rhon=R.neutral.solver[0].iterations))
+                                    rhon=R.neutral.solver[0].iterations),
+                    phi_first=R.phi.first.as_dict())
 
     def check_cfl(self, dt: float, CFL: float, masse: float, rmin: float, dr: float, flag_adp_dt: int = 0,
                   stream=None) -> dict:

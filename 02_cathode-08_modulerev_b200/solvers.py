@@ -206,6 +206,19 @@ class Grid:
         capi.check(rc)
         return st
 
+    def smg_solve_guess_dev(self, aP, aE, aW, aN, aS, b, x0, solution, max_guess_relres=1.0, maxITR=30,
+                            error_cnv=1e-10, precision=capi.CTH_PREC_FP64, stream=None) -> capi.Status:
+        """smg_solve_dev from the initial guess x0 (a device plane); the guess is
+        rejected (zero start) when ||b - A x0|| > max_guess_relres ||b||."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        st = capi.Status()
+        rc = self._L.cth_smg_solve_guess_dev(self._h, *[_ptr(a) for a in (aP, aE, aW, aN, aS, b, x0)],
+                                             max_guess_relres, maxITR, error_cnv, precision, _ptr(solution),
+                                             s.cuda_stream, ctypes.byref(st))
+        capi.check(rc)
+        return st
+
     def sor_solve_dev(self, aP, aE, aW, aN, aS, b, solution, alpha_SOR=1.9, maxITR=2000,
                       error_cnv=1e-8, stream=None) -> capi.Status:
         import torch

@@ -329,13 +329,14 @@ def main():
     eb = torch.zeros((NJ + 2, gb.ld), dtype=torch.complex128, device=dev)
     grids = (g, gx, gr, gb)
 
-    def reset(prec):
+    def reset(prec, warm_start=0):
         for k, v in init.items():
             fs.upload(k, v)
         P = {k: (dict(v) if isinstance(v, dict) else v) for k, v in cfg["params"].items()}
         for blk in ("ion", "rhoe", "eps", "neutral"):
             P[blk]["precision"] = prec
         P["phi"]["precision"] = prec
+        P["phi"].update(warm_start=warm_start, guess_max_relres=1.0)
         fs.update_transport_coef(P["transport"])
         torch.cuda.synchronize(dev)
         return P
@@ -356,8 +357,8 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    def timed(prec, steps, warmup):
-        P = reset(prec)
+    def timed(prec, steps, warmup, warm_start=0, first=None):
+        P = reset(prec, warm_start)
         for _ in range(warmup):
             step(P)
         barrier()
@@ -374,6 +375,8 @@ def main():
             e1.synchronize()
             ms += e0.elapsed_time(e1)
             mw_solves += int("mw" in last)
+            if first is not None:
+                first.append(last["phi_first"])
             if last["solver_rc"] != 0:
                 raise RuntimeError(f"an inner solve did not converge: {last}")
         launches = sum(x.launch_count() for x in grids) - l0
@@ -388,6 +391,13 @@ def main():
     ms_mixed, launches, last_mixed, mw_mixed, P_mixed = timed(capi.CTH_PREC_MIXED, args.steps, args.warmup)
     barrier()
     ms_fp64, _, last_fp64, _, _ = timed(capi.CTH_PREC_FP64, args.steps, args.warmup)
+    barrier()
+    # the same mixed steps with the first potential solve of each step started from
+    # the previous step's correction (plain warm start, threshold 1)
+    first_prev = []
+    ms_prev, _, _, _, _ = timed(capi.CTH_PREC_MIXED, args.steps, args.warmup, warm_start=2, first=first_prev)
+    first_zero = []
+    timed(capi.CTH_PREC_MIXED, min(args.steps, 20), 1, warm_start=0, first=first_zero)
     barrier()
     clocks = clk.stop()
 
@@ -475,6 +485,14 @@ def main():
         "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms_fp64 / args.steps},
         "mixed_over_fp64": value / fp64_value,
         "learned_warm_start": "not built: the reported steps/s are the mixed-precision path without it",
+        "warm_start": {
+            "previous_step": {"value": world * args.steps / (ms_prev / 1e3), "unit": UNIT,
+                              "first_phi_solve_cycles_mean": float(np.mean([f["iterations"] for f in first_prev])),
+                              "guess_residual_mean": float(np.mean([f["guess_residual"] for f in first_prev])),
+                              "fallback_rate": float(np.mean([f["guess"] != 1 for f in first_prev]))},
+            "zero_start_first_phi_solve_cycles_mean": float(np.mean([f["iterations"] for f in first_zero])),
+            "note": "mixed precision; the first potential solve of each step starts from the previous step's "
+                    "correction (threshold ||b-Ax0|| <= ||b||); same stopping rule"},
         "microwave_solves_in_timed_steps": mw_mixed,
         "inner_iterations_last_step": last_mixed["iterations"],
         "step_breakdown_ms": parts,

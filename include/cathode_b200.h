@@ -53,9 +53,11 @@ typedef struct cth_status {
     int iterations;          /* V-cycles (SMG replacement) or sweeps (SOR replacement) */
     int converged;           /* 1 when the stopping rule was met                        */
     int nonfinite;           /* 1 when a NaN/Inf residual or update was seen             */
-    int reserved;
+    int guess;               /* SMG: 0 started from zero; 1 from the caller's guess;
+                                -1 guess rejected by its threshold (started from zero)  */
     double residual;         /* SMG: final ||b-Ax||_2/||b||_2; SOR: last max relative update */
     double initial_residual; /* SMG: ||b||_2 of the grid cells; SOR: 0                  */
+    double guess_residual;   /* SMG: ||b-A x0||_2/||b||_2 of the guess (-1: no guess)   */
 } cth_status;
 
 typedef struct cth_grid cth_grid; /* opaque: grid shape, block union, device workspace */
@@ -127,6 +129,16 @@ int cth_smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const dou
                       const double* aN, const double* aS, const double* b, int maxITR,
                       double error_cnv, int precision, double* solution, void* stream,
                       cth_status* st);
+/* Same solve from the device plane x0 as initial guess (no counterpart in the
+ * reference, whose SMG always starts from zero): the cycles start from x0 when
+ * ||b - A x0||_2 <= max_guess_relres ||b||_2, otherwise from zero (the plain
+ * solve is the fallback); st->guess / guess_residual report which.  The
+ * stopping rule is unchanged, so the converged residual is the same; x0 may
+ * alias solution. */
+int cth_smg_solve_guess_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                            const double* aN, const double* aS, const double* b, const double* x0,
+                            double max_guess_relres, int maxITR, double error_cnv, int precision,
+                            double* solution, void* stream, cth_status* st);
 
 /* SOR replacement (host arrays) ----------------------------------------------
  * Drop-in for solver_SOR (include/solverFuncs.hpp:169-217) with red-black
@@ -250,6 +262,15 @@ typedef struct cth_phi_params {
     int flag_error;     /* calcRes mode 0..3 (miniFuncs.hpp:292-376) */
     int flag_iter_phi;  /* 0: SOR, otherwise SMG                     */
     int precision;      /* CTH_PREC_MIXED or CTH_PREC_FP64           */
+    /* initial guess of the first inner (SMG) solve; no counterpart in the
+     * reference, whose solves start from zero.  0: zero (reference);
+     * 1: the store's plane "dphi_guess" (written by the caller, e.g. the
+     * learned predictor); 2: the plane "dphi_prev" = the first-iteration
+     * correction of the previous call.  With warm_start != 0 the first
+     * iteration's correction is copied into "dphi_prev".  A guess whose
+     * relative residual exceeds guess_max_relres is dropped (zero start). */
+    int warm_start;
+    double guess_max_relres;
 } cth_phi_params;
 
 typedef struct cth_pc_result {
@@ -259,6 +280,7 @@ typedef struct cth_pc_result {
     double error_iter[3];  /* calcRes of the last iteration (phi, nUex, nUer)      */
     cth_status solver;     /* status of the last inner solve                      */
     double Ii_Anode, Ie_Anode, I_Anode;  /* anode currents (density sweep only)    */
+    cth_status first;      /* status of the first inner solve (initial-guess report) */
 } cth_pc_result;
 int cth_solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, void* stream, cth_pc_result* res);
 
@@ -389,6 +411,10 @@ typedef struct cth_step_params {
     cth_sg_params rhoe, eps;
     cth_neutral_params neutral;
     cth_transport_params transport;
+    /* learned warm start (no counterpart in the reference): with phi.warm_start
+     * == 1 and net not null, cth_unet_predict_dphi fills "dphi_guess" right
+     * before the potential predictor-corrector */
+    struct cth_unet* net;
 } cth_step_params;
 typedef struct cth_step_result {
     cth_ion_result ion;
@@ -427,6 +453,46 @@ int cth_residual_noalloc(int ni, int nj, int ld, const int* i_bl, const int* j_b
                          const double* aP, const double* aE, const double* aW, const double* aN,
                          const double* aS, const double* b, const double* x, double* r,
                          double* rnorm, double* bnorm, void* stream);
+
+/* Learned warm start ---------------------------------------------------------
+ * No counterpart in the reference.  A 4-level convolutional U-Net (3x3
+ * convolutions, ReLU, 2x2 average pooling, nearest upsampling, skip
+ * concatenations; channels 32/64/128/256; 1x1 linear output layer), bfloat16
+ * weights and activations with FP32 accumulation on the tensor cores, FP32
+ * master parameters and Adam.  Images are NHWC FP32 device arrays of H x W
+ * pixels (H, W multiples of 8; cin, cout <= 32 channels; base must be 32).
+ * Parameter order (FP32): per convolution, in forward order e0a e0b e1a e1b
+ * e2a e2b ba bb d2a d2b d1a d1b d0a d0b, weights [cout][3][3][cin] then bias
+ * [cout]; last the output layer [cout][32] and its bias.  The first
+ * convolution takes the input zero-padded to 32 channels. */
+typedef struct cth_unet cth_unet;
+cth_unet* cth_unet_create(int H, int W, int cin, int cout, int base, int device);
+void cth_unet_destroy(cth_unet* n);
+long long cth_unet_nparams(const cth_unet* n);
+int cth_unet_set_params(cth_unet* n, const float* host, long long count);  /* resets Adam */
+int cth_unet_get_params(const cth_unet* n, float* host, long long count);
+int cth_unet_get_grads(const cth_unet* n, float* host, long long count);
+int cth_unet_set_loss_weights(cth_unet* n, const float* w_host);          /* cout values */
+int cth_unet_forward(cth_unet* n, const float* in, float* out, void* stream);
+/* gradients of sum(dout * output) with respect to the parameters, after
+ * cth_unet_forward on the same stream */
+int cth_unet_backward(cth_unet* n, const float* dout, void* stream);
+/* forward, weighted masked MSE against target (mask: one value per pixel,
+ * msum its sum), backward and one Adam step (t >= 1); *loss = loss before it */
+int cth_unet_train_step(cth_unet* n, const float* in, const float* target, const float* mask, double msum,
+                        float lr, int t, void* stream, double* loss);
+/* Warm start of the potential predictor-corrector from a field store (grid of
+ * at most H x W cells, cell (i, j) -> pixel (j-1, i-1)).  Input channels
+ * (cin = 6): log10 rhoe, log10 nu_m, |B| from Bx and Br, two zero channels
+ * reserved for the microwave field, and "dphi_prev"; each normalised with the
+ * stats (mean[6], std[6]); output channel 2, de-normalised (output mean[3],
+ * std[3]), is the change of the first-iteration correction from "dphi_prev"
+ * (a zero output reproduces the previous-step guess).  cth_unet_features writes the
+ * input (H x W x 6 FP32, device); cth_unet_predict_dphi runs the network and
+ * writes the plane "dphi_guess" read by cth_solve_phi_pc with warm_start = 1. */
+int cth_unet_set_stats(cth_unet* n, const float* stats);
+int cth_unet_features(cth_unet* n, cth_fields* fs, float* out, void* stream);
+int cth_unet_predict_dphi(cth_unet* n, cth_fields* fs, void* stream);
 
 /* Layout helpers (device arrays): copy between the reference's [i][j] layout
  * and the library layout. */

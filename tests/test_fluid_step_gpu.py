@@ -118,3 +118,38 @@ def test_steps_match_oracle(pkg, orc, cuda_device, kind):
     fs.close()
     for x in (g, gx, gr):
         x.close()
+
+
+def test_previous_step_warm_start(pkg, orc, cuda_device):
+    """warm_start = 2: the first potential solve of each step starts from the
+    previous step's first correction.  Same stopping rule, so the fields stay
+    within the whole-step tolerance of the oracle (which starts from zero), and
+    the first solves of later steps need fewer cycles."""
+    nstep = 4
+    geo, ogeo, st, cfg = setup(pkg, "rectangle")
+    ref, Po = oracle_run(geo, ogeo, st, cfg, nstep)
+    alt, _ = oracle_run(geo, ogeo, st, cfg, nstep, perturb=True)
+    its = {}
+    for ws in (0, 2):
+        g, gx, gr, fs = device_fields(pkg, geo, st, cfg)
+        P = {k: (dict(v) if isinstance(v, dict) else v) for k, v in cfg["params"].items()}
+        P["phi"].update(warm_start=ws, guess_max_relres=1.0)
+        its[ws] = []
+        for step in range(nstep):
+            r = fs.fluid_step(gx, gr, P)
+            assert r["solver_rc"] == 0, r
+            its[ws].append(r["phi_first"]["iterations"])
+            if ws == 2:
+                assert r["phi_first"]["guess"] == 1
+                assert r["phi_first"]["residual"] <= P["phi"]["error_cnv_SOR_phi"]
+            else:
+                assert r["phi_first"]["guess"] == 0
+        for k in CHECK:
+            got = fs.download(k)
+            tol = max(1e-8, 4.0 * _rel(alt[k], ref[k]))
+            assert _rel(got, ref[k]) <= tol, (ws, k, _rel(got, ref[k]), tol)
+        fs.close()
+        for x in (g, gx, gr):
+            x.close()
+    assert its[2][0] == its[0][0]
+    assert sum(its[2][1:]) < sum(its[0][1:]), its

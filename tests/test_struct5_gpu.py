@@ -190,3 +190,37 @@ def test_complex_fused_tail_matches_level_launches(pkg, cuda_device):
     assert out[0][0] == out[1][0]
     assert np.linalg.norm(out[0][1] - out[1][1]) <= 1e-10 * np.linalg.norm(out[1][1])
     g.close()
+
+
+def test_smg_initial_guess(pkg, cuda_device):
+    """Solve from a caller's guess: accepted when its relative residual is below
+    the threshold (fewer cycles, same stopping rule), rejected otherwise (then
+    bit-identical to the zero start); an exact guess stops before any cycle."""
+    import torch
+    s = pkg.workloads.poisson_slab(ni=200, nj=100, seed=5)
+    g = pkg.Grid(s["ni"], s["nj"], s["i_bl"], s["j_bl"])
+    planes = [g.to_device(s[k]) for k in ("aP", "aE", "aW", "aN", "aS", "b")]
+    for prec in (0, 1):
+        x_ref = g.device_plane(1)[0]
+        st0 = g.smg_solve_dev(*planes, x_ref, maxITR=30, error_cnv=1e-11, precision=prec)
+        assert st0.converged == 1 and st0.guess == 0 and st0.guess_residual == -1.0
+        gen = torch.Generator(device=x_ref.device).manual_seed(1)
+        near = x_ref * (1.0 + 1e-3 * torch.randn(x_ref.shape, generator=gen, device=x_ref.device,
+                                                 dtype=x_ref.dtype))
+        x1 = g.device_plane(1)[0]
+        st1 = g.smg_solve_guess_dev(*planes, near, x1, max_guess_relres=0.5, maxITR=30, error_cnv=1e-11,
+                                    precision=prec)
+        assert st1.converged == 1 and st1.guess == 1 and 0.0 < st1.guess_residual < 0.5
+        assert st1.iterations < st0.iterations and st1.residual < 1e-11
+        far = 1e6 * torch.randn(x_ref.shape, generator=gen, device=x_ref.device, dtype=x_ref.dtype)
+        x2 = g.device_plane(1)[0]
+        st2 = g.smg_solve_guess_dev(*planes, far, x2, max_guess_relres=0.5, maxITR=30, error_cnv=1e-11,
+                                    precision=prec)
+        assert st2.guess == -1 and st2.guess_residual > 0.5
+        assert st2.iterations == st0.iterations and bool((x2 == x_ref).all())
+        x3 = x_ref.clone()
+        st3 = g.smg_solve_guess_dev(*planes, x3, x3, max_guess_relres=0.5, maxITR=30, error_cnv=1e-10,
+                                    precision=prec)
+        assert st3.guess == 1 and st3.iterations == 0 and st3.converged == 1
+        assert bool((x3 == x_ref).all())
+    g.close()

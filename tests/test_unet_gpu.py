@@ -1,0 +1,117 @@
+"""The learned warm-start network on the GPU: forward output and parameter
+gradients of the library's tensor-core kernels against the numpy oracle (bf16
+rounding points emulated for the output, 2e-2 relative L2; gradients judged
+against the exact float64 network, see the test), training
+on a synthetic regression, and the warm start of the potential solve against
+the plain zero start and the previous-step guess."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("shape", [(16, 32), (24, 40)])
+def test_forward_and_gradients_match_oracle(pkg, cuda_device, shape):
+    """Device output and gradients against the oracle.  The exact network
+    (float64) is the reference for the gradients: the device's error per layer
+    must stay within 2.5x (+0.03) of the error that the oracle's own bf16
+    rounding points produce (about 0.04-0.17 per layer here: bf16 activations
+    flip ReLU gates), and the whole gradient must point the same way."""
+    import torch
+    from oracle import unet
+    H, W = shape
+    rng = np.random.default_rng(2)
+    vec = unet.init_params(seed=4)
+    vec = vec + (0.01 * rng.normal(size=vec.size)).astype(np.float32)
+    vec[-(3 * 32 + 3):] = rng.normal(0.0, 0.2, size=3 * 32 + 3)
+    x = rng.normal(size=(H, W, 6)).astype(np.float32)
+    dout = rng.normal(size=(H, W, 3)).astype(np.float32)
+    net = pkg.learned.UNet(H, W, params=vec)
+    xt = torch.from_numpy(x).cuda()
+    out = net.forward(xt).cpu().numpy()
+    ref, cache = unet.forward(vec, x, bf16=True)
+    assert _rel(out, ref) < 2e-2, _rel(out, ref)
+    net.backward(torch.from_numpy(dout).cuda())
+    torch.cuda.synchronize()
+    g = net.grads()
+    gb = unet.backward(vec, cache, dout)
+    _, c64 = unet.forward(vec.astype(np.float64), x.astype(np.float64), bf16=False)
+    g64 = unet.backward(vec.astype(np.float64), c64, dout.astype(np.float64))
+    off = 0
+    rows = []
+    for name, ci, co, _ in unet.layer_shapes():
+        n = co * 9 * ci + co
+        e_dev, e_bf = _rel(g[off:off + n], g64[off:off + n]), _rel(gb[off:off + n], g64[off:off + n])
+        rows.append((name, round(e_dev, 4), round(e_bf, 4)))
+        off += n
+    print(shape, rows)
+    for name, e_dev, e_bf in rows:
+        assert e_dev <= 2.5 * e_bf + 0.03, (name, e_dev, e_bf)
+    cos = float(g @ g64 / (np.linalg.norm(g) * np.linalg.norm(g64)))
+    cos_bf = float(gb @ g64 / (np.linalg.norm(gb) * np.linalg.norm(g64)))
+    assert cos > cos_bf - 0.01 and cos > 0.95, (cos, cos_bf)
+    net.close()
+
+
+def test_training_reduces_loss(pkg, cuda_device):
+    """Adam on a smooth synthetic target (a blurred, rescaled input channel)."""
+    import torch
+    H, W = 32, 64
+    net = pkg.learned.UNet(H, W, seed=0)
+    net.set_loss_weights([0.0, 0.0, 1.0])
+    g = torch.Generator(device="cuda").manual_seed(0)
+    X = torch.randn((8, H, W, 6), generator=g, device="cuda")
+    k = torch.ones((1, 1, 5, 5), device="cuda") / 25.0
+    Y = torch.zeros((8, H, W, 3), device="cuda")
+    Y[..., 2] = 3.0 * torch.nn.functional.conv2d(X[..., 0].unsqueeze(1), k, padding=2).squeeze(1) + 0.5
+    mask = torch.ones((H, W), device="cuda")
+    first = last = None
+    for ep in range(60):
+        tot = 0.0
+        for q in range(8):
+            tot += net.train_step(X[q].contiguous(), Y[q].contiguous(), mask, H * W, 2e-3)
+        if first is None:
+            first = tot / 8
+        last = tot / 8
+    assert last < 0.1 * first, (first, last)
+    net.close()
+
+
+def test_learned_warm_start_of_the_potential(pkg, cuda_device):
+    """Snapshots of plain runs (64 x 128 cells, two seeds), training, then steps
+    of an unseen discharge with the first potential solve started from zero,
+    from the previous step's correction and from the network's guess (the
+    previous correction plus the predicted change).  All reach the same
+    stopping rule; the trained guess is better than zero and no worse than the
+    previous-step guess it refines."""
+    L = pkg.learned
+    ni, nj = 128, 64
+    net = L.UNet(nj, ni, seed=0)
+    X, Y, mask = L.collect_snapshots(pkg, net, ni, nj, nsteps=30, seeds=[11, 12, 13])
+    stats = L.fit_stats(X, Y, mask)
+    net.set_stats(stats)
+    Xn, Yn = L.normalise(X, Y, stats)
+    losses = L.train(net, Xn, Yn, mask, epochs=10, lr=5e-4)
+    assert losses[-1] < losses[0]
+    recs = {}
+    for ws in (0, 2, 1):
+        c = L.make_case(pkg, ni, nj, seed=99, V_bias=25.0)
+        L.run_steps(pkg, c, 3, warm_start=2)  # same history for every variant
+        recs[ws] = L.run_steps(pkg, c, 6, warm_start=ws, net=net)
+        L.close_case(c)
+    for ws, rec in recs.items():
+        for r in rec:
+            assert r["residual"] <= 1e-10
+    learned = recs[1]
+    assert all(r["guess"] in (1, -1) for r in learned)
+    res = [r["guess_residual"] for r in learned]
+    prev = [r["guess_residual"] for r in recs[2]]
+    print("first-solve cycles zero/prev/learned:", [np.mean([r["cycles"] for r in recs[w]]) for w in (0, 2, 1)],
+          "guess residual prev/learned:", np.mean(prev), np.mean(res))
+    # the network refines the previous-step guess it starts from
+    assert np.mean(res) < 1.0 and np.mean(res) <= 1.1 * np.mean(prev)
+    net.close()
