@@ -285,7 +285,7 @@ int cth_grid_create(int ni, int nj, const int* i_bl, const int* j_bl, int n_bl, 
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.x64[0], n0 * sizeof(double)), "cudaMalloc x64");
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.x64[1], n0 * sizeof(double)), "cudaMalloc x64");
     // partial-sum blocks: enough for 256-wide blocks over the full padded index space, twice
-    g->ws.npart = 2 * (((ni + 2 + 255) / 256) * (nj + 2) + 64);
+    g->ws.npart = 3 * (((ni + 2 + 255) / 256) * (nj + 2) + 64);
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.part, (size_t)g->ws.npart * sizeof(double)), "cudaMalloc part");
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.stat, 32 * sizeof(double)), "cudaMalloc stat");
     if (rc == CTH_OK) chk(cudaMemset(g->ws.stat, 0, 32 * sizeof(double)), "memset stat");
@@ -439,7 +439,7 @@ int cth_smg_solve_guess_dev(cth_grid* g, const double* aP, const double* aE, con
                             double max_guess_relres, int maxITR, double error_cnv, int precision,
                             double* solution, void* stream, cth_status* st) {
     if (!g || !aP || !aE || !aW || !aN || !aS || !b || !x0 || !solution || maxITR < 0 ||
-        !(max_guess_relres >= 0.0)) {
+        !(max_guess_relres >= 0.0 && max_guess_relres <= 10.0)) {
         set_error("cth_smg_solve_guess_dev: invalid arguments");
         return CTH_ERR_ARG;
     }

@@ -290,6 +290,9 @@ void cth_fields_destroy(cth_fields* fs) {
     for (auto& kv : fs->tables) cudaFree(kv.second.first);
     if (fs->flags) cudaFree(fs->flags);
     if (fs->ghost_rules) cudaFree(fs->ghost_rules);
+    if (fs->net_stream) cudaStreamDestroy(fs->net_stream);
+    for (int k = 0; k < 2; k++)
+        if (fs->net_event[k]) cudaEventDestroy(fs->net_event[k]);
     if (fs->aux_ready) {
         for (int k = 0; k < 2; k++) cudaStreamDestroy(fs->aux_stream[k]);
         for (int k = 0; k < 3; k++) cudaEventDestroy(fs->aux_event[k]);

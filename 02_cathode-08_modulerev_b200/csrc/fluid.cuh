@@ -23,7 +23,9 @@ struct cth_fields {
     int* ion_boxes[4] = {};                    // residual boxes (rhoi, Uix, Uir, Uip)
     int ion_nbox[4] = {};
     int ion_box_total[4] = {};
-    bool aux_ready = false;                    // streams / events of the concurrent ion solves
+    bool aux_ready = false;
+    cudaStream_t net_stream = nullptr;   // learned warm-start inference, concurrent with the ion step
+    cudaEvent_t net_event[2] = {nullptr, nullptr};                    // streams / events of the concurrent ion solves
     cudaStream_t aux_stream[2] = {};
     cudaEvent_t aux_event[3] = {};
     std::map<std::string, double*> planes;

@@ -86,11 +86,13 @@ struct SolveArgs {
     int maxit;
     int pad;
     const double* x0;   // initial guess (null: zero, the reference's start)
-    double guess_tol;   // the guess is used when ||b - A x0|| <= guess_tol ||b||
+    const double* x0b;  // second candidate (null: none); the better of the two is used
+    double guess_tol;   // a guess is used when ||b - A x0|| <= guess_tol ||b|| (guess_tol <= 10)
 };
 
 // device status words of a solve (double array).  ST_GUESS: 0 no guess;
-// 1 + r0 guess used; -(1 + r0) guess rejected (r0 = its relative residual)
+// 1 + r0 first candidate used; 100 + r0 second candidate used; -(1 + r0)
+// guesses rejected (r0 = relative residual of the used / the better guess)
 enum StatWord { ST_RR = 0, ST_RELRES = 1, ST_BB = 2, ST_NONFINITE = 3, ST_ITER = 4, ST_CONV = 5, ST_KEEP = 6,
                 ST_GUESS = 7 };
 
@@ -177,7 +179,7 @@ int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double*
 int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
                      const double* aS, const double* b, int maxITR, double error_cnv, int precision,
                      double* solution, cudaStream_t s, int* pending, double* h_dst,
-                     const double* x0 = nullptr, double guess_tol = 0.0);
+                     const double* x0 = nullptr, double guess_tol = 0.0, const double* x0b = nullptr);
 int solve_finish(cth_grid* g, int pending, cth_status* st);
 int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st);
 int sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,

@@ -335,10 +335,12 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
     double* out = fs->scal + 16;
     const double* guess = nullptr;
     double* dphi_prev = nullptr;
+    double* dphi_prev2 = nullptr;
     if (prm->warm_start != 0 && prm->flag_iter_phi != 0) {
         dphi_prev = field_ptr(fs, "dphi_prev");
+        dphi_prev2 = field_ptr(fs, "dphi_prev2");
         guess = (prm->warm_start == 1) ? field_ptr(fs, "dphi_guess") : dphi_prev;
-        if (!dphi_prev || !guess) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
+        if (!dphi_prev || !dphi_prev2 || !guess) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
     }
     cth_status st_first{};
     k_phi_begin<<<grd, blk, 0, s>>>(A);
@@ -362,10 +364,13 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
         else
             rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR_phi,
                                   prm->error_cnv_SOR_phi, prm->precision, A.dphi, s, &pend, fs->h_solve,
-                                  ncount == 1 ? guess : nullptr, prm->guess_max_relres);
+                                  ncount == 1 ? guess : nullptr, prm->guess_max_relres,
+                                  prm->warm_start == 1 ? dphi_prev : nullptr);
         if (rc < 0) return rc;
-        if (ncount == 1 && dphi_prev)
+        if (ncount == 1 && dphi_prev) {
+            CTH_CUDA(cudaMemcpyAsync(dphi_prev2, dphi_prev, g->plane * sizeof(double), cudaMemcpyDeviceToDevice, s));
             CTH_CUDA(cudaMemcpyAsync(dphi_prev, A.dphi, g->plane * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        }
         k_phi_correct_a<<<grd, blk, 0, s>>>(A);
         k_phi_correct_b<<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out);
         g->launches += 2;
@@ -406,7 +411,7 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
 extern "C" int cth_solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, void* stream, cth_pc_result* res) {
     if (!fs || !prm || prm->dx <= 0.0 || prm->dr <= 0.0 || prm->maxITR_HES_phi < 1 || prm->flag_error < 0 ||
         prm->flag_error > 3 || prm->warm_start < 0 || prm->warm_start > 2 ||
-        (prm->warm_start != 0 && !(prm->guess_max_relres >= 0.0))) {
+        (prm->warm_start != 0 && !(prm->guess_max_relres >= 0.0 && prm->guess_max_relres <= 10.0))) {
         cth::set_error("cth_solve_phi_pc: invalid arguments");
         return CTH_ERR_ARG;
     }

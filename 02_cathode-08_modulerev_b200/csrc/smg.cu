@@ -48,10 +48,9 @@ template <typename T> constexpr bool kFac = !std::is_same<T, cd>::value;
 // the cycle loop runs at all (sets the graph's loop condition when use_cond).
 // ---------------------------------------------------------------------------
 // FP64 residual r = b - A x0 of one grid cell (couplings to non-grid cells dropped)
-__device__ __forceinline__ double guess_resid(const SolveArgs* __restrict__ args,
+__device__ __forceinline__ double guess_resid(const SolveArgs* __restrict__ args, const double* __restrict__ x0,
                                               const unsigned char* __restrict__ mask, size_t p, size_t q,
                                               int c, int r, int ncol, int nrow, int ldl, int ld_u) {
-    const double* x0 = args->x0;
     double v = args->b[q] - args->aP[q] * x0[q];
     if (c > 0 && mask[p - 1]) v += args->aW[q] * x0[q - 1];
     if (c + 1 < ncol && mask[p + 1]) v += args->aE[q] * x0[q + 1];
@@ -60,9 +59,10 @@ __device__ __forceinline__ double guess_resid(const SolveArgs* __restrict__ args
     return v;
 }
 
-// Initial-guess test: ||b - A x0||^2 and ||b||^2 over the grid cells; the last
-// block records in ST_GUESS whether k_prep0 starts from x0 (relative residual
-// at most guess_tol) or from zero.  No guess: one thread writes 0.
+// Initial-guess test: ||b - A x||^2 of the candidates and ||b||^2 over the grid
+// cells; the last block records in ST_GUESS which candidate k_prep0 starts
+// from (the smaller relative residual, if at most guess_tol) or zero.  No
+// guess: one thread writes 0.
 __global__ void k_guess(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask, int ld_u,
                         int i0, int j0, int ncol, int nrow, int ldl, double* __restrict__ part,
                         unsigned int* counter, double* __restrict__ stat) {
@@ -73,22 +73,31 @@ __global__ void k_guess(const SolveArgs* __restrict__ args, const unsigned char*
     }
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
-    double v[2] = {0.0, 0.0};
+    const double* xb = args->x0b;
+    double v[3] = {0.0, 0.0, 0.0};  // ||r(x0)||^2, ||r(x0b)||^2, ||b||^2
     if (c < ncol) {
         const size_t p = (size_t)r * ldl + c;
         const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
         if (mask[p]) {
-            const double rv = guess_resid(args, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
+            const double ra = guess_resid(args, args->x0, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
+            v[0] = ra * ra;
+            if (xb) {
+                const double rb = guess_resid(args, xb, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
+                v[1] = rb * rb;
+            }
             const double bv = args->b[q];
-            v[0] = rv * rv;
-            v[1] = bv * bv;
+            v[2] = bv * bv;
         }
     }
-    double tot[2];
-    if (last_block_sumk<2>(v, part, counter, red, tot) && threadIdx.x == 0) {
-        const double r0 = (tot[1] > 0.0) ? sqrt(tot[0] / tot[1]) : 0.0;
-        const bool use = isfinite(tot[0]) && tot[1] > 0.0 && r0 <= args->guess_tol;
-        stat[ST_GUESS] = use ? 1.0 + r0 : -(1.0 + (isfinite(r0) ? r0 : 0.0));
+    double tot[3];
+    if (last_block_sumk<3>(v, part, counter, red, tot) && threadIdx.x == 0) {
+        const double bb = tot[2];
+        const double ra = (bb > 0.0) ? sqrt(tot[0] / bb) : 0.0;
+        const double rb = (xb && bb > 0.0) ? sqrt(tot[1] / bb) : INFINITY;
+        const bool second = isfinite(rb) && !(ra <= rb);
+        const double r0 = second ? rb : ra;
+        const bool use = isfinite(r0) && bb > 0.0 && r0 <= args->guess_tol;
+        stat[ST_GUESS] = use ? (second ? 100.0 : 1.0) + r0 : -(1.0 + (isfinite(r0) ? fmin(r0, 1e30) : 1e30));
     }
 }
 
@@ -101,7 +110,9 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
     __shared__ double red[32];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
-    const bool guess = stat[ST_GUESS] >= 1.0;
+    const double gw = stat[ST_GUESS];
+    const bool guess = gw >= 1.0;
+    const double* xg = (gw >= 100.0) ? args->x0b : args->x0;
     double v2[2] = {0.0, 0.0};  // ||r0||^2, ||b||^2
     if (c < ncol) {
         const double* __restrict__ aP = args->aP;
@@ -118,10 +129,10 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
             const double bv = args->b[q];
             v2[1] = bv * bv;
             if (guess) {
-                const double rv = guess_resid(args, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
+                const double rv = guess_resid(args, xg, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
                 vb = (T)rv;
                 v2[0] = rv * rv;
-                x64[p] = args->x0[q];
+                x64[p] = xg[q];
             } else {
                 vb = (T)bv;
                 v2[0] = v2[1];
@@ -1136,14 +1147,14 @@ template <typename T>
 static int solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW,
                         const double* aN, const double* aS, const double* b, int maxITR,
                         double tol, double* solution, cudaStream_t s, int prec, int* pending,
-                        double* h_dst, const double* x0, double guess_tol) {
+                        double* h_dst, const double* x0, double guess_tol, const double* x0b) {
     *pending = 0;
     int rc = alloc_hierarchy<T>(g);
     if (rc != CTH_OK) return rc;
     Workspace& w = g->ws;
     {
         dim3 grd((g->ncol + 255) / 256, g->nrow[0]);
-        if (2 * (int)(grd.x * grd.y) > w.npart) {
+        if (3 * (int)(grd.x * grd.y) > w.npart) {
             set_error("partial-sum buffer too small");
             return CTH_ERR_ALLOC;
         }
@@ -1154,6 +1165,7 @@ static int solve_launch(cth_grid* g, const double* aP, const double* aE, const d
     ha->tol = tol;
     ha->maxit = maxITR;
     ha->x0 = x0;
+    ha->x0b = x0 ? x0b : nullptr;
     ha->guess_tol = guess_tol;
     k_set_args<<<1, 1, 0, s>>>(*ha, w.d_args);
     const bool graph = g->use_graphs && !g->prof.on;
@@ -1196,8 +1208,8 @@ int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st) {
     loc.nonfinite = h[ST_NONFINITE] != 0.0;
     loc.converged = h[ST_CONV] != 0.0;
     const double gw = h[ST_GUESS];
-    loc.guess = gw >= 1.0 ? 1 : (gw <= -1.0 ? -1 : 0);
-    loc.guess_residual = gw >= 1.0 ? gw - 1.0 : (gw <= -1.0 ? -gw - 1.0 : -1.0);
+    loc.guess = gw >= 100.0 ? 2 : (gw >= 1.0 ? 1 : (gw <= -1.0 ? -1 : 0));
+    loc.guess_residual = gw >= 100.0 ? gw - 100.0 : (gw >= 1.0 ? gw - 1.0 : (gw <= -1.0 ? -gw - 1.0 : -1.0));
     if (st) *st = loc;
     if (loc.nonfinite) return CTH_NONFINITE;
     return loc.converged ? CTH_OK : CTH_NOT_CONVERGED;
@@ -1211,13 +1223,17 @@ int solve_finish(cth_grid* g, int pending, cth_status* st) {
 int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
                      const double* aS, const double* b, int maxITR, double error_cnv, int precision,
                      double* solution, cudaStream_t s, int* pending, double* h_dst, const double* x0,
-                     double guess_tol) {
+                     double guess_tol, const double* x0b) {
+    if (x0 && !(guess_tol >= 0.0 && guess_tol <= 10.0)) {
+        set_error("initial-guess threshold must be in [0, 10]");
+        return CTH_ERR_ARG;
+    }
     if (precision == CTH_PREC_MIXED)
         return solve_launch<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending,
-                                   h_dst, x0, guess_tol);
+                                   h_dst, x0, guess_tol, x0b);
     if (precision == CTH_PREC_FP64)
         return solve_launch<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending,
-                                    h_dst, x0, guess_tol);
+                                    h_dst, x0, guess_tol, x0b);
     set_error("unknown precision mode");
     return CTH_ERR_ARG;
 }

@@ -33,16 +33,29 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     p->neutral.ndt_n = p->ndt_n;
     p->neutral.ndt_m = p->ndt_m;
     int worst = 0;
+    // the learned warm start reads rhoe, nu_m, B and the previous corrections,
+    // which the ion step does not change: it runs on its own stream, concurrent
+    // with the ion step, and joins before the potential sweep
+    const bool learned = p->net && p->phi.warm_start == 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (learned) {
+        if (!fs->net_stream) {
+            CTH_CUDA(cudaStreamCreateWithFlags(&fs->net_stream, cudaStreamNonBlocking));
+            for (int k = 0; k < 2; k++) CTH_CUDA(cudaEventCreateWithFlags(&fs->net_event[k], cudaEventDisableTiming));
+        }
+        CTH_CUDA(cudaEventRecord(fs->net_event[0], s));
+        CTH_CUDA(cudaStreamWaitEvent(fs->net_stream, fs->net_event[0], 0));
+        rc = cth_unet_predict_dphi(p->net, fs, fs->net_stream);
+        if (rc < 0) return rc;
+        CTH_CUDA(cudaEventRecord(fs->net_event[1], fs->net_stream));
+    }
     if (p->itime % p->ndt_i == 0) {
         rc = cth_ion_step(fs, gx, gr, &p->ion, stream, &R->ion);
         if (rc < 0) return rc;
         R->ran_ion = 1;
         if (R->ion.solver_rc > worst) worst = R->ion.solver_rc;
     }
-    if (p->net && p->phi.warm_start == 1) {
-        rc = cth_unet_predict_dphi(p->net, fs, stream);
-        if (rc < 0) return rc;
-    }
+    if (learned) CTH_CUDA(cudaStreamWaitEvent(s, fs->net_event[1], 0));
     rc = cth_solve_phi_pc(fs, &p->phi, stream, &R->phi);
     if (rc < 0) return rc;
     if (R->phi.solver_rc > worst) worst = R->phi.solver_rc;

@@ -446,12 +446,14 @@ struct Stats {
 
 // input channels of the warm-start network from the field planes (library
 // layout, grid cell (i, j) -> pixel (j-1, i-1)): log10 n_e, log10 nu_m, |B|,
-// Re / Im of the microwave field (zero here), previous potential correction;
-// normalised, zero outside the grid
+// the microwave field (zero here), the first potential corrections of the
+// steps before the previous one and of the previous one; normalised, zero
+// outside the grid.  With the two previous corrections the network can follow
+// the plasma oscillation of the correction (period a few steps at 1e17 m^-3).
 __global__ void k_features(const double* __restrict__ rhoe, const double* __restrict__ nu_m,
                            const double* __restrict__ Bx, const double* __restrict__ Br,
-                           const double* __restrict__ dphi_prev, int ni, int nj, int ld, int H, int W, Stats st,
-                           float* __restrict__ out) {
+                           const double* __restrict__ dphi_prev2, const double* __restrict__ dphi_prev, int ni,
+                           int nj, int ld, int H, int W, Stats st, float* __restrict__ out) {
     const int npix = H * W;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npix; q += gridDim.x * blockDim.x) {
         const int y = q / W, x = q % W;
@@ -461,6 +463,7 @@ __global__ void k_features(const double* __restrict__ rhoe, const double* __rest
             f[0] = (float)log10(fmax(rhoe[p], 1.0));
             f[1] = (float)log10(fmax(nu_m[p], 1.0));
             f[2] = (float)sqrt(Bx[p] * Bx[p] + Br[p] * Br[p]);
+            f[4] = (float)dphi_prev2[p];
             f[5] = (float)dphi_prev[p];
 #pragma unroll
             for (int c = 0; c < 6; c++) f[c] = (f[c] - st.in_mean[c]) / st.in_std[c];
@@ -535,6 +538,7 @@ struct cth_unet {
     float* cw = nullptr;     // per-output-channel loss weights
     Stats stats{};
     float* feat = nullptr;   // input features of the warm-start prediction
+    long long launches = 0;  // kernels launched by the forward passes and predictions
     struct Pool { TensorRef src; bf16* dst; int C, Ho, Wo; bf16* ddst; };
     struct Up { bf16* src; int C, Hi, Wi; TensorRef dst; bf16* dsrc; TensorRef ddst; };
     std::vector<Pool> pools;
@@ -712,6 +716,7 @@ void conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
 
 int forward(cth_unet* n, const float* in, cudaStream_t s) {
     const size_t npx = (size_t)n->H * n->W;
+    n->launches += 2 + (long long)n->convs.size() + (long long)n->pools.size() + (long long)n->ups.size();
     k_pack<<<grid1(npx * n->cpad), 256, 0, s>>>(in, n->cin, (int)npx, n->cpad, n->x_in);
     const auto& C = n->convs;
     int up = 0;
@@ -801,6 +806,8 @@ void cth_unet_destroy(cth_unet* n) {
 }
 
 long long cth_unet_nparams(const cth_unet* n) { return n ? (long long)n->nparam : -1; }
+
+long long cth_unet_launch_count(const cth_unet* n) { return n ? n->launches : -1; }
 
 int cth_unet_set_params(cth_unet* n, const float* host, long long count) {
     if (!n || !host || count != (long long)n->nparam) { set_error("cth_unet_set_params: invalid arguments"); return CTH_ERR_ARG; }
@@ -914,16 +921,16 @@ int cth_unet_features(cth_unet* n, cth_fields* fs, float* out, void* stream) {
         return CTH_ERR_ARG;
     }
     CTH_CUDA(cudaSetDevice(n->device));
-    const char* names[5] = {"rhoe", "nu_m", "Bx", "Br", "dphi_prev"};
-    const double* q[5];
-    for (int k = 0; k < 5; k++) {
+    const char* names[6] = {"rhoe", "nu_m", "Bx", "Br", "dphi_prev2", "dphi_prev"};
+    const double* q[6];
+    for (int k = 0; k < 6; k++) {
         q[k] = field_ptr(fs, names[k]);
         if (!q[k]) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
     }
     cudaStream_t s = (cudaStream_t)stream;
     const size_t npx = (size_t)n->H * n->W;
-    k_features<<<grid1(npx), 256, 0, s>>>(q[0], q[1], q[2], q[3], q[4], fs->g->ni, fs->g->nj, fs->g->ld, n->H, n->W,
-                                          n->stats, out);
+    k_features<<<grid1(npx), 256, 0, s>>>(q[0], q[1], q[2], q[3], q[4], q[5], fs->g->ni, fs->g->nj, fs->g->ld,
+                                          n->H, n->W, n->stats, out);
     CTH_CUDA(cudaGetLastError());
     return CTH_OK;
 }
@@ -946,6 +953,7 @@ int cth_unet_predict_dphi(cth_unet* n, cth_fields* fs, void* stream) {
     const int ncell = fs->g->ni * fs->g->nj;
     k_unpack<<<grid1((size_t)ncell), 256, 0, s>>>(n->out, n->cout, 2, fs->g->ni, fs->g->nj, fs->g->ld, n->W,
                                                    n->stats.out_mean[2], n->stats.out_std[2], prev, dst);
+    n->launches += 2;  // features, unpack
     CTH_CUDA(cudaGetLastError());
     return CTH_OK;
 }

@@ -3,8 +3,8 @@
 No counterpart in the reference (its SMG solves always start from zero).  A
 4-level U-Net of the device library (``cth_unet_*``: hand-written bf16
 tensor-core convolutions, forward and backward, Adam) maps the state before the
-potential sweep -- log10 n_e, log10 nu_m, |B| and the previous step's first
-correction -- to the change of this step's first correction from the previous
+potential sweep -- log10 n_e, log10 nu_m, |B| and the first corrections of
+the two previous steps -- to the change of this step's first correction from the previous
 one; the guess is the previous correction plus that change (an untrained,
 zero-output network is the plain previous-step guess).  The multigrid then
 starts from that guess and converges to the unchanged tolerance; a guess whose
@@ -26,7 +26,7 @@ import numpy as np
 from . import capi
 
 CIN, COUT, BASE = 6, 3, 32
-CHANNELS_IN = ("log10_ne", "log10_nu_m", "absB", "re_E_mw", "im_E_mw", "dphi_prev")
+CHANNELS_IN = ("log10_ne", "log10_nu_m", "absB", "E_mw", "dphi_prev2", "dphi_prev")
 CHANNELS_OUT = ("re_E_mw", "im_E_mw", "dphi")
 
 
@@ -105,6 +105,10 @@ class UNet:
         v = np.empty(self.n, np.float32)
         capi.check(self._L.cth_unet_get_grads(self.handle, v.ctypes.data, self.n), allow_positive=False)
         return v
+
+    def launch_count(self) -> int:
+        """Kernels launched by forward passes and predictions since creation."""
+        return int(self._L.cth_unet_launch_count(self.handle))
 
     def set_stats(self, stats):
         self.stats = np.ascontiguousarray(stats, dtype=np.float32).copy()
@@ -198,7 +202,8 @@ def close_case(c):
 
 def collect_snapshots(pkg, net, ni, nj, nsteps, seeds, bias_range=(-10.0, 60.0), precision=1, skip=2,
                       device=0):
-    """Plain runs (zero start) of nsteps steps per seed; snapshot k pairs the
+    """Plain runs (previous-step warm start, same stopping rule as from zero) of
+    nsteps steps per seed; snapshot k pairs the
     state before step k (features, previous correction) with the change of
     step k's first potential correction from the previous one.  Returns (X [n, H, W, 6], Y [n, H, W, 3], mask [H, W])
     as un-normalised CUDA tensors (net's stats must be the identity)."""
@@ -210,7 +215,7 @@ def collect_snapshots(pkg, net, ni, nj, nsteps, seeds, bias_range=(-10.0, 60.0),
         fs, P = c["fs"], c["P"]
         for blk in ("ion", "rhoe", "eps", "neutral"):
             P[blk]["precision"] = precision
-        P["phi"].update(precision=precision, warm_start=1, guess_max_relres=1.0)
+        P["phi"].update(precision=precision, warm_start=2, guess_max_relres=1.0)
         for k in range(nsteps):
             x = net.features(fs)
             r = fs.fluid_step(c["gx"], c["gr"], P)
@@ -243,8 +248,7 @@ def fit_stats(X, Y, mask):
         return mu.cpu().numpy(), sd.cpu().numpy()
     im, isd = ms(xin)
     om, osd = ms(yout)
-    for k in (3, 4):
-        im[k], isd[k] = 0.0, 1.0
+    im[3], isd[3] = 0.0, 1.0
     for k in (0, 1):
         om[k], osd[k] = 0.0, 1.0
     return np.concatenate([im, isd, om, osd]).astype(np.float32)

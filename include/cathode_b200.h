@@ -53,7 +53,8 @@ typedef struct cth_status {
     int iterations;          /* V-cycles (SMG replacement) or sweeps (SOR replacement) */
     int converged;           /* 1 when the stopping rule was met                        */
     int nonfinite;           /* 1 when a NaN/Inf residual or update was seen             */
-    int guess;               /* SMG: 0 started from zero; 1 from the caller's guess;
+    int guess;               /* SMG: 0 started from zero; 1 from the caller's guess
+                                (2: from the second candidate, see warm_start 1);
                                 -1 guess rejected by its threshold (started from zero)  */
     double residual;         /* SMG: final ||b-Ax||_2/||b||_2; SOR: last max relative update */
     double initial_residual; /* SMG: ||b||_2 of the grid cells; SOR: 0                  */
@@ -131,7 +132,7 @@ int cth_smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const dou
                       cth_status* st);
 /* Same solve from the device plane x0 as initial guess (no counterpart in the
  * reference, whose SMG always starts from zero): the cycles start from x0 when
- * ||b - A x0||_2 <= max_guess_relres ||b||_2, otherwise from zero (the plain
+ * ||b - A x0||_2 <= max_guess_relres ||b||_2 (at most 10), otherwise from zero (the plain
  * solve is the fallback); st->guess / guess_residual report which.  The
  * stopping rule is unchanged, so the converged residual is the same; x0 may
  * alias solution. */
@@ -264,11 +265,13 @@ typedef struct cth_phi_params {
     int precision;      /* CTH_PREC_MIXED or CTH_PREC_FP64           */
     /* initial guess of the first inner (SMG) solve; no counterpart in the
      * reference, whose solves start from zero.  0: zero (reference);
-     * 1: the store's plane "dphi_guess" (written by the caller, e.g. the
-     * learned predictor); 2: the plane "dphi_prev" = the first-iteration
-     * correction of the previous call.  With warm_start != 0 the first
-     * iteration's correction is copied into "dphi_prev".  A guess whose
-     * relative residual exceeds guess_max_relres is dropped (zero start). */
+     * 1: the better (smaller residual) of the store's plane "dphi_guess"
+     * (written by the caller, e.g. the learned predictor) and "dphi_prev";
+     * 2: "dphi_prev" = the first-iteration correction of the previous call.
+     * With warm_start != 0 the first iteration's correction is copied into
+     * "dphi_prev" (its former content into "dphi_prev2").  A guess whose
+     * relative residual exceeds guess_max_relres
+     * (at most 10) is dropped (zero start). */
     int warm_start;
     double guess_max_relres;
 } cth_phi_params;
@@ -469,6 +472,7 @@ typedef struct cth_unet cth_unet;
 cth_unet* cth_unet_create(int H, int W, int cin, int cout, int base, int device);
 void cth_unet_destroy(cth_unet* n);
 long long cth_unet_nparams(const cth_unet* n);
+long long cth_unet_launch_count(const cth_unet* n);  /* kernels of forward passes and predictions */
 int cth_unet_set_params(cth_unet* n, const float* host, long long count);  /* resets Adam */
 int cth_unet_get_params(const cth_unet* n, float* host, long long count);
 int cth_unet_get_grads(const cth_unet* n, float* host, long long count);
@@ -483,8 +487,9 @@ int cth_unet_train_step(cth_unet* n, const float* in, const float* target, const
                         float lr, int t, void* stream, double* loss);
 /* Warm start of the potential predictor-corrector from a field store (grid of
  * at most H x W cells, cell (i, j) -> pixel (j-1, i-1)).  Input channels
- * (cin = 6): log10 rhoe, log10 nu_m, |B| from Bx and Br, two zero channels
- * reserved for the microwave field, and "dphi_prev"; each normalised with the
+ * (cin = 6): log10 rhoe, log10 nu_m, |B| from Bx and Br, a zero channel
+ * reserved for the microwave field, "dphi_prev2" and "dphi_prev" (the first
+ * corrections of the two previous steps); each normalised with the
  * stats (mean[6], std[6]); output channel 2, de-normalised (output mean[3],
  * std[3]), is the change of the first-iteration correction from "dphi_prev"
  * (a zero output reproduces the previous-step guess).  cth_unet_features writes the

@@ -107,11 +107,11 @@ def test_learned_warm_start_of_the_potential(pkg, cuda_device):
         for r in rec:
             assert r["residual"] <= 1e-10
     learned = recs[1]
-    assert all(r["guess"] in (1, -1) for r in learned)
+    assert all(r["guess"] in (1, 2, -1) for r in learned)
     res = [r["guess_residual"] for r in learned]
     prev = [r["guess_residual"] for r in recs[2]]
     print("first-solve cycles zero/prev/learned:", [np.mean([r["cycles"] for r in recs[w]]) for w in (0, 2, 1)],
           "guess residual prev/learned:", np.mean(prev), np.mean(res))
-    # the network refines the previous-step guess it starts from
-    assert np.mean(res) < 1.0 and np.mean(res) <= 1.1 * np.mean(prev)
+    # the device takes the better of the network's guess and the previous step's
+    assert np.mean(res) < 1.0 and np.mean(res) <= np.mean(prev) * (1.0 + 1e-9)
     net.close()
