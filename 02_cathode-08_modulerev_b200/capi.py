@@ -35,6 +35,7 @@ EXPORTS = (
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
     "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
+    "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_params", "cth_unet_get_params",
     "cth_unet_get_grads", "cth_unet_set_loss_weights", "cth_unet_forward", "cth_unet_backward",
     "cth_unet_train_step", "cth_unet_set_stats", "cth_unet_features", "cth_unet_predict_dphi",
@@ -59,6 +60,16 @@ class Status(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class CMat2(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double * 2) for k in ("A", "B", "C", "D")]
+
+
+class SParamParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("S11_mag", "S11_arg_deg", "S21_mag", "S21_arg_deg", "S12_mag",
+                                               "S12_arg_deg", "S22_mag", "S22_arg_deg", "Z0", "phase_pre_deg",
+                                               "omegam", "epsr_diele", "h0_stab", "dh_stab", "dl_cable")]
 
 
 class MWParams(ctypes.Structure):
@@ -232,6 +243,18 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_smg_solve_guess_dev.argtypes = [_vp] + [_vp] * 7 + [ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                                               ctypes.c_int, _vp, _vp, ctypes.POINTER(Status)]
     L.cth_smg_solve_guess_dev.restype = ctypes.c_int
+    _c2 = ctypes.c_double * 2
+    L.cth_cmat2_mul.argtypes = [ctypes.POINTER(CMat2)] * 3
+    L.cth_cmat2_mul.restype = ctypes.c_int
+    L.cth_cmat2_inv.argtypes = [ctypes.POINTER(CMat2)] * 2
+    L.cth_cmat2_inv.restype = ctypes.c_int
+    L.cth_sparam_to_abcd.argtypes = [ctypes.POINTER(_c2)] * 4 + [ctypes.c_double, ctypes.POINTER(CMat2)]
+    L.cth_sparam_to_abcd.restype = ctypes.c_int
+    L.cth_abcd_to_sparam.argtypes = [ctypes.POINTER(CMat2), ctypes.c_double] + [ctypes.POINTER(_c2)] * 4
+    L.cth_abcd_to_sparam.restype = ctypes.c_int
+    L.cth_sparam_setup.argtypes = [ctypes.POINTER(SParamParams), ctypes.POINTER(_c2 * 4),
+                                   ctypes.POINTER(ctypes.c_double)]
+    L.cth_sparam_setup.restype = ctypes.c_int
     L.cth_unet_create.argtypes = [ctypes.c_int] * 6
     L.cth_unet_create.restype = _vp
     L.cth_unet_destroy.argtypes = [_vp]

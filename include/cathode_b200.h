@@ -457,6 +457,29 @@ int cth_residual_noalloc(int ni, int nj, int ld, const int* i_bl, const int* j_b
                          const double* aS, const double* b, const double* x, double* r,
                          double* rnorm, double* bnorm, void* stream);
 
+/* Two-port feed helpers (host) -------------------------------------------------
+ * CmpMat2 (cmpMat2.hpp:8-34): 2x2 complex matrices, complex values as
+ * {re, im}.  sParamToABCD / ABCDToSParam (initialModule.hpp:1689-1739) for the
+ * reference impedance Z0: CTH_ERR_ARG where the reference throws (|S21| or the
+ * denominator below 1e-14).  cth_sparam_setup: the S-parameter set-up of
+ * initialModule.hpp:107-192 (polar input in degrees; pre-line of phase
+ * phase_pre_deg; stub length h0_stab -> h0_stab + dh_stab in a dielectric of
+ * epsr_diele at omegam, applied as a shunt admittance at the stub junction;
+ * cable length change dl_cable as a phase factor); S = {S11, S21, S12, S22}. */
+typedef struct cth_cmat2 {
+    double A[2], B[2], C[2], D[2];
+} cth_cmat2;
+typedef struct cth_sparam_params {
+    double S11_mag, S11_arg_deg, S21_mag, S21_arg_deg, S12_mag, S12_arg_deg, S22_mag, S22_arg_deg;
+    double Z0, phase_pre_deg, omegam, epsr_diele, h0_stab, dh_stab, dl_cable;
+} cth_sparam_params;
+int cth_cmat2_mul(const cth_cmat2* X, const cth_cmat2* Y, cth_cmat2* out);
+int cth_cmat2_inv(const cth_cmat2* X, cth_cmat2* out);
+int cth_sparam_to_abcd(const double S11[2], const double S21[2], const double S12[2], const double S22[2], double Z0,
+                       cth_cmat2* T);
+int cth_abcd_to_sparam(const cth_cmat2* T, double Z0, double S11[2], double S21[2], double S12[2], double S22[2]);
+int cth_sparam_setup(const cth_sparam_params* p, double S[4][2], double* cable_phase_deg);
+
 /* Learned warm start ---------------------------------------------------------
  * No counterpart in the reference.  A 4-level convolutional U-Net (3x3
  * convolutions, ReLU, 2x2 average pooling, nearest upsampling, skip

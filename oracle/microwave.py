@@ -289,3 +289,48 @@ def er_rect_system(ne: np.ndarray, nu: np.ndarray, epsr: np.ndarray, p: dict):
         aN[i, j] = 0.0
         aS[i, 2] = 0.0
     return dict(aP=aP, aE=aE, aW=aW, aN=aN, aS=aS, b=b, mask=mask)
+
+
+# ---------------------------------------------------------------------------
+# two-port feed helpers (include/cmpMat2.hpp:8-34, include/initialModule.hpp:
+# 107-192 and 1689-1739), restated with numpy complex scalars
+# ---------------------------------------------------------------------------
+def s_to_abcd(S11, S21, S12, S22, Z0):
+    """sParamToABCD (initialModule.hpp:1689-1710); ValueError where the reference throws."""
+    if abs(S21) < 1.0e-14:
+        raise ValueError("S21 is too small")
+    den = 2.0 * S21
+    return np.array([[((1 + S11) * (1 - S22) + S12 * S21) / den, Z0 * ((1 + S11) * (1 + S22) - S12 * S21) / den],
+                     [1.0 / Z0 * ((1 - S11) * (1 - S22) - S12 * S21) / den,
+                      ((1 - S11) * (1 + S22) + S12 * S21) / den]])
+
+
+def abcd_to_s(T, Z0):
+    """ABCDToSParam (initialModule.hpp:1717-1739)."""
+    A, B, C, D = T[0, 0], T[0, 1], T[1, 0], T[1, 1]
+    den = A + B / Z0 + C * Z0 + D
+    if abs(den) < 1.0e-14:
+        raise ValueError("denominator is too small")
+    return ((A + B / Z0 - C * Z0 - D) / den, 2.0 / den, 2.0 * (A * D - B * C) / den, (-A + B / Z0 - C * Z0 + D) / den)
+
+
+def sparam_setup(p: dict):
+    """S-parameters after the stub and cable corrections (initialModule.hpp:107-192)."""
+    def polar(mag, arg):
+        return complex(mag * np.cos(arg / 180.0 * np.pi), mag * np.sin(arg / 180.0 * np.pi))
+    S = [polar(p[f"{n}_mag"], p[f"{n}_arg_deg"]) for n in ("S11", "S21", "S12", "S22")]
+    ph = p["phase_pre_deg"] / 180.0 * np.pi
+    Z0 = p["Z0"]
+    Tpre = np.array([[np.cos(ph), 1j * Z0 * np.sin(ph)], [1j * np.sin(ph) / Z0, np.cos(ph)]])
+    Tbase = s_to_abcd(*S, Z0)
+    c0 = np.sqrt(1.0 / (8.8541878128e-12 * p["epsr_diele"] * 1.2566370614e-6))
+    beta = p["omegam"] / c0
+    t0, t1 = np.tan(beta * p["h0_stab"]), np.tan(beta * (p["h0_stab"] + p["dh_stab"]))
+    if abs(t0) < 1e-14 or abs(t1) < 1e-14:
+        raise ValueError("tan(beta*l) is too small")
+    dYs = (-1j / Z0 / t1) - (-1j / Z0 / t0)
+    Tcorr = np.array([[1.0, 0.0], [dYs, 1.0]])
+    Tstub = Tpre @ Tcorr @ np.linalg.inv(Tpre) @ Tbase
+    S11, S21, S12, S22 = abcd_to_s(Tstub, Z0)
+    q = np.exp(-1j * beta * p["dl_cable"])
+    return (S11, S21 * q, S12 * q, S22 * q * q), beta * p["dl_cable"] / np.pi * 180.0
