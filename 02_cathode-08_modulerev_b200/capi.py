@@ -35,7 +35,7 @@ EXPORTS = (
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
     "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
-    "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
+    "cth_update_energy_profile", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_params", "cth_unet_get_params",
     "cth_unet_get_grads", "cth_unet_set_loss_weights", "cth_unet_forward", "cth_unet_backward",
     "cth_unet_train_step", "cth_unet_set_stats", "cth_unet_features", "cth_unet_predict_dphi",
@@ -60,6 +60,14 @@ class Status(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class EnergyParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("dx", "dr", "rmin", "omegam", "masse")]
+
+
+class EnergyResult(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("Px", "Pr", "Pp", "power_sum")]
 
 
 class CMat2(ctypes.Structure):
@@ -243,6 +251,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_smg_solve_guess_dev.argtypes = [_vp] + [_vp] * 7 + [ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                                               ctypes.c_int, _vp, _vp, ctypes.POINTER(Status)]
     L.cth_smg_solve_guess_dev.restype = ctypes.c_int
+    L.cth_update_energy_profile.argtypes = [_vp, _vp, _vp, ctypes.POINTER(EnergyParams)] + [_vp] * 7 + \
+        [ctypes.POINTER(EnergyResult)]
+    L.cth_update_energy_profile.restype = ctypes.c_int
     _c2 = ctypes.c_double * 2
     L.cth_cmat2_mul.argtypes = [ctypes.POINTER(CMat2)] * 3
     L.cth_cmat2_mul.restype = ctypes.c_int

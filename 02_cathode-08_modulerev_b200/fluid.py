@@ -221,6 +221,17 @@ class Fields:
                                     rhon=R.neutral.solver[0].iterations),
                     phi_first=R.phi.first.as_dict())
 
+    def update_energy_profile(self, grid_x, grid_r, prm: dict, E1x, E1r, E1p, J1x, J1r, J1p, stream=None) -> dict:
+        """Absorbed microwave power (emfieldModule.hpp:7630-7790): complex128 device
+        planes (nj+2, ld) in, J planes and the store's Pabsx/Pabsr/Pabsp/Pabs out."""
+        p = capi.EnergyParams(**{k: prm[k] for k, _ in capi.EnergyParams._fields_})
+        r = capi.EnergyResult()
+        s = 0 if stream is None else stream.cuda_stream
+        ptr = [ctypes.c_void_p(t.data_ptr()) for t in (E1x, E1r, E1p, J1x, J1r, J1p)]
+        capi.check(self._L.cth_update_energy_profile(self._h, grid_x._h, grid_r._h, ctypes.byref(p), *ptr, s,
+                                                     ctypes.byref(r)), allow_positive=False)
+        return {k: getattr(r, k) for k, _ in capi.EnergyResult._fields_}
+
     def check_cfl(self, dt: float, CFL: float, masse: float, rmin: float, dr: float, flag_adp_dt: int = 0,
                   stream=None) -> dict:
         """FluidModule::check_CFL (fluidModule.hpp:57-115); returns dt, CFL and the maxima."""

@@ -457,6 +457,26 @@ int cth_residual_noalloc(int ni, int nj, int ld, const int* i_bl, const int* j_b
                          const double* aS, const double* b, const double* x, double* r,
                          double* rnorm, double* bnorm, void* stream);
 
+/* Absorbed microwave power: the volume part of EmfieldModule::
+ * update_energy_profile (emfieldModule.hpp:7630-7790).  E1x, E1r, E1p are
+ * complex (re, im interleaved) device planes of the library layout holding the
+ * field on the x-faces (gx.E1x, face i-1/2), r-faces (gr.E1r, face j-1/2) and
+ * cells (gc.E1p); gx / gr are grids over the x-face / r-face block unions
+ * (the store's grid gives the cell blocks).  Writes J1x, J1r, J1p (complex
+ * planes: J = sigma E with the magnetised cold-plasma tensor of rhoe, nu_m1,
+ * Bx, Br), the store's planes Pabsx, Pabsr, Pabsp (Re(J.E*)/2) and Pabs (their
+ * cell profile) on the block cells, and the volume integrals.  The port,
+ * reflection and field-rescaling part (flag_mwRef, :7792-8105) is not here. */
+typedef struct cth_energy_params {
+    double dx, dr, rmin, omegam, masse;
+} cth_energy_params;
+typedef struct cth_energy_result {
+    double Px, Pr, Pp, power_sum;  /* W: integrals over the x-faces, r-faces, cells */
+} cth_energy_result;
+int cth_update_energy_profile(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_energy_params* prm,
+                              const void* E1x, const void* E1r, const void* E1p, void* J1x, void* J1r,
+                              void* J1p, void* stream, cth_energy_result* res);
+
 /* Two-port feed helpers (host) -------------------------------------------------
  * CmpMat2 (cmpMat2.hpp:8-34): 2x2 complex matrices, complex values as
  * {re, im}.  sParamToABCD / ABCDToSParam (initialModule.hpp:1689-1739) for the

@@ -334,3 +334,70 @@ def sparam_setup(p: dict):
     S11, S21, S12, S22 = abcd_to_s(Tstub, Z0)
     q = np.exp(-1j * beta * p["dl_cable"])
     return (S11, S21 * q, S12 * q, S22 * q * q), beta * p["dl_cable"] / np.pi * 180.0
+
+
+def energy_profile(E1x, E1r, E1p, rhoe, nu_m1, Bx, Br, p, xblocks, rblocks, cblocks):
+    """Absorbed-power part of update_energy_profile (emfieldModule.hpp:7630-7790)
+    on [i][j] arrays; blocks are (i0, i1, j0, j1) inclusive index boxes (a cell
+    in several boxes is counted once, as a block union).  Returns J1x, J1r,
+    J1p, Pabsx, Pabsr, Pabsp, Pabs (zero outside the blocks) and (Px, Pr, Pp)."""
+    e0, me, w = 1.60217662e-19, p["masse"], p["omegam"]
+    dx, dr = p["dx"], p["dr"]
+    ni2, nj2 = rhoe.shape
+    r = p["rmin"] + (np.arange(nj2) - 0.5) * dr
+    EPS = 1e-100 + 1e-100j
+
+    def mask(blocks):
+        m = np.zeros((ni2, nj2), bool)
+        for i0, i1, j0, j1 in blocks:
+            m[i0:i1 + 1, j0:j1 + 1] = True
+        return m
+
+    def sig(nu, rho, bx, br):
+        den = me * (nu + 1j * w) + EPS
+        hx, hr = e0 * bx / den, e0 * br / den
+        coef = rho * e0 * e0 / den / (1.0 + hx * hx + hr * hr + EPS)
+        return coef, hx, hr
+
+    out = {k: np.zeros((ni2, nj2), complex) for k in ("J1x", "J1r", "J1p")}
+    out.update({k: np.zeros((ni2, nj2)) for k in ("Pabsx", "Pabsr", "Pabsp", "Pabs")})
+    P = [0.0, 0.0, 0.0]
+    mx, mr, mc = mask(xblocks), mask(rblocks), mask(cblocks)
+    for i, j in zip(*np.nonzero(mx)):
+        rL, rR = (r[j] + r[j - 1]) / 2, (r[j] + r[j + 1]) / 2
+        c, hx, hr = sig((nu_m1[i, j] + nu_m1[i - 1, j]) / 2, (rhoe[i, j] + rhoe[i - 1, j]) / 2,
+                        (Bx[i, j] + Bx[i - 1, j]) / 2, (Br[i, j] + Br[i - 1, j]) / 2)
+        Ex = E1x[i, j]
+        Er = (rL * (E1r[i, j] + E1r[i - 1, j]) + rR * (E1r[i, j + 1] + E1r[i - 1, j + 1])) / (4 * r[j])
+        Ep = (E1p[i, j] + E1p[i - 1, j]) / 2
+        J = c * hx * hr * Er + c * hr * Ep + c * (1 + hx * hx) * Ex
+        out["J1x"][i, j] = J
+        out["Pabsx"][i, j] = 0.5 * (J * np.conj(Ex)).real
+        P[0] += out["Pabsx"][i, j] * dx * dr * 2 * np.pi * r[j]
+    for i, j in zip(*np.nonzero(mr)):
+        rt = (r[j - 1] + r[j]) / 2
+        c, hx, hr = sig((nu_m1[i, j] + nu_m1[i, j - 1]) / 2, (rhoe[i, j] + rhoe[i, j - 1]) / 2,
+                        (r[j] * Bx[i, j] + r[j - 1] * Bx[i, j - 1]) / (2 * rt),
+                        (r[j] * Br[i, j] + r[j - 1] * Br[i, j - 1]) / (2 * rt))
+        Ex = (r[j] * (E1x[i, j] + E1x[i + 1, j]) + r[j - 1] * (E1x[i, j - 1] + E1x[i + 1, j - 1])) / (4 * rt)
+        Er = E1r[i, j]
+        Ep = (r[j] * E1p[i, j] + r[j - 1] * E1p[i, j - 1]) / (2 * rt)
+        J = c * (1 + hr * hr) * Er + c * (-hx) * Ep + c * hx * hr * Ex
+        out["J1r"][i, j] = J
+        out["Pabsr"][i, j] = 0.5 * (J * np.conj(Er)).real
+        P[1] += out["Pabsr"][i, j] * dx * dr * 2 * np.pi * rt
+    for i, j in zip(*np.nonzero(mc)):
+        qL = (r[j - 1] + r[j]) / 2 / (r[j] + 1e-100)
+        qR = (r[j + 1] + r[j]) / 2 / (r[j] + 1e-100)
+        c, hx, hr = sig(nu_m1[i, j], rhoe[i, j], Bx[i, j], Br[i, j])
+        Ex = (E1x[i, j] + E1x[i + 1, j]) / 2
+        Er = (qR * E1r[i, j + 1] + qL * E1r[i, j]) / 2
+        Ep = E1p[i, j]
+        J = c * hx * Er + c * Ep + c * (-hr) * Ex
+        out["J1p"][i, j] = J
+        out["Pabsp"][i, j] = 0.5 * (J * np.conj(Ep)).real
+        P[2] += out["Pabsp"][i, j] * dx * dr * 2 * np.pi * r[j]
+    for i, j in zip(*np.nonzero(mc)):
+        out["Pabs"][i, j] = ((out["Pabsx"][i, j] + out["Pabsx"][i + 1, j]) / 2
+                             + (out["Pabsr"][i, j] + out["Pabsr"][i, j + 1]) / 2 + out["Pabsp"][i, j])
+    return out, tuple(P)

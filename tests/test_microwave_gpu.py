@@ -131,3 +131,45 @@ def test_mw_er_full_size(pkg, cuda_device):
     m[1:ni + 1, 2:nj + 1] = True
     assert np.linalg.norm(r[m]) / np.linalg.norm(A[5][m]) < 2e-10
     g.close()
+
+
+@pytest.mark.parametrize("kind", ["rectangle", "cathode"])
+def test_energy_profile_matches_oracle(pkg, cuda_device, kind):
+    """Absorbed microwave power (update_energy_profile, emfieldModule.hpp:7630-7790)
+    with the magnetised conductivity tensor: J, Pabs planes and the volume
+    integrals against the oracle, random fields, relative 1e-12."""
+    import torch
+    from oracle import microwave as omw
+    geo = pkg.fluid.cathode_geometry() if kind == "cathode" else pkg.fluid.rectangle_geometry(48, 24)
+    ni, nj = geo["ni"], geo["nj"]
+    rng = np.random.default_rng(7)
+    shp = (ni + 2, nj + 2)
+    E = {k: rng.normal(size=shp) * 100 + 1j * rng.normal(size=shp) * 100 for k in ("E1x", "E1r", "E1p")}
+    f = dict(rhoe=10 ** rng.uniform(15, 18, shp), nu_m1=10 ** rng.uniform(8, 10, shp),
+             Bx=rng.uniform(-0.25, 0.25, shp), Br=rng.uniform(-0.25, 0.25, shp))
+    dr = 5e-3 / nj
+    prm = dict(dx=10e-3 / ni, dr=dr, rmin=0.0, omegam=2.67e10, masse=9.10938356e-31)
+    g = pkg.Grid(ni, nj, geo["ib"], geo["jb"])
+    gx = pkg.Grid(ni, nj, geo["fxi"], geo["fxj"])
+    gr = pkg.Grid(ni, nj, geo["fri"], geo["frj"])
+    fs = pkg.Fields(g)
+    for k, v in f.items():
+        fs.upload(k, v)
+    dev = {k: torch.complex(g.to_device(v.real), g.to_device(v.imag)).contiguous() for k, v in E.items()}
+    J = [torch.zeros_like(dev["E1x"]) for _ in range(3)]
+    r = fs.update_energy_profile(gx, gr, prm, dev["E1x"], dev["E1r"], dev["E1p"], *J)
+    blocks = lambda I, Jb: [(int(I[b][0]), int(I[b][1]), int(Jb[b][0]), int(Jb[b][1])) for b in range(len(I))]
+    ref, P = omw.energy_profile(E["E1x"], E["E1r"], E["E1p"], f["rhoe"], f["nu_m1"], f["Bx"], f["Br"], prm,
+                                blocks(geo["fxi"], geo["fxj"]), blocks(geo["fri"], geo["frj"]),
+                                blocks(geo["ib"], geo["jb"]))
+    for k, t in zip(("J1x", "J1r", "J1p"), J):
+        got = t[:, :ni + 2].cpu().numpy().T
+        assert np.abs(got - ref[k]).max() <= 1e-12 * np.abs(ref[k]).max(), k
+    for k in ("Pabsx", "Pabsr", "Pabsp", "Pabs"):
+        got = fs.download(k)
+        assert np.abs(got - ref[k]).max() <= 1e-12 * np.abs(ref[k]).max(), k
+    for a, b in zip((r["Px"], r["Pr"], r["Pp"]), P):
+        assert a == pytest.approx(b, rel=1e-11)
+    fs.close()
+    for x in (g, gx, gr):
+        x.close()
