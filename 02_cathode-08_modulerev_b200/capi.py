@@ -35,7 +35,7 @@ EXPORTS = (
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
     "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
-    "cth_update_energy_profile", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
+    "cth_batch_steps", "cth_update_energy_profile", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_params", "cth_unet_get_params",
     "cth_unet_get_grads", "cth_unet_set_loss_weights", "cth_unet_forward", "cth_unet_backward",
     "cth_unet_train_step", "cth_unet_set_stats", "cth_unet_features", "cth_unet_predict_dphi",
@@ -157,6 +157,12 @@ class StepParams(ctypes.Structure):
                 ("net", ctypes.c_void_p)]
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [("fs", ctypes.c_void_p), ("gx", ctypes.c_void_p), ("gr", ctypes.c_void_p),
+                ("params", ctypes.POINTER(StepParams)), ("rc", ctypes.c_int), ("steps_done", ctypes.c_int),
+                ("seconds", ctypes.c_double)]
+
+
 class StepResult(ctypes.Structure):
     _fields_ = [("ion", IonResult), ("phi", PCResult), ("rhoe", PCResult), ("eps", PCResult),
                 ("neutral", NeutralResult), ("cfl", CFL), ("ran_ion", ctypes.c_int), ("ran_rhon", ctypes.c_int),
@@ -251,6 +257,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_smg_solve_guess_dev.argtypes = [_vp] + [_vp] * 7 + [ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                                               ctypes.c_int, _vp, _vp, ctypes.POINTER(Status)]
     L.cth_smg_solve_guess_dev.restype = ctypes.c_int
+    L.cth_batch_steps.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_double)]
+    L.cth_batch_steps.restype = ctypes.c_int
     L.cth_update_energy_profile.argtypes = [_vp, _vp, _vp, ctypes.POINTER(EnergyParams)] + [_vp] * 7 + \
         [ctypes.POINTER(EnergyResult)]
     L.cth_update_energy_profile.restype = ctypes.c_int

@@ -74,6 +74,33 @@ def _param_fields(cls, prm: dict) -> dict:
     return {k: (prm[k] if k in prm or k not in _PARAM_DEFAULTS else _PARAM_DEFAULTS[k]) for k, _ in cls._fields_}
 
 
+def step_params(params: dict) -> capi.StepParams:
+    """cth_step_params from a parameter dict (step fields + the sub-step blocks)."""
+    P = capi.StepParams()
+    for k in ("itime", "ndt_i", "ndt_n", "ndt_m", "flag_adp_dt", "dt", "CFL", "gtime"):
+        setattr(P, k, params[k])
+    for blk, cls in (("ion", capi.IonParams), ("phi", capi.PhiParams), ("rhoe", capi.SGParams),
+                     ("eps", capi.SGParams), ("transport", capi.TransportParams)):
+        setattr(P, blk, cls(**_param_fields(cls, params[blk])))
+    net = params.get("net")
+    P.net = net.handle if net is not None else None
+    nb = params["neutral"]
+    P.neutral = capi.NeutralParams(**{k: nb[k] for k, _ in capi.NeutralParams._fields_
+                                      if k not in ("n_pos_box", "pos_box", "do_rhon", "do_rhom")})
+    boxes = params.get("pos_boxes", [])
+    P.neutral.n_pos_box = len(boxes)
+    for q, bx in enumerate(boxes):
+        for k in range(4):
+            P.neutral.pos_box[q][k] = int(bx[k])
+    return P
+
+
+def step_params_back(P: capi.StepParams, params: dict):
+    """Copy the step fields the step updates (itime, dt, CFL, gtime) back into the dict."""
+    for k in ("itime", "dt", "CFL", "gtime"):
+        params[k] = getattr(P, k)
+
+
 class Fields:
     """A cth_fields store bound to a Grid."""
 
@@ -189,28 +216,12 @@ class Fields:
         """One time step (src/main.cpp:170-251) through cth_fluid_step; params holds
         the step fields and the sub-step blocks (ion, phi, rhoe, eps, neutral,
         transport) as dicts, plus pos_boxes; itime, dt, CFL and gtime are updated."""
-        P = capi.StepParams()
-        for k in ("itime", "ndt_i", "ndt_n", "ndt_m", "flag_adp_dt", "dt", "CFL", "gtime"):
-            setattr(P, k, params[k])
-        for blk, cls in (("ion", capi.IonParams), ("phi", capi.PhiParams), ("rhoe", capi.SGParams),
-                         ("eps", capi.SGParams), ("transport", capi.TransportParams)):
-            setattr(P, blk, cls(**_param_fields(cls, params[blk])))
-        net = params.get("net")
-        P.net = net.handle if net is not None else None
-        nb = params["neutral"]
-        P.neutral = capi.NeutralParams(**{k: nb[k] for k, _ in capi.NeutralParams._fields_
-                                          if k not in ("n_pos_box", "pos_box", "do_rhon", "do_rhom")})
-        boxes = params.get("pos_boxes", [])
-        P.neutral.n_pos_box = len(boxes)
-        for q, bx in enumerate(boxes):
-            for k in range(4):
-                P.neutral.pos_box[q][k] = int(bx[k])
+        P = step_params(params)
         R = capi.StepResult()
         s = 0 if stream is None else stream.cuda_stream
         capi.check(self._L.cth_fluid_step(self._h, grid_x._h, grid_r._h, ctypes.byref(P), s, ctypes.byref(R)),
                    allow_positive=False)
-        for k in ("itime", "dt", "CFL", "gtime"):
-            params[k] = getattr(P, k)
+        step_params_back(P, params)
         return dict(solver_rc=R.solver_rc, ran_ion=R.ran_ion, cfl=R.cfl.CFL, dt=R.cfl.dt,
                     errors=dict(rhoi=R.ion.error_rhoi, Uix=R.ion.error_Uix, Uir=R.ion.error_Uir, Uip=R.ion.error_Uip,
                                 phi=R.phi.error_phi, rhoe=R.rhoe.error_phi, rhoeps=R.eps.error_phi,

@@ -62,6 +62,7 @@ MAXIT = 30
 
 NDIV_MW = 100
 LEARN_SEEDS, LEARN_STEPS, LEARN_EPOCHS = 3, 110, 8  # snapshots: seeds x (steps - 2), the timed range
+BATCH_N, BATCH_STEPS = 64, 10                       # batched sweep: instances, timed steps each
 PROGNOSTIC = ("rhoe", "rhoi", "rhoeps", "Te", "rhon", "rhom", "phi", "Ex", "Er", "Uix", "Uir", "Uip")
 STATE = ("rhoe", "rhoi", "rhon", "rhom", "Te", "Bx", "Br", "rhoeps", "rhoe_old")
 
@@ -287,6 +288,46 @@ def linear_systems(pkg, dev, stream, steps=10):
 
 
 # --------------------------------------------------------------------------
+def batched_sweep(pkg, device, rank, n=BATCH_N, steps=BATCH_STEPS):
+    """Config 2: n seeded discharges (grid sizes 64x128 .. 256x512, bias -10..60 V,
+    microwave power 2..16 W) advanced together by host worker threads with the
+    autotuned cycle shapes and mixed precision, against the same steps run one
+    instance after another with plain FP64 multigrid from zero."""
+    import numpy as np
+    import torch
+    B = pkg.batch
+    t0 = time.perf_counter()
+    cases = B.sweep_instances(pkg, n=n, seed=3 + rank, device=device)
+    setup_s = time.perf_counter() - t0
+    threads = max(1, min(n, os.cpu_count() or 1))
+    B.batch_steps(cases, steps=2, nthreads=threads)                # graphs, lazily allocated planes
+    tuned = B.autotune(cases, steps=2)
+    B.batch_steps(cases, steps=1, nthreads=threads)
+    wall, rc, secs = B.batch_steps(cases, steps=steps, nthreads=threads)
+    cells = sum(c["ni"] * c["nj"] for c in cases)
+    for c in cases:
+        B.set_precision(c, pkg.capi.CTH_PREC_FP64)
+        B.set_cycle(c, 1, 1, True)
+    B.sequential_steps(cases, steps=1)
+    seq = B.sequential_steps(cases, steps=steps)
+    by = {}
+    for c, t in zip(cases, secs):
+        by.setdefault(f"{c['nj']}x{c['ni']}", []).append(steps / t)
+    B.close(cases)
+    torch.cuda.synchronize()
+    return {
+        "instances": n, "steps_each": steps, "threads": threads, "rc": max(rc),
+        "instance_steps_per_s": n * steps / wall, "cell_steps_per_s": cells * steps / wall,
+        "sequential_fp64": {"instance_steps_per_s": n * steps / seq, "cell_steps_per_s": cells * steps / seq},
+        "speedup_vs_sequential_fp64": seq / wall,
+        "steps_per_s_per_instance_by_size": {k: float(np.mean(v)) for k, v in sorted(by.items())},
+        "autotune": tuned, "setup_s": setup_s,
+        "timing": "host wall clock around the batch call (all instance streams synchronised inside)",
+        "workload": "seeded instances, sizes drawn from 64x128, 128x256, 192x384, 256x512 (r x z), "
+                    "bias U(-10, 60) V, Pmw U(2, 16) W (recorded; absorbed power is an input field)",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -504,6 +545,7 @@ def main():
     e2e_s = float(te.item())
 
     lin = linear_systems(pkg, dev, stream) if rank == 0 else None
+    sweep = batched_sweep(pkg, local, rank) if rank == 0 else None
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -545,6 +587,7 @@ def main():
                     "(previous correction + the network's predicted change) and the previous correction, judged "
                     "on the device by the initial residual; zero start when both exceed ||b||"},
         "mixed_zero_start": {"value": world * args.steps / (ms_plain / 1e3), "unit": UNIT},
+        "batched_sweep": sweep,
         "warm_start": {
             "previous_step": {"value": world * args.steps / (ms_prev / 1e3), "unit": UNIT,
                               "first_phi_solve_cycles_mean": float(np.mean([f["iterations"] for f in first_prev])),

@@ -457,6 +457,26 @@ int cth_residual_noalloc(int ni, int nj, int ld, const int* i_bl, const int* j_b
                          const double* aS, const double* b, const double* x, double* r,
                          double* rnorm, double* bnorm, void* stream);
 
+/* Batched instances (the I-V sweeps; no counterpart in the reference, which runs
+ * one discharge per process) -------------------------------------------------
+ * cth_batch_steps advances n independent instances (own grids, store, step
+ * parameters) by `steps` time steps each, with min(nthreads, n) host worker
+ * threads; instance k belongs to thread k % T, which interleaves its instances
+ * step by step on one stream per instance.  Results are those of the same
+ * steps run one instance after another.  Returns the worst status (negative if
+ * an instance failed; that instance stops, the others continue); per item: rc,
+ * steps done, wall seconds; *wall_seconds = the whole batch. */
+typedef struct cth_batch_item {
+    cth_fields* fs;
+    cth_grid* gx;
+    cth_grid* gr;
+    cth_step_params* params;
+    int rc;
+    int steps_done;
+    double seconds;
+} cth_batch_item;
+int cth_batch_steps(cth_batch_item* items, int n, int steps, int nthreads, double* wall_seconds);
+
 /* Absorbed microwave power: the volume part of EmfieldModule::
  * update_energy_profile (emfieldModule.hpp:7630-7790).  E1x, E1r, E1p are
  * complex (re, im interleaved) device planes of the library layout holding the
