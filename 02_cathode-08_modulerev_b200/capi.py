@@ -166,7 +166,7 @@ class BatchItem(ctypes.Structure):
 class StepResult(ctypes.Structure):
     _fields_ = [("ion", IonResult), ("phi", PCResult), ("rhoe", PCResult), ("eps", PCResult),
                 ("neutral", NeutralResult), ("cfl", CFL), ("ran_ion", ctypes.c_int), ("ran_rhon", ctypes.c_int),
-                ("ran_rhom", ctypes.c_int), ("solver_rc", ctypes.c_int)]
+                ("ran_rhom", ctypes.c_int), ("net_ran", ctypes.c_int), ("solver_rc", ctypes.c_int)]
 
 
 class CathodeError(RuntimeError):

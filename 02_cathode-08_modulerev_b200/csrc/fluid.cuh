@@ -25,7 +25,9 @@ struct cth_fields {
     int ion_box_total[4] = {};
     bool aux_ready = false;
     cudaStream_t net_stream = nullptr;   // learned warm-start inference, concurrent with the ion step
-    cudaEvent_t net_event[2] = {nullptr, nullptr};                    // streams / events of the concurrent ion solves
+    cudaEvent_t net_event[2] = {nullptr, nullptr};
+    int net_misses = 0;                  // consecutive predictions that the device judge did not choose
+    long long net_runs = 0, net_wins = 0;                    // streams / events of the concurrent ion solves
     cudaStream_t aux_stream[2] = {};
     cudaEvent_t aux_event[3] = {};
     std::map<std::string, double*> planes;
@@ -129,27 +131,35 @@ __device__ void grid_reduce(const double (&s)[K], unsigned maxmask, double* __re
     if (!am_last) return;
     __threadfence();
     // the last block combines the partials with all its threads: thread t takes the
-    // partials t, t + blockDim, ... in order, then a fixed warp / cross-warp tree
-    __shared__ double fin[32];
+    // partials t, t + blockDim, ... in order (the K entries side by side, so their
+    // L2 loads are in flight together), then a fixed warp / cross-warp tree
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] = 0.0;
+#pragma unroll 2
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+        double u[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) u[k] = __ldcg(part + (size_t)k * nb + q);
+#pragma unroll
+        for (int k = 0; k < K; k++) acc[k] = ((maxmask >> k) & 1u) ? fmax(acc[k], u[k]) : acc[k] + u[k];
+    }
+#pragma unroll
     for (int k = 0; k < K; k++) {
         const bool mx = (maxmask >> k) & 1u;
-        double v = 0.0;
-        for (int q = threadIdx.x; q < nb; q += blockDim.x) {
-            const double u = __ldcg(part + (size_t)k * nb + q);
-            v = mx ? fmax(v, u) : v + u;
-        }
+        double v = acc[k];
         for (int o = 16; o > 0; o >>= 1) {
             const double u = __shfl_down_sync(0xffffffffu, v, o);
             v = mx ? fmax(v, u) : v + u;
         }
-        if (lane == 0) fin[wid] = v;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t = fin[0];
-            for (int w = 1; w < nw; w++) t = mx ? fmax(t, fin[w]) : t + fin[w];
-            out[k] = t;
-        }
-        __syncthreads();
+        if (lane == 0) red[k][wid] = v;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const bool mx = (maxmask >> k) & 1u;
+        double t = red[k][0];
+        for (int w = 1; w < nw; w++) t = mx ? fmax(t, red[k][w]) : t + red[k][w];
+        out[k] = t;
     }
     if (threadIdx.x == 0) *counter = 0u;
 }

@@ -158,7 +158,7 @@ struct cth_grid {
     cudaStream_t cap[2] = {nullptr, nullptr};  // capture streams
     bool use_graphs = true;
     bool pdl = true;  // relaxations launched with programmatic dependent launch
-    bool tail = true; // coarse levels of at most 16 rows run as one cluster launch
+    bool tail = false; // coarse levels of at most 16 rows run as one cluster launch (off: measured slower)
     int tail_types = 0;  // bit per precision (float, double, complex) whose tail kernel fits
     cudaStream_t pending_stream = nullptr;  // stream of the last enqueued graph solve
 };

@@ -52,6 +52,7 @@ static __device__ inline bool last_block_sum(double v, double* part, unsigned in
     if (!am_last) return false;
     __threadfence();
     double acc = 0.0;
+#pragma unroll 4
     for (int k = threadIdx.x; k < nb; k += blockDim.x) acc += __ldcg(part + k);
     acc = block_sum(acc, red);
     if (threadIdx.x == 0) {
@@ -497,12 +498,23 @@ static __device__ inline bool last_block_sumk(const double (&v)[K], double* part
     __syncthreads();
     if (!am_last) return false;
     __threadfence();
+    // the K partial sums of one position are loaded together (their L2 loads in
+    // flight at once); each sum keeps its order over the positions
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] = 0.0;
+#pragma unroll 2
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        double u[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) u[k] = __ldcg(part + k * nb + b);
+#pragma unroll
+        for (int k = 0; k < K; k++) acc[k] += u[k];
+    }
 #pragma unroll
     for (int k = 0; k < K; k++) {
-        double acc = 0.0;
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += __ldcg(part + k * nb + b);
-        acc = block_sum(acc, red);
-        if (threadIdx.x == 0) total[k] = acc;
+        const double t = block_sum(acc[k], red);
+        if (threadIdx.x == 0) total[k] = t;
     }
     if (threadIdx.x == 0) *counter = 0u;
     return true;

@@ -36,7 +36,14 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     // the learned warm start reads rhoe, nu_m, B and the previous corrections,
     // which the ion step does not change: it runs on its own stream, concurrent
     // with the ion step, and joins before the potential sweep
-    const bool learned = p->net && p->phi.warm_start == 1;
+    // a predictor that the judge has not chosen for kNetPatience predictions runs
+    // only every kNetProbe steps (the other steps start from the previous
+    // correction), so it costs nothing while it does not help
+    constexpr int kNetPatience = 4, kNetProbe = 8;
+    const bool learned = p->net && p->phi.warm_start == 1 &&
+                         (fs->net_misses < kNetPatience || p->itime % kNetProbe == 0);
+    cth_phi_params phi = p->phi;
+    if (p->phi.warm_start == 1 && !learned) phi.warm_start = 2;
     cudaStream_t s = (cudaStream_t)stream;
     if (learned) {
         if (!fs->net_stream) {
@@ -56,7 +63,13 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
         if (R->ion.solver_rc > worst) worst = R->ion.solver_rc;
     }
     if (learned) CTH_CUDA(cudaStreamWaitEvent(s, fs->net_event[1], 0));
-    rc = cth_solve_phi_pc(fs, &p->phi, stream, &R->phi);
+    rc = cth_solve_phi_pc(fs, &phi, stream, &R->phi);
+    if (learned && rc >= 0) {
+        fs->net_runs++;
+        if (R->phi.first.guess == 1) { fs->net_wins++; fs->net_misses = 0; }
+        else fs->net_misses++;
+    }
+    R->net_ran = learned ? 1 : 0;
     if (rc < 0) return rc;
     if (R->phi.solver_rc > worst) worst = R->phi.solver_rc;
     rc = cth_solve_rhoe_pc(fs, &p->rhoe, stream, &R->rhoe);

@@ -222,7 +222,7 @@ class Fields:
         capi.check(self._L.cth_fluid_step(self._h, grid_x._h, grid_r._h, ctypes.byref(P), s, ctypes.byref(R)),
                    allow_positive=False)
         step_params_back(P, params)
-        return dict(solver_rc=R.solver_rc, ran_ion=R.ran_ion, cfl=R.cfl.CFL, dt=R.cfl.dt,
+        return dict(solver_rc=R.solver_rc, ran_ion=R.ran_ion, net_ran=R.net_ran, cfl=R.cfl.CFL, dt=R.cfl.dt,
                     errors=dict(rhoi=R.ion.error_rhoi, Uix=R.ion.error_Uix, Uir=R.ion.error_Uir, Uip=R.ion.error_Uip,
                                 phi=R.phi.error_phi, rhoe=R.rhoe.error_phi, rhoeps=R.eps.error_phi,
                                 rhon=R.neutral.error_rhon, rhom=R.neutral.error_rhom),

@@ -313,7 +313,8 @@ def run_steps(pkg, c, nsteps, warm_start, net=None, precision=1):
             raise RuntimeError(f"solve did not converge: {r}")
         f = r["phi_first"]
         rec.append(dict(cycles=f["iterations"], guess=f["guess"], guess_residual=f["guess_residual"],
-                        residual=f["residual"], ms=e0.elapsed_time(e1), phi_iterations=r["iterations"]["phi"]))
+                        residual=f["residual"], ms=e0.elapsed_time(e1), phi_iterations=r["iterations"]["phi"],
+                        net_ran=r["net_ran"]))
     P["net"] = None
     return rec
 

@@ -95,7 +95,7 @@ class Grid:
         capi.check(self._L.cth_grid_set_graphs(self._h, int(enable)), allow_positive=False)
 
     def set_tail(self, enable: bool):
-        """Fused coarse tail (levels of at most 16 rows in one cluster launch) on / off."""
+        """Fused coarse tail (levels of at most 16 rows in one cluster launch) on / off (default off)."""
         capi.check(self._L.cth_grid_set_tail(self._h, int(enable)), allow_positive=False)
 
     def set_cycle(self, nu_pre: int, nu_post: int):

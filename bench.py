@@ -335,6 +335,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cathode", choices=["cathode", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="profiling mode: after --warmup steps run this many mixed steps inside the NVTX range "
+                         "'timed_step' and exit (no other legs, no JSON line)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch every multigrid kernel individually (profilers cannot see kernels inside "
+                         "conditional graphs); same kernels, host convergence checks")
     args = ap.parse_args()
     rank, world, local = env_rank()
     if args.impl == "reference":
@@ -428,7 +434,7 @@ def main():
             ms += e0.elapsed_time(e1)
             mw_solves += int("mw" in last)
             if first is not None:
-                first.append(last["phi_first"])
+                first.append(dict(last["phi_first"], net_ran=last["net_ran"]))
             if last["solver_rc"] != 0:
                 raise RuntimeError(f"an inner solve did not converge: {last}")
         launches = sum(x.launch_count() for x in grids) + (net.launch_count() if net is not None else 0) - l0
@@ -436,6 +442,22 @@ def main():
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item()), launches, last, mw_solves, P
+
+    if args.no_graphs:
+        for x in grids:
+            x.set_graphs(False)
+    if args.profile_steps > 0:
+        P = reset(capi.CTH_PREC_MIXED)
+        for _ in range(args.warmup):
+            step(P)
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_push("timed_step")
+        for _ in range(args.profile_steps):
+            step(P)
+        torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_pop()
+        print(f"profiled {args.profile_steps} mixed steps after {args.warmup} warm-up steps", flush=True)
+        return 0
 
     # learned warm start: snapshots of plain mixed runs of other seeded discharges
     # (same grid, biases drawn in -10..60 V), training on the device, then the timed
@@ -576,7 +598,8 @@ def main():
             "first_phi_solve_cycles_mean": float(np.mean([f["iterations"] for f in first_learned])),
             "guess_residual_mean": float(np.mean([f["guess_residual"] for f in first_learned])),
             "fallback_rate": float(np.mean([f["guess"] == -1 for f in first_learned])),
-            "network_guess_chosen_rate": float(np.mean([f["guess"] == 1 for f in first_learned])),
+            "network_ran_steps": int(sum(f["net_ran"] for f in first_learned)),
+            "network_guess_chosen_steps": int(sum(f["net_ran"] and f["guess"] == 1 for f in first_learned)),
             "inference_ms": infer_ms,
             "network": "4-level U-Net 32/64/128/256 ch, 3x3 conv, bf16 mma.sync tensor cores, FP32 accumulate",
             "training": {"snapshots": n_snap, "held_out": n_hold, "epochs": LEARN_EPOCHS,
@@ -585,7 +608,8 @@ def main():
                          "data": f"{LEARN_SEEDS} seeded discharges x {LEARN_STEPS} plain mixed steps"},
             "note": "value = these steps: the first potential solve of each step starts from the better of "
                     "(previous correction + the network's predicted change) and the previous correction, judged "
-                    "on the device by the initial residual; zero start when both exceed ||b||"},
+                    "on the device by the initial residual; zero start when both exceed ||b||.  After 4 "
+                    "predictions in a row that the judge did not choose, the network runs every 8th step only"},
         "mixed_zero_start": {"value": world * args.steps / (ms_plain / 1e3), "unit": UNIT},
         "batched_sweep": sweep,
         "warm_start": {

@@ -86,10 +86,11 @@ int cth_grid_set_cycle(cth_grid* g, int nu_pre, int nu_post);
  * disabled, or while profiling is on, kernels are launched one by one and the
  * host tests convergence after every cycle.  Results are identical. */
 int cth_grid_set_graphs(cth_grid* g, int enable);
-/* enable (default) or disable the fused coarse tail: the multigrid levels of
+/* enable or disable (default) the fused coarse tail: the multigrid levels of
  * at most 16 rows run as one thread-block-cluster launch per cycle instead of
  * one launch per relaxation.  Same sweeps in the same order; results agree to
- * rounding. */
+ * rounding.  Off by default: the separate launches with programmatic
+ * dependent launch measured faster on the 512 x 1024 step. */
 int cth_grid_set_tail(cth_grid* g, int enable);
 
 /* Instrumentation ------------------------------------------------------------
@@ -415,8 +416,11 @@ typedef struct cth_step_params {
     cth_neutral_params neutral;
     cth_transport_params transport;
     /* learned warm start (no counterpart in the reference): with phi.warm_start
-     * == 1 and net not null, cth_unet_predict_dphi fills "dphi_guess" right
-     * before the potential predictor-corrector */
+     * == 1 and net not null, cth_unet_predict_dphi fills "dphi_guess" before the
+     * potential predictor-corrector (concurrently with the ion step).  After 4
+     * consecutive predictions that the device judge did not choose, the network
+     * runs only on steps with itime % 8 == 0 until it is chosen again; the other
+     * steps start from the previous correction (warm_start 2). */
     struct cth_unet* net;
 } cth_step_params;
 typedef struct cth_step_result {
@@ -425,6 +429,7 @@ typedef struct cth_step_result {
     cth_neutral_result neutral;
     cth_cfl cfl;
     int ran_ion, ran_rhon, ran_rhom;
+    int net_ran;          /* the learned predictor ran in this step */
     int solver_rc;             /* largest positive inner-solve return          */
 } cth_step_result;
 int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_step_params* p, void* stream,

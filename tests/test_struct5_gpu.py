@@ -155,6 +155,7 @@ def test_smg_fused_tail_matches_level_launches(pkg, cuda_device, shape):
     g = pkg.Grid(s["ni"], s["nj"], s["i_bl"], s["j_bl"])
     planes = [g.to_device(s[k]) for k in ("aP", "aE", "aW", "aN", "aS", "b")]
     for prec in (0, 1):
+        g.set_tail(True)
         x1 = g.device_plane(1)[0]
         n0 = g.launch_count()
         st1 = g.smg_solve_dev(*planes, x1, maxITR=30, error_cnv=1e-11, precision=prec)
@@ -164,7 +165,6 @@ def test_smg_fused_tail_matches_level_launches(pkg, cuda_device, shape):
         n0 = g.launch_count()
         st2 = g.smg_solve_dev(*planes, x2, maxITR=30, error_cnv=1e-11, precision=prec)
         n_level = g.launch_count() - n0
-        g.set_tail(True)
         assert st1.converged == 1 and st2.converged == 1
         assert st1.iterations == st2.iterations
         a, b = x1.cpu().numpy(), x2.cpu().numpy()

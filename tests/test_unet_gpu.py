@@ -108,6 +108,7 @@ def test_learned_warm_start_of_the_potential(pkg, cuda_device):
             assert r["residual"] <= 1e-10
     learned = recs[1]
     assert all(r["guess"] in (1, 2, -1) for r in learned)
+    assert learned[0]["net_ran"] == 1
     res = [r["guess_residual"] for r in learned]
     prev = [r["guess_residual"] for r in recs[2]]
     print("first-solve cycles zero/prev/learned:", [np.mean([r["cycles"] for r in recs[w]]) for w in (0, 2, 1)],
