@@ -308,6 +308,16 @@ void cth_fields_destroy(cth_fields* fs) {
     delete fs;
 }
 
+int cth_fields_set_warm_start(cth_fields* fs, int enable, double max_relres) {
+    if (!fs || !(max_relres >= 0.0 && max_relres <= 10.0)) {
+        set_error("cth_fields_set_warm_start: invalid arguments (threshold in [0, 10])");
+        return CTH_ERR_ARG;
+    }
+    fs->warm_fields = enable != 0;
+    fs->warm_tol = max_relres;
+    return CTH_OK;
+}
+
 double* cth_field(cth_fields* fs, const char* name) {
     if (!fs || !name) { set_error("cth_field: invalid arguments"); return nullptr; }
     cudaSetDevice(fs->g->device);

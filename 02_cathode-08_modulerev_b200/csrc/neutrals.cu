@@ -305,7 +305,8 @@ static int update_neutrals(cth_fields* fs, const cth_neutral_params* prm, cudaSt
             if (rc > solver_rc) solver_rc = rc;
         } else {
             rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                                  prm->precision, x, s, &pend[k], fs->h_solve + 8 * k);
+                                  prm->precision, x, s, &pend[k], fs->h_solve + 8 * k,
+                                  fs->warm_fields ? x : nullptr, fs->warm_tol);
         }
         return rc;
     };

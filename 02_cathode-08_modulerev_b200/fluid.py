@@ -127,6 +127,12 @@ class Fields:
             raise capi.CathodeError(capi.CTH_ERR_ALLOC, capi.last_error())
         return p
 
+    def set_warm_start(self, enable: bool, max_relres: float = 1.0):
+        """Field-valued solves (ion velocities, rhoi, rhon, rhom) start from the
+        field's current values (guess threshold max_relres); default off."""
+        capi.check(self._L.cth_fields_set_warm_start(self._h, int(enable), float(max_relres)),
+                   allow_positive=False)
+
     def plane(self, name: str):
         """Zero-copy torch view (nj+2, ld) float64 of a device plane (library layout)."""
         import torch
@@ -230,7 +236,13 @@ class Fields:
                     iterations=dict(phi=R.phi.solver.iterations, rhoe=R.rhoe.solver.iterations,
                                     eps=R.eps.solver.iterations, rhoi=R.ion.solver[3].iterations,
                                     rhon=R.neutral.solver[0].iterations),
-                    phi_first=R.phi.first.as_dict())
+                    phi_first=R.phi.first.as_dict(),
+                    guess=dict(Uix=R.ion.solver[0].guess, Uir=R.ion.solver[1].guess, Uip=R.ion.solver[2].guess,
+                               rhoi=R.ion.solver[3].guess, rhon=R.neutral.solver[0].guess,
+                               rhom=R.neutral.solver[1].guess),
+                    all_iterations=dict(Uix=R.ion.solver[0].iterations, Uir=R.ion.solver[1].iterations,
+                                        Uip=R.ion.solver[2].iterations, rhoi=R.ion.solver[3].iterations,
+                                        rhon=R.neutral.solver[0].iterations, rhom=R.neutral.solver[1].iterations))
 
     def update_energy_profile(self, grid_x, grid_r, prm: dict, E1x, E1r, E1p, J1x, J1r, J1p, stream=None) -> dict:
         """Absorbed microwave power (emfieldModule.hpp:7630-7790): complex128 device

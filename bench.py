@@ -395,6 +395,9 @@ def main():
         P["phi"]["precision"] = prec
         P["phi"].update(warm_start=warm_start, guess_max_relres=1.0)
         P["net"] = net if warm_start == 1 else None
+        # the warm-start modes also start the field-valued solves (ion velocities and
+        # density, neutrals) from the previous step's fields
+        fs.set_warm_start(warm_start != 0)
         fs.update_transport_coef(P["transport"])
         torch.cuda.synchronize(dev)
         return P
@@ -431,10 +434,11 @@ def main():
             last = step(P)
             e1.record(stream)
             e1.synchronize()
-            ms += e0.elapsed_time(e1)
+            t_step = e0.elapsed_time(e1)
+            ms += t_step
             mw_solves += int("mw" in last)
             if first is not None:
-                first.append(dict(last["phi_first"], net_ran=last["net_ran"]))
+                first.append(dict(last["phi_first"], net_ran=last["net_ran"], ms=t_step))
             if last["solver_rc"] != 0:
                 raise RuntimeError(f"an inner solve did not converge: {last}")
         launches = sum(x.launch_count() for x in grids) + (net.launch_count() if net is not None else 0) - l0
@@ -476,7 +480,12 @@ def main():
     held = pkg.learned.heldout_error(net, Xn[-n_hold:], Yn[-n_hold:], lmask)
     n_snap = int(Xn.shape[0])
     del Xn, Yn
+    # training leaves gigabytes of snapshot tensors in torch's cache and Python
+    # garbage behind: release both before any timed leg
+    import gc
+    gc.collect()
     torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
     t_learn = time.perf_counter() - t_learn
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -601,6 +610,9 @@ def main():
             "network_ran_steps": int(sum(f["net_ran"] for f in first_learned)),
             "network_guess_chosen_steps": int(sum(f["net_ran"] and f["guess"] == 1 for f in first_learned)),
             "inference_ms": infer_ms,
+            "step_ms_median": float(np.median([f["ms"] for f in first_learned])),
+            "step_ms_median_network_ran": float(np.median([f["ms"] for f in first_learned if f["net_ran"]]))
+            if any(f["net_ran"] for f in first_learned) else None,
             "network": "4-level U-Net 32/64/128/256 ch, 3x3 conv, bf16 mma.sync tensor cores, FP32 accumulate",
             "training": {"snapshots": n_snap, "held_out": n_hold, "epochs": LEARN_EPOCHS,
                          "loss_first_epoch": losses[0], "loss_last_epoch": losses[-1],
@@ -609,17 +621,20 @@ def main():
             "note": "value = these steps: the first potential solve of each step starts from the better of "
                     "(previous correction + the network's predicted change) and the previous correction, judged "
                     "on the device by the initial residual; zero start when both exceed ||b||.  After 4 "
-                    "predictions in a row that the judge did not choose, the network runs every 8th step only"},
+                    "predictions in a row that the judge did not choose, the network runs every 8th step only.  "
+                    "The ion and neutral solves start from the previous step's fields (same judge)"},
         "mixed_zero_start": {"value": world * args.steps / (ms_plain / 1e3), "unit": UNIT},
         "batched_sweep": sweep,
         "warm_start": {
             "previous_step": {"value": world * args.steps / (ms_prev / 1e3), "unit": UNIT,
+                              "step_ms_median": float(np.median([f["ms"] for f in first_prev])),
                               "first_phi_solve_cycles_mean": float(np.mean([f["iterations"] for f in first_prev])),
                               "guess_residual_mean": float(np.mean([f["guess_residual"] for f in first_prev])),
                               "fallback_rate": float(np.mean([f["guess"] != 1 for f in first_prev]))},
             "zero_start_first_phi_solve_cycles_mean": float(np.mean([f["iterations"] for f in first_zero])),
             "note": "mixed precision; the first potential solve of each step starts from the previous step's "
-                    "correction (threshold ||b-Ax0|| <= ||b||); same stopping rule"},
+                    "correction and the ion / neutral solves from the previous step's fields (threshold "
+                    "||b-Ax0|| <= ||b||); same stopping rule"},
         "microwave_solves_in_timed_steps": mw_mixed,
         "inner_iterations_last_step": last_mixed["iterations"],
         "step_breakdown_ms": parts,

@@ -307,6 +307,14 @@ int cth_check_cfl(cth_fields* fs, cth_cfl* io, void* stream);
  * copied).  Later rules win where targets coincide. */
 int cth_ghost_rules_upload(cth_fields* fs, const int* rules, int n);
 
+/* Warm start of the field-valued solves (no counterpart in the reference, whose
+ * solves start from zero): with enable != 0 the ion momentum (Uix, Uir, Uip),
+ * ion continuity (rhoi) and neutral (rhon, rhom) solves of the SMG path start
+ * from the field's values at the solve (the previous step's), when that
+ * guess's relative residual is at most max_relres (<= 10), otherwise from zero.
+ * Same stopping rule.  Default off. */
+int cth_fields_set_warm_start(cth_fields* fs, int enable, double max_relres);
+
 /* Scharfetter-Gummel predictor-correctors of the electron density
  * (cth_solve_rhoe_pc: FluidModule::solve_rhoe_wdTe_wSEE_PC, fluidModule.hpp:3082-3970)
  * and energy (cth_solve_Te_pc: solve_Te_wdTe_wSEE_PC, fluidModule.hpp:4006-4957).

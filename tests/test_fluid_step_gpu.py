@@ -153,3 +153,39 @@ def test_previous_step_warm_start(pkg, orc, cuda_device):
             x.close()
     assert its[2][0] == its[0][0]
     assert sum(its[2][1:]) < sum(its[0][1:]), its
+
+
+def test_field_warm_start(pkg, orc, cuda_device):
+    """Field-valued solves (ion velocities and density, neutrals) started from
+    the previous step's fields: every guess is judged on the device (most are
+    taken; one worse than zero falls back to the zero start), the stopping rule
+    is the same (fields within the whole-step tolerance of the oracle) and the
+    solves need no more cycles in total than from zero."""
+    nstep = 4
+    geo, ogeo, st, cfg = setup(pkg, "rectangle")
+    ref, Po = oracle_run(geo, ogeo, st, cfg, nstep)
+    alt, _ = oracle_run(geo, ogeo, st, cfg, nstep, perturb=True)
+    its = {}
+    for warm in (False, True):
+        g, gx, gr, fs = device_fields(pkg, geo, st, cfg)
+        fs.set_warm_start(warm)
+        P = {k: (dict(v) if isinstance(v, dict) else v) for k, v in cfg["params"].items()}
+        its[warm] = []
+        for step in range(nstep):
+            r = fs.fluid_step(gx, gr, P)
+            assert r["solver_rc"] == 0, r
+            its[warm].append(sum(r["all_iterations"].values()))
+            if warm:
+                # every guess is judged; one worse than zero is dropped (-1)
+                assert all(v in (1, -1) for v in r["guess"].values()), r["guess"]
+                assert sum(v == 1 for v in r["guess"].values()) >= 4, r["guess"]
+            else:
+                assert all(v == 0 for v in r["guess"].values()), r["guess"]
+        for k in CHECK:
+            got = fs.download(k)
+            tol = max(1e-8, 4.0 * _rel(alt[k], ref[k]))
+            assert _rel(got, ref[k]) <= tol, (warm, k, _rel(got, ref[k]), tol)
+        fs.close()
+        for x in (g, gx, gr):
+            x.close()
+    assert sum(its[True]) <= sum(its[False]), its
