@@ -31,7 +31,8 @@ EXPORTS = (
     "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
     "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs", "cth_grid_set_tail",
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
-    "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_field", "cth_field_upload", "cth_field_download",
+    "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_fields_upload_many",
+    "cth_fields_download_many", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
     "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
@@ -257,6 +258,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_smg_solve_guess_dev.argtypes = [_vp] + [_vp] * 7 + [ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                                               ctypes.c_int, _vp, _vp, ctypes.POINTER(Status)]
     L.cth_smg_solve_guess_dev.restype = ctypes.c_int
+    for f in ("cth_fields_upload_many", "cth_fields_download_many"):
+        getattr(L, f).argtypes = [_vp, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_vp), ctypes.c_int, _vp]
+        getattr(L, f).restype = ctypes.c_int
     L.cth_fields_set_warm_start.argtypes = [_vp, ctypes.c_int, ctypes.c_double]
     L.cth_fields_set_warm_start.restype = ctypes.c_int
     L.cth_batch_steps.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_int, ctypes.c_int,

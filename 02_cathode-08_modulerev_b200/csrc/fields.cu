@@ -301,6 +301,7 @@ void cth_fields_destroy(cth_fields* fs) {
         if (fs->ion_ops[k]) cudaFree(fs->ion_ops[k]);
     for (int k = 0; k < 4; k++)
         if (fs->ion_boxes[k]) cudaFree(fs->ion_boxes[k]);
+    if (fs->stage_many) cudaFree(fs->stage_many);
     if (fs->part) cudaFree(fs->part);
     if (fs->scal) cudaFree(fs->scal);
     if (fs->h_scal) cudaFreeHost(fs->h_scal);
@@ -355,6 +356,71 @@ int cth_field_download(cth_fields* fs, const char* name, double* host_ij) {
     const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
     CTH_CUDA(cudaMemcpyAsync(host_ij, g->ws.stage_ij, nij * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
     CTH_CUDA(cudaStreamSynchronize(g->stream));
+    return CTH_OK;
+}
+
+// staging for n [i][j] planes of the batched transfers (allocated on first use)
+static int ensure_stage_many(cth_fields* fs, int n) {
+    if (fs->stage_planes >= n) return CTH_OK;
+    cth_grid* g = fs->g;
+    if (fs->stage_many) CTH_CUDA(cudaFree(fs->stage_many));
+    fs->stage_many = nullptr;
+    fs->stage_planes = 0;
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    CTH_CUDA(cudaMalloc(&fs->stage_many, (size_t)n * nij * sizeof(double)));
+    fs->stage_planes = n;
+    return CTH_OK;
+}
+
+int cth_fields_upload_many(cth_fields* fs, const char* const* names, const double* const* host_ij, int n,
+                           void* stream) {
+    if (!fs || !names || !host_ij || n < 1) { set_error("cth_fields_upload_many: invalid arguments"); return CTH_ERR_ARG; }
+    cth_grid* g = fs->g;
+    CTH_CUDA(cudaSetDevice(g->device));
+    int rc = ensure_stage_many(fs, n);
+    if (rc != CTH_OK) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    for (int k = 0; k < n; k++) {
+        if (!names[k] || !host_ij[k]) { set_error("cth_fields_upload_many: null name or array"); return CTH_ERR_ARG; }
+        CTH_CUDA(cudaMemcpyAsync(fs->stage_many + k * nij, host_ij[k], nij * sizeof(double), cudaMemcpyHostToDevice,
+                                 s));
+    }
+    for (int k = 0; k < n; k++) {
+        double* dst = field_ptr(fs, names[k]);
+        if (!dst) { set_error("cth_fields_upload_many: allocation failed"); return CTH_ERR_ALLOC; }
+        rc = to_device_layout(g, fs->stage_many + k * nij, dst, s);
+        if (rc != CTH_OK) return rc;
+    }
+    CTH_CUDA(cudaStreamSynchronize(s));
+    return CTH_OK;
+}
+
+int cth_fields_download_many(cth_fields* fs, const char* const* names, double* const* host_ij, int n, void* stream) {
+    if (!fs || !names || !host_ij || n < 1) {
+        set_error("cth_fields_download_many: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    cth_grid* g = fs->g;
+    CTH_CUDA(cudaSetDevice(g->device));
+    int rc = ensure_stage_many(fs, n);
+    if (rc != CTH_OK) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    for (int k = 0; k < n; k++) {
+        if (!names[k] || !host_ij[k]) { set_error("cth_fields_download_many: null name or array"); return CTH_ERR_ARG; }
+        auto it = fs->planes.find(names[k]);
+        if (it == fs->planes.end()) {
+            set_error(std::string("cth_fields_download_many: no field ") + names[k]);
+            return CTH_ERR_ARG;
+        }
+        rc = from_device_layout(g, it->second, fs->stage_many + k * nij, s);
+        if (rc != CTH_OK) return rc;
+    }
+    for (int k = 0; k < n; k++)
+        CTH_CUDA(cudaMemcpyAsync(host_ij[k], fs->stage_many + k * nij, nij * sizeof(double), cudaMemcpyDeviceToHost,
+                                 s));
+    CTH_CUDA(cudaStreamSynchronize(s));
     return CTH_OK;
 }
 

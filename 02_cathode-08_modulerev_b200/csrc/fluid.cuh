@@ -26,6 +26,8 @@ struct cth_fields {
     bool aux_ready = false;
     cudaStream_t net_stream = nullptr;   // learned warm-start inference, concurrent with the ion step
     cudaEvent_t net_event[2] = {nullptr, nullptr};
+    double* stage_many = nullptr;        // staging of the batched transfers, stage_planes [i][j] planes
+    int stage_planes = 0;
     int warm_fields = 0;                 // field-valued solves start from the field's current values
     double warm_tol = 1.0;               // their guess threshold (relative residual)
     int net_misses = 0;                  // consecutive predictions that the device judge did not choose

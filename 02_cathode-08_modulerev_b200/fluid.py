@@ -157,6 +157,29 @@ class Fields:
         capi.check(self._L.cth_field_download(self._h, name.encode(), out.ctypes.data), allow_positive=False)
         return out
 
+    def _many(self, arrays: dict, fn, writable: bool, stream):
+        g = self.grid
+        names = list(arrays)
+        arrs = [arrays[k] for k in names]
+        for k, a in zip(names, arrs):
+            ok = (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and
+                  a.shape == (g.ni + 2, g.nj + 2) and (a.flags.writeable or not writable))
+            if not ok:
+                raise ValueError(f"{k}: need a C-contiguous float64 array of shape {(g.ni + 2, g.nj + 2)}")
+        n = len(names)
+        cn = (ctypes.c_char_p * n)(*[k.encode() for k in names])
+        cp = (ctypes.c_void_p * n)(*[a.ctypes.data for a in arrs])
+        s = 0 if stream is None else stream.cuda_stream
+        capi.check(fn(self._h, cn, cp, n, s), allow_positive=False)
+
+    def upload_many(self, arrays: dict, stream=None):
+        """Upload {name: [i][j] array} in one batch (one synchronisation; pinned arrays copy fastest)."""
+        self._many(arrays, self._L.cth_fields_upload_many, False, stream)
+
+    def download_many(self, arrays: dict, stream=None):
+        """Download into the given {name: [i][j] array} in one batch, after the work queued on `stream`."""
+        self._many(arrays, self._L.cth_fields_download_many, True, stream)
+
     def set_flags(self, flags: np.ndarray):
         f = np.ascontiguousarray(flags, dtype=np.uint8)
         capi.check(self._L.cth_flags_upload(self._h, f.ctypes.data), allow_positive=False)

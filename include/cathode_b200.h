@@ -226,6 +226,15 @@ void cth_fields_destroy(cth_fields* fs);
 double* cth_field(cth_fields* fs, const char* name);
 int cth_field_upload(cth_fields* fs, const char* name, const double* host_ij);
 int cth_field_download(cth_fields* fs, const char* name, double* host_ij);
+/* Batched transfers of n fields ([i][j] host arrays as for cth_field_upload /
+ * cth_field_download): all copies and layout transposes are queued on `stream`
+ * (NULL: the grid's stream), then one synchronisation.  With pinned host arrays
+ * the copies run at full link speed; the staging for n planes is allocated on
+ * the first call.  Ordered after earlier work on `stream` (pass the stream of
+ * the time step). */
+int cth_fields_upload_many(cth_fields* fs, const char* const* names, const double* const* host_ij, int n,
+                           void* stream);
+int cth_fields_download_many(cth_fields* fs, const char* const* names, double* const* host_ij, int n, void* stream);
 int cth_flags_upload(cth_fields* fs, const unsigned char* host_ij);
 /* table names: nu_elas_N nu_exc_N nu_excReso_N nu_excMeta_N nu_ionz_N nu_ionzStep_N
  * nu_excStep_N nu_super_N rate_eloss_n_N rate_eloss_m_N nui_m_N */

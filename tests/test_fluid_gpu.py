@@ -101,3 +101,25 @@ def test_check_cfl(pkg, cuda_device, adp):
     assert got["ue_max"] == pytest.approx(ref["ue_max"], rel=1e-13)
     fs.close()
     g.close()
+
+
+def test_batched_field_transfers(pkg, cuda_device):
+    """upload_many / download_many move the same bits as the per-field calls."""
+    import torch
+    g = pkg.Grid(40, 24, np.array([[1, 40]]), np.array([[1, 24]]))
+    fs = pkg.Fields(g)
+    rng = np.random.default_rng(0)
+    names = ("rhoe", "rhoi", "Te", "phi")
+    src = {k: torch.from_numpy(rng.normal(size=(42, 26))).pin_memory().numpy() for k in names}
+    fs.upload_many(src)
+    for k in names:
+        assert np.array_equal(fs.download(k), src[k]), k
+    other = {k: rng.normal(size=(42, 26)) for k in names}
+    for k in names:
+        fs.upload(k, other[k])
+    out = {k: np.zeros((42, 26)) for k in names}
+    fs.download_many(out, stream=torch.cuda.current_stream())
+    for k in names:
+        assert np.array_equal(out[k], other[k]), k
+    fs.close()
+    g.close()
