@@ -29,7 +29,7 @@ EXPORTS = (
     "cth_version", "cth_last_error", "cth_grid_create", "cth_grid_destroy", "cth_grid_ld",
     "cth_grid_levels", "cth_grid_set_cycle", "cth_smg_solve", "cth_smg_solve_dev", "cth_smg_solve_guess_dev", "cth_sor_solve",
     "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
-    "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs", "cth_grid_set_tail",
+    "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs", "cth_grid_set_tail", "cth_grid_time_relax",
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_fields_upload_many",
     "cth_fields_download_many", "cth_field", "cth_field_upload", "cth_field_download",
@@ -245,6 +245,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         getattr(L, nm).restype = ctypes.c_int
     L.cth_grid_set_graphs.argtypes = [_vp, ctypes.c_int]
     L.cth_grid_set_graphs.restype = ctypes.c_int
+    L.cth_grid_time_relax.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.cth_grid_time_relax.restype = ctypes.c_int
     L.cth_grid_set_tail.argtypes = [_vp, ctypes.c_int]
     L.cth_grid_set_tail.restype = ctypes.c_int
     L.cth_grid_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]

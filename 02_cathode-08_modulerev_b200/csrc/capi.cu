@@ -322,6 +322,17 @@ int cth_profile(cth_grid* g, int enable) {
     return CTH_OK;
 }
 
+int cth_grid_time_relax(cth_grid* g, int precision, int level, int reps, double* us_per_launch,
+                        double* bytes_per_launch) {
+    if (!g || !us_per_launch || !bytes_per_launch) {
+        set_error("cth_grid_time_relax: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    CTH_CUDA(cudaStreamSynchronize(g->stream));
+    return time_relax(g, precision, level, reps, us_per_launch, bytes_per_launch);
+}
+
 int cth_profile_read(const cth_grid* g, int cls, double* ms, long long* launches, double* bytes) {
     if (!g || cls < 0 || cls >= PROF_NCLASS) { set_error("cth_profile_read: invalid arguments"); return CTH_ERR_ARG; }
     if (ms) *ms = g->prof.ms[cls];

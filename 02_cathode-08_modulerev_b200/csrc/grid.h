@@ -181,6 +181,7 @@ int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const doub
                      double* solution, cudaStream_t s, int* pending, double* h_dst,
                      const double* x0 = nullptr, double guess_tol = 0.0, const double* x0b = nullptr);
 int solve_finish(cth_grid* g, int pending, cth_status* st);
+int time_relax(cth_grid* g, int precision, int level, int reps, double* us, double* bytes);
 int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st);
 int sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
                   const double* aN, const double* aS, const double* b, double alpha,

@@ -1266,6 +1266,66 @@ int cmg_vcycle(cth_grid* g, cudaStream_t s) {
     return n;
 }
 
+// Device time of the z-line relaxation of one level in its operating mode: reps
+// pairs of (even rows, odd rows) captured in one graph with programmatic
+// dependent launch, as the smoother runs inside a cycle, timed with CUDA events
+// on the grid's stream.  Uses the level's operator and factors of the last
+// solve of that precision; the level's x is overwritten (scratch of the cycle).
+template <typename T>
+static int time_relax_impl(cth_grid* g, int l, int reps, double* us, double* bytes) {
+    Hierarchy<T>& h = hier<T>(g);
+    if (!h.allocated) {
+        set_error("cth_grid_time_relax: no solve of this precision has run on the grid");
+        return CTH_ERR_ARG;
+    }
+    cudaStream_t cs = g->cap[0];
+    const bool prof = g->prof.on;
+    g->prof.on = false;
+    const long long l0 = g->launches;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CTH_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    for (int r = 0; r < reps; r++) {
+        relax<T>(g, l, 0, 0, 0, cs);
+        relax<T>(g, l, 1, 0, 0, cs);
+    }
+    cudaError_t e = cudaStreamEndCapture(cs, &graph);
+    g->launches = l0;
+    g->prof.on = prof;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, g->stream);  // warm
+    if (e == cudaSuccess) e = cudaEventRecord(e0, g->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, g->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, g->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cth_grid_time_relax");
+    const int nr = g->nrow[l];
+    *us = 1e3 * (double)ms / (2.0 * reps);
+    // algorithmic bytes per launch (one colour): rows x cells x 8 words
+    *bytes = 0.5 * (double)nr * g->ncol * 8.0 * sizeof(T);
+    return CTH_OK;
+}
+
+int time_relax(cth_grid* g, int precision, int level, int reps, double* us, double* bytes) {
+    if (level < 0 || level >= g->nlev || reps < 1 || reps > 1000) {
+        set_error("cth_grid_time_relax: level or repetitions out of range");
+        return CTH_ERR_ARG;
+    }
+    if (precision == CTH_PREC_MIXED) return time_relax_impl<float>(g, level, reps, us, bytes);
+    if (precision == CTH_PREC_FP64) return time_relax_impl<double>(g, level, reps, us, bytes);
+    set_error("unknown precision mode");
+    return CTH_ERR_ARG;
+}
+
 // dynamic shared memory limits for the line kernels (called once per grid)
 int configure_kernels(cth_grid* g) {
     const int smem64 = (int)line_smem<double>(g->bd, 2);

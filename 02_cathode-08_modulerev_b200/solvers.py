@@ -98,6 +98,14 @@ class Grid:
         """Fused coarse tail (levels of at most 16 rows in one cluster launch) on / off (default off)."""
         capi.check(self._L.cth_grid_set_tail(self._h, int(enable)), allow_positive=False)
 
+    def time_relax(self, precision: int, level: int = 0, reps: int = 50):
+        """(µs per launch, algorithmic bytes per launch) of one level's z-line
+        relaxation, back-to-back in a graph as inside a cycle."""
+        us, by = ctypes.c_double(), ctypes.c_double()
+        capi.check(self._L.cth_grid_time_relax(self._h, precision, level, reps, ctypes.byref(us), ctypes.byref(by)),
+                   allow_positive=False)
+        return us.value, by.value
+
     def set_cycle(self, nu_pre: int, nu_post: int):
         capi.check(self._L.cth_grid_set_cycle(self._h, nu_pre, nu_post), allow_positive=False)
 

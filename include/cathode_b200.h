@@ -110,6 +110,15 @@ int cth_grid_set_tail(cth_grid* g, int enable);
 long long cth_launch_count(const cth_grid* g);
 int cth_profile(cth_grid* g, int enable);
 int cth_profile_read(const cth_grid* g, int cls, double* ms, long long* launches, double* bytes);
+/* cth_grid_time_relax: device time per launch of the z-line relaxation of one
+ * multigrid level in its operating mode -- `reps` pairs of (even rows, odd
+ * rows) captured in one CUDA graph with programmatic dependent launch, as the
+ * smoother runs inside a cycle -- and the algorithmic bytes of one launch
+ * (rows of one colour x cells x 8 words).  Needs a previous solve of that
+ * precision on the grid (its operator and factors); overwrites that level's
+ * cycle scratch.  Synchronises the grid's stream. */
+int cth_grid_time_relax(cth_grid* g, int precision, int level, int reps, double* us_per_launch,
+                        double* bytes_per_launch);
 
 /* SMG replacement (host arrays) ----------------------------------------------
  * Drop-in for solver_SMG (include/solverFuncs.hpp:26-163): solves the 5-point

@@ -224,3 +224,20 @@ def test_smg_initial_guess(pkg, cuda_device):
         assert st3.guess == 1 and st3.iterations == 0 and st3.converged == 1
         assert bool((x3 == x_ref).all())
     g.close()
+
+
+def test_time_relax_reports_level_times(pkg, cuda_device):
+    """The pipelined relaxation timing runs on the last solve's operator and
+    leaves the next solve's result unchanged."""
+    s = pkg.workloads.poisson_slab(ni=200, nj=100, seed=2)
+    g = pkg.Grid(s["ni"], s["nj"], s["i_bl"], s["j_bl"])
+    planes = [g.to_device(s[k]) for k in ("aP", "aE", "aW", "aN", "aS", "b")]
+    x1 = g.device_plane(1)[0]
+    st1 = g.smg_solve_dev(*planes, x1, maxITR=30, error_cnv=1e-11, precision=1)
+    for level in (0, 1):
+        us, by = g.time_relax(1, level, reps=5)
+        assert us > 0 and by > 0
+    x2 = g.device_plane(1)[0]
+    st2 = g.smg_solve_dev(*planes, x2, maxITR=30, error_cnv=1e-11, precision=1)
+    assert st1.iterations == st2.iterations and bool((x1 == x2).all())
+    g.close()
