@@ -485,6 +485,180 @@ __global__ void k_unpack(const float* __restrict__ o, int cout, int c, int ni, i
     }
 }
 
+// ---------------------------------------------------------------------------
+// 3x3 convolution on the 5th-generation tensor cores (tcgen05, accumulator in
+// tensor memory).  CTA = 128 consecutive pixels of one image row (the MMA's M)
+// x N output channels, 4 warps.  Per 16 input channels the CTA stages in
+// shared memory, in the canonical K-major layout without swizzle (8-row core
+// matrices of 16 bytes, the two 8-channel halves LBO apart):
+//   A: the 3 halo rows of 130 pixels      (pixel p of halo row r at (r*130+p)*16)
+//   B: the 9 tap slabs of N x 16 weights  (channel co of tap t at (t*2N + co)*16)
+// so the A operand of tap (dy, dx) is the same layout started (dy*130+dx)*16
+// bytes further: one descriptor offset per tap, no copy.  One thread issues
+// the 9 MMAs (M=128, N, K=16), commits them to an mbarrier, and the CTA waits
+// (bounded) before the next chunk overwrites the tiles.  The epilogue reads
+// the accumulator rows (TMEM lane = pixel) with tcgen05.ld.
+// ---------------------------------------------------------------------------
+constexpr int TC_M = 128;                // pixels per CTA
+constexpr int TC_HW = TC_M + 2;          // halo row width
+constexpr int TC_A_BYTES = 2 * 3 * TC_HW * 16;
+constexpr int TC_SMEM_MIN = 46 * 1024;   // at most 4 CTAs per SM: 4 x 128 TMEM columns <= 512
+
+__host__ __device__ constexpr int tc_b_bytes(int N) { return 9 * 2 * N * 16; }
+__host__ __device__ constexpr int tc_a_off() { return 0; }
+__host__ __device__ constexpr int tc_b_off() { return (TC_A_BYTES + 127) / 128 * 128; }
+__host__ __device__ constexpr int tc_bar_off(int N) { return tc_b_off() + tc_b_bytes(N); }
+__host__ __device__ constexpr int tc_smem(int N) {
+    return (tc_bar_off(N) + 16 > TC_SMEM_MIN) ? tc_bar_off(N) + 16 : TC_SMEM_MIN;
+}
+__host__ __device__ constexpr int tc_cols(int N) { return N <= 32 ? 32 : (N <= 64 ? 64 : 128); }
+
+// shared-memory matrix descriptor, K-major without swizzle (SM100 format:
+// start >> 4 in [0,14), leading byte offset >> 4 in [16,30), stride byte
+// offset >> 4 in [32,46), version 1 in [46,48), layout type 0 in [61,64))
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// instruction descriptor of kind::f16: D F32, A and B BF16, both K-major, M = 128
+__host__ __device__ constexpr uint32_t tc_idesc(int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+    for (int it = 0; it < (1 << 20); it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) k_conv3_tc(ConvArgs a, int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char tsm[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * TC_M, y = blockIdx.y, co0 = blockIdx.z * N;
+    bf16* sA = reinterpret_cast<bf16*>(tsm + tc_a_off());
+    bf16* sB = reinterpret_cast<bf16*>(tsm + tc_b_off());
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + tc_bar_off(N));
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(tsm + tc_bar_off(N) + 8);
+    const uint32_t bar_a = smem_u32(bar);
+    constexpr uint32_t kCols = tc_cols(N);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tslot;
+    const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
+    bool ok = true;
+    int phase = 0;
+    for (int c0 = 0; c0 < a.Cin && ok; c0 += 16, phase ^= 1) {
+        // A: 3 halo rows x 130 pixels x two 8-channel halves
+        for (int idx = tid; idx < 2 * 3 * TC_HW; idx += 128) {
+            const int half = idx / (3 * TC_HW), hp = idx % (3 * TC_HW);
+            const int gy = y + hp / TC_HW - 1, gx = x0 + hp % TC_HW - 1;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W)
+                v = *reinterpret_cast<const uint4*>(a.in + ((size_t)gy * a.W + gx) * a.in_cs + a.in_coff + c0 +
+                                                    half * 8);
+            *reinterpret_cast<uint4*>(sA + ((size_t)half * 3 * TC_HW + hp) * 8) = v;
+        }
+        // B: 9 taps x two halves x N output channels
+        for (int idx = tid; idx < 9 * 2 * N; idx += 128) {
+            const int co = idx % N, half = (idx / N) % 2, tap = idx / (2 * N);
+            const uint4 v = *reinterpret_cast<const uint4*>(a.w + ((size_t)(co0 + co) * 9 + tap) * a.Cin + c0 + half * 8);
+            *reinterpret_cast<uint4*>(sB + ((size_t)tap * 2 * N + half * N + co) * 8) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t idesc = tc_idesc(N);
+#pragma unroll
+            for (int tap = 0; tap < 9; tap++) {
+                const int dy = tap / 3, dx = tap % 3;
+                const uint64_t da = tc_desc(a_base + (uint32_t)((dy * TC_HW + dx) * 16), 3 * TC_HW * 16, 128);
+                const uint64_t db = tc_desc(b_base + (uint32_t)(tap * 2 * N * 16), N * 16, 128);
+                const uint32_t acc = (c0 > 0 || tap > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                    :
+                    : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
+                         : "memory");
+        }
+        // CTA-uniform outcome, so every thread takes the same path at the barriers
+        ok = __syncthreads_and(tc_wait(bar_a, (uint32_t)phase) ? 1 : 0) != 0;
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int gx = x0 + tid;
+        const size_t pix = (size_t)y * a.W + gx;
+#pragma unroll
+        for (int cb = 0; cb < N / 32; cb++) {
+            uint32_t r[32];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 32);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (gx < a.W) {
+#pragma unroll
+                for (int j = 0; j < 32; j += 2) {
+                    const int co = co0 + cb * 32 + j;
+                    float v0 = __uint_as_float(r[j]), v1 = __uint_as_float(r[j + 1]);
+                    if (a.bias) { v0 += a.bias[co]; v1 += a.bias[co + 1]; }
+                    if (a.relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+                    if (a.gate) {
+                        const __nv_bfloat162 g =
+                            *reinterpret_cast<const __nv_bfloat162*>(a.gate + pix * a.gate_cs + a.gate_coff + co);
+                        if (!(__bfloat162float(g.x) > 0.f)) v0 = 0.f;
+                        if (!(__bfloat162float(g.y) > 0.f)) v1 = 0.f;
+                    }
+                    __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(a.out + pix * a.out_cs + a.out_coff + co);
+                    if (a.accumulate) {
+                        const __nv_bfloat162 q = *o;
+                        v0 += __bfloat162float(q.x);
+                        v1 += __bfloat162float(q.y);
+                    }
+                    *o = __floats2bfloat162_rn(v0, v1);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+}
+
 inline dim3 grid1(size_t n, int bs = 256) {
     size_t b = (n + bs - 1) / bs;
     if (b > 148 * 32) b = 148 * 32;
@@ -539,6 +713,8 @@ struct cth_unet {
     Stats stats{};
     float* feat = nullptr;   // input features of the warm-start prediction
     long long launches = 0;  // kernels launched by the forward passes and predictions
+    bool use_tc = false;     // convolutions on tcgen05 (false: warp-level mma.sync kernel)
+    int* err = nullptr;      // device flag: a tensor-core wait gave up
     struct Pool { TensorRef src; bf16* dst; int C, Ho, Wo; bf16* ddst; };
     struct Up { bf16* src; int C, Hi, Wi; TensorRef dst; bf16* dsrc; TensorRef ddst; };
     std::vector<Pool> pools;
@@ -653,6 +829,12 @@ int build(cth_unet* n) {
     CTH_CUDA(cudaMalloc(&n->dout, npx0 * n->cout * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->loss, sizeof(double)));
     CTH_CUDA(cudaMalloc(&n->cw, n->cout * sizeof(float)));
+    CTH_CUDA(cudaMalloc(&n->err, sizeof(int)));
+    CTH_CUDA(cudaMemset(n->err, 0, sizeof(int)));
+    CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(128)));
+    CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(96)));
+    CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(64)));
+    CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(32)));
     std::vector<float> ones(n->cout, 1.f);
     CTH_CUDA(cudaMemcpy(n->cw, ones.data(), n->cout * sizeof(float), cudaMemcpyHostToDevice));
     return CTH_OK;
@@ -669,6 +851,29 @@ int sync_weights(cth_unet* n, cudaStream_t s) {
     return CTH_OK;
 }
 
+// largest tcgen05 tile width (output channels) dividing Cout
+int tc_n(int cout) {
+    for (int nn : {128, 96, 64, 32})
+        if (cout % nn == 0) return nn;
+    return 0;
+}
+
+void launch_conv(cth_unet* n, const ConvArgs& a, cudaStream_t s) {
+    const int nn = n->use_tc ? tc_n(a.Cout) : 0;
+    if (nn && a.Cin % 16 == 0) {
+        dim3 grd((a.W + TC_M - 1) / TC_M, a.H, a.Cout / nn);
+        switch (nn) {
+            case 128: k_conv3_tc<128><<<grd, 128, tc_smem(128), s>>>(a, n->err); break;
+            case 96: k_conv3_tc<96><<<grd, 128, tc_smem(96), s>>>(a, n->err); break;
+            case 64: k_conv3_tc<64><<<grd, 128, tc_smem(64), s>>>(a, n->err); break;
+            default: k_conv3_tc<32><<<grd, 128, tc_smem(32), s>>>(a, n->err); break;
+        }
+        return;
+    }
+    dim3 grd((a.W + TW - 1) / TW, (a.H + TH - 1) / TH, a.Cout / 32);
+    k_conv3_fwd<<<grd, 128, 0, s>>>(a);
+}
+
 void conv_fwd(cth_unet* n, const Conv& c, cudaStream_t s) {
     ConvArgs a{};
     a.in = c.in.p; a.in_cs = c.in.cs; a.in_coff = c.in.coff; a.Cin = c.cin;
@@ -677,8 +882,7 @@ void conv_fwd(cth_unet* n, const Conv& c, cudaStream_t s) {
     a.out = c.out.p; a.out_cs = c.out.cs; a.out_coff = c.out.coff; a.Cout = c.cout;
     a.H = c.H; a.W = c.W;
     a.relu = 1;
-    dim3 grd((c.W + TW - 1) / TW, (c.H + TH - 1) / TH, c.cout / 32);
-    k_conv3_fwd<<<grd, 128, 0, s>>>(a);
+    launch_conv(n, a, s);
 }
 
 void conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
@@ -710,8 +914,7 @@ void conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
     a.gate = c.out_gate_for_din;
     a.gate_cs = c.din.cs; a.gate_coff = c.din.coff;
     a.accumulate = c.din_accumulate;
-    dim3 grd((c.W + TW - 1) / TW, (c.H + TH - 1) / TH, c.cin / 32);
-    k_conv3_fwd<<<grd, 128, 0, s>>>(a);
+    launch_conv(n, a, s);
 }
 
 int forward(cth_unet* n, const float* in, cudaStream_t s) {
@@ -800,7 +1003,7 @@ void cth_unet_destroy(cth_unet* n) {
     cudaDeviceSynchronize();
     for (void* p : n->bufs) cudaFree(p);
     for (void* p : {(void*)n->prm, (void*)n->grad, (void*)n->adam_m, (void*)n->adam_v, (void*)n->wb, (void*)n->wt,
-                    (void*)n->out, (void*)n->dout, (void*)n->loss, (void*)n->cw, (void*)n->feat})
+                    (void*)n->out, (void*)n->dout, (void*)n->loss, (void*)n->cw, (void*)n->feat, (void*)n->err})
         if (p) cudaFree(p);
     delete n;
 }
@@ -808,6 +1011,25 @@ void cth_unet_destroy(cth_unet* n) {
 long long cth_unet_nparams(const cth_unet* n) { return n ? (long long)n->nparam : -1; }
 
 long long cth_unet_launch_count(const cth_unet* n) { return n ? n->launches : -1; }
+
+int cth_unet_set_tensor_cores(cth_unet* n, int tcgen05) {
+    if (!n) { set_error("cth_unet_set_tensor_cores: null network"); return CTH_ERR_ARG; }
+    n->use_tc = tcgen05 != 0;
+    return CTH_OK;
+}
+
+int cth_unet_check(cth_unet* n) {
+    if (!n) { set_error("cth_unet_check: null network"); return CTH_ERR_ARG; }
+    CTH_CUDA(cudaSetDevice(n->device));
+    CTH_CUDA(cudaDeviceSynchronize());
+    int e = 0;
+    CTH_CUDA(cudaMemcpy(&e, n->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        set_error("cth_unet: a tensor-core convolution gave up waiting for its MMAs");
+        return CTH_ERR_CUDA;
+    }
+    return CTH_OK;
+}
 
 int cth_unet_set_params(cth_unet* n, const float* host, long long count) {
     if (!n || !host || count != (long long)n->nparam) { set_error("cth_unet_set_params: invalid arguments"); return CTH_ERR_ARG; }

@@ -110,6 +110,14 @@ class UNet:
         """Kernels launched by forward passes and predictions since creation."""
         return int(self._L.cth_unet_launch_count(self.handle))
 
+    def set_tensor_cores(self, tcgen05: bool):
+        """Convolutions on tcgen05 or on the warp-level mma.sync kernel (default)."""
+        capi.check(self._L.cth_unet_set_tensor_cores(self.handle, int(tcgen05)), allow_positive=False)
+
+    def check(self):
+        """Synchronise and raise if a tensor-core convolution's wait gave up."""
+        capi.check(self._L.cth_unet_check(self.handle), allow_positive=False)
+
     def set_stats(self, stats):
         self.stats = np.ascontiguousarray(stats, dtype=np.float32).copy()
         capi.check(self._L.cth_unet_set_stats(self.handle, self.stats.ctypes.data), allow_positive=False)

@@ -116,3 +116,30 @@ def test_learned_warm_start_of_the_potential(pkg, cuda_device):
     # the device takes the better of the network's guess and the previous step's
     assert np.mean(res) < 1.0 and np.mean(res) <= np.mean(prev) * (1.0 + 1e-9)
     net.close()
+
+
+@pytest.mark.parametrize("shape", [(24, 40), (16, 296)])
+def test_tensor_core_paths_agree(pkg, cuda_device, shape):
+    """The tcgen05 convolutions (accumulator in tensor memory) and the warp-level
+    mma.sync convolutions give the same network output and gradients up to
+    accumulation order (bf16 activations: relative 1e-2 / 3e-2), over partial
+    and several 128-pixel tiles."""
+    import torch
+    from oracle import unet
+    H, W = shape
+    rng = np.random.default_rng(5)
+    vec = unet.init_params(seed=6)
+    vec[-(3 * 32 + 3):] = rng.normal(0.0, 0.2, size=3 * 32 + 3)
+    x = torch.from_numpy(rng.normal(size=(H, W, 6)).astype(np.float32)).cuda()
+    dout = torch.from_numpy(rng.normal(size=(H, W, 3)).astype(np.float32)).cuda()
+    res = {}
+    for tc in (True, False):
+        net = pkg.learned.UNet(H, W, params=vec)
+        net.set_tensor_cores(tc)
+        out = net.forward(x)
+        net.backward(dout)
+        net.check()
+        res[tc] = (out.cpu().numpy(), net.grads())
+        net.close()
+    assert _rel(res[True][0], res[False][0]) < 1e-2, _rel(res[True][0], res[False][0])
+    assert _rel(res[True][1], res[False][1]) < 3e-2, _rel(res[True][1], res[False][1])
