@@ -13,6 +13,7 @@
 //   weight grad   dW[co][tap][ci] = sum_pixel dY[pixel][co] X[pixel+tap][ci]
 // The ReLU derivative is applied by every kernel that writes a gradient into a
 // ReLU output (gate = that output > 0), so no pre-activations are stored.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -67,6 +68,7 @@ struct ConvArgs {
     const bf16* in;
     int in_cs, in_coff, Cin;
     const bf16* w;       // [Cout][9][Cin]
+    const bf16* wtc;     // the same weights [Cin/8][9][Cout][8] (tcgen05 path)
     const float* bias;   // null: none
     bf16* out;
     int out_cs, out_coff, Cout;
@@ -255,144 +257,265 @@ __global__ void __launch_bounds__(288) k_conv3_wgrad(WgradArgs a) {
             }
 }
 
-// bias gradient db[c] += sum over pixels of dy[.][c]; 256 threads, C <= 512
-__global__ void k_bias_grad(const bf16* __restrict__ dy, int cs, int coff, int C, int npix, int ppb,
-                            float* __restrict__ db) {
-    const int c = threadIdx.x;
-    const int p0 = blockIdx.x * ppb, p1 = min(npix, p0 + ppb);
-    for (int cc = c; cc < C; cc += blockDim.x) {
-        float s = 0.f;
-        for (int p = p0; p < p1; p++) s += __bfloat162float(dy[(size_t)p * cs + coff + cc]);
-        atomicAdd(db + cc, s);
+// 8 bf16 <-> 8 floats (16-byte vectors; channel slices start on multiples of 8)
+__device__ __forceinline__ void unpack8(const uint4& v, float f[8]) {
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        f[2 * j] = __bfloat162float(h[j].x);
+        f[2 * j + 1] = __bfloat162float(h[j].y);
+    }
+}
+__device__ __forceinline__ uint4 pack8(const float f[8]) {
+    uint4 v;
+    __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&v);
+#pragma unroll
+    for (int j = 0; j < 4; j++) h[j] = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+    return v;
+}
+__device__ __forceinline__ uint4 ld8(const bf16* p) { return *reinterpret_cast<const uint4*>(p); }
+__device__ __forceinline__ void st8(bf16* p, const uint4& v) { *reinterpret_cast<uint4*>(p) = v; }
+
+// bias gradient db[c] += sum over pixels of dy[.][c].  256 threads: thread t
+// sums channels 8g..8g+7 (g = t % G, G = C/8) of every (256/G)-th pixel of the
+// block's share; the lanes are then reduced in shared memory and each channel
+// gets one atomic per block.  C a multiple of 8, at most 256.
+__global__ void __launch_bounds__(256) k_bias_grad(const bf16* __restrict__ dy, int cs, int coff, int C, int npix,
+                                                   float* __restrict__ db) {
+    __shared__ float red[256 * 8];
+    const int G = C >> 3, L = 256 / G, tid = threadIdx.x;
+    const int g = tid % G, lane = tid / G;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (lane < L)
+        for (int p = blockIdx.x * L + lane; p < npix; p += gridDim.x * L) {
+            float f[8];
+            unpack8(ld8(dy + (size_t)p * cs + coff + 8 * g), f);
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc[j] += f[j];
+        }
+#pragma unroll
+    for (int j = 0; j < 8; j++) red[tid * 8 + j] = acc[j];
+    __syncthreads();
+    if (tid < C) {
+        const int gg = tid >> 3, j = tid & 7;
+        float sum = 0.f;
+        for (int l = 0; l < L; l++) sum += red[(l * G + gg) * 8 + j];
+        atomicAdd(db + tid, sum);
     }
 }
 
-// W'[ci][tap][co] = W[co][8-tap][ci]
-__global__ void k_wtrans(const bf16* __restrict__ w, int Cout, int Cin, bf16* __restrict__ wt) {
+// bf16 copies of one convolution's FP32 weights W[co][tap][ci]: W itself, the
+// flipped transpose W'[ci][tap][co] = W[co][8-tap][ci] (input gradients), and
+// both again in the tcgen05 layout [Cin/8][9][Cout][8] (wbt of W, wtt of W')
+__global__ void k_weights(const float* __restrict__ w, int Cout, int Cin, bf16* __restrict__ wb,
+                          bf16* __restrict__ wt, bf16* __restrict__ wbt, bf16* __restrict__ wtt) {
     const size_t n = (size_t)Cout * 9 * Cin;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         const int ci = (int)(e % Cin);
         const int tap = (int)((e / Cin) % 9);
         const int co = (int)(e / ((size_t)Cin * 9));
-        wt[((size_t)ci * 9 + (8 - tap)) * Cout + co] = w[e];
+        const bf16 v = __float2bfloat16_rn(w[e]);
+        wb[e] = v;
+        wt[((size_t)ci * 9 + (8 - tap)) * Cout + co] = v;
+        wbt[(((size_t)(ci >> 3) * 9 + tap) * Cout + co) * 8 + (ci & 7)] = v;
+        // W' has Cout' = Cin and Cin' = Cout: element (co' = ci, tap' = 8 - tap, ci' = co)
+        wtt[(((size_t)(co >> 3) * 9 + (8 - tap)) * Cin + ci) * 8 + (co & 7)] = v;
     }
 }
 
-// 2x2 average pooling: out[y][x][c] = mean of in[2y..2y+1][2x..2x+1][c]
+// 2x2 average pooling: out[y][x][c] = mean of in[2y..2y+1][2x..2x+1][c]; one
+// thread per output pixel and 8 channels
 __global__ void k_pool2(const bf16* __restrict__ in, int in_cs, int in_coff, int C, int Ho, int Wo,
                         bf16* __restrict__ out, int out_cs) {
-    const size_t n = (size_t)Ho * Wo * C;
+    const int G = C >> 3, Wi = 2 * Wo;
+    const size_t n = (size_t)Ho * Wo * G;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        const size_t pix = e / C;
+        const int g = (int)(e % G);
+        const size_t pix = e / G;
         const int y = (int)(pix / Wo), x = (int)(pix % Wo);
-        const int Wi = 2 * Wo;
-        float s = 0.f;
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int k = 0; k < 4; k++)
-            s += __bfloat162float(in[((size_t)(2 * y + (k >> 1)) * Wi + 2 * x + (k & 1)) * in_cs + in_coff + c]);
-        out[pix * out_cs + c] = __float2bfloat16_rn(0.25f * s);
+        for (int k = 0; k < 4; k++) {
+            float f[8];
+            unpack8(ld8(in + ((size_t)(2 * y + (k >> 1)) * Wi + 2 * x + (k & 1)) * in_cs + in_coff + 8 * g), f);
+#pragma unroll
+            for (int j = 0; j < 8; j++) s[j] += f[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 8; j++) s[j] *= 0.25f;
+        st8(out + pix * out_cs + 8 * g, pack8(s));
     }
 }
 
 // gradient of k_pool2 added into the ReLU output it pooled:
-// din[2y+a][2x+b][c] += dout[y][x][c] / 4 where x_in > 0
+// din[2y+a][2x+b][c] += dout[y][x][c] / 4 where x_in > 0; one thread per input
+// pixel and 8 channels
 __global__ void k_pool2_bwd(const bf16* __restrict__ dout, int dout_cs, int C, int Ho, int Wo,
                             bf16* __restrict__ din, int din_cs, int din_coff, const bf16* __restrict__ gate,
                             int gate_cs, int gate_coff) {
-    const int Wi = 2 * Wo;
-    const size_t n = (size_t)4 * Ho * Wo * C;
+    const int G = C >> 3, Wi = 2 * Wo;
+    const size_t n = (size_t)4 * Ho * Wo * G;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        const size_t pi = e / C;
+        const int g = (int)(e % G);
+        const size_t pi = e / G;
         const int yi = (int)(pi / Wi), xi = (int)(pi % Wi);
-        const float g = 0.25f * __bfloat162float(dout[((size_t)(yi >> 1) * Wo + (xi >> 1)) * dout_cs + c]);
-        const bool on = __bfloat162float(gate[pi * gate_cs + gate_coff + c]) > 0.f;
-        bf16* d = din + pi * din_cs + din_coff + c;
-        *d = __float2bfloat16_rn(__bfloat162float(*d) + (on ? g : 0.f));
+        float gd[8], on[8], d[8];
+        unpack8(ld8(dout + ((size_t)(yi >> 1) * Wo + (xi >> 1)) * dout_cs + 8 * g), gd);
+        unpack8(ld8(gate + pi * gate_cs + gate_coff + 8 * g), on);
+        bf16* dp = din + pi * din_cs + din_coff + 8 * g;
+        unpack8(ld8(dp), d);
+#pragma unroll
+        for (int j = 0; j < 8; j++) d[j] = d[j] + (on[j] > 0.f ? 0.25f * gd[j] : 0.f);
+        st8(dp, pack8(d));
     }
 }
 
-// nearest 2x upsampling into a channel slice: out[y][x][c] = in[y/2][x/2][c]
+// nearest 2x upsampling into a channel slice: out[y][x][c] = in[y/2][x/2][c];
+// one thread per input pixel and 8 channels, writing the 4 children
 __global__ void k_up2(const bf16* __restrict__ in, int in_cs, int C, int Hi, int Wi, bf16* __restrict__ out,
                       int out_cs, int out_coff) {
-    const int Wo = 2 * Wi;
-    const size_t n = (size_t)4 * Hi * Wi * C;
+    const int G = C >> 3, Wo = 2 * Wi;
+    const size_t n = (size_t)Hi * Wi * G;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        const size_t po = e / C;
-        const int y = (int)(po / Wo), x = (int)(po % Wo);
-        out[po * out_cs + out_coff + c] = in[((size_t)(y >> 1) * Wi + (x >> 1)) * in_cs + c];
-    }
-}
-
-// gradient of k_up2: din[y][x][c] = sum of the 4 children's gradients
-__global__ void k_up2_bwd(const bf16* __restrict__ dout, int dout_cs, int dout_coff, int C, int Hi, int Wi,
-                          bf16* __restrict__ din, int din_cs) {
-    const int Wo = 2 * Wi;
-    const size_t n = (size_t)Hi * Wi * C;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        const size_t pi = e / C;
+        const int g = (int)(e % G);
+        const size_t pi = e / G;
         const int y = (int)(pi / Wi), x = (int)(pi % Wi);
-        float s = 0.f;
+        const uint4 v = ld8(in + pi * in_cs + 8 * g);
 #pragma unroll
         for (int k = 0; k < 4; k++)
-            s += __bfloat162float(dout[((size_t)(2 * y + (k >> 1)) * Wo + 2 * x + (k & 1)) * dout_cs + dout_coff + c]);
-        din[pi * din_cs + c] = __float2bfloat16_rn(s);
+            st8(out + ((size_t)(2 * y + (k >> 1)) * Wo + 2 * x + (k & 1)) * out_cs + out_coff + 8 * g, v);
     }
 }
 
-// FP32 NHWC input (cin channels) -> bf16 with cpad channels (zeros beyond cin)
-__global__ void k_pack(const float* __restrict__ in, int cin, int npix, int cpad, bf16* __restrict__ out) {
-    const size_t n = (size_t)npix * cpad;
+// gradient of k_up2: din[y][x][c] = sum of the 4 children's gradients; one
+// thread per input pixel and 8 channels
+__global__ void k_up2_bwd(const bf16* __restrict__ dout, int dout_cs, int dout_coff, int C, int Hi, int Wi,
+                          bf16* __restrict__ din, int din_cs) {
+    const int G = C >> 3, Wo = 2 * Wi;
+    const size_t n = (size_t)Hi * Wi * G;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % cpad);
-        const size_t p = e / cpad;
-        out[e] = __float2bfloat16_rn(c < cin ? in[p * cin + c] : 0.f);
+        const int g = (int)(e % G);
+        const size_t pi = e / G;
+        const int y = (int)(pi / Wi), x = (int)(pi % Wi);
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            float f[8];
+            unpack8(ld8(dout + ((size_t)(2 * y + (k >> 1)) * Wo + 2 * x + (k & 1)) * dout_cs + dout_coff + 8 * g), f);
+#pragma unroll
+            for (int j = 0; j < 8; j++) s[j] += f[j];
+        }
+        st8(din + pi * din_cs + 8 * g, pack8(s));
     }
 }
 
-// 1x1 output layer (linear): out[p][c] = sum_k wh[c][k] y[p][k] + bh[c], FP32
+// FP32 NHWC input (cin channels) -> bf16 with cpad channels (zeros beyond cin);
+// one thread per pixel
+__global__ void k_pack(const float* __restrict__ in, int cin, int npix, int cpad, bf16* __restrict__ out) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        for (int c0 = 0; c0 < cpad; c0 += 8) {
+            float f[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) f[j] = (c0 + j < cin) ? in[(size_t)p * cin + c0 + j] : 0.f;
+            st8(out + (size_t)p * cpad + c0, pack8(f));
+        }
+    }
+}
+
+// 1x1 output layer (linear): out[p][c] = sum_k wh[c][k] y[p][k] + bh[c], FP32;
+// one thread per pixel, the layer's weights in shared memory; C, cout <= 32
 __global__ void k_head_fwd(const bf16* __restrict__ y, int C, int npix, const float* __restrict__ wh,
                            const float* __restrict__ bh, int cout, float* __restrict__ out) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npix) return;
-    for (int c = 0; c < cout; c++) {
-        float s = bh[c];
-        for (int k = 0; k < C; k++) s += wh[c * C + k] * __bfloat162float(y[(size_t)p * C + k]);
-        out[(size_t)p * cout + c] = s;
+    __shared__ float s_w[32 * 32], s_b[32];
+    for (int e = threadIdx.x; e < cout * C; e += blockDim.x) s_w[e] = wh[e];
+    for (int e = threadIdx.x; e < cout; e += blockDim.x) s_b[e] = bh[e];
+    __syncthreads();
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        float yv[32];
+#pragma unroll
+        for (int k0 = 0; k0 < 32; k0 += 8)
+            if (k0 < C) unpack8(ld8(y + (size_t)p * C + k0), yv + k0);
+        for (int c = 0; c < cout; c++) {
+            float s = s_b[c];
+#pragma unroll
+            for (int k = 0; k < 32; k++)
+                if (k < C) s += s_w[c * C + k] * yv[k];
+            out[(size_t)p * cout + c] = s;
+        }
     }
 }
 
-// backward of the output layer: dy = wh^T dout where y > 0 (bf16), dwh, dbh
-// accumulated per block (shared memory) and added with atomics.  C, cout <= 32.
-__global__ void k_head_bwd(const bf16* __restrict__ y, int C, int npix, const float* __restrict__ wh, int cout,
-                           const float* __restrict__ dout, bf16* __restrict__ dy, float* __restrict__ dwh,
-                           float* __restrict__ dbh) {
-    __shared__ float s_dw[32 * 33];
-    for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) s_dw[e] = 0.f;
+// backward of the output layer: dy = wh^T dout where y > 0 (bf16), and the
+// layer's gradients dwh[c][k] = sum_p dout[p][c] y[p][k], dbh[c] = sum_p
+// dout[p][c].  128 threads per block over tiles of 128 pixels: each thread
+// writes its pixel's dy and parks y and dout in shared memory, then thread e
+// accumulates entry e of [dwh | dbh] over the tile; one atomic per entry and
+// block at the end.  C, cout <= 32.
+__global__ void __launch_bounds__(128) k_head_bwd(const bf16* __restrict__ y, int C, int npix,
+                                                  const float* __restrict__ wh, int cout,
+                                                  const float* __restrict__ dout, bf16* __restrict__ dy,
+                                                  float* __restrict__ dwh, float* __restrict__ dbh) {
+    constexpr int kT = 128, kE = 9;  // tile, entries per thread (32 x 33 <= 128 x 9)
+    __shared__ float s_y[kT * 33], s_d[kT * 33], s_w[32 * 32];
+    const int tid = threadIdx.x, ne = cout * (C + 1);
+    for (int e = tid; e < cout * C; e += kT) s_w[e] = wh[e];
+    float acc[kE];
+#pragma unroll
+    for (int j = 0; j < kE; j++) acc[j] = 0.f;
     __syncthreads();
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < npix) {
-        float d[32];
-        for (int c = 0; c < cout; c++) d[c] = dout[(size_t)p * cout + c];
-        for (int k = 0; k < C; k++) {
-            const float yk = __bfloat162float(y[(size_t)p * C + k]);
-            float g = 0.f;
+    for (int p0 = blockIdx.x * kT; p0 < npix; p0 += gridDim.x * kT) {
+        const int p = p0 + tid;
+        if (p < npix) {
+            float yv[32], g[32];
+#pragma unroll
+            for (int k0 = 0; k0 < 32; k0 += 8)
+                if (k0 < C) unpack8(ld8(y + (size_t)p * C + k0), yv + k0);
+#pragma unroll
+            for (int k = 0; k < 32; k++) g[k] = 0.f;
             for (int c = 0; c < cout; c++) {
-                g += wh[c * C + k] * d[c];
-                atomicAdd(&s_dw[c * 33 + k], d[c] * yk);
+                const float dc = dout[(size_t)p * cout + c];
+                s_d[tid * 33 + c] = dc;
+#pragma unroll
+                for (int k = 0; k < 32; k++)
+                    if (k < C) g[k] += s_w[c * C + k] * dc;
             }
-            dy[(size_t)p * C + k] = __float2bfloat16_rn(yk > 0.f ? g : 0.f);
+#pragma unroll
+            for (int k0 = 0; k0 < 32; k0 += 8)
+                if (k0 < C) {
+                    float gk[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) gk[j] = yv[k0 + j] > 0.f ? g[k0 + j] : 0.f;
+                    st8(dy + (size_t)p * C + k0, pack8(gk));
+                }
+#pragma unroll
+            for (int k = 0; k < 32; k++)
+                if (k < C) s_y[tid * 33 + k] = yv[k];
+            s_y[tid * 33 + C] = 1.f;
+        } else {
+            for (int k = 0; k <= C; k++) s_y[tid * 33 + k] = 0.f;
+            for (int c = 0; c < cout; c++) s_d[tid * 33 + c] = 0.f;
         }
-        for (int c = 0; c < cout; c++) atomicAdd(&s_dw[c * 33 + 32], d[c]);
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kE; j++) {
+            const int e = tid + j * kT;
+            if (e < ne) {
+                const int c = e / (C + 1), k = e % (C + 1);
+                float s = 0.f;
+                for (int q = 0; q < kT; q++) s += s_d[q * 33 + c] * s_y[q * 33 + k];
+                acc[j] += s;
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    for (int e = threadIdx.x; e < cout * 33; e += blockDim.x) {
-        const int c = e / 33, k = e % 33;
-        if (k < C) atomicAdd(dwh + c * C + k, s_dw[e]);
-        else if (k == 32) atomicAdd(dbh + c, s_dw[e]);
+#pragma unroll
+    for (int j = 0; j < kE; j++) {
+        const int e = tid + j * kT;
+        if (e < ne) {
+            const int c = e / (C + 1), k = e % (C + 1);
+            if (k < C) atomicAdd(dwh + c * C + k, acc[j]);
+            else atomicAdd(dbh + c, acc[j]);
+        }
     }
 }
 
@@ -432,11 +555,6 @@ __global__ void k_adam(float* __restrict__ prm, const float* __restrict__ g, flo
         v[e] = vi;
         prm[e] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
     }
-}
-
-__global__ void k_to_bf16(const float* __restrict__ src, bf16* __restrict__ dst, size_t n) {
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
-        dst[e] = __float2bfloat16_rn(src[e]);
 }
 
 // normalisation of the network's input and output channels
@@ -487,31 +605,46 @@ __global__ void k_unpack(const float* __restrict__ o, int cout, int c, int ni, i
 
 // ---------------------------------------------------------------------------
 // 3x3 convolution on the 5th-generation tensor cores (tcgen05, accumulator in
-// tensor memory).  CTA = 128 consecutive pixels of one image row (the MMA's M)
-// x N output channels, 4 warps.  Per 16 input channels the CTA stages in
-// shared memory, in the canonical K-major layout without swizzle (8-row core
-// matrices of 16 bytes, the two 8-channel halves LBO apart):
-//   A: the 3 halo rows of 130 pixels      (pixel p of halo row r at (r*130+p)*16)
-//   B: the 9 tap slabs of N x 16 weights  (channel co of tap t at (t*2N + co)*16)
-// so the A operand of tap (dy, dx) is the same layout started (dy*130+dx)*16
-// bytes further: one descriptor offset per tap, no copy.  One thread issues
-// the 9 MMAs (M=128, N, K=16), commits them to an mbarrier, and the CTA waits
-// (bounded) before the next chunk overwrites the tiles.  The epilogue reads
-// the accumulator rows (TMEM lane = pixel) with tcgen05.ld.
+// tensor memory) with operands brought in by the tensor memory accelerator.
+// CTA = R image rows x 128 consecutive pixels (the MMA's M: one TMEM lane per
+// pixel) x N output channels, 4 warps.  Input channels go in chunks of 16
+// through a ring of S shared-memory stages in the canonical K-major layout
+// without swizzle (8-row core matrices of 16 bytes; the two 8-channel halves
+// of a chunk are one TMA box each, LBO apart):
+//   A: R+2 halo rows x 130 pixels      (pixel p of halo row h at (h*130+p)*16)
+//   B: 9 tap slabs of N x 16 weights   (channel co of tap t at (t*N+co)*16)
+// so the A operand of output row r and tap (dy, dx) is the same tile started
+// ((r+dy)*130+dx)*16 bytes further: one descriptor offset per (row, tap), and
+// the R output rows share their halo rows.  Thread 0 issues the loads (the
+// stage's full barrier counts the transaction bytes), thread 32 the MMAs
+// (M=128, N, K=16) and releases each stage by tcgen05.commit to its empty
+// barrier; the last commit releases the epilogue, where each warp reads its 32
+// TMEM lanes with tcgen05.ld.  Every wait is bounded: one that gives up sets the
+// error flag, and the CTA waits (bounded) for its copies and MMAs in flight and
+// writes nothing.  The weights have a layout of their own, [Cin/8][9][Cout][8],
+// so that the B half of a chunk is one box.
 // ---------------------------------------------------------------------------
-constexpr int TC_M = 128;                // pixels per CTA
-constexpr int TC_HW = TC_M + 2;          // halo row width
-constexpr int TC_A_BYTES = 2 * 3 * TC_HW * 16;
-constexpr int TC_SMEM_MIN = 46 * 1024;   // at most 4 CTAs per SM: 4 x 128 TMEM columns <= 512
+constexpr int TC_M = 128;        // pixels per row tile
+constexpr int TC_HW = TC_M + 2;  // halo row width
 
-__host__ __device__ constexpr int tc_b_bytes(int N) { return 9 * 2 * N * 16; }
-__host__ __device__ constexpr int tc_a_off() { return 0; }
-__host__ __device__ constexpr int tc_b_off() { return (TC_A_BYTES + 127) / 128 * 128; }
-__host__ __device__ constexpr int tc_bar_off(int N) { return tc_b_off() + tc_b_bytes(N); }
-__host__ __device__ constexpr int tc_smem(int N) {
-    return (tc_bar_off(N) + 16 > TC_SMEM_MIN) ? tc_bar_off(N) + 16 : TC_SMEM_MIN;
-}
-__host__ __device__ constexpr int tc_cols(int N) { return N <= 32 ? 32 : (N <= 64 ? 64 : 128); }
+template <int N, int R>
+struct TcShape {
+    static constexpr int kAHalf = ((R + 2) * TC_HW * 16 + 127) / 128 * 128;
+    static constexpr int kBHalf = 9 * N * 16;
+    static constexpr int kStage = 2 * kAHalf + 2 * kBHalf;
+    static constexpr int kFit = (112 * 1024) / kStage;  // two CTAs per SM
+    static constexpr int kStages = kFit < 2 ? 2 : (kFit > 4 ? 4 : kFit);
+    static constexpr int kBar = kStages * kStage;       // full[S], empty[S], done, TMEM address
+    static constexpr int kSmem = kBar + (2 * kStages + 2) * 8;
+    static constexpr uint32_t kTx = (uint32_t)(2 * (R + 2) * TC_HW * 16 + 2 * kBHalf);
+    static constexpr uint32_t kCols = R * N <= 32 ? 32 : (R * N <= 64 ? 64 : (R * N <= 128 ? 128 : 256));
+    static_assert(R * N <= 256, "two CTAs per SM share the 512 TMEM columns");
+    static_assert(kSmem <= 113 * 1024, "two CTAs per SM");
+};
+
+// the (N, R) tiles instantiated
+#define CTH_TC_TILES(X) \
+    X(128, 2) X(128, 1) X(96, 2) X(96, 1) X(64, 4) X(64, 2) X(64, 1) X(32, 4) X(32, 2) X(32, 1)
 
 // shared-memory matrix descriptor, K-major without swizzle (SM100 format:
 // start >> 4 in [0,14), leading byte offset >> 4 in [16,30), stride byte
@@ -543,120 +676,177 @@ __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
-template <int N>
-__global__ void __launch_bounds__(128) k_conv3_tc(ConvArgs a, int* __restrict__ err) {
-    extern __shared__ __align__(128) unsigned char tsm[];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int x0 = blockIdx.x * TC_M, y = blockIdx.y, co0 = blockIdx.z * N;
-    bf16* sA = reinterpret_cast<bf16*>(tsm + tc_a_off());
-    bf16* sB = reinterpret_cast<bf16*>(tsm + tc_b_off());
-    uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + tc_bar_off(N));
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(tsm + tc_bar_off(N) + 8);
-    const uint32_t bar_a = smem_u32(bar);
-    constexpr uint32_t kCols = tc_cols(N);
+__device__ __forceinline__ void tc_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// 3-D tiled TMA load into this CTA's shared memory, completion on bar
+__device__ __forceinline__ void tc_load3(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int N, int R>
+__global__ void __launch_bounds__(128) k_conv3_tc(const __grid_constant__ CUtensorMap tin,
+                                                  const __grid_constant__ CUtensorMap tw, ConvArgs a,
+                                                  int* __restrict__ err) {
+    using T = TcShape<N, R>;
+    constexpr int S = T::kStages;
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int x0 = blockIdx.x * TC_M, y0 = blockIdx.y * R, co0 = blockIdx.z * N;
+    const uint32_t base = smem_u32(tsm);
+    const uint32_t bars = base + (uint32_t)T::kBar;  // full[s] at bars + 8s, empty[s] at bars + 8(S+s)
+    const uint32_t done = bars + 16u * S;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(tsm + T::kBar + (2 * S + 1) * 8);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(kCols));
+                     "r"(T::kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+    if (tid == 32) {
+        for (int b = 0; b < 2 * S + 1; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bars + 8u * b));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tslot;
-    const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
-    bool ok = true;
-    int phase = 0;
-    for (int c0 = 0; c0 < a.Cin && ok; c0 += 16, phase ^= 1) {
-        // A: 3 halo rows x 130 pixels x two 8-channel halves
-        for (int idx = tid; idx < 2 * 3 * TC_HW; idx += 128) {
-            const int half = idx / (3 * TC_HW), hp = idx % (3 * TC_HW);
-            const int gy = y + hp / TC_HW - 1, gx = x0 + hp % TC_HW - 1;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W)
-                v = *reinterpret_cast<const uint4*>(a.in + ((size_t)gy * a.W + gx) * a.in_cs + a.in_coff + c0 +
-                                                    half * 8);
-            *reinterpret_cast<uint4*>(sA + ((size_t)half * 3 * TC_HW + hp) * 8) = v;
-        }
-        // B: 9 taps x two halves x N output channels
-        for (int idx = tid; idx < 9 * 2 * N; idx += 128) {
-            const int co = idx % N, half = (idx / N) % 2, tap = idx / (2 * N);
-            const uint4 v = *reinterpret_cast<const uint4*>(a.w + ((size_t)(co0 + co) * 9 + tap) * a.Cin + c0 + half * 8);
-            *reinterpret_cast<uint4*>(sB + ((size_t)tap * 2 * N + half * N + co) * 8) = v;
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t idesc = tc_idesc(N);
-#pragma unroll
-            for (int tap = 0; tap < 9; tap++) {
-                const int dy = tap / 3, dx = tap % 3;
-                const uint64_t da = tc_desc(a_base + (uint32_t)((dy * TC_HW + dx) * 16), 3 * TC_HW * 16, 128);
-                const uint64_t db = tc_desc(b_base + (uint32_t)(tap * 2 * N * 16), N * 16, 128);
-                const uint32_t acc = (c0 > 0 || tap > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                    :
-                    : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+    const int nk = a.Cin / 16;
+    int fail = 0, issued = 0;
+    if (tid == 0) {
+        // producer: chunk k into stage k % S once the MMAs of chunk k - S released it
+        for (int k = 0; k < nk; k++) {
+            const int s = k % S;
+            if (k >= S && !tc_wait(bars + 8u * (S + s), (uint32_t)((k / S - 1) & 1))) {
+                fail = 1;
+                break;
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
-                         : "memory");
+            const uint32_t st = base + (uint32_t)(s * T::kStage), fb = bars + 8u * s;
+            tc_expect(fb, T::kTx);
+            tc_load3(st, &tin, fb, 16 * k, x0 - 1, y0 - 1);
+            tc_load3(st + T::kAHalf, &tin, fb, 16 * k + 8, x0 - 1, y0 - 1);
+            tc_load3(st + 2 * T::kAHalf, &tw, fb, 0, co0, 18 * k);
+            tc_load3(st + 2 * T::kAHalf + T::kBHalf, &tw, fb, 0, co0, 18 * k + 9);
+            issued = k + 1;
         }
-        // CTA-uniform outcome, so every thread takes the same path at the barriers
-        ok = __syncthreads_and(tc_wait(bar_a, (uint32_t)phase) ? 1 : 0) != 0;
+    } else if (tid == 32) {
+        // MMA issuer: R x 9 MMAs per chunk, accumulating over taps and chunks
+        constexpr uint32_t idesc = tc_idesc(N);
+        for (int k = 0; k < nk; k++) {
+            const int s = k % S;
+            if (!tc_wait(bars + 8u * s, (uint32_t)((k / S) & 1))) {
+                fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = base + (uint32_t)(s * T::kStage);
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+#pragma unroll
+                for (int tap = 0; tap < 9; tap++) {
+                    const int dy = tap / 3, dx = tap % 3;
+                    const uint64_t da = tc_desc(st + (uint32_t)(((r + dy) * TC_HW + dx) * 16), T::kAHalf, 128);
+                    const uint64_t db = tc_desc(st + (uint32_t)(2 * T::kAHalf + tap * N * 16), T::kBHalf, 128);
+                    tc_mma(tmem + (uint32_t)(r * N), da, db, idesc, (k > 0 || tap > 0) ? 1u : 0u);
+                }
+            }
+            tc_commit(bars + 8u * (S + s));
+        }
+        tc_commit(done);
     }
+    __syncwarp();
+    // CTA-uniform outcome, so every thread takes the same path at the barriers
+    const bool ok = __syncthreads_and((fail == 0 && tc_wait(done, 0u)) ? 1 : 0) != 0;
     if (!ok) {
-        if (tid == 0) atomicExch(err, 1);
+        if (tid == 0) {
+            atomicExch(err, 1);
+            for (int k = issued > S ? issued - S : 0; k < issued; k++)
+                tc_wait(bars + 8u * (k % S), (uint32_t)((k / S) & 1));
+        }
+        tc_wait(done, 0u);
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int gx = x0 + tid;
-        const size_t pix = (size_t)y * a.W + gx;
+#pragma unroll 1
+        for (int r = 0; r < R; r++) {
+            const int gy = y0 + r;
+            const bool live = gx < a.W && gy < a.H;
+            const size_t pix = (size_t)gy * a.W + gx;
+#pragma unroll 1
+            for (int cb = 0; cb < N / 32; cb++) {
+                uint32_t v[32];
+                tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(r * N + cb * 32), v);
+                if (!live) continue;
 #pragma unroll
-        for (int cb = 0; cb < N / 32; cb++) {
-            uint32_t r[32];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 32);
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (gx < a.W) {
+                for (int q = 0; q < 4; q++) {
+                    const int co = co0 + cb * 32 + q * 8;
+                    float f[8];
 #pragma unroll
-                for (int j = 0; j < 32; j += 2) {
-                    const int co = co0 + cb * 32 + j;
-                    float v0 = __uint_as_float(r[j]), v1 = __uint_as_float(r[j + 1]);
-                    if (a.bias) { v0 += a.bias[co]; v1 += a.bias[co + 1]; }
-                    if (a.relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+                    for (int j = 0; j < 8; j++) {
+                        f[j] = __uint_as_float(v[q * 8 + j]);
+                        if (a.bias) f[j] += a.bias[co + j];
+                        if (a.relu) f[j] = fmaxf(f[j], 0.f);
+                    }
                     if (a.gate) {
-                        const __nv_bfloat162 g =
-                            *reinterpret_cast<const __nv_bfloat162*>(a.gate + pix * a.gate_cs + a.gate_coff + co);
-                        if (!(__bfloat162float(g.x) > 0.f)) v0 = 0.f;
-                        if (!(__bfloat162float(g.y) > 0.f)) v1 = 0.f;
+                        const uint4 g = *reinterpret_cast<const uint4*>(a.gate + pix * a.gate_cs + a.gate_coff + co);
+                        const __nv_bfloat162* gh = reinterpret_cast<const __nv_bfloat162*>(&g);
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            if (!(__bfloat162float(gh[j].x) > 0.f)) f[2 * j] = 0.f;
+                            if (!(__bfloat162float(gh[j].y) > 0.f)) f[2 * j + 1] = 0.f;
+                        }
                     }
-                    __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(a.out + pix * a.out_cs + a.out_coff + co);
+                    uint4* o = reinterpret_cast<uint4*>(a.out + pix * a.out_cs + a.out_coff + co);
                     if (a.accumulate) {
-                        const __nv_bfloat162 q = *o;
-                        v0 += __bfloat162float(q.x);
-                        v1 += __bfloat162float(q.y);
+                        const uint4 old = *o;
+                        const __nv_bfloat162* oh = reinterpret_cast<const __nv_bfloat162*>(&old);
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            f[2 * j] += __bfloat162float(oh[j].x);
+                            f[2 * j + 1] += __bfloat162float(oh[j].y);
+                        }
                     }
-                    *o = __floats2bfloat162_rn(v0, v1);
+                    uint4 res;
+                    __nv_bfloat162* rh = reinterpret_cast<__nv_bfloat162*>(&res);
+#pragma unroll
+                    for (int j = 0; j < 4; j++) rh[j] = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+                    *o = res;
                 }
             }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(T::kCols));
 }
 
 inline dim3 grid1(size_t n, int bs = 256) {
@@ -702,6 +892,8 @@ struct cth_unet {
     float* adam_v = nullptr;
     bf16* wb = nullptr;    // bf16 conv weights
     bf16* wt = nullptr;    // transposed / flipped conv weights (input gradients)
+    bf16* wbt = nullptr;   // wb and wt in the tcgen05 layout [Cin/8][9][Cout][8]
+    bf16* wtt = nullptr;
     std::vector<void*> bufs;
     bf16* x_in = nullptr;  // packed input
     bf16* y_last = nullptr;  // last decoder activation (input of the head)
@@ -713,8 +905,8 @@ struct cth_unet {
     Stats stats{};
     float* feat = nullptr;   // input features of the warm-start prediction
     long long launches = 0;  // kernels launched by the forward passes and predictions
-    bool use_tc = false;     // convolutions on tcgen05 (false: warp-level mma.sync kernel)
-    int* err = nullptr;      // device flag: a tensor-core wait gave up
+    bool use_tc = true;      // convolutions on tcgen05 (false: warp-level mma.sync kernel)
+    int* err = nullptr;      // device flag: a bounded wait of a tcgen05 convolution gave up
     struct Pool { TensorRef src; bf16* dst; int C, Ho, Wo; bf16* ddst; };
     struct Up { bf16* src; int C, Hi, Wi; TensorRef dst; bf16* dsrc; TensorRef ddst; };
     std::vector<Pool> pools;
@@ -825,16 +1017,19 @@ int build(cth_unet* n) {
     CTH_CUDA(cudaMemset(n->adam_v, 0, off * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->wb, woff * sizeof(bf16)));
     CTH_CUDA(cudaMalloc(&n->wt, woff * sizeof(bf16)));
+    CTH_CUDA(cudaMalloc(&n->wbt, woff * sizeof(bf16)));
+    CTH_CUDA(cudaMalloc(&n->wtt, woff * sizeof(bf16)));
     CTH_CUDA(cudaMalloc(&n->out, npx0 * n->cout * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->dout, npx0 * n->cout * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->loss, sizeof(double)));
     CTH_CUDA(cudaMalloc(&n->cw, n->cout * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->err, sizeof(int)));
     CTH_CUDA(cudaMemset(n->err, 0, sizeof(int)));
-    CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(128)));
-    CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(96)));
-    CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(64)));
-    CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(32)));
+#define CTH_TC_ATTR(NN, RR)                                                                   \
+    CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<NN, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  TcShape<NN, RR>::kSmem));
+    CTH_TC_TILES(CTH_TC_ATTR)
+#undef CTH_TC_ATTR
     std::vector<float> ones(n->cout, 1.f);
     CTH_CUDA(cudaMemcpy(n->cw, ones.data(), n->cout * sizeof(float), cudaMemcpyHostToDevice));
     return CTH_OK;
@@ -844,48 +1039,104 @@ int build(cth_unet* n) {
 int sync_weights(cth_unet* n, cudaStream_t s) {
     for (const Conv& c : n->convs) {
         const size_t nw = (size_t)c.cout * 9 * c.cin;
-        k_to_bf16<<<grid1(nw), 256, 0, s>>>(n->prm + c.w_off, n->wb + c.wb_off, nw);
-        k_wtrans<<<grid1(nw), 256, 0, s>>>(n->wb + c.wb_off, c.cout, c.cin, n->wt + c.wb_off);
+        k_weights<<<grid1(nw), 256, 0, s>>>(n->prm + c.w_off, c.cout, c.cin, n->wb + c.wb_off, n->wt + c.wb_off,
+                                            n->wbt + c.wb_off, n->wtt + c.wb_off);
     }
     CTH_CUDA(cudaGetLastError());
     return CTH_OK;
 }
 
-// largest tcgen05 tile width (output channels) dividing Cout
-int tc_n(int cout) {
-    for (int nn : {128, 96, 64, 32})
-        if (cout % nn == 0) return nn;
-    return 0;
+// cuTensorMapEncodeTiled from the driver (no link against it)
+typedef CUresult (*TmapEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+TmapEncodeFn tmap_encode() {
+    static const TmapEncodeFn fn = []() -> TmapEncodeFn {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<TmapEncodeFn>(p);
+    }();
+    return fn;
 }
 
-void launch_conv(cth_unet* n, const ConvArgs& a, cudaStream_t s) {
-    const int nn = n->use_tc ? tc_n(a.Cout) : 0;
-    if (nn && a.Cin % 16 == 0) {
-        dim3 grd((a.W + TC_M - 1) / TC_M, a.H, a.Cout / nn);
-        switch (nn) {
-            case 128: k_conv3_tc<128><<<grd, 128, tc_smem(128), s>>>(a, n->err); break;
-            case 96: k_conv3_tc<96><<<grd, 128, tc_smem(96), s>>>(a, n->err); break;
-            case 64: k_conv3_tc<64><<<grd, 128, tc_smem(64), s>>>(a, n->err); break;
-            default: k_conv3_tc<32><<<grd, 128, tc_smem(32), s>>>(a, n->err); break;
+// 3-D bf16 tensor map: extents d0 (contiguous), d1, d2; byte strides s1, s2 of
+// dimensions 1 and 2; box b0 x b1 x b2; zero fill outside the extents
+bool tmap3(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1, uint64_t s2,
+           uint32_t b0, uint32_t b1, uint32_t b2) {
+    const TmapEncodeFn fn = tmap_encode();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {d0, d1, d2}, strides[2] = {s1, s2};
+    cuuint32_t box[3] = {b0, b1, b2}, es[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// tcgen05 tile of a convolution: the widest N (output channels) dividing Cout,
+// then the most rows R whose grid still gives every SM two CTAs; without such
+// a tiling the widest N with one row
+struct TcTile {
+    int n, r;
+};
+TcTile tc_tile(int cout, int H, int W) {
+    const int cols = (W + TC_M - 1) / TC_M;
+    for (int N : {128, 96, 64, 32}) {
+        if (cout % N) continue;
+        for (int R : {4, 2, 1}) {
+            if (R * N > 256) continue;
+            if ((long)cols * ((H + R - 1) / R) * (cout / N) >= 2 * 148) return {N, R};
         }
-        return;
+    }
+    for (int N : {128, 96, 64, 32})
+        if (cout % N == 0) return {N, 1};
+    return {0, 0};
+}
+
+int launch_conv(cth_unet* n, const ConvArgs& a, cudaStream_t s) {
+    const TcTile t = n->use_tc ? tc_tile(a.Cout, a.H, a.W) : TcTile{0, 0};
+    if (t.n && a.Cin % 16 == 0 && a.in_cs % 8 == 0 && a.in_coff % 8 == 0) {
+        CUtensorMap ti, tw;
+        if (!tmap3(&ti, a.in + a.in_coff, (uint64_t)a.Cin, (uint64_t)a.W, (uint64_t)a.H, (uint64_t)a.in_cs * 2,
+                   (uint64_t)a.W * a.in_cs * 2, 8, TC_HW, (uint32_t)(t.r + 2)) ||
+            !tmap3(&tw, a.wtc, 8, (uint64_t)a.Cout, (uint64_t)9 * a.Cin / 8, 16, (uint64_t)a.Cout * 16, 8,
+                   (uint32_t)t.n, 9)) {
+            set_error("cth_unet: tensor map encoding failed");
+            return CTH_ERR_CUDA;
+        }
+        const dim3 grd((a.W + TC_M - 1) / TC_M, (a.H + t.r - 1) / t.r, a.Cout / t.n);
+#define CTH_TC_LAUNCH(NN, RR)                                                                  \
+    if (t.n == NN && t.r == RR) {                                                              \
+        k_conv3_tc<NN, RR><<<grd, 128, TcShape<NN, RR>::kSmem, s>>>(ti, tw, a, n->err);        \
+        return CTH_OK;                                                                         \
+    }
+        CTH_TC_TILES(CTH_TC_LAUNCH)
+#undef CTH_TC_LAUNCH
+        set_error("cth_unet: no tcgen05 tile for this convolution");
+        return CTH_ERR_ARG;
     }
     dim3 grd((a.W + TW - 1) / TW, (a.H + TH - 1) / TH, a.Cout / 32);
     k_conv3_fwd<<<grd, 128, 0, s>>>(a);
+    return CTH_OK;
 }
 
-void conv_fwd(cth_unet* n, const Conv& c, cudaStream_t s) {
+int conv_fwd(cth_unet* n, const Conv& c, cudaStream_t s) {
     ConvArgs a{};
     a.in = c.in.p; a.in_cs = c.in.cs; a.in_coff = c.in.coff; a.Cin = c.cin;
     a.w = n->wb + c.wb_off;
+    a.wtc = n->wbt + c.wb_off;
     a.bias = n->prm + c.b_off;
     a.out = c.out.p; a.out_cs = c.out.cs; a.out_coff = c.out.coff; a.Cout = c.cout;
     a.H = c.H; a.W = c.W;
     a.relu = 1;
-    launch_conv(n, a, s);
+    return launch_conv(n, a, s);
 }
 
-void conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
+int conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
     // weight and bias gradients
     WgradArgs w{};
     w.dy = c.dout.p; w.dy_cs = c.dout.cs; w.dy_coff = c.dout.coff; w.Cout = c.cout;
@@ -900,13 +1151,16 @@ void conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
     dim3 gw((npatch + ppc - 1) / ppc, c.cout / 32, c.cin / 32);
     k_conv3_wgrad<<<gw, 288, 0, s>>>(w);
     const int npix = c.H * c.W;
-    const int ppb = 256;
-    k_bias_grad<<<(npix + ppb - 1) / ppb, 256, 0, s>>>(c.dout.p, c.dout.cs, c.dout.coff, c.cout, npix, ppb,
-                                                       n->grad + c.b_off);
-    if (!c.din.p) return;
+    {
+        const int lanes = 256 / (c.cout / 8);
+        const int nb = std::max(1, std::min(2 * 148, (npix + lanes - 1) / lanes));
+        k_bias_grad<<<nb, 256, 0, s>>>(c.dout.p, c.dout.cs, c.dout.coff, c.cout, npix, n->grad + c.b_off);
+    }
+    if (!c.din.p) return CTH_OK;
     ConvArgs a{};
     a.in = c.dout.p; a.in_cs = c.dout.cs; a.in_coff = c.dout.coff; a.Cin = c.cout;
     a.w = n->wt + c.wb_off;
+    a.wtc = n->wtt + c.wb_off;
     a.bias = nullptr;
     a.out = c.din.p; a.out_cs = c.din.cs; a.out_coff = c.din.coff; a.Cout = c.cin;
     a.H = c.H; a.W = c.W;
@@ -914,30 +1168,31 @@ void conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
     a.gate = c.out_gate_for_din;
     a.gate_cs = c.din.cs; a.gate_coff = c.din.coff;
     a.accumulate = c.din_accumulate;
-    launch_conv(n, a, s);
+    return launch_conv(n, a, s);
 }
 
 int forward(cth_unet* n, const float* in, cudaStream_t s) {
     const size_t npx = (size_t)n->H * n->W;
     n->launches += 2 + (long long)n->convs.size() + (long long)n->pools.size() + (long long)n->ups.size();
-    k_pack<<<grid1(npx * n->cpad), 256, 0, s>>>(in, n->cin, (int)npx, n->cpad, n->x_in);
+    k_pack<<<grid1(npx), 256, 0, s>>>(in, n->cin, (int)npx, n->cpad, n->x_in);
     const auto& C = n->convs;
     int up = 0;
     for (size_t k = 0; k < C.size(); k++) {
-        conv_fwd(n, C[k], s);
+        const int rc = conv_fwd(n, C[k], s);
+        if (rc != CTH_OK) return rc;
         if (k == 1 || k == 3 || k == 5) {
             const auto& p = n->pools[k / 2];
-            k_pool2<<<grid1((size_t)p.Ho * p.Wo * p.C), 256, 0, s>>>(p.src.p, p.src.cs, p.src.coff, p.C, p.Ho, p.Wo,
+            k_pool2<<<grid1((size_t)p.Ho * p.Wo * p.C / 8), 256, 0, s>>>(p.src.p, p.src.cs, p.src.coff, p.C, p.Ho, p.Wo,
                                                                       p.dst, p.C);
         }
         if (k == 7 || k == 9 || k == 11) {
             const auto& u = n->ups[up++];
-            k_up2<<<grid1((size_t)4 * u.Hi * u.Wi * u.C), 256, 0, s>>>(u.src, u.C, u.C, u.Hi, u.Wi, u.dst.p, u.dst.cs,
+            k_up2<<<grid1((size_t)u.Hi * u.Wi * u.C / 8), 256, 0, s>>>(u.src, u.C, u.C, u.Hi, u.Wi, u.dst.p, u.dst.cs,
                                                                         u.dst.coff);
         }
     }
     const int B = n->base;
-    k_head_fwd<<<(unsigned)((npx + 255) / 256), 256, 0, s>>>(n->y_last, B, (int)npx, n->prm + n->head_w,
+    k_head_fwd<<<grid1(npx), 256, 0, s>>>(n->y_last, B, (int)npx, n->prm + n->head_w,
                                                              n->prm + n->head_b, n->cout, n->out);
     CTH_CUDA(cudaGetLastError());
     return CTH_OK;
@@ -946,23 +1201,25 @@ int forward(cth_unet* n, const float* in, cudaStream_t s) {
 int backward(cth_unet* n, const float* dout, cudaStream_t s) {
     const size_t npx = (size_t)n->H * n->W;
     const int B = n->base;
-    k_head_bwd<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(n->y_last, B, (int)npx, n->prm + n->head_w, n->cout,
+    const unsigned nhb = std::max<unsigned>(1, std::min<unsigned>(4 * 148, (unsigned)((npx + 127) / 128)));
+    k_head_bwd<<<nhb, 128, 0, s>>>(n->y_last, B, (int)npx, n->prm + n->head_w, n->cout,
                                                             dout, n->dy_last, n->grad + n->head_w,
                                                             n->grad + n->head_b);
     const auto& C = n->convs;
     // the decoder convs write the concatenation gradients whole; the pooling
     // gradients are then added into their skip channels
     for (int k = (int)C.size() - 1; k >= 0; k--) {
-        conv_bwd(n, C[k], s);
+        const int rc = conv_bwd(n, C[k], s);
+        if (rc != CTH_OK) return rc;
         if (k == 12 || k == 10 || k == 8) {
             const auto& u = n->ups[(k - 8) / 2];
-            k_up2_bwd<<<grid1((size_t)u.Hi * u.Wi * u.C), 256, 0, s>>>(u.ddst.p, u.ddst.cs, u.ddst.coff, u.C, u.Hi,
+            k_up2_bwd<<<grid1((size_t)u.Hi * u.Wi * u.C / 8), 256, 0, s>>>(u.ddst.p, u.ddst.cs, u.ddst.coff, u.C, u.Hi,
                                                                       u.Wi, u.dsrc, u.C);
         }
         if (k == 6 || k == 4 || k == 2) {
             const auto& p = n->pools[k / 2 - 1];
             const TensorRef dskip = n->convs[k - 1].dout;
-            k_pool2_bwd<<<grid1((size_t)4 * p.Ho * p.Wo * p.C), 256, 0, s>>>(p.ddst, p.C, p.C, p.Ho, p.Wo, dskip.p,
+            k_pool2_bwd<<<grid1((size_t)4 * p.Ho * p.Wo * p.C / 8), 256, 0, s>>>(p.ddst, p.C, p.C, p.Ho, p.Wo, dskip.p,
                                                                              dskip.cs, dskip.coff, p.src.p, p.src.cs,
                                                                              p.src.coff);
         }
@@ -1003,6 +1260,7 @@ void cth_unet_destroy(cth_unet* n) {
     cudaDeviceSynchronize();
     for (void* p : n->bufs) cudaFree(p);
     for (void* p : {(void*)n->prm, (void*)n->grad, (void*)n->adam_m, (void*)n->adam_v, (void*)n->wb, (void*)n->wt,
+                    (void*)n->wbt, (void*)n->wtt,
                     (void*)n->out, (void*)n->dout, (void*)n->loss, (void*)n->cw, (void*)n->feat, (void*)n->err})
         if (p) cudaFree(p);
     delete n;

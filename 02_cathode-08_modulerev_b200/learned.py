@@ -111,7 +111,7 @@ class UNet:
         return int(self._L.cth_unet_launch_count(self.handle))
 
     def set_tensor_cores(self, tcgen05: bool):
-        """Convolutions on tcgen05 or on the warp-level mma.sync kernel (default)."""
+        """Convolutions on tcgen05 (default) or on the warp-level mma.sync kernel."""
         capi.check(self._L.cth_unet_set_tensor_cores(self.handle, int(tcgen05)), allow_positive=False)
 
     def check(self):

@@ -567,8 +567,9 @@ cth_unet* cth_unet_create(int H, int W, int cin, int cout, int base, int device)
 void cth_unet_destroy(cth_unet* n);
 long long cth_unet_nparams(const cth_unet* n);
 long long cth_unet_launch_count(const cth_unet* n);  /* kernels of forward passes and predictions */
-/* convolutions on the tcgen05 tensor cores with the accumulator in tensor
- * memory (1) or on the warp-level mma.sync kernel (0, default) */
+/* convolutions on the tcgen05 tensor cores with TMA-fed operands and the
+ * accumulator in tensor memory (1, default) or on the warp-level mma.sync
+ * kernel (0) */
 int cth_unet_set_tensor_cores(cth_unet* n, int tcgen05);
 /* synchronises; CTH_ERR_CUDA if a tensor-core convolution's bounded wait for
  * its MMAs gave up (the output of that call is then not valid) */
