@@ -13,6 +13,6 @@ The directory name is not a Python identifier; load it with
 """
 from . import batch, capi, feed, fluid, learned, workloads  # noqa: F401
 from .fluid import Fields  # noqa: F401
-from .solvers import Grid, solver_SMG, solver_SOR  # noqa: F401
+from .solvers import Grid, Microwave3, solver_SMG, solver_SOR  # noqa: F401
 
-__all__ = ["batch", "capi", "feed", "fluid", "learned", "workloads", "Fields", "Grid", "solver_SMG", "solver_SOR"]
+__all__ = ["batch", "capi", "feed", "fluid", "learned", "workloads", "Fields", "Grid", "Microwave3", "solver_SMG", "solver_SOR"]

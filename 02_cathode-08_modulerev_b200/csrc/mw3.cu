@@ -1,0 +1,697 @@
+// mw3.cu — the magnetised 3-component microwave system on the device.
+//
+// EmfieldModule::solve_Microwave (include/emfieldModule.hpp:2249-2998) couples
+// three complex fields through the magnetised cold-plasma conductivity:
+//   Ex on x-faces (i-1/2, j), Er on r-faces (i, j-1/2), Ephi on cells (i, j),
+// each row an 11-point stencil (its own 5-point operator plus the face or cell
+// averages of the other two components, :2300-2453), assembled into one sparse
+// matrix of unknown-to-unknown couplings (:2785-2990) and factorised with Eigen
+// SparseLU (:2995-2998).  Here, on the r-z rectangle r in [0, R], z in [0, L]
+// with the reference's own boundary codes (the same codes as the oracle's
+// mag_rect_system):
+//   Ex   Gauss (code 2) at z = 0 and z = L, conductor (code 0) at r = R;
+//   Er   port excitation (code 7) on the z = 0 faces with r1 <= r <= r2, open
+//        (code 1) on the other z = 0 faces and at z = L, Gauss (code 2) at r = R;
+//   Ephi open (code 1) at z = 0, conductor (code 0) at z = L and r = R;
+// on the axis the r-weights of the Ex and Ephi south couplings vanish and the
+// Er axis face is not an unknown.  Unknowns: Ex i = 2..ni, j = 1..nj; Er
+// i = 1..ni, j = 2..nj; Ephi i = 1..ni, j = 1..nj.
+//
+// Solver: BiCGStab in complex FP64 on the coupled operator, right-
+// preconditioned block-diagonally by one complex semicoarsening V-cycle per
+// field (the smg.cu hierarchy of a grid whose single box is that field's
+// unknowns, built on the field's own 5-point block).  Vectors live in the
+// library layout (row j, column i, leading dimension ld), one plane per field,
+// and stay exactly zero off their unknowns, so the coupled apply needs no
+// neighbour tests: a coupling to a non-unknown multiplies a zero, which is the
+// reference's dropped matrix entry.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "grid.h"
+#include "line.cuh"
+
+namespace cth {
+
+int cmg_alloc(cth_grid* g);
+int cmg_setup(cth_grid* g, cudaStream_t s);
+int cmg_vcycle(cth_grid* g, cudaStream_t s);
+
+namespace m3 {
+
+constexpr double kE0 = 1.60217662e-19;      // constants.hpp:6
+constexpr double kEPS0 = 8.8541878128e-12;  // constants.hpp:7
+constexpr double kMU0 = 1.2566370614e-6;    // constants.hpp:8
+
+// coefficient slots of one field's rows; C0..C5 are the couplings:
+//   Ex   C0..C3 = Er at NE (i, j+1), SE (i, j), NW (i-1, j+1), SW (i-1, j);  C4, C5 = Ephi at (i, j), (i-1, j)
+//   Er   C0..C3 = Ex at NE (i+1, j), SE (i+1, j-1), NW (i, j), SW (i, j-1);  C4, C5 = Ephi at (i, j), (i, j-1)
+//   Ephi C0, C1 = Ex at (i+1, j), (i, j);  C2, C3 = Er at (i, j+1), (i, j)
+enum Slot3 { QP = 0, QE, QW, QN, QS, C0, C1, C2, C3, C4, C5, NQ };
+
+// scalar words of the recurrence
+enum Word3 {
+    RHO = 0, RHO_OLD = 2, ALPHA = 4, OMEGA = 6, BETA = 8,
+    BB = 10, RR = 11, RELRES = 12, ITER = 13, CONV = 14, BAD = 15, KEEP = 16, NWORDS = 24
+};
+
+struct Lev0 {
+    cd* b[3];   // preconditioner right-hand side, level 0 of each field's hierarchy
+    cd* x[3];   // preconditioner result
+    int i0[3], j0[3], ldl[3];
+};
+
+struct Dev3 {
+    cd* a;  // [3][NQ] planes
+    cd* b;  // [3] planes
+    cd *x, *r, *rh, *p, *ph, *v, *s, *sh, *t;  // [3] planes each
+    double* sc;
+    int ni, nj, ld;
+    size_t pl;
+};
+
+__device__ __forceinline__ bool unknown(int c, int i, int j, int ni, int nj) {
+    if (c == 0) return i >= 2 && i <= ni && j >= 1 && j <= nj;
+    if (c == 1) return i >= 1 && i <= ni && j >= 2 && j <= nj;
+    return i >= 1 && i <= ni && j >= 1 && j <= nj;
+}
+
+__device__ __forceinline__ cd sc_c(const double* sc, int w) { return cd(sc[w], sc[w + 1]); }
+__device__ __forceinline__ void sc_set(double* sc, int w, cd v) { sc[w] = v.x; sc[w + 1] = v.y; }
+
+// (A X)_row of field c at (i, j); X = three planes, zero off their unknowns
+__device__ __forceinline__ cd apply3(const Dev3& D, const cd* __restrict__ X, int c, int i, int j) {
+    const size_t pl = D.pl, q = (size_t)j * D.ld + i;
+    const int ld = D.ld;
+    const cd* A = D.a + (size_t)c * NQ * pl;
+    const cd* F = X + (size_t)c * pl;
+    const cd* Ex = X;
+    const cd* Er = X + pl;
+    const cd* Ep = X + 2 * pl;
+    cd y = A[QP * pl + q] * F[q];
+    y -= A[QE * pl + q] * F[q + 1];
+    y -= A[QW * pl + q] * F[q - 1];
+    y -= A[QN * pl + q] * F[q + ld];
+    y -= A[QS * pl + q] * F[q - ld];
+    if (c == 0) {
+        y -= A[C0 * pl + q] * Er[q + ld];
+        y -= A[C1 * pl + q] * Er[q];
+        y -= A[C2 * pl + q] * Er[q - 1 + ld];
+        y -= A[C3 * pl + q] * Er[q - 1];
+        y -= A[C4 * pl + q] * Ep[q];
+        y -= A[C5 * pl + q] * Ep[q - 1];
+    } else if (c == 1) {
+        y -= A[C0 * pl + q] * Ex[q + 1];
+        y -= A[C1 * pl + q] * Ex[q + 1 - ld];
+        y -= A[C2 * pl + q] * Ex[q];
+        y -= A[C3 * pl + q] * Ex[q - ld];
+        y -= A[C4 * pl + q] * Ep[q];
+        y -= A[C5 * pl + q] * Ep[q - ld];
+    } else {
+        y -= A[C0 * pl + q] * Ex[q + 1];
+        y -= A[C1 * pl + q] * Ex[q];
+        y -= A[C2 * pl + q] * Er[q + ld];
+        y -= A[C3 * pl + q] * Er[q];
+    }
+    return y;
+}
+
+// ---------------------------------------------------------------------------
+// assembly
+// ---------------------------------------------------------------------------
+struct Sig {
+    cd coef, hx, hr;
+};
+
+// coef and Hall factors of the conductivity (emfieldModule.hpp:2312-2318), with
+// the reference's EPS = 1e-100 (1 + i) guards
+__device__ __forceinline__ Sig sigma(double rho, double nu, double bx, double br, double w, double me) {
+    const cd den(me * nu + 1e-100, me * w + 1e-100);
+    Sig s;
+    s.hx = cdiv(cd(kE0 * bx), den);
+    s.hr = cdiv(cd(kE0 * br), den);
+    const cd mag2 = s.hx * s.hx + s.hr * s.hr;
+    s.coef = cdiv(cdiv(cd(rho * kE0 * kE0), den), cd(1.0 + 1e-100, 1e-100) + mag2);
+    return s;
+}
+
+// first-order open boundary factor R of codes 1 (:2579-2588)
+__device__ __forceinline__ cd open_r(double eps_t, double w, double dx) {
+    const double c0 = sqrt(1.0 / (kEPS0 * eps_t * kMU0));
+    const double deno = (2.0 * c0) * (2.0 * c0) + (w * dx) * (w * dx) + 1e-100;
+    return cd(((2.0 * c0) * (2.0 * c0) - (w * dx) * (w * dx)) / deno, (-4.0 * c0 * w * dx) / deno);
+}
+
+__global__ void k_m3_assemble(const double* __restrict__ ne, const double* __restrict__ nu,
+                              const double* __restrict__ Bx, const double* __restrict__ Br,
+                              const double* __restrict__ epsr, cth_mw_params prm, Dev3 D) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    if (i > D.ni) return;
+    const int ni = D.ni, nj = D.nj, ld = D.ld;
+    const size_t pl = D.pl, q = (size_t)j * ld + i;
+    const double dx = prm.dx, dr = prm.dr, w = prm.omegam, me = prm.masse;
+    const double g2 = dx * dx * dr * dr;
+    const cd iwm(0.0, w * kMU0);
+    auto r_of = [&](int jj) { return prm.rmin + (jj - 0.5) * dr; };
+    const double rj = r_of(j), rjm = r_of(j - 1), rjp = r_of(j + 1);
+    // ---- Ex (x-face between cells i-1 and i), :2300-2348 ----
+    if (unknown(0, i, j, ni, nj)) {
+        cd* A = D.a;
+        const double qL = (rjm + rj) / 2.0 / (rj + 1e-100);
+        const double qR = (rjp + rj) / 2.0 / (rj + 1e-100);
+        const Sig s = sigma((ne[q] + ne[q - 1]) / 2.0, (nu[q] + nu[q - 1]) / 2.0, (Bx[q] + Bx[q - 1]) / 2.0,
+                            (Br[q] + Br[q - 1]) / 2.0, w, me);
+        const double eps_t = (epsr[q] + epsr[q - 1]) / 2.0;
+        const cd s_xr = s.coef * (s.hx * s.hr), s_xp = s.coef * s.hr, s_xx = s.coef * (cd(1.0) + s.hx * s.hx);
+        cd aP = cd(2.0 * dx * dx + 2.0 * dr * dr - kEPS0 * eps_t * kMU0 * w * w * g2) + iwm * s_xx * cd(g2);
+        cd aE(dr * dr), aW(dr * dr), aN(qR * dx * dx), aS(qL * dx * dx);
+        const cd kp = iwm * s_xp * cd(-0.5 * g2), kr = iwm * s_xr * cd(-0.25 * g2);
+        cd cNE = kr * cd(qR), cSE = kr * cd(qL), cNW = kr * cd(qR), cSW = kr * cd(qL);
+        if (i == 2) {  // z = 0: Gauss (code 2, :2464-2471)
+            aP -= aW;
+            cNW += aW * cd(dx / dr * qR);
+            cSW -= aW * cd(dx / dr * qL);
+            aW = cd();
+        }
+        if (i == ni) {  // z = L: Gauss (code 2, :2497-2504)
+            aP -= aE;
+            cNE -= aE * cd(dx / dr * qR);
+            cSE += aE * cd(dx / dr * qL);
+            aE = cd();
+        }
+        if (j == nj) {  // r = R: conductor (code 0, :2536-2538)
+            aP += cd(rj / rjp) * aN;
+            aN = cd();
+        }
+        A[QP * pl + q] = aP; A[QE * pl + q] = aE; A[QW * pl + q] = aW; A[QN * pl + q] = aN; A[QS * pl + q] = aS;
+        A[C0 * pl + q] = cNE; A[C1 * pl + q] = cSE; A[C2 * pl + q] = cNW; A[C3 * pl + q] = cSW;
+        A[C4 * pl + q] = kp; A[C5 * pl + q] = kp;
+        D.b[q] = cd();
+    }
+    // ---- Er (r-face between cells j-1 and j), :2352-2411 ----
+    if (unknown(1, i, j, ni, nj)) {
+        cd* A = D.a + (size_t)NQ * pl;
+        const double rjmm = r_of(j - 2);
+        const double r_t = (rjm + rj) / 2.0, rR = (rj + rjp) / 2.0, rL = (rjmm + rjm) / 2.0;
+        const Sig s = sigma((ne[q] + ne[q - ld]) / 2.0, (nu[q] + nu[q - ld]) / 2.0,
+                            (rj * Bx[q] + rjm * Bx[q - ld]) / (2.0 * r_t), (rj * Br[q] + rjm * Br[q - ld]) / (2.0 * r_t),
+                            w, me);
+        const double eps_t = (epsr[q] + epsr[q - ld]) / 2.0;
+        const cd s_rr = s.coef * (cd(1.0) + s.hr * s.hr), s_rp = s.coef * (-s.hx), s_rx = s.coef * (s.hx * s.hr);
+        cd aP = cd(r_t * (1.0 / rj + 1.0 / rjm) * dx * dx + 2.0 * dr * dr - kEPS0 * eps_t * kMU0 * w * w * g2) +
+                iwm * s_rr * cd(g2);
+        cd aE(dr * dr), aW(dr * dr), aN(rR / rj * dx * dx), aS(rL / rjm * dx * dx);
+        const cd kp = iwm * s_rp * cd(-0.5 * g2), kx = iwm * s_rx * cd(-0.25 * g2);
+        const cd cNN = kp * cd(rj / r_t), cSS = kp * cd(rjm / r_t);
+        cd cNE = kx * cd(rj / r_t), cNW = kx * cd(rj / r_t), cSE = kx * cd(rjm / r_t), cSW = kx * cd(rjm / r_t);
+        cd bb;
+        if (i == 1) {
+            const double c0 = sqrt(1.0 / (kEPS0 * eps_t * kMU0));
+            if (r_t >= prm.r1 && r_t <= prm.r2) {  // port excitation (code 7, :2606-2621)
+                const cd deno(2.0 * c0 + 1e-100, w * dx);
+                const cd R(2.0 * c0, -w * dx);
+                const double Er_Fw = prm.J1r_exc / r_t / log(prm.r2 / prm.r1) * 1e3;
+                const cd S = cd(0.0, 4.0 * w * dx) * cd(Er_Fw);
+                aP -= aW * cdiv(R, deno);
+                bb += aW * cdiv(S, deno);
+            } else {  // open (code 1, :2579-2588)
+                aP -= aW * open_r(eps_t, w, dx);
+            }
+            aW = cd();
+        }
+        if (i == ni) {  // z = L: open (code 1, :2630-2645)
+            aP -= aE * open_r(eps_t, w, dx);
+            aE = cd();
+        }
+        if (j == nj) {  // r = R: Gauss (code 2, :2687-2694)
+            const double rRn = (rjp + rj) / 2.0, rLn = (rj + rjm) / 2.0;
+            aP -= aN * cd(rLn / rRn);
+            cNE -= aN * cd(dr / dx * rj / rRn);
+            cNW += aN * cd(dr / dx * rj / rRn);
+            aN = cd();
+        }
+        A[QP * pl + q] = aP; A[QE * pl + q] = aE; A[QW * pl + q] = aW; A[QN * pl + q] = aN; A[QS * pl + q] = aS;
+        A[C0 * pl + q] = cNE; A[C1 * pl + q] = cSE; A[C2 * pl + q] = cNW; A[C3 * pl + q] = cSW;
+        A[C4 * pl + q] = cNN; A[C5 * pl + q] = cSS;
+        D.b[pl + q] = bb;
+    }
+    // ---- Ephi (cell), :2414-2453 ----
+    if (unknown(2, i, j, ni, nj)) {
+        cd* A = D.a + (size_t)2 * NQ * pl;
+        const double qL = (rjm + rj) / 2.0 / (rj + 1e-100);
+        const double qR = (rjp + rj) / 2.0 / (rj + 1e-100);
+        const Sig s = sigma(ne[q], nu[q], Bx[q], Br[q], w, me);
+        const cd s_pr = s.coef * s.hx, s_pp = s.coef, s_px = s.coef * (-s.hr);
+        cd aP = cd(2.0 * dx * dx + 2.0 * dr * dr + g2 / (rj * rj) - kEPS0 * epsr[q] * kMU0 * w * w * g2) +
+                iwm * s_pp * cd(g2);
+        cd aE(dr * dr), aW(dr * dr), aN(qR * dx * dx), aS(qL * dx * dx);
+        const cd kx = iwm * s_px * cd(-0.5 * g2), kr = iwm * s_pr * cd(-0.5 * g2);
+        if (i == 1) {  // z = 0: open (code 1, :2720-2729)
+            aP -= aW * open_r(epsr[q], w, dx);
+            aW = cd();
+        }
+        if (i == ni) {  // z = L: conductor (code 0, :2737-2739)
+            aP += aE;
+            aE = cd();
+        }
+        if (j == nj) {  // r = R: conductor (code 0, :2755-2757)
+            aP += cd(rj / rjp) * aN;
+            aN = cd();
+        }
+        A[QP * pl + q] = aP; A[QE * pl + q] = aE; A[QW * pl + q] = aW; A[QN * pl + q] = aN; A[QS * pl + q] = aS;
+        A[C0 * pl + q] = kx; A[C1 * pl + q] = kx; A[C2 * pl + q] = kr * cd(qR); A[C3 * pl + q] = kr * cd(qL);
+        A[C4 * pl + q] = cd(); A[C5 * pl + q] = cd();
+        D.b[2 * pl + q] = cd();
+    }
+}
+
+// level-0 operator of field c's preconditioner hierarchy: its own 5-point block
+// (couplings leaving the box dropped)
+__global__ void k_m3_block(Dev3 D, int c, cd* __restrict__ a0, int i0, int j0, int ncol, int nrow, int ldl) {
+    const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+    const int rr = blockIdx.y;
+    if (cc >= ncol) return;
+    const size_t n0 = (size_t)nrow * ldl, p = (size_t)rr * ldl + cc;
+    const int i = cc + i0, j = rr + j0;
+    const size_t pl = D.pl, q = (size_t)j * D.ld + i;
+    const cd* A = D.a + (size_t)c * NQ * pl;
+    a0[P * n0 + p] = A[QP * pl + q];
+    a0[W * n0 + p] = cc > 0 ? A[QW * pl + q] : cd();
+    a0[E * n0 + p] = cc + 1 < ncol ? A[QE * pl + q] : cd();
+    a0[S * n0 + p] = rr > 0 ? A[QS * pl + q] : cd();
+    a0[N * n0 + p] = rr + 1 < nrow ? A[QN * pl + q] : cd();
+}
+
+// r = rh = b, x = p = v = 0 on the unknowns; ||b||^2 and the recurrence's start
+__global__ void k_m3_prep(Dev3 D, int maxit, double* __restrict__ part, unsigned int* counter) {
+    __shared__ double red[32];
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    double bb = 0.0;
+    if (i <= D.ni) {
+        for (int c = 0; c < 3; c++) {
+            if (!unknown(c, i, j, D.ni, D.nj)) continue;
+            const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+            const cd b = D.b[q];
+            D.r[q] = b; D.rh[q] = b;
+            D.x[q] = cd(); D.p[q] = cd(); D.v[q] = cd();
+            bb += abs2(b);
+        }
+    }
+    double tot;
+    if (last_block_sum(bb, part, counter, red, &tot) && threadIdx.x == 0) {
+        double* sc = D.sc;
+        const bool fin = isfinite(tot);
+        sc_set(sc, RHO, cd(tot));
+        sc_set(sc, RHO_OLD, cd(1.0));
+        sc_set(sc, ALPHA, cd(1.0));
+        sc_set(sc, OMEGA, cd(1.0));
+        sc_set(sc, BETA, cd(0.0));
+        sc[BB] = tot;
+        sc[RR] = tot;
+        sc[RELRES] = tot > 0.0 ? 1.0 : 0.0;
+        sc[ITER] = 0.0;
+        sc[CONV] = (fin && tot == 0.0) ? 1.0 : 0.0;
+        sc[BAD] = fin ? 0.0 : 1.0;
+        sc[KEEP] = (fin && tot > 0.0 && maxit > 0) ? 1.0 : 0.0;
+    }
+}
+
+// MODE 0: p = r + beta (p - omega v);  MODE 1: s = r - alpha v.  The vector is
+// also scattered into the fields' preconditioner right-hand sides.
+template <int MODE>
+__global__ void k_m3_vec(Dev3 D, Lev0 L) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    if (i > D.ni) return;
+    const cd beta = sc_c(D.sc, BETA), omega = sc_c(D.sc, OMEGA), alpha = sc_c(D.sc, ALPHA);
+    for (int c = 0; c < 3; c++) {
+        if (!unknown(c, i, j, D.ni, D.nj)) continue;
+        const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+        cd y;
+        if (MODE == 0) {
+            y = D.r[q] + beta * (D.p[q] - omega * D.v[q]);
+            D.p[q] = y;
+        } else {
+            y = D.r[q] - alpha * D.v[q];
+            D.s[q] = y;
+        }
+        L.b[c][(size_t)(j - L.j0[c]) * L.ldl[c] + (i - L.i0[c])] = y;
+    }
+}
+
+// the preconditioner results into dst (ph or sh)
+__global__ void k_m3_gather(Dev3 D, Lev0 L, cd* __restrict__ dst) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    if (i > D.ni) return;
+    for (int c = 0; c < 3; c++) {
+        if (!unknown(c, i, j, D.ni, D.nj)) continue;
+        dst[(size_t)c * D.pl + (size_t)j * D.ld + i] = L.x[c][(size_t)(j - L.j0[c]) * L.ldl[c] + (i - L.i0[c])];
+    }
+}
+
+// MODE 0: v = A ph, alpha = rho / <rh, v>;  MODE 1: t = A sh, omega = <t, s> / <t, t>
+template <int MODE>
+__global__ void k_m3_mv(Dev3 D, double* __restrict__ part, unsigned int* counter) {
+    __shared__ double red[32];
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (i <= D.ni) {
+        for (int c = 0; c < 3; c++) {
+            if (!unknown(c, i, j, D.ni, D.nj)) continue;
+            const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+            if (MODE == 0) {
+                const cd y = apply3(D, D.ph, c, i, j);
+                D.v[q] = y;
+                const cd h = conj(D.rh[q]) * y;
+                acc[0] += h.x; acc[1] += h.y;
+            } else {
+                const cd y = apply3(D, D.sh, c, i, j);
+                D.t[q] = y;
+                const cd h = conj(y) * D.s[q];
+                acc[0] += h.x; acc[1] += h.y; acc[2] += abs2(y);
+            }
+        }
+    }
+    double tot[3];
+    if (last_block_sumk<3>(acc, part, counter, red, tot) && threadIdx.x == 0) {
+        double* sc = D.sc;
+        if (MODE == 0) {
+            const cd den(tot[0], tot[1]);
+            if (abs2(den) == 0.0 || !isfinite(tot[0]) || !isfinite(tot[1])) {
+                sc[BAD] = 1.0;
+                sc_set(sc, ALPHA, cd(0.0));
+            } else {
+                sc_set(sc, ALPHA, cdiv(sc_c(sc, RHO), den));
+            }
+        } else {
+            if (tot[2] == 0.0 || !isfinite(tot[2])) {
+                sc_set(sc, OMEGA, cd(0.0));
+                if (!(tot[2] == 0.0)) sc[BAD] = 1.0;
+            } else {
+                sc_set(sc, OMEGA, cd(tot[0] / tot[2], tot[1] / tot[2]));
+            }
+        }
+    }
+}
+
+// x += alpha ph + omega sh; r = s - omega t; stopping rule and next beta
+__global__ void k_m3_upd(Dev3 D, int maxit, double tol, double* __restrict__ part, unsigned int* counter) {
+    __shared__ double red[32];
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (i <= D.ni) {
+        const cd alpha = sc_c(D.sc, ALPHA), omega = sc_c(D.sc, OMEGA);
+        for (int c = 0; c < 3; c++) {
+            if (!unknown(c, i, j, D.ni, D.nj)) continue;
+            const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+            D.x[q] = D.x[q] + alpha * D.ph[q] + omega * D.sh[q];
+            const cd rn = D.s[q] - omega * D.t[q];
+            D.r[q] = rn;
+            const cd h = conj(D.rh[q]) * rn;
+            acc[0] += abs2(rn); acc[1] += h.x; acc[2] += h.y;
+        }
+    }
+    double tot[3];
+    if (last_block_sumk<3>(acc, part, counter, red, tot) && threadIdx.x == 0) {
+        double* sc = D.sc;
+        const int it = (int)sc[ITER] + 1;
+        const double bb = sc[BB];
+        const double rel = bb > 0.0 ? sqrt(tot[0] / bb) : 0.0;
+        const bool fin = isfinite(tot[0]) && isfinite(tot[1]) && isfinite(tot[2]);
+        const cd rho_old = sc_c(sc, RHO), rho(tot[1], tot[2]);
+        const cd alpha = sc_c(sc, ALPHA), omega = sc_c(sc, OMEGA);
+        bool bad = sc[BAD] != 0.0 || !fin;
+        const bool conv = fin && rel < tol;
+        if (!conv && (abs2(rho_old) == 0.0 || abs2(omega) == 0.0)) bad = true;
+        const cd beta = bad ? cd(0.0) : cdiv(rho, rho_old) * cdiv(alpha, omega);
+        sc_set(sc, RHO_OLD, rho_old);
+        sc_set(sc, RHO, rho);
+        sc_set(sc, BETA, beta);
+        sc[RR] = tot[0];
+        sc[RELRES] = rel;
+        sc[ITER] = (double)it;
+        sc[CONV] = conv ? 1.0 : 0.0;
+        sc[BAD] = bad ? 1.0 : 0.0;
+        sc[KEEP] = (!conv && !bad && it < maxit) ? 1.0 : 0.0;
+    }
+}
+
+// dst = src on the unknowns, zero elsewhere (3 planes)
+__global__ void k_m3_mask(Dev3 D, const cd* __restrict__ src, cd* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= D.ld) return;
+    for (int c = 0; c < 3; c++) {
+        const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+        dst[q] = unknown(c, i, j, D.ni, D.nj) ? src[q] : cd();
+    }
+}
+
+// y = A x on the unknowns (zero elsewhere)
+__global__ void k_m3_apply(Dev3 D, const cd* __restrict__ x, cd* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= D.ld) return;
+    for (int c = 0; c < 3; c++) {
+        const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+        y[q] = unknown(c, i, j, D.ni, D.nj) ? apply3(D, x, c, i, j) : cd();
+    }
+}
+
+}  // namespace m3
+}  // namespace cth
+
+using namespace cth;
+using namespace cth::m3;
+
+struct cth_mw3 {
+    int device = 0, ni = 0, nj = 0, ld = 0;
+    size_t pl = 0;
+    cth_grid* g[3] = {nullptr, nullptr, nullptr};
+    cd* a = nullptr;    // [3][NQ] planes
+    cd* b = nullptr;    // [3] planes
+    cd* vec = nullptr;  // 9 vectors x [3] planes
+    cd* tmp = nullptr;  // [3] planes (masked copy of an apply input)
+    double* sc = nullptr;
+    double* h_sc = nullptr;  // pinned
+    double* part = nullptr;
+    unsigned int* counter = nullptr;
+    bool assembled = false;
+    long long launches = 0;
+};
+
+namespace {
+
+Dev3 dev3(cth_mw3* m) {
+    Dev3 D;
+    D.a = m->a;
+    D.b = m->b;
+    cd** f[9] = {&D.x, &D.r, &D.rh, &D.p, &D.ph, &D.v, &D.s, &D.sh, &D.t};
+    for (int k = 0; k < 9; k++) *f[k] = m->vec + (size_t)k * 3 * m->pl;
+    D.sc = m->sc;
+    D.ni = m->ni;
+    D.nj = m->nj;
+    D.ld = m->ld;
+    D.pl = m->pl;
+    return D;
+}
+
+Lev0 lev0(cth_mw3* m) {
+    Lev0 L;
+    for (int c = 0; c < 3; c++) {
+        cth_grid* g = m->g[c];
+        L.b[c] = g->hc.b[0];
+        L.x[c] = g->hc.x[0];
+        L.i0[c] = g->i0;
+        L.j0[c] = g->j0;
+        L.ldl[c] = g->ldl;
+    }
+    return L;
+}
+
+void destroy(cth_mw3* m) {
+    if (!m) return;
+    cudaSetDevice(m->device);
+    cudaDeviceSynchronize();
+    for (int c = 0; c < 3; c++)
+        if (m->g[c]) cth_grid_destroy(m->g[c]);
+    for (void* p : {(void*)m->a, (void*)m->b, (void*)m->vec, (void*)m->tmp, (void*)m->sc, (void*)m->part,
+                    (void*)m->counter})
+        if (p) cudaFree(p);
+    if (m->h_sc) cudaFreeHost(m->h_sc);
+    delete m;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cth_mw3_create(int ni, int nj, int device, cth_mw3** out) {
+    if (!out || ni < 4 || nj < 4) {
+        set_error("cth_mw3_create: invalid arguments (ni, nj >= 4)");
+        return CTH_ERR_ARG;
+    }
+    *out = nullptr;
+    cth_mw3* m = new cth_mw3();
+    m->device = device;
+    m->ni = ni;
+    m->nj = nj;
+    const int boxes[3][4] = {{2, ni, 1, nj}, {1, ni, 2, nj}, {1, ni, 1, nj}};
+    for (int c = 0; c < 3; c++) {
+        const int ib[2] = {boxes[c][0], boxes[c][1]}, jb[2] = {boxes[c][2], boxes[c][3]};
+        const int rc = cth_grid_create(ni, nj, ib, jb, 1, device, &m->g[c]);
+        if (rc != CTH_OK) {
+            destroy(m);
+            return rc;
+        }
+        const int rc2 = cmg_alloc(m->g[c]);
+        if (rc2 != CTH_OK) {
+            destroy(m);
+            return rc2;
+        }
+    }
+    m->ld = m->g[2]->ld;
+    m->pl = m->g[2]->plane;
+    const size_t pl = m->pl;
+    const int nb = ((ni + 127) / 128) * nj;
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMalloc(&m->a, (size_t)3 * NQ * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cudaMalloc(&m->b, (size_t)3 * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cudaMalloc(&m->vec, (size_t)27 * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cudaMalloc(&m->tmp, (size_t)3 * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cudaMalloc(&m->sc, NWORDS * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&m->part, (size_t)(3 * nb + 8) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&m->counter, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMallocHost(&m->h_sc, NWORDS * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(m->a, 0, (size_t)3 * NQ * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cudaMemset(m->b, 0, (size_t)3 * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cudaMemset(m->vec, 0, (size_t)27 * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cudaMemset(m->sc, 0, NWORDS * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(m->counter, 0, sizeof(unsigned int));
+    if (e != cudaSuccess) {
+        destroy(m);
+        return cuda_fail(e, "cth_mw3_create");
+    }
+    *out = m;
+    return CTH_OK;
+}
+
+void cth_mw3_destroy(cth_mw3* m) { destroy(m); }
+
+int cth_mw3_ld(const cth_mw3* m) { return m ? m->ld : -1; }
+
+long long cth_mw3_launch_count(const cth_mw3* m) {
+    if (!m) return -1;
+    long long n = m->launches;
+    for (int c = 0; c < 3; c++) n += cth_launch_count(m->g[c]);
+    return n;
+}
+
+int cth_mw3_copy_planes(const cth_mw3* m, double* a_dst, double* b_dst, void* stream) {
+    if (!m || !a_dst || !b_dst) {
+        set_error("cth_mw3_copy_planes: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(m->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    CTH_CUDA(cudaMemcpyAsync(a_dst, m->a, (size_t)3 * NQ * m->pl * sizeof(cd), cudaMemcpyDeviceToDevice, s));
+    CTH_CUDA(cudaMemcpyAsync(b_dst, m->b, (size_t)3 * m->pl * sizeof(cd), cudaMemcpyDeviceToDevice, s));
+    return CTH_OK;
+}
+
+int cth_mw3_assemble_dev(cth_mw3* m, const double* ne, const double* nu, const double* Bx, const double* Br,
+                         const double* epsr, const cth_mw_params* prm, void* stream) {
+    if (!m || !ne || !nu || !Bx || !Br || !epsr || !prm || prm->dx <= 0.0 || prm->dr <= 0.0 ||
+        prm->rmin != 0.0 || !(prm->r2 > prm->r1) || prm->r1 <= 0.0 || prm->omegam <= 0.0 || prm->masse <= 0.0) {
+        set_error("cth_mw3_assemble_dev: invalid arguments (the rectangle starts on the axis: rmin = 0)");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(m->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    Dev3 D = dev3(m);
+    dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
+    k_m3_assemble<<<grd, blk, 0, s>>>(ne, nu, Bx, Br, epsr, *prm, D);
+    m->launches++;
+    CTH_CUDA(cudaGetLastError());
+    m->assembled = true;
+    return CTH_OK;
+}
+
+int cth_mw3_apply_dev(cth_mw3* m, const double* x3, double* y3, void* stream) {
+    if (!m || !x3 || !y3 || !m->assembled) {
+        set_error("cth_mw3_apply_dev: invalid arguments or system not assembled");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(m->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    Dev3 D = dev3(m);
+    dim3 blk(128), grd((m->ld + 127) / 128, m->nj + 2);
+    k_m3_mask<<<grd, blk, 0, s>>>(D, reinterpret_cast<const cd*>(x3), m->tmp);
+    k_m3_apply<<<grd, blk, 0, s>>>(D, m->tmp, reinterpret_cast<cd*>(y3));
+    m->launches += 2;
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* stream, cth_status* st) {
+    if (!m || !E3 || maxit < 0 || !(tol > 0.0) || !m->assembled) {
+        set_error("cth_mw3_solve_dev: invalid arguments or system not assembled");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(m->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    Dev3 D = dev3(m);
+    Lev0 L = lev0(m);
+    dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
+    // preconditioner hierarchies from the fields' own 5-point blocks
+    for (int c = 0; c < 3; c++) {
+        cth_grid* g = m->g[c];
+        dim3 gb(256), gg((g->ncol + 255) / 256, g->nrow[0]);
+        k_m3_block<<<gg, gb, 0, s>>>(D, c, g->hc.a[0], g->i0, g->j0, g->ncol, g->nrow[0], g->ldl);
+        m->launches++;
+        m->launches += cmg_setup(g, s);
+    }
+    k_m3_prep<<<grd, blk, 0, s>>>(D, maxit, m->part, m->counter);
+    m->launches++;
+    auto precond = [&]() {
+        for (int c = 0; c < 3; c++) m->launches += cmg_vcycle(m->g[c], s);
+    };
+    for (;;) {
+        CTH_CUDA(cudaMemcpyAsync(m->h_sc, m->sc, NWORDS * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CTH_CUDA(cudaStreamSynchronize(s));
+        if (m->h_sc[KEEP] == 0.0) break;
+        k_m3_vec<0><<<grd, blk, 0, s>>>(D, L);
+        precond();
+        k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.ph);
+        k_m3_mv<0><<<grd, blk, 0, s>>>(D, m->part, m->counter);
+        k_m3_vec<1><<<grd, blk, 0, s>>>(D, L);
+        precond();
+        k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.sh);
+        k_m3_mv<1><<<grd, blk, 0, s>>>(D, m->part, m->counter);
+        k_m3_upd<<<grd, blk, 0, s>>>(D, maxit, tol, m->part, m->counter);
+        m->launches += 7;
+        CTH_CUDA(cudaGetLastError());
+    }
+    CTH_CUDA(cudaMemcpyAsync(E3, D.x, (size_t)3 * m->pl * sizeof(cd), cudaMemcpyDeviceToDevice, s));
+    CTH_CUDA(cudaStreamSynchronize(s));
+    const double* h = m->h_sc;
+    cth_status loc{};
+    loc.iterations = (int)h[ITER];
+    loc.residual = h[RELRES];
+    loc.initial_residual = std::sqrt(h[BB]);
+    loc.converged = h[CONV] != 0.0;
+    loc.nonfinite = h[BAD] != 0.0 && !loc.converged;
+    loc.guess_residual = -1.0;
+    if (st) *st = loc;
+    if (loc.nonfinite) return CTH_NONFINITE;
+    return loc.converged ? CTH_OK : CTH_NOT_CONVERGED;
+}
+
+}  // extern "C"

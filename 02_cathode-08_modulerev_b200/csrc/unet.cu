@@ -606,40 +606,49 @@ __global__ void k_unpack(const float* __restrict__ o, int cout, int c, int ni, i
 // ---------------------------------------------------------------------------
 // 3x3 convolution on the 5th-generation tensor cores (tcgen05, accumulator in
 // tensor memory) with operands brought in by the tensor memory accelerator.
-// CTA = R image rows x 128 consecutive pixels (the MMA's M: one TMEM lane per
-// pixel) x N output channels, 4 warps.  Input channels go in chunks of 16
-// through a ring of S shared-memory stages in the canonical K-major layout
-// without swizzle (8-row core matrices of 16 bytes; the two 8-channel halves
-// of a chunk are one TMA box each, LBO apart):
+// A tile = R image rows x 128 consecutive pixels (the MMA's M: one TMEM lane
+// per pixel) x N output channels.  Input channels go in chunks of 16 through a
+// ring of S shared-memory stages in the canonical K-major layout without
+// swizzle (8-row core matrices of 16 bytes; the two 8-channel halves of a chunk
+// are one TMA box each, LBO apart):
 //   A: R+2 halo rows x 130 pixels      (pixel p of halo row h at (h*130+p)*16)
 //   B: 9 tap slabs of N x 16 weights   (channel co of tap t at (t*N+co)*16)
 // so the A operand of output row r and tap (dy, dx) is the same tile started
 // ((r+dy)*130+dx)*16 bytes further: one descriptor offset per (row, tap), and
-// the R output rows share their halo rows.  Thread 0 issues the loads (the
-// stage's full barrier counts the transaction bytes), thread 32 the MMAs
-// (M=128, N, K=16) and releases each stage by tcgen05.commit to its empty
-// barrier; the last commit releases the epilogue, where each warp reads its 32
-// TMEM lanes with tcgen05.ld.  Every wait is bounded: one that gives up sets the
-// error flag, and the CTA waits (bounded) for its copies and MMAs in flight and
-// writes nothing.  The weights have a layout of their own, [Cin/8][9][Cout][8],
-// so that the B half of a chunk is one box.
+// the R output rows share their halo rows.  The weights have a layout of their
+// own, [Cin/8][9][Cout][8], so that the B half of a chunk is one box.
+//
+// Persistent and warp-specialised: one CTA per SM walks the tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...; warp 0 issues the loads (the
+// stage's full barrier counts the transaction bytes), warp 1 the MMAs (M=128,
+// N, K=16; tcgen05.commit to the stage's empty barrier releases it), and warps
+// 2-5 drain the accumulator with tcgen05.ld (warp w reads TMEM lanes
+// 32(w%4)..+31).  Two accumulator buffers in TMEM let the epilogue of one tile
+// run under the loads and MMAs of the next.  Every wait is bounded: one that
+// gives up sets the error flag (the call's output is then not valid), and the
+// CTA waits, again bounded, for its copies and MMAs in flight before it frees
+// its tensor memory.
 // ---------------------------------------------------------------------------
 constexpr int TC_M = 128;        // pixels per row tile
 constexpr int TC_HW = TC_M + 2;  // halo row width
+constexpr int TC_THREADS = 192;  // producer warp, MMA warp, 4 epilogue warps
 
 template <int N, int R>
 struct TcShape {
     static constexpr int kAHalf = ((R + 2) * TC_HW * 16 + 127) / 128 * 128;
     static constexpr int kBHalf = 9 * N * 16;
     static constexpr int kStage = 2 * kAHalf + 2 * kBHalf;
-    static constexpr int kFit = (112 * 1024) / kStage;  // two CTAs per SM
-    static constexpr int kStages = kFit < 2 ? 2 : (kFit > 4 ? 4 : kFit);
-    static constexpr int kBar = kStages * kStage;       // full[S], empty[S], done, TMEM address
-    static constexpr int kSmem = kBar + (2 * kStages + 2) * 8;
+    static constexpr int kFit = (200 * 1024) / kStage;
+    static constexpr int kStages = kFit < 2 ? 2 : (kFit > 8 ? 8 : kFit);
+    // barriers after the stages: full[S], empty[S], tfull[2], tempty[2], fin; then the TMEM address
+    static constexpr int kBar = kStages * kStage;
+    static constexpr int kNBar = 2 * kStages + 5;
+    static constexpr int kUsed = kBar + kNBar * 8 + 8;
+    static constexpr int kSmem = kUsed < 120 * 1024 ? 120 * 1024 : kUsed;  // one CTA per SM
     static constexpr uint32_t kTx = (uint32_t)(2 * (R + 2) * TC_HW * 16 + 2 * kBHalf);
-    static constexpr uint32_t kCols = R * N <= 32 ? 32 : (R * N <= 64 ? 64 : (R * N <= 128 ? 128 : 256));
-    static_assert(R * N <= 256, "two CTAs per SM share the 512 TMEM columns");
-    static_assert(kSmem <= 113 * 1024, "two CTAs per SM");
+    static constexpr uint32_t kCols = 2 * R * N <= 64 ? 64 : (2 * R * N <= 128 ? 128 : (2 * R * N <= 256 ? 256 : 512));
+    static_assert(2 * R * N <= 512, "two accumulator buffers in the 512 TMEM columns");
+    static_assert(kUsed <= 227 * 1024, "shared memory per CTA");
 };
 
 // the (N, R) tiles instantiated
@@ -712,137 +721,175 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tc_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 template <int N, int R>
-__global__ void __launch_bounds__(128) k_conv3_tc(const __grid_constant__ CUtensorMap tin,
-                                                  const __grid_constant__ CUtensorMap tw, ConvArgs a,
-                                                  int* __restrict__ err) {
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_conv3_tc(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tw, ConvArgs a,
+               int* __restrict__ err) {
     using T = TcShape<N, R>;
     constexpr int S = T::kStages;
     extern __shared__ __align__(1024) unsigned char tsm[];
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int x0 = blockIdx.x * TC_M, y0 = blockIdx.y * R, co0 = blockIdx.z * N;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tx = (a.W + TC_M - 1) / TC_M, ty = (a.H + R - 1) / R;
+    const int ntiles = tx * ty * (a.Cout / N), nk = a.Cin / 16;
     const uint32_t base = smem_u32(tsm);
-    const uint32_t bars = base + (uint32_t)T::kBar;  // full[s] at bars + 8s, empty[s] at bars + 8(S+s)
-    const uint32_t done = bars + 16u * S;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(tsm + T::kBar + (2 * S + 1) * 8);
+    const uint32_t bars = base + (uint32_t)T::kBar;
+    const uint32_t full0 = bars, empty0 = bars + 8u * S, tfull0 = bars + 16u * S, tempty0 = tfull0 + 16u,
+                   fin = tempty0 + 16u;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(tsm + T::kBar + T::kNBar * 8);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                      "r"(T::kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 32) {
-        for (int b = 0; b < 2 * S + 1; b++)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bars + 8u * b));
+        for (int b = 0; b < 2 * S; b++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bars + 8u * b));
+        for (int b = 0; b < 2; b++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tfull0 + 8u * b));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tempty0 + 8u * b));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(fin));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tslot;
-    const int nk = a.Cin / 16;
     int fail = 0, issued = 0;
     if (tid == 0) {
-        // producer: chunk k into stage k % S once the MMAs of chunk k - S released it
-        for (int k = 0; k < nk; k++) {
-            const int s = k % S;
-            if (k >= S && !tc_wait(bars + 8u * (S + s), (uint32_t)((k / S - 1) & 1))) {
-                fail = 1;
-                break;
+        // producer: chunk after chunk of every tile through the ring
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles && !fail; t += gridDim.x) {
+            const int x0 = (t % tx) * TC_M, y0 = ((t / tx) % ty) * R, co0 = (t / (tx * ty)) * N;
+            for (int k = 0; k < nk; k++, it++) {
+                const int s = it % S;
+                if (it >= S && !tc_wait(empty0 + 8u * s, (uint32_t)((it / S - 1) & 1))) {
+                    fail = 1;
+                    break;
+                }
+                const uint32_t st = base + (uint32_t)(s * T::kStage), fb = full0 + 8u * s;
+                tc_expect(fb, T::kTx);
+                tc_load3(st, &tin, fb, 16 * k, x0 - 1, y0 - 1);
+                tc_load3(st + T::kAHalf, &tin, fb, 16 * k + 8, x0 - 1, y0 - 1);
+                tc_load3(st + 2 * T::kAHalf, &tw, fb, 0, co0, 18 * k);
+                tc_load3(st + 2 * T::kAHalf + T::kBHalf, &tw, fb, 0, co0, 18 * k + 9);
+                issued = it + 1;
             }
-            const uint32_t st = base + (uint32_t)(s * T::kStage), fb = bars + 8u * s;
-            tc_expect(fb, T::kTx);
-            tc_load3(st, &tin, fb, 16 * k, x0 - 1, y0 - 1);
-            tc_load3(st + T::kAHalf, &tin, fb, 16 * k + 8, x0 - 1, y0 - 1);
-            tc_load3(st + 2 * T::kAHalf, &tw, fb, 0, co0, 18 * k);
-            tc_load3(st + 2 * T::kAHalf + T::kBHalf, &tw, fb, 0, co0, 18 * k + 9);
-            issued = k + 1;
         }
     } else if (tid == 32) {
-        // MMA issuer: R x 9 MMAs per chunk, accumulating over taps and chunks
+        // MMA issuer: R x 9 MMAs per chunk into accumulator buffer (local tile & 1)
         constexpr uint32_t idesc = tc_idesc(N);
-        for (int k = 0; k < nk; k++) {
-            const int s = k % S;
-            if (!tc_wait(bars + 8u * s, (uint32_t)((k / S) & 1))) {
+        int it = 0, lt = 0;
+        for (int t = blockIdx.x; t < ntiles && !fail; t += gridDim.x, lt++) {
+            const int b = lt & 1;
+            if (lt >= 2 && !tc_wait(tempty0 + 8u * b, (uint32_t)((lt / 2 - 1) & 1))) {
                 fail = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t st = base + (uint32_t)(s * T::kStage);
+            const uint32_t acc = tmem + (uint32_t)(b * R * N);
+            for (int k = 0; k < nk; k++, it++) {
+                const int s = it % S;
+                if (!tc_wait(full0 + 8u * s, (uint32_t)((it / S) & 1))) {
+                    fail = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t st = base + (uint32_t)(s * T::kStage);
 #pragma unroll
+                for (int r = 0; r < R; r++) {
+#pragma unroll
+                    for (int tap = 0; tap < 9; tap++) {
+                        const int dy = tap / 3, dx = tap % 3;
+                        const uint64_t da = tc_desc(st + (uint32_t)(((r + dy) * TC_HW + dx) * 16), T::kAHalf, 128);
+                        const uint64_t db = tc_desc(st + (uint32_t)(2 * T::kAHalf + tap * N * 16), T::kBHalf, 128);
+                        tc_mma(acc + (uint32_t)(r * N), da, db, idesc, (k > 0 || tap > 0) ? 1u : 0u);
+                    }
+                }
+                tc_commit(empty0 + 8u * s);
+            }
+            if (!fail) tc_commit(tfull0 + 8u * b);
+        }
+        tc_commit(fin);
+    } else if (warp >= 2) {
+        // epilogue: pixel 32 (warp % 4) + lane of the tile, all R rows and N channels
+        const int q = warp & 3;
+        const float* __restrict__ bias = a.bias;
+        const bf16* __restrict__ gate = a.gate;
+        bf16* __restrict__ out = a.out;
+        int lt = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
+            const int b = lt & 1;
+            if (!tc_wait(tfull0 + 8u * b, (uint32_t)((lt / 2) & 1))) {
+                fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int x0 = (t % tx) * TC_M, y0 = ((t / tx) % ty) * R, co0 = (t / (tx * ty)) * N;
+            const int gx = x0 + 32 * q + lane;
+#pragma unroll 1
             for (int r = 0; r < R; r++) {
+                const int gy = y0 + r;
+                const bool live = gx < a.W && gy < a.H;
+                const size_t pix = (size_t)gy * a.W + gx;
+#pragma unroll 1
+                for (int cb = 0; cb < N / 32; cb++) {
+                    uint32_t v[32];
+                    tc_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * R * N + r * N + cb * 32), v);
+                    if (!live) continue;
+                    const int c0 = co0 + cb * 32;
+                    uint4 gv[4], ov[4];
+                    if (gate)
 #pragma unroll
-                for (int tap = 0; tap < 9; tap++) {
-                    const int dy = tap / 3, dx = tap % 3;
-                    const uint64_t da = tc_desc(st + (uint32_t)(((r + dy) * TC_HW + dx) * 16), T::kAHalf, 128);
-                    const uint64_t db = tc_desc(st + (uint32_t)(2 * T::kAHalf + tap * N * 16), T::kBHalf, 128);
-                    tc_mma(tmem + (uint32_t)(r * N), da, db, idesc, (k > 0 || tap > 0) ? 1u : 0u);
+                        for (int g = 0; g < 4; g++) gv[g] = ld8(gate + pix * a.gate_cs + a.gate_coff + c0 + 8 * g);
+                    if (a.accumulate)
+#pragma unroll
+                        for (int g = 0; g < 4; g++) ov[g] = ld8(out + pix * a.out_cs + a.out_coff + c0 + 8 * g);
+#pragma unroll
+                    for (int g = 0; g < 4; g++) {
+                        float f[8];
+#pragma unroll
+                        for (int j = 0; j < 8; j++) {
+                            f[j] = __uint_as_float(v[8 * g + j]);
+                            if (bias) f[j] += __ldg(bias + c0 + 8 * g + j);
+                            if (a.relu) f[j] = fmaxf(f[j], 0.f);
+                        }
+                        if (gate) {
+                            float gf[8];
+                            unpack8(gv[g], gf);
+#pragma unroll
+                            for (int j = 0; j < 8; j++)
+                                if (!(gf[j] > 0.f)) f[j] = 0.f;
+                        }
+                        if (a.accumulate) {
+                            float of[8];
+                            unpack8(ov[g], of);
+#pragma unroll
+                            for (int j = 0; j < 8; j++) f[j] += of[j];
+                        }
+                        st8(out + pix * a.out_cs + a.out_coff + c0 + 8 * g, pack8(f));
+                    }
                 }
             }
-            tc_commit(bars + 8u * (S + s));
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) tc_arrive(tempty0 + 8u * b);
         }
-        tc_commit(done);
     }
     __syncwarp();
     // CTA-uniform outcome, so every thread takes the same path at the barriers
-    const bool ok = __syncthreads_and((fail == 0 && tc_wait(done, 0u)) ? 1 : 0) != 0;
+    const bool ok = __syncthreads_and(fail == 0 ? 1 : 0) != 0;
     if (!ok) {
         if (tid == 0) {
             atomicExch(err, 1);
             for (int k = issued > S ? issued - S : 0; k < issued; k++)
-                tc_wait(bars + 8u * (k % S), (uint32_t)((k / S) & 1));
-        }
-        tc_wait(done, 0u);
-    } else {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int gx = x0 + tid;
-#pragma unroll 1
-        for (int r = 0; r < R; r++) {
-            const int gy = y0 + r;
-            const bool live = gx < a.W && gy < a.H;
-            const size_t pix = (size_t)gy * a.W + gx;
-#pragma unroll 1
-            for (int cb = 0; cb < N / 32; cb++) {
-                uint32_t v[32];
-                tc_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(r * N + cb * 32), v);
-                if (!live) continue;
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const int co = co0 + cb * 32 + q * 8;
-                    float f[8];
-#pragma unroll
-                    for (int j = 0; j < 8; j++) {
-                        f[j] = __uint_as_float(v[q * 8 + j]);
-                        if (a.bias) f[j] += a.bias[co + j];
-                        if (a.relu) f[j] = fmaxf(f[j], 0.f);
-                    }
-                    if (a.gate) {
-                        const uint4 g = *reinterpret_cast<const uint4*>(a.gate + pix * a.gate_cs + a.gate_coff + co);
-                        const __nv_bfloat162* gh = reinterpret_cast<const __nv_bfloat162*>(&g);
-#pragma unroll
-                        for (int j = 0; j < 4; j++) {
-                            if (!(__bfloat162float(gh[j].x) > 0.f)) f[2 * j] = 0.f;
-                            if (!(__bfloat162float(gh[j].y) > 0.f)) f[2 * j + 1] = 0.f;
-                        }
-                    }
-                    uint4* o = reinterpret_cast<uint4*>(a.out + pix * a.out_cs + a.out_coff + co);
-                    if (a.accumulate) {
-                        const uint4 old = *o;
-                        const __nv_bfloat162* oh = reinterpret_cast<const __nv_bfloat162*>(&old);
-#pragma unroll
-                        for (int j = 0; j < 4; j++) {
-                            f[2 * j] += __bfloat162float(oh[j].x);
-                            f[2 * j + 1] += __bfloat162float(oh[j].y);
-                        }
-                    }
-                    uint4 res;
-                    __nv_bfloat162* rh = reinterpret_cast<__nv_bfloat162*>(&res);
-#pragma unroll
-                    for (int j = 0; j < 4; j++) rh[j] = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
-                    *o = res;
-                }
-            }
+                tc_wait(full0 + 8u * (k % S), (uint32_t)((k / S) & 1));
         }
     }
+    tc_wait(fin, 0u);  // the MMAs are complete before the tensor memory is freed
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
@@ -881,6 +928,7 @@ struct Conv {
 
 struct cth_unet {
     int device = 0;
+    int sms = 148;  // multiprocessors of the device (persistent grids)
     int H = 0, W = 0, cin = 0, cout = 0, base = 0;
     int cpad = 32;
     std::vector<Conv> convs;
@@ -1024,6 +1072,7 @@ int build(cth_unet* n) {
     CTH_CUDA(cudaMalloc(&n->loss, sizeof(double)));
     CTH_CUDA(cudaMalloc(&n->cw, n->cout * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->err, sizeof(int)));
+    CTH_CUDA(cudaDeviceGetAttribute(&n->sms, cudaDevAttrMultiProcessorCount, n->device));
     CTH_CUDA(cudaMemset(n->err, 0, sizeof(int)));
 #define CTH_TC_ATTR(NN, RR)                                                                   \
     CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<NN, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
@@ -1078,7 +1127,7 @@ bool tmap3(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t 
 }
 
 // tcgen05 tile of a convolution: the widest N (output channels) dividing Cout,
-// then the most rows R whose grid still gives every SM two CTAs; without such
+// then the most rows R that still give every SM two tiles; without such
 // a tiling the widest N with one row
 struct TcTile {
     int n, r;
@@ -1108,11 +1157,13 @@ int launch_conv(cth_unet* n, const ConvArgs& a, cudaStream_t s) {
             set_error("cth_unet: tensor map encoding failed");
             return CTH_ERR_CUDA;
         }
-        const dim3 grd((a.W + TC_M - 1) / TC_M, (a.H + t.r - 1) / t.r, a.Cout / t.n);
-#define CTH_TC_LAUNCH(NN, RR)                                                                  \
-    if (t.n == NN && t.r == RR) {                                                              \
-        k_conv3_tc<NN, RR><<<grd, 128, TcShape<NN, RR>::kSmem, s>>>(ti, tw, a, n->err);        \
-        return CTH_OK;                                                                         \
+        // persistent: at most one CTA per SM, each walking its share of the tiles
+        const long tiles = (long)((a.W + TC_M - 1) / TC_M) * ((a.H + t.r - 1) / t.r) * (a.Cout / t.n);
+        const unsigned grd = (unsigned)std::min<long>(tiles, n->sms);
+#define CTH_TC_LAUNCH(NN, RR)                                                                   \
+    if (t.n == NN && t.r == RR) {                                                               \
+        k_conv3_tc<NN, RR><<<grd, TC_THREADS, TcShape<NN, RR>::kSmem, s>>>(ti, tw, a, n->err);  \
+        return CTH_OK;                                                                          \
     }
         CTH_TC_TILES(CTH_TC_LAUNCH)
 #undef CTH_TC_LAUNCH

@@ -293,3 +293,72 @@ def solver_SOR(aP, aE, aW, aN, aS, b, i_bl, j_bl, n_bl, alpha_SOR, maxITR, error
     if flag_msg == 1:
         print(f"ncount = {st.iterations} error_max = {st.residual}")
     return st
+
+
+class Microwave3:
+    """The magnetised 3-component microwave system of solve_Microwave
+    (include/emfieldModule.hpp:2249-2998) on the r-z rectangle (cth_mw3):
+    device assembly, the coupled operator and the preconditioned BiCGStab
+    solve.  Field planes are torch complex128 of shape (3, nj+2, ld): Ex, Er,
+    Ephi in the library layout."""
+
+    NQ = 11
+
+    def __init__(self, ni: int, nj: int, device: int = 0):
+        L = capi.load()
+        h = ctypes.c_void_p()
+        capi.check(L.cth_mw3_create(ni, nj, device, ctypes.byref(h)), allow_positive=False)
+        self._h, self._L = h, L
+        self.ni, self.nj, self.device = ni, nj, device
+        self.ld = L.cth_mw3_ld(h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.cth_mw3_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def launch_count(self) -> int:
+        return int(self._L.cth_mw3_launch_count(self._h))
+
+    def _stream(self, stream):
+        import torch
+        return (stream if stream is not None else torch.cuda.current_stream(self.device)).cuda_stream
+
+    def planes(self, n: int = 3):
+        import torch
+        return torch.zeros((n, self.nj + 2, self.ld), dtype=torch.complex128, device=f"cuda:{self.device}")
+
+    def assemble_dev(self, ne, nu, Bx, Br, epsr, params: dict, stream=None):
+        """Assemble from real device planes of cell values (library layout)."""
+        prm = capi.MWParams(**{k: float(params[k]) for k, _ in capi.MWParams._fields_})
+        capi.check(self._L.cth_mw3_assemble_dev(self._h, _ptr(ne), _ptr(nu), _ptr(Bx), _ptr(Br), _ptr(epsr),
+                                                ctypes.byref(prm), self._stream(stream)), allow_positive=False)
+
+    def coefficients(self, stream=None):
+        """(a, b): a of shape (3, 11, nj+2, ld), b of shape (3, nj+2, ld)."""
+        a = self.planes(3 * self.NQ)
+        b = self.planes(3)
+        capi.check(self._L.cth_mw3_copy_planes(self._h, _ptr(a), _ptr(b), self._stream(stream)),
+                   allow_positive=False)
+        return a.reshape(3, self.NQ, self.nj + 2, self.ld), b
+
+    def apply_dev(self, x3, stream=None):
+        y = self.planes(3)
+        capi.check(self._L.cth_mw3_apply_dev(self._h, _ptr(x3), _ptr(y), self._stream(stream)),
+                   allow_positive=False)
+        return y
+
+    def solve_dev(self, maxITR: int = 500, error_cnv: float = 1e-10, out=None, stream=None):
+        """Returns (E3, status); E3 of shape (3, nj+2, ld)."""
+        E = out if out is not None else self.planes(3)
+        st = capi.Status()
+        rc = self._L.cth_mw3_solve_dev(self._h, int(maxITR), float(error_cnv), _ptr(E), self._stream(stream),
+                                       ctypes.byref(st))
+        capi.check(rc)
+        return E, st

@@ -151,6 +151,25 @@ def mw_er_rect(ni: int = 1024, nj: int = 512, seed: int = 2, omegam: float = 2.6
                 i_bl=np.array([[1, ni]], dtype=np.int32), j_bl=np.array([[2, nj]], dtype=np.int32))
 
 
+def mw3_rect(ni: int = 1024, nj: int = 512, seed: int = 2, omegam: float = 2.67e10, bmax: float = 0.05) -> dict:
+    """Magnetised microwave system on the 10 mm (z) x 5 mm (r) rectangle.
+
+    n_e, nu and epsr as mw_er_rect (same generator and draws), plus the field of
+    a magnet near the port: Bx = bmax exp(-((z - 2 mm) / 3 mm)^2) and
+    Br = -(r / 2) dBx/dz (divergence-free to first order in r), on the cell
+    centres.  bmax = 0.05 T puts the electron cyclotron frequency at a third of
+    w = 2.67e10 rad/s.
+    """
+    w = mw_er_rect(ni, nj, seed=seed, omegam=omegam)
+    dx, dr, x, r = grid(ni, nj)
+    z0, wz = 2.0e-3, 3.0e-3
+    X, R = np.meshgrid(x, r, indexing="ij")
+    g = np.exp(-((X - z0) / wz) ** 2)
+    w["Bx"] = bmax * g
+    w["Br"] = -(R / 2.0) * bmax * g * (-2.0 * (X - z0) / wz ** 2)
+    return w
+
+
 MASSE = 9.10938356e-31               # params.hpp:34
 MASSI_XE = 131.293e-3 / 6.02214076e23  # params.hpp:35
 

@@ -624,7 +624,11 @@ def main():
             "step_ms_median": float(np.median([f["ms"] for f in first_learned])),
             "step_ms_median_network_ran": float(np.median([f["ms"] for f in first_learned if f["net_ran"]]))
             if any(f["net_ran"] for f in first_learned) else None,
-            "network": "4-level U-Net 32/64/128/256 ch, 3x3 conv, bf16 mma.sync tensor cores, FP32 accumulate",
+            "step_ms_max": float(max(f["ms"] for f in first_learned)),
+            "step_max_index": int(np.argmax([f["ms"] for f in first_learned])),
+            "step_max_network_ran": bool(first_learned[int(np.argmax([f["ms"] for f in first_learned]))]["net_ran"]),
+            "network": "4-level U-Net 32/64/128/256 ch, 3x3 conv on tcgen05 (TMA-fed, accumulators in tensor "
+                       "memory), bf16 operands, FP32 accumulate",
             "training": {"snapshots": n_snap, "held_out": n_hold, "epochs": LEARN_EPOCHS,
                          "loss_first_epoch": losses[0], "loss_last_epoch": losses[-1],
                          "heldout_rel_err_of_change": float(np.mean(held)), "collect_and_train_s": t_learn,
@@ -639,6 +643,8 @@ def main():
         "warm_start": {
             "previous_step": {"value": world * args.steps / (ms_prev / 1e3), "unit": UNIT,
                               "step_ms_median": float(np.median([f["ms"] for f in first_prev])),
+                              "step_ms_max": float(max(f["ms"] for f in first_prev)),
+                              "step_max_index": int(np.argmax([f["ms"] for f in first_prev])),
                               "first_phi_solve_cycles_mean": float(np.mean([f["iterations"] for f in first_prev])),
                               "guess_residual_mean": float(np.mean([f["guess_residual"] for f in first_prev])),
                               "fallback_rate": float(np.mean([f["guess"] != 1 for f in first_prev]))},

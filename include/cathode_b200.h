@@ -210,6 +210,41 @@ int cth_mw_er_assemble_dev(cth_grid* g, const double* ne, const double* nu, cons
                            const cth_mw_params* prm, double* aP, double* aE, double* aW, double* aN,
                            double* aS, double* b, void* stream);
 
+/* Magnetised 3-component microwave system of solve_Microwave
+ * (include/emfieldModule.hpp:2249-2998): Ex on x-faces, Er on r-faces, Ephi on
+ * cells, coupled through the magnetised cold-plasma conductivity (11-point
+ * rows, :2300-2453), on the r-z rectangle r in [0, R] (prm->rmin must be 0),
+ * z in [0, L], with the reference's boundary codes: Ex Gauss (2) at z = 0, L
+ * and conductor (0) at r = R; Er port (7) on [r1, r2] at z = 0, open (1) on
+ * the other z = 0 faces and at z = L, Gauss (2) at r = R; Ephi open (1) at
+ * z = 0, conductor (0) at z = L and r = R.  Unknowns: Ex i = 2..ni, j = 1..nj;
+ * Er i = 1..ni, j = 2..nj; Ephi i = 1..ni, j = 1..nj.  Replaces the assembly of
+ * :2785-2990 and the Eigen SparseLU factorisation (:2995-2998) by complex FP64
+ * BiCGStab, right-preconditioned block-diagonally by one complex
+ * semicoarsening V-cycle per field.
+ * Field planes (x3, y3, E3): three consecutive complex planes Ex, Er, Ephi of
+ * (nj+2) x ld complex values each (library layout, ld = cth_mw3_ld). */
+typedef struct cth_mw3 cth_mw3;
+int cth_mw3_create(int ni, int nj, int device, cth_mw3** out);
+void cth_mw3_destroy(cth_mw3* m);
+int cth_mw3_ld(const cth_mw3* m);
+long long cth_mw3_launch_count(const cth_mw3* m);
+/* ne, nu, Bx, Br, epsr: real device planes of cell values (library layout) */
+int cth_mw3_assemble_dev(cth_mw3* m, const double* ne, const double* nu, const double* Bx, const double* Br,
+                         const double* epsr, const cth_mw_params* prm, void* stream);
+/* copies the assembled coefficients into a_dst: 3 fields x 11 complex planes
+ * (P, E, W, N, S, then the couplings C0..C5 of the field: Ex rows Er at
+ * (i,j+1), (i,j), (i-1,j+1), (i-1,j) and Ephi at (i,j), (i-1,j); Er rows Ex at
+ * (i+1,j), (i+1,j-1), (i,j), (i,j-1) and Ephi at (i,j), (i,j-1); Ephi rows Ex
+ * at (i+1,j), (i,j) and Er at (i,j+1), (i,j)), and the 3 right-hand sides
+ * into b_dst (device buffers; asynchronous on stream) */
+int cth_mw3_copy_planes(const cth_mw3* m, double* a_dst, double* b_dst, void* stream);
+/* y3 = A x3 on the unknowns (x3 is read on the unknowns only; y3 is zero elsewhere) */
+int cth_mw3_apply_dev(cth_mw3* m, const double* x3, double* y3, void* stream);
+/* solve from a zero start until ||b - A E||_2 / ||b||_2 < tol; E3 receives the
+ * three fields (zero off the unknowns).  CTH_NOT_CONVERGED after maxit. */
+int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* stream, cth_status* st);
+
 /* Fluid state in HBM -----------------------------------------------------------
  * A field store holds named device planes of the grid's library layout (cell
  * arrays and the x-face (i-1/2) / r-face (j-1/2) arrays share the (ni+2)x(nj+2)

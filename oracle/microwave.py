@@ -401,3 +401,237 @@ def energy_profile(E1x, E1r, E1p, rhoe, nu_m1, Bx, Br, p, xblocks, rblocks, cblo
         out["Pabs"][i, j] = ((out["Pabsx"][i, j] + out["Pabsx"][i + 1, j]) / 2
                              + (out["Pabsr"][i, j] + out["Pabsr"][i, j + 1]) / 2 + out["Pabsp"][i, j])
     return out, tuple(P)
+
+
+# ---------------------------------------------------------------------------
+# magnetised 3-component system of EmfieldModule::solve_Microwave
+# (include/emfieldModule.hpp:2249-2998) on the rectangle r in [0, R], z in [0, L]
+# ---------------------------------------------------------------------------
+MAG_X = ("P", "E", "W", "N", "S", "NE", "SE", "NW", "SW", "EE", "WW")   # Ex rows: Er at NE..SW, Ephi at EE, WW
+MAG_R = ("P", "E", "W", "N", "S", "NE", "SE", "NW", "SW", "NN", "SS")   # Er rows: Ex at NE..SW, Ephi at NN, SS
+MAG_P = ("P", "E", "W", "N", "S", "EE", "WW", "NN", "SS")               # Ephi rows: Ex at EE, WW, Er at NN, SS
+
+
+def mag_masks(ni: int, nj: int):
+    """Unknowns of the rectangle: Ex x-faces i = 2..ni (the z = 0 and z = L faces
+    are eliminated by the Gauss law), j = 1..nj; Er r-faces i = 1..ni, j = 2..nj
+    (the axis face is not an unknown, the r = R face is eliminated by the Gauss
+    law); Ephi cells i = 1..ni, j = 1..nj."""
+    mx = np.zeros((ni + 2, nj + 2), bool); mx[2:ni + 1, 1:nj + 1] = True
+    mr = np.zeros((ni + 2, nj + 2), bool); mr[1:ni + 1, 2:nj + 1] = True
+    mp = np.zeros((ni + 2, nj + 2), bool); mp[1:ni + 1, 1:nj + 1] = True
+    return mx, mr, mp
+
+
+def _sigma_terms(rho, nu, bx, br, w, me):
+    """coef and the Hall factors of the magnetised cold-plasma conductivity
+    (emfieldModule.hpp:2312-2318), with the reference's EPS = 1e-100 (1 + i) guards."""
+    EPS = complex(1e-100, 1e-100)
+    nu_c = nu + 1j * w
+    hx = E0 * bx / (me * nu_c + EPS)
+    hr = E0 * br / (me * nu_c + EPS)
+    mag2 = hx * hx + hr * hr
+    coef = rho * E0 * E0 / (me * nu_c + EPS) / (1.0 + mag2 + EPS)
+    return coef, hx, hr
+
+
+def mag_rect_system(ne, nu, Bx, Br, epsr, p: dict):
+    """Coefficients of the three field equations after the boundary surgery.
+
+    Interior: Ex (emfieldModule.hpp:2300-2348), Er (:2352-2411), Ephi
+    (:2414-2453), stencil convention aP x_P - sum a_k x_k = b.  Boundary codes of
+    the rectangle (the reference's own codes): Ex Gauss (code 2, :2464-2471 and
+    :2497-2504) at z = 0 and z = L, conductor (code 0, :2536-2538) at r = R; Er
+    port excitation (code 7, :2606-2621) on the z = 0 faces with r1 <= r <= r2
+    and open (code 1, :2579-2588) on the others, open (code 1, :2630-2645) at
+    z = L, Gauss (code 2, :2687-2694) at r = R; Ephi open (code 1, :2720-2729) at
+    z = 0, conductor (code 0, :2737-2739 and :2755-2757) at z = L and r = R.  On
+    the axis the r-weights of the Ex and Ephi south couplings vanish and the Er
+    axis face is not an unknown, so no code is needed there.
+
+    Returns {"x": {name: array}, "r": {...}, "p": {...}, "b": (bx, br, bp), masks}
+    with complex (ni+2, nj+2) arrays in the reference's [i][j] order."""
+    ni, nj, dx, dr, w, me = p["ni"], p["nj"], p["dx"], p["dr"], p["omegam"], p["masse"]
+    r = p["r"]
+    sh = (ni + 2, nj + 2)
+    iwm = complex(0.0, w * MU0)
+    D = dx * dx * dr * dr
+    X = {k: np.zeros(sh, complex) for k in MAG_X}
+    Rr = {k: np.zeros(sh, complex) for k in MAG_R}
+    Pp = {k: np.zeros(sh, complex) for k in MAG_P}
+    bx = np.zeros(sh, complex); br = np.zeros(sh, complex); bp = np.zeros(sh, complex)
+    mx, mr, mp = mag_masks(ni, nj)
+    # --- Ex on x-faces (i between cells i-1 and i) ---
+    I, J = np.nonzero(mx)
+    qL = (r[J - 1] + r[J]) / 2.0 / (r[J] + 1e-100)
+    qR = (r[J + 1] + r[J]) / 2.0 / (r[J] + 1e-100)
+    coef, hx, hr = _sigma_terms((ne[I, J] + ne[I - 1, J]) / 2.0, (nu[I, J] + nu[I - 1, J]) / 2.0,
+                                (Bx[I, J] + Bx[I - 1, J]) / 2.0, (Br[I, J] + Br[I - 1, J]) / 2.0, w, me)
+    eps_t = (epsr[I, J] + epsr[I - 1, J]) / 2.0
+    s_xr, s_xp, s_xx = coef * (hx * hr), coef * hr, coef * (1.0 + hx * hx)
+    X["P"][I, J] = 2.0 * dx * dx + 2.0 * dr * dr - EPS0 * eps_t * MU0 * w * w * D + iwm * s_xx * D
+    X["E"][I, J] = dr * dr; X["W"][I, J] = dr * dr
+    X["N"][I, J] = qR * dx * dx; X["S"][I, J] = qL * dx * dx
+    X["EE"][I, J] = -iwm * s_xp * 0.5 * D; X["WW"][I, J] = -iwm * s_xp * 0.5 * D
+    X["NE"][I, J] = -iwm * s_xr * 0.25 * qR * D; X["NW"][I, J] = -iwm * s_xr * 0.25 * qR * D
+    X["SE"][I, J] = -iwm * s_xr * 0.25 * qL * D; X["SW"][I, J] = -iwm * s_xr * 0.25 * qL * D
+    # --- Er on r-faces (j between cells j-1 and j) ---
+    I, J = np.nonzero(mr)
+    r_t = (r[J - 1] + r[J]) / 2.0
+    rR = (r[J] + r[J + 1]) / 2.0
+    rL = (r[J - 2] + r[J - 1]) / 2.0
+    coef, hx, hr = _sigma_terms((ne[I, J] + ne[I, J - 1]) / 2.0, (nu[I, J] + nu[I, J - 1]) / 2.0,
+                                (r[J] * Bx[I, J] + r[J - 1] * Bx[I, J - 1]) / (2.0 * r_t),
+                                (r[J] * Br[I, J] + r[J - 1] * Br[I, J - 1]) / (2.0 * r_t), w, me)
+    eps_t = (epsr[I, J] + epsr[I, J - 1]) / 2.0
+    s_rr, s_rp, s_rx = coef * (1.0 + hr * hr), coef * (-hx), coef * (hx * hr)
+    Rr["P"][I, J] = (r_t * (1.0 / r[J] + 1.0 / r[J - 1]) * dx * dx + 2.0 * dr * dr
+                     - EPS0 * eps_t * MU0 * w * w * D + iwm * s_rr * D)
+    Rr["E"][I, J] = dr * dr; Rr["W"][I, J] = dr * dr
+    Rr["N"][I, J] = rR / r[J] * dx * dx; Rr["S"][I, J] = rL / r[J - 1] * dx * dx
+    Rr["NN"][I, J] = -iwm * s_rp * 0.5 * r[J] / r_t * D
+    Rr["SS"][I, J] = -iwm * s_rp * 0.5 * r[J - 1] / r_t * D
+    Rr["NE"][I, J] = -iwm * s_rx * 0.25 * r[J] / r_t * D; Rr["NW"][I, J] = -iwm * s_rx * 0.25 * r[J] / r_t * D
+    Rr["SE"][I, J] = -iwm * s_rx * 0.25 * r[J - 1] / r_t * D; Rr["SW"][I, J] = -iwm * s_rx * 0.25 * r[J - 1] / r_t * D
+    # --- Ephi on cells ---
+    I, J = np.nonzero(mp)
+    qL = (r[J - 1] + r[J]) / 2.0 / (r[J] + 1e-100)
+    qR = (r[J + 1] + r[J]) / 2.0 / (r[J] + 1e-100)
+    coef, hx, hr = _sigma_terms(ne[I, J], nu[I, J], Bx[I, J], Br[I, J], w, me)
+    s_pr, s_pp, s_px = coef * hx, coef, coef * (-hr)
+    Pp["P"][I, J] = (2.0 * dx * dx + 2.0 * dr * dr + D / (r[J] * r[J])
+                     - EPS0 * epsr[I, J] * MU0 * w * w * D + iwm * s_pp * D)
+    Pp["E"][I, J] = dr * dr; Pp["W"][I, J] = dr * dr
+    Pp["N"][I, J] = qR * dx * dx; Pp["S"][I, J] = qL * dx * dx
+    Pp["EE"][I, J] = -iwm * s_px * 0.5 * D; Pp["WW"][I, J] = -iwm * s_px * 0.5 * D
+    Pp["NN"][I, J] = -iwm * s_pr * 0.5 * qR * D; Pp["SS"][I, J] = -iwm * s_pr * 0.5 * qL * D
+
+    def open_R(eps_t):
+        c0 = np.sqrt(1.0 / (EPS0 * eps_t * MU0))
+        deno = (2.0 * c0) ** 2 + (w * dx) ** 2
+        return complex((2.0 * c0) ** 2 - (w * dx) ** 2, -4.0 * c0 * w * dx) / (deno + 1e-100)
+
+    for j in range(1, nj + 1):
+        qL = (r[j - 1] + r[j]) / 2.0 / (r[j] + 1e-100)
+        qR = (r[j + 1] + r[j]) / 2.0 / (r[j] + 1e-100)
+        # Ex, z = 0 (first unknown face i = 2): Gauss
+        i = 2
+        a = X["W"][i, j]
+        X["P"][i, j] -= a
+        X["NW"][i, j] += a * dx / dr * qR
+        X["SW"][i, j] -= a * dx / dr * qL
+        X["W"][i, j] = 0.0
+        # Ex, z = L (last unknown face i = ni): Gauss
+        i = ni
+        a = X["E"][i, j]
+        X["P"][i, j] -= a
+        X["NE"][i, j] -= a * dx / dr * qR
+        X["SE"][i, j] += a * dx / dr * qL
+        X["E"][i, j] = 0.0
+        # Ephi, z = 0: open; z = L: conductor
+        i = 1
+        Pp["P"][i, j] -= Pp["W"][i, j] * open_R(epsr[i, j])
+        Pp["W"][i, j] = 0.0
+        i = ni
+        Pp["P"][i, j] += Pp["E"][i, j]
+        Pp["E"][i, j] = 0.0
+    for j in range(2, nj + 1):
+        # Er, z = 0: port excitation on [r1, r2], open elsewhere
+        i = 1
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        r_t = (r[j] + r[j - 1]) / 2.0
+        if p["r1"] <= r_t <= p["r2"]:
+            c0 = np.sqrt(1.0 / (EPS0 * eps_t * MU0))
+            deno = complex(2.0 * c0, w * dx)
+            Rq = complex(2.0 * c0, -w * dx)
+            Er_Fw = p["J1r_exc"] / r_t / np.log(p["r2"] / p["r1"]) * 1e3
+            S = complex(0.0, 4.0 * w * dx) * Er_Fw
+            Rr["P"][i, j] -= Rr["W"][i, j] * Rq / (deno + 1e-100)
+            br[i, j] += Rr["W"][i, j] * S / (deno + 1e-100)
+        else:
+            Rr["P"][i, j] -= Rr["W"][i, j] * open_R(eps_t)
+        Rr["W"][i, j] = 0.0
+        # Er, z = L: open
+        i = ni
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        Rr["P"][i, j] -= Rr["E"][i, j] * open_R(eps_t)
+        Rr["E"][i, j] = 0.0
+    for i in range(1, ni + 1):
+        j = nj
+        rR = (r[j + 1] + r[j]) / 2.0
+        rL = (r[j] + r[j - 1]) / 2.0
+        # Er, r = R: Gauss
+        a = Rr["N"][i, j]
+        Rr["P"][i, j] -= a * rL / rR
+        Rr["NE"][i, j] -= a * dr / dx * r[j] / rR
+        Rr["NW"][i, j] += a * dr / dx * r[j] / rR
+        Rr["N"][i, j] = 0.0
+        # Ex (i >= 2) and Ephi, r = R: conductor
+        if i >= 2:
+            X["P"][i, j] += r[j] / r[j + 1] * X["N"][i, j]
+            X["N"][i, j] = 0.0
+        Pp["P"][i, j] += r[j] / r[j + 1] * Pp["N"][i, j]
+        Pp["N"][i, j] = 0.0
+    return dict(x=X, r=Rr, p=Pp, b=(bx, br, bp), masks=(mx, mr, mp))
+
+
+# neighbour offsets (di, dj, target component) of each coupling
+_NB_X = {"E": (1, 0, 0), "W": (-1, 0, 0), "N": (0, 1, 0), "S": (0, -1, 0),
+         "NE": (0, 1, 1), "SE": (0, 0, 1), "NW": (-1, 1, 1), "SW": (-1, 0, 1), "EE": (0, 0, 2), "WW": (-1, 0, 2)}
+_NB_R = {"E": (1, 0, 1), "W": (-1, 0, 1), "N": (0, 1, 1), "S": (0, -1, 1),
+         "NE": (1, 0, 0), "SE": (1, -1, 0), "NW": (0, 0, 0), "SW": (0, -1, 0), "NN": (0, 0, 2), "SS": (0, -1, 2)}
+_NB_P = {"E": (1, 0, 2), "W": (-1, 0, 2), "N": (0, 1, 2), "S": (0, -1, 2),
+         "EE": (1, 0, 0), "WW": (0, 0, 0), "NN": (0, 1, 1), "SS": (0, 0, 1)}
+
+
+def mag_rect_matrix(sysd: dict):
+    """Sparse matrix of the three equations (unknown order: Ex, Er, Ephi, each
+    row-major over (i, j) as the reference numbers them, :2790-2820), inserting
+    only unknown-to-unknown couplings (:2822-2990).  Returns (A csr, b, keys)."""
+    import scipy.sparse as sp
+    masks = sysd["masks"]
+    sh = masks[0].shape
+    kmap = []
+    off = 0
+    for m in masks:
+        k = -np.ones(sh, np.int64)
+        k[m] = off + np.arange(int(m.sum()))
+        kmap.append(k)
+        off += int(m.sum())
+    rows, cols, vals = [], [], []
+    for comp, (coefs, nb) in enumerate(((sysd["x"], _NB_X), (sysd["r"], _NB_R), (sysd["p"], _NB_P))):
+        I, J = np.nonzero(masks[comp])
+        krow = kmap[comp][I, J]
+        rows.append(krow); cols.append(krow); vals.append(coefs["P"][I, J])
+        for name, (di, dj, tc) in nb.items():
+            kc = kmap[tc][I + di, J + dj]
+            ok = kc >= 0
+            rows.append(krow[ok]); cols.append(kc[ok]); vals.append(-coefs[name][I, J][ok])
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(off, off))
+    b = np.concatenate([sysd["b"][c][masks[c]] for c in range(3)])
+    return A, b, kmap
+
+
+def mag_rect_solve(sysd: dict):
+    """Direct sparse solve (SuperLU; the reference factorises with Eigen
+    SparseLU, :2995-2998).  Returns Ex, Er, Ephi as (ni+2, nj+2) complex arrays."""
+    import scipy.sparse.linalg as spl
+    A, b, _ = mag_rect_matrix(sysd)
+    x = spl.splu(A.tocsc()).solve(b)
+    return mag_unpack(sysd, x)
+
+
+def mag_unpack(sysd: dict, x):
+    masks = sysd["masks"]
+    out, off = [], 0
+    for m in masks:
+        f = np.zeros(m.shape, complex)
+        n = int(m.sum())
+        f[m] = x[off:off + n]
+        out.append(f)
+        off += n
+    return tuple(out)
+
+
+def mag_pack(sysd: dict, fields):
+    return np.concatenate([fields[c][sysd["masks"][c]] for c in range(3)])

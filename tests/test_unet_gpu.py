@@ -118,12 +118,13 @@ def test_learned_warm_start_of_the_potential(pkg, cuda_device):
     net.close()
 
 
-@pytest.mark.parametrize("shape", [(24, 40), (16, 296)])
+@pytest.mark.parametrize("shape", [(24, 40), (16, 296), (160, 1024), (512, 1024)])
 def test_tensor_core_paths_agree(pkg, cuda_device, shape):
     """The tcgen05 convolutions (accumulator in tensor memory) and the warp-level
     mma.sync convolutions give the same network output and gradients up to
     accumulation order (bf16 activations: relative 1e-2 / 3e-2), over partial
-    and several 128-pixel tiles."""
+    and several 128-pixel tiles; the two larger images reach the tiles of two
+    and four output rows per tensor-core tile."""
     import torch
     from oracle import unet
     H, W = shape
