@@ -485,6 +485,8 @@ struct cth_mw3 {
     unsigned int* counter = nullptr;
     bool assembled = false;
     long long launches = 0;
+    cudaStream_t side[2] = {nullptr, nullptr};  // the Er and Ephi V-cycles run beside the Ex one
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -526,6 +528,11 @@ void destroy(cth_mw3* m) {
                     (void*)m->counter})
         if (p) cudaFree(p);
     if (m->h_sc) cudaFreeHost(m->h_sc);
+    for (int k = 0; k < 2; k++) {
+        if (m->side[k]) cudaStreamDestroy(m->side[k]);
+        if (m->join[k]) cudaEventDestroy(m->join[k]);
+    }
+    if (m->fork) cudaEventDestroy(m->fork);
     delete m;
 }
 
@@ -575,6 +582,11 @@ int cth_mw3_create(int ni, int nj, int device, cth_mw3** out) {
     if (e == cudaSuccess) e = cudaMemset(m->vec, 0, (size_t)27 * pl * sizeof(cd));
     if (e == cudaSuccess) e = cudaMemset(m->sc, 0, NWORDS * sizeof(double));
     if (e == cudaSuccess) e = cudaMemset(m->counter, 0, sizeof(unsigned int));
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+        e = cudaStreamCreateWithFlags(&m->side[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->join[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->fork, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         destroy(m);
         return cuda_fail(e, "cth_mw3_create");
@@ -650,29 +662,49 @@ int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* strea
     Dev3 D = dev3(m);
     Lev0 L = lev0(m);
     dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
-    // preconditioner hierarchies from the fields' own 5-point blocks
+    // preconditioner hierarchies from the fields' own 5-point blocks, the three
+    // set-ups side by side
+    CTH_CUDA(cudaEventRecord(m->fork, s));
+    for (int k = 0; k < 2; k++) CTH_CUDA(cudaStreamWaitEvent(m->side[k], m->fork, 0));
     for (int c = 0; c < 3; c++) {
         cth_grid* g = m->g[c];
+        cudaStream_t sc = c == 0 ? s : m->side[c - 1];
         dim3 gb(256), gg((g->ncol + 255) / 256, g->nrow[0]);
-        k_m3_block<<<gg, gb, 0, s>>>(D, c, g->hc.a[0], g->i0, g->j0, g->ncol, g->nrow[0], g->ldl);
+        k_m3_block<<<gg, gb, 0, sc>>>(D, c, g->hc.a[0], g->i0, g->j0, g->ncol, g->nrow[0], g->ldl);
         m->launches++;
-        m->launches += cmg_setup(g, s);
+        m->launches += cmg_setup(g, sc);
+    }
+    for (int k = 0; k < 2; k++) {
+        CTH_CUDA(cudaEventRecord(m->join[k], m->side[k]));
+        CTH_CUDA(cudaStreamWaitEvent(s, m->join[k], 0));
     }
     k_m3_prep<<<grd, blk, 0, s>>>(D, maxit, m->part, m->counter);
     m->launches++;
-    auto precond = [&]() {
-        for (int c = 0; c < 3; c++) m->launches += cmg_vcycle(m->g[c], s);
+    // the three fields' V-cycles are independent: Ex on the caller's stream, Er
+    // and Ephi on two side streams, joined before the gather
+    auto precond = [&]() -> cudaError_t {
+        cudaError_t err = cudaEventRecord(m->fork, s);
+        for (int k = 0; k < 2 && err == cudaSuccess; k++) err = cudaStreamWaitEvent(m->side[k], m->fork, 0);
+        if (err != cudaSuccess) return err;
+        m->launches += cmg_vcycle(m->g[0], s);
+        for (int k = 0; k < 2; k++) {
+            m->launches += cmg_vcycle(m->g[1 + k], m->side[k]);
+            err = cudaEventRecord(m->join[k], m->side[k]);
+            if (err == cudaSuccess) err = cudaStreamWaitEvent(s, m->join[k], 0);
+            if (err != cudaSuccess) return err;
+        }
+        return cudaSuccess;
     };
     for (;;) {
         CTH_CUDA(cudaMemcpyAsync(m->h_sc, m->sc, NWORDS * sizeof(double), cudaMemcpyDeviceToHost, s));
         CTH_CUDA(cudaStreamSynchronize(s));
         if (m->h_sc[KEEP] == 0.0) break;
         k_m3_vec<0><<<grd, blk, 0, s>>>(D, L);
-        precond();
+        CTH_CUDA(precond());
         k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.ph);
         k_m3_mv<0><<<grd, blk, 0, s>>>(D, m->part, m->counter);
         k_m3_vec<1><<<grd, blk, 0, s>>>(D, L);
-        precond();
+        CTH_CUDA(precond());
         k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.sh);
         k_m3_mv<1><<<grd, blk, 0, s>>>(D, m->part, m->counter);
         k_m3_upd<<<grd, blk, 0, s>>>(D, maxit, tol, m->part, m->counter);

@@ -10,7 +10,9 @@ continuity + correction, potential predictor-corrector (2 iterations), electron
 density and energy Scharfetter-Gummel predictor-correctors (2 iterations each),
 ground-state and metastable neutrals, transport coefficients: 12 implicit
 5-point solves to 1e-10 relative residual, as input/setup.yaml sets them) plus
-the microwave Er solve every 100 steps (ndiv_MW).
+the microwave solve every 100 steps (ndiv_MW): the magnetised 3-component
+system (Ex, Er, Ephi coupled through the cold-plasma tensor of the discharge's
+density, collision frequency and cusp field).
 
 Reported line (rank 0):
   value        time steps/s with every inner solve on the mixed-precision path
@@ -31,8 +33,9 @@ Reported line (rank 0):
   roofline     finest-level z-line relaxation kernel of the cell-grid solves:
                algorithmic bytes / CUDA-event time vs the measured HBM copy
                bandwidth
-  linear_systems  the isolated 512 x 1024 potential (slab epsr 3.8) and
-               microwave Er systems, mixed vs FP64, to 1e-10
+  linear_systems  the isolated 512 x 1024 potential (slab epsr 3.8), the
+               microwave Er system (B = 0) and the magnetised 3-component
+               microwave system, to 1e-10
   cpu_baseline the CPU restatement of the step (oracle: numpy assembly, the
                semicoarsening MG in C with OpenMP) on a bounded sample
 
@@ -71,11 +74,12 @@ def workload_config(extra=None):
     c = {
         "workload": "synthetic xenon discharge, 512 (r) x 1024 (z) r-z rectangle: one predictor-corrector time step "
                     "(ions, potential, electron density and energy, neutrals, transport: 12 implicit 5-point "
-                    "solves to 1e-10) + the microwave Er solve every 100 steps",
+                    "solves to 1e-10) + the magnetised 3-component microwave solve every 100 steps",
         "ni_z": NI, "nj_r": NJ, "tol": TOL, "maxit": MAXIT, "dt": 1e-10, "ndiv_mw": NDIV_MW,
         "l2": "no flush: the step's working set (~60 planes x 4.2 MB) exceeds the 126 MB L2",
         "method": "semicoarsening MG (z-line zebra smoother, Galerkin), FP32 cycles + FP64 defect correction; "
-                  "microwave: complex FP64 BiCGStab preconditioned by one complex semicoarsening V-cycle",
+                  "microwave: complex FP64 BiCGStab on the coupled Ex/Er/Ephi operator, preconditioned by one "
+                  "complex semicoarsening V-cycle per field",
     }
     if extra:
         c.update(extra)
@@ -280,8 +284,29 @@ def linear_systems(pkg, dev, stream, steps=10):
     out["helmholtz_ms"] = e0.elapsed_time(e1) / steps
     out["helmholtz_iterations"] = stb.iterations
     out["poisson_mixed_over_fp64"] = out["poisson_fp64_ms"] / out["poisson_mixed_ms"]
+    # (c) the magnetised 3-component system
+    w3 = pkg.workloads.mw3_rect(NI, NJ, seed=2)
+    m3 = pkg.Microwave3(NI, NJ, device=dev.index)
+    f3 = [gb.to_device(w3[k]) for k in ("ne", "nu", "Bx", "Br", "epsr")]
+    e3 = m3.planes(3)
+    for _ in range(2):
+        m3.assemble_dev(*f3, w3["params"], stream=stream)
+        m3.solve_dev(maxITR=200, error_cnv=TOL, out=e3, stream=stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        m3.assemble_dev(*f3, w3["params"], stream=stream)
+        _, st3 = m3.solve_dev(maxITR=200, error_cnv=TOL, out=e3, stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    out["microwave3_ms"] = e0.elapsed_time(e1) / steps
+    out["microwave3_iterations"] = st3.iterations
+    out["microwave3_unknowns"] = 3 * NI * NJ - NI - NJ
     out["workload"] = ("(a) potential with a 1:3.8 dielectric slab, electrodes 0/20 V, axis; (b) microwave Er, "
-                       "B = 0 cold plasma (n_e 1e15-1e18, nu 1e8-1e10), port/open/Gauss; each to 1e-10 from zero")
+                       "B = 0 cold plasma (n_e 1e15-1e18, nu 1e8-1e10), port/open/Gauss; (c) magnetised Ex/Er/Ephi "
+                       "system, same plasma, magnet field of 0.05 T near the port; each to 1e-10 from zero")
+    m3.close()
     g.close()
     gb.close()
     return out
@@ -338,6 +363,9 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="profiling mode: after --warmup steps run this many mixed steps inside the NVTX range "
                          "'timed_step' and exit (no other legs, no JSON line)")
+    ap.add_argument("--profile-network", type=int, default=0,
+                    help="profiling mode: the warm-start network alone at 512 x 1024 -- after --warmup forward "
+                         "passes and training steps, this many more of each on seeded inputs, then exit")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every multigrid kernel individually (profilers cannot see kernels inside "
                          "conditional graphs); same kernels, host convergence checks")
@@ -355,6 +383,20 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.profile_network > 0:
+        net = pkg.learned.UNet(NJ, NI, seed=0)
+        gen = torch.Generator(device=dev).manual_seed(0)
+        x = torch.randn((NJ, NI, 6), device=dev, generator=gen)
+        y = torch.randn((NJ, NI, 3), device=dev, generator=gen)
+        m = torch.ones((NJ, NI), device=dev)
+        for _ in range(args.warmup + args.profile_network):
+            net.forward(x)
+            net.train_step(x, y, m, NI * NJ, 1e-4)
+        net.check()
+        print(f"profiled {args.profile_network} network forward passes and training steps after "
+              f"{args.warmup} warm-up ones", flush=True)
+        net.close()
+        return 0
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
@@ -382,7 +424,7 @@ def main():
         fs.set_table(k, v)
     fs.upload("epsr_mw", np.ones((NI + 2, NJ + 2)))
     eb = torch.zeros((NJ + 2, gb.ld), dtype=torch.complex128, device=dev)
-    grids = (g, gx, gr, gb)
+    grids = [g, gx, gr, gb]
 
     def reset(prec, warm_start=0, net=None):
         for k, v in init.items():
@@ -402,10 +444,15 @@ def main():
         torch.cuda.synchronize(dev)
         return P
 
+    m3 = pkg.Microwave3(NI, NJ, device=local)
+    e3 = m3.planes(3)
+    grids.append(m3)
+
     def microwave():
-        ne, nu, ep = (_Plane(fs.ptr(k)) for k in ("rhoe", "nu_m", "epsr_mw"))
-        pb = gb.mw_er_assemble_dev(ne, nu, ep, wb["params"], stream=stream)
-        return gb.c5_solve_dev(*pb, eb, maxITR=200, error_cnv=TOL, stream=stream)
+        # solve_Microwave: the magnetised 3-component system on the discharge's fields
+        f3 = [_Plane(fs.ptr(k)) for k in ("rhoe", "nu_m", "Bx", "Br", "epsr_mw")]
+        m3.assemble_dev(*f3, wb["params"], stream=stream)
+        return m3.solve_dev(maxITR=200, error_cnv=TOL, out=e3, stream=stream)[1]
 
     def step(P):
         r = fs.fluid_step(gx, gr, P, stream=stream)
@@ -448,7 +495,7 @@ def main():
         return float(t.item()), launches, last, mw_solves, P
 
     if args.no_graphs:
-        for x in grids:
+        for x in (g, gx, gr, gb):
             x.set_graphs(False)
     if args.profile_steps > 0:
         P = reset(capi.CTH_PREC_MIXED)
