@@ -591,6 +591,25 @@ __global__ void k_features(const double* __restrict__ rhoe, const double* __rest
     }
 }
 
+// one pass of a 5-point smoother on channel c of the network output over the
+// first ny x nx pixels (the grid cells): v <- (4 v + vN + vS + vE + vW) / 8, a
+// neighbour outside the cells replaced by v itself (no flux through the edges)
+__global__ void k_smooth5(const float* __restrict__ src, float* __restrict__ dst, int cout, int c, int ny, int nx,
+                          int W) {
+    const int n = ny * nx;
+    const size_t row = (size_t)W * cout;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int y = q / nx, x = q % nx;
+        const size_t p = ((size_t)y * W + x) * cout + c;
+        const float v = src[p];
+        const float vn = y + 1 < ny ? src[p + row] : v;
+        const float vs = y > 0 ? src[p - row] : v;
+        const float ve = x + 1 < nx ? src[p + cout] : v;
+        const float vw = x > 0 ? src[p - cout] : v;
+        dst[p] = (4.f * v + vn + vs + ve + vw) * 0.125f;
+    }
+}
+
 // guess = base + channel c of the network output (de-normalised) in the grid
 // cells: the network predicts the change from the previous step's correction
 __global__ void k_unpack(const float* __restrict__ o, int cout, int c, int ni, int nj, int ld, int W, float om,
@@ -952,6 +971,8 @@ struct cth_unet {
     float* cw = nullptr;     // per-output-channel loss weights
     Stats stats{};
     float* feat = nullptr;   // input features of the warm-start prediction
+    float* smooth = nullptr; // ping-pong buffer of the prediction smoother
+    int smooth_passes = 0;   // 5-point smoothing passes on the predicted change
     long long launches = 0;  // kernels launched by the forward passes and predictions
     bool use_tc = true;      // convolutions on tcgen05 (false: warp-level mma.sync kernel)
     int* err = nullptr;      // device flag: a bounded wait of a tcgen05 convolution gave up
@@ -1312,7 +1333,8 @@ void cth_unet_destroy(cth_unet* n) {
     for (void* p : n->bufs) cudaFree(p);
     for (void* p : {(void*)n->prm, (void*)n->grad, (void*)n->adam_m, (void*)n->adam_v, (void*)n->wb, (void*)n->wt,
                     (void*)n->wbt, (void*)n->wtt,
-                    (void*)n->out, (void*)n->dout, (void*)n->loss, (void*)n->cw, (void*)n->feat, (void*)n->err})
+                    (void*)n->out, (void*)n->dout, (void*)n->loss, (void*)n->cw, (void*)n->feat, (void*)n->err,
+                    (void*)n->smooth})
         if (p) cudaFree(p);
     delete n;
 }
@@ -1324,6 +1346,15 @@ long long cth_unet_launch_count(const cth_unet* n) { return n ? n->launches : -1
 int cth_unet_set_tensor_cores(cth_unet* n, int tcgen05) {
     if (!n) { set_error("cth_unet_set_tensor_cores: null network"); return CTH_ERR_ARG; }
     n->use_tc = tcgen05 != 0;
+    return CTH_OK;
+}
+
+int cth_unet_set_smoothing(cth_unet* n, int passes) {
+    if (!n || passes < 0 || passes > 64) {
+        set_error("cth_unet_set_smoothing: passes in [0, 64]");
+        return CTH_ERR_ARG;
+    }
+    n->smooth_passes = passes;
     return CTH_OK;
 }
 
@@ -1482,7 +1513,18 @@ int cth_unet_predict_dphi(cth_unet* n, cth_fields* fs, void* stream) {
     const double* prev = field_ptr(fs, "dphi_prev");
     if (!dst || !prev) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
     const int ncell = fs->g->ni * fs->g->nj;
-    k_unpack<<<grid1((size_t)ncell), 256, 0, s>>>(n->out, n->cout, 2, fs->g->ni, fs->g->nj, fs->g->ld, n->W,
+    const float* o = n->out;
+    if (n->smooth_passes > 0) {
+        if (!n->smooth) CTH_CUDA(cudaMalloc(&n->smooth, npx * n->cout * sizeof(float)));
+        float* buf[2] = {n->out, n->smooth};
+        for (int k = 0; k < n->smooth_passes; k++) {
+            k_smooth5<<<grid1((size_t)ncell), 256, 0, s>>>(buf[k & 1], buf[(k + 1) & 1], n->cout, 2, fs->g->nj,
+                                                           fs->g->ni, n->W);
+        }
+        o = buf[n->smooth_passes & 1];
+        n->launches += n->smooth_passes;
+    }
+    k_unpack<<<grid1((size_t)ncell), 256, 0, s>>>(o, n->cout, 2, fs->g->ni, fs->g->nj, fs->g->ld, n->W,
                                                    n->stats.out_mean[2], n->stats.out_std[2], prev, dst);
     n->launches += 2;  // features, unpack
     CTH_CUDA(cudaGetLastError());

@@ -110,6 +110,11 @@ class UNet:
         """Kernels launched by forward passes and predictions since creation."""
         return int(self._L.cth_unet_launch_count(self.handle))
 
+    def set_smoothing(self, passes: int):
+        """5-point smoothing passes applied to the predicted change before it
+        becomes the potential solve's guess (default 0)."""
+        capi.check(self._L.cth_unet_set_smoothing(self.handle, int(passes)), allow_positive=False)
+
     def set_tensor_cores(self, tcgen05: bool):
         """Convolutions on tcgen05 (default) or on the warp-level mma.sync kernel."""
         capi.check(self._L.cth_unet_set_tensor_cores(self.handle, int(tcgen05)), allow_positive=False)

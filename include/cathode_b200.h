@@ -606,6 +606,10 @@ long long cth_unet_launch_count(const cth_unet* n);  /* kernels of forward passe
  * accumulator in tensor memory (1, default) or on the warp-level mma.sync
  * kernel (0) */
 int cth_unet_set_tensor_cores(cth_unet* n, int tcgen05);
+/* passes (0..64, default 0) of a 5-point smoother, (4 v + neighbours) / 8 with
+ * edge-replicating neighbours, applied to the predicted change of the first
+ * potential correction before cth_unet_predict_dphi forms the guess */
+int cth_unet_set_smoothing(cth_unet* n, int passes);
 /* synchronises; CTH_ERR_CUDA if a tensor-core convolution's bounded wait for
  * its MMAs gave up (the output of that call is then not valid) */
 int cth_unet_check(cth_unet* n);

@@ -83,8 +83,10 @@ def test_mw3_operator_matches_oracle(pkg, cuda_device):
     m.close(); g.close()
 
 
-@pytest.mark.parametrize("shape,bmax", [((64, 32), 0.05), ((96, 40), 0.02), ((64, 32), 0.0)])
+@pytest.mark.parametrize("shape,bmax", [((64, 32), 0.05), ((96, 40), 0.02), ((64, 32), 0.0), ((128, 64), 0.2)])
 def test_mw3_solve_matches_direct(pkg, cuda_device, shape, bmax):
+    """Against the sparse direct solve; bmax = 0.2 T puts the electron cyclotron
+    resonance (0.152 T at w = 2.67e10 rad/s) inside the domain."""
     ni, nj = shape
     w, p, mw = _case(pkg, ni, nj, bmax=bmax)
     ref = mw.mag_rect_system(w["ne"], w["nu"], w["Bx"], w["Br"], w["epsr"], p)
