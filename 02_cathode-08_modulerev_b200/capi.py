@@ -32,7 +32,7 @@ EXPORTS = (
     "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs", "cth_grid_set_tail", "cth_grid_time_relax",
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_mw3_create", "cth_mw3_destroy", "cth_mw3_ld", "cth_mw3_launch_count", "cth_mw3_assemble_dev",
-    "cth_mw3_copy_planes", "cth_mw3_apply_dev", "cth_mw3_solve_dev",
+    "cth_mw3_copy_planes", "cth_mw3_apply_dev", "cth_mw3_solve_dev", "cth_mw3_set_graphs",
     "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_fields_upload_many",
     "cth_fields_download_many", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
@@ -226,6 +226,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_mw3_apply_dev.restype = ctypes.c_int
     L.cth_mw3_solve_dev.argtypes = [_vp, ctypes.c_int, ctypes.c_double, _vp, _vp, ctypes.POINTER(Status)]
     L.cth_mw3_solve_dev.restype = ctypes.c_int
+    L.cth_mw3_set_graphs.argtypes = [_vp, ctypes.c_int]
+    L.cth_mw3_set_graphs.restype = ctypes.c_int
     L.cth_fields_create.argtypes = [_vp, ctypes.POINTER(_vp)]
     L.cth_fields_create.restype = ctypes.c_int
     L.cth_fields_destroy.argtypes = [_vp]

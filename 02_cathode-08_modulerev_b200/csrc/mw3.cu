@@ -63,6 +63,13 @@ struct Lev0 {
     int i0[3], j0[3], ldl[3];
 };
 
+// per-call arguments, in device memory so that one captured graph serves every call
+struct Args3 {
+    int maxit;
+    double tol;
+    cd* out;  // three field planes
+};
+
 struct Dev3 {
     cd* a;  // [3][NQ] planes
     cd* b;  // [3] planes
@@ -286,7 +293,8 @@ __global__ void k_m3_block(Dev3 D, int c, cd* __restrict__ a0, int i0, int j0, i
 }
 
 // r = rh = b, x = p = v = 0 on the unknowns; ||b||^2 and the recurrence's start
-__global__ void k_m3_prep(Dev3 D, int maxit, double* __restrict__ part, unsigned int* counter) {
+__global__ void k_m3_prep(Dev3 D, const Args3* __restrict__ args, double* __restrict__ part, unsigned int* counter,
+                          cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ double red[32];
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y;
@@ -316,7 +324,9 @@ __global__ void k_m3_prep(Dev3 D, int maxit, double* __restrict__ part, unsigned
         sc[ITER] = 0.0;
         sc[CONV] = (fin && tot == 0.0) ? 1.0 : 0.0;
         sc[BAD] = fin ? 0.0 : 1.0;
-        sc[KEEP] = (fin && tot > 0.0 && maxit > 0) ? 1.0 : 0.0;
+        const bool keep = fin && tot > 0.0 && args->maxit > 0;
+        sc[KEEP] = keep ? 1.0 : 0.0;
+        if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
     }
 }
 
@@ -401,7 +411,8 @@ __global__ void k_m3_mv(Dev3 D, double* __restrict__ part, unsigned int* counter
 }
 
 // x += alpha ph + omega sh; r = s - omega t; stopping rule and next beta
-__global__ void k_m3_upd(Dev3 D, int maxit, double tol, double* __restrict__ part, unsigned int* counter) {
+__global__ void k_m3_upd(Dev3 D, const Args3* __restrict__ args, double* __restrict__ part, unsigned int* counter,
+                         cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ double red[32];
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y;
@@ -428,7 +439,7 @@ __global__ void k_m3_upd(Dev3 D, int maxit, double tol, double* __restrict__ par
         const cd rho_old = sc_c(sc, RHO), rho(tot[1], tot[2]);
         const cd alpha = sc_c(sc, ALPHA), omega = sc_c(sc, OMEGA);
         bool bad = sc[BAD] != 0.0 || !fin;
-        const bool conv = fin && rel < tol;
+        const bool conv = fin && rel < args->tol;
         if (!conv && (abs2(rho_old) == 0.0 || abs2(omega) == 0.0)) bad = true;
         const cd beta = bad ? cd(0.0) : cdiv(rho, rho_old) * cdiv(alpha, omega);
         sc_set(sc, RHO_OLD, rho_old);
@@ -439,7 +450,20 @@ __global__ void k_m3_upd(Dev3 D, int maxit, double tol, double* __restrict__ par
         sc[ITER] = (double)it;
         sc[CONV] = conv ? 1.0 : 0.0;
         sc[BAD] = bad ? 1.0 : 0.0;
-        sc[KEEP] = (!conv && !bad && it < maxit) ? 1.0 : 0.0;
+        const bool keep = !conv && !bad && it < args->maxit;
+        sc[KEEP] = keep ? 1.0 : 0.0;
+        if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
+    }
+}
+
+// the solution (three planes, zero off the unknowns) into the caller's planes
+__global__ void k_m3_store(Dev3 D, const Args3* __restrict__ args) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= D.ld) return;
+    for (int c = 0; c < 3; c++) {
+        const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+        args->out[q] = D.x[q];
     }
 }
 
@@ -485,8 +509,18 @@ struct cth_mw3 {
     unsigned int* counter = nullptr;
     bool assembled = false;
     long long launches = 0;
-    cudaStream_t side[2] = {nullptr, nullptr};  // the Er and Ephi V-cycles run beside the Ex one
-    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    // the Er and Ephi kernels run beside the Ex ones: set 0 for the set-up, set 1
+    // for the iteration (a stream that joined a capture stays in it until the
+    // capture ends, so the loop body's own capture needs its own side streams)
+    cudaStream_t side[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaEvent_t fork[2] = {nullptr, nullptr}, join[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaStream_t cap[2] = {nullptr, nullptr};   // capture streams of the solve graph
+    Args3* d_args = nullptr;
+    Args3* h_args = nullptr;                    // pinned
+    bool use_graphs = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int n_pre = 0, n_body = 0, n_post = 0;      // kernels per section of the graph
 };
 
 namespace {
@@ -528,12 +562,145 @@ void destroy(cth_mw3* m) {
                     (void*)m->counter})
         if (p) cudaFree(p);
     if (m->h_sc) cudaFreeHost(m->h_sc);
-    for (int k = 0; k < 2; k++) {
-        if (m->side[k]) cudaStreamDestroy(m->side[k]);
-        if (m->join[k]) cudaEventDestroy(m->join[k]);
+    for (int u = 0; u < 2; u++) {
+        for (int k = 0; k < 2; k++) {
+            if (m->side[u][k]) cudaStreamDestroy(m->side[u][k]);
+            if (m->join[u][k]) cudaEventDestroy(m->join[u][k]);
+        }
+        if (m->fork[u]) cudaEventDestroy(m->fork[u]);
     }
-    if (m->fork) cudaEventDestroy(m->fork);
+    for (int k = 0; k < 2; k++)
+        if (m->cap[k]) cudaStreamDestroy(m->cap[k]);
+    if (m->exec) cudaGraphExecDestroy(m->exec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    if (m->d_args) cudaFree(m->d_args);
+    if (m->h_args) cudaFreeHost(m->h_args);
     delete m;
+}
+
+// the three fields' kernels side by side: field 0 on s, fields 1 and 2 on the side
+// streams (inside a capture the side streams join it through the fork event)
+cudaError_t fork3(cth_mw3* m, int u, cudaStream_t s) {
+    cudaError_t e = cudaEventRecord(m->fork[u], s);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) e = cudaStreamWaitEvent(m->side[u][k], m->fork[u], 0);
+    return e;
+}
+
+cudaError_t join3(cth_mw3* m, int u, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+        e = cudaEventRecord(m->join[u][k], m->side[u][k]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, m->join[u][k], 0);
+    }
+    return e;
+}
+
+// preconditioner hierarchies from the fields' own 5-point blocks, then the
+// recurrence's start
+cudaError_t solve_pre(cth_mw3* m, cudaStream_t s, cudaGraphConditionalHandle cond, int use_cond, int* n) {
+    Dev3 D = dev3(m);
+    cudaError_t e = fork3(m, 0, s);
+    if (e != cudaSuccess) return e;
+    for (int c = 0; c < 3; c++) {
+        cth_grid* g = m->g[c];
+        cudaStream_t sc = c == 0 ? s : m->side[0][c - 1];
+        dim3 gb(256), gg((g->ncol + 255) / 256, g->nrow[0]);
+        k_m3_block<<<gg, gb, 0, sc>>>(D, c, g->hc.a[0], g->i0, g->j0, g->ncol, g->nrow[0], g->ldl);
+        *n += 1 + cmg_setup(g, sc);
+    }
+    e = join3(m, 0, s);
+    if (e != cudaSuccess) return e;
+    dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
+    k_m3_prep<<<grd, blk, 0, s>>>(D, m->d_args, m->part, m->counter, cond, use_cond);
+    *n += 1;
+    return cudaGetLastError();
+}
+
+// one BiCGStab iteration; the three fields' V-cycles of each preconditioner
+// application run side by side
+cudaError_t solve_body(cth_mw3* m, cudaStream_t s, cudaGraphConditionalHandle cond, int use_cond, int* n) {
+    Dev3 D = dev3(m);
+    Lev0 L = lev0(m);
+    dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
+    auto precond = [&]() -> cudaError_t {
+        cudaError_t e = fork3(m, 1, s);
+        if (e != cudaSuccess) return e;
+        *n += cmg_vcycle(m->g[0], s);
+        for (int k = 0; k < 2; k++) *n += cmg_vcycle(m->g[1 + k], m->side[1][k]);
+        return join3(m, 1, s);
+    };
+    k_m3_vec<0><<<grd, blk, 0, s>>>(D, L);
+    cudaError_t e = precond();
+    if (e != cudaSuccess) return e;
+    k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.ph);
+    k_m3_mv<0><<<grd, blk, 0, s>>>(D, m->part, m->counter);
+    k_m3_vec<1><<<grd, blk, 0, s>>>(D, L);
+    e = precond();
+    if (e != cudaSuccess) return e;
+    k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.sh);
+    k_m3_mv<1><<<grd, blk, 0, s>>>(D, m->part, m->counter);
+    k_m3_upd<<<grd, blk, 0, s>>>(D, m->d_args, m->part, m->counter, cond, use_cond);
+    *n += 7;
+    return cudaGetLastError();
+}
+
+int solve_post(cth_mw3* m, cudaStream_t s) {
+    dim3 blk(128), grd((m->ld + 127) / 128, m->nj + 2);
+    k_m3_store<<<grd, blk, 0, s>>>(dev3(m), m->d_args);
+    return 1;
+}
+
+// the whole solve as one graph: set-up, a conditional WHILE node around the
+// iteration (its condition set by the reduction kernels), the store
+int build_graph(cth_mw3* m) {
+    if (m->exec) return CTH_OK;
+    cudaStream_t cs = m->cap[0], cs2 = m->cap[1];
+    CTH_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps);
+    cudaGraphConditionalHandle cond = 0;
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault);
+    int n_pre = 0, n_body = 0;
+    if (e == cudaSuccess) e = solve_pre(m, cs, cond, 1, &n_pre);
+    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps);
+    cudaGraphNode_t cnode = nullptr;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, deps, ndeps, &cp);
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+        e = cudaStreamBeginCaptureToGraph(cs2, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            e = solve_body(m, cs2, cond, 1, &n_body);
+            cudaGraph_t bout = nullptr;
+            const cudaError_t e2 = cudaStreamEndCapture(cs2, &bout);
+            if (e == cudaSuccess) e = e2;
+        }
+    }
+    int n_post = 0;
+    if (e == cudaSuccess) n_post = solve_post(m, cs);
+    cudaGraph_t out = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(cs, &out);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&m->exec, out, 0);
+    if (e != cudaSuccess) {
+        if (out) cudaGraphDestroy(out);
+        m->exec = nullptr;
+        cudaGetLastError();
+        return cuda_fail(e, "magnetised microwave solve graph capture");
+    }
+    m->graph = out;
+    m->n_pre = n_pre;
+    m->n_body = n_body;
+    m->n_post = n_post;
+    return CTH_OK;
 }
 
 }  // namespace
@@ -582,11 +749,16 @@ int cth_mw3_create(int ni, int nj, int device, cth_mw3** out) {
     if (e == cudaSuccess) e = cudaMemset(m->vec, 0, (size_t)27 * pl * sizeof(cd));
     if (e == cudaSuccess) e = cudaMemset(m->sc, 0, NWORDS * sizeof(double));
     if (e == cudaSuccess) e = cudaMemset(m->counter, 0, sizeof(unsigned int));
-    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
-        e = cudaStreamCreateWithFlags(&m->side[k], cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->join[k], cudaEventDisableTiming);
+    for (int u = 0; u < 2; u++) {
+        for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+            e = cudaStreamCreateWithFlags(&m->side[u][k], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->join[u][k], cudaEventDisableTiming);
+        }
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->fork[u], cudaEventDisableTiming);
     }
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->fork, cudaEventDisableTiming);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) e = cudaStreamCreateWithFlags(&m->cap[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_args, sizeof(Args3));
+    if (e == cudaSuccess) e = cudaMallocHost(&m->h_args, sizeof(Args3));
     if (e != cudaSuccess) {
         destroy(m);
         return cuda_fail(e, "cth_mw3_create");
@@ -652,6 +824,15 @@ int cth_mw3_apply_dev(cth_mw3* m, const double* x3, double* y3, void* stream) {
     return CTH_OK;
 }
 
+int cth_mw3_set_graphs(cth_mw3* m, int enable) {
+    if (!m) {
+        set_error("cth_mw3_set_graphs: null handle");
+        return CTH_ERR_ARG;
+    }
+    m->use_graphs = enable != 0;
+    return CTH_OK;
+}
+
 int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* stream, cth_status* st) {
     if (!m || !E3 || maxit < 0 || !(tol > 0.0) || !m->assembled) {
         set_error("cth_mw3_solve_dev: invalid arguments or system not assembled");
@@ -659,60 +840,33 @@ int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* strea
     }
     CTH_CUDA(cudaSetDevice(m->device));
     cudaStream_t s = (cudaStream_t)stream;
-    Dev3 D = dev3(m);
-    Lev0 L = lev0(m);
-    dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
-    // preconditioner hierarchies from the fields' own 5-point blocks, the three
-    // set-ups side by side
-    CTH_CUDA(cudaEventRecord(m->fork, s));
-    for (int k = 0; k < 2; k++) CTH_CUDA(cudaStreamWaitEvent(m->side[k], m->fork, 0));
-    for (int c = 0; c < 3; c++) {
-        cth_grid* g = m->g[c];
-        cudaStream_t sc = c == 0 ? s : m->side[c - 1];
-        dim3 gb(256), gg((g->ncol + 255) / 256, g->nrow[0]);
-        k_m3_block<<<gg, gb, 0, sc>>>(D, c, g->hc.a[0], g->i0, g->j0, g->ncol, g->nrow[0], g->ldl);
-        m->launches++;
-        m->launches += cmg_setup(g, sc);
-    }
-    for (int k = 0; k < 2; k++) {
-        CTH_CUDA(cudaEventRecord(m->join[k], m->side[k]));
-        CTH_CUDA(cudaStreamWaitEvent(s, m->join[k], 0));
-    }
-    k_m3_prep<<<grd, blk, 0, s>>>(D, maxit, m->part, m->counter);
-    m->launches++;
-    // the three fields' V-cycles are independent: Ex on the caller's stream, Er
-    // and Ephi on two side streams, joined before the gather
-    auto precond = [&]() -> cudaError_t {
-        cudaError_t err = cudaEventRecord(m->fork, s);
-        for (int k = 0; k < 2 && err == cudaSuccess; k++) err = cudaStreamWaitEvent(m->side[k], m->fork, 0);
-        if (err != cudaSuccess) return err;
-        m->launches += cmg_vcycle(m->g[0], s);
-        for (int k = 0; k < 2; k++) {
-            m->launches += cmg_vcycle(m->g[1 + k], m->side[k]);
-            err = cudaEventRecord(m->join[k], m->side[k]);
-            if (err == cudaSuccess) err = cudaStreamWaitEvent(s, m->join[k], 0);
-            if (err != cudaSuccess) return err;
-        }
-        return cudaSuccess;
-    };
-    for (;;) {
+    m->h_args->maxit = maxit;
+    m->h_args->tol = tol;
+    m->h_args->out = reinterpret_cast<cd*>(E3);
+    CTH_CUDA(cudaMemcpyAsync(m->d_args, m->h_args, sizeof(Args3), cudaMemcpyHostToDevice, s));
+    if (m->use_graphs) {
+        int rc = build_graph(m);
+        if (rc != CTH_OK) return rc;
+        CTH_CUDA(cudaGraphLaunch(m->exec, s));
         CTH_CUDA(cudaMemcpyAsync(m->h_sc, m->sc, NWORDS * sizeof(double), cudaMemcpyDeviceToHost, s));
         CTH_CUDA(cudaStreamSynchronize(s));
-        if (m->h_sc[KEEP] == 0.0) break;
-        k_m3_vec<0><<<grd, blk, 0, s>>>(D, L);
-        CTH_CUDA(precond());
-        k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.ph);
-        k_m3_mv<0><<<grd, blk, 0, s>>>(D, m->part, m->counter);
-        k_m3_vec<1><<<grd, blk, 0, s>>>(D, L);
-        CTH_CUDA(precond());
-        k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.sh);
-        k_m3_mv<1><<<grd, blk, 0, s>>>(D, m->part, m->counter);
-        k_m3_upd<<<grd, blk, 0, s>>>(D, maxit, tol, m->part, m->counter);
-        m->launches += 7;
-        CTH_CUDA(cudaGetLastError());
+        m->launches += m->n_pre + (long long)m->n_body * (long long)m->h_sc[ITER] + m->n_post;
+    } else {
+        int n = 0;
+        CTH_CUDA(solve_pre(m, s, 0, 0, &n));
+        m->launches += n;
+        for (;;) {
+            CTH_CUDA(cudaMemcpyAsync(m->h_sc, m->sc, NWORDS * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CTH_CUDA(cudaStreamSynchronize(s));
+            if (m->h_sc[KEEP] == 0.0) break;
+            n = 0;
+            CTH_CUDA(solve_body(m, s, 0, 0, &n));
+            m->launches += n;
+        }
+        m->launches += solve_post(m, s);
+        CTH_CUDA(cudaStreamSynchronize(s));
     }
-    CTH_CUDA(cudaMemcpyAsync(E3, D.x, (size_t)3 * m->pl * sizeof(cd), cudaMemcpyDeviceToDevice, s));
-    CTH_CUDA(cudaStreamSynchronize(s));
+    CTH_CUDA(cudaGetLastError());
     const double* h = m->h_sc;
     cth_status loc{};
     loc.iterations = (int)h[ITER];

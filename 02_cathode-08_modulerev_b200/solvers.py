@@ -326,6 +326,10 @@ class Microwave3:
     def launch_count(self) -> int:
         return int(self._L.cth_mw3_launch_count(self._h))
 
+    def set_graphs(self, enable: bool):
+        """One captured graph per solve (default) or kernel-by-kernel launches."""
+        capi.check(self._L.cth_mw3_set_graphs(self._h, int(enable)), allow_positive=False)
+
     def _stream(self, stream):
         import torch
         return (stream if stream is not None else torch.cuda.current_stream(self.device)).cuda_stream

@@ -244,6 +244,10 @@ int cth_mw3_apply_dev(cth_mw3* m, const double* x3, double* y3, void* stream);
 /* solve from a zero start until ||b - A E||_2 / ||b||_2 < tol; E3 receives the
  * three fields (zero off the unknowns).  CTH_NOT_CONVERGED after maxit. */
 int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* stream, cth_status* st);
+/* run the solve as one captured CUDA graph with a device-side conditional loop
+ * (default, 1) or kernel by kernel with a host convergence test per iteration
+ * (0); same kernels, same results */
+int cth_mw3_set_graphs(cth_mw3* m, int enable);
 
 /* Fluid state in HBM -----------------------------------------------------------
  * A field store holds named device planes of the grid's library layout (cell

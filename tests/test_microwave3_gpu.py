@@ -121,3 +121,25 @@ def test_mw3_full_size(pkg, cuda_device):
     rel = float(torch.linalg.vector_norm(r) / torch.linalg.vector_norm(b))
     assert rel < 2e-10, rel
     m.close(); g.close()
+
+
+def test_mw3_graph_equals_launches(pkg, cuda_device):
+    """The captured graph with its device-side loop and the kernel-by-kernel
+    path give the same fields bit for bit and the same iteration count."""
+    ni, nj = 96, 40
+    w, p, mw = _case(pkg, ni, nj)
+    g, planes = _device(pkg, w)
+    out = {}
+    for graphs in (True, False):
+        m = pkg.Microwave3(ni, nj)
+        m.set_graphs(graphs)
+        m.assemble_dev(*planes, w["params"])
+        E, st = m.solve_dev(maxITR=200, error_cnv=1e-11)
+        E2, st2 = m.solve_dev(maxITR=200, error_cnv=1e-11)  # second call reuses the graph
+        assert st.converged == 1 and st2.iterations == st.iterations
+        assert np.array_equal(E.cpu().numpy(), E2.cpu().numpy())
+        out[graphs] = (E.cpu().numpy(), st.iterations)
+        m.close()
+    assert out[True][1] == out[False][1]
+    assert np.array_equal(out[True][0], out[False][0])
+    g.close()
