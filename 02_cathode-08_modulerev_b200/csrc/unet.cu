@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(256) k_bias_grad(const bf16* __restrict__ dy, 
 
 // bf16 copies of one convolution's FP32 weights W[co][tap][ci]: W itself, the
 // flipped transpose W'[ci][tap][co] = W[co][8-tap][ci] (input gradients), and
-// both again in the tcgen05 layout [Cin/8][9][Cout][8] (wbt of W, wtt of W')
+// both again in the tcgen05 layout [Cin/32][9][Cout][32] (wbt of W, wtt of W';
+// Cin and Cout multiples of 32)
 __global__ void k_weights(const float* __restrict__ w, int Cout, int Cin, bf16* __restrict__ wb,
                           bf16* __restrict__ wt, bf16* __restrict__ wbt, bf16* __restrict__ wtt) {
     const size_t n = (size_t)Cout * 9 * Cin;
@@ -317,9 +318,9 @@ __global__ void k_weights(const float* __restrict__ w, int Cout, int Cin, bf16* 
         const bf16 v = __float2bfloat16_rn(w[e]);
         wb[e] = v;
         wt[((size_t)ci * 9 + (8 - tap)) * Cout + co] = v;
-        wbt[(((size_t)(ci >> 3) * 9 + tap) * Cout + co) * 8 + (ci & 7)] = v;
+        wbt[(((size_t)(ci >> 5) * 9 + tap) * Cout + co) * 32 + (ci & 31)] = v;
         // W' has Cout' = Cin and Cin' = Cout: element (co' = ci, tap' = 8 - tap, ci' = co)
-        wtt[(((size_t)(co >> 3) * 9 + (8 - tap)) * Cin + ci) * 8 + (co & 7)] = v;
+        wtt[(((size_t)(co >> 5) * 9 + (8 - tap)) * Cin + ci) * 32 + (co & 31)] = v;
     }
 }
 
@@ -654,17 +655,19 @@ constexpr int TC_THREADS = 192;  // producer warp, MMA warp, 4 epilogue warps
 
 template <int N, int R>
 struct TcShape {
-    static constexpr int kAHalf = ((R + 2) * TC_HW * 16 + 127) / 128 * 128;
-    static constexpr int kBHalf = 9 * N * 16;
-    static constexpr int kStage = 2 * kAHalf + 2 * kBHalf;
-    static constexpr int kFit = (200 * 1024) / kStage;
+    // one stage = 32 input channels: the A box (R+2 halo rows x 130 pixels x 64 B)
+    // and the B box (9 taps x N output channels x 64 B), each 1024-byte aligned
+    static constexpr int kA = ((R + 2) * TC_HW * 64 + 1023) / 1024 * 1024;
+    static constexpr int kB = (9 * N * 64 + 1023) / 1024 * 1024;
+    static constexpr int kStage = kA + kB;
+    static constexpr int kFit = (210 * 1024) / kStage;
     static constexpr int kStages = kFit < 2 ? 2 : (kFit > 8 ? 8 : kFit);
     // barriers after the stages: full[S], empty[S], tfull[2], tempty[2], fin; then the TMEM address
     static constexpr int kBar = kStages * kStage;
     static constexpr int kNBar = 2 * kStages + 5;
-    static constexpr int kUsed = kBar + kNBar * 8 + 8;
+    static constexpr int kUsed = kBar + kNBar * 8 + 8 + 1024;  // + alignment slack of the dynamic base
     static constexpr int kSmem = kUsed < 120 * 1024 ? 120 * 1024 : kUsed;  // one CTA per SM
-    static constexpr uint32_t kTx = (uint32_t)(2 * (R + 2) * TC_HW * 16 + 2 * kBHalf);
+    static constexpr uint32_t kTx = (uint32_t)((R + 2) * TC_HW * 64 + 9 * N * 64);
     static constexpr uint32_t kCols = 2 * R * N <= 64 ? 64 : (2 * R * N <= 128 ? 128 : (2 * R * N <= 256 ? 256 : 512));
     static_assert(2 * R * N <= 512, "two accumulator buffers in the 512 TMEM columns");
     static_assert(kUsed <= 227 * 1024, "shared memory per CTA");
@@ -674,15 +677,23 @@ struct TcShape {
 #define CTH_TC_TILES(X) \
     X(128, 2) X(128, 1) X(96, 2) X(96, 1) X(64, 4) X(64, 2) X(64, 1) X(32, 4) X(32, 2) X(32, 1)
 
-// shared-memory matrix descriptor, K-major without swizzle (SM100 format:
-// start >> 4 in [0,14), leading byte offset >> 4 in [16,30), stride byte
-// offset >> 4 in [32,46), version 1 in [46,48), layout type 0 in [61,64))
-__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+#ifndef CTH_TC_BOFF
+#define CTH_TC_BOFF 0
+#endif
+// shared-memory matrix descriptor, K-major with the 64-byte swizzle (rows of 64
+// bytes = 32 bf16 along K, 8-row groups 512 bytes apart, layout type 4 in
+// [61,64)); the start may sit on any 64-byte row: its phase in the 512-byte
+// swizzle pattern goes into the base offset, bits [49,52)
+__device__ __forceinline__ uint64_t tc_desc_sw64(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)1 << 16;              // leading byte offset 16 (unused within the 64-byte row)
+    d |= (uint64_t)(512 >> 4) << 32;     // stride byte offset: next 8-row group
+    d |= (uint64_t)1 << 46;              // version
+#if CTH_TC_BOFF
+    d |= (uint64_t)((saddr >> 7) & 7u) << 49;
+#endif
+    d |= (uint64_t)4 << 61;              // SWIZZLE_64B
     return d;
 }
 
@@ -753,12 +764,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     extern __shared__ __align__(1024) unsigned char tsm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tx = (a.W + TC_M - 1) / TC_M, ty = (a.H + R - 1) / R;
-    const int ntiles = tx * ty * (a.Cout / N), nk = a.Cin / 16;
-    const uint32_t base = smem_u32(tsm);
+    const int ntiles = tx * ty * (a.Cout / N), nk = a.Cin / 32;
+    // the swizzled boxes want 1024-byte aligned stages
+    const uint32_t base = (smem_u32(tsm) + 1023u) & ~1023u;
+    unsigned char* tbase = tsm + (base - smem_u32(tsm));
     const uint32_t bars = base + (uint32_t)T::kBar;
     const uint32_t full0 = bars, empty0 = bars + 8u * S, tfull0 = bars + 16u * S, tempty0 = tfull0 + 16u,
                    fin = tempty0 + 16u;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(tsm + T::kBar + T::kNBar * 8);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(tbase + T::kBar + T::kNBar * 8);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                      "r"(T::kCols));
@@ -791,10 +804,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 const uint32_t st = base + (uint32_t)(s * T::kStage), fb = full0 + 8u * s;
                 tc_expect(fb, T::kTx);
-                tc_load3(st, &tin, fb, 16 * k, x0 - 1, y0 - 1);
-                tc_load3(st + T::kAHalf, &tin, fb, 16 * k + 8, x0 - 1, y0 - 1);
-                tc_load3(st + 2 * T::kAHalf, &tw, fb, 0, co0, 18 * k);
-                tc_load3(st + 2 * T::kAHalf + T::kBHalf, &tw, fb, 0, co0, 18 * k + 9);
+                tc_load3(st, &tin, fb, 32 * k, x0 - 1, y0 - 1);
+                tc_load3(st + T::kA, &tw, fb, 0, co0, 9 * k);
                 issued = it + 1;
             }
         }
@@ -823,9 +834,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
                     for (int tap = 0; tap < 9; tap++) {
                         const int dy = tap / 3, dx = tap % 3;
-                        const uint64_t da = tc_desc(st + (uint32_t)(((r + dy) * TC_HW + dx) * 16), T::kAHalf, 128);
-                        const uint64_t db = tc_desc(st + (uint32_t)(2 * T::kAHalf + tap * N * 16), T::kBHalf, 128);
-                        tc_mma(acc + (uint32_t)(r * N), da, db, idesc, (k > 0 || tap > 0) ? 1u : 0u);
+#pragma unroll
+                        for (int kk = 0; kk < 2; kk++) {
+                            const uint64_t da =
+                                tc_desc_sw64(st + (uint32_t)(((r + dy) * TC_HW + dx) * 64 + kk * 32));
+                            const uint64_t db = tc_desc_sw64(st + (uint32_t)(T::kA + tap * N * 64 + kk * 32));
+                            tc_mma(acc + (uint32_t)(r * N), da, db, idesc, (k > 0 || tap > 0 || kk > 0) ? 1u : 0u);
+                        }
                     }
                 }
                 tc_commit(empty0 + 8u * s);
@@ -1135,15 +1150,15 @@ TmapEncodeFn tmap_encode() {
 }
 
 // 3-D bf16 tensor map: extents d0 (contiguous), d1, d2; byte strides s1, s2 of
-// dimensions 1 and 2; box b0 x b1 x b2; zero fill outside the extents
+// dimensions 1 and 2; box b0 x b1 x b2; zero fill outside the extents; swizzle swz
 bool tmap3(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1, uint64_t s2,
-           uint32_t b0, uint32_t b1, uint32_t b2) {
+           uint32_t b0, uint32_t b1, uint32_t b2, CUtensorMapSwizzle swz) {
     const TmapEncodeFn fn = tmap_encode();
     if (!fn) return false;
     cuuint64_t dims[3] = {d0, d1, d2}, strides[2] = {s1, s2};
     cuuint32_t box[3] = {b0, b1, b2}, es[3] = {1, 1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, es,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -1169,12 +1184,14 @@ TcTile tc_tile(int cout, int H, int W) {
 
 int launch_conv(cth_unet* n, const ConvArgs& a, cudaStream_t s) {
     const TcTile t = n->use_tc ? tc_tile(a.Cout, a.H, a.W) : TcTile{0, 0};
-    if (t.n && a.Cin % 16 == 0 && a.in_cs % 8 == 0 && a.in_coff % 8 == 0) {
+    if (t.n && a.Cin % 32 == 0 && a.Cout % 32 == 0 && a.in_cs % 8 == 0 && a.in_coff % 8 == 0) {
+        // A: 32 channels x 130 pixels x R+2 rows per box; B: the [Cin/32][9][Cout][32]
+        // weights, 32 channels x N x 9 taps per box; both in 64-byte swizzled rows
         CUtensorMap ti, tw;
         if (!tmap3(&ti, a.in + a.in_coff, (uint64_t)a.Cin, (uint64_t)a.W, (uint64_t)a.H, (uint64_t)a.in_cs * 2,
-                   (uint64_t)a.W * a.in_cs * 2, 8, TC_HW, (uint32_t)(t.r + 2)) ||
-            !tmap3(&tw, a.wtc, 8, (uint64_t)a.Cout, (uint64_t)9 * a.Cin / 8, 16, (uint64_t)a.Cout * 16, 8,
-                   (uint32_t)t.n, 9)) {
+                   (uint64_t)a.W * a.in_cs * 2, 32, TC_HW, (uint32_t)(t.r + 2), CU_TENSOR_MAP_SWIZZLE_64B) ||
+            !tmap3(&tw, a.wtc, 32, (uint64_t)a.Cout, (uint64_t)9 * a.Cin / 32, 64, (uint64_t)a.Cout * 64, 32,
+                   (uint32_t)t.n, 9, CU_TENSOR_MAP_SWIZZLE_64B)) {
             set_error("cth_unet: tensor map encoding failed");
             return CTH_ERR_CUDA;
         }
