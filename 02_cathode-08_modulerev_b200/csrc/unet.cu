@@ -677,22 +677,17 @@ struct TcShape {
 #define CTH_TC_TILES(X) \
     X(128, 2) X(128, 1) X(96, 2) X(96, 1) X(64, 4) X(64, 2) X(64, 1) X(32, 4) X(32, 2) X(32, 1)
 
-#ifndef CTH_TC_BOFF
-#define CTH_TC_BOFF 0
-#endif
 // shared-memory matrix descriptor, K-major with the 64-byte swizzle (rows of 64
 // bytes = 32 bf16 along K, 8-row groups 512 bytes apart, layout type 4 in
-// [61,64)); the start may sit on any 64-byte row: its phase in the 512-byte
-// swizzle pattern goes into the base offset, bits [49,52)
+// [61,64)).  TMA and the MMA both apply the swizzle to the absolute
+// shared-memory address of a 1024-byte aligned tile, so a start on any 64-byte
+// row reads the rows TMA wrote there; the base offset (bits [49,52)) stays 0.
 __device__ __forceinline__ uint64_t tc_desc_sw64(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
     d |= (uint64_t)1 << 16;              // leading byte offset 16 (unused within the 64-byte row)
     d |= (uint64_t)(512 >> 4) << 32;     // stride byte offset: next 8-row group
     d |= (uint64_t)1 << 46;              // version
-#if CTH_TC_BOFF
-    d |= (uint64_t)((saddr >> 7) & 7u) << 49;
-#endif
     d |= (uint64_t)4 << 61;              // SWIZZLE_64B
     return d;
 }
