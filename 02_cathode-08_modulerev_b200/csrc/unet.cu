@@ -77,6 +77,8 @@ struct ConvArgs {
     const bf16* gate;    // null: none; else out *= (gate > 0)
     int gate_cs, gate_coff;
     int accumulate;      // add to the existing output
+    int wait_polls;      // tcgen05 path: polls of each mbarrier wait before it gives up
+    int stall;           // tcgen05 path, test of the bounded waits: no loads are issued
 };
 
 // 3x3 convolution, SAME zero padding.  CTA: 8 x 16 output pixels x 32 output
@@ -697,8 +699,8 @@ __host__ __device__ constexpr uint32_t tc_idesc(int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
 }
 
-__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
-    for (int it = 0; it < (1 << 20); it++) {
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, int polls) {
+    for (int it = 0; it < polls; it++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
@@ -786,14 +788,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tslot;
     int fail = 0, issued = 0;
-    if (tid == 0) {
+    if (tid == 0 && !a.stall) {
         // producer: chunk after chunk of every tile through the ring
         int it = 0;
         for (int t = blockIdx.x; t < ntiles && !fail; t += gridDim.x) {
             const int x0 = (t % tx) * TC_M, y0 = ((t / tx) % ty) * R, co0 = (t / (tx * ty)) * N;
             for (int k = 0; k < nk; k++, it++) {
                 const int s = it % S;
-                if (it >= S && !tc_wait(empty0 + 8u * s, (uint32_t)((it / S - 1) & 1))) {
+                if (it >= S && !tc_wait(empty0 + 8u * s, (uint32_t)((it / S - 1) & 1), a.wait_polls)) {
                     fail = 1;
                     break;
                 }
@@ -810,7 +812,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         int it = 0, lt = 0;
         for (int t = blockIdx.x; t < ntiles && !fail; t += gridDim.x, lt++) {
             const int b = lt & 1;
-            if (lt >= 2 && !tc_wait(tempty0 + 8u * b, (uint32_t)((lt / 2 - 1) & 1))) {
+            if (lt >= 2 && !tc_wait(tempty0 + 8u * b, (uint32_t)((lt / 2 - 1) & 1), a.wait_polls)) {
                 fail = 1;
                 break;
             }
@@ -818,7 +820,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const uint32_t acc = tmem + (uint32_t)(b * R * N);
             for (int k = 0; k < nk; k++, it++) {
                 const int s = it % S;
-                if (!tc_wait(full0 + 8u * s, (uint32_t)((it / S) & 1))) {
+                if (!tc_wait(full0 + 8u * s, (uint32_t)((it / S) & 1), a.wait_polls)) {
                     fail = 1;
                     break;
                 }
@@ -852,7 +854,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         int lt = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
             const int b = lt & 1;
-            if (!tc_wait(tfull0 + 8u * b, (uint32_t)((lt / 2) & 1))) {
+            if (!tc_wait(tfull0 + 8u * b, (uint32_t)((lt / 2) & 1), a.wait_polls)) {
                 fail = 1;
                 break;
             }
@@ -915,10 +917,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (tid == 0) {
             atomicExch(err, 1);
             for (int k = issued > S ? issued - S : 0; k < issued; k++)
-                tc_wait(full0 + 8u * (k % S), (uint32_t)((k / S) & 1));
+                tc_wait(full0 + 8u * (k % S), (uint32_t)((k / S) & 1), a.wait_polls);
         }
     }
-    tc_wait(fin, 0u);  // the MMAs are complete before the tensor memory is freed
+    tc_wait(fin, 0u, a.wait_polls);  // the MMAs are complete before the tensor memory is freed
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
@@ -985,6 +987,8 @@ struct cth_unet {
     int smooth_passes = 0;   // 5-point smoothing passes on the predicted change
     long long launches = 0;  // kernels launched by the forward passes and predictions
     bool use_tc = true;      // convolutions on tcgen05 (false: warp-level mma.sync kernel)
+    int wait_polls = 1 << 20;  // polls of each mbarrier wait of the tcgen05 kernel
+    int stall = 0;             // test of the bounded waits: the tcgen05 kernel issues no loads
     int* err = nullptr;      // device flag: a bounded wait of a tcgen05 convolution gave up
     struct Pool { TensorRef src; bf16* dst; int C, Ho, Wo; bf16* ddst; };
     struct Up { bf16* src; int C, Hi, Wi; TensorRef dst; bf16* dsrc; TensorRef ddst; };
@@ -1193,10 +1197,13 @@ int launch_conv(cth_unet* n, const ConvArgs& a, cudaStream_t s) {
         // persistent: at most one CTA per SM, each walking its share of the tiles
         const long tiles = (long)((a.W + TC_M - 1) / TC_M) * ((a.H + t.r - 1) / t.r) * (a.Cout / t.n);
         const unsigned grd = (unsigned)std::min<long>(tiles, n->sms);
-#define CTH_TC_LAUNCH(NN, RR)                                                                   \
-    if (t.n == NN && t.r == RR) {                                                               \
-        k_conv3_tc<NN, RR><<<grd, TC_THREADS, TcShape<NN, RR>::kSmem, s>>>(ti, tw, a, n->err);  \
-        return CTH_OK;                                                                          \
+        ConvArgs ta = a;
+        ta.wait_polls = n->wait_polls;
+        ta.stall = n->stall;
+#define CTH_TC_LAUNCH(NN, RR)                                                                    \
+    if (t.n == NN && t.r == RR) {                                                                \
+        k_conv3_tc<NN, RR><<<grd, TC_THREADS, TcShape<NN, RR>::kSmem, s>>>(ti, tw, ta, n->err);  \
+        return CTH_OK;                                                                           \
     }
         CTH_TC_TILES(CTH_TC_LAUNCH)
 #undef CTH_TC_LAUNCH
@@ -1377,9 +1384,21 @@ int cth_unet_check(cth_unet* n) {
     int e = 0;
     CTH_CUDA(cudaMemcpy(&e, n->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
-        set_error("cth_unet: a tensor-core convolution gave up waiting for its MMAs");
+        // reported once: the flag is cleared for the following calls
+        CTH_CUDA(cudaMemset(n->err, 0, sizeof(int)));
+        set_error("cth_unet: a tensor-core convolution gave up waiting (its output is not valid)");
         return CTH_ERR_CUDA;
     }
+    return CTH_OK;
+}
+
+int cth_unet_set_wait_test(cth_unet* n, int stall, int polls) {
+    if (!n || polls < 1) {
+        set_error("cth_unet_set_wait_test: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    n->stall = stall != 0;
+    n->wait_polls = polls;
     return CTH_OK;
 }
 

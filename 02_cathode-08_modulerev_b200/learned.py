@@ -110,6 +110,11 @@ class UNet:
         """Kernels launched by forward passes and predictions since creation."""
         return int(self._L.cth_unet_launch_count(self.handle))
 
+    def set_wait_test(self, stall: bool, polls: int = 1 << 20):
+        """Test of the tensor-core kernel's bounded waits: with stall the kernel
+        issues no loads, every wait runs out and check() reports it."""
+        capi.check(self._L.cth_unet_set_wait_test(self.handle, int(stall), int(polls)), allow_positive=False)
+
     def set_smoothing(self, passes: int):
         """5-point smoothing passes applied to the predicted change before it
         becomes the potential solve's guess (default 0)."""

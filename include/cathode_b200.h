@@ -614,9 +614,14 @@ int cth_unet_set_tensor_cores(cth_unet* n, int tcgen05);
  * edge-replicating neighbours, applied to the predicted change of the first
  * potential correction before cth_unet_predict_dphi forms the guess */
 int cth_unet_set_smoothing(cth_unet* n, int passes);
-/* synchronises; CTH_ERR_CUDA if a tensor-core convolution's bounded wait for
- * its MMAs gave up (the output of that call is then not valid) */
+/* synchronises; CTH_ERR_CUDA if a tensor-core convolution's bounded wait gave
+ * up since the last check (the output of that call is then not valid) */
 int cth_unet_check(cth_unet* n);
+/* test of the bounded waits of the tcgen05 convolutions: with stall != 0 the
+ * kernel issues no loads, so every wait runs out after `polls` polls (default
+ * 2^20), the kernel sets the flag that cth_unet_check reports (once) and frees
+ * its tensor memory; nothing is in flight.  stall = 0 restores normal work. */
+int cth_unet_set_wait_test(cth_unet* n, int stall, int polls);
 int cth_unet_set_params(cth_unet* n, const float* host, long long count);  /* resets Adam */
 int cth_unet_get_params(const cth_unet* n, float* host, long long count);
 int cth_unet_get_grads(const cth_unet* n, float* host, long long count);

@@ -152,3 +152,29 @@ def test_tensor_core_paths_agree(pkg, cuda_device, shape):
     print(shape, "output", _rel(res[True][0], res[False][0]), "gradients", _rel(g1, g0), "cosine", cos)
     assert _rel(res[True][0], res[False][0]) < 1e-2, _rel(res[True][0], res[False][0])
     assert _rel(g1, g0) < 0.2 and cos > 0.97, (_rel(g1, g0), cos)
+
+
+def test_bounded_waits_report_and_recover(pkg, cuda_device):
+    """The tcgen05 kernel's mbarrier waits are bounded: with the loads withheld
+    (nothing in flight) every wait runs out, the kernel frees its tensor memory
+    and returns, check() reports the failure once, and the next forward pass on
+    the same network is correct again."""
+    import torch
+    from oracle import unet
+    H, W = 16, 40
+    rng = np.random.default_rng(3)
+    vec = unet.init_params(seed=4)
+    vec[-(3 * 32 + 3):] = rng.normal(0.0, 0.2, size=3 * 32 + 3)
+    x = rng.normal(size=(H, W, 6)).astype(np.float32)
+    net = pkg.learned.UNet(H, W, params=vec)
+    net.set_wait_test(True, polls=2048)
+    net.forward(torch.from_numpy(x).cuda())
+    with pytest.raises(RuntimeError, match="gave up waiting"):
+        net.check()
+    net.check()  # reported once
+    net.set_wait_test(False)
+    out = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    net.check()
+    ref, _ = unet.forward(vec, x, bf16=True)
+    assert _rel(out, ref) < 2e-2
+    net.close()
