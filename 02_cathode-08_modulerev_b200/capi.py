@@ -39,7 +39,7 @@ EXPORTS = (
     "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
     "cth_batch_steps", "cth_update_energy_profile", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
-    "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_tensor_cores", "cth_unet_set_smoothing", "cth_unet_set_wait_test", "cth_unet_check", "cth_unet_set_params", "cth_unet_get_params",
+    "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_tensor_cores", "cth_unet_set_smoothing", "cth_unet_set_wait_test", "cth_unet_set_grid_limit", "cth_unet_check", "cth_unet_set_params", "cth_unet_get_params",
     "cth_unet_get_grads", "cth_unet_set_loss_weights", "cth_unet_forward", "cth_unet_backward",
     "cth_unet_train_step", "cth_unet_set_stats", "cth_unet_features", "cth_unet_predict_dphi",
 )
@@ -316,6 +316,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_unet_set_smoothing.restype = ctypes.c_int
     L.cth_unet_set_wait_test.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
     L.cth_unet_set_wait_test.restype = ctypes.c_int
+    L.cth_unet_set_grid_limit.argtypes = [_vp, ctypes.c_int]
+    L.cth_unet_set_grid_limit.restype = ctypes.c_int
     L.cth_unet_check.argtypes = [_vp]
     L.cth_unet_check.restype = ctypes.c_int
     L.cth_unet_launch_count.argtypes = [_vp]

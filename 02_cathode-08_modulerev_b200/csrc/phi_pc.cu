@@ -339,7 +339,7 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
     if (prm->warm_start != 0 && prm->flag_iter_phi != 0) {
         dphi_prev = field_ptr(fs, "dphi_prev");
         dphi_prev2 = field_ptr(fs, "dphi_prev2");
-        guess = (prm->warm_start == 1) ? field_ptr(fs, "dphi_guess") : dphi_prev;
+        guess = (prm->warm_start == 1 || prm->warm_start == 3) ? field_ptr(fs, "dphi_guess") : dphi_prev;
         if (!dphi_prev || !dphi_prev2 || !guess) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
     }
     cth_status st_first{};
@@ -410,7 +410,7 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
 
 extern "C" int cth_solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, void* stream, cth_pc_result* res) {
     if (!fs || !prm || prm->dx <= 0.0 || prm->dr <= 0.0 || prm->maxITR_HES_phi < 1 || prm->flag_error < 0 ||
-        prm->flag_error > 3 || prm->warm_start < 0 || prm->warm_start > 2 ||
+        prm->flag_error > 3 || prm->warm_start < 0 || prm->warm_start > 3 ||
         (prm->warm_start != 0 && !(prm->guess_max_relres >= 0.0 && prm->guess_max_relres <= 10.0))) {
         cth::set_error("cth_solve_phi_pc: invalid arguments");
         return CTH_ERR_ARG;

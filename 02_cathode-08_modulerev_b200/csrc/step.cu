@@ -40,10 +40,10 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     // only every kNetProbe steps (the other steps start from the previous
     // correction), so it costs nothing while it does not help
     constexpr int kNetPatience = 4, kNetProbe = 8;
-    const bool learned = p->net && p->phi.warm_start == 1 &&
-                         (fs->net_misses < kNetPatience || p->itime % kNetProbe == 0);
+    const bool wants_net = p->phi.warm_start == 1 || p->phi.warm_start == 3;
+    const bool learned = p->net && wants_net && (fs->net_misses < kNetPatience || p->itime % kNetProbe == 0);
     cth_phi_params phi = p->phi;
-    if (p->phi.warm_start == 1 && !learned) phi.warm_start = 2;
+    if (wants_net && !learned) phi.warm_start = 2;
     cudaStream_t s = (cudaStream_t)stream;
     if (learned) {
         if (!fs->net_stream) {

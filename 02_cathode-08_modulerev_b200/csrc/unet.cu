@@ -960,6 +960,7 @@ struct Conv {
 struct cth_unet {
     int device = 0;
     int sms = 148;  // multiprocessors of the device (persistent grids)
+    int max_ctas = 0;  // cap of the persistent convolution grid (0: one CTA per SM)
     int H = 0, W = 0, cin = 0, cout = 0, base = 0;
     int cpad = 32;
     std::vector<Conv> convs;
@@ -1196,7 +1197,8 @@ int launch_conv(cth_unet* n, const ConvArgs& a, cudaStream_t s) {
         }
         // persistent: at most one CTA per SM, each walking its share of the tiles
         const long tiles = (long)((a.W + TC_M - 1) / TC_M) * ((a.H + t.r - 1) / t.r) * (a.Cout / t.n);
-        const unsigned grd = (unsigned)std::min<long>(tiles, n->sms);
+        const long cap = n->max_ctas > 0 ? std::min(n->max_ctas, n->sms) : n->sms;
+        const unsigned grd = (unsigned)std::min<long>(tiles, cap);
         ConvArgs ta = a;
         ta.wait_polls = n->wait_polls;
         ta.stall = n->stall;
@@ -1389,6 +1391,15 @@ int cth_unet_check(cth_unet* n) {
         set_error("cth_unet: a tensor-core convolution gave up waiting (its output is not valid)");
         return CTH_ERR_CUDA;
     }
+    return CTH_OK;
+}
+
+int cth_unet_set_grid_limit(cth_unet* n, int ctas) {
+    if (!n || ctas < 0) {
+        set_error("cth_unet_set_grid_limit: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    n->max_ctas = ctas;
     return CTH_OK;
 }
 

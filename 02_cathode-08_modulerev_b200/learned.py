@@ -110,6 +110,10 @@ class UNet:
         """Kernels launched by forward passes and predictions since creation."""
         return int(self._L.cth_unet_launch_count(self.handle))
 
+    def set_grid_limit(self, ctas: int):
+        """At most ctas CTAs for the persistent tensor-core convolutions (0: all SMs)."""
+        capi.check(self._L.cth_unet_set_grid_limit(self.handle, int(ctas)), allow_positive=False)
+
     def set_wait_test(self, stall: bool, polls: int = 1 << 20):
         """Test of the tensor-core kernel's bounded waits: with stall the kernel
         issues no loads, every wait runs out and check() reports it."""
@@ -318,7 +322,7 @@ def run_steps(pkg, c, nsteps, warm_start, net=None, precision=1):
     for blk in ("ion", "rhoe", "eps", "neutral"):
         P[blk]["precision"] = precision
     P["phi"].update(precision=precision, warm_start=warm_start, guess_max_relres=1.0)
-    P["net"] = net if warm_start == 1 else None
+    P["net"] = net if warm_start in (1, 3) else None
     rec = []
     s = torch.cuda.current_stream()
     for _ in range(nsteps):

@@ -64,7 +64,7 @@ MAXIT = 30
 
 
 NDIV_MW = 100
-LEARN_SEEDS, LEARN_STEPS, LEARN_EPOCHS = 3, 110, 8  # snapshots: seeds x (steps - 2), the timed range
+LEARN_SEEDS, LEARN_STEPS, LEARN_EPOCHS = 3, 110, 24  # snapshots: seeds x (steps - 2), the timed range
 BATCH_N, BATCH_STEPS = 64, 10                       # batched sweep: instances, timed steps each
 PROGNOSTIC = ("rhoe", "rhoi", "rhoeps", "Te", "rhon", "rhom", "phi", "Ex", "Er", "Uix", "Uir", "Uip")
 STATE = ("rhoe", "rhoi", "rhon", "rhom", "Te", "Bx", "Br", "rhoeps", "rhoe_old")
@@ -436,7 +436,7 @@ def main():
             P[blk]["precision"] = prec
         P["phi"]["precision"] = prec
         P["phi"].update(warm_start=warm_start, guess_max_relres=1.0)
-        P["net"] = net if warm_start == 1 else None
+        P["net"] = net if warm_start in (1, 3) else None
         # the warm-start modes also start the field-valued solves (ion velocities and
         # density, neutrals) from the previous step's fields
         fs.set_warm_start(warm_start != 0)

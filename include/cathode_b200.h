@@ -325,7 +325,8 @@ typedef struct cth_phi_params {
      * reference, whose solves start from zero.  0: zero (reference);
      * 1: the better (smaller residual) of the store's plane "dphi_guess"
      * (written by the caller, e.g. the learned predictor) and "dphi_prev";
-     * 2: "dphi_prev" = the first-iteration correction of the previous call.
+     * 2: "dphi_prev" = the first-iteration correction of the previous call;
+     * 3: "dphi_guess" alone (judged only against the zero start).
      * With warm_start != 0 the first iteration's correction is copied into
      * "dphi_prev" (its former content into "dphi_prev2").  A guess whose
      * relative residual exceeds guess_max_relres
@@ -622,6 +623,10 @@ int cth_unet_check(cth_unet* n);
  * 2^20), the kernel sets the flag that cth_unet_check reports (once) and frees
  * its tensor memory; nothing is in flight.  stall = 0 restores normal work. */
 int cth_unet_set_wait_test(cth_unet* n, int stall, int polls);
+/* at most `ctas` CTAs (one per SM) for the persistent tcgen05 convolutions
+ * (0, default: every SM), leaving the other SMs to work that runs beside the
+ * network, e.g. the ion step beside the warm-start prediction */
+int cth_unet_set_grid_limit(cth_unet* n, int ctas);
 int cth_unet_set_params(cth_unet* n, const float* host, long long count);  /* resets Adam */
 int cth_unet_get_params(const cth_unet* n, float* host, long long count);
 int cth_unet_get_grads(const cth_unet* n, float* host, long long count);
