@@ -98,7 +98,7 @@ def test_learned_warm_start_of_the_potential(pkg, cuda_device):
     losses = L.train(net, Xn, Yn, mask, epochs=10, lr=5e-4)
     assert losses[-1] < losses[0]
     recs = {}
-    for ws in (0, 2, 1):
+    for ws in (0, 2, 1, 3):
         c = L.make_case(pkg, ni, nj, seed=99, V_bias=25.0)
         L.run_steps(pkg, c, 3, warm_start=2)  # same history for every variant
         recs[ws] = L.run_steps(pkg, c, 6, warm_start=ws, net=net)
@@ -115,6 +115,11 @@ def test_learned_warm_start_of_the_potential(pkg, cuda_device):
           "guess residual prev/learned:", np.mean(prev), np.mean(res))
     # the device takes the better of the network's guess and the previous step's
     assert np.mean(res) < 1.0 and np.mean(res) <= np.mean(prev) * (1.0 + 1e-9)
+    # the network's guess alone (mode 3): taken whenever its residual is below
+    # the threshold, same stopping rule, no more cycles than from zero
+    alone = recs[3]
+    assert all(r["net_ran"] == 1 and r["guess"] in (1, -1) for r in alone)
+    assert np.mean([r["cycles"] for r in alone]) <= np.mean([r["cycles"] for r in recs[0]])
     net.close()
 
 
