@@ -1168,13 +1168,13 @@ bool tmap3(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t 
 struct TcTile {
     int n, r;
 };
-TcTile tc_tile(int cout, int H, int W) {
+TcTile tc_tile(int cout, int H, int W, int sms) {
     const int cols = (W + TC_M - 1) / TC_M;
     for (int N : {128, 96, 64, 32}) {
         if (cout % N) continue;
         for (int R : {4, 2, 1}) {
             if (R * N > 256) continue;
-            if ((long)cols * ((H + R - 1) / R) * (cout / N) >= 2 * 148) return {N, R};
+            if ((long)cols * ((H + R - 1) / R) * (cout / N) >= 2L * sms) return {N, R};
         }
     }
     for (int N : {128, 96, 64, 32})
@@ -1183,7 +1183,7 @@ TcTile tc_tile(int cout, int H, int W) {
 }
 
 int launch_conv(cth_unet* n, const ConvArgs& a, cudaStream_t s) {
-    const TcTile t = n->use_tc ? tc_tile(a.Cout, a.H, a.W) : TcTile{0, 0};
+    const TcTile t = n->use_tc ? tc_tile(a.Cout, a.H, a.W, n->sms) : TcTile{0, 0};
     if (t.n && a.Cin % 32 == 0 && a.Cout % 32 == 0 && a.in_cs % 8 == 0 && a.in_coff % 8 == 0) {
         // A: 32 channels x 130 pixels x R+2 rows per box; B: the [Cin/32][9][Cout][32]
         // weights, 32 channels x N x 9 taps per box; both in 64-byte swizzled rows
@@ -1238,7 +1238,7 @@ int conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
     w.dw = n->grad + c.w_off;
     const int npatch = ((c.W + TW - 1) / TW) * ((c.H + TH - 1) / TH);
     const int tiles = (c.cout / 32) * (c.cin / 32);
-    int ppc = (int)std::ceil((double)npatch * tiles / (148.0 * 4.0));
+    int ppc = (int)std::ceil((double)npatch * tiles / (n->sms * 4.0));
     ppc = std::max(1, std::min(ppc, npatch));
     w.patches_per_cta = ppc;
     dim3 gw((npatch + ppc - 1) / ppc, c.cout / 32, c.cin / 32);
@@ -1246,7 +1246,7 @@ int conv_bwd(cth_unet* n, const Conv& c, cudaStream_t s) {
     const int npix = c.H * c.W;
     {
         const int lanes = 256 / (c.cout / 8);
-        const int nb = std::max(1, std::min(2 * 148, (npix + lanes - 1) / lanes));
+        const int nb = std::max(1, std::min(2 * n->sms, (npix + lanes - 1) / lanes));
         k_bias_grad<<<nb, 256, 0, s>>>(c.dout.p, c.dout.cs, c.dout.coff, c.cout, npix, n->grad + c.b_off);
     }
     if (!c.din.p) return CTH_OK;
@@ -1294,7 +1294,7 @@ int forward(cth_unet* n, const float* in, cudaStream_t s) {
 int backward(cth_unet* n, const float* dout, cudaStream_t s) {
     const size_t npx = (size_t)n->H * n->W;
     const int B = n->base;
-    const unsigned nhb = std::max<unsigned>(1, std::min<unsigned>(4 * 148, (unsigned)((npx + 127) / 128)));
+    const unsigned nhb = std::max<unsigned>(1, std::min<unsigned>(4u * n->sms, (unsigned)((npx + 127) / 128)));
     k_head_bwd<<<nhb, 128, 0, s>>>(n->y_last, B, (int)npx, n->prm + n->head_w, n->cout,
                                                             dout, n->dy_last, n->grad + n->head_w,
                                                             n->grad + n->head_b);
