@@ -291,6 +291,9 @@ void cth_fields_destroy(cth_fields* fs) {
     if (fs->flags) cudaFree(fs->flags);
     if (fs->ghost_rules) cudaFree(fs->ghost_rules);
     if (fs->net_stream) cudaStreamDestroy(fs->net_stream);
+    if (fs->ion_stream) cudaStreamDestroy(fs->ion_stream);
+    for (int k = 0; k < 2; k++)
+        if (fs->ion_event[k]) cudaEventDestroy(fs->ion_event[k]);
     for (int k = 0; k < 2; k++)
         if (fs->net_event[k]) cudaEventDestroy(fs->net_event[k]);
     if (fs->aux_ready) {

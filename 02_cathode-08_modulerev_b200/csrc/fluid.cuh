@@ -25,6 +25,8 @@ struct cth_fields {
     int ion_box_total[4] = {};
     bool aux_ready = false;
     cudaStream_t net_stream = nullptr;   // learned warm-start inference, concurrent with the ion step
+    cudaStream_t ion_stream = nullptr;   // the ion step beside an inference, at the highest priority
+    cudaEvent_t ion_event[2] = {nullptr, nullptr};
     cudaEvent_t net_event[2] = {nullptr, nullptr};
     double* stage_many = nullptr;        // staging of the batched transfers, stage_planes [i][j] planes
     int stage_planes = 0;

@@ -488,7 +488,12 @@ static int ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_pa
         }
     } else {
         if (!fs->aux_ready) {
-            for (int k = 0; k < 2; k++) CTH_CUDA(cudaStreamCreateWithFlags(&fs->aux_stream[k], cudaStreamNonBlocking));
+            // highest priority: when a prediction runs beside the ion step, the
+            // latency-bound solve chain is scheduled first
+            int lo = 0, hi = 0;
+            CTH_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            for (int k = 0; k < 2; k++)
+                CTH_CUDA(cudaStreamCreateWithPriority(&fs->aux_stream[k], cudaStreamNonBlocking, hi));
             for (int k = 0; k < 3; k++) CTH_CUDA(cudaEventCreateWithFlags(&fs->aux_event[k], cudaEventDisableTiming));
             fs->aux_ready = true;
         }

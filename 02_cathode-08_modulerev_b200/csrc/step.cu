@@ -47,8 +47,15 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     cudaStream_t s = (cudaStream_t)stream;
     if (learned) {
         if (!fs->net_stream) {
-            CTH_CUDA(cudaStreamCreateWithFlags(&fs->net_stream, cudaStreamNonBlocking));
-            for (int k = 0; k < 2; k++) CTH_CUDA(cudaEventCreateWithFlags(&fs->net_event[k], cudaEventDisableTiming));
+            // the prediction at the lowest priority, the ion step beside it at the highest
+            int lo = 0, hi = 0;
+            CTH_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            CTH_CUDA(cudaStreamCreateWithPriority(&fs->net_stream, cudaStreamNonBlocking, lo));
+            CTH_CUDA(cudaStreamCreateWithPriority(&fs->ion_stream, cudaStreamNonBlocking, hi));
+            for (int k = 0; k < 2; k++) {
+                CTH_CUDA(cudaEventCreateWithFlags(&fs->net_event[k], cudaEventDisableTiming));
+                CTH_CUDA(cudaEventCreateWithFlags(&fs->ion_event[k], cudaEventDisableTiming));
+            }
         }
         CTH_CUDA(cudaEventRecord(fs->net_event[0], s));
         CTH_CUDA(cudaStreamWaitEvent(fs->net_stream, fs->net_event[0], 0));
@@ -57,7 +64,18 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
         CTH_CUDA(cudaEventRecord(fs->net_event[1], fs->net_stream));
     }
     if (p->itime % p->ndt_i == 0) {
-        rc = cth_ion_step(fs, gx, gr, &p->ion, stream, &R->ion);
+        // beside a prediction the ion step runs on the high-priority stream
+        void* ion_s = stream;
+        if (learned) {
+            CTH_CUDA(cudaEventRecord(fs->ion_event[0], s));
+            CTH_CUDA(cudaStreamWaitEvent(fs->ion_stream, fs->ion_event[0], 0));
+            ion_s = (void*)fs->ion_stream;
+        }
+        rc = cth_ion_step(fs, gx, gr, &p->ion, ion_s, &R->ion);
+        if (learned) {
+            CTH_CUDA(cudaEventRecord(fs->ion_event[1], fs->ion_stream));
+            CTH_CUDA(cudaStreamWaitEvent(s, fs->ion_event[1], 0));
+        }
         if (rc < 0) return rc;
         R->ran_ion = 1;
         if (R->ion.solver_rc > worst) worst = R->ion.solver_rc;
