@@ -291,6 +291,13 @@ void cth_fields_destroy(cth_fields* fs) {
     if (fs->flags) cudaFree(fs->flags);
     if (fs->ghost_rules) cudaFree(fs->ghost_rules);
     if (fs->net_stream) cudaStreamDestroy(fs->net_stream);
+    if (fs->copy_stream) {
+        cudaStreamSynchronize(fs->copy_stream);
+        cudaStreamDestroy(fs->copy_stream);
+    }
+    if (fs->copy_ready) cudaEventDestroy(fs->copy_ready);
+    if (fs->copy_done) cudaEventDestroy(fs->copy_done);
+    if (fs->plan_stage) cudaFree(fs->plan_stage);
     if (fs->ion_stream) cudaStreamDestroy(fs->ion_stream);
     for (int k = 0; k < 2; k++)
         if (fs->ion_event[k]) cudaEventDestroy(fs->ion_event[k]);
@@ -375,11 +382,120 @@ static int ensure_stage_many(cth_fields* fs, int n) {
     return CTH_OK;
 }
 
+}  // extern "C"
+
+// the sweep of the step after which a field keeps its value for the rest of the
+// step (main.cpp:170-251 order: ions, potential, electron density, electron
+// energy, neutrals, transport); 0: not listed, copied at the end of the step
+static int final_stage(const std::string& f) {
+    static const char* s1[] = {"Uix", "Uir", "Uip", "rhoi", "rhoUix", "rhoUir", "rhoUix_wall", "rhoUir_wall"};
+    static const char* s2[] = {"phi", "Ex", "Er"};
+    for (const char* n : s1)
+        if (f == n) return 1;
+    for (const char* n : s2)
+        if (f == n) return 2;
+    if (f == "rhoe") return 3;
+    if (f == "Te" || f == "rhoeps") return 4;
+    if (f == "rhon" || f == "rhom") return 5;
+    return 0;
+}
+
+int plan_flush(cth_fields* fs, int stage, cudaStream_t s) {
+    if (fs->plan_names.empty()) return CTH_OK;
+    cth_grid* g = fs->g;
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    bool any = false;
+    for (size_t k = 0; k < fs->plan_names.size(); k++) {
+        if (fs->plan_queued[k]) continue;
+        if (stage != 0 && final_stage(fs->plan_names[k]) != stage) continue;
+        if (!any) {
+            CTH_CUDA(cudaEventRecord(fs->copy_ready, s));
+            CTH_CUDA(cudaStreamWaitEvent(fs->copy_stream, fs->copy_ready, 0));
+            any = true;
+        }
+        int rc = from_device_layout(g, fs->planes.at(fs->plan_names[k]), fs->plan_stage + k * nij, fs->copy_stream);
+        if (rc != CTH_OK) return rc;
+        CTH_CUDA(cudaMemcpyAsync(fs->plan_host[k], fs->plan_stage + k * nij, nij * sizeof(double),
+                                 cudaMemcpyDeviceToHost, fs->copy_stream));
+        fs->plan_queued[k] = 1;
+    }
+    if (any) {
+        CTH_CUDA(cudaEventRecord(fs->copy_done, fs->copy_stream));
+        fs->copies_pending = true;
+    }
+    if (stage == 0)
+        for (auto& q : fs->plan_queued) q = 0;  // the next step queues them again
+    return CTH_OK;
+}
+
+int copies_wait(cth_fields* fs, cudaStream_t s) {
+    if (fs->copies_pending) CTH_CUDA(cudaStreamWaitEvent(s, fs->copy_done, 0));
+    return CTH_OK;
+}
+
+extern "C" {
+
+int cth_fields_set_download_plan(cth_fields* fs, const char* const* names, double* const* host_ij, int n) {
+    if (!fs || n < 0 || (n > 0 && (!names || !host_ij))) {
+        set_error("cth_fields_set_download_plan: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    cth_grid* g = fs->g;
+    CTH_CUDA(cudaSetDevice(g->device));
+    if (fs->copies_pending) {
+        CTH_CUDA(cudaStreamSynchronize(fs->copy_stream));
+        fs->copies_pending = false;
+    }
+    std::vector<std::string> nm;
+    std::vector<double*> hp;
+    for (int k = 0; k < n; k++) {
+        if (!names[k] || !host_ij[k] || fs->planes.find(names[k]) == fs->planes.end()) {
+            set_error(std::string("cth_fields_set_download_plan: no field ") + (names[k] ? names[k] : "(null)"));
+            return CTH_ERR_ARG;
+        }
+        nm.emplace_back(names[k]);
+        hp.push_back(host_ij[k]);
+    }
+    if (n > fs->plan_cap) {
+        if (fs->plan_stage) CTH_CUDA(cudaFree(fs->plan_stage));
+        fs->plan_stage = nullptr;
+        fs->plan_cap = 0;
+        const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+        CTH_CUDA(cudaMalloc(&fs->plan_stage, (size_t)n * nij * sizeof(double)));
+        fs->plan_cap = n;
+    }
+    if (!fs->copy_stream) {
+        CTH_CUDA(cudaStreamCreateWithFlags(&fs->copy_stream, cudaStreamNonBlocking));
+        CTH_CUDA(cudaEventCreateWithFlags(&fs->copy_ready, cudaEventDisableTiming));
+        CTH_CUDA(cudaEventCreateWithFlags(&fs->copy_done, cudaEventDisableTiming));
+    }
+    fs->plan_names = nm;
+    fs->plan_host = hp;
+    fs->plan_queued.assign(n, 0);
+    return CTH_OK;
+}
+
+int cth_fields_download_wait(cth_fields* fs) {
+    if (!fs) {
+        set_error("cth_fields_download_wait: null store");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(fs->g->device));
+    if (fs->copies_pending) CTH_CUDA(cudaStreamSynchronize(fs->copy_stream));
+    fs->copies_pending = false;
+    return CTH_OK;
+}
+
 int cth_fields_upload_many(cth_fields* fs, const char* const* names, const double* const* host_ij, int n,
                            void* stream) {
     if (!fs || !names || !host_ij || n < 1) { set_error("cth_fields_upload_many: invalid arguments"); return CTH_ERR_ARG; }
     cth_grid* g = fs->g;
     CTH_CUDA(cudaSetDevice(g->device));
+    {
+        // planned downloads still reading the planes finish first
+        const int rcw = copies_wait(fs, stream ? (cudaStream_t)stream : g->stream);
+        if (rcw != CTH_OK) return rcw;
+    }
     int rc = ensure_stage_many(fs, n);
     if (rc != CTH_OK) return rc;
     cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;

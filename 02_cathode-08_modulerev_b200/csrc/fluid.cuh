@@ -29,11 +29,22 @@ struct cth_fields {
     cudaEvent_t ion_event[2] = {nullptr, nullptr};
     cudaEvent_t net_event[2] = {nullptr, nullptr};
     double* stage_many = nullptr;        // staging of the batched transfers, stage_planes [i][j] planes
+    // planned downloads (cth_fields_set_download_plan): each field is copied to its
+    // host array on copy_stream as soon as the step's sweep that finalises it is done
+    std::vector<std::string> plan_names;
+    std::vector<double*> plan_host;
+    std::vector<char> plan_queued;
+    double* plan_stage = nullptr;        // one [i][j] staging plane per planned field
+    int plan_cap = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ready = nullptr, copy_done = nullptr;
+    bool copies_pending = false;
     int stage_planes = 0;
     int warm_fields = 0;                 // field-valued solves start from the field's current values
     double warm_tol = 1.0;               // their guess threshold (relative residual)
     int net_misses = 0;                  // consecutive predictions that the device judge did not choose
-    long long net_runs = 0, net_wins = 0;                    // streams / events of the concurrent ion solves
+    long long net_runs = 0, net_wins = 0;  // predictions run / chosen by the judge
+    // streams / events of the concurrent ion solves
     cudaStream_t aux_stream[2] = {};
     cudaEvent_t aux_event[3] = {};
     std::map<std::string, double*> planes;
@@ -45,6 +56,13 @@ struct cth_fields {
     double* part = nullptr;          // per-block partials, CTH_FS_NPART_PER_BLOCK per block
     int npart = 0;
 };
+
+// planned downloads: queue (on the copy stream, after the work queued on s) the
+// planned fields that the step's stage `stage` finalises (1 ions, 2 potential,
+// 3 electron density, 4 electron energy, 5 neutrals; 0: every field not yet
+// queued); copies_wait makes s wait for copies still in flight
+int plan_flush(cth_fields* fs, int stage, cudaStream_t s);
+int copies_wait(cth_fields* fs, cudaStream_t s);
 
 namespace cth {
 

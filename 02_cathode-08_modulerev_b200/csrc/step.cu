@@ -14,6 +14,9 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     cth_step_result local{};
     cth_step_result* R = res ? res : &local;
     *R = cth_step_result{};
+    // planned downloads of the previous step still reading the planes finish first
+    int rc0 = copies_wait(fs, (cudaStream_t)stream);
+    if (rc0 < 0) return rc0;
     // check_CFL: dt (adaptive) or CFL (fixed dt)
     R->cfl.dt = p->dt;
     R->cfl.CFL = p->CFL;
@@ -80,6 +83,8 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
         R->ran_ion = 1;
         if (R->ion.solver_rc > worst) worst = R->ion.solver_rc;
     }
+    rc = plan_flush(fs, 1, s);
+    if (rc < 0) return rc;
     if (learned) CTH_CUDA(cudaStreamWaitEvent(s, fs->net_event[1], 0));
     rc = cth_solve_phi_pc(fs, &phi, stream, &R->phi);
     if (learned && rc >= 0) {
@@ -90,12 +95,18 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     R->net_ran = learned ? 1 : 0;
     if (rc < 0) return rc;
     if (R->phi.solver_rc > worst) worst = R->phi.solver_rc;
+    rc = plan_flush(fs, 2, s);
+    if (rc < 0) return rc;
     rc = cth_solve_rhoe_pc(fs, &p->rhoe, stream, &R->rhoe);
     if (rc < 0) return rc;
     if (R->rhoe.solver_rc > worst) worst = R->rhoe.solver_rc;
+    rc = plan_flush(fs, 3, s);
+    if (rc < 0) return rc;
     rc = cth_solve_Te_pc(fs, &p->eps, stream, &R->eps);
     if (rc < 0) return rc;
     if (R->eps.solver_rc > worst) worst = R->eps.solver_rc;
+    rc = plan_flush(fs, 4, s);
+    if (rc < 0) return rc;
     p->neutral.do_rhon = (p->itime % p->ndt_n == 0);
     p->neutral.do_rhom = (p->itime % p->ndt_m == 0);
     if (p->neutral.do_rhon || p->neutral.do_rhom) {
@@ -105,7 +116,11 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     }
     R->ran_rhon = p->neutral.do_rhon;
     R->ran_rhom = p->neutral.do_rhom;
+    rc = plan_flush(fs, 5, s);
+    if (rc < 0) return rc;
     rc = cth_update_transport_coef(fs, &p->transport, stream);
+    if (rc < 0) return rc;
+    rc = plan_flush(fs, 0, s);
     if (rc < 0) return rc;
     R->solver_rc = worst;
     return CTH_OK;

@@ -180,6 +180,26 @@ class Fields:
         """Download into the given {name: [i][j] array} in one batch, after the work queued on `stream`."""
         self._many(arrays, self._L.cth_fields_download_many, True, stream)
 
+    def set_download_plan(self, arrays: dict):
+        """The following fluid steps copy these fields into the given [i][j] host
+        arrays (pinned for full speed) as soon as each is final within the step,
+        overlapping the remaining sweeps; download_wait() waits for them."""
+        g = self.grid
+        names = list(arrays)
+        for k in names:
+            a = arrays[k]
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and
+                    a.flags.writeable and a.shape == (g.ni + 2, g.nj + 2)):
+                raise ValueError(f"{k}: need a writable C-contiguous float64 array of shape {(g.ni + 2, g.nj + 2)}")
+        n = len(names)
+        cn = (ctypes.c_char_p * max(n, 1))(*[k.encode() for k in names])
+        cp = (ctypes.c_void_p * max(n, 1))(*[arrays[k].ctypes.data for k in names])
+        self._plan = dict(arrays)  # the arrays must outlive the copies
+        capi.check(self._L.cth_fields_set_download_plan(self._h, cn, cp, n), allow_positive=False)
+
+    def download_wait(self):
+        capi.check(self._L.cth_fields_download_wait(self._h), allow_positive=False)
+
     def set_flags(self, flags: np.ndarray):
         f = np.ascontiguousarray(flags, dtype=np.uint8)
         capi.check(self._L.cth_flags_upload(self._h, f.ctypes.data), allow_positive=False)

@@ -373,6 +373,18 @@ int cth_ghost_rules_upload(cth_fields* fs, const int* rules, int n);
  * Same stopping rule.  Default off. */
 int cth_fields_set_warm_start(cth_fields* fs, int enable, double max_relres);
 
+/* Planned downloads (no counterpart in the reference): the next cth_fluid_step
+ * calls copy each listed field into its host array ([i][j] layout, pinned for
+ * full speed) on a copy stream of the store as soon as the sweep that finalises
+ * it is done -- the ion fields after the ion step, phi / Ex / Er after the
+ * potential, rhoe after the electron density, Te / rhoeps after the energy,
+ * rhon / rhom after the neutrals, any other field at the end -- so the copies
+ * overlap the remaining sweeps.  cth_fields_download_wait returns when the
+ * copies of the last step have landed; a following step or upload waits for
+ * them on the device by itself.  n = 0 clears the plan. */
+int cth_fields_set_download_plan(cth_fields* fs, const char* const* names, double* const* host_ij, int n);
+int cth_fields_download_wait(cth_fields* fs);
+
 /* Scharfetter-Gummel predictor-correctors of the electron density
  * (cth_solve_rhoe_pc: FluidModule::solve_rhoe_wdTe_wSEE_PC, fluidModule.hpp:3082-3970)
  * and energy (cth_solve_Te_pc: solve_Te_wdTe_wSEE_PC, fluidModule.hpp:4006-4957).

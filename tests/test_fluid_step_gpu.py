@@ -189,3 +189,40 @@ def test_field_warm_start(pkg, orc, cuda_device):
         for x in (g, gx, gr):
             x.close()
     assert sum(its[True]) <= sum(its[False]), its
+
+
+@pytest.mark.parametrize("kind", ["rectangle", "cathode"])
+def test_planned_downloads(pkg, cuda_device, kind):
+    """Downloads queued inside the step as each field becomes final (the ion
+    fields after the ion step, the potential after its sweep, ...) land the
+    same bits as downloading the whole state after the step, over several
+    steps (the planned fields include every one the step writes), and a step
+    issued before the caller waits does not overwrite planes still in flight."""
+    import torch
+    geo, ogeo, st, cfg = setup(pkg, kind)
+    g, gx, gr, fs = device_fields(pkg, geo, st, cfg)
+    names = list(CHECK) + ["rhoUix", "rhoUir", "nUex", "nUer", "rhoUex", "rhoUer", "Gx", "Gr", "nu_m"]
+    names = [k for k in dict.fromkeys(names)]
+    shape = (geo["ni"] + 2, geo["nj"] + 2)
+    bufs = [{k: torch.zeros(shape, dtype=torch.float64).pin_memory().numpy() for k in names} for _ in range(2)]
+    P = {k: (dict(v) if isinstance(v, dict) else v) for k, v in cfg["params"].items()}
+    for step in range(3):
+        plan = bufs[step % 2]
+        fs.set_download_plan(plan)
+        r = fs.fluid_step(gx, gr, P)
+        assert r["solver_rc"] == 0, r
+        fs.download_wait()
+        for k in names:
+            assert np.array_equal(plan[k], fs.download(k)), (kind, step, k)
+    # two steps back to back without waiting in between: the second waits on the
+    # device for the first one's copies
+    fs.set_download_plan(bufs[0])
+    fs.fluid_step(gx, gr, P)
+    fs.fluid_step(gx, gr, P)
+    fs.download_wait()
+    for k in names:
+        assert np.array_equal(bufs[0][k], fs.download(k)), (kind, "back to back", k)
+    fs.set_download_plan({})
+    fs.close()
+    for x in (g, gx, gr):
+        x.close()
