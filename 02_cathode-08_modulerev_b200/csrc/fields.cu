@@ -298,6 +298,9 @@ void cth_fields_destroy(cth_fields* fs) {
     if (fs->copy_ready) cudaEventDestroy(fs->copy_ready);
     if (fs->copy_done) cudaEventDestroy(fs->copy_done);
     if (fs->plan_stage) cudaFree(fs->plan_stage);
+    if (fs->up_stage) cudaFree(fs->up_stage);
+    for (int k = 0; k < 3; k++)
+        if (fs->up_ready[k]) cudaEventDestroy(fs->up_ready[k]);
     if (fs->ion_stream) cudaStreamDestroy(fs->ion_stream);
     for (int k = 0; k < 2; k++)
         if (fs->ion_event[k]) cudaEventDestroy(fs->ion_event[k]);
@@ -433,6 +436,63 @@ int copies_wait(cth_fields* fs, cudaStream_t s) {
     return CTH_OK;
 }
 
+// the first sweep of the step that reads a field: 1 the electron energy sweep
+// (rhoeps), 2 the neutral sweep (rhon, rhom; the transport update after it reads
+// them too); 0 any earlier point (check_CFL, ions, potential, electron density)
+static int first_read(const std::string& f) {
+    if (f == "rhoeps") return 1;
+    if (f == "rhon" || f == "rhom") return 2;
+    return 0;
+}
+
+static int ensure_copy_stream(cth_fields* fs) {
+    if (fs->copy_stream) return CTH_OK;
+    CTH_CUDA(cudaStreamCreateWithFlags(&fs->copy_stream, cudaStreamNonBlocking));
+    CTH_CUDA(cudaEventCreateWithFlags(&fs->copy_ready, cudaEventDisableTiming));
+    CTH_CUDA(cudaEventCreateWithFlags(&fs->copy_done, cudaEventDisableTiming));
+    return CTH_OK;
+}
+
+int plan_upload(cth_fields* fs, cudaStream_t s) {
+    for (int k = 0; k < 3; k++) fs->up_wait[k] = false;
+    if (fs->up_names.empty()) return CTH_OK;
+    cth_grid* g = fs->g;
+    const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+    // nothing queued before this step may still read a plane that is overwritten
+    CTH_CUDA(cudaEventRecord(fs->copy_ready, s));
+    CTH_CUDA(cudaStreamWaitEvent(fs->copy_stream, fs->copy_ready, 0));
+    for (int grp = 0; grp < 3; grp++) {
+        bool any = false;
+        for (size_t k = 0; k < fs->up_names.size(); k++) {
+            if (first_read(fs->up_names[k]) != grp) continue;
+            CTH_CUDA(cudaMemcpyAsync(fs->up_stage + k * nij, fs->up_host[k], nij * sizeof(double),
+                                     cudaMemcpyHostToDevice, fs->copy_stream));
+            double* dst = field_ptr(fs, fs->up_names[k].c_str());
+            if (!dst) { set_error("planned upload: allocation failed"); return CTH_ERR_ALLOC; }
+            const int rc = to_device_layout(g, fs->up_stage + k * nij, dst, fs->copy_stream);
+            if (rc != CTH_OK) return rc;
+            any = true;
+        }
+        if (any) {
+            CTH_CUDA(cudaEventRecord(fs->up_ready[grp], fs->copy_stream));
+            fs->up_wait[grp] = true;
+        }
+    }
+    CTH_CUDA(cudaEventRecord(fs->copy_done, fs->copy_stream));
+    fs->copies_pending = true;
+    fs->up_names.clear();  // one step
+    fs->up_host.clear();
+    return upload_wait(fs, 0, s);
+}
+
+int upload_wait(cth_fields* fs, int group, cudaStream_t s) {
+    if (fs->up_wait[group]) {
+        CTH_CUDA(cudaStreamWaitEvent(s, fs->up_ready[group], 0));
+        fs->up_wait[group] = false;
+    }
+    return CTH_OK;
+}
+
 extern "C" {
 
 int cth_fields_set_download_plan(cth_fields* fs, const char* const* names, double* const* host_ij, int n) {
@@ -464,14 +524,50 @@ int cth_fields_set_download_plan(cth_fields* fs, const char* const* names, doubl
         CTH_CUDA(cudaMalloc(&fs->plan_stage, (size_t)n * nij * sizeof(double)));
         fs->plan_cap = n;
     }
-    if (!fs->copy_stream) {
-        CTH_CUDA(cudaStreamCreateWithFlags(&fs->copy_stream, cudaStreamNonBlocking));
-        CTH_CUDA(cudaEventCreateWithFlags(&fs->copy_ready, cudaEventDisableTiming));
-        CTH_CUDA(cudaEventCreateWithFlags(&fs->copy_done, cudaEventDisableTiming));
+    {
+        const int rce = ensure_copy_stream(fs);
+        if (rce != CTH_OK) return rce;
     }
     fs->plan_names = nm;
     fs->plan_host = hp;
     fs->plan_queued.assign(n, 0);
+    return CTH_OK;
+}
+
+int cth_fields_set_upload_plan(cth_fields* fs, const char* const* names, const double* const* host_ij, int n) {
+    if (!fs || n < 0 || (n > 0 && (!names || !host_ij))) {
+        set_error("cth_fields_set_upload_plan: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    cth_grid* g = fs->g;
+    CTH_CUDA(cudaSetDevice(g->device));
+    std::vector<std::string> nm;
+    std::vector<const double*> hp;
+    for (int k = 0; k < n; k++) {
+        if (!names[k] || !host_ij[k]) {
+            set_error("cth_fields_set_upload_plan: null name or array");
+            return CTH_ERR_ARG;
+        }
+        nm.emplace_back(names[k]);
+        hp.push_back(host_ij[k]);
+    }
+    if (n > fs->up_cap) {
+        if (fs->copies_pending) CTH_CUDA(cudaStreamSynchronize(fs->copy_stream));
+        if (fs->up_stage) CTH_CUDA(cudaFree(fs->up_stage));
+        fs->up_stage = nullptr;
+        fs->up_cap = 0;
+        const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
+        CTH_CUDA(cudaMalloc(&fs->up_stage, (size_t)n * nij * sizeof(double)));
+        fs->up_cap = n;
+    }
+    {
+        const int rce = ensure_copy_stream(fs);
+        if (rce != CTH_OK) return rce;
+    }
+    for (int k = 0; k < 3; k++)
+        if (!fs->up_ready[k]) CTH_CUDA(cudaEventCreateWithFlags(&fs->up_ready[k], cudaEventDisableTiming));
+    fs->up_names = nm;
+    fs->up_host = hp;
     return CTH_OK;
 }
 

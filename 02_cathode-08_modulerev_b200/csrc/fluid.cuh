@@ -39,6 +39,15 @@ struct cth_fields {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_ready = nullptr, copy_done = nullptr;
     bool copies_pending = false;
+    // planned uploads (cth_fields_set_upload_plan), consumed by the next step: the
+    // fields that the step reads first in its energy (rhoeps) or neutral (rhon,
+    // rhom) sweep arrive while the sweeps before them run
+    std::vector<std::string> up_names;
+    std::vector<const double*> up_host;
+    double* up_stage = nullptr;
+    int up_cap = 0;
+    cudaEvent_t up_ready[3] = {nullptr, nullptr, nullptr};  // fields read from the start / energy / neutrals
+    bool up_wait[3] = {false, false, false};
     int stage_planes = 0;
     int warm_fields = 0;                 // field-valued solves start from the field's current values
     double warm_tol = 1.0;               // their guess threshold (relative residual)
@@ -63,6 +72,11 @@ struct cth_fields {
 // queued); copies_wait makes s wait for copies still in flight
 int plan_flush(cth_fields* fs, int stage, cudaStream_t s);
 int copies_wait(cth_fields* fs, cudaStream_t s);
+// planned uploads: issue them on the copy stream (the compute stream waits for the
+// fields read from the start); upload_wait(fs, k, s) makes s wait for group k
+// (1: read first by the energy sweep, 2: by the neutral sweep)
+int plan_upload(cth_fields* fs, cudaStream_t s);
+int upload_wait(cth_fields* fs, int group, cudaStream_t s);
 
 namespace cth {
 

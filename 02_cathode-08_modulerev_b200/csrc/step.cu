@@ -17,6 +17,8 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     // planned downloads of the previous step still reading the planes finish first
     int rc0 = copies_wait(fs, (cudaStream_t)stream);
     if (rc0 < 0) return rc0;
+    rc0 = plan_upload(fs, (cudaStream_t)stream);
+    if (rc0 < 0) return rc0;
     // check_CFL: dt (adaptive) or CFL (fixed dt)
     R->cfl.dt = p->dt;
     R->cfl.CFL = p->CFL;
@@ -102,10 +104,14 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     if (R->rhoe.solver_rc > worst) worst = R->rhoe.solver_rc;
     rc = plan_flush(fs, 3, s);
     if (rc < 0) return rc;
+    rc = upload_wait(fs, 1, s);
+    if (rc < 0) return rc;
     rc = cth_solve_Te_pc(fs, &p->eps, stream, &R->eps);
     if (rc < 0) return rc;
     if (R->eps.solver_rc > worst) worst = R->eps.solver_rc;
     rc = plan_flush(fs, 4, s);
+    if (rc < 0) return rc;
+    rc = upload_wait(fs, 2, s);
     if (rc < 0) return rc;
     p->neutral.do_rhon = (p->itime % p->ndt_n == 0);
     p->neutral.do_rhom = (p->itime % p->ndt_m == 0);

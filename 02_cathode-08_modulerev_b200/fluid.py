@@ -200,6 +200,23 @@ class Fields:
     def download_wait(self):
         capi.check(self._L.cth_fields_download_wait(self._h), allow_positive=False)
 
+    def set_upload_plan(self, arrays: dict):
+        """The next fluid step copies these [i][j] host arrays (pinned for full
+        speed) in at its start without a host synchronisation; rhoeps, rhon and
+        rhom arrive while the sweeps before their first use run."""
+        g = self.grid
+        names = list(arrays)
+        for k in names:
+            a = arrays[k]
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and
+                    a.shape == (g.ni + 2, g.nj + 2)):
+                raise ValueError(f"{k}: need a C-contiguous float64 array of shape {(g.ni + 2, g.nj + 2)}")
+        n = len(names)
+        cn = (ctypes.c_char_p * max(n, 1))(*[k.encode() for k in names])
+        cp = (ctypes.c_void_p * max(n, 1))(*[arrays[k].ctypes.data for k in names])
+        self._up_plan = dict(arrays)  # the arrays must outlive the copies
+        capi.check(self._L.cth_fields_set_upload_plan(self._h, cn, cp, n), allow_positive=False)
+
     def set_flags(self, flags: np.ndarray):
         f = np.ascontiguousarray(flags, dtype=np.uint8)
         capi.check(self._L.cth_flags_upload(self._h, f.ctypes.data), allow_positive=False)

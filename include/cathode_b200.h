@@ -384,6 +384,14 @@ int cth_fields_set_warm_start(cth_fields* fs, int enable, double max_relres);
  * them on the device by itself.  n = 0 clears the plan. */
 int cth_fields_set_download_plan(cth_fields* fs, const char* const* names, double* const* host_ij, int n);
 int cth_fields_download_wait(cth_fields* fs);
+/* Planned uploads for the next cth_fluid_step only: the listed fields are copied
+ * from their host arrays ([i][j], pinned for full speed) on the store's copy
+ * stream at the start of the step; the step waits for the fields it reads from
+ * the start at once, for rhoeps only before the electron energy sweep and for
+ * rhon / rhom only before the neutral sweep, so those copies overlap the sweeps
+ * before.  No host synchronisation; the host arrays must stay valid until the
+ * next cth_fields_download_wait (or a synchronisation of the step's stream). */
+int cth_fields_set_upload_plan(cth_fields* fs, const char* const* names, const double* const* host_ij, int n);
 
 /* Scharfetter-Gummel predictor-correctors of the electron density
  * (cth_solve_rhoe_pc: FluidModule::solve_rhoe_wdTe_wSEE_PC, fluidModule.hpp:3082-3970)
