@@ -366,6 +366,10 @@ def main():
     ap.add_argument("--profile-network", type=int, default=0,
                     help="profiling mode: the warm-start network alone at 512 x 1024 -- after --warmup forward "
                          "passes and training steps, this many more of each on seeded inputs, then exit")
+    ap.add_argument("--profile-microwave", type=int, default=0,
+                    help="profiling mode: this many solves of the magnetised 3-component microwave system at "
+                         "512 x 1024 (seeded magnet workload) after --warmup ones, launched kernel by kernel "
+                         "(profilers cannot see kernels inside conditional graphs), then exit")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every multigrid kernel individually (profilers cannot see kernels inside "
                          "conditional graphs); same kernels, host convergence checks")
@@ -383,6 +387,22 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.profile_microwave > 0:
+        w3 = pkg.workloads.mw3_rect(NI, NJ, seed=2)
+        gm = pkg.Grid(NI, NJ, [[1, NI]], [[1, NJ]], device=local)
+        m3 = pkg.Microwave3(NI, NJ, device=local)
+        m3.set_graphs(False)
+        f3 = [gm.to_device(w3[k]) for k in ("ne", "nu", "Bx", "Br", "epsr")]
+        e3 = m3.planes(3)
+        for _ in range(args.warmup + args.profile_microwave):
+            m3.assemble_dev(*f3, w3["params"])
+            _, st3 = m3.solve_dev(maxITR=200, error_cnv=TOL, out=e3)
+        torch.cuda.synchronize(dev)
+        print(f"profiled {args.profile_microwave} magnetised microwave solves after {args.warmup} warm-up ones "
+              f"({st3.iterations} iterations each)", flush=True)
+        m3.close()
+        gm.close()
+        return 0
     if args.profile_network > 0:
         net = pkg.learned.UNet(NJ, NI, seed=0)
         gen = torch.Generator(device=dev).manual_seed(0)
