@@ -51,8 +51,8 @@ struct cth_fields {
     int stage_planes = 0;
     int warm_fields = 0;                 // field-valued solves start from the field's current values
     double warm_tol = 1.0;               // their guess threshold (relative residual)
-    int net_misses = 0;                  // consecutive predictions that the device judge did not choose
-    long long net_runs = 0, net_wins = 0;  // predictions run / chosen by the judge
+    int net_misses = 0;                  // consecutive predictions that the device-side guess selection did not take
+    long long net_runs = 0, net_wins = 0;  // predictions run / taken by the guess selection
     // streams / events of the concurrent ion solves
     cudaStream_t aux_stream[2] = {};
     cudaEvent_t aux_event[3] = {};

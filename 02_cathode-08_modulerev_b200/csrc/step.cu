@@ -41,7 +41,7 @@ extern "C" int cth_fluid_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, cth_st
     // the learned warm start reads rhoe, nu_m, B and the previous corrections,
     // which the ion step does not change: it runs on its own stream, concurrent
     // with the ion step, and joins before the potential sweep
-    // a predictor that the judge has not chosen for kNetPatience predictions runs
+    // a predictor that the guess selection has not taken for kNetPatience predictions runs
     // only every kNetProbe steps (the other steps start from the previous
     // correction), so it costs nothing while it does not help
     constexpr int kNetPatience = 4, kNetProbe = 8;

@@ -9,7 +9,7 @@ one; the guess is the previous correction plus that change (an untrained,
 zero-output network is the plain previous-step guess).  The multigrid then
 starts from that guess and converges to the unchanged tolerance; a guess whose
 relative residual exceeds ``guess_max_relres`` is dropped on the device and
-the solve starts from zero (the plain method stays the fallback and judge).
+the solve starts from zero (the plain method stays the fallback and the reference point).
 
 This module drives the library: network handle, snapshot collection from plain
 runs, training, and the warm-started time step.  Tensors are torch CUDA tensors

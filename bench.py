@@ -705,10 +705,10 @@ def main():
                          "heldout_rel_err_of_change": float(np.mean(held)), "collect_and_train_s": t_learn,
                          "data": f"{LEARN_SEEDS} seeded discharges x {LEARN_STEPS} plain mixed steps"},
             "note": "value = these steps: the first potential solve of each step starts from the better of "
-                    "(previous correction + the network's predicted change) and the previous correction, judged "
+                    "(previous correction + the network's predicted change) and the previous correction, chosen "
                     "on the device by the initial residual; zero start when both exceed ||b||.  After 4 "
-                    "predictions in a row that the judge did not choose, the network runs every 8th step only.  "
-                    "The ion and neutral solves start from the previous step's fields (same judge)"},
+                    "predictions in a row that the device-side selection did not take, the network runs every 8th step only.  "
+                    "The ion and neutral solves start from the previous step's fields (same selection)"},
         "mixed_zero_start": {"value": world * args.steps / (ms_plain / 1e3), "unit": UNIT},
         "batched_sweep": sweep,
         "warm_start": {

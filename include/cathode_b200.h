@@ -326,7 +326,7 @@ typedef struct cth_phi_params {
      * 1: the better (smaller residual) of the store's plane "dphi_guess"
      * (written by the caller, e.g. the learned predictor) and "dphi_prev";
      * 2: "dphi_prev" = the first-iteration correction of the previous call;
-     * 3: "dphi_guess" alone (judged only against the zero start).
+     * 3: "dphi_guess" alone (tested only against the zero start).
      * With warm_start != 0 the first iteration's correction is copied into
      * "dphi_prev" (its former content into "dphi_prev2").  A guess whose
      * relative residual exceeds guess_max_relres
@@ -504,7 +504,7 @@ typedef struct cth_step_params {
     /* learned warm start (no counterpart in the reference): with phi.warm_start
      * == 1 and net not null, cth_unet_predict_dphi fills "dphi_guess" before the
      * potential predictor-corrector (concurrently with the ion step).  After 4
-     * consecutive predictions that the device judge did not choose, the network
+     * consecutive predictions that the device-side guess selection did not take, the network
      * runs only on steps with itime % 8 == 0 until it is chosen again; the other
      * steps start from the previous correction (warm_start 2). */
     struct cth_unet* net;

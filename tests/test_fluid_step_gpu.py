@@ -157,7 +157,7 @@ def test_previous_step_warm_start(pkg, orc, cuda_device):
 
 def test_field_warm_start(pkg, orc, cuda_device):
     """Field-valued solves (ion velocities and density, neutrals) started from
-    the previous step's fields: every guess is judged on the device (most are
+    the previous step's fields: every guess is tested on the device (most are
     taken; one worse than zero falls back to the zero start), the stopping rule
     is the same (fields within the whole-step tolerance of the oracle) and the
     solves need no more cycles in total than from zero."""
@@ -176,7 +176,7 @@ def test_field_warm_start(pkg, orc, cuda_device):
             assert r["solver_rc"] == 0, r
             its[warm].append(sum(r["all_iterations"].values()))
             if warm:
-                # every guess is judged; one worse than zero is dropped (-1)
+                # every guess is tested; one worse than zero is dropped (-1)
                 assert all(v in (1, -1) for v in r["guess"].values()), r["guess"]
                 assert sum(v == 1 for v in r["guess"].values()) >= 4, r["guess"]
             else:

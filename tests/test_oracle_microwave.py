@@ -41,7 +41,7 @@ def test_coax_oracle_matches_reference_fixture(coax, n):
     assert np.linalg.norm(Er - g) / np.linalg.norm(g) < 5e-6
     assert np.max(np.abs(Er - g)) / np.max(np.abs(g)) < 1e-5
     assert np.linalg.norm(An - ga) / np.linalg.norm(ga) < 5e-6
-    # the reference's own error against the analytic TEM field (SURVEY-quoted 1.04e-4)
+    # the reference's own error against the analytic TEM field (1.04e-4)
     assert abs(np.linalg.norm(g - ga) / np.linalg.norm(ga) - 1.04e-4) < 0.02e-4
 
 

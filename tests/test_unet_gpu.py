@@ -1,6 +1,6 @@
 """The learned warm-start network on the GPU: forward output and parameter
 gradients of the library's tensor-core kernels against the numpy oracle (bf16
-rounding points emulated for the output, 2e-2 relative L2; gradients judged
+rounding points emulated for the output, 2e-2 relative L2; gradients measured
 against the exact float64 network, see the test), training
 on a synthetic regression, and the warm start of the potential solve against
 the plain zero start and the previous-step guess."""
