@@ -433,3 +433,26 @@ def discharge_params(geo: dict, dr: float, rmax: float) -> dict:
     p["eps"] = dict(p["rhoe"])
     return dict(params=p, tables=tb, see=dict(coefEISEE_eb_table=np.zeros(201), coefEISEE_rd_table=np.zeros(201),
                                                coefEISEE_ts_table=np.zeros(201)))
+
+
+def mw3_cathode(ni: int = 194, nj: int = 70, seed: int = 2, omegam: float = 2.67e10, bmax: float = 0.05,
+                xR: float = 0.0388, rmax: float = 0.014) -> dict:
+    """Magnetised microwave system on the cathode geometry (38.8 mm x 14 mm,
+    six blocks per field with the coax feed).
+
+    n_e log-uniform in [1e15, 1e18] m^-3 and nu log-uniform in [1e8, 1e10] s^-1,
+    drawn from default_rng(seed) in that order as (ni+2, nj+2) cell arrays;
+    epsr = 1; a magnet field Bx = bmax exp(-((z - 20 mm) / 8 mm)^2) with
+    Br = -(r / 2) dBx/dz on the cell centres."""
+    rng = np.random.default_rng(seed)
+    ne = 10.0 ** rng.uniform(15.0, 18.0, size=(ni + 2, nj + 2))
+    nu = 10.0 ** rng.uniform(8.0, 10.0, size=(ni + 2, nj + 2))
+    epsr = np.ones((ni + 2, nj + 2))
+    dx, dr, x, r = grid(ni, nj, xR, rmax)
+    z0, wz = 20.0e-3, 8.0e-3
+    X, R = np.meshgrid(x, r, indexing="ij")
+    g = np.exp(-((X - z0) / wz) ** 2)
+    params = dict(dx=dx, dr=dr, rmin=0.0, omegam=omegam, J1r_exc=0.212687, r1=0.6e-3, r2=2.0e-3,
+                  masse=9.10938356e-31)
+    return dict(ni=ni, nj=nj, ne=ne, nu=nu, epsr=epsr, Bx=bmax * g, Br=-(R / 2.0) * bmax * g * (-2.0 * (X - z0) / wz ** 2),
+                params=params, xR=xR, rmax=rmax)

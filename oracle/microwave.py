@@ -17,6 +17,8 @@ Arrays follow the reference: (ni+2, nj+2) complex128, [i][j], Er at r-faces j-1/
 """
 from __future__ import annotations
 
+import re
+
 import numpy as np
 
 E0 = 1.60217662e-19
@@ -435,22 +437,9 @@ def _sigma_terms(rho, nu, bx, br, w, me):
     return coef, hx, hr
 
 
-def mag_rect_system(ne, nu, Bx, Br, epsr, p: dict):
-    """Coefficients of the three field equations after the boundary surgery.
-
-    Interior: Ex (emfieldModule.hpp:2300-2348), Er (:2352-2411), Ephi
-    (:2414-2453), stencil convention aP x_P - sum a_k x_k = b.  Boundary codes of
-    the rectangle (the reference's own codes): Ex Gauss (code 2, :2464-2471 and
-    :2497-2504) at z = 0 and z = L, conductor (code 0, :2536-2538) at r = R; Er
-    port excitation (code 7, :2606-2621) on the z = 0 faces with r1 <= r <= r2
-    and open (code 1, :2579-2588) on the others, open (code 1, :2630-2645) at
-    z = L, Gauss (code 2, :2687-2694) at r = R; Ephi open (code 1, :2720-2729) at
-    z = 0, conductor (code 0, :2737-2739 and :2755-2757) at z = L and r = R.  On
-    the axis the r-weights of the Ex and Ephi south couplings vanish and the Er
-    axis face is not an unknown, so no code is needed there.
-
-    Returns {"x": {name: array}, "r": {...}, "p": {...}, "b": (bx, br, bp), masks}
-    with complex (ni+2, nj+2) arrays in the reference's [i][j] order."""
+def _mag_interior(ne, nu, Bx, Br, epsr, p: dict, masks):
+    """Interior coefficients of the three field equations on their unknowns
+    (emfieldModule.hpp:2300-2453), before any boundary surgery."""
     ni, nj, dx, dr, w, me = p["ni"], p["nj"], p["dx"], p["dr"], p["omegam"], p["masse"]
     r = p["r"]
     sh = (ni + 2, nj + 2)
@@ -460,7 +449,7 @@ def mag_rect_system(ne, nu, Bx, Br, epsr, p: dict):
     Rr = {k: np.zeros(sh, complex) for k in MAG_R}
     Pp = {k: np.zeros(sh, complex) for k in MAG_P}
     bx = np.zeros(sh, complex); br = np.zeros(sh, complex); bp = np.zeros(sh, complex)
-    mx, mr, mp = mag_masks(ni, nj)
+    mx, mr, mp = masks
     # --- Ex on x-faces (i between cells i-1 and i) ---
     I, J = np.nonzero(mx)
     qL = (r[J - 1] + r[J]) / 2.0 / (r[J] + 1e-100)
@@ -505,6 +494,30 @@ def mag_rect_system(ne, nu, Bx, Br, epsr, p: dict):
     Pp["N"][I, J] = qR * dx * dx; Pp["S"][I, J] = qL * dx * dx
     Pp["EE"][I, J] = -iwm * s_px * 0.5 * D; Pp["WW"][I, J] = -iwm * s_px * 0.5 * D
     Pp["NN"][I, J] = -iwm * s_pr * 0.5 * qR * D; Pp["SS"][I, J] = -iwm * s_pr * 0.5 * qL * D
+
+    return X, Rr, Pp, (bx, br, bp)
+
+
+def mag_rect_system(ne, nu, Bx, Br, epsr, p: dict):
+    """Coefficients of the three field equations after the boundary surgery.
+
+    Interior: Ex (emfieldModule.hpp:2300-2348), Er (:2352-2411), Ephi
+    (:2414-2453), stencil convention aP x_P - sum a_k x_k = b.  Boundary codes of
+    the rectangle (the reference's own codes): Ex Gauss (code 2, :2464-2471 and
+    :2497-2504) at z = 0 and z = L, conductor (code 0, :2536-2538) at r = R; Er
+    port excitation (code 7, :2606-2621) on the z = 0 faces with r1 <= r <= r2
+    and open (code 1, :2579-2588) on the others, open (code 1, :2630-2645) at
+    z = L, Gauss (code 2, :2687-2694) at r = R; Ephi open (code 1, :2720-2729) at
+    z = 0, conductor (code 0, :2737-2739 and :2755-2757) at z = L and r = R.  On
+    the axis the r-weights of the Ex and Ephi south couplings vanish and the Er
+    axis face is not an unknown, so no code is needed there.
+
+    Returns {"x": {name: array}, "r": {...}, "p": {...}, "b": (bx, br, bp), masks}
+    with complex (ni+2, nj+2) arrays in the reference's [i][j] order."""
+    ni, nj, dx, dr, w = p["ni"], p["nj"], p["dx"], p["dr"], p["omegam"]
+    r = p["r"]
+    masks = mag_masks(ni, nj)
+    X, Rr, Pp, (bx, br, bp) = _mag_interior(ne, nu, Bx, Br, epsr, p, masks)
 
     def open_R(eps_t):
         c0 = np.sqrt(1.0 / (EPS0 * eps_t * MU0))
@@ -572,7 +585,7 @@ def mag_rect_system(ne, nu, Bx, Br, epsr, p: dict):
             X["N"][i, j] = 0.0
         Pp["P"][i, j] += r[j] / r[j + 1] * Pp["N"][i, j]
         Pp["N"][i, j] = 0.0
-    return dict(x=X, r=Rr, p=Pp, b=(bx, br, bp), masks=(mx, mr, mp))
+    return dict(x=X, r=Rr, p=Pp, b=(bx, br, bp), masks=masks)
 
 
 # neighbour offsets (di, dj, target component) of each coupling
@@ -635,3 +648,247 @@ def mag_unpack(sysd: dict, x):
 
 def mag_pack(sysd: dict, fields):
     return np.concatenate([fields[c][sysd["masks"][c]] for c in range(3)])
+
+
+# ---------------------------------------------------------------------------
+# the magnetised system on the reference's cathode geometry: six blocks per
+# field (initialModule.hpp:219-345; block 5 is the coax feed) and the boundary
+# lists of InitialModule::makeBoundary (initialModule.hpp:420-1055), read from
+# the segment table tests/golden/mw_lists_cathode.json
+# ---------------------------------------------------------------------------
+def cathode_mw_params(ni: int = 194, nj: int = 70, xR: float = 0.0388, rmax: float = 0.014,
+                      omegam: float = 2.67e10, J1r_exc: float = 0.212687) -> dict:
+    """Grid and microwave parameters of the cathode geometry; r1, r2 as
+    makeBoundary sets them (initialModule.hpp:217-218); rmin = 0."""
+    dx, dr = xR / ni, rmax / nj
+    return dict(ni=ni, nj=nj, dx=dx, dr=dr, xR=xR, rmax=rmax, omegam=omegam, J1r_exc=J1r_exc, r1=0.6e-3,
+                r2=2.0e-3, masse=9.10938356e-31, x=(np.arange(ni + 2) - 0.5) * dx, r=(np.arange(nj + 2) - 0.5) * dr)
+
+
+def cathode_mw_blocks(p: dict):
+    """(cells, x-faces, r-faces): each a pair (i_bl, j_bl) of 6 blocks
+    (initialModule.hpp:219-345 with the feed block 5)."""
+    dx, dr, xR, rmax = p["dx"], p["dr"], p["xR"], p["rmax"]
+    x1, x2, x3, x4, x5, x6 = 0.0, 5.6e-3 + 7.8e-3, 10.0e-3 + 7.8e-3, 15.0e-3 + 7.8e-3, 20.0e-3 + 7.8e-3, 7.8e-3
+    r1, r2, r3, r4, r5 = 0.6e-3, 2.0e-3, 4.0e-3, 9.0e-3, 2.0e-3
+    lo = lambda v, d, k: int(v / d + 0.5) + k
+    hi = lambda v, d, k: int(v / d - 0.5) + k
+    ci = [[lo(x6, dx, 1), hi(x2, dx, 1)], [lo(x2, dx, 1), hi(x4, dx, 1)], [lo(x2, dx, 1), hi(x3, dx, 1)],
+          [lo(x3, dx, 1), hi(x5, dx, 1)], [lo(x5, dx, 1), hi(xR, dx, 1)], [lo(x1, dx, 1), hi(x2, dx, 1)]]
+    cj = [[lo(r3, dr, 1), hi(r4, dr, 1)], [lo(r5, dr, 1), hi(r4, dr, 1)], [lo(r1, dr, 1), hi(r5, dr, 1)],
+          [lo(0.0, dr, 1), hi(r5, dr, 1)], [lo(0.0, dr, 1), hi(rmax, dr, 1)], [lo(r1, dr, 1), hi(r2, dr, 1)]]
+    xi = [[lo(x6, dx, 2), hi(x2, dx, 2)], [lo(x2, dx, 2), hi(x4, dx, 1)], [lo(x2, dx, 2), hi(x3, dx, 2)],
+          [lo(x3, dx, 2), hi(x5, dx, 2)], [lo(x5, dx, 2), hi(xR, dx, 1)], [lo(x1, dx, 2), hi(x2, dx, 2)]]
+    xj = cj
+    ri = ci
+    rj = [[lo(r3, dr, 2), hi(r4, dr, 1)], [lo(r5, dr, 1), hi(r4, dr, 1)], [lo(r1, dr, 2), hi(r5, dr, 1)],
+          [lo(0.0, dr, 2), hi(r5, dr, 1)], [lo(0.0, dr, 2), hi(rmax, dr, 1)], [lo(r1, dr, 2), hi(r2, dr, 1)]]
+    a = lambda v: np.array(v, np.int32)
+    return (a(ci), a(cj)), (a(xi), a(xj)), (a(ri), a(rj))
+
+
+def block_mask(ni: int, nj: int, ib, jb) -> np.ndarray:
+    m = np.zeros((ni + 2, nj + 2), bool)
+    for (a, b), (c, d) in zip(ib, jb):
+        m[a:b + 1, c:d + 1] = True
+    return m
+
+
+def cathode_mw_lists(cells, table: dict) -> dict:
+    """The 12 boundary lists {(field, side): [(i, j, code), ...]} in the
+    reference's order, evaluated from the segment table on the cell blocks."""
+    blocks = {"ic": cells[0], "jc": cells[1]}
+    form = re.compile(r"([ij]c)\[(\d)\]\[([01])\]([+-]\d+)?")
+
+    def ev(e: str) -> int:  # the table's one form: ic[b][k] or jc[b][k], plus or minus a constant
+        m = form.fullmatch(e)
+        if not m:
+            raise ValueError(f"unexpected bound expression: {e}")
+        return int(blocks[m.group(1)][int(m.group(2))][int(m.group(3))]) + int(m.group(4) or 0)
+
+    out = {(f, sd): [] for f in "xrp" for sd in "WESN"}
+    for sg in table["segments"]:
+        key = (sg["field"], sg["side"])
+        if sg["kind"] == "point":
+            out[key].append((ev(sg["i"]), ev(sg["j"]), sg["code"]))
+        else:
+            fix = ev(sg["fix"])
+            for v in range(ev(sg["lo"]), ev(sg["hi"]) + 1):
+                out[key].append((fix, v, sg["code"]) if sg["var"] == "j" else (v, fix, sg["code"]))
+    return out
+
+
+def mag_system_lists(ne, nu, Bx, Br, epsr, p: dict, masks, lists: dict, jflc00: int):
+    """The three field equations on the given unknowns with the boundary surgery
+    of solve_Microwave applied list by list in the reference's order (Ex, Er,
+    Ephi; sides W, E, S, N; emfieldModule.hpp:2456-2784).  jflc00 is
+    gc.j_flc_bl[0][0], which the Er code 3 on the south side compares with r
+    (a radius against an index: the reference's special case at :2672)."""
+    dx, dr, w = p["dx"], p["dr"], p["omegam"]
+    r, J1 = p["r"], p["J1r_exc"]
+    X, Rr, Pp, (bx, br, bp) = _mag_interior(ne, nu, Bx, Br, epsr, p, masks)
+
+    def c0_of(e):
+        return np.sqrt(1.0 / (EPS0 * e * MU0))
+
+    def open_x(e):  # code 1 along z (:2579-2588, :2720-2729), normalised
+        c0 = c0_of(e)
+        deno = (2.0 * c0) ** 2 + (w * dx) ** 2
+        return complex((2.0 * c0) ** 2 - (w * dx) ** 2, -4.0 * c0 * w * dx) / (deno + 1e-100)
+
+    def open_r(e, j):  # code 1 along r (:2553-2566, :2771-2782)
+        c0 = c0_of(e)
+        rt = (r[j + 1] + r[j]) / 2.0
+        qL, qR = r[j] / (rt + 1e-100), r[j + 1] / (rt + 1e-100)
+        deno = (2.0 * c0 * np.sqrt(qR)) ** 2 + (w * dr * qR) ** 2
+        R = complex((2.0 * c0) ** 2 * np.sqrt(qL * qR) - (w * dr) ** 2 * qL * qR,
+                    -2.0 * c0 * w * dr * (qL * np.sqrt(qR) + qR * np.sqrt(qL)))
+        return R / (deno + 1e-100)
+
+    for i, j, c in lists[("x", "W")]:  # :2458-2489
+        qL = (r[j - 1] + r[j]) / 2.0 / (r[j] + 1e-100); qR = (r[j + 1] + r[j]) / 2.0 / (r[j] + 1e-100)
+        a = X["W"][i, j]
+        if c == 0:
+            X["W"][i, j] = 0.0
+        elif c == 2:
+            X["P"][i, j] -= a; X["NW"][i, j] += a * dx / dr * qR; X["SW"][i, j] -= a * dx / dr * qL; X["W"][i, j] = 0.0
+        elif c == 3:
+            deno = 1.0 + dx / dr * qL
+            X["P"][i, j] -= a / deno; X["NW"][i, j] += a * (dx / dr * qR) / deno; X["W"][i, j] = 0.0
+        elif c == 4:
+            deno = 1.0 + dx / dr * qR
+            X["P"][i, j] -= a / deno; X["SW"][i, j] -= a * (dx / dr * qL) / deno; X["W"][i, j] = 0.0
+    for i, j, c in lists[("x", "E")]:  # :2491-2514
+        qL = (r[j - 1] + r[j]) / 2.0 / (r[j] + 1e-100); qR = (r[j + 1] + r[j]) / 2.0 / (r[j] + 1e-100)
+        a = X["E"][i, j]
+        if c == 0:
+            X["E"][i, j] = 0.0
+        elif c == 2:
+            X["P"][i, j] -= a; X["NE"][i, j] -= a * dx / dr * qR; X["SE"][i, j] += a * dx / dr * qL; X["E"][i, j] = 0.0
+        elif c == 4:
+            deno = 1.0 + dx / dr * qR
+            X["P"][i, j] -= a / deno; X["SE"][i, j] += a * (dx / dr * qL) / deno; X["E"][i, j] = 0.0
+    for i, j, c in lists[("x", "S")]:  # :2516-2531
+        a = X["S"][i, j]
+        if c == 0:
+            X["P"][i, j] += r[j] / r[j - 1] * a; X["S"][i, j] = 0.0
+        elif c == 6:
+            rR, rL = (r[j + 1] + r[j]) / 2.0, (r[j] + r[j - 1]) / 2.0
+            X["P"][i, j] -= a * (dr / dx * r[j] / rL); X["W"][i, j] += a * (-dr / dx * r[j] / rL)
+            X["NW"][i, j] += a * (rR / rL); X["S"][i, j] = 0.0
+    for i, j, c in lists[("x", "N")]:  # :2533-2571
+        a = X["N"][i, j]
+        rR, rL = (r[j + 1] + r[j]) / 2.0, (r[j] + r[j - 1]) / 2.0
+        if c == 0:
+            X["P"][i, j] += r[j] / r[j + 1] * a; X["N"][i, j] = 0.0
+        elif c == 1:
+            X["P"][i, j] -= a * open_r((epsr[i, j] + epsr[i - 1, j]) / 2.0, j); X["N"][i, j] = 0.0
+        elif c == 5:
+            X["P"][i, j] -= a * (dr / dx * r[j] / rR); X["E"][i, j] += a * (-dr / dx * r[j] / rR)
+            X["SE"][i, j] += a * (rL / rR); X["N"][i, j] = 0.0
+        elif c == 6:
+            X["P"][i, j] -= a * (dr / dx * r[j] / rR); X["W"][i, j] += a * (-dr / dx * r[j] / rR)
+            X["SW"][i, j] += a * (-rL / rR); X["N"][i, j] = 0.0
+    for i, j, c in lists[("r", "W")]:  # :2574-2622
+        a = Rr["W"][i, j]
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        if c == 0:
+            Rr["P"][i, j] += a; Rr["W"][i, j] = 0.0
+        elif c == 1:
+            Rr["P"][i, j] -= a * open_x(eps_t); Rr["W"][i, j] = 0.0
+        elif c == 5:
+            rR, rL = (r[j + 1] + r[j]) / 2.0, (r[j] + r[j - 1]) / 2.0
+            Rr["P"][i, j] -= a * (dx / dr * rL / r[j]); Rr["N"][i, j] += a * (-dx / dr * rR / r[j])
+            Rr["NE"][i, j] += a * (-1.0); Rr["W"][i, j] = 0.0
+        elif c == 6:
+            rR, rL = (r[j] + r[j - 1]) / 2.0, (r[j - 1] + r[j - 2]) / 2.0
+            Rr["P"][i, j] -= a * (dx / dr * rR / r[j - 1]); Rr["S"][i, j] += a * (-dx / dr * rL / r[j - 1])
+            Rr["SE"][i, j] += a * 1.0; Rr["W"][i, j] = 0.0
+        elif c == 7:
+            c0 = c0_of(eps_t)
+            deno, Rq = complex(2.0 * c0, w * dx), complex(2.0 * c0, -w * dx)
+            rt = (r[j] + r[j - 1]) / 2.0
+            S = complex(0.0, 4.0 * w * dx) * (J1 / rt / np.log(p["r2"] / p["r1"]) * 1e3)
+            Rr["P"][i, j] -= a * Rq / (deno + 1e-100); br[i, j] += a * S / (deno + 1e-100); Rr["W"][i, j] = 0.0
+    for i, j, c in lists[("r", "E")]:  # :2624-2656
+        a = Rr["E"][i, j]
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        if c == 0:
+            Rr["P"][i, j] += a; Rr["E"][i, j] = 0.0
+        elif c == 1:
+            c0 = c0_of(eps_t)
+            deno = (2.0 * c0) ** 2 + (w * dx) ** 2
+            R = complex((2.0 * c0) ** 2 - (w * dx) ** 2, -4.0 * c0 * w * dx)
+            Rr["P"][i, j] -= a * R / (deno + 1e-100); Rr["E"][i, j] = 0.0
+        elif c == 5:
+            rR, rL = (r[j + 1] + r[j]) / 2.0, (r[j] + r[j - 1]) / 2.0
+            Rr["P"][i, j] -= a * (dx / dr * rL / r[j]); Rr["N"][i, j] += a * (-dx / dr * rR / r[j])
+            Rr["NW"][i, j] += a * 1.0; Rr["E"][i, j] = 0.0
+    for i, j, c in lists[("r", "S")]:  # :2658-2681
+        a = Rr["S"][i, j]
+        rR, rL = (r[j] + r[j - 1]) / 2.0, (r[j - 1] + r[j - 2]) / 2.0
+        if c == 2:
+            Rr["P"][i, j] -= a * rR / rL; Rr["SE"][i, j] += a * dr / dx * r[j - 1] / rL
+            Rr["SW"][i, j] -= a * dr / dx * r[j - 1] / rL; Rr["S"][i, j] = 0.0
+        elif c == 3:
+            deno = dr / dx * r[j - 1] / rL
+            if r[j] < jflc00:
+                deno = 1.0
+            Rr["P"][i, j] -= a * rR / rL / deno; Rr["NE"][i, j] += a * dr / dx * r[j - 1] / rL / deno
+            Rr["S"][i, j] = 0.0
+    for i, j, c in lists[("r", "N")]:  # :2683-2711
+        a = Rr["N"][i, j]
+        rR, rL = (r[j + 1] + r[j]) / 2.0, (r[j] + r[j - 1]) / 2.0
+        if c == 2:
+            Rr["P"][i, j] -= a * rL / rR; Rr["NE"][i, j] -= a * dr / dx * r[j] / rR
+            Rr["NW"][i, j] += a * dr / dx * r[j] / rR; Rr["N"][i, j] = 0.0
+        elif c == 3:
+            deno = dr / dx * r[j] / rR
+            Rr["P"][i, j] -= a * rL / rR / deno; Rr["SE"][i, j] -= a * dr / dx * r[j] / rR / deno; Rr["N"][i, j] = 0.0
+        elif c == 4:
+            deno = dr / dx * r[j] / rR
+            Rr["P"][i, j] -= a * rL / rR / deno; Rr["SW"][i, j] += a * dr / dx * r[j] / rR / deno; Rr["N"][i, j] = 0.0
+    for i, j, c in lists[("p", "W")]:  # :2713-2730
+        a = Pp["W"][i, j]
+        if c == 0:
+            Pp["P"][i, j] += a; Pp["W"][i, j] = 0.0
+        elif c == 1:
+            Pp["P"][i, j] -= a * open_x(epsr[i, j]); Pp["W"][i, j] = 0.0
+    for i, j, c in lists[("p", "E")]:  # :2731-2739
+        if c == 0:
+            Pp["P"][i, j] += Pp["E"][i, j]; Pp["E"][i, j] = 0.0
+    for i, j, c in lists[("p", "S")]:  # :2741-2749
+        if c == 0:
+            Pp["P"][i, j] += r[j] / r[j - 1] * Pp["S"][i, j]; Pp["S"][i, j] = 0.0
+    for i, j, c in lists[("p", "N")]:  # :2751-2784
+        a = Pp["N"][i, j]
+        if c == 0:
+            Pp["P"][i, j] += r[j] / r[j + 1] * a; Pp["N"][i, j] = 0.0
+        elif c == 1:
+            Pp["P"][i, j] -= a * open_r(epsr[i, j], j); Pp["N"][i, j] = 0.0
+    return dict(x=X, r=Rr, p=Pp, b=(bx, br, bp), masks=masks)
+
+
+def rect_mw_lists(ni: int, nj: int, p: dict) -> dict:
+    """The rectangle's boundary rules (those of mag_rect_system) as the
+    reference's 12 lists: Ex Gauss (2) at z = 0, L and conductor (0) at r = R;
+    Er port (7) on the z = 0 faces with r1 <= r <= r2, open (1) on the other
+    z = 0 faces and at z = L, Gauss (2) at r = R; Ephi open (1) at z = 0,
+    conductor (0) at z = L and r = R."""
+    r = p["r"]
+    L = {(f, sd): [] for f in "xrp" for sd in "WESN"}
+    for j in range(1, nj + 1):
+        L[("x", "W")].append((2, j, 2))
+        L[("x", "E")].append((ni, j, 2))
+        L[("p", "W")].append((1, j, 1))
+        L[("p", "E")].append((ni, j, 0))
+    for j in range(2, nj + 1):
+        rt = (r[j] + r[j - 1]) / 2.0
+        L[("r", "W")].append((1, j, 7 if p["r1"] <= rt <= p["r2"] else 1))
+        L[("r", "E")].append((ni, j, 1))
+    for i in range(1, ni + 1):
+        L[("r", "N")].append((i, nj, 2))
+        if i >= 2:
+            L[("x", "N")].append((i, nj, 0))
+        L[("p", "N")].append((i, nj, 0))
+    return L

@@ -52,3 +52,70 @@ def test_hall_couplings_scale_with_field():
     a1, a2 = s1["r"]["NN"][2:-2, 3:-2], s2["r"]["NN"][2:-2, 3:-2]
     # second-order terms are of relative size (hall factor)^2 ~ 4e-7 here
     assert np.max(np.abs(a2 - 2 * a1)) <= 1e-5 * np.max(np.abs(a2))
+
+
+# ---------------------------------------------------------------------------
+# the cathode geometry: blocks of initialModule.hpp:219-345 and the boundary
+# lists of InitialModule::makeBoundary read from the committed segment table
+# ---------------------------------------------------------------------------
+def _cathode(ni=194, nj=70, bmax=0.05, seed=2):
+    import json
+    import os
+    from importlib import import_module
+    wl = import_module("02_cathode-08_modulerev_b200.workloads")
+    from oracle import microwave as mw
+    w = wl.mw3_cathode(ni, nj, seed=seed, bmax=bmax)
+    p = mw.cathode_mw_params(ni, nj)
+    cells, xf, rf = mw.cathode_mw_blocks(p)
+    masks = (mw.block_mask(ni, nj, *xf), mw.block_mask(ni, nj, *rf), mw.block_mask(ni, nj, *cells))
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "mw_lists_cathode.json")) as f:
+        table = json.load(f)
+    lists = mw.cathode_mw_lists(cells, table)
+    return w, p, mw, masks, lists, int(cells[1][0][0])
+
+
+def test_cathode_lists_are_boundary_rows():
+    """Every list entry is an unknown of its field, no entry repeats within a
+    list, and the table's 59 segments cover the fixed counts of the 194 x 70
+    grid."""
+    w, p, mw, masks, lists, _ = _cathode()
+    counts = {k: len(v) for k, v in lists.items()}
+    assert sum(counts.values()) == 1644, counts
+    for (f, side), ent in lists.items():
+        m = masks["xrp".index(f)]
+        ij = [(i, j) for i, j, _ in ent]
+        assert len(set(ij)) == len(ij), (f, side)
+        assert all(m[i, j] for i, j in ij), (f, side)
+        assert all(0 <= c <= 7 for _, _, c in ent)
+
+
+def test_cathode_direct_solution():
+    w, p, mw, masks, lists, jflc = _cathode()
+    s = mw.mag_system_lists(w["ne"], w["nu"], w["Bx"], w["Br"], w["epsr"], p, masks, lists, jflc)
+    A, b, _ = mw.mag_rect_matrix(s)
+    assert A.shape[0] == sum(int(m.sum()) for m in masks)
+    assert np.max(np.diff(A.indptr)) <= 11
+    E = mw.mag_rect_solve(s)
+    x = mw.mag_pack(s, E)
+    assert np.linalg.norm(A @ x - b) / np.linalg.norm(b) < 1e-11
+    assert np.abs(E[1]).max() > 0.0  # driven by the feed (Er west, code 7)
+    # without a field Ephi decouples and has no source
+    s0 = mw.mag_system_lists(w["ne"], w["nu"], 0 * w["Bx"], 0 * w["Br"], w["epsr"], p, masks, lists, jflc)
+    assert np.max(np.abs(mw.mag_rect_solve(s0)[2])) == 0.0
+
+
+def test_rectangle_surgery_as_lists():
+    """The rectangle's boundary rules written as the reference's lists give the
+    same system through the list-driven surgery."""
+    w, p, mw = _case()
+    ni, nj = w["ni"], w["nj"]
+    ref = mw.mag_rect_system(w["ne"], w["nu"], w["Bx"], w["Br"], w["epsr"], p)
+    lists = mw.rect_mw_lists(ni, nj, p)
+    s = mw.mag_system_lists(w["ne"], w["nu"], w["Bx"], w["Br"], w["epsr"], p, ref["masks"], lists, 0)
+    for comp in ("x", "r", "p"):
+        for k, v in ref[comp].items():
+            scale = np.abs(v).max() + 1e-300
+            assert np.max(np.abs(s[comp][k] - v)) <= 1e-14 * scale, (comp, k)
+    for c in range(3):
+        assert np.max(np.abs(s["b"][c] - ref["b"][c])) <= 1e-14 * (np.abs(ref["b"][c]).max() + 1e-300)
