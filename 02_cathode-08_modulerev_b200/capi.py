@@ -33,6 +33,7 @@ EXPORTS = (
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_mw3_create", "cth_mw3_destroy", "cth_mw3_ld", "cth_mw3_launch_count", "cth_mw3_assemble_dev",
     "cth_mw3_copy_planes", "cth_mw3_apply_dev", "cth_mw3_solve_dev", "cth_mw3_set_graphs",
+    "cth_mw3_create_blocks", "cth_mw3_set_boundary",
     "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_fields_set_download_plan", "cth_fields_download_wait", "cth_fields_set_upload_plan", "cth_fields_upload_many",
     "cth_fields_download_many", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
@@ -81,6 +82,11 @@ class SParamParams(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("S11_mag", "S11_arg_deg", "S21_mag", "S21_arg_deg", "S12_mag",
                                                "S12_arg_deg", "S22_mag", "S22_arg_deg", "Z0", "phase_pre_deg",
                                                "omegam", "epsr_diele", "h0_stab", "dh_stab", "dl_cable")]
+
+
+class BCList(ctypes.Structure):
+    """cth_bc_list: one boundary list of MicrowaveBC (i, j, code arrays)."""
+    _fields_ = [("i", ctypes.c_void_p), ("j", ctypes.c_void_p), ("code", ctypes.c_void_p), ("n", ctypes.c_int)]
 
 
 class MWParams(ctypes.Structure):
@@ -228,6 +234,11 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_mw3_solve_dev.restype = ctypes.c_int
     L.cth_mw3_set_graphs.argtypes = [_vp, ctypes.c_int]
     L.cth_mw3_set_graphs.restype = ctypes.c_int
+    L.cth_mw3_create_blocks.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp, _vp, ctypes.c_int] * 3 + \
+        [ctypes.c_int, ctypes.POINTER(_vp)]
+    L.cth_mw3_create_blocks.restype = ctypes.c_int
+    L.cth_mw3_set_boundary.argtypes = [_vp, ctypes.POINTER(BCList), ctypes.c_int]
+    L.cth_mw3_set_boundary.restype = ctypes.c_int
     L.cth_fields_create.argtypes = [_vp, ctypes.POINTER(_vp)]
     L.cth_fields_create.restype = ctypes.c_int
     L.cth_fields_destroy.argtypes = [_vp]

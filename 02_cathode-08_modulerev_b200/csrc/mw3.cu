@@ -6,22 +6,30 @@
 // each row an 11-point stencil (its own 5-point operator plus the face or cell
 // averages of the other two components, :2300-2453), assembled into one sparse
 // matrix of unknown-to-unknown couplings (:2785-2990) and factorised with Eigen
-// SparseLU (:2995-2998).  Here, on the r-z rectangle r in [0, R], z in [0, L]
-// with the reference's own boundary codes (the same codes as the oracle's
-// mag_rect_system):
+// SparseLU (:2995-2998).
+//
+// Geometry: each field's unknowns are the union of its block table (the x-face,
+// r-face and cell blocks gx.i_flx_bl / gr.i_flr_bl / gc.i_flc_bl, six blocks on
+// the cathode with the coax feed), held as the masks of three grids.  Assembly
+// is the interior stencil on every unknown, then the boundary surgery of the
+// reference's 12 lists (MicrowaveBC, include/arrays.hpp:649: for Ex, Er, Ephi in
+// turn the W, E, S, N lists, each entry (i, j, code) with codes 0-7,
+// :2456-2784), one launch per list in the reference's order; entries of one
+// list are distinct rows, so a list's threads never touch the same
+// coefficient.  The r-z rectangle (r in [0, R], z in [0, L]) is the special
+// case of one block per field and the lists of its walls:
 //   Ex   Gauss (code 2) at z = 0 and z = L, conductor (code 0) at r = R;
 //   Er   port excitation (code 7) on the z = 0 faces with r1 <= r <= r2, open
 //        (code 1) on the other z = 0 faces and at z = L, Gauss (code 2) at r = R;
 //   Ephi open (code 1) at z = 0, conductor (code 0) at z = L and r = R;
-// on the axis the r-weights of the Ex and Ephi south couplings vanish and the
-// Er axis face is not an unknown.  Unknowns: Ex i = 2..ni, j = 1..nj; Er
-// i = 1..ni, j = 2..nj; Ephi i = 1..ni, j = 1..nj.
+// Ex i = 2..ni, j = 1..nj; Er i = 1..ni, j = 2..nj; Ephi i = 1..ni, j = 1..nj.
 //
 // Solver: BiCGStab in complex FP64 on the coupled operator, right-
 // preconditioned block-diagonally by one complex semicoarsening V-cycle per
-// field (the smg.cu hierarchy of a grid whose single box is that field's
-// unknowns, built on the field's own 5-point block).  Vectors live in the
-// library layout (row j, column i, leading dimension ld), one plane per field,
+// field (the smg.cu hierarchy of the field's grid, built on the field's own
+// 5-point block; rows of the bounding box off the unknowns are identity rows).
+// Vectors live in the library layout (row j, column i, leading dimension ld),
+// one plane per field,
 // and stay exactly zero off their unknowns, so the coupled apply needs no
 // neighbour tests: a coupling to a non-unknown multiplies a zero, which is the
 // reference's dropped matrix entry.
@@ -29,6 +37,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "grid.h"
 #include "line.cuh"
@@ -75,15 +84,10 @@ struct Dev3 {
     cd* b;  // [3] planes
     cd *x, *r, *rh, *p, *ph, *v, *s, *sh, *t;  // [3] planes each
     double* sc;
+    const unsigned char* mk[3];  // unknowns of each field (library layout)
     int ni, nj, ld;
     size_t pl;
 };
-
-__device__ __forceinline__ bool unknown(int c, int i, int j, int ni, int nj) {
-    if (c == 0) return i >= 2 && i <= ni && j >= 1 && j <= nj;
-    if (c == 1) return i >= 1 && i <= ni && j >= 2 && j <= nj;
-    return i >= 1 && i <= ni && j >= 1 && j <= nj;
-}
 
 __device__ __forceinline__ cd sc_c(const double* sc, int w) { return cd(sc[w], sc[w + 1]); }
 __device__ __forceinline__ void sc_set(double* sc, int w, cd v) { sc[w] = v.x; sc[w + 1] = v.y; }
@@ -144,20 +148,38 @@ __device__ __forceinline__ Sig sigma(double rho, double nu, double bx, double br
     return s;
 }
 
-// first-order open boundary factor R of codes 1 (:2579-2588)
-__device__ __forceinline__ cd open_r(double eps_t, double w, double dx) {
+__device__ __forceinline__ cd mulr(cd a, double v) { return cd(a.x * v, a.y * v); }
+__device__ __forceinline__ cd divr(cd a, double v) { return cd(a.x / v, a.y / v); }
+
+// first-order open boundary factor along z of codes 1 (:2579-2588, :2720-2729)
+__device__ __forceinline__ cd open_z(double eps_t, double w, double dx) {
     const double c0 = sqrt(1.0 / (kEPS0 * eps_t * kMU0));
     const double deno = (2.0 * c0) * (2.0 * c0) + (w * dx) * (w * dx) + 1e-100;
     return cd(((2.0 * c0) * (2.0 * c0) - (w * dx) * (w * dx)) / deno, (-4.0 * c0 * w * dx) / deno);
 }
 
+// the same along r, on the r-weighted stencil of the north faces (:2553-2566,
+// :2771-2782); r(j) and r(j+1) are the cell radii either side of the face
+__device__ __forceinline__ cd open_rad(double eps_t, double w, double dr, double rj, double rjp) {
+    const double c0 = sqrt(1.0 / (kEPS0 * eps_t * kMU0));
+    const double rt = (rjp + rj) / 2.0;
+    const double qL = rj / (rt + 1e-100), qR = rjp / (rt + 1e-100);
+    const double t1 = 2.0 * c0 * sqrt(qR), t2 = w * dr * qR;
+    const double deno = t1 * t1 + t2 * t2 + 1e-100;
+    const cd R((2.0 * c0) * (2.0 * c0) * sqrt(qL * qR) - (w * dr) * (w * dr) * qL * qR,
+               -2.0 * c0 * w * dr * (qL * sqrt(qR) + qR * sqrt(qL)));
+    return divr(R, deno);
+}
+
+// interior stencils of the three fields on their unknowns (the boundary
+// surgery follows, list by list)
 __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __restrict__ nu,
                               const double* __restrict__ Bx, const double* __restrict__ Br,
                               const double* __restrict__ epsr, cth_mw_params prm, Dev3 D) {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y;
     if (i > D.ni) return;
-    const int ni = D.ni, nj = D.nj, ld = D.ld;
+    const int ld = D.ld;
     const size_t pl = D.pl, q = (size_t)j * ld + i;
     const double dx = prm.dx, dr = prm.dr, w = prm.omegam, me = prm.masse;
     const double g2 = dx * dx * dr * dr;
@@ -165,7 +187,7 @@ __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __res
     auto r_of = [&](int jj) { return prm.rmin + (jj - 0.5) * dr; };
     const double rj = r_of(j), rjm = r_of(j - 1), rjp = r_of(j + 1);
     // ---- Ex (x-face between cells i-1 and i), :2300-2348 ----
-    if (unknown(0, i, j, ni, nj)) {
+    if (D.mk[0][q]) {
         cd* A = D.a;
         const double qL = (rjm + rj) / 2.0 / (rj + 1e-100);
         const double qR = (rjp + rj) / 2.0 / (rj + 1e-100);
@@ -173,33 +195,17 @@ __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __res
                             (Br[q] + Br[q - 1]) / 2.0, w, me);
         const double eps_t = (epsr[q] + epsr[q - 1]) / 2.0;
         const cd s_xr = s.coef * (s.hx * s.hr), s_xp = s.coef * s.hr, s_xx = s.coef * (cd(1.0) + s.hx * s.hx);
-        cd aP = cd(2.0 * dx * dx + 2.0 * dr * dr - kEPS0 * eps_t * kMU0 * w * w * g2) + iwm * s_xx * cd(g2);
-        cd aE(dr * dr), aW(dr * dr), aN(qR * dx * dx), aS(qL * dx * dx);
+        const cd aP = cd(2.0 * dx * dx + 2.0 * dr * dr - kEPS0 * eps_t * kMU0 * w * w * g2) + iwm * s_xx * cd(g2);
+        const cd aE(dr * dr), aW(dr * dr), aN(qR * dx * dx), aS(qL * dx * dx);
         const cd kp = iwm * s_xp * cd(-0.5 * g2), kr = iwm * s_xr * cd(-0.25 * g2);
-        cd cNE = kr * cd(qR), cSE = kr * cd(qL), cNW = kr * cd(qR), cSW = kr * cd(qL);
-        if (i == 2) {  // z = 0: Gauss (code 2, :2464-2471)
-            aP -= aW;
-            cNW += aW * cd(dx / dr * qR);
-            cSW -= aW * cd(dx / dr * qL);
-            aW = cd();
-        }
-        if (i == ni) {  // z = L: Gauss (code 2, :2497-2504)
-            aP -= aE;
-            cNE -= aE * cd(dx / dr * qR);
-            cSE += aE * cd(dx / dr * qL);
-            aE = cd();
-        }
-        if (j == nj) {  // r = R: conductor (code 0, :2536-2538)
-            aP += cd(rj / rjp) * aN;
-            aN = cd();
-        }
+        const cd cNE = kr * cd(qR), cSE = kr * cd(qL), cNW = kr * cd(qR), cSW = kr * cd(qL);
         A[QP * pl + q] = aP; A[QE * pl + q] = aE; A[QW * pl + q] = aW; A[QN * pl + q] = aN; A[QS * pl + q] = aS;
         A[C0 * pl + q] = cNE; A[C1 * pl + q] = cSE; A[C2 * pl + q] = cNW; A[C3 * pl + q] = cSW;
         A[C4 * pl + q] = kp; A[C5 * pl + q] = kp;
         D.b[q] = cd();
     }
     // ---- Er (r-face between cells j-1 and j), :2352-2411 ----
-    if (unknown(1, i, j, ni, nj)) {
+    if (D.mk[1][q]) {
         cd* A = D.a + (size_t)NQ * pl;
         const double rjmm = r_of(j - 2);
         const double r_t = (rjm + rj) / 2.0, rR = (rj + rjp) / 2.0, rL = (rjmm + rjm) / 2.0;
@@ -208,66 +214,28 @@ __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __res
                             w, me);
         const double eps_t = (epsr[q] + epsr[q - ld]) / 2.0;
         const cd s_rr = s.coef * (cd(1.0) + s.hr * s.hr), s_rp = s.coef * (-s.hx), s_rx = s.coef * (s.hx * s.hr);
-        cd aP = cd(r_t * (1.0 / rj + 1.0 / rjm) * dx * dx + 2.0 * dr * dr - kEPS0 * eps_t * kMU0 * w * w * g2) +
+        const cd aP = cd(r_t * (1.0 / rj + 1.0 / rjm) * dx * dx + 2.0 * dr * dr - kEPS0 * eps_t * kMU0 * w * w * g2) +
                 iwm * s_rr * cd(g2);
-        cd aE(dr * dr), aW(dr * dr), aN(rR / rj * dx * dx), aS(rL / rjm * dx * dx);
+        const cd aE(dr * dr), aW(dr * dr), aN(rR / rj * dx * dx), aS(rL / rjm * dx * dx);
         const cd kp = iwm * s_rp * cd(-0.5 * g2), kx = iwm * s_rx * cd(-0.25 * g2);
         const cd cNN = kp * cd(rj / r_t), cSS = kp * cd(rjm / r_t);
-        cd cNE = kx * cd(rj / r_t), cNW = kx * cd(rj / r_t), cSE = kx * cd(rjm / r_t), cSW = kx * cd(rjm / r_t);
-        cd bb;
-        if (i == 1) {
-            const double c0 = sqrt(1.0 / (kEPS0 * eps_t * kMU0));
-            if (r_t >= prm.r1 && r_t <= prm.r2) {  // port excitation (code 7, :2606-2621)
-                const cd deno(2.0 * c0 + 1e-100, w * dx);
-                const cd R(2.0 * c0, -w * dx);
-                const double Er_Fw = prm.J1r_exc / r_t / log(prm.r2 / prm.r1) * 1e3;
-                const cd S = cd(0.0, 4.0 * w * dx) * cd(Er_Fw);
-                aP -= aW * cdiv(R, deno);
-                bb += aW * cdiv(S, deno);
-            } else {  // open (code 1, :2579-2588)
-                aP -= aW * open_r(eps_t, w, dx);
-            }
-            aW = cd();
-        }
-        if (i == ni) {  // z = L: open (code 1, :2630-2645)
-            aP -= aE * open_r(eps_t, w, dx);
-            aE = cd();
-        }
-        if (j == nj) {  // r = R: Gauss (code 2, :2687-2694)
-            const double rRn = (rjp + rj) / 2.0, rLn = (rj + rjm) / 2.0;
-            aP -= aN * cd(rLn / rRn);
-            cNE -= aN * cd(dr / dx * rj / rRn);
-            cNW += aN * cd(dr / dx * rj / rRn);
-            aN = cd();
-        }
+        const cd cNE = kx * cd(rj / r_t), cNW = kx * cd(rj / r_t), cSE = kx * cd(rjm / r_t), cSW = kx * cd(rjm / r_t);
         A[QP * pl + q] = aP; A[QE * pl + q] = aE; A[QW * pl + q] = aW; A[QN * pl + q] = aN; A[QS * pl + q] = aS;
         A[C0 * pl + q] = cNE; A[C1 * pl + q] = cSE; A[C2 * pl + q] = cNW; A[C3 * pl + q] = cSW;
         A[C4 * pl + q] = cNN; A[C5 * pl + q] = cSS;
-        D.b[pl + q] = bb;
+        D.b[pl + q] = cd();
     }
     // ---- Ephi (cell), :2414-2453 ----
-    if (unknown(2, i, j, ni, nj)) {
+    if (D.mk[2][q]) {
         cd* A = D.a + (size_t)2 * NQ * pl;
         const double qL = (rjm + rj) / 2.0 / (rj + 1e-100);
         const double qR = (rjp + rj) / 2.0 / (rj + 1e-100);
         const Sig s = sigma(ne[q], nu[q], Bx[q], Br[q], w, me);
         const cd s_pr = s.coef * s.hx, s_pp = s.coef, s_px = s.coef * (-s.hr);
-        cd aP = cd(2.0 * dx * dx + 2.0 * dr * dr + g2 / (rj * rj) - kEPS0 * epsr[q] * kMU0 * w * w * g2) +
+        const cd aP = cd(2.0 * dx * dx + 2.0 * dr * dr + g2 / (rj * rj) - kEPS0 * epsr[q] * kMU0 * w * w * g2) +
                 iwm * s_pp * cd(g2);
-        cd aE(dr * dr), aW(dr * dr), aN(qR * dx * dx), aS(qL * dx * dx);
+        const cd aE(dr * dr), aW(dr * dr), aN(qR * dx * dx), aS(qL * dx * dx);
         const cd kx = iwm * s_px * cd(-0.5 * g2), kr = iwm * s_pr * cd(-0.5 * g2);
-        if (i == 1) {  // z = 0: open (code 1, :2720-2729)
-            aP -= aW * open_r(epsr[q], w, dx);
-            aW = cd();
-        }
-        if (i == ni) {  // z = L: conductor (code 0, :2737-2739)
-            aP += aE;
-            aE = cd();
-        }
-        if (j == nj) {  // r = R: conductor (code 0, :2755-2757)
-            aP += cd(rj / rjp) * aN;
-            aN = cd();
-        }
         A[QP * pl + q] = aP; A[QE * pl + q] = aE; A[QW * pl + q] = aW; A[QN * pl + q] = aN; A[QS * pl + q] = aS;
         A[C0 * pl + q] = kx; A[C1 * pl + q] = kx; A[C2 * pl + q] = kr * cd(qR); A[C3 * pl + q] = kr * cd(qL);
         A[C4 * pl + q] = cd(); A[C5 * pl + q] = cd();
@@ -275,8 +243,165 @@ __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __res
     }
 }
 
-// level-0 operator of field c's preconditioner hierarchy: its own 5-point block
-// (couplings leaving the box dropped)
+// boundary surgery of one list (list = 4 field + side; fields Ex, Er, Ephi;
+// sides W, E, S, N), one entry (i, j, code) per thread, after
+// emfieldModule.hpp:2456-2784.  Codes the reference does not define for a list
+// leave the row as it is, as there.  jflc is gc.j_flc_bl[0][0], which the Er
+// south code 3 compares with the cell radius (:2672).
+__global__ void k_m3_bc(Dev3 D, const int* __restrict__ ent, int n, int list, const double* __restrict__ epsr,
+                        cth_mw_params prm, double jflc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = ent[3 * k], j = ent[3 * k + 1], code = ent[3 * k + 2];
+    const int ld = D.ld;
+    const size_t pl = D.pl, q = (size_t)j * ld + i;
+    const int c = list >> 2, side = list & 3;
+    cd* A = D.a + (size_t)c * NQ * pl + q;
+    const double dx = prm.dx, dr = prm.dr, w = prm.omegam;
+    auto r = [&](int jj) { return prm.rmin + (jj - 0.5) * dr; };
+#define AT(slot) A[(size_t)(slot) * pl]
+    if (c == 0) {
+        const double qL = (r(j - 1) + r(j)) / 2.0 / (r(j) + 1e-100), qR = (r(j + 1) + r(j)) / 2.0 / (r(j) + 1e-100);
+        if (side == 0) {  // :2458-2489
+            const cd a = AT(QW);
+            if (code == 0) {
+                AT(QW) = cd();
+            } else if (code == 2) {
+                AT(QP) -= a; AT(C2) += mulr(divr(mulr(a, dx), dr), qR); AT(C3) -= mulr(divr(mulr(a, dx), dr), qL);
+                AT(QW) = cd();
+            } else if (code == 3) {
+                const double deno = 1.0 + dx / dr * qL;
+                AT(QP) -= divr(a, deno); AT(C2) += divr(mulr(a, dx / dr * qR), deno); AT(QW) = cd();
+            } else if (code == 4) {
+                const double deno = 1.0 + dx / dr * qR;
+                AT(QP) -= divr(a, deno); AT(C3) -= divr(mulr(a, dx / dr * qL), deno); AT(QW) = cd();
+            }
+        } else if (side == 1) {  // :2491-2514
+            const cd a = AT(QE);
+            if (code == 0) {
+                AT(QE) = cd();
+            } else if (code == 2) {
+                AT(QP) -= a; AT(C0) -= mulr(divr(mulr(a, dx), dr), qR); AT(C1) += mulr(divr(mulr(a, dx), dr), qL);
+                AT(QE) = cd();
+            } else if (code == 4) {
+                const double deno = 1.0 + dx / dr * qR;
+                AT(QP) -= divr(a, deno); AT(C1) += divr(mulr(a, dx / dr * qL), deno); AT(QE) = cd();
+            }
+        } else if (side == 2) {  // :2516-2531
+            const cd a = AT(QS);
+            if (code == 0) {
+                AT(QP) += mulr(a, r(j) / r(j - 1)); AT(QS) = cd();
+            } else if (code == 6) {
+                const double rR = (r(j + 1) + r(j)) / 2.0, rL = (r(j) + r(j - 1)) / 2.0;
+                AT(QP) -= mulr(a, dr / dx * r(j) / rL); AT(QW) += mulr(a, -dr / dx * r(j) / rL);
+                AT(C2) += mulr(a, rR / rL); AT(QS) = cd();
+            }
+        } else {  // :2533-2571
+            const cd a = AT(QN);
+            const double rR = (r(j + 1) + r(j)) / 2.0, rL = (r(j) + r(j - 1)) / 2.0;
+            if (code == 0) {
+                AT(QP) += mulr(a, r(j) / r(j + 1)); AT(QN) = cd();
+            } else if (code == 1) {
+                AT(QP) -= a * open_rad((epsr[q] + epsr[q - 1]) / 2.0, w, dr, r(j), r(j + 1)); AT(QN) = cd();
+            } else if (code == 5) {
+                AT(QP) -= mulr(a, dr / dx * r(j) / rR); AT(QE) += mulr(a, -dr / dx * r(j) / rR);
+                AT(C1) += mulr(a, rL / rR); AT(QN) = cd();
+            } else if (code == 6) {
+                AT(QP) -= mulr(a, dr / dx * r(j) / rR); AT(QW) += mulr(a, -dr / dx * r(j) / rR);
+                AT(C3) += mulr(a, -rL / rR); AT(QN) = cd();
+            }
+        }
+    } else if (c == 1) {
+        const double eps_t = (epsr[q] + epsr[q - ld]) / 2.0;
+        if (side == 0) {  // :2574-2622
+            const cd a = AT(QW);
+            if (code == 0) {
+                AT(QP) += a; AT(QW) = cd();
+            } else if (code == 1) {
+                AT(QP) -= a * open_z(eps_t, w, dx); AT(QW) = cd();
+            } else if (code == 5) {
+                const double rR = (r(j + 1) + r(j)) / 2.0, rL = (r(j) + r(j - 1)) / 2.0;
+                AT(QP) -= mulr(a, dx / dr * rL / r(j)); AT(QN) += mulr(a, -dx / dr * rR / r(j));
+                AT(C0) += mulr(a, -1.0); AT(QW) = cd();
+            } else if (code == 6) {
+                const double rR = (r(j) + r(j - 1)) / 2.0, rL = (r(j - 1) + r(j - 2)) / 2.0;
+                AT(QP) -= mulr(a, dx / dr * rR / r(j - 1)); AT(QS) += mulr(a, -dx / dr * rL / r(j - 1));
+                AT(C1) += mulr(a, 1.0); AT(QW) = cd();
+            } else if (code == 7) {  // port excitation (:2606-2621)
+                const double c0 = sqrt(1.0 / (kEPS0 * eps_t * kMU0));
+                const cd deno(2.0 * c0 + 1e-100, w * dx);
+                const cd Rq(2.0 * c0, -w * dx);
+                const double rt = (r(j) + r(j - 1)) / 2.0;
+                const cd S = cd(0.0, 4.0 * w * dx) * cd(prm.J1r_exc / rt / log(prm.r2 / prm.r1) * 1e3);
+                AT(QP) -= cdiv(a * Rq, deno);
+                D.b[pl + q] += cdiv(a * S, deno);
+                AT(QW) = cd();
+            }
+        } else if (side == 1) {  // :2624-2656
+            const cd a = AT(QE);
+            if (code == 0) {
+                AT(QP) += a; AT(QE) = cd();
+            } else if (code == 1) {
+                const double c0 = sqrt(1.0 / (kEPS0 * eps_t * kMU0));
+                const double deno = (2.0 * c0) * (2.0 * c0) + (w * dx) * (w * dx);
+                const cd R((2.0 * c0) * (2.0 * c0) - (w * dx) * (w * dx), -4.0 * c0 * w * dx);
+                AT(QP) -= divr(a * R, deno + 1e-100); AT(QE) = cd();
+            } else if (code == 5) {
+                const double rR = (r(j + 1) + r(j)) / 2.0, rL = (r(j) + r(j - 1)) / 2.0;
+                AT(QP) -= mulr(a, dx / dr * rL / r(j)); AT(QN) += mulr(a, -dx / dr * rR / r(j));
+                AT(C2) += mulr(a, 1.0); AT(QE) = cd();
+            }
+        } else if (side == 2) {  // :2658-2681
+            const cd a = AT(QS);
+            const double rR = (r(j) + r(j - 1)) / 2.0, rL = (r(j - 1) + r(j - 2)) / 2.0;
+            const cd g = divr(mulr(divr(mulr(a, dr), dx), r(j - 1)), rL);
+            if (code == 2) {
+                AT(QP) -= divr(mulr(a, rR), rL); AT(C1) += g; AT(C3) -= g; AT(QS) = cd();
+            } else if (code == 3) {
+                double deno = dr / dx * r(j - 1) / rL;
+                if (r(j) < jflc) deno = 1.0;
+                AT(QP) -= divr(divr(mulr(a, rR), rL), deno); AT(C0) += divr(g, deno); AT(QS) = cd();
+            }
+        } else {  // :2683-2711
+            const cd a = AT(QN);
+            const double rR = (r(j + 1) + r(j)) / 2.0, rL = (r(j) + r(j - 1)) / 2.0;
+            const cd g = divr(mulr(divr(mulr(a, dr), dx), r(j)), rR);
+            if (code == 2) {
+                AT(QP) -= divr(mulr(a, rL), rR); AT(C0) -= g; AT(C2) += g; AT(QN) = cd();
+            } else if (code == 3 || code == 4) {
+                const double deno = dr / dx * r(j) / rR;
+                AT(QP) -= divr(divr(mulr(a, rL), rR), deno);
+                if (code == 3) AT(C1) -= divr(g, deno);
+                else AT(C3) += divr(g, deno);
+                AT(QN) = cd();
+            }
+        }
+    } else {
+        if (side == 0) {  // :2713-2730
+            const cd a = AT(QW);
+            if (code == 0) {
+                AT(QP) += a; AT(QW) = cd();
+            } else if (code == 1) {
+                AT(QP) -= a * open_z(epsr[q], w, dx); AT(QW) = cd();
+            }
+        } else if (side == 1) {  // :2731-2739
+            if (code == 0) { AT(QP) += AT(QE); AT(QE) = cd(); }
+        } else if (side == 2) {  // :2741-2749
+            if (code == 0) { AT(QP) += mulr(AT(QS), r(j) / r(j - 1)); AT(QS) = cd(); }
+        } else {  // :2751-2784
+            const cd a = AT(QN);
+            if (code == 0) {
+                AT(QP) += mulr(a, r(j) / r(j + 1)); AT(QN) = cd();
+            } else if (code == 1) {
+                AT(QP) -= a * open_rad(epsr[q], w, dr, r(j), r(j + 1)); AT(QN) = cd();
+            }
+        }
+    }
+#undef AT
+}
+
+// level-0 operator of field c's preconditioner hierarchy: its own 5-point block,
+// couplings to non-unknowns dropped, identity rows off the unknowns
 __global__ void k_m3_block(Dev3 D, int c, cd* __restrict__ a0, int i0, int j0, int ncol, int nrow, int ldl) {
     const int cc = blockIdx.x * blockDim.x + threadIdx.x;
     const int rr = blockIdx.y;
@@ -285,11 +410,20 @@ __global__ void k_m3_block(Dev3 D, int c, cd* __restrict__ a0, int i0, int j0, i
     const int i = cc + i0, j = rr + j0;
     const size_t pl = D.pl, q = (size_t)j * D.ld + i;
     const cd* A = D.a + (size_t)c * NQ * pl;
-    a0[P * n0 + p] = A[QP * pl + q];
-    a0[W * n0 + p] = cc > 0 ? A[QW * pl + q] : cd();
-    a0[E * n0 + p] = cc + 1 < ncol ? A[QE * pl + q] : cd();
-    a0[S * n0 + p] = rr > 0 ? A[QS * pl + q] : cd();
-    a0[N * n0 + p] = rr + 1 < nrow ? A[QN * pl + q] : cd();
+    const unsigned char* mk = D.mk[c];
+    cd vP(1.0), vW, vE, vS, vN;
+    if (mk[q]) {
+        vP = A[QP * pl + q];
+        if (cc > 0 && mk[q - 1]) vW = A[QW * pl + q];
+        if (cc + 1 < ncol && mk[q + 1]) vE = A[QE * pl + q];
+        if (rr > 0 && mk[q - D.ld]) vS = A[QS * pl + q];
+        if (rr + 1 < nrow && mk[q + D.ld]) vN = A[QN * pl + q];
+    }
+    a0[P * n0 + p] = vP;
+    a0[W * n0 + p] = vW;
+    a0[E * n0 + p] = vE;
+    a0[S * n0 + p] = vS;
+    a0[N * n0 + p] = vN;
 }
 
 // r = rh = b, x = p = v = 0 on the unknowns; ||b||^2 and the recurrence's start
@@ -301,8 +435,8 @@ __global__ void k_m3_prep(Dev3 D, const Args3* __restrict__ args, double* __rest
     double bb = 0.0;
     if (i <= D.ni) {
         for (int c = 0; c < 3; c++) {
-            if (!unknown(c, i, j, D.ni, D.nj)) continue;
             const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+            if (!D.mk[c][q - (size_t)c * D.pl]) continue;
             const cd b = D.b[q];
             D.r[q] = b; D.rh[q] = b;
             D.x[q] = cd(); D.p[q] = cd(); D.v[q] = cd();
@@ -339,8 +473,9 @@ __global__ void k_m3_vec(Dev3 D, Lev0 L) {
     if (i > D.ni) return;
     const cd beta = sc_c(D.sc, BETA), omega = sc_c(D.sc, OMEGA), alpha = sc_c(D.sc, ALPHA);
     for (int c = 0; c < 3; c++) {
-        if (!unknown(c, i, j, D.ni, D.nj)) continue;
-        const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+        const size_t q0 = (size_t)j * D.ld + i;
+        if (!D.mk[c][q0]) continue;
+        const size_t q = (size_t)c * D.pl + q0;
         cd y;
         if (MODE == 0) {
             y = D.r[q] + beta * (D.p[q] - omega * D.v[q]);
@@ -359,8 +494,9 @@ __global__ void k_m3_gather(Dev3 D, Lev0 L, cd* __restrict__ dst) {
     const int j = 1 + blockIdx.y;
     if (i > D.ni) return;
     for (int c = 0; c < 3; c++) {
-        if (!unknown(c, i, j, D.ni, D.nj)) continue;
-        dst[(size_t)c * D.pl + (size_t)j * D.ld + i] = L.x[c][(size_t)(j - L.j0[c]) * L.ldl[c] + (i - L.i0[c])];
+        const size_t q0 = (size_t)j * D.ld + i;
+        if (!D.mk[c][q0]) continue;
+        dst[(size_t)c * D.pl + q0] = L.x[c][(size_t)(j - L.j0[c]) * L.ldl[c] + (i - L.i0[c])];
     }
 }
 
@@ -373,8 +509,8 @@ __global__ void k_m3_mv(Dev3 D, double* __restrict__ part, unsigned int* counter
     double acc[3] = {0.0, 0.0, 0.0};
     if (i <= D.ni) {
         for (int c = 0; c < 3; c++) {
-            if (!unknown(c, i, j, D.ni, D.nj)) continue;
             const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+            if (!D.mk[c][q - (size_t)c * D.pl]) continue;
             if (MODE == 0) {
                 const cd y = apply3(D, D.ph, c, i, j);
                 D.v[q] = y;
@@ -420,8 +556,8 @@ __global__ void k_m3_upd(Dev3 D, const Args3* __restrict__ args, double* __restr
     if (i <= D.ni) {
         const cd alpha = sc_c(D.sc, ALPHA), omega = sc_c(D.sc, OMEGA);
         for (int c = 0; c < 3; c++) {
-            if (!unknown(c, i, j, D.ni, D.nj)) continue;
             const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+            if (!D.mk[c][q - (size_t)c * D.pl]) continue;
             D.x[q] = D.x[q] + alpha * D.ph[q] + omega * D.sh[q];
             const cd rn = D.s[q] - omega * D.t[q];
             D.r[q] = rn;
@@ -474,7 +610,7 @@ __global__ void k_m3_mask(Dev3 D, const cd* __restrict__ src, cd* __restrict__ d
     if (i >= D.ld) return;
     for (int c = 0; c < 3; c++) {
         const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
-        dst[q] = unknown(c, i, j, D.ni, D.nj) ? src[q] : cd();
+        dst[q] = D.mk[c][q - (size_t)c * D.pl] ? src[q] : cd();
     }
 }
 
@@ -485,7 +621,7 @@ __global__ void k_m3_apply(Dev3 D, const cd* __restrict__ x, cd* __restrict__ y)
     if (i >= D.ld) return;
     for (int c = 0; c < 3; c++) {
         const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
-        y[q] = unknown(c, i, j, D.ni, D.nj) ? apply3(D, x, c, i, j) : cd();
+        y[q] = D.mk[c][q - (size_t)c * D.pl] ? apply3(D, x, c, i, j) : cd();
     }
 }
 
@@ -521,6 +657,17 @@ struct cth_mw3 {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int n_pre = 0, n_body = 0, n_post = 0;      // kernels per section of the graph
+    // unknowns (host copies of the grids' masks, [i * (nj + 2) + j]) and the
+    // boundary lists: (i, j, code) entries of the 12 lists back to back
+    std::vector<unsigned char> hmask[3];
+    int* lst = nullptr;
+    size_t lst_cap = 0;
+    int cnt[12] = {}, off[12] = {};
+    double jflc = 0.0;
+    bool has_bc = false;
+    // rectangle: its lists follow the port radii and cell size of each assembly
+    bool rect = false;
+    double rect_key[4] = {0.0, 0.0, 0.0, 0.0};
 };
 
 namespace {
@@ -532,6 +679,7 @@ Dev3 dev3(cth_mw3* m) {
     cd** f[9] = {&D.x, &D.r, &D.rh, &D.p, &D.ph, &D.v, &D.s, &D.sh, &D.t};
     for (int k = 0; k < 9; k++) *f[k] = m->vec + (size_t)k * 3 * m->pl;
     D.sc = m->sc;
+    for (int c = 0; c < 3; c++) D.mk[c] = m->g[c]->mask_full;
     D.ni = m->ni;
     D.nj = m->nj;
     D.ld = m->ld;
@@ -575,6 +723,7 @@ void destroy(cth_mw3* m) {
     if (m->graph) cudaGraphDestroy(m->graph);
     if (m->d_args) cudaFree(m->d_args);
     if (m->h_args) cudaFreeHost(m->h_args);
+    if (m->lst) cudaFree(m->lst);
     delete m;
 }
 
@@ -703,13 +852,97 @@ int build_graph(cth_mw3* m) {
     return CTH_OK;
 }
 
+// the lists into device memory (set-up time: waits for the device first, since
+// earlier assemblies may still read the old lists)
+int upload_lists(cth_mw3* m, const std::vector<int>& ent, const int cnt[12]) {
+    CTH_CUDA(cudaDeviceSynchronize());
+    const size_t n = ent.size() / 3;
+    if (n > m->lst_cap) {
+        if (m->lst) cudaFree(m->lst);
+        m->lst = nullptr;
+        m->lst_cap = 0;
+        CTH_CUDA(cudaMalloc(&m->lst, n * 3 * sizeof(int)));
+        m->lst_cap = n;
+    }
+    if (n) CTH_CUDA(cudaMemcpy(m->lst, ent.data(), n * 3 * sizeof(int), cudaMemcpyHostToDevice));
+    int o = 0;
+    for (int L = 0; L < 12; L++) {
+        m->cnt[L] = cnt[L];
+        m->off[L] = o;
+        o += cnt[L];
+    }
+    m->has_bc = true;
+    m->assembled = false;
+    return CTH_OK;
+}
+
+// the rectangle's walls as the 12 lists (port code 7 on the z = 0 Er faces with
+// r1 <= r <= r2, else 1), rebuilt when the cell size or port radii change
+int rect_lists(cth_mw3* m, const cth_mw_params* prm, cudaStream_t s) {
+    const double key[4] = {prm->dr, prm->rmin, prm->r1, prm->r2};
+    if (m->has_bc && std::memcmp(key, m->rect_key, sizeof(key)) == 0) return CTH_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CTH_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+        set_error("cth_mw3_assemble_dev: the rectangle's boundary lists change (new cell size or port radii) "
+                  "inside a stream capture");
+        return CTH_ERR_ARG;
+    }
+    const int ni = m->ni, nj = m->nj;
+    std::vector<int> L[12];
+    auto put = [&](int l, int i, int j, int code) { L[l].insert(L[l].end(), {i, j, code}); };
+    auto r = [&](int jj) { return prm->rmin + (jj - 0.5) * prm->dr; };
+    for (int j = 1; j <= nj; j++) {
+        put(0, 2, j, 2);   // Ex W: Gauss
+        put(1, ni, j, 2);  // Ex E: Gauss
+        put(8, 1, j, 1);   // Ephi W: open
+        put(9, ni, j, 0);  // Ephi E: conductor
+    }
+    for (int j = 2; j <= nj; j++) {
+        const double rt = (r(j) + r(j - 1)) / 2.0;
+        put(4, 1, j, (rt >= prm->r1 && rt <= prm->r2) ? 7 : 1);  // Er W: port or open
+        put(5, ni, j, 1);                                         // Er E: open
+    }
+    for (int i = 1; i <= ni; i++) {
+        put(7, i, nj, 2);                // Er N: Gauss
+        if (i >= 2) put(3, i, nj, 0);    // Ex N: conductor
+        put(11, i, nj, 0);               // Ephi N: conductor
+    }
+    std::vector<int> ent;
+    int cnt[12];
+    for (int l = 0; l < 12; l++) {
+        ent.insert(ent.end(), L[l].begin(), L[l].end());
+        cnt[l] = (int)L[l].size() / 3;
+    }
+    const int rc = upload_lists(m, ent, cnt);
+    if (rc == CTH_OK) std::memcpy(m->rect_key, key, sizeof(key));
+    return rc;
+}
+
 }  // namespace
 
 extern "C" {
 
-int cth_mw3_create(int ni, int nj, int device, cth_mw3** out) {
-    if (!out || ni < 4 || nj < 4) {
-        set_error("cth_mw3_create: invalid arguments (ni, nj >= 4)");
+int cth_mw3_create_blocks(int ni, int nj, const int* xi_bl, const int* xj_bl, int nx_bl, const int* ri_bl,
+                          const int* rj_bl, int nr_bl, const int* ci_bl, const int* cj_bl, int nc_bl, int device,
+                          cth_mw3** out) {
+    const int* ib[3] = {xi_bl, ri_bl, ci_bl};
+    const int* jb[3] = {xj_bl, rj_bl, cj_bl};
+    const int nb[3] = {nx_bl, nr_bl, nc_bl};
+    bool ok = out && ni >= 4 && nj >= 4;
+    // every unknown inside [1, ni] x [1, nj] (the stencils read one ghost layer);
+    // Er faces above the axis face (j >= 2)
+    for (int c = 0; c < 3 && ok; c++) {
+        ok = ib[c] && jb[c] && nb[c] >= 1;
+        for (int b = 0; b < nb[c] && ok; b++) {
+            const int a0 = ib[c][2 * b], a1 = ib[c][2 * b + 1], b0 = jb[c][2 * b], b1 = jb[c][2 * b + 1];
+            if (a0 > a1 || b0 > b1) continue;  // empty block
+            ok = a0 >= 1 && a1 <= ni && b0 >= (c == 1 ? 2 : 1) && b1 <= nj;
+        }
+    }
+    if (!ok) {
+        set_error("cth_mw3_create_blocks: invalid arguments (ni, nj >= 4; blocks inside [1, ni] x [1, nj], "
+                  "Er blocks from j = 2)");
         return CTH_ERR_ARG;
     }
     *out = nullptr;
@@ -717,10 +950,12 @@ int cth_mw3_create(int ni, int nj, int device, cth_mw3** out) {
     m->device = device;
     m->ni = ni;
     m->nj = nj;
-    const int boxes[3][4] = {{2, ni, 1, nj}, {1, ni, 2, nj}, {1, ni, 1, nj}};
     for (int c = 0; c < 3; c++) {
-        const int ib[2] = {boxes[c][0], boxes[c][1]}, jb[2] = {boxes[c][2], boxes[c][3]};
-        const int rc = cth_grid_create(ni, nj, ib, jb, 1, device, &m->g[c]);
+        m->hmask[c].assign((size_t)(ni + 2) * (nj + 2), 0);
+        for (int b = 0; b < nb[c]; b++)
+            for (int i = ib[c][2 * b]; i <= ib[c][2 * b + 1]; i++)
+                for (int j = jb[c][2 * b]; j <= jb[c][2 * b + 1]; j++) m->hmask[c][(size_t)i * (nj + 2) + j] = 1;
+        const int rc = cth_grid_create(ni, nj, ib[c], jb[c], nb[c], device, &m->g[c]);
         if (rc != CTH_OK) {
             destroy(m);
             return rc;
@@ -734,14 +969,14 @@ int cth_mw3_create(int ni, int nj, int device, cth_mw3** out) {
     m->ld = m->g[2]->ld;
     m->pl = m->g[2]->plane;
     const size_t pl = m->pl;
-    const int nb = ((ni + 127) / 128) * nj;
+    const int nparts = ((ni + 127) / 128) * nj;
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMalloc(&m->a, (size_t)3 * NQ * pl * sizeof(cd));
     if (e == cudaSuccess) e = cudaMalloc(&m->b, (size_t)3 * pl * sizeof(cd));
     if (e == cudaSuccess) e = cudaMalloc(&m->vec, (size_t)27 * pl * sizeof(cd));
     if (e == cudaSuccess) e = cudaMalloc(&m->tmp, (size_t)3 * pl * sizeof(cd));
     if (e == cudaSuccess) e = cudaMalloc(&m->sc, NWORDS * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&m->part, (size_t)(3 * nb + 8) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&m->part, (size_t)(3 * nparts + 8) * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&m->counter, sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMallocHost(&m->h_sc, NWORDS * sizeof(double));
     if (e == cudaSuccess) e = cudaMemset(m->a, 0, (size_t)3 * NQ * pl * sizeof(cd));
@@ -764,6 +999,57 @@ int cth_mw3_create(int ni, int nj, int device, cth_mw3** out) {
         return cuda_fail(e, "cth_mw3_create");
     }
     *out = m;
+    return CTH_OK;
+}
+
+int cth_mw3_create(int ni, int nj, int device, cth_mw3** out) {
+    if (!out || ni < 4 || nj < 4) {
+        set_error("cth_mw3_create: invalid arguments (ni, nj >= 4)");
+        return CTH_ERR_ARG;
+    }
+    const int xi[2] = {2, ni}, xj[2] = {1, nj}, ri[2] = {1, ni}, rj[2] = {2, nj}, ci[2] = {1, ni}, cj[2] = {1, nj};
+    const int rc = cth_mw3_create_blocks(ni, nj, xi, xj, 1, ri, rj, 1, ci, cj, 1, device, out);
+    if (rc == CTH_OK) (*out)->rect = true;
+    return rc;
+}
+
+int cth_mw3_set_boundary(cth_mw3* m, const cth_bc_list* lists, int j_flc_00) {
+    if (!m || !lists) {
+        set_error("cth_mw3_set_boundary: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    const int nj2 = m->nj + 2;
+    std::vector<int> ent;
+    int cnt[12];
+    std::vector<int> seen((size_t)(m->ni + 2) * nj2, -1);
+    for (int L = 0; L < 12; L++) {
+        const cth_bc_list& l = lists[L];
+        if (l.n < 0 || (l.n > 0 && (!l.i || !l.j || !l.code))) {
+            set_error("cth_mw3_set_boundary: list with a negative length or a null array");
+            return CTH_ERR_ARG;
+        }
+        const std::vector<unsigned char>& hm = m->hmask[L >> 2];
+        for (int k = 0; k < l.n; k++) {
+            const int i = l.i[k], j = l.j[k], code = l.code[k];
+            const bool ok = i >= 1 && i <= m->ni && j >= 1 && j <= m->nj && code >= 0 && code <= 7 &&
+                            hm[(size_t)i * nj2 + j] && seen[(size_t)i * nj2 + j] != L;
+            if (!ok) {
+                set_error("cth_mw3_set_boundary: an entry is not an unknown of its field, repeats within its list, "
+                          "or has a code outside 0-7");
+                return CTH_ERR_ARG;
+            }
+            seen[(size_t)i * nj2 + j] = L;
+            ent.push_back(i);
+            ent.push_back(j);
+            ent.push_back(code);
+        }
+        cnt[L] = l.n;
+    }
+    CTH_CUDA(cudaSetDevice(m->device));
+    const int rc = upload_lists(m, ent, cnt);
+    if (rc != CTH_OK) return rc;
+    m->jflc = (double)j_flc_00;
+    m->rect = false;
     return CTH_OK;
 }
 
@@ -794,15 +1080,29 @@ int cth_mw3_assemble_dev(cth_mw3* m, const double* ne, const double* nu, const d
                          const double* epsr, const cth_mw_params* prm, void* stream) {
     if (!m || !ne || !nu || !Bx || !Br || !epsr || !prm || prm->dx <= 0.0 || prm->dr <= 0.0 ||
         prm->rmin != 0.0 || !(prm->r2 > prm->r1) || prm->r1 <= 0.0 || prm->omegam <= 0.0 || prm->masse <= 0.0) {
-        set_error("cth_mw3_assemble_dev: invalid arguments (the rectangle starts on the axis: rmin = 0)");
+        set_error("cth_mw3_assemble_dev: invalid arguments (the domain starts on the axis: rmin = 0)");
         return CTH_ERR_ARG;
     }
     CTH_CUDA(cudaSetDevice(m->device));
     cudaStream_t s = (cudaStream_t)stream;
+    if (m->rect) {
+        const int rc = rect_lists(m, prm, s);
+        if (rc != CTH_OK) return rc;
+    } else if (!m->has_bc) {
+        set_error("cth_mw3_assemble_dev: boundary lists not set (cth_mw3_set_boundary)");
+        return CTH_ERR_ARG;
+    }
     Dev3 D = dev3(m);
     dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
     k_m3_assemble<<<grd, blk, 0, s>>>(ne, nu, Bx, Br, epsr, *prm, D);
     m->launches++;
+    // the lists in the reference's order; entries of one list are distinct rows
+    for (int L = 0; L < 12; L++) {
+        if (m->cnt[L] == 0) continue;
+        k_m3_bc<<<(m->cnt[L] + 127) / 128, 128, 0, s>>>(D, m->lst + 3 * (size_t)m->off[L], m->cnt[L], L, epsr, *prm,
+                                                         m->jflc);
+        m->launches++;
+    }
     CTH_CUDA(cudaGetLastError());
     m->assembled = true;
     return CTH_OK;

@@ -297,20 +297,48 @@ def solver_SOR(aP, aE, aW, aN, aS, b, i_bl, j_bl, n_bl, alpha_SOR, maxITR, error
 
 class Microwave3:
     """The magnetised 3-component microwave system of solve_Microwave
-    (include/emfieldModule.hpp:2249-2998) on the r-z rectangle (cth_mw3):
-    device assembly, the coupled operator and the preconditioned BiCGStab
-    solve.  Field planes are torch complex128 of shape (3, nj+2, ld): Ex, Er,
-    Ephi in the library layout."""
+    (include/emfieldModule.hpp:2249-2998) (cth_mw3): device assembly, the
+    coupled operator and the preconditioned BiCGStab solve.  Field planes are
+    torch complex128 of shape (3, nj+2, ld): Ex, Er, Ephi in the library layout.
+
+    blocks=None is the r-z rectangle with its walls' boundary lists; otherwise
+    blocks = ((xi_bl, xj_bl), (ri_bl, rj_bl), (ci_bl, cj_bl)), the x-face,
+    r-face and cell block tables ([n_bl][2] each), and the boundary lists follow
+    with set_boundary."""
 
     NQ = 11
+    FIELDS, SIDES = "xrp", "WESN"
 
-    def __init__(self, ni: int, nj: int, device: int = 0):
+    def __init__(self, ni: int, nj: int, device: int = 0, blocks=None):
         L = capi.load()
         h = ctypes.c_void_p()
-        capi.check(L.cth_mw3_create(ni, nj, device, ctypes.byref(h)), allow_positive=False)
+        if blocks is None:
+            capi.check(L.cth_mw3_create(ni, nj, device, ctypes.byref(h)), allow_positive=False)
+        else:
+            tabs = [np.ascontiguousarray(np.asarray(t, dtype=np.int32).reshape(-1, 2)) for pair in blocks for t in pair]
+            args = []
+            for f in range(3):
+                ib, jb = tabs[2 * f], tabs[2 * f + 1]
+                if ib.shape != jb.shape:
+                    raise ValueError("i and j block tables of a field differ in length")
+                args += [ib.ctypes.data, jb.ctypes.data, ib.shape[0]]
+            capi.check(L.cth_mw3_create_blocks(ni, nj, *args, device, ctypes.byref(h)), allow_positive=False)
         self._h, self._L = h, L
         self.ni, self.nj, self.device = ni, nj, device
         self.ld = L.cth_mw3_ld(h)
+
+    def set_boundary(self, lists: dict, j_flc_00: int):
+        """lists[(field, side)] = sequence of (i, j, code), field in "xrp" (Ex,
+        Er, Ephi), side in "WESN": the 12 lists of MicrowaveBC
+        (include/arrays.hpp:649) as makeBoundary builds them; j_flc_00 =
+        gc.j_flc_bl[0][0]."""
+        keep, arr = [], (capi.BCList * 12)()
+        for k, (f, sd) in enumerate((f, sd) for f in self.FIELDS for sd in self.SIDES):
+            e = np.asarray(lists.get((f, sd), []), dtype=np.int32).reshape(-1, 3)
+            cols = [np.ascontiguousarray(e[:, c]) for c in range(3)]
+            keep += cols
+            arr[k] = capi.BCList(cols[0].ctypes.data, cols[1].ctypes.data, cols[2].ctypes.data, e.shape[0])
+        capi.check(self._L.cth_mw3_set_boundary(self._h, arr, int(j_flc_00)), allow_positive=False)
 
     def close(self):
         if getattr(self, "_h", None):

@@ -213,19 +213,46 @@ int cth_mw_er_assemble_dev(cth_grid* g, const double* ne, const double* nu, cons
 /* Magnetised 3-component microwave system of solve_Microwave
  * (include/emfieldModule.hpp:2249-2998): Ex on x-faces, Er on r-faces, Ephi on
  * cells, coupled through the magnetised cold-plasma conductivity (11-point
- * rows, :2300-2453), on the r-z rectangle r in [0, R] (prm->rmin must be 0),
- * z in [0, L], with the reference's boundary codes: Ex Gauss (2) at z = 0, L
- * and conductor (0) at r = R; Er port (7) on [r1, r2] at z = 0, open (1) on
- * the other z = 0 faces and at z = L, Gauss (2) at r = R; Ephi open (1) at
- * z = 0, conductor (0) at z = L and r = R.  Unknowns: Ex i = 2..ni, j = 1..nj;
- * Er i = 1..ni, j = 2..nj; Ephi i = 1..ni, j = 1..nj.  Replaces the assembly of
- * :2785-2990 and the Eigen SparseLU factorisation (:2995-2998) by complex FP64
- * BiCGStab, right-preconditioned block-diagonally by one complex
- * semicoarsening V-cycle per field.
+ * rows, :2300-2453), with the reference's boundary codes 0-7 (:2456-2784).
+ * Replaces the assembly of :2785-2990 and the Eigen SparseLU factorisation
+ * (:2995-2998) by complex FP64 BiCGStab, right-preconditioned block-diagonally
+ * by one complex semicoarsening V-cycle per field.  The domain starts on the
+ * axis (prm->rmin must be 0).
  * Field planes (x3, y3, E3): three consecutive complex planes Ex, Er, Ephi of
  * (nj+2) x ld complex values each (library layout, ld = cth_mw3_ld). */
 typedef struct cth_mw3 cth_mw3;
+/* The r-z rectangle r in [0, R], z in [0, L]: unknowns Ex i = 2..ni,
+ * j = 1..nj; Er i = 1..ni, j = 2..nj; Ephi i = 1..ni, j = 1..nj; boundary lists
+ * of its walls (rebuilt from prm at each assembly): Ex Gauss (2) at z = 0, L and
+ * conductor (0) at r = R; Er port (7) on [r1, r2] at z = 0, open (1) on the
+ * other z = 0 faces and at z = L, Gauss (2) at r = R; Ephi open (1) at z = 0,
+ * conductor (0) at z = L and r = R. */
 int cth_mw3_create(int ni, int nj, int device, cth_mw3** out);
+/* A general geometry: the unknowns of each field are the union of its blocks,
+ * i_bl / j_bl = n_bl pairs [lo, hi] each (inclusive; the x-face, r-face and
+ * cell blocks gx.i_flx_bl, gr.i_flr_bl, gc.i_flc_bl of the reference,
+ * initialModule.hpp:219-345, six blocks on the cathode).  Every block inside
+ * [1, ni] x [1, nj]; Er blocks from j = 2.  Boundary lists follow with
+ * cth_mw3_set_boundary. */
+int cth_mw3_create_blocks(int ni, int nj, const int* xi_bl, const int* xj_bl, int nx_bl, const int* ri_bl,
+                          const int* rj_bl, int nr_bl, const int* ci_bl, const int* cj_bl, int nc_bl, int device,
+                          cth_mw3** out);
+/* One boundary list of MicrowaveBC (include/arrays.hpp:649): the entries
+ * (i[k], j[k], code[k]), k < n, of iBnd / jBnd / sBnd for one side and field. */
+typedef struct cth_bc_list {
+    const int* i;
+    const int* j;
+    const int* code;
+    int n;
+} cth_bc_list;
+/* lists[12]: Ex W, E, S, N (iBndWx .. iBndNx), Er W, E, S, N (iBndWr ..), Ephi
+ * W, E, S, N (iBndWp ..), as InitialModule::makeBoundary builds them
+ * (initialModule.hpp:420-1055), applied at each assembly in that order.  Every
+ * entry must be an unknown of its field, appear once in its list and carry a
+ * code in 0..7 (CTH_ERR_ARG otherwise).  j_flc_00 = gc.j_flc_bl[0][0], which the
+ * reference's Er south code 3 compares with the cell radius (:2672).  Host
+ * arrays; copied (waits for the device). */
+int cth_mw3_set_boundary(cth_mw3* m, const cth_bc_list* lists, int j_flc_00);
 void cth_mw3_destroy(cth_mw3* m);
 int cth_mw3_ld(const cth_mw3* m);
 long long cth_mw3_launch_count(const cth_mw3* m);

@@ -143,3 +143,108 @@ def test_mw3_graph_equals_launches(pkg, cuda_device):
     assert out[True][1] == out[False][1]
     assert np.array_equal(out[True][0], out[False][0])
     g.close()
+
+
+# ---------------------------------------------------------------------------
+# the cathode geometry: six blocks per field and the boundary lists of
+# InitialModule::makeBoundary (the committed segment table, evaluated on the
+# grid's cell blocks)
+# ---------------------------------------------------------------------------
+SLOTS = ({"P": 0, "E": 1, "W": 2, "N": 3, "S": 4, "NE": 5, "SE": 6, "NW": 7, "SW": 8, "EE": 9, "WW": 10},
+         {"P": 0, "E": 1, "W": 2, "N": 3, "S": 4, "NE": 5, "SE": 6, "NW": 7, "SW": 8, "NN": 9, "SS": 10},
+         {"P": 0, "E": 1, "W": 2, "N": 3, "S": 4, "EE": 5, "WW": 6, "NN": 7, "SS": 8})
+
+
+def _cathode(pkg, ni=194, nj=70, bmax=0.05, seed=2):
+    import json
+    import os
+    from oracle import microwave as mw
+    w = pkg.workloads.mw3_cathode(ni, nj, seed=seed, bmax=bmax)
+    p = mw.cathode_mw_params(ni, nj)
+    for k in ("dx", "dr", "omegam", "J1r_exc", "r1", "r2", "masse"):
+        assert p[k] == pytest.approx(w["params"][k], rel=1e-15)
+    cells, xf, rf = mw.cathode_mw_blocks(p)
+    masks = (mw.block_mask(ni, nj, *xf), mw.block_mask(ni, nj, *rf), mw.block_mask(ni, nj, *cells))
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "mw_lists_cathode.json")) as f:
+        lists = mw.cathode_mw_lists(cells, json.load(f))
+    jflc = int(cells[1][0][0])
+    ref = mw.mag_system_lists(w["ne"], w["nu"], w["Bx"], w["Br"], w["epsr"], p, masks, lists, jflc)
+    m = pkg.Microwave3(ni, nj, blocks=(xf, rf, cells))
+    m.set_boundary(lists, jflc)
+    g, planes = _device(pkg, w)
+    m.assemble_dev(*planes, w["params"])
+    return w, mw, ref, m, g
+
+
+def test_mw3_cathode_assembly_matches_oracle(pkg, cuda_device):
+    ni, nj = 194, 70
+    w, mw, ref, m, g = _cathode(pkg, ni, nj)
+    a, b = m.coefficients()
+    a, b = _to_ij(a, ni), _to_ij(b, ni)
+    for c, comp in enumerate(("x", "r", "p")):
+        for name, want in ref[comp].items():
+            got = a[c, SLOTS[c][name]]
+            scale = np.abs(want).max() + 1e-300
+            assert np.max(np.abs(got - want)) / scale < 1e-12, (comp, name)
+        scale = np.abs(ref["b"][c]).max() + 1e-300
+        assert np.max(np.abs(b[c] - ref["b"][c])) / scale < 1e-12, (comp, "b")
+    assert np.abs(ref["b"][1]).max() > 0.0  # the feed drives Er
+    m.close(); g.close()
+
+
+def test_mw3_cathode_operator_matches_oracle(pkg, cuda_device):
+    import torch
+    ni, nj = 194, 70
+    w, mw, ref, m, g = _cathode(pkg, ni, nj)
+    A, _, _ = mw.mag_rect_matrix(ref)
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal(A.shape[0]) + 1j * rng.standard_normal(A.shape[0])
+    fields = mw.mag_unpack(ref, x)
+    x3 = m.planes(3)
+    for c in range(3):
+        full = fields[c] + (~ref["masks"][c]) * (1.0 + 1.0j)  # junk off the unknowns is ignored
+        x3[c, :, :ni + 2] = torch.from_numpy(np.ascontiguousarray(full.T)).to(x3.device)
+    y = _to_ij(m.apply_dev(x3), ni)
+    y_ref = mw.mag_unpack(ref, A @ x)
+    for c in range(3):
+        assert _rel(y[c], y_ref[c]) < 1e-13, c
+        assert np.all(y[c][~ref["masks"][c]] == 0)
+    m.close(); g.close()
+
+
+@pytest.mark.parametrize("bmax", [0.05, 0.0, 0.2])
+def test_mw3_cathode_solve_matches_direct(pkg, cuda_device, bmax):
+    """Against the sparse direct solve of the oracle's system on the cathode
+    (194 x 70); bmax = 0.2 T crosses the electron cyclotron resonance."""
+    ni, nj = 194, 70
+    w, mw, ref, m, g = _cathode(pkg, ni, nj, bmax=bmax)
+    E_ref = mw.mag_rect_solve(ref)
+    E, st = m.solve_dev(maxITR=600, error_cnv=1e-12)
+    print("mw3 cathode", bmax, st.as_dict())
+    assert st.converged == 1, st.as_dict()
+    E = _to_ij(E, ni)
+    x, x_ref = mw.mag_pack(ref, E), mw.mag_pack(ref, E_ref)
+    assert _rel(x, x_ref) < 1e-8, (_rel(x, x_ref), st.as_dict())
+    for c in range(3):
+        assert np.all(E[c][~ref["masks"][c]] == 0)
+    if bmax == 0.0:
+        assert np.max(np.abs(E[2])) == 0.0
+    m.close(); g.close()
+
+
+def test_mw3_set_boundary_rejects_bad_lists(pkg, cuda_device):
+    from oracle import microwave as mw
+    ni, nj = 194, 70
+    p = mw.cathode_mw_params(ni, nj)
+    cells, xf, rf = mw.cathode_mw_blocks(p)
+    m = pkg.Microwave3(ni, nj, blocks=(xf, rf, cells))
+    i0, j0 = int(cells[0][0][0]), int(cells[1][0][0])
+    bad = [{("p", "W"): [(i0, j0, 0), (i0, j0, 0)]},          # repeated within a list
+           {("p", "W"): [(1, 1, 0)]},                          # not an unknown (inside the cathode body)
+           {("p", "W"): [(i0, j0, 8)]}]                        # code outside 0..7
+    for lists in bad:
+        with pytest.raises(pkg.capi.CathodeError):
+            m.set_boundary(lists, j0)
+    m.set_boundary({("p", "W"): [(i0, j0, 0)], ("p", "E"): [(i0, j0, 0)]}, j0)  # same row in two lists is fine
+    m.close()
