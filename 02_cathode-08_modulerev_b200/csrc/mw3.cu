@@ -400,6 +400,113 @@ __global__ void k_m3_bc(Dev3 D, const int* __restrict__ ent, int n, int list, co
 #undef AT
 }
 
+// ghost values of one list after the solve (emfieldModule.hpp:3026-3264), one
+// entry per thread, lists in the reference's order.  The ghosts a list writes
+// are no unknowns of their field (checked when the lists are set), so no thread
+// reads a value that another thread of the same list writes; values off the
+// unknowns that a list reads are the ghosts of earlier lists or calls, as in
+// the reference's persistent fields.  er_dc is gr.Er, which the Er east code 1
+// reads, dividing by its deno twice (:3162).
+__global__ void k_m3_ghost(const int* __restrict__ ent, int n, int list, cd* __restrict__ E,
+                           const double* __restrict__ er_dc, const double* __restrict__ epsr, cth_mw_params prm,
+                           double jflc, int ld, size_t pl) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = ent[3 * k], j = ent[3 * k + 1], code = ent[3 * k + 2];
+    const size_t q = (size_t)j * ld + i;
+    const int c = list >> 2, side = list & 3;
+    cd* Ex = E;
+    cd* Er = E + pl;
+    cd* Ep = E + 2 * pl;
+    const double dx = prm.dx, dr = prm.dr, w = prm.omegam;
+    auto r = [&](int jj) { return prm.rmin + (jj - 0.5) * dr; };
+    if (c == 0) {
+        const double qL = (r(j - 1) + r(j)) / 2.0 / (r(j) + 1e-100), qR = (r(j + 1) + r(j)) / 2.0 / (r(j) + 1e-100);
+        if (side == 0) {  // :3028-3053
+            if (code == 0) {
+                Ex[q - 1] = cd();
+            } else if (code == 2) {
+                Ex[q - 1] = Ex[q] + mulr(mulr(Er[q - 1 + ld], qR) - mulr(Er[q - 1], qL), dx / dr);
+            } else if (code == 3) {
+                const double deno = 1.0 + dx / dr * qL;
+                Ex[q - 1] = divr(Ex[q], deno) + divr(mulr(mulr(Er[q - 1 + ld], qR), dx / dr), deno);
+            } else if (code == 4) {
+                const double deno = 1.0 + dx / dr * qR;
+                Ex[q - 1] = divr(Ex[q], deno) - divr(mulr(mulr(Er[q - 1], qL), dx / dr), deno);
+            }
+        } else if (side == 1) {  // :3054-3073
+            if (code == 0) {
+                Ex[q + 1] = cd();
+            } else if (code == 2) {
+                Ex[q + 1] = Ex[q] - mulr(mulr(Er[q + ld], qR) - mulr(Er[q], qL), dx / dr);
+            } else if (code == 4) {
+                const double deno = 1.0 + dx / dr * qR;
+                Ex[q + 1] = divr(Ex[q], deno) + divr(mulr(Er[q], dx / dr * qL), deno);
+            }
+        } else if (side == 2) {  // :3074-3083
+            if (code == 0) Ex[q - ld] = mulr(Ex[q], -r(j) / r(j - 1));
+        } else {  // :3084-3107
+            if (code == 0) Ex[q + ld] = mulr(Ex[q], -r(j) / r(j + 1));
+            else if (code == 1) Ex[q + ld] = open_rad((epsr[q] + epsr[q - 1]) / 2.0, w, dr, r(j), r(j + 1)) * Ex[q];
+        }
+    } else if (c == 1) {
+        const double eps_t = (epsr[q] + epsr[q - ld]) / 2.0;
+        if (side == 0) {  // :3109-3143
+            if (code == 0) {
+                Er[q - 1] = -Er[q];
+            } else if (code == 1) {
+                Er[q - 1] = open_z(eps_t, w, dx) * Er[q];
+            } else if (code == 7) {
+                const double c0 = sqrt(1.0 / (kEPS0 * eps_t * kMU0));
+                const cd deno(2.0 * c0 + 1e-100, w * dx);
+                const cd Rq(2.0 * c0, -w * dx);
+                const double rt = (r(j) + r(j - 1)) / 2.0;
+                const cd S = cd(0.0, 4.0 * w * dx) * cd(prm.J1r_exc / rt / log(prm.r2 / prm.r1) * 1e3);
+                Er[q - 1] = cdiv(Rq, deno) * Er[q] + cdiv(S, deno);
+            }
+        } else if (side == 1) {  // :3144-3166
+            if (code == 0) {
+                Er[q + 1] = -Er[q];
+            } else if (code == 1) {
+                const double c0 = sqrt(1.0 / (kEPS0 * eps_t * kMU0));
+                const double deno = (2.0 * c0) * (2.0 * c0) + (w * dx) * (w * dx);
+                const cd R = divr(cd((2.0 * c0) * (2.0 * c0) - (w * dx) * (w * dx), -4.0 * c0 * w * dx), deno + 1e-100);
+                Er[q + 1] = mulr(divr(R, deno + 1e-100), er_dc[q]);
+            }
+        } else if (side == 2) {  // :3167-3187
+            const double rR = (r(j) + r(j - 1)) / 2.0, rL = (r(j - 1) + r(j - 2)) / 2.0;
+            if (code == 2) {
+                Er[q - ld] = mulr(Er[q], rR / rL) + mulr(Ex[q + 1 - ld] - Ex[q - ld], dr / dx * r(j - 1) / rL);
+            } else if (code == 3) {
+                double deno = dr / dx * r(j - 1) / rL;
+                if (r(j) < jflc) deno = 1.0;
+                Er[q - ld] = divr(mulr(Er[q], rR / rL), deno) + divr(mulr(Ex[q + 1 - ld], dr / dx * r(j - 1) / rL), deno);
+            }
+        } else {  // :3188-3212
+            const double rR = (r(j + 1) + r(j)) / 2.0, rL = (r(j) + r(j - 1)) / 2.0;
+            const double deno = dr / dx * r(j) / rR;
+            if (code == 2)
+                Er[q + ld] = mulr(Er[q], rL / rR) - mulr(Ex[q + 1] - Ex[q], dr / dx * r(j) / rR);
+            else if (code == 3)
+                Er[q + ld] = divr(mulr(Er[q], rL / rR), deno) - divr(mulr(Ex[q + 1], dr / dx * r(j) / rR), deno);
+            else if (code == 4)
+                Er[q + ld] = divr(mulr(Er[q], rL / rR), deno) + divr(mulr(Ex[q], dr / dx * r(j) / rR), deno);
+        }
+    } else {
+        if (side == 0) {  // :3213-3229
+            if (code == 0) Ep[q - 1] = -Ep[q];
+            else if (code == 1) Ep[q - 1] = open_z(epsr[q], w, dx) * Ep[q];
+        } else if (side == 1) {  // :3230-3236, every code
+            Ep[q + 1] = -Ep[q];
+        } else if (side == 2) {  // :3237-3243, every code
+            Ep[q - ld] = mulr(Ep[q], -r(j) / r(j - 1));
+        } else {  // :3244-3264
+            if (code == 0) Ep[q + ld] = mulr(Ep[q], -r(j) / r(j + 1));
+            else if (code == 1) Ep[q + ld] = open_rad(epsr[q], w, dr, r(j), r(j + 1)) * Ep[q];
+        }
+    }
+}
+
 // level-0 operator of field c's preconditioner hierarchy: its own 5-point block,
 // couplings to non-unknowns dropped, identity rows off the unknowns
 __global__ void k_m3_block(Dev3 D, int c, cd* __restrict__ a0, int i0, int j0, int ncol, int nrow, int ldl) {
@@ -592,13 +699,16 @@ __global__ void k_m3_upd(Dev3 D, const Args3* __restrict__ args, double* __restr
     }
 }
 
-// the solution (three planes, zero off the unknowns) into the caller's planes
+// the solution into the caller's planes on the unknowns; entries off the
+// unknowns (ghosts) keep their values, as the reference's fields do
 __global__ void k_m3_store(Dev3 D, const Args3* __restrict__ args) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= D.ld) return;
     for (int c = 0; c < 3; c++) {
-        const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+        const size_t q0 = (size_t)j * D.ld + i;
+        if (!D.mk[c][q0]) continue;
+        const size_t q = (size_t)c * D.pl + q0;
         args->out[q] = D.x[q];
     }
 }
@@ -665,6 +775,8 @@ struct cth_mw3 {
     int cnt[12] = {}, off[12] = {};
     double jflc = 0.0;
     bool has_bc = false;
+    bool ghosts_ok = false;   // no list writes a ghost onto an unknown
+    bool needs_er_dc = false; // the Er east list has code-1 entries (they read gr.Er)
     // rectangle: its lists follow the port radii and cell size of each assembly
     bool rect = false;
     double rect_key[4] = {0.0, 0.0, 0.0, 0.0};
@@ -855,6 +967,23 @@ int build_graph(cth_mw3* m) {
 // the lists into device memory (set-up time: waits for the device first, since
 // earlier assemblies may still read the old lists)
 int upload_lists(cth_mw3* m, const std::vector<int>& ent, const int cnt[12]) {
+    // which ghost each (list, code) writes (emfieldModule.hpp:3026-3264)
+    static const int off_i[4] = {-1, 1, 0, 0}, off_j[4] = {0, 0, -1, 1};
+    static const unsigned char writes[12] = {  // bit per code
+        0x1D, 0x15, 0x01, 0x03, 0x83, 0x03, 0x0C, 0x1C, 0x03, 0xFF, 0xFF, 0x03};
+    bool ok = true, er_dc = false;
+    size_t e = 0;
+    for (int L = 0; L < 12; L++) {
+        const std::vector<unsigned char>& hm = m->hmask[L >> 2];
+        for (int k = 0; k < cnt[L]; k++, e += 3) {
+            const int i = ent[e], j = ent[e + 1], code = ent[e + 2];
+            if (L == 5 && code == 1) er_dc = true;
+            if (!(writes[L] >> code & 1)) continue;
+            if (hm[(size_t)(i + off_i[L & 3]) * (m->nj + 2) + (j + off_j[L & 3])]) ok = false;
+        }
+    }
+    m->ghosts_ok = ok;
+    m->needs_er_dc = er_dc;
     CTH_CUDA(cudaDeviceSynchronize());
     const size_t n = ent.size() / 3;
     if (n > m->lst_cap) {
@@ -1130,6 +1259,40 @@ int cth_mw3_set_graphs(cth_mw3* m, int enable) {
         return CTH_ERR_ARG;
     }
     m->use_graphs = enable != 0;
+    return CTH_OK;
+}
+
+int cth_mw3_fill_ghosts(cth_mw3* m, double* E3, const double* epsr, const double* Er_dc, const cth_mw_params* prm,
+                        void* stream) {
+    if (!m || !E3 || !epsr || !prm || prm->dx <= 0.0 || prm->dr <= 0.0 || prm->rmin != 0.0 || prm->omegam <= 0.0) {
+        set_error("cth_mw3_fill_ghosts: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(m->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (m->rect) {
+        const int rc = rect_lists(m, prm, s);
+        if (rc != CTH_OK) return rc;
+    } else if (!m->has_bc) {
+        set_error("cth_mw3_fill_ghosts: boundary lists not set (cth_mw3_set_boundary)");
+        return CTH_ERR_ARG;
+    }
+    if (!m->ghosts_ok) {
+        set_error("cth_mw3_fill_ghosts: a boundary list writes a ghost onto an unknown of its field");
+        return CTH_ERR_UNSUPPORTED;
+    }
+    if (m->needs_er_dc && !Er_dc) {
+        set_error("cth_mw3_fill_ghosts: the Er east list has code-1 entries, which read gr.Er (Er_dc)");
+        return CTH_ERR_ARG;
+    }
+    for (int L = 0; L < 12; L++) {
+        if (m->cnt[L] == 0) continue;
+        k_m3_ghost<<<(m->cnt[L] + 127) / 128, 128, 0, s>>>(m->lst + 3 * (size_t)m->off[L], m->cnt[L], L,
+                                                           reinterpret_cast<cd*>(E3), Er_dc, epsr, *prm, m->jflc,
+                                                           m->ld, m->pl);
+        m->launches++;
+    }
+    CTH_CUDA(cudaGetLastError());
     return CTH_OK;
 }
 

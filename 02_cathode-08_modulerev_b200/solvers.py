@@ -386,8 +386,19 @@ class Microwave3:
                    allow_positive=False)
         return y
 
+    def fill_ghosts(self, E3, epsr, params: dict, Er_dc=None, stream=None):
+        """Ghost values of E3 (in place) from its unknowns, the boundary
+        post-processing of solve_Microwave (emfieldModule.hpp:3026-3264);
+        Er_dc = gr.Er as a real device plane (needed when the Er east list has
+        open entries)."""
+        prm = capi.MWParams(**{k: float(params[k]) for k, _ in capi.MWParams._fields_})
+        capi.check(self._L.cth_mw3_fill_ghosts(self._h, _ptr(E3), _ptr(epsr),
+                                               _ptr(Er_dc) if Er_dc is not None else None, ctypes.byref(prm),
+                                               self._stream(stream)), allow_positive=False)
+
     def solve_dev(self, maxITR: int = 500, error_cnv: float = 1e-10, out=None, stream=None):
-        """Returns (E3, status); E3 of shape (3, nj+2, ld)."""
+        """Returns (E3, status); E3 of shape (3, nj+2, ld), written on the
+        unknowns (other entries of `out` keep their values)."""
         E = out if out is not None else self.planes(3)
         st = capi.Status()
         rc = self._L.cth_mw3_solve_dev(self._h, int(maxITR), float(error_cnv), _ptr(E), self._stream(stream),

@@ -269,8 +269,18 @@ int cth_mw3_copy_planes(const cth_mw3* m, double* a_dst, double* b_dst, void* st
 /* y3 = A x3 on the unknowns (x3 is read on the unknowns only; y3 is zero elsewhere) */
 int cth_mw3_apply_dev(cth_mw3* m, const double* x3, double* y3, void* stream);
 /* solve from a zero start until ||b - A E||_2 / ||b||_2 < tol; E3 receives the
- * three fields (zero off the unknowns).  CTH_NOT_CONVERGED after maxit. */
+ * three fields on the unknowns (:3007-3024); its entries off the unknowns keep
+ * their values (the ghosts of earlier calls, as in the reference's persistent
+ * fields).  CTH_NOT_CONVERGED after maxit. */
 int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* stream, cth_status* st);
+/* the boundary post-processing of solve_Microwave (:3026-3264): ghost values of
+ * E1x, E1r, E1p written from E3's unknowns list by list in the reference's
+ * order (reading the ghosts of earlier lists and calls where the reference
+ * does).  Er_dc = gr.Er (real plane, library layout), which the Er east code 1
+ * reads (:3162); it may be NULL when no such entry exists.  CTH_ERR_UNSUPPORTED
+ * when a list would write a ghost onto an unknown of its field. */
+int cth_mw3_fill_ghosts(cth_mw3* m, double* E3, const double* epsr, const double* Er_dc, const cth_mw_params* prm,
+                        void* stream);
 /* run the solve as one captured CUDA graph with a device-side conditional loop
  * (default, 1) or kernel by kernel with a host convergence test per iteration
  * (0); same kernels, same results */

@@ -892,3 +892,135 @@ def rect_mw_lists(ni: int, nj: int, p: dict) -> dict:
             L[("x", "N")].append((i, nj, 0))
         L[("p", "N")].append((i, nj, 0))
     return L
+
+
+# which ghost each (list, code) writes: (di, dj) from the entry, per field/side
+_GHOST = {("x", "W"): ((-1, 0), (0, 2, 3, 4)), ("x", "E"): ((1, 0), (0, 2, 4)), ("x", "S"): ((0, -1), (0,)),
+          ("x", "N"): ((0, 1), (0, 1)), ("r", "W"): ((-1, 0), (0, 1, 7)), ("r", "E"): ((1, 0), (0, 1)),
+          ("r", "S"): ((0, -1), (2, 3)), ("r", "N"): ((0, 1), (2, 3, 4)), ("p", "W"): ((-1, 0), (0, 1)),
+          ("p", "E"): ((1, 0), tuple(range(8))), ("p", "S"): ((0, -1), tuple(range(8))),
+          ("p", "N"): ((0, 1), (0, 1))}
+
+
+def ghost_targets(lists: dict):
+    """{field: set of (i, j)} the ghost pass writes."""
+    out = {f: set() for f in "xrp"}
+    for (f, sd), ent in lists.items():
+        (di, dj), codes = _GHOST[(f, sd)]
+        for i, j, c in ent:
+            if c in codes:
+                out[f].add((i + di, j + dj))
+    return out
+
+
+def mag_ghosts(E, Er_dc, epsr, p: dict, lists: dict, jflc00: int):
+    """The boundary post-processing of solve_Microwave
+    (emfieldModule.hpp:3026-3260): ghost values of E1x, E1r, E1p written from
+    the solution list by list in the reference's order.  E = (Ex, Er, Ep) full
+    (ni+2, nj+2) complex arrays (solution on the unknowns, earlier ghosts
+    elsewhere); returns new arrays.  Er_dc is the real field gr.Er, which the
+    Er east code 1 reads (:3162), dividing by its deno twice, as there."""
+    Ex, Er, Ep = (np.array(e, dtype=complex) for e in E)
+    dx, dr, w, r = p["dx"], p["dr"], p["omegam"], p["r"]
+
+    def c0_of(e):
+        return np.sqrt(1.0 / (EPS0 * e * MU0))
+
+    def open_x(e):
+        c0 = c0_of(e)
+        deno = (2.0 * c0) ** 2 + (w * dx) ** 2
+        return complex((2.0 * c0) ** 2 - (w * dx) ** 2, -4.0 * c0 * w * dx) / (deno + 1e-100)
+
+    def open_r(e, j):
+        c0 = c0_of(e)
+        rt = (r[j + 1] + r[j]) / 2.0
+        qL, qR = r[j] / (rt + 1e-100), r[j + 1] / (rt + 1e-100)
+        deno = (2.0 * c0 * np.sqrt(qR)) ** 2 + (w * dr * qR) ** 2
+        R = complex((2.0 * c0) ** 2 * np.sqrt(qL * qR) - (w * dr) ** 2 * qL * qR,
+                    -2.0 * c0 * w * dr * (qL * np.sqrt(qR) + qR * np.sqrt(qL)))
+        return R / (deno + 1e-100)
+
+    for i, j, c in lists[("x", "W")]:  # :3028-3053
+        qL = (r[j - 1] + r[j]) / 2.0 / (r[j] + 1e-100); qR = (r[j + 1] + r[j]) / 2.0 / (r[j] + 1e-100)
+        if c == 0:
+            Ex[i - 1, j] = 0.0
+        elif c == 2:
+            Ex[i - 1, j] = Ex[i, j] + dx / dr * (qR * Er[i - 1, j + 1] - qL * Er[i - 1, j])
+        elif c == 3:
+            deno = 1.0 + dx / dr * qL
+            Ex[i - 1, j] = Ex[i, j] / deno + dx / dr * (qR * Er[i - 1, j + 1]) / deno
+        elif c == 4:
+            deno = 1.0 + dx / dr * qR
+            Ex[i - 1, j] = Ex[i, j] / deno - dx / dr * (qL * Er[i - 1, j]) / deno
+    for i, j, c in lists[("x", "E")]:  # :3054-3073
+        qL = (r[j - 1] + r[j]) / 2.0 / (r[j] + 1e-100); qR = (r[j + 1] + r[j]) / 2.0 / (r[j] + 1e-100)
+        if c == 0:
+            Ex[i + 1, j] = 0.0
+        elif c == 2:
+            Ex[i + 1, j] = Ex[i, j] - dx / dr * (qR * Er[i, j + 1] - qL * Er[i, j])
+        elif c == 4:
+            deno = 1.0 + dx / dr * qR
+            Ex[i + 1, j] = Ex[i, j] / deno + dx / dr * qL * Er[i, j] / deno
+    for i, j, c in lists[("x", "S")]:  # :3074-3083
+        if c == 0:
+            Ex[i, j - 1] = -r[j] / r[j - 1] * Ex[i, j]
+    for i, j, c in lists[("x", "N")]:  # :3084-3107
+        if c == 0:
+            Ex[i, j + 1] = -r[j] / r[j + 1] * Ex[i, j]
+        elif c == 1:
+            Ex[i, j + 1] = open_r((epsr[i, j] + epsr[i - 1, j]) / 2.0, j) * Ex[i, j]
+    for i, j, c in lists[("r", "W")]:  # :3109-3143
+        eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+        if c == 0:
+            Er[i - 1, j] = -Er[i, j]
+        elif c == 1:
+            Er[i - 1, j] = open_x(eps_t) * Er[i, j]
+        elif c == 7:
+            c0 = c0_of(eps_t)
+            deno, Rq = complex(2.0 * c0, w * dx), complex(2.0 * c0, -w * dx)
+            rt = (r[j] + r[j - 1]) / 2.0
+            S = complex(0.0, 4.0 * w * dx) * (p["J1r_exc"] / rt / np.log(p["r2"] / p["r1"]) * 1e3)
+            Er[i - 1, j] = Rq / (deno + 1e-100) * Er[i, j] + S / (deno + 1e-100)
+    for i, j, c in lists[("r", "E")]:  # :3144-3166
+        if c == 0:
+            Er[i + 1, j] = -Er[i, j]
+        elif c == 1:
+            eps_t = (epsr[i, j] + epsr[i, j - 1]) / 2.0
+            c0 = c0_of(eps_t)
+            deno = (2.0 * c0) ** 2 + (w * dx) ** 2
+            R = complex((2.0 * c0) ** 2 - (w * dx) ** 2, -4.0 * c0 * w * dx) / (deno + 1e-100)
+            Er[i + 1, j] = R / (deno + 1e-100) * Er_dc[i, j]
+    for i, j, c in lists[("r", "S")]:  # :3167-3187
+        rR, rL = (r[j] + r[j - 1]) / 2.0, (r[j - 1] + r[j - 2]) / 2.0
+        if c == 2:
+            Er[i, j - 1] = rR / rL * Er[i, j] + dr / dx * r[j - 1] / rL * (Ex[i + 1, j - 1] - Ex[i, j - 1])
+        elif c == 3:
+            deno = dr / dx * r[j - 1] / rL
+            if r[j] < jflc00:
+                deno = 1.0
+            Er[i, j - 1] = rR / rL * Er[i, j] / deno + dr / dx * r[j - 1] / rL * (Ex[i + 1, j - 1]) / deno
+    for i, j, c in lists[("r", "N")]:  # :3188-3212
+        rR, rL = (r[j + 1] + r[j]) / 2.0, (r[j] + r[j - 1]) / 2.0
+        if c == 2:
+            Er[i, j + 1] = rL / rR * Er[i, j] - dr / dx * r[j] / rR * (Ex[i + 1, j] - Ex[i, j])
+        elif c == 3:
+            deno = dr / dx * r[j] / rR
+            Er[i, j + 1] = rL / rR * Er[i, j] / deno - dr / dx * r[j] / rR * (Ex[i + 1, j]) / deno
+        elif c == 4:
+            deno = dr / dx * r[j] / rR
+            Er[i, j + 1] = rL / rR * Er[i, j] / deno + dr / dx * r[j] / rR * (Ex[i, j]) / deno
+    for i, j, c in lists[("p", "W")]:  # :3213-3229
+        if c == 0:
+            Ep[i - 1, j] = -Ep[i, j]
+        elif c == 1:
+            Ep[i - 1, j] = open_x(epsr[i, j]) * Ep[i, j]
+    for i, j, c in lists[("p", "E")]:  # :3230-3236, every code
+        Ep[i + 1, j] = -Ep[i, j]
+    for i, j, c in lists[("p", "S")]:  # :3237-3243, every code
+        Ep[i, j - 1] = -r[j] / r[j - 1] * Ep[i, j]
+    for i, j, c in lists[("p", "N")]:  # :3244-3264
+        if c == 0:
+            Ep[i, j + 1] = -r[j] / r[j + 1] * Ep[i, j]
+        elif c == 1:
+            Ep[i, j + 1] = open_r(epsr[i, j], j) * Ep[i, j]
+    return Ex, Er, Ep

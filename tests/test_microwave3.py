@@ -119,3 +119,34 @@ def test_rectangle_surgery_as_lists():
             assert np.max(np.abs(s[comp][k] - v)) <= 1e-14 * scale, (comp, k)
     for c in range(3):
         assert np.max(np.abs(s["b"][c] - ref["b"][c])) <= 1e-14 * (np.abs(ref["b"][c]).max() + 1e-300)
+
+
+def test_ghosts_never_overwrite_unknowns():
+    """On the cathode's and the rectangle's lists the post-processing writes only
+    entries off the unknowns (what lets the device run a list's entries in
+    parallel)."""
+    w, p, mw, masks, lists, _ = _cathode()
+    T = mw.ghost_targets(lists)
+    for f, m in zip("xrp", masks):
+        assert T[f] and not any(m[i, j] for i, j in T[f]), f
+    pr = mw.er_rect_params(40, 16)
+    T = mw.ghost_targets(mw.rect_mw_lists(40, 16, pr))
+    for f, m in zip("xrp", mw.mag_masks(40, 16)):
+        assert T[f] and not any(m[i, j] for i, j in T[f]), f
+
+
+def test_ghost_pass_is_linear_in_the_solution():
+    """With the port source off (J1r_exc = 0) and gr.Er = 0 the ghosts are
+    linear in the planes (a size-independent property of :3026-3264)."""
+    w, p, mw, masks, lists, jflc = _cathode()
+    p = dict(p, J1r_exc=0.0)
+    rng = np.random.default_rng(3)
+    sh = masks[0].shape
+    A = [rng.standard_normal(sh) + 1j * rng.standard_normal(sh) for _ in range(3)]
+    B = [rng.standard_normal(sh) + 1j * rng.standard_normal(sh) for _ in range(3)]
+    z = np.zeros(sh)
+    ga = mw.mag_ghosts(A, z, w["epsr"], p, lists, jflc)
+    gb = mw.mag_ghosts(B, z, w["epsr"], p, lists, jflc)
+    gs = mw.mag_ghosts([a + 2.0 * b for a, b in zip(A, B)], z, w["epsr"], p, lists, jflc)
+    for c in range(3):
+        assert np.max(np.abs(gs[c] - (ga[c] + 2.0 * gb[c]))) <= 1e-12 * np.max(np.abs(gs[c]))

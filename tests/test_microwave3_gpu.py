@@ -248,3 +248,82 @@ def test_mw3_set_boundary_rejects_bad_lists(pkg, cuda_device):
             m.set_boundary(lists, j0)
     m.set_boundary({("p", "W"): [(i0, j0, 0)], ("p", "E"): [(i0, j0, 0)]}, j0)  # same row in two lists is fine
     m.close()
+
+
+def _junk_planes(m, ni, seed):
+    """Complex planes with values everywhere: the unknowns and earlier ghosts."""
+    import torch
+    rng = np.random.default_rng(seed)
+    full = [rng.standard_normal((ni + 2, m.nj + 2)) + 1j * rng.standard_normal((ni + 2, m.nj + 2)) for _ in range(3)]
+    x3 = m.planes(3)
+    for c in range(3):
+        x3[c, :, :ni + 2] = torch.from_numpy(np.ascontiguousarray(full[c].T)).to(x3.device)
+    return full, x3
+
+
+@pytest.mark.parametrize("geometry", ["cathode", "rectangle"])
+def test_mw3_ghosts_match_oracle(pkg, cuda_device, geometry):
+    """The boundary post-processing on planes with values everywhere (the ghosts
+    read before they are written are earlier ones), gr.Er random: every entry of
+    the three planes as the oracle's restatement, to rounding."""
+    import torch
+    if geometry == "cathode":
+        ni, nj = 194, 70
+        w, mw, ref, m, g = _cathode(pkg, ni, nj)
+        from oracle import microwave as omw
+        p = omw.cathode_mw_params(ni, nj)
+        cells, _, _ = omw.cathode_mw_blocks(p)
+        import json, os
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mw_lists_cathode.json")) as f:
+            lists = omw.cathode_mw_lists(cells, json.load(f))
+        jflc = int(cells[1][0][0])
+    else:
+        ni, nj = 64, 32
+        w, p, mw = _case(pkg, ni, nj)
+        g, planes = _device(pkg, w)
+        m = pkg.Microwave3(ni, nj)
+        m.assemble_dev(*planes, w["params"])
+        lists, jflc = mw.rect_mw_lists(ni, nj, p), 0
+    full, x3 = _junk_planes(m, ni, 5)
+    er_dc = np.random.default_rng(6).standard_normal((ni + 2, nj + 2))
+    m.fill_ghosts(x3, g.to_device(w["epsr"]), w["params"], Er_dc=g.to_device(er_dc))
+    got = _to_ij(x3, ni)
+    want = mw.mag_ghosts(full, er_dc, w["epsr"], p, lists, jflc)
+    targets = mw.ghost_targets(lists)
+    for c, f in enumerate("xrp"):
+        assert np.max(np.abs(got[c] - want[c])) <= 1e-14 * np.max(np.abs(want[c])), f
+        changed = np.argwhere(want[c] != full[c])
+        assert len(changed) > 0 and all((int(a), int(b)) in targets[f] for a, b in changed)
+    m.close(); g.close()
+
+
+def test_mw3_solve_then_ghosts_matches_direct(pkg, cuda_device):
+    """solve_Microwave end to end on the cathode: the solve writes the unknowns
+    and keeps the earlier ghosts, the post-processing writes the new ones; all
+    entries against the oracle's direct solve and ghost pass."""
+    ni, nj = 194, 70
+    w, mw, ref, m, g = _cathode(pkg, ni, nj)
+    from oracle import microwave as omw
+    import json, os
+    p = omw.cathode_mw_params(ni, nj)
+    cells, _, _ = omw.cathode_mw_blocks(p)
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mw_lists_cathode.json")) as f:
+        lists = omw.cathode_mw_lists(cells, json.load(f))
+    full, E = _junk_planes(m, ni, 9)
+    E, st = m.solve_dev(maxITR=600, error_cnv=1e-12, out=E)
+    assert st.converged == 1
+    got0 = _to_ij(E, ni)
+    for c in range(3):
+        off = ~ref["masks"][c]
+        assert np.array_equal(got0[c][off], full[c][off])  # ghosts kept
+    er_dc = np.zeros((ni + 2, nj + 2))
+    m.fill_ghosts(E, g.to_device(w["epsr"]), w["params"], Er_dc=g.to_device(er_dc))
+    got = _to_ij(E, ni)
+    E_ref = mw.mag_rect_solve(ref)
+    start = [np.where(ref["masks"][c], E_ref[c], full[c]) for c in range(3)]
+    want = mw.mag_ghosts(start, er_dc, w["epsr"], p, lists, int(cells[1][0][0]))
+    for c in range(3):
+        on = ref["masks"][c]
+        assert _rel(got[c][on], want[c][on]) < 1e-8, c
+        assert _rel(got[c], want[c]) < 1e-8, c
+    m.close(); g.close()
