@@ -472,7 +472,10 @@ def main():
         # solve_Microwave: the magnetised 3-component system on the discharge's fields
         f3 = [_Plane(fs.ptr(k)) for k in ("rhoe", "nu_m", "Bx", "Br", "epsr_mw")]
         m3.assemble_dev(*f3, wb["params"], stream=stream)
-        return m3.solve_dev(maxITR=200, error_cnv=TOL, out=e3, stream=stream)[1]
+        st = m3.solve_dev(maxITR=200, error_cnv=TOL, out=e3, stream=stream)[1]
+        # the boundary post-processing: ghosts of the three fields (gr.Er for the open east faces)
+        m3.fill_ghosts(e3, f3[4], wb["params"], Er_dc=_Plane(fs.ptr("Er")), stream=stream)
+        return st
 
     def step(P):
         r = fs.fluid_step(gx, gr, P, stream=stream)
