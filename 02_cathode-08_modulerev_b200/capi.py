@@ -39,7 +39,7 @@ EXPORTS = (
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
     "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
-    "cth_batch_steps", "cth_update_energy_profile", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
+    "cth_batch_steps", "cth_update_energy_profile", "cth_mw_port_rescale", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_tensor_cores", "cth_unet_set_smoothing", "cth_unet_set_wait_test", "cth_unet_set_grid_limit", "cth_unet_check", "cth_unet_set_params", "cth_unet_get_params",
     "cth_unet_get_grads", "cth_unet_set_loss_weights", "cth_unet_forward", "cth_unet_backward",
     "cth_unet_train_step", "cth_unet_set_stats", "cth_unet_features", "cth_unet_predict_dphi",
@@ -72,6 +72,20 @@ class EnergyParams(ctypes.Structure):
 
 class EnergyResult(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("Px", "Pr", "Pp", "power_sum")]
+
+
+class MWPortParams(ctypes.Structure):
+    """cth_mw_port_params: the port / reflection / rescale part of update_energy_profile."""
+    _fields_ = [(k, ctypes.c_double) for k in ("dx", "dr", "rmin", "omegam", "r1", "r2", "Z0", "Pmw")] + \
+        [(k, ctypes.c_double * 2) for k in ("S11", "S21", "S12", "S22")] + \
+        [(k, ctypes.c_int) for k in ("flag_mwRef", "i_ref", "j_out", "i_out0", "i_out1", "jf0", "jf1")]
+
+
+class MWPortResult(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("P_out", "P_fwd", "P_ref", "P_fwd_all", "P_ref_all", "P_err",
+                                                 "power_sum", "ratio", "pabs_factor", "field_factor",
+                                                 "J1r_exc_factor")] + \
+        [(k, ctypes.c_double * 2) for k in ("I_ref", "V_ref", "Gamma_p", "Zp", "Gamma_all", "Zall")]
 
 
 class CMat2(ctypes.Structure):
@@ -311,6 +325,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_update_energy_profile.argtypes = [_vp, _vp, _vp, ctypes.POINTER(EnergyParams)] + [_vp] * 7 + \
         [ctypes.POINTER(EnergyResult)]
     L.cth_update_energy_profile.restype = ctypes.c_int
+    L.cth_mw_port_rescale.argtypes = [_vp, ctypes.POINTER(MWPortParams), ctypes.c_double] + [_vp] * 10 + \
+        [ctypes.POINTER(MWPortResult)]
+    L.cth_mw_port_rescale.restype = ctypes.c_int
     _c2 = ctypes.c_double * 2
     L.cth_cmat2_mul.argtypes = [ctypes.POINTER(CMat2)] * 3
     L.cth_cmat2_mul.restype = ctypes.c_int

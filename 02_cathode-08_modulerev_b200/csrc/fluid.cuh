@@ -11,7 +11,7 @@
 
 #include "grid.h"
 
-#define CTH_FS_NSCAL 64
+#define CTH_FS_NSCAL 96
 #define CTH_FS_NPART_PER_BLOCK 16
 
 struct cth_fields {

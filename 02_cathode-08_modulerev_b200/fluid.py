@@ -315,6 +315,31 @@ class Fields:
                                                      ctypes.byref(r)), allow_positive=False)
         return {k: getattr(r, k) for k, _ in capi.EnergyResult._fields_}
 
+    def mw_port_rescale(self, prm: dict, power_sum: float, E1x=None, E1r=None, E1p=None, J1x=None, J1r=None,
+                        J1p=None, J1x_exc=None, J1r_exc=None, J1p_exc=None, stream=None) -> dict:
+        """The port / reflection / rescale part of update_energy_profile
+        (emfieldModule.hpp:7792-8105) on complex128 device planes; prm holds
+        the cth_mw_port_params fields (S-parameters as complex numbers).
+        Returns the reported quantities (complex ones as complex)."""
+        p = capi.MWPortParams()
+        for k, t in capi.MWPortParams._fields_:
+            v = prm[k]
+            if k.startswith("S"):
+                getattr(p, k)[0], getattr(p, k)[1] = complex(v).real, complex(v).imag
+            else:
+                setattr(p, k, v)
+        r = capi.MWPortResult()
+        s = 0 if stream is None else stream.cuda_stream
+        ptr = [ctypes.c_void_p(t.data_ptr()) if t is not None else None
+               for t in (E1x, E1r, E1p, J1x, J1r, J1p, J1x_exc, J1r_exc, J1p_exc)]
+        rc = self._L.cth_mw_port_rescale(self._h, ctypes.byref(p), float(power_sum), *ptr, s, ctypes.byref(r))
+        capi.check(rc, allow_positive=False)
+        out = {}
+        for k, t in capi.MWPortResult._fields_:
+            v = getattr(r, k)
+            out[k] = complex(v[0], v[1]) if hasattr(v, "__len__") else v
+        return out
+
     def check_cfl(self, dt: float, CFL: float, masse: float, rmin: float, dr: float, flag_adp_dt: int = 0,
                   stream=None) -> dict:
         """FluidModule::check_CFL (fluidModule.hpp:57-115); returns dt, CFL and the maxima."""

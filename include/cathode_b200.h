@@ -614,7 +614,8 @@ int cth_batch_steps(cth_batch_item* items, int n, int steps, int nthreads, doubl
  * planes: J = sigma E with the magnetised cold-plasma tensor of rhoe, nu_m1,
  * Bx, Br), the store's planes Pabsx, Pabsr, Pabsp (Re(J.E*)/2) and Pabs (their
  * cell profile) on the block cells, and the volume integrals.  The port,
- * reflection and field-rescaling part (flag_mwRef, :7792-8105) is not here. */
+ * reflection and field-rescaling part (flag_mwRef, :7792-8105) is
+ * cth_mw_port_rescale, below. */
 typedef struct cth_energy_params {
     double dx, dr, rmin, omegam, masse;
 } cth_energy_params;
@@ -624,6 +625,44 @@ typedef struct cth_energy_result {
 int cth_update_energy_profile(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_energy_params* prm,
                               const void* E1x, const void* E1r, const void* E1p, void* J1x, void* J1r,
                               void* J1p, void* stream, cth_energy_result* res);
+
+/* The rest of update_energy_profile (emfieldModule.hpp:7792-8105), after
+ * cth_update_energy_profile (power_sum = its result's power_sum).
+ * flag_mwRef = 1: the Poynting flux out through the upper faces of the outlet
+ * row j_out, columns i_out0..i_out1 (mWLoss_at_boundary_rR, :8631-8664; the
+ * reference passes gc.j_flc_bl[4][1]-1 and gc.i_flc_bl[4][0..1]); the port
+ * current (from H_phi) and voltage (mean r Er times ln(r2/r1)) on column i_ref
+ * (int(x_ref/dx + 0.5) + 1 with x_ref = 0) over the feed's Er faces jf0..jf1
+ * (gr.j_flr_bl[n_bl-1]); the wave amplitudes a2, b2 for Z0, de-embedded
+ * through the feed's S-parameters (S11, S21, S12, S22 as {re, im}) to a1, b1;
+ * ratio = Pmw / |a1|^2 and ratio_eff = ratio (power_sum + P_err) / power_sum;
+ * then Pabs *= ratio_eff and E1x, E1r, E1p, J1x, J1r, J1p and the optional
+ * excitation planes J1x_exc, J1r_exc, J1p_exc (NULL: absent) *= sqrt(ratio_eff)
+ * over the whole index space.  flag_mwRef = 0: ratio = Pmw / power_sum and
+ * Pabs *= ratio only (:8073-8095; the planes may be NULL).  The caller
+ * multiplies its J1r_exc by res->J1r_exc_factor (sqrt(ratio)), as the reference
+ * updates pm.J1r_exc.  res holds the reference's reported quantities after its
+ * rescaling.  Complex planes: library layout, (re, im) interleaved.  Waits for
+ * the stream (the result is read back).  CTH_NONFINITE, with nothing
+ * rescaled, when the ratio is not finite. */
+typedef struct cth_mw_port_params {
+    double dx, dr, rmin, omegam;
+    double r1, r2;                     /* coax radii of the feed           */
+    double Z0, Pmw;                    /* line impedance, incident power   */
+    double S11[2], S21[2], S12[2], S22[2];
+    int flag_mwRef;
+    int i_ref;
+    int j_out, i_out0, i_out1;
+    int jf0, jf1;
+} cth_mw_port_params;
+typedef struct cth_mw_port_result {
+    double P_out, P_fwd, P_ref, P_fwd_all, P_ref_all, P_err, power_sum; /* W, after the rescale */
+    double ratio, pabs_factor, field_factor, J1r_exc_factor;
+    double I_ref[2], V_ref[2], Gamma_p[2], Zp[2], Gamma_all[2], Zall[2];
+} cth_mw_port_result;
+int cth_mw_port_rescale(cth_fields* fs, const cth_mw_port_params* prm, double power_sum, void* E1x, void* E1r,
+                        void* E1p, void* J1x, void* J1r, void* J1p, void* J1x_exc, void* J1r_exc, void* J1p_exc,
+                        void* stream, cth_mw_port_result* res);
 
 /* Two-port feed helpers (host) -------------------------------------------------
  * CmpMat2 (cmpMat2.hpp:8-34): 2x2 complex matrices, complex values as

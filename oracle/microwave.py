@@ -1024,3 +1024,81 @@ def mag_ghosts(E, Er_dc, epsr, p: dict, lists: dict, jflc00: int):
         elif c == 1:
             Ep[i, j + 1] = open_r(epsr[i, j], j) * Ep[i, j]
     return Ex, Er, Ep
+
+
+def mw_loss_rR(j, i0, i1, E1x, E1r, E1p, r, dx, dr, w):
+    """mWLoss_at_boundary_rR (emfieldModule.hpp:8631-8664): the Poynting flux
+    through the upper faces of row j, columns i0..i1."""
+    P = 0.0
+    iwm = complex(0.0, 1.0 / (w * MU0))
+    for i in range(i0, i1 + 1):
+        rt = (r[j] + r[j + 1]) / 2.0
+        dRdx_L = (E1r[i, j + 1] - E1r[i - 1, j + 1]) / dx
+        dXdr_L = (E1x[i, j + 1] - E1x[i, j]) / dr
+        dRdx_R = (E1r[i + 1, j + 1] - E1r[i, j + 1]) / dx
+        dXdr_R = (E1x[i + 1, j + 1] - E1x[i + 1, j]) / dr
+        H1p = (iwm * (dRdx_R - dXdr_R) + iwm * (dRdx_L - dXdr_L)) / 2.0
+        H1x = iwm * ((r[j + 1] * E1p[i, j + 1] - r[j] * E1p[i, j]) / (rt * dr))
+        Ep = (r[j + 1] * E1p[i, j + 1] + r[j] * E1p[i, j]) / (2.0 * rt)
+        Ex_L = (r[j + 1] * E1x[i, j + 1] + r[j] * E1x[i, j]) / (2.0 * rt)
+        Ex_R = (r[j + 1] * E1x[i + 1, j + 1] + r[j] * E1x[i + 1, j]) / (2.0 * rt)
+        Ex = (Ex_R + Ex_L) / 2.0
+        S = 0.5 * (Ep * np.conj(H1x) - Ex * np.conj(H1p)).real
+        P += 2.0 * np.pi * rt * S * dx
+    return P
+
+
+def mw_port_rescale(E1x, E1r, E1p, J, Jexc, Pabs, power_sum, p: dict):
+    """The port / reflection / rescale part of update_energy_profile
+    (emfieldModule.hpp:7792-8105).  p: dx, dr, rmin, omegam, r1, r2, Z0, Pmw,
+    S11, S21, S12, S22 (complex), flag_mwRef, i_ref, j_out, i_out0, i_out1,
+    jf0, jf1.  Returns (planes, result): planes = dict of the rescaled arrays
+    (E1x, E1r, E1p, J1x, J1r, J1p, the excitation planes, Pabs), result = the
+    reported quantities after the reference's rescaling."""
+    dx, dr, w = p["dx"], p["dr"], p["omegam"]
+    nj2 = E1x.shape[1]
+    r = p["rmin"] + (np.arange(nj2) - 0.5) * dr
+    out = dict(E1x=E1x.copy(), E1r=E1r.copy(), E1p=E1p.copy(), J1x=J[0].copy(), J1r=J[1].copy(), J1p=J[2].copy(),
+               Pabs=Pabs.copy())
+    for k, v in zip(("J1x_exc", "J1r_exc", "J1p_exc"), Jexc or (None,) * 3):
+        if v is not None:
+            out[k] = v.copy()
+    if not p["flag_mwRef"]:  # :8073-8095
+        ratio = p["Pmw"] / power_sum
+        out["Pabs"] = out["Pabs"] * ratio
+        return out, dict(ratio=ratio, pabs_factor=ratio, field_factor=1.0, J1r_exc_factor=np.sqrt(ratio),
+                         power_sum=power_sum)
+    P_out = mw_loss_rR(p["j_out"], p["i_out0"], p["i_out1"], E1x, E1r, E1p, r, dx, dr, w)  # :7848-7849
+    i = p["i_ref"]
+    I = 0.0j
+    V = 0.0j
+    n = 0
+    for j in range(p["jf0"], p["jf1"] + 1):  # :7866-7920
+        rt = (r[j] + r[j - 1]) / 2.0
+        H = (E1r[i, j] - E1r[i - 1, j]) / dx / (w * MU0) * 1j
+        I = I + 2.0 * np.pi * rt * H
+        V = V + (E1r[i, j] + E1r[i - 1, j]) / 2.0 * rt
+        n += 1
+    I_ref = I / n
+    V_ref = V / n * np.log(p["r2"] / p["r1"])
+    Z0 = p["Z0"]
+    a2 = (V_ref - Z0 * I_ref) / (2.0 * np.sqrt(2.0 * Z0))  # :7930-7935
+    b2 = (V_ref + Z0 * I_ref) / (2.0 * np.sqrt(2.0 * Z0))
+    P_fwd, P_ref = abs(b2) ** 2, abs(a2) ** 2
+    P_err = P_fwd - P_ref - power_sum - P_out
+    a1 = (b2 - p["S22"] * a2) / p["S21"]
+    b1 = p["S11"] * a1 + p["S12"] * a2
+    P_fwd_all, P_ref_all = abs(a1) ** 2, abs(b1) ** 2
+    ratio = p["Pmw"] / P_fwd_all  # :7988
+    ratio_eff = ratio * (power_sum + P_err) / power_sum
+    out["Pabs"] = out["Pabs"] * ratio_eff  # :7993-8015
+    for k in ("E1x", "E1r", "E1p", "J1x", "J1r", "J1p", "J1x_exc", "J1r_exc", "J1p_exc"):
+        if k in out:
+            out[k] = out[k] * np.sqrt(ratio_eff)
+    Gp, Ga = a2 / b2, b1 / a1
+    res = dict(P_out=P_out * ratio, P_fwd=P_fwd * ratio, P_ref=P_ref * ratio, P_fwd_all=P_fwd_all * ratio,
+               P_ref_all=P_ref_all * ratio, P_err=P_err * ratio, power_sum=(power_sum + P_err) * ratio,
+               ratio=ratio, pabs_factor=ratio_eff, field_factor=np.sqrt(ratio_eff), J1r_exc_factor=np.sqrt(ratio),
+               I_ref=I_ref, V_ref=V_ref, Gamma_p=Gp, Zp=Z0 * (1.0 + Gp) / (1.0 - Gp), Gamma_all=Ga,
+               Zall=Z0 * (1.0 + Ga) / (1.0 - Ga))
+    return out, res

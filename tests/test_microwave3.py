@@ -150,3 +150,33 @@ def test_ghost_pass_is_linear_in_the_solution():
     gs = mw.mag_ghosts([a + 2.0 * b for a, b in zip(A, B)], z, w["epsr"], p, lists, jflc)
     for c in range(3):
         assert np.max(np.abs(gs[c] - (ga[c] + 2.0 * gb[c]))) <= 1e-12 * np.max(np.abs(gs[c]))
+
+
+def test_port_of_a_matched_coax_wave():
+    """A forward TEM wave Er = A / r exp(-i k z) in the feed seen through the
+    reference plane's current and voltage (emfieldModule.hpp:7866-7935): the
+    impedance is the coax's eta ln(r2/r1) / (2 pi) to the difference scheme's
+    O((k dx)^2), so with that Z0 the plasma reflection vanishes, and with S = the
+    identity two-port the forward power at the amplifier is the port's."""
+    from oracle import microwave as mw
+    ni, nj = 194, 70
+    p = mw.cathode_mw_params(ni, nj)
+    cells, xf, rf = mw.cathode_mw_blocks(p)
+    eta = np.sqrt(mw.MU0 / mw.EPS0)
+    Zc = eta * np.log(p["r2"] / p["r1"]) / (2.0 * np.pi)
+    k = p["omegam"] * np.sqrt(mw.EPS0 * mw.MU0)
+    x = (np.arange(ni + 2) - 0.5) * p["dx"]
+    rface = np.maximum((np.arange(nj + 2) - 1.0) * p["dr"], p["dr"])
+    A = 1e3
+    E1r = A / rface[None, :] * np.exp(-1j * k * x)[:, None]
+    z = np.zeros_like(E1r)
+    prm = dict(dx=p["dx"], dr=p["dr"], rmin=0.0, omegam=p["omegam"], r1=p["r1"], r2=p["r2"], Z0=Zc, Pmw=8.0,
+               S11=0j, S21=1 + 0j, S12=1 + 0j, S22=0j, flag_mwRef=1, i_ref=1, j_out=int(cells[1][4][1]) - 1,
+               i_out0=int(cells[0][4][0]), i_out1=int(cells[0][4][1]), jf0=int(rf[1][5][0]), jf1=int(rf[1][5][1]))
+    _, res = mw.mw_port_rescale(z, E1r, z, [z, z, z], None, np.ones(z.shape), 1.0, prm)
+    assert abs(res["Zp"] / Zc - 1.0) < 1e-3
+    assert abs(res["Gamma_p"]) < 1e-3
+    assert res["P_fwd_all"] == pytest.approx(res["P_fwd"], rel=1e-12)
+    assert res["P_fwd_all"] == pytest.approx(8.0, rel=1e-12)  # rescaled to Pmw
+    # without any other field the power through the outlet row is zero
+    assert res["P_out"] == 0.0

@@ -173,3 +173,85 @@ def test_energy_profile_matches_oracle(pkg, cuda_device, kind):
     fs.close()
     for x in (g, gx, gr):
         x.close()
+
+
+# ---------------------------------------------------------------------------
+# the port / reflection / rescale part of update_energy_profile (:7792-8105)
+# ---------------------------------------------------------------------------
+def _port_case(pkg, seed=4, Z0=50.0):
+    """Cathode grid; Er a forward TEM wave A / r exp(-i k z) on every r-face plus
+    noise, Ex and Ephi noise; random Pabs and excitation current."""
+    from oracle import microwave as omw
+    geo = pkg.fluid.cathode_geometry()
+    ni, nj = geo["ni"], geo["nj"]
+    p = omw.cathode_mw_params(ni, nj)
+    cells, xf, rf = omw.cathode_mw_blocks(p)
+    rng = np.random.default_rng(seed)
+    shp = (ni + 2, nj + 2)
+    k = p["omegam"] * np.sqrt(omw.EPS0 * omw.MU0)
+    x = (np.arange(ni + 2) - 0.5) * p["dx"]
+    rf_ = (np.arange(nj + 2) - 1.0) * p["dr"]
+    rf_[rf_ <= 0] = p["dr"]
+    noise = lambda s: s * (rng.standard_normal(shp) + 1j * rng.standard_normal(shp))
+    A = 1e3
+    E = dict(E1x=noise(5.0), E1r=A / rf_[None, :] * np.exp(-1j * k * x)[:, None] + noise(5.0), E1p=noise(5.0))
+    J = [noise(1e4) for _ in range(3)]
+    Jexc = [None, noise(1e3), None]
+    Pabs = 10 ** rng.uniform(3, 6, shp)
+    prm = dict(dx=p["dx"], dr=p["dr"], rmin=0.0, omegam=p["omegam"], r1=p["r1"], r2=p["r2"], Z0=Z0, Pmw=8.0,
+               S11=0.1 + 0.05j, S21=0.9 - 0.2j, S12=0.9 - 0.2j, S22=-0.05 + 0.1j, flag_mwRef=1, i_ref=1,
+               j_out=int(cells[1][4][1]) - 1, i_out0=int(cells[0][4][0]), i_out1=int(cells[0][4][1]),
+               jf0=int(rf[1][5][0]), jf1=int(rf[1][5][1]))
+    # an absorbed power below the net forward power, so that the rescale is defined
+    _, r1 = omw.mw_port_rescale(E["E1x"], E["E1r"], E["E1p"], J, Jexc, Pabs, 1.0, prm)
+    power_sum = 0.3 * r1["P_fwd"] / r1["ratio"]
+    return geo, E, J, Jexc, Pabs, prm, power_sum
+
+
+def _cplx_dev(g, v):
+    import torch
+    return torch.complex(g.to_device(v.real), g.to_device(v.imag)).contiguous()
+
+
+@pytest.mark.parametrize("flag", [1, 0])
+def test_mw_port_rescale_matches_oracle(pkg, cuda_device, flag):
+    from oracle import microwave as omw
+    geo, E, J, Jexc, Pabs, prm, power_sum = _port_case(pkg)
+    prm["flag_mwRef"] = flag
+    ni, nj = geo["ni"], geo["nj"]
+    g = pkg.Grid(ni, nj, geo["ib"], geo["jb"])
+    fs = pkg.Fields(g)
+    fs.upload("Pabs", Pabs)
+    dev = {k: _cplx_dev(g, v) for k, v in E.items()}
+    dJ = [_cplx_dev(g, v) for v in J]
+    dX = [_cplx_dev(g, v) if v is not None else None for v in Jexc]
+    res = fs.mw_port_rescale(prm, power_sum, dev["E1x"], dev["E1r"], dev["E1p"], *dJ, *dX)
+    want, ref = omw.mw_port_rescale(E["E1x"], E["E1r"], E["E1p"], J, Jexc, Pabs, power_sum, prm)
+    for k, v in ref.items():
+        assert complex(res[k]) == pytest.approx(complex(v), rel=1e-10, abs=1e-300), k
+    if flag:
+        assert 0.0 < abs(ref["Gamma_p"]) < 1.0 and ref["pabs_factor"] > 0.0
+    got = {"E1x": dev["E1x"], "E1r": dev["E1r"], "E1p": dev["E1p"], "J1x": dJ[0], "J1r": dJ[1], "J1p": dJ[2],
+           "J1r_exc": dX[1]}
+    for k, t in got.items():
+        a = t[:, :ni + 2].cpu().numpy().T
+        assert np.abs(a - want[k]).max() <= 1e-12 * np.abs(want[k]).max(), k
+        if not flag:
+            assert np.array_equal(a, {**E, "J1x": J[0], "J1r": J[1], "J1p": J[2], "J1r_exc": Jexc[1]}[k]), k
+    assert np.abs(fs.download("Pabs") - want["Pabs"]).max() <= 1e-12 * np.abs(want["Pabs"]).max()
+    fs.close(); g.close()
+
+
+def test_mw_port_rescale_nonfinite_leaves_planes(pkg, cuda_device):
+    """A zero absorbed power (flag_mwRef = 0) gives an infinite ratio: the call
+    reports it and rescales nothing."""
+    geo, E, J, Jexc, Pabs, prm, _ = _port_case(pkg)
+    prm["flag_mwRef"] = 0
+    g = pkg.Grid(geo["ni"], geo["nj"], geo["ib"], geo["jb"])
+    fs = pkg.Fields(g)
+    fs.upload("Pabs", Pabs)
+    with pytest.raises(pkg.capi.CathodeError):
+        fs.mw_port_rescale(prm, 0.0)
+    assert np.array_equal(fs.download("Pabs")[1:-1, 1:-1], Pabs[1:-1, 1:-1]) or \
+        np.array_equal(fs.download("Pabs"), Pabs)
+    fs.close(); g.close()
