@@ -10,9 +10,12 @@ continuity + correction, potential predictor-corrector (2 iterations), electron
 density and energy Scharfetter-Gummel predictor-correctors (2 iterations each),
 ground-state and metastable neutrals, transport coefficients: 12 implicit
 5-point solves to 1e-10 relative residual, as input/setup.yaml sets them) plus
-the microwave solve every 100 steps (ndiv_MW): the magnetised 3-component
-system (Ex, Er, Ephi coupled through the cold-plasma tensor of the discharge's
-density, collision frequency and cusp field).
+the microwave update every 100 steps (ndiv_MW), as the reference's loop runs
+it: solve_Microwave (the magnetised 3-component system, Ex, Er, Ephi coupled
+through the cold-plasma tensor of the discharge's density, collision frequency
+nu_m1 and cusp field; then its ghost post-processing) and
+update_energy_profile (absorbed power, rescaled to Pmw = 8 W, which the next
+energy sweeps read as Pabs).
 
 Reported line (rank 0):
   value        time steps/s with every inner solve on the mixed-precision path
@@ -74,7 +77,8 @@ def workload_config(extra=None):
     c = {
         "workload": "synthetic xenon discharge, 512 (r) x 1024 (z) r-z rectangle: one predictor-corrector time step "
                     "(ions, potential, electron density and energy, neutrals, transport: 12 implicit 5-point "
-                    "solves to 1e-10) + the magnetised 3-component microwave solve every 100 steps",
+                    "solves to 1e-10) + every 100 steps the microwave update (magnetised 3-component solve, ghosts, "
+                    "absorbed power rescaled to Pmw = 8 W, feeding the energy equation)",
         "ni_z": NI, "nj_r": NJ, "tol": TOL, "maxit": MAXIT, "dt": 1e-10, "ndiv_mw": NDIV_MW,
         "l2": "no flush: the step's working set (~60 planes x 4.2 MB) exceeds the 126 MB L2",
         "method": "semicoarsening MG (z-line zebra smoother, Galerkin), FP32 cycles + FP64 defect correction; "
@@ -449,6 +453,10 @@ def main():
     def reset(prec, warm_start=0, net=None):
         for k, v in init.items():
             fs.upload(k, v)
+        # the microwave fields (their ghosts persist between updates), currents and port excitation
+        e3.zero_()
+        j3.zero_()
+        mw_state["J1r_exc"] = wb["params"]["J1r_exc"]
         for k in ("dphi_prev", "dphi_prev2", "dphi_guess"):
             fs.plane(k).zero_()
         P = {k: (dict(v) if isinstance(v, dict) else v) for k, v in cfg["params"].items()}
@@ -468,13 +476,27 @@ def main():
     e3 = m3.planes(3)
     grids.append(m3)
 
+    j3 = m3.planes(3)
+    mw_state = {"J1r_exc": wb["params"]["J1r_exc"]}
+    eprm = {k: (wb["params"][k] if k in wb["params"] else 0.0) for k in ("dx", "dr", "rmin", "omegam", "masse")}
+    # update_energy_profile without the reflection model (flag_mwRef = 0): the absorbed
+    # power is rescaled to Pmw and the port excitation by its square root
+    port = dict(eprm, r1=wb["params"]["r1"], r2=wb["params"]["r2"], Z0=50.0, Pmw=8.0, S11=0j, S21=1 + 0j,
+                S12=1 + 0j, S22=0j, flag_mwRef=0, i_ref=1, j_out=0, i_out0=0, i_out1=0, jf0=0, jf1=0)
+    port.pop("masse")
+
     def microwave():
-        # solve_Microwave: the magnetised 3-component system on the discharge's fields
-        f3 = [_Plane(fs.ptr(k)) for k in ("rhoe", "nu_m", "Bx", "Br", "epsr_mw")]
-        m3.assemble_dev(*f3, wb["params"], stream=stream)
+        # solve_Microwave on the discharge's fields (the reference reads gc.nu_m1)
+        f3 = [_Plane(fs.ptr(k)) for k in ("rhoe", "nu_m1", "Bx", "Br", "epsr_mw")]
+        prm = dict(wb["params"], J1r_exc=mw_state["J1r_exc"])
+        m3.assemble_dev(*f3, prm, stream=stream)
         st = m3.solve_dev(maxITR=200, error_cnv=TOL, out=e3, stream=stream)[1]
         # the boundary post-processing: ghosts of the three fields (gr.Er for the open east faces)
-        m3.fill_ghosts(e3, f3[4], wb["params"], Er_dc=_Plane(fs.ptr("Er")), stream=stream)
+        m3.fill_ghosts(e3, f3[4], prm, Er_dc=_Plane(fs.ptr("Er")), stream=stream)
+        # update_energy_profile: J, Pabs, the integrals, the rescale to Pmw
+        er = fs.update_energy_profile(gx, gr, eprm, e3[0], e3[1], e3[2], j3[0], j3[1], j3[2], stream=stream)
+        pr = fs.mw_port_rescale(port, er["power_sum"], stream=stream)
+        mw_state["J1r_exc"] *= pr["J1r_exc_factor"]
         return st
 
     def step(P):
