@@ -428,6 +428,68 @@ def cathode_geometry(ni=194, nj=70, xR=0.0388, rmax=0.014, width_neutIn=0.0055) 
                                                       for b in range(2)])
 
 
+def block_union_size(ib, jb) -> int:
+    """Number of (i, j) in the union of the blocks [ib[b][0], ib[b][1]] x [jb[b][0], jb[b][1]]."""
+    cells = set()
+    for (a, b), (c, d) in zip(np.asarray(ib), np.asarray(jb)):
+        cells.update((i, j) for i in range(int(a), int(b) + 1) for j in range(int(c), int(d) + 1))
+    return len(cells)
+
+
+def cathode_microwave(ni=194, nj=70, xR=0.0388, rmax=0.014) -> dict:
+    """The microwave geometry of the cathode for Microwave3: the six cell, x-face
+    and r-face blocks (initialModule.hpp:219-345: the five fluid blocks and the
+    coax feed, block 5) and the 12 boundary lists of MicrowaveBC as
+    InitialModule::makeBoundary builds them (initialModule.hpp:420-1055), from
+    the package's segment table data/mw_lists_cathode.json: one record per
+    segment (field, side, code, a loop over i or j with the other index fixed,
+    or one entry), bounds written over the cell blocks as ic[b][k] / jc[b][k]
+    plus a constant, so that the table serves every resolution.
+    Returns dict(blocks=((xi, xj), (ri, rj), (ci, cj)), lists={(field, side):
+    [(i, j, code), ...]}, j_flc_00) for Microwave3(..., blocks=) and
+    set_boundary."""
+    import json
+    import os
+    import re
+    dx, dr = xR / ni, rmax / nj
+    x1, x6 = 0.0, 7.8e-3
+    x2, x3, x4, x5 = 5.6e-3 + x6, 10.0e-3 + x6, 15.0e-3 + x6, 20.0e-3 + x6
+    r1, r2, r3, r4, r5 = 0.6e-3, 2.0e-3, 4.0e-3, 9.0e-3, 2.0e-3
+    lo = lambda v, d, k: int(v / d + 0.5) + k
+    hi = lambda v, d, k: int(v / d - 0.5) + k
+    zs = [(x6, x2), (x2, x4), (x2, x3), (x3, x5), (x5, xR), (x1, x2)]
+    rs = [(r3, r4), (r5, r4), (r1, r5), (0.0, r5), (0.0, rmax), (r1, r2)]
+    ci = np.array([[lo(a, dx, 1), hi(b, dx, 1)] for a, b in zs], np.int32)
+    cj = np.array([[lo(a, dr, 1), hi(b, dr, 1)] for a, b in rs], np.int32)
+    # x-faces: both ends one further (the face i-1/2 of the block's first cell is a wall),
+    # except the right ends of blocks 1 and 4; r-faces: the lower end one further, except block 1
+    xi = np.array([[lo(a, dx, 2), hi(b, dx, 1 if b_ in (1, 4) else 2)] for b_, (a, b) in enumerate(zs)], np.int32)
+    rj = np.array([[lo(a, dr, 1 if b_ == 1 else 2), hi(b, dr, 1)] for b_, (a, b) in enumerate(rs)], np.int32)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "mw_lists_cathode.json")
+    with open(path) as f:
+        table = json.load(f)
+    blocks = {"ic": ci, "jc": cj}
+    form = re.compile(r"([ij]c)\[(\d)\]\[([01])\]([+-]\d+)?")
+
+    def ev(e):
+        m = form.fullmatch(e)
+        if not m:
+            raise ValueError(f"segment table: unexpected bound {e!r}")
+        return int(blocks[m.group(1)][int(m.group(2))][int(m.group(3))]) + int(m.group(4) or 0)
+
+    lists = {(f_, sd): [] for f_ in "xrp" for sd in "WESN"}
+    for sg in table["segments"]:
+        key = (sg["field"], sg["side"])
+        if sg["kind"] == "point":
+            lists[key].append((ev(sg["i"]), ev(sg["j"]), sg["code"]))
+            continue
+        fix = ev(sg["fix"])
+        for v in range(ev(sg["lo"]), ev(sg["hi"]) + 1):
+            lists[key].append((fix, v, sg["code"]) if sg["var"] == "j" else (v, fix, sg["code"]))
+    return dict(blocks=((xi, cj), (ci, rj), (ci, cj)), lists=lists, j_flc_00=int(cj[0][0]), ni=ni, nj=nj,
+                dx=dx, dr=dr)
+
+
 def rectangle_geometry(ni, nj, Lz=10e-3, Lr=5e-3, width_neutIn=0.0) -> dict:
     """The r-z rectangle as one fluid block: z = 0 grounded wall (the reference's
     z0), z = L the biased electrode (z5), r = R a grounded wall (x1) with the neutral

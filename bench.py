@@ -250,7 +250,8 @@ class _Plane:
 
 
 def linear_systems(pkg, dev, stream, steps=10):
-    """The isolated 512 x 1024 potential and microwave Er systems: ms per solve."""
+    """The isolated potential and microwave systems: ms per solve."""
+    import numpy as np
     import torch
     capi = pkg.capi
     sa = pkg.workloads.poisson_slab(NI, NJ, seed=1)
@@ -307,10 +308,35 @@ def linear_systems(pkg, dev, stream, steps=10):
     out["microwave3_ms"] = e0.elapsed_time(e1) / steps
     out["microwave3_iterations"] = st3.iterations
     out["microwave3_unknowns"] = 3 * NI * NJ - NI - NJ
+    m3.close()
+    # (d) the same system on the cathode geometry (six blocks per field, the makeBoundary
+    # lists), at four times the reference's 194 x 70 in each direction: solve + ghost pass
+    cg = pkg.fluid.cathode_microwave(776, 280)
+    wc = pkg.workloads.mw3_cathode(776, 280, seed=2)
+    gcm = pkg.Grid(776, 280, [[1, 776]], [[1, 280]], device=dev.index)
+    mc = pkg.Microwave3(776, 280, device=dev.index, blocks=cg["blocks"])
+    mc.set_boundary(cg["lists"], cg["j_flc_00"])
+    fc = [gcm.to_device(wc[k]) for k in ("ne", "nu", "Bx", "Br", "epsr")]
+    erc = gcm.to_device(np.zeros((778, 282)))
+    ec = mc.planes(3)
+    for it in range(steps + 2):
+        if it == 2:
+            e0.record(stream)
+        mc.assemble_dev(*fc, wc["params"], stream=stream)
+        _, stc = mc.solve_dev(maxITR=400, error_cnv=TOL, out=ec, stream=stream)
+        mc.fill_ghosts(ec, fc[4], wc["params"], Er_dc=erc, stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    out["microwave3_cathode_ms"] = e0.elapsed_time(e1) / steps
+    out["microwave3_cathode_iterations"] = stc.iterations
+    out["microwave3_cathode_unknowns"] = int(sum(pkg.fluid.block_union_size(*b) for b in cg["blocks"]))
+    mc.close()
+    gcm.close()
     out["workload"] = ("(a) potential with a 1:3.8 dielectric slab, electrodes 0/20 V, axis; (b) microwave Er, "
                        "B = 0 cold plasma (n_e 1e15-1e18, nu 1e8-1e10), port/open/Gauss; (c) magnetised Ex/Er/Ephi "
-                       "system, same plasma, magnet field of 0.05 T near the port; each to 1e-10 from zero")
-    m3.close()
+                       "system, same plasma, magnet field of 0.05 T near the port; (d) the magnetised system on the "
+                       "cathode geometry (38.8 x 14 mm, six blocks per field, the makeBoundary lists) at 776 x 280, "
+                       "same plasma model, magnet 0.05 T at z = 20 mm, solve + ghost pass; each to 1e-10 from zero")
     g.close()
     gb.close()
     return out

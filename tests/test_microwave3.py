@@ -180,3 +180,29 @@ def test_port_of_a_matched_coax_wave():
     assert res["P_fwd_all"] == pytest.approx(8.0, rel=1e-12)  # rescaled to Pmw
     # without any other field the power through the outlet row is zero
     assert res["P_out"] == 0.0
+
+
+@pytest.mark.parametrize("shape", [(194, 70), (97, 35), (388, 140)])
+def test_package_cathode_microwave_matches_oracle(shape):
+    """The package's cathode microwave geometry (blocks and lists, used without
+    the oracle by the bench) equals the oracle's, and its segment table is the
+    golden fixture."""
+    import json
+    import os
+    from importlib import import_module
+    fl = import_module("02_cathode-08_modulerev_b200.fluid")
+    from oracle import microwave as mw
+    ni, nj = shape
+    got = fl.cathode_microwave(ni, nj)
+    p = mw.cathode_mw_params(ni, nj)
+    cells, xf, rf = mw.cathode_mw_blocks(p)
+    for a, b in zip(got["blocks"], (xf, rf, cells)):
+        for x, y in zip(a, b):
+            assert np.array_equal(np.asarray(x), np.asarray(y))
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "mw_lists_cathode.json")) as f:
+        fixture = json.load(f)
+    with open(os.path.join(here, "..", "02_cathode-08_modulerev_b200", "data", "mw_lists_cathode.json")) as f:
+        assert json.load(f) == fixture
+    assert got["lists"] == mw.cathode_mw_lists(cells, fixture)
+    assert got["j_flc_00"] == int(cells[1][0][0])
