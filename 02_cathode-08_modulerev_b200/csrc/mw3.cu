@@ -1253,6 +1253,25 @@ int cth_mw3_apply_dev(cth_mw3* m, const double* x3, double* y3, void* stream) {
     return CTH_OK;
 }
 
+int cth_mw3_set_cycle(cth_mw3* m, int nu_pre, int nu_post) {
+    if (!m || nu_pre < 1 || nu_post < 1 || nu_pre > 8 || nu_post > 8) {
+        set_error("cth_mw3_set_cycle: sweeps must be in 1..8");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(m->device));
+    CTH_CUDA(cudaDeviceSynchronize());
+    for (int c = 0; c < 3; c++) {
+        m->g[c]->nu1 = nu_pre;
+        m->g[c]->nu2 = nu_post;
+    }
+    // the captured solve holds the old cycle: capture again on the next solve
+    if (m->exec) cudaGraphExecDestroy(m->exec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    m->exec = nullptr;
+    m->graph = nullptr;
+    return CTH_OK;
+}
+
 int cth_mw3_set_graphs(cth_mw3* m, int enable) {
     if (!m) {
         set_error("cth_mw3_set_graphs: null handle");

@@ -358,6 +358,10 @@ class Microwave3:
         """One captured graph per solve (default) or kernel-by-kernel launches."""
         capi.check(self._L.cth_mw3_set_graphs(self._h, int(enable)), allow_positive=False)
 
+    def set_cycle(self, nu_pre: int, nu_post: int):
+        """Smoothing sweeps per level of the three fields' V-cycles (default 1, 1)."""
+        capi.check(self._L.cth_mw3_set_cycle(self._h, int(nu_pre), int(nu_post)), allow_positive=False)
+
     def _stream(self, stream):
         import torch
         return (stream if stream is not None else torch.cuda.current_stream(self.device)).cuda_stream

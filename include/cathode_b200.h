@@ -285,6 +285,9 @@ int cth_mw3_fill_ghosts(cth_mw3* m, double* E3, const double* epsr, const double
  * (default, 1) or kernel by kernel with a host convergence test per iteration
  * (0); same kernels, same results */
 int cth_mw3_set_graphs(cth_mw3* m, int enable);
+/* smoothing sweeps per level of the three fields' V-cycles (pre, post in 1..8;
+ * default 1, 1); waits for the device and drops the captured solve */
+int cth_mw3_set_cycle(cth_mw3* m, int nu_pre, int nu_post);
 
 /* Fluid state in HBM -----------------------------------------------------------
  * A field store holds named device planes of the grid's library layout (cell

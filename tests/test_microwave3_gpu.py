@@ -327,3 +327,24 @@ def test_mw3_solve_then_ghosts_matches_direct(pkg, cuda_device):
         assert _rel(got[c][on], want[c][on]) < 1e-8, c
         assert _rel(got[c], want[c]) < 1e-8, c
     m.close(); g.close()
+
+
+def test_mw3_set_cycle(pkg, cuda_device):
+    """More smoothing per level re-captures the solve and reaches the same
+    solution; sweeps outside 1..8 are refused."""
+    ni, nj = 64, 32
+    w, p, mw = _case(pkg, ni, nj)
+    ref = mw.mag_rect_system(w["ne"], w["nu"], w["Bx"], w["Br"], w["epsr"], p)
+    x_ref = mw.mag_pack(ref, mw.mag_rect_solve(ref))
+    g, planes = _device(pkg, w)
+    m = pkg.Microwave3(ni, nj)
+    m.assemble_dev(*planes, w["params"])
+    for nu in ((1, 1), (2, 3), (1, 1)):
+        m.set_cycle(*nu)
+        E, st = m.solve_dev(maxITR=200, error_cnv=1e-12)
+        assert st.converged == 1
+        assert _rel(mw.mag_pack(ref, _to_ij(E, ni)), x_ref) < 1e-8, nu
+    for bad in ((0, 1), (1, 9)):
+        with pytest.raises(pkg.capi.CathodeError):
+            m.set_cycle(*bad)
+    m.close(); g.close()
