@@ -33,7 +33,7 @@ EXPORTS = (
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_mw3_create", "cth_mw3_destroy", "cth_mw3_ld", "cth_mw3_launch_count", "cth_mw3_assemble_dev",
     "cth_mw3_copy_planes", "cth_mw3_apply_dev", "cth_mw3_solve_dev", "cth_mw3_set_graphs",
-    "cth_mw3_create_blocks", "cth_mw3_set_boundary", "cth_mw3_fill_ghosts", "cth_mw3_set_cycle",
+    "cth_mw3_create_blocks", "cth_mw3_set_boundary", "cth_mw3_fill_ghosts", "cth_mw3_set_cycle", "cth_mw3_set_preconditioner",
     "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_fields_set_download_plan", "cth_fields_download_wait", "cth_fields_set_upload_plan", "cth_fields_upload_many",
     "cth_fields_download_many", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
@@ -257,6 +257,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_mw3_fill_ghosts.restype = ctypes.c_int
     L.cth_mw3_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
     L.cth_mw3_set_cycle.restype = ctypes.c_int
+    L.cth_mw3_set_preconditioner.argtypes = [_vp, ctypes.c_int]
+    L.cth_mw3_set_preconditioner.restype = ctypes.c_int
     L.cth_fields_create.argtypes = [_vp, ctypes.POINTER(_vp)]
     L.cth_fields_create.restype = ctypes.c_int
     L.cth_fields_destroy.argtypes = [_vp]

@@ -607,6 +607,44 @@ __global__ void k_m3_gather(Dev3 D, Lev0 L, cd* __restrict__ dst) {
     }
 }
 
+// one field's preconditioner result into dst
+template <int F>
+__global__ void k_m3_gather1(Dev3 D, Lev0 L, cd* __restrict__ dst) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    if (i > D.ni) return;
+    const size_t q0 = (size_t)j * D.ld + i;
+    if (!D.mk[F][q0]) return;
+    dst[(size_t)F * D.pl + q0] = L.x[F][(size_t)(j - L.j0[F]) * L.ldl[F] + (i - L.i0[F])];
+}
+
+// block Gauss-Seidel across the fields (Ex, then Er, then Ephi): field F's
+// preconditioner right-hand side is its part of y (p for MODE 0, s for MODE 1)
+// minus the couplings of its rows to the fields already preconditioned, whose
+// results z are in dst's planes (Er rows: Ex; Ephi rows: Ex and Er)
+template <int MODE, int F>
+__global__ void k_m3_gs(Dev3 D, Lev0 L, const cd* __restrict__ z) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    if (i > D.ni) return;
+    const int ld = D.ld;
+    const size_t pl = D.pl, q = (size_t)j * ld + i;
+    if (!D.mk[F][q]) return;
+    const cd* Y = (MODE == 0 ? D.p : D.s) + (size_t)F * pl;
+    const cd* A = D.a + (size_t)F * NQ * pl;
+    const cd* zx = z;
+    const cd* zr = z + pl;
+    cd b = Y[q];
+    if (F == 1) {
+        b += A[C0 * pl + q] * zx[q + 1] + A[C1 * pl + q] * zx[q + 1 - ld] + A[C2 * pl + q] * zx[q] +
+             A[C3 * pl + q] * zx[q - ld];
+    } else {
+        b += A[C0 * pl + q] * zx[q + 1] + A[C1 * pl + q] * zx[q] + A[C2 * pl + q] * zr[q + ld] +
+             A[C3 * pl + q] * zr[q];
+    }
+    L.b[F][(size_t)(j - L.j0[F]) * L.ldl[F] + (i - L.i0[F])] = b;
+}
+
 // MODE 0: v = A ph, alpha = rho / <rh, v>;  MODE 1: t = A sh, omega = <t, s> / <t, t>
 template <int MODE>
 __global__ void k_m3_mv(Dev3 D, double* __restrict__ part, unsigned int* counter) {
@@ -780,6 +818,7 @@ struct cth_mw3 {
     // rectangle: its lists follow the port radii and cell size of each assembly
     bool rect = false;
     double rect_key[4] = {0.0, 0.0, 0.0, 0.0};
+    bool gauss_seidel = false;  // preconditioner: block Jacobi (default) or block Gauss-Seidel across the fields
 };
 
 namespace {
@@ -883,25 +922,43 @@ cudaError_t solve_body(cth_mw3* m, cudaStream_t s, cudaGraphConditionalHandle co
     Dev3 D = dev3(m);
     Lev0 L = lev0(m);
     dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
-    auto precond = [&]() -> cudaError_t {
-        cudaError_t e = fork3(m, 1, s);
-        if (e != cudaSuccess) return e;
+    // the preconditioner applied to p (mode 0) or s (mode 1), result into dst
+    auto precond = [&](int mode, cd* dst) -> cudaError_t {
+        if (!m->gauss_seidel) {  // block Jacobi: the three V-cycles side by side
+            cudaError_t e = fork3(m, 1, s);
+            if (e != cudaSuccess) return e;
+            *n += cmg_vcycle(m->g[0], s);
+            for (int k = 0; k < 2; k++) *n += cmg_vcycle(m->g[1 + k], m->side[1][k]);
+            e = join3(m, 1, s);
+            if (e != cudaSuccess) return e;
+            k_m3_gather<<<grd, blk, 0, s>>>(D, L, dst);
+            *n += 1;
+            return cudaGetLastError();
+        }
+        // block Gauss-Seidel: Ex, then Er and Ephi with the known fields' couplings taken out
         *n += cmg_vcycle(m->g[0], s);
-        for (int k = 0; k < 2; k++) *n += cmg_vcycle(m->g[1 + k], m->side[1][k]);
-        return join3(m, 1, s);
+        k_m3_gather1<0><<<grd, blk, 0, s>>>(D, L, dst);
+        if (mode == 0) k_m3_gs<0, 1><<<grd, blk, 0, s>>>(D, L, dst);
+        else k_m3_gs<1, 1><<<grd, blk, 0, s>>>(D, L, dst);
+        *n += cmg_vcycle(m->g[1], s);
+        k_m3_gather1<1><<<grd, blk, 0, s>>>(D, L, dst);
+        if (mode == 0) k_m3_gs<0, 2><<<grd, blk, 0, s>>>(D, L, dst);
+        else k_m3_gs<1, 2><<<grd, blk, 0, s>>>(D, L, dst);
+        *n += cmg_vcycle(m->g[2], s);
+        k_m3_gather1<2><<<grd, blk, 0, s>>>(D, L, dst);
+        *n += 5;
+        return cudaGetLastError();
     };
     k_m3_vec<0><<<grd, blk, 0, s>>>(D, L);
-    cudaError_t e = precond();
+    cudaError_t e = precond(0, D.ph);
     if (e != cudaSuccess) return e;
-    k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.ph);
     k_m3_mv<0><<<grd, blk, 0, s>>>(D, m->part, m->counter);
     k_m3_vec<1><<<grd, blk, 0, s>>>(D, L);
-    e = precond();
+    e = precond(1, D.sh);
     if (e != cudaSuccess) return e;
-    k_m3_gather<<<grd, blk, 0, s>>>(D, L, D.sh);
     k_m3_mv<1><<<grd, blk, 0, s>>>(D, m->part, m->counter);
     k_m3_upd<<<grd, blk, 0, s>>>(D, m->d_args, m->part, m->counter, cond, use_cond);
-    *n += 7;
+    *n += 5;
     return cudaGetLastError();
 }
 
@@ -1265,6 +1322,21 @@ int cth_mw3_set_cycle(cth_mw3* m, int nu_pre, int nu_post) {
         m->g[c]->nu2 = nu_post;
     }
     // the captured solve holds the old cycle: capture again on the next solve
+    if (m->exec) cudaGraphExecDestroy(m->exec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    m->exec = nullptr;
+    m->graph = nullptr;
+    return CTH_OK;
+}
+
+int cth_mw3_set_preconditioner(cth_mw3* m, int mode) {
+    if (!m || mode < 0 || mode > 1) {
+        set_error("cth_mw3_set_preconditioner: mode 0 (block Jacobi) or 1 (block Gauss-Seidel)");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(m->device));
+    CTH_CUDA(cudaDeviceSynchronize());
+    m->gauss_seidel = mode == 1;
     if (m->exec) cudaGraphExecDestroy(m->exec);
     if (m->graph) cudaGraphDestroy(m->graph);
     m->exec = nullptr;

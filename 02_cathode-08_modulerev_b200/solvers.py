@@ -106,6 +106,11 @@ class Grid:
                    allow_positive=False)
         return us.value, by.value
 
+    def set_preconditioner(self, mode: int):
+        """0: block Jacobi (the fields' V-cycles side by side, default); 1: block
+        Gauss-Seidel across Ex, Er, Ephi."""
+        capi.check(self._L.cth_mw3_set_preconditioner(self._h, int(mode)), allow_positive=False)
+
     def set_cycle(self, nu_pre: int, nu_post: int):
         capi.check(self._L.cth_grid_set_cycle(self._h, nu_pre, nu_post), allow_positive=False)
 
@@ -357,6 +362,11 @@ class Microwave3:
     def set_graphs(self, enable: bool):
         """One captured graph per solve (default) or kernel-by-kernel launches."""
         capi.check(self._L.cth_mw3_set_graphs(self._h, int(enable)), allow_positive=False)
+
+    def set_preconditioner(self, mode: int):
+        """0: block Jacobi (the fields' V-cycles side by side, default); 1: block
+        Gauss-Seidel across Ex, Er, Ephi."""
+        capi.check(self._L.cth_mw3_set_preconditioner(self._h, int(mode)), allow_positive=False)
 
     def set_cycle(self, nu_pre: int, nu_post: int):
         """Smoothing sweeps per level of the three fields' V-cycles (default 1, 1)."""

@@ -288,6 +288,12 @@ int cth_mw3_set_graphs(cth_mw3* m, int enable);
 /* smoothing sweeps per level of the three fields' V-cycles (pre, post in 1..8;
  * default 1, 1); waits for the device and drops the captured solve */
 int cth_mw3_set_cycle(cth_mw3* m, int nu_pre, int nu_post);
+/* preconditioner: 0 = block Jacobi, the three fields' V-cycles side by side
+ * (default); 1 = block Gauss-Seidel, Ex then Er then Ephi, each V-cycle's
+ * right-hand side with the couplings to the fields before it taken out (the
+ * V-cycles run one after another).  Waits for the device, drops the captured
+ * solve. */
+int cth_mw3_set_preconditioner(cth_mw3* m, int mode);
 
 /* Fluid state in HBM -----------------------------------------------------------
  * A field store holds named device planes of the grid's library layout (cell

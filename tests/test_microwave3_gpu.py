@@ -348,3 +348,33 @@ def test_mw3_set_cycle(pkg, cuda_device):
         with pytest.raises(pkg.capi.CathodeError):
             m.set_cycle(*bad)
     m.close(); g.close()
+
+
+@pytest.mark.parametrize("geometry", ["rectangle", "cathode"])
+def test_mw3_gauss_seidel_matches_direct(pkg, cuda_device, geometry):
+    """The block Gauss-Seidel preconditioner reaches the direct solution, in the
+    captured graph and kernel by kernel alike."""
+    if geometry == "cathode":
+        w, mw, ref, m, g = _cathode(pkg, 194, 70)
+        ni = 194
+    else:
+        ni, nj = 96, 40
+        w, p, mw = _case(pkg, ni, nj)
+        ref = mw.mag_rect_system(w["ne"], w["nu"], w["Bx"], w["Br"], w["epsr"], p)
+        g, planes = _device(pkg, w)
+        m = pkg.Microwave3(ni, nj)
+        m.assemble_dev(*planes, w["params"])
+    x_ref = mw.mag_pack(ref, mw.mag_rect_solve(ref))
+    m.set_preconditioner(1)
+    its = []
+    for graphs in (True, False):
+        m.set_graphs(graphs)
+        E, st = m.solve_dev(maxITR=600, error_cnv=1e-12)
+        assert st.converged == 1, st.as_dict()
+        assert _rel(mw.mag_pack(ref, _to_ij(E, ni)), x_ref) < 1e-8
+        its.append(st.iterations)
+    assert its[0] == its[1]
+    print("mw3 gauss-seidel", geometry, its[0])
+    with pytest.raises(pkg.capi.CathodeError):
+        m.set_preconditioner(2)
+    m.close(); g.close()
