@@ -396,6 +396,8 @@ def main():
     ap.add_argument("--profile-network", type=int, default=0,
                     help="profiling mode: the warm-start network alone at 512 x 1024 -- after --warmup forward "
                          "passes and training steps, this many more of each on seeded inputs, then exit")
+    ap.add_argument("--mw-geometry", choices=("rectangle", "cathode"), default="rectangle",
+                    help="geometry of --profile-microwave: the 512 x 1024 rectangle or the cathode at 776 x 280")
     ap.add_argument("--profile-microwave", type=int, default=0,
                     help="profiling mode: this many solves of the magnetised 3-component microwave system at "
                          "512 x 1024 (seeded magnet workload) after --warmup ones, launched kernel by kernel "
@@ -418,18 +420,28 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if args.profile_microwave > 0:
-        w3 = pkg.workloads.mw3_rect(NI, NJ, seed=2)
-        gm = pkg.Grid(NI, NJ, [[1, NI]], [[1, NJ]], device=local)
-        m3 = pkg.Microwave3(NI, NJ, device=local)
+        if args.mw_geometry == "cathode":  # 776 x 280 cathode: blocks and makeBoundary lists, solve + ghosts
+            ni3, nj3 = 776, 280
+            cg = pkg.fluid.cathode_microwave(ni3, nj3)
+            w3 = pkg.workloads.mw3_cathode(ni3, nj3, seed=2)
+            m3 = pkg.Microwave3(ni3, nj3, device=local, blocks=cg["blocks"])
+            m3.set_boundary(cg["lists"], cg["j_flc_00"])
+        else:
+            ni3, nj3 = NI, NJ
+            w3 = pkg.workloads.mw3_rect(NI, NJ, seed=2)
+            m3 = pkg.Microwave3(NI, NJ, device=local)
+        gm = pkg.Grid(ni3, nj3, [[1, ni3]], [[1, nj3]], device=local)
         m3.set_graphs(False)
         f3 = [gm.to_device(w3[k]) for k in ("ne", "nu", "Bx", "Br", "epsr")]
+        erdc = gm.to_device(np.zeros((ni3 + 2, nj3 + 2)))
         e3 = m3.planes(3)
         for _ in range(args.warmup + args.profile_microwave):
             m3.assemble_dev(*f3, w3["params"])
-            _, st3 = m3.solve_dev(maxITR=200, error_cnv=TOL, out=e3)
+            _, st3 = m3.solve_dev(maxITR=400, error_cnv=TOL, out=e3)
+            m3.fill_ghosts(e3, f3[4], w3["params"], Er_dc=erdc)
         torch.cuda.synchronize(dev)
-        print(f"profiled {args.profile_microwave} magnetised microwave solves after {args.warmup} warm-up ones "
-              f"({st3.iterations} iterations each)", flush=True)
+        print(f"profiled {args.profile_microwave} magnetised microwave solves ({args.mw_geometry}, {ni3} x {nj3}) "
+              f"after {args.warmup} warm-up ones ({st3.iterations} iterations each)", flush=True)
         m3.close()
         gm.close()
         return 0
