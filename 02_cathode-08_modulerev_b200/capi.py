@@ -37,7 +37,7 @@ EXPORTS = (
     "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_fields_set_download_plan", "cth_fields_download_wait", "cth_fields_set_upload_plan", "cth_fields_upload_many",
     "cth_fields_download_many", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
-    "cth_ghost_rules_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
+    "cth_ghost_rules_upload", "cth_energy_keep_walls_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
     "cth_batch_steps", "cth_update_energy_profile", "cth_mw_port_rescale", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_tensor_cores", "cth_unet_set_smoothing", "cth_unet_set_wait_test", "cth_unet_set_grid_limit", "cth_unet_check", "cth_unet_set_params", "cth_unet_get_params",
@@ -291,6 +291,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_check_cfl.restype = ctypes.c_int
     L.cth_ghost_rules_upload.argtypes = [_vp, _vp, ctypes.c_int]
     L.cth_ghost_rules_upload.restype = ctypes.c_int
+    L.cth_energy_keep_walls_upload.argtypes = [_vp, _vp, ctypes.c_int]
+    L.cth_energy_keep_walls_upload.restype = ctypes.c_int
     for nm in ("cth_solve_rhoe_pc", "cth_solve_Te_pc"):
         getattr(L, nm).argtypes = [_vp, ctypes.POINTER(SGParams), _vp, ctypes.POINTER(PCResult)]
         getattr(L, nm).restype = ctypes.c_int

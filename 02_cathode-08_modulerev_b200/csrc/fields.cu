@@ -676,6 +676,24 @@ int cth_ghost_rules_upload(cth_fields* fs, const int* rules, int n) {
     return CTH_OK;
 }
 
+int cth_energy_keep_walls_upload(cth_fields* fs, const int* boxes, int n) {
+    if (!fs || n < 0 || n > CTH_KEEP_WALL_MAX || (n > 0 && !boxes)) {
+        set_error("cth_energy_keep_walls_upload: invalid arguments (at most 4 boxes)");
+        return CTH_ERR_ARG;
+    }
+    const cth_grid* g = fs->g;
+    for (int q = 0; q < n; q++) {
+        const int* B = boxes + 4 * q;
+        if (!(B[0] <= B[1] && B[2] <= B[3] && B[0] >= 0 && B[1] <= g->ni + 1 && B[2] >= 0 && B[3] <= g->nj + 1)) {
+            set_error("cth_energy_keep_walls_upload: a box must be a non-empty range of the index space");
+            return CTH_ERR_ARG;
+        }
+    }
+    for (int q = 0; q < 4 * n; q++) fs->keep_wall[q] = boxes[q];
+    fs->n_keep_wall = n;
+    return CTH_OK;
+}
+
 int cth_check_cfl(cth_fields* fs, cth_cfl* io, void* stream) {
     if (!fs || !io) { set_error("cth_check_cfl: invalid arguments"); return CTH_ERR_ARG; }
     cth_grid* g = fs->g;

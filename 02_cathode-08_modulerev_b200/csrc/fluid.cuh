@@ -13,11 +13,14 @@
 
 #define CTH_FS_NSCAL 96
 #define CTH_FS_NPART_PER_BLOCK 16
+#define CTH_KEEP_WALL_MAX 4
 
 struct cth_fields {
     cth_grid* g = nullptr;
     int* ghost_rules = nullptr;      // device, 7 ints per rule (i0, i1, j0, j1, di, dj, rhoe_mode)
     int n_ghost_rules = 0;
+    int keep_wall[4 * CTH_KEEP_WALL_MAX] = {};  // r-face boxes where the energy sweep keeps Gr_wall
+    int n_keep_wall = 0;
     cth_ion_op* ion_ops[CTH_ION_NPROG] = {};  // wall programs of the ion step
     int ion_nops[CTH_ION_NPROG] = {};
     int* ion_boxes[4] = {};                    // residual boxes (rhoi, Uix, Uir, Uip)

@@ -37,6 +37,8 @@ struct SgArgs {
     Tab eb, rd, ts;
     cth_sg_params prm;
     int ni, nj, ld;
+    int nkw;                               // energy sweep: r-face boxes whose Gr_wall is kept
+    int kw[4 * CTH_KEEP_WALL_MAX];
 };
 
 #define FL(ii, jj) flag_at(A.flags, (ii), (jj), A.ni, A.nj, A.ld)
@@ -182,13 +184,17 @@ __global__ void k_sg_predict(SgArgs A) {
         const double sg = EN ? (f.A() * A.n[p - ld] - f.B() * A.n[p]) * fac / 3.0 : f.A() * A.n[p - ld] - f.B() * A.n[p];
         vr = sg + A.Fr_t[p] - f.mst * (ixr * Fx_i + irr * A.Fr_t[p]);
     }
+    bool rec = true;  // energy sweep: the lower wall x2 sets Gr but not Gr_wall (fluidModule.hpp:4428-4449)
+    if (EN)
+        for (int q = 0; q < A.nkw; q++)
+            if (i >= A.kw[4 * q] && i <= A.kw[4 * q + 1] && j >= A.kw[4 * q + 2] && j <= A.kw[4 * q + 3]) rec = false;
     if (fc && !(fc & F_BLR_WALL)) {
         vr = sg_wall<EN>(A, p, A.Er[p], A.Uir[p], A.rhoUmr[p], dr, -1.0);
-        A.Fr_w[p] = vr;
+        if (rec) A.Fr_w[p] = vr;
     }
     if (fs && !(fs & F_BRR_WALL)) {
         vr = sg_wall<EN>(A, p - ld, A.Er[p], A.Uir[p], A.rhoUmr[p], dr, 1.0);
-        A.Fr_w[p] = vr;
+        if (rec) A.Fr_w[p] = vr;
     }
     if (fs && !(fs & F_BRR_OPEN)) {
         vr = EN ? 5.0 / 2.0 * kBoltz * A.Te_old[p - ld] * fmax(A.rhoUer[p], 0.0) : A.rhoi[p - ld] * A.Uir[p];
@@ -365,6 +371,8 @@ static int solve_sg_pc(cth_fields* fs, const cth_sg_params* prm, cudaStream_t s,
     }
     A.flags = fs->flags;
     A.prm = *prm;
+    A.nkw = fs->n_keep_wall;
+    for (int q = 0; q < 4 * CTH_KEEP_WALL_MAX; q++) A.kw[q] = fs->keep_wall[q];
     A.ni = g->ni;
     A.nj = g->nj;
     A.ld = g->ld;

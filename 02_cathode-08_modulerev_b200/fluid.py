@@ -25,7 +25,10 @@ TABLES = ("nu_elas_N", "nu_exc_N", "nu_excReso_N", "nu_excMeta_N", "nu_ionz_N", 
 def cathode_blocks(ni=194, nj=70, xR=0.0388, rmax=0.014):
     """Fluid cell blocks 0..4 of InitialModule::makeBoundary (initialModule.hpp:219-263)."""
     dx, dr = xR / ni, rmax / nj
-    x2, x3, x4, x5, x6 = 13.4e-3, 17.8e-3, 22.8e-3, 27.8e-3, 7.8e-3
+    # formed as the reference forms them (initialModule.hpp:225-230): the sums round differently
+    # from the literals, which moves a block edge where x / dx lands on .5 (97 x 35)
+    x6 = 0.0e-3 + 7.8e-3
+    x2, x3, x4, x5 = 5.6e-3 + 7.8e-3, 10.0e-3 + 7.8e-3, 15.0e-3 + 7.8e-3, 20.0e-3 + 7.8e-3
     r1, r3, r4, r5 = 0.6e-3, 4.0e-3, 9.0e-3, 2.0e-3
     lo = lambda v, d: int(v / d + 0.5) + 1
     hi = lambda v, d: int(v / d - 0.5) + 1
@@ -353,6 +356,18 @@ class Fields:
         a = np.ascontiguousarray(np.asarray(rules, dtype=np.int32).reshape(-1, 7))
         capi.check(self._L.cth_ghost_rules_upload(self._h, a.ctypes.data, a.shape[0]), allow_positive=False)
 
+    def set_energy_keep_walls(self, boxes):
+        """r-face boxes (i0, i1, j0, j1) whose wall flux Gr_wall the energy sweep leaves unchanged
+        (the cathode's lower wall x2, fluidModule.hpp:4428-4449); at most 4."""
+        a = np.ascontiguousarray(np.asarray(boxes, dtype=np.int32).reshape(-1, 4))
+        capi.check(self._L.cth_energy_keep_walls_upload(self._h, a.ctypes.data, a.shape[0]), allow_positive=False)
+
+    def set_geometry(self, geo):
+        """Side flags, electron ghost rules and the energy sweep's kept walls of a geometry dict."""
+        self.set_flags(geo["flags"])
+        self.set_ghost_rules(geo["ghosts"])
+        self.set_energy_keep_walls(geo.get("energy_keep_walls", []))
+
     def _sg(self, fn, prm, stream):
         p = capi.SGParams(**{k: prm[k] for k, _ in capi.SGParams._fields_})
         res = capi.PCResult()
@@ -388,7 +403,10 @@ def cathode_geometry(ni=194, nj=70, xR=0.0388, rmax=0.014, width_neutIn=0.0055) 
     sweeps on the cell, x-face and r-face index sets (fluidModule.hpp:218-360,
     :700-800, :1130-1200)."""
     dx, dr = xR / ni, rmax / nj
-    x2, x3, x4, x5, x6 = 13.4e-3, 17.8e-3, 22.8e-3, 27.8e-3, 7.8e-3
+    # formed as the reference forms them (initialModule.hpp:225-230): the sums round differently
+    # from the literals, which moves a block edge where x / dx lands on .5 (97 x 35)
+    x6 = 0.0e-3 + 7.8e-3
+    x2, x3, x4, x5 = 5.6e-3 + 7.8e-3, 10.0e-3 + 7.8e-3, 15.0e-3 + 7.8e-3, 20.0e-3 + 7.8e-3
     r1, r3, r4, r5 = 0.6e-3, 4.0e-3, 9.0e-3, 2.0e-3
     lo = lambda v, d, k: int(v / d + 0.5) + k
     hi = lambda v, d, k: int(v / d - 0.5) + k
@@ -425,7 +443,10 @@ def cathode_geometry(ni=194, nj=70, xR=0.0388, rmax=0.014, width_neutIn=0.0055) 
     return dict(ni=ni, nj=nj, dx=dx, dr=dr, ib=ib, jb=jb, fxi=fxi, fxj=fxj, fri=fri, frj=frj, flags=flags,
                 ghosts=[tuple(int(v) for v in g) for g in ghosts], seg=seg, x6=x6, xL=0.0,
                 width_neutIn=width_neutIn, pos_boxes=[tuple(int(v) for v in (ib[b][0], ib[b][1], jb[b][0], jb[b][1]))
-                                                      for b in range(2)])
+                                                      for b in range(2)],
+                # the energy sweep's lower-wall loop x2 sets Gr there but leaves Gr_wall as it was
+                # (fluidModule.hpp:4428-4449, unlike x0 at :4423): r-faces (i0, i1, j0, j1)
+                energy_keep_walls=[(int(ib[2][0]), int(ib[2][1]), int(jb[2][0]), int(jb[2][0]))])
 
 
 def block_union_size(ib, jb) -> int:
@@ -507,7 +528,7 @@ def rectangle_geometry(ni, nj, Lz=10e-3, Lr=5e-3, width_neutIn=0.0) -> dict:
             flags[i, nj] |= F_BRR_INLET
     return dict(ni=ni, nj=nj, dx=dx, dr=Lr / nj, ib=one(1, ni), jb=one(1, nj), fxi=one(2, ni), fxj=one(1, nj),
                 fri=one(1, ni), frj=one(2, nj), flags=flags, ghosts=ghosts, seg=seg, x6=0.0, xL=0.0,
-                width_neutIn=width_neutIn, pos_boxes=[(1, ni, 1, nj)])
+                width_neutIn=width_neutIn, pos_boxes=[(1, ni, 1, nj)], energy_keep_walls=[])
 
 
 _K = dict(WALL_FOLD=1, ZERO_COEF=2, FOLD_SUB=3, OPEN_FOLD=4, SET_WALL=5, SET_ZERO=6, COPY=7, SET_OPEN=8)

@@ -202,6 +202,7 @@ def make_case(pkg, ni, nj, seed, V_bias, device=0, Lz=10e-3, Lr=5e-3):
     fs = pkg.Fields(g)
     fs.set_flags(geo["flags"])
     fs.set_ghost_rules(geo["ghosts"])
+    fs.set_energy_keep_walls(geo.get("energy_keep_walls", []))
     fs.set_ion_geometry(geo)
     for k, v in cfg["tables"].items():
         fs.set_table(k, v)

@@ -479,6 +479,7 @@ def main():
     fs = pkg.Fields(g)
     fs.set_flags(geo["flags"])
     fs.set_ghost_rules(geo["ghosts"])
+    fs.set_energy_keep_walls(geo.get("energy_keep_walls", []))
     fs.set_ion_geometry(geo)
     for k, v in cfg["tables"].items():
         fs.set_table(k, v)

@@ -411,6 +411,13 @@ int cth_check_cfl(cth_fields* fs, cth_cfl* io, void* stream);
  * copied).  Later rules win where targets coincide. */
 int cth_ghost_rules_upload(cth_fields* fs, const int* rules, int n);
 
+/* r-face boxes whose recorded wall flux Gr_wall the electron energy sweep leaves
+ * unchanged: the reference's lower-wall loop x2 of solve_Te_wdTe_wSEE_PC sets
+ * gr.Gr there but not gr.Gr_wall (fluidModule.hpp:4428-4449; the other walls
+ * record it, :4423, :4470, :4494, :4504).  n boxes of 4 ints (i0, i1, j0, j1),
+ * inclusive r-face indices, n <= 4; n = 0 records every wall (the default). */
+int cth_energy_keep_walls_upload(cth_fields* fs, const int* boxes, int n);
+
 /* Warm start of the field-valued solves (no counterpart in the reference, whose
  * solves start from zero): with enable != 0 the ion momentum (Uix, Uir, Uip),
  * ion continuity (rhoi) and neutral (rhon, rhom) solves of the SMG path start

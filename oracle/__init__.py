@@ -24,10 +24,13 @@ _u8p = ctypes.POINTER(ctypes.c_ubyte)
 
 
 def build(force: bool = False) -> str:
-    """Compile liboracle.so (and complex/assembly parts) with the Makefile."""
+    """Compile liboracle.so with the Makefile and, when the reference sources are
+    present, the checker library oracle/_ref/libref.so compiled from them (ref.py)."""
     so = os.path.join(_HERE, "liboracle.so")
     if force or not os.path.exists(so) or _stale(so):
         subprocess.run(["make", "-C", _HERE, "-s"], check=True)
+    from . import ref
+    ref.build(force=force)
     return so
 
 
@@ -67,6 +70,26 @@ def _declare(L):
     L.orc_calc_res.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, ctypes.c_int, _dp, _dp,
                                ctypes.c_double, ctypes.c_int]
     L.orc_calc_res.restype = ctypes.c_double
+    for name in ("orc_exp", "orc_erf"):
+        getattr(L, name).argtypes = [ctypes.c_size_t, _dp, _dp]
+        getattr(L, name).restype = None
+
+
+def _elementwise(name, x):
+    a = np.array(x, dtype=np.float64, order="C")   # keeps 0-d inputs 0-d
+    out = np.empty_like(a)
+    getattr(lib(), name)(a.size, a.ctypes.data_as(_dp), out.ctypes.data_as(_dp))
+    return out if out.ndim else float(out)
+
+
+def libm_exp(x):
+    """exp() of the C library, element-wise (the reference's exp)."""
+    return _elementwise("orc_exp", x)
+
+
+def libm_erf(x):
+    """erf() of the C library, element-wise (the reference's erf)."""
+    return _elementwise("orc_erf", x)
 
 
 def _d(a: np.ndarray):

@@ -9,6 +9,13 @@ from __future__ import annotations
 
 import numpy as np
 
+
+def _exp(x):
+    """exp() of the C library, as the reference evaluates it (numpy's vectorised exp
+    differs by one ulp on a few per cent of arguments)."""
+    import oracle
+    return oracle.libm_exp(x)
+
 BOLTZ = 1.380649e-23
 E0 = 1.60217662e-19
 EPS0 = 8.8541878128e-12
@@ -210,7 +217,7 @@ def synthetic_tables(n_e: int = 1801, n_i: int = 40, d_eps_eV: float = 150.0 / 1
     eps = np.arange(n_e) * d_eps_eV
     Te = 2.0 / 3.0 * eps
     with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
-        kion = np.where(Te > 0, 1e-13 * np.sqrt(Te) * np.exp(-12.13 / np.maximum(Te, 1e-30)), 0.0)
+        kion = np.where(Te > 0, 1e-13 * np.sqrt(Te) * _exp(-12.13 / np.maximum(Te, 1e-30)), 0.0)
     kel = np.full(n_e, 2e-13)
     tb = {k: np.zeros(n_e) for k in TABLES if k != "nui_m_N"}
     tb["nu_elas_N"] = kel
@@ -304,9 +311,12 @@ def cathode_geometry(ni: int = 194, nj: int = 70, xR: float = 0.0388, rmax: floa
               (ib[0][0], ib[0][1], jb[0][0], jb[0][0], 0, -1, 0),            # antenna
               (ib[1][1], ib[1][1], jb[1][0], jb[1][1], 1, 0, 1),             # right open
               (ib[0][0], ib[1][1], jb[0][1], jb[0][1], 0, 1, 1)]             # upper open
+    # the energy sweep's lower-wall loop x2 (fluidModule.hpp:4428-4449) sets Gr but not Gr_wall:
+    # r-face box (i0, i1, j0, j1) where Gr_wall keeps its value
+    keep = [(int(ib[2][0]), int(ib[2][1]), int(jb[2][0]), int(jb[2][0]))]
     return dict(ni=ni, nj=nj, dx=dx, dr=dr, ib=ib, jb=jb, fxi=np.array(fxi), fxj=np.array(fxj),
                 fri=np.array(fri), frj=np.array(frj), segs=segs, flags=cathode_flags(ni, nj, ib, jb),
-                ghosts=ghosts)
+                ghosts=ghosts, energy_keep_walls=keep)
 
 
 def rectangle_geometry(ni: int, nj: int, Lz: float = 10e-3, Lr: float = 5e-3) -> dict:
@@ -343,7 +353,7 @@ def _wall_flux(Te, rhoe, rhoe_old, rhoi, Ui, rhoUm, E_old, h, sign, prm, see):
     sign -1 for a wall on the low side of the cell, +1 on the high side."""
     vth = np.sqrt(8.0 * BOLTZ * Te / (np.pi * prm["masse"]))
     delta_phi = np.fmax(sign * E_old * h / 2.0, 0.0)
-    gpn = sign * 0.25 * vth * np.exp(np.fmin(-E0 * delta_phi / (BOLTZ * Te + 1e-100), 100.0))
+    gpn = sign * 0.25 * vth * _exp(np.fmin(-E0 * delta_phi / (BOLTZ * Te + 1e-100), 100.0))
     eb, rd, ts, dTe_SEE = see
     c = func_Te(eb, Te, dTe_SEE) + func_Te(rd, Te, dTe_SEE) + func_Te(ts, Te, dTe_SEE)
     see_flux = -prm["coefIISEE_ts"] * rhoi * Ui - c * rhoe_old * gpn - prm["coefMISEE_ts"] * rhoUm
@@ -569,7 +579,7 @@ EPS_VD = 1.0e-3  # fluidModule.hpp:3100
 
 def _sg(vd, z):
     """Upwind / downwind weights vd/(1-e^-z), vd/(e^z-1) with the exponent clipped at 100."""
-    return vd / (1.0 - np.exp(np.fmin(-z, LIM_EXP))), vd / (np.exp(np.fmin(z, LIM_EXP)) - 1.0)
+    return vd / (1.0 - _exp(np.fmin(-z, LIM_EXP))), vd / (_exp(np.fmin(z, LIM_EXP)) - 1.0)
 
 
 def _sg_face_x(Te, Ex, mu_perp, I, J, dx):
@@ -601,7 +611,7 @@ def _energy_wall(Te_old, Te, E, rhoeps, rhoeps_old, rhoe_old, rhoi, Ui, rhoUm, h
     """Electron energy flux through a wall face (fluidModule.hpp:4175-4190)."""
     vth = np.sqrt(8.0 * BOLTZ * Te_old / (np.pi * prm["masse"]))
     delta_phi = np.fmax(sign * E * h / 2.0, 0.0)
-    ex = np.exp(np.fmin(-E0 * delta_phi / (BOLTZ * Te_old + 1e-100), LIM_EXP))
+    ex = _exp(np.fmin(-E0 * delta_phi / (BOLTZ * Te_old + 1e-100), LIM_EXP))
     gpn_eps = sign * vth * ex / 3.0 * 1.0
     eps_emit = 2.0 * E0 * prm["Te_emitSEE_eV"]
     gpn = sign * 0.25 * 1.0 * vth * ex
@@ -719,7 +729,12 @@ def solve_sg_pc(st: dict, prm: dict, geo: dict, see, solve, species: str) -> dic
                     v = _wall_flux(Te[I, c], n[I, c], n_old[I, c], g["rhoi"][I, c], g["Uir"][I, f], g["rhoUmr"][I, f],
                                    Er[I, f], dr, sg, prm, see)
                 Fr[I, f] = v
-                Fr_w[I, f] = v
+                rec = np.ones(I.size, bool)
+                if en:
+                    for (a, b, c0, c1) in geo.get("energy_keep_walls", ()):
+                        if c0 <= f <= c1:
+                            rec &= ~((I >= a) & (I <= b))
+                Fr_w[I[rec], f] = v[rec]
             elif kind == "O":
                 if en:
                     Fr[I, j0 + 1] = 5.0 / 2.0 * BOLTZ * Te_old[I, j0] * np.fmax(g["rhoUer"][I, j0 + 1], 0.0)
@@ -740,7 +755,7 @@ def solve_sg_pc(st: dict, prm: dict, geo: dict, see, solve, species: str) -> dic
             _, vLr, zLr = _sg_face_r(Tsg, Er, mu_perp, I, J, dr)
             _, vRr, zRr = _sg_face_r(Tsg, Er, mu_perp, I, J + 1, dr)
             bLx, bRx, bLr, bRr = m["bLx"][I, J], m["bRx"][I, J], m["bLr"][I, J], m["bRr"][I, J]
-            ex = np.exp
+            ex = _exp
             tterm = 3.0 / 5.0 * dx * dr / dt if en else dx * dr / dt
             aP[I, J] = (vRx / (1.0 - ex(np.fmin(-zRx, LIM_EXP))) * bRx * dr
                         + vLx / (ex(np.fmin(zLx, LIM_EXP)) - 1.0) * bLx * dr
@@ -889,8 +904,8 @@ def _ui_wall(Uold, phi_a, phi_b, sign, bias, prm):
 
 
 def _erf(x):
-    from scipy.special import erf
-    return erf(x)
+    import oracle
+    return oracle.libm_erf(x)
 
 
 def ion_step(st: dict, prm: dict, geo: dict, solve_c, solve_x, solve_r) -> dict:
@@ -1108,13 +1123,13 @@ def ion_step(st: dict, prm: dict, geo: dict, solve_c, solve_x, solve_r) -> dict:
         bLx, bRx, bLr, bRr = m["bLx"][I, J], m["bRx"][I, J], m["bLr"][I, J], m["bRrw"][I, J]
         bLrw = m["bLrw"][I, J]
         utx = ULx / (um + 1e-100)
-        GLx = np.where(bLx, 0.0, -0.25 * vth * (np.exp(-utx * utx) + utx * sq * (_erf(utx) - 1.0)))
+        GLx = np.where(bLx, 0.0, -0.25 * vth * (_exp(-utx * utx) + utx * sq * (_erf(utx) - 1.0)))
         utx = URx / (um + 1e-100)
-        GRx = np.where(bRx, 0.0, 0.25 * vth * (np.exp(-utx * utx) + utx * sq * (_erf(utx) + 1.0)))
+        GRx = np.where(bRx, 0.0, 0.25 * vth * (_exp(-utx * utx) + utx * sq * (_erf(utx) + 1.0)))
         utr = ULr / (um + 1e-100)
-        GLr = np.where(bLrw, 0.0, -0.25 * vth * (np.exp(-utr * utr) + utr * sq * (_erf(utr) - 1.0)))
+        GLr = np.where(bLrw, 0.0, -0.25 * vth * (_exp(-utr * utr) + utr * sq * (_erf(utr) - 1.0)))
         utr = URr / (um + 1e-100)
-        GRr = np.where(bRr, 0.0, 0.25 * vth * (np.exp(-utr * utr) + utr * sq * (_erf(utr) + 1.0)))
+        GRr = np.where(bRr, 0.0, 0.25 * vth * (_exp(-utr * utr) + utr * sq * (_erf(utr) + 1.0)))
         aP[I, J] = ((URx + np.abs(URx)) / (2.0 * dx) * bRx - (ULx - np.abs(ULx)) / (2.0 * dx) * bLx
                     + qR * (URr + np.abs(URr)) / (2.0 * dr) * bRr - qL * (ULr - np.abs(ULr)) / (2.0 * dr) * bLr
                     + ((DRx * bRx + DLx * bLx) / (dx * dx) + (qR * DRr * bRr + qL * DLr * bLr) / (dr * dr))
@@ -1138,7 +1153,7 @@ def ion_step(st: dict, prm: dict, geo: dict, solve_c, solve_x, solve_r) -> dict:
 
     def gpn(u, sign):
         ut = u / (um + 1e-100)
-        return sign * 0.25 * vth * (np.exp(-ut * ut) + ut * sq * (_erf(ut) + sign * 1.0))
+        return sign * 0.25 * vth * (_exp(-ut * ut) + ut * sq * (_erf(ut) + sign * 1.0))
 
     for name in ("z0", "z1", "z2", "z4"):
         for i, j in _pts(C[name]):

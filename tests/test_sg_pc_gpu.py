@@ -35,6 +35,7 @@ def _setup(pkg, geo, seed, Lz, Lr, species, **over):
         fs.upload(k, f[k])
     fs.set_flags(geo["flags"])
     fs.set_ghost_rules(geo["ghosts"])
+    fs.set_energy_keep_walls(geo.get("energy_keep_walls", []))
     for k in ("coefEISEE_eb_table", "coefEISEE_rd_table", "coefEISEE_ts_table"):
         fs.set_table(k, z[k])
     see = (z["coefEISEE_eb_table"], z["coefEISEE_rd_table"], z["coefEISEE_ts_table"], float(z["dTe_SEE"]))
