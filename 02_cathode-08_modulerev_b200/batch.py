@@ -17,21 +17,58 @@ from . import capi, fluid, learned
 SIZES = ((64, 128), (128, 256), (192, 384), (256, 512))   # (r cells, z cells)
 
 
-def sweep_instances(pkg, n=64, seed=3, sizes=SIZES, device=0, precision=1):
-    """Seeded instances of the sweep: grid size drawn from ``sizes``, bias
-    U(-10, 60) V, microwave power U(2, 16) W (recorded; the fluid step reads the
-    absorbed power as a field), discharge state seeded per instance."""
+def instance_specs(n=64, seed=3, sizes=SIZES):
+    """The whole sweep as seeded specs, drawn in one order so that an instance does
+    not depend on how the sweep is later split: index, grid size drawn from
+    ``sizes`` (ni z cells, nj r cells), bias U(-10, 60) V, microwave power
+    U(2, 16) W, and the seed of its discharge state."""
     rng = np.random.default_rng(seed)
-    cases = []
+    specs = []
     for k in range(n):
         nj, ni = sizes[int(rng.integers(len(sizes)))]
         V = float(rng.uniform(-10.0, 60.0))
         Pmw = float(rng.uniform(2.0, 16.0))
-        c = learned.make_case(pkg, ni, nj, seed=int(rng.integers(1 << 30)), V_bias=V, device=device)
-        c.update(ni=ni, nj=nj, V_bias=V, Pmw=Pmw)
+        specs.append(dict(index=k, ni=int(ni), nj=int(nj), V_bias=V, Pmw=Pmw, seed=int(rng.integers(1 << 30))))
+    return specs
+
+
+def partition(specs, world: int, steps=None):
+    """Split the instances over ``world`` ranks, balanced by cells x steps: the
+    largest cost first, each to the rank with the least cost so far (ties to the
+    lower rank).  ``steps`` is one count for all or a list per instance.  Returns
+    one sorted list of instance indices per rank; deterministic, so every rank
+    computes the same split without communicating."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    n = len(specs)
+    st = [steps] * n if steps is None or np.isscalar(steps) else list(steps)
+    cost = [s["ni"] * s["nj"] * (1 if st[k] is None else st[k]) for k, s in enumerate(specs)]
+    order = sorted(range(n), key=lambda k: (-cost[k], specs[k]["index"]))
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += cost[k]
+        out[r].append(specs[k]["index"])
+    return [sorted(x) for x in out]
+
+
+def make_instances(pkg, specs, device=0, precision=1):
+    """Build the instances of ``specs`` on one GPU (grids, field store, parameters)."""
+    cases = []
+    for sp in specs:
+        c = learned.make_case(pkg, sp["ni"], sp["nj"], seed=sp["seed"], V_bias=sp["V_bias"], device=device)
+        c.update(ni=sp["ni"], nj=sp["nj"], V_bias=sp["V_bias"], Pmw=sp["Pmw"], index=sp["index"])
         set_precision(c, precision)
         cases.append(c)
     return cases
+
+
+def sweep_instances(pkg, n=64, seed=3, sizes=SIZES, device=0, precision=1):
+    """Seeded instances of the sweep: grid size drawn from ``sizes``, bias
+    U(-10, 60) V, microwave power U(2, 16) W (recorded; the fluid step reads the
+    absorbed power as a field), discharge state seeded per instance."""
+    return make_instances(pkg, instance_specs(n, seed, sizes), device=device, precision=precision)
 
 
 def set_precision(c, precision):
@@ -63,11 +100,66 @@ def batch_steps(cases, steps: int, nthreads: int):
         items[k].params = ctypes.pointer(sp)
     wall = ctypes.c_double()
     rc = L.cth_batch_steps(items, n, steps, nthreads, ctypes.byref(wall))
-    for c, sp in zip(cases, keep):
+    for k, (c, sp) in enumerate(zip(cases, keep)):
         fluid.step_params_back(sp, c["P"])
+        c["anode"] = dict(I=items[k].I_Anode, Ii=items[k].Ii_Anode, Ie=items[k].Ie_Anode)
     if rc < 0:
         raise capi.CathodeError(rc, capi.last_error())
     return wall.value, [items[k].rc for k in range(n)], [items[k].seconds for k in range(n)]
+
+
+def summary(c) -> dict:
+    """The I-V point of one instance after its steps: bias, power, anode currents."""
+    a = c.get("anode", {})
+    return dict(index=int(c["index"]), ni=int(c["ni"]), nj=int(c["nj"]), V_bias=float(c["V_bias"]),
+                Pmw=float(c["Pmw"]), itime=int(c["P"]["itime"]), I_Anode=float(a.get("I", 0.0)),
+                Ii_Anode=float(a.get("Ii", 0.0)), Ie_Anode=float(a.get("Ie", 0.0)))
+
+
+def run_shard(specs, indices, runner):
+    """Run this rank's share of the sweep: ``runner(selected_specs)`` returns one
+    summary dict per spec (on a GPU: make_instances + batch_steps + summary)."""
+    sel = [s for s in specs if s["index"] in set(indices)]
+    return runner(sel)
+
+
+def gather(local: list, world: int, group=None) -> list:
+    """All instances' summaries on every rank, ordered by instance index: one
+    all-gather of the per-rank lists (no collective while the instances run)."""
+    if world == 1:
+        allv = [local]
+    else:
+        import torch.distributed as dist
+        allv = [None] * world
+        dist.all_gather_object(allv, local, group=group)
+    out = [x for part in allv for x in part]
+    idx = [x["index"] for x in out]
+    if len(set(idx)) != len(idx):
+        raise RuntimeError("an instance was run on more than one rank")
+    return sorted(out, key=lambda x: x["index"])
+
+
+def gpu_runner(pkg, steps, device=0, nthreads=None, precision=1):
+    """The runner of run_shard on one GPU: builds the specs' instances, advances
+    them ``steps`` steps with cth_batch_steps and returns their summaries."""
+    import os
+
+    def run(sel):
+        if not sel:
+            return []
+        cases = make_instances(pkg, sel, device=device, precision=precision)
+        try:
+            T = max(1, min(len(cases), nthreads or os.cpu_count() or 1))
+            _, rc, _ = batch_steps(cases, steps=steps, nthreads=T)
+            out = []
+            for c, r in zip(cases, rc):
+                d = summary(c)
+                d["rc"] = int(r)
+                out.append(d)
+            return out
+        finally:
+            close(cases)
+    return run
 
 
 def sequential_steps(cases, steps: int):

@@ -37,7 +37,7 @@ EXPORTS = (
     "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_fields_set_download_plan", "cth_fields_download_wait", "cth_fields_set_upload_plan", "cth_fields_upload_many",
     "cth_fields_download_many", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
-    "cth_ghost_rules_upload", "cth_energy_keep_walls_upload", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
+    "cth_ghost_rules_upload", "cth_energy_keep_walls_upload", "cth_restart_write", "cth_restart_wait", "cth_restart_read", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
     "cth_batch_steps", "cth_update_energy_profile", "cth_mw_port_rescale", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_tensor_cores", "cth_unet_set_smoothing", "cth_unet_set_wait_test", "cth_unet_set_grid_limit", "cth_unet_check", "cth_unet_set_params", "cth_unet_get_params",
@@ -135,6 +135,14 @@ class SGParams(ctypes.Structure):
                [(k, ctypes.c_int) for k in ("maxITR_HES", "maxITR_SOR", "flag_error", "flag_iter", "precision")]
 
 
+class RestartParams(ctypes.Structure):
+    _fields_ = [("dx", ctypes.c_double), ("dr", ctypes.c_double), ("V_bias", ctypes.c_double)]
+
+
+class RestartInfo(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_int), ("variables_read", ctypes.c_int), ("unknown_columns", ctypes.c_int)]
+
+
 class CFL(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("CFL", ctypes.c_double), ("masse", ctypes.c_double),
                 ("rmin", ctypes.c_double), ("dr", ctypes.c_double), ("flag_adp_dt", ctypes.c_int)] + \
@@ -183,7 +191,8 @@ class StepParams(ctypes.Structure):
 class BatchItem(ctypes.Structure):
     _fields_ = [("fs", ctypes.c_void_p), ("gx", ctypes.c_void_p), ("gr", ctypes.c_void_p),
                 ("params", ctypes.POINTER(StepParams)), ("rc", ctypes.c_int), ("steps_done", ctypes.c_int),
-                ("seconds", ctypes.c_double)]
+                ("seconds", ctypes.c_double), ("I_Anode", ctypes.c_double), ("Ii_Anode", ctypes.c_double),
+                ("Ie_Anode", ctypes.c_double)]
 
 
 class StepResult(ctypes.Structure):
@@ -293,6 +302,13 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_ghost_rules_upload.restype = ctypes.c_int
     L.cth_energy_keep_walls_upload.argtypes = [_vp, _vp, ctypes.c_int]
     L.cth_energy_keep_walls_upload.restype = ctypes.c_int
+    L.cth_restart_write.argtypes = [_vp, ctypes.c_char_p, _vp, _vp, _vp]
+    L.cth_restart_write.restype = ctypes.c_int
+    L.cth_restart_wait.argtypes = [_vp]
+    L.cth_restart_wait.restype = ctypes.c_int
+    L.cth_restart_read.argtypes = [_vp, _vp, _vp, ctypes.c_char_p, _vp, _vp, ctypes.POINTER(RestartParams), _vp,
+                                   ctypes.POINTER(RestartInfo)]
+    L.cth_restart_read.restype = ctypes.c_int
     for nm in ("cth_solve_rhoe_pc", "cth_solve_Te_pc"):
         getattr(L, nm).argtypes = [_vp, ctypes.POINTER(SGParams), _vp, ctypes.POINTER(PCResult)]
         getattr(L, nm).restype = ctypes.c_int

@@ -27,6 +27,7 @@ extern "C" int cth_batch_steps(cth_batch_item* items, int n, int steps, int nthr
         items[k].rc = 0;
         items[k].steps_done = 0;
         items[k].seconds = 0.0;
+        items[k].I_Anode = items[k].Ii_Anode = items[k].Ie_Anode = 0.0;
     }
     std::vector<cudaStream_t> streams(n, nullptr);
     for (int k = 0; k < n; k++) {
@@ -50,6 +51,9 @@ extern "C" int cth_batch_steps(cth_batch_item* items, int n, int steps, int nthr
                 if (rc < 0) { it.rc = rc; continue; }
                 if (rc > it.rc) it.rc = rc;
                 it.steps_done++;
+                it.I_Anode = r.rhoe.I_Anode;
+                it.Ii_Anode = r.rhoe.Ii_Anode;
+                it.Ie_Anode = r.rhoe.Ie_Anode;
             }
         }
         for (size_t q = 0; q < mine.size(); q++) {

@@ -141,7 +141,7 @@ int ensure_staging(cth_grid* g) {
     CTH_CUDA(cudaSetDevice(g->device));
     const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
     CTH_CUDA(cudaMalloc(&w.stage, 7 * g->plane * sizeof(double)));
-    CTH_CUDA(cudaMemset(w.stage, 0, 7 * g->plane * sizeof(double)));
+    CTH_CUDA(cth::zero_fill(w.stage, 7 * g->plane * sizeof(double)));
     CTH_CUDA(cudaMalloc(&w.stage_ij, nij * sizeof(double)));
     return CTH_OK;
 }
@@ -288,12 +288,12 @@ int cth_grid_create(int ni, int nj, const int* i_bl, const int* j_bl, int n_bl, 
     g->ws.npart = 3 * (((ni + 2 + 255) / 256) * (nj + 2) + 64);
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.part, (size_t)g->ws.npart * sizeof(double)), "cudaMalloc part");
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.stat, 32 * sizeof(double)), "cudaMalloc stat");
-    if (rc == CTH_OK) chk(cudaMemset(g->ws.stat, 0, 32 * sizeof(double)), "memset stat");
+    if (rc == CTH_OK) chk(cth::zero_fill(g->ws.stat, 32 * sizeof(double)), "memset stat");
     if (rc == CTH_OK) chk(cudaMallocHost(&g->ws.h_stat, 32 * sizeof(double)), "cudaMallocHost");
     if (rc == CTH_OK) chk(cudaMallocHost(&g->ws.h_args, sizeof(cth::SolveArgs)), "cudaMallocHost args");
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.d_args, sizeof(cth::SolveArgs)), "cudaMalloc args");
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.counter, 64), "cudaMalloc counter");
-    if (rc == CTH_OK) chk(cudaMemset(g->ws.counter, 0, 64), "memset counter");
+    if (rc == CTH_OK) chk(cth::zero_fill(g->ws.counter, 64), "memset counter");
     if (rc == CTH_OK) chk(cudaStreamCreateWithFlags(&g->cap[0], cudaStreamNonBlocking), "capture stream");
     if (rc == CTH_OK) chk(cudaStreamCreateWithFlags(&g->cap[1], cudaStreamNonBlocking), "capture stream");
     if (rc == CTH_OK) rc = configure_kernels(g);
@@ -523,7 +523,7 @@ int cth_c5_solve(cth_grid* g, const double* aP, const double* aE, const double* 
     const size_t nij = (size_t)(g->ni + 2) * (g->nj + 2);
     if (!c.cstage) {
         CTH_CUDA(cudaMalloc(&c.cstage, 7 * g->plane * 2 * sizeof(double)));
-        CTH_CUDA(cudaMemset(c.cstage, 0, 7 * g->plane * 2 * sizeof(double)));
+        CTH_CUDA(cth::zero_fill(c.cstage, 7 * g->plane * 2 * sizeof(double)));
         CTH_CUDA(cudaMalloc(&c.cstage_ij, nij * 2 * sizeof(double)));
     }
     const double* src[6] = {aP, aE, aW, aN, aS, b};

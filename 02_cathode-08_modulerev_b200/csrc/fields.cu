@@ -182,7 +182,7 @@ double* field_ptr(cth_fields* fs, const std::string& name) {
     double* p = nullptr;
     const size_t bytes = fs->g->plane * sizeof(double);
     if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
-    if (cudaMemset(p, 0, bytes) != cudaSuccess) { cudaFree(p); return nullptr; }
+    if (cth::zero_fill(p, bytes) != cudaSuccess) { cudaFree(p); return nullptr; }
     fs->planes[name] = p;
     return p;
 }
@@ -278,7 +278,7 @@ int cth_fields_create(cth_grid* g, cth_fields** out) {
         set_error("cth_fields_create: allocation failed");
         return CTH_ERR_ALLOC;
     }
-    cudaMemset(fs->scal, 0, CTH_FS_NSCAL * sizeof(double));
+    cth::zero_fill(fs->scal, CTH_FS_NSCAL * sizeof(double));
     *out = fs;
     return CTH_OK;
 }
@@ -286,6 +286,7 @@ int cth_fields_create(cth_grid* g, cth_fields** out) {
 void cth_fields_destroy(cth_fields* fs) {
     if (!fs) return;
     cudaSetDevice(fs->g->device);
+    restart_release(fs);
     for (auto& kv : fs->planes) cudaFree(kv.second);
     for (auto& kv : fs->tables) cudaFree(kv.second.first);
     if (fs->flags) cudaFree(fs->flags);

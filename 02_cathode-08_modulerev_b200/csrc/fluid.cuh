@@ -15,8 +15,11 @@
 #define CTH_FS_NPART_PER_BLOCK 16
 #define CTH_KEEP_WALL_MAX 4
 
+namespace cth { struct RestartWriter; }
+
 struct cth_fields {
     cth_grid* g = nullptr;
+    cth::RestartWriter* restart = nullptr;  // restart-file writer (restart.cu): pinned staging, writer thread
     int* ghost_rules = nullptr;      // device, 7 ints per rule (i0, i1, j0, j1, di, dj, rhoe_mode)
     int n_ghost_rules = 0;
     int keep_wall[4 * CTH_KEEP_WALL_MAX] = {};  // r-face boxes where the energy sweep keeps Gr_wall
@@ -229,6 +232,7 @@ __global__ void k_max_flagged(const double* __restrict__ v, const unsigned char*
 
 // ghost rules of the fluid store applied in order to a plane (fields.cu);
 // which = 0: rhoe (rule mode 0 zeroes, 1 copies), 1: copy always
+void restart_release(cth_fields* fs);
 void apply_ghost_rules(cth_fields* fs, double* plane, int which, cudaStream_t s);
 
 // named device planes of the store (created zeroed on first use), and tables

@@ -21,6 +21,16 @@
 
 namespace cth {
 
+// Zero freshly allocated device memory before any stream can use it.  cudaMemset
+// on device memory returns before the fill is done and runs on the legacy
+// default stream, which does not order work on non-blocking streams (the batched
+// instances' streams): wait for it here, once per allocation.
+inline cudaError_t zero_fill(void* p, size_t bytes) {
+    cudaError_t e = cudaMemset(p, 0, bytes);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+    return e;
+}
+
 // complex double of the frequency-domain solves; interleaved (re, im) in memory
 struct cd {
     double x, y;

@@ -261,9 +261,9 @@ static int c5_alloc(cth_grid* g) {
     if (rc != CTH_OK) return rc;
     const size_t n0 = (size_t)g->nrow[0] * g->ldl;
     CTH_CUDA(cudaMalloc(&w.buf, 9 * n0 * sizeof(cd)));
-    CTH_CUDA(cudaMemset(w.buf, 0, 9 * n0 * sizeof(cd)));
+    CTH_CUDA(cth::zero_fill(w.buf, 9 * n0 * sizeof(cd)));
     CTH_CUDA(cudaMalloc(&w.sc, C5_NWORDS * sizeof(double)));
-    CTH_CUDA(cudaMemset(w.sc, 0, C5_NWORDS * sizeof(double)));
+    CTH_CUDA(cth::zero_fill(w.sc, C5_NWORDS * sizeof(double)));
     const int nb = ((g->ncol + 255) / 256) * g->nrow[0];
     w.npart = 3 * nb + 8;
     CTH_CUDA(cudaMalloc(&w.part, w.npart * sizeof(double)));

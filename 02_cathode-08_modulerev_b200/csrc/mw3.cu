@@ -1165,11 +1165,11 @@ int cth_mw3_create_blocks(int ni, int nj, const int* xi_bl, const int* xj_bl, in
     if (e == cudaSuccess) e = cudaMalloc(&m->part, (size_t)(3 * nparts + 8) * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&m->counter, sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMallocHost(&m->h_sc, NWORDS * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemset(m->a, 0, (size_t)3 * NQ * pl * sizeof(cd));
-    if (e == cudaSuccess) e = cudaMemset(m->b, 0, (size_t)3 * pl * sizeof(cd));
-    if (e == cudaSuccess) e = cudaMemset(m->vec, 0, (size_t)27 * pl * sizeof(cd));
-    if (e == cudaSuccess) e = cudaMemset(m->sc, 0, NWORDS * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemset(m->counter, 0, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cth::zero_fill(m->a, (size_t)3 * NQ * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cth::zero_fill(m->b, (size_t)3 * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cth::zero_fill(m->vec, (size_t)27 * pl * sizeof(cd));
+    if (e == cudaSuccess) e = cth::zero_fill(m->sc, NWORDS * sizeof(double));
+    if (e == cudaSuccess) e = cth::zero_fill(m->counter, sizeof(unsigned int));
     for (int u = 0; u < 2; u++) {
         for (int k = 0; k < 2 && e == cudaSuccess; k++) {
             e = cudaStreamCreateWithFlags(&m->side[u][k], cudaStreamNonBlocking);

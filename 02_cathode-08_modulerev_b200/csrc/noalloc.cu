@@ -4,13 +4,17 @@
 // Who needs this: code that may not call cudaMalloc at the moment it wants a
 // residual norm.  Examples are a host program that hands all device memory to
 // its own pool allocator up front and forbids libraries from allocating
-// afterwards, a caller that is recording work into a CUDA stream capture
-// (cudaMalloc there can fail or force a device-wide synchronisation), and a
-// real-time loop that cannot afford the implicit synchronisation an
-// allocation may cause.  Such callers cannot create a cth_grid (its
-// constructor allocates the mask, the multigrid hierarchy and the reduction
-// buffers), so this entry point takes the block table directly and keeps all
-// of its scratch in one file-scope device array instead.
+// afterwards, and a real-time loop that cannot afford the implicit
+// synchronisation an allocation may cause.  Such callers cannot create a
+// cth_grid (its constructor allocates the mask, the multigrid hierarchy and
+// the reduction buffers), so this entry point takes the block table directly
+// and keeps all of its scratch in one file-scope device array instead.
+//
+// Set-up: the first call on a device looks up the array's device address
+// (cudaGetSymbolAddress, once per device, with that device current); make that
+// first call before any stream capture.  Every call then waits for its stream:
+// it copies the two sums to the host and synchronises, and returns with the
+// norms on the host.
 //
 // Scratch: g_noalloc_scratch, CTH_NOALLOC_SCRATCH_BYTES = 8 MiB per GPU that
 // loads the library, held until the process exits.  The first 256 KiB hold

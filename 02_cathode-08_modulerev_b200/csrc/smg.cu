@@ -824,15 +824,15 @@ static int alloc_hierarchy(cth_grid* g) {
         CTH_CUDA(cudaMalloc(&h.b[l], n * sizeof(T)));
         CTH_CUDA(cudaMalloc(&h.wS[l], n * sizeof(T)));
         CTH_CUDA(cudaMalloc(&h.wN[l], n * sizeof(T)));
-        CTH_CUDA(cudaMemset(h.a[l], 0, n * npt * sizeof(T)));
-        CTH_CUDA(cudaMemset(h.x[l], 0, n * sizeof(T)));
-        CTH_CUDA(cudaMemset(h.b[l], 0, n * sizeof(T)));
-        CTH_CUDA(cudaMemset(h.wS[l], 0, n * sizeof(T)));
-        CTH_CUDA(cudaMemset(h.wN[l], 0, n * sizeof(T)));
+        CTH_CUDA(cth::zero_fill(h.a[l], n * npt * sizeof(T)));
+        CTH_CUDA(cth::zero_fill(h.x[l], n * sizeof(T)));
+        CTH_CUDA(cth::zero_fill(h.b[l], n * sizeof(T)));
+        CTH_CUDA(cth::zero_fill(h.wS[l], n * sizeof(T)));
+        CTH_CUDA(cth::zero_fill(h.wN[l], n * sizeof(T)));
         if constexpr (kFac<T>) {
             const size_t nf = (size_t)g->nrow[l] * line_fac_size<T>(g->bd);
             CTH_CUDA(cudaMalloc(&h.fac[l], nf * sizeof(T)));
-            CTH_CUDA(cudaMemset(h.fac[l], 0, nf * sizeof(T)));
+            CTH_CUDA(cth::zero_fill(h.fac[l], nf * sizeof(T)));
         }
     }
     h.allocated = true;

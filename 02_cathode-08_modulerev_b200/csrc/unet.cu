@@ -1002,7 +1002,7 @@ namespace {
 bf16* alloc_bf16(cth_unet* n, size_t count) {
     void* p = nullptr;
     if (cudaMalloc(&p, count * sizeof(bf16)) != cudaSuccess) return nullptr;
-    cudaMemset(p, 0, count * sizeof(bf16));
+    cth::zero_fill(p, count * sizeof(bf16));
     n->bufs.push_back(p);
     return (bf16*)p;
 }
@@ -1095,10 +1095,10 @@ int build(cth_unet* n) {
     CTH_CUDA(cudaMalloc(&n->grad, off * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->adam_m, off * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->adam_v, off * sizeof(float)));
-    CTH_CUDA(cudaMemset(n->prm, 0, off * sizeof(float)));
-    CTH_CUDA(cudaMemset(n->grad, 0, off * sizeof(float)));
-    CTH_CUDA(cudaMemset(n->adam_m, 0, off * sizeof(float)));
-    CTH_CUDA(cudaMemset(n->adam_v, 0, off * sizeof(float)));
+    CTH_CUDA(cth::zero_fill(n->prm, off * sizeof(float)));
+    CTH_CUDA(cth::zero_fill(n->grad, off * sizeof(float)));
+    CTH_CUDA(cth::zero_fill(n->adam_m, off * sizeof(float)));
+    CTH_CUDA(cth::zero_fill(n->adam_v, off * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->wb, woff * sizeof(bf16)));
     CTH_CUDA(cudaMalloc(&n->wt, woff * sizeof(bf16)));
     CTH_CUDA(cudaMalloc(&n->wbt, woff * sizeof(bf16)));
@@ -1109,7 +1109,7 @@ int build(cth_unet* n) {
     CTH_CUDA(cudaMalloc(&n->cw, n->cout * sizeof(float)));
     CTH_CUDA(cudaMalloc(&n->err, sizeof(int)));
     CTH_CUDA(cudaDeviceGetAttribute(&n->sms, cudaDevAttrMultiProcessorCount, n->device));
-    CTH_CUDA(cudaMemset(n->err, 0, sizeof(int)));
+    CTH_CUDA(cth::zero_fill(n->err, sizeof(int)));
 #define CTH_TC_ATTR(NN, RR)                                                                   \
     CTH_CUDA(cudaFuncSetAttribute(k_conv3_tc<NN, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                   TcShape<NN, RR>::kSmem));
@@ -1387,7 +1387,7 @@ int cth_unet_check(cth_unet* n) {
     CTH_CUDA(cudaMemcpy(&e, n->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
         // reported once: the flag is cleared for the following calls
-        CTH_CUDA(cudaMemset(n->err, 0, sizeof(int)));
+        CTH_CUDA(cth::zero_fill(n->err, sizeof(int)));
         set_error("cth_unet: a tensor-core convolution gave up waiting (its output is not valid)");
         return CTH_ERR_CUDA;
     }
@@ -1417,8 +1417,8 @@ int cth_unet_set_params(cth_unet* n, const float* host, long long count) {
     if (!n || !host || count != (long long)n->nparam) { set_error("cth_unet_set_params: invalid arguments"); return CTH_ERR_ARG; }
     CTH_CUDA(cudaSetDevice(n->device));
     CTH_CUDA(cudaMemcpy(n->prm, host, n->nparam * sizeof(float), cudaMemcpyHostToDevice));
-    CTH_CUDA(cudaMemset(n->adam_m, 0, n->nparam * sizeof(float)));
-    CTH_CUDA(cudaMemset(n->adam_v, 0, n->nparam * sizeof(float)));
+    CTH_CUDA(cth::zero_fill(n->adam_m, n->nparam * sizeof(float)));
+    CTH_CUDA(cth::zero_fill(n->adam_v, n->nparam * sizeof(float)));
     int rc = sync_weights(n, 0);
     if (rc != CTH_OK) return rc;
     CTH_CUDA(cudaDeviceSynchronize());

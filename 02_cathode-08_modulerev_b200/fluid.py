@@ -10,6 +10,7 @@ or for the r-z rectangle of the synthetic workloads.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -356,6 +357,36 @@ class Fields:
         a = np.ascontiguousarray(np.asarray(rules, dtype=np.int32).reshape(-1, 7))
         capi.check(self._L.cth_ghost_rules_upload(self._h, a.ctypes.data, a.shape[0]), allow_positive=False)
 
+    # restart files (the reference's restart<nOut>.csv) ----------------------------------------
+    def write_restart(self, path: str, x, r, stream=None):
+        """Queue the write of a restart file of the reference's format (OutputModule::output,
+        outputModule.hpp:429-470); returns once the copies are queued on ``stream``.
+        x, r: the cell-centre coordinates gc.x (ni+2) and gc.r (nj+2)."""
+        g = self.grid
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        if x.shape != (g.ni + 2,) or r.shape != (g.nj + 2,):
+            raise ValueError("x must have ni+2 and r nj+2 entries")
+        s = 0 if stream is None else stream.cuda_stream
+        capi.check(self._L.cth_restart_write(self._h, os.fsencode(path), x.ctypes.data, r.ctypes.data, s),
+                   allow_positive=False)
+
+    def restart_wait(self):
+        """Wait for the restart file being written; raises if writing it failed."""
+        capi.check(self._L.cth_restart_wait(self._h), allow_positive=False)
+
+    def read_restart(self, path: str, gx, gr, x, r, dx: float, dr: float, V_bias: float, stream=None) -> dict:
+        """Read a restart file into the store with the reference's checks and
+        post-processing (InputModule::input_restart_data, inputModule.hpp:667-1157)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        p = capi.RestartParams(dx=dx, dr=dr, V_bias=V_bias)
+        info = capi.RestartInfo()
+        s = 0 if stream is None else stream.cuda_stream
+        capi.check(self._L.cth_restart_read(self._h, gx._h, gr._h, os.fsencode(path), x.ctypes.data, r.ctypes.data,
+                                            ctypes.byref(p), s, ctypes.byref(info)), allow_positive=False)
+        return dict(rows=info.rows, variables_read=info.variables_read, unknown_columns=info.unknown_columns)
+
     def set_energy_keep_walls(self, boxes):
         """r-face boxes (i0, i1, j0, j1) whose wall flux Gr_wall the energy sweep leaves unchanged
         (the cathode's lower wall x2, fluidModule.hpp:4428-4449); at most 4."""
@@ -395,6 +426,12 @@ class Fields:
 # ---------------------------------------------------------------------------
 # geometries: cell / face blocks, wall segments, ghost rules, ion wall programs
 # ---------------------------------------------------------------------------
+
+def cell_coordinates(ni, nj, dx, dr, xL=0.0, rmin=0.0):
+    """Cell-centre coordinates gc.x (ni+2) and gc.r (nj+2) as InitialModule::iniParam
+    forms them (initialModule.hpp:80-85): x_i = xL + (i - 0.5) dx, r_j = rmin + (j - 0.5) dr."""
+    return xL + (np.arange(ni + 2) - 0.5) * dx, rmin + (np.arange(nj + 2) - 0.5) * dr
+
 
 def cathode_geometry(ni=194, nj=70, xR=0.0388, rmax=0.014, width_neutIn=0.0055) -> dict:
     """The cathode's fluid blocks with their x-face and r-face blocks

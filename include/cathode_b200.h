@@ -584,8 +584,8 @@ int cth_residual_dev(cth_grid* g, const double* aP, const double* aE, const doub
 /* Residual without allocation (device arrays) ---------------------------------
  * No counterpart in the reference.  For callers that may not allocate device
  * memory when they need a residual (a program whose own pool owns all device
- * memory, work being recorded into a stream capture, a loop that cannot take
- * the synchronisation an allocation can cause): same result as
+ * memory, a loop that cannot take the synchronisation an allocation can
+ * cause): same result as
  * cth_residual_dev, but it needs no cth_grid and calls no allocator.  Its
  * scratch is one static device array of CTH_NOALLOC_SCRATCH_BYTES per GPU
  * (held until exit); (nj+2)*ld may not exceed CTH_NOALLOC_MAX_PLANE and n_bl
@@ -593,13 +593,47 @@ int cth_residual_dev(cth_grid* g, const double* aP, const double* aE, const doub
  * dimension of the library layout.  The first call on a device looks up the
  * array's device address; make that first call before any stream capture.
  * Calls share the array: calls that overlap on the GPU race and may return
- * wrong norms.  Returns after the norms are on the host. */
+ * wrong norms.  The call synchronises `stream` and returns after the norms are
+ * on the host. */
 #define CTH_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
 #define CTH_NOALLOC_MAX_PLANE (CTH_NOALLOC_SCRATCH_BYTES - 256u * 1024u)
 int cth_residual_noalloc(int ni, int nj, int ld, const int* i_bl, const int* j_bl, int n_bl,
                          const double* aP, const double* aE, const double* aW, const double* aN,
                          const double* aS, const double* b, const double* x, double* r,
                          double* rnorm, double* bnorm, void* stream);
+
+/* Restart files ---------------------------------------------------------------
+ * The reference's restart CSV: OutputModule::output writes restart<nOut>.csv
+ * (outputModule.hpp:429-470: i, j, x, r, 49 fields, zero; %.17e reals, |v| <
+ * 1e-100 written as 0, Te and Te_old in eV), InputModule::input_restart_data
+ * reads it (inputModule.hpp:667-1157).  x[ni+2], r[nj+2] are the cell-centre
+ * coordinates gc.x, gc.r (x_i = xL + (i - 1/2) dx, r_j = rmin + (j - 1/2) dr).
+ *
+ * cth_restart_write queues the device-to-host copies of the 49 fields on
+ * `stream` (later work on that stream cannot change what is written) and
+ * returns; a host thread formats and writes the file.  cth_restart_wait joins
+ * that thread and returns its status; a second write waits for the first.
+ *
+ * cth_restart_read reads a file into the store: the 39 variables of the
+ * reference's registry that the header holds (the wall fluxes are written but
+ * not read), Te from eV; the index range, duplicate and missing cells and the
+ * coordinates (1e-12 + 1e-10 relative) are checked (CTH_ERR_ARG with the line
+ * where the reference aborts).  Then the reference's post-processing on the
+ * device: rhoe = 0 outside the fluid cells, Ex / Er from phi on the interior
+ * face blocks of gx / gr, the wall ghosts of phi (V_bias on the biased wall),
+ * E on the wall faces, Er = 0 on the axis.  Synchronises `stream`. */
+typedef struct cth_restart_params {
+    double dx, dr, V_bias;
+} cth_restart_params;
+typedef struct cth_restart_info {
+    int rows;              /* cells read: (ni+2)*(nj+2)                          */
+    int variables_read;    /* registry variables present in the header (<= 39)   */
+    int unknown_columns;   /* header columns neither registry, coordinate, wall flux nor zero */
+} cth_restart_info;
+int cth_restart_write(cth_fields* fs, const char* path, const double* x, const double* r, void* stream);
+int cth_restart_wait(cth_fields* fs);
+int cth_restart_read(cth_fields* fs, cth_grid* gx, cth_grid* gr, const char* path, const double* x,
+                     const double* r, const cth_restart_params* prm, void* stream, cth_restart_info* info);
 
 /* Batched instances (the I-V sweeps; no counterpart in the reference, which runs
  * one discharge per process) -------------------------------------------------
@@ -609,7 +643,9 @@ int cth_residual_noalloc(int ni, int nj, int ld, const int* i_bl, const int* j_b
  * step by step on one stream per instance.  Results are those of the same
  * steps run one instance after another.  Returns the worst status (negative if
  * an instance failed; that instance stops, the others continue); per item: rc,
- * steps done, wall seconds; *wall_seconds = the whole batch. */
+ * steps done, wall seconds and the anode currents of its last step
+ * (FluidModule::solve_rhoe_wdTe_wSEE_PC, fluidModule.hpp:3944-3964);
+ * *wall_seconds = the whole batch. */
 typedef struct cth_batch_item {
     cth_fields* fs;
     cth_grid* gx;
@@ -618,6 +654,7 @@ typedef struct cth_batch_item {
     int rc;
     int steps_done;
     double seconds;
+    double I_Anode, Ii_Anode, Ie_Anode;  /* anode currents of the last step (the I-V point) */
 } cth_batch_item;
 int cth_batch_steps(cth_batch_item* items, int n, int steps, int nthreads, double* wall_seconds);
 

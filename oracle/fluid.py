@@ -1472,7 +1472,8 @@ def fluid_step(st: dict, P: dict, geo: dict, see, tb: dict, solve) -> dict:
     s.update({k: v for k, v in solve_phi_pc(s, P["phi"], geo, see, solve).items()
               if k in ("phi", "Ex", "Er", "nUex", "nUer")})
     s.update({k: v for k, v in solve_sg_pc(s, P["rhoe"], geo, see, solve, "rhoe").items()
-              if k in ("rhoe", "rhoUex", "rhoUer", "rhoUex_wall", "rhoUer_wall", "rhoe_old")})
+              if k in ("rhoe", "rhoUex", "rhoUer", "rhoUex_wall", "rhoUer_wall", "rhoe_old", "I_Anode", "Ii_Anode",
+                       "Ie_Anode")})
     s.update({k: v for k, v in solve_sg_pc(s, P["eps"], geo, see, solve, "rhoeps").items()
               if k in ("rhoeps", "Gx", "Gr", "Gx_wall", "Gr_wall", "Te", "Te_old")})
     if P["itime"] % P["ndt_n"] == 0 and P["itime"] % P["ndt_m"] == 0:

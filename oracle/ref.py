@@ -17,7 +17,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libref.so")
-_LIB = None
+# the same driver with the product's GPU drop-in (include/cathode_solver.hpp) as solverFuncs.hpp
+DROPIN_PATH = os.path.join(_HERE, "_ref", "libref_dropin.so")
+_LIBS: dict = {}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -37,27 +39,32 @@ def reference_dir() -> str:
 
 
 def build(force: bool = False) -> str | None:
-    """Build libref.so when the reference sources are present; returns its path or None."""
+    """Build libref.so (and libref_dropin.so, once the product library exists) when the
+    reference sources are present; returns the path of libref.so or None."""
     ref = reference_dir()
     if not os.path.isdir(os.path.join(ref, "include")):
         return LIB_PATH if os.path.exists(LIB_PATH) else None
-    args = ["make", "-C", _HERE, "-s", f"REF={ref}", "ref"]
+    targets = ["ref"]
+    if os.path.exists(os.path.join(_HERE, "..", "02_cathode-08_modulerev_b200", "libcathode_b200.so")):
+        targets.append("ref-dropin")
+    args = ["make", "-C", _HERE, "-s", f"REF={ref}"] + targets
     if force:
         args.insert(1, "-B")
     subprocess.run(args, check=True, stderr=subprocess.DEVNULL)
     return LIB_PATH
 
 
-def available() -> bool:
-    return os.path.exists(LIB_PATH)
+def available(dropin: bool = False) -> bool:
+    return os.path.exists(DROPIN_PATH if dropin else LIB_PATH)
 
 
-def lib() -> ctypes.CDLL:
-    global _LIB
-    if _LIB is None:
-        if not available():
-            raise FileNotFoundError(f"{LIB_PATH} not built (needs the reference sources; oracle/Makefile ref)")
-        L = ctypes.CDLL(LIB_PATH)
+def lib(dropin: bool = False) -> ctypes.CDLL:
+    key = "dropin" if dropin else "exact"
+    if key not in _LIBS:
+        path = DROPIN_PATH if dropin else LIB_PATH
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (needs the reference sources; oracle/Makefile ref)")
+        L = ctypes.CDLL(path)
         L.ref_create.argtypes = [ctypes.c_int, ctypes.c_int]
         L.ref_create.restype = _vp
         L.ref_destroy.argtypes = [_vp]
@@ -79,23 +86,27 @@ def lib() -> ctypes.CDLL:
         L.ref_capture.restype = None
         L.ref_captured_plane.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int]
         L.ref_captured_blocks.argtypes = [ctypes.c_int, _ip, _ip, ctypes.c_int]
-        _LIB = L
-    return _LIB
+        L.ref_dropin_precision.argtypes = [ctypes.c_int]
+        L.ref_output.argtypes = [_vp, _cs]
+        _LIBS[key] = L
+    return _LIBS[key]
 
 
 class RefCase:
     """One reference state (Params + GridCenter + GridInterfaceX/R + MicrowaveBC + tables)."""
 
-    def __init__(self, ni: int, nj: int, quiet: bool = True):
+    def __init__(self, ni: int, nj: int, quiet: bool = True, dropin: bool = False):
+        """dropin=True: the reference's solves go to the product's GPU drop-in."""
         self.ni, self.nj = int(ni), int(nj)
-        self._h = lib().ref_create(self.ni, self.nj)
+        self._L = lib(dropin)
+        self._h = self._L.ref_create(self.ni, self.nj)
         if not self._h:
             raise ValueError("ref_create failed")
-        lib().ref_set_quiet(self._h, int(quiet))
+        self._L.ref_set_quiet(self._h, int(quiet))
 
     def close(self):
         if self._h:
-            lib().ref_destroy(self._h)
+            self._L.ref_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -106,7 +117,7 @@ class RefCase:
 
     # parameters -------------------------------------------------------------------------------
     def set_param(self, name: str, value: float) -> bool:
-        return lib().ref_set_param(self._h, name.encode(), float(value)) == 0
+        return self._L.ref_set_param(self._h, name.encode(), float(value)) == 0
 
     def set_params(self, prm: dict) -> list:
         """Set every scalar entry of prm that is a Params member; returns the names not taken."""
@@ -121,7 +132,7 @@ class RefCase:
 
     def param(self, name: str) -> float:
         v = ctypes.c_double()
-        if lib().ref_get_param(self._h, name.encode(), ctypes.byref(v)) != 0:
+        if self._L.ref_get_param(self._h, name.encode(), ctypes.byref(v)) != 0:
             raise KeyError(name)
         return v.value
 
@@ -130,7 +141,7 @@ class RefCase:
         a = np.ascontiguousarray(a, dtype=np.float64)
         if a.shape != (self.ni + 2, self.nj + 2):
             raise ValueError(f"{name}: shape {a.shape}")
-        if lib().ref_set_field(self._h, name.encode(), a.ctypes.data_as(_dp)) != 0:
+        if self._L.ref_set_field(self._h, name.encode(), a.ctypes.data_as(_dp)) != 0:
             raise KeyError(name)
 
     def set_fields(self, fields: dict, names=None) -> list:
@@ -148,13 +159,13 @@ class RefCase:
 
     def field(self, name: str) -> np.ndarray:
         out = np.empty((self.ni + 2, self.nj + 2))
-        if lib().ref_get_field(self._h, name.encode(), out.ctypes.data_as(_dp)) != 0:
+        if self._L.ref_get_field(self._h, name.encode(), out.ctypes.data_as(_dp)) != 0:
             raise KeyError(name)
         return out
 
     def int_field(self, name: str) -> np.ndarray:
         out = np.empty((self.ni + 2, self.nj + 2), np.int32)
-        if lib().ref_get_int_field(self._h, name.encode(), out.ctypes.data_as(_ip)) != 0:
+        if self._L.ref_get_int_field(self._h, name.encode(), out.ctypes.data_as(_ip)) != 0:
             raise KeyError(name)
         return out
 
@@ -165,35 +176,42 @@ class RefCase:
     # tables -----------------------------------------------------------------------------------
     def set_table(self, name: str, v) -> None:
         v = np.ascontiguousarray(v, dtype=np.float64)
-        if lib().ref_set_table(self._h, name.encode(), v.ctypes.data_as(_dp), v.size) != 0:
+        if self._L.ref_set_table(self._h, name.encode(), v.ctypes.data_as(_dp), v.size) != 0:
             raise KeyError(name)
 
     def table(self, name: str) -> np.ndarray:
-        n = lib().ref_table_size(self._h, name.encode())
+        n = self._L.ref_table_size(self._h, name.encode())
         if n < 0:
             raise KeyError(name)
         out = np.empty(n)
-        lib().ref_get_table(self._h, name.encode(), out.ctypes.data_as(_dp))
+        self._L.ref_get_table(self._h, name.encode(), out.ctypes.data_as(_dp))
         return out
 
     # geometry and methods ---------------------------------------------------------------------
     def make_boundary(self) -> None:
-        lib().ref_make_boundary(self._h)
+        self._L.ref_make_boundary(self._h)
 
     def mw_list(self, name: str) -> np.ndarray:
         """(n, 3) array of (i, j, code) of one MicrowaveBC list, e.g. 'BndWx'."""
         cols = []
         for p in "ijs":
-            n = lib().ref_mw_list(self._h, (p + name).encode(), None, 0)
+            n = self._L.ref_mw_list(self._h, (p + name).encode(), None, 0)
             if n < 0:
                 raise KeyError(name)
             buf = np.empty(max(n, 1), np.int32)
-            lib().ref_mw_list(self._h, (p + name).encode(), buf.ctypes.data_as(_ip), n)
+            self._L.ref_mw_list(self._h, (p + name).encode(), buf.ctypes.data_as(_ip), n)
             cols.append(buf[:n])
         return np.stack(cols, axis=1)
 
+    def output(self, directory: str) -> str:
+        """OutputModule::output into directory/results; returns the restart file's path."""
+        n = int(self.param("nOut"))
+        if self._L.ref_output(self._h, os.fsencode(directory)) != 0:
+            raise OSError("ref_output failed")
+        return os.path.join(directory, "results", f"restart{n}.csv")
+
     def call(self, method: str) -> int:
-        rc = lib().ref_call(self._h, method.encode())
+        rc = self._L.ref_call(self._h, method.encode())
         if rc < 0:
             raise KeyError(method)
         if rc:
@@ -232,3 +250,9 @@ def captured_planes(ni: int, nj: int) -> list:
         d["i_bl"], d["j_bl"] = ib[:2 * nb].reshape(nb, 2).copy(), jb[:2 * nb].reshape(nb, 2).copy()
         out.append(d)
     return out
+
+
+def dropin_precision(p: int) -> None:
+    """Precision of the GPU drop-in's solver_SMG: 1 mixed (FP32 cycles + FP64 defect correction), 0 FP64."""
+    if lib(True).ref_dropin_precision(int(p)) != 0:
+        raise RuntimeError("not the drop-in build")

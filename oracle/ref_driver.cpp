@@ -16,7 +16,9 @@
  * (initialModule.hpp:207-1058) on the reference's Params / GridCenter /
  * GridInterfaceX / GridInterfaceR / MicrowaveBC / SeeVec / BolsigVec types.
  * Only the linear solves differ: refshim/solverFuncs.hpp replaces HYPRE by
- * the exact solve that SMG converges to.
+ * the exact solve that SMG converges to; built with -DREF_DROPIN against
+ * refshim_dropin/solverFuncs.hpp, the solves are the product's GPU drop-in
+ * (include/cathode_solver.hpp over libcathode_b200.so) instead.
  *
  * Written here (not the reference's): the name registries that copy planes,
  * parameters and tables in and out ([i][j] row-major, (ni+2) x (nj+2)), the
@@ -30,12 +32,18 @@
 #include <string>
 #include <vector>
 
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include "fluidModule.hpp"
 #include "initialModule.hpp"
+#include "outputModule.hpp"
 
+#ifndef REF_DROPIN
 extern "C" {
 #include "oracle.h"
 }
+#endif
 
 /* ---------------------------------------------------------------- shim state */
 namespace refshim {
@@ -78,6 +86,7 @@ void record(const VV* planes[6], const std::vector<int>& ib, const std::vector<i
 
 }  // namespace
 
+#ifndef REF_DROPIN
 void solver_SMG(VV aP, VV aE, VV aW, VV aN, VV aS, VV b, VI i_bl, VI j_bl, int n_bl, int maxITR,
                 double error_cnv, int /*flag_msg*/, VV& solution) {
     refshim::calls()++;
@@ -126,6 +135,8 @@ void solver_SOR(VV aP, VV aE, VV aW, VV aN, VV aS, VV b, VI i_bl, VI j_bl, int n
         std::memcpy(solution[i].data(), &x[(size_t)i * (nj + 2)], (nj + 2) * sizeof(double));
 }
 
+#endif  // REF_DROPIN
+
 /* ------------------------------------------------------------------ the case */
 namespace {
 
@@ -139,6 +150,7 @@ struct RefCase {
     BolsigVec bo;
     FluidModule flu;
     InitialModule ini;
+    OutputModule out;
     bool quiet = true;
     RefCase(int ni, int nj) : gc(ni, nj), gx(ni, nj), gr(ni, nj) {
         pm.ni = ni;
@@ -392,6 +404,34 @@ int ref_call(void* h, const char* m) {
     else if (!std::strcmp(m, "step")) step(c);
     else return -1;
     return refshim::failures() == f0 ? 0 : 1;
+}
+
+/* Precision of the drop-in's solver_SMG (CTH_PREC_MIXED 1 / CTH_PREC_FP64 0); -1 when
+ * this build uses the exact solve instead. */
+int ref_dropin_precision(int p) {
+#ifdef REF_DROPIN
+    cathode_b200::precision() = p;
+    return 0;
+#else
+    (void)p;
+    return -1;
+#endif
+}
+
+/* The reference's own writer: OutputModule::output (outputModule.hpp:185-1051) run
+ * with `dir` as the working directory, so that its results/result<nOut>.csv,
+ * results/restart<nOut>.csv and results/current_sum<nOut>.csv land in dir/results. */
+int ref_output(void* h, const char* dir) {
+    RefCase& c = *static_cast<RefCase*>(h);
+    char old[4096];
+    if (!getcwd(old, sizeof old)) return -1;
+    if (chdir(dir) != 0) return -1;
+    mkdir("results", 0777);
+    {
+        Quiet q(c.quiet);
+        c.out.output(c.pm, c.gc, c.gx, c.gr, c.bo);
+    }
+    return chdir(old) == 0 ? 0 : -1;
 }
 
 /* Linear-solve hooks of the shim. */

@@ -9,15 +9,23 @@ cathode's cell blocks gc.i_flc_bl / gc.j_flc_bl, written ic[b][k] / jc[b][k],
 so that the table serves any grid resolution.  Segments keep the reference's
 order (the order of the boundary surgery) and cite their source line.
 
-Run in a checkout that has the reference under /root/reference.
+Usage: python <this script> <reference checkout>  (or set CATHODE_REFERENCE).
 """
 import json
 import os
+import sys
 import re
 
-SRC = "/root/reference/include/initialModule.hpp"
 FIRST, LAST = 420, 1056
 HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def reference_root() -> str:
+    """The reference checkout: the first command-line argument, else $CATHODE_REFERENCE."""
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CATHODE_REFERENCE")
+    if not root or not os.path.isdir(root):
+        sys.exit(f"usage: python {os.path.basename(__file__)} <reference checkout> (or set CATHODE_REFERENCE)")
+    return root
 
 EXPR = r"([^;]+?)"
 LOOP = re.compile(r"for\s*\(\s*int\s+([ij])\s*=\s*" + EXPR + r"\s*;\s*\1\s*<=\s*" + EXPR + r"\s*;\s*\1\s*\+\+\s*\)\s*\{"
@@ -37,6 +45,7 @@ def expr(e: str) -> str:
 
 
 def main():
+    SRC = os.path.join(reference_root(), "include", "initialModule.hpp")
     lines = open(SRC, encoding="utf-8").read().splitlines()
     text = "\n".join(lines[FIRST - 1:LAST])
     # drop comments but keep the line structure (for the citations)

@@ -7,21 +7,29 @@ restated by oracle.fluid.bolsig_tables -> rate_tables.npz with the eleven
 BolsigVec tables and the steps dTe (K) and dEi (J); input/coefEISEE.csv read as
 InputModule::input_SEE_data (inputModule.hpp:605-657), oracle.fluid.see_tables
 -> see_tables.npz with the EB, RD, TS yields and dTe_SEE (K).
-Run in a checkout that has the reference under /root/reference.
+Usage: python <this script> <reference checkout>  (or set CATHODE_REFERENCE).
 """
 import os
 import sys
 
 import numpy as np
 
-SRC = "/root/reference/input"
 HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def reference_root() -> str:
+    """The reference checkout: the first command-line argument, else $CATHODE_REFERENCE."""
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CATHODE_REFERENCE")
+    if not root or not os.path.isdir(root):
+        sys.exit(f"usage: python {os.path.basename(__file__)} <reference checkout> (or set CATHODE_REFERENCE)")
+    return root
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import fluid  # noqa: E402
 
 
 def main():
+    SRC = os.path.join(reference_root(), "input")
     te = open(os.path.join(SRC, "rateCoef_e.csv")).read()
     ti = open(os.path.join(SRC, "rateCoef_i.csv")).read()
     tb, dTe, dEi = fluid.bolsig_tables(te, ti)

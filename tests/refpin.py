@@ -25,10 +25,11 @@ def expand(prm: dict, block: str | None) -> dict:
     return out
 
 
-def case(ni=194, nj=70, xR=0.0388, rmax=0.014, width_neutIn=0.0055):
-    """A reference case on the cathode geometry at ni x nj (makeBoundary run)."""
+def case(ni=194, nj=70, xR=0.0388, rmax=0.014, width_neutIn=0.0055, dropin=False):
+    """A reference case on the cathode geometry at ni x nj (makeBoundary run); with
+    dropin=True its linear solves run on the GPU through include/cathode_solver.hpp."""
     from oracle import ref
-    c = ref.RefCase(ni, nj)
+    c = ref.RefCase(ni, nj, dropin=dropin)
     for k, v in dict(xR=xR, rmax=rmax, width_neutIn=width_neutIn).items():
         assert c.set_param(k, v), k
     c.make_boundary()

@@ -1,11 +1,13 @@
 """The allocation-free residual entry point agrees with the grid-based one.
 
 cth_residual_noalloc exists for callers that may not allocate device memory
-when they need a residual (their own pool owns the device memory, or they are
-recording into a stream capture).  It keeps its scratch in a static device
-array shared by all calls, so this test calls it twice in a row with
-different inputs (the second call must not see the first call's mask or
-partial sums) and compares each result with cth_residual_dev.
+when they need a residual (their own pool owns the device memory, or a loop
+cannot take the synchronisation an allocation may cause).  It keeps its
+scratch in a static device array shared by all calls, so this test calls it
+several times in a row with different inputs, small then large then small
+again (a later call must not see an earlier call's mask or partial sums, in
+particular the leftovers of a larger plane), and compares each result with
+cth_residual_dev.
 This file is collected last so that a stop-at-first-failure run has already
 run every other test.
 """
@@ -38,7 +40,7 @@ def test_residual_noalloc_matches_grid_entry_point(pkg, cuda_device):
         pkg.workloads.random_mmatrix(96, 40, seed=21, blocks=([[1, 60], [61, 96]], [[1, 40], [8, 30]])),
         pkg.workloads.poisson_slab(ni=200, nj=100, seed=3),
     ]
-    for s in cases:
+    for s in cases + cases[::-1]:
         g = pkg.Grid(s["ni"], s["nj"], s["i_bl"], s["j_bl"])
         planes = [g.to_device(s[k]) for k in ("aP", "aE", "aW", "aN", "aS", "b")]
         rng = np.random.default_rng(s["ni"])
