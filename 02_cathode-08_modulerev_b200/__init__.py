@@ -11,8 +11,8 @@ Layers:
 The directory name is not a Python identifier; load it with
 ``__graft_entry__.load_package()`` (registered as ``cathode_b200``).
 """
-from . import batch, capi, feed, fluid, learned, workloads  # noqa: F401
+from . import batch, capi, discharge, feed, fluid, learned, workloads  # noqa: F401
 from .fluid import Fields  # noqa: F401
 from .solvers import Grid, Microwave3, solver_SMG, solver_SOR  # noqa: F401
 
-__all__ = ["batch", "capi", "feed", "fluid", "learned", "workloads", "Fields", "Grid", "Microwave3", "solver_SMG", "solver_SOR"]
+__all__ = ["batch", "capi", "discharge", "feed", "fluid", "learned", "workloads", "Fields", "Grid", "Microwave3", "solver_SMG", "solver_SOR"]

@@ -33,11 +33,11 @@ EXPORTS = (
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_mw3_create", "cth_mw3_destroy", "cth_mw3_ld", "cth_mw3_launch_count", "cth_mw3_assemble_dev",
     "cth_mw3_copy_planes", "cth_mw3_apply_dev", "cth_mw3_solve_dev", "cth_mw3_set_graphs",
-    "cth_mw3_create_blocks", "cth_mw3_set_boundary", "cth_mw3_fill_ghosts", "cth_mw3_set_cycle", "cth_mw3_set_preconditioner",
+    "cth_mw3_create_blocks", "cth_mw3_set_boundary", "cth_mw3_assemble_explicit_dev", "cth_mw3_fill_ghosts", "cth_mw3_set_cycle", "cth_mw3_set_preconditioner", "cth_mw3_set_precision",
     "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_fields_set_download_plan", "cth_fields_download_wait", "cth_fields_set_upload_plan", "cth_fields_upload_many",
     "cth_fields_download_many", "cth_field", "cth_field_upload", "cth_field_download",
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
-    "cth_ghost_rules_upload", "cth_energy_keep_walls_upload", "cth_restart_write", "cth_restart_wait", "cth_restart_read", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
+    "cth_ghost_rules_upload", "cth_energy_keep_walls_upload", "cth_restart_write", "cth_restart_wait", "cth_restart_read", "cth_mw_impedance_test", "cth_mw_divergence", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
     "cth_batch_steps", "cth_update_energy_profile", "cth_mw_port_rescale", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_tensor_cores", "cth_unet_set_smoothing", "cth_unet_set_wait_test", "cth_unet_set_grid_limit", "cth_unet_check", "cth_unet_set_params", "cth_unet_get_params",
@@ -49,6 +49,7 @@ CTH_PROF_RELAX0 = 0
 CTH_PROF_UPDATE = 1
 CTH_PROF_RESTRICT0 = 2
 CTH_PROF_SETUP = 3
+CTH_PROF_RELAXC = 4
 
 
 class Status(ctypes.Structure):
@@ -133,6 +134,16 @@ class SGParams(ctypes.Structure):
                                                "dTe_SEE", "Te_emitSEE_eV", "ratioEngy_EISEE_rd", "error_cnv_HES",
                                                "error_cnv_SOR")] + \
                [(k, ctypes.c_int) for k in ("maxITR_HES", "maxITR_SOR", "flag_error", "flag_iter", "precision")]
+
+
+class ImpedanceParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("dx", "dr", "rmin", "omegam", "J1r_exc", "r1", "r2", "Z0", "Pmw")]
+
+
+class ImpedanceResult(ctypes.Structure):
+    _fields_ = [("V", ctypes.c_double * 2), ("I", ctypes.c_double * 2), ("P_fwd", ctypes.c_double),
+                ("P_ref", ctypes.c_double), ("ratio", ctypes.c_double), ("J1r_exc_factor", ctypes.c_double),
+                ("solve", Status)]
 
 
 class RestartParams(ctypes.Structure):
@@ -262,6 +273,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_mw3_create_blocks.restype = ctypes.c_int
     L.cth_mw3_set_boundary.argtypes = [_vp, ctypes.POINTER(BCList), ctypes.c_int]
     L.cth_mw3_set_boundary.restype = ctypes.c_int
+    L.cth_mw3_set_precision.argtypes = [_vp, ctypes.c_int]
+    L.cth_mw3_set_precision.restype = ctypes.c_int
+    L.cth_mw3_assemble_explicit_dev.argtypes = [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(MWParams), _vp]
+    L.cth_mw3_assemble_explicit_dev.restype = ctypes.c_int
     L.cth_mw3_fill_ghosts.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(MWParams), _vp]
     L.cth_mw3_fill_ghosts.restype = ctypes.c_int
     L.cth_mw3_set_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
@@ -302,6 +317,12 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_ghost_rules_upload.restype = ctypes.c_int
     L.cth_energy_keep_walls_upload.argtypes = [_vp, _vp, ctypes.c_int]
     L.cth_energy_keep_walls_upload.restype = ctypes.c_int
+    L.cth_mw_impedance_test.argtypes = [_vp, _vp, ctypes.POINTER(ImpedanceParams), ctypes.c_int, ctypes.c_double,
+                                        _vp, _vp, ctypes.POINTER(ImpedanceResult)]
+    L.cth_mw_impedance_test.restype = ctypes.c_int
+    L.cth_mw_divergence.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_double] * 4 + [_vp] * 3 + \
+        [ctypes.POINTER(ctypes.c_double), _vp]
+    L.cth_mw_divergence.restype = ctypes.c_int
     L.cth_restart_write.argtypes = [_vp, ctypes.c_char_p, _vp, _vp, _vp]
     L.cth_restart_write.restype = ctypes.c_int
     L.cth_restart_wait.argtypes = [_vp]

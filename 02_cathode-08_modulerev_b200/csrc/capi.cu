@@ -156,6 +156,10 @@ static void free_grid(cth_grid* g) {
         for (auto p : *v) fr(p);
     for (auto* v : {&g->h64.a, &g->h64.x, &g->h64.b, &g->h64.wS, &g->h64.wN, &g->h64.fac})
         for (auto p : *v) fr(p);
+    for (auto* v : {&g->hc.a, &g->hc.x, &g->hc.b, &g->hc.wS, &g->hc.wN, &g->hc.fac})
+        for (auto p : *v) fr(p);
+    for (auto* v : {&g->hcf.a, &g->hcf.x, &g->hcf.b, &g->hcf.wS, &g->hcf.wN, &g->hcf.fac})
+        for (auto p : *v) fr(p);
     fr(g->ws.x64[0]);
     fr(g->ws.x64[1]);
     fr(g->ws.part);
@@ -240,6 +244,7 @@ int cth_grid_create(int ni, int nj, const int* i_bl, const int* j_bl, int n_bl, 
     }
     g->ncol = g->i1 - g->i0 + 1;
     g->ldl = ((g->ncol + 31) / 32) * 32;
+    g->qref = (size_t)g->jbl[0] * g->ld + g->ibl[0];
     if (g->ncol > 4096) {
         set_error("cth_grid_create: z-lines longer than 4096 cells are not supported");
         free_grid(g);

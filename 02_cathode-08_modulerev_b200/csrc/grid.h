@@ -53,6 +53,26 @@ __host__ __device__ inline cd cdiv(cd a, cd b) {
     return cd((a.x * b.x + a.y * b.y) * s, (a.y * b.x - a.x * b.y) * s);
 }
 
+// complex float: the FP32 preconditioner hierarchy of the complex solves (mixed precision);
+// interleaved (re, im) in memory
+struct cf {
+    float x, y;
+    __host__ __device__ cf() : x(0.f), y(0.f) {}
+    __host__ __device__ cf(float r) : x(r), y(0.f) {}
+    __host__ __device__ cf(float r, float i) : x(r), y(i) {}
+    __host__ __device__ explicit cf(cd a) : x((float)a.x), y((float)a.y) {}
+};
+__host__ __device__ inline cf operator+(cf a, cf b) { return cf(a.x + b.x, a.y + b.y); }
+__host__ __device__ inline cf operator-(cf a, cf b) { return cf(a.x - b.x, a.y - b.y); }
+__host__ __device__ inline cf operator-(cf a) { return cf(-a.x, -a.y); }
+__host__ __device__ inline cf operator*(cf a, cf b) { return cf(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__host__ __device__ inline cf& operator+=(cf& a, cf b) { a.x += b.x; a.y += b.y; return a; }
+__host__ __device__ inline cf& operator-=(cf& a, cf b) { a.x -= b.x; a.y -= b.y; return a; }
+__host__ __device__ inline bool operator==(cf a, cf b) { return a.x == b.x && a.y == b.y; }
+__host__ __device__ inline bool operator!=(cf a, cf b) { return !(a == b); }
+__host__ __device__ inline cf conj(cf a) { return cf(a.x, -a.y); }
+__host__ __device__ inline float abs2(cf a) { return a.x * a.x + a.y * a.y; }
+
 // stencil slots: level 0 stores the first 5, coarse levels all 9.
 // Convention of the reference: (A x)_P = a[P] x_P - sum_k a[k] x_k.
 enum Slot { P = 0, W = 1, E = 2, S = 3, N = 4, SW = 5, SE = 6, NW = 7, NE = 8 };
@@ -69,7 +89,7 @@ struct Hierarchy {
 };
 
 // per-kernel-class timing with CUDA events on the launching stream
-enum ProfClass { PROF_RELAX0 = 0, PROF_UPDATE = 1, PROF_RESTRICT0 = 2, PROF_SETUP = 3, PROF_NCLASS = 4 };
+enum ProfClass { PROF_RELAX0 = 0, PROF_UPDATE = 1, PROF_RESTRICT0 = 2, PROF_SETUP = 3, PROF_RELAXC = 4, PROF_NCLASS = 5 };
 
 struct Profiler {
     bool on = false;
@@ -77,9 +97,9 @@ struct Profiler {
     std::vector<int> cls;             // class of each pair
     std::vector<double> bytes;        // algorithmic bytes of each pair
     size_t used = 0;
-    double ms[PROF_NCLASS] = {0, 0, 0, 0};
-    long long n[PROF_NCLASS] = {0, 0, 0, 0};
-    double nbytes[PROF_NCLASS] = {0, 0, 0, 0};
+    double ms[PROF_NCLASS] = {};
+    long long n[PROF_NCLASS] = {};
+    double nbytes[PROF_NCLASS] = {};
 };
 
 // caller arguments of one solve, read by the kernels from device memory so
@@ -103,8 +123,10 @@ struct SolveArgs {
 // device status words of a solve (double array).  ST_GUESS: 0 no guess;
 // 1 + r0 first candidate used; 100 + r0 second candidate used; -(1 + r0)
 // guesses rejected (r0 = relative residual of the used / the better guess)
+// ST_ASCALE, ST_XSCALE (device only): the powers of two that the working-precision
+// cycle's operator and right-hand side are scaled by (see k_prep0 / k_update).
 enum StatWord { ST_RR = 0, ST_RELRES = 1, ST_BB = 2, ST_NONFINITE = 3, ST_ITER = 4, ST_CONV = 5, ST_KEEP = 6,
-                ST_GUESS = 7 };
+                ST_GUESS = 7, ST_ASCALE = 8, ST_XSCALE = 9 };
 
 struct SolveGraph {
     bool valid = false;
@@ -148,6 +170,7 @@ struct cth_grid {
     int ld = 0;          // device layout leading dimension
     size_t plane = 0;    // (nj+2)*ld
     int i0 = 0, i1 = -1, j0 = 0, j1 = -1;
+    size_t qref = 0;  // a grid cell (the first block's first cell) in the caller's layout: operator scale
     int ncol = 0, ldl = 0;
     int nlev = 0;
     std::vector<int> nrow;
@@ -164,6 +187,7 @@ struct cth_grid {
     cth::SolveGraph graphs[2]; // per precision (CTH_PREC_FP64, CTH_PREC_MIXED)
     cth::C5Work c5;
     cth::Hierarchy<cth::cd> hc;    // complex hierarchy (preconditioner of the complex solves)
+    cth::Hierarchy<cth::cf> hcf;   // its FP32 twin (mixed-precision preconditioner)
     cth::SolveGraph c5graph;
     cudaStream_t cap[2] = {nullptr, nullptr};  // capture streams
     bool use_graphs = true;

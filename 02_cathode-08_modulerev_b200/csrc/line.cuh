@@ -477,6 +477,22 @@ __device__ __forceinline__ void st4(cd* p, const cd v[4]) {
     for (int k = 0; k < 4; k++) q[k] = make_double2(v[k].x, v[k].y);
 }
 
+// complex float (the FP32 preconditioner hierarchy): 4 values = two 16-byte accesses
+__device__ __forceinline__ cf rcp(cf a) {
+    const float s = rcp(a.x * a.x + a.y * a.y);
+    return cf(a.x * s, -a.y * s);
+}
+__device__ __forceinline__ void ld4(const cf* p, cf v[4]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 a = q[0], b = q[1];
+    v[0] = cf(a.x, a.y); v[1] = cf(a.z, a.w); v[2] = cf(b.x, b.y); v[3] = cf(b.z, b.w);
+}
+__device__ __forceinline__ void st4(cf* p, const cf v[4]) {
+    float4* q = reinterpret_cast<float4*>(p);
+    q[0] = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+    q[1] = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
+}
+
 // Deterministic grid-wide sums of K values (same last-block scheme as
 // last_block_sum); part holds K*nblocks doubles.
 template <int K>

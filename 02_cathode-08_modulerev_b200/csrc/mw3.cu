@@ -47,6 +47,9 @@ namespace cth {
 int cmg_alloc(cth_grid* g);
 int cmg_setup(cth_grid* g, cudaStream_t s);
 int cmg_vcycle(cth_grid* g, cudaStream_t s);
+int cmg32_alloc(cth_grid* g);
+int cmg32_setup(cth_grid* g, cudaStream_t s);
+int cmg32_vcycle(cth_grid* g, cudaStream_t s);
 
 namespace m3 {
 
@@ -173,9 +176,13 @@ __device__ __forceinline__ cd open_rad(double eps_t, double w, double dr, double
 
 // interior stencils of the three fields on their unknowns (the boundary
 // surgery follows, list by list)
+// J3 != nullptr: the explicit variant solve_Microwave_explicit (:3328-4400): no plasma
+// conductivity in the operator (ne, nu, Bx, Br are not read) and b = -i w mu0 dx^2 dr^2 J on
+// the unknowns, J = sigma E of the previous field (J3[0..2]: J1x, J1r, J1p planes)
 __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __restrict__ nu,
                               const double* __restrict__ Bx, const double* __restrict__ Br,
-                              const double* __restrict__ epsr, cth_mw_params prm, Dev3 D) {
+                              const double* __restrict__ epsr, cth_mw_params prm, Dev3 D, const cd* J1x,
+                              const cd* J1r, const cd* J1p) {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y;
     if (i > D.ni) return;
@@ -191,8 +198,8 @@ __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __res
         cd* A = D.a;
         const double qL = (rjm + rj) / 2.0 / (rj + 1e-100);
         const double qR = (rjp + rj) / 2.0 / (rj + 1e-100);
-        const Sig s = sigma((ne[q] + ne[q - 1]) / 2.0, (nu[q] + nu[q - 1]) / 2.0, (Bx[q] + Bx[q - 1]) / 2.0,
-                            (Br[q] + Br[q - 1]) / 2.0, w, me);
+        const Sig s = J1x ? Sig{} : sigma((ne[q] + ne[q - 1]) / 2.0, (nu[q] + nu[q - 1]) / 2.0,
+                                          (Bx[q] + Bx[q - 1]) / 2.0, (Br[q] + Br[q - 1]) / 2.0, w, me);
         const double eps_t = (epsr[q] + epsr[q - 1]) / 2.0;
         const cd s_xr = s.coef * (s.hx * s.hr), s_xp = s.coef * s.hr, s_xx = s.coef * (cd(1.0) + s.hx * s.hx);
         const cd aP = cd(2.0 * dx * dx + 2.0 * dr * dr - kEPS0 * eps_t * kMU0 * w * w * g2) + iwm * s_xx * cd(g2);
@@ -202,16 +209,16 @@ __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __res
         A[QP * pl + q] = aP; A[QE * pl + q] = aE; A[QW * pl + q] = aW; A[QN * pl + q] = aN; A[QS * pl + q] = aS;
         A[C0 * pl + q] = cNE; A[C1 * pl + q] = cSE; A[C2 * pl + q] = cNW; A[C3 * pl + q] = cSW;
         A[C4 * pl + q] = kp; A[C5 * pl + q] = kp;
-        D.b[q] = cd();
+        D.b[q] = J1x ? cd(0.0, -w * kMU0 * g2) * J1x[q] : cd();
     }
     // ---- Er (r-face between cells j-1 and j), :2352-2411 ----
     if (D.mk[1][q]) {
         cd* A = D.a + (size_t)NQ * pl;
         const double rjmm = r_of(j - 2);
         const double r_t = (rjm + rj) / 2.0, rR = (rj + rjp) / 2.0, rL = (rjmm + rjm) / 2.0;
-        const Sig s = sigma((ne[q] + ne[q - ld]) / 2.0, (nu[q] + nu[q - ld]) / 2.0,
-                            (rj * Bx[q] + rjm * Bx[q - ld]) / (2.0 * r_t), (rj * Br[q] + rjm * Br[q - ld]) / (2.0 * r_t),
-                            w, me);
+        const Sig s = J1r ? Sig{} : sigma((ne[q] + ne[q - ld]) / 2.0, (nu[q] + nu[q - ld]) / 2.0,
+                                          (rj * Bx[q] + rjm * Bx[q - ld]) / (2.0 * r_t),
+                                          (rj * Br[q] + rjm * Br[q - ld]) / (2.0 * r_t), w, me);
         const double eps_t = (epsr[q] + epsr[q - ld]) / 2.0;
         const cd s_rr = s.coef * (cd(1.0) + s.hr * s.hr), s_rp = s.coef * (-s.hx), s_rx = s.coef * (s.hx * s.hr);
         const cd aP = cd(r_t * (1.0 / rj + 1.0 / rjm) * dx * dx + 2.0 * dr * dr - kEPS0 * eps_t * kMU0 * w * w * g2) +
@@ -223,14 +230,14 @@ __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __res
         A[QP * pl + q] = aP; A[QE * pl + q] = aE; A[QW * pl + q] = aW; A[QN * pl + q] = aN; A[QS * pl + q] = aS;
         A[C0 * pl + q] = cNE; A[C1 * pl + q] = cSE; A[C2 * pl + q] = cNW; A[C3 * pl + q] = cSW;
         A[C4 * pl + q] = cNN; A[C5 * pl + q] = cSS;
-        D.b[pl + q] = cd();
+        D.b[pl + q] = J1r ? cd(0.0, -w * kMU0 * g2) * J1r[q] : cd();
     }
     // ---- Ephi (cell), :2414-2453 ----
     if (D.mk[2][q]) {
         cd* A = D.a + (size_t)2 * NQ * pl;
         const double qL = (rjm + rj) / 2.0 / (rj + 1e-100);
         const double qR = (rjp + rj) / 2.0 / (rj + 1e-100);
-        const Sig s = sigma(ne[q], nu[q], Bx[q], Br[q], w, me);
+        const Sig s = J1p ? Sig{} : sigma(ne[q], nu[q], Bx[q], Br[q], w, me);
         const cd s_pr = s.coef * s.hx, s_pp = s.coef, s_px = s.coef * (-s.hr);
         const cd aP = cd(2.0 * dx * dx + 2.0 * dr * dr + g2 / (rj * rj) - kEPS0 * epsr[q] * kMU0 * w * w * g2) +
                 iwm * s_pp * cd(g2);
@@ -239,7 +246,7 @@ __global__ void k_m3_assemble(const double* __restrict__ ne, const double* __res
         A[QP * pl + q] = aP; A[QE * pl + q] = aE; A[QW * pl + q] = aW; A[QN * pl + q] = aN; A[QS * pl + q] = aS;
         A[C0 * pl + q] = kx; A[C1 * pl + q] = kx; A[C2 * pl + q] = kr * cd(qR); A[C3 * pl + q] = kr * cd(qL);
         A[C4 * pl + q] = cd(); A[C5 * pl + q] = cd();
-        D.b[2 * pl + q] = cd();
+        D.b[2 * pl + q] = J1p ? cd(0.0, -w * kMU0 * g2) * J1p[q] : cd();
     }
 }
 
@@ -819,6 +826,7 @@ struct cth_mw3 {
     bool rect = false;
     double rect_key[4] = {0.0, 0.0, 0.0, 0.0};
     bool gauss_seidel = false;  // preconditioner: block Jacobi (default) or block Gauss-Seidel across the fields
+    int precision = CTH_PREC_FP64;  // the preconditioner's V-cycles: complex FP64, or FP32 (CTH_PREC_MIXED)
 };
 
 namespace {
@@ -906,7 +914,7 @@ cudaError_t solve_pre(cth_mw3* m, cudaStream_t s, cudaGraphConditionalHandle con
         cudaStream_t sc = c == 0 ? s : m->side[0][c - 1];
         dim3 gb(256), gg((g->ncol + 255) / 256, g->nrow[0]);
         k_m3_block<<<gg, gb, 0, sc>>>(D, c, g->hc.a[0], g->i0, g->j0, g->ncol, g->nrow[0], g->ldl);
-        *n += 1 + cmg_setup(g, sc);
+        *n += 1 + (m->precision == CTH_PREC_MIXED ? cmg32_setup(g, sc) : cmg_setup(g, sc));
     }
     e = join3(m, 0, s);
     if (e != cudaSuccess) return e;
@@ -923,12 +931,16 @@ cudaError_t solve_body(cth_mw3* m, cudaStream_t s, cudaGraphConditionalHandle co
     Lev0 L = lev0(m);
     dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
     // the preconditioner applied to p (mode 0) or s (mode 1), result into dst
+    // one field's V-cycle: complex FP64, or FP32 with the right-hand side rounded and the result widened
+    auto vcyc = [&](cth_grid* g, cudaStream_t st) -> int {
+        return m->precision == CTH_PREC_MIXED ? cmg32_vcycle(g, st) : cmg_vcycle(g, st);
+    };
     auto precond = [&](int mode, cd* dst) -> cudaError_t {
         if (!m->gauss_seidel) {  // block Jacobi: the three V-cycles side by side
             cudaError_t e = fork3(m, 1, s);
             if (e != cudaSuccess) return e;
-            *n += cmg_vcycle(m->g[0], s);
-            for (int k = 0; k < 2; k++) *n += cmg_vcycle(m->g[1 + k], m->side[1][k]);
+            *n += vcyc(m->g[0], s);
+            for (int k = 0; k < 2; k++) *n += vcyc(m->g[1 + k], m->side[1][k]);
             e = join3(m, 1, s);
             if (e != cudaSuccess) return e;
             k_m3_gather<<<grd, blk, 0, s>>>(D, L, dst);
@@ -936,15 +948,15 @@ cudaError_t solve_body(cth_mw3* m, cudaStream_t s, cudaGraphConditionalHandle co
             return cudaGetLastError();
         }
         // block Gauss-Seidel: Ex, then Er and Ephi with the known fields' couplings taken out
-        *n += cmg_vcycle(m->g[0], s);
+        *n += vcyc(m->g[0], s);
         k_m3_gather1<0><<<grd, blk, 0, s>>>(D, L, dst);
         if (mode == 0) k_m3_gs<0, 1><<<grd, blk, 0, s>>>(D, L, dst);
         else k_m3_gs<1, 1><<<grd, blk, 0, s>>>(D, L, dst);
-        *n += cmg_vcycle(m->g[1], s);
+        *n += vcyc(m->g[1], s);
         k_m3_gather1<1><<<grd, blk, 0, s>>>(D, L, dst);
         if (mode == 0) k_m3_gs<0, 2><<<grd, blk, 0, s>>>(D, L, dst);
         else k_m3_gs<1, 2><<<grd, blk, 0, s>>>(D, L, dst);
-        *n += cmg_vcycle(m->g[2], s);
+        *n += vcyc(m->g[2], s);
         k_m3_gather1<2><<<grd, blk, 0, s>>>(D, L, dst);
         *n += 5;
         return cudaGetLastError();
@@ -1262,13 +1274,9 @@ int cth_mw3_copy_planes(const cth_mw3* m, double* a_dst, double* b_dst, void* st
     return CTH_OK;
 }
 
-int cth_mw3_assemble_dev(cth_mw3* m, const double* ne, const double* nu, const double* Bx, const double* Br,
-                         const double* epsr, const cth_mw_params* prm, void* stream) {
-    if (!m || !ne || !nu || !Bx || !Br || !epsr || !prm || prm->dx <= 0.0 || prm->dr <= 0.0 ||
-        prm->rmin != 0.0 || !(prm->r2 > prm->r1) || prm->r1 <= 0.0 || prm->omegam <= 0.0 || prm->masse <= 0.0) {
-        set_error("cth_mw3_assemble_dev: invalid arguments (the domain starts on the axis: rmin = 0)");
-        return CTH_ERR_ARG;
-    }
+static int mw3_assemble(cth_mw3* m, const double* ne, const double* nu, const double* Bx, const double* Br,
+                        const double* epsr, const cth_mw_params* prm, void* stream, const void* J1x, const void* J1r,
+                        const void* J1p) {
     CTH_CUDA(cudaSetDevice(m->device));
     cudaStream_t s = (cudaStream_t)stream;
     if (m->rect) {
@@ -1280,7 +1288,8 @@ int cth_mw3_assemble_dev(cth_mw3* m, const double* ne, const double* nu, const d
     }
     Dev3 D = dev3(m);
     dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
-    k_m3_assemble<<<grd, blk, 0, s>>>(ne, nu, Bx, Br, epsr, *prm, D);
+    k_m3_assemble<<<grd, blk, 0, s>>>(ne, nu, Bx, Br, epsr, *prm, D, static_cast<const cd*>(J1x),
+                                      static_cast<const cd*>(J1r), static_cast<const cd*>(J1p));
     m->launches++;
     // the lists in the reference's order; entries of one list are distinct rows
     for (int L = 0; L < 12; L++) {
@@ -1292,6 +1301,29 @@ int cth_mw3_assemble_dev(cth_mw3* m, const double* ne, const double* nu, const d
     CTH_CUDA(cudaGetLastError());
     m->assembled = true;
     return CTH_OK;
+}
+
+static bool mw3_params_ok(const cth_mw_params* prm) {
+    return prm->dx > 0.0 && prm->dr > 0.0 && prm->rmin == 0.0 && prm->r2 > prm->r1 && prm->r1 > 0.0 &&
+           prm->omegam > 0.0 && prm->masse > 0.0;
+}
+
+int cth_mw3_assemble_dev(cth_mw3* m, const double* ne, const double* nu, const double* Bx, const double* Br,
+                         const double* epsr, const cth_mw_params* prm, void* stream) {
+    if (!m || !ne || !nu || !Bx || !Br || !epsr || !prm || !mw3_params_ok(prm)) {
+        set_error("cth_mw3_assemble_dev: invalid arguments (the domain starts on the axis: rmin = 0)");
+        return CTH_ERR_ARG;
+    }
+    return mw3_assemble(m, ne, nu, Bx, Br, epsr, prm, stream, nullptr, nullptr, nullptr);
+}
+
+int cth_mw3_assemble_explicit_dev(cth_mw3* m, const double* epsr, const void* J1x, const void* J1r,
+                                  const void* J1p, const cth_mw_params* prm, void* stream) {
+    if (!m || !epsr || !J1x || !J1r || !J1p || !prm || !mw3_params_ok(prm)) {
+        set_error("cth_mw3_assemble_explicit_dev: invalid arguments (the domain starts on the axis: rmin = 0)");
+        return CTH_ERR_ARG;
+    }
+    return mw3_assemble(m, nullptr, nullptr, nullptr, nullptr, epsr, prm, stream, J1x, J1r, J1p);
 }
 
 int cth_mw3_apply_dev(cth_mw3* m, const double* x3, double* y3, void* stream) {
@@ -1337,6 +1369,26 @@ int cth_mw3_set_preconditioner(cth_mw3* m, int mode) {
     CTH_CUDA(cudaSetDevice(m->device));
     CTH_CUDA(cudaDeviceSynchronize());
     m->gauss_seidel = mode == 1;
+    if (m->exec) cudaGraphExecDestroy(m->exec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    m->exec = nullptr;
+    m->graph = nullptr;
+    return CTH_OK;
+}
+
+int cth_mw3_set_precision(cth_mw3* m, int precision) {
+    if (!m || (precision != CTH_PREC_FP64 && precision != CTH_PREC_MIXED)) {
+        set_error("cth_mw3_set_precision: CTH_PREC_FP64 or CTH_PREC_MIXED");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(m->device));
+    CTH_CUDA(cudaDeviceSynchronize());
+    if (precision == CTH_PREC_MIXED)
+        for (int c = 0; c < 3; c++) {
+            const int rc = cmg32_alloc(m->g[c]);
+            if (rc != CTH_OK) return rc;
+        }
+    m->precision = precision;
     if (m->exec) cudaGraphExecDestroy(m->exec);
     if (m->graph) cudaGraphDestroy(m->graph);
     m->exec = nullptr;

@@ -169,7 +169,10 @@ __global__ void k_restart_ghosts(RestartFix A) {
     A.phi[p] = v;
 }
 
-// E on the wall faces from the new ghosts; Er = 0 on the axis (x6)
+// E on the wall faces; Er = 0 on the axis (x6).  Each wall face takes the ghost value of its own
+// segment, as the reference computes E right after that segment's ghost: at a concave corner a
+// later segment overwrites the shared ghost cell, but not the face E already computed (e.g. the
+// z1 face at the x0 corner, inputModule.hpp:1030-1035 then :1070-1075)
 __global__ void k_restart_walls(RestartFix A) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
@@ -178,11 +181,28 @@ __global__ void k_restart_walls(RestartFix A) {
     if (!fc) return;
     const int ld = A.ld;
     const size_t p = (size_t)j * ld + i;
-    if (!(fc & F_BLX)) A.Ex[p] = -(A.phi[p] - A.phi[p - 1]) / A.dx;
-    if (!(fc & F_BRX)) A.Ex[p + 1] = -(A.phi[p + 1] - A.phi[p]) / A.dx;
-    if (!(fc & F_BLR_WALL)) A.Er[p] = -(A.phi[p] - A.phi[p - ld]) / A.dr;
+    const double ph = A.phi[p];
+    if (!(fc & F_BLX)) {
+        const double g = -ph;
+        A.Ex[p] = -(ph - g) / A.dx;
+    }
+    if (!(fc & F_BRX)) {
+        const double g = (fc & F_BRX_BIAS) ? 2.0 * A.V_bias - ph : -ph;
+        A.Ex[p + 1] = -(g - ph) / A.dx;
+    }
+    if (!(fc & F_BLR_WALL)) {
+        const double g = -ph;
+        A.Er[p] = -(ph - g) / A.dr;
+    }
     if (!(fc & F_BLR_CEN)) A.Er[p] = 0.0;
-    if (!(fc & F_BRR_WALL) || !(fc & F_BRR_OPEN)) A.Er[p + ld] = -(A.phi[p + ld] - A.phi[p]) / A.dr;
+    if (!(fc & F_BRR_WALL)) {
+        const double g = -ph;
+        A.Er[p + ld] = -(g - ph) / A.dr;
+    }
+    if (!(fc & F_BRR_OPEN)) {
+        const double g = ph;
+        A.Er[p + ld] = -(g - ph) / A.dr;
+    }
 }
 
 #undef RFL

@@ -11,7 +11,13 @@
 //   * Galerkin coarse operators R A P with R = P^T (9-point on coarse levels);
 //   * outer loop = defect correction: FP64 residual b - A x on the caller's
 //     FP64 coefficients, V-cycle on the residual in the working precision
-//     (FP32 for CTH_PREC_MIXED, FP64 for CTH_PREC_FP64), x += e.
+//     (FP32 for CTH_PREC_MIXED, FP64 for CTH_PREC_FP64), x += e.  The cycle
+//     sees the operator times a power of two sA that brings one diagonal
+//     coefficient to [1, 2) and each residual times a power of two that brings
+//     sA times the previous residual's norm there: the reference's systems
+//     carry coefficients near 1e-18 and right-hand sides down to 1e-38, which
+//     FP32 holds only as subnormals (powers of two are exact, so the FP64
+//     cycles give the same bits as unscaled).
 // Stopping rule of HYPRE SMG: ||b - A x||_2 / ||b||_2 < tol, at most maxITR
 // cycles, zero initial guess (solverFuncs.hpp:106-126).
 #include <cuda_runtime.h>
@@ -39,7 +45,7 @@ struct LevelArgs {
 
 // the real precisions relax with factorised line operators; the complex
 // hierarchy eliminates each line in every relaxation
-template <typename T> constexpr bool kFac = !std::is_same<T, cd>::value;
+template <typename T> constexpr bool kFac = !std::is_same<T, cd>::value && !std::is_same<T, cf>::value;
 
 // ---------------------------------------------------------------------------
 // level-0 preparation: masked copy of the caller's FP64 planes into the level
@@ -101,15 +107,21 @@ __global__ void k_guess(const SolveArgs* __restrict__ args, const unsigned char*
     }
 }
 
+// power of two 2^-e with |v| 2^-e in [1, 2); 1 for zero or non-finite v
+__device__ __forceinline__ double pow2_scale(double v) {
+    return (isfinite(v) && v != 0.0) ? ldexp(1.0, -ilogb(v)) : 1.0;
+}
+
 template <typename T>
 __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask,
-                        int ld_u, int i0, int j0, int ncol, int nrow, int ldl, T* __restrict__ a0,
+                        int ld_u, int i0, int j0, int ncol, int nrow, int ldl, size_t qref, T* __restrict__ a0,
                         T* __restrict__ b0, double* __restrict__ x64, double* __restrict__ part,
                         unsigned int* counter, double* __restrict__ stat, cudaGraphConditionalHandle cond,
                         int use_cond) {
     __shared__ double red[32];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
+    const double sA = pow2_scale(args->aP[qref]);
     const double gw = stat[ST_GUESS];
     const bool guess = gw >= 1.0;
     const double* xg = (gw >= 100.0) ? args->x0b : args->x0;
@@ -121,20 +133,20 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
         const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
         T vP = T(1), vW = T(0), vE = T(0), vS = T(0), vN = T(0), vb = T(0);
         if (mask[p]) {
-            vP = (T)aP[q];
-            if (c > 0 && mask[p - 1]) vW = (T)args->aW[q];
-            if (c + 1 < ncol && mask[p + 1]) vE = (T)args->aE[q];
-            if (r > 0 && mask[p - ldl]) vS = (T)args->aS[q];
-            if (r + 1 < nrow && mask[p + ldl]) vN = (T)args->aN[q];
+            vP = (T)(aP[q] * sA);
+            if (c > 0 && mask[p - 1]) vW = (T)(args->aW[q] * sA);
+            if (c + 1 < ncol && mask[p + 1]) vE = (T)(args->aE[q] * sA);
+            if (r > 0 && mask[p - ldl]) vS = (T)(args->aS[q] * sA);
+            if (r + 1 < nrow && mask[p + ldl]) vN = (T)(args->aN[q] * sA);
             const double bv = args->b[q];
             v2[1] = bv * bv;
             if (guess) {
                 const double rv = guess_resid(args, xg, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
-                vb = (T)rv;
+                vb = (T)(rv * sA);
                 v2[0] = rv * rv;
                 x64[p] = xg[q];
             } else {
-                vb = (T)bv;
+                vb = (T)(bv * sA);
                 v2[0] = v2[1];
             }
         }
@@ -160,6 +172,8 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
         stat[ST_ITER] = 0.0;
         stat[ST_CONV] = (fin && (rr == 0.0 || met)) ? 1.0 : 0.0;
         stat[ST_KEEP] = keep ? 1.0 : 0.0;
+        stat[ST_ASCALE] = sA;
+        stat[ST_XSCALE] = 1.0;
         if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
     }
 }
@@ -424,6 +438,19 @@ __device__ __forceinline__ void ld4cg(const double* p, double v[4]) {
     const double2 q0 = __ldcg(reinterpret_cast<const double2*>(p));
     const double2 q1 = __ldcg(reinterpret_cast<const double2*>(p) + 1);
     v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+}
+template <bool CG> __device__ __forceinline__ cf ldg(const cf* p) {
+    if constexpr (CG) {
+        const float2 q = __ldcg(reinterpret_cast<const float2*>(p));
+        return cf(q.x, q.y);
+    } else {
+        return *p;
+    }
+}
+__device__ __forceinline__ void ld4cg(const cf* p, cf v[4]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 a = __ldcg(q), b = __ldcg(q + 1);
+    v[0] = cf(a.x, a.y); v[1] = cf(a.z, a.w); v[2] = cf(b.x, b.y); v[3] = cf(b.z, b.w);
 }
 __device__ __forceinline__ void ld4cg(const cd* p, cd v[4]) {
     const double2* q = reinterpret_cast<const double2*>(p);
@@ -745,21 +772,27 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
     double* __restrict__ xout = (it & 1) ? x64b : x64a;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
+    // e solves the cycle's system for xs x (the previous right-hand side's scale);
+    // this right-hand side is scaled so that sA times the previous residual norm is O(1)
+    const double sA = stat[ST_ASCALE];
+    const double ie = 1.0 / stat[ST_XSCALE];
+    const double xs = pow2_scale(sqrt(stat[ST_RR]) * sA);
+    const double sb = sA * xs;
     double rr = 0.0;
     if (c < ncol) {
         const size_t p = (size_t)r * ldl + c;
-        const double xc = xin[p] + (double)e[p];
+        const double xc = xin[p] + (double)e[p] * ie;
         double res = 0.0;
         if (mask[p]) {
             const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
             res = args->b[q] - args->aP[q] * xc;
-            if (c + 1 < ncol) res += args->aE[q] * (xin[p + 1] + (double)e[p + 1]);
-            if (c > 0) res += args->aW[q] * (xin[p - 1] + (double)e[p - 1]);
-            if (r + 1 < nrow) res += args->aN[q] * (xin[p + ldl] + (double)e[p + ldl]);
-            if (r > 0) res += args->aS[q] * (xin[p - ldl] + (double)e[p - ldl]);
+            if (c + 1 < ncol) res += args->aE[q] * (xin[p + 1] + (double)e[p + 1] * ie);
+            if (c > 0) res += args->aW[q] * (xin[p - 1] + (double)e[p - 1] * ie);
+            if (r + 1 < nrow) res += args->aN[q] * (xin[p + ldl] + (double)e[p + ldl] * ie);
+            if (r > 0) res += args->aS[q] * (xin[p - ldl] + (double)e[p - ldl] * ie);
         }
         xout[p] = xc;
-        b0[p] = (T)res;
+        b0[p] = (T)(res * sb);
         rr = res * res;
     }
     double tot;
@@ -775,6 +808,7 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
         stat[ST_ITER] = (double)it;
         stat[ST_CONV] = conv ? 1.0 : 0.0;
         stat[ST_KEEP] = keep ? 1.0 : 0.0;
+        stat[ST_XSCALE] = xs;
         if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
     }
 }
@@ -804,6 +838,8 @@ template <>
 Hierarchy<double>& hier<double>(cth_grid* g) { return g->h64; }
 template <>
 Hierarchy<cd>& hier<cd>(cth_grid* g) { return g->hc; }
+template <>
+Hierarchy<cf>& hier<cf>(cth_grid* g) { return g->hcf; }
 
 template <typename T>
 static int alloc_hierarchy(cth_grid* g) {
@@ -887,6 +923,8 @@ static void launch_relax(cth_grid* g, int l, int parity, int zero_guess, int pro
     if (l == 0) slot = prof_mark(g, PROF_RELAX0, (double)rows * g->ncol * 8.0 * sizeof(T), s);
     else if (l == 1 && NPTF > 0)
         slot = prof_mark(g, PROF_RESTRICT0, (double)g->nrow[1] * g->ncol * (9.0 + 8.0) * sizeof(T), s);
+    else  // coarse levels: NPT coefficients + b + x in + x out per cell of the colour
+        slot = prof_mark(g, PROF_RELAXC, (double)rows * g->ncol * (NPT + 3.0) * sizeof(T), s);
     if (g->pdl) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(rows);
@@ -954,6 +992,7 @@ static void launch_tail(cth_grid* g, int l0, cudaStream_t s) {
 template <typename T> constexpr int tail_bit() { return 1; }
 template <> constexpr int tail_bit<double>() { return 2; }
 template <> constexpr int tail_bit<cd>() { return 4; }
+template <> constexpr int tail_bit<cf>() { return 8; }   // no fused tail for the FP32 complex hierarchy
 
 template <typename T>
 static bool tail_from(const cth_grid* g, int l) {
@@ -1043,7 +1082,7 @@ static int enqueue_pre(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle c
     cudaMemsetAsync(w.x64[0], 0, sizeof(double) * (size_t)nrow0 * ldl, s);
     k_guess<<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, w.part, w.counter,
                                 w.stat);
-    k_prep0<T><<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, h.a[0],
+    k_prep0<T><<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, g->qref, h.a[0],
                                    h.b[0], w.x64[0], w.part, w.counter, w.stat, cond, use_cond);
     const long long l0 = g->launches;
     setup_levels<T>(g, s);
@@ -1266,6 +1305,38 @@ int cmg_vcycle(cth_grid* g, cudaStream_t s) {
     return n;
 }
 
+// the same preconditioner with an FP32 complex hierarchy (mixed precision): the level-0
+// operator and right-hand side are rounded from the FP64 ones, the result widened back
+__global__ void k_cd_to_cf(const cd* __restrict__ src, cf* __restrict__ dst, size_t n) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[k] = cf(src[k]);
+}
+__global__ void k_cf_to_cd(const cf* __restrict__ src, cd* __restrict__ dst, size_t n) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[k] = cd(src[k].x, src[k].y);
+}
+int cmg32_alloc(cth_grid* g) { return alloc_hierarchy<cf>(g); }
+int cmg32_setup(cth_grid* g, cudaStream_t s) {
+    const size_t n = (size_t)5 * g->nrow[0] * g->ldl;
+    k_cd_to_cf<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g->hc.a[0], g->hcf.a[0], n);
+    const long long l0 = g->launches;
+    setup_levels<cf>(g, s);
+    const int k = 1 + (int)(g->launches - l0);
+    g->launches = l0;
+    return k;
+}
+int cmg32_vcycle(cth_grid* g, cudaStream_t s) {
+    const size_t n = (size_t)g->nrow[0] * g->ldl;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    k_cd_to_cf<<<nb, 256, 0, s>>>(g->hc.b[0], g->hcf.b[0], n);
+    const long long l0 = g->launches;
+    vcycle<cf>(g, 0, s);
+    const int k = 2 + (int)(g->launches - l0);
+    g->launches = l0;
+    k_cf_to_cd<<<nb, 256, 0, s>>>(g->hcf.x[0], g->hc.x[0], n);
+    return k;
+}
+
 // Device time of the z-line relaxation of one level in its operating mode: reps
 // pairs of (even rows, odd rows) captured in one graph with programmatic
 // dependent launch, as the smoother runs inside a cycle, timed with CUDA events
@@ -1349,6 +1420,12 @@ int configure_kernels(cth_grid* g) {
         CTH_ATTR((k_relax<cd, 5, 0>), smemc); CTH_ATTR((k_relax<cd, 9, 0>), smemc);
         CTH_ATTR((k_relax<cd, 9, 5>), smemc); CTH_ATTR((k_relax<cd, 9, 9>), smemc);
         CTH_ATTR((k_weights<cd, 5>), smemc); CTH_ATTR((k_weights<cd, 9>), smemc);
+    }
+    const int smemcf = (int)line_smem<cf>(g->bd, 2);
+    if (smemcf > 48 * 1024) {
+        CTH_ATTR((k_relax<cf, 5, 0>), smemcf); CTH_ATTR((k_relax<cf, 9, 0>), smemcf);
+        CTH_ATTR((k_relax<cf, 9, 5>), smemcf); CTH_ATTR((k_relax<cf, 9, 9>), smemcf);
+        CTH_ATTR((k_weights<cf, 5>), smemcf); CTH_ATTR((k_weights<cf, 9>), smemcf);
     }
     if (smem32 > 48 * 1024) {
         CTH_ATTR((k_relax<float, 5, 0>), smem32); CTH_ATTR((k_relax<float, 9, 0>), smem32);

@@ -170,6 +170,35 @@ class Grid:
         capi.check(rc)
         return st
 
+    def impedance_test(self, epsr, params: dict, E1r, maxITR=400, error_cnv=1e-12, stream=None) -> dict:
+        """The reference's impedance test (solve_Microwave_impedanceTest, emfieldModule.hpp:5528-6099)
+        on this grid (single block: the Er faces [1, ni] x [2, nj]): assembly, solve, ghosts, port
+        and rescale to Pmw on the device.  epsr: real device plane; E1r: torch complex128 (nj+2, ld),
+        written in place.  params: dx, dr, rmin, omegam, J1r_exc, r1, r2, Z0, Pmw."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        prm = capi.ImpedanceParams(**{k: float(params[k]) for k, _ in capi.ImpedanceParams._fields_})
+        res = capi.ImpedanceResult()
+        rc = self._L.cth_mw_impedance_test(self._h, _ptr(epsr), ctypes.byref(prm), int(maxITR), float(error_cnv),
+                                           _ptr(E1r), s.cuda_stream, ctypes.byref(res))
+        capi.check(rc)
+        return dict(V=complex(res.V[0], res.V[1]), I=complex(res.I[0], res.I[1]), P_fwd=res.P_fwd, P_ref=res.P_ref,
+                    ratio=res.ratio, J1r_exc_factor=res.J1r_exc_factor, solve=res.solve.as_dict())
+
+    def mw_divergence(self, E1x, E1r, E1p, J1x, J1r, J1p, dx, dr, rmin, omegam, stream=None):
+        """output_phase's divE, divJ, div(E + J) columns (outputModule.hpp:43-105) on this
+        grid's cells: torch complex128 (nj+2, ld) planes in; returns (divE, divJ, divEJ, Emag_rep)."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        out = [torch.zeros((self.nj + 2, self.ld), dtype=torch.complex128, device=f"cuda:{self.device}")
+               for _ in range(3)]
+        rep = ctypes.c_double()
+        rc = self._L.cth_mw_divergence(self._h, *[_ptr(a) for a in (E1x, E1r, E1p, J1x, J1r, J1p)], float(dx),
+                                       float(dr), float(rmin), float(omegam), *[_ptr(a) for a in out],
+                                       ctypes.byref(rep), s.cuda_stream)
+        capi.check(rc)
+        return out[0], out[1], out[2], rep.value
+
     def mw_er_assemble_dev(self, ne, nu, epsr, params: dict, stream=None):
         """Er system of the microwave path on the device: returns complex planes
         (aP, aE, aW, aN, aS, b), each torch complex128 of shape (nj+2, ld)."""
@@ -367,6 +396,10 @@ class Microwave3:
         """0: block Jacobi (the fields' V-cycles side by side, default); 1: block
         Gauss-Seidel across Ex, Er, Ephi."""
         capi.check(self._L.cth_mw3_set_preconditioner(self._h, int(mode)), allow_positive=False)
+
+    def set_precision(self, precision: int):
+        """CTH_PREC_FP64 (default) or CTH_PREC_MIXED: FP32 complex V-cycles inside the FP64 BiCGStab."""
+        capi.check(self._L.cth_mw3_set_precision(self._h, int(precision)), allow_positive=False)
 
     def set_cycle(self, nu_pre: int, nu_post: int):
         """Smoothing sweeps per level of the three fields' V-cycles (default 1, 1)."""

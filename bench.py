@@ -313,6 +313,17 @@ def linear_systems(pkg, dev, stream, steps=10):
     out["microwave3_ms"] = e0.elapsed_time(e1) / steps
     out["microwave3_iterations"] = st3.iterations
     out["microwave3_unknowns"] = 3 * NI * NJ - NI - NJ
+    # the same solves with FP32 complex V-cycles inside the FP64 BiCGStab
+    m3.set_precision(pkg.capi.CTH_PREC_MIXED)
+    for it in range(steps + 2):
+        if it == 2:
+            e0.record(stream)
+        m3.assemble_dev(*f3, w3["params"], stream=stream)
+        _, st3 = m3.solve_dev(maxITR=200, error_cnv=TOL, out=e3, stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    out["microwave3_mixed_ms"] = e0.elapsed_time(e1) / steps
+    out["microwave3_mixed_iterations"] = st3.iterations
     m3.close()
     # (d) the same system on the cathode geometry (six blocks per field, the makeBoundary
     # lists), at four times the reference's 194 x 70 in each direction: solve + ghost pass
@@ -335,6 +346,17 @@ def linear_systems(pkg, dev, stream, steps=10):
     out["microwave3_cathode_ms"] = e0.elapsed_time(e1) / steps
     out["microwave3_cathode_iterations"] = stc.iterations
     out["microwave3_cathode_unknowns"] = int(sum(pkg.fluid.block_union_size(*b) for b in cg["blocks"]))
+    mc.set_precision(pkg.capi.CTH_PREC_MIXED)
+    for it in range(steps + 2):
+        if it == 2:
+            e0.record(stream)
+        mc.assemble_dev(*fc, wc["params"], stream=stream)
+        _, stc = mc.solve_dev(maxITR=400, error_cnv=TOL, out=ec, stream=stream)
+        mc.fill_ghosts(ec, fc[4], wc["params"], Er_dc=erc, stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    out["microwave3_cathode_mixed_ms"] = e0.elapsed_time(e1) / steps
+    out["microwave3_cathode_mixed_iterations"] = stc.iterations
     mc.close()
     gcm.close()
     out["workload"] = ("(a) potential with a 1:3.8 dielectric slab, electrodes 0/20 V, axis; (b) microwave Er, "
@@ -685,13 +707,18 @@ def main():
     for _ in range(2):
         step(P)
     torch.cuda.synchronize(dev)
-    g.profile(True)
+    for x in (g, gx, gr):
+        x.profile(True)
     nprof = 5
     for _ in range(nprof):
         step(P)
     torch.cuda.synchronize(dev)
-    prof = {c: g.profile_read(c) for c in (capi.CTH_PROF_RELAX0, capi.CTH_PROF_UPDATE, capi.CTH_PROF_SETUP)}
-    g.profile(False)
+    classes = (capi.CTH_PROF_RELAX0, capi.CTH_PROF_UPDATE, capi.CTH_PROF_RESTRICT0, capi.CTH_PROF_SETUP,
+               capi.CTH_PROF_RELAXC)
+    # summed over the cell grid and the ion face grids: (ms, launches, algorithmic bytes) per class
+    prof = {c: tuple(sum(v) for v in zip(*(x.profile_read(c) for x in (g, gx, gr)))) for c in classes}
+    for x in (g, gx, gr):
+        x.profile(False)
     # the finest relaxation in its operating mode: even / odd pairs back to back in a
     # graph with programmatic dependent launch, on the operator of the last solve
     relax_us, relax_bytes = g.time_relax(capi.CTH_PREC_MIXED, 0, 50)
@@ -759,13 +786,18 @@ def main():
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     r_ms, r_n, r_bytes = prof[capi.CTH_PROF_RELAX0]
     achieved_single = (r_bytes / r_n) / (r_ms / r_n / 1e3) / 1e9 if r_n else None
-    achieved = relax_bytes / (relax_us * 1e-6) / 1e9
+    achieved_pairs = relax_bytes / (relax_us * 1e-6) / 1e9
+    c_ms, c_n, c_bytes = prof[capi.CTH_PROF_RELAXC]
+    achieved_coarse = c_bytes / (c_ms / 1e3) / 1e9 if c_n else None
     u_ms, u_n, u_bytes = prof[capi.CTH_PROF_UPDATE]
     upd = (u_bytes / u_n) / (u_ms / u_n / 1e3) / 1e9 if u_n else None
+    mg_bytes_step = sum(prof[c][2] for c in classes) / nprof
+    step_s = ms_mixed / args.steps / 1e3
     traffic = ncu_traffic()
 
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": value, "fp64_value": fp64_value, "mixed_over_fp64": value / fp64_value,
+        "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 MG cycles + f64 residuals/assembly; complex f64 (mw); bf16 network, f32 accumulate",
         "data": "synthetic (seeded)",
@@ -823,25 +855,45 @@ def main():
                           "rhoeps, rhon, rhom arriving during the sweeps before their first use -- and planned "
                           "downloads, which overlap the sweeps after the one that finalises each field; the wait "
                           "for the copies)"},
-        "roofline": {"bound": "hbm", "kernel": "k_relax<float,5,0> (finest-level z-line relaxation, cell-grid solves)",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None,
-                     "traffic": traffic,
+        "roofline": {"bound": "hbm",
+                     "kernel": "k_relax<float,9,*> (z-line relaxations of the coarse multigrid levels, the step's "
+                               "dominant kernel: 54 % of its kernel time in profiles/launches_step_mixed_512x1024.md)",
+                     "achieved": achieved_coarse, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved_coarse / peak) if achieved_coarse else None,
+                     "traffic": None,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650",
-                     "launch_us": relax_us, "algorithmic_bytes_per_launch": relax_bytes,
-                     "method": "achieved = 8 words per cell of one colour / average device time per launch of 50 "
-                               "even-odd pairs back to back in one CUDA graph with programmatic dependent "
-                               "launch (as the smoother runs inside a cycle), CUDA events on the launching stream; "
-                               "the level's ~23 MB (factors, couplings, b, x) stay L2-resident across the pairs as "
-                               "within one solve, so this is effective bandwidth, not DRAM traffic",
-                     "single_launch": {"launch_us": 1e3 * r_ms / r_n if r_n else None,
-                                       "achieved": achieved_single,
-                                       "frac": (achieved_single / peak) if achieved_single else None,
-                                       "method": "each launch bracketed by CUDA events in the profile pass "
-                                                 "(no overlap with the previous kernel)"}},
+                     "launch_us": 1e3 * c_ms / c_n if c_n else None,
+                     "algorithmic_bytes_per_launch": c_bytes / c_n if c_n else None,
+                     "launches_per_step": c_n / nprof,
+                     "method": "in the step: every launch of the class bracketed by CUDA events on its stream "
+                               "(cell and ion face grids, 5 steps, solves launched kernel by kernel); achieved = "
+                               "algorithmic bytes (9 coefficients + b + x in + x out per cell of the colour) / "
+                               "summed launch time",
+                     "traffic_note": "not measured in this run; a coarse launch moves 0.1-4 MB from L2 (the level "
+                                     "fits), so DRAM bytes do not bound it: the launches are latency chains",
+                     "finest_level": {"kernel": "k_relax<float,5,0>", "launch_us": 1e3 * r_ms / r_n if r_n else None,
+                                      "achieved": achieved_single,
+                                      "frac": (achieved_single / peak) if achieved_single else None,
+                                      "traffic": traffic,
+                                      "traffic_source": "committed ncu summary (profiles/traffic.json), a cold "
+                                                        "launch, not measured in this run",
+                                      "method": "in the step, each launch bracketed by CUDA events"},
+                     "step": {"multigrid_bytes_per_step": mg_bytes_step,
+                              "achieved": mg_bytes_step / step_s / 1e9,
+                              "frac": mg_bytes_step / step_s / 1e9 / peak,
+                              "method": "algorithmic bytes of every multigrid kernel class of one step (relaxations, "
+                                        "restriction, FP64 update, set-up excluded) / the timed step time; the "
+                                        "fluid sweeps' bytes are not counted"},
+                     "l2_resident_pairs": {"launch_us": relax_us, "achieved": achieved_pairs,
+                                           "frac": achieved_pairs / peak,
+                                           "method": "the finest relaxation, 50 even-odd pairs back to back in one "
+                                                     "graph with programmatic dependent launch on the last "
+                                                     "operator; its ~23 MB stay L2-resident, so this is an effective "
+                                                     "bandwidth, not an HBM figure"}},
         "kernels": {
             "update_fp64_residual": {"GB/s": upd, "launch_us": 1e3 * u_ms / u_n if u_n else None},
             "relax0_share_of_step": (r_ms / nprof) / (ms_mixed / args.steps),
+            "coarse_relax_ms_per_step": c_ms / nprof,
         },
         "linear_systems": lin,
         "clocks": clocks,

@@ -102,11 +102,14 @@ int cth_grid_set_tail(cth_grid* g, int enable);
  *   CTH_PROF_RELAX0    finest-level z-line relaxation (one colour per launch)
  *   CTH_PROF_UPDATE    FP64 defect-correction residual
  *   CTH_PROF_RESTRICT0 finest-level restriction
- *   CTH_PROF_SETUP     per-solve set-up (weights + Galerkin products) */
+ *   CTH_PROF_SETUP     per-solve set-up (weights + Galerkin products)
+ *   CTH_PROF_RELAXC    z-line relaxations of the coarse levels (9-point stencils;
+ *                      bytes: 12 words per cell of the colour) */
 #define CTH_PROF_RELAX0 0
 #define CTH_PROF_UPDATE 1
 #define CTH_PROF_RESTRICT0 2
 #define CTH_PROF_SETUP 3
+#define CTH_PROF_RELAXC 4
 long long cth_launch_count(const cth_grid* g);
 int cth_profile(cth_grid* g, int enable);
 int cth_profile_read(const cth_grid* g, int cls, double* ms, long long* launches, double* bytes);
@@ -210,6 +213,48 @@ int cth_mw_er_assemble_dev(cth_grid* g, const double* ne, const double* nu, cons
                            const cth_mw_params* prm, double* aP, double* aE, double* aW, double* aN,
                            double* aS, double* b, void* stream);
 
+/* Impedance test (device arrays) ----------------------------------------------
+ * The reference's calibration mode (flag_impTest == 1, src/main.cpp:126-132):
+ * the coax of InitialModule::makeBoundary_impedanceTest (initialModule.hpp:
+ * 1061-1330: r in [rmin, rmax] = [r1, r2], epsr = epsr_diele in the cells) and
+ * EmfieldModule::solve_Microwave_impedanceTest (emfieldModule.hpp:5528-6099)
+ * without plasma: the Er equation on the faces i = 1..ni, j = 2..nj with the
+ * port excitation (code 7) at the left end, the open end (code 1) at the right,
+ * Gauss (code 2) on both conductors; the complex BiCGStab solve of
+ * cth_c5_solve_dev to tol; then the ghosts of the code-7 and Gauss walls, the
+ * port current and voltage at x_ref = 0, the wave amplitudes for Z0, and E1r
+ * (every entry) scaled by sqrt(Pmw / P_fwd).  g: a grid whose single block is
+ * [1, ni] x [2, nj]; epsr: real device plane of cell values; E1r: complex device
+ * plane (library layout, (re, im) interleaved).  The caller multiplies its
+ * J1r_exc by res->J1r_exc_factor as the reference does (:6036).  Waits for the
+ * stream. */
+typedef struct cth_impedance_params {
+    double dx, dr, rmin;      /* r_j = rmin + (j - 1/2) dr                  */
+    double omegam, J1r_exc;   /* angular frequency, port excitation current */
+    double r1, r2;            /* conductor radii                            */
+    double Z0, Pmw;           /* line impedance, forward power              */
+} cth_impedance_params;
+typedef struct cth_impedance_result {
+    double V[2], I[2];        /* port voltage and current (re, im)          */
+    double P_fwd, P_ref;      /* |b2|^2, |a2|^2 before the rescale (W)      */
+    double ratio, J1r_exc_factor;
+    cth_status solve;
+} cth_impedance_result;
+int cth_mw_impedance_test(cth_grid* g, const double* epsr, const cth_impedance_params* prm, int maxITR,
+                          double tol, double* E1r, void* stream, cth_impedance_result* res);
+
+/* Microwave diagnostics of OutputModule::output_phase (outputModule.hpp:38-184):
+ * Emag_rep = sqrt(mean over cells i = 1..ni, j = 1..nj of |E|^2 at the cell
+ * centre), and on the cells of g's blocks (gc.jdgBnd_Ep: the six cell blocks)
+ * the normalised divergences divE = div(E) dx / Emag_rep, divJ = div(J) dx /
+ * (Emag_rep w eps0) and divEJ = (divJ + i w eps0 divE) dx / (Emag_rep w eps0)
+ * (normalising the already normalised values, as the reference does); zero
+ * elsewhere.  Complex planes of the library layout; r_j = rmin + (j-1/2) dr.
+ * Waits for the stream. */
+int cth_mw_divergence(cth_grid* g, const double* E1x, const double* E1r, const double* E1p, const double* J1x,
+                      const double* J1r, const double* J1p, double dx, double dr, double rmin, double omegam,
+                      double* divE, double* divJ, double* divEJ, double* Emag_rep, void* stream);
+
 /* Magnetised 3-component microwave system of solve_Microwave
  * (include/emfieldModule.hpp:2249-2998): Ex on x-faces, Er on r-faces, Ephi on
  * cells, coupled through the magnetised cold-plasma conductivity (11-point
@@ -259,6 +304,17 @@ long long cth_mw3_launch_count(const cth_mw3* m);
 /* ne, nu, Bx, Br, epsr: real device planes of cell values (library layout) */
 int cth_mw3_assemble_dev(cth_mw3* m, const double* ne, const double* nu, const double* Bx, const double* Br,
                          const double* epsr, const cth_mw_params* prm, void* stream);
+/* The explicit variant, EmfieldModule::solve_Microwave_explicit
+ * (emfieldModule.hpp:3328-4400): the plasma conductivity is left out of the
+ * operator (vacuum + epsr interior rows, no Hall couplings) and enters the
+ * right-hand side as b = -i w mu0 dx^2 dr^2 J on each field's unknowns, J =
+ * sigma E of the field before the solve (complex planes J1x, J1r, J1p of the
+ * library layout; cth_update_energy_profile computes exactly this J,
+ * :7636-7730 being the same formulas as :3384-3470); the boundary lists are
+ * applied as in cth_mw3_assemble_dev.  Solve and ghost pass as for the implicit
+ * system. */
+int cth_mw3_assemble_explicit_dev(cth_mw3* m, const double* epsr, const void* J1x, const void* J1r,
+                                  const void* J1p, const cth_mw_params* prm, void* stream);
 /* copies the assembled coefficients into a_dst: 3 fields x 11 complex planes
  * (P, E, W, N, S, then the couplings C0..C5 of the field: Ex rows Er at
  * (i,j+1), (i,j), (i-1,j+1), (i-1,j) and Ephi at (i,j), (i-1,j); Er rows Ex at
@@ -294,6 +350,13 @@ int cth_mw3_set_cycle(cth_mw3* m, int nu_pre, int nu_post);
  * V-cycles run one after another).  Waits for the device, drops the captured
  * solve. */
 int cth_mw3_set_preconditioner(cth_mw3* m, int mode);
+/* precision of the preconditioner's V-cycles: CTH_PREC_FP64 (complex double,
+ * default) or CTH_PREC_MIXED (complex float hierarchy: each field's level-0
+ * operator and right-hand side rounded to FP32, the result widened back; the
+ * BiCGStab recurrence, its matrix products, residuals and stopping test stay
+ * FP64, so the solve reaches the same tolerance).  Waits for the device, drops
+ * the captured solve. */
+int cth_mw3_set_precision(cth_mw3* m, int precision);
 
 /* Fluid state in HBM -----------------------------------------------------------
  * A field store holds named device planes of the grid's library layout (cell

@@ -39,6 +39,31 @@ inline int& device() {
     return d;
 }
 
+// counts over the solver_SMG / solver_SOR calls of this process (the reference
+// reports nothing; a caller reads these to see whether every solve met its
+// tolerance within maxITR)
+struct SolveStats {
+    long calls = 0;
+    long not_converged = 0;     // CTH_NOT_CONVERGED: maxITR reached above the tolerance
+    int last_iterations = 0;
+    double last_residual = 0.0;
+    double worst_residual = 0.0;  // largest final relative residual of a non-converged call
+};
+inline SolveStats& stats() {
+    static SolveStats s;
+    return s;
+}
+inline void record(int rc, const cth_status& st) {
+    SolveStats& s = stats();
+    s.calls++;
+    s.last_iterations = st.iterations;
+    s.last_residual = st.residual;
+    if (rc == CTH_NOT_CONVERGED) {
+        s.not_converged++;
+        if (st.residual > s.worst_residual) s.worst_residual = st.residual;
+    }
+}
+
 typedef std::tuple<int, int, std::vector<int>, std::vector<int>> GridKey;
 
 // one cth_grid per (shape, block table): the HYPRE grid/stencil/solver set-up
@@ -101,6 +126,7 @@ inline void solver_SMG(const std::vector<std::vector<double> >& aP, const std::v
     int rc = cth_smg_solve(g, f[0].data(), f[1].data(), f[2].data(), f[3].data(), f[4].data(), f[5].data(),
                            maxITR, error_cnv, precision(), f[6].data(), &st);
     if (rc < 0) throw std::runtime_error(std::string("cth_smg_solve: ") + cth_last_error());
+    record(rc, st);
     unflatten_blocks(f[6], i_bl, j_bl, n_bl, solution);
     if (flag_msg == 1) {
         std::printf("Number of Iterations: %d\n", st.iterations);
@@ -125,6 +151,7 @@ inline void solver_SOR(const std::vector<std::vector<double> >& aP, const std::v
     int rc = cth_sor_solve(g, f[0].data(), f[1].data(), f[2].data(), f[3].data(), f[4].data(), f[5].data(),
                            alpha_SOR, maxITR, error_cnv, f[6].data(), &st);
     if (rc < 0) throw std::runtime_error(std::string("cth_sor_solve: ") + cth_last_error());
+    record(rc, st);
     unflatten_blocks(f[6], i_bl, j_bl, n_bl, solution);
     if (flag_msg == 1) std::printf("ncount = %d error_max = %g\n", st.iterations, st.residual);
 }

@@ -1102,3 +1102,38 @@ def mw_port_rescale(E1x, E1r, E1p, J, Jexc, Pabs, power_sum, p: dict):
                I_ref=I_ref, V_ref=V_ref, Gamma_p=Gp, Zp=Z0 * (1.0 + Gp) / (1.0 - Gp), Gamma_all=Ga,
                Zall=Z0 * (1.0 + Ga) / (1.0 - Ga))
     return out, res
+
+
+def divergence(E1x, E1r, E1p, J1x, J1r, J1p, p: dict, mask):
+    """output_phase's representative field and divE, divJ, div(E+J) columns
+    (outputModule.hpp:43-105), loop by loop; mask = gc.jdgBnd_Ep (the six cell
+    blocks).  Returns (divE, divJ, divEJ) as (ni+2, nj+2) arrays and Emag_rep."""
+    ni, nj = E1x.shape[0] - 2, E1x.shape[1] - 2
+    dx, dr, w = p["dx"], p["dr"], p["omegam"]
+    r = p.get("rmin", 0.0) + (np.arange(nj + 2) - 0.5) * dr
+    tot, n = 0.0, 0
+    for i in range(1, ni + 1):
+        for j in range(1, nj + 1):
+            rL = (r[j - 1] + r[j]) / 2.0
+            rR = (r[j + 1] + r[j]) / 2.0
+            ex = (E1x[i, j] + E1x[i + 1, j]) / 2.0
+            er = (rR * E1r[i, j + 1] + rL * E1r[i, j]) / (2.0 * r[j])
+            tot += abs(ex) ** 2 + abs(er) ** 2 + abs(E1p[i, j]) ** 2
+            n += 1
+    rep = np.sqrt(tot / n)
+    out = [np.zeros(E1x.shape, complex) for _ in range(3)]
+    for i in range(1, ni + 1):
+        for j in range(1, nj + 1):
+            if not mask[i, j]:
+                continue
+            rL = (r[j - 1] + r[j]) / 2.0
+            rR = (r[j + 1] + r[j]) / 2.0
+            dE = (rR * E1r[i, j + 1] - rL * E1r[i, j]) / (dr * r[j]) + (E1x[i + 1, j] - E1x[i, j]) / dx
+            dJ = (rR * J1r[i, j + 1] - rL * J1r[i, j]) / (dr * r[j]) + (J1x[i + 1, j] - J1x[i, j]) / dx
+            divE = dE * (dx / rep)
+            divJ = dJ * (dx / (rep * w * EPS0))
+            out[0][i, j] = divE
+            out[1][i, j] = divJ
+            out[2][i, j] = (divJ + 1j * w * EPS0 * divE) * (dx / (rep * w * EPS0))
+    return out[0], out[1], out[2], rep
+

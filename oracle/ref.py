@@ -87,7 +87,12 @@ def lib(dropin: bool = False) -> ctypes.CDLL:
         L.ref_captured_plane.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int]
         L.ref_captured_blocks.argtypes = [ctypes.c_int, _ip, _ip, ctypes.c_int]
         L.ref_dropin_precision.argtypes = [ctypes.c_int]
+        L.ref_dropin_stats.argtypes = [ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long), _dp]
         L.ref_output.argtypes = [_vp, _cs]
+        L.ref_set_cfield.argtypes = [_vp, _cs, _dp]
+        L.ref_get_cfield.argtypes = [_vp, _cs, _dp]
+        L.ref_set_sparam.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.ref_microwave.argtypes = [_vp, _cs, ctypes.c_double, ctypes.c_int, _dp]
         _LIBS[key] = L
     return _LIBS[key]
 
@@ -203,6 +208,32 @@ class RefCase:
             cols.append(buf[:n])
         return np.stack(cols, axis=1)
 
+    def set_cfield(self, name: str, a) -> None:
+        """A complex plane (E1x, E1r, E1p, J1x, J1r, J1p, J1x_exc, J1r_exc, J1p_exc)."""
+        a = np.ascontiguousarray(a, dtype=np.complex128)
+        if a.shape != (self.ni + 2, self.nj + 2):
+            raise ValueError(f"{name}: shape {a.shape}")
+        if self._L.ref_set_cfield(self._h, name.encode(), a.view(np.float64).ctypes.data_as(_dp)) != 0:
+            raise KeyError(name)
+
+    def cfield(self, name: str) -> np.ndarray:
+        out = np.empty((self.ni + 2, self.nj + 2), np.complex128)
+        if self._L.ref_get_cfield(self._h, name.encode(), out.view(np.float64).ctypes.data_as(_dp)) != 0:
+            raise KeyError(name)
+        return out
+
+    def set_sparams(self, S11, S21, S12, S22) -> None:
+        for k, v in enumerate((S11, S21, S12, S22)):
+            self._L.ref_set_sparam(self._h, k, complex(v).real, complex(v).imag)
+
+    def microwave(self, which: str, tol: float = 1e-12, maxit: int = 2000) -> dict:
+        """The drop-in's EmfieldModule::solve_Microwave or update_energy_profile (drop-in build)."""
+        out = (ctypes.c_double * 3)()
+        rc = self._L.ref_microwave(self._h, which.encode(), float(tol), int(maxit), out)
+        if rc != 0:
+            raise RuntimeError(f"{which}: drop-in microwave call failed ({rc})")
+        return dict(iterations=int(out[0]), residual=out[1], converged=int(out[2]))
+
     def output(self, directory: str) -> str:
         """OutputModule::output into directory/results; returns the restart file's path."""
         n = int(self.param("nOut"))
@@ -250,6 +281,15 @@ def captured_planes(ni: int, nj: int) -> list:
         d["i_bl"], d["j_bl"] = ib[:2 * nb].reshape(nb, 2).copy(), jb[:2 * nb].reshape(nb, 2).copy()
         out.append(d)
     return out
+
+
+def dropin_stats() -> dict:
+    """The GPU drop-in's solve counts since the last call: calls, not_converged (maxITR
+    reached above the tolerance), worst (largest final relative residual of those)."""
+    c, n, w = ctypes.c_long(), ctypes.c_long(), np.zeros(1)
+    if lib(True).ref_dropin_stats(ctypes.byref(c), ctypes.byref(n), w) != 0:
+        raise RuntimeError("not the drop-in build")
+    return dict(calls=c.value, not_converged=n.value, worst=float(w[0]))
 
 
 def dropin_precision(p: int) -> None:

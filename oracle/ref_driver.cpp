@@ -38,6 +38,9 @@
 #include "fluidModule.hpp"
 #include "initialModule.hpp"
 #include "outputModule.hpp"
+#ifdef REF_DROPIN
+#include "cathode_emfield.hpp"   // the product's EmfieldModule drop-in (GPU)
+#endif
 
 #ifndef REF_DROPIN
 extern "C" {
@@ -151,6 +154,9 @@ struct RefCase {
     FluidModule flu;
     InitialModule ini;
     OutputModule out;
+#ifdef REF_DROPIN
+    EmfieldModule emf;
+#endif
     bool quiet = true;
     RefCase(int ni, int nj) : gc(ni, nj), gx(ni, nj), gr(ni, nj) {
         pm.ni = ni;
@@ -228,6 +234,15 @@ int* iparam(Params& p, const char* n) {
     I(flag_autoFinish) I(flag_chk) I(flag_gnuRes) I(ndiv_fout) I(flag_impTest) I(n_bl) I(itime) I(itime_PC_phi)
     I(itime_PC_rhoe) I(itime_PC_rhoeps) I(nOut) I(flag_restart)
 #undef I
+    return nullptr;
+}
+
+using VC = std::vector<std::vector<std::complex<double> > >;
+
+VC* cplane(RefCase& c, const char* n) {
+#define M(s, m) if (!std::strcmp(n, #m)) return &c.s.m;
+    M(gx, E1x) M(gx, J1x) M(gx, J1x_exc) M(gr, E1r) M(gr, J1r) M(gr, J1r_exc) M(gc, E1p) M(gc, J1p) M(gc, J1p_exc)
+#undef M
     return nullptr;
 }
 
@@ -382,6 +397,69 @@ int ref_mw_list(void* h, const char* name, int* dst, int cap) {
     return n;
 }
 
+/* Complex planes (E1x, E1r, E1p and the currents), re / im interleaved, [i][j]. */
+int ref_set_cfield(void* h, const char* name, const double* src) {
+    RefCase& c = *static_cast<RefCase*>(h);
+    VC* a = cplane(c, name);
+    if (!a) return -1;
+    const size_t C = c.pm.nj + 2;
+    for (int i = 0; i < c.pm.ni + 2; ++i)
+        for (size_t j = 0; j < C; ++j) (*a)[i][j] = std::complex<double>(src[2 * (i * C + j)], src[2 * (i * C + j) + 1]);
+    return 0;
+}
+
+int ref_get_cfield(void* h, const char* name, double* dst) {
+    RefCase& c = *static_cast<RefCase*>(h);
+    VC* a = cplane(c, name);
+    if (!a) return -1;
+    const size_t C = c.pm.nj + 2;
+    for (int i = 0; i < c.pm.ni + 2; ++i)
+        for (size_t j = 0; j < C; ++j) {
+            dst[2 * (i * C + j)] = (*a)[i][j].real();
+            dst[2 * (i * C + j) + 1] = (*a)[i][j].imag();
+        }
+    return 0;
+}
+
+/* The complex members of Params: S11, S21, S12, S22 (k = 0..3). */
+int ref_set_sparam(void* h, int k, double re, double im) {
+    Params& p = static_cast<RefCase*>(h)->pm;
+    std::complex<double>* s[4] = {&p.S11, &p.S21, &p.S12, &p.S22};
+    if (k < 0 || k > 3) return -1;
+    *s[k] = std::complex<double>(re, im);
+    return 0;
+}
+
+/* The drop-in microwave update (REF_DROPIN builds): the product's EmfieldModule
+ * solve_Microwave / update_energy_profile on this case.  out[0..2] = iterations,
+ * relative residual and convergence of the solve. */
+int ref_microwave(void* h, const char* which, double tol, int maxit, double* out) {
+#ifdef REF_DROPIN
+    RefCase& c = *static_cast<RefCase*>(h);
+    try {
+        c.emf.error_cnv = tol;
+        c.emf.maxITR = maxit;
+        if (!std::strcmp(which, "solve_Microwave")) c.emf.solve_Microwave(c.pm, c.gc, c.gx, c.gr, c.mb);
+        else if (!std::strcmp(which, "solve_Microwave_explicit"))
+            c.emf.solve_Microwave_explicit(c.pm, c.gc, c.gx, c.gr, c.mb);
+        else if (!std::strcmp(which, "update_energy_profile")) c.emf.update_energy_profile(c.pm, c.gc, c.gx, c.gr);
+        else return -1;
+    } catch (const std::exception& e) {
+        std::cerr << e.what() << std::endl;
+        return -2;
+    }
+    if (out) {
+        out[0] = c.emf.last_status.iterations;
+        out[1] = c.emf.last_status.residual;
+        out[2] = c.emf.last_status.converged;
+    }
+    return 0;
+#else
+    (void)h; (void)which; (void)tol; (void)maxit; (void)out;
+    return -1;
+#endif
+}
+
 /* Run one reference method by name, or "step" (the time-loop body). */
 int ref_call(void* h, const char* m) {
     RefCase& c = *static_cast<RefCase*>(h);
@@ -414,6 +492,23 @@ int ref_dropin_precision(int p) {
     return 0;
 #else
     (void)p;
+    return -1;
+#endif
+}
+
+/* The drop-in's solve counts since the last call (calls, not converged, worst final
+ * residual of a non-converged call); -1 when this build uses the exact solve. */
+int ref_dropin_stats(long* calls, long* not_converged, double* worst) {
+#ifdef REF_DROPIN
+    cathode_b200::SolveStats& s = cathode_b200::stats();
+    *calls = s.calls;
+    *not_converged = s.not_converged;
+    *worst = s.worst_residual;
+    s = cathode_b200::SolveStats();
+    return 0;
+#else
+    *calls = *not_converged = 0;
+    *worst = 0.0;
     return -1;
 #endif
 }

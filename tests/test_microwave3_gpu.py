@@ -378,3 +378,44 @@ def test_mw3_gauss_seidel_matches_direct(pkg, cuda_device, geometry):
     with pytest.raises(pkg.capi.CathodeError):
         m.set_preconditioner(2)
     m.close(); g.close()
+
+
+@pytest.mark.parametrize("geometry,bmax,prec", [("rectangle", 0.05, 0), ("rectangle", 0.2, 1), ("cathode", 0.05, 0),
+                                                ("cathode", 0.2, 0), ("cathode", 0.05, 1)])
+def test_mw3_mixed_precision_matches_direct(pkg, cuda_device, geometry, bmax, prec):
+    """FP32 complex V-cycles inside the FP64 BiCGStab reach the direct solution
+    to the same tolerance as the FP64 preconditioner (the recurrence, the
+    operator products and the stopping test stay FP64), in the captured graph
+    and kernel by kernel alike; switching back to FP64 gives the FP64 result."""
+    if geometry == "cathode":
+        w, mw, ref, m, g = _cathode(pkg, 194, 70, bmax=bmax)
+        ni = 194
+    else:
+        ni, nj = 96, 40
+        w, p, mw = _case(pkg, ni, nj, bmax=bmax)
+        ref = mw.mag_rect_system(w["ne"], w["nu"], w["Bx"], w["Br"], w["epsr"], p)
+        g, planes = _device(pkg, w)
+        m = pkg.Microwave3(ni, nj)
+        m.assemble_dev(*planes, w["params"])
+    x_ref = mw.mag_pack(ref, mw.mag_rect_solve(ref))
+    m.set_preconditioner(prec)
+    E64, st64 = m.solve_dev(maxITR=800, error_cnv=1e-12)
+    assert st64.converged == 1, st64.as_dict()
+    m.set_precision(pkg.capi.CTH_PREC_MIXED)
+    its = []
+    for graphs in (True, False):
+        m.set_graphs(graphs)
+        E, st = m.solve_dev(maxITR=800, error_cnv=1e-12)
+        assert st.converged == 1, st.as_dict()
+        assert _rel(mw.mag_pack(ref, _to_ij(E, ni)), x_ref) < 1e-8
+        its.append(st.iterations)
+    assert its[0] == its[1]
+    print("mw3 mixed", geometry, bmax, prec, "iterations fp64", st64.iterations, "mixed", its[0])
+    assert its[0] <= st64.iterations + max(3, st64.iterations // 5)
+    m.set_precision(pkg.capi.CTH_PREC_FP64)
+    E2, st2 = m.solve_dev(maxITR=800, error_cnv=1e-12)
+    assert st2.iterations == st64.iterations
+    assert np.array_equal(E2.cpu().numpy(), E64.cpu().numpy())
+    with pytest.raises(pkg.capi.CathodeError):
+        m.set_precision(7)
+    m.close(); g.close()

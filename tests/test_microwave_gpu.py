@@ -35,6 +35,36 @@ def test_coax_gpu_solve_reproduces_reference_fixture(pkg, cuda_device):
     g.close()
 
 
+def test_impedance_test_entry_point_reproduces_reference_fixture(pkg, cuda_device):
+    """The impedance test as a product entry point (cth_mw_impedance_test: assembly,
+    solve, ghosts, port and rescale on the device) against the reference's own
+    calibration output (test/校正/result_deg0, 5 at print precision) and against the
+    oracle's direct solve and post-processing."""
+    import torch
+    from oracle import microwave as mw
+    p = mw.coax_params()
+    ni, nj = p["ni"], p["nj"]
+    g = pkg.Grid(ni, nj, [[1, ni]], [[2, nj]])
+    epsr = g.to_device(p["epsr"])
+    E = torch.zeros((nj + 2, g.ld), dtype=torch.complex128, device="cuda")
+    prm = {k: p[k] for k in ("dx", "dr", "omegam", "J1r_exc", "r1", "r2", "Z0", "Pmw")}
+    prm["rmin"] = p["rmin"]
+    res = g.impedance_test(epsr, prm, E, maxITR=400, error_cnv=1e-13)
+    assert res["solve"]["converged"] == 1, res
+    got = np.ascontiguousarray(E[:, :ni + 2].cpu().numpy().T)
+    s = mw.coax_er_system(p)
+    Es, J, port = mw.coax_postprocess(mw.solve_c5_direct(s), p)
+    assert np.linalg.norm(got - Es) / np.linalg.norm(Es) < 1e-9
+    assert res["P_fwd"] == pytest.approx(port["P_fwd"], rel=1e-9)
+    assert res["V"] == pytest.approx(port["V"], rel=1e-9)
+    assert p["J1r_exc"] * res["J1r_exc_factor"] == pytest.approx(J, rel=1e-9)
+    for n in (0, 5):
+        Er, _ = mw.coax_output(got, p["J1r_exc"] * res["J1r_exc_factor"], p, n)
+        gold = _golden(n)
+        assert np.linalg.norm(Er - gold) / np.linalg.norm(gold) < 5e-6
+    g.close()
+
+
 def _plasma_helmholtz(ni, nj, seed, nu_lo=1e8, nu_hi=1e10, ne_hi=1e18):
     """Eφ-type complex 5-point system: r-weighted Laplacian + k0^2 eps_p with the
     cold-plasma permittivity eps_p = 1 - wp^2 / (w (w - i nu)), Dirichlet walls."""
@@ -255,3 +285,25 @@ def test_mw_port_rescale_nonfinite_leaves_planes(pkg, cuda_device):
     assert np.array_equal(fs.download("Pabs")[1:-1, 1:-1], Pabs[1:-1, 1:-1]) or \
         np.array_equal(fs.download("Pabs"), Pabs)
     fs.close(); g.close()
+
+
+def test_mw_divergence_matches_oracle(pkg, cuda_device):
+    """output_phase's divergence diagnostics (cth_mw_divergence, outputModule.hpp:43-105)
+    on the cathode's six cell blocks at 97 x 35 against the oracle's loops."""
+    from oracle import microwave as omw
+    ni, nj = 97, 35
+    p = omw.cathode_mw_params(ni, nj)
+    cells, _, _ = omw.cathode_mw_blocks(p)
+    g = pkg.Grid(ni, nj, cells[0], cells[1])
+    rng = np.random.default_rng(12)
+    shp = (ni + 2, nj + 2)
+    F = [rng.standard_normal(shp) + 1j * rng.standard_normal(shp) for _ in range(6)]
+    F[3:] = [1e3 * f for f in F[3:]]
+    dev = [_cplx_dev(g, f) for f in F]
+    divE, divJ, divEJ, rep = g.mw_divergence(*dev, p["dx"], p["dr"], 0.0, p["omegam"])
+    want = omw.divergence(*F, dict(p, rmin=0.0), omw.block_mask(ni, nj, *cells))
+    assert rep == pytest.approx(want[3], rel=1e-13)
+    for got, ref in zip((divE, divJ, divEJ), want[:3]):
+        got = np.swapaxes(got[:, :ni + 2].cpu().numpy(), 0, 1)
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    g.close()

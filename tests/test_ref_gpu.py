@@ -49,7 +49,9 @@ def _norms(get_a, c, m):
 def test_dropin_runs_the_reference_time_step_on_gpu(pkg, orc, cuda_device, ref, precision):
     """Three whole steps of the reference's own loop body, once with every
     solver_SMG call (ions, potential, electron density and energy, neutrals) on
-    the GPU through the header-only drop-in and once with the exact solve."""
+    the GPU through the header-only drop-in and once with the exact solve, within
+    the north-star bar of 1e-8 rel-L2 (measured 4e-9: the solves stop at 1e-13
+    relative residual, and the Scharfetter-Gummel weights amplify the rest)."""
     nstep = 3
     geo, ogeo, st, cfg = T.setup(pkg, "cathode", fp64=True)
     for blk in ("ion", "rhoe", "eps", "neutral"):
@@ -58,13 +60,17 @@ def test_dropin_runs_the_reference_time_step_on_gpu(pkg, orc, cuda_device, ref, 
     ref.dropin_precision(precision)
     exact = _reference_case(geo, st, cfg)
     gpu = _reference_case(geo, st, cfg, dropin=True)
+    ref.dropin_stats()
     for _ in range(nstep):
         exact.call("step")
         gpu.call("step")
+    stats = ref.dropin_stats()
     m = refpin.fluid_mask(exact)
     norms = _norms(gpu.field, exact, m)
+    print("drop-in", "mixed" if precision else "fp64", stats, {k: f"{v:.1e}" for k, v in norms.items()})
+    assert stats["calls"] > 0 and stats["not_converged"] == 0, stats
     for k, v in norms.items():
-        assert v < 1e-9, (k, v)
+        assert v < 1e-8, (k, v)
 
 
 def test_device_steps_match_reference_code(pkg, orc, cuda_device, ref):
@@ -90,3 +96,39 @@ def test_device_steps_match_reference_code(pkg, orc, cuda_device, ref):
     fs.close()
     for x in (g, gx, gr):
         x.close()
+
+
+def test_mixed_precision_solves_of_the_reference_systems(pkg, orc, cuda_device, ref):
+    """Every system the reference assembles in one step (recorded at its
+    solver_SMG calls), solved on the GPU to 1e-13 in FP64 and in mixed precision:
+    both converge within the reference's budget of 100 cycles and agree with the
+    exact solve.  The potential's systems carry coefficients near 1e-18 and
+    right-hand sides down to 1e-38 (FP32 subnormals): the mixed cycles work on
+    the operator and residual scaled by powers of two."""
+    import oracle
+    geo, ogeo, st, cfg = T.setup(pkg, "cathode", fp64=True)
+    c = _reference_case(geo, st, cfg)
+    ref.capture(True)
+    c.call("step")
+    systems = ref.captured_planes(c.ni, c.nj)
+    ref.capture(False)
+    assert len(systems) >= 10
+    for k, s in enumerate(systems):
+        if not np.any(s["b"]):
+            continue
+        n_bl = len(s["i_bl"])
+        m = np.zeros_like(s["aP"], bool)
+        for (i0, i1), (j0, j1) in zip(s["i_bl"], s["j_bl"]):
+            m[i0:i1 + 1, j0:j1 + 1] = True
+        exact = oracle.direct_solve(dict(ni=c.ni, nj=c.nj, i_bl=s["i_bl"], j_bl=s["j_bl"], aP=s["aP"], aE=s["aE"],
+                                         aW=s["aW"], aN=s["aN"], aS=s["aS"], b=s["b"]))
+        its = {}
+        for prec in (pkg.capi.CTH_PREC_FP64, pkg.capi.CTH_PREC_MIXED):
+            x = np.zeros_like(s["aP"])
+            stt = pkg.solver_SMG(s["aP"], s["aE"], s["aW"], s["aN"], s["aS"], s["b"], s["i_bl"], s["j_bl"], n_bl,
+                                 100, 1e-13, 0, x, precision=prec)
+            assert stt.converged == 1 and stt.residual < 1e-13, (k, prec, stt.as_dict())
+            err = np.linalg.norm(x[m] - exact[m]) / np.linalg.norm(exact[m])
+            assert err <= 1e-9, (k, prec, err)
+            its[prec] = (stt.iterations, f"{err:.1e}")
+        print("system", k, "cycles, error against the exact solve (fp64, mixed):", its)

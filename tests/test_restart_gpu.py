@@ -89,6 +89,8 @@ def test_write_is_ordered_before_later_work_on_its_stream(pkg, cuda_device, step
     for k in ("Bx", "Br", "Ex", "Er", "nu_ano", "nu_ano_IAT", "Pabs", "rhoUex_wall", "rhoUer_wall"):
         fs.upload(k, c.field(k))
     fs.update_transport_coef(cfg["params"]["transport"])
+    for k, v in state.items():      # the reference's planes again (the transport update recomputed rate_ionize)
+        fs.upload(k, v)
     x, r = _coords(pkg, c)
     s = torch.cuda.Stream()
     out = os.path.join(stepped["dir"], "device_restart_async.csv")
@@ -158,6 +160,7 @@ def test_reader_rejects_broken_files(pkg, cuda_device, stepped):
         "required column": [lines[0].replace("i,j,x,r,", "i,j,x,rr,")] + lines[1:],
         "index out of range": lines[:9] + ["999" + lines[9][lines[9].index(","):]] + lines[10:],
     }
+    fs.upload("rhoe", c.field("rhoe"))
     before = fs.download("rhoe")
     for msg, ls in cases.items():
         p = os.path.join(stepped["dir"], "broken.csv")
