@@ -53,22 +53,35 @@ def partition(specs, world: int, steps=None):
     return [sorted(x) for x in out]
 
 
-def make_instances(pkg, specs, device=0, precision=1):
-    """Build the instances of ``specs`` on one GPU (grids, field store, parameters)."""
+def make_instances(pkg, specs, device=0, precision=1, microwave=False, ndiv_mw=100):
+    """Build the instances of ``specs`` on one GPU (grids, field store, parameters).
+    microwave=True gives each instance the loop's microwave update every
+    ``ndiv_mw`` steps (its own magnetised system, absorbed power rescaled to the
+    instance's Pmw), so that the power axis of the sweep drives the heating."""
+    from .discharge import MicrowaveUpdate, rect_port
+    from .solvers import Microwave3
     cases = []
     for sp in specs:
         c = learned.make_case(pkg, sp["ni"], sp["nj"], seed=sp["seed"], V_bias=sp["V_bias"], device=device)
         c.update(ni=sp["ni"], nj=sp["nj"], V_bias=sp["V_bias"], Pmw=sp["Pmw"], index=sp["index"])
         set_precision(c, precision)
+        if microwave:
+            ni, nj = sp["ni"], sp["nj"]
+            c["fs"].upload("epsr_mw", np.ones((ni + 2, nj + 2)))
+            prm = dict(pkg.workloads.mw_er_rect(ni, nj, seed=2)["params"])
+            c["m3"] = Microwave3(ni, nj, device=device)
+            c["mwu"] = MicrowaveUpdate(c["fs"], c["m3"], prm, rect_port(prm, sp["Pmw"]), ndiv_mw=ndiv_mw)
         cases.append(c)
     return cases
 
 
-def sweep_instances(pkg, n=64, seed=3, sizes=SIZES, device=0, precision=1):
+def sweep_instances(pkg, n=64, seed=3, sizes=SIZES, device=0, precision=1, microwave=False):
     """Seeded instances of the sweep: grid size drawn from ``sizes``, bias
-    U(-10, 60) V, microwave power U(2, 16) W (recorded; the fluid step reads the
-    absorbed power as a field), discharge state seeded per instance."""
-    return make_instances(pkg, instance_specs(n, seed, sizes), device=device, precision=precision)
+    U(-10, 60) V, microwave power U(2, 16) W (with microwave=True the instance's
+    microwave update rescales its absorbed power to it), discharge state seeded
+    per instance."""
+    return make_instances(pkg, instance_specs(n, seed, sizes), device=device, precision=precision,
+                          microwave=microwave)
 
 
 def set_precision(c, precision):
@@ -98,11 +111,18 @@ def batch_steps(cases, steps: int, nthreads: int):
         items[k].gx = c["gx"]._h
         items[k].gr = c["gr"]._h
         items[k].params = ctypes.pointer(sp)
+        if c.get("mwu") is not None:
+            items[k].mw = c["mwu"]._h
     wall = ctypes.c_double()
     rc = L.cth_batch_steps(items, n, steps, nthreads, ctypes.byref(wall))
     for k, (c, sp) in enumerate(zip(cases, keep)):
         fluid.step_params_back(sp, c["P"])
         c["anode"] = dict(I=items[k].I_Anode, Ii=items[k].Ii_Anode, Ie=items[k].Ie_Anode)
+        if c.get("mwu") is not None:
+            m = c.setdefault("mw_stats", dict(runs=0))
+            m["runs"] += items[k].mw_runs
+            if items[k].mw_runs:
+                m.update(power_sum=items[k].mw_power_sum, J1r_exc=items[k].mw_J1r_exc)
     if rc < 0:
         raise capi.CathodeError(rc, capi.last_error())
     return wall.value, [items[k].rc for k in range(n)], [items[k].seconds for k in range(n)]
@@ -111,9 +131,13 @@ def batch_steps(cases, steps: int, nthreads: int):
 def summary(c) -> dict:
     """The I-V point of one instance after its steps: bias, power, anode currents."""
     a = c.get("anode", {})
-    return dict(index=int(c["index"]), ni=int(c["ni"]), nj=int(c["nj"]), V_bias=float(c["V_bias"]),
-                Pmw=float(c["Pmw"]), itime=int(c["P"]["itime"]), I_Anode=float(a.get("I", 0.0)),
-                Ii_Anode=float(a.get("Ii", 0.0)), Ie_Anode=float(a.get("Ie", 0.0)))
+    out = dict(index=int(c["index"]), ni=int(c["ni"]), nj=int(c["nj"]), V_bias=float(c["V_bias"]),
+               Pmw=float(c["Pmw"]), itime=int(c["P"]["itime"]), I_Anode=float(a.get("I", 0.0)),
+               Ii_Anode=float(a.get("Ii", 0.0)), Ie_Anode=float(a.get("Ie", 0.0)))
+    if "mw_stats" in c:
+        m = c["mw_stats"]
+        out.update(mw_runs=int(m["runs"]), mw_power_before_rescale=float(m.get("power_sum", 0.0)))
+    return out
 
 
 def run_shard(specs, indices, runner):
@@ -139,7 +163,7 @@ def gather(local: list, world: int, group=None) -> list:
     return sorted(out, key=lambda x: x["index"])
 
 
-def gpu_runner(pkg, steps, device=0, nthreads=None, precision=1):
+def gpu_runner(pkg, steps, device=0, nthreads=None, precision=1, microwave=False):
     """The runner of run_shard on one GPU: builds the specs' instances, advances
     them ``steps`` steps with cth_batch_steps and returns their summaries."""
     import os
@@ -147,7 +171,7 @@ def gpu_runner(pkg, steps, device=0, nthreads=None, precision=1):
     def run(sel):
         if not sel:
             return []
-        cases = make_instances(pkg, sel, device=device, precision=precision)
+        cases = make_instances(pkg, sel, device=device, precision=precision, microwave=microwave)
         try:
             T = max(1, min(len(cases), nthreads or os.cpu_count() or 1))
             _, rc, _ = batch_steps(cases, steps=steps, nthreads=T)
@@ -163,7 +187,8 @@ def gpu_runner(pkg, steps, device=0, nthreads=None, precision=1):
 
 
 def sequential_steps(cases, steps: int):
-    """The same steps one case after another on the caller's thread (host clock)."""
+    """The same steps one case after another on the caller's thread (host clock),
+    with each case's microwave update where it has one."""
     import time
     import torch
     t0 = time.perf_counter()
@@ -172,6 +197,8 @@ def sequential_steps(cases, steps: int):
             r = c["fs"].fluid_step(c["gx"], c["gr"], c["P"])
             if r["solver_rc"] != 0:
                 raise RuntimeError(f"solve did not converge: {r}")
+            if c.get("mwu") is not None and c["mwu"].due(c["P"]["itime"]):
+                c["mwu"].run(c["gx"], c["gr"])
     torch.cuda.synchronize()
     return time.perf_counter() - t0
 
@@ -212,4 +239,7 @@ def autotune(cases, candidates=None, steps=3):
 
 def close(cases):
     for c in cases:
+        if c.get("mwu") is not None:
+            c["mwu"].close()
+            c["m3"].close()
         learned.close_case(c)

@@ -39,7 +39,8 @@ EXPORTS = (
     "cth_flags_upload", "cth_table_upload", "cth_update_transport_coef", "cth_solve_phi_pc",
     "cth_ghost_rules_upload", "cth_energy_keep_walls_upload", "cth_restart_write", "cth_restart_wait", "cth_restart_read", "cth_mw_impedance_test", "cth_mw_divergence", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
-    "cth_batch_steps", "cth_update_energy_profile", "cth_mw_port_rescale", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
+    "cth_batch_steps", "cth_mw_update_create", "cth_mw_update_destroy", "cth_mw_update_due", "cth_mw_update_plane",
+    "cth_mw_update_run", "cth_mw_update_prepare", "cth_update_energy_profile", "cth_mw_port_rescale", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_tensor_cores", "cth_unet_set_smoothing", "cth_unet_set_wait_test", "cth_unet_set_grid_limit", "cth_unet_check", "cth_unet_set_params", "cth_unet_get_params",
     "cth_unet_get_grads", "cth_unet_set_loss_weights", "cth_unet_forward", "cth_unet_backward",
     "cth_unet_train_step", "cth_unet_set_stats", "cth_unet_features", "cth_unet_predict_dphi",
@@ -203,7 +204,19 @@ class BatchItem(ctypes.Structure):
     _fields_ = [("fs", ctypes.c_void_p), ("gx", ctypes.c_void_p), ("gr", ctypes.c_void_p),
                 ("params", ctypes.POINTER(StepParams)), ("rc", ctypes.c_int), ("steps_done", ctypes.c_int),
                 ("seconds", ctypes.c_double), ("I_Anode", ctypes.c_double), ("Ii_Anode", ctypes.c_double),
-                ("Ie_Anode", ctypes.c_double)]
+                ("Ie_Anode", ctypes.c_double), ("mw", ctypes.c_void_p), ("mw_runs", ctypes.c_int),
+                ("mw_power_sum", ctypes.c_double), ("mw_J1r_exc", ctypes.c_double)]
+
+
+class MWUpdateParams(ctypes.Structure):
+    """cth_mw_update_params: the microwave update of the time loop."""
+    _fields_ = [("mw", MWParams), ("port", MWPortParams), ("ndiv_mw", ctypes.c_int), ("maxit", ctypes.c_int),
+                ("tol", ctypes.c_double)]
+
+
+class MWUpdateResult(ctypes.Structure):
+    _fields_ = [("solve", Status), ("power_sum", ctypes.c_double), ("ratio", ctypes.c_double),
+                ("J1r_exc", ctypes.c_double), ("rescale_rc", ctypes.c_int)]
 
 
 class StepResult(ctypes.Structure):
@@ -365,6 +378,18 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_batch_steps.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_double)]
     L.cth_batch_steps.restype = ctypes.c_int
+    L.cth_mw_update_create.argtypes = [_vp, _vp, ctypes.POINTER(MWUpdateParams), _vp, _vp, ctypes.POINTER(_vp)]
+    L.cth_mw_update_create.restype = ctypes.c_int
+    L.cth_mw_update_destroy.argtypes = [_vp]
+    L.cth_mw_update_destroy.restype = None
+    L.cth_mw_update_due.argtypes = [_vp, ctypes.c_int]
+    L.cth_mw_update_due.restype = ctypes.c_int
+    L.cth_mw_update_plane.argtypes = [_vp, ctypes.c_int]
+    L.cth_mw_update_plane.restype = ctypes.c_void_p
+    L.cth_mw_update_run.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(MWUpdateResult)]
+    L.cth_mw_update_run.restype = ctypes.c_int
+    L.cth_mw_update_prepare.argtypes = [_vp, _vp]
+    L.cth_mw_update_prepare.restype = ctypes.c_int
     L.cth_update_energy_profile.argtypes = [_vp, _vp, _vp, ctypes.POINTER(EnergyParams)] + [_vp] * 7 + \
         [ctypes.POINTER(EnergyResult)]
     L.cth_update_energy_profile.restype = ctypes.c_int

@@ -28,6 +28,8 @@ extern "C" int cth_batch_steps(cth_batch_item* items, int n, int steps, int nthr
         items[k].steps_done = 0;
         items[k].seconds = 0.0;
         items[k].I_Anode = items[k].Ii_Anode = items[k].Ie_Anode = 0.0;
+        items[k].mw_runs = 0;
+        items[k].mw_power_sum = items[k].mw_J1r_exc = 0.0;
     }
     std::vector<cudaStream_t> streams(n, nullptr);
     for (int k = 0; k < n; k++) {
@@ -54,6 +56,15 @@ extern "C" int cth_batch_steps(cth_batch_item* items, int n, int steps, int nthr
                 it.I_Anode = r.rhoe.I_Anode;
                 it.Ii_Anode = r.rhoe.Ii_Anode;
                 it.Ie_Anode = r.rhoe.Ie_Anode;
+                if (it.mw && cth_mw_update_due(it.mw, it.params->itime)) {
+                    cth_mw_update_result mr;
+                    const int mrc = cth_mw_update_run(it.mw, it.gx, it.gr, streams[mine[q]], &mr);
+                    if (mrc < 0) { it.rc = mrc; continue; }
+                    if (mrc > it.rc) it.rc = mrc;
+                    it.mw_runs++;
+                    it.mw_power_sum = mr.power_sum;
+                    it.mw_J1r_exc = mr.J1r_exc;
+                }
             }
         }
         for (size_t q = 0; q < mine.size(); q++) {

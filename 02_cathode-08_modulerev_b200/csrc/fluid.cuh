@@ -100,31 +100,43 @@ constexpr double kBoltz = 1.380649e-23;    // constants.hpp:5
 constexpr double kE0f = 1.60217662e-19;    // constants.hpp:6
 constexpr double kEps0f = 8.8541878128e-12;// constants.hpp:7
 
-// uniform-step table lookups of miniFuncs.hpp:35-91
+// uniform-step table lookups of miniFuncs.hpp:35-91.  In range the arithmetic is
+// the reference's.  Outside it the reference indexes its vector with whatever
+// (int)(x / dx) gives: below zero that reads before the table, and past INT_MAX
+// iL + 1 wraps negative -- values a diverging run produces.  Here the index is
+// formed only after the range test: a negative argument extrapolates from the
+// first interval, a large one takes the reference's end-of-table branch, NaN
+// stays NaN.
+__device__ __forceinline__ int lookup_left(double t) { return t > 0.0 ? (int)t : 0; }
+
 __device__ __forceinline__ double d_func_Te(const double* __restrict__ v, int n, double Te, double dTe) {
-    const int iL = (int)(Te / dTe);
+    const double t = Te / dTe;
+    if (isnan(t)) return t;
+    if (!(t < (double)(n - 2))) return v[n - 1];
+    const int iL = lookup_left(t);
     const int iR = iL + 1;
     const double Te_L = iL * dTe;
-    if (iR < n - 1) return (v[iR] - v[iL]) / (dTe + 1e-100) * (Te - Te_L) + v[iL];
-    return v[n - 1];
+    return (v[iR] - v[iL]) / (dTe + 1e-100) * (Te - Te_L) + v[iL];
 }
 
 __device__ __forceinline__ double d_func_dTe(const double* __restrict__ v, int n, double Te, double dTe) {
-    int iL = (int)(Te / dTe);
-    int iR = iL + 1;
-    if (iR >= n - 1) {
-        iL = n - 2;
-        iR = n - 1;
-    }
+    const double t = Te / dTe;
+    if (isnan(t)) return t;
+    const int iL = (t < (double)(n - 2)) ? lookup_left(t) : n - 2;
+    const int iR = iL + 1;
     return (v[iR] - v[iL]) / (iR * dTe - iL * dTe + 1e-100);
 }
 
 __device__ __forceinline__ double d_func_Ei(const double* __restrict__ v, int n, double Ei, double dEi,
                                             double massi) {
-    const int iL = (int)(Ei / dEi);
-    const int iR = iL + 1;
-    const double Ei_L = iL * dEi;
-    if (iR < n - 1) return (v[iR] - v[iL]) / (dEi + 1e-100) * (Ei - Ei_L) + v[iL];
+    const double t = Ei / dEi;
+    if (isnan(t)) return t;
+    if (t < (double)(n - 2)) {
+        const int iL = lookup_left(t);
+        const int iR = iL + 1;
+        const double Ei_L = iL * dEi;
+        return (v[iR] - v[iL]) / (dEi + 1e-100) * (Ei - Ei_L) + v[iL];
+    }
     const double imax = n - 1;
     const double v_max = sqrt(imax * dEi / massi);
     const double v_tmp = sqrt(Ei / massi);

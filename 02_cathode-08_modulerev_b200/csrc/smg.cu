@@ -241,10 +241,9 @@ __global__ void k_weights(LevelArgs<T> L, const unsigned char* __restrict__ mask
 // weights (two right-hand sides through the fresh factors).
 // ---------------------------------------------------------------------------
 template <typename T, int NPT>
-__global__ void k_factor(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ fac,
-                         T* __restrict__ wS, T* __restrict__ wN, int weights) {
-    __shared__ T sh[(8 + LG_N) * 32];
-    const int j = blockIdx.x;
+__device__ __forceinline__ void factor_row(const LevelArgs<T>& L, const unsigned char* __restrict__ mask,
+                                           T* __restrict__ fac, T* __restrict__ wS, T* __restrict__ wN,
+                                           int weights, int j, T* sh) {
     const int n = L.ncol, s0 = CH * threadIdx.x;
     const int cnt = max(0, min(CH, n - s0));
     const size_t pl = L.plane;
@@ -301,6 +300,13 @@ __global__ void k_factor(LevelArgs<T> L, const unsigned char* __restrict__ mask,
     }
 }
 
+template <typename T, int NPT>
+__global__ void k_factor(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ fac,
+                         T* __restrict__ wS, T* __restrict__ wN, int weights) {
+    __shared__ T sh[(8 + LG_N) * 32];
+    factor_row<T, NPT>(L, mask, fac, wS, wN, weights, blockIdx.x, sh);
+}
+
 // P(g, i -> J): weight of coarse row J in fine row g at column i
 template <typename T>
 __device__ __forceinline__ T pw(const unsigned char* __restrict__ mask, const T* __restrict__ wS,
@@ -316,12 +322,10 @@ __device__ __forceinline__ T pw(const unsigned char* __restrict__ mask, const T*
 // Galerkin coarse operator: one thread per coarse cell.
 // ---------------------------------------------------------------------------
 template <typename T, int NPT>
-__global__ void k_galerkin(LevelArgs<T> F, const unsigned char* __restrict__ maskf,
-                           const T* __restrict__ wS, const T* __restrict__ wN, T* __restrict__ ac,
-                           int nrowc, const unsigned char* __restrict__ maskc) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int J = blockIdx.y;
-    if (i >= F.ncol) return;
+__device__ __forceinline__ void galerkin_cell(const LevelArgs<T>& F, const unsigned char* __restrict__ maskf,
+                                              const T* __restrict__ wS, const T* __restrict__ wN,
+                                              T* __restrict__ ac, int nrowc, const unsigned char* __restrict__ maskc,
+                                              int i, int J) {
     const int ld = F.ld, ncol = F.ncol;
     const size_t plc = (size_t)nrowc * ld;
     const size_t q = (size_t)J * ld + i;
@@ -396,6 +400,34 @@ __global__ void k_galerkin(LevelArgs<T> F, const unsigned char* __restrict__ mas
         const T v = acc[oj[k] + 1][oi[k] + 1];
         ac[k * plc + q] = (k == P) ? v : -v;
     }
+}
+
+template <typename T, int NPT>
+__global__ void k_galerkin(LevelArgs<T> F, const unsigned char* __restrict__ maskf,
+                           const T* __restrict__ wS, const T* __restrict__ wN, T* __restrict__ ac,
+                           int nrowc, const unsigned char* __restrict__ maskc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F.ncol) return;
+    galerkin_cell<T, NPT>(F, maskf, wS, wN, ac, nrowc, maskc, i, blockIdx.y);
+}
+
+// Galerkin operator of coarse row J = blockIdx.x and, in the same CTA, that row's
+// line factorisation (and its interpolation weights when it is an F row of a
+// non-coarsest level): one launch per level of the set-up instead of two.  Each
+// thread computes the cells CH*threadIdx.x .. +CH-1 of the row, which are the
+// cells it reads back in the factorisation (its own writes), so no barrier is
+// needed between the two parts.  Same arithmetic as k_galerkin + k_factor.
+template <typename T, int NPTF>
+__global__ void k_galfac(LevelArgs<T> F, const unsigned char* __restrict__ maskf, const T* __restrict__ wSf,
+                         const T* __restrict__ wNf, LevelArgs<T> C, const unsigned char* __restrict__ maskc,
+                         T* __restrict__ facc, T* __restrict__ wSc, T* __restrict__ wNc, int weights) {
+    __shared__ T sh[(8 + LG_N) * 32];
+    const int J = blockIdx.x;
+    const int s0 = CH * threadIdx.x;
+#pragma unroll 1
+    for (int k = 0; k < CH; k++)
+        if (s0 + k < F.ncol) galerkin_cell<T, NPTF>(F, maskf, wSf, wNf, const_cast<T*>(C.a), C.nrow, maskc, s0 + k, J);
+    factor_row<T, 9>(C, maskc, facc, wSc, wNc, weights, J, sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -1032,20 +1064,23 @@ static void setup_levels(cth_grid* g, cudaStream_t s) {
     if constexpr (kFac<T>) {
         // per level: factorise every line (and the F-row weights), then the
         // Galerkin operator of the next level
-        for (int l = 0; l < g->nlev; l++) {
-            LevelArgs<T> L = level_args<T>(g, l);
-            const int wts = l + 1 < g->nlev;
-            if (l == 0) k_factor<T, 5><<<g->nrow[l], g->bd, 0, s>>>(L, g->mask[l], h.fac[l], h.wS[l], h.wN[l], wts);
-            else k_factor<T, 9><<<g->nrow[l], g->bd, 0, s>>>(L, g->mask[l], h.fac[l], h.wS[l], h.wN[l], wts);
+        // level 0: factors (+ F-row weights); then per level one launch that forms
+        // the next level's Galerkin operator row by row and factorises each row
+        {
+            LevelArgs<T> L = level_args<T>(g, 0);
+            k_factor<T, 5><<<g->nrow[0], g->bd, 0, s>>>(L, g->mask[0], h.fac[0], h.wS[0], h.wN[0], g->nlev > 1);
             g->launches++;
-            if (!wts) break;
-            dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
+        }
+        for (int l = 0; l + 1 < g->nlev; l++) {
+            LevelArgs<T> L = level_args<T>(g, l);
+            LevelArgs<T> Lc = level_args<T>(g, l + 1);
+            const int wts = l + 2 < g->nlev;
             if (l == 0)
-                k_galerkin<T, 5><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
-                                                     g->nrow[l + 1], g->mask[l + 1]);
+                k_galfac<T, 5><<<g->nrow[1], g->bd, 0, s>>>(L, g->mask[0], h.wS[0], h.wN[0], Lc, g->mask[1],
+                                                            h.fac[1], h.wS[1], h.wN[1], wts);
             else
-                k_galerkin<T, 9><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
-                                                     g->nrow[l + 1], g->mask[l + 1]);
+                k_galfac<T, 9><<<g->nrow[l + 1], g->bd, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], Lc, g->mask[l + 1],
+                                                                h.fac[l + 1], h.wS[l + 1], h.wN[l + 1], wts);
             g->launches++;
         }
     } else {
@@ -1305,11 +1340,31 @@ int cmg_vcycle(cth_grid* g, cudaStream_t s) {
     return n;
 }
 
-// the same preconditioner with an FP32 complex hierarchy (mixed precision): the level-0
-// operator and right-hand side are rounded from the FP64 ones, the result widened back
+// the same preconditioner with an FP32 complex hierarchy (mixed precision): the
+// operators of every level and the interpolation weights are set up in FP64 (the
+// Galerkin sums of an indefinite operator cancel, which FP32 accumulation does not
+// survive on the coarse levels) and then rounded; the cycle runs in FP32 on the
+// rounded right-hand side and its result is widened back
 __global__ void k_cd_to_cf(const cd* __restrict__ src, cf* __restrict__ dst, size_t n) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) dst[k] = cf(src[k]);
+}
+constexpr int kMaxSeg = 48;
+struct CvtSegs {
+    const cd* src[kMaxSeg];
+    cf* dst[kMaxSeg];
+    size_t n[kMaxSeg];
+    int count;
+};
+// grid-stride rounding of up to kMaxSeg arrays in one launch (blockIdx.y = segment)
+__global__ void k_cd_to_cf_segs(CvtSegs S) {
+    const int sgi = blockIdx.y;
+    if (sgi >= S.count) return;
+    const cd* __restrict__ src = S.src[sgi];
+    cf* __restrict__ dst = S.dst[sgi];
+    const size_t n = S.n[sgi];
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        dst[k] = cf(src[k]);
 }
 __global__ void k_cf_to_cd(const cf* __restrict__ src, cd* __restrict__ dst, size_t n) {
     const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1317,12 +1372,33 @@ __global__ void k_cf_to_cd(const cf* __restrict__ src, cd* __restrict__ dst, siz
 }
 int cmg32_alloc(cth_grid* g) { return alloc_hierarchy<cf>(g); }
 int cmg32_setup(cth_grid* g, cudaStream_t s) {
-    const size_t n = (size_t)5 * g->nrow[0] * g->ldl;
-    k_cd_to_cf<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g->hc.a[0], g->hcf.a[0], n);
     const long long l0 = g->launches;
-    setup_levels<cf>(g, s);
-    const int k = 1 + (int)(g->launches - l0);
+    setup_levels<cd>(g, s);
+    int k = (int)(g->launches - l0);
     g->launches = l0;
+    CvtSegs S{};
+    for (int l = 0; l < g->nlev; l++) {
+        const size_t n = (size_t)g->nrow[l] * g->ldl;
+        const int npt = (l == 0) ? 5 : 9;
+        const cd* src[3] = {g->hc.a[l], g->hc.wS[l], g->hc.wN[l]};
+        cf* dst[3] = {g->hcf.a[l], g->hcf.wS[l], g->hcf.wN[l]};
+        const size_t cnt[3] = {n * npt, n, n};
+        for (int t = 0; t < 3; t++) {
+            if (S.count == kMaxSeg) {
+                k_cd_to_cf_segs<<<dim3(64, S.count), 256, 0, s>>>(S);
+                k++;
+                S.count = 0;
+            }
+            S.src[S.count] = src[t];
+            S.dst[S.count] = dst[t];
+            S.n[S.count] = cnt[t];
+            S.count++;
+        }
+    }
+    if (S.count > 0) {
+        k_cd_to_cf_segs<<<dim3(64, S.count), 256, 0, s>>>(S);
+        k++;
+    }
     return k;
 }
 int cmg32_vcycle(cth_grid* g, cudaStream_t s) {

@@ -14,14 +14,70 @@ from . import capi
 from .solvers import Grid, Microwave3
 
 
-class _Plane:
-    """A raw device pointer with the data_ptr() of a torch tensor."""
+def rect_port(mw_params: dict, Pmw: float) -> dict:
+    """Port settings of the rectangle's microwave update: no feed block, so no
+    reflection model (flag_mwRef = 0): the absorbed power is rescaled to Pmw."""
+    return dict(dx=mw_params["dx"], dr=mw_params["dr"], rmin=mw_params.get("rmin", 0.0),
+                omegam=mw_params["omegam"], r1=mw_params["r1"], r2=mw_params["r2"], Z0=50.0, Pmw=float(Pmw),
+                S11=0j, S21=1 + 0j, S12=1 + 0j, S22=0j, flag_mwRef=0, i_ref=1, j_out=0, i_out0=0, i_out1=0, jf0=0,
+                jf1=0)
 
-    def __init__(self, p):
-        self.p = p
 
-    def data_ptr(self):
-        return self.p
+class MicrowaveUpdate:
+    """cth_mw_update: the microwave update of the time loop (src/main.cpp:254-257)
+    on a field store -- assembly from rhoe, nu_m1, Bx, Br, epsr_mw, solve, ghost
+    pass, update_energy_profile, port / rescale to port["Pmw"] -- every ``ndiv_mw``
+    steps.  E3 / J3: (3, nj+2, ld) complex128 device planes (None: the library
+    allocates them)."""
+
+    def __init__(self, fs, m3, mw_params: dict, port: dict, ndiv_mw=100, maxit=400, tol=1e-10, E3=None, J3=None):
+        import ctypes
+        self._L = capi.load()
+        p = capi.MWUpdateParams()
+        for k, _ in capi.MWParams._fields_:
+            setattr(p.mw, k, float(mw_params.get(k, 0.0)))
+        for k, _ in capi.MWPortParams._fields_:
+            v = port[k]
+            if k.startswith("S"):
+                getattr(p.port, k)[0], getattr(p.port, k)[1] = complex(v).real, complex(v).imag
+            else:
+                setattr(p.port, k, v)
+        p.ndiv_mw, p.maxit, p.tol = int(ndiv_mw), int(maxit), float(tol)
+        self._keep = (E3, J3)
+        h = ctypes.c_void_p()
+        capi.check(self._L.cth_mw_update_create(fs._h, m3._h, ctypes.byref(p),
+                                                E3.data_ptr() if E3 is not None else None,
+                                                J3.data_ptr() if J3 is not None else None, ctypes.byref(h)),
+                   allow_positive=False)
+        self._h = h
+
+    def due(self, itime: int) -> bool:
+        return bool(self._L.cth_mw_update_due(self._h, int(itime)))
+
+    def run(self, gx, gr, stream=None) -> dict:
+        import ctypes
+        r = capi.MWUpdateResult()
+        s = 0 if stream is None else stream.cuda_stream
+        rc = self._L.cth_mw_update_run(self._h, gx._h, gr._h, s, ctypes.byref(r))
+        capi.check(rc)
+        return dict(solve=r.solve.as_dict(), power_sum=r.power_sum, ratio=r.ratio, J1r_exc=r.J1r_exc, rc=rc)
+
+    def prepare(self, stream=None):
+        """Build the solve's hierarchy and graph (assembly + solve only; the
+        discharge's state is left as it was)."""
+        capi.check(self._L.cth_mw_update_prepare(self._h, 0 if stream is None else stream.cuda_stream),
+                   allow_positive=False)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.cth_mw_update_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 FIELDS = ("rhoe", "rhoi", "rhon", "rhom", "Te", "Bx", "Br", "rhoeps", "phi", "Ex", "Er", "nUex", "nUer", "Uix",
@@ -79,30 +135,21 @@ class RectangleDischarge:
         self.m3 = Microwave3(ni, nj, device=device)
         self.e3 = self.m3.planes(3)
         self.j3 = self.m3.planes(3)
-        self.eprm = {k: self.mw_params.get(k, 0.0) for k in ("dx", "dr", "rmin", "omegam", "masse")}
-        self.port = dict(dx=self.eprm["dx"], dr=self.eprm["dr"], rmin=self.eprm["rmin"], omegam=self.eprm["omegam"],
-                         r1=self.mw_params["r1"], r2=self.mw_params["r2"], Z0=50.0, Pmw=Pmw, S11=0j, S21=1 + 0j,
-                         S12=1 + 0j, S22=0j, flag_mwRef=0, i_ref=1, j_out=0, i_out0=0, i_out1=0, jf0=0, jf1=0)
+        self.port = rect_port(self.mw_params, Pmw)
+        self.mw = MicrowaveUpdate(self.fs, self.m3, self.mw_params, self.port, ndiv_mw=ndiv_mw, maxit=mw_maxit,
+                                  tol=mw_tol, E3=self.e3, J3=self.j3)
 
     def microwave(self, stream=None) -> dict:
         """solve_Microwave + update_energy_profile (flag_mwRef = 0) on the current state."""
-        fs = self.fs
-        f3 = [_Plane(fs.ptr(k)) for k in ("rhoe", "nu_m1", "Bx", "Br", "epsr_mw")]
-        prm = dict(self.mw_params, J1r_exc=self.J1r_exc)
-        self.m3.assemble_dev(*f3, prm, stream=stream)
-        st = self.m3.solve_dev(maxITR=self.mw_maxit, error_cnv=self.mw_tol, out=self.e3, stream=stream)[1]
-        self.m3.fill_ghosts(self.e3, f3[4], prm, Er_dc=_Plane(fs.ptr("Er")), stream=stream)
-        er = fs.update_energy_profile(self.gx, self.gr, self.eprm, self.e3[0], self.e3[1], self.e3[2], self.j3[0],
-                                      self.j3[1], self.j3[2], stream=stream)
-        pr = fs.mw_port_rescale(self.port, er["power_sum"], stream=stream)
-        self.J1r_exc *= pr["J1r_exc_factor"]
-        return dict(solve=st.as_dict(), power_sum=er["power_sum"], ratio=pr["ratio"])
+        out = self.mw.run(self.gx, self.gr, stream=stream)
+        self.J1r_exc = out["J1r_exc"]
+        return out
 
     def step(self, stream=None) -> dict:
         r = self.fs.fluid_step(self.gx, self.gr, self.P, stream=stream)
         if r["solver_rc"] < 0:
             raise capi.CathodeError(r["solver_rc"], "fluid step failed")
-        if self.P["itime"] % self.ndiv_mw == 0:
+        if self.mw.due(self.P["itime"]):
             r["mw"] = self.microwave(stream=stream)
         return r
 
@@ -114,6 +161,7 @@ class RectangleDischarge:
         return [np.ascontiguousarray(self.e3[c, :, :self.ni + 2].cpu().numpy().T) for c in range(3)]
 
     def close(self):
+        self.mw.close()
         self.m3.close()
         self.fs.close()
         for x in (self.g, self.gx, self.gr):

@@ -68,7 +68,7 @@ MAXIT = 30
 
 NDIV_MW = 100
 LEARN_SEEDS, LEARN_STEPS, LEARN_EPOCHS = 3, 110, 24  # snapshots: seeds x (steps - 2), the timed range
-BATCH_N, BATCH_STEPS = 64, 10                       # batched sweep: instances, timed steps each
+BATCH_N, BATCH_STEPS = 64, 100                      # batched sweep: instances, timed steps each (one microwave update)
 PROGNOSTIC = ("rhoe", "rhoi", "rhoeps", "Te", "rhon", "rhom", "phi", "Ex", "Er", "Uix", "Uir", "Uip")
 STATE = ("rhoe", "rhoi", "rhon", "rhom", "Te", "Bx", "Br", "rhoeps", "rhoe_old")
 
@@ -153,12 +153,14 @@ def measured_peaks():
 
 
 def ncu_traffic():
-    """DRAM bytes per launch of the finest-level relaxation from the committed ncu summary."""
+    """DRAM bytes per launch from the committed ncu summaries: the finest-level
+    relaxation (a cold launch) and the coarse-level relaxations (the step's L2
+    state, and cold)."""
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        return d.get("relax0_dram_bytes_per_launch")
+        return d
     except Exception:
-        return None
+        return {}
 
 
 # --------------------------------------------------------------------------
@@ -376,9 +378,11 @@ def batched_sweep(pkg, device, rank, world, n=BATCH_N, steps=BATCH_STEPS):
     (batch.partition; one GPU per rank, no collective while they run), each
     rank's share advanced together by host worker threads with the autotuned
     cycle shapes and mixed precision, against the same steps run one instance
-    after another with plain FP64 multigrid from zero.  The I-V points (anode
-    currents per instance) are gathered with one all-gather at the end; the wall
-    time is the max over ranks."""
+    after another with plain FP64 multigrid from zero.  Every instance carries
+    the loop's microwave update every 100 steps (its own magnetised system, the
+    absorbed power rescaled to its Pmw), so the 100 timed steps hold one update
+    per instance.  The I-V points (anode currents per instance) are gathered
+    with one all-gather at the end; the wall time is the max over ranks."""
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -386,26 +390,34 @@ def batched_sweep(pkg, device, rank, world, n=BATCH_N, steps=BATCH_STEPS):
     t0 = time.perf_counter()
     specs = B.instance_specs(n, seed=3)
     mine = B.partition(specs, world, steps=steps)[rank]
-    cases = B.make_instances(pkg, [specs[i] for i in mine], device=device)
+    sel = [specs[i] for i in mine]
+    cases = B.make_instances(pkg, sel, device=device, microwave=True)
     setup_s = time.perf_counter() - t0
     threads = max(1, min(len(cases), os.cpu_count() or 1))
     B.batch_steps(cases, steps=2, nthreads=threads)                # graphs, lazily allocated planes
     tuned = B.autotune(cases, steps=2)
     B.batch_steps(cases, steps=1, nthreads=threads)
+    for c in cases:                     # each microwave solve's hierarchy and graph, built once
+        c["mwu"].prepare()
+    torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     wall, rc, secs = B.batch_steps(cases, steps=steps, nthreads=threads)
     table = B.gather([dict(B.summary(c), rc=int(r)) for c, r in zip(cases, rc)], world)
     cells = sum(c["ni"] * c["nj"] for c in cases)
-    for c in cases:
-        B.set_precision(c, pkg.capi.CTH_PREC_FP64)
-        B.set_cycle(c, 1, 1, True)
-    B.sequential_steps(cases, steps=1)
-    seq = B.sequential_steps(cases, steps=steps)
     by = {}
     for c, t in zip(cases, secs):
         by.setdefault(f"{c['nj']}x{c['ni']}", []).append(steps / t)
     B.close(cases)
+    # the baseline: the same instances from the same initial state, plain FP64, one after another
+    base = B.make_instances(pkg, sel, device=device, precision=pkg.capi.CTH_PREC_FP64, microwave=True)
+    for c in base:
+        B.set_cycle(c, 1, 1, True)
+    B.sequential_steps(base, steps=1)
+    for c in base:
+        c["mwu"].prepare()
+    seq = B.sequential_steps(base, steps=steps)
+    B.close(base)
     torch.cuda.synchronize()
     tw = torch.tensor([wall, seq, float(cells)], dtype=torch.float64, device=torch.device("cuda", device))
     if world > 1:
@@ -421,13 +433,63 @@ def batched_sweep(pkg, device, rank, world, n=BATCH_N, steps=BATCH_STEPS):
         "sequential_fp64": {"instance_steps_per_s": n * steps / seq, "cell_steps_per_s": cells * steps / seq},
         "speedup_vs_sequential_fp64": seq / wall,
         "steps_per_s_per_instance_by_size": {k: float(np.mean(v)) for k, v in sorted(by.items())},
-        "iv_points": [{k: t[k] for k in ("index", "V_bias", "Pmw", "I_Anode")} for t in table[:8]],
+        "iv_points": [{k: t[k] for k in ("index", "V_bias", "Pmw", "I_Anode", "mw_runs", "mw_power_before_rescale")}
+                      for t in table[:8]],
+        "microwave_updates": sum(t.get("mw_runs", 0) for t in table),
         "autotune": tuned, "setup_s": setup_s,
         "timing": "host wall clock around the batch call (all instance streams synchronised inside), max over ranks",
         "workload": "seeded instances, sizes drawn from 64x128, 128x256, 192x384, 256x512 (r x z), "
-                    "bias U(-10, 60) V, Pmw U(2, 16) W (recorded; absorbed power is an input field); "
+                    "bias U(-10, 60) V, Pmw U(2, 16) W (each instance's microwave update every 100 steps "
+                    "rescales its absorbed power to its Pmw; 100 timed steps = one update per instance); "
                     "split over the ranks by cells x steps, I-V points gathered at the end",
     }
+
+
+def production(pkg, device, steps, warmup, ni=2048, nj=1024):
+    """Config 4 at bounded length: the seeded discharge scaled to 1024 (r) x 2048
+    (z) cells, the loop's microwave update every 100 steps, ``steps`` steps in
+    plain FP64 (zero start) and in mixed precision with the previous-step warm
+    start; steps/s by CUDA events, the anode ion current per step and its
+    relative change over the last 100 steps (the steady-state criterion is
+    < 1e-6)."""
+    import numpy as np
+    import torch
+    out = {"workload": f"{nj} (r) x {ni} (z) rectangle, physics of the 100 x 200 discharge scaled to the grid, "
+                       "microwave update every 100 steps (Pmw 8 W)", "steps": steps, "warmup": warmup, "modes": {}}
+    for name, prec, warm in (("fp64", pkg.capi.CTH_PREC_FP64, False), ("mixed_warm", pkg.capi.CTH_PREC_MIXED, True)):
+        d = pkg.discharge.RectangleDischarge(pkg, ni, nj, seed=0, device=device, precision=prec)
+        if warm:
+            d.P["phi"].update(warm_start=2, guess_max_relres=1.0)
+            d.fs.set_warm_start(True)
+        s = torch.cuda.current_stream(device)
+        for _ in range(warmup):
+            d.step(stream=s)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        cur, nonconv = [], 0
+        e0.record(s)
+        for _ in range(steps):
+            r = d.step(stream=s)
+            cur.append(r["anode"]["Ii"])
+            nonconv += int(r["solver_rc"] != 0)
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        c = np.array(cur)
+        w = c[-100:] if c.size >= 100 else c
+        out["modes"][name] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
+                              "steps_with_unconverged_solve": nonconv, "Ii_Anode_first": float(c[0]),
+                              "Ii_Anode_last": float(c[-1]),
+                              "Ii_rel_change_per_step_last_window": float(np.max(np.abs(np.diff(w))) /
+                                                                          max(abs(float(w[-1])), 1e-300))
+                              if w.size > 1 else None,
+                              "projected_hours_for_1e5_steps": 1e5 * ms / steps / 3.6e6}
+        d.close()
+        torch.cuda.synchronize(device)
+    f, m = out["modes"]["fp64"], out["modes"]["mixed_warm"]
+    out["mixed_warm_over_fp64"] = m["steps_per_s"] / f["steps_per_s"]
+    print(json.dumps(out), flush=True)
+    return 0
 
 
 def main():
@@ -449,6 +511,10 @@ def main():
                     help="profiling mode: this many solves of the magnetised 3-component microwave system at "
                          "512 x 1024 (seeded magnet workload) after --warmup ones, launched kernel by kernel "
                          "(profilers cannot see kernels inside conditional graphs), then exit")
+    ap.add_argument("--production", type=int, default=0,
+                    help="production-size mode: this many time steps of the 1024 (r) x 2048 (z) discharge (microwave "
+                         "update every 100 steps) in plain FP64 and in mixed precision with the previous-step warm "
+                         "start, after --warmup steps each; prints one JSON line and exits")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every multigrid kernel individually (profilers cannot see kernels inside "
                          "conditional graphs); same kernels, host convergence checks")
@@ -492,6 +558,8 @@ def main():
         m3.close()
         gm.close()
         return 0
+    if args.production > 0:
+        return production(pkg, local, args.production, args.warmup)
     if args.profile_network > 0:
         net = pkg.learned.UNet(NJ, NI, seed=0)
         gen = torch.Generator(device=dev).manual_seed(0)
@@ -860,7 +928,8 @@ def main():
                                "dominant kernel: 54 % of its kernel time in profiles/launches_step_mixed_512x1024.md)",
                      "achieved": achieved_coarse, "peak": peak, "unit": "GB/s",
                      "frac": (achieved_coarse / peak) if achieved_coarse else None,
-                     "traffic": None,
+                     "traffic": traffic.get("coarse_relax_dram_bytes_per_launch"),
+                     "traffic_cold": traffic.get("coarse_relax_dram_bytes_per_launch_cold"),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650",
                      "launch_us": 1e3 * c_ms / c_n if c_n else None,
                      "algorithmic_bytes_per_launch": c_bytes / c_n if c_n else None,
@@ -869,12 +938,15 @@ def main():
                                "(cell and ion face grids, 5 steps, solves launched kernel by kernel); achieved = "
                                "algorithmic bytes (9 coefficients + b + x in + x out per cell of the colour) / "
                                "summed launch time",
-                     "traffic_note": "not measured in this run; a coarse launch moves 0.1-4 MB from L2 (the level "
-                                     "fits), so DRAM bytes do not bound it: the launches are latency chains",
+                     "traffic_note": "from the committed ncu capture of the same step (profiles/traffic.json, "
+                                     "profiles/k_relax_coarse_f32_512x1024.md), not this run: mean DRAM read+write per "
+                                     "launch over the first 300 launches of the class, with the step's own L2 state "
+                                     "(traffic) and with caches flushed (traffic_cold); below the algorithmic bytes "
+                                     "because the coarse levels stay in L2 -- the launches are latency chains",
                      "finest_level": {"kernel": "k_relax<float,5,0>", "launch_us": 1e3 * r_ms / r_n if r_n else None,
                                       "achieved": achieved_single,
                                       "frac": (achieved_single / peak) if achieved_single else None,
-                                      "traffic": traffic,
+                                      "traffic": traffic.get("relax0_dram_bytes_per_launch"),
                                       "traffic_source": "committed ncu summary (profiles/traffic.json), a cold "
                                                         "launch, not measured in this run",
                                       "method": "in the step, each launch bracketed by CUDA events"},

@@ -698,6 +698,8 @@ int cth_restart_wait(cth_fields* fs);
 int cth_restart_read(cth_fields* fs, cth_grid* gx, cth_grid* gr, const char* path, const double* x,
                      const double* r, const cth_restart_params* prm, void* stream, cth_restart_info* info);
 
+typedef struct cth_mw_update cth_mw_update;  /* the microwave update, declared below */
+
 /* Batched instances (the I-V sweeps; no counterpart in the reference, which runs
  * one discharge per process) -------------------------------------------------
  * cth_batch_steps advances n independent instances (own grids, store, step
@@ -708,7 +710,10 @@ int cth_restart_read(cth_fields* fs, cth_grid* gx, cth_grid* gr, const char* pat
  * an instance failed; that instance stops, the others continue); per item: rc,
  * steps done, wall seconds and the anode currents of its last step
  * (FluidModule::solve_rhoe_wdTe_wSEE_PC, fluidModule.hpp:3944-3964);
- * *wall_seconds = the whole batch. */
+ * *wall_seconds = the whole batch.  An item with mw set also runs that
+ * microwave update after every step whose itime it is due on (its Pmw then
+ * drives the instance's heating); mw_runs counts them and mw_power_sum /
+ * mw_J1r_exc report the last one. */
 typedef struct cth_batch_item {
     cth_fields* fs;
     cth_grid* gx;
@@ -718,6 +723,9 @@ typedef struct cth_batch_item {
     int steps_done;
     double seconds;
     double I_Anode, Ii_Anode, Ie_Anode;  /* anode currents of the last step (the I-V point) */
+    cth_mw_update* mw;                   /* optional microwave update (NULL: none)          */
+    int mw_runs;
+    double mw_power_sum, mw_J1r_exc;
 } cth_batch_item;
 int cth_batch_steps(cth_batch_item* items, int n, int steps, int nthreads, double* wall_seconds);
 
@@ -779,6 +787,48 @@ typedef struct cth_mw_port_result {
 int cth_mw_port_rescale(cth_fields* fs, const cth_mw_port_params* prm, double power_sum, void* E1x, void* E1r,
                         void* E1p, void* J1x, void* J1r, void* J1p, void* J1x_exc, void* J1r_exc, void* J1p_exc,
                         void* stream, cth_mw_port_result* res);
+
+/* The microwave update of the time loop (src/main.cpp:254-257) on a discharge's
+ * device state -----------------------------------------------------------------
+ * Every ndiv_mw steps the reference calls EmfieldModule::solve_Microwave and
+ * update_energy_profile.  cth_mw_update_run does both on the store fs with the
+ * system m (rectangle or block geometry, boundary lists set): assembly from the
+ * store's rhoe, nu_m1, Bx, Br and epsr_mw planes (upload epsr_mw, the cells'
+ * relative permittivity, before the first run), the solve to tol within maxit
+ * iterations, the ghost pass (Er of the store for open east faces), the
+ * absorbed power into the store's Pabs and the J planes, the port part with
+ * port.Pmw (the store's Pabs rescaled to Pmw; flag_mwRef as given), and the
+ * excitation current J1r_exc for the next run multiplied by the root of the
+ * ratio.  E3 / J3: the caller's device buffers of 3 complex planes each in m's
+ * layout (E1x, E1r, E1p / J1x, J1r, J1p), or NULL for planes the handle
+ * allocates (zero) and frees; cth_mw_update_plane: 0-2 E, 3-5 J.  They persist
+ * between runs as the reference's fields do.  Returns the solve's
+ * status (CTH_NOT_CONVERGED after maxit) or the rescale's (CTH_NONFINITE: not
+ * rescaled); the stream is synchronised (the integrals are read back). */
+typedef struct cth_mw_update_params {
+    cth_mw_params mw;           /* the system; mw.J1r_exc is the initial excitation */
+    cth_mw_port_params port;    /* port / reflection / rescale, with Pmw            */
+    int ndiv_mw;                /* run every ndiv_mw steps                          */
+    int maxit;
+    double tol;
+} cth_mw_update_params;
+typedef struct cth_mw_update_result {
+    cth_status solve;
+    double power_sum;           /* absorbed power before the rescale (W)            */
+    double ratio;               /* Pmw / delivered power                            */
+    double J1r_exc;             /* excitation current for the next run              */
+    int rescale_rc;
+} cth_mw_update_result;
+int cth_mw_update_create(cth_fields* fs, cth_mw3* m, const cth_mw_update_params* p, double* E3, double* J3,
+                         cth_mw_update** out);
+void cth_mw_update_destroy(cth_mw_update* u);
+int cth_mw_update_due(const cth_mw_update* u, int itime);
+double* cth_mw_update_plane(cth_mw_update* u, int which);
+int cth_mw_update_run(cth_mw_update* u, cth_grid* gx, cth_grid* gr, void* stream, cth_mw_update_result* res);
+/* the first solve of a handle builds its hierarchy and solve graph: this runs the
+ * assembly and the solve alone (E's unknowns written, nothing else: no ghosts,
+ * no absorbed power, no rescale), so that the build happens before a timed run */
+int cth_mw_update_prepare(cth_mw_update* u, void* stream);
 
 /* Two-port feed helpers (host) -------------------------------------------------
  * CmpMat2 (cmpMat2.hpp:8-34): 2x2 complex matrices, complex values as

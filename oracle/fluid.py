@@ -81,9 +81,11 @@ def rectangle_flags(ni, nj) -> np.ndarray:
 
 
 def func_Te(value, Te, dTe):
-    """miniFuncs.hpp:35-46 (elementwise)."""
+    """miniFuncs.hpp:35-46 (elementwise).  Below the table (Te / dTe <= -1, where
+    the reference reads before its vector) the first interval is extrapolated,
+    as the device does."""
     value = np.asarray(value)
-    iL = np.trunc(Te / dTe).astype(np.int64)
+    iL = np.maximum(np.trunc(Te / dTe), 0).astype(np.int64)
     iR = iL + 1
     Te_L = iL * dTe
     ok = iR < value.size - 1
@@ -94,9 +96,9 @@ def func_Te(value, Te, dTe):
 
 
 def func_dTe(value, Te, dTe):
-    """miniFuncs.hpp:53-68 (elementwise)."""
+    """miniFuncs.hpp:53-68 (elementwise); below the table the first interval's slope."""
     value = np.asarray(value)
-    iL = np.trunc(Te / dTe).astype(np.int64)
+    iL = np.maximum(np.trunc(Te / dTe), 0).astype(np.int64)
     iR = iL + 1
     hi = iR >= value.size - 1
     iL = np.where(hi, value.size - 2, iL)
@@ -105,9 +107,9 @@ def func_dTe(value, Te, dTe):
 
 
 def func_Ei(value, Ei, dEi, massi):
-    """miniFuncs.hpp:75-91 (elementwise)."""
+    """miniFuncs.hpp:75-91 (elementwise); below the table the first interval extrapolated."""
     value = np.asarray(value)
-    iL = np.trunc(Ei / dEi).astype(np.int64)
+    iL = np.maximum(np.trunc(Ei / dEi), 0).astype(np.int64)
     iR = iL + 1
     Ei_L = iL * dEi
     ok = iR < value.size - 1

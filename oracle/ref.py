@@ -87,7 +87,8 @@ def lib(dropin: bool = False) -> ctypes.CDLL:
         L.ref_captured_plane.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int]
         L.ref_captured_blocks.argtypes = [ctypes.c_int, _ip, _ip, ctypes.c_int]
         L.ref_dropin_precision.argtypes = [ctypes.c_int]
-        L.ref_dropin_stats.argtypes = [ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long), _dp]
+        L.ref_dropin_stats.argtypes = [ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long),
+                                       ctypes.POINTER(ctypes.c_double)]
         L.ref_output.argtypes = [_vp, _cs]
         L.ref_set_cfield.argtypes = [_vp, _cs, _dp]
         L.ref_get_cfield.argtypes = [_vp, _cs, _dp]
@@ -286,10 +287,10 @@ def captured_planes(ni: int, nj: int) -> list:
 def dropin_stats() -> dict:
     """The GPU drop-in's solve counts since the last call: calls, not_converged (maxITR
     reached above the tolerance), worst (largest final relative residual of those)."""
-    c, n, w = ctypes.c_long(), ctypes.c_long(), np.zeros(1)
-    if lib(True).ref_dropin_stats(ctypes.byref(c), ctypes.byref(n), w) != 0:
+    c, n, w = ctypes.c_long(), ctypes.c_long(), ctypes.c_double()
+    if lib(True).ref_dropin_stats(ctypes.byref(c), ctypes.byref(n), ctypes.byref(w)) != 0:
         raise RuntimeError("not the drop-in build")
-    return dict(calls=c.value, not_converged=n.value, worst=float(w[0]))
+    return dict(calls=c.value, not_converged=n.value, worst=w.value)
 
 
 def dropin_precision(p: int) -> None:

@@ -34,3 +34,28 @@ def test_autotune_keeps_solves_converged(pkg, cuda_device):
     wall, rc, _ = B.batch_steps(cases, steps=2, nthreads=3)
     assert rc == [0, 0, 0]
     B.close(cases)
+
+
+def test_batched_microwave_updates_follow_each_instance_power(pkg, cuda_device):
+    """Instances with the loop's microwave update (here every 3 steps): the
+    batched run equals the sequential one bit for bit, each instance ran its
+    updates, and its absorbed power was rescaled to its own Pmw (the store's
+    Pabs integrates to Pmw after the update, as the port part reports)."""
+    B = pkg.batch
+    specs = B.instance_specs(4, seed=7, sizes=((32, 64), (64, 128)))
+    a = B.make_instances(pkg, specs, microwave=True, ndiv_mw=3)
+    b = B.make_instances(pkg, specs, microwave=True, ndiv_mw=3)
+    wall, rc, _ = B.batch_steps(a, steps=6, nthreads=2)
+    assert rc == [0] * 4
+    B.sequential_steps(b, steps=6)
+    for ca, cb in zip(a, b):
+        assert ca["mw_stats"]["runs"] == 2
+        for k in FIELDS + ("Pabs",):
+            assert np.array_equal(ca["fs"].download(k), cb["fs"].download(k)), k
+        # one more update on the batched instance: its power after the rescale is the instance's Pmw
+        out = ca["mwu"].run(ca["gx"], ca["gr"])
+        assert out["rc"] == 0 and out["solve"]["converged"] == 1
+        assert out["power_sum"] * out["ratio"] == pytest.approx(ca["Pmw"], rel=1e-9)
+    assert len({round(c["Pmw"], 6) for c in a}) == 4
+    B.close(a)
+    B.close(b)
