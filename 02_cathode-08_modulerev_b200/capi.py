@@ -32,7 +32,7 @@ EXPORTS = (
     "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs", "cth_grid_set_tail", "cth_grid_time_relax",
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_mw3_create", "cth_mw3_destroy", "cth_mw3_ld", "cth_mw3_launch_count", "cth_mw3_assemble_dev",
-    "cth_mw3_copy_planes", "cth_mw3_apply_dev", "cth_mw3_solve_dev", "cth_mw3_set_graphs",
+    "cth_mw3_copy_planes", "cth_mw3_apply_dev", "cth_mw3_solve_dev", "cth_mw3_solve_guess_dev", "cth_mw3_set_graphs",
     "cth_mw3_create_blocks", "cth_mw3_set_boundary", "cth_mw3_assemble_explicit_dev", "cth_mw3_fill_ghosts", "cth_mw3_set_cycle", "cth_mw3_set_preconditioner", "cth_mw3_set_precision",
     "cth_fields_create", "cth_fields_destroy", "cth_fields_set_warm_start", "cth_fields_set_download_plan", "cth_fields_download_wait", "cth_fields_set_upload_plan", "cth_fields_upload_many",
     "cth_fields_download_many", "cth_field", "cth_field_upload", "cth_field_download",
@@ -44,6 +44,7 @@ EXPORTS = (
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_tensor_cores", "cth_unet_set_smoothing", "cth_unet_set_wait_test", "cth_unet_set_grid_limit", "cth_unet_check", "cth_unet_set_params", "cth_unet_get_params",
     "cth_unet_get_grads", "cth_unet_set_loss_weights", "cth_unet_forward", "cth_unet_backward",
     "cth_unet_train_step", "cth_unet_set_stats", "cth_unet_features", "cth_unet_predict_dphi",
+    "cth_unet_mw_features", "cth_unet_mw_guess", "cth_mw_update_set_net",
 )
 
 CTH_PROF_RELAX0 = 0
@@ -211,7 +212,7 @@ class BatchItem(ctypes.Structure):
 class MWUpdateParams(ctypes.Structure):
     """cth_mw_update_params: the microwave update of the time loop."""
     _fields_ = [("mw", MWParams), ("port", MWPortParams), ("ndiv_mw", ctypes.c_int), ("maxit", ctypes.c_int),
-                ("tol", ctypes.c_double)]
+                ("tol", ctypes.c_double), ("warm_start", ctypes.c_int)]
 
 
 class MWUpdateResult(ctypes.Structure):
@@ -279,6 +280,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_mw3_apply_dev.restype = ctypes.c_int
     L.cth_mw3_solve_dev.argtypes = [_vp, ctypes.c_int, ctypes.c_double, _vp, _vp, ctypes.POINTER(Status)]
     L.cth_mw3_solve_dev.restype = ctypes.c_int
+    L.cth_mw3_solve_guess_dev.argtypes = [_vp, ctypes.c_int, ctypes.c_double, _vp, _vp, ctypes.c_double, _vp,
+                                          ctypes.POINTER(Status)]
+    L.cth_mw3_solve_guess_dev.restype = ctypes.c_int
     L.cth_mw3_set_graphs.argtypes = [_vp, ctypes.c_int]
     L.cth_mw3_set_graphs.restype = ctypes.c_int
     L.cth_mw3_create_blocks.argtypes = [ctypes.c_int, ctypes.c_int] + [_vp, _vp, ctypes.c_int] * 3 + \
@@ -443,6 +447,12 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_unet_features.restype = ctypes.c_int
     L.cth_unet_predict_dphi.argtypes = [_vp, _vp, _vp]
     L.cth_unet_predict_dphi.restype = ctypes.c_int
+    L.cth_unet_mw_features.argtypes = [_vp, _vp, _vp, ctypes.c_double, _vp, _vp]
+    L.cth_unet_mw_features.restype = ctypes.c_int
+    L.cth_unet_mw_guess.argtypes = [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp, _vp]
+    L.cth_unet_mw_guess.restype = ctypes.c_int
+    L.cth_mw_update_set_net.argtypes = [_vp, _vp]
+    L.cth_mw_update_set_net.restype = ctypes.c_int
     L.cth_sor_solve.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_double, ctypes.c_int, ctypes.c_double, _vp,
                                                     ctypes.POINTER(Status)]
     L.cth_sor_solve.restype = ctypes.c_int

@@ -193,6 +193,7 @@ struct cth_grid {
     bool use_graphs = true;
     bool pdl = true;  // relaxations launched with programmatic dependent launch
     bool tail = false; // coarse levels of at most 16 rows run as one cluster launch (off: measured slower)
+    int bnd = 256;       // launch bounds of the line kernels: 256, 512 or 1024 (>= bd)
     int tail_types = 0;  // bit per precision (float, double, complex) whose tail kernel fits
     cudaStream_t pending_stream = nullptr;  // stream of the last enqueued graph solve
 };

@@ -66,7 +66,9 @@ enum Slot3 { QP = 0, QE, QW, QN, QS, C0, C1, C2, C3, C4, C5, NQ };
 // scalar words of the recurrence
 enum Word3 {
     RHO = 0, RHO_OLD = 2, ALPHA = 4, OMEGA = 6, BETA = 8,
-    BB = 10, RR = 11, RELRES = 12, ITER = 13, CONV = 14, BAD = 15, KEEP = 16, NWORDS = 24
+    BB = 10, RR = 11, RELRES = 12, ITER = 13, CONV = 14, BAD = 15, KEEP = 16,
+    GUESS = 17,   // 0 no guess; 1 + r0: started from the guess; -(1 + r0): guess rejected (r0 its relative residual)
+    NWORDS = 24
 };
 
 struct Lev0 {
@@ -80,6 +82,8 @@ struct Args3 {
     int maxit;
     double tol;
     cd* out;  // three field planes
+    const cd* x0;      // initial guess (three field planes, read on the unknowns) or null: zero start
+    double guess_tol;  // the guess is used when ||b - A x0|| <= guess_tol ||b||
 };
 
 struct Dev3 {
@@ -540,39 +544,91 @@ __global__ void k_m3_block(Dev3 D, int c, cd* __restrict__ a0, int i0, int j0, i
     a0[N * n0 + p] = vN;
 }
 
-// r = rh = b, x = p = v = 0 on the unknowns; ||b||^2 and the recurrence's start
+// x = the caller's guess on the unknowns (zero without one; zero off the unknowns,
+// so that the coupled apply needs no neighbour tests)
+__global__ void k_m3_x0(Dev3 D, const Args3* __restrict__ args) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    if (i > D.ni) return;
+    const cd* __restrict__ x0 = args->x0;
+    for (int c = 0; c < 3; c++) {
+        const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+        if (!D.mk[c][q - (size_t)c * D.pl]) continue;
+        D.x[q] = x0 ? x0[q] : cd();
+    }
+}
+
+// r = b - A x of the guess, its norm and ||b||; the last block decides (sc[GUESS])
+__global__ void k_m3_guess(Dev3 D, const Args3* __restrict__ args, double* __restrict__ part,
+                           unsigned int* counter) {
+    __shared__ double red[32];
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    double acc[2] = {0.0, 0.0};
+    if (i <= D.ni && args->x0) {
+        for (int c = 0; c < 3; c++) {
+            const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
+            if (!D.mk[c][q - (size_t)c * D.pl]) continue;
+            const cd r = D.b[q] - apply3(D, D.x, c, i, j);
+            D.r[q] = r;
+            acc[0] += abs2(r);
+            acc[1] += abs2(D.b[q]);
+        }
+    }
+    double tot[2];
+    if (last_block_sumk<2>(acc, part, counter, red, tot) && threadIdx.x == 0) {
+        if (!args->x0) {
+            D.sc[GUESS] = 0.0;
+        } else {
+            const double r0 = tot[1] > 0.0 ? sqrt(tot[0] / tot[1]) : INFINITY;
+            const bool use = isfinite(r0) && r0 <= args->guess_tol;
+            D.sc[GUESS] = use ? 1.0 + r0 : -(1.0 + (isfinite(r0) ? fmin(r0, 1e30) : 1e30));
+        }
+    }
+}
+
+// from the guess (sc[GUESS] >= 1): r = rh = b - A x0, x = x0; otherwise r = rh = b,
+// x = 0.  p = v = 0 on the unknowns; ||b||^2, ||r||^2 and the recurrence's start
 __global__ void k_m3_prep(Dev3 D, const Args3* __restrict__ args, double* __restrict__ part, unsigned int* counter,
                           cudaGraphConditionalHandle cond, int use_cond) {
     __shared__ double red[32];
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y;
-    double bb = 0.0;
+    const bool guess = D.sc[GUESS] >= 1.0;
+    double acc[2] = {0.0, 0.0};  // ||b||^2, ||r||^2
     if (i <= D.ni) {
         for (int c = 0; c < 3; c++) {
             const size_t q = (size_t)c * D.pl + (size_t)j * D.ld + i;
             if (!D.mk[c][q - (size_t)c * D.pl]) continue;
             const cd b = D.b[q];
-            D.r[q] = b; D.rh[q] = b;
-            D.x[q] = cd(); D.p[q] = cd(); D.v[q] = cd();
-            bb += abs2(b);
+            const cd r = guess ? D.r[q] : b;
+            D.r[q] = r; D.rh[q] = r;
+            if (!guess) D.x[q] = cd();
+            D.p[q] = cd(); D.v[q] = cd();
+            acc[0] += abs2(b);
+            acc[1] += abs2(r);
         }
     }
-    double tot;
-    if (last_block_sum(bb, part, counter, red, &tot) && threadIdx.x == 0) {
+    double tot[2];
+    if (last_block_sumk<2>(acc, part, counter, red, tot) && threadIdx.x == 0) {
         double* sc = D.sc;
-        const bool fin = isfinite(tot);
-        sc_set(sc, RHO, cd(tot));
+        const double bb = tot[0], rr = tot[1];
+        const bool fin = isfinite(bb) && isfinite(rr);
+        const double rel = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+        sc_set(sc, RHO, cd(rr));
         sc_set(sc, RHO_OLD, cd(1.0));
         sc_set(sc, ALPHA, cd(1.0));
         sc_set(sc, OMEGA, cd(1.0));
         sc_set(sc, BETA, cd(0.0));
-        sc[BB] = tot;
-        sc[RR] = tot;
-        sc[RELRES] = tot > 0.0 ? 1.0 : 0.0;
+        sc[BB] = bb;
+        sc[RR] = rr;
+        sc[RELRES] = bb > 0.0 ? rel : 0.0;
         sc[ITER] = 0.0;
-        sc[CONV] = (fin && tot == 0.0) ? 1.0 : 0.0;
+        // from zero: at least one iteration unless b = 0; from a guess: stop at once when it meets the tolerance
+        const bool met = rr == 0.0 || (guess && rel < args->tol);
+        sc[CONV] = (fin && met) ? 1.0 : 0.0;
         sc[BAD] = fin ? 0.0 : 1.0;
-        const bool keep = fin && tot > 0.0 && args->maxit > 0;
+        const bool keep = fin && !met && args->maxit > 0;
         sc[KEEP] = keep ? 1.0 : 0.0;
         if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
     }
@@ -919,8 +975,10 @@ cudaError_t solve_pre(cth_mw3* m, cudaStream_t s, cudaGraphConditionalHandle con
     e = join3(m, 0, s);
     if (e != cudaSuccess) return e;
     dim3 blk(128), grd((m->ni + 127) / 128, m->nj);
+    k_m3_x0<<<grd, blk, 0, s>>>(D, m->d_args);
+    k_m3_guess<<<grd, blk, 0, s>>>(D, m->d_args, m->part, m->counter);
     k_m3_prep<<<grd, blk, 0, s>>>(D, m->d_args, m->part, m->counter, cond, use_cond);
-    *n += 1;
+    *n += 3;
     return cudaGetLastError();
 }
 
@@ -1439,8 +1497,9 @@ int cth_mw3_fill_ghosts(cth_mw3* m, double* E3, const double* epsr, const double
     return CTH_OK;
 }
 
-int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* stream, cth_status* st) {
-    if (!m || !E3 || maxit < 0 || !(tol > 0.0) || !m->assembled) {
+int cth_mw3_solve_guess_dev(cth_mw3* m, int maxit, double tol, double* E3, const double* x0, double guess_tol,
+                            void* stream, cth_status* st) {
+    if (!m || !E3 || maxit < 0 || !(tol > 0.0) || !m->assembled || (x0 && !(guess_tol >= 0.0))) {
         set_error("cth_mw3_solve_dev: invalid arguments or system not assembled");
         return CTH_ERR_ARG;
     }
@@ -1449,6 +1508,8 @@ int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* strea
     m->h_args->maxit = maxit;
     m->h_args->tol = tol;
     m->h_args->out = reinterpret_cast<cd*>(E3);
+    m->h_args->x0 = reinterpret_cast<const cd*>(x0);
+    m->h_args->guess_tol = guess_tol;
     CTH_CUDA(cudaMemcpyAsync(m->d_args, m->h_args, sizeof(Args3), cudaMemcpyHostToDevice, s));
     if (m->use_graphs) {
         int rc = build_graph(m);
@@ -1480,10 +1541,15 @@ int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* strea
     loc.initial_residual = std::sqrt(h[BB]);
     loc.converged = h[CONV] != 0.0;
     loc.nonfinite = h[BAD] != 0.0 && !loc.converged;
-    loc.guess_residual = -1.0;
+    loc.guess = h[GUESS] >= 1.0 ? 1 : (h[GUESS] <= -1.0 ? -1 : 0);
+    loc.guess_residual = loc.guess == 0 ? -1.0 : std::fabs(h[GUESS]) - 1.0;
     if (st) *st = loc;
     if (loc.nonfinite) return CTH_NONFINITE;
     return loc.converged ? CTH_OK : CTH_NOT_CONVERGED;
+}
+
+int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* stream, cth_status* st) {
+    return cth_mw3_solve_guess_dev(m, maxit, tol, E3, nullptr, 0.0, stream, st);
 }
 
 }  // extern "C"

@@ -9,6 +9,7 @@
 // own), which persist between updates as the reference's fields do.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <new>
 
@@ -17,19 +18,30 @@
 struct cth_mw_update {
     cth_fields* fs = nullptr;
     cth_mw3* m = nullptr;
-    int device = 0, ndiv = 100, maxit = 400;
+    int device = 0, ndiv = 100, maxit = 400, warm = 0, runs = 0;
     double tol = 1e-10;
     cth_mw_params mw{};
     cth_energy_params ep{};
     cth_mw_port_params port{};
-    double J1r_exc = 0.0;
+    double J1r_exc = 0.0;      // the excitation of the next solve
+    double J_solved = 0.0;     // the excitation the fields in E3 were solved with
     size_t pl = 0;         // complex entries of one plane
     double* E3 = nullptr;  // 3 complex planes (E1x, E1r, E1p)
     double* J3 = nullptr;  // 3 complex planes (J1x, J1r, J1p)
     bool own_E = false, own_J = false;
+    cth_unet* net = nullptr;   // learned guess (9 input, 6 output channels) or none
+    double* G3 = nullptr;      // 3 complex planes: the network's guess
 };
 
 using cth::set_error;
+
+namespace {
+// dst = ratio * src over n complex entries (the previous fields scaled to the new excitation)
+__global__ void k_scale_planes(const double* __restrict__ src, double ratio, double* __restrict__ dst, size_t n) {
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < 2 * n; k += (size_t)gridDim.x * blockDim.x)
+        dst[k] = ratio * src[k];
+}
+}  // namespace
 
 extern "C" int cth_mw_update_create(cth_fields* fs, cth_mw3* m, const cth_mw_update_params* p, double* E3,
                                     double* J3, cth_mw_update** out) {
@@ -54,6 +66,7 @@ extern "C" int cth_mw_update_create(cth_fields* fs, cth_mw3* m, const cth_mw_upd
     u->ndiv = p->ndiv_mw;
     u->maxit = p->maxit;
     u->tol = p->tol;
+    u->warm = p->warm_start;
     u->mw = p->mw;
     u->port = p->port;
     u->ep = cth_energy_params{p->mw.dx, p->mw.dr, p->mw.rmin, p->mw.omegam, p->mw.masse};
@@ -86,7 +99,17 @@ extern "C" void cth_mw_update_destroy(cth_mw_update* u) {
     cudaSetDevice(u->device);
     if (u->own_E && u->E3) cudaFree(u->E3);
     if (u->own_J && u->J3) cudaFree(u->J3);
+    if (u->G3) cudaFree(u->G3);
     delete u;
+}
+
+extern "C" int cth_mw_update_set_net(cth_mw_update* u, cth_unet* net) {
+    if (!u) {
+        set_error("cth_mw_update_set_net: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    u->net = net;
+    return CTH_OK;
 }
 
 extern "C" int cth_mw_update_due(const cth_mw_update* u, int itime) {
@@ -144,8 +167,30 @@ extern "C" int cth_mw_update_run(cth_mw_update* u, cth_grid* gx, cth_grid* gr, v
     int rc = cth_mw3_assemble_dev(u->m, ne, nu, Bx, Br, epsr, &prm, stream);
     if (rc < 0) return rc;
     cth_status st{};
-    const int rs = cth_mw3_solve_dev(u->m, u->maxit, u->tol, u->E3, stream, &st);
+    // the start: the network's guess (the previous fields plus its predicted change),
+    // else the previous fields, else zero; a guess is taken only when its residual
+    // is at most ||b|| (decided on the device)
+    const double* x0 = nullptr;
+    if (u->runs > 0 && (u->net || u->warm) && u->J_solved != 0.0) {
+        if (!u->G3) {
+            CTH_CUDA(cudaMalloc(&u->G3, 3 * u->pl * 2 * sizeof(double)));
+            CTH_CUDA(cth::zero_fill(u->G3, 3 * u->pl * 2 * sizeof(double)));
+        }
+        if (u->net) {
+            rc = cth_unet_mw_guess(u->net, fs, u->E3, u->J_solved, prm.J1r_exc, u->G3, stream);
+            if (rc < 0) return rc;
+        } else {
+            const size_t n = 3 * u->pl;
+            k_scale_planes<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0,
+                             static_cast<cudaStream_t>(stream)>>>(u->E3, prm.J1r_exc / u->J_solved, u->G3, n);
+            CTH_CUDA(cudaGetLastError());
+        }
+        x0 = u->G3;
+    }
+    const int rs = cth_mw3_solve_guess_dev(u->m, u->maxit, u->tol, u->E3, x0, 1.0, stream, &st);
     if (rs < 0) return rs;
+    u->runs++;
+    u->J_solved = prm.J1r_exc;
     rc = cth_mw3_fill_ghosts(u->m, u->E3, epsr, Er, &prm, stream);
     if (rc < 0) return rc;
     cth_energy_result er{};

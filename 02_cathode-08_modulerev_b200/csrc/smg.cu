@@ -182,8 +182,13 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
 // interpolation weights of the F rows (odd rows) of one level: two line solves
 // per F row, right-hand sides = lumped couplings toward the C rows.
 // ---------------------------------------------------------------------------
-template <typename T, int NPT>
-__global__ void k_weights(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ wS,
+// The line kernels run one CTA of bd threads per z-line (4 cells per thread).
+// BND is their __launch_bounds__: 256 for lines of up to 1024 cells (registers
+// unconstrained), 512 and 1024 for the longer lines, where the register budget
+// of a CTA of bd threads caps the registers per thread (the FP64 and complex
+// relaxations then spill; without the cap they could not launch at all).
+template <typename T, int NPT, int BND = 256>
+__global__ void __launch_bounds__(BND) k_weights(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ wS,
                           T* __restrict__ wN) {
     const int j = 2 * blockIdx.x + 1;
     if (j >= L.nrow) return;
@@ -300,8 +305,8 @@ __device__ __forceinline__ void factor_row(const LevelArgs<T>& L, const unsigned
     }
 }
 
-template <typename T, int NPT>
-__global__ void k_factor(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ fac,
+template <typename T, int NPT, int BND = 256>
+__global__ void __launch_bounds__(BND) k_factor(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ fac,
                          T* __restrict__ wS, T* __restrict__ wN, int weights) {
     __shared__ T sh[(8 + LG_N) * 32];
     factor_row<T, NPT>(L, mask, fac, wS, wN, weights, blockIdx.x, sh);
@@ -411,24 +416,6 @@ __global__ void k_galerkin(LevelArgs<T> F, const unsigned char* __restrict__ mas
     galerkin_cell<T, NPT>(F, maskf, wS, wN, ac, nrowc, maskc, i, blockIdx.y);
 }
 
-// Galerkin operator of coarse row J = blockIdx.x and, in the same CTA, that row's
-// line factorisation (and its interpolation weights when it is an F row of a
-// non-coarsest level): one launch per level of the set-up instead of two.  Each
-// thread computes the cells CH*threadIdx.x .. +CH-1 of the row, which are the
-// cells it reads back in the factorisation (its own writes), so no barrier is
-// needed between the two parts.  Same arithmetic as k_galerkin + k_factor.
-template <typename T, int NPTF>
-__global__ void k_galfac(LevelArgs<T> F, const unsigned char* __restrict__ maskf, const T* __restrict__ wSf,
-                         const T* __restrict__ wNf, LevelArgs<T> C, const unsigned char* __restrict__ maskc,
-                         T* __restrict__ facc, T* __restrict__ wSc, T* __restrict__ wNc, int weights) {
-    __shared__ T sh[(8 + LG_N) * 32];
-    const int J = blockIdx.x;
-    const int s0 = CH * threadIdx.x;
-#pragma unroll 1
-    for (int k = 0; k < CH; k++)
-        if (s0 + k < F.ncol) galerkin_cell<T, NPTF>(F, maskf, wSf, wNf, const_cast<T*>(C.a), C.nrow, maskc, s0 + k, J);
-    factor_row<T, 9>(C, maskc, facc, wSc, wNc, weights, J, sh);
-}
 
 // ---------------------------------------------------------------------------
 // zebra z-line relaxation: one CTA per row of the given parity.
@@ -704,8 +691,8 @@ __device__ __forceinline__ void relax_line(const LevelArgs<T>& L, int j, int zer
     if (cnt > 0) st4(L.x + p, x[0]);
 }
 
-template <typename T, int NPT, int NPTF>
-__global__ void k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong, ProlongArgs<T> pa,
+template <typename T, int NPT, int NPTF, int BND = 256>
+__global__ void __launch_bounds__(BND) k_relax(LevelArgs<T> L, int parity, int zero_guess, int prolong, ProlongArgs<T> pa,
                         LevelArgs<T> F) {
     const int j = 2 * blockIdx.x + parity;
     if (j >= L.nrow) return;
@@ -957,6 +944,9 @@ static void launch_relax(cth_grid* g, int l, int parity, int zero_guess, int pro
         slot = prof_mark(g, PROF_RESTRICT0, (double)g->nrow[1] * g->ncol * (9.0 + 8.0) * sizeof(T), s);
     else  // coarse levels: NPT coefficients + b + x in + x out per cell of the colour
         slot = prof_mark(g, PROF_RELAXC, (double)rows * g->ncol * (NPT + 3.0) * sizeof(T), s);
+    auto kern = g->bnd == 1024 ? k_relax<T, NPT, NPTF, 1024>
+              : g->bnd == 512  ? k_relax<T, NPT, NPTF, 512>
+                               : k_relax<T, NPT, NPTF, 256>;
     if (g->pdl) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(rows);
@@ -968,9 +958,9 @@ static void launch_relax(cth_grid* g, int l, int parity, int zero_guess, int pro
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, k_relax<T, NPT, NPTF>, L, parity, zero_guess, prolong, pa, F);
+        cudaLaunchKernelEx(&cfg, kern, L, parity, zero_guess, prolong, pa, F);
     } else {
-        k_relax<T, NPT, NPTF><<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa, F);
+        kern<<<rows, g->bd, smem, s>>>(L, parity, zero_guess, prolong, pa, F);
     }
     g->launches++;
     if (slot >= 0) prof_done(g, slot, s);
@@ -1064,23 +1054,23 @@ static void setup_levels(cth_grid* g, cudaStream_t s) {
     if constexpr (kFac<T>) {
         // per level: factorise every line (and the F-row weights), then the
         // Galerkin operator of the next level
-        // level 0: factors (+ F-row weights); then per level one launch that forms
-        // the next level's Galerkin operator row by row and factorises each row
-        {
-            LevelArgs<T> L = level_args<T>(g, 0);
-            k_factor<T, 5><<<g->nrow[0], g->bd, 0, s>>>(L, g->mask[0], h.fac[0], h.wS[0], h.wN[0], g->nlev > 1);
-            g->launches++;
-        }
-        for (int l = 0; l + 1 < g->nlev; l++) {
+        for (int l = 0; l < g->nlev; l++) {
             LevelArgs<T> L = level_args<T>(g, l);
-            LevelArgs<T> Lc = level_args<T>(g, l + 1);
-            const int wts = l + 2 < g->nlev;
+            const int wts = l + 1 < g->nlev;
+            auto kf = l == 0 ? (g->bnd == 1024 ? k_factor<T, 5, 1024> : g->bnd == 512 ? k_factor<T, 5, 512>
+                                                                                      : k_factor<T, 5, 256>)
+                             : (g->bnd == 1024 ? k_factor<T, 9, 1024> : g->bnd == 512 ? k_factor<T, 9, 512>
+                                                                                      : k_factor<T, 9, 256>);
+            kf<<<g->nrow[l], g->bd, 0, s>>>(L, g->mask[l], h.fac[l], h.wS[l], h.wN[l], wts);
+            g->launches++;
+            if (!wts) break;
+            dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
             if (l == 0)
-                k_galfac<T, 5><<<g->nrow[1], g->bd, 0, s>>>(L, g->mask[0], h.wS[0], h.wN[0], Lc, g->mask[1],
-                                                            h.fac[1], h.wS[1], h.wN[1], wts);
+                k_galerkin<T, 5><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
+                                                     g->nrow[l + 1], g->mask[l + 1]);
             else
-                k_galfac<T, 9><<<g->nrow[l + 1], g->bd, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], Lc, g->mask[l + 1],
-                                                                h.fac[l + 1], h.wS[l + 1], h.wN[l + 1], wts);
+                k_galerkin<T, 9><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
+                                                     g->nrow[l + 1], g->mask[l + 1]);
             g->launches++;
         }
     } else {
@@ -1089,8 +1079,11 @@ static void setup_levels(cth_grid* g, cudaStream_t s) {
             const int frows = g->nrow[l] / 2;
             const size_t smem = line_smem<T>(g->bd, 2);
             if (frows > 0) {
-                if (l == 0) k_weights<T, 5><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
-                else k_weights<T, 9><<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
+                auto kw = l == 0 ? (g->bnd == 1024 ? k_weights<T, 5, 1024> : g->bnd == 512 ? k_weights<T, 5, 512>
+                                                                                          : k_weights<T, 5, 256>)
+                                 : (g->bnd == 1024 ? k_weights<T, 9, 1024> : g->bnd == 512 ? k_weights<T, 9, 512>
+                                                                                          : k_weights<T, 9, 256>);
+                kw<<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
                 g->launches++;
             }
             dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
@@ -1473,6 +1466,26 @@ int time_relax(cth_grid* g, int precision, int level, int reps, double* us, doub
     return CTH_ERR_ARG;
 }
 
+template <typename T, int B>
+static cudaError_t line_smem_attr_b(int bytes) {
+    const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e = cudaFuncSetAttribute(k_relax<T, 5, 0, B>, A, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_relax<T, 9, 0, B>, A, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_relax<T, 9, 5, B>, A, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_relax<T, 9, 9, B>, A, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_weights<T, 5, B>, A, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_weights<T, 9, B>, A, bytes);
+    return e;
+}
+
+// the dynamic shared memory limit of the line kernels of type T at launch bound bnd
+template <typename T>
+static cudaError_t line_smem_attr(int bnd, int bytes) {
+    return bnd == 1024 ? line_smem_attr_b<T, 1024>(bytes)
+         : bnd == 512  ? line_smem_attr_b<T, 512>(bytes)
+                       : line_smem_attr_b<T, 256>(bytes);
+}
+
 // dynamic shared memory limits for the line kernels (called once per grid)
 int configure_kernels(cth_grid* g) {
     const int smem64 = (int)line_smem<double>(g->bd, 2);
@@ -1482,32 +1495,18 @@ int configure_kernels(cth_grid* g) {
         return CTH_ERR_UNSUPPORTED;
     }
 #define CTH_ATTR(K, BYTES) CTH_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, BYTES))
-    if (smem64 > 48 * 1024) {
-        CTH_ATTR((k_relax<double, 5, 0>), smem64); CTH_ATTR((k_relax<double, 9, 0>), smem64);
-        CTH_ATTR((k_relax<double, 9, 5>), smem64); CTH_ATTR((k_relax<double, 9, 9>), smem64);
-        CTH_ATTR((k_weights<double, 5>), smem64); CTH_ATTR((k_weights<double, 9>), smem64);
-    }
+    // launch bounds of the line kernels for this line's thread count
+    g->bnd = g->bd <= 256 ? 256 : (g->bd <= 512 ? 512 : 1024);
+    if (smem64 > 48 * 1024) CTH_CUDA(line_smem_attr<double>(g->bnd, smem64));
     const int smemc = (int)line_smem<cd>(g->bd, 2);
     if (smemc > 227 * 1024) {
         set_error("z-line too long for the shared-memory complex line solver");
         return CTH_ERR_UNSUPPORTED;
     }
-    if (smemc > 48 * 1024) {
-        CTH_ATTR((k_relax<cd, 5, 0>), smemc); CTH_ATTR((k_relax<cd, 9, 0>), smemc);
-        CTH_ATTR((k_relax<cd, 9, 5>), smemc); CTH_ATTR((k_relax<cd, 9, 9>), smemc);
-        CTH_ATTR((k_weights<cd, 5>), smemc); CTH_ATTR((k_weights<cd, 9>), smemc);
-    }
+    if (smemc > 48 * 1024) CTH_CUDA(line_smem_attr<cd>(g->bnd, smemc));
     const int smemcf = (int)line_smem<cf>(g->bd, 2);
-    if (smemcf > 48 * 1024) {
-        CTH_ATTR((k_relax<cf, 5, 0>), smemcf); CTH_ATTR((k_relax<cf, 9, 0>), smemcf);
-        CTH_ATTR((k_relax<cf, 9, 5>), smemcf); CTH_ATTR((k_relax<cf, 9, 9>), smemcf);
-        CTH_ATTR((k_weights<cf, 5>), smemcf); CTH_ATTR((k_weights<cf, 9>), smemcf);
-    }
-    if (smem32 > 48 * 1024) {
-        CTH_ATTR((k_relax<float, 5, 0>), smem32); CTH_ATTR((k_relax<float, 9, 0>), smem32);
-        CTH_ATTR((k_relax<float, 9, 5>), smem32); CTH_ATTR((k_relax<float, 9, 9>), smem32);
-        CTH_ATTR((k_weights<float, 5>), smem32); CTH_ATTR((k_weights<float, 9>), smem32);
-    }
+    if (smemcf > 48 * 1024) CTH_CUDA(line_smem_attr<cf>(g->bnd, smemcf));
+    if (smem32 > 48 * 1024) CTH_CUDA(line_smem_attr<float>(g->bnd, smem32));
     // the fused tail runs only where a CTA of the line's width fits the registers
     g->tail_types = 0;
     cudaFuncAttributes fa;

@@ -560,9 +560,9 @@ __global__ void k_adam(float* __restrict__ prm, const float* __restrict__ g, flo
     }
 }
 
-// normalisation of the network's input and output channels
+// normalisation of the network's input and output channels (up to 32 each)
 struct Stats {
-    float in_mean[6], in_std[6], out_mean[3], out_std[3];
+    float in_mean[32], in_std[32], out_mean[32], out_std[32];
 };
 
 // input channels of the warm-start network from the field planes (library
@@ -591,6 +591,61 @@ __global__ void k_features(const double* __restrict__ rhoe, const double* __rest
         }
 #pragma unroll
         for (int c = 0; c < 6; c++) out[(size_t)q * 6 + c] = f[c];
+    }
+}
+
+// input channels of the microwave warm-start network: log10 n_e, log10 nu_m1, |B|
+// and the real and imaginary parts of the previous microwave fields Ex, Er, Ephi
+// per unit excitation current (interleaved complex planes times escale, plane
+// stride pl), grid cell (i, j) -> pixel (j-1, i-1); normalised, zero outside
+__global__ void k_mw_features(const double* __restrict__ rhoe, const double* __restrict__ nu_m1,
+                              const double* __restrict__ Bx, const double* __restrict__ Br,
+                              const double* __restrict__ E3, double escale, size_t pl, int ni, int nj, int ld,
+                              int H, int W, Stats st, float* __restrict__ out) {
+    const int npix = H * W;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npix; q += gridDim.x * blockDim.x) {
+        const int y = q / W, x = q % W;
+        float f[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (y < nj && x < ni) {
+            const size_t p = (size_t)(y + 1) * ld + (x + 1);
+            f[0] = (float)log10(fmax(rhoe[p], 1.0));
+            f[1] = (float)log10(fmax(nu_m1[p], 1.0));
+            f[2] = (float)sqrt(Bx[p] * Bx[p] + Br[p] * Br[p]);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                f[3 + 2 * c] = (float)(E3[2 * (c * pl + p)] * escale);
+                f[4 + 2 * c] = (float)(E3[2 * (c * pl + p) + 1] * escale);
+            }
+#pragma unroll
+            for (int c = 0; c < 9; c++) f[c] = (f[c] - st.in_mean[c]) / st.in_std[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 9; c++) out[(size_t)q * 9 + c] = f[c];
+    }
+}
+
+// the microwave guess: E_guess = ratio E_prev + jnow x the network's predicted
+// change of the field per unit excitation (channels 2c, 2c+1 = real, imaginary
+// part of field c, de-normalised) on the grid cells i = 1..ni, j = 1..nj;
+// ratio E_prev elsewhere.  ratio = jnow / jprev: the system is linear in the
+// excitation, so the previous fields scaled to the new excitation are the guess
+// of an unchanged plasma
+__global__ void k_mw_unpack(const float* __restrict__ o, int W, Stats st, const double* __restrict__ Eprev,
+                            double ratio, double jnow, double* __restrict__ Eguess, size_t pl, int ni, int nj,
+                            int ld) {
+    const size_t n = 3 * pl;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(k / pl);
+        const size_t p = k % pl;
+        const int j = (int)(p / ld), i = (int)(p % ld);
+        double re = ratio * Eprev[2 * k], im = ratio * Eprev[2 * k + 1];
+        if (i >= 1 && i <= ni && j >= 1 && j <= nj) {
+            const size_t q = ((size_t)(j - 1) * W + (i - 1)) * 6;
+            re += jnow * (double)(o[q + 2 * c] * st.out_std[2 * c] + st.out_mean[2 * c]);
+            im += jnow * (double)(o[q + 2 * c + 1] * st.out_std[2 * c + 1] + st.out_mean[2 * c + 1]);
+        }
+        Eguess[2 * k] = re;
+        Eguess[2 * k + 1] = im;
     }
 }
 
@@ -984,6 +1039,7 @@ struct cth_unet {
     float* cw = nullptr;     // per-output-channel loss weights
     Stats stats{};
     float* feat = nullptr;   // input features of the warm-start prediction
+    float* feat_mw = nullptr; // input features of the microwave prediction
     float* smooth = nullptr; // ping-pong buffer of the prediction smoother
     int smooth_passes = 0;   // 5-point smoothing passes on the predicted change
     long long launches = 0;  // kernels launched by the forward passes and predictions
@@ -1355,7 +1411,7 @@ void cth_unet_destroy(cth_unet* n) {
     for (void* p : {(void*)n->prm, (void*)n->grad, (void*)n->adam_m, (void*)n->adam_v, (void*)n->wb, (void*)n->wt,
                     (void*)n->wbt, (void*)n->wtt,
                     (void*)n->out, (void*)n->dout, (void*)n->loss, (void*)n->cw, (void*)n->feat, (void*)n->err,
-                    (void*)n->smooth})
+                    (void*)n->smooth, (void*)n->feat_mw})
         if (p) cudaFree(p);
     delete n;
 }
@@ -1503,16 +1559,17 @@ int cth_unet_train_step(cth_unet* n, const float* in, const float* target, const
     return CTH_OK;
 }
 
-// 18 values: input mean[6], input std[6], output mean[3], output std[3]
+// 2 cin + 2 cout values: input mean[cin], input std[cin], output mean[cout], output std[cout]
 int cth_unet_set_stats(cth_unet* n, const float* stats) {
     if (!n || !stats) { set_error("cth_unet_set_stats: invalid arguments"); return CTH_ERR_ARG; }
-    for (int k = 0; k < 6; k++) {
+    const int ci = n->cin, co = n->cout;
+    for (int k = 0; k < ci; k++) {
         n->stats.in_mean[k] = stats[k];
-        n->stats.in_std[k] = stats[6 + k] > 0.f ? stats[6 + k] : 1.f;
+        n->stats.in_std[k] = stats[ci + k] > 0.f ? stats[ci + k] : 1.f;
     }
-    for (int k = 0; k < 3; k++) {
-        n->stats.out_mean[k] = stats[12 + k];
-        n->stats.out_std[k] = stats[15 + k] > 0.f ? stats[15 + k] : 1.f;
+    for (int k = 0; k < co; k++) {
+        n->stats.out_mean[k] = stats[2 * ci + k];
+        n->stats.out_std[k] = stats[2 * ci + co + k] > 0.f ? stats[2 * ci + co + k] : 1.f;
     }
     return CTH_OK;
 }
@@ -1569,6 +1626,56 @@ int cth_unet_predict_dphi(cth_unet* n, cth_fields* fs, void* stream) {
     k_unpack<<<grid1((size_t)ncell), 256, 0, s>>>(o, n->cout, 2, fs->g->ni, fs->g->nj, fs->g->ld, n->W,
                                                    n->stats.out_mean[2], n->stats.out_std[2], prev, dst);
     n->launches += 2;  // features, unpack
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+// the microwave network (9 input, 6 output channels): features from the store and
+// the previous fields E3 (three interleaved complex planes of the store's layout)
+int cth_unet_mw_features(cth_unet* n, cth_fields* fs, const double* E3, double escale, float* out, void* stream) {
+    if (!n || !fs || !E3 || !out || n->cin != 9 || fs->g->ni > n->W || fs->g->nj > n->H) {
+        set_error("cth_unet_mw_features: invalid arguments (9 input channels, grid within the image)");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(n->device));
+    const char* names[4] = {"rhoe", "nu_m1", "Bx", "Br"};
+    const double* q[4];
+    for (int k = 0; k < 4; k++) {
+        q[k] = field_ptr(fs, names[k]);
+        if (!q[k]) { set_error("field allocation failed"); return CTH_ERR_ALLOC; }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t npx = (size_t)n->H * n->W;
+    const size_t pl = (size_t)(fs->g->nj + 2) * fs->g->ld;
+    k_mw_features<<<grid1(npx), 256, 0, s>>>(q[0], q[1], q[2], q[3], E3, escale, pl, fs->g->ni, fs->g->nj,
+                                             fs->g->ld, n->H, n->W, n->stats, out);
+    n->launches++;
+    CTH_CUDA(cudaGetLastError());
+    return CTH_OK;
+}
+
+// the microwave guess: features -> network -> Eguess = Eprev + predicted change
+// (Eguess may not alias Eprev)
+int cth_unet_mw_guess(cth_unet* n, cth_fields* fs, const double* Eprev, double jprev, double jnow, double* Eguess,
+                      void* stream) {
+    if (!n || !fs || !Eprev || !Eguess || Eprev == Eguess || n->cin != 9 || n->cout != 6 || !(jprev != 0.0) ||
+        !std::isfinite(jprev) || !std::isfinite(jnow)) {
+        set_error("cth_unet_mw_guess: invalid arguments (9 input, 6 output channels; distinct planes; finite, "
+                  "nonzero excitations)");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(n->device));
+    const size_t npx = (size_t)n->H * n->W;
+    if (!n->feat_mw) CTH_CUDA(cudaMalloc(&n->feat_mw, npx * 9 * sizeof(float)));
+    int rc = cth_unet_mw_features(n, fs, Eprev, 1.0 / jprev, n->feat_mw, stream);
+    if (rc != CTH_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = forward(n, n->feat_mw, s);
+    if (rc != CTH_OK) return rc;
+    const size_t pl = (size_t)(fs->g->nj + 2) * fs->g->ld;
+    k_mw_unpack<<<grid1(3 * pl), 256, 0, s>>>(n->out, n->W, n->stats, Eprev, jnow / jprev, jnow, Eguess, pl,
+                                              fs->g->ni, fs->g->nj, fs->g->ld);
+    n->launches++;
     CTH_CUDA(cudaGetLastError());
     return CTH_OK;
 }

@@ -28,9 +28,11 @@ class MicrowaveUpdate:
     on a field store -- assembly from rhoe, nu_m1, Bx, Br, epsr_mw, solve, ghost
     pass, update_energy_profile, port / rescale to port["Pmw"] -- every ``ndiv_mw``
     steps.  E3 / J3: (3, nj+2, ld) complex128 device planes (None: the library
-    allocates them)."""
+    allocates them).  warm_start: each solve after the first starts from the
+    previous update's fields when they pass the device-side residual test."""
 
-    def __init__(self, fs, m3, mw_params: dict, port: dict, ndiv_mw=100, maxit=400, tol=1e-10, E3=None, J3=None):
+    def __init__(self, fs, m3, mw_params: dict, port: dict, ndiv_mw=100, maxit=400, tol=1e-10, E3=None, J3=None,
+                 warm_start=False):
         import ctypes
         self._L = capi.load()
         p = capi.MWUpdateParams()
@@ -42,7 +44,7 @@ class MicrowaveUpdate:
                 getattr(p.port, k)[0], getattr(p.port, k)[1] = complex(v).real, complex(v).imag
             else:
                 setattr(p.port, k, v)
-        p.ndiv_mw, p.maxit, p.tol = int(ndiv_mw), int(maxit), float(tol)
+        p.ndiv_mw, p.maxit, p.tol, p.warm_start = int(ndiv_mw), int(maxit), float(tol), int(bool(warm_start))
         self._keep = (E3, J3)
         h = ctypes.c_void_p()
         capi.check(self._L.cth_mw_update_create(fs._h, m3._h, ctypes.byref(p),
@@ -50,6 +52,13 @@ class MicrowaveUpdate:
                                                 J3.data_ptr() if J3 is not None else None, ctypes.byref(h)),
                    allow_positive=False)
         self._h = h
+
+    def set_net(self, net):
+        """A trained microwave network (learned.UNet with 9 input, 6 output
+        channels) whose guess starts each solve after the first; None: none."""
+        capi.check(self._L.cth_mw_update_set_net(self._h, net.handle if net is not None else None),
+                   allow_positive=False)
+        self._net = net
 
     def due(self, itime: int) -> bool:
         return bool(self._L.cth_mw_update_due(self._h, int(itime)))
@@ -93,7 +102,7 @@ class RectangleDischarge:
     maxit override the inner solves' stopping rule when given."""
 
     def __init__(self, pkg, ni, nj, seed=0, device=0, precision=capi.CTH_PREC_MIXED, tol=None, maxit=None,
-                 ndiv_mw=100, Pmw=8.0, mw_tol=1e-10, mw_maxit=400):
+                 ndiv_mw=100, Pmw=8.0, mw_tol=1e-10, mw_maxit=400, V_bias=None):
         self.ni, self.nj, self.ndiv_mw, self.mw_tol, self.mw_maxit = ni, nj, ndiv_mw, mw_tol, mw_maxit
         geo = pkg.fluid.rectangle_geometry(ni, nj, width_neutIn=2.03e-3)
         ds = pkg.workloads.discharge_state(ni, nj, seed=seed)
@@ -123,6 +132,8 @@ class RectangleDischarge:
             if maxit is not None:
                 P[blk].update(maxITR_SOR=maxit)
         P["phi"]["precision"] = precision
+        if V_bias is not None:
+            P["phi"]["V_bias"] = float(V_bias)
         if tol is not None:
             P["phi"].update(error_cnv_SOR_phi=tol)
         if maxit is not None:

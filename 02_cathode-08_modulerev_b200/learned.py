@@ -26,6 +26,7 @@ import numpy as np
 from . import capi
 
 CIN, COUT, BASE = 6, 3, 32
+MW_CIN, MW_COUT = 9, 6     # the microwave network: log n_e, log nu_m1, |B|, previous E; change of E
 CHANNELS_IN = ("log10_ne", "log10_nu_m", "absB", "E_mw", "dphi_prev2", "dphi_prev")
 CHANNELS_OUT = ("re_E_mw", "im_E_mw", "dphi")
 
@@ -63,18 +64,20 @@ def init_params(seed=0, cin=CIN, cout=COUT, base=BASE):
 
 
 class UNet:
-    """Handle of a device U-Net of H x W pixels (6 input, 3 output channels)."""
+    """Handle of a device U-Net of H x W pixels (cin input, cout output channels:
+    6 / 3 for the potential correction, 9 / 6 for the microwave fields)."""
 
-    def __init__(self, H: int, W: int, device: int = 0, seed: int = 0, params=None):
+    def __init__(self, H: int, W: int, device: int = 0, seed: int = 0, params=None, cin: int = CIN,
+                 cout: int = COUT):
         self._L = capi.load()
-        self.H, self.W, self.device = H, W, device
-        self.handle = self._L.cth_unet_create(H, W, CIN, COUT, BASE, device)
+        self.H, self.W, self.device, self.cin, self.cout = H, W, device, cin, cout
+        self.handle = self._L.cth_unet_create(H, W, cin, cout, BASE, device)
         if not self.handle:
             raise RuntimeError(capi.last_error())
         self.n = int(self._L.cth_unet_nparams(self.handle))
         self.t = 0
-        self.stats = np.array([0.0] * 6 + [1.0] * 6 + [0.0] * 3 + [1.0] * 3, np.float32)
-        self.set_params(init_params(seed) if params is None else params)
+        self.stats = np.array([0.0] * cin + [1.0] * cin + [0.0] * cout + [1.0] * cout, np.float32)
+        self.set_params(init_params(seed, cin, cout) if params is None else params)
         self.set_stats(self.stats)
 
     def close(self):
@@ -141,12 +144,14 @@ class UNet:
         capi.check(self._L.cth_unet_set_loss_weights(self.handle, a.ctypes.data), allow_positive=False)
 
     def save(self, path):
-        np.savez(path, params=self.params(), stats=self.stats, H=self.H, W=self.W)
+        np.savez(path, params=self.params(), stats=self.stats, H=self.H, W=self.W, cin=self.cin, cout=self.cout)
 
     @classmethod
     def load(cls, path, device=0):
         z = np.load(path)
-        net = cls(int(z["H"]), int(z["W"]), device=device, params=z["params"])
+        cin = int(z["cin"]) if "cin" in z else CIN
+        cout = int(z["cout"]) if "cout" in z else COUT
+        net = cls(int(z["H"]), int(z["W"]), device=device, params=z["params"], cin=cin, cout=cout)
         net.set_stats(z["stats"])
         return net
 
@@ -156,9 +161,9 @@ class UNet:
         return (stream if stream is not None else torch.cuda.current_stream(self.device)).cuda_stream
 
     def forward(self, x, stream=None):
-        """x: (H, W, 6) float32 CUDA tensor -> (H, W, 3) float32."""
+        """x: (H, W, cin) float32 CUDA tensor -> (H, W, cout) float32."""
         import torch
-        out = torch.empty((self.H, self.W, COUT), dtype=torch.float32, device=x.device)
+        out = torch.empty((self.H, self.W, self.cout), dtype=torch.float32, device=x.device)
         capi.check(self._L.cth_unet_forward(self.handle, _ptr(x.contiguous()), _ptr(out), self._stream(stream)),
                    allow_positive=False)
         return out
@@ -181,6 +186,25 @@ class UNet:
         out = torch.empty((self.H, self.W, CIN), dtype=torch.float32, device=f"cuda:{self.device}")
         capi.check(self._L.cth_unet_features(self.handle, fields._h, _ptr(out), self._stream(stream)),
                    allow_positive=False)
+        return out
+
+    def mw_features(self, fields, E3, escale=1.0, stream=None):
+        """Input of the microwave network (H, W, 9) from the store and the previous
+        fields E3 ((3, nj+2, ld) complex128, the store's layout) times escale
+        (1 / the excitation they were solved with)."""
+        import torch
+        out = torch.empty((self.H, self.W, MW_CIN), dtype=torch.float32, device=f"cuda:{self.device}")
+        capi.check(self._L.cth_unet_mw_features(self.handle, fields._h, _ptr(E3), float(escale), _ptr(out),
+                                                self._stream(stream)), allow_positive=False)
+        return out
+
+    def mw_guess(self, fields, Eprev, jprev=1.0, jnow=1.0, stream=None):
+        """(jnow / jprev) Eprev + jnow x the predicted change per unit excitation,
+        same layout (jprev: the excitation Eprev was solved with; jnow: the next)."""
+        import torch
+        out = torch.empty_like(Eprev)
+        capi.check(self._L.cth_unet_mw_guess(self.handle, fields._h, _ptr(Eprev), float(jprev), float(jnow),
+                                             _ptr(out), self._stream(stream)), allow_positive=False)
         return out
 
     def predict_dphi(self, fields, stream=None):
@@ -344,3 +368,175 @@ def run_steps(pkg, c, nsteps, warm_start, net=None, precision=1):
 
 def now():
     return time.perf_counter()
+
+
+# ---------------------------------------------------------------------------
+# the microwave warm start: a second network (9 input, 6 output channels) maps
+# log n_e, log nu_m1, |B| and the previous microwave fields to their change;
+# the solve starts from previous + change when the device-side residual test
+# takes it (cth_mw_update_set_net), so the network never changes the answer
+# ---------------------------------------------------------------------------
+def mw_target(E_new, j_new, E_prev, j_prev, ni, nj, H, W):
+    """(H, W, 6) float32: real and imaginary parts of the change of Ex, Er, Ephi
+    per unit excitation (E_new / j_new - E_prev / j_prev) at grid cell (i, j) ->
+    pixel (j-1, i-1) (E planes: (3, nj+2, ld) complex128)."""
+    import torch
+    d = (E_new / j_new - E_prev / j_prev)[:, 1:nj + 1, 1:ni + 1]
+    y = torch.zeros((H, W, MW_COUT), dtype=torch.float32, device=E_new.device)
+    for c in range(3):
+        y[:nj, :ni, 2 * c] = d[c].real.to(torch.float32)
+        y[:nj, :ni, 2 * c + 1] = d[c].imag.to(torch.float32)
+    return y
+
+
+def collect_mw_snapshots(pkg, net, ni, nj, runs, nsteps, ndiv_mw, seed=2024, device=0, precision=1):
+    """Plain discharges (``runs`` of them: state seed, bias U(-10, 60) V and
+    microwave power U(2, 16) W drawn from ``seed``) with the microwave update
+    every ``ndiv_mw`` steps for ``nsteps`` steps; one snapshot per update after
+    the first pairs the network's input before the solve (the state and the
+    previous fields) with the change of the fields.  Returns (X [n, H, W, 9],
+    Y [n, H, W, 6], mask [H, W]) un-normalised (the net's stats must be the
+    identity)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    Xs, Ys = [], []
+    for _ in range(runs):
+        d = pkg.discharge.RectangleDischarge(pkg, ni, nj, seed=int(rng.integers(1 << 30)), device=device,
+                                             precision=precision, ndiv_mw=ndiv_mw,
+                                             Pmw=float(rng.uniform(2.0, 16.0)), V_bias=float(rng.uniform(-10.0, 60.0)))
+        try:
+            updates, j_prev = 0, None
+            for _ in range(nsteps):
+                r = d.fs.fluid_step(d.gx, d.gr, d.P)
+                if r["solver_rc"] != 0:
+                    break
+                if d.mw.due(d.P["itime"]):
+                    E_prev = d.e3.clone()
+                    j_now = d.J1r_exc
+                    x = net.mw_features(d.fs, E_prev, escale=1.0 / j_prev) if updates > 0 else None
+                    out = d.microwave()
+                    if out["rc"] != 0:
+                        break
+                    if updates > 0:
+                        Xs.append(x)
+                        Ys.append(mw_target(d.e3, j_now, E_prev, j_prev, ni, nj, net.H, net.W))
+                    updates += 1
+                    j_prev = j_now
+        finally:
+            d.close()
+    mask = torch.zeros((net.H, net.W), dtype=torch.float32, device=Xs[0].device)
+    mask[:nj, :ni] = 1.0
+    return torch.stack(Xs), torch.stack(Ys), mask
+
+
+def mw_fit_stats(X, Y, mask):
+    """Per-channel mean and standard deviation over the masked pixels (inputs
+    and outputs), in the library's layout (2 cin + 2 cout values)."""
+    import torch
+    m = mask.bool()
+
+    def ms(a):
+        v = a[:, m, :].reshape(-1, a.shape[-1]).to(torch.float64)
+        mu = v.mean(0)
+        sd = v.std(0)
+        sd = torch.where(sd > 1e-30, sd, torch.ones_like(sd))
+        return mu.cpu().numpy(), sd.cpu().numpy()
+    im, isd = ms(X)
+    om, osd = ms(Y)
+    return np.concatenate([im, isd, om, osd]).astype(np.float32)
+
+
+def mw_normalise(X, Y, stats):
+    import torch
+    st = torch.as_tensor(stats, device=X.device)
+    ci, co = MW_CIN, MW_COUT
+    Xn = (X - st[0:ci]) / st[ci:2 * ci]
+    Yn = (Y - st[2 * ci:2 * ci + co]) / st[2 * ci + co:2 * ci + 2 * co]
+    return Xn.contiguous(), Yn.contiguous()
+
+
+def mw_train(net, Xn, Yn, mask, epochs=8, lr=5e-4, seed=0, log=None):
+    """Adam on the masked MSE of all six output channels, one snapshot per step."""
+    net.set_loss_weights([1.0] * MW_COUT)
+    msum = float(mask.sum().item())
+    rng = np.random.default_rng(seed)
+    losses = []
+    for ep in range(epochs):
+        order = rng.permutation(Xn.shape[0])
+        tot = 0.0
+        for q in order:
+            tot += net.train_step(Xn[q], Yn[q], mask, msum, lr)
+        losses.append(tot / len(order))
+        if log:
+            log(f"epoch {ep}: mean loss {losses[-1]:.4e}")
+    return losses
+
+
+def mw_evaluate(pkg, net, ni, nj, runs, nsteps, ndiv_mw, tol=1e-8, seed=7, device=0, precision=1):
+    """Held-out discharges: at every microwave update after the first, the same
+    assembled system solved to ``tol`` from zero (the state advances with this
+    solution), from the previous fields and from the network's guess.  Returns
+    per-start iteration counts and solve times, the network's inference time and
+    how often the device-side test rejected its guess (fallback to zero)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    rec = dict(zero=[], previous=[], network=[], zero_ms=[], previous_ms=[], network_ms=[], inference_ms=[],
+               network_guess_residual=[], previous_guess_residual=[], network_rejected=0, previous_rejected=0,
+               updates=0)
+    s = torch.cuda.current_stream()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        out = fn()
+        e1.record(s)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    for _ in range(runs):
+        d = pkg.discharge.RectangleDischarge(pkg, ni, nj, seed=int(rng.integers(1 << 30)), device=device,
+                                             precision=precision, ndiv_mw=ndiv_mw, mw_tol=tol,
+                                             Pmw=float(rng.uniform(2.0, 16.0)), V_bias=float(rng.uniform(-10.0, 60.0)))
+        try:
+            j_prev = None
+            for _ in range(nsteps):
+                r = d.fs.fluid_step(d.gx, d.gr, d.P)
+                if r["solver_rc"] != 0:
+                    break
+                if not d.mw.due(d.P["itime"]):
+                    continue
+                E_prev = d.e3.clone()
+                j_now = d.J1r_exc
+                if j_prev is None:                 # the first update: nothing to start from
+                    out = d.microwave(stream=s)
+                    if out["rc"] != 0:
+                        break
+                    j_prev = j_now
+                    continue
+                guess, t_inf = timed(lambda: net.mw_guess(d.fs, E_prev, j_prev, j_now, stream=s))
+                prev = E_prev * (j_now / j_prev)   # the previous fields at the new excitation
+                out = d.microwave(stream=s)        # assembles, solves from zero, advances the discharge
+                if out["rc"] != 0:
+                    break
+                j_prev = j_now
+                scratch = d.m3.planes(3)
+                (_, sz), t0 = timed(lambda: d.m3.solve_dev(maxITR=400, error_cnv=tol, out=scratch, stream=s))
+                (_, sp), t1 = timed(lambda: d.m3.solve_dev(maxITR=400, error_cnv=tol, out=scratch, x0=prev,
+                                                           stream=s))
+                (_, sn), t2 = timed(lambda: d.m3.solve_dev(maxITR=400, error_cnv=tol, out=scratch, x0=guess,
+                                                           stream=s))
+                rec["zero"].append(sz.iterations)
+                rec["previous"].append(sp.iterations)
+                rec["network"].append(sn.iterations)
+                rec["zero_ms"].append(t0)
+                rec["previous_ms"].append(t1)
+                rec["network_ms"].append(t2)
+                rec["inference_ms"].append(t_inf)
+                rec["previous_guess_residual"].append(sp.guess_residual)
+                rec["network_guess_residual"].append(sn.guess_residual)
+                rec["network_rejected"] += int(sn.guess == -1)
+                rec["previous_rejected"] += int(sp.guess == -1)
+                rec["updates"] += 1
+        finally:
+            d.close()
+    return rec

@@ -443,12 +443,16 @@ class Microwave3:
                                                _ptr(Er_dc) if Er_dc is not None else None, ctypes.byref(prm),
                                                self._stream(stream)), allow_positive=False)
 
-    def solve_dev(self, maxITR: int = 500, error_cnv: float = 1e-10, out=None, stream=None):
+    def solve_dev(self, maxITR: int = 500, error_cnv: float = 1e-10, out=None, stream=None, x0=None,
+                  guess_tol: float = 1.0):
         """Returns (E3, status); E3 of shape (3, nj+2, ld), written on the
-        unknowns (other entries of `out` keep their values)."""
+        unknowns (other entries of `out` keep their values).  x0: an initial
+        guess in the same layout (may be `out`), used when its relative residual
+        is at most guess_tol (decided on the device), else the zero start."""
         E = out if out is not None else self.planes(3)
         st = capi.Status()
-        rc = self._L.cth_mw3_solve_dev(self._h, int(maxITR), float(error_cnv), _ptr(E), self._stream(stream),
-                                       ctypes.byref(st))
+        rc = self._L.cth_mw3_solve_guess_dev(self._h, int(maxITR), float(error_cnv), _ptr(E),
+                                             _ptr(x0) if x0 is not None else None, float(guess_tol),
+                                             self._stream(stream), ctypes.byref(st))
         capi.check(rc)
         return E, st

@@ -329,6 +329,15 @@ int cth_mw3_apply_dev(cth_mw3* m, const double* x3, double* y3, void* stream);
  * their values (the ghosts of earlier calls, as in the reference's persistent
  * fields).  CTH_NOT_CONVERGED after maxit. */
 int cth_mw3_solve_dev(cth_mw3* m, int maxit, double tol, double* E3, void* stream, cth_status* st);
+/* the same from an initial guess (no counterpart in the reference, whose
+ * SparseLU has no start): x0 holds three field planes in E3's layout, read on
+ * the unknowns (x0 may be E3 itself: the previous solution).  The guess is used
+ * when ||b - A x0||_2 <= guess_tol ||b||_2, decided on the device; otherwise the
+ * solve starts from zero, as cth_mw3_solve_dev.  Same stopping rule; a guess that
+ * already meets it ends the solve with 0 iterations.  st->guess: 1 used, -1
+ * rejected; st->guess_residual its relative residual. */
+int cth_mw3_solve_guess_dev(cth_mw3* m, int maxit, double tol, double* E3, const double* x0, double guess_tol,
+                            void* stream, cth_status* st);
 /* the boundary post-processing of solve_Microwave (:3026-3264): ghost values of
  * E1x, E1r, E1p written from E3's unknowns list by list in the reference's
  * order (reading the ghosts of earlier lists and calls where the reference
@@ -699,6 +708,7 @@ int cth_restart_read(cth_fields* fs, cth_grid* gx, cth_grid* gr, const char* pat
                      const double* r, const cth_restart_params* prm, void* stream, cth_restart_info* info);
 
 typedef struct cth_mw_update cth_mw_update;  /* the microwave update, declared below */
+struct cth_unet;                              /* the network, declared below */
 
 /* Batched instances (the I-V sweeps; no counterpart in the reference, which runs
  * one discharge per process) -------------------------------------------------
@@ -811,6 +821,11 @@ typedef struct cth_mw_update_params {
     int ndiv_mw;                /* run every ndiv_mw steps                          */
     int maxit;
     double tol;
+    int warm_start;             /* 1: the solve starts from the previous update's
+                                   fields scaled to the new excitation (the system
+                                   is linear in J1r_exc) when their residual is
+                                   <= ||b|| (device-side choice,
+                                   cth_mw3_solve_guess_dev); 0: zero */
 } cth_mw_update_params;
 typedef struct cth_mw_update_result {
     cth_status solve;
@@ -825,6 +840,11 @@ void cth_mw_update_destroy(cth_mw_update* u);
 int cth_mw_update_due(const cth_mw_update* u, int itime);
 double* cth_mw_update_plane(cth_mw_update* u, int which);
 int cth_mw_update_run(cth_mw_update* u, cth_grid* gx, cth_grid* gr, void* stream, cth_mw_update_result* res);
+/* a trained microwave network (cth_unet of 9 input, 6 output channels, see
+ * cth_unet_mw_guess) whose guess starts every solve after the first (NULL: none);
+ * the guess is taken when its residual is at most ||b||, else the solve starts
+ * from the previous fields (warm_start) or zero.  res->solve.guess reports it. */
+int cth_mw_update_set_net(cth_mw_update* u, struct cth_unet* net);
 /* the first solve of a handle builds its hierarchy and solve graph: this runs the
  * assembly and the solve alone (E's unknowns written, nothing else: no ghosts,
  * no absorbed power, no rescale), so that the build happens before a timed run */
@@ -914,6 +934,21 @@ int cth_unet_train_step(cth_unet* n, const float* in, const float* target, const
 int cth_unet_set_stats(cth_unet* n, const float* stats);
 int cth_unet_features(cth_unet* n, cth_fields* fs, float* out, void* stream);
 int cth_unet_predict_dphi(cth_unet* n, cth_fields* fs, void* stream);
+/* The microwave warm start (9 input, 6 output channels).  The system is linear
+ * in the port excitation J1r_exc, which the rescale changes between updates, so
+ * the network works on fields per unit excitation: input = log10 n_e, log10
+ * nu_m1, |B| and the real and imaginary parts of the previous fields E1x, E1r,
+ * E1p times escale (E3: three interleaved complex planes of the store's layout)
+ * at grid cell (i, j) -> pixel (j-1, i-1), normalised by the stats; output =
+ * the normalised change of the six parts per unit excitation.
+ * cth_unet_mw_features writes the input (H x W x 9 FP32, device);
+ * cth_unet_mw_guess (escale = 1 / jprev) runs the network and writes Eguess =
+ * (jnow / jprev) Eprev + jnow x the de-normalised change on the grid cells
+ * ((jnow / jprev) Eprev elsewhere), jprev the excitation Eprev was solved with,
+ * jnow the next solve's; Eguess distinct from Eprev. */
+int cth_unet_mw_features(cth_unet* n, cth_fields* fs, const double* E3, double escale, float* out, void* stream);
+int cth_unet_mw_guess(cth_unet* n, cth_fields* fs, const double* Eprev, double jprev, double jnow, double* Eguess,
+                      void* stream);
 
 /* Layout helpers (device arrays): copy between the reference's [i][j] layout
  * and the library layout. */

@@ -1,0 +1,63 @@
+"""The small FP64 discharge end to end: the 100 (r) x 200 (z) rectangle with the
+loop's microwave update every 100 steps (Pmw = 8 W), on the device
+(discharge.RectangleDischarge) against the restated loop with exact solves
+(tests/golden/config0_rect_100x200.npz, made by tests/golden/make_config0.py).
+
+Bar: relative L2 over the cells <= 1e-8 on phi, n_e, n_i, Te and the
+cell-centred |E| (outputModule.hpp:310-311) in plain FP64 at the reference's
+solver settings (1e-10 relative residual, 30 cycles, as input/setup.yaml), after
+step 100 (the first microwave update included); the mixed form (FP32 cycles +
+FP64 defect correction) reaches the same converged residual and the same bar.
+
+Why not step 1000: after the first update the 8 W heat the electrons of this
+small volume to hundreds of eV, and the loop itself amplifies differences: the
+restated loop started from a density changed by a relative 1e-12 differs from
+itself by 7.6e-5 in Te at step 150, 6.5e-3 at step 200 and O(1) at step 1000
+(tests/golden/config0_sensitivity.json, checked by tests/test_config0.py).  Past
+step 100 no two implementations -- nor one implementation with two solver
+tolerances -- agree to 1e-8; step 150 is printed for the record."""
+import os
+
+import numpy as np
+import pytest
+
+import refpin
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+NI, NJ = 200, 100
+FIELDS = ("phi", "rhoe", "rhoi", "Te")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return np.load(os.path.join(HERE, "golden", "config0_rect_100x200.npz"))
+
+
+def _norms(d, z, n, mask, r):
+    out = {k: refpin.rel_l2(d.fs.download(k), z[f"s{n:04d}_{k}"], mask) for k in FIELDS}
+    out["|E|"] = refpin.rel_l2(refpin.emag(d.fs.download("Ex"), d.fs.download("Er"), r),
+                               refpin.emag(z[f"s{n:04d}_Ex"], z[f"s{n:04d}_Er"], r), mask)
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_small_discharge_through_the_first_microwave_update(pkg, cuda_device, golden, precision):
+    mask = np.zeros((NI + 2, NJ + 2), bool)
+    mask[1:NI + 1, 1:NJ + 1] = True
+    r = (np.arange(NJ + 2) - 0.5) * (5e-3 / NJ)
+    d = pkg.discharge.RectangleDischarge(pkg, NI, NJ, seed=0, precision=precision)
+    done = 0
+    for n in (100, 150):
+        for _ in range(n - done):
+            rr = d.step()
+            assert rr["solver_rc"] == 0, (done, rr)
+            if "mw" in rr:
+                assert rr["mw"]["rc"] == 0 and rr["mw"]["solve"]["converged"] == 1, rr["mw"]
+        done = n
+        norms = _norms(d, golden, n, mask, r)
+        print("small discharge", "mixed" if precision else "fp64", n, {k: f"{v:.1e}" for k, v in norms.items()})
+        if n == 100:
+            for k, v in norms.items():
+                assert v <= 1e-8, (n, k, v)
+    d.close()

@@ -423,3 +423,47 @@ def test_mw3_mixed_precision_matches_direct(pkg, cuda_device, geometry, bmax, pr
     with pytest.raises(pkg.capi.CathodeError):
         m.set_precision(7)
     m.close(); g.close()
+
+
+@pytest.mark.parametrize("geometry", ["rectangle", "cathode"])
+def test_mw3_initial_guess(pkg, cuda_device, geometry):
+    """The solve from an initial guess: the converged solution itself ends the
+    solve at once (0 iterations, or 1 where its true residual b - A x sits just
+    above the tolerance that the recurrence's residual met); a perturbed solution (a later time
+    step's start) converges in fewer iterations to the direct solution; a guess
+    worse than zero is rejected on the device and the result is the zero-start
+    solve bit for bit, in the graph and kernel by kernel."""
+    import torch
+    if geometry == "cathode":
+        w, mw, ref, m, g = _cathode(pkg, 194, 70)
+        ni = 194
+    else:
+        ni, nj = 96, 40
+        w, p, mw = _case(pkg, ni, nj)
+        ref = mw.mag_rect_system(w["ne"], w["nu"], w["Bx"], w["Br"], w["epsr"], p)
+        g, planes = _device(pkg, w)
+        m = pkg.Microwave3(ni, nj)
+        m.assemble_dev(*planes, w["params"])
+    x_ref = mw.mag_pack(ref, mw.mag_rect_solve(ref))
+    for graphs in (True, False):
+        m.set_graphs(graphs)
+        E0, st0 = m.solve_dev(maxITR=600, error_cnv=1e-12)
+        assert st0.converged == 1 and st0.guess == 0
+        E1, st1 = m.solve_dev(maxITR=600, error_cnv=1e-12, x0=E0)
+        assert st1.guess == 1 and st1.iterations <= 1 and st1.converged == 1, st1.as_dict()
+        if st1.iterations == 0:
+            assert torch.equal(E1, E0)
+        assert _rel(mw.mag_pack(ref, _to_ij(E1, ni)), x_ref) < 1e-8
+        gen = torch.Generator(device=E0.device).manual_seed(5)
+        noise = torch.randn(E0.shape, dtype=torch.float64, device=E0.device, generator=gen)
+        Ep = E0 * (1.0 + 1e-3 * noise)
+        E2, st2 = m.solve_dev(maxITR=600, error_cnv=1e-12, x0=Ep)
+        assert st2.guess == 1 and 0 < st2.guess_residual < 1 and st2.converged == 1
+        assert st2.iterations < st0.iterations, (st2.iterations, st0.iterations)
+        assert _rel(mw.mag_pack(ref, _to_ij(E2, ni)), x_ref) < 1e-8
+        E3, st3 = m.solve_dev(maxITR=600, error_cnv=1e-12, x0=E0 * 1e6)
+        assert st3.guess == -1 and st3.iterations == st0.iterations
+        assert torch.equal(E3, E0)
+        print("mw3 guess", geometry, graphs, "zero", st0.iterations, "perturbed", st2.iterations,
+              f"guess residual {st2.guess_residual:.1e}")
+    m.close(); g.close()
