@@ -429,8 +429,9 @@ def test_mw3_mixed_precision_matches_direct(pkg, cuda_device, geometry, bmax, pr
 def test_mw3_initial_guess(pkg, cuda_device, geometry):
     """The solve from an initial guess: the converged solution itself ends the
     solve at once (0 iterations, or 1 where its true residual b - A x sits just
-    above the tolerance that the recurrence's residual met); a perturbed solution (a later time
-    step's start) converges in fewer iterations to the direct solution; a guess
+    above the tolerance that the recurrence's residual met); the solution scaled
+    by 1.001 (relative residual 1e-3) converges in fewer iterations to the direct
+    solution; a guess
     worse than zero is rejected on the device and the result is the zero-start
     solve bit for bit, in the graph and kernel by kernel."""
     import torch
@@ -454,11 +455,10 @@ def test_mw3_initial_guess(pkg, cuda_device, geometry):
         if st1.iterations == 0:
             assert torch.equal(E1, E0)
         assert _rel(mw.mag_pack(ref, _to_ij(E1, ni)), x_ref) < 1e-8
-        gen = torch.Generator(device=E0.device).manual_seed(5)
-        noise = torch.randn(E0.shape, dtype=torch.float64, device=E0.device, generator=gen)
-        Ep = E0 * (1.0 + 1e-3 * noise)
+        # the solution at 1.001 times the excitation: residual 1e-3 ||b|| (the system is linear)
+        Ep = E0 * 1.001
         E2, st2 = m.solve_dev(maxITR=600, error_cnv=1e-12, x0=Ep)
-        assert st2.guess == 1 and 0 < st2.guess_residual < 1 and st2.converged == 1
+        assert st2.guess == 1 and st2.guess_residual == pytest.approx(1e-3, rel=1e-3) and st2.converged == 1
         assert st2.iterations < st0.iterations, (st2.iterations, st0.iterations)
         assert _rel(mw.mag_pack(ref, _to_ij(E2, ni)), x_ref) < 1e-8
         E3, st3 = m.solve_dev(maxITR=600, error_cnv=1e-12, x0=E0 * 1e6)
