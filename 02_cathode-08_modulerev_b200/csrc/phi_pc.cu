@@ -244,15 +244,23 @@ constexpr int kNStat = 12;  // (phi, nUex, nUer) x (vs iteration start, vs call 
 
 // interior fields and flux corrections, then the residual reductions
 // (fluidModule.hpp:2932-3046); the last block writes the 12 totals to out
+// kCorrCells consecutive cells of a row per thread: a block covers kCorrCells x
+// blockDim cells, so the deterministic reduction's per-block tree and its
+// last-block combine (one partial per block and statistic) stay short
+constexpr int kCorrCells = 4;
+
 __global__ void k_phi_correct_b(PhiArgs A, double* __restrict__ part, unsigned int* counter,
                                 double* __restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = kCorrCells * (blockIdx.x * blockDim.x + threadIdx.x);
     const int j = blockIdx.y;
     const int mode = A.prm.flag_error;
     double s[kNStat];
 #pragma unroll
     for (int k = 0; k < kNStat; k++) s[k] = 0.0;
-    if (i <= A.ni + 1) {
+#pragma unroll
+    for (int kc = 0; kc < kCorrCells; kc++) {
+        const int i = i0 + kc;
+        if (i > A.ni + 1) break;
         const int ld = A.ld;
         const size_t p = (size_t)j * ld + i;
         const double dx = A.prm.dx, dr = A.prm.dr;
@@ -372,7 +380,8 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
             CTH_CUDA(cudaMemcpyAsync(dphi_prev, A.dphi, g->plane * sizeof(double), cudaMemcpyDeviceToDevice, s));
         }
         k_phi_correct_a<<<grd, blk, 0, s>>>(A);
-        k_phi_correct_b<<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out);
+        k_phi_correct_b<<<dim3((g->ni + 2 + 256 * kCorrCells - 1) / (256 * kCorrCells), g->nj + 2), 256, 0, s>>>(
+            A, fs->part, g->ws.counter, out);
         g->launches += 2;
         CTH_CUDA(cudaGetLastError());
         CTH_CUDA(cudaMemcpyAsync(fs->h_scal, out, kNStat * sizeof(double), cudaMemcpyDeviceToHost, s));

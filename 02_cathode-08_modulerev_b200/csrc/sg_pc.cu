@@ -253,15 +253,23 @@ __global__ void k_sg_assemble(SgArgs A) {
 
 constexpr int kSgStat = 14;  // calcRes pairs (n, Fx, Fr) x (iteration, call) + anode Ii, Ie
 
+// kCorrCells consecutive cells of a row per thread: a block covers kCorrCells x
+// blockDim cells, so the deterministic reduction's per-block tree and its
+// last-block combine (one partial per block and statistic) stay short
+constexpr int kCorrCells = 4;
+
 template <bool EN>
 __global__ void k_sg_correct(SgArgs A, double* __restrict__ part, unsigned int* counter, double* __restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = kCorrCells * (blockIdx.x * blockDim.x + threadIdx.x);
     const int j = blockIdx.y;
     const int mode = A.prm.flag_error;
     double s[kSgStat];
 #pragma unroll
     for (int k = 0; k < kSgStat; k++) s[k] = 0.0;
-    if (i <= A.ni + 1) {
+#pragma unroll
+    for (int kc = 0; kc < kCorrCells; kc++) {
+        const int i = i0 + kc;
+        if (i > A.ni + 1) break;
         const int ld = A.ld;
         const size_t p = (size_t)j * ld + i;
         const double dx = A.prm.dx, dr = A.prm.dr;
@@ -293,8 +301,8 @@ __global__ void k_sg_correct(SgArgs A, double* __restrict__ part, unsigned int* 
             res_stat(mode, v, A.n_old[p], s[6], s[7]);
             if (!EN && (fc & F_BRX_BIAS)) {
                 const double rj = A.prm.rmin + (j - 0.5) * dr;
-                s[12] = A.rhoUix_wall[p + 1] * 2.0 * M_PI * rj * dr * (kE0f);
-                s[13] = A.Fx_w[p + 1] * 2.0 * M_PI * rj * dr * (-kE0f);
+                s[12] += A.rhoUix_wall[p + 1] * 2.0 * M_PI * rj * dr * (kE0f);
+                s[13] += A.Fx_w[p + 1] * 2.0 * M_PI * rj * dr * (-kE0f);
             }
         }
     }
@@ -404,7 +412,8 @@ static int solve_sg_pc(cth_fields* fs, const cth_sg_params* prm, cudaStream_t s,
             rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
                                   prm->precision, A.d, s, &pend, fs->h_solve);
         if (rc < 0) return rc;
-        k_sg_correct<EN><<<grd, blk, 0, s>>>(A, fs->part, g->ws.counter, out);
+        k_sg_correct<EN><<<dim3((g->ni + 2 + 256 * kCorrCells - 1) / (256 * kCorrCells), g->nj + 2), 256, 0, s>>>(
+            A, fs->part, g->ws.counter, out);
         g->launches++;
         CTH_CUDA(cudaGetLastError());
         CTH_CUDA(cudaMemcpyAsync(fs->h_scal, out, kSgStat * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -112,6 +112,9 @@ __device__ __forceinline__ double pow2_scale(double v) {
     return (isfinite(v) && v != 0.0) ? ldexp(1.0, -ilogb(v)) : 1.0;
 }
 
+// cells per thread of k_prep0
+constexpr int PREP_CELLS = 4;
+
 template <typename T>
 __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask,
                         int ld_u, int i0, int j0, int ncol, int nrow, int ldl, size_t qref, T* __restrict__ a0,
@@ -119,14 +122,18 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
                         unsigned int* counter, double* __restrict__ stat, cudaGraphConditionalHandle cond,
                         int use_cond) {
     __shared__ double red[32];
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c0 = PREP_CELLS * (blockIdx.x * blockDim.x + threadIdx.x);
     const int r = blockIdx.y;
     const double sA = pow2_scale(args->aP[qref]);
     const double gw = stat[ST_GUESS];
     const bool guess = gw >= 1.0;
     const double* xg = (gw >= 100.0) ? args->x0b : args->x0;
     double v2[2] = {0.0, 0.0};  // ||r0||^2, ||b||^2
-    if (c < ncol) {
+    // PREP_CELLS consecutive cells of row r per thread, their loads in flight together
+#pragma unroll
+    for (int k = 0; k < PREP_CELLS; k++) {
+        const int c = c0 + k;
+        if (c >= ncol) break;
         const double* __restrict__ aP = args->aP;
         const size_t plane = (size_t)nrow * ldl;
         const size_t p = (size_t)r * ldl + c;
@@ -139,15 +146,15 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
             if (r > 0 && mask[p - ldl]) vS = (T)(args->aS[q] * sA);
             if (r + 1 < nrow && mask[p + ldl]) vN = (T)(args->aN[q] * sA);
             const double bv = args->b[q];
-            v2[1] = bv * bv;
+            v2[1] += bv * bv;
             if (guess) {
                 const double rv = guess_resid(args, xg, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
                 vb = (T)(rv * sA);
-                v2[0] = rv * rv;
+                v2[0] += rv * rv;
                 x64[p] = xg[q];
             } else {
                 vb = (T)(bv * sA);
-                v2[0] = v2[1];
+                v2[0] += bv * bv;
             }
         }
         a0[P * plane + p] = vP;
@@ -772,6 +779,9 @@ __global__ void k_tail(TailArgs<T> A) {
     }
 }
 
+// cells per thread of k_update
+constexpr int UPD_CELLS = 4;
+
 // ---------------------------------------------------------------------------
 // defect correction, iteration it = stat[ST_ITER] + 1: x_it = x_{it-1} + e with
 // x_k in x64[k & 1]; r = b - A x_it with the caller's FP64 coefficients; next
@@ -789,7 +799,9 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
     const int it = (int)stat[ST_ITER] + 1;
     const double* __restrict__ xin = (it & 1) ? x64a : x64b;
     double* __restrict__ xout = (it & 1) ? x64b : x64a;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    // UPD_CELLS consecutive cells of row r per thread: their loads are in flight
+    // together and the west / east neighbours come from the thread's own cells
+    const int c0 = UPD_CELLS * (blockIdx.x * blockDim.x + threadIdx.x);
     const int r = blockIdx.y;
     // e solves the cycle's system for xs x (the previous right-hand side's scale);
     // this right-hand side is scaled so that sA times the previous residual norm is O(1)
@@ -798,21 +810,33 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
     const double xs = pow2_scale(sqrt(stat[ST_RR]) * sA);
     const double sb = sA * xs;
     double rr = 0.0;
-    if (c < ncol) {
-        const size_t p = (size_t)r * ldl + c;
-        const double xc = xin[p] + (double)e[p] * ie;
-        double res = 0.0;
-        if (mask[p]) {
-            const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
-            res = args->b[q] - args->aP[q] * xc;
-            if (c + 1 < ncol) res += args->aE[q] * (xin[p + 1] + (double)e[p + 1] * ie);
-            if (c > 0) res += args->aW[q] * (xin[p - 1] + (double)e[p - 1] * ie);
-            if (r + 1 < nrow) res += args->aN[q] * (xin[p + ldl] + (double)e[p + ldl] * ie);
-            if (r > 0) res += args->aS[q] * (xin[p - ldl] + (double)e[p - ldl] * ie);
+    if (c0 < ncol) {
+        const size_t p0 = (size_t)r * ldl + c0;
+        const size_t q0 = (size_t)(r + j0) * ld_u + (c0 + i0);
+        // x + e on cells c0-1 .. c0+UPD_CELLS of this row (the ends only where they exist)
+        double xc[UPD_CELLS + 2];
+#pragma unroll
+        for (int k = 0; k < UPD_CELLS + 2; k++) {
+            const int c = c0 - 1 + k;
+            xc[k] = (c >= 0 && c < ncol) ? xin[p0 - 1 + k] + (double)e[p0 - 1 + k] * ie : 0.0;
         }
-        xout[p] = xc;
-        b0[p] = (T)(res * sb);
-        rr = res * res;
+#pragma unroll
+        for (int k = 0; k < UPD_CELLS; k++) {
+            const int c = c0 + k;
+            if (c >= ncol) break;
+            const size_t p = p0 + k, q = q0 + k;
+            double res = 0.0;
+            if (mask[p]) {
+                res = args->b[q] - args->aP[q] * xc[k + 1];
+                if (c + 1 < ncol) res += args->aE[q] * xc[k + 2];
+                if (c > 0) res += args->aW[q] * xc[k];
+                if (r + 1 < nrow) res += args->aN[q] * (xin[p + ldl] + (double)e[p + ldl] * ie);
+                if (r > 0) res += args->aS[q] * (xin[p - ldl] + (double)e[p - ldl] * ie);
+            }
+            xout[p] = xc[k + 1];
+            b0[p] = (T)(res * sb);
+            rr += res * res;
+        }
     }
     double tot;
     if (last_block_sum(rr, part, counter, red, &tot) && threadIdx.x == 0) {
@@ -1107,10 +1131,11 @@ static int enqueue_pre(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle c
     Workspace& w = g->ws;
     const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
     dim3 blk(256), grd((ncol + 255) / 256, nrow0);
+    dim3 grdp((ncol + 256 * PREP_CELLS - 1) / (256 * PREP_CELLS), nrow0);
     cudaMemsetAsync(w.x64[0], 0, sizeof(double) * (size_t)nrow0 * ldl, s);
     k_guess<<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, w.part, w.counter,
                                 w.stat);
-    k_prep0<T><<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, g->qref, h.a[0],
+    k_prep0<T><<<grdp, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, g->qref, h.a[0],
                                    h.b[0], w.x64[0], w.part, w.counter, w.stat, cond, use_cond);
     const long long l0 = g->launches;
     setup_levels<T>(g, s);
@@ -1124,7 +1149,7 @@ static int enqueue_body(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle 
     Hierarchy<T>& h = hier<T>(g);
     Workspace& w = g->ws;
     const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
-    dim3 blk(256), grd((ncol + 255) / 256, nrow0);
+    dim3 blk(256), grd((ncol + 256 * UPD_CELLS - 1) / (256 * UPD_CELLS), nrow0);
     const long long l0 = g->launches;
     vcycle<T>(g, 0, s);
     const int slot = prof_mark(g, PROF_UPDATE, (double)nrow0 * ncol * (8.0 * 8.0 + 2.0 * sizeof(T) + 1.0), s);
