@@ -40,7 +40,7 @@ EXPORTS = (
     "cth_ghost_rules_upload", "cth_energy_keep_walls_upload", "cth_restart_write", "cth_restart_wait", "cth_restart_read", "cth_mw_impedance_test", "cth_mw_divergence", "cth_solve_rhoe_pc", "cth_solve_Te_pc", "cth_check_cfl",
     "cth_ion_program_upload", "cth_ion_boxes_upload", "cth_ion_step", "cth_update_neutrals", "cth_fluid_step",
     "cth_batch_steps", "cth_mw_update_create", "cth_mw_update_destroy", "cth_mw_update_due", "cth_mw_update_plane",
-    "cth_mw_update_run", "cth_mw_update_prepare", "cth_update_energy_profile", "cth_mw_port_rescale", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
+    "cth_mw_update_run", "cth_mw_update_prepare", "cth_mw_update_prepared", "cth_update_energy_profile", "cth_mw_port_rescale", "cth_cmat2_mul", "cth_cmat2_inv", "cth_sparam_to_abcd", "cth_abcd_to_sparam", "cth_sparam_setup",
     "cth_unet_create", "cth_unet_destroy", "cth_unet_nparams", "cth_unet_launch_count", "cth_unet_set_tensor_cores", "cth_unet_set_smoothing", "cth_unet_set_wait_test", "cth_unet_set_grid_limit", "cth_unet_check", "cth_unet_set_params", "cth_unet_get_params",
     "cth_unet_get_grads", "cth_unet_set_loss_weights", "cth_unet_forward", "cth_unet_backward",
     "cth_unet_train_step", "cth_unet_set_stats", "cth_unet_features", "cth_unet_predict_dphi",
@@ -394,6 +394,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_mw_update_run.restype = ctypes.c_int
     L.cth_mw_update_prepare.argtypes = [_vp, _vp]
     L.cth_mw_update_prepare.restype = ctypes.c_int
+    L.cth_mw_update_prepared.argtypes = [_vp]
+    L.cth_mw_update_prepared.restype = ctypes.c_int
     L.cth_update_energy_profile.argtypes = [_vp, _vp, _vp, ctypes.POINTER(EnergyParams)] + [_vp] * 7 + \
         [ctypes.POINTER(EnergyResult)]
     L.cth_update_energy_profile.restype = ctypes.c_int

@@ -36,6 +36,16 @@ extern "C" int cth_batch_steps(cth_batch_item* items, int n, int steps, int nthr
         CTH_CUDA(cudaSetDevice(items[k].fs->g->device));
         CTH_CUDA(cudaStreamCreateWithFlags(&streams[k], cudaStreamNonBlocking));
     }
+    // the first solve of a microwave handle builds its hierarchy and solve graph:
+    // done here, one handle after another on this thread, not in the workers
+    for (int k = 0; k < n; k++) {
+        cth_mw_update* mw = items[k].mw;
+        if (!mw || cth_mw_update_prepared(mw)) continue;
+        CTH_CUDA(cudaSetDevice(items[k].fs->g->device));
+        const int rc = cth_mw_update_prepare(mw, streams[k]);
+        if (rc < 0) return rc;
+        CTH_CUDA(cudaStreamSynchronize(streams[k]));
+    }
     const int T = std::min(nthreads, n);
     auto worker = [&](int t) {
         std::vector<int> mine;

@@ -230,6 +230,16 @@ __device__ __forceinline__ void res_stat(int mode, double nw, double od, double&
     else { a = d * d; b = od * od; }
 }
 
+// the same statistics accumulated over several cells of one thread (the modes'
+// max or sum, as the grid reduction combines them afterwards)
+__device__ __forceinline__ void res_acc(int mode, double nw, double od, double& a, double& b) {
+    const double d = nw - od;
+    if (mode == 0) { a = fmax(a, fabs(d)); }
+    else if (mode == 1) { a += (d * d) / (od * od + 1e-100); b += 1.0; }
+    else if (mode == 2) { a = fmax(a, fabs(d)); b = fmax(b, fabs(od)); }
+    else { a += d * d; b += od * od; }
+}
+
 inline double finish_res(int mode, double a, double b) {
     if (mode == 0) return a;
     if (mode == 1) return sqrt(a / b);

@@ -19,6 +19,7 @@ struct cth_mw_update {
     cth_fields* fs = nullptr;
     cth_mw3* m = nullptr;
     int device = 0, ndiv = 100, maxit = 400, warm = 0, runs = 0;
+    bool prepared = false;     // the solve's hierarchy and graph are built
     double tol = 1e-10;
     cth_mw_params mw{};
     cth_energy_params ep{};
@@ -90,6 +91,14 @@ extern "C" int cth_mw_update_create(cth_fields* fs, cth_mw3* m, const cth_mw_upd
         cth_mw_update_destroy(u);
         return cth::cuda_fail(e, "cth_mw_update_create");
     }
+    // every store plane the update reads or writes exists from here on, so that no
+    // later run allocates (runs may come from the worker threads of a batch)
+    for (const char* name : {"rhoe", "nu_m1", "Bx", "Br", "epsr_mw", "Er", "Pabsx", "Pabsr", "Pabsp", "Pabs"}) {
+        if (!cth_field(fs, name)) {
+            cth_mw_update_destroy(u);
+            return CTH_ERR_ALLOC;
+        }
+    }
     *out = u;
     return CTH_OK;
 }
@@ -142,8 +151,12 @@ extern "C" int cth_mw_update_prepare(cth_mw_update* u, void* stream) {
     if (rc < 0) return rc;
     cth_status st{};
     rc = cth_mw3_solve_dev(u->m, u->maxit, u->tol, u->E3, stream, &st);
-    return rc < 0 ? rc : CTH_OK;
+    if (rc < 0) return rc;
+    u->prepared = true;
+    return CTH_OK;
 }
+
+extern "C" int cth_mw_update_prepared(const cth_mw_update* u) { return (u && u->prepared) ? 1 : 0; }
 
 extern "C" int cth_mw_update_run(cth_mw_update* u, cth_grid* gx, cth_grid* gr, void* stream,
                                  cth_mw_update_result* res) {

@@ -271,8 +271,8 @@ __global__ void k_phi_correct_b(PhiArgs A, double* __restrict__ part, unsigned i
             const double rho_t = (A.rhoe[p] + A.rhoe[p - 1]) / 2.0;
             const double v = A.nUex[p] + mst * rho_t * ((A.dphi[p] - A.dphi[p - 1]) / dx);
             A.nUex[p] = v;
-            res_stat(mode, v, A.nUex_t[p], s[2], s[3]);
-            res_stat(mode, v, A.nUex_old[p], s[8], s[9]);
+            res_acc(mode, v, A.nUex_t[p], s[2], s[3]);
+            res_acc(mode, v, A.nUex_old[p], s[8], s[9]);
         }
         if (fc && fs) {
             A.Er[p] = -(A.phi[p] - A.phi[p - ld]) / dr;
@@ -280,13 +280,13 @@ __global__ void k_phi_correct_b(PhiArgs A, double* __restrict__ part, unsigned i
             const double rho_t = (A.rhoe[p] + A.rhoe[p - ld]) / 2.0;
             const double v = A.nUer[p] + mst * rho_t * ((A.dphi[p] - A.dphi[p - ld]) / dr);
             A.nUer[p] = v;
-            res_stat(mode, v, A.nUer_t[p], s[4], s[5]);
-            res_stat(mode, v, A.nUer_old[p], s[10], s[11]);
+            res_acc(mode, v, A.nUer_t[p], s[4], s[5]);
+            res_acc(mode, v, A.nUer_old[p], s[10], s[11]);
         }
         if (fc) {
             const double v = A.phi[p];
-            res_stat(mode, v, A.phi_t[p], s[0], s[1]);
-            res_stat(mode, v, A.phi_old[p], s[6], s[7]);
+            res_acc(mode, v, A.phi_t[p], s[0], s[1]);
+            res_acc(mode, v, A.phi_old[p], s[6], s[7]);
         }
     }
     grid_reduce<kNStat>(s, (mode == 0 || mode == 2) ? 0xfffu : 0u, part, counter, out);

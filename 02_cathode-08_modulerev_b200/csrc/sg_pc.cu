@@ -120,9 +120,7 @@ __device__ __forceinline__ double sg_wall(const SgArgs& A, size_t c, double E, d
 }
 
 template <bool EN>
-__global__ void k_sg_predict(SgArgs A) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
+__device__ __forceinline__ void sg_predict_cell(const SgArgs& A, int i, int j) {
     if (i > A.ni + 1) return;
     const int ld = A.ld;
     const size_t p = (size_t)j * ld + i;
@@ -203,10 +201,18 @@ __global__ void k_sg_predict(SgArgs A) {
     A.Fr[p] = vr;
 }
 
+// kSweepCells consecutive cells of a row per thread (their loads in flight together)
+constexpr int kSweepCells = 4;
+
 template <bool EN>
-__global__ void k_sg_assemble(SgArgs A) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
+__global__ void k_sg_predict(SgArgs A) {
+    const int i0 = kSweepCells * (blockIdx.x * blockDim.x + threadIdx.x);
+#pragma unroll
+    for (int k = 0; k < kSweepCells; k++) sg_predict_cell<EN>(A, i0 + k, blockIdx.y);
+}
+
+template <bool EN>
+__device__ __forceinline__ void sg_assemble_cell(const SgArgs& A, int i, int j) {
     if (i > A.ni + 1) return;
     const int ld = A.ld;
     const size_t p = (size_t)j * ld + i;
@@ -251,6 +257,13 @@ __global__ void k_sg_assemble(SgArgs A) {
     A.aP[p] = vP; A.aE[p] = vE; A.aW[p] = vW; A.aN[p] = vN; A.aS[p] = vS; A.b[p] = vb;
 }
 
+template <bool EN>
+__global__ void k_sg_assemble(SgArgs A) {
+    const int i0 = kSweepCells * (blockIdx.x * blockDim.x + threadIdx.x);
+#pragma unroll
+    for (int k = 0; k < kSweepCells; k++) sg_assemble_cell<EN>(A, i0 + k, blockIdx.y);
+}
+
 constexpr int kSgStat = 14;  // calcRes pairs (n, Fx, Fr) x (iteration, call) + anode Ii, Ie
 
 // kCorrCells consecutive cells of a row per thread: a block covers kCorrCells x
@@ -279,16 +292,16 @@ __global__ void k_sg_correct(SgArgs A, double* __restrict__ part, unsigned int* 
             const double dF = EN ? (f.A() * A.d[p - 1] - f.B() * A.d[p]) * 5.0 / 3.0 : f.A() * A.d[p - 1] - f.B() * A.d[p];
             const double v = A.Fx[p] + dF;
             A.Fx[p] = v;
-            res_stat(mode, v, A.Fx_t[p], s[2], s[3]);
-            res_stat(mode, v, A.Fx_old[p], s[8], s[9]);
+            res_acc(mode, v, A.Fx_t[p], s[2], s[3]);
+            res_acc(mode, v, A.Fx_old[p], s[8], s[9]);
         }
         if (fc && fs) {
             const SgFace f = sg_face(A, p - ld, p, A.Er[p], dr);
             const double dF = EN ? (f.A() * A.d[p - ld] - f.B() * A.d[p]) * 5.0 / 3.0 : f.A() * A.d[p - ld] - f.B() * A.d[p];
             const double v = A.Fr[p] + dF;
             A.Fr[p] = v;
-            res_stat(mode, v, A.Fr_t[p], s[4], s[5]);
-            res_stat(mode, v, A.Fr_old[p], s[10], s[11]);
+            res_acc(mode, v, A.Fr_t[p], s[4], s[5]);
+            res_acc(mode, v, A.Fr_old[p], s[10], s[11]);
         }
         if (fc) {
             double v = A.n[p];
@@ -297,8 +310,8 @@ __global__ void k_sg_correct(SgArgs A, double* __restrict__ part, unsigned int* 
                 v = nn;
                 A.n[p] = v;
             }
-            res_stat(mode, v, A.n_t[p], s[0], s[1]);
-            res_stat(mode, v, A.n_old[p], s[6], s[7]);
+            res_acc(mode, v, A.n_t[p], s[0], s[1]);
+            res_acc(mode, v, A.n_old[p], s[6], s[7]);
             if (!EN && (fc & F_BRX_BIAS)) {
                 const double rj = A.prm.rmin + (j - 0.5) * dr;
                 s[12] += A.rhoUix_wall[p + 1] * 2.0 * M_PI * rj * dr * (kE0f);
@@ -400,8 +413,9 @@ static int solve_sg_pc(cth_fields* fs, const cth_sg_params* prm, cudaStream_t s,
     for (;;) {
         ncount++;
         k_sg_save<<<grd, blk, 0, s>>>(A);
-        k_sg_predict<EN><<<grd, blk, 0, s>>>(A);
-        k_sg_assemble<EN><<<grd, blk, 0, s>>>(A);
+        const dim3 grd4((g->ni + 2 + 128 * kSweepCells - 1) / (128 * kSweepCells), g->nj + 2);
+        k_sg_predict<EN><<<grd4, blk, 0, s>>>(A);
+        k_sg_assemble<EN><<<grd4, blk, 0, s>>>(A);
         g->launches += 3;
         CTH_CUDA(cudaGetLastError());
         int rc, pend = 0;

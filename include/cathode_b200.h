@@ -849,6 +849,7 @@ int cth_mw_update_set_net(cth_mw_update* u, struct cth_unet* net);
  * assembly and the solve alone (E's unknowns written, nothing else: no ghosts,
  * no absorbed power, no rescale), so that the build happens before a timed run */
 int cth_mw_update_prepare(cth_mw_update* u, void* stream);
+int cth_mw_update_prepared(const cth_mw_update* u);   /* 1 once prepare (or a batch) built it */
 
 /* Two-port feed helpers (host) -------------------------------------------------
  * CmpMat2 (cmpMat2.hpp:8-34): 2x2 complex matrices, complex values as
