@@ -62,7 +62,7 @@ sys.path.insert(0, ROOT)
 METRIC = "steps/s at 512x1024 r-z: learned+mixed vs plain FP64 GPU at 1e-8 residual"
 UNIT = "steps/s"
 NI, NJ = 1024, 512
-TOL = 1e-10                 # the isolated linear systems (config 1: both to 1e-10)
+TOL = 1e-10                 # the isolated linear systems (both precisions to 1e-10)
 STEP_TOL = 1e-8             # the time step's 12 solves: the metric's residual (input/setup.yaml has 1e-10,
                             # timed too, as reference_tolerance)
 MAXIT = 30
@@ -376,7 +376,7 @@ def linear_systems(pkg, dev, stream, steps=10):
 
 # --------------------------------------------------------------------------
 def batched_sweep(pkg, device, rank, world, n=BATCH_N, steps=BATCH_STEPS):
-    """Config 2: n seeded discharges (grid sizes 64x128 .. 256x512, bias -10..60 V,
+    """The batched I-V sweep: n seeded discharges (grid sizes 64x128 .. 256x512, bias -10..60 V,
     microwave power 2..16 W), split over the ranks by cells x steps
     (batch.partition; one GPU per rank, no collective while they run), each
     rank's share advanced together by host worker threads with the autotuned
@@ -449,7 +449,7 @@ def batched_sweep(pkg, device, rank, world, n=BATCH_N, steps=BATCH_STEPS):
 
 
 def production(pkg, device, steps, warmup, ni=2048, nj=1024):
-    """Config 4 at bounded length: the seeded discharge scaled to 1024 (r) x 2048
+    """The production size at bounded length: the seeded discharge scaled to 1024 (r) x 2048
     (z) cells, the loop's microwave update every 100 steps, ``steps`` steps in
     plain FP64 (zero start) and in mixed precision with the previous-step warm
     start; steps/s by CUDA events, the anode ion current per step and its
@@ -503,7 +503,7 @@ def production(pkg, device, steps, warmup, ni=2048, nj=1024):
 
 
 def learned_microwave(pkg, device, runs, ni=512, nj=256, nsteps=120, ndiv=10, epochs=8):
-    """Config 3 for the microwave solve, bounded: snapshots from ``runs`` plain
+    """The learned warm start of the microwave solve at 256 (r) x 512 (z), bounded: snapshots from ``runs`` plain
     discharges (state seed, bias U(-10, 60) V, Pmw U(2, 16) W; update every
     ``ndiv`` steps for ``nsteps`` steps), training on the device (10 % of the
     snapshots held out), then held-out discharges: iterations to 1e-8 and solve
@@ -577,7 +577,7 @@ def main():
                          "update every 100 steps) in plain FP64 and in mixed precision with the previous-step warm "
                          "start, after --warmup steps each; prints one JSON line and exits")
     ap.add_argument("--learned-microwave", type=int, default=0,
-                    help="config-3 mode: train the microwave warm-start network on this many plain discharges at "
+                    help="learned-microwave mode: train the microwave warm-start network on this many plain discharges at "
                          "256 (r) x 512 (z) (microwave update every 10 steps) and report iterations to 1e-8 from "
                          "zero, the previous fields and the network's guess on held-out discharges; prints one JSON "
                          "line and exits")

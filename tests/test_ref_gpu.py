@@ -50,7 +50,7 @@ def test_dropin_runs_the_reference_time_step_on_gpu(pkg, orc, cuda_device, ref, 
     """Three whole steps of the reference's own loop body, once with every
     solver_SMG call (ions, potential, electron density and energy, neutrals) on
     the GPU through the header-only drop-in and once with the exact solve.  FP64:
-    within the north-star bar of 1e-8 rel-L2 (measured 4e-9: the solves stop at
+    within the parity bar of 1e-8 rel-L2 (measured 4e-9: the solves stop at
     1e-13 relative residual, and the Scharfetter-Gummel weights amplify the
     rest).  Mixed precision: every call converges to the same residual (no call
     reaches maxITR); Te within 1e-7 (measured 6.3e-8), the rest within 1e-8."""
@@ -71,7 +71,7 @@ def test_dropin_runs_the_reference_time_step_on_gpu(pkg, orc, cuda_device, ref, 
     norms = _norms(gpu.field, exact, m)
     print("drop-in", "mixed" if precision else "fp64", stats, {k: f"{v:.1e}" for k, v in norms.items()})
     assert stats["calls"] > 0 and stats["not_converged"] == 0, stats
-    # FP64: the north-star bar.  Mixed: every solve reaches the same 1e-13 residual;
+    # FP64: the parity bar.  Mixed: every solve reaches the same 1e-13 residual;
     # measured Te 6.3e-8, the other fields <= 4e-9
     for k, v in norms.items():
         assert v < (1e-7 if (precision == 1 and k == "Te") else 1e-8), (k, v)
