@@ -152,10 +152,12 @@ static void free_grid(cth_grid* g) {
     auto fr = [](void* p) { if (p) cudaFree(p); };
     fr(g->mask_full);
     for (auto p : g->mask) fr(p);
-    for (auto* v : {&g->h32.a, &g->h32.x, &g->h32.b, &g->h32.wS, &g->h32.wN, &g->h32.fac})
-        for (auto p : *v) fr(p);
-    for (auto* v : {&g->h64.a, &g->h64.x, &g->h64.b, &g->h64.wS, &g->h64.wN, &g->h64.fac})
-        for (auto p : *v) fr(p);
+    for (int k = 0; k < cth::kHier; k++) {
+        for (auto* v : {&g->h32[k].a, &g->h32[k].x, &g->h32[k].b, &g->h32[k].wS, &g->h32[k].wN, &g->h32[k].fac})
+            for (auto p : *v) fr(p);
+        for (auto* v : {&g->h64[k].a, &g->h64[k].x, &g->h64[k].b, &g->h64[k].wS, &g->h64[k].wN, &g->h64[k].fac})
+            for (auto p : *v) fr(p);
+    }
     for (auto* v : {&g->hc.a, &g->hc.x, &g->hc.b, &g->hc.wS, &g->hc.wN, &g->hc.fac})
         for (auto p : *v) fr(p);
     for (auto* v : {&g->hcf.a, &g->hcf.x, &g->hcf.b, &g->hcf.wS, &g->hcf.wN, &g->hcf.fac})
@@ -170,6 +172,7 @@ static void free_grid(cth_grid* g) {
     if (g->ws.h_args) cudaFreeHost(g->ws.h_args);
     fr(g->ws.d_args);
     fr(g->ws.counter);
+    fr(g->ws.slotstat);
     fr(g->c5.buf);
     fr(g->c5.sc);
     fr(g->c5.part);
@@ -177,10 +180,11 @@ static void free_grid(cth_grid* g) {
     fr(g->c5.cstage_ij);
     if (g->c5graph.exec) cudaGraphExecDestroy(g->c5graph.exec);
     if (g->c5graph.graph) cudaGraphDestroy(g->c5graph.graph);
-    for (auto& G : g->graphs) {
-        if (G.exec) cudaGraphExecDestroy(G.exec);
-        if (G.graph) cudaGraphDestroy(G.graph);
-    }
+    for (auto& row : g->graphs)
+        for (auto& G : row) {
+            if (G.exec) cudaGraphExecDestroy(G.exec);
+            if (G.graph) cudaGraphDestroy(G.graph);
+        }
     for (auto c : g->cap) if (c) cudaStreamDestroy(c);
     if (g->stream) cudaStreamDestroy(g->stream);
     for (auto e : g->prof.ev) cudaEventDestroy(e);
@@ -299,6 +303,11 @@ int cth_grid_create(int ni, int nj, const int* i_bl, const int* j_bl, int n_bl, 
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.d_args, sizeof(cth::SolveArgs)), "cudaMalloc args");
     if (rc == CTH_OK) chk(cudaMalloc(&g->ws.counter, 64), "cudaMalloc counter");
     if (rc == CTH_OK) chk(cth::zero_fill(g->ws.counter, 64), "memset counter");
+    {
+        const size_t nss = (2 * cth::kSlots * cth::kSlotWords + 1) * sizeof(double);
+        if (rc == CTH_OK) chk(cudaMalloc(&g->ws.slotstat, nss), "cudaMalloc slot words");
+        if (rc == CTH_OK) chk(cth::zero_fill(g->ws.slotstat, nss), "memset slot words");
+    }
     if (rc == CTH_OK) chk(cudaStreamCreateWithFlags(&g->cap[0], cudaStreamNonBlocking), "capture stream");
     if (rc == CTH_OK) chk(cudaStreamCreateWithFlags(&g->cap[1], cudaStreamNonBlocking), "capture stream");
     if (rc == CTH_OK) rc = configure_kernels(g);
@@ -366,10 +375,38 @@ int cth_grid_set_tail(cth_grid* g, int enable) {
         CTH_CUDA(cudaSetDevice(g->device));
         CTH_CUDA(cudaDeviceSynchronize());
         g->tail = enable != 0;
-        drop_graph(g->graphs[0]);
-        drop_graph(g->graphs[1]);
+        for (auto& row : g->graphs)
+            for (auto& G : row) drop_graph(G);
         drop_graph(g->c5graph);
     }
+    return CTH_OK;
+}
+
+int cth_grid_set_reuse(cth_grid* g, double tol, int slot) {
+    if (!g || !(tol >= 0.0) || slot < -1 || slot >= cth::kSlots) {
+        set_error("cth_grid_set_reuse: tolerance must be >= 0 and the slot in -1..14");
+        return CTH_ERR_ARG;
+    }
+    g->reuse_tol = tol;
+    g->api_slot = slot;
+    return CTH_OK;
+}
+
+int cth_grid_reuse_stats(cth_grid* g, int precision, int slot, double* out) {
+    if (!g || !out || slot < 0 || slot >= cth::kSlots || (precision != CTH_PREC_FP64 && precision != CTH_PREC_MIXED)) {
+        set_error("cth_grid_reuse_stats: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    CTH_CUDA(cudaDeviceSynchronize());
+    double w[cth::kSlotWords];
+    CTH_CUDA(cudaMemcpy(w, g->ws.slotstat + ((size_t)precision * cth::kSlots + slot) * cth::kSlotWords, sizeof(w),
+                        cudaMemcpyDeviceToHost));
+    out[0] = w[cth::SW_SETUPS];
+    out[1] = w[cth::SW_REUSES];
+    out[2] = w[cth::SW_CHANGE];
+    out[3] = w[cth::SW_LASTITER];
+    out[4] = w[cth::SW_RETRIES];
     return CTH_OK;
 }
 

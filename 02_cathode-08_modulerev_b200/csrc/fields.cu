@@ -271,7 +271,7 @@ int cth_fields_create(cth_grid* g, cth_fields** out) {
     if (cudaMalloc(&fs->part, fs->npart * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&fs->scal, CTH_FS_NSCAL * sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&fs->h_scal, CTH_FS_NSCAL * sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&fs->h_solve, 8 * 8 * sizeof(double)) != cudaSuccess) {
+        cudaMallocHost(&fs->h_solve, 8 * cth::kStatStride * sizeof(double)) != cudaSuccess) {
         if (fs->part) cudaFree(fs->part);
         if (fs->scal) cudaFree(fs->scal);
         delete fs;

@@ -118,6 +118,7 @@ struct SolveArgs {
     const double* x0;   // initial guess (null: zero, the reference's start)
     const double* x0b;  // second candidate (null: none); the better of the two is used
     double guess_tol;   // a guess is used when ||b - A x0|| <= guess_tol ||b|| (guess_tol <= 10)
+    double reuse_tol;   // hierarchy slots: largest row-relative operator change that keeps the hierarchy
 };
 
 // device status words of a solve (double array).  ST_GUESS: 0 no guess;
@@ -125,8 +126,32 @@ struct SolveArgs {
 // guesses rejected (r0 = relative residual of the used / the better guess)
 // ST_ASCALE, ST_XSCALE (device only): the powers of two that the working-precision
 // cycle's operator and right-hand side are scaled by (see k_prep0 / k_update).
+// ST_SETUP: 1 when this solve builds its hierarchy (before its cycles or after a
+// retry), 0 while it runs on a kept one.  ST_RETRY: 1 when a cycle on a kept
+// hierarchy reduced the residual by less than kRetryRate and the solve rebuilt
+// the hierarchy from its operator and went on from the current iterate.
 enum StatWord { ST_RR = 0, ST_RELRES = 1, ST_BB = 2, ST_NONFINITE = 3, ST_ITER = 4, ST_CONV = 5, ST_KEEP = 6,
-                ST_GUESS = 7, ST_ASCALE = 8, ST_XSCALE = 9 };
+                ST_GUESS = 7, ST_ASCALE = 8, ST_XSCALE = 9, ST_SETUP = 10, ST_RETRY = 11 };
+constexpr double kRetryRate = 0.5;
+
+// Hierarchy slots.  Hierarchy 0 serves the solves that build their hierarchy
+// every time (the reference's SMG set-up per solve); hierarchies 1..kSlots
+// belong to the slots 0..kSlots-1 of the solves that keep theirs while the
+// operator stays within a tolerance of the one it was built from.  Per slot and
+// precision the device keeps kSlotWords words (SlotWord).
+constexpr int kSlots = 15;
+constexpr int kHier = kSlots + 1;
+constexpr int kSlotWords = 8;
+// hierarchy slots of the time step's equations: one per operator that recurs
+// step after step (the predictor and the corrector of a predictor-corrector
+// iteration solve with the same operator and share a slot)
+enum EqSlot { SLOT_ION_MOMENTUM = 0, SLOT_ION_CONTINUITY = 1, SLOT_PHI = 2, SLOT_RHOE = 3, SLOT_EPS = 4,
+              SLOT_RHON = 5, SLOT_RHOM = 6 };
+// doubles between the pinned host status copies of concurrent solves (the copy
+// holds the words ST_RR..ST_RETRY)
+constexpr int kStatStride = 16;
+enum SlotWord { SW_VALID = 0, SW_ASCALE = 1, SW_SETUPS = 2, SW_REUSES = 3, SW_CHANGE = 4, SW_LASTCONV = 5,
+                SW_LASTITER = 6, SW_RETRIES = 7 };
 
 struct SolveGraph {
     bool valid = false;
@@ -134,6 +159,7 @@ struct SolveGraph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int n_pre = 0, n_body = 0, n_post = 0;  // kernels per section
+    int n_setup = 0;                        // kernels of the conditional set-up (hierarchy slots)
 };
 
 // complex 5-point solver workspace (level-0 layout, 14 complex planes)
@@ -159,6 +185,9 @@ struct Workspace {
     SolveArgs* d_args = nullptr;
     SolveArgs* h_args = nullptr;          // pinned
     unsigned int* counter = nullptr;      // last-block reduction counter
+    // 2 precisions x kSlots x kSlotWords slot words, then one word (as a 64-bit
+    // integer) for the largest operator change of the running solve
+    double* slotstat = nullptr;
 };
 
 }  // namespace cth
@@ -178,13 +207,16 @@ struct cth_grid {
     int bd = 32, ept = 1;      // line solve: threads per z-line / cells per thread (chunk)
     unsigned char* mask_full = nullptr;          // device layout
     std::vector<unsigned char*> mask;            // per level, level layout
-    cth::Hierarchy<float> h32;
-    cth::Hierarchy<double> h64;
+    cth::Hierarchy<float> h32[cth::kHier];   // [0]: rebuilt every solve; [1 + s]: slot s
+    cth::Hierarchy<double> h64[cth::kHier];
+    int cur = 0;               // hierarchy the host driver is working on
+    double reuse_tol = 0.0;    // > 0: solves given a slot keep their hierarchy (see kSlots)
+    int api_slot = -1;         // slot of the solves entered through the C ABI (-1: none)
     cth::Workspace ws;
     cudaStream_t stream = nullptr;
     long long launches = 0;    // kernels launched by this grid since creation
     cth::Profiler prof;
-    cth::SolveGraph graphs[2]; // per precision (CTH_PREC_FP64, CTH_PREC_MIXED)
+    cth::SolveGraph graphs[2][cth::kHier]; // per precision (CTH_PREC_FP64, CTH_PREC_MIXED) and hierarchy
     cth::C5Work c5;
     cth::Hierarchy<cth::cd> hc;    // complex hierarchy (preconditioner of the complex solves)
     cth::Hierarchy<cth::cf> hcf;   // its FP32 twin (mixed-precision preconditioner)
@@ -211,10 +243,13 @@ int smg_solve_dev(cth_grid* g, const double* aP, const double* aE, const double*
 // split form of smg_solve_dev: enqueue on s with the status copied to h_dst (pinned
 // host, 8 doubles; null = the grid's own), then either solve_finish (synchronise and
 // read the grid's copy) or, after the caller's own synchronisation, solve_parse(h_dst)
+// slot: hierarchy slot of the equation (0..kSlots-1; used when g->reuse_tol > 0),
+// -1: the C ABI's slot (g->api_slot), i.e. none unless the caller chose one.
 int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
                      const double* aS, const double* b, int maxITR, double error_cnv, int precision,
                      double* solution, cudaStream_t s, int* pending, double* h_dst,
-                     const double* x0 = nullptr, double guess_tol = 0.0, const double* x0b = nullptr);
+                     const double* x0 = nullptr, double guess_tol = 0.0, const double* x0b = nullptr,
+                     int slot = -1);
 int solve_finish(cth_grid* g, int pending, cth_status* st);
 int time_relax(cth_grid* g, int precision, int level, int reps, double* us, double* bytes);
 int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st);

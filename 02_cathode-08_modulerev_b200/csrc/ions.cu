@@ -503,18 +503,18 @@ static int ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_pa
         CTH_CUDA(cudaStreamWaitEvent(s2, fs->aux_event[0], 0));
         int pend[3] = {0, 0, 0};
         int rc = smg_solve_launch(gx, AX.aP, AX.aE, AX.aW, AX.aN, AX.aS, AX.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                                  prm->precision, A.Uix, s1, &pend[0], fs->h_solve + 0,
-                                  fs->warm_fields ? A.Uix : nullptr, fs->warm_tol);
+                                  prm->precision, A.Uix, s1, &pend[0], fs->h_solve + 0 * kStatStride,
+                                  fs->warm_fields ? A.Uix : nullptr, fs->warm_tol, nullptr, SLOT_ION_MOMENTUM);
         if (rc < 0) return rc;
         program(AX, CTH_ION_PROG_UIX_POST, A.Uix, A.Uix_old, s1);
         rc = smg_solve_launch(gr, AR.aP, AR.aE, AR.aW, AR.aN, AR.aS, AR.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                              prm->precision, A.Uir, s2, &pend[1], fs->h_solve + 8,
-                              fs->warm_fields ? A.Uir : nullptr, fs->warm_tol);
+                              prm->precision, A.Uir, s2, &pend[1], fs->h_solve + 1 * kStatStride,
+                              fs->warm_fields ? A.Uir : nullptr, fs->warm_tol, nullptr, SLOT_ION_MOMENTUM);
         if (rc < 0) return rc;
         program(AR, CTH_ION_PROG_UIR_POST, A.Uir, A.Uir_old, s2);
         rc = smg_solve_launch(g, AC.aP, AC.aE, AC.aW, AC.aN, AC.aS, AC.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                              prm->precision, A.Uip, s, &pend[2], fs->h_solve + 16,
-                              fs->warm_fields ? A.Uip : nullptr, fs->warm_tol);
+                              prm->precision, A.Uip, s, &pend[2], fs->h_solve + 2 * kStatStride,
+                              fs->warm_fields ? A.Uip : nullptr, fs->warm_tol, nullptr, SLOT_ION_MOMENTUM);
         if (rc < 0) return rc;
         program(AC, CTH_ION_PROG_UIP_POST, A.Uip, A.Uip_old, s);
         CTH_CUDA(cudaEventRecord(fs->aux_event[1], s1));
@@ -532,8 +532,9 @@ static int ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_pa
         if (solve(g, A.rhoi, 3) < 0) return CTH_ERR_CUDA;
     } else {
         const int rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                                        prm->precision, A.rhoi, s, &pend_m[3], fs->h_solve + 24,
-                                        fs->warm_fields ? A.rhoi : nullptr, fs->warm_tol);
+                                        prm->precision, A.rhoi, s, &pend_m[3], fs->h_solve + 3 * kStatStride,
+                                        fs->warm_fields ? A.rhoi : nullptr, fs->warm_tol, nullptr,
+                                        SLOT_ION_CONTINUITY);
         if (rc < 0) return rc;
     }
     k_rhoi_post<<<grd, blk, 0, s>>>(A);
@@ -556,7 +557,7 @@ static int ion_step(cth_fields* fs, cth_grid* gx, cth_grid* gr, const cth_ion_pa
     if (prm->flag_iter != 0) {
         cth_grid* gs[4] = {gx, gr, g, g};
         for (int c = 0; c < 4; c++) {
-            const int rc = solve_parse(gs[c], pend_m[c], fs->h_solve + 8 * c, &st[c]);
+            const int rc = solve_parse(gs[c], pend_m[c], fs->h_solve + kStatStride * c, &st[c]);
             if (rc < 0) return rc;
             if (rc > solver_rc) solver_rc = rc;
         }

@@ -305,8 +305,8 @@ static int update_neutrals(cth_fields* fs, const cth_neutral_params* prm, cudaSt
             if (rc > solver_rc) solver_rc = rc;
         } else {
             rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                                  prm->precision, x, s, &pend[k], fs->h_solve + 8 * k,
-                                  fs->warm_fields ? x : nullptr, fs->warm_tol);
+                                  prm->precision, x, s, &pend[k], fs->h_solve + kStatStride * k,
+                                  fs->warm_fields ? x : nullptr, fs->warm_tol, nullptr, SLOT_RHON + k);
         }
         return rc;
     };
@@ -337,7 +337,7 @@ static int update_neutrals(cth_fields* fs, const cth_neutral_params* prm, cudaSt
     CTH_CUDA(cudaStreamSynchronize(s));
     for (int k = 0; k < 2; k++) {
         if (!pend[k]) continue;
-        const int rc = solve_parse(g, pend[k], fs->h_solve + 8 * k, &st[k]);
+        const int rc = solve_parse(g, pend[k], fs->h_solve + kStatStride * k, &st[k]);
         if (rc < 0) return rc;
         if (rc > solver_rc) solver_rc = rc;
     }

@@ -373,7 +373,7 @@ int solve_phi_pc(cth_fields* fs, const cth_phi_params* prm, cudaStream_t s, cth_
             rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR_phi,
                                   prm->error_cnv_SOR_phi, prm->precision, A.dphi, s, &pend, fs->h_solve,
                                   ncount == 1 ? guess : nullptr, prm->guess_max_relres,
-                                  prm->warm_start == 1 ? dphi_prev : nullptr);
+                                  prm->warm_start == 1 ? dphi_prev : nullptr, SLOT_PHI);
         if (rc < 0) return rc;
         if (ncount == 1 && dphi_prev) {
             CTH_CUDA(cudaMemcpyAsync(dphi_prev2, dphi_prev, g->plane * sizeof(double), cudaMemcpyDeviceToDevice, s));

@@ -424,7 +424,8 @@ static int solve_sg_pc(cth_fields* fs, const cth_sg_params* prm, cudaStream_t s,
                                &st_last);
         else
             rc = smg_solve_launch(g, A.aP, A.aE, A.aW, A.aN, A.aS, A.b, prm->maxITR_SOR, prm->error_cnv_SOR,
-                                  prm->precision, A.d, s, &pend, fs->h_solve);
+                                  prm->precision, A.d, s, &pend, fs->h_solve, nullptr, 0.0, nullptr,
+                                  EN == 0 ? SLOT_RHOE : SLOT_EPS);
         if (rc < 0) return rc;
         k_sg_correct<EN><<<dim3((g->ni + 2 + 256 * kCorrCells - 1) / (256 * kCorrCells), g->nj + 2), 256, 0, s>>>(
             A, fs->part, g->ws.counter, out);

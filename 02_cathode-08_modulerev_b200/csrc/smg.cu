@@ -107,6 +107,12 @@ __global__ void k_guess(const SolveArgs* __restrict__ args, const unsigned char*
     }
 }
 
+// programmatic dependent launch: wait for the preceding kernel of the stream / graph
+// (a no-op when the kernel was launched without the attribute), and let the next
+// kernel start its own prologue
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // power of two 2^-e with |v| 2^-e in [1, 2); 1 for zero or non-finite v
 __device__ __forceinline__ double pow2_scale(double v) {
     return (isfinite(v) && v != 0.0) ? ldexp(1.0, -ilogb(v)) : 1.0;
@@ -115,12 +121,43 @@ __device__ __forceinline__ double pow2_scale(double v) {
 // cells per thread of k_prep0
 constexpr int PREP_CELLS = 4;
 
-template <typename T>
+// largest of the non-negative values v over the block, then over the grid into
+// *gmax (a double's bits as a 64-bit integer: for v >= 0 the integer order is the
+// numeric order, so the result does not depend on the order of the blocks)
+__device__ __forceinline__ void grid_max_nonneg(double v, double* red, unsigned long long* gmax) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) m = fmax(m, red[k]);
+        atomicMax(gmax, (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
+}
+
+// Preparation of a solve: the initial residual (from the chosen guess or zero),
+// the scaled first right-hand side b0, the statistics and the loop condition.
+// REUSE = false: also writes the scaled working-precision operator a0 of the
+// hierarchy, which the set-up that follows factorises.  REUSE = true (hierarchy
+// slots): a0 holds the operator the slot's hierarchy was built from; the kernel
+// measures the largest row-relative change max_m |a_m - a0_m| / |a_P| of the new
+// scaled operator against it and decides on the device whether the set-up runs
+// (stat[ST_SETUP], the conditional node cond_setup): when the slot is new, when
+// the slot's last solve did not converge, or when the change exceeds
+// args->reuse_tol.  The cycle then uses the
+// hierarchy of the kept operator as the preconditioner of the FP64 defect
+// correction, whose residuals and stopping rule use the caller's operator.
+template <typename T, bool REUSE>
 __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask,
                         int ld_u, int i0, int j0, int ncol, int nrow, int ldl, size_t qref, T* __restrict__ a0,
                         T* __restrict__ b0, double* __restrict__ x64, double* __restrict__ part,
                         unsigned int* counter, double* __restrict__ stat, cudaGraphConditionalHandle cond,
-                        int use_cond) {
+                        int use_cond, double* __restrict__ sst, unsigned long long* gmax,
+                        cudaGraphConditionalHandle cond_setup) {
     __shared__ double red[32];
     const int c0 = PREP_CELLS * (blockIdx.x * blockDim.x + threadIdx.x);
     const int r = blockIdx.y;
@@ -129,6 +166,7 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
     const bool guess = gw >= 1.0;
     const double* xg = (gw >= 100.0) ? args->x0b : args->x0;
     double v2[2] = {0.0, 0.0};  // ||r0||^2, ||b||^2
+    double dmax = 0.0;          // REUSE: largest row-relative change of this thread's cells
     // PREP_CELLS consecutive cells of row r per thread, their loads in flight together
 #pragma unroll
     for (int k = 0; k < PREP_CELLS; k++) {
@@ -157,13 +195,28 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
                 v2[0] += bv * bv;
             }
         }
-        a0[P * plane + p] = vP;
-        a0[W * plane + p] = vW;
-        a0[E * plane + p] = vE;
-        a0[S * plane + p] = vS;
-        a0[N * plane + p] = vN;
+        if constexpr (REUSE) {
+            if (mask[p]) {
+                const double oP = a0[P * plane + p], oW = a0[W * plane + p], oE = a0[E * plane + p];
+                const double oS = a0[S * plane + p], oN = a0[N * plane + p];
+                double d = fabs((double)vP - oP);
+                d = fmax(d, fabs((double)vW - oW));
+                d = fmax(d, fabs((double)vE - oE));
+                d = fmax(d, fabs((double)vS - oS));
+                d = fmax(d, fabs((double)vN - oN));
+                const double rel = d / fabs((double)vP);
+                dmax = fmax(dmax, (rel >= 0.0) ? rel : INFINITY);   // NaN counts as a change
+            }
+        } else {
+            a0[P * plane + p] = vP;
+            a0[W * plane + p] = vW;
+            a0[E * plane + p] = vE;
+            a0[S * plane + p] = vS;
+            a0[N * plane + p] = vN;
+        }
         b0[p] = vb;
     }
+    if constexpr (REUSE) grid_max_nonneg(dmax, red, gmax);
     double t2[2];
     if (last_block_sumk<2>(v2, part, counter, red, t2) && threadIdx.x == 0) {
         const double rr = t2[0], bb = t2[1];
@@ -181,7 +234,57 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
         stat[ST_KEEP] = keep ? 1.0 : 0.0;
         stat[ST_ASCALE] = sA;
         stat[ST_XSCALE] = 1.0;
+        stat[ST_SETUP] = 1.0;
+        stat[ST_RETRY] = 0.0;
         if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
+        if constexpr (REUSE) {
+            const double change = __longlong_as_double((long long)atomicExch(gmax, 0ull));
+            // the change compares the scaled operators, so a new power-of-two scale alone
+            // (both operators scaled to the same reference coefficient) keeps the hierarchy
+            const bool setup = sst[SW_VALID] == 0.0 || sst[SW_LASTCONV] == 0.0 || !(change <= args->reuse_tol);
+            stat[ST_SETUP] = setup ? 1.0 : 0.0;
+            if (setup) {
+                sst[SW_VALID] = 1.0;
+                sst[SW_ASCALE] = sA;
+                sst[SW_SETUPS] += 1.0;
+            } else {
+                sst[SW_REUSES] += 1.0;
+            }
+            sst[SW_CHANGE] = change;
+            if (use_cond) cudaGraphSetConditional(cond_setup, setup ? 1u : 0u);
+        }
+    }
+}
+
+// the scaled working-precision operator a0 of a slot's hierarchy, written when its
+// set-up runs (the same values k_prep0<T, false> writes)
+template <typename T>
+__global__ void k_prep_op(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask, int ld_u,
+                          int i0, int j0, int ncol, int nrow, int ldl, T* __restrict__ a0,
+                          const double* __restrict__ stat) {
+    const int c0 = PREP_CELLS * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int r = blockIdx.y;
+    const double sA = stat[ST_ASCALE];
+#pragma unroll
+    for (int k = 0; k < PREP_CELLS; k++) {
+        const int c = c0 + k;
+        if (c >= ncol) break;
+        const size_t plane = (size_t)nrow * ldl;
+        const size_t p = (size_t)r * ldl + c;
+        const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
+        T vP = T(1), vW = T(0), vE = T(0), vS = T(0), vN = T(0);
+        if (mask[p]) {
+            vP = (T)(args->aP[q] * sA);
+            if (c > 0 && mask[p - 1]) vW = (T)(args->aW[q] * sA);
+            if (c + 1 < ncol && mask[p + 1]) vE = (T)(args->aE[q] * sA);
+            if (r > 0 && mask[p - ldl]) vS = (T)(args->aS[q] * sA);
+            if (r + 1 < nrow && mask[p + ldl]) vN = (T)(args->aN[q] * sA);
+        }
+        a0[P * plane + p] = vP;
+        a0[W * plane + p] = vW;
+        a0[E * plane + p] = vE;
+        a0[S * plane + p] = vS;
+        a0[N * plane + p] = vN;
     }
 }
 
@@ -316,6 +419,9 @@ template <typename T, int NPT, int BND = 256>
 __global__ void __launch_bounds__(BND) k_factor(LevelArgs<T> L, const unsigned char* __restrict__ mask, T* __restrict__ fac,
                          T* __restrict__ wS, T* __restrict__ wN, int weights) {
     __shared__ T sh[(8 + LG_N) * 32];
+    // the level's operator comes from the preceding kernel (programmatic dependent launch)
+    griddep_wait();
+    griddep_launch();
     factor_row<T, NPT>(L, mask, fac, wS, wN, weights, blockIdx.x, sh);
 }
 
@@ -331,64 +437,87 @@ __device__ __forceinline__ T pw(const unsigned char* __restrict__ mask, const T*
 }
 
 // ---------------------------------------------------------------------------
-// Galerkin coarse operator: one thread per coarse cell.
+// Galerkin coarse operator R A P (R = P^T): one thread per coarse cell.
+// Launched with programmatic dependent launch after the factorisation of the
+// fine level, which writes the interpolation weights: the fine operator (made
+// by the kernel before that one) and the masks are loaded before the wait, the
+// weights after it.  The sums run in a fixed order (fine rows 2J-1, 2J, 2J+1,
+// stencil points, coarse rows), the same for every launch configuration.
 // ---------------------------------------------------------------------------
 template <typename T, int NPT>
-__device__ __forceinline__ void galerkin_cell(const LevelArgs<T>& F, const unsigned char* __restrict__ maskf,
-                                              const T* __restrict__ wS, const T* __restrict__ wN,
-                                              T* __restrict__ ac, int nrowc, const unsigned char* __restrict__ maskc,
-                                              int i, int J) {
+__global__ void k_galerkin(LevelArgs<T> F, const unsigned char* __restrict__ maskf,
+                           const T* __restrict__ wS, const T* __restrict__ wN, T* __restrict__ ac,
+                           int nrowc, const unsigned char* __restrict__ maskc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F.ncol) return;
+    const int J = blockIdx.y;
     const int ld = F.ld, ncol = F.ncol;
     const size_t plc = (size_t)nrowc * ld;
     const size_t q = (size_t)J * ld + i;
     const int oi[9] = {0, -1, 1, 0, 0, -1, 1, -1, 1};
     const int oj[9] = {0, 0, 0, -1, 1, -1, -1, 1, 1};
+    const bool active = maskc[q] != 0;
+    // A[gf - 1][k]: stencil point k of fine row f = 2J - 2 + gf (zero where the
+    // row or the neighbour lies outside the level)
+    T A[3][NPT];
+    // W[gg][ci][jj]: weight of fine point (2J - 2 + gg, i - 1 + ci) toward coarse
+    // row J - 1 + jj (P couples rows only: semicoarsening)
+    T W[5][3][3];
+#pragma unroll
+    for (int gg = 0; gg < 5; gg++)
+#pragma unroll
+        for (int ci = 0; ci < 3; ci++)
+#pragma unroll
+            for (int jj = 0; jj < 3; jj++) W[gg][ci][jj] = T(0);
+#pragma unroll
+    for (int gf = 1; gf <= 3; gf++) {
+        const int f = 2 * J - 2 + gf;
+        const size_t pf = (size_t)f * ld + i;
+#pragma unroll
+        for (int k = 0; k < NPT; k++) {
+            const int ii = i + oi[k], g = f + oj[k];
+            const bool in = active && f >= 0 && f < F.nrow && ii >= 0 && ii < ncol && g >= 0 && g < F.nrow;
+            A[gf - 1][k] = in ? F.a[k * F.plane + pf] : T(0);
+        }
+    }
+#pragma unroll
+    for (int gg = 0; gg < 5; gg += 2) {
+        const int g = 2 * J - 2 + gg;
+#pragma unroll
+        for (int ci = 0; ci < 3; ci++) {
+            const int ii = i - 1 + ci;
+            if (active && g >= 0 && g < F.nrow && ii >= 0 && ii < ncol)
+                W[gg][ci][gg / 2] = maskf[(size_t)g * ld + ii] ? T(1) : T(0);
+        }
+    }
+    griddep_wait();
+    griddep_launch();
+#pragma unroll
+    for (int gg = 1; gg < 5; gg += 2) {
+        const int g = 2 * J - 2 + gg;
+#pragma unroll
+        for (int ci = 0; ci < 3; ci++) {
+            const int ii = i - 1 + ci;
+            if (active && g >= 0 && g < F.nrow && ii >= 0 && ii < ncol) {
+                const size_t pp = (size_t)g * ld + ii;
+                W[gg][ci][(gg - 1) / 2] = wS[pp];
+                W[gg][ci][(gg + 1) / 2] = wN[pp];
+            }
+        }
+    }
     T acc[3][3];
 #pragma unroll
     for (int u = 0; u < 3; u++)
 #pragma unroll
         for (int v = 0; v < 3; v++) acc[u][v] = T(0);
-    const bool active = maskc[q] != 0;
     if (active) {
-        // interpolation weights of the fine points (2J-2+gg, i-1+ci) toward the
-        // coarse rows J-1+jj, gathered once (P couples rows only: semicoarsening)
-        T W[5][3][3];
-#pragma unroll
-        for (int gg = 0; gg < 5; gg++)
-#pragma unroll
-            for (int ci = 0; ci < 3; ci++)
-#pragma unroll
-                for (int jj = 0; jj < 3; jj++) W[gg][ci][jj] = T(0);
-#pragma unroll
-        for (int gg = 0; gg < 5; gg++) {
-            const int g = 2 * J - 2 + gg;
-            if (g < 0 || g >= F.nrow) continue;
-#pragma unroll
-            for (int ci = 0; ci < 3; ci++) {
-                const int ii = i - 1 + ci;
-                if (ii < 0 || ii >= ncol) continue;
-                const size_t pp = (size_t)g * ld + ii;
-                if ((gg & 1) == 0) {
-                    W[gg][ci][gg / 2] = maskf[pp] ? T(1) : T(0);
-                } else {
-                    W[gg][ci][(gg - 1) / 2] = wS[pp];
-                    W[gg][ci][(gg + 1) / 2] = wN[pp];
-                }
-            }
-        }
-        const int c = 2 * J;
 #pragma unroll
         for (int gf = 1; gf <= 3; gf++) {
-            const int f = c - 2 + gf;
-            if (f < 0 || f >= F.nrow) continue;
             const T rw = W[gf][1][1];
             if (rw == T(0)) continue;
-            const size_t pf = (size_t)f * ld + i;
 #pragma unroll
             for (int k = 0; k < NPT; k++) {
-                const int ii = i + oi[k], g = f + oj[k];
-                if (ii < 0 || ii >= ncol || g < 0 || g >= F.nrow) continue;
-                const T av = F.a[k * F.plane + pf];
+                const T av = A[gf - 1][k];
                 if (av == T(0)) continue;
                 const T mv = (k == P) ? av : -av;
 #pragma unroll
@@ -412,15 +541,6 @@ __device__ __forceinline__ void galerkin_cell(const LevelArgs<T>& F, const unsig
         const T v = acc[oj[k] + 1][oi[k] + 1];
         ac[k * plc + q] = (k == P) ? v : -v;
     }
-}
-
-template <typename T, int NPT>
-__global__ void k_galerkin(LevelArgs<T> F, const unsigned char* __restrict__ maskf,
-                           const T* __restrict__ wS, const T* __restrict__ wN, T* __restrict__ ac,
-                           int nrowc, const unsigned char* __restrict__ maskc) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= F.ncol) return;
-    galerkin_cell<T, NPT>(F, maskf, wS, wN, ac, nrowc, maskc, i, blockIdx.y);
 }
 
 
@@ -580,11 +700,6 @@ __device__ __forceinline__ void resid4(const LevelArgs<T>& F, int f, int s0, T r
 //   NPTF > 0:   (with zero_guess, C rows) the right-hand side is the residual
 //               of the finer level F restricted on the fly (its C rows 2j and
 //               2j+2), stored into this level's b for rows j and j+1.
-// programmatic dependent launch: wait for the preceding kernel of the stream / graph
-// (a no-op when the kernel was launched without the attribute), and let the next
-// kernel start its own prologue
-__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // The coefficients of a level are never written inside a cycle, so they are read
 // before the wait; b, the restricted residual and x come from earlier kernels of
@@ -794,7 +909,8 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
                          double* __restrict__ x64a, double* __restrict__ x64b,
                          const T* __restrict__ e, T* __restrict__ b0, double* __restrict__ part,
                          unsigned int* counter, double* __restrict__ stat,
-                         cudaGraphConditionalHandle cond, int use_cond) {
+                         cudaGraphConditionalHandle cond, int use_cond, double* __restrict__ sst,
+                         cudaGraphConditionalHandle cond_rs, cudaGraphConditionalHandle cond2) {
     __shared__ double red[32];
     const int it = (int)stat[ST_ITER] + 1;
     const double* __restrict__ xin = (it & 1) ? x64a : x64b;
@@ -845,6 +961,10 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
         const bool fin = isfinite(tot);
         const bool conv = fin && rel < args->tol;
         const bool keep = fin && !conv && it < args->maxit;
+        // a hierarchy slot's first loop (sst): a cycle on the kept hierarchy that
+        // reduced the residual by less than kRetryRate ends the loop; the solve
+        // rebuilds the hierarchy from its operator and continues in a second loop
+        const bool retry = sst && keep && stat[ST_SETUP] == 0.0 && !(tot <= kRetryRate * kRetryRate * stat[ST_RR]);
         stat[ST_RR] = tot;
         stat[ST_RELRES] = rel;
         stat[ST_NONFINITE] = fin ? 0.0 : 1.0;
@@ -852,7 +972,19 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
         stat[ST_CONV] = conv ? 1.0 : 0.0;
         stat[ST_KEEP] = keep ? 1.0 : 0.0;
         stat[ST_XSCALE] = xs;
-        if (use_cond) cudaGraphSetConditional(cond, keep ? 1u : 0u);
+        if (retry) {
+            stat[ST_SETUP] = 1.0;
+            stat[ST_RETRY] = 1.0;
+            sst[SW_SETUPS] += 1.0;
+            sst[SW_RETRIES] += 1.0;
+        }
+        if (use_cond) {
+            cudaGraphSetConditional(cond, (keep && !retry) ? 1u : 0u);
+            if (retry) {
+                cudaGraphSetConditional(cond_rs, 1u);
+                cudaGraphSetConditional(cond2, 1u);
+            }
+        }
     }
 }
 
@@ -860,9 +992,13 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
 __global__ void k_store(const SolveArgs* __restrict__ args, const double* __restrict__ x64a,
                         const double* __restrict__ x64b, const double* __restrict__ stat,
                         const unsigned char* __restrict__ mask, int ncol, int nrow, int ldl,
-                        int ld_u, int i0, int j0) {
+                        int ld_u, int i0, int j0, double* __restrict__ sst) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
+    if (sst && c == 0 && r == 0) {   // the slot's record of its last solve
+        sst[SW_LASTCONV] = stat[ST_CONV];
+        sst[SW_LASTITER] = stat[ST_ITER];
+    }
     if (c >= ncol) return;
     const int it = (int)stat[ST_ITER];
     const double* __restrict__ x = (it & 1) ? x64b : x64a;
@@ -876,9 +1012,9 @@ __global__ void k_store(const SolveArgs* __restrict__ args, const double* __rest
 template <typename T>
 static Hierarchy<T>& hier(cth_grid* g);
 template <>
-Hierarchy<float>& hier<float>(cth_grid* g) { return g->h32; }
+Hierarchy<float>& hier<float>(cth_grid* g) { return g->h32[g->cur]; }
 template <>
-Hierarchy<double>& hier<double>(cth_grid* g) { return g->h64; }
+Hierarchy<double>& hier<double>(cth_grid* g) { return g->h64[g->cur]; }
 template <>
 Hierarchy<cd>& hier<cd>(cth_grid* g) { return g->hc; }
 template <>
@@ -1071,6 +1207,41 @@ static void vcycle(cth_grid* g, int l, cudaStream_t s) {
     }
 }
 
+// launch of a kernel that calls griddep_wait() before it reads what the kernels
+// before it wrote: with programmatic dependent launch when the grid uses it
+template <typename... KArgs, typename... Args>
+static void launch_dep(cth_grid* g, void (*kern)(KArgs...), dim3 grd, dim3 blk, cudaStream_t s, Args... args) {
+    if (g->pdl) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grd;
+        cfg.blockDim = blk;
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, kern, args...);
+    } else {
+        kern<<<grd, blk, 0, s>>>(args...);
+    }
+    g->launches++;
+}
+
+// Galerkin operator of level l + 1 from level l
+template <typename T>
+static void galerkin(cth_grid* g, int l, const LevelArgs<T>& L, cudaStream_t s) {
+    Hierarchy<T>& h = hier<T>(g);
+    const dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
+    if (l == 0)
+        launch_dep(g, k_galerkin<T, 5>, grd, blk, s, L, (const unsigned char*)g->mask[l], (const T*)h.wS[l],
+                   (const T*)h.wN[l], h.a[l + 1], g->nrow[l + 1], (const unsigned char*)g->mask[l + 1]);
+    else
+        launch_dep(g, k_galerkin<T, 9>, grd, blk, s, L, (const unsigned char*)g->mask[l], (const T*)h.wS[l],
+                   (const T*)h.wN[l], h.a[l + 1], g->nrow[l + 1], (const unsigned char*)g->mask[l + 1]);
+}
+
 template <typename T>
 static void setup_levels(cth_grid* g, cudaStream_t s) {
     Hierarchy<T>& h = hier<T>(g);
@@ -1085,17 +1256,9 @@ static void setup_levels(cth_grid* g, cudaStream_t s) {
                                                                                       : k_factor<T, 5, 256>)
                              : (g->bnd == 1024 ? k_factor<T, 9, 1024> : g->bnd == 512 ? k_factor<T, 9, 512>
                                                                                       : k_factor<T, 9, 256>);
-            kf<<<g->nrow[l], g->bd, 0, s>>>(L, g->mask[l], h.fac[l], h.wS[l], h.wN[l], wts);
-            g->launches++;
+            launch_dep(g, kf, dim3(g->nrow[l]), dim3(g->bd), s, L, g->mask[l], h.fac[l], h.wS[l], h.wN[l], wts);
             if (!wts) break;
-            dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
-            if (l == 0)
-                k_galerkin<T, 5><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
-                                                     g->nrow[l + 1], g->mask[l + 1]);
-            else
-                k_galerkin<T, 9><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
-                                                     g->nrow[l + 1], g->mask[l + 1]);
-            g->launches++;
+            galerkin<T>(g, l, L, s);
         }
     } else {
         for (int l = 0; l + 1 < g->nlev; l++) {
@@ -1110,14 +1273,7 @@ static void setup_levels(cth_grid* g, cudaStream_t s) {
                 kw<<<frows, g->bd, smem, s>>>(L, g->mask[l], h.wS[l], h.wN[l]);
                 g->launches++;
             }
-            dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
-            if (l == 0)
-                k_galerkin<T, 5><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
-                                                     g->nrow[l + 1], g->mask[l + 1]);
-            else
-                k_galerkin<T, 9><<<grd, blk, 0, s>>>(L, g->mask[l], h.wS[l], h.wN[l], h.a[l + 1],
-                                                     g->nrow[l + 1], g->mask[l + 1]);
-            g->launches++;
+            galerkin<T>(g, l, L, s);
         }
     }
     prof_done(g, slot, s);
@@ -1125,18 +1281,28 @@ static void setup_levels(cth_grid* g, cudaStream_t s) {
 
 // kernel sequence of one solve, split into the part before the cycle loop,
 // one loop iteration, and the part after it; each returns its kernel count
+// sst: the slot words of a hierarchy slot (null: the set-up runs in this part)
 template <typename T>
-static int enqueue_pre(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle cond, int use_cond) {
+static int enqueue_pre(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle cond, int use_cond,
+                       double* sst = nullptr, cudaGraphConditionalHandle cond_setup = 0) {
     Hierarchy<T>& h = hier<T>(g);
     Workspace& w = g->ws;
     const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
     dim3 blk(256), grd((ncol + 255) / 256, nrow0);
     dim3 grdp((ncol + 256 * PREP_CELLS - 1) / (256 * PREP_CELLS), nrow0);
+    unsigned long long* gmax = reinterpret_cast<unsigned long long*>(w.slotstat + 2 * kSlots * kSlotWords);
     cudaMemsetAsync(w.x64[0], 0, sizeof(double) * (size_t)nrow0 * ldl, s);
     k_guess<<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, w.part, w.counter,
                                 w.stat);
-    k_prep0<T><<<grdp, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, g->qref, h.a[0],
-                                   h.b[0], w.x64[0], w.part, w.counter, w.stat, cond, use_cond);
+    if (sst) {
+        k_prep0<T, true><<<grdp, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, g->qref,
+                                              h.a[0], h.b[0], w.x64[0], w.part, w.counter, w.stat, cond, use_cond,
+                                              sst, gmax, cond_setup);
+        return 2;
+    }
+    k_prep0<T, false><<<grdp, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, g->qref,
+                                           h.a[0], h.b[0], w.x64[0], w.part, w.counter, w.stat, cond, use_cond,
+                                           nullptr, gmax, 0);
     const long long l0 = g->launches;
     setup_levels<T>(g, s);
     const int n = 2 + (int)(g->launches - l0);
@@ -1144,8 +1310,27 @@ static int enqueue_pre(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle c
     return n;
 }
 
+// the set-up of a slot's hierarchy (run when k_prep0<T, true> decided so)
 template <typename T>
-static int enqueue_body(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle cond, int use_cond) {
+static int enqueue_setup(cth_grid* g, cudaStream_t s) {
+    Hierarchy<T>& h = hier<T>(g);
+    Workspace& w = g->ws;
+    const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
+    dim3 blk(256), grdp((ncol + 256 * PREP_CELLS - 1) / (256 * PREP_CELLS), nrow0);
+    k_prep_op<T><<<grdp, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, h.a[0], w.stat);
+    const long long l0 = g->launches;
+    setup_levels<T>(g, s);
+    const int n = 1 + (int)(g->launches - l0);
+    g->launches = l0;
+    return n;
+}
+
+// sst (a slot's first loop): the cycle may end the loop for a rebuild (k_update,
+// handles cond_rs / cond2 of the rebuild and the second loop)
+template <typename T>
+static int enqueue_body(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle cond, int use_cond,
+                        double* sst = nullptr, cudaGraphConditionalHandle cond_rs = 0,
+                        cudaGraphConditionalHandle cond2 = 0) {
     Hierarchy<T>& h = hier<T>(g);
     Workspace& w = g->ws;
     const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
@@ -1154,24 +1339,57 @@ static int enqueue_body(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle 
     vcycle<T>(g, 0, s);
     const int slot = prof_mark(g, PROF_UPDATE, (double)nrow0 * ncol * (8.0 * 8.0 + 2.0 * sizeof(T) + 1.0), s);
     k_update<T><<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, w.x64[0],
-                                    w.x64[1], h.x[0], h.b[0], w.part, w.counter, w.stat, cond, use_cond);
+                                    w.x64[1], h.x[0], h.b[0], w.part, w.counter, w.stat, cond, use_cond, sst,
+                                    cond_rs, cond2);
     prof_done(g, slot, s);
     const int n = 1 + (int)(g->launches - l0);
     g->launches = l0;
     return n;
 }
 
-static int enqueue_post(cth_grid* g, cudaStream_t s) {
+static int enqueue_post(cth_grid* g, cudaStream_t s, double* sst = nullptr) {
     Workspace& w = g->ws;
     dim3 blk(256), grd((g->ncol + 255) / 256, g->nrow[0]);
     k_store<<<grd, blk, 0, s>>>(w.d_args, w.x64[0], w.x64[1], w.stat, g->mask[0], g->ncol, g->nrow[0],
-                                g->ldl, g->ld, g->i0, g->j0);
+                                g->ldl, g->ld, g->i0, g->j0, sst);
     return 1;
 }
 
-// capture the whole solve as one graph: pre -> while(keep){ body } -> post
+// a conditional node (IF or WHILE on handle c) after the current capture
+// dependencies of cs, its body captured from cs2 by fill(cs2); cs then continues
+// after the node
+template <typename F>
+static cudaError_t capture_conditional(cudaStream_t cs, cudaStream_t cs2, cudaGraphConditionalHandle c,
+                                       cudaGraphConditionalNodeType type, F fill) {
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps);
+    cudaGraphNode_t cnode = nullptr;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = c;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, deps, ndeps, &cp);
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(cs2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            fill(cs2);
+            cudaGraph_t bout = nullptr;
+            e = cudaStreamEndCapture(cs2, &bout);
+        }
+    }
+    return e;
+}
+
+// capture the whole solve as one graph: pre -> while(keep){ body } -> post; with
+// a hierarchy slot (sst): pre -> if(setup){ set-up } -> while(keep){ body } -> post
 template <typename T>
-static int build_graph(cth_grid* g, SolveGraph& G) {
+static int build_graph(cth_grid* g, SolveGraph& G, double* sst) {
     if (G.valid && G.nu1 == g->nu1 && G.nu2 == g->nu2) return CTH_OK;
     if (G.exec) { cudaGraphExecDestroy(G.exec); G.exec = nullptr; }
     if (G.graph) { cudaGraphDestroy(G.graph); G.graph = nullptr; }
@@ -1180,37 +1398,37 @@ static int build_graph(cth_grid* g, SolveGraph& G) {
     CTH_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
     cudaStreamCaptureStatus cst;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    cudaError_t e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps);
-    cudaGraphConditionalHandle cond = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, nullptr, nullptr);
+    cudaGraphConditionalHandle cond = 0, cond_setup = 0;
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess && sst)
+        e = cudaGraphConditionalHandleCreate(&cond_setup, graph, 1, cudaGraphCondAssignDefault);
     if (e != cudaSuccess) {
         cudaGraph_t junk;
         cudaStreamEndCapture(cs, &junk);
         if (junk) cudaGraphDestroy(junk);
         return cuda_fail(e, "graph conditional handle");
     }
-    G.n_pre = enqueue_pre<T>(g, cs, cond, 1);
-    e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps);
-    cudaGraphNode_t cnode = nullptr;
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = cond;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    if (e == cudaSuccess) e = cudaGraphAddNode(&cnode, graph, deps, ndeps, &cp);
-    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies);
-    if (e == cudaSuccess) {
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        e = cudaStreamBeginCaptureToGraph(cs2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            G.n_body = enqueue_body<T>(g, cs2, cond, 1);
-            cudaGraph_t bout = nullptr;
-            e = cudaStreamEndCapture(cs2, &bout);
-        }
-    }
-    if (e == cudaSuccess) G.n_post = enqueue_post(g, cs);
+    cudaGraphConditionalHandle cond_rs = 0, cond2 = 0;
+    if (e == cudaSuccess && sst) e = cudaGraphConditionalHandleCreate(&cond_rs, graph, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess && sst) e = cudaGraphConditionalHandleCreate(&cond2, graph, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) G.n_pre = enqueue_pre<T>(g, cs, cond, 1, sst, cond_setup);
+    G.n_setup = 0;
+    if (e == cudaSuccess && sst)
+        e = capture_conditional(cs, cs2, cond_setup, cudaGraphCondTypeIf,
+                                [&](cudaStream_t st) { G.n_setup = enqueue_setup<T>(g, st); });
+    if (e == cudaSuccess)
+        e = capture_conditional(cs, cs2, cond, cudaGraphCondTypeWhile, [&](cudaStream_t st) {
+            G.n_body = enqueue_body<T>(g, st, cond, 1, sst, cond_rs, cond2);
+        });
+    // a slot's rebuild after a slow cycle on the kept hierarchy, and the second loop
+    if (e == cudaSuccess && sst)
+        e = capture_conditional(cs, cs2, cond_rs, cudaGraphCondTypeIf,
+                                [&](cudaStream_t st) { enqueue_setup<T>(g, st); });
+    if (e == cudaSuccess && sst)
+        e = capture_conditional(cs, cs2, cond2, cudaGraphCondTypeWhile,
+                                [&](cudaStream_t st) { enqueue_body<T>(g, st, cond2, 1); });
+    if (e == cudaSuccess) G.n_post = enqueue_post(g, cs, sst);
     cudaGraph_t out = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(cs, &out);
     if (e == cudaSuccess) e = e2;
@@ -1235,12 +1453,16 @@ static int build_graph(cth_grid* g, SolveGraph& G) {
 // the host may enqueue the next solve on the same grid before this one has run
 __global__ void k_set_args(SolveArgs a, SolveArgs* dst) { *dst = a; }
 
+// words of the device status copied to the host after a solve
+constexpr int kStatCopy = ST_RETRY + 1;
+
 template <typename T>
-static int solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW,
-                        const double* aN, const double* aS, const double* b, int maxITR,
-                        double tol, double* solution, cudaStream_t s, int prec, int* pending,
-                        double* h_dst, const double* x0, double guess_tol, const double* x0b) {
+static int solve_launch_h(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                          const double* aN, const double* aS, const double* b, int maxITR,
+                          double tol, double* solution, cudaStream_t s, int prec, int* pending,
+                          double* h_dst, const double* x0, double guess_tol, const double* x0b, int slot) {
     *pending = 0;
+    const bool reuse = slot >= 0;
     int rc = alloc_hierarchy<T>(g);
     if (rc != CTH_OK) return rc;
     Workspace& w = g->ws;
@@ -1251,6 +1473,7 @@ static int solve_launch(cth_grid* g, const double* aP, const double* aE, const d
             return CTH_ERR_ALLOC;
         }
     }
+    double* sst = reuse ? w.slotstat + ((size_t)prec * kSlots + slot) * kSlotWords : nullptr;
     SolveArgs* ha = w.h_args;
     ha->aP = aP; ha->aE = aE; ha->aW = aW; ha->aN = aN; ha->aS = aS; ha->b = b;
     ha->solution = solution;
@@ -1259,38 +1482,63 @@ static int solve_launch(cth_grid* g, const double* aP, const double* aE, const d
     ha->x0 = x0;
     ha->x0b = x0 ? x0b : nullptr;
     ha->guess_tol = guess_tol;
+    ha->reuse_tol = g->reuse_tol;
     k_set_args<<<1, 1, 0, s>>>(*ha, w.d_args);
     const bool graph = g->use_graphs && !g->prof.on;
     if (graph) {
-        SolveGraph& G = g->graphs[prec];
-        rc = build_graph<T>(g, G);
+        SolveGraph& G = g->graphs[prec][g->cur];
+        rc = build_graph<T>(g, G, sst);
         if (rc != CTH_OK) return rc;
         CTH_CUDA(cudaGraphLaunch(G.exec, s));
-        CTH_CUDA(cudaMemcpyAsync(h_dst ? h_dst : w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CTH_CUDA(cudaMemcpyAsync(h_dst ? h_dst : w.h_stat, w.stat, kStatCopy * sizeof(double),
+                                 cudaMemcpyDeviceToHost, s));
         g->pending_stream = s;
-        *pending = 1 + prec;
+        *pending = 1 + prec + 2 * g->cur;
         return CTH_OK;
     }
-    g->launches += enqueue_pre<T>(g, s, 0, 0);
-    CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    g->launches += enqueue_pre<T>(g, s, 0, 0, sst);
+    CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, kStatCopy * sizeof(double), cudaMemcpyDeviceToHost, s));
     CTH_CUDA(cudaStreamSynchronize(s));
+    if (sst && w.h_stat[ST_SETUP] != 0.0) g->launches += enqueue_setup<T>(g, s);
+    bool retried = false;
     while (w.h_stat[ST_KEEP] != 0.0) {
-        g->launches += enqueue_body<T>(g, s, 0, 0);
-        CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (sst && !retried && w.h_stat[ST_RETRY] != 0.0) {
+            g->launches += enqueue_setup<T>(g, s);
+            retried = true;
+        }
+        g->launches += enqueue_body<T>(g, s, 0, 0, retried ? nullptr : sst);
+        CTH_CUDA(cudaMemcpyAsync(w.h_stat, w.stat, kStatCopy * sizeof(double), cudaMemcpyDeviceToHost, s));
         CTH_CUDA(cudaStreamSynchronize(s));
     }
-    g->launches += enqueue_post(g, s);
+    g->launches += enqueue_post(g, s, sst);
     CTH_CUDA(cudaGetLastError());
     CTH_CUDA(cudaStreamSynchronize(s));
     prof_collect(g);
-    if (h_dst) std::memcpy(h_dst, w.h_stat, 8 * sizeof(double));
+    if (h_dst) std::memcpy(h_dst, w.h_stat, kStatCopy * sizeof(double));
     return CTH_OK;
+}
+
+// the solve on hierarchy 0 (set up every solve) or on the hierarchy of a slot
+template <typename T>
+static int solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW,
+                        const double* aN, const double* aS, const double* b, int maxITR,
+                        double tol, double* solution, cudaStream_t s, int prec, int* pending,
+                        double* h_dst, const double* x0, double guess_tol, const double* x0b, int slot) {
+    const int sl = (g->reuse_tol > 0.0 && slot >= 0 && slot < kSlots) ? slot : -1;
+    g->cur = sl >= 0 ? 1 + sl : 0;
+    const int rc = solve_launch_h<T>(g, aP, aE, aW, aN, aS, b, maxITR, tol, solution, s, prec, pending, h_dst, x0,
+                                     guess_tol, x0b, sl);
+    g->cur = 0;
+    return rc;
 }
 
 int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st) {
     if (pending) {
-        const SolveGraph& G = g->graphs[pending - 1];
-        g->launches += G.n_pre + (long long)G.n_body * (long long)h[ST_ITER] + G.n_post;
+        const SolveGraph& G = g->graphs[(pending - 1) & 1][(pending - 1) >> 1];
+        // a slot's set-up runs once when ST_SETUP is set: before the cycles, or after
+        // the first loop when a cycle on the kept hierarchy was slow (ST_RETRY)
+        g->launches += G.n_pre + (h[ST_SETUP] != 0.0 ? G.n_setup : 0) + (long long)G.n_body * (long long)h[ST_ITER] +
+                       G.n_post;
     }
     CTH_CUDA(cudaGetLastError());
     cth_status loc{};
@@ -1315,17 +1563,18 @@ int solve_finish(cth_grid* g, int pending, cth_status* st) {
 int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const double* aW, const double* aN,
                      const double* aS, const double* b, int maxITR, double error_cnv, int precision,
                      double* solution, cudaStream_t s, int* pending, double* h_dst, const double* x0,
-                     double guess_tol, const double* x0b) {
+                     double guess_tol, const double* x0b, int slot) {
+    if (slot < 0) slot = g->api_slot;
     if (x0 && !(guess_tol >= 0.0 && guess_tol <= 10.0)) {
         set_error("initial-guess threshold must be in [0, 10]");
         return CTH_ERR_ARG;
     }
     if (precision == CTH_PREC_MIXED)
         return solve_launch<float>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending,
-                                   h_dst, x0, guess_tol, x0b);
+                                   h_dst, x0, guess_tol, x0b, slot);
     if (precision == CTH_PREC_FP64)
         return solve_launch<double>(g, aP, aE, aW, aN, aS, b, maxITR, error_cnv, solution, s, precision, pending,
-                                    h_dst, x0, guess_tol, x0b);
+                                    h_dst, x0, guess_tol, x0b, slot);
     set_error("unknown precision mode");
     return CTH_ERR_ARG;
 }
@@ -1485,8 +1734,25 @@ int time_relax(cth_grid* g, int precision, int level, int reps, double* us, doub
         set_error("cth_grid_time_relax: level or repetitions out of range");
         return CTH_ERR_ARG;
     }
-    if (precision == CTH_PREC_MIXED) return time_relax_impl<float>(g, level, reps, us, bytes);
-    if (precision == CTH_PREC_FP64) return time_relax_impl<double>(g, level, reps, us, bytes);
+    // the first hierarchy of the precision that a solve has built (slot hierarchies included)
+    auto first = [&](auto* hs) {
+        for (int k = 0; k < kHier; k++)
+            if (hs[k].allocated) return k;
+        return 0;
+    };
+    int rc;
+    if (precision == CTH_PREC_MIXED) {
+        g->cur = first(g->h32);
+        rc = time_relax_impl<float>(g, level, reps, us, bytes);
+        g->cur = 0;
+        return rc;
+    }
+    if (precision == CTH_PREC_FP64) {
+        g->cur = first(g->h64);
+        rc = time_relax_impl<double>(g, level, reps, us, bytes);
+        g->cur = 0;
+        return rc;
+    }
     set_error("unknown precision mode");
     return CTH_ERR_ARG;
 }

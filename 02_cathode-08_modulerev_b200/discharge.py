@@ -99,10 +99,12 @@ class RectangleDischarge:
     """The seeded discharge of workloads.discharge_state / discharge_params on the
     ni (z) x nj (r) rectangle with its microwave update every ``ndiv_mw`` steps.
     precision: CTH_PREC_MIXED or CTH_PREC_FP64 for every inner solve; tol /
-    maxit override the inner solves' stopping rule when given."""
+    maxit override the inner solves' stopping rule when given; reuse_tol > 0
+    keeps each equation's multigrid hierarchy while its operator changes by at
+    most that much (Grid.set_reuse on the three grids)."""
 
     def __init__(self, pkg, ni, nj, seed=0, device=0, precision=capi.CTH_PREC_MIXED, tol=None, maxit=None,
-                 ndiv_mw=100, Pmw=8.0, mw_tol=1e-10, mw_maxit=400, V_bias=None):
+                 ndiv_mw=100, Pmw=8.0, mw_tol=1e-10, mw_maxit=400, V_bias=None, reuse_tol=0.0):
         self.ni, self.nj, self.ndiv_mw, self.mw_tol, self.mw_maxit = ni, nj, ndiv_mw, mw_tol, mw_maxit
         geo = pkg.fluid.rectangle_geometry(ni, nj, width_neutIn=2.03e-3)
         ds = pkg.workloads.discharge_state(ni, nj, seed=seed)
@@ -114,6 +116,8 @@ class RectangleDischarge:
         self.g = Grid(ni, nj, geo["ib"], geo["jb"], device=device)
         self.gx = Grid(ni, nj, geo["fxi"], geo["fxj"], device=device)
         self.gr = Grid(ni, nj, geo["fri"], geo["frj"], device=device)
+        for gg in (self.g, self.gx, self.gr):
+            gg.set_reuse(reuse_tol)
         self.fs = pkg.Fields(self.g)
         self.fs.set_geometry(geo)
         self.fs.set_ion_geometry(geo)

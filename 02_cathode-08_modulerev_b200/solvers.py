@@ -98,6 +98,22 @@ class Grid:
         """Fused coarse tail (levels of at most 16 rows in one cluster launch) on / off (default off)."""
         capi.check(self._L.cth_grid_set_tail(self._h, int(enable)), allow_positive=False)
 
+    def set_reuse(self, tol: float, slot: int = -1):
+        """Hierarchy reuse: with tol > 0 a solve given a slot keeps its multigrid
+        hierarchy while the largest row-relative change of its operator stays at
+        most tol (the time step's sweeps use their own slots; ``slot`` is the slot
+        of the solves called on this grid directly, -1 none).  tol = 0: rebuild in
+        every solve (default)."""
+        capi.check(self._L.cth_grid_set_reuse(self._h, float(tol), int(slot)), allow_positive=False)
+
+    def reuse_stats(self, precision: int, slot: int) -> dict:
+        """Set-ups, reuses, last measured operator change, last cycle count and retries
+        (rebuilds after a slow cycle on the kept hierarchy) of a slot."""
+        out = (ctypes.c_double * 5)()
+        capi.check(self._L.cth_grid_reuse_stats(self._h, precision, slot, out), allow_positive=False)
+        return dict(setups=int(out[0]), reuses=int(out[1]), change=out[2], iterations=int(out[3]),
+                    retries=int(out[4]))
+
     def time_relax(self, precision: int, level: int = 0, reps: int = 50):
         """(µs per launch, algorithmic bytes per launch) of one level's z-line
         relaxation, back-to-back in a graph as inside a cycle."""

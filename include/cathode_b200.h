@@ -92,6 +92,36 @@ int cth_grid_set_graphs(cth_grid* g, int enable);
  * rounding.  Off by default: the separate launches with programmatic
  * dependent launch measured faster on the 512 x 1024 step. */
 int cth_grid_set_tail(cth_grid* g, int enable);
+/* Hierarchy reuse (no counterpart in the reference, whose SMG builds its
+ * hierarchy -- line factorisations, interpolation weights, Galerkin operators
+ * -- in every solve).  With tol > 0, a solve given a slot (0..14) keeps the
+ * hierarchy of that slot while its operator stays close to the one the
+ * hierarchy was built from: before the cycles, a device kernel measures the
+ * largest row-relative change max_k |a_k - a_k'| / |a_P| of the scaled
+ * operator against the kept one and rebuilds the hierarchy when it exceeds
+ * tol (both operators are compared after scaling to the same reference
+ * coefficient), when the slot is new or when the slot's previous solve did
+ * not converge.  A small coefficient change can still matter (a change of the
+ * row sums of a nearly singular operator), so the cycles check themselves: a
+ * cycle on the kept hierarchy that reduces the residual by less than a factor
+ * 2 ends the first loop, the hierarchy is rebuilt from the solve's operator and
+ * a second loop continues from the current iterate.  The kept hierarchy is
+ * only the preconditioner of the FP64 defect correction: residuals and the
+ * stopping rule use the caller's operator, so every solve meets the same
+ * tolerance.  The time step's sweeps give each recurring equation its own
+ * slot (cth_fields_* solves on this grid); `slot` (-1: none) is the slot of
+ * the solves entered through this header's cth_smg_solve* calls.  tol = 0
+ * (default): the hierarchy is built in every solve.  Each slot holds its own
+ * hierarchy once used (about 150 bytes per grid cell in FP32, twice that in
+ * FP64). */
+int cth_grid_set_reuse(cth_grid* g, double tol, int slot);
+/* out[0..4]: set-ups, reuses, the last measured change, the last solve's cycle
+ * count and the retries of a slot's hierarchy of the given precision
+ * (synchronises the device).  A retry: a cycle on the kept hierarchy reduced
+ * the residual by less than a factor 2, so the solve rebuilt the hierarchy
+ * from its operator and continued from its current iterate (counted among the
+ * set-ups too). */
+int cth_grid_reuse_stats(cth_grid* g, int precision, int slot, double* out);
 
 /* Instrumentation ------------------------------------------------------------
  * cth_launch_count: kernels this grid has launched since creation.

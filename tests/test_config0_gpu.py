@@ -41,12 +41,14 @@ def _norms(d, z, n, mask, r):
     return out
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_small_discharge_through_the_first_microwave_update(pkg, cuda_device, golden, precision):
+@pytest.mark.parametrize("precision,reuse_tol", [(0, 0.0), (1, 0.0), (1, 1e-3)])
+def test_small_discharge_through_the_first_microwave_update(pkg, cuda_device, golden, precision, reuse_tol):
+    """reuse_tol > 0: each equation keeps its multigrid hierarchy while its operator
+    changes by at most that much (Grid.set_reuse); same bar."""
     mask = np.zeros((NI + 2, NJ + 2), bool)
     mask[1:NI + 1, 1:NJ + 1] = True
     r = (np.arange(NJ + 2) - 0.5) * (5e-3 / NJ)
-    d = pkg.discharge.RectangleDischarge(pkg, NI, NJ, seed=0, precision=precision)
+    d = pkg.discharge.RectangleDischarge(pkg, NI, NJ, seed=0, precision=precision, reuse_tol=reuse_tol)
     done = 0
     for n in (100, 150):
         for _ in range(n - done):
@@ -56,8 +58,15 @@ def test_small_discharge_through_the_first_microwave_update(pkg, cuda_device, go
                 assert rr["mw"]["rc"] == 0 and rr["mw"]["solve"]["converged"] == 1, rr["mw"]
         done = n
         norms = _norms(d, golden, n, mask, r)
-        print("small discharge", "mixed" if precision else "fp64", n, {k: f"{v:.1e}" for k, v in norms.items()})
+        print("small discharge", "mixed" if precision else "fp64", "reuse" if reuse_tol else "", n,
+              {k: f"{v:.1e}" for k, v in norms.items()})
         if n == 100:
             for k, v in norms.items():
                 assert v <= 1e-8, (n, k, v)
+    if reuse_tol:
+        stats = {slot: d.g.reuse_stats(precision, slot) for slot in range(7)}
+        print("hierarchy slots of the cell grid", stats)
+        # the potential and the neutrals keep their hierarchies through the run
+        for slot in (2, 5, 6):
+            assert stats[slot]["reuses"] >= 0.9 * (stats[slot]["reuses"] + stats[slot]["setups"]), stats[slot]
     d.close()

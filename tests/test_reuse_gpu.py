@@ -1,0 +1,139 @@
+"""Hierarchy reuse (Grid.set_reuse): a solve given a slot keeps the multigrid
+hierarchy of that slot while the largest row-relative change of its scaled
+operator stays within the tolerance; the kept hierarchy only preconditions the
+FP64 defect correction, so every solve still meets the caller's tolerance on
+the caller's operator.  Checked here through the C ABI on the slab system
+against the oracle's exact solve (relative L2 <= 1e-8 after converging to
+||b - Ax|| / ||b|| < 1e-11), bit for bit against the solve that builds its
+hierarchy when the operator is the same, and through the rebuild rules (new
+slot, change above the tolerance, previous solve not converged)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_SOLVE = 1e-11
+TOL_PARITY = 1e-8
+SLOT = 2
+KEYS = ("aP", "aE", "aW", "aN", "aS", "b")
+
+
+def _grid(pkg, s):
+    return pkg.solvers.Grid(s["ni"], s["nj"], s["i_bl"], s["j_bl"])
+
+
+def _solve(g, s, prec, maxITR=40):
+    x = np.zeros((s["ni"] + 2, s["nj"] + 2))
+    st = g.smg_solve(*(s[k] for k in KEYS), x, maxITR=maxITR, error_cnv=TOL_SOLVE, precision=prec)
+    return x, st
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_same_operator_reuses_bit_for_bit(pkg, cuda_device, prec):
+    s = pkg.workloads.poisson_slab(ni=200, nj=100, seed=1)
+    g = _grid(pkg, s)
+    x_ref, st_ref = _solve(g, s, prec)          # hierarchy built in the solve (no slot)
+    g.set_reuse(1e-3, slot=SLOT)
+    x1, st1 = _solve(g, s, prec)                 # the slot's first solve builds its hierarchy
+    x2, st2 = _solve(g, s, prec)                 # the same operator: kept
+    r = g.reuse_stats(prec, SLOT)
+    assert r["setups"] == 1 and r["reuses"] == 1 and r["change"] == 0.0, r
+    assert np.array_equal(x1, x_ref) and np.array_equal(x2, x_ref)
+    assert st1.iterations == st2.iterations == st_ref.iterations
+    # the same system times a power of two: the scaled operator is the same, the
+    # hierarchy is kept, and every step of the iteration scales exactly
+    s4 = {k: (4.0 * v if k in KEYS else v) for k, v in s.items()}
+    x4, st4 = _solve(g, s4, prec)
+    r = g.reuse_stats(prec, SLOT)
+    assert r["setups"] == 1 and r["reuses"] == 2, r
+    assert np.array_equal(x4, x_ref) and st4.iterations == st_ref.iterations
+    g.close()
+
+
+def _smooth(s, delta):
+    """every coefficient times one smooth field 1 + delta sin(3z) cos(2r): the kind
+    of change a time step makes (row sums change in proportion)"""
+    z = np.linspace(0.0, 1.0, s["ni"] + 2)[:, None]
+    r = np.linspace(0.0, 1.0, s["nj"] + 2)[None, :]
+    f = 1.0 + delta * np.sin(3.0 * z) * np.cos(2.0 * r)
+    return dict(s, **{k: s[k] * f for k in KEYS[:5]})
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_changed_operator(pkg, orc, cuda_device, prec):
+    """(a) a smooth change below the tolerance keeps the hierarchy and converges at
+    the usual rate; (b) aE alone times 1 - 1e-3: the row sums of the nearly singular
+    potential operator move (the exact inverse of the old operator gives a
+    spectral radius of 1.28 for I - A_old^-1 A_new on this system, so the kept
+    hierarchy cannot converge), the change is still below the tolerance, the
+    cycles on the kept hierarchy stall and the solve rebuilds and goes on (one
+    retry); (c) a change above the tolerance rebuilds before the cycles.  Every
+    solve matches the exact solve."""
+    s = pkg.workloads.poisson_slab(ni=200, nj=100, seed=1)
+    g = _grid(pkg, s)
+    g.set_reuse(1e-3, slot=SLOT)
+    _, st0 = _solve(g, s, prec)
+    cases = [("smooth", _smooth(s, 5e-4), 0, 0),
+             ("row sums", dict(s, aE=s["aE"] * (1.0 - 1e-3)), 1, 1),
+             ("large", _smooth(s, 0.2), 1, 0)]
+    for name, sk, new_setups, new_retries in cases:
+        before = g.reuse_stats(prec, SLOT)
+        x, st = _solve(g, sk, prec)
+        after = g.reuse_stats(prec, SLOT)
+        assert st.converged == 1 and st.residual < TOL_SOLVE, (name, st.as_dict())
+        assert after["setups"] - before["setups"] == new_setups, (name, after)
+        assert after["retries"] - before["retries"] == new_retries, (name, after)
+        if name == "smooth":
+            assert after["change"] <= 1e-3 and st.iterations <= st0.iterations + 1, (st.iterations, after)
+        if name == "large":
+            assert after["change"] > 1e-3
+        ref = orc.direct_solve(sk)
+        err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+        assert err < TOL_PARITY, (name, err)
+        _, rn, bn = orc.residual(sk, x)
+        assert rn / bn < 2 * TOL_SOLVE
+    g.close()
+
+
+def test_unconverged_solve_rebuilds_next_time(pkg, cuda_device):
+    s = pkg.workloads.poisson_slab(ni=200, nj=100, seed=1)
+    g = _grid(pkg, s)
+    g.set_reuse(1e-3, slot=SLOT)
+    _solve(g, s, 1)
+    _, st = _solve(g, s, 1, maxITR=1)            # kept hierarchy, stopped before the tolerance
+    assert st.converged == 0
+    assert g.reuse_stats(1, SLOT)["setups"] == 1
+    x, st = _solve(g, s, 1)
+    r = g.reuse_stats(1, SLOT)
+    assert r["setups"] == 2 and r["reuses"] == 1, r
+    assert st.converged == 1
+    # the slots are separate: another slot builds its own hierarchy
+    g.set_reuse(1e-3, slot=SLOT + 1)
+    _solve(g, s, 1)
+    assert g.reuse_stats(1, SLOT + 1)["setups"] == 1 and g.reuse_stats(1, SLOT)["setups"] == 2
+    g.close()
+
+
+def test_graphs_off_agrees(pkg, cuda_device):
+    """The host-driven path (graphs off) takes the same decisions (keep, rebuild,
+    retry) and returns the same results bit for bit."""
+    s = pkg.workloads.poisson_slab(ni=96, nj=48, seed=1)
+    # on this coarser grid a row-sum shift of 5e-3 (spectral radius 1.46 with the old
+    # operator's exact inverse) is below the tolerance 1e-2 and stalls the kept hierarchy
+    systems = [s, _smooth(s, 5e-4), dict(s, aE=s["aE"] * (1.0 - 5e-3)), _smooth(s, 0.2)]
+    out = []
+    for graphs in (True, False):
+        g = _grid(pkg, s)
+        g.set_graphs(graphs)
+        g.set_reuse(1e-2, slot=SLOT)
+        xs, its = [], []
+        for sk in systems:
+            x, st = _solve(g, sk, 1)
+            xs.append(x)
+            its.append(st.iterations)
+        out.append((xs, its, g.reuse_stats(1, SLOT)))
+        g.close()
+    (xa, ia, ra), (xb, ib, rb) = out
+    assert ra == rb and ia == ib, (ra, rb, ia, ib)
+    assert ra["setups"] == 3 and ra["reuses"] == 2 and ra["retries"] == 1, ra
+    assert all(np.array_equal(a, b) for a, b in zip(xa, xb))
