@@ -904,7 +904,8 @@ constexpr int UPD_CELLS = 4;
 // FP64 norm, the iteration count, the stopping rule and the loop condition.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask,
+__global__ void __launch_bounds__(256, 4) k_update(const SolveArgs* __restrict__ args,
+                                                  const unsigned char* __restrict__ mask,
                          int ld_u, int i0, int j0, int ncol, int nrow, int ldl,
                          double* __restrict__ x64a, double* __restrict__ x64b,
                          const T* __restrict__ e, T* __restrict__ b0, double* __restrict__ part,
@@ -915,9 +916,11 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
     const int it = (int)stat[ST_ITER] + 1;
     const double* __restrict__ xin = (it & 1) ? x64a : x64b;
     double* __restrict__ xout = (it & 1) ? x64b : x64a;
-    // UPD_CELLS consecutive cells of row r per thread: their loads are in flight
-    // together and the west / east neighbours come from the thread's own cells
-    const int c0 = UPD_CELLS * (blockIdx.x * blockDim.x + threadIdx.x);
+    // a warp covers 32 * UPD_CELLS consecutive cells of row r; lane l owns the cells
+    // base + 32 k + l, so every load and store instruction of the warp reads one
+    // contiguous run, and the west / east neighbours come from the adjacent lanes
+    const int lane = threadIdx.x & 31;
+    const int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 * UPD_CELLS);
     const int r = blockIdx.y;
     // e solves the cycle's system for xs x (the previous right-hand side's scale);
     // this right-hand side is scaled so that sA times the previous residual norm is O(1)
@@ -926,30 +929,58 @@ __global__ void k_update(const SolveArgs* __restrict__ args, const unsigned char
     const double xs = pow2_scale(sqrt(stat[ST_RR]) * sA);
     const double sb = sA * xs;
     double rr = 0.0;
-    if (c0 < ncol) {
-        const size_t p0 = (size_t)r * ldl + c0;
-        const size_t q0 = (size_t)(r + j0) * ld_u + (c0 + i0);
-        // x + e on cells c0-1 .. c0+UPD_CELLS of this row (the ends only where they exist)
-        double xc[UPD_CELLS + 2];
-#pragma unroll
-        for (int k = 0; k < UPD_CELLS + 2; k++) {
-            const int c = c0 - 1 + k;
-            xc[k] = (c >= 0 && c < ncol) ? xin[p0 - 1 + k] + (double)e[p0 - 1 + k] * ie : 0.0;
-        }
+    if (base < ncol) {   // uniform over the warp
+        const size_t prow = (size_t)r * ldl;
+        const size_t qrow = (size_t)(r + j0) * ld_u + i0;
+        // addresses clamped into the level (the row's end, the missing neighbour rows);
+        // the values that do not exist are left out below
+        const int rn = (r + 1 < nrow) ? r + 1 : r, rs = (r > 0) ? r - 1 : r;
+        double xr[UPD_CELLS];
+        T er[UPD_CELLS];
 #pragma unroll
         for (int k = 0; k < UPD_CELLS; k++) {
-            const int c = c0 + k;
-            if (c >= ncol) break;
-            const size_t p = p0 + k, q = q0 + k;
+            const int c = min(base + 32 * k + lane, ncol - 1);
+            xr[k] = xin[prow + c];
+            er[k] = e[prow + c];
+        }
+        // the cells just outside the warp's run: base - 1 (lane 0) and base + 32 UPD_CELLS (lane 31)
+        const int cl = base - 1, cr = base + 32 * UPD_CELLS;
+        double xl = 0.0, xrr = 0.0;
+        if (lane == 0 && cl >= 0) xl = xin[prow + cl] + (double)e[prow + cl] * ie;
+        if (lane == 31 && cr < ncol) xrr = xin[prow + cr] + (double)e[prow + cr] * ie;
+        // x + e of the own cells (zero beyond the row's end)
+        double xc[UPD_CELLS];
+#pragma unroll
+        for (int k = 0; k < UPD_CELLS; k++)
+            xc[k] = (base + 32 * k + lane < ncol) ? xr[k] + (double)er[k] * ie : 0.0;
+#pragma unroll
+        for (int k = 0; k < UPD_CELLS; k++) {
+            const int c = base + 32 * k + lane;
+            const int cc = min(c, ncol - 1);
+            const size_t q = qrow + cc;
+            const double vP = __ldg(args->aP + q), vE = __ldg(args->aE + q), vW = __ldg(args->aW + q);
+            const double vN = __ldg(args->aN + q), vS = __ldg(args->aS + q), vb = __ldg(args->b + q);
+            const unsigned char mk = mask[prow + cc];
+            const double xn = xin[(size_t)rn * ldl + cc], xsr = xin[(size_t)rs * ldl + cc];
+            const T en = e[(size_t)rn * ldl + cc], esr = e[(size_t)rs * ldl + cc];
+            // west / east neighbours from the adjacent lanes (the run's ends from the next k)
+            const double up = __shfl_up_sync(0xffffffffu, xc[k], 1);
+            const double dn = __shfl_down_sync(0xffffffffu, xc[k], 1);
+            const double prevlast = __shfl_sync(0xffffffffu, xc[k > 0 ? k - 1 : 0], 31);
+            const double nextfirst = __shfl_sync(0xffffffffu, xc[k + 1 < UPD_CELLS ? k + 1 : k], 0);
+            const double xw = (lane > 0) ? up : (k > 0 ? prevlast : xl);
+            const double xe = (lane < 31) ? dn : (k + 1 < UPD_CELLS ? nextfirst : xrr);
+            if (c >= ncol) continue;
+            const size_t p = prow + c;
             double res = 0.0;
-            if (mask[p]) {
-                res = args->b[q] - args->aP[q] * xc[k + 1];
-                if (c + 1 < ncol) res += args->aE[q] * xc[k + 2];
-                if (c > 0) res += args->aW[q] * xc[k];
-                if (r + 1 < nrow) res += args->aN[q] * (xin[p + ldl] + (double)e[p + ldl] * ie);
-                if (r > 0) res += args->aS[q] * (xin[p - ldl] + (double)e[p - ldl] * ie);
+            if (mk) {
+                res = vb - vP * xc[k];
+                if (c + 1 < ncol) res += vE * xe;
+                if (c > 0) res += vW * xw;
+                if (r + 1 < nrow) res += vN * (xn + (double)en * ie);
+                if (r > 0) res += vS * (xsr + (double)esr * ie);
             }
-            xout[p] = xc[k + 1];
+            xout[p] = xc[k];
             b0[p] = (T)(res * sb);
             rr += res * res;
         }
