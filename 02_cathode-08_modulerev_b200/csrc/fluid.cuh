@@ -230,6 +230,13 @@ __device__ __forceinline__ void res_stat(int mode, double nw, double od, double&
     else { a = d * d; b = od * od; }
 }
 
+// first cell of this thread when a warp covers 32 * cells consecutive cells of a
+// row and lane l owns the cells first + 32 k: every load and store instruction of
+// the warp then touches one contiguous run
+__device__ __forceinline__ int warp_strided_first(int cells) {
+    return (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 * cells) + (threadIdx.x & 31);
+}
+
 // the same statistics accumulated over several cells of one thread (the modes'
 // max or sum, as the grid reduction combines them afterwards)
 __device__ __forceinline__ void res_acc(int mode, double nw, double od, double& a, double& b) {

@@ -244,14 +244,14 @@ constexpr int kNStat = 12;  // (phi, nUex, nUer) x (vs iteration start, vs call 
 
 // interior fields and flux corrections, then the residual reductions
 // (fluidModule.hpp:2932-3046); the last block writes the 12 totals to out
-// kCorrCells consecutive cells of a row per thread: a block covers kCorrCells x
-// blockDim cells, so the deterministic reduction's per-block tree and its
-// last-block combine (one partial per block and statistic) stay short
+// kCorrCells cells of a row per thread (warp-strided, warp_strided_first): a block
+// covers kCorrCells x blockDim cells, so the deterministic reduction's per-block
+// tree and its last-block combine (one partial per block and statistic) stay short
 constexpr int kCorrCells = 4;
 
 __global__ void k_phi_correct_b(PhiArgs A, double* __restrict__ part, unsigned int* counter,
                                 double* __restrict__ out) {
-    const int i0 = kCorrCells * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int i0 = warp_strided_first(kCorrCells);
     const int j = blockIdx.y;
     const int mode = A.prm.flag_error;
     double s[kNStat];
@@ -259,7 +259,7 @@ __global__ void k_phi_correct_b(PhiArgs A, double* __restrict__ part, unsigned i
     for (int k = 0; k < kNStat; k++) s[k] = 0.0;
 #pragma unroll
     for (int kc = 0; kc < kCorrCells; kc++) {
-        const int i = i0 + kc;
+        const int i = i0 + 32 * kc;
         if (i > A.ni + 1) break;
         const int ld = A.ld;
         const size_t p = (size_t)j * ld + i;

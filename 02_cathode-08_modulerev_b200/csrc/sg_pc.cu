@@ -201,7 +201,8 @@ __device__ __forceinline__ void sg_predict_cell(const SgArgs& A, int i, int j) {
     A.Fr[p] = vr;
 }
 
-// kSweepCells consecutive cells of a row per thread (their loads in flight together)
+// kSweepCells cells of a row per thread: consecutive in the prediction (measured
+// faster there), warp-strided (warp_strided_first) in the assembly
 constexpr int kSweepCells = 4;
 
 template <bool EN>
@@ -259,16 +260,17 @@ __device__ __forceinline__ void sg_assemble_cell(const SgArgs& A, int i, int j) 
 
 template <bool EN>
 __global__ void k_sg_assemble(SgArgs A) {
-    const int i0 = kSweepCells * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int i0 = warp_strided_first(kSweepCells);
 #pragma unroll
-    for (int k = 0; k < kSweepCells; k++) sg_assemble_cell<EN>(A, i0 + k, blockIdx.y);
+    for (int k = 0; k < kSweepCells; k++) sg_assemble_cell<EN>(A, i0 + 32 * k, blockIdx.y);
 }
 
 constexpr int kSgStat = 14;  // calcRes pairs (n, Fx, Fr) x (iteration, call) + anode Ii, Ie
 
-// kCorrCells consecutive cells of a row per thread: a block covers kCorrCells x
-// blockDim cells, so the deterministic reduction's per-block tree and its
-// last-block combine (one partial per block and statistic) stay short
+// kCorrCells consecutive cells of a row per thread (measured faster here than the
+// warp-strided order): a block covers kCorrCells x blockDim cells, so the
+// deterministic reduction's per-block tree and its last-block combine (one partial
+// per block and statistic) stay short
 constexpr int kCorrCells = 4;
 
 template <bool EN>

@@ -159,7 +159,9 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
                         int use_cond, double* __restrict__ sst, unsigned long long* gmax,
                         cudaGraphConditionalHandle cond_setup) {
     __shared__ double red[32];
-    const int c0 = PREP_CELLS * (blockIdx.x * blockDim.x + threadIdx.x);
+    // a warp covers 32 * PREP_CELLS consecutive cells of row r, lane l the cells
+    // base + 32 k + l (each load instruction of the warp reads one contiguous run)
+    const int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 * PREP_CELLS) + (threadIdx.x & 31);
     const int r = blockIdx.y;
     const double sA = pow2_scale(args->aP[qref]);
     const double gw = stat[ST_GUESS];
@@ -167,10 +169,9 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
     const double* xg = (gw >= 100.0) ? args->x0b : args->x0;
     double v2[2] = {0.0, 0.0};  // ||r0||^2, ||b||^2
     double dmax = 0.0;          // REUSE: largest row-relative change of this thread's cells
-    // PREP_CELLS consecutive cells of row r per thread, their loads in flight together
 #pragma unroll
     for (int k = 0; k < PREP_CELLS; k++) {
-        const int c = c0 + k;
+        const int c = base + 32 * k;
         if (c >= ncol) break;
         const double* __restrict__ aP = args->aP;
         const size_t plane = (size_t)nrow * ldl;
@@ -262,12 +263,12 @@ template <typename T>
 __global__ void k_prep_op(const SolveArgs* __restrict__ args, const unsigned char* __restrict__ mask, int ld_u,
                           int i0, int j0, int ncol, int nrow, int ldl, T* __restrict__ a0,
                           const double* __restrict__ stat) {
-    const int c0 = PREP_CELLS * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 * PREP_CELLS) + (threadIdx.x & 31);
     const int r = blockIdx.y;
     const double sA = stat[ST_ASCALE];
 #pragma unroll
     for (int k = 0; k < PREP_CELLS; k++) {
-        const int c = c0 + k;
+        const int c = base + 32 * k;
         if (c >= ncol) break;
         const size_t plane = (size_t)nrow * ldl;
         const size_t p = (size_t)r * ldl + c;

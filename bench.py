@@ -1038,7 +1038,7 @@ def main():
                           "for the copies)"},
         "roofline": {"bound": "hbm",
                      "kernel": "k_relax<float,9,*> (z-line relaxations of the coarse multigrid levels, the step's "
-                               "dominant kernel: 53 % of its kernel time in profiles/launches_step_mixed_512x1024.md)",
+                               "dominant kernel: 57 % of its kernel time in profiles/launches_step_mixed_512x1024.md)",
                      "achieved": achieved_coarse, "peak": peak, "unit": "GB/s",
                      "frac": (achieved_coarse / peak) if achieved_coarse else None,
                      "traffic": traffic.get("coarse_relax_dram_bytes_per_launch"),
