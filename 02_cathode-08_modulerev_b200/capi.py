@@ -29,7 +29,7 @@ EXPORTS = (
     "cth_version", "cth_last_error", "cth_grid_create", "cth_grid_destroy", "cth_grid_ld",
     "cth_grid_levels", "cth_grid_set_cycle", "cth_smg_solve", "cth_smg_solve_dev", "cth_smg_solve_guess_dev", "cth_sor_solve",
     "cth_sor_solve_dev", "cth_residual_dev", "cth_to_device_layout", "cth_from_device_layout",
-    "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs", "cth_grid_set_tail", "cth_grid_set_reuse", "cth_grid_reuse_stats", "cth_grid_time_relax",
+    "cth_launch_count", "cth_profile", "cth_profile_read", "cth_residual_noalloc", "cth_grid_set_graphs", "cth_grid_set_tail", "cth_grid_set_reuse", "cth_grid_reuse_stats", "cth_grid_time_relax", "cth_grid_time_cycle",
     "cth_c5_solve", "cth_c5_solve_dev", "cth_mw_er_assemble_dev",
     "cth_mw3_create", "cth_mw3_destroy", "cth_mw3_ld", "cth_mw3_launch_count", "cth_mw3_assemble_dev",
     "cth_mw3_copy_planes", "cth_mw3_apply_dev", "cth_mw3_solve_dev", "cth_mw3_solve_guess_dev", "cth_mw3_set_graphs",
@@ -357,6 +357,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cth_grid_time_relax.restype = ctypes.c_int
     L.cth_grid_set_tail.argtypes = [_vp, ctypes.c_int]
     L.cth_grid_set_tail.restype = ctypes.c_int
+    L.cth_grid_time_cycle.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.cth_grid_time_cycle.restype = ctypes.c_int
     L.cth_grid_set_reuse.argtypes = [_vp, ctypes.c_double, ctypes.c_int]
     L.cth_grid_set_reuse.restype = ctypes.c_int
     L.cth_grid_reuse_stats.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]

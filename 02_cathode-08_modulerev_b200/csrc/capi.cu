@@ -347,6 +347,16 @@ int cth_grid_time_relax(cth_grid* g, int precision, int level, int reps, double*
     return time_relax(g, precision, level, reps, us_per_launch, bytes_per_launch);
 }
 
+int cth_grid_time_cycle(cth_grid* g, int precision, int reps, int with_update, double* us_per_cycle) {
+    if (!g || !us_per_cycle) {
+        set_error("cth_grid_time_cycle: invalid arguments");
+        return CTH_ERR_ARG;
+    }
+    CTH_CUDA(cudaSetDevice(g->device));
+    CTH_CUDA(cudaStreamSynchronize(g->stream));
+    return time_cycle(g, precision, reps, with_update, us_per_cycle);
+}
+
 int cth_profile_read(const cth_grid* g, int cls, double* ms, long long* launches, double* bytes) {
     if (!g || cls < 0 || cls >= PROF_NCLASS) { set_error("cth_profile_read: invalid arguments"); return CTH_ERR_ARG; }
     if (ms) *ms = g->prof.ms[cls];

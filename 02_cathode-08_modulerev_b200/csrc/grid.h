@@ -252,6 +252,7 @@ int smg_solve_launch(cth_grid* g, const double* aP, const double* aE, const doub
                      int slot = -1);
 int solve_finish(cth_grid* g, int pending, cth_status* st);
 int time_relax(cth_grid* g, int precision, int level, int reps, double* us, double* bytes);
+int time_cycle(cth_grid* g, int precision, int reps, int with_update, double* us);
 int solve_parse(cth_grid* g, int pending, const double* h, cth_status* st);
 int sor_solve_dev(cth_grid* g, const double* aP, const double* aE, const double* aW,
                   const double* aN, const double* aS, const double* b, double alpha,

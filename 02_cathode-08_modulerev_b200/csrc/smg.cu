@@ -1761,6 +1761,75 @@ static int time_relax_impl(cth_grid* g, int l, int reps, double* us, double* byt
     return CTH_OK;
 }
 
+// reps cycles (V-cycle + FP64 update, or the V-cycle alone) captured one after
+// another in one graph without the conditional loop, on the hierarchy of the last
+// solve; the solve's state is left undefined (the next solve prepares its own)
+template <typename T>
+static int time_cycle_impl(cth_grid* g, int reps, int with_update, double* us) {
+    Hierarchy<T>& h = hier<T>(g);
+    if (!h.allocated) {
+        set_error("cth_grid_time_cycle: no solve of this precision has run on the grid");
+        return CTH_ERR_ARG;
+    }
+    cudaStream_t cs = g->cap[0];
+    const bool prof = g->prof.on;
+    g->prof.on = false;
+    const long long l0 = g->launches;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CTH_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    for (int r = 0; r < reps; r++) {
+        if (with_update) enqueue_body<T>(g, cs, 0, 0);
+        else vcycle<T>(g, 0, cs);
+    }
+    cudaError_t e = cudaStreamEndCapture(cs, &graph);
+    g->launches = l0;
+    g->prof.on = prof;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, g->stream);  // warm
+    if (e == cudaSuccess) e = cudaEventRecord(e0, g->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, g->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, g->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cth_grid_time_cycle");
+    *us = 1e3 * (double)ms / reps;
+    return CTH_OK;
+}
+
+int time_cycle(cth_grid* g, int precision, int reps, int with_update, double* us) {
+    if (reps < 1 || reps > 1000) {
+        set_error("cth_grid_time_cycle: repetitions out of range");
+        return CTH_ERR_ARG;
+    }
+    auto first = [&](auto* hs) {
+        for (int k = 0; k < kHier; k++)
+            if (hs[k].allocated) return k;
+        return 0;
+    };
+    int rc;
+    if (precision == CTH_PREC_MIXED) {
+        g->cur = first(g->h32);
+        rc = time_cycle_impl<float>(g, reps, with_update, us);
+    } else if (precision == CTH_PREC_FP64) {
+        g->cur = first(g->h64);
+        rc = time_cycle_impl<double>(g, reps, with_update, us);
+    } else {
+        set_error("unknown precision mode");
+        rc = CTH_ERR_ARG;
+    }
+    g->cur = 0;
+    return rc;
+}
+
 int time_relax(cth_grid* g, int precision, int level, int reps, double* us, double* bytes) {
     if (level < 0 || level >= g->nlev || reps < 1 || reps > 1000) {
         set_error("cth_grid_time_relax: level or repetitions out of range");

@@ -98,6 +98,14 @@ class Grid:
         """Fused coarse tail (levels of at most 16 rows in one cluster launch) on / off (default off)."""
         capi.check(self._L.cth_grid_set_tail(self._h, int(enable)), allow_positive=False)
 
+    def time_cycle(self, precision: int, reps: int = 20, with_update: bool = True) -> float:
+        """µs per multigrid cycle of ``reps`` cycles captured one after another in one
+        graph without the solve's loop node (with or without the FP64 update)."""
+        us = ctypes.c_double()
+        capi.check(self._L.cth_grid_time_cycle(self._h, precision, reps, int(with_update), ctypes.byref(us)),
+                   allow_positive=False)
+        return us.value
+
     def set_reuse(self, tol: float, slot: int = -1):
         """Hierarchy reuse: with tol > 0 a solve given a slot keeps its multigrid
         hierarchy while the largest row-relative change of its operator stays at

@@ -152,6 +152,14 @@ int cth_profile_read(const cth_grid* g, int cls, double* ms, long long* launches
  * cycle scratch.  Synchronises the grid's stream. */
 int cth_grid_time_relax(cth_grid* g, int precision, int level, int reps, double* us_per_launch,
                         double* bytes_per_launch);
+/* cth_grid_time_cycle: device time per cycle of `reps` multigrid cycles captured
+ * one after another in one CUDA graph, without the solve's device-side loop
+ * node: V-cycle + FP64 defect correction (with_update = 1) or the V-cycle
+ * alone.  Against the per-cycle time of a solve it separates the loop node's
+ * cost.  Needs a previous solve of that precision on the grid; leaves the
+ * grid's solve state undefined (the next solve prepares its own).
+ * Synchronises the grid's stream. */
+int cth_grid_time_cycle(cth_grid* g, int precision, int reps, int with_update, double* us_per_cycle);
 
 /* SMG replacement (host arrays) ----------------------------------------------
  * Drop-in for solver_SMG (include/solverFuncs.hpp:26-163): solves the 5-point
