@@ -52,16 +52,32 @@ template <typename T> constexpr bool kFac = !std::is_same<T, cd>::value && !std:
 // layout in precision T (couplings to non-grid cells dropped, non-grid cells
 // identity), b0 = b (grid cells); the last block records ||b||^2 and whether
 // the cycle loop runs at all (sets the graph's loop condition when use_cond).
+// L2 policy for streams that should leave the cache to other data first
+__device__ __forceinline__ unsigned long long l2_evict_first() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ double ld_hint(const double* p, unsigned long long pol) {
+    double v;
+    asm("ld.global.L2::cache_hint.f64 %0, [%1], %2;\n" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_hint(double* p, double v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;\n" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // FP64 residual r = b - A x0 of one grid cell (couplings to non-grid cells dropped)
 __device__ __forceinline__ double guess_resid(const SolveArgs* __restrict__ args, const double* __restrict__ x0,
                                               const unsigned char* __restrict__ mask, size_t p, size_t q,
-                                              int c, int r, int ncol, int nrow, int ldl, int ld_u) {
-    double v = args->b[q] - args->aP[q] * x0[q];
-    if (c > 0 && mask[p - 1]) v += args->aW[q] * x0[q - 1];
-    if (c + 1 < ncol && mask[p + 1]) v += args->aE[q] * x0[q + 1];
-    if (r > 0 && mask[p - ldl]) v += args->aS[q] * x0[q - ld_u];
-    if (r + 1 < nrow && mask[p + ldl]) v += args->aN[q] * x0[q + ld_u];
+                                              int c, int r, int ncol, int nrow, int ldl, int ld_u,
+                                              unsigned long long pol) {
+    double v = ld_hint(args->b + q, pol) - ld_hint(args->aP + q, pol) * ld_hint(x0 + q, pol);
+    if (c > 0 && mask[p - 1]) v += ld_hint(args->aW + q, pol) * ld_hint(x0 + q - 1, pol);
+    if (c + 1 < ncol && mask[p + 1]) v += ld_hint(args->aE + q, pol) * ld_hint(x0 + q + 1, pol);
+    if (r > 0 && mask[p - ldl]) v += ld_hint(args->aS + q, pol) * ld_hint(x0 + q - ld_u, pol);
+    if (r + 1 < nrow && mask[p + ldl]) v += ld_hint(args->aN + q, pol) * ld_hint(x0 + q + ld_u, pol);
     return v;
 }
 
@@ -80,18 +96,19 @@ __global__ void k_guess(const SolveArgs* __restrict__ args, const unsigned char*
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
     const double* xb = args->x0b;
+    const unsigned long long pol = l2_evict_first();   // the FP64 streams leave L2 first
     double v[3] = {0.0, 0.0, 0.0};  // ||r(x0)||^2, ||r(x0b)||^2, ||b||^2
     if (c < ncol) {
         const size_t p = (size_t)r * ldl + c;
         const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
         if (mask[p]) {
-            const double ra = guess_resid(args, args->x0, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
+            const double ra = guess_resid(args, args->x0, mask, p, q, c, r, ncol, nrow, ldl, ld_u, pol);
             v[0] = ra * ra;
             if (xb) {
-                const double rb = guess_resid(args, xb, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
+                const double rb = guess_resid(args, xb, mask, p, q, c, r, ncol, nrow, ldl, ld_u, pol);
                 v[1] = rb * rb;
             }
-            const double bv = args->b[q];
+            const double bv = ld_hint(args->b + q, pol);
             v[2] = bv * bv;
         }
     }
@@ -169,6 +186,7 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
     const double* xg = (gw >= 100.0) ? args->x0b : args->x0;
     double v2[2] = {0.0, 0.0};  // ||r0||^2, ||b||^2
     double dmax = 0.0;          // REUSE: largest row-relative change of this thread's cells
+    const unsigned long long pol = l2_evict_first();   // the FP64 streams leave L2 first
 #pragma unroll
     for (int k = 0; k < PREP_CELLS; k++) {
         const int c = base + 32 * k;
@@ -179,18 +197,18 @@ __global__ void k_prep0(const SolveArgs* __restrict__ args, const unsigned char*
         const size_t q = (size_t)(r + j0) * ld_u + (c + i0);
         T vP = T(1), vW = T(0), vE = T(0), vS = T(0), vN = T(0), vb = T(0);
         if (mask[p]) {
-            vP = (T)(aP[q] * sA);
-            if (c > 0 && mask[p - 1]) vW = (T)(args->aW[q] * sA);
-            if (c + 1 < ncol && mask[p + 1]) vE = (T)(args->aE[q] * sA);
-            if (r > 0 && mask[p - ldl]) vS = (T)(args->aS[q] * sA);
-            if (r + 1 < nrow && mask[p + ldl]) vN = (T)(args->aN[q] * sA);
-            const double bv = args->b[q];
+            vP = (T)(ld_hint(aP + q, pol) * sA);
+            if (c > 0 && mask[p - 1]) vW = (T)(ld_hint(args->aW + q, pol) * sA);
+            if (c + 1 < ncol && mask[p + 1]) vE = (T)(ld_hint(args->aE + q, pol) * sA);
+            if (r > 0 && mask[p - ldl]) vS = (T)(ld_hint(args->aS + q, pol) * sA);
+            if (r + 1 < nrow && mask[p + ldl]) vN = (T)(ld_hint(args->aN + q, pol) * sA);
+            const double bv = ld_hint(args->b + q, pol);
             v2[1] += bv * bv;
             if (guess) {
-                const double rv = guess_resid(args, xg, mask, p, q, c, r, ncol, nrow, ldl, ld_u);
+                const double rv = guess_resid(args, xg, mask, p, q, c, r, ncol, nrow, ldl, ld_u, pol);
                 vb = (T)(rv * sA);
                 v2[0] += rv * rv;
-                x64[p] = xg[q];
+                st_hint(x64 + p, ld_hint(xg + q, pol), pol);
             } else {
                 vb = (T)(bv * sA);
                 v2[0] += bv * bv;
@@ -895,8 +913,24 @@ __global__ void k_tail(TailArgs<T> A) {
     }
 }
 
-// cells per thread of k_update
+// cells per thread and threads per block of k_update
 constexpr int UPD_CELLS = 4;
+constexpr int UPD_THREADS = 256;
+constexpr size_t kUpdSmem = 6 * UPD_CELLS * UPD_THREADS * sizeof(double);
+
+// 8-byte asynchronous global -> shared copy (completion per thread: cp_async_wait_all)
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+// the same with an L2 eviction-priority policy (createpolicy)
+__device__ __forceinline__ void cp_async8_hint(void* smem, const void* gmem, unsigned long long pol) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // defect correction, iteration it = stat[ST_ITER] + 1: x_it = x_{it-1} + e with
@@ -905,8 +939,8 @@ constexpr int UPD_CELLS = 4;
 // FP64 norm, the iteration count, the stopping rule and the loop condition.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256, 4) k_update(const SolveArgs* __restrict__ args,
-                                                  const unsigned char* __restrict__ mask,
+__global__ void __launch_bounds__(UPD_THREADS, 4) k_update(const SolveArgs* __restrict__ args,
+                                                          const unsigned char* __restrict__ mask,
                          int ld_u, int i0, int j0, int ncol, int nrow, int ldl,
                          double* __restrict__ x64a, double* __restrict__ x64b,
                          const T* __restrict__ e, T* __restrict__ b0, double* __restrict__ part,
@@ -914,15 +948,42 @@ __global__ void __launch_bounds__(256, 4) k_update(const SolveArgs* __restrict__
                          cudaGraphConditionalHandle cond, int use_cond, double* __restrict__ sst,
                          cudaGraphConditionalHandle cond_rs, cudaGraphConditionalHandle cond2) {
     __shared__ double red[32];
-    const int it = (int)stat[ST_ITER] + 1;
-    const double* __restrict__ xin = (it & 1) ? x64a : x64b;
-    double* __restrict__ xout = (it & 1) ? x64b : x64a;
+    // dynamic shared memory (kUpdSmem): the caller's aP, aE, aW, aN, aS and b of this
+    // thread's cells, [6][UPD_CELLS][UPD_THREADS]
+    extern __shared__ double upd_smem[];
+    double(*sco)[UPD_CELLS][UPD_THREADS] = reinterpret_cast<double(*)[UPD_CELLS][UPD_THREADS]>(upd_smem);
     // a warp covers 32 * UPD_CELLS consecutive cells of row r; lane l owns the cells
     // base + 32 k + l, so every load and store instruction of the warp reads one
     // contiguous run, and the west / east neighbours come from the adjacent lanes
     const int lane = threadIdx.x & 31;
     const int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 * UPD_CELLS);
     const int r = blockIdx.y;
+    const bool run = base < ncol;   // uniform over the warp
+    const size_t prow = (size_t)r * ldl;
+    const size_t qrow = (size_t)(r + j0) * ld_u + i0;
+    // before the wait on the cycle's last relaxation (programmatic dependent launch):
+    // the caller's operator and right-hand side, constant during the solve, start
+    // their asynchronous copies into shared memory, and the static mask is read
+    // the FP64 streams (the caller's operator and b, the FP64 iterate) are read and
+    // written evict-first in L2, so that they do not push the cycle's hierarchy out
+    const unsigned long long pol = l2_evict_first();
+    unsigned char mk[UPD_CELLS];
+    if (run) {
+        const double* __restrict__ src[6] = {args->aP, args->aE, args->aW, args->aN, args->aS, args->b};
+#pragma unroll
+        for (int k = 0; k < UPD_CELLS; k++) {
+            const int c = min(base + 32 * k + lane, ncol - 1);
+#pragma unroll
+            for (int m = 0; m < 6; m++) cp_async8_hint(&sco[m][k][threadIdx.x], src[m] + qrow + c, pol);
+            mk[k] = mask[prow + c];
+        }
+    }
+    cp_async_commit();
+    griddep_wait();
+    griddep_launch();
+    const int it = (int)stat[ST_ITER] + 1;
+    const double* __restrict__ xin = (it & 1) ? x64a : x64b;
+    double* __restrict__ xout = (it & 1) ? x64b : x64a;
     // e solves the cycle's system for xs x (the previous right-hand side's scale);
     // this right-hand side is scaled so that sA times the previous residual norm is O(1)
     const double sA = stat[ST_ASCALE];
@@ -930,19 +991,21 @@ __global__ void __launch_bounds__(256, 4) k_update(const SolveArgs* __restrict__
     const double xs = pow2_scale(sqrt(stat[ST_RR]) * sA);
     const double sb = sA * xs;
     double rr = 0.0;
-    if (base < ncol) {   // uniform over the warp
-        const size_t prow = (size_t)r * ldl;
-        const size_t qrow = (size_t)(r + j0) * ld_u + i0;
+    if (run) {
         // addresses clamped into the level (the row's end, the missing neighbour rows);
         // the values that do not exist are left out below
         const int rn = (r + 1 < nrow) ? r + 1 : r, rs = (r > 0) ? r - 1 : r;
-        double xr[UPD_CELLS];
-        T er[UPD_CELLS];
+        double xr[UPD_CELLS], xn[UPD_CELLS], xsr[UPD_CELLS];
+        T er[UPD_CELLS], en[UPD_CELLS], esr[UPD_CELLS];
 #pragma unroll
         for (int k = 0; k < UPD_CELLS; k++) {
             const int c = min(base + 32 * k + lane, ncol - 1);
-            xr[k] = xin[prow + c];
+            xr[k] = ld_hint(xin + prow + c, pol);
             er[k] = e[prow + c];
+            xn[k] = ld_hint(xin + (size_t)rn * ldl + c, pol);
+            en[k] = e[(size_t)rn * ldl + c];
+            xsr[k] = ld_hint(xin + (size_t)rs * ldl + c, pol);
+            esr[k] = e[(size_t)rs * ldl + c];
         }
         // the cells just outside the warp's run: base - 1 (lane 0) and base + 32 UPD_CELLS (lane 31)
         const int cl = base - 1, cr = base + 32 * UPD_CELLS;
@@ -954,16 +1017,10 @@ __global__ void __launch_bounds__(256, 4) k_update(const SolveArgs* __restrict__
 #pragma unroll
         for (int k = 0; k < UPD_CELLS; k++)
             xc[k] = (base + 32 * k + lane < ncol) ? xr[k] + (double)er[k] * ie : 0.0;
+        cp_async_wait_all();   // this thread's own copies: no barrier needed
 #pragma unroll
         for (int k = 0; k < UPD_CELLS; k++) {
             const int c = base + 32 * k + lane;
-            const int cc = min(c, ncol - 1);
-            const size_t q = qrow + cc;
-            const double vP = __ldg(args->aP + q), vE = __ldg(args->aE + q), vW = __ldg(args->aW + q);
-            const double vN = __ldg(args->aN + q), vS = __ldg(args->aS + q), vb = __ldg(args->b + q);
-            const unsigned char mk = mask[prow + cc];
-            const double xn = xin[(size_t)rn * ldl + cc], xsr = xin[(size_t)rs * ldl + cc];
-            const T en = e[(size_t)rn * ldl + cc], esr = e[(size_t)rs * ldl + cc];
             // west / east neighbours from the adjacent lanes (the run's ends from the next k)
             const double up = __shfl_up_sync(0xffffffffu, xc[k], 1);
             const double dn = __shfl_down_sync(0xffffffffu, xc[k], 1);
@@ -973,18 +1030,22 @@ __global__ void __launch_bounds__(256, 4) k_update(const SolveArgs* __restrict__
             const double xe = (lane < 31) ? dn : (k + 1 < UPD_CELLS ? nextfirst : xrr);
             if (c >= ncol) continue;
             const size_t p = prow + c;
+            const double vP = sco[0][k][threadIdx.x], vE = sco[1][k][threadIdx.x], vW = sco[2][k][threadIdx.x];
+            const double vN = sco[3][k][threadIdx.x], vS = sco[4][k][threadIdx.x], vb = sco[5][k][threadIdx.x];
             double res = 0.0;
-            if (mk) {
+            if (mk[k]) {
                 res = vb - vP * xc[k];
                 if (c + 1 < ncol) res += vE * xe;
                 if (c > 0) res += vW * xw;
-                if (r + 1 < nrow) res += vN * (xn + (double)en * ie);
-                if (r > 0) res += vS * (xsr + (double)esr * ie);
+                if (r + 1 < nrow) res += vN * (xn[k] + (double)en[k] * ie);
+                if (r > 0) res += vS * (xsr[k] + (double)esr[k] * ie);
             }
-            xout[p] = xc[k];
+            st_hint(xout + p, xc[k], pol);
             b0[p] = (T)(res * sb);
             rr += res * res;
         }
+    } else {
+        cp_async_wait_all();
     }
     double tot;
     if (last_block_sum(rr, part, counter, red, &tot) && threadIdx.x == 0) {
@@ -1242,12 +1303,13 @@ static void vcycle(cth_grid* g, int l, cudaStream_t s) {
 // launch of a kernel that calls griddep_wait() before it reads what the kernels
 // before it wrote: with programmatic dependent launch when the grid uses it
 template <typename... KArgs, typename... Args>
-static void launch_dep(cth_grid* g, void (*kern)(KArgs...), dim3 grd, dim3 blk, cudaStream_t s, Args... args) {
+static void launch_dep(cth_grid* g, void (*kern)(KArgs...), dim3 grd, dim3 blk, size_t smem, cudaStream_t s,
+                       Args... args) {
     if (g->pdl) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = grd;
         cfg.blockDim = blk;
-        cfg.dynamicSmemBytes = 0;
+        cfg.dynamicSmemBytes = smem;
         cfg.stream = s;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1256,7 +1318,7 @@ static void launch_dep(cth_grid* g, void (*kern)(KArgs...), dim3 grd, dim3 blk, 
         cfg.numAttrs = 1;
         cudaLaunchKernelEx(&cfg, kern, args...);
     } else {
-        kern<<<grd, blk, 0, s>>>(args...);
+        kern<<<grd, blk, smem, s>>>(args...);
     }
     g->launches++;
 }
@@ -1267,10 +1329,10 @@ static void galerkin(cth_grid* g, int l, const LevelArgs<T>& L, cudaStream_t s) 
     Hierarchy<T>& h = hier<T>(g);
     const dim3 blk(128), grd((g->ncol + 127) / 128, g->nrow[l + 1]);
     if (l == 0)
-        launch_dep(g, k_galerkin<T, 5>, grd, blk, s, L, (const unsigned char*)g->mask[l], (const T*)h.wS[l],
+        launch_dep(g, k_galerkin<T, 5>, grd, blk, 0, s, L, (const unsigned char*)g->mask[l], (const T*)h.wS[l],
                    (const T*)h.wN[l], h.a[l + 1], g->nrow[l + 1], (const unsigned char*)g->mask[l + 1]);
     else
-        launch_dep(g, k_galerkin<T, 9>, grd, blk, s, L, (const unsigned char*)g->mask[l], (const T*)h.wS[l],
+        launch_dep(g, k_galerkin<T, 9>, grd, blk, 0, s, L, (const unsigned char*)g->mask[l], (const T*)h.wS[l],
                    (const T*)h.wN[l], h.a[l + 1], g->nrow[l + 1], (const unsigned char*)g->mask[l + 1]);
 }
 
@@ -1288,7 +1350,7 @@ static void setup_levels(cth_grid* g, cudaStream_t s) {
                                                                                       : k_factor<T, 5, 256>)
                              : (g->bnd == 1024 ? k_factor<T, 9, 1024> : g->bnd == 512 ? k_factor<T, 9, 512>
                                                                                       : k_factor<T, 9, 256>);
-            launch_dep(g, kf, dim3(g->nrow[l]), dim3(g->bd), s, L, g->mask[l], h.fac[l], h.wS[l], h.wN[l], wts);
+            launch_dep(g, kf, dim3(g->nrow[l]), dim3(g->bd), 0, s, L, g->mask[l], h.fac[l], h.wS[l], h.wN[l], wts);
             if (!wts) break;
             galerkin<T>(g, l, L, s);
         }
@@ -1366,15 +1428,16 @@ static int enqueue_body(cth_grid* g, cudaStream_t s, cudaGraphConditionalHandle 
     Hierarchy<T>& h = hier<T>(g);
     Workspace& w = g->ws;
     const int ncol = g->ncol, nrow0 = g->nrow[0], ldl = g->ldl;
-    dim3 blk(256), grd((ncol + 256 * UPD_CELLS - 1) / (256 * UPD_CELLS), nrow0);
+    dim3 blk(UPD_THREADS), grd((ncol + UPD_THREADS * UPD_CELLS - 1) / (UPD_THREADS * UPD_CELLS), nrow0);
     const long long l0 = g->launches;
     vcycle<T>(g, 0, s);
     const int slot = prof_mark(g, PROF_UPDATE, (double)nrow0 * ncol * (8.0 * 8.0 + 2.0 * sizeof(T) + 1.0), s);
-    k_update<T><<<grd, blk, 0, s>>>(w.d_args, g->mask[0], g->ld, g->i0, g->j0, ncol, nrow0, ldl, w.x64[0],
-                                    w.x64[1], h.x[0], h.b[0], w.part, w.counter, w.stat, cond, use_cond, sst,
-                                    cond_rs, cond2);
+    // programmatic dependent launch: the caller's operator is copied in before the wait
+    launch_dep(g, k_update<T>, grd, blk, kUpdSmem, s, (const SolveArgs*)w.d_args, (const unsigned char*)g->mask[0], g->ld,
+               g->i0, g->j0, ncol, nrow0, ldl, w.x64[0], w.x64[1], (const T*)h.x[0], h.b[0], w.part, w.counter,
+               w.stat, cond, use_cond, sst, cond_rs, cond2);
     prof_done(g, slot, s);
-    const int n = 1 + (int)(g->launches - l0);
+    const int n = (int)(g->launches - l0);
     g->launches = l0;
     return n;
 }
@@ -1910,6 +1973,9 @@ int configure_kernels(cth_grid* g) {
     if (line_smem<cd>(g->bd, 1) > 48 * 1024) CTH_ATTR((k_tail<cd>), (int)line_smem<cd>(g->bd, 1));
     if (line_smem<double>(g->bd, 1) > 48 * 1024) CTH_ATTR((k_tail<double>), (int)line_smem<double>(g->bd, 1));
     if (line_smem<float>(g->bd, 1) > 48 * 1024) CTH_ATTR((k_tail<float>), (int)line_smem<float>(g->bd, 1));
+    // the defect correction's shared copy of the caller's operator (plus its static reduction words)
+    CTH_ATTR((k_update<float>), (int)kUpdSmem);
+    CTH_ATTR((k_update<double>), (int)kUpdSmem);
 #undef CTH_ATTR
     return CTH_OK;
 }
