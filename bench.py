@@ -555,6 +555,50 @@ def learned_microwave(pkg, device, runs, ni=512, nj=256, nsteps=120, ndiv=10, ep
     return 0
 
 
+def cycle_cost(pkg, local):
+    """Where one multigrid cycle's time goes, on the 512 x 1024 slab potential system:
+    the solve's time per cycle ((T(16) - T(8)) / 8 cycles with an unreachable
+    tolerance), the same cycles captured one after another in one graph without the
+    solve's loop node (Grid.time_cycle, with and without the FP64 update) and each
+    level's relaxation back to back (Grid.time_relax), both precisions."""
+    import numpy as np
+    import torch
+    capi = pkg.capi
+    s = pkg.workloads.poisson_slab(ni=NI, nj=NJ, seed=1)
+    g = pkg.Grid(NI, NJ, s["i_bl"], s["j_bl"], device=local)
+    planes = [g.to_device(s[k]) for k in ("aP", "aE", "aW", "aN", "aS", "b")]
+    sol = g.to_device(np.zeros((NI + 2, NJ + 2)))
+
+    def solve_ms(n, prec, reps=5):
+        best = 1e9
+        for _ in range(reps):
+            sol.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            g.smg_solve_dev(*planes, sol, maxITR=n, error_cnv=1e-300, precision=prec)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    out = {"workload": f"potential with a dielectric slab, {NJ} (r) x {NI} (z), V(1,1) cycles", "unit": "us"}
+    for name, prec in (("mixed", capi.CTH_PREC_MIXED), ("fp64", capi.CTH_PREC_FP64)):
+        t1, t8, t16 = solve_ms(1, prec), solve_ms(8, prec), solve_ms(16, prec)
+        per = (t16 - t8) / 8 * 1e3
+        levels = []
+        for lev in range(g.levels):
+            levels.append(round(g.time_relax(prec, lev, 50)[0], 2))
+        out[name] = {"solve_per_cycle": round(per, 1), "solve_fixed": round(t1 * 1e3 - per, 1),
+                     "graph_cycle_with_update": round(min(g.time_cycle(prec, 20, True) for _ in range(3)), 1),
+                     "graph_vcycle_alone": round(min(g.time_cycle(prec, 20, False) for _ in range(3)), 1),
+                     "relax_per_launch_by_level": levels}
+    g.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -583,6 +627,10 @@ def main():
                          "256 (r) x 512 (z) (microwave update every 10 steps) and report iterations to 1e-8 from "
                          "zero, the previous fields and the network's guess on held-out discharges; prints one JSON "
                          "line and exits")
+    ap.add_argument("--cycle-cost", action="store_true",
+                    help="per-cycle cost of the 512 x 1024 slab potential solve: solve time per cycle, the "
+                         "same cycles as a straight-line graph with and without the FP64 update, and each "
+                         "level's relaxation (one JSON line; not a bench value)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every multigrid kernel individually (profilers cannot see kernels inside "
                          "conditional graphs); same kernels, host convergence checks")
@@ -626,6 +674,8 @@ def main():
         m3.close()
         gm.close()
         return 0
+    if args.cycle_cost:
+        return cycle_cost(pkg, local)
     if args.production > 0:
         return production(pkg, local, args.production, args.warmup)
     if args.learned_microwave > 0:
