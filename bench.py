@@ -938,6 +938,11 @@ def main():
     # the finest relaxation in its operating mode: even / odd pairs back to back in a
     # graph with programmatic dependent launch, on the operator of the last solve
     relax_us, relax_bytes = g.time_relax(capi.CTH_PREC_MIXED, 0, 50)
+    # every level's relaxation the same way (back to back in a graph, on the cell grid's last operator)
+    per_level = []
+    for lev in range(g.levels):
+        us_l, by_l = g.time_relax(capi.CTH_PREC_MIXED, lev, 50)
+        per_level.append((lev, us_l, by_l))
     parts = {}
     sub = [("ions", lambda: fs.ion_step(gx, gr, P["ion"], stream=stream)),
            ("potential_pc", lambda: fs.solve_phi_pc(P["phi"], stream=stream)),
@@ -1119,6 +1124,15 @@ def main():
                               "method": "algorithmic bytes of every multigrid kernel class of one step (relaxations, "
                                         "restriction, FP64 update, set-up excluded) / the timed step time; the "
                                         "fluid sweeps' bytes are not counted"},
+                     "per_level": {
+                         "levels": [{"level": lev, "launch_us": round(us_l, 3), "algorithmic_bytes": by_l,
+                                     "achieved_gbs": round(by_l / (us_l * 1e-6) / 1e9, 1),
+                                     "frac": round(by_l / (us_l * 1e-6) / 1e9 / peak, 4)} for lev, us_l, by_l in per_level],
+                         "method": "each level's relaxation (one colour), 50 even-odd pairs back to back in one graph "
+                                   "with programmatic dependent launch on the cell grid's last mixed operator; "
+                                   "algorithmic bytes = rows of the colour x cells x 8 words; the levels are "
+                                   "L2-resident, so the coarse ones show the launch floor (~1.5-2 us), not a "
+                                   "bandwidth"},
                      "l2_resident_pairs": {"launch_us": relax_us, "achieved": achieved_pairs,
                                            "frac": achieved_pairs / peak,
                                            "method": "the finest relaxation, 50 even-odd pairs back to back in one "
