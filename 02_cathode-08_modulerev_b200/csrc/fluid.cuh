@@ -93,7 +93,8 @@ enum { F_BLX = 1, F_BRX = 2, F_BLR_WALL = 4, F_BLR_CEN = 8, F_BRR_WALL = 16, F_B
 // flag of cell (i, j); 0 outside the (ni+2) x (nj+2) index space
 __device__ __forceinline__ unsigned flag_at(const unsigned char* __restrict__ f, int i, int j, int ni, int nj,
                                             int ld) {
-    return (i >= 0 && i <= ni + 1 && j >= 0 && j <= nj + 1) ? f[(size_t)j * ld + i] : 0u;
+    // the flag plane is never written by a kernel: read-only loads, free to move
+    return (i >= 0 && i <= ni + 1 && j >= 0 && j <= nj + 1) ? __ldg(f + (size_t)j * ld + i) : 0u;
 }
 
 constexpr double kBoltz = 1.380649e-23;    // constants.hpp:5

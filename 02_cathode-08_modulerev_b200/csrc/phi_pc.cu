@@ -265,28 +265,30 @@ __global__ void k_phi_correct_b(PhiArgs A, double* __restrict__ part, unsigned i
         const size_t p = (size_t)j * ld + i;
         const double dx = A.prm.dx, dr = A.prm.dr;
         const unsigned fc = FL(i, j), fw = FL(i - 1, j), fs = FL(i, j - 1);
+        // everything but Ex, Er, nUex, nUer is read only here: read-only loads, which the
+        // compiler may issue ahead of this kernel's stores
         if (fc && fw) {
-            A.Ex[p] = -(A.phi[p] - A.phi[p - 1]) / dx;
-            const double mst = (A.mu_perp[p] + A.mu_perp[p - 1]) / 2.0 * 1.0;
-            const double rho_t = (A.rhoe[p] + A.rhoe[p - 1]) / 2.0;
-            const double v = A.nUex[p] + mst * rho_t * ((A.dphi[p] - A.dphi[p - 1]) / dx);
+            A.Ex[p] = -(__ldg(A.phi + p) - __ldg(A.phi + p - 1)) / dx;
+            const double mst = (__ldg(A.mu_perp + p) + __ldg(A.mu_perp + p - 1)) / 2.0 * 1.0;
+            const double rho_t = (__ldg(A.rhoe + p) + __ldg(A.rhoe + p - 1)) / 2.0;
+            const double v = A.nUex[p] + mst * rho_t * ((__ldg(A.dphi + p) - __ldg(A.dphi + p - 1)) / dx);
             A.nUex[p] = v;
-            res_acc(mode, v, A.nUex_t[p], s[2], s[3]);
-            res_acc(mode, v, A.nUex_old[p], s[8], s[9]);
+            res_acc(mode, v, __ldg(A.nUex_t + p), s[2], s[3]);
+            res_acc(mode, v, __ldg(A.nUex_old + p), s[8], s[9]);
         }
         if (fc && fs) {
-            A.Er[p] = -(A.phi[p] - A.phi[p - ld]) / dr;
-            const double mst = (A.mu_perp[p] + A.mu_perp[p - ld]) / 2.0 * 1.0;
-            const double rho_t = (A.rhoe[p] + A.rhoe[p - ld]) / 2.0;
-            const double v = A.nUer[p] + mst * rho_t * ((A.dphi[p] - A.dphi[p - ld]) / dr);
+            A.Er[p] = -(__ldg(A.phi + p) - __ldg(A.phi + p - ld)) / dr;
+            const double mst = (__ldg(A.mu_perp + p) + __ldg(A.mu_perp + p - ld)) / 2.0 * 1.0;
+            const double rho_t = (__ldg(A.rhoe + p) + __ldg(A.rhoe + p - ld)) / 2.0;
+            const double v = A.nUer[p] + mst * rho_t * ((__ldg(A.dphi + p) - __ldg(A.dphi + p - ld)) / dr);
             A.nUer[p] = v;
-            res_acc(mode, v, A.nUer_t[p], s[4], s[5]);
-            res_acc(mode, v, A.nUer_old[p], s[10], s[11]);
+            res_acc(mode, v, __ldg(A.nUer_t + p), s[4], s[5]);
+            res_acc(mode, v, __ldg(A.nUer_old + p), s[10], s[11]);
         }
         if (fc) {
-            const double v = A.phi[p];
-            res_acc(mode, v, A.phi_t[p], s[0], s[1]);
-            res_acc(mode, v, A.phi_old[p], s[6], s[7]);
+            const double v = __ldg(A.phi + p);
+            res_acc(mode, v, __ldg(A.phi_t + p), s[0], s[1]);
+            res_acc(mode, v, __ldg(A.phi_old + p), s[6], s[7]);
         }
     }
     grid_reduce<kNStat>(s, (mode == 0 || mode == 2) ? 0xfffu : 0u, part, counter, out);

@@ -80,9 +80,13 @@ struct SgFace {
 __device__ __forceinline__ SgFace sg_face(const SgArgs& A, size_t c0, size_t c1, double E, double h) {
     const double* T = A.Te_old;
     SgFace f;
-    f.mst = (A.mu_perp[c1] + A.mu_perp[c0]) / 2.0 * 1.0;
-    const double Tt = (T[c1] + T[c0]) / 2.0;
-    const double dT = (T[c1] - T[c0]) / h;
+    // mobility and old temperature are inputs of every kernel that calls this:
+    // read-only loads, which the compiler may issue ahead of the kernel's stores
+    const double m1 = __ldg(A.mu_perp + c1), m0 = __ldg(A.mu_perp + c0);
+    const double T1 = __ldg(T + c1), T0 = __ldg(T + c0);
+    f.mst = (m1 + m0) / 2.0 * 1.0;
+    const double Tt = (T1 + T0) / 2.0;
+    const double dT = (T1 - T0) / h;
     f.vd = f.mst * (-E - kBoltz / kE0f * dT) + kEpsVd;
     const double D = kBoltz * Tt / kE0f * f.mst;
     const double z = f.vd * h / D;
@@ -129,73 +133,76 @@ __device__ __forceinline__ void sg_predict_cell(const SgArgs& A, int i, int j) {
     const double rj = P.rmin + (j - 0.5) * dr;
     const unsigned fc = FL(i, j), fw = FL(i - 1, j), fs = FL(i, j - 1);
     const double fac = EN ? 5.0 : 1.0;
+    // the fluxes of the last corrector, mobilities, fields, density and ion / neutral
+    // fluxes are read only here (the kernel writes Fx, Fr and the wall fluxes):
+    // read-only loads, free to move ahead of the stores
 
     // x face i-1/2
-    double vx = A.Fx_t[p];
+    double vx = __ldg(A.Fx_t + p);
     if (fc && fw) {
         const double rjm = P.rmin + (j - 1.5) * dr, rjp = P.rmin + (j + 0.5) * dr;
         const double rL = (rj + rjm) / 2.0, rR = (rj + rjp) / 2.0;
-        const double mpa = (A.mu_para[p] + A.mu_para[p - 1]) / 2.0;
-        const double mpe = (A.mu_perp[p] + A.mu_perp[p - 1]) / 2.0;
-        const double mrr = (A.mu_rr[p] + A.mu_rr[p - 1]) / 2.0;
-        const double mxr = (A.mu_xr[p] + A.mu_xr[p - 1]) / 2.0;
+        const double mpa = (__ldg(A.mu_para + p) + __ldg(A.mu_para + p - 1)) / 2.0;
+        const double mpe = (__ldg(A.mu_perp + p) + __ldg(A.mu_perp + p - 1)) / 2.0;
+        const double mrr = (__ldg(A.mu_rr + p) + __ldg(A.mu_rr + p - 1)) / 2.0;
+        const double mxr = (__ldg(A.mu_xr + p) + __ldg(A.mu_xr + p - 1)) / 2.0;
         const double ixx = mrr / (mpa * mpe);
         const double ixr = -mxr / (mpa * mpe);
-        const SgFace f = sg_face(A, p - 1, p, A.Ex[p], dx);
+        const SgFace f = sg_face(A, p - 1, p, __ldg(A.Ex + p), dx);
         const double bLr = ((fc & F_BLR_WALL) && (fc & F_BLR_CEN)) ? 1.0 : 0.0;
         const double bLrD = ((fw & F_BLR_WALL) && (fw & F_BLR_CEN)) ? 1.0 : 0.0;
         const double bRr = (fc & F_BRR_WALL) ? 1.0 : 0.0;
         const double bRrD = (fw & F_BRR_WALL) ? 1.0 : 0.0;
-        const double Fr_i = (rR * A.Fr_t[p + ld] * bRr + rL * A.Fr_t[p] * bLr + rR * A.Fr_t[p - 1 + ld] * bRrD +
-                             rL * A.Fr_t[p - 1] * bLrD) /
+        const double Fr_i = (rR * __ldg(A.Fr_t + p + ld) * bRr + rL * __ldg(A.Fr_t + p) * bLr + rR * __ldg(A.Fr_t + p - 1 + ld) * bRrD +
+                             rL * __ldg(A.Fr_t + p - 1) * bLrD) /
                             (4.0 * rj);
-        const double sg = EN ? (f.A() * A.n[p - 1] - f.B() * A.n[p]) * fac / 3.0 : f.A() * A.n[p - 1] - f.B() * A.n[p];
-        vx = sg + A.Fx_t[p] - f.mst * (ixx * A.Fx_t[p] + ixr * Fr_i);
+        const double sg = EN ? (f.A() * __ldg(A.n + p - 1) - f.B() * __ldg(A.n + p)) * fac / 3.0 : f.A() * __ldg(A.n + p - 1) - f.B() * __ldg(A.n + p);
+        vx = sg + __ldg(A.Fx_t + p) - f.mst * (ixx * __ldg(A.Fx_t + p) + ixr * Fr_i);
     }
     if (fc && !(fc & F_BLX)) {
-        vx = sg_wall<EN>(A, p, A.Ex[p], A.Uix[p], A.rhoUmx[p], dx, -1.0);
+        vx = sg_wall<EN>(A, p, __ldg(A.Ex + p), __ldg(A.Uix + p), __ldg(A.rhoUmx + p), dx, -1.0);
         A.Fx_w[p] = vx;
     }
     if (fw && !(fw & F_BRX)) {
-        vx = sg_wall<EN>(A, p - 1, A.Ex[p], A.Uix[p], A.rhoUmx[p], dx, 1.0);
+        vx = sg_wall<EN>(A, p - 1, __ldg(A.Ex + p), __ldg(A.Uix + p), __ldg(A.rhoUmx + p), dx, 1.0);
         A.Fx_w[p] = vx;
     }
     A.Fx[p] = vx;
 
     // r face j-1/2
-    double vr = A.Fr_t[p];
+    double vr = __ldg(A.Fr_t + p);
     if (fc && fs) {
         const double rjm = P.rmin + (j - 1.5) * dr;
         const double r_t = (rj + rjm) / 2.0;
-        const double mpa = (A.mu_para[p] + A.mu_para[p - ld]) / 2.0;
-        const double mpe = (A.mu_perp[p] + A.mu_perp[p - ld]) / 2.0;
-        const double mxx = (A.mu_xx[p] + A.mu_xx[p - ld]) / 2.0;
-        const double mxr = (A.mu_xr[p] + A.mu_xr[p - ld]) / 2.0;
+        const double mpa = (__ldg(A.mu_para + p) + __ldg(A.mu_para + p - ld)) / 2.0;
+        const double mpe = (__ldg(A.mu_perp + p) + __ldg(A.mu_perp + p - ld)) / 2.0;
+        const double mxx = (__ldg(A.mu_xx + p) + __ldg(A.mu_xx + p - ld)) / 2.0;
+        const double mxr = (__ldg(A.mu_xr + p) + __ldg(A.mu_xr + p - ld)) / 2.0;
         const double irr = mxx / (mpa * mpe);
         const double ixr = -mxr / (mpa * mpe);
-        const SgFace f = sg_face(A, p - ld, p, A.Er[p], dr);
+        const SgFace f = sg_face(A, p - ld, p, __ldg(A.Er + p), dr);
         const double bLx = (fc & F_BLX) ? 1.0 : 0.0, bLxD = (fs & F_BLX) ? 1.0 : 0.0;
         const double bRx = (fc & F_BRX) ? 1.0 : 0.0, bRxD = (fs & F_BRX) ? 1.0 : 0.0;
-        const double Fx_i = (rj * A.Fx_t[p + 1] * bRx + rj * A.Fx_t[p] * bLx + rjm * A.Fx_t[p + 1 - ld] * bRxD +
-                             rjm * A.Fx_t[p - ld] * bLxD) /
+        const double Fx_i = (rj * __ldg(A.Fx_t + p + 1) * bRx + rj * __ldg(A.Fx_t + p) * bLx + rjm * __ldg(A.Fx_t + p + 1 - ld) * bRxD +
+                             rjm * __ldg(A.Fx_t + p - ld) * bLxD) /
                             (4.0 * r_t);
-        const double sg = EN ? (f.A() * A.n[p - ld] - f.B() * A.n[p]) * fac / 3.0 : f.A() * A.n[p - ld] - f.B() * A.n[p];
-        vr = sg + A.Fr_t[p] - f.mst * (ixr * Fx_i + irr * A.Fr_t[p]);
+        const double sg = EN ? (f.A() * __ldg(A.n + p - ld) - f.B() * __ldg(A.n + p)) * fac / 3.0 : f.A() * __ldg(A.n + p - ld) - f.B() * __ldg(A.n + p);
+        vr = sg + __ldg(A.Fr_t + p) - f.mst * (ixr * Fx_i + irr * __ldg(A.Fr_t + p));
     }
     bool rec = true;  // energy sweep: the lower wall x2 sets Gr but not Gr_wall (fluidModule.hpp:4428-4449)
     if (EN)
         for (int q = 0; q < A.nkw; q++)
             if (i >= A.kw[4 * q] && i <= A.kw[4 * q + 1] && j >= A.kw[4 * q + 2] && j <= A.kw[4 * q + 3]) rec = false;
     if (fc && !(fc & F_BLR_WALL)) {
-        vr = sg_wall<EN>(A, p, A.Er[p], A.Uir[p], A.rhoUmr[p], dr, -1.0);
+        vr = sg_wall<EN>(A, p, __ldg(A.Er + p), __ldg(A.Uir + p), __ldg(A.rhoUmr + p), dr, -1.0);
         if (rec) A.Fr_w[p] = vr;
     }
     if (fs && !(fs & F_BRR_WALL)) {
-        vr = sg_wall<EN>(A, p - ld, A.Er[p], A.Uir[p], A.rhoUmr[p], dr, 1.0);
+        vr = sg_wall<EN>(A, p - ld, __ldg(A.Er + p), __ldg(A.Uir + p), __ldg(A.rhoUmr + p), dr, 1.0);
         if (rec) A.Fr_w[p] = vr;
     }
     if (fs && !(fs & F_BRR_OPEN)) {
-        vr = EN ? 5.0 / 2.0 * kBoltz * A.Te_old[p - ld] * fmax(A.rhoUer[p], 0.0) : A.rhoi[p - ld] * A.Uir[p];
+        vr = EN ? 5.0 / 2.0 * kBoltz * A.Te_old[p - ld] * fmax(A.rhoUer[p], 0.0) : A.rhoi[p - ld] * __ldg(A.Uir + p);
         A.Fr_w[p] = 0.0;
     }
     A.Fr[p] = vr;
@@ -218,6 +225,8 @@ __device__ __forceinline__ void sg_assemble_cell(const SgArgs& A, int i, int j) 
     const int ld = A.ld;
     const size_t p = (size_t)j * ld + i;
     const unsigned fc = FL(i, j);
+    // inputs through read-only loads (the kernel writes only the coefficient planes), so
+    // the compiler may issue the next cell's loads ahead of this cell's stores
     double vP = 0.0, vE = 0.0, vW = 0.0, vN = 0.0, vS = 0.0, vb = 0.0;
     if (fc) {
         const cth_sg_params& P = A.prm;
@@ -227,10 +236,10 @@ __device__ __forceinline__ void sg_assemble_cell(const SgArgs& A, int i, int j) 
         const double rR = (rj + rjp) / 2.0, rL = (rj + rjm) / 2.0;
         const double qR = (rj + rjp) / 2.0 / rj;
         const double qL = (rj + rjm) / 2.0 / rj;
-        const SgFace Lx = sg_face(A, p - 1, p, A.Ex[p], dx);
-        const SgFace Rx = sg_face(A, p, p + 1, A.Ex[p + 1], dx);
-        const SgFace Lr = sg_face(A, p - ld, p, A.Er[p], dr);
-        const SgFace Rr = sg_face(A, p, p + ld, A.Er[p + ld], dr);
+        const SgFace Lx = sg_face(A, p - 1, p, __ldg(A.Ex + p), dx);
+        const SgFace Rx = sg_face(A, p, p + 1, __ldg(A.Ex + p + 1), dx);
+        const SgFace Lr = sg_face(A, p - ld, p, __ldg(A.Er + p), dr);
+        const SgFace Rr = sg_face(A, p, p + ld, __ldg(A.Er + p + ld), dr);
         const double bLx = (fc & F_BLX) ? 1.0 : 0.0, bRx = (fc & F_BRX) ? 1.0 : 0.0;
         const double bLr = ((fc & F_BLR_WALL) && (fc & F_BLR_CEN)) ? 1.0 : 0.0;
         const double bRr = ((fc & F_BRR_WALL) && (fc & F_BRR_OPEN)) ? 1.0 : 0.0;
@@ -241,18 +250,18 @@ __device__ __forceinline__ void sg_assemble_cell(const SgArgs& A, int i, int j) 
         vW = Lx.vd / Lx.da * bLx * dr;
         vN = qR * Rr.vd / Rr.db * bRr * dx;
         vS = qL * Lr.vd / Lr.da * bLr * dx;
-        const double div = (A.Fx[p + 1] - A.Fx[p]) / dx + (qR * A.Fr[p + ld] - qL * A.Fr[p]) / dr;
+        const double div = (__ldg(A.Fx + p + 1) - __ldg(A.Fx + p)) / dx + (qR * __ldg(A.Fr + p + ld) - qL * __ldg(A.Fr + p)) / dr;
         if (EN) {
             const double bRxw = bRx, bLxw = bLx;
             const double bLrw = (fc & F_BLR_WALL) ? 1.0 : 0.0, bRrw = (fc & F_BRR_WALL) ? 1.0 : 0.0;
-            const double jx = -kE0f * (A.rhoUex[p + 1] * A.Ex[p + 1] * bRxw + A.rhoUex[p] * A.Ex[p] * bLxw) / 2.0;
-            const double jr = -kE0f * (rR * A.rhoUer[p + ld] * A.Er[p + ld] * bRrw + rL * A.rhoUer[p] * A.Er[p] * bLrw) /
+            const double jx = -kE0f * (__ldg(A.rhoUex + p + 1) * __ldg(A.Ex + p + 1) * bRxw + __ldg(A.rhoUex + p) * __ldg(A.Ex + p) * bLxw) / 2.0;
+            const double jr = -kE0f * (rR * __ldg(A.rhoUer + p + ld) * __ldg(A.Er + p + ld) * bRrw + rL * __ldg(A.rhoUer + p) * __ldg(A.Er + p) * bLrw) /
                               (2.0 * rj);
-            const double R1 = (-A.n[p] + A.n_old[p]) / dt;
-            const double R3 = A.Pabs[p] - A.rhoe[p] * A.rate_eloss[p];
+            const double R1 = (-__ldg(A.n + p) + __ldg(A.n_old + p)) / dt;
+            const double R3 = __ldg(A.Pabs + p) - __ldg(A.rhoe + p) * __ldg(A.rate_eloss + p);
             vb = 3.0 / 5.0 * (R1 + (jx + jr) + R3 + (-div)) * dx * dr;
         } else {
-            vb = (-div + A.rate_ionize[p] - (A.n[p] - A.n_old[p]) / dt) * dx * dr;
+            vb = (-div + __ldg(A.rate_ionize + p) - (__ldg(A.n + p) - __ldg(A.n_old + p)) / dt) * dx * dr;
         }
     }
     A.aP[p] = vP; A.aE[p] = vE; A.aW[p] = vW; A.aN[p] = vN; A.aS[p] = vS; A.b[p] = vb;
@@ -289,31 +298,35 @@ __global__ void k_sg_correct(SgArgs A, double* __restrict__ part, unsigned int* 
         const size_t p = (size_t)j * ld + i;
         const double dx = A.prm.dx, dr = A.prm.dr;
         const unsigned fc = FL(i, j), fw = FL(i - 1, j), fs = FL(i, j - 1);
+        // d, E and the reference copies are not written here: read-only loads
+        const double dc = __ldg(A.d + p);
         if (fc && fw) {
-            const SgFace f = sg_face(A, p - 1, p, A.Ex[p], dx);
-            const double dF = EN ? (f.A() * A.d[p - 1] - f.B() * A.d[p]) * 5.0 / 3.0 : f.A() * A.d[p - 1] - f.B() * A.d[p];
+            const SgFace f = sg_face(A, p - 1, p, __ldg(A.Ex + p), dx);
+            const double dw = __ldg(A.d + p - 1);
+            const double dF = EN ? (f.A() * dw - f.B() * dc) * 5.0 / 3.0 : f.A() * dw - f.B() * dc;
             const double v = A.Fx[p] + dF;
             A.Fx[p] = v;
-            res_acc(mode, v, A.Fx_t[p], s[2], s[3]);
-            res_acc(mode, v, A.Fx_old[p], s[8], s[9]);
+            res_acc(mode, v, __ldg(A.Fx_t + p), s[2], s[3]);
+            res_acc(mode, v, __ldg(A.Fx_old + p), s[8], s[9]);
         }
         if (fc && fs) {
-            const SgFace f = sg_face(A, p - ld, p, A.Er[p], dr);
-            const double dF = EN ? (f.A() * A.d[p - ld] - f.B() * A.d[p]) * 5.0 / 3.0 : f.A() * A.d[p - ld] - f.B() * A.d[p];
+            const SgFace f = sg_face(A, p - ld, p, __ldg(A.Er + p), dr);
+            const double ds = __ldg(A.d + p - ld);
+            const double dF = EN ? (f.A() * ds - f.B() * dc) * 5.0 / 3.0 : f.A() * ds - f.B() * dc;
             const double v = A.Fr[p] + dF;
             A.Fr[p] = v;
-            res_acc(mode, v, A.Fr_t[p], s[4], s[5]);
-            res_acc(mode, v, A.Fr_old[p], s[10], s[11]);
+            res_acc(mode, v, __ldg(A.Fr_t + p), s[4], s[5]);
+            res_acc(mode, v, __ldg(A.Fr_old + p), s[10], s[11]);
         }
         if (fc) {
             double v = A.n[p];
-            const double nn = v + A.d[p];
+            const double nn = v + dc;
             if (nn > 0.0) {
                 v = nn;
                 A.n[p] = v;
             }
-            res_acc(mode, v, A.n_t[p], s[0], s[1]);
-            res_acc(mode, v, A.n_old[p], s[6], s[7]);
+            res_acc(mode, v, __ldg(A.n_t + p), s[0], s[1]);
+            res_acc(mode, v, __ldg(A.n_old + p), s[6], s[7]);
             if (!EN && (fc & F_BRX_BIAS)) {
                 const double rj = A.prm.rmin + (j - 0.5) * dr;
                 s[12] += A.rhoUix_wall[p + 1] * 2.0 * M_PI * rj * dr * (kE0f);
