@@ -53,11 +53,13 @@ def partition(specs, world: int, steps=None):
     return [sorted(x) for x in out]
 
 
-def make_instances(pkg, specs, device=0, precision=1, microwave=False, ndiv_mw=100):
+def make_instances(pkg, specs, device=0, precision=1, microwave=False, ndiv_mw=100, reuse_tol=0.0):
     """Build the instances of ``specs`` on one GPU (grids, field store, parameters).
     microwave=True gives each instance the loop's microwave update every
     ``ndiv_mw`` steps (its own magnetised system, absorbed power rescaled to the
-    instance's Pmw), so that the power axis of the sweep drives the heating."""
+    instance's Pmw), so that the power axis of the sweep drives the heating.
+    reuse_tol > 0 lets each instance's equations keep their multigrid hierarchies
+    (Grid.set_reuse on its three grids)."""
     from .discharge import MicrowaveUpdate, rect_port
     from .solvers import Microwave3
     cases = []
@@ -65,6 +67,8 @@ def make_instances(pkg, specs, device=0, precision=1, microwave=False, ndiv_mw=1
         c = learned.make_case(pkg, sp["ni"], sp["nj"], seed=sp["seed"], V_bias=sp["V_bias"], device=device)
         c.update(ni=sp["ni"], nj=sp["nj"], V_bias=sp["V_bias"], Pmw=sp["Pmw"], index=sp["index"])
         set_precision(c, precision)
+        for k in ("g", "gx", "gr"):
+            c[k].set_reuse(reuse_tol)
         if microwave:
             ni, nj = sp["ni"], sp["nj"]
             c["fs"].upload("epsr_mw", np.ones((ni + 2, nj + 2)))

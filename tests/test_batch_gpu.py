@@ -10,14 +10,21 @@ pytestmark = pytest.mark.gpu
 FIELDS = ("rhoe", "rhoi", "Te", "phi", "rhon", "rhom", "Uix")
 
 
-def test_batched_steps_equal_sequential(pkg, cuda_device):
+@pytest.mark.parametrize("reuse_tol", [0.0, 1e-3])
+def test_batched_steps_equal_sequential(pkg, cuda_device, reuse_tol):
+    """reuse_tol > 0: the instances keep their multigrid hierarchies; the decisions
+    are made on each instance's own device words, so batched = sequential still."""
     B = pkg.batch
     sizes = ((32, 64), (64, 128))
-    a = B.sweep_instances(pkg, n=6, seed=5, sizes=sizes)
-    b = B.sweep_instances(pkg, n=6, seed=5, sizes=sizes)
+    specs = B.instance_specs(6, 5, sizes)
+    a = B.make_instances(pkg, specs, reuse_tol=reuse_tol)
+    b = B.make_instances(pkg, specs, reuse_tol=reuse_tol)
     wall, rc, secs = B.batch_steps(a, steps=3, nthreads=3)
     assert rc == [0] * 6 and wall > 0
     B.sequential_steps(b, steps=3)
+    if reuse_tol:
+        reused = sum(c["g"].reuse_stats(1, slot)["reuses"] for c in a for slot in range(7))
+        assert reused > 0
     for ca, cb in zip(a, b):
         assert ca["P"]["itime"] == cb["P"]["itime"] == 3
         for k in FIELDS:
