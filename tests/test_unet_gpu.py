@@ -57,6 +57,53 @@ def test_forward_and_gradients_match_oracle(pkg, cuda_device, shape):
     net.close()
 
 
+@pytest.mark.parametrize("shape", [(16, 32), (40, 64)])
+def test_open_gates_match_oracle_tightly(pkg, cuda_device, shape):
+    """With positive inputs, weights and biases every ReLU gate stays open, so the
+    bf16 rounding of the activations cannot flip a gate and the network is linear:
+    the device (bf16 operands, FP32 accumulation in tensor memory) and the oracle's
+    bf16 emulation differ only by accumulation order and the bf16 rounding it moves
+    (one unit in the last place, 2^-8 relative, in a few elements).  Measured:
+    output 2.1-2.6e-4 relative L2, gradients 1e-5 ... 2.6e-4 per layer against the
+    oracle's bf16 gradients.  Bars: 1e-3 and 2e-3 (cosine > 0.99999), twenty to a
+    hundred times tighter than the bounds of the gate-flipping case above."""
+    import torch
+    from oracle import unet
+    H, W = shape
+    rng = np.random.default_rng(11)
+    parts = []
+    for name, ci, co, _ in unet.layer_shapes():
+        fan = 9 * (6 if name == "e0a" else ci)
+        w = rng.uniform(0.0, 2.0 / fan, size=(co, 3, 3, ci))
+        if name == "e0a":
+            w[..., 6:] = 0.0
+        parts += [w.ravel(), np.full(co, 0.1)]
+    parts += [rng.normal(0.0, 0.2, size=3 * 32), rng.normal(0.0, 0.2, size=3)]
+    vec = np.concatenate(parts).astype(np.float32)
+    x = rng.uniform(0.5, 1.5, size=(H, W, 6)).astype(np.float32)
+    dout = rng.normal(size=(H, W, 3)).astype(np.float32)
+    net = pkg.learned.UNet(H, W, params=vec)
+    out = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    ref, cache = unet.forward(vec, x, bf16=True)
+    assert min(float(a.min()) for k, a in cache["act"].items() if k != "in") > 0.0   # every gate open
+    e_out = _rel(out, ref)
+    net.backward(torch.from_numpy(dout).cuda())
+    torch.cuda.synchronize()
+    g = net.grads()
+    gb = unet.backward(vec, cache, dout)
+    off, rows = 0, []
+    for name, ci, co, _ in unet.layer_shapes():
+        n = co * 9 * ci + co
+        rows.append((name, round(_rel(g[off:off + n], gb[off:off + n]), 5)))
+        off += n
+    cos = float(g @ gb / (np.linalg.norm(g) * np.linalg.norm(gb)))
+    print(shape, "output", e_out, "gradients per layer", rows, "cosine", cos)
+    assert e_out < 1e-3, e_out
+    assert all(e < 2e-3 for _, e in rows), rows
+    assert cos > 0.99999, cos
+    net.close()
+
+
 def test_training_reduces_loss(pkg, cuda_device):
     """Adam on a smooth synthetic target (a blurred, rescaled input channel)."""
     import torch
