@@ -283,7 +283,8 @@ constexpr int kSgStat = 14;  // calcRes pairs (n, Fx, Fr) x (iteration, call) + 
 constexpr int kCorrCells = 4;
 
 template <bool EN>
-__global__ void k_sg_correct(SgArgs A, double* __restrict__ part, unsigned int* counter, double* __restrict__ out) {
+__global__ void __launch_bounds__(256, 3) k_sg_correct(SgArgs A, double* __restrict__ part, unsigned int* counter,
+                                                       double* __restrict__ out) {
     const int i0 = kCorrCells * (blockIdx.x * blockDim.x + threadIdx.x);
     const int j = blockIdx.y;
     const int mode = A.prm.flag_error;
