@@ -6,7 +6,8 @@ the caller's operator.  Checked here through the C ABI on the slab system
 against the oracle's exact solve (relative L2 <= 1e-8 after converging to
 ||b - Ax|| / ||b|| < 1e-11), bit for bit against the solve that builds its
 hierarchy when the operator is the same, and through the rebuild rules (new
-slot, change above the tolerance, previous solve not converged)."""
+slot, change above the tolerance, previous solve not converged, and the retry
+inside a solve after a cycle on the kept hierarchy stalled)."""
 import numpy as np
 import pytest
 
